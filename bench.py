@@ -1,0 +1,330 @@
+#!/usr/bin/env python3
+"""Throughput of the batched banded seed extension on B200.
+
+Workload (one step): 1,000,000 right extensions of 151-bp reads (per-read indel rate
+from {0, 0.1%, 1%, 3%}, 1% substitutions, seed 19-51 bp at the read start, h0 = seed
+length, target = suffix length + 100), scoring A=1 B=4 N=-1 O=6 E=1, w=100, zdrop=100,
+end bonus 5 -- seeded synthetic data with the shapes of the reference's workload.
+Results are bit-exact to the oracle (checked on a sample every run).
+
+value   : alignments/s with inputs resident in HBM (device-resident C ABI call,
+          longest-first device ordering inside the timed region).
+e2e     : alignments/s through the host C ABI call fa_ext_batch from pinned host buffers,
+          host->device copies of jobs and sequences and the device->host copy of the
+          results inside the timed region.
+GCUPS   : cells = sum over rows of the adaptive band width (end - beg), the oracle's count.
+
+--impl reference times the CPU oracle (a restatement of the reference's ksw_extend2;
+the Rust reference cannot be built here) on all host cores over a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "GCUPS & alignments/s @151bp, learned-band vs plain-band on B200, bit-exact"
+N_JOBS = 1_000_000
+CPU_SAMPLE = 200_000
+DPX_OPS_PER_CELL_PAIR = 9   # int16x2 ops per packed cell pair in the roofline model
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def make_workload(rank: int, n: int):
+    from ferrousalign_b200 import synth
+    t0 = time.time()
+    b = synth.workload_ext_1m(n, seed=2 + 1000 * rank)
+    log(f"[rank {rank}] generated {n} jobs in {time.time() - t0:.1f}s "
+        f"(query {b.qseq.nbytes / 1e6:.0f} MB, target {b.tseq.nbytes / 1e6:.0f} MB)")
+    return b
+
+
+def cpu_oracle_rate(b, p, sample: int):
+    """Oracle (restated ksw_extend2) on all host threads over the first `sample` jobs."""
+    from oracle import ksw_oracle as O
+    jobs = b.jobs[:sample]
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    out, tr = O.ext_batch(p, jobs, b.qseq, b.tseq, threads=threads)
+    dt = time.perf_counter() - t0
+    return out, tr, dt, threads
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    import ferrousalign_b200 as fa
+    b = make_workload(0, N_JOBS)
+    p = fa.BandedPairWiseSW().to_struct()
+    sample = min(CPU_SAMPLE, N_JOBS)
+    for _ in range(args.warmup):
+        cpu_oracle_rate(b, p, min(sample, 20_000))
+    times, cells = [], 0
+    for _ in range(args.steps):
+        _, tr, dt, threads = cpu_oracle_rate(b, p, sample)
+        times.append(dt)
+        cells = int(tr["cells"].sum())
+    dt = sum(times) / len(times)
+    aln = sample / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": aln, "unit": "alignments/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": "1M right extensions, 151 bp reads (sample of the batch per step)",
+                   "sample_jobs": sample, "w": 100, "zdrop": 100, "end_bonus": 5},
+        "gcups": cells / dt / 1e9,
+        "cpu_baseline": {"value": aln, "unit": "alignments/s", "cores": threads, "kind": "port",
+                         "sample": f"first {sample} of the 1M jobs, all host threads"},
+        "e2e": {"value": aln, "unit": "alignments/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "gpu_launches": 0,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--jobs", type=int, default=N_JOBS)
+    ap.add_argument("--skip-cpu", action="store_true", help="omit the CPU baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    import ferrousalign_b200 as fa
+    from ferrousalign_b200 import _native as N
+    n = args.jobs
+    b = make_workload(rank, n)
+    sw = fa.BandedPairWiseSW()
+    p = sw.to_struct()
+    ctx = fa.Context(local)
+    lib = N.load()
+
+    # ---- device-resident inputs -------------------------------------------------
+    d_jobs = torch.from_numpy(b.jobs.view(np.uint8)).to(dev)
+    d_q = torch.from_numpy(b.qseq).to(dev)
+    d_t = torch.from_numpy(b.tseq).to(dev)
+    d_out = torch.empty(n * 6, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    # L2 flush buffer (inputs are > L2 already; flushing keeps every step cold)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+
+    def step_device():
+        N.check(lib.fa_ext_batch_device(ctx.handle, N.ptr(p), d_jobs.data_ptr(), n, d_q.data_ptr(), d_t.data_ptr(),
+                                        None, d_out.data_ptr(), stream.cuda_stream))
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        step_device()
+    N.check(lib.fa_ctx_sync(ctx.handle))
+    torch.cuda.synchronize()
+
+    # ---- timed: device-resident ------------------------------------------------
+    times = []
+    launches = 0
+    with ClockSampler(local) as clk:
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step_device()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+            launches += lib.fa_ctx_last_launches(ctx.handle)
+        torch.cuda.synchronize()
+        if ws > 1:
+            torch.distributed.barrier()
+    N.check(lib.fa_ctx_sync(ctx.handle))
+    clocks = clk.summary()
+    ms_step = float(np.mean(times))
+    if ws > 1:
+        t = torch.tensor([ms_step], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_step = float(t.item())
+
+    # correctness on the timed outputs: a sample against the oracle, plus the cell count
+    out = d_out.view(torch.int32).cpu().numpy().view(N.EXT_RESULT_DT).reshape(-1)
+    from oracle import ksw_oracle as O
+    chk = np.arange(0, n, max(1, n // 20000))
+    sub = b.jobs[chk]
+    ref_out, ref_tr = O.ext_batch(p, sub, b.qseq, b.tseq)
+    exact = bool(np.array_equal(out[chk], ref_out))
+
+    # per-batch stats (cells, kernel time) from the host API run, also the e2e timing
+    pin_jobs = torch.from_numpy(b.jobs.view(np.uint8)).pin_memory().numpy().view(N.JOB_DT)
+    pin_q = torch.from_numpy(b.qseq).pin_memory().numpy()
+    pin_t = torch.from_numpy(b.tseq).pin_memory().numpy()
+    out_h = torch.empty(n * 24, dtype=torch.uint8).pin_memory().numpy().view(N.EXT_RESULT_DT)
+    stats = np.zeros(1, N.STATS_DT)
+
+    def step_host(st=None):
+        N.check(lib.fa_ext_batch(ctx.handle, N.ptr(p), N.ptr(pin_jobs), n, N.ptr(pin_q), pin_q.nbytes,
+                                 N.ptr(pin_t), pin_t.nbytes, out_h.ctypes.data, N.ptr(st)))
+
+    step_host(stats)            # cells and kernel time of one batch (untimed)
+    for _ in range(max(1, args.warmup) - 1):
+        step_host()
+    e2e_times = []
+    if ws > 1:
+        torch.distributed.barrier()
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        step_host()
+        e2e_times.append((time.perf_counter() - t0) * 1e3)
+    e2e_ms = float(np.mean(e2e_times))
+    if ws > 1:
+        t = torch.tensor([e2e_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    cells = int(stats[0]["cells"])
+    exact = exact and np.array_equal(out_h[chk], ref_out)
+
+    if rank != 0:
+        if ws > 1:
+            torch.distributed.destroy_process_group()
+        return 0
+
+    # roofline: DPX int16x2 issue rate measured on this GPU
+    import ctypes
+    v = ctypes.c_double()
+    ms = ctypes.c_float()
+    N.check(lib.fa_probe_int_peak(ctx.handle, 0, ctypes.byref(v), ctypes.byref(ms)))
+    peak_ops = v.value
+    N.check(lib.fa_probe_int_peak(ctx.handle, 2, ctypes.byref(v), ctypes.byref(ms)))
+    peak_s32 = v.value
+    peak_gcups = peak_ops * 2 / DPX_OPS_PER_CELL_PAIR / 1e9
+    kernel_ms = float(stats[0]["kernel_ms"])
+    achieved_gcups = cells / (kernel_ms * 1e-3) / 1e9
+    total_aln = n * ws
+    value = total_aln / (ms_step * 1e-3)
+    gcups_step = cells * ws / (ms_step * 1e-3) / 1e9
+    bytes_in = int(b.jobs.nbytes + b.qseq.nbytes + b.tseq.nbytes)
+    bytes_out = n * 24
+    line = {
+        "metric": METRIC, "value": value, "unit": "alignments/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": "1M right extensions, 151 bp reads, indel rate {0,0.1,1,3}%, w=100",
+                   "jobs_per_gpu": n, "w": 100, "zdrop": 100, "end_bonus": 5, "scoring": "A1 B4 N-1 O6 E1",
+                   "l2": "inputs (%d MB) larger than L2; 256 MB flush between steps" % (bytes_in // 10**6),
+                   "parallelism": f"replicas x{ws}"},
+        "gcups": gcups_step,
+        "bit_exact_sample": exact,
+        "roofline": {"bound": "dpx", "achieved": achieved_gcups, "peak": peak_gcups, "unit": "Gcell/s",
+                     "frac": achieved_gcups / peak_gcups, "traffic": None,
+                     "peak_source": f"measured __viaddmax_s16x2_relu rate {peak_ops / 1e12:.2f} Tops/s x2/"
+                                    f"{DPX_OPS_PER_CELL_PAIR}; s32 DPX {peak_s32 / 1e12:.2f} Tops/s",
+                     "hbm": {"achieved_gbs": (bytes_in + bytes_out) / (kernel_ms * 1e-3) / 1e9,
+                             "peak_gbs": 6546.6, "peak_source": "MEASURED_PEAKS.json hbm_gbs"}},
+        "e2e": {"value": total_aln / (e2e_ms * 1e-3), "unit": "alignments/s", "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": bytes_in + n * 4, "d2h_bytes_per_step": bytes_out},
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if not args.skip_cpu:
+        ref2, tr2, dt, threads = cpu_oracle_rate(b, p, min(CPU_SAMPLE, n))
+        line["cpu_baseline"] = {"value": min(CPU_SAMPLE, n) / dt, "unit": "alignments/s", "cores": threads,
+                                "kind": "port", "gcups": float(tr2["cells"].sum()) / dt / 1e9,
+                                "sample": f"first {min(CPU_SAMPLE, n)} jobs of the batch, oracle on all host threads"}
+    print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,15 @@
+"""B200-native batched banded seed extension and mate-rescue Smith-Waterman.
+
+A drop-in for FerrousAlign's batch-extension call (execute_batch_simd_scoring) and
+its mate-rescue ksw_align2 calls, computed by hand-written sm_100a CUDA kernels behind
+the C ABI in include/ferrous_b200.h.
+"""
+from ._native import Context, NativeError, default_context, load  # noqa: F401
+from .batch_extension import (BandedPairWiseSW, BatchedExtensionJob, BatchExtensionResult,  # noqa: F401
+                              ExtensionDirection, ExtensionJobBatch, bwa_fill_scmat,
+                              execute_batch_simd_scoring, extend_batch, make_policy)
+from .mate_rescue import (MATE_RESCUE_SCORING_MATRIX, Kswr, MateRescueJob, MateRescueResult,  # noqa: F401
+                          execute_mate_rescue_batch_with_engine, make_mate_params, mate_sw_batch,
+                          mate_xtra)
+
+__version__ = "0.1.0"

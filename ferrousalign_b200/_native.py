@@ -1,0 +1,153 @@
+"""ctypes binding of libferrous_b200.so (the C ABI in include/ferrous_b200.h).
+
+The library is the only compute path: if it is missing or cannot create a CUDA
+context the calls raise, they never fall back to host code.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libferrous_b200.so"
+
+FA_OK, FA_ERR_ARG, FA_ERR_CAPACITY, FA_ERR_CUDA, FA_ERR_TIMEOUT, FA_ERR_STATE = range(6)
+FA_POLICY_SINGLE, FA_POLICY_BWA, FA_POLICY_LEARNED = 0, 1, 2
+FA_JUDGE_CERT, FA_JUDGE_MAXOFF = 1, 2
+FA_DIR_LEFT, FA_DIR_RIGHT = 0, 1
+KSW_XBYTE, KSW_XSTOP, KSW_XSUBO, KSW_XSTART = 0x10000, 0x20000, 0x40000, 0x80000
+FA_MAX_QLEN, FA_MAX_TLEN = 4096, 65535
+
+PARAMS_DT = np.dtype([("mat", "i1", 25), ("_pad", "i1", 3), ("m", "<i4"), ("o_del", "<i4"),
+                      ("e_del", "<i4"), ("o_ins", "<i4"), ("e_ins", "<i4"), ("zdrop", "<i4"),
+                      ("end_bonus", "<i4"), ("pen_clip5", "<i4"), ("pen_clip3", "<i4")])
+JOB_DT = np.dtype([("q_off", "<u8"), ("t_off", "<u8"), ("qlen", "<i4"), ("tlen", "<i4"),
+                   ("h0", "<i4"), ("w", "<i4"), ("dir", "<i4"), ("_pad", "<i4")])
+EXT_RESULT_DT = np.dtype([("score", "<i4"), ("qle", "<i4"), ("tle", "<i4"), ("gtle", "<i4"),
+                          ("gscore", "<i4"), ("max_off", "<i4")])
+POLICY_DT = np.dtype([("mode", "<i4"), ("max_tries", "<i4"), ("judge", "<i4"), ("w_min", "<i4")])
+STATS_DT = np.dtype([("cells", "<u8"), ("cells_executed", "<u8"), ("jobs", "<u4"), ("retries", "<u4"),
+                     ("misses", "<u4"), ("kernel_launches", "<u4"), ("kernel_ms", "<f4"),
+                     ("total_ms", "<f4")])
+MATE_PARAMS_DT = np.dtype([("mat", "i1", 25), ("_pad", "i1", 3), ("m", "<i4"), ("o_del", "<i4"),
+                           ("e_del", "<i4"), ("o_ins", "<i4"), ("e_ins", "<i4")])
+MATE_JOB_DT = np.dtype([("q_off", "<u8"), ("t_off", "<u8"), ("qlen", "<i4"), ("tlen", "<i4"),
+                        ("xtra", "<u4"), ("_pad", "<i4")])
+KSWR_DT = np.dtype([("score", "<i4"), ("te", "<i4"), ("qe", "<i4"), ("score2", "<i4"),
+                    ("te2", "<i4"), ("tb", "<i4"), ("qb", "<i4")])
+
+assert PARAMS_DT.itemsize == 64 and JOB_DT.itemsize == 40 and EXT_RESULT_DT.itemsize == 24
+assert STATS_DT.itemsize == 40 and MATE_PARAMS_DT.itemsize == 48 and MATE_JOB_DT.itemsize == 32
+assert KSWR_DT.itemsize == 28
+
+# Every symbol the header declares, with its ctypes signature.
+_P = C.c_void_p
+SIGNATURES = {
+    "fa_ctx_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    "fa_ctx_destroy": (None, [_P]),
+    "fa_last_error": (C.c_char_p, []),
+    "fa_version": (C.c_char_p, []),
+    "fa_mate_xtra": (C.c_uint32, [C.c_int32, C.c_int32, C.c_int32]),
+    "fa_device_info": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "fa_probe_int_peak": (C.c_int, [_P, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_float)]),
+    "fa_ext_batch": (C.c_int, [_P, _P, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64, _P, _P]),
+    "fa_ext_batch_policy": (C.c_int, [_P, _P, _P, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64,
+                                      _P, _P, _P, _P]),
+    "fa_ext_batch_device": (C.c_int, [_P, _P, _P, C.c_uint32, _P, _P, _P, _P, _P]),
+    "fa_ctx_sync": (C.c_int, [_P]),
+    "fa_ctx_last_launches": (C.c_int, [_P]),
+    "fa_mate_sw_batch": (C.c_int, [_P, _P, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64, _P, _P]),
+}
+
+
+class NativeError(RuntimeError):
+    """A non-zero status from the C ABI."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load(path: Path | None = None) -> C.CDLL:
+    """Loads the shared library (raising if it has not been built)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            p = Path(path) if path else LIB_PATH
+            if not p.exists():
+                raise RuntimeError(f"{p} is missing: run ferrousalign_b200.build.build_all() first")
+            lib = C.CDLL(str(p))
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = lib
+        return _lib
+
+
+def check(rc: int) -> None:
+    if rc != FA_OK:
+        msg = load().fa_last_error()
+        raise NativeError(rc, msg.decode() if msg else "")
+
+
+def ptr(a: np.ndarray | None) -> int | None:
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"], "arrays passed to the C ABI must be contiguous"
+    return a.ctypes.data
+
+
+class Context:
+    """One CUDA context handle of the library (one per host thread)."""
+
+    def __init__(self, device: int = 0):
+        lib = load()
+        h = C.c_void_p()
+        check(lib.fa_ctx_create(device, C.byref(h)))
+        self._h = h
+        self.device = device
+
+    @property
+    def handle(self) -> C.c_void_p:
+        if self._h is None:
+            raise RuntimeError("context closed")
+        return self._h
+
+    def close(self) -> None:
+        if self._h is not None:
+            load().fa_ctx_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default: dict[int, Context] = {}
+_tls = threading.local()
+
+
+def default_context(device: int = 0) -> Context:
+    """A lazily created context per (thread, device)."""
+    d = getattr(_tls, "ctx", None)
+    if d is None:
+        d = _tls.ctx = {}
+    if device not in d:
+        d[device] = Context(device)
+    return d[device]

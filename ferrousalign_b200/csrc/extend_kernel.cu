@@ -1,0 +1,200 @@
+// extend_kernel.cu -- banded seed extension (ksw_extend2 semantics) on sm_100a.
+//
+// One thread owns one extension job (inter-sequence parallelism, as the reference's
+// SIMD lanes do) and runs the exact row recurrence of ksw_extend2
+// (src/core/alignment/ksw_affine_gap.rs:952-1169), including its adaptive beg/end
+// rescans, stale band-edge cells, first-column max rule, z-drop with diagonal
+// correction and the earliest-row gscore rule.  Jobs are processed in
+// length-sorted order so the 32 jobs of a warp have similar row counts.
+//
+// Per-thread column state lives in shared memory, one 32-bit word per query
+// column, interleaved with stride blockDim.x so every access is bank-conflict
+// free whatever column each lane is on:
+//     word = H(16 bits) << 16 | E(13 bits) << 3 | query code (3 bits)
+// The packed form is exact while h0 + max(mat) * qlen < 8192, which bounds every
+// H and E the recurrence can produce; the host routes other jobs elsewhere.
+// Cell updates use the Blackwell DPX integer instructions (3-way max, fused
+// add-max with ReLU).
+
+#include "fa_device.cuh"
+#include "fa_kernels.h"
+
+namespace fa {
+
+// PRMT in the generic mode: selector nibble bit 3 replicates the sign of the
+// selected byte, so (q, q|8, q|8, q|8) sign-extends table byte q to 32 bits.
+__device__ __forceinline__ int32_t prmt_s8(uint32_t lo, uint32_t hi, uint32_t sel) {
+    uint32_t r;
+    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(lo), "r"(hi), "r"(sel));
+    return static_cast<int32_t>(r);
+}
+
+__global__ void __launch_bounds__(kExtThreads)
+ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ order,
+                  uint32_t n, const uint32_t *__restrict__ n_dev, const uint8_t *__restrict__ qseq,
+                  const uint8_t *__restrict__ tseq, const ExtParams p, int qcap,
+                  const int32_t *__restrict__ w_try, fa_ext_result *__restrict__ out,
+                  uint8_t *__restrict__ clamped_out, uint32_t *__restrict__ cells_job,
+                  unsigned long long *__restrict__ cells_out, uint32_t *__restrict__ status)
+{
+    extern __shared__ uint32_t smem[];
+    constexpr int T = kExtThreads;
+    const uint32_t gi = blockIdx.x * T + threadIdx.x;
+    uint32_t cells = 0;
+    if (n_dev) n = min(n, *n_dev);   // device-side job count (retry rounds)
+
+    if (gi < n) {
+        const uint32_t jid = order ? order[gi] : gi;
+        const fa_job jb = jobs[jid];
+        uint32_t *col = smem + threadIdx.x;
+        const int qlen = jb.qlen, tlen = jb.tlen, h0 = jb.h0;
+        if (h0 <= 0 || qlen <= 0 || tlen < 0) {
+            atomicOr(status, ST_ARG);
+        } else if (qlen > qcap || h0 + p.max_score * qlen > kPackedHMax) {
+            atomicOr(status, ST_CAPACITY);
+        } else {
+            const int w = ext_band_clamp(qlen, w_try ? w_try[jid] : jb.w, p);
+            const int oe_del = p.o_del + p.e_del, oe_ins = p.o_ins + p.e_ins;
+            const int e_del = p.e_del, e_ins = p.e_ins;
+            const uint8_t *Q = qseq + jb.q_off;
+            const uint8_t *Tg = tseq + jb.t_off;
+            // scoring rows as PRMT tables, indexed only with constants
+            uint32_t rlo[5], rhi[5];
+#pragma unroll
+            for (int t = 0; t < 5; ++t) {
+                rlo[t] = (uint8_t)p.mat[t * 5] | (uint32_t)(uint8_t)p.mat[t * 5 + 1] << 8 |
+                         (uint32_t)(uint8_t)p.mat[t * 5 + 2] << 16 | (uint32_t)(uint8_t)p.mat[t * 5 + 3] << 24;
+                rhi[t] = (uint8_t)p.mat[t * 5 + 4];
+            }
+
+            // Query codes and the first row: eh[0]=h0, eh[1]=h0-oe_ins, then -e_ins
+            // while the previous value exceeds e_ins (ksw_affine_gap.rs:1017-1025).
+            uint32_t bad = 0;
+            int hp = h0;
+            bool filling = true;
+            for (int j = 0; j <= qlen; ++j) {
+                uint32_t q = 0;
+                if (j < qlen) {
+                    q = Q[j];
+                    bad |= q >= (uint32_t)p.m;
+                    q &= 7u;
+                }
+                int h;
+                if (j == 0) h = h0;
+                else if (j == 1) h = h0 > oe_ins ? h0 - oe_ins : 0;
+                else if (filling && hp > e_ins) h = hp - e_ins;
+                else { filling = false; h = 0; }
+                hp = h;
+                col[j * T] = (uint32_t)h << 16 | q;
+            }
+
+            int best = h0, max_i = -1, max_j = -1, max_ie = -1, gscore = -1, max_off = 0;
+            int beg = 0, end = qlen, clamped = 0;
+            for (int i = 0; i < tlen; ++i) {
+                const uint32_t tb = Tg[i];
+                if (tb >= (uint32_t)p.m) { bad = 1; break; }
+                uint32_t row_lo = rlo[0], row_hi = rhi[0];
+#pragma unroll
+                for (int t = 1; t < 5; ++t)
+                    if (tb == (uint32_t)t) { row_lo = rlo[t]; row_hi = rhi[t]; }
+
+                const int beg_a = beg, end_a = end < qlen ? end : qlen;
+                if (beg < i - w) beg = i - w;
+                if (end > i + w + 1) end = i + w + 1;
+                if (end > qlen) end = qlen;
+                clamped |= (beg != beg_a) | (end != end_a);
+
+                int h1 = 0;
+                if (beg == 0) {
+                    h1 = h0 - (p.o_del + e_del * (i + 1));
+                    if (h1 < 0) h1 = 0;
+                }
+                int f = 0, key = 0;
+#pragma unroll 4
+                for (int j = beg; j < end; ++j) {
+                    const uint32_t wd = col[j * T];
+                    const int M = (int)(wd >> 16);
+                    const int e = (int)((wd >> 3) & 0x1FFFu);
+                    const uint32_t q = wd & 7u;
+                    const int s = prmt_s8(row_lo, row_hi, q * 0x1111u + 0x8880u);
+                    const int Mp = M ? M + s : 0;
+                    const int h = __vimax3_s32(Mp, e, f);
+                    const int e_new = __viaddmax_s32_relu(e, -e_del, Mp - oe_del);
+                    f = __viaddmax_s32_relu(f, -e_ins, Mp - oe_ins);
+                    key = max(key, (h << 12) | (4095 - j));   // first column of the row max
+                    col[j * T] = (uint32_t)h1 << 16 | (uint32_t)e_new << 3 | q;
+                    h1 = h;
+                }
+                {
+                    const uint32_t wd = col[end * T];
+                    col[end * T] = (uint32_t)h1 << 16 | (wd & 7u);
+                }
+                if (end > beg) cells += end - beg;
+                if (end == qlen && gscore < h1) { gscore = h1; max_ie = i; }
+                const int m_row = key >> 12;
+                const int mj = 4095 - (key & 4095);
+                if (m_row == 0) break;
+                if (m_row > best) {
+                    best = m_row; max_i = i; max_j = mj;
+                    const int off = mj > i ? mj - i : i - mj;
+                    if (max_off < off) max_off = off;
+                } else if (p.zdrop > 0) {
+                    const int di = i - max_i, dj = mj - max_j;
+                    if (di > dj) {
+                        if (best - m_row - (di - dj) * e_del > p.zdrop) break;
+                    } else if (best - m_row - (dj - di) * e_ins > p.zdrop) {
+                        break;
+                    }
+                }
+                int nb = beg;
+                while (nb < end && (col[nb * T] >> 3) == 0) ++nb;
+                beg = nb;
+                int ne = end;
+                while (ne > beg && (col[ne * T] >> 3) == 0) --ne;
+                end = ne + 2 < qlen ? ne + 2 : qlen;
+            }
+            if (bad) atomicOr(status, ST_BAD_CODE);
+            fa_ext_result r;
+            r.score = best;
+            r.qle = max_j + 1;
+            r.tle = max_i + 1;
+            r.gtle = max_ie + 1;
+            r.gscore = gscore;
+            r.max_off = max_off;
+            out[jid] = r;
+            if (clamped_out) clamped_out[jid] = (uint8_t)clamped;
+            if (cells_job) cells_job[jid] = cells;
+        }
+    }
+    if (cells_out) {
+        unsigned long long c = cells;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+        if ((threadIdx.x & 31) == 0 && c) atomicAdd(cells_out, c);
+    }
+}
+
+size_t ext_packed_smem_bytes(int qcap) {
+    return (size_t)(qcap + 1) * kExtThreads * sizeof(uint32_t);
+}
+
+cudaError_t launch_ext_packed(const fa_job *d_jobs, const uint32_t *d_order, uint32_t n,
+                              const uint32_t *d_n, const uint8_t *d_qseq, const uint8_t *d_tseq,
+                              const ExtParams &p, int qcap, const int32_t *d_w_try,
+                              fa_ext_result *d_out, uint8_t *d_clamped, uint32_t *d_cells_job,
+                              unsigned long long *d_cells, uint32_t *d_status,
+                              cudaStream_t stream)
+{
+    if (n == 0) return cudaSuccess;
+    const size_t smem = ext_packed_smem_bytes(qcap);
+    cudaError_t err = cudaFuncSetAttribute(ext_packed_kernel,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return err;
+    const uint32_t blocks = (n + kExtThreads - 1) / kExtThreads;
+    ext_packed_kernel<<<blocks, kExtThreads, smem, stream>>>(d_jobs, d_order, n, d_n, d_qseq, d_tseq, p,
+                                                             qcap, d_w_try, d_out, d_clamped,
+                                                             d_cells_job, d_cells, d_status);
+    return cudaGetLastError();
+}
+
+}  // namespace fa

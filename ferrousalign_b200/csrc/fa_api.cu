@@ -1,0 +1,560 @@
+// fa_api.cu -- C ABI of the B200 seed-extension / mate-rescue library.
+//
+// Host side of the drop-in for execute_batch_simd_scoring
+// (src/pipelines/linear/batch_extension/dispatch.rs:31-86) and for the ksw_align2
+// calls of execute_mate_rescue_batch_with_engine
+// (src/pipelines/linear/paired/mate_rescue.rs:595-685): validation (the reference's
+// panics become FA_ERR_ARG), length ordering, device buffers, the band-retry rounds
+// and the copies in and out.  There is no CPU fallback: every result comes from the
+// CUDA kernels of this library.
+
+#include <algorithm>
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "fa_kernels.h"
+
+using namespace fa;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define FA_CUDA(call)                                                                   \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess)                                                          \
+            return fail(FA_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));   \
+    } while (0)
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= cap) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = std::max(bytes, (size_t)256);
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+    void release() { if (p) cudaFree(p); p = nullptr; cap = 0; }
+    template <class T> T *as() const { return static_cast<T *>(p); }
+};
+
+// Largest query a packed-column launch can hold: (qcap+1) words per thread.
+int packed_qcap_limit(size_t smem_optin) {
+    return (int)(smem_optin / (kExtThreads * sizeof(uint32_t))) - 1;
+}
+
+}  // namespace
+
+struct fa_ctx {
+    int device = 0;
+    int sm_count = 0;
+    size_t smem_optin = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    DevBuf jobs, order, qseq, tseq, out, clamped, cells_job, misc;
+    DevBuf w_first, w_cur, prev, kk, w_final, tries, missed, list_a, list_b, hist;
+    uint32_t last_launches = 0;
+};
+
+namespace {
+
+// misc buffer layout: [0] status u32, [2] cells u64, [4] count A u32, [5] count B u32
+struct Misc {
+    uint32_t *status;
+    unsigned long long *cells;
+    uint32_t *cnt_a, *cnt_b;
+};
+Misc misc_of(fa_ctx *c) {
+    char *b = c->misc.as<char>();
+    return Misc{(uint32_t *)b, (unsigned long long *)(b + 8), (uint32_t *)(b + 16), (uint32_t *)(b + 20)};
+}
+
+int check_params(const fa_params *p) {
+    if (!p) return fail(FA_ERR_ARG, "null params");
+    if (p->m != 5) return fail(FA_ERR_ARG, "alphabet size m=%d unsupported (must be 5)", p->m);
+    if (p->o_del < 0 || p->e_del < 0 || p->o_ins < 0 || p->e_ins < 0)
+        return fail(FA_ERR_ARG, "negative gap penalties are not supported");
+    return FA_OK;
+}
+
+ExtParams ext_params_of(const fa_params *p) {
+    ExtParams k;
+    memcpy(k.mat, p->mat, 25);
+    k.m = p->m;
+    k.o_del = p->o_del; k.e_del = p->e_del; k.o_ins = p->o_ins; k.e_ins = p->e_ins;
+    k.zdrop = p->zdrop; k.end_bonus = p->end_bonus;
+    int ms = 0;
+    for (int i = 0; i < 25; ++i) if (p->mat[i] > (int8_t)ms) ms = p->mat[i];
+    k.max_score = ms;
+    return k;
+}
+
+// Validation mirrors the reference's panics (h0 <= 0 asserts at ksw_affine_gap.rs:968,
+// out-of-range slices) and this library's limits.
+int check_jobs(const fa_job *jobs, uint32_t n, uint64_t qlen_buf, uint64_t tlen_buf,
+               const ExtParams &k, int qcap_limit, int *max_qlen) {
+    int mq = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        const fa_job &j = jobs[i];
+        if (j.qlen <= 0) return fail(FA_ERR_ARG, "job %u: qlen=%d must be > 0", i, j.qlen);
+        if (j.tlen < 0) return fail(FA_ERR_ARG, "job %u: tlen=%d must be >= 0", i, j.tlen);
+        if (j.h0 <= 0) return fail(FA_ERR_ARG, "job %u: h0=%d must be > 0", i, j.h0);
+        if (j.qlen > FA_MAX_QLEN || j.tlen > FA_MAX_TLEN)
+            return fail(FA_ERR_CAPACITY, "job %u: lengths %d/%d exceed %d/%d", i, j.qlen, j.tlen,
+                        FA_MAX_QLEN, FA_MAX_TLEN);
+        if (j.q_off + (uint64_t)j.qlen > qlen_buf || j.t_off + (uint64_t)j.tlen > tlen_buf)
+            return fail(FA_ERR_ARG, "job %u: sequence range outside the buffers", i);
+        if ((int64_t)j.h0 + (int64_t)k.max_score * j.qlen > kPackedHMax)
+            return fail(FA_ERR_CAPACITY, "job %u: h0 + max(mat)*qlen = %lld exceeds %d", i,
+                        (long long)j.h0 + (long long)k.max_score * j.qlen, kPackedHMax);
+        if (j.qlen > qcap_limit)
+            return fail(FA_ERR_CAPACITY, "job %u: qlen=%d exceeds %d", i, j.qlen, qcap_limit);
+        mq = std::max(mq, j.qlen);
+    }
+    *max_qlen = mq;
+    return FA_OK;
+}
+
+// Counting sort by query length, longest first; returns [begin,end) segments of
+// the order that share a shared-memory capacity class.
+void length_order(const fa_job *jobs, uint32_t n, std::vector<uint32_t> &order,
+                  std::vector<std::pair<uint32_t, int>> &segs) {
+    std::vector<uint32_t> cnt(FA_MAX_QLEN + 2, 0);
+    for (uint32_t i = 0; i < n; ++i) cnt[jobs[i].qlen]++;
+    std::vector<uint32_t> start(FA_MAX_QLEN + 2, 0);
+    uint32_t acc = 0;
+    for (int q = FA_MAX_QLEN; q >= 0; --q) { start[q] = acc; acc += cnt[q]; }
+    order.resize(n);
+    for (uint32_t i = 0; i < n; ++i) order[start[jobs[i].qlen]++] = i;
+    // capacity classes: multiples of 32 columns
+    segs.clear();
+    uint32_t b = 0;
+    while (b < n) {
+        const int q = jobs[order[b]].qlen;
+        const int cap = (q + 31) / 32 * 32;
+        uint32_t e = b;
+        while (e < n && jobs[order[e]].qlen > cap - 32) ++e;
+        segs.push_back({e, std::min(cap, q)});
+        b = e;
+    }
+}
+
+int ensure_ext_buffers(fa_ctx *c, uint32_t n, uint64_t qb, uint64_t tb) {
+    FA_CUDA(c->jobs.ensure(sizeof(fa_job) * (size_t)n));
+    FA_CUDA(c->order.ensure(sizeof(uint32_t) * (size_t)n));
+    FA_CUDA(c->qseq.ensure(qb));
+    FA_CUDA(c->tseq.ensure(tb));
+    FA_CUDA(c->out.ensure(sizeof(fa_ext_result) * (size_t)n));
+    FA_CUDA(c->clamped.ensure(n));
+    FA_CUDA(c->cells_job.ensure(sizeof(uint32_t) * (size_t)n));
+    FA_CUDA(c->misc.ensure(64));
+    return FA_OK;
+}
+
+int ensure_policy_buffers(fa_ctx *c, uint32_t n) {
+    const size_t b = sizeof(int32_t) * (size_t)n;
+    FA_CUDA(c->w_first.ensure(b));
+    FA_CUDA(c->w_cur.ensure(b));
+    FA_CUDA(c->prev.ensure(b));
+    FA_CUDA(c->kk.ensure(b));
+    FA_CUDA(c->w_final.ensure(b));
+    FA_CUDA(c->tries.ensure(b));
+    FA_CUDA(c->missed.ensure(n));
+    FA_CUDA(c->list_a.ensure(b));
+    FA_CUDA(c->list_b.ensure(b));
+    return FA_OK;
+}
+
+int read_status(fa_ctx *c, cudaStream_t s) {
+    uint32_t st = 0;
+    FA_CUDA(cudaMemcpyAsync(&st, misc_of(c).status, 4, cudaMemcpyDeviceToHost, s));
+    FA_CUDA(cudaStreamSynchronize(s));
+    if (st & ST_BAD_CODE) return fail(FA_ERR_ARG, "a sequence byte is outside the alphabet (codes 0-4)");
+    if (st & ST_CAPACITY) return fail(FA_ERR_CAPACITY, "a job exceeded the launch capacity");
+    if (st & ST_BLIST) return fail(FA_ERR_CAPACITY, "mate-SW run list overflow");
+    if (st & ST_ARG) return fail(FA_ERR_ARG, "a job has h0 <= 0, qlen <= 0 or tlen < 0");
+    return FA_OK;
+}
+
+// Runs the extension rounds on device data.  order/segs describe the first round;
+// retry rounds reuse the widest capacity class.
+int run_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n,
+            const std::vector<std::pair<uint32_t, int>> &segs, int qcap_all, const fa_job *d_jobs,
+            const uint32_t *d_order, const uint8_t *d_q, const uint8_t *d_t, const int32_t *d_wfirst,
+            fa_ext_result *d_out, cudaStream_t s, fa_ext_stats *stats, int32_t *h_wfinal) {
+    Misc m = misc_of(c);
+    FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
+    const int mode = pol ? pol->mode : FA_POLICY_SINGLE;
+    uint32_t launches = 0;
+    FA_CUDA(cudaEventRecord(c->ev0, s));
+    if (mode == FA_POLICY_SINGLE) {
+        uint32_t b = 0;
+        for (auto &sg : segs) {
+            FA_CUDA(launch_ext_packed(d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp, sg.second,
+                                      nullptr, d_out, nullptr, c->cells_job.as<uint32_t>(), m.cells,
+                                      m.status, s));
+            ++launches;
+            b = sg.first;
+        }
+    } else {
+        if (int rc = ensure_policy_buffers(c, n)) return rc;
+        PolicyState st{c->w_cur.as<int32_t>(), c->prev.as<int32_t>(), c->kk.as<int32_t>(),
+                       c->w_final.as<int32_t>(), c->tries.as<int32_t>(), c->missed.as<uint8_t>()};
+        const int learned = mode == FA_POLICY_LEARNED;
+        FA_CUDA(launch_policy_init(d_jobs, n, d_wfirst, pol->w_min, learned, st, s));
+        ++launches;
+        const int max_tries = std::max(1, pol->max_tries);
+        // worst case rounds: narrow ladder (<= 12 doublings) + bwa tries
+        const int max_rounds = (learned ? 13 : 0) + max_tries;
+        const uint32_t *list = d_order;
+        const uint32_t *cnt = nullptr;
+        uint32_t *next = c->list_a.as<uint32_t>(), *next_cnt = m.cnt_a;
+        uint32_t *spare = c->list_b.as<uint32_t>(), *spare_cnt = m.cnt_b;
+        for (int r = 0; r < max_rounds; ++r) {
+            if (r == 0) {
+                uint32_t b = 0;
+                for (auto &sg : segs) {
+                    FA_CUDA(launch_ext_packed(d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp,
+                                              sg.second, st.w_cur, d_out, c->clamped.as<uint8_t>(),
+                                              c->cells_job.as<uint32_t>(), m.cells, m.status, s));
+                    ++launches;
+                    b = sg.first;
+                }
+            } else {
+                FA_CUDA(launch_ext_packed(d_jobs, list, n, cnt, d_q, d_t, kp, qcap_all, st.w_cur, d_out,
+                                          c->clamped.as<uint8_t>(), c->cells_job.as<uint32_t>(), m.cells,
+                                          m.status, s));
+                ++launches;
+            }
+            FA_CUDA(cudaMemsetAsync(next_cnt, 0, 4, s));
+            FA_CUDA(launch_policy_step(d_jobs, list, cnt, n, d_out, c->clamped.as<uint8_t>(), st, max_tries,
+                                       pol->judge, next, next_cnt, s));
+            ++launches;
+            uint32_t h_cnt = 0;
+            FA_CUDA(cudaMemcpyAsync(&h_cnt, next_cnt, 4, cudaMemcpyDeviceToHost, s));
+            FA_CUDA(cudaStreamSynchronize(s));
+            if (h_cnt == 0) break;
+            if (stats) stats->retries += h_cnt;
+            list = next; cnt = next_cnt;
+            std::swap(next, spare);
+            std::swap(next_cnt, spare_cnt);
+        }
+    }
+    FA_CUDA(cudaEventRecord(c->ev1, s));
+    if (int rc = read_status(c, s)) return rc;
+    if (stats) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        unsigned long long cells = 0;
+        FA_CUDA(cudaMemcpy(&cells, m.cells, 8, cudaMemcpyDeviceToHost));
+        stats->cells_executed = cells;
+        stats->kernel_ms = ms;
+        stats->kernel_launches = launches;
+        stats->jobs = n;
+        std::vector<uint32_t> cj(n);
+        FA_CUDA(cudaMemcpy(cj.data(), c->cells_job.p, 4ull * n, cudaMemcpyDeviceToHost));
+        uint64_t acc = 0;
+        for (uint32_t i = 0; i < n; ++i) acc += cj[i];
+        stats->cells = acc;
+        if (mode == FA_POLICY_LEARNED) {
+            std::vector<uint8_t> ms_(n);
+            FA_CUDA(cudaMemcpy(ms_.data(), c->missed.p, n, cudaMemcpyDeviceToHost));
+            uint32_t miss = 0;
+            for (uint32_t i = 0; i < n; ++i) miss += ms_[i];
+            stats->misses = miss;
+        }
+    }
+    if (h_wfinal && mode != FA_POLICY_SINGLE)
+        FA_CUDA(cudaMemcpy(h_wfinal, c->w_final.p, 4ull * n, cudaMemcpyDeviceToHost));
+    return FA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *fa_last_error(void) { return g_err.c_str(); }
+const char *fa_version(void) { return "ferrous_b200 0.1 (sm_100a)"; }
+
+int fa_ctx_create(int device, fa_ctx **out) {
+    if (!out) return fail(FA_ERR_ARG, "null out");
+    *out = nullptr;
+    int ndev = 0;
+    FA_CUDA(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) return fail(FA_ERR_ARG, "device %d not present (%d)", device, ndev);
+    FA_CUDA(cudaSetDevice(device));
+    fa_ctx *c = new fa_ctx();
+    c->device = device;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major < 10) {
+        delete c;
+        return fail(FA_ERR_CUDA, "device %d is not sm_100-class", device);
+    }
+    c->sm_count = prop.multiProcessorCount;
+    c->smem_optin = prop.sharedMemPerBlockOptin;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+        delete c;
+        return fail(FA_ERR_CUDA, "stream/event creation failed");
+    }
+    *out = c;
+    return FA_OK;
+}
+
+void fa_ctx_destroy(fa_ctx *c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    for (DevBuf *b : {&c->jobs, &c->order, &c->qseq, &c->tseq, &c->out, &c->clamped, &c->cells_job,
+                      &c->misc, &c->w_first, &c->w_cur, &c->prev, &c->kk, &c->w_final, &c->tries,
+                      &c->missed, &c->list_a, &c->list_b, &c->hist})
+        b->release();
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+int fa_probe_int_peak(fa_ctx *c, int kind, double *ops_per_s, float *ms) {
+    if (!c || !ops_per_s) return fail(FA_ERR_ARG, "null argument");
+    if (kind < 0 || kind > 4) return fail(FA_ERR_ARG, "unknown probe kind %d", kind);
+    FA_CUDA(cudaSetDevice(c->device));
+    const double r = probe_int_peak(kind, c->sm_count, c->stream, ms);
+    if (r <= 0) return fail(FA_ERR_CUDA, "probe kernel failed");
+    *ops_per_s = r;
+    return FA_OK;
+}
+
+int fa_device_info(fa_ctx *c, int *sm_count, int *smem_optin_bytes) {
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    if (sm_count) *sm_count = c->sm_count;
+    if (smem_optin_bytes) *smem_optin_bytes = (int)c->smem_optin;
+    return FA_OK;
+}
+
+uint32_t fa_mate_xtra(int32_t mate_len, int32_t match_score, int32_t min_seed_len) {
+    uint32_t x = FA_KSW_XSUBO | FA_KSW_XSTART;
+    if (mate_len * match_score < 250) x |= FA_KSW_XBYTE;
+    return x | (uint32_t)(min_seed_len * match_score);
+}
+
+int fa_ext_batch_policy(fa_ctx *c, const fa_params *p, const fa_policy *pol, const fa_job *jobs,
+                        uint32_t n, const uint8_t *qseq, uint64_t qseq_len, const uint8_t *tseq,
+                        uint64_t tseq_len, const int32_t *w_first, fa_ext_result *out,
+                        int32_t *w_final, fa_ext_stats *stats) {
+    auto t0 = std::chrono::steady_clock::now();
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    if (int rc = check_params(p)) return rc;
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (n == 0) return FA_OK;
+    if (!jobs || !out || !qseq || !tseq) return fail(FA_ERR_ARG, "null buffer");
+    if (pol && (pol->mode < FA_POLICY_SINGLE || pol->mode > FA_POLICY_LEARNED))
+        return fail(FA_ERR_ARG, "unknown policy mode %d", pol->mode);
+    if (pol && pol->mode == FA_POLICY_LEARNED && !w_first)
+        return fail(FA_ERR_STATE, "learned policy needs w_first (or a loaded band model)");
+    FA_CUDA(cudaSetDevice(c->device));
+    const ExtParams kp = ext_params_of(p);
+    int max_q = 0;
+    if (int rc = check_jobs(jobs, n, qseq_len, tseq_len, kp, packed_qcap_limit(c->smem_optin), &max_q))
+        return rc;
+    std::vector<uint32_t> order;
+    std::vector<std::pair<uint32_t, int>> segs;
+    length_order(jobs, n, order, segs);
+    if (int rc = ensure_ext_buffers(c, n, qseq_len, tseq_len)) return rc;
+    cudaStream_t s = c->stream;
+    FA_CUDA(cudaMemcpyAsync(c->jobs.p, jobs, sizeof(fa_job) * (size_t)n, cudaMemcpyHostToDevice, s));
+    FA_CUDA(cudaMemcpyAsync(c->order.p, order.data(), 4ull * n, cudaMemcpyHostToDevice, s));
+    FA_CUDA(cudaMemcpyAsync(c->qseq.p, qseq, qseq_len, cudaMemcpyHostToDevice, s));
+    FA_CUDA(cudaMemcpyAsync(c->tseq.p, tseq, tseq_len, cudaMemcpyHostToDevice, s));
+    if (pol && pol->mode == FA_POLICY_LEARNED) {
+        if (int rc = ensure_policy_buffers(c, n)) return rc;
+        FA_CUDA(cudaMemcpyAsync(c->w_first.p, w_first, 4ull * n, cudaMemcpyHostToDevice, s));
+    }
+    int rc = run_ext(c, kp, pol, n, segs, max_q, c->jobs.as<fa_job>(), c->order.as<uint32_t>(),
+                     c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(),
+                     (pol && pol->mode == FA_POLICY_LEARNED) ? c->w_first.as<int32_t>() : nullptr,
+                     c->out.as<fa_ext_result>(), s, stats, w_final);
+    if (rc) return rc;
+    FA_CUDA(cudaMemcpyAsync(out, c->out.p, sizeof(fa_ext_result) * (size_t)n, cudaMemcpyDeviceToHost, s));
+    FA_CUDA(cudaStreamSynchronize(s));
+    if (w_final && (!pol || pol->mode == FA_POLICY_SINGLE))
+        for (uint32_t i = 0; i < n; ++i) w_final[i] = jobs[i].w;
+    if (stats)
+        stats->total_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return FA_OK;
+}
+
+int fa_ext_batch(fa_ctx *c, const fa_params *p, const fa_job *jobs, uint32_t n, const uint8_t *qseq,
+                 uint64_t qseq_len, const uint8_t *tseq, uint64_t tseq_len, fa_ext_result *out,
+                 fa_ext_stats *stats) {
+    return fa_ext_batch_policy(c, p, nullptr, jobs, n, qseq, qseq_len, tseq, tseq_len, nullptr, out,
+                               nullptr, stats);
+}
+
+int fa_ext_batch_device(fa_ctx *c, const fa_params *p, const fa_job *d_jobs, uint32_t n,
+                        const uint8_t *d_qseq, const uint8_t *d_tseq, const uint32_t *d_order,
+                        fa_ext_result *d_out, void *stream) {
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    if (int rc = check_params(p)) return rc;
+    if (n == 0) return FA_OK;
+    if (!d_jobs || !d_qseq || !d_tseq || !d_out) return fail(FA_ERR_ARG, "null buffer");
+    FA_CUDA(cudaSetDevice(c->device));
+    const ExtParams kp = ext_params_of(p);
+    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    FA_CUDA(c->misc.ensure(64));
+    FA_CUDA(c->hist.ensure(sizeof(uint32_t) * (FA_MAX_QLEN + 1)));
+    Misc m = misc_of(c);
+    FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
+    // query-length histogram -> launch classes (one 16 KB read-back per batch)
+    FA_CUDA(launch_qlen_hist(d_jobs, n, c->hist.as<uint32_t>(), c->sm_count, s));
+    std::vector<uint32_t> hist(FA_MAX_QLEN + 1);
+    FA_CUDA(cudaMemcpyAsync(hist.data(), c->hist.p, 4 * hist.size(), cudaMemcpyDeviceToHost, s));
+    FA_CUDA(cudaStreamSynchronize(s));
+    const int qlimit = packed_qcap_limit(c->smem_optin);
+    std::vector<uint32_t> start(FA_MAX_QLEN + 1, 0);
+    std::vector<std::pair<uint32_t, int>> segs;
+    uint32_t acc = 0, seg_end = 0;
+    int seg_cap = -1;
+    for (int q = FA_MAX_QLEN; q >= 0; --q) {
+        start[q] = acc;
+        if (!hist[q]) continue;
+        if (q > qlimit) return fail(FA_ERR_CAPACITY, "a job has qlen=%d > %d", q, qlimit);
+        if (seg_cap < 0 || q <= ((seg_cap + 31) / 32 - 1) * 32) {
+            if (seg_cap >= 0) segs.push_back({seg_end, seg_cap});
+            seg_cap = q;
+        }
+        acc += hist[q];
+        seg_end = acc;
+    }
+    if (seg_cap >= 0) segs.push_back({seg_end, seg_cap});
+    const uint32_t *order = d_order;
+    if (!order) {
+        FA_CUDA(c->order.ensure(4ull * n));
+        FA_CUDA(cudaMemcpyAsync(c->hist.p, start.data(), 4 * start.size(), cudaMemcpyHostToDevice, s));
+        FA_CUDA(launch_qlen_scatter(d_jobs, n, c->hist.as<uint32_t>(), c->order.as<uint32_t>(), s));
+        order = c->order.as<uint32_t>();
+    } else {
+        segs.assign(1, {n, std::max(0, segs.empty() ? 0 : segs.front().second)});
+    }
+    uint32_t b = 0;
+    for (auto &sg : segs) {
+        FA_CUDA(launch_ext_packed(d_jobs, order + b, sg.first - b, nullptr, d_qseq, d_tseq, kp, sg.second,
+                                  nullptr, d_out, nullptr, nullptr, nullptr, m.status, s));
+        b = sg.first;
+    }
+    c->last_launches = (uint32_t)segs.size() + (d_order ? 1u : 2u);
+    return FA_OK;
+}
+
+int fa_ctx_sync(fa_ctx *c) {
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    FA_CUDA(cudaSetDevice(c->device));
+    FA_CUDA(cudaStreamSynchronize(c->stream));
+    if (c->misc.p) return read_status(c, c->stream);
+    return FA_OK;
+}
+
+int fa_ctx_last_launches(fa_ctx *c) { return c ? (int)c->last_launches : -1; }
+
+int fa_mate_sw_batch(fa_ctx *c, const fa_mate_params *p, const fa_mate_job *jobs, uint32_t n,
+                     const uint8_t *qseq, uint64_t qseq_len, const uint8_t *tseq, uint64_t tseq_len,
+                     fa_kswr *out, fa_ext_stats *stats) {
+    auto t0 = std::chrono::steady_clock::now();
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    if (!p || p->m != 5) return fail(FA_ERR_ARG, "alphabet size must be 5");
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (n == 0) return FA_OK;
+    if (!jobs || !out || !qseq || !tseq) return fail(FA_ERR_ARG, "null buffer");
+    int mn = 127, mx = 0;
+    for (int i = 0; i < 25; ++i) { mn = std::min<int>(mn, p->mat[i]); mx = std::max<int>(mx, p->mat[i]); }
+    if (mx <= 0) return fail(FA_ERR_ARG, "scoring matrix needs a positive entry");
+    MateParams mp;
+    memcpy(mp.mat, p->mat, 25);
+    mp.m = 5;
+    mp.o_del = p->o_del; mp.e_del = p->e_del; mp.o_ins = p->o_ins; mp.e_ins = p->e_ins;
+    mp.shift = (uint8_t)(256 - mn);
+    mp.max = mx;
+    std::vector<uint32_t> byte_list, word_list;
+    int mq_b = 0, mq_w = 0, mt = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        const fa_mate_job &j = jobs[i];
+        if (j.qlen <= 0 || j.tlen < 0) return fail(FA_ERR_ARG, "mate job %u: bad lengths", i);
+        if (j.tlen > FA_MAX_TLEN) return fail(FA_ERR_CAPACITY, "mate job %u: tlen too long", i);
+        if (j.q_off + (uint64_t)j.qlen > qseq_len || j.t_off + (uint64_t)j.tlen > tseq_len)
+            return fail(FA_ERR_ARG, "mate job %u: sequence range outside the buffers", i);
+        const bool byte = (j.xtra & FA_KSW_XBYTE) != 0;
+        if (byte ? j.qlen > 16 * 32 : j.qlen > 8 * 32)
+            return fail(FA_ERR_CAPACITY, "mate job %u: qlen=%d exceeds the %s-lane limit", i, j.qlen,
+                        byte ? "u8" : "i16");
+        (byte ? byte_list : word_list).push_back(i);
+        if (byte) mq_b = std::max(mq_b, j.qlen); else mq_w = std::max(mq_w, j.qlen);
+        mt = std::max(mt, j.tlen);
+    }
+    FA_CUDA(cudaSetDevice(c->device));
+    cudaStream_t s = c->stream;
+    FA_CUDA(c->jobs.ensure(sizeof(fa_mate_job) * (size_t)n));
+    FA_CUDA(c->order.ensure(4ull * n));
+    FA_CUDA(c->qseq.ensure(qseq_len));
+    FA_CUDA(c->tseq.ensure(tseq_len));
+    FA_CUDA(c->out.ensure(sizeof(fa_kswr) * (size_t)n));
+    FA_CUDA(c->misc.ensure(64));
+    Misc m = misc_of(c);
+    FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
+    std::vector<uint32_t> order(byte_list);
+    order.insert(order.end(), word_list.begin(), word_list.end());
+    FA_CUDA(cudaMemcpyAsync(c->jobs.p, jobs, sizeof(fa_mate_job) * (size_t)n, cudaMemcpyHostToDevice, s));
+    FA_CUDA(cudaMemcpyAsync(c->order.p, order.data(), 4ull * n, cudaMemcpyHostToDevice, s));
+    FA_CUDA(cudaMemcpyAsync(c->qseq.p, qseq, qseq_len, cudaMemcpyHostToDevice, s));
+    FA_CUDA(cudaMemcpyAsync(c->tseq.p, tseq, tseq_len, cudaMemcpyHostToDevice, s));
+    FA_CUDA(cudaEventRecord(c->ev0, s));
+    uint32_t launches = 0;
+    if (!byte_list.empty()) {
+        FA_CUDA(launch_mate_sw(true, c->jobs.as<fa_mate_job>(), c->order.as<uint32_t>(),
+                               (uint32_t)byte_list.size(), c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(), mp,
+                               mq_b, mt, c->out.as<fa_kswr>(), m.cells, m.status, s));
+        ++launches;
+    }
+    if (!word_list.empty()) {
+        FA_CUDA(launch_mate_sw(false, c->jobs.as<fa_mate_job>(), c->order.as<uint32_t>() + byte_list.size(),
+                               (uint32_t)word_list.size(), c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(), mp,
+                               mq_w, mt, c->out.as<fa_kswr>(), m.cells, m.status, s));
+        ++launches;
+    }
+    FA_CUDA(cudaEventRecord(c->ev1, s));
+    if (int rc = read_status(c, s)) return rc;
+    FA_CUDA(cudaMemcpyAsync(out, c->out.p, sizeof(fa_kswr) * (size_t)n, cudaMemcpyDeviceToHost, s));
+    FA_CUDA(cudaStreamSynchronize(s));
+    if (stats) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        unsigned long long cells = 0;
+        FA_CUDA(cudaMemcpy(&cells, m.cells, 8, cudaMemcpyDeviceToHost));
+        stats->cells = stats->cells_executed = cells;
+        stats->kernel_ms = ms;
+        stats->kernel_launches = launches;
+        stats->jobs = n;
+        stats->total_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return FA_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,57 @@
+// fa_device.cuh -- device-side types and helpers shared by the B200 kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/ferrous_b200.h"
+
+namespace fa {
+
+// Device status word bits (written with atomicOr, read back by the host).
+enum : uint32_t {
+    ST_BAD_CODE = 1u << 0,   // a sequence byte >= alphabet size
+    ST_CAPACITY = 1u << 1,   // a job exceeded the launch's length limit
+    ST_BLIST    = 1u << 2,   // mate-SW run list overflowed its buffer
+    ST_ARG      = 1u << 3,   // a job violates an argument rule (h0 <= 0, qlen <= 0, tlen < 0)
+};
+
+// Scoring parameters in the form the extension kernel consumes.
+struct ExtParams {
+    int8_t  mat[25];
+    int32_t m;
+    int32_t o_del, e_del, o_ins, e_ins;
+    int32_t zdrop, end_bonus;
+    int32_t max_score;      // max(0, max(mat))  (ksw_affine_gap.rs:1000-1005)
+};
+
+struct MateParams {
+    int8_t  mat[25];
+    int32_t m;
+    int32_t o_del, e_del, o_ins, e_ins;
+    int32_t shift, max;     // ksw_qinit shift / max (ksw_affine_gap.rs:88-101)
+};
+
+// Rust `f64 as i32`: truncation toward zero with saturation, NaN -> 0.
+__host__ __device__ inline int32_t rust_f64_as_i32(double x) {
+    if (x != x) return 0;
+    if (x >= 2147483647.0) return INT32_MAX;
+    if (x <= -2147483648.0) return INT32_MIN;
+    return static_cast<int32_t>(x);
+}
+
+// Band after the max_ins / max_del clamp of ksw_extend2 (ksw_affine_gap.rs:1007-1018),
+// evaluated in the same double-precision order as the reference.
+__host__ __device__ inline int32_t ext_band_clamp(int32_t qlen, int32_t w, const ExtParams &p) {
+    int32_t max_ins = rust_f64_as_i32(((double)qlen * (double)p.max_score + (double)p.end_bonus -
+                                       (double)p.o_ins) / (double)p.e_ins + 1.0);
+    if (max_ins < 1) max_ins = 1;
+    if (w > max_ins) w = max_ins;
+    int32_t max_del = rust_f64_as_i32(((double)qlen * (double)p.max_score + (double)p.end_bonus -
+                                       (double)p.o_del) / (double)p.e_del + 1.0);
+    if (max_del < 1) max_del = 1;
+    if (w > max_del) w = max_del;
+    return w;
+}
+
+}  // namespace fa

@@ -1,0 +1,54 @@
+// fa_kernels.h -- internal launcher declarations (C++ linkage, not part of the C ABI).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "fa_device.cuh"
+
+namespace fa {
+
+constexpr int kExtThreads = 128;     // threads (= jobs) per extension block
+constexpr int kPackedHMax = 8191;    // largest H/E the packed column word holds
+
+size_t ext_packed_smem_bytes(int qcap);
+cudaError_t launch_ext_packed(const fa_job *d_jobs, const uint32_t *d_order, uint32_t n,
+                              const uint32_t *d_n, const uint8_t *d_qseq, const uint8_t *d_tseq,
+                              const ExtParams &p, int qcap, const int32_t *d_w_try,
+                              fa_ext_result *d_out, uint8_t *d_clamped, uint32_t *d_cells_job,
+                              unsigned long long *d_cells, uint32_t *d_status,
+                              cudaStream_t stream);
+
+// Band-retry policy step over the jobs of the last extension round (see policy_kernel.cu).
+struct PolicyState {
+    int32_t *w_cur;      // band of the run just finished / next run
+    int32_t *prev;       // previous try's score (bwa-mem2 break rule)
+    int32_t *k;          // bwa try index; -1 while on the learned narrow ladder
+    int32_t *w_final;    // band of the accepted run
+    int32_t *tries;      // runs per job
+    uint8_t *missed;     // learned path: first narrow run not accepted
+};
+cudaError_t launch_policy_step(const fa_job *d_jobs, const uint32_t *d_list, const uint32_t *d_count,
+                               uint32_t n_max, const fa_ext_result *d_out, const uint8_t *d_clamped,
+                               PolicyState st, int max_tries, int judge, uint32_t *d_next,
+                               uint32_t *d_next_count, cudaStream_t stream);
+cudaError_t launch_policy_init(const fa_job *d_jobs, uint32_t n, const int32_t *d_w_first, int w_min,
+                               int learned, PolicyState st, cudaStream_t stream);
+
+// Mate-rescue local SW.  `byte_lanes` selects the u8 (16-lane) or i16 (8-lane)
+// emulation of the reference's striped kernels; d_order lists the jobs of that kind.
+cudaError_t launch_mate_sw(bool byte_lanes, const fa_mate_job *d_jobs, const uint32_t *d_order,
+                           uint32_t n, const uint8_t *d_qseq, const uint8_t *d_tseq,
+                           const MateParams &p, int max_qlen, int max_tlen, fa_kswr *d_out,
+                           unsigned long long *d_cells, uint32_t *d_status, cudaStream_t stream);
+
+// Device-side longest-first ordering by query length (order_kernel.cu).
+cudaError_t launch_qlen_hist(const fa_job *d_jobs, uint32_t n, uint32_t *d_hist, int sm_count, cudaStream_t s);
+cudaError_t launch_qlen_scatter(const fa_job *d_jobs, uint32_t n, uint32_t *d_cursor, uint32_t *d_order,
+                                cudaStream_t s);
+
+// Integer / DPX instruction throughput (ops per second) for the roofline denominator.
+double probe_int_peak(int kind, int sm_count, cudaStream_t s, float *ms_out);
+
+}  // namespace fa

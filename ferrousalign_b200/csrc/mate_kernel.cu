@@ -1,0 +1,306 @@
+// mate_kernel.cu -- mate-rescue local Smith-Waterman (ksw_align2 semantics) on sm_100a.
+//
+// The reference runs ksw_align2 with its 128-bit striped engine
+// (src/core/alignment/ksw_affine_gap.rs:773-861): 16 u8 lanes when KSW_XBYTE is set,
+// otherwise 8 i16 lanes.  Its results depend on that striping -- E is built from the
+// H values before the lazy-F correction, F is restarted at every stripe boundary and
+// the lazy-F loop stops after the first pass that changes nothing, padding columns
+// score 0 and take part in the row maxima, and the query end is searched over
+// sign-interpreted lanes.  This kernel reproduces the striped machine exactly by
+// giving every SIMD lane of the reference its own GPU lane: a group of P = 16 (u8)
+// or 8 (i16) lanes owns one job, lane l holds stripe l (query positions
+// j + l*slen) in registers, the diagonal crosses stripes with one shuffle per row,
+// lazy-F passes move the F carry one lane per pass, and row maxima, the query-end
+// search and the second-best scan are group reductions.  The forward pass and the
+// KSW_XSTART reverse pass share the same code.
+
+#include <climits>
+
+#include "fa_device.cuh"
+#include "fa_kernels.h"
+
+namespace fa {
+
+constexpr int kMateThreads = 128;
+
+__device__ __forceinline__ uint32_t prmt(uint32_t lo, uint32_t hi, uint32_t sel) {
+    uint32_t r;
+    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(lo), "r"(hi), "r"(sel));
+    return r;
+}
+
+__device__ __forceinline__ int sat16(int x) { return min(max(x, -32768), 32767); }
+
+struct SeqView {
+    const uint8_t *s;
+    int rev_last;   // >= 0: positions 0..rev_last are read reversed (ksw_align2 XSTART pass)
+    __device__ __forceinline__ uint32_t at(int k) const {
+        return rev_last >= 0 && k <= rev_last ? s[rev_last - k] : s[k];
+    }
+};
+
+// One ksw_u8_impl / ksw_i16_impl run (ksw_affine_gap.rs:267-494 / 503-735) for the job
+// owned by this lane group.  All lanes of the group return the same result.
+template <int P, int SMAX>
+__device__ fa_kswr sw_pass(SeqView Q, int qlen, SeqView Tg, int tlen, uint32_t xtra,
+                           const MateParams &p, uint32_t gmask, int l, uint32_t *blist,
+                           int bcap, unsigned long long &cells, uint32_t &status)
+{
+    constexpr bool U8 = (P == 16);
+    constexpr int NQW = SMAX / 8;
+    const int slen = (qlen + P - 1) / P;
+    const int off = SMAX - slen;   // segment j lives at register index j + off
+    const uint32_t minsc = (xtra & FA_KSW_XSUBO) ? (xtra & 0xffffu) : 0x10000u;
+    const uint32_t endsc = (xtra & FA_KSW_XSTOP) ? (xtra & 0xffffu) : 0x10000u;
+    const int oe_del = p.o_del + p.e_del, oe_ins = p.o_ins + p.e_ins;
+    const int e_del = p.e_del, e_ins = p.e_ins, shift = p.shift;
+
+    // Query codes of this stripe as nibbles; 5 marks padding (profile score 0).
+    uint32_t qw[NQW];
+#pragma unroll
+    for (int w = 0; w < NQW; ++w) qw[w] = 0x55555555u;
+    uint32_t bad = 0;
+#pragma unroll
+    for (int a = 0; a < SMAX; ++a) {
+        if (a >= off) {
+            const int k = (a - off) + l * slen;
+            if (k < qlen) {
+                uint32_t c = Q.at(k);
+                bad |= c > 4u;
+                c = c > 4u ? 4u : c;
+                qw[a / 8] = (qw[a / 8] & ~(0xFu << (4 * (a % 8)))) | (c << (4 * (a % 8)));
+            }
+        }
+    }
+
+    int H0[SMAX], H1[SMAX], E[SMAX], Hm[SMAX];
+#pragma unroll
+    for (int a = 0; a < SMAX; ++a) { H0[a] = 0; H1[a] = 0; E[a] = 0; Hm[a] = 0; }
+
+    // profile rows as PRMT tables (u8: mat + shift mod 256, padding = shift; i16: mat, padding = 0),
+    // indexed only with constants
+    uint32_t rlo[5], rhi[5];
+#pragma unroll
+    for (int t = 0; t < 5; ++t) {
+        const int sh = U8 ? shift : 0;
+        rlo[t] = (uint8_t)(p.mat[t * 5] + sh) | (uint32_t)(uint8_t)(p.mat[t * 5 + 1] + sh) << 8 |
+                 (uint32_t)(uint8_t)(p.mat[t * 5 + 2] + sh) << 16 |
+                 (uint32_t)(uint8_t)(p.mat[t * 5 + 3] + sh) << 24;
+        rhi[t] = (uint8_t)(p.mat[t * 5 + 4] + sh) | (uint32_t)(uint8_t)sh << 8;
+    }
+
+    int gmax = 0, te = -1;
+    int nb = 0, last_row = -2, last_sc = 0;
+
+    for (int i = 0; i < tlen; ++i) {
+        const uint32_t tb = Tg.at(i);
+        if (tb > 4u) { bad = 1; break; }
+        uint32_t lo = rlo[0], hi = rhi[0];
+#pragma unroll
+        for (int t = 1; t < 5; ++t)
+            if (tb == (uint32_t)t) { lo = rlo[t]; hi = rhi[t]; }
+        cells += (unsigned long long)qlen;
+
+        int hd = __shfl_up_sync(gmask, H0[SMAX - 1], 1, P);
+        if (l == 0) hd = 0;
+        int f = 0, mx = 0;
+#pragma unroll
+        for (int a = 0; a < SMAX; ++a) {
+            if (a >= off) {
+                const uint32_t c = (qw[a / 8] >> (4 * (a % 8))) & 0xFu;
+                int h;
+                if (U8) {
+                    const int s = (int)prmt(lo, hi, c | 0x7770u);
+                    h = min(hd + s, 255);
+                    h = max(h - shift, 0);
+                } else {
+                    const int s = (int)prmt(lo, hi, c * 0x1111u + 0x8880u);
+                    h = sat16(hd + s);
+                }
+                const int e = E[a];
+                h = max(h, e);
+                h = max(h, f);
+                mx = max(mx, h);
+                H1[a] = h;
+                if (U8) {
+                    E[a] = __viaddmax_s32_relu(e, -e_del, h - oe_del);
+                    f = __viaddmax_s32_relu(f, -e_ins, h - oe_ins);
+                } else {
+                    E[a] = max(sat16(e - e_del), sat16(h - oe_del));
+                    f = max(sat16(f - e_ins), sat16(h - oe_ins));
+                }
+                hd = H0[a];
+            }
+        }
+        // lazy-F: one lane further per pass, stop after a pass that changed nothing
+        for (int pass = 0; pass < P; ++pass) {
+            f = __shfl_up_sync(gmask, f, 1, P);
+            if (l == 0) f = 0;
+            int changed = 0;
+#pragma unroll
+            for (int a = 0; a < SMAX; ++a) {
+                if (a >= off) {
+                    const int hb = H1[a];
+                    const int hn = max(hb, f);
+                    changed |= hn != hb;
+                    H1[a] = hn;
+                    f = U8 ? max(f - e_ins, 0) : sat16(f - e_ins);
+                }
+            }
+            if (!__any_sync(gmask, changed)) break;
+        }
+        const int imax = (int)__reduce_max_sync(gmask, (unsigned)mx);
+        if ((uint32_t)imax >= minsc) {
+            if (nb == 0 || last_row + 1 != i) {
+                if (nb < bcap) {
+                    if (l == 0) blist[nb] = (uint32_t)imax << 16 | (uint32_t)i;
+                } else {
+                    status |= ST_BLIST;
+                }
+                ++nb;
+                last_row = i;
+                last_sc = imax;
+            } else if (last_sc < imax) {
+                if (l == 0 && nb - 1 < bcap) blist[nb - 1] = (uint32_t)imax << 16 | (uint32_t)i;
+                last_row = i;
+                last_sc = imax;
+            }
+        }
+        if (imax > gmax) {
+            gmax = imax;
+            te = i;
+#pragma unroll
+            for (int a = 0; a < SMAX; ++a) Hm[a] = H1[a];
+            const bool sat = U8 ? (gmax + shift >= 255) : (gmax >= 0x7FFF);
+            if (sat || (uint32_t)gmax >= endsc) break;
+        }
+#pragma unroll
+        for (int a = 0; a < SMAX; ++a) H0[a] = H1[a];
+    }
+    if (bad) status |= ST_BAD_CODE;
+
+    fa_kswr r;
+    r.score = U8 ? (gmax + shift < 255 ? gmax : 255) : gmax;
+    r.te = te;
+    r.qe = -1; r.score2 = -1; r.te2 = -1; r.tb = -1; r.qb = -1;
+    if (r.score != (U8 ? 255 : 0x7FFF)) {
+        // query end: smallest position holding the largest sign-interpreted lane value
+        int bv = -1, bk = -1;
+#pragma unroll
+        for (int a = 0; a < SMAX; ++a) {
+            if (a >= off) {
+                const int k = (a - off) + l * slen;
+                if (k < qlen) {
+                    const int v = U8 ? (int)(int8_t)(uint8_t)Hm[a] : (int)(int16_t)Hm[a];
+                    if (v > bv) { bv = v; bk = k; }
+                }
+            }
+        }
+        const int gv = __reduce_max_sync(gmask, bv);
+        r.qe = __reduce_min_sync(gmask, bv == gv ? bk : INT_MAX);
+        if (r.qe == INT_MAX) r.qe = -1;
+        if (nb > 0) {
+            __syncwarp(gmask);
+            const int iv = (r.score + p.max - 1) / p.max;
+            const int low = te - iv, high = te + iv;
+            const int cnt = nb < bcap ? nb : bcap;
+            int s2 = -1, e2 = INT_MAX;
+            for (int e = l; e < cnt; e += P) {
+                const uint32_t b = blist[e];
+                const int row = (int)(b & 0xffffu), sc = (int)(b >> 16);
+                if ((row < low || row > high) && sc > s2) { s2 = sc; e2 = e; }
+            }
+            const int gs2 = __reduce_max_sync(gmask, s2);
+            const int ge2 = __reduce_min_sync(gmask, s2 == gs2 ? e2 : INT_MAX);
+            if (gs2 >= 0 && ge2 != INT_MAX) {
+                r.score2 = gs2;
+                r.te2 = (int)(blist[ge2] & 0xffffu);
+            }
+            __syncwarp(gmask);
+        }
+    }
+    return r;
+}
+
+template <int P, int SMAX>
+__global__ void __launch_bounds__(kMateThreads)
+mate_sw_kernel(const fa_mate_job *__restrict__ jobs, const uint32_t *__restrict__ order, uint32_t n,
+               const uint8_t *__restrict__ qseq, const uint8_t *__restrict__ tseq, const MateParams p,
+               int bcap, fa_kswr *__restrict__ out, unsigned long long *__restrict__ cells_out,
+               uint32_t *__restrict__ status)
+{
+    extern __shared__ uint32_t bsm[];
+    const uint32_t gtid = blockIdx.x * kMateThreads + threadIdx.x;
+    const uint32_t gidx = gtid / P;
+    const int lane = threadIdx.x & 31;
+    const int l = lane % P;
+    const uint32_t gmask = (P == 32 ? 0xffffffffu : ((1u << P) - 1u)) << (lane - l);
+    unsigned long long cells = 0;
+    uint32_t st = 0;
+    if (gidx < n) {
+        const uint32_t jid = order ? order[gidx] : gidx;
+        const fa_mate_job jb = jobs[jid];
+        uint32_t *blist = bsm + (threadIdx.x / P) * bcap;
+        SeqView Q{qseq + jb.q_off, -1}, Tg{tseq + jb.t_off, -1};
+        fa_kswr r = sw_pass<P, SMAX>(Q, jb.qlen, Tg, jb.tlen, jb.xtra, p, gmask, l, blist, bcap,
+                                     cells, st);
+        const uint32_t xtra = jb.xtra;
+        const bool find_start = (xtra & FA_KSW_XSTART) &&
+                                !((xtra & FA_KSW_XSUBO) && r.score < (int)(xtra & 0xffffu));
+        if (find_start && r.qe >= 0 && r.te >= 0) {
+            SeqView Q2{qseq + jb.q_off, r.qe}, T2{tseq + jb.t_off, r.te};
+            const fa_kswr rr = sw_pass<P, SMAX>(Q2, r.qe + 1, T2, jb.tlen,
+                                                FA_KSW_XSTOP | (uint32_t)r.score, p, gmask, l,
+                                                blist, bcap, cells, st);
+            if (rr.score >= r.score) { r.tb = r.te - rr.te; r.qb = r.qe - rr.qe; }
+        }
+        st = __reduce_or_sync(gmask, st);
+        if (l == 0) {
+            out[jid] = r;
+            if (st) atomicOr(status, st);
+        } else {
+            cells = 0;
+        }
+    }
+    if (cells_out) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) cells += __shfl_down_sync(0xffffffffu, cells, o);
+        if (lane == 0 && cells) atomicAdd(cells_out, cells);
+    }
+}
+
+template <int P, int SMAX>
+static cudaError_t launch_mate_t(const fa_mate_job *d_jobs, const uint32_t *d_order, uint32_t n,
+                                 const uint8_t *d_qseq, const uint8_t *d_tseq, const MateParams &p,
+                                 int bcap, fa_kswr *d_out, unsigned long long *d_cells,
+                                 uint32_t *d_status, cudaStream_t stream)
+{
+    const size_t smem = (size_t)(kMateThreads / P) * bcap * sizeof(uint32_t);
+    cudaError_t err = cudaFuncSetAttribute(mate_sw_kernel<P, SMAX>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return err;
+    const uint64_t threads = (uint64_t)n * P;
+    const uint32_t blocks = (uint32_t)((threads + kMateThreads - 1) / kMateThreads);
+    mate_sw_kernel<P, SMAX><<<blocks, kMateThreads, smem, stream>>>(d_jobs, d_order, n, d_qseq, d_tseq,
+                                                                    p, bcap, d_out, d_cells, d_status);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mate_sw(bool byte_lanes, const fa_mate_job *d_jobs, const uint32_t *d_order,
+                           uint32_t n, const uint8_t *d_qseq, const uint8_t *d_tseq,
+                           const MateParams &p, int max_qlen, int max_tlen, fa_kswr *d_out,
+                           unsigned long long *d_cells, uint32_t *d_status, cudaStream_t stream)
+{
+    if (n == 0) return cudaSuccess;
+    const int bcap = (max_tlen + 1) / 2 + 2;   // consecutive list rows differ by >= 2
+    if (byte_lanes) {
+        if (max_qlen <= 16 * 16)
+            return launch_mate_t<16, 16>(d_jobs, d_order, n, d_qseq, d_tseq, p, bcap, d_out, d_cells, d_status, stream);
+        return launch_mate_t<16, 32>(d_jobs, d_order, n, d_qseq, d_tseq, p, bcap, d_out, d_cells, d_status, stream);
+    }
+    if (max_qlen <= 8 * 16)
+        return launch_mate_t<8, 16>(d_jobs, d_order, n, d_qseq, d_tseq, p, bcap, d_out, d_cells, d_status, stream);
+    return launch_mate_t<8, 32>(d_jobs, d_order, n, d_qseq, d_tseq, p, bcap, d_out, d_cells, d_status, stream);
+}
+
+}  // namespace fa

@@ -1,0 +1,76 @@
+// probe_kernel.cu -- integer / DPX instruction-throughput probe.
+//
+// The roofline of the DP kernels is the SM integer pipe, for which no measured peak
+// exists on this hardware; this probe measures it.  Each thread keeps 8 independent
+// accumulator chains and applies one instruction kind per step, so the issue rate,
+// not latency, bounds the run.
+
+#include <cstdio>
+
+#include "fa_kernels.h"
+
+namespace fa {
+
+template <int KIND>
+__global__ void __launch_bounds__(256) probe_kernel(uint32_t b, uint32_t c, int iters, uint32_t *sink)
+{
+    uint32_t acc[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) acc[k] = threadIdx.x * 2654435761u + k * 40503u + blockIdx.x;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (KIND == 0) acc[k] = __viaddmax_s16x2_relu(acc[k], b, c);
+            else if (KIND == 1) acc[k] = __vimax3_s16x2_relu(acc[k], b, c);
+            else if (KIND == 2) acc[k] = (uint32_t)__viaddmax_s32_relu((int)acc[k], (int)b, (int)c);
+            else if (KIND == 3) acc[k] = (uint32_t)__vimax3_s32((int)acc[k], (int)b, (int)c);
+            else acc[k] = (uint32_t)max((int)acc[k] + (int)b, (int)c);
+        }
+        b ^= acc[it & 7] & 1u;   // keeps the operands live without a long dependency
+    }
+    uint32_t x = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x ^= acc[k];
+    if (x == 0x9e3779b9u) sink[0] = x;
+}
+
+// ops/s for one instruction kind (0: viaddmax_s16x2_relu, 1: vimax3_s16x2_relu,
+// 2: viaddmax_s32_relu, 3: vimax3_s32, 4: add+max as two plain instructions).
+double probe_int_peak(int kind, int sm_count, cudaStream_t s, float *ms_out)
+{
+    uint32_t *sink = nullptr;
+    if (cudaMalloc(&sink, 4) != cudaSuccess) return -1.0;
+    const int iters = 4096, threads = 256, blocks = sm_count * 8;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    auto launch = [&]() {
+        switch (kind) {
+            case 0: probe_kernel<0><<<blocks, threads, 0, s>>>(0x00010001u, 0x00020002u, iters, sink); break;
+            case 1: probe_kernel<1><<<blocks, threads, 0, s>>>(0x00010001u, 0x00020002u, iters, sink); break;
+            case 2: probe_kernel<2><<<blocks, threads, 0, s>>>(1u, 2u, iters, sink); break;
+            case 3: probe_kernel<3><<<blocks, threads, 0, s>>>(1u, 2u, iters, sink); break;
+            default: probe_kernel<4><<<blocks, threads, 0, s>>>(1u, 2u, iters, sink); break;
+        }
+    };
+    for (int w = 0; w < 3; ++w) launch();
+    float best = 1e30f;
+    for (int r = 0; r < 5; ++r) {
+        cudaEventRecord(e0, s);
+        launch();
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) best = ms;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(sink);
+    if (cudaGetLastError() != cudaSuccess) return -1.0;
+    if (ms_out) *ms_out = best;
+    const double ops = (double)blocks * threads * iters * 8.0 * (kind == 4 ? 2.0 : 1.0);
+    return ops / (best * 1e-3);
+}
+
+}  // namespace fa

@@ -1,0 +1,100 @@
+"""Mate-rescue local Smith-Waterman over the B200 kernels.
+
+Mirrors ``execute_mate_rescue_batch_with_engine``
+(src/pipelines/linear/paired/mate_rescue.rs:595-685): one ``ksw_align2`` per job with
+the reference's flags (XSUBO | XSTART | XBYTE when mate_len * match_score < 250, and
+min_seed_len * match_score as the sub-optimal threshold), the rescue scoring matrix
+(mate_rescue.rs:116-122: match 1, mismatch -4, N 0) and gaps 6/1.  Results are
+``Kswr`` records (src/core/alignment/ksw_affine_gap.rs:51-61) in job order.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native as N
+
+MATE_RESCUE_SCORING_MATRIX = np.array([
+    1, -4, -4, -4, 0,
+    -4, 1, -4, -4, 0,
+    -4, -4, 1, -4, 0,
+    -4, -4, -4, 1, 0,
+    0, 0, 0, 0, 0], dtype=np.int8)
+
+
+@dataclass
+class Kswr:
+    score: int
+    te: int
+    qe: int
+    score2: int
+    te2: int
+    tb: int
+    qb: int
+
+
+@dataclass
+class MateRescueJob:
+    """The fields of mate_rescue.rs:37-64 that the SW call consumes."""
+    query_seq: bytes
+    ref_seq: bytes
+    mate_len: int
+    min_seed_len: int = 19
+    match_score: int = 1
+    pair_index: int = 0
+    extra: dict = field(default_factory=dict)
+
+
+@dataclass
+class MateRescueResult:
+    job_index: int
+    aln: Kswr
+
+
+def mate_xtra(mate_len: int, match_score: int, min_seed_len: int) -> int:
+    """mate_rescue.rs:314-321"""
+    x = N.KSW_XSUBO | N.KSW_XSTART
+    if mate_len * match_score < 250:
+        x |= N.KSW_XBYTE
+    return x | (min_seed_len * match_score)
+
+
+def make_mate_params(mat=MATE_RESCUE_SCORING_MATRIX, o_del=6, e_del=1, o_ins=6, e_ins=1) -> np.ndarray:
+    p = np.zeros(1, dtype=N.MATE_PARAMS_DT)
+    p["mat"][0] = np.asarray(mat, dtype=np.int8).reshape(25)
+    p["m"] = 5
+    p["o_del"], p["e_del"], p["o_ins"], p["e_ins"] = o_del, e_del, o_ins, e_ins
+    return p
+
+
+def mate_sw_batch(params: np.ndarray, jobs: np.ndarray, qseq: np.ndarray, tseq: np.ndarray,
+                  ctx: N.Context | None = None):
+    """Array-level call of fa_mate_sw_batch.  Returns (kswr records, stats)."""
+    lib = N.load()
+    ctx = ctx or N.default_context()
+    jobs = np.ascontiguousarray(jobs, dtype=N.MATE_JOB_DT)
+    qseq = np.ascontiguousarray(qseq, dtype=np.uint8)
+    tseq = np.ascontiguousarray(tseq, dtype=np.uint8)
+    out = np.zeros(len(jobs), dtype=N.KSWR_DT)
+    stats = np.zeros(1, dtype=N.STATS_DT)
+    N.check(lib.fa_mate_sw_batch(ctx.handle, N.ptr(params), N.ptr(jobs), len(jobs), N.ptr(qseq), qseq.nbytes,
+                                 N.ptr(tseq), tseq.nbytes, N.ptr(out), N.ptr(stats)))
+    return out, stats[0]
+
+
+def execute_mate_rescue_batch_with_engine(jobs: list[MateRescueJob], engine=None) -> list[MateRescueResult]:
+    """mate_rescue.rs:595-637.  ``engine`` is accepted for signature compatibility."""
+    if not jobs:
+        return []
+    arr = np.zeros(len(jobs), dtype=N.MATE_JOB_DT)
+    qb, tb = bytearray(), bytearray()
+    for i, j in enumerate(jobs):
+        q, t = bytes(bytearray(j.query_seq)), bytes(bytearray(j.ref_seq))
+        arr[i] = (len(qb), len(tb), j.mate_len, len(t), mate_xtra(j.mate_len, j.match_score, j.min_seed_len), 0)
+        qb += q[:j.mate_len]
+        tb += t
+    q = np.frombuffer(bytes(qb), dtype=np.uint8) if qb else np.zeros(1, np.uint8)
+    t = np.frombuffer(bytes(tb), dtype=np.uint8) if tb else np.zeros(1, np.uint8)
+    out, _ = mate_sw_batch(make_mate_params(), arr, q, t)
+    return [MateRescueResult(i, Kswr(*(int(v) for v in o))) for i, o in enumerate(out)]

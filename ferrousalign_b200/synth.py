@@ -1,0 +1,160 @@
+"""Seeded synthetic workloads (ctypes binding of libfa_synth.so).
+
+Named workloads:
+  ext_plain        10,000 right extensions: 1 Mbp i.i.d. reference with 0.1% N, 151 bp reads,
+                   1% substitutions, 0.1% indels (geometric, mean 2), seed 19-51 bp at the
+                   read start, h0 = seed length, target = suffix length + w, w = 100.
+  ext_1m           1,000,000 right extensions from the same generator, per-read indel rate
+                   drawn from {0, 0.1%, 1%, 3%}.
+  ext_uneven       2,000,000 mixed left+right extensions, reads 50-300 bp, seed position
+                   uniform, 100 Mbp reference with 5% dinucleotide-repeat tracts.
+  ext_train        the ext_1m generator with a 3% indel-rate mixture (band-model training).
+  mate_rescue      500,000 2x151 bp pairs, insert ~ N(400, 50); the mate's window covers
+                   mean +- 4 sd plus the read length (551 bp).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+from . import _native as N
+
+LIB_PATH = Path(__file__).resolve().parent / "libfa_synth.so"
+
+EXT_INFO_DT = np.dtype([("seed_len", "<i4"), ("diag_spread", "<i4"), ("has_partner", "<i4"),
+                        ("read_idx", "<i4"), ("indel_rate_ppm", "<i4"), ("_pad", "<i4")])
+
+
+class ExtCfg(C.Structure):
+    _fields_ = [("read_len_min", C.c_int32), ("read_len_max", C.c_int32),
+                ("seed_len_min", C.c_int32), ("seed_len_max", C.c_int32),
+                ("seed_at_start", C.c_int32), ("w", C.c_int32), ("match_score", C.c_int32),
+                ("n_indel_rates", C.c_int32), ("indel_rates", C.c_double * 4),
+                ("sub_rate", C.c_double), ("indel_mean", C.c_double)]
+
+
+class MateCfg(C.Structure):
+    _fields_ = [("read_len", C.c_int32), ("match_score", C.c_int32), ("min_seed_len", C.c_int32),
+                ("_pad", C.c_int32), ("insert_mean", C.c_double), ("insert_sd", C.c_double),
+                ("sub_rate", C.c_double), ("indel_rate", C.c_double)]
+
+
+_lib = None
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} missing: run ferrousalign_b200.build.build_all()")
+        lib = C.CDLL(str(LIB_PATH))
+        lib.fa_synth_reference.restype = C.c_int
+        lib.fa_synth_reference.argtypes = [C.c_uint64, C.c_uint64, C.c_double, C.c_double, C.c_void_p]
+        lib.fa_synth_ext_jobs.restype = C.c_int64
+        lib.fa_synth_ext_jobs.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, C.POINTER(ExtCfg), C.c_uint32,
+                                          C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p,
+                                          C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+        lib.fa_synth_mate_jobs.restype = C.c_int64
+        lib.fa_synth_mate_jobs.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, C.POINTER(MateCfg), C.c_uint32,
+                                           C.c_int, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64,
+                                           C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+        _lib = lib
+    return _lib
+
+
+def reference(length: int, seed: int = 1, n_rate: float = 0.001, repeat_frac: float = 0.0) -> np.ndarray:
+    out = np.empty(length, dtype=np.uint8)
+    rc = _load().fa_synth_reference(seed, length, n_rate, repeat_frac, out.ctypes.data)
+    if rc:
+        raise RuntimeError(f"fa_synth_reference failed ({rc})")
+    return out
+
+
+@dataclass
+class ExtBatch:
+    jobs: np.ndarray     # JOB_DT
+    qseq: np.ndarray     # uint8 codes
+    tseq: np.ndarray
+    info: np.ndarray     # EXT_INFO_DT
+
+
+def ext_jobs(ref: np.ndarray, n: int, seed: int = 7, read_len=(151, 151), seed_len=(19, 51),
+             seed_at_start=True, w=100, match_score=1, indel_rates=(0.001,), sub_rate=0.01,
+             indel_mean=2.0, threads: int = 0) -> ExtBatch:
+    cfg = ExtCfg()
+    cfg.read_len_min, cfg.read_len_max = read_len
+    cfg.seed_len_min, cfg.seed_len_max = seed_len
+    cfg.seed_at_start = int(seed_at_start)
+    cfg.w, cfg.match_score = w, match_score
+    cfg.n_indel_rates = len(indel_rates)
+    for i, r in enumerate(indel_rates):
+        cfg.indel_rates[i] = r
+    cfg.sub_rate, cfg.indel_mean = sub_rate, indel_mean
+    jobs = np.zeros(n, dtype=N.JOB_DT)
+    info = np.zeros(n, dtype=EXT_INFO_DT)
+    qcap = n * read_len[1]
+    tcap = n * (read_len[1] + w)
+    q = np.empty(max(qcap, 1), dtype=np.uint8)
+    t = np.empty(max(tcap, 1), dtype=np.uint8)
+    qu, tu = C.c_uint64(), C.c_uint64()
+    got = _load().fa_synth_ext_jobs(ref.ctypes.data, len(ref), seed, C.byref(cfg), n, threads, jobs.ctypes.data,
+                                    info.ctypes.data, q.ctypes.data, qcap, t.ctypes.data, tcap, C.byref(qu),
+                                    C.byref(tu))
+    if got != n:
+        raise RuntimeError(f"fa_synth_ext_jobs produced {got} of {n} jobs")
+    return ExtBatch(jobs, q[:max(qu.value, 1)].copy(), t[:max(tu.value, 1)].copy(), info)
+
+
+@dataclass
+class MateBatch:
+    jobs: np.ndarray     # MATE_JOB_DT
+    qseq: np.ndarray
+    tseq: np.ndarray
+
+
+def mate_jobs(ref: np.ndarray, n: int, seed: int = 11, read_len=151, insert_mean=400.0, insert_sd=50.0,
+              sub_rate=0.01, indel_rate=0.001, match_score=1, min_seed_len=19, threads: int = 0) -> MateBatch:
+    cfg = MateCfg()
+    cfg.read_len, cfg.match_score, cfg.min_seed_len = read_len, match_score, min_seed_len
+    cfg.insert_mean, cfg.insert_sd, cfg.sub_rate, cfg.indel_rate = insert_mean, insert_sd, sub_rate, indel_rate
+    tcap_one = int(8 * insert_sd) + read_len + 8
+    jobs = np.zeros(n, dtype=N.MATE_JOB_DT)
+    q = np.empty(max(n * read_len, 1), dtype=np.uint8)
+    t = np.empty(max(n * tcap_one, 1), dtype=np.uint8)
+    qu, tu = C.c_uint64(), C.c_uint64()
+    got = _load().fa_synth_mate_jobs(ref.ctypes.data, len(ref), seed, C.byref(cfg), n, threads, jobs.ctypes.data,
+                                     q.ctypes.data, q.nbytes, t.ctypes.data, t.nbytes, C.byref(qu), C.byref(tu))
+    if got != n:
+        raise RuntimeError(f"fa_synth_mate_jobs produced {got} of {n} jobs")
+    return MateBatch(jobs, q[:max(qu.value, 1)].copy(), t[:max(tu.value, 1)].copy())
+
+
+# ---- named workloads --------------------------------------------------------
+
+def workload_ext_plain(n: int = 10_000, seed: int = 1) -> ExtBatch:
+    ref = reference(1_000_000, seed=seed, n_rate=0.001)
+    return ext_jobs(ref, n, seed=seed + 100, indel_rates=(0.001,))
+
+
+def workload_ext_1m(n: int = 1_000_000, seed: int = 2, ref_len: int = 1_000_000) -> ExtBatch:
+    ref = reference(ref_len, seed=seed, n_rate=0.001)
+    return ext_jobs(ref, n, seed=seed + 100, indel_rates=(0.0, 0.001, 0.01, 0.03))
+
+
+def workload_ext_uneven(n: int = 2_000_000, seed: int = 3, ref_len: int = 100_000_000) -> ExtBatch:
+    ref = reference(ref_len, seed=seed, n_rate=0.001, repeat_frac=0.05)
+    return ext_jobs(ref, n, seed=seed + 100, read_len=(50, 300), seed_at_start=False,
+                    indel_rates=(0.001,))
+
+
+def workload_ext_train(n: int = 5_000_000, seed: int = 4) -> ExtBatch:
+    ref = reference(1_000_000, seed=seed, n_rate=0.001)
+    return ext_jobs(ref, n, seed=seed + 100, indel_rates=(0.0, 0.001, 0.01, 0.03))
+
+
+def workload_mate(n: int = 500_000, seed: int = 5, ref_len: int = 10_000_000) -> MateBatch:
+    ref = reference(ref_len, seed=seed, n_rate=0.001)
+    return mate_jobs(ref, n, seed=seed + 100)

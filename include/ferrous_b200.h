@@ -1,0 +1,192 @@
+/*
+ * ferrous_b200.h -- C ABI of the B200 seed-extension / mate-rescue library.
+ *
+ * Every entry point takes plain pointers and sizes.  Sequences are byte codes
+ * A=0 C=1 G=2 T=3 N=4 (classic_base_to_code, src/core/compute/encoding.rs:208),
+ * left-extension jobs already reversed by the caller, exactly as the reference
+ * hands them to its kernels (src/pipelines/linear/batch_extension/collect_soa.rs:150-209).
+ * Host buffers are owned by the caller; device buffers by the context.
+ * A context is used by one host thread at a time; create one per thread.
+ * All functions return FA_OK (0) or an FA_ERR_* code; fa_last_error() gives the
+ * message of the last failure on the calling thread.
+ */
+#ifndef FERROUS_B200_H
+#define FERROUS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FA_OK            0
+#define FA_ERR_ARG       1   /* malformed job or parameter (reference: panic)   */
+#define FA_ERR_CAPACITY  2   /* job exceeds a kernel limit or device memory     */
+#define FA_ERR_CUDA      3   /* CUDA runtime failure                            */
+#define FA_ERR_TIMEOUT   4   /* a bounded device wait ran out                   */
+#define FA_ERR_STATE     5   /* e.g. no band model loaded                       */
+
+/* Largest query / target lengths a job may have. */
+#define FA_MAX_QLEN  4096
+#define FA_MAX_TLEN  65535
+
+/* Scoring parameters: mirrors BandedPairWiseSW (src/core/alignment/banded_swa/types.rs:106-120).
+ * mat is row-major [target_base * 5 + query_base], as ksw_extend2 indexes it
+ * (ksw_affine_gap.rs:990-997, 1042). */
+typedef struct {
+    int8_t  mat[25];
+    int8_t  _pad[3];
+    int32_t m;          /* alphabet size; must be 5 */
+    int32_t o_del, e_del, o_ins, e_ins;
+    int32_t zdrop;
+    int32_t end_bonus;
+    int32_t pen_clip5, pen_clip3;   /* carried for the region merge; unused by the DP */
+} fa_params;
+
+#define FA_DIR_LEFT  0
+#define FA_DIR_RIGHT 1
+
+/* One extension job: mirrors BatchedExtensionJob (batch_extension/types.rs:20-41)
+ * without the read/chain/seed ids, which the caller keeps (results come back in
+ * job order). */
+typedef struct {
+    uint64_t q_off;     /* offset of the query in the query buffer   */
+    uint64_t t_off;     /* offset of the target in the target buffer */
+    int32_t  qlen;      /* query_len                                  */
+    int32_t  tlen;      /* ref_len                                    */
+    int32_t  h0;        /* initial score; must be > 0 (ksw_affine_gap.rs:968) */
+    int32_t  w;         /* band_width                                 */
+    int32_t  dir;       /* FA_DIR_LEFT / FA_DIR_RIGHT                 */
+    int32_t  _pad;
+} fa_job;
+
+/* KswExtendResult (ksw_affine_gap.rs:902-916), same field order. */
+typedef struct {
+    int32_t score, qle, tle, gtle, gscore, max_off;
+} fa_ext_result;
+
+/* Band-retry policies.
+ * FA_POLICY_SINGLE : one ksw_extend2 run at job.w (what execute_batch_simd_scoring returns).
+ * FA_POLICY_BWA    : bwa-mem2 mem_chain2aln: try w << k for k < max_tries; stop when the
+ *                    score equals the previous try's (first "previous" = 0 for left jobs,
+ *                    h0 for right jobs) or max_off < (w>>1)+(w>>2).
+ * FA_POLICY_LEARNED: start at w_first[i] (from the band model or the caller), double up to
+ *                    job.w; accept a narrow run per `judge`; at job.w continue as FA_POLICY_BWA. */
+#define FA_POLICY_SINGLE  0
+#define FA_POLICY_BWA     1
+#define FA_POLICY_LEARNED 2
+
+#define FA_JUDGE_CERT    1  /* accept a narrow run only when its band clamp never bound (sound) */
+#define FA_JUDGE_MAXOFF  2  /* also accept when max_off < (w>>1)+(w>>2) (the bwa-mem2 test)    */
+
+typedef struct {
+    int32_t mode;
+    int32_t max_tries;   /* bwa-mem2 MAX_BAND_TRY = 2 */
+    int32_t judge;       /* FA_JUDGE_* for FA_POLICY_LEARNED */
+    int32_t w_min;       /* smallest band the learned path may start at */
+} fa_policy;
+
+typedef struct {
+    uint64_t cells;          /* sum of (end-beg) of the final accepted runs      */
+    uint64_t cells_executed; /* every row range actually computed, retries incl. */
+    uint32_t jobs;
+    uint32_t retries;        /* extra runs beyond the first, summed over jobs    */
+    uint32_t misses;         /* learned path: jobs whose first narrow run failed */
+    uint32_t kernel_launches;
+    float    kernel_ms;      /* device time of the DP kernels                    */
+    float    total_ms;       /* wall time of the call                            */
+} fa_ext_stats;
+
+/* Mate-rescue local SW: ksw_align2 flags (ksw_affine_gap.rs:17-21). */
+#define FA_KSW_XBYTE  0x10000u
+#define FA_KSW_XSTOP  0x20000u
+#define FA_KSW_XSUBO  0x40000u
+#define FA_KSW_XSTART 0x80000u
+
+typedef struct {
+    int8_t  mat[25];
+    int8_t  _pad[3];
+    int32_t m;                  /* must be 5 */
+    int32_t o_del, e_del, o_ins, e_ins;
+} fa_mate_params;
+
+typedef struct {
+    uint64_t q_off, t_off;
+    int32_t  qlen, tlen;
+    uint32_t xtra;              /* ksw_align2 xtra word */
+    int32_t  _pad;
+} fa_mate_job;
+
+/* Kswr (ksw_affine_gap.rs:51-61), same field order. */
+typedef struct {
+    int32_t score, te, qe, score2, te2, tb, qb;
+} fa_kswr;
+
+typedef struct fa_ctx fa_ctx;
+
+/* ---- context ---------------------------------------------------------- */
+int         fa_ctx_create(int device, fa_ctx **out);
+void        fa_ctx_destroy(fa_ctx *ctx);
+const char *fa_last_error(void);
+const char *fa_version(void);
+
+/* Diagnostics (no reference counterpart): SM count / opt-in shared memory of the
+ * context's device, and the measured throughput of one integer instruction kind
+ * (0: __viaddmax_s16x2_relu, 1: __vimax3_s16x2_relu, 2: __viaddmax_s32_relu,
+ *  3: __vimax3_s32, 4: add + max as two instructions), used as the roofline peak. */
+int fa_device_info(fa_ctx *ctx, int *sm_count, int *smem_optin_bytes);
+int fa_probe_int_peak(fa_ctx *ctx, int kind, double *ops_per_s, float *ms);
+
+/* xtra word the reference builds for a mate-rescue job
+ * (src/pipelines/linear/paired/mate_rescue.rs:314-321, 653-659). */
+uint32_t fa_mate_xtra(int32_t mate_len, int32_t match_score, int32_t min_seed_len);
+
+/* ---- seed extension ----------------------------------------------------
+ * Replaces execute_batch_simd_scoring (src/pipelines/linear/batch_extension/dispatch.rs:31-86):
+ * one result per job, in job order.  Host buffers; copies in and out inside the call.
+ * qseq/tseq hold qseq_len/tseq_len bytes; every job's range must lie inside them. */
+int fa_ext_batch(fa_ctx *ctx, const fa_params *p, const fa_job *jobs, uint32_t n,
+                 const uint8_t *qseq, uint64_t qseq_len,
+                 const uint8_t *tseq, uint64_t tseq_len,
+                 fa_ext_result *out, fa_ext_stats *stats);
+
+/* Same, with a band-retry policy.  w_first may be NULL (then the loaded band model
+ * predicts it for FA_POLICY_LEARNED).  w_final (may be NULL) receives the band of
+ * the accepted run per job. */
+int fa_ext_batch_policy(fa_ctx *ctx, const fa_params *p, const fa_policy *pol,
+                        const fa_job *jobs, uint32_t n,
+                        const uint8_t *qseq, uint64_t qseq_len,
+                        const uint8_t *tseq, uint64_t tseq_len,
+                        const int32_t *w_first, fa_ext_result *out,
+                        int32_t *w_final, fa_ext_stats *stats);
+
+/* Device-resident variant (no reference counterpart): every pointer is device memory
+ * and the kernels run asynchronously on `stream` (a cudaStream_t, NULL = the
+ * context's stream) after one small synchronous read of the query-length histogram.
+ * d_order (may be NULL) is a permutation of [0,n) giving the processing order; when
+ * NULL the jobs are ordered longest-first on the device.  Results are written at the
+ * job's own index.  Job ranges must lie inside the sequence buffers (not checked);
+ * argument and capacity violations found by the kernels are reported by the next
+ * fa_ctx_sync(). */
+int fa_ext_batch_device(fa_ctx *ctx, const fa_params *p, const fa_job *d_jobs, uint32_t n,
+                        const uint8_t *d_qseq, const uint8_t *d_tseq,
+                        const uint32_t *d_order, fa_ext_result *d_out, void *stream);
+
+/* Waits for the context's stream and reports kernel-detected errors of the last
+ * device-resident call; fa_ctx_last_launches gives its kernel launch count. */
+int fa_ctx_sync(fa_ctx *ctx);
+int fa_ctx_last_launches(fa_ctx *ctx);
+
+/* ---- mate rescue -------------------------------------------------------
+ * Replaces the ksw_align2 calls of execute_mate_rescue_batch_with_engine
+ * (src/pipelines/linear/paired/mate_rescue.rs:595-685). */
+int fa_mate_sw_batch(fa_ctx *ctx, const fa_mate_params *p, const fa_mate_job *jobs, uint32_t n,
+                     const uint8_t *qseq, uint64_t qseq_len,
+                     const uint8_t *tseq, uint64_t tseq_len,
+                     fa_kswr *out, fa_ext_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FERROUS_B200_H */

@@ -1,0 +1,153 @@
+"""Extension kernel parity: the CUDA path through the C ABI against the CPU oracle,
+bit-exact on all six KswExtendResult fields."""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import ferrousalign_b200 as fa
+from ferrousalign_b200 import _native as N
+from ferrousalign_b200 import synth
+from oracle import ksw_oracle as O
+
+pytestmark = pytest.mark.gpu
+GOLD = Path(__file__).resolve().parent / "golden"
+
+
+def params_of(c):
+    p = np.zeros(1, N.PARAMS_DT)
+    p["mat"][0] = np.array(c["mat"], np.int8)
+    p["m"] = 5
+    for k in ("o_del", "e_del", "o_ins", "e_ins", "zdrop", "end_bonus"):
+        p[k] = c[k]
+    return p
+
+
+def one_job_arrays(q, t, h0, w):
+    jobs = np.zeros(1, N.JOB_DT)
+    jobs[0] = (0, 0, len(q), len(t), h0, w, 1, 0)
+    qa = np.array(q if len(q) else [0], np.uint8)
+    ta = np.array(t if len(t) else [0], np.uint8)
+    return jobs, qa, ta
+
+
+def diff_report(a, b):
+    bad = np.nonzero(a != b)[0]
+    return f"{len(bad)} mismatches, first {bad[:5]}: gpu={a[bad[:3]]} oracle={b[bad[:3]]}"
+
+
+@pytest.mark.parametrize("case", json.loads((GOLD / "ext_cases.json").read_text()), ids=lambda c: c["name"])
+def test_golden_case(ctx, case):
+    jobs, q, t = one_job_arrays(case["query"], case["target"], case["h0"], case["w"])
+    out, _, _ = fa.extend_batch(params_of(case), jobs, q, t, ctx=ctx)
+    assert list(out[0]) == case["expect"]
+
+
+def run_both(ctx, p, b, threads=0):
+    out, stats, _ = fa.extend_batch(p, b.jobs, b.qseq, b.tseq, ctx=ctx)
+    ref, tr = O.ext_batch(p, b.jobs, b.qseq, b.tseq, threads=threads)
+    return out, stats, ref, tr
+
+
+def test_plain_10k_bit_exact(ctx):
+    b = synth.workload_ext_plain(10_000)
+    p = fa.BandedPairWiseSW().to_struct()
+    out, stats, ref, tr = run_both(ctx, p, b)
+    assert np.array_equal(out, ref), diff_report(out, ref)
+    assert stats["cells"] == tr["cells"].sum()      # same visited-cell count as the oracle
+
+
+def test_indel_mixture_200k_bit_exact(ctx):
+    b = synth.workload_ext_1m(200_000)
+    p = fa.BandedPairWiseSW().to_struct()
+    out, stats, ref, tr = run_both(ctx, p, b)
+    assert np.array_equal(out, ref), diff_report(out, ref)
+    assert stats["cells"] == tr["cells"].sum()
+
+
+def test_uneven_left_right_bit_exact(ctx):
+    ref_seq = synth.reference(20_000_000, seed=3, n_rate=0.001, repeat_frac=0.05)
+    b = synth.ext_jobs(ref_seq, 60_000, seed=103, read_len=(50, 300), seed_at_start=False)
+    p = fa.BandedPairWiseSW().to_struct()
+    out, _, ref, _ = run_both(ctx, p, b)
+    assert np.array_equal(out, ref), diff_report(out, ref)
+
+
+@pytest.mark.parametrize("a,b_,n,gaps,w,zdrop,eb", [
+    (1, 4, -1, (6, 1, 6, 1), 100, 100, 5),
+    (2, 3, 0, (5, 2, 3, 1), 30, 40, 0),
+    (1, 1, -2, (0, 1, 0, 1), 10, 0, 5),
+    (3, 5, -1, (6, 1, 4, 3), 5, 20, 10),
+    (1, 4, -1, (4, 0, 4, 1), 50, 100, 5),
+])
+def test_parameter_sweep_bit_exact(ctx, a, b_, n, gaps, w, zdrop, eb):
+    ref_seq = synth.reference(500_000, seed=11, n_rate=0.01)
+    b = synth.ext_jobs(ref_seq, 20_000, seed=17, read_len=(30, 200), seed_len=(5, 40), w=w,
+                       indel_rates=(0.0, 0.01, 0.05), sub_rate=0.03)
+    sw = fa.BandedPairWiseSW(o_del=gaps[0], e_del=gaps[1], o_ins=gaps[2], e_ins=gaps[3], zdrop=zdrop,
+                             end_bonus=eb, mat=fa.bwa_fill_scmat(a, b_, n))
+    p = sw.to_struct()
+    out, _, ref, _ = run_both(ctx, p, b)
+    assert np.array_equal(out, ref), diff_report(out, ref)
+
+
+def test_policies_match_oracle(ctx):
+    b = synth.workload_ext_1m(30_000, seed=21)
+    p = fa.BandedPairWiseSW().to_struct()
+    pol = fa.make_policy(N.FA_POLICY_BWA, 2)
+    out, st, wfin = fa.extend_batch(p, b.jobs, b.qseq, b.tseq, policy=pol, ctx=ctx)
+    ref, rwfin, rtries, _ = O.ext_batch_policy(p, pol, b.jobs, b.qseq, b.tseq)
+    assert np.array_equal(out, ref), diff_report(out, ref)
+    assert np.array_equal(wfin, rwfin)
+    assert st["retries"] == (rtries - 1).sum()
+    rng = np.random.default_rng(5)
+    wf = rng.choice([5, 10, 20, 40], size=len(b.jobs)).astype(np.int32)
+    for judge in (N.FA_JUDGE_CERT, N.FA_JUDGE_CERT | N.FA_JUDGE_MAXOFF):
+        pol = fa.make_policy(N.FA_POLICY_LEARNED, 2, judge, 1)
+        out, st, wfin = fa.extend_batch(p, b.jobs, b.qseq, b.tseq, policy=pol, w_first=wf, ctx=ctx)
+        ref, rwfin, rtries, _ = O.ext_batch_policy(p, pol, b.jobs, b.qseq, b.tseq, wf)
+        assert np.array_equal(out, ref), diff_report(out, ref)
+        assert np.array_equal(wfin, rwfin)
+
+
+def test_reference_style_interface(ctx):
+    batch = fa.ExtensionJobBatch()
+    sw = fa.BandedPairWiseSW()
+    rng = np.random.default_rng(3)
+    for k in range(50):
+        q = rng.integers(0, 4, 80).astype(np.uint8)
+        t = np.concatenate([q, rng.integers(0, 4, 60).astype(np.uint8)])
+        batch.add_job(k, 0, 0, fa.ExtensionDirection.Right, q, t, 20, 100)
+    res = fa.execute_batch_simd_scoring(sw, batch)
+    assert len(res) == 50
+    for k, r in enumerate(res):
+        o, _ = O.ksw_extend2(batch.get_query_seq(k), batch.get_ref_seq(k), sw.mat, 6, 1, 6, 1, 100, 5, 100, 20)
+        assert (r.score, r.query_end, r.ref_end, r.gref_end, r.gscore, r.max_off) == tuple(o)
+        assert r.read_idx == k
+    assert fa.execute_batch_simd_scoring(sw, fa.ExtensionJobBatch()) == []
+
+
+def test_errors_are_reported(ctx):
+    p = fa.BandedPairWiseSW().to_struct()
+    jobs, q, t = one_job_arrays([0, 1, 2], [0, 1, 2], 0, 100)        # h0 = 0 panics in the reference
+    with pytest.raises(N.NativeError) as e:
+        fa.extend_batch(p, jobs, q, t, ctx=ctx)
+    assert e.value.code == N.FA_ERR_ARG
+    jobs, q, t = one_job_arrays([0, 7, 2], [0, 1, 2], 5, 100)        # code outside the alphabet
+    with pytest.raises(N.NativeError) as e:
+        fa.extend_batch(p, jobs, q, t, ctx=ctx)
+    assert e.value.code == N.FA_ERR_ARG
+    jobs, q, t = one_job_arrays([0, 1, 2], [0, 1, 2], 5, 100)
+    jobs["t_off"] = 10                                               # range outside the buffer
+    with pytest.raises(N.NativeError) as e:
+        fa.extend_batch(p, jobs, q, t, ctx=ctx)
+    assert e.value.code == N.FA_ERR_ARG
+    jobs, q, t = one_job_arrays([0] * 10, [0] * 10, 9000, 100)       # beyond the packed-column bound
+    with pytest.raises(N.NativeError) as e:
+        fa.extend_batch(p, jobs, q, t, ctx=ctx)
+    assert e.value.code == N.FA_ERR_CAPACITY
+    # the context stays usable after errors
+    jobs, q, t = one_job_arrays([0, 1, 2, 3], [0, 1, 2, 3], 10, 50)
+    out, _, _ = fa.extend_batch(p, jobs, q, t, ctx=ctx)
+    assert out[0]["qle"] == 4 and out[0]["tle"] == 4

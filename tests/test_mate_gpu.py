@@ -1,0 +1,68 @@
+"""Mate-rescue kernel parity: ksw_align2 semantics through the C ABI against the oracle."""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import ferrousalign_b200 as fa
+from ferrousalign_b200 import _native as N
+from ferrousalign_b200 import synth
+from oracle import ksw_oracle as O
+
+pytestmark = pytest.mark.gpu
+GOLD = Path(__file__).resolve().parent / "golden"
+
+
+def diff_report(a, b):
+    bad = np.nonzero(a != b)[0]
+    return f"{len(bad)} mismatches, first {bad[:5]}: gpu={a[bad[:3]]} oracle={b[bad[:3]]}"
+
+
+@pytest.mark.parametrize("case", json.loads((GOLD / "mate_cases.json").read_text()), ids=lambda c: c["name"])
+def test_golden_case(ctx, case):
+    p = fa.make_mate_params(case["mat"], case["o_del"], case["e_del"], case["o_ins"], case["e_ins"])
+    jobs = np.zeros(1, N.MATE_JOB_DT)
+    jobs[0] = (0, 0, len(case["query"]), len(case["target"]), case["xtra"], 0)
+    q = np.array(case["query"], np.uint8)
+    t = np.array(case["target"] if case["target"] else [0], np.uint8)
+    out, _ = fa.mate_sw_batch(p, jobs, q, t, ctx=ctx)
+    assert list(out[0]) == case["expect"]
+
+
+def test_mate_workload_bit_exact(ctx):
+    b = synth.workload_mate(20_000)
+    p = fa.make_mate_params()
+    out, stats = fa.mate_sw_batch(p, b.jobs, b.qseq, b.tseq, ctx=ctx)
+    ref, cells = O.mate_batch(p, b.jobs, b.qseq, b.tseq)
+    assert np.array_equal(out, ref), diff_report(out, ref)
+    assert stats["cells"] == cells.sum()
+
+
+def test_i16_lanes_and_random_flags_bit_exact(ctx):
+    ref_seq = synth.reference(2_000_000, seed=8, n_rate=0.005)
+    b = synth.mate_jobs(ref_seq, 4000, seed=9, read_len=200, insert_sd=30.0, sub_rate=0.03, indel_rate=0.01)
+    rng = np.random.default_rng(1)
+    flags = rng.choice([0, N.KSW_XSTART, N.KSW_XSUBO | N.KSW_XSTART | 19, N.KSW_XSUBO | 40, N.KSW_XBYTE,
+                        N.KSW_XBYTE | N.KSW_XSTART | N.KSW_XSUBO | 19], size=len(b.jobs))
+    b.jobs["xtra"] = flags.astype(np.uint32)
+    for mat in (fa.MATE_RESCUE_SCORING_MATRIX, fa.bwa_fill_scmat(2, 3, -1)):
+        p = fa.make_mate_params(mat, 5, 2, 4, 1)
+        out, _ = fa.mate_sw_batch(p, b.jobs, b.qseq, b.tseq, ctx=ctx)
+        ref, _ = O.mate_batch(p, b.jobs, b.qseq, b.tseq)
+        assert np.array_equal(out, ref), diff_report(out, ref)
+
+
+def test_reference_style_interface(ctx):
+    rng = np.random.default_rng(2)
+    jobs = []
+    for k in range(40):
+        q = rng.integers(0, 4, 151).astype(np.uint8)
+        t = np.concatenate([rng.integers(0, 4, 200), q, rng.integers(0, 4, 200)]).astype(np.uint8)
+        jobs.append(fa.MateRescueJob(q, t, 151))
+    res = fa.execute_mate_rescue_batch_with_engine(jobs)
+    for k, r in enumerate(res):
+        o = O.ksw_align2(jobs[k].query_seq, jobs[k].ref_seq, fa.MATE_RESCUE_SCORING_MATRIX, 6, 1, 6, 1,
+                         fa.mate_xtra(151, 1, 19))
+        assert (r.aln.score, r.aln.te, r.aln.qe, r.aln.score2, r.aln.te2, r.aln.tb, r.aln.qb) == tuple(o)
+    assert fa.execute_mate_rescue_batch_with_engine([]) == []
