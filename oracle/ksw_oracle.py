@@ -49,9 +49,14 @@ def _p(a):
     return None if a is None else a.ctypes.data
 
 
+def _codes(x):
+    if isinstance(x, (bytes, bytearray, memoryview)):
+        return np.frombuffer(bytes(x), dtype=np.uint8)
+    return np.ascontiguousarray(x, dtype=np.uint8)
+
+
 def ksw_extend2(query, target, mat, o_del, e_del, o_ins, e_ins, w, end_bonus, zdrop, h0):
-    q = np.ascontiguousarray(query, dtype=np.uint8)
-    t = np.ascontiguousarray(target, dtype=np.uint8)
+    q, t = _codes(query), _codes(target)
     m = np.ascontiguousarray(mat, dtype=np.int8)
     out = np.zeros(1, EXT_RESULT_DT)
     tr = np.zeros(1, TRACE_DT)
@@ -63,8 +68,7 @@ def ksw_extend2(query, target, mat, o_del, e_del, o_ins, e_ins, w, end_bonus, zd
 
 
 def ksw_align2(query, target, mat, o_del, e_del, o_ins, e_ins, xtra):
-    q = np.ascontiguousarray(query, dtype=np.uint8)
-    t = np.ascontiguousarray(target, dtype=np.uint8)
+    q, t = _codes(query), _codes(target)
     m = np.ascontiguousarray(mat, dtype=np.int8)
     out = np.zeros(1, KSWR_DT)
     cells = np.zeros(1, np.int64)
