@@ -58,7 +58,8 @@ SIGNATURES = {
                                       _P, _P, _P, _P]),
     "fa_ext_batch_device": (C.c_int, [_P, _P, _P, C.c_uint32, _P, _P, _P, _P, _P]),
     "fa_ctx_sync": (C.c_int, [_P]),
-    "fa_ctx_last_launches": (C.c_int, [_P]),
+    "fa_ctx_set_timing": (C.c_int, [_P, C.c_int]),
+    "fa_ctx_last_timing": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_int)]),
     "fa_mate_sw_batch": (C.c_int, [_P, _P, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64, _P, _P]),
 }
 

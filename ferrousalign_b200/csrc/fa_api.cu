@@ -74,6 +74,8 @@ struct fa_ctx {
     DevBuf jobs, order, qseq, tseq, out, clamped, cells_job, misc;
     DevBuf w_first, w_cur, prev, kk, w_final, tries, missed, list_a, list_b, hist;
     uint32_t last_launches = 0;
+    bool timing = false;
+    cudaEvent_t kev0 = nullptr, kev1 = nullptr;   // bracket the extension kernels of a device call
 };
 
 namespace {
@@ -328,6 +330,8 @@ void fa_ctx_destroy(fa_ctx *c) {
                       &c->misc, &c->w_first, &c->w_cur, &c->prev, &c->kk, &c->w_final, &c->tries,
                       &c->missed, &c->list_a, &c->list_b, &c->hist})
         b->release();
+    if (c->kev0) cudaEventDestroy(c->kev0);
+    if (c->kev1) cudaEventDestroy(c->kev1);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -456,12 +460,38 @@ int fa_ext_batch_device(fa_ctx *c, const fa_params *p, const fa_job *d_jobs, uin
         segs.assign(1, {n, std::max(0, segs.empty() ? 0 : segs.front().second)});
     }
     uint32_t b = 0;
+    if (c->timing) FA_CUDA(cudaEventRecord(c->kev0, s));
     for (auto &sg : segs) {
         FA_CUDA(launch_ext_packed(d_jobs, order + b, sg.first - b, nullptr, d_qseq, d_tseq, kp, sg.second,
                                   nullptr, d_out, nullptr, nullptr, nullptr, m.status, s));
         b = sg.first;
     }
+    if (c->timing) FA_CUDA(cudaEventRecord(c->kev1, s));
     c->last_launches = (uint32_t)segs.size() + (d_order ? 1u : 2u);
+    return FA_OK;
+}
+
+int fa_ctx_set_timing(fa_ctx *c, int enable) {
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    FA_CUDA(cudaSetDevice(c->device));
+    if (enable && !c->kev0) {
+        FA_CUDA(cudaEventCreate(&c->kev0));
+        FA_CUDA(cudaEventCreate(&c->kev1));
+    }
+    c->timing = enable != 0;
+    return FA_OK;
+}
+
+int fa_ctx_last_timing(fa_ctx *c, float *kernel_ms, int *launches) {
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    if (launches) *launches = (int)c->last_launches;
+    if (kernel_ms) {
+        *kernel_ms = 0.f;
+        if (c->timing && c->kev0) {
+            FA_CUDA(cudaEventSynchronize(c->kev1));
+            FA_CUDA(cudaEventElapsedTime(kernel_ms, c->kev0, c->kev1));
+        }
+    }
     return FA_OK;
 }
 
@@ -472,8 +502,6 @@ int fa_ctx_sync(fa_ctx *c) {
     if (c->misc.p) return read_status(c, c->stream);
     return FA_OK;
 }
-
-int fa_ctx_last_launches(fa_ctx *c) { return c ? (int)c->last_launches : -1; }
 
 int fa_mate_sw_batch(fa_ctx *c, const fa_mate_params *p, const fa_mate_job *jobs, uint32_t n,
                      const uint8_t *qseq, uint64_t qseq_len, const uint8_t *tseq, uint64_t tseq_len,

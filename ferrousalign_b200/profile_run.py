@@ -1,0 +1,39 @@
+"""One device-resident extension batch of the bench workload, for ncu captures.
+
+Usage: python -m ferrousalign_b200.profile_run [n_jobs] [probe]
+"""
+import ctypes
+import sys
+
+import numpy as np
+import torch
+
+import ferrousalign_b200 as fa
+from ferrousalign_b200 import _native as N, synth
+
+n = int(sys.argv[1]) if len(sys.argv) > 1 else 1_000_000
+b = synth.workload_ext_1m(n)
+p = fa.BandedPairWiseSW().to_struct()
+ctx = fa.Context(0)
+lib = N.load()
+dev = torch.device("cuda", 0)
+st = torch.cuda.Stream(dev)
+with torch.cuda.stream(st):
+    d_jobs = torch.from_numpy(b.jobs.view(np.uint8)).to(dev)
+    d_q = torch.from_numpy(b.qseq).to(dev)
+    d_t = torch.from_numpy(b.tseq).to(dev)
+    d_out = torch.empty(n * 6, dtype=torch.int32, device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    N.check(lib.fa_ext_batch_device(ctx.handle, N.ptr(p), d_jobs.data_ptr(), n, d_q.data_ptr(), d_t.data_ptr(),
+                                    None, d_out.data_ptr(), ctypes.c_void_p(st.cuda_stream)))
+    e1.record(st)
+st.synchronize()
+N.check(lib.fa_ctx_sync(ctx.handle))
+print("batch ms", e0.elapsed_time(e1))
+if len(sys.argv) > 2 and sys.argv[2] == "probe":
+    v, ms = ctypes.c_double(), ctypes.c_float()
+    for k, name in enumerate(["viaddmax_s16x2_relu", "vimax3_s16x2_relu", "viaddmax_s32_relu", "vimax3_s32",
+                              "add+max (2 instr)"]):
+        N.check(lib.fa_probe_int_peak(ctx.handle, k, ctypes.byref(v), ctypes.byref(ms)))
+        print(f"probe {name}: {v.value / 1e12:.2f} Tops/s")

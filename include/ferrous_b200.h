@@ -174,9 +174,15 @@ int fa_ext_batch_device(fa_ctx *ctx, const fa_params *p, const fa_job *d_jobs, u
                         const uint32_t *d_order, fa_ext_result *d_out, void *stream);
 
 /* Waits for the context's stream and reports kernel-detected errors of the last
- * device-resident call; fa_ctx_last_launches gives its kernel launch count. */
+ * device-resident call. */
 int fa_ctx_sync(fa_ctx *ctx);
-int fa_ctx_last_launches(fa_ctx *ctx);
+
+/* Kernel timing of device-resident calls (no reference counterpart): with timing on,
+ * fa_ext_batch_device brackets its extension kernels with CUDA events on the call's
+ * stream; fa_ctx_last_timing waits for them and returns their device time and the
+ * number of kernels the last call launched. */
+int fa_ctx_set_timing(fa_ctx *ctx, int enable);
+int fa_ctx_last_timing(fa_ctx *ctx, float *kernel_ms, int *launches);
 
 /* ---- mate rescue -------------------------------------------------------
  * Replaces the ksw_align2 calls of execute_mate_rescue_batch_with_engine
