@@ -20,6 +20,7 @@ FA_JUDGE_CERT, FA_JUDGE_MAXOFF = 1, 2
 FA_DIR_LEFT, FA_DIR_RIGHT = 0, 1
 KSW_XBYTE, KSW_XSTOP, KSW_XSUBO, KSW_XSTART = 0x10000, 0x20000, 0x40000, 0x80000
 FA_MAX_QLEN, FA_MAX_TLEN = 4096, 65535
+FA_NOALLOC_MAX_JOBS = 1 << 18
 
 PARAMS_DT = np.dtype([("mat", "i1", 25), ("_pad", "i1", 3), ("m", "<i4"), ("o_del", "<i4"),
                       ("e_del", "<i4"), ("o_ins", "<i4"), ("e_ins", "<i4"), ("zdrop", "<i4"),
@@ -60,6 +61,7 @@ SIGNATURES = {
     "fa_ctx_sync": (C.c_int, [_P]),
     "fa_ctx_set_timing": (C.c_int, [_P, C.c_int]),
     "fa_ctx_last_timing": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_int)]),
+    "fa_ext_batch_device_noalloc": (C.c_int, [_P, _P, C.c_uint32, _P, _P, _P, _P]),
     "fa_mate_sw_batch": (C.c_int, [_P, _P, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64, _P, _P]),
 }
 

@@ -65,6 +65,11 @@ int packed_qcap_limit(size_t smem_optin) {
 
 }  // namespace
 
+int fa::set_last_error(int code, const char *msg) {
+    g_err = msg ? msg : "";
+    return code;
+}
+
 struct fa_ctx {
     int device = 0;
     int sm_count = 0;

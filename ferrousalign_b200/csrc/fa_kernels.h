@@ -48,6 +48,9 @@ cudaError_t launch_qlen_hist(const fa_job *d_jobs, uint32_t n, uint32_t *d_hist,
 cudaError_t launch_qlen_scatter(const fa_job *d_jobs, uint32_t n, uint32_t *d_cursor, uint32_t *d_order,
                                 cudaStream_t s);
 
+// Records the calling thread's fa_last_error() message and returns `code` (fa_api.cu).
+int set_last_error(int code, const char *msg);
+
 // Integer / DPX instruction throughput (ops per second) for the roofline denominator.
 double probe_int_peak(int kind, int sm_count, cudaStream_t s, float *ms_out);
 

@@ -184,6 +184,24 @@ int fa_ctx_sync(fa_ctx *ctx);
 int fa_ctx_set_timing(fa_ctx *ctx, int enable);
 int fa_ctx_last_timing(fa_ctx *ctx, float *kernel_ms, int *launches);
 
+/* No reference counterpart.  Device-resident extension for callers that cannot
+ * allocate device memory (a pool allocator owns the device memory, a fixed memory
+ * budget, or an allocation-free latency path): same arguments and results as
+ * fa_ext_batch_device without the context, and no cudaMalloc/cudaFree or other
+ * allocation.  Its scratch (query-length histogram, job order, status word) lives in
+ * one file-scope device array of about 1 MiB that every GPU loading the library keeps
+ * until exit, so a call takes at most FA_NOALLOC_MAX_JOBS jobs (more -> FA_ERR_CAPACITY).
+ * It runs on the current device and on `stream` (a cudaStream_t; NULL = legacy default
+ * stream) and returns once the results are in d_out, reporting kernel-detected
+ * argument errors.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) and caches it; make that first call before any stream
+ * capture.  All calls share the one array: calls that overlap on the GPU (from several
+ * host threads or streams at once) race and must be serialised by the caller. */
+#define FA_NOALLOC_MAX_JOBS (1u << 18)
+int fa_ext_batch_device_noalloc(const fa_params *p, const fa_job *d_jobs, uint32_t n,
+                                const uint8_t *d_qseq, const uint8_t *d_tseq,
+                                fa_ext_result *d_out, void *stream);
+
 /* ---- mate rescue -------------------------------------------------------
  * Replaces the ksw_align2 calls of execute_mate_rescue_batch_with_engine
  * (src/pipelines/linear/paired/mate_rescue.rs:595-685). */
