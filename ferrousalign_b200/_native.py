@@ -18,6 +18,7 @@ FA_OK, FA_ERR_ARG, FA_ERR_CAPACITY, FA_ERR_CUDA, FA_ERR_TIMEOUT, FA_ERR_STATE = 
 FA_POLICY_SINGLE, FA_POLICY_BWA, FA_POLICY_LEARNED = 0, 1, 2
 FA_JUDGE_CERT, FA_JUDGE_MAXOFF = 1, 2
 FA_DIR_LEFT, FA_DIR_RIGHT = 0, 1
+FA_KERNEL_AUTO, FA_KERNEL_INT32, FA_KERNEL_INT16X2 = 0, 1, 2
 KSW_XBYTE, KSW_XSTOP, KSW_XSUBO, KSW_XSTART = 0x10000, 0x20000, 0x40000, 0x80000
 FA_MAX_QLEN, FA_MAX_TLEN = 4096, 65535
 FA_NOALLOC_MAX_JOBS = 1 << 18
@@ -60,6 +61,7 @@ SIGNATURES = {
     "fa_ext_batch_device": (C.c_int, [_P, _P, _P, C.c_uint32, _P, _P, _P, _P, _P]),
     "fa_ctx_sync": (C.c_int, [_P]),
     "fa_ctx_set_timing": (C.c_int, [_P, C.c_int]),
+    "fa_ctx_set_kernel": (C.c_int, [_P, C.c_int]),
     "fa_ctx_last_timing": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_int)]),
     "fa_ext_batch_device_noalloc": (C.c_int, [_P, _P, C.c_uint32, _P, _P, _P, _P]),
     "fa_mate_sw_batch": (C.c_int, [_P, _P, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64, _P, _P]),
@@ -123,6 +125,9 @@ class Context:
         if self._h is None:
             raise RuntimeError("context closed")
         return self._h
+
+    def set_kernel(self, kernel: int) -> None:
+        check(load().fa_ctx_set_kernel(self.handle, kernel))
 
     def close(self) -> None:
         if self._h is not None:

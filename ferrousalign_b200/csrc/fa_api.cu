@@ -80,6 +80,7 @@ struct fa_ctx {
     DevBuf w_first, w_cur, prev, kk, w_final, tries, missed, list_a, list_b, hist;
     uint32_t last_launches = 0;
     bool timing = false;
+    int kernel = FA_KERNEL_AUTO;
     cudaEvent_t kev0 = nullptr, kev1 = nullptr;   // bracket the extension kernels of a device call
 };
 
@@ -94,6 +95,19 @@ struct Misc {
 Misc misc_of(fa_ctx *c) {
     char *b = c->misc.as<char>();
     return Misc{(uint32_t *)b, (unsigned long long *)(b + 8), (uint32_t *)(b + 16), (uint32_t *)(b + 20)};
+}
+
+// Extension launch: the int16x2 two-jobs-per-thread kernel for bwa-form matrices,
+// the int32 one-job-per-thread kernel otherwise.  Both are exact.
+cudaError_t launch_ext(int kernel, const fa_job *d_jobs, const uint32_t *d_order, uint32_t n,
+                       const uint32_t *d_n, const uint8_t *d_q, const uint8_t *d_t, const ExtParams &kp, int qcap,
+                       const int32_t *d_w_try, fa_ext_result *d_out, uint8_t *d_clamped, uint32_t *d_cells_job,
+                       unsigned long long *d_cells, uint32_t *d_status, cudaStream_t s) {
+    if (kernel != FA_KERNEL_INT32 && ext_pair_eligible(kp))
+        return launch_ext_pair(d_jobs, d_order, n, d_n, d_q, d_t, kp, qcap, d_w_try, d_out, d_clamped,
+                               d_cells_job, d_cells, d_status, s);
+    return launch_ext_packed(d_jobs, d_order, n, d_n, d_q, d_t, kp, qcap, d_w_try, d_out, d_clamped,
+                             d_cells_job, d_cells, d_status, s);
 }
 
 int check_params(const fa_params *p) {
@@ -217,9 +231,8 @@ int run_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n,
     if (mode == FA_POLICY_SINGLE) {
         uint32_t b = 0;
         for (auto &sg : segs) {
-            FA_CUDA(launch_ext_packed(d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp, sg.second,
-                                      nullptr, d_out, nullptr, c->cells_job.as<uint32_t>(), m.cells,
-                                      m.status, s));
+            FA_CUDA(launch_ext(c->kernel, d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp, sg.second,
+                               nullptr, d_out, nullptr, c->cells_job.as<uint32_t>(), m.cells, m.status, s));
             ++launches;
             b = sg.first;
         }
@@ -241,16 +254,15 @@ int run_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n,
             if (r == 0) {
                 uint32_t b = 0;
                 for (auto &sg : segs) {
-                    FA_CUDA(launch_ext_packed(d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp,
-                                              sg.second, st.w_cur, d_out, c->clamped.as<uint8_t>(),
-                                              c->cells_job.as<uint32_t>(), m.cells, m.status, s));
+                    FA_CUDA(launch_ext(c->kernel, d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp, sg.second,
+                                       st.w_cur, d_out, c->clamped.as<uint8_t>(), c->cells_job.as<uint32_t>(),
+                                       m.cells, m.status, s));
                     ++launches;
                     b = sg.first;
                 }
             } else {
-                FA_CUDA(launch_ext_packed(d_jobs, list, n, cnt, d_q, d_t, kp, qcap_all, st.w_cur, d_out,
-                                          c->clamped.as<uint8_t>(), c->cells_job.as<uint32_t>(), m.cells,
-                                          m.status, s));
+                FA_CUDA(launch_ext(c->kernel, d_jobs, list, n, cnt, d_q, d_t, kp, qcap_all, st.w_cur, d_out,
+                                   c->clamped.as<uint8_t>(), c->cells_job.as<uint32_t>(), m.cells, m.status, s));
                 ++launches;
             }
             FA_CUDA(cudaMemsetAsync(next_cnt, 0, 4, s));
@@ -467,12 +479,20 @@ int fa_ext_batch_device(fa_ctx *c, const fa_params *p, const fa_job *d_jobs, uin
     uint32_t b = 0;
     if (c->timing) FA_CUDA(cudaEventRecord(c->kev0, s));
     for (auto &sg : segs) {
-        FA_CUDA(launch_ext_packed(d_jobs, order + b, sg.first - b, nullptr, d_qseq, d_tseq, kp, sg.second,
-                                  nullptr, d_out, nullptr, nullptr, nullptr, m.status, s));
+        FA_CUDA(launch_ext(c->kernel, d_jobs, order + b, sg.first - b, nullptr, d_qseq, d_tseq, kp, sg.second,
+                           nullptr, d_out, nullptr, nullptr, nullptr, m.status, s));
         b = sg.first;
     }
     if (c->timing) FA_CUDA(cudaEventRecord(c->kev1, s));
     c->last_launches = (uint32_t)segs.size() + (d_order ? 1u : 2u);
+    return FA_OK;
+}
+
+int fa_ctx_set_kernel(fa_ctx *c, int kernel) {
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    if (kernel < FA_KERNEL_AUTO || kernel > FA_KERNEL_INT16X2)
+        return fail(FA_ERR_ARG, "unknown kernel choice %d", kernel);
+    c->kernel = kernel;
     return FA_OK;
 }
 

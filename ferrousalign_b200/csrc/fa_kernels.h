@@ -11,6 +11,7 @@ namespace fa {
 
 constexpr int kExtThreads = 128;     // threads (= jobs) per extension block
 constexpr int kPackedHMax = 8191;    // largest H/E the packed column word holds
+constexpr int kPairThreads = 32;     // threads per int16x2 extension block (2 jobs each)
 
 size_t ext_packed_smem_bytes(int qcap);
 cudaError_t launch_ext_packed(const fa_job *d_jobs, const uint32_t *d_order, uint32_t n,
@@ -19,6 +20,16 @@ cudaError_t launch_ext_packed(const fa_job *d_jobs, const uint32_t *d_order, uin
                               fa_ext_result *d_out, uint8_t *d_clamped, uint32_t *d_cells_job,
                               unsigned long long *d_cells, uint32_t *d_status,
                               cudaStream_t stream);
+
+// int16x2 variant: two jobs per thread (extend_pair_kernel.cu).  Eligible for
+// bwa-form scoring matrices; same arguments and results as launch_ext_packed.
+bool ext_pair_eligible(const ExtParams &p);
+size_t ext_pair_smem_bytes(int qcap);
+cudaError_t launch_ext_pair(const fa_job *d_jobs, const uint32_t *d_order, uint32_t n, const uint32_t *d_n,
+                            const uint8_t *d_qseq,
+                            const uint8_t *d_tseq, const ExtParams &p, int qcap, const int32_t *d_w_try,
+                            fa_ext_result *d_out, uint8_t *d_clamped, uint32_t *d_cells_job,
+                            unsigned long long *d_cells, uint32_t *d_status, cudaStream_t stream);
 
 // Band-retry policy step over the jobs of the last extension round (see policy_kernel.cu).
 struct PolicyState {

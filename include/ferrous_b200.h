@@ -177,6 +177,18 @@ int fa_ext_batch_device(fa_ctx *ctx, const fa_params *p, const fa_job *d_jobs, u
  * device-resident call. */
 int fa_ctx_sync(fa_ctx *ctx);
 
+/* Extension kernel choice for this context (no reference counterpart):
+ * FA_KERNEL_AUTO     int16x2 two-jobs-per-thread kernel when the scoring matrix has the
+ *                    bwa form (a on the diagonal with 1 <= a <= 3, -b off it, N = -1 or 0),
+ *                    the int32 one-job-per-thread kernel otherwise;
+ * FA_KERNEL_INT32    always the int32 kernel;
+ * FA_KERNEL_INT16X2  the int16x2 kernel where eligible (else int32).
+ * Every choice gives identical results. */
+#define FA_KERNEL_AUTO    0
+#define FA_KERNEL_INT32   1
+#define FA_KERNEL_INT16X2 2
+int fa_ctx_set_kernel(fa_ctx *ctx, int kernel);
+
 /* Kernel timing of device-resident calls (no reference counterpart): with timing on,
  * fa_ext_batch_device brackets its extension kernels with CUDA events on the call's
  * stream; fa_ctx_last_timing waits for them and returns their device time and the

@@ -92,6 +92,27 @@ def test_parameter_sweep_bit_exact(ctx, a, b_, n, gaps, w, zdrop, eb):
     assert np.array_equal(out, ref), diff_report(out, ref)
 
 
+@pytest.mark.parametrize("kernel", [N.FA_KERNEL_INT32, N.FA_KERNEL_INT16X2])
+def test_kernel_variants_bit_exact(ctx, kernel):
+    """Both extension kernels (int32 one job per thread, int16x2 two jobs per thread)."""
+    b = synth.workload_ext_1m(100_000, seed=31)
+    p = fa.BandedPairWiseSW().to_struct()
+    ctx.set_kernel(kernel)
+    try:
+        out, stats, ref, tr = run_both(ctx, p, b)
+        ref_seq = synth.reference(5_000_000, seed=6, n_rate=0.01, repeat_frac=0.05)
+        u = synth.ext_jobs(ref_seq, 30_000, seed=66, read_len=(20, 300), seed_at_start=False, seed_len=(10, 40))
+        out2, _, ref2, _ = run_both(ctx, p, u)
+        sw = fa.BandedPairWiseSW(o_del=5, e_del=2, o_ins=3, e_ins=1, mat=fa.bwa_fill_scmat(3, 2, 0), zdrop=30)
+        out3, _, ref3, _ = run_both(ctx, sw.to_struct(), u)
+    finally:
+        ctx.set_kernel(N.FA_KERNEL_AUTO)
+    assert np.array_equal(out, ref), diff_report(out, ref)
+    assert stats["cells"] == tr["cells"].sum()
+    assert np.array_equal(out2, ref2), diff_report(out2, ref2)
+    assert np.array_equal(out3, ref3), diff_report(out3, ref3)
+
+
 def test_policies_match_oracle(ctx):
     b = synth.workload_ext_1m(30_000, seed=21)
     p = fa.BandedPairWiseSW().to_struct()

@@ -1,0 +1,98 @@
+"""The int16x2 extension kernel's thread body, compiled for the host by nvcc, against
+the oracle (no GPU needed).  This runs the exact kernel source, two jobs per thread,
+including the segment logic that keeps the two jobs' band edges apart."""
+import ctypes as C
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE / "kernel_host"))
+
+import ferrousalign_b200 as fa  # noqa: E402
+from ferrousalign_b200 import _native as N  # noqa: E402
+from ferrousalign_b200 import synth  # noqa: E402
+from oracle import ksw_oracle as O  # noqa: E402
+
+
+@pytest.fixture(scope="module")
+def host_lib(built):
+    import build_host
+    lib = C.CDLL(str(build_host.build()))
+    lib.pair_host_run.restype = C.c_int
+    lib.pair_host_run.argtypes = [C.c_void_p] * 3 + [C.c_uint32, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                                      C.c_void_p]
+    return lib
+
+
+def run_host(lib, p, jobs, qseq, tseq):
+    """Longest-first order and 32-column capacity classes, as the library launches them."""
+    q = jobs["qlen"]
+    n = len(q)
+    order = np.array(sorted(range(n), key=lambda i: (-int(q[i]), i)), np.uint32)
+    out = np.zeros(n, N.EXT_RESULT_DT)
+    st = np.zeros(1, np.uint32)
+    s0 = 0
+    while s0 < n:
+        cap = (int(q[order[s0]]) + 31) // 32 * 32
+        e0 = s0
+        while e0 < n and q[order[e0]] > cap - 32:
+            e0 += 1
+        sub = np.ascontiguousarray(order[s0:e0])
+        rc = lib.pair_host_run(p.ctypes.data, jobs.ctypes.data, sub.ctypes.data, len(sub), qseq.ctypes.data,
+                               tseq.ctypes.data, int(q[order[s0]]), out.ctypes.data, st.ctypes.data)
+        assert rc == 0
+        s0 = e0
+    return out, int(st[0])
+
+
+def test_pairs_of_151bp_jobs(host_lib):
+    b = synth.workload_ext_plain(3000)
+    p = fa.BandedPairWiseSW().to_struct()
+    out, st = run_host(host_lib, p, b.jobs, b.qseq, b.tseq)
+    ref, _ = O.ext_batch(p, b.jobs, b.qseq, b.tseq)
+    assert st == 0
+    assert np.array_equal(out, ref), np.nonzero(out != ref)[0][:10]
+
+
+@pytest.mark.parametrize("a,b_,n,gaps,w,zdrop", [(1, 4, -1, (6, 1, 6, 1), 100, 100), (2, 3, 0, (5, 2, 3, 1), 20, 30),
+                                                 (3, 1, -1, (0, 1, 2, 2), 7, 0)])
+def test_uneven_pairs_and_parameters(host_lib, a, b_, n, gaps, w, zdrop):
+    ref_seq = synth.reference(400_000, seed=12, n_rate=0.02, repeat_frac=0.05)
+    b = synth.ext_jobs(ref_seq, 1500, seed=19, read_len=(10, 160), seed_len=(3, 30), seed_at_start=False, w=w,
+                       indel_rates=(0.0, 0.02, 0.06), sub_rate=0.04)
+    sw = fa.BandedPairWiseSW(o_del=gaps[0], e_del=gaps[1], o_ins=gaps[2], e_ins=gaps[3], zdrop=zdrop,
+                             mat=fa.bwa_fill_scmat(a, b_, n))
+    p = sw.to_struct()
+    out, st = run_host(host_lib, p, b.jobs, b.qseq, b.tseq)
+    ref, _ = O.ext_batch(p, b.jobs, b.qseq, b.tseq)
+    assert st == 0
+    assert np.array_equal(out, ref), np.nonzero(out != ref)[0][:10]
+
+
+def test_golden_cases_as_pairs(host_lib):
+    """Every golden case with a bwa-form matrix, paired with the next such case."""
+    cases = [c for c in json.loads((HERE / "golden" / "ext_cases.json").read_text())
+             if c["mat"][0] in (1, 2, 3) and c["mat"][4] in (-1, 0) and all(
+                 c["mat"][t * 5 + q] == (c["mat"][4] if 4 in (t, q) else (c["mat"][0] if t == q else c["mat"][1]))
+                 for t in range(5) for q in range(5)) and (c["mat"][4] == 0 or c["mat"][1] <= -1)]
+    assert len(cases) > 10
+    for c0, c1 in zip(cases[::2], cases[1::2]):
+        if any(c0[k] != c1[k] for k in ("mat", "o_del", "e_del", "o_ins", "e_ins", "zdrop", "end_bonus")):
+            c1 = dict(c1, **{k: c0[k] for k in ("mat", "o_del", "e_del", "o_ins", "e_ins", "zdrop", "end_bonus")})
+        p = np.zeros(1, N.PARAMS_DT)
+        p["mat"][0] = np.array(c0["mat"], np.int8)
+        p["m"] = 5
+        for k in ("o_del", "e_del", "o_ins", "e_ins", "zdrop", "end_bonus"):
+            p[k] = c0[k]
+        qs = np.array(c0["query"] + c1["query"], np.uint8)
+        ts = np.array(c0["target"] + c1["target"] + [0], np.uint8)
+        jobs = np.zeros(2, N.JOB_DT)
+        jobs[0] = (0, 0, len(c0["query"]), len(c0["target"]), c0["h0"], c0["w"], 1, 0)
+        jobs[1] = (len(c0["query"]), len(c0["target"]), len(c1["query"]), len(c1["target"]), c1["h0"], c1["w"], 1, 0)
+        out, st = run_host(host_lib, p, jobs, qs, ts)
+        ref, _ = O.ext_batch(p, jobs, qs, ts)
+        assert np.array_equal(out, ref), (c0["name"], c1["name"], out, ref)
