@@ -18,8 +18,8 @@
 // two column ranges in at most three segments; in a segment each half is either in its
 // job's range, to the left of it (its results there are never read again and are
 // discarded: its F/H/max chains restart where its range begins), or to the right of it
-// (frozen: stores keep that half's previous contents, which later rows read as the
-// reference's stale band-edge cells).  Exact while h0 + a*qlen < 8192 and a <= 3.
+// (frozen: a store mask keeps that half's previous contents, which later rows read as
+// the reference's stale band-edge cells).  All segments share one loop body.  Exact while h0 + a*qlen < 8192 and a <= 3.
 
 #include <vector>
 
@@ -91,14 +91,17 @@ struct PairConsts {
     uint32_t kmul;                    // 2 or 4: k*M >= M + a for every M >= 1
 };
 
-// One segment [j0, j1) of a row.  FZ: 0 = both halves live, 1 = low half (A) frozen,
-// 2 = high half (B) frozen.
-template <int FZ, bool SYM>
+// One segment [j0, j1) of a row.  `live` selects the halves whose stores take the new
+// values; the other half (a job whose range ended left of j0) keeps its previous
+// contents.  Every segment runs this same loop body, so threads of a warp that sit in
+// different kinds of segment do not diverge.
+template <bool SYM, int T>
 __host__ __device__ __forceinline__ void pair_segment(uint2 *__restrict__ col, const uint16_t *__restrict__ qs,
-                                                      int T, int j0, int j1, uint32_t tsel, const PairConsts &k,
-                                                      uint32_t &f, uint32_t &h1, uint32_t &m, int &mjA, int &mjB)
+                                                      int j0, int j1, uint32_t tsel, const PairConsts &k,
+                                                      uint32_t live, uint32_t &f, uint32_t &h1, uint32_t &m,
+                                                      int &mjA, int &mjB)
 {
-#pragma unroll 2
+#pragma unroll 4
     for (int j = j0; j < j1; ++j) {
         const uint2 w = col[j * T];
         const uint32_t sel = (uint32_t)qs[j * T] ^ tsel;
@@ -117,10 +120,8 @@ __host__ __device__ __forceinline__ void pair_segment(uint2 *__restrict__ col, c
         }
         max_argmax_s16x2(m, h, j, mjA, mjB);
         uint2 o;
-        o.x = h1;
-        o.y = enew;
-        if (FZ == 1) { o.x = (o.x & 0xffff0000u) | (w.x & 0xffffu); o.y = (o.y & 0xffff0000u) | (w.y & 0xffffu); }
-        if (FZ == 2) { o.x = (o.x & 0xffffu) | (w.x & 0xffff0000u); o.y = (o.y & 0xffffu) | (w.y & 0xffff0000u); }
+        o.x = (h1 & live) | (w.x & ~live);
+        o.y = (enew & live) | (w.y & ~live);
         col[j * T] = o;
         h1 = h;
     }
@@ -142,11 +143,13 @@ struct JobState {
 };
 
 // The work of one thread: jobs order[2*pair] and order[2*pair+1].  col/qs point at the
-// thread's first column word; consecutive columns are T words apart.  Returns the cells
+// thread's first column word; consecutive columns are T words apart (a compile-time
+// stride, so the compiler can overlap a column's loads with the previous column's
+// stores).  Returns the cells
 // of both jobs.  Host-callable so the CPU tests can run this exact code.
-template <bool SYM>
-__host__ __device__ unsigned long long ext_pair_thread(
-    uint32_t pair, uint2 *col, uint16_t *qs, int T, const fa_job *__restrict__ jobs,
+template <bool SYM, int T>
+__host__ __device__ __forceinline__ unsigned long long ext_pair_thread(
+    uint32_t pair, uint2 *__restrict__ col, uint16_t *__restrict__ qs, const fa_job *__restrict__ jobs,
     const uint32_t *__restrict__ order, uint32_t n, const uint8_t *__restrict__ qseq,
     const uint8_t *__restrict__ tseq, const ExtParams &p, const PairConsts &kc, int n_code_t, int qcap,
     const int32_t *__restrict__ w_try, fa_ext_result *__restrict__ out, uint8_t *__restrict__ clamped_out,
@@ -158,6 +161,7 @@ __host__ __device__ unsigned long long ext_pair_thread(
     if (ia < n) {
         JobState J[2];
         uint32_t bad = 0;
+#pragma unroll
         for (int x = 0; x < 2; ++x) {
             JobState &s = J[x];
             const uint32_t gi = x ? ib : ia;
@@ -220,6 +224,7 @@ __host__ __device__ unsigned long long ext_pair_thread(
             // per-job row setup: band clamp, first column, target selector nibbles
             int b[2], e[2], h1i[2];
             uint32_t tsel = 0;
+#pragma unroll
             for (int x = 0; x < 2; ++x) {
                 JobState &s = J[x];
                 if (s.live && i >= s.tlen) s.live = 0;
@@ -281,17 +286,14 @@ __host__ __device__ unsigned long long ext_pair_thread(
                     const bool frzB = actB ? j0 >= e[1] : false;
                     if (actA && j0 == e[0]) { hEndA = (int)(h1 & 0xffffu); mSave = set_lo(mSave, m); mjSaveA = mjA; }
                     if (actB && j0 == e[1]) { hEndB = (int)(h1 >> 16); mSave = set_hi(mSave, m >> 16); mjSaveB = mjB; }
-                    if (frzA)
-                        pair_segment<1, SYM>(col, qs, T, j0, j1, tsel, kc, f, h1, m, mjA, mjB);
-                    else if (frzB)
-                        pair_segment<2, SYM>(col, qs, T, j0, j1, tsel, kc, f, h1, m, mjA, mjB);
-                    else
-                        pair_segment<0, SYM>(col, qs, T, j0, j1, tsel, kc, f, h1, m, mjA, mjB);
+                    const uint32_t live = (frzA ? 0u : 0x0000ffffu) | (frzB ? 0u : 0xffff0000u);
+                    pair_segment<SYM, T>(col, qs, j0, j1, tsel, kc, live, f, h1, m, mjA, mjB);
                 }
                 if (actA && e[0] == hi) { hEndA = (int)(h1 & 0xffffu); mSave = set_lo(mSave, m); mjSaveA = mjA; }
                 if (actB && e[1] == hi) { hEndB = (int)(h1 >> 16); mSave = set_hi(mSave, m >> 16); mjSaveB = mjB; }
             }
             // eh[end] = {h1, 0} for each job (after every segment wrote its words)
+#pragma unroll
             for (int x = 0; x < 2; ++x) {
                 JobState &s = J[x];
                 if (!s.live) continue;
@@ -301,6 +303,7 @@ __host__ __device__ unsigned long long ext_pair_thread(
                 else { wd.x = set_lo(wd.x, (uint32_t)hEnd); wd.y &= 0xffff0000u; }
                 col[s.end * T] = wd;
             }
+#pragma unroll
             for (int x = 0; x < 2; ++x) {
                 JobState &s = J[x];
                 if (!s.live) continue;
@@ -341,6 +344,7 @@ __host__ __device__ unsigned long long ext_pair_thread(
             }
         }
         if (bad) status_or(status, ST_BAD_CODE);
+#pragma unroll
         for (int x = 0; x < 2; ++x) {
             JobState &s = J[x];
             const uint32_t gi = x ? ib : ia;
@@ -373,7 +377,7 @@ ext_pair_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ or
                    threadIdx.x;
     if (n_dev) n = min(n, *n_dev);   // device-side job count (retry rounds)
     unsigned long long cells_total =
-        ext_pair_thread<SYM>(blockIdx.x * T + threadIdx.x, col, qs, T, jobs, order, n, qseq, tseq, p, kc, n_code_t,
+        ext_pair_thread<SYM, T>(blockIdx.x * T + threadIdx.x, col, qs, jobs, order, n, qseq, tseq, p, kc, n_code_t,
                              qcap, w_try, out, clamped_out, cells_job, status);
     if (cells_out) {
 #pragma unroll
@@ -411,10 +415,10 @@ int ext_pair_host(const fa_job *jobs, const uint32_t *order, uint32_t n, const u
     std::vector<uint16_t> qs((size_t)(qcap + 1));
     for (uint32_t pr = 0; pr < (n + 1) / 2; ++pr) {
         if (sym)
-            ext_pair_thread<true>(pr, col.data(), qs.data(), 1, jobs, order, n, qseq, tseq, p, kc, n_code_t, qcap,
+            ext_pair_thread<true, 1>(pr, col.data(), qs.data(), jobs, order, n, qseq, tseq, p, kc, n_code_t, qcap,
                                   nullptr, out, nullptr, nullptr, status);
         else
-            ext_pair_thread<false>(pr, col.data(), qs.data(), 1, jobs, order, n, qseq, tseq, p, kc, n_code_t, qcap,
+            ext_pair_thread<false, 1>(pr, col.data(), qs.data(), jobs, order, n, qseq, tseq, p, kc, n_code_t, qcap,
                                    nullptr, out, nullptr, nullptr, status);
     }
     return 0;

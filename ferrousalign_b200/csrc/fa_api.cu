@@ -97,13 +97,15 @@ Misc misc_of(fa_ctx *c) {
     return Misc{(uint32_t *)b, (unsigned long long *)(b + 8), (uint32_t *)(b + 16), (uint32_t *)(b + 20)};
 }
 
-// Extension launch: the int16x2 two-jobs-per-thread kernel for bwa-form matrices,
-// the int32 one-job-per-thread kernel otherwise.  Both are exact.
+// Extension launch: the int32 one-job-per-thread kernel, or on request the int16x2
+// two-jobs-per-thread kernel for bwa-form matrices.  Both are exact; the int32 kernel
+// is faster on B200 (the int16x2 one holds twice the shared memory per thread, so
+// half the warps), hence the default.
 cudaError_t launch_ext(int kernel, const fa_job *d_jobs, const uint32_t *d_order, uint32_t n,
                        const uint32_t *d_n, const uint8_t *d_q, const uint8_t *d_t, const ExtParams &kp, int qcap,
                        const int32_t *d_w_try, fa_ext_result *d_out, uint8_t *d_clamped, uint32_t *d_cells_job,
                        unsigned long long *d_cells, uint32_t *d_status, cudaStream_t s) {
-    if (kernel != FA_KERNEL_INT32 && ext_pair_eligible(kp))
+    if (kernel == FA_KERNEL_INT16X2 && ext_pair_eligible(kp))
         return launch_ext_pair(d_jobs, d_order, n, d_n, d_q, d_t, kp, qcap, d_w_try, d_out, d_clamped,
                                d_cells_job, d_cells, d_status, s);
     return launch_ext_packed(d_jobs, d_order, n, d_n, d_q, d_t, kp, qcap, d_w_try, d_out, d_clamped,

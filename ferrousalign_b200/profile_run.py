@@ -1,6 +1,6 @@
 """One device-resident extension batch of the bench workload, for ncu captures.
 
-Usage: python -m ferrousalign_b200.profile_run [n_jobs] [probe]
+Usage: python -m ferrousalign_b200.profile_run [n_jobs] [probe|-] [kernel: 0 auto, 1 int32, 2 int16x2] [reps]
 """
 import ctypes
 import sys
@@ -16,6 +16,9 @@ b = synth.workload_ext_1m(n)
 p = fa.BandedPairWiseSW().to_struct()
 ctx = fa.Context(0)
 lib = N.load()
+if len(sys.argv) > 3:
+    ctx.set_kernel(int(sys.argv[3]))
+reps = int(sys.argv[4]) if len(sys.argv) > 4 else 1
 dev = torch.device("cuda", 0)
 st = torch.cuda.Stream(dev)
 with torch.cuda.stream(st):
@@ -23,14 +26,15 @@ with torch.cuda.stream(st):
     d_q = torch.from_numpy(b.qseq).to(dev)
     d_t = torch.from_numpy(b.tseq).to(dev)
     d_out = torch.empty(n * 6, dtype=torch.int32, device=dev)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(st)
-    N.check(lib.fa_ext_batch_device(ctx.handle, N.ptr(p), d_jobs.data_ptr(), n, d_q.data_ptr(), d_t.data_ptr(),
-                                    None, d_out.data_ptr(), ctypes.c_void_p(st.cuda_stream)))
-    e1.record(st)
-st.synchronize()
-N.check(lib.fa_ctx_sync(ctx.handle))
-print("batch ms", e0.elapsed_time(e1))
+    for r in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        N.check(lib.fa_ext_batch_device(ctx.handle, N.ptr(p), d_jobs.data_ptr(), n, d_q.data_ptr(),
+                                        d_t.data_ptr(), None, d_out.data_ptr(), ctypes.c_void_p(st.cuda_stream)))
+        e1.record(st)
+        st.synchronize()
+        N.check(lib.fa_ctx_sync(ctx.handle))
+        print("batch ms", e0.elapsed_time(e1))
 if len(sys.argv) > 2 and sys.argv[2] == "probe":
     v, ms = ctypes.c_double(), ctypes.c_float()
     for k, name in enumerate(["viaddmax_s16x2_relu", "vimax3_s16x2_relu", "viaddmax_s32_relu", "vimax3_s32",

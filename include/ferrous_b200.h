@@ -178,11 +178,10 @@ int fa_ext_batch_device(fa_ctx *ctx, const fa_params *p, const fa_job *d_jobs, u
 int fa_ctx_sync(fa_ctx *ctx);
 
 /* Extension kernel choice for this context (no reference counterpart):
- * FA_KERNEL_AUTO     int16x2 two-jobs-per-thread kernel when the scoring matrix has the
- *                    bwa form (a on the diagonal with 1 <= a <= 3, -b off it, N = -1 or 0),
- *                    the int32 one-job-per-thread kernel otherwise;
- * FA_KERNEL_INT32    always the int32 kernel;
- * FA_KERNEL_INT16X2  the int16x2 kernel where eligible (else int32).
+ * FA_KERNEL_AUTO     the fastest measured kernel (currently the int32 one);
+ * FA_KERNEL_INT32    int32 cells, one job per thread;
+ * FA_KERNEL_INT16X2  int16x2 cells, two jobs per thread, for bwa-form scoring matrices
+ *                    (a on the diagonal with 1 <= a <= 3, -b off it, N = -1 or 0; else int32).
  * Every choice gives identical results. */
 #define FA_KERNEL_AUTO    0
 #define FA_KERNEL_INT32   1
