@@ -37,6 +37,8 @@ sys.path.insert(0, str(ROOT))
 METRIC = "GCUPS & alignments/s @151bp, learned-band vs plain-band on B200, bit-exact"
 N_JOBS = 1_000_000
 CPU_SAMPLE = 200_000
+MATE_JOBS = 500_000
+MATE_CPU_SAMPLE = 20_000
 DPX_OPS_PER_CELL_PAIR = 9   # int16x2 ops per packed cell pair in the roofline model
 
 
@@ -127,6 +129,72 @@ def cpu_oracle_rate(b, p, sample: int):
     return out, tr, dt, threads
 
 
+def bench_mate(args, ctx, lib, dev, stream, flush, skip_cpu=False):
+    """Mate-rescue local SW on 500,000 2x151 bp pairs (insert ~ N(400, 50), window 551 bp),
+    device-resident, same step/warm-up counts as the extension line."""
+    import ctypes
+    import torch
+    import ferrousalign_b200 as fa
+    from ferrousalign_b200 import _native as N
+    from ferrousalign_b200 import synth
+    t0 = time.time()
+    m = synth.workload_mate(MATE_JOBS)
+    log(f"mate workload: {MATE_JOBS} jobs in {time.time() - t0:.1f}s")
+    mp = fa.make_mate_params()
+    with torch.cuda.stream(stream):
+        d_jobs = torch.from_numpy(m.jobs.view(np.uint8)).to(dev)
+        d_q = torch.from_numpy(m.qseq).to(dev)
+        d_t = torch.from_numpy(m.tseq).to(dev)
+        d_out = torch.empty(MATE_JOBS * 7, dtype=torch.int32, device=dev)
+    stream.synchronize()
+    k_ms, k_n, cells = ctypes.c_float(), ctypes.c_int(), ctypes.c_ulonglong()
+
+    def step():
+        N.check(lib.fa_mate_sw_batch_device(ctx.handle, N.ptr(mp), d_jobs.data_ptr(), MATE_JOBS, d_q.data_ptr(),
+                                            d_t.data_ptr(), d_out.data_ptr(), ctypes.c_void_p(stream.cuda_stream)))
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            flush.zero_()
+            step()
+    N.check(lib.fa_ctx_sync(ctx.handle))
+    times, ktimes, launches = [], [], 0
+    with torch.cuda.stream(stream):
+        for _ in range(max(3, args.steps // 3)):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+            N.check(lib.fa_ctx_last_timing(ctx.handle, ctypes.byref(k_ms), ctypes.byref(k_n)))
+            ktimes.append(k_ms.value)
+            launches += k_n.value
+    N.check(lib.fa_ctx_sync(ctx.handle))
+    N.check(lib.fa_ctx_last_cells(ctx.handle, ctypes.byref(cells)))
+    ms = float(np.mean(times))
+    kms = float(np.mean(ktimes))
+    out = d_out.cpu().numpy().view(N.KSWR_DT).reshape(-1)
+    from oracle import ksw_oracle as O
+    chk = np.arange(0, MATE_JOBS, max(1, MATE_JOBS // 2000))
+    ref, _ = O.mate_batch(mp, m.jobs[chk], m.qseq, m.tseq)
+    res = {"workload": "500k 2x151bp pairs, insert N(400,50), 551 bp window, ksw_align2 u8 + XSTART",
+           "value": MATE_JOBS / (ms * 1e-3), "unit": "alignments/s", "ms_per_step": ms,
+           "gcups": cells.value / (kms * 1e-3) / 1e9, "kernel_ms_per_step": kms,
+           "cells_per_step": int(cells.value), "bit_exact_sample": bool(np.array_equal(out[chk], ref)),
+           "gpu_launches": launches}
+    if not skip_cpu:
+        sample = m.jobs[:MATE_CPU_SAMPLE]
+        t0 = time.perf_counter()
+        _, cc = O.mate_batch(mp, sample, m.qseq, m.tseq, threads=os.cpu_count() or 1)
+        dt = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": MATE_CPU_SAMPLE / dt, "unit": "alignments/s", "cores": os.cpu_count(),
+                               "kind": "port", "gcups": float(cc.sum()) / dt / 1e9,
+                               "sample": f"first {MATE_CPU_SAMPLE} jobs, oracle on all host threads"}
+    return res
+
+
 def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
@@ -168,6 +236,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--jobs", type=int, default=N_JOBS)
     ap.add_argument("--skip-cpu", action="store_true", help="omit the CPU baseline leg")
+    ap.add_argument("--skip-mate", action="store_true", help="omit the mate-rescue section")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -326,6 +395,8 @@ def main():
         "gpu_launches": launches,
         "clocks": clocks,
     }
+    if not args.skip_mate:
+        line["mate_rescue"] = bench_mate(args, ctx, lib, dev, stream, flush, skip_cpu=args.skip_cpu)
     if not args.skip_cpu:
         ref2, tr2, dt, threads = cpu_oracle_rate(b, p, min(CPU_SAMPLE, n))
         line["cpu_baseline"] = {"value": min(CPU_SAMPLE, n) / dt, "unit": "alignments/s", "cores": threads,

@@ -64,6 +64,8 @@ SIGNATURES = {
     "fa_ctx_set_kernel": (C.c_int, [_P, C.c_int]),
     "fa_ctx_last_timing": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_int)]),
     "fa_ext_batch_device_noalloc": (C.c_int, [_P, _P, C.c_uint32, _P, _P, _P, _P]),
+    "fa_mate_sw_batch_device": (C.c_int, [_P, _P, _P, C.c_uint32, _P, _P, _P, _P]),
+    "fa_ctx_last_cells": (C.c_int, [_P, C.POINTER(C.c_ulonglong)]),
     "fa_mate_sw_batch": (C.c_int, [_P, _P, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64, _P, _P]),
 }
 

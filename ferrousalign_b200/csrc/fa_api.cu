@@ -81,6 +81,7 @@ struct fa_ctx {
     uint32_t last_launches = 0;
     bool timing = false;
     int kernel = FA_KERNEL_AUTO;
+    cudaStream_t last_stream = nullptr;   // stream of the last device-resident call
     cudaEvent_t kev0 = nullptr, kev1 = nullptr;   // bracket the extension kernels of a device call
 };
 
@@ -487,6 +488,7 @@ int fa_ext_batch_device(fa_ctx *c, const fa_params *p, const fa_job *d_jobs, uin
     }
     if (c->timing) FA_CUDA(cudaEventRecord(c->kev1, s));
     c->last_launches = (uint32_t)segs.size() + (d_order ? 1u : 2u);
+    c->last_stream = s;
     return FA_OK;
 }
 
@@ -525,8 +527,66 @@ int fa_ctx_last_timing(fa_ctx *c, float *kernel_ms, int *launches) {
 int fa_ctx_sync(fa_ctx *c) {
     if (!c) return fail(FA_ERR_ARG, "null context");
     FA_CUDA(cudaSetDevice(c->device));
-    FA_CUDA(cudaStreamSynchronize(c->stream));
-    if (c->misc.p) return read_status(c, c->stream);
+    cudaStream_t s = c->last_stream ? c->last_stream : c->stream;
+    FA_CUDA(cudaStreamSynchronize(s));
+    if (c->misc.p) return read_status(c, s);
+    return FA_OK;
+}
+
+int fa_mate_sw_batch_device(fa_ctx *c, const fa_mate_params *p, const fa_mate_job *d_jobs, uint32_t n,
+                            const uint8_t *d_qseq, const uint8_t *d_tseq, fa_kswr *d_out, void *stream) {
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    if (!p || p->m != 5) return fail(FA_ERR_ARG, "alphabet size must be 5");
+    if (n == 0) return FA_OK;
+    if (!d_jobs || !d_qseq || !d_tseq || !d_out) return fail(FA_ERR_ARG, "null buffer");
+    int mn = 127, mx = 0;
+    for (int i = 0; i < 25; ++i) { mn = std::min<int>(mn, p->mat[i]); mx = std::max<int>(mx, p->mat[i]); }
+    if (mx <= 0) return fail(FA_ERR_ARG, "scoring matrix needs a positive entry");
+    MateParams mp;
+    memcpy(mp.mat, p->mat, 25);
+    mp.m = 5;
+    mp.o_del = p->o_del; mp.e_del = p->e_del; mp.o_ins = p->o_ins; mp.e_ins = p->e_ins;
+    mp.shift = (uint8_t)(256 - mn);
+    mp.max = mx;
+    FA_CUDA(cudaSetDevice(c->device));
+    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    FA_CUDA(c->misc.ensure(64));
+    FA_CUDA(c->order.ensure(4ull * n));
+    FA_CUDA(c->list_a.ensure(4ull * n));
+    FA_CUDA(c->hist.ensure(sizeof(uint32_t) * (FA_MAX_QLEN + 1)));
+    Misc m = misc_of(c);
+    FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
+    uint32_t *info = c->hist.as<uint32_t>();
+    FA_CUDA(launch_mate_split(d_jobs, n, c->order.as<uint32_t>(), c->list_a.as<uint32_t>(), info, s));
+    uint32_t h[8];
+    FA_CUDA(cudaMemcpyAsync(h, info, sizeof(h), cudaMemcpyDeviceToHost, s));
+    FA_CUDA(cudaStreamSynchronize(s));
+    if (h[5]) return fail(FA_ERR_ARG, "a mate job has qlen <= 0 or tlen < 0");
+    if (h[2] > 16 * 32 || h[3] > 8 * 32) return fail(FA_ERR_CAPACITY, "a mate job's query exceeds the lane limit");
+    if (h[4] > FA_MAX_TLEN) return fail(FA_ERR_CAPACITY, "a mate job's target is too long");
+    uint32_t launches = 1;
+    if (c->timing) FA_CUDA(cudaEventRecord(c->kev0, s));
+    if (h[0]) {
+        FA_CUDA(launch_mate_sw(true, d_jobs, c->order.as<uint32_t>(), h[0], d_qseq, d_tseq, mp, (int)h[2], (int)h[4],
+                               d_out, m.cells, m.status, s));
+        ++launches;
+    }
+    if (h[1]) {
+        FA_CUDA(launch_mate_sw(false, d_jobs, c->list_a.as<uint32_t>(), h[1], d_qseq, d_tseq, mp, (int)h[3],
+                               (int)h[4], d_out, m.cells, m.status, s));
+        ++launches;
+    }
+    if (c->timing) FA_CUDA(cudaEventRecord(c->kev1, s));
+    c->last_launches = launches;
+    c->last_stream = s;
+    return FA_OK;
+}
+
+int fa_ctx_last_cells(fa_ctx *c, unsigned long long *cells) {
+    if (!c || !cells) return fail(FA_ERR_ARG, "null argument");
+    *cells = 0;
+    if (!c->misc.p) return FA_OK;
+    FA_CUDA(cudaMemcpy(cells, misc_of(c).cells, 8, cudaMemcpyDeviceToHost));
     return FA_OK;
 }
 

@@ -62,6 +62,11 @@ cudaError_t launch_qlen_scatter(const fa_job *d_jobs, uint32_t n, uint32_t *d_cu
 // Records the calling thread's fa_last_error() message and returns `code` (fa_api.cu).
 int set_last_error(int code, const char *msg);
 
+// Mate-rescue jobs split by lane width into two order lists; info (8 words) =
+// {n_byte, n_word, max_q_byte, max_q_word, max_t, bad_lengths, -, -}.
+cudaError_t launch_mate_split(const fa_mate_job *d_jobs, uint32_t n, uint32_t *d_order_b, uint32_t *d_order_w,
+                              uint32_t *d_info, cudaStream_t s);
+
 // Integer / DPX instruction throughput (ops per second) for the roofline denominator.
 double probe_int_peak(int kind, int sm_count, cudaStream_t s, float *ms_out);
 

@@ -173,8 +173,8 @@ int fa_ext_batch_device(fa_ctx *ctx, const fa_params *p, const fa_job *d_jobs, u
                         const uint8_t *d_qseq, const uint8_t *d_tseq,
                         const uint32_t *d_order, fa_ext_result *d_out, void *stream);
 
-/* Waits for the context's stream and reports kernel-detected errors of the last
- * device-resident call. */
+/* Waits for the stream of the last device-resident call and reports the errors its
+ * kernels detected. */
 int fa_ctx_sync(fa_ctx *ctx);
 
 /* Extension kernel choice for this context (no reference counterpart):
@@ -220,6 +220,17 @@ int fa_mate_sw_batch(fa_ctx *ctx, const fa_mate_params *p, const fa_mate_job *jo
                      const uint8_t *qseq, uint64_t qseq_len,
                      const uint8_t *tseq, uint64_t tseq_len,
                      fa_kswr *out, fa_ext_stats *stats);
+
+/* Device-resident variant (no reference counterpart): device pointers, kernels
+ * asynchronous on `stream` after one small synchronous read of the batch's job
+ * counts and longest query/target; results at each job's own index.  Job ranges must
+ * lie inside the sequence buffers (not checked); kernel-detected errors come back from
+ * the next fa_ctx_sync(), the cell count of the last device call from
+ * fa_ctx_last_cells().  With fa_ctx_set_timing on, fa_ctx_last_timing covers the SW
+ * kernels. */
+int fa_mate_sw_batch_device(fa_ctx *ctx, const fa_mate_params *p, const fa_mate_job *d_jobs, uint32_t n,
+                            const uint8_t *d_qseq, const uint8_t *d_tseq, fa_kswr *d_out, void *stream);
+int fa_ctx_last_cells(fa_ctx *ctx, unsigned long long *cells);
 
 #ifdef __cplusplus
 }

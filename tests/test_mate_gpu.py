@@ -66,3 +66,31 @@ def test_reference_style_interface(ctx):
                          fa.mate_xtra(151, 1, 19))
         assert (r.aln.score, r.aln.te, r.aln.qe, r.aln.score2, r.aln.te2, r.aln.tb, r.aln.qb) == tuple(o)
     assert fa.execute_mate_rescue_batch_with_engine([]) == []
+
+
+def test_device_entry_point_matches_host_entry_point(ctx):
+    import ctypes
+    import torch
+    b = synth.workload_mate(6000, seed=41)
+    rng = np.random.default_rng(9)
+    b.jobs["xtra"] = np.where(rng.random(len(b.jobs)) < 0.3, b.jobs["xtra"] & ~np.uint32(N.KSW_XBYTE),
+                              b.jobs["xtra"]).astype(np.uint32)
+    p = fa.make_mate_params()
+    ref, st = fa.mate_sw_batch(p, b.jobs, b.qseq, b.tseq, ctx=ctx)
+    lib = N.load()
+    dev = torch.device("cuda", 0)
+    s = torch.cuda.Stream(dev)
+    with torch.cuda.stream(s):
+        d_jobs = torch.from_numpy(b.jobs.view(np.uint8)).to(dev)
+        d_q = torch.from_numpy(b.qseq).to(dev)
+        d_t = torch.from_numpy(b.tseq).to(dev)
+        d_out = torch.zeros(len(b.jobs) * 7, dtype=torch.int32, device=dev)
+    s.synchronize()
+    N.check(lib.fa_mate_sw_batch_device(ctx.handle, N.ptr(p), d_jobs.data_ptr(), len(b.jobs), d_q.data_ptr(),
+                                        d_t.data_ptr(), d_out.data_ptr(), ctypes.c_void_p(s.cuda_stream)))
+    N.check(lib.fa_ctx_sync(ctx.handle))
+    cells = ctypes.c_ulonglong()
+    N.check(lib.fa_ctx_last_cells(ctx.handle, ctypes.byref(cells)))
+    out = d_out.cpu().numpy().view(N.KSWR_DT).reshape(-1)
+    assert np.array_equal(out, ref), diff_report(out, ref)
+    assert cells.value == st["cells"]
