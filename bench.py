@@ -129,6 +129,36 @@ def cpu_oracle_rate(b, p, sample: int):
     return out, tr, dt, threads
 
 
+def bench_learned(args, ctx, b, p):
+    """Learned band vs plain band on the same 1M batch: the plain bwa-mem2 retry policy at
+    w=100 against the learned path (GPU features + MLP first band, judge, retry), both
+    through the host ABI; rates from the device time of their kernels; outputs compared."""
+    import ferrousalign_b200 as fa
+    from ferrousalign_b200 import _native as N
+    from ferrousalign_b200 import band_model as B
+    bwa = fa.make_policy(N.FA_POLICY_BWA, 2)
+    model = B.BandModel.load()
+    hints = B.hints_from_info(b.info)
+    plain_ms, learned_ms = [], []
+    plain = learned = None
+    for _ in range(max(2, args.steps // 10)):
+        plain, pst, _ = fa.extend_batch(p, b.jobs, b.qseq, b.tseq, policy=bwa, ctx=ctx)
+        plain_ms.append(float(pst["kernel_ms"]))
+        learned, lst, wf, _ = B.extend_batch_learned(p, b.jobs, b.qseq, b.tseq, model, hints=hints, ctx=ctx)
+        learned_ms.append(float(lst["kernel_ms"]))
+    n = len(b.jobs)
+    pm, lm = float(np.median(plain_ms)), float(np.median(learned_ms))
+    return {"plain": {"policy": "bwa-mem2 w=100 then 200", "value": n / (pm * 1e-3), "unit": "alignments/s",
+                      "kernel_ms": pm, "cells_executed": int(pst["cells_executed"])},
+            "learned": {"policy": "MLP first band (>= 16), max_off + end-to-end judge, doubling / full-band retry",
+                        "value": n / (lm * 1e-3), "unit": "alignments/s", "kernel_ms": lm,
+                        "cells_executed": int(lst["cells_executed"]),
+                        "cells_saved_frac": 1.0 - float(lst["cells_executed"]) / float(pst["cells_executed"]),
+                        "miss_rate": float(lst["misses"]) / n, "first_band_median": float(np.median(wf))},
+            "speedup": pm / lm, "identical_outputs": bool(np.array_equal(plain, learned)),
+            "identical_frac": float(np.mean(plain == learned))}
+
+
 def bench_mate(args, ctx, lib, dev, stream, flush, skip_cpu=False):
     """Mate-rescue local SW on 500,000 2x151 bp pairs (insert ~ N(400, 50), window 551 bp),
     device-resident, same step/warm-up counts as the extension line."""
@@ -237,6 +267,7 @@ def main():
     ap.add_argument("--jobs", type=int, default=N_JOBS)
     ap.add_argument("--skip-cpu", action="store_true", help="omit the CPU baseline leg")
     ap.add_argument("--skip-mate", action="store_true", help="omit the mate-rescue section")
+    ap.add_argument("--skip-learned", action="store_true", help="omit the learned-band section")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -395,6 +426,8 @@ def main():
         "gpu_launches": launches,
         "clocks": clocks,
     }
+    if not args.skip_learned:
+        line["learned_band"] = bench_learned(args, ctx, b, p)
     if not args.skip_mate:
         line["mate_rescue"] = bench_mate(args, ctx, lib, dev, stream, flush, skip_cpu=args.skip_cpu)
     if not args.skip_cpu:

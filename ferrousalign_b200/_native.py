@@ -16,12 +16,13 @@ LIB_PATH = PKG / "libferrous_b200.so"
 
 FA_OK, FA_ERR_ARG, FA_ERR_CAPACITY, FA_ERR_CUDA, FA_ERR_TIMEOUT, FA_ERR_STATE = range(6)
 FA_POLICY_SINGLE, FA_POLICY_BWA, FA_POLICY_LEARNED = 0, 1, 2
-FA_JUDGE_CERT, FA_JUDGE_MAXOFF = 1, 2
+FA_JUDGE_CERT, FA_JUDGE_MAXOFF, FA_JUDGE_GLOBAL = 1, 2, 4
 FA_DIR_LEFT, FA_DIR_RIGHT = 0, 1
 FA_KERNEL_AUTO, FA_KERNEL_INT32, FA_KERNEL_INT16X2 = 0, 1, 2
 KSW_XBYTE, KSW_XSTOP, KSW_XSUBO, KSW_XSTART = 0x10000, 0x20000, 0x40000, 0x80000
 FA_MAX_QLEN, FA_MAX_TLEN = 4096, 65535
 FA_NOALLOC_MAX_JOBS = 1 << 18
+FA_BAND_NPARAMS = 3201
 
 PARAMS_DT = np.dtype([("mat", "i1", 25), ("_pad", "i1", 3), ("m", "<i4"), ("o_del", "<i4"),
                       ("e_del", "<i4"), ("o_ins", "<i4"), ("e_ins", "<i4"), ("zdrop", "<i4"),
@@ -66,6 +67,19 @@ SIGNATURES = {
     "fa_ext_batch_device_noalloc": (C.c_int, [_P, _P, C.c_uint32, _P, _P, _P, _P]),
     "fa_mate_sw_batch_device": (C.c_int, [_P, _P, _P, C.c_uint32, _P, _P, _P, _P]),
     "fa_ctx_last_cells": (C.c_int, [_P, C.POINTER(C.c_ulonglong)]),
+    "fa_band_model_create": (C.c_int, [C.c_uint64, C.POINTER(C.c_void_p)]),
+    "fa_band_model_destroy": (None, [_P]),
+    "fa_band_model_get": (C.c_int, [_P, _P, _P, _P]),
+    "fa_band_model_set": (C.c_int, [_P, _P, _P, _P]),
+    "fa_band_model_save": (C.c_int, [_P, C.c_char_p]),
+    "fa_band_model_load": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    "fa_band_model_fit_norm": (C.c_int, [_P, _P, C.c_uint32]),
+    "fa_band_features": (C.c_int, [_P, _P, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64, _P, _P]),
+    "fa_band_predict": (C.c_int, [_P, _P, _P, _P, C.c_uint32, C.c_float, C.c_int, _P, _P]),
+    "fa_band_grad": (C.c_int, [_P, _P, _P, _P, C.c_uint32, C.c_float, _P, _P]),
+    "fa_band_train": (C.c_int, [_P, _P, _P, _P, C.c_uint32, C.c_int, C.c_uint32, C.c_float, C.c_float, C.c_uint64, _P]),
+    "fa_ext_batch_learned": (C.c_int, [_P, _P, _P, _P, C.c_float, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64,
+                                       _P, _P, _P, _P, _P]),
     "fa_mate_sw_batch": (C.c_int, [_P, _P, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64, _P, _P]),
 }
 

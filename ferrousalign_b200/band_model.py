@@ -1,0 +1,174 @@
+"""Learned band predictor: Python side of the band-model C ABI.
+
+A 16-64-32-1 MLP (BF16 weights, FP32 accumulation) maps 16 features of an extension job
+to log2 of the narrowest band that still reproduces the full-band result and passes the
+acceptance judge.  Features, prediction and training (forward, backward, Adam) run in
+this library's own CUDA kernels; `make_labels` derives training labels from the plain
+extension itself, run at a ladder of bands.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+from . import _native as N
+
+LADDER = (4, 6, 8, 12, 16, 24, 32, 48, 64)
+HINT_DT = np.dtype([("diag_spread", "<i4"), ("has_partner", "<i4")])
+DEFAULT_MODEL = Path(__file__).resolve().parent / "band_model_151bp.bin"
+JUDGE_FAST = N.FA_JUDGE_CERT | N.FA_JUDGE_MAXOFF | N.FA_JUDGE_GLOBAL
+
+
+class BandModel:
+    def __init__(self, handle: C.c_void_p):
+        self._h = handle
+
+    @classmethod
+    def create(cls, seed: int = 1) -> "BandModel":
+        h = C.c_void_p()
+        N.check(N.load().fa_band_model_create(seed, C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def load(cls, path: str | Path = DEFAULT_MODEL) -> "BandModel":
+        h = C.c_void_p()
+        N.check(N.load().fa_band_model_load(str(path).encode(), C.byref(h)))
+        return cls(h)
+
+    def save(self, path: str | Path) -> None:
+        N.check(N.load().fa_band_model_save(self._h, str(path).encode()))
+
+    def close(self) -> None:
+        if self._h is not None:
+            N.load().fa_band_model_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def get(self):
+        w = np.zeros(N.FA_BAND_NPARAMS, np.float32)
+        mu = np.zeros(16, np.float32)
+        sd = np.zeros(16, np.float32)
+        N.check(N.load().fa_band_model_get(self._h, w.ctypes.data, mu.ctypes.data, sd.ctypes.data))
+        return w, mu, sd
+
+    def set(self, w=None, mean=None, std=None) -> None:
+        args = [None if a is None else np.ascontiguousarray(a, np.float32) for a in (w, mean, std)]
+        N.check(N.load().fa_band_model_set(self._h, *[None if a is None else a.ctypes.data for a in args]))
+
+    def fit_norm(self, x: np.ndarray) -> None:
+        x = np.ascontiguousarray(x, np.float32)
+        N.check(N.load().fa_band_model_fit_norm(self._h, x.ctypes.data, len(x)))
+
+    def predict(self, x: np.ndarray, jobs: np.ndarray | None = None, margin: float = 0.0, w_min: int = 4,
+                ctx: N.Context | None = None):
+        ctx = ctx or N.default_context()
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.zeros(len(x), np.float32)
+        w = np.zeros(len(x), np.int32)
+        j = None if jobs is None else np.ascontiguousarray(jobs, N.JOB_DT)
+        N.check(N.load().fa_band_predict(ctx.handle, self._h, x.ctypes.data, N.ptr(j), len(x), margin, w_min,
+                                         y.ctypes.data, w.ctypes.data))
+        return y, w
+
+    def grad(self, x: np.ndarray, target: np.ndarray, tau: float, ctx: N.Context | None = None):
+        ctx = ctx or N.default_context()
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(target, np.float32)
+        g = np.zeros(N.FA_BAND_NPARAMS, np.float32)
+        loss = C.c_float()
+        N.check(N.load().fa_band_grad(ctx.handle, self._h, x.ctypes.data, t.ctypes.data, len(x), tau, g.ctypes.data,
+                                      C.byref(loss)))
+        return g, loss.value
+
+    def train(self, x: np.ndarray, target: np.ndarray, epochs: int = 8, batch: int = 4096, lr: float = 2e-3,
+              tau: float = 0.85, seed: int = 1, ctx: N.Context | None = None) -> np.ndarray:
+        ctx = ctx or N.default_context()
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(target, np.float32)
+        losses = np.zeros(epochs, np.float32)
+        N.check(N.load().fa_band_train(ctx.handle, self._h, x.ctypes.data, t.ctypes.data, len(x), epochs, batch, lr,
+                                       tau, seed, losses.ctypes.data))
+        return losses
+
+
+def features(params: np.ndarray, jobs: np.ndarray, qseq: np.ndarray, tseq: np.ndarray, hints: np.ndarray | None = None,
+             ctx: N.Context | None = None) -> np.ndarray:
+    ctx = ctx or N.default_context()
+    jobs = np.ascontiguousarray(jobs, N.JOB_DT)
+    x = np.zeros((len(jobs), 16), np.float32)
+    h = None if hints is None else np.ascontiguousarray(hints, HINT_DT)
+    N.check(N.load().fa_band_features(ctx.handle, N.ptr(params), jobs.ctypes.data, len(jobs), N.ptr(qseq), qseq.nbytes,
+                                      N.ptr(tseq), tseq.nbytes, N.ptr(h), x.ctypes.data))
+    return x
+
+
+def hints_from_info(info: np.ndarray) -> np.ndarray:
+    h = np.zeros(len(info), HINT_DT)
+    h["diag_spread"] = info["diag_spread"]
+    h["has_partner"] = info["has_partner"]
+    return h
+
+
+def judge_accepts(out: np.ndarray, w: int, judge: int = JUDGE_FAST) -> np.ndarray:
+    """The policy's acceptance test for a narrow run at band w (without the clamp
+    certificate, which never fires on the 151-bp workload)."""
+    ok = np.zeros(len(out), bool)
+    if judge & N.FA_JUDGE_MAXOFF:
+        ok = out["max_off"] < (w >> 1) + (w >> 2)
+        if judge & N.FA_JUDGE_GLOBAL:
+            ok &= out["gscore"] == out["score"]
+    return ok
+
+
+def make_labels(params: np.ndarray, jobs: np.ndarray, qseq: np.ndarray, tseq: np.ndarray, plain: np.ndarray,
+                judge: int = JUDGE_FAST, ladder=LADDER, ctx: N.Context | None = None):
+    """Smallest ladder band whose single run equals the plain result and passes the
+    judge; the configured band (job.w) when none does.  Returns (labels, cells per band)."""
+    from .batch_extension import extend_batch
+    n = len(jobs)
+    label = jobs["w"].astype(np.int32).copy()
+    done = np.zeros(n, bool)
+    cells = {}
+    for w in ladder:
+        j = jobs.copy()
+        j["w"] = np.minimum(j["w"], w)
+        out, st, _ = extend_batch(params, j, qseq, tseq, ctx=ctx)
+        cells[w] = int(st["cells"])
+        good = (out == plain) & judge_accepts(out, w, judge)
+        newly = good & ~done
+        label[newly] = np.minimum(w, jobs["w"][newly])
+        done |= good
+    return label, cells
+
+
+def extend_batch_learned(params: np.ndarray, jobs: np.ndarray, qseq: np.ndarray, tseq: np.ndarray,
+                         model: BandModel, hints: np.ndarray | None = None, judge: int = JUDGE_FAST,
+                         margin: float = 0.0, w_min: int = 16, max_tries: int = 2, ctx: N.Context | None = None):
+    """fa_ext_batch_learned: predicted first band, judge, doubling up to job.w, then the
+    bwa-mem2 policy.  Returns (results, stats, w_first, w_final)."""
+    from .batch_extension import make_policy
+    ctx = ctx or N.default_context()
+    jobs = np.ascontiguousarray(jobs, N.JOB_DT)
+    n = len(jobs)
+    out = np.zeros(n, N.EXT_RESULT_DT)
+    stats = np.zeros(1, N.STATS_DT)
+    wf = np.zeros(n, np.int32)
+    wfin = np.zeros(n, np.int32)
+    pol = make_policy(N.FA_POLICY_LEARNED, max_tries, judge, w_min)
+    h = None if hints is None else np.ascontiguousarray(hints, HINT_DT)
+    N.check(N.load().fa_ext_batch_learned(ctx.handle, N.ptr(params), N.ptr(pol), model.handle, margin,
+                                          jobs.ctypes.data, n, N.ptr(qseq), qseq.nbytes, N.ptr(tseq), tseq.nbytes,
+                                          N.ptr(h), out.ctypes.data, wf.ctypes.data, wfin.ctypes.data,
+                                          stats.ctypes.data))
+    return out, stats[0], wf, wfin

@@ -1,0 +1,360 @@
+// band_model.cu -- the learned band predictor: feature extraction, a 16-64-32-1 MLP
+// (BF16 weights, FP32 accumulation) and its training kernels.
+//
+// The predictor guesses, per extension, the narrowest band that reproduces the full-band
+// result, from facts available before the DP runs: seed length, query/target lengths,
+// h0, the chain's seed-diagonal spread and mismatch counts along the seed diagonal and
+// its neighbours.  The extension kernels then start at the predicted band and the
+// band-retry policy (policy_kernel.cu) accepts or widens it.
+//
+// Training: quantile (pinball) loss on log2(band) so the prediction sits above most
+// labels; per-block minibatch backward with the activations in shared memory and
+// gradient products computed from them, then Adam on FP32 master weights with a BF16
+// copy for inference.
+
+#include <cuda_bf16.h>
+
+#include "fa_device.cuh"
+#include "fa_kernels.h"
+
+namespace fa {
+
+// ---------------------------------------------------------------- features
+// x[0..15] per job (raw, normalised later by the model):
+//  0 seed length (h0 / max score)   1 qlen
+//  2 query end - last mismatch on the seed diagonal     3 the same on the best shifted diagonal
+//  4 seed-diagonal spread (hint)    5 has partner     6 mismatching 8-blocks on the diagonal
+//  7 their fraction                 8 first mismatching block / blocks
+//  9 mismatching blocks in the last quarter           10 diagonal mismatches / positions
+// 11 longest matching block run / blocks              12 N bases in the query
+// 13 tlen - qlen                    14 |best shift| of the second half (diagonals -4..4)
+// 15 mismatch fraction of the second half on that best shifted diagonal
+// One warp per job, one pass over the query: lane l takes positions l, l+32, ...; every
+// load instruction of the warp touches consecutive bytes, and counts and extremes are
+// warp reductions (redux.sync).
+__global__ void __launch_bounds__(128) band_features_kernel(const fa_job *__restrict__ jobs, uint32_t n,
+                                                            const uint8_t *__restrict__ qseq,
+                                                            const uint8_t *__restrict__ tseq,
+                                                            const fa_band_hint *__restrict__ hints, int max_score,
+                                                            float *__restrict__ x)
+{
+    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;                       // whole warps exit together
+    const fa_job jb = jobs[i];
+    const uint8_t *Q = qseq + jb.q_off, *T = tseq + jb.t_off;
+    const int qlen = jb.qlen, tlen = jb.tlen;
+    const int L = min(qlen, tlen);
+    const int nblk = (L + 7) / 8;
+    const int half = qlen / 2;
+    int mm = 0, last_mm = -1, nq = 0;
+    int c[9], cnt[9], last_s[9];
+#pragma unroll
+    for (int s = 0; s < 9; ++s) { c[s] = 0; cnt[s] = 0; last_s[s] = -1; }
+    int mmblk = 0, first = -1, lastq = 0, best_run = 0, run = 0;
+    for (int k0 = 0; k0 < qlen; k0 += 32) {
+        const int k = k0 + lane;
+        uint32_t q = 5;
+        if (k < qlen) {
+            q = Q[k];
+            nq += q > 3;
+        }
+        const int d = (k < L) ? (q != T[k] || q > 3) : 0;
+        mm += d;
+        if (d) last_mm = k;
+        if (k < qlen && k >= half) {
+#pragma unroll
+            for (int s = 0; s < 9; ++s) {
+                const int t = k + s - 4;
+                if (t >= 0 && t < tlen) {
+                    const int dd = q != T[t] || q > 3;
+                    c[s] += dd;
+                    ++cnt[s];
+                    if (dd) last_s[s] = k;
+                }
+            }
+        }
+        // 8-position blocks of this 32-position step (steps are block aligned)
+        const unsigned bal = __ballot_sync(0xffffffffu, d);
+        for (int qb = 0; qb < 4; ++qb) {
+            const int bidx = k0 / 8 + qb;
+            if (bidx >= nblk) break;
+            if ((bal >> (8 * qb)) & 0xffu) {
+                ++mmblk;
+                if (first < 0) first = bidx;
+                if (bidx * 4 >= nblk * 3) ++lastq;
+                run = 0;
+            } else {
+                best_run = max(best_run, ++run);
+            }
+        }
+    }
+    mm = __reduce_add_sync(0xffffffffu, mm);
+    nq = __reduce_add_sync(0xffffffffu, nq);
+    last_mm = __reduce_max_sync(0xffffffffu, last_mm);
+    int best_s = 0, best_c = 1 << 30, best_n = 1, best_last = -1;
+#pragma unroll
+    for (int s = 0; s < 9; ++s) {
+        const int cs = __reduce_add_sync(0xffffffffu, c[s]);
+        const int ns = __reduce_add_sync(0xffffffffu, cnt[s]);
+        const int ls = __reduce_max_sync(0xffffffffu, last_s[s]);
+        const int sh = s - 4;
+        if (ns > 0 && (cs * best_n < best_c * ns || (cs * best_n == best_c * ns && abs(sh) < abs(best_s)))) {
+            best_c = cs; best_n = ns; best_s = sh; best_last = ls;
+        }
+    }
+    if (lane != 0) return;
+    float *o = x + (size_t)i * 16;
+    const float fb = (float)max(nblk, 1);
+    o[0] = max_score > 0 ? (float)jb.h0 / (float)max_score : (float)jb.h0;
+    o[1] = (float)qlen;
+    o[2] = (float)(qlen - last_mm);
+    o[3] = (float)(qlen - max(best_last, half - 1));
+    o[4] = hints ? (float)hints[i].diag_spread : 0.f;
+    o[5] = hints ? (float)(hints[i].has_partner != 0) : 0.f;
+    o[6] = (float)mmblk;
+    o[7] = (float)mmblk / fb;
+    o[8] = first < 0 ? 1.f : (float)first / fb;
+    o[9] = (float)lastq;
+    o[10] = (float)mm / (float)max(L, 1);
+    o[11] = (float)best_run / fb;
+    o[12] = (float)nq;
+    o[13] = (float)(tlen - qlen);
+    o[14] = (float)abs(best_s);
+    o[15] = best_c >= (1 << 30) ? 1.f : (float)best_c / (float)best_n;
+}
+
+cudaError_t launch_band_features(const fa_job *d_jobs, uint32_t n, const uint8_t *d_q, const uint8_t *d_t,
+                                 const fa_band_hint *d_hints, int max_score, float *d_x, cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    const uint64_t threads = (uint64_t)n * 32;
+    band_features_kernel<<<(uint32_t)((threads + 127) / 128), 128, 0, s>>>(d_jobs, n, d_q, d_t, d_hints, max_score,
+                                                                           d_x);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- MLP
+// Parameter layout (floats): W1[64][16] b1[64] W2[32][64] b2[32] W3[32] b3[1]
+constexpr int kIn = 16, kH1 = 64, kH2 = 32;
+constexpr int oW1 = 0, oB1 = oW1 + kH1 * kIn, oW2 = oB1 + kH1, oB2 = oW2 + kH2 * kH1, oW3 = oB2 + kH2,
+              oB3 = oW3 + kH2, kNParams = oB3 + 1;
+static_assert(kNParams == FA_BAND_NPARAMS, "parameter count");
+
+struct NormConsts {
+    float mean[kIn], inv_std[kIn];
+};
+
+// forward of one sample with weights staged in shared memory as float
+// Every loop is fully unrolled so h1/h2 stay in registers.
+__device__ __forceinline__ float mlp_forward(const float *__restrict__ w, const float *x, float *h1, float *h2)
+{
+#pragma unroll
+    for (int u = 0; u < kH1; ++u) {
+        float a = w[oB1 + u];
+#pragma unroll
+        for (int k = 0; k < kIn; ++k) a = fmaf(w[oW1 + u * kIn + k], x[k], a);
+        h1[u] = fmaxf(a, 0.f);
+    }
+#pragma unroll
+    for (int u = 0; u < kH2; ++u) {
+        float a = w[oB2 + u];
+#pragma unroll
+        for (int k = 0; k < kH1; ++k) a = fmaf(w[oW2 + u * kH1 + k], h1[k], a);
+        h2[u] = fmaxf(a, 0.f);
+    }
+    float y = w[oB3];
+#pragma unroll
+    for (int k = 0; k < kH2; ++k) y = fmaf(w[oW3 + k], h2[k], y);
+    return y;
+}
+
+__device__ __forceinline__ void load_norm(const float *__restrict__ xr, const NormConsts &nc, float *x)
+{
+#pragma unroll
+    for (int k = 0; k < kIn; ++k) x[k] = (xr[k] - nc.mean[k]) * nc.inv_std[k];
+}
+
+// Inference: y = MLP(x) in log2(band) units; band = ceil(2^(y + margin)) raised to
+// w_min.  A band above 2*w_min starts at the configured band: such jobs are mostly
+// rejected by the acceptance judge at any narrow band, and a rejected mid-size first
+// run costs more than starting wide.
+__global__ void __launch_bounds__(128) band_predict_kernel(const __nv_bfloat16 *__restrict__ wbf, NormConsts nc,
+                                                           const float *__restrict__ x, const fa_job *__restrict__ jobs,
+                                                           uint32_t n, float margin, int w_min,
+                                                           float *__restrict__ y_out, int32_t *__restrict__ w_out)
+{
+    __shared__ float w[kNParams];
+    for (int k = threadIdx.x; k < kNParams; k += blockDim.x) w[k] = __bfloat162float(wbf[k]);
+    __syncthreads();
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float xi[kIn], h1[kH1], h2[kH2];
+    load_norm(x + (size_t)i * kIn, nc, xi);
+    const float y = mlp_forward(w, xi, h1, h2);
+    if (y_out) y_out[i] = y;
+    if (w_out) {
+        const int wj = jobs ? jobs[i].w : 100;
+        const float e = fminf(fmaxf(y + margin, 0.f), 16.f);
+        int band = (int)ceilf(exp2f(e));
+        band = max(band, w_min);
+        if (band > 2 * w_min) band = wj;
+        band = min(band, wj);
+        w_out[i] = band;
+    }
+}
+
+// Backward over one minibatch of up to kMB samples per block: activations in shared
+// memory, then every thread accumulates a slice of the gradient as sums over the
+// block's samples.  Loss: pinball(tau) on y - target, averaged over `n_total`.
+constexpr int kMB = 128;
+struct BwdSmem {             // rows padded by one float so per-sample rows map to distinct banks
+    float w[kNParams];
+    float x[kMB][kIn + 1];
+    float h1[kMB][kH1 + 1];
+    float h2[kMB][kH2 + 1];
+    float d2[kMB][kH2 + 1];   // dL/d(pre-activation of layer 2)
+    float d1[kMB][kH1 + 1];   // dL/d(pre-activation of layer 1)
+    float dy[kMB];
+};
+
+__global__ void __launch_bounds__(kMB) band_backward_kernel(const __nv_bfloat16 *__restrict__ wbf, NormConsts nc,
+                                                            const float *__restrict__ x, const float *__restrict__ target,
+                                                            uint32_t n, float tau, float inv_total,
+                                                            float *__restrict__ grad, float *__restrict__ loss_sum)
+{
+    extern __shared__ __align__(16) unsigned char bsm_raw[];
+    BwdSmem &S = *reinterpret_cast<BwdSmem *>(bsm_raw);
+    for (int k = threadIdx.x; k < kNParams; k += blockDim.x) S.w[k] = __bfloat162float(wbf[k]);
+    __syncthreads();
+    const int t = threadIdx.x;
+    const uint32_t i = blockIdx.x * kMB + t;
+    const bool live = i < n;
+    float loss = 0.f;
+    {
+        float xi[kIn], h1[kH1], h2[kH2];
+        if (live) {
+            load_norm(x + (size_t)i * kIn, nc, xi);
+        } else {
+#pragma unroll
+            for (int k = 0; k < kIn; ++k) xi[k] = 0.f;
+        }
+        const float y = mlp_forward(S.w, xi, h1, h2);
+        float dy = 0.f;
+        if (live) {
+            const float r = target[i] - y;
+            loss = r >= 0.f ? tau * r : (tau - 1.f) * r;
+            dy = (r > 0.f ? -tau : (r < 0.f ? 1.f - tau : 0.f)) * inv_total;
+        }
+#pragma unroll
+        for (int k = 0; k < kIn; ++k) S.x[t][k] = xi[k];
+#pragma unroll
+        for (int k = 0; k < kH1; ++k) S.h1[t][k] = h1[k];
+#pragma unroll
+        for (int k = 0; k < kH2; ++k) {
+            S.h2[t][k] = h2[k];
+            S.d2[t][k] = h2[k] > 0.f ? dy * S.w[oW3 + k] : 0.f;
+        }
+        S.dy[t] = dy;
+        // d1 = W2^T d2, masked by ReLU'; h1 read back from shared memory so the loop
+        // can stay rolled without indexing a register array
+        for (int u = 0; u < kH1; ++u) {
+            float a = 0.f;
+#pragma unroll
+            for (int v = 0; v < kH2; ++v) a = fmaf(S.w[oW2 + v * kH1 + u], S.d2[t][v], a);
+            S.d1[t][u] = S.h1[t][u] > 0.f ? a : 0.f;
+        }
+    }
+    __syncthreads();
+    // gradient slices: each thread owns parameters p = t, t + kMB, ...
+    for (int p = t; p < kNParams; p += kMB) {
+        float g = 0.f;
+        if (p < oB1) {                       // W1[u][k] = sum d1[u] * x[k]
+            const int u = (p - oW1) / kIn, k = (p - oW1) % kIn;
+            for (int s = 0; s < kMB; ++s) g = fmaf(S.d1[s][u], S.x[s][k], g);
+        } else if (p < oW2) {                // b1[u]
+            const int u = p - oB1;
+            for (int s = 0; s < kMB; ++s) g += S.d1[s][u];
+        } else if (p < oB2) {                // W2[u][k] = sum d2[u] * h1[k]
+            const int u = (p - oW2) / kH1, k = (p - oW2) % kH1;
+            for (int s = 0; s < kMB; ++s) g = fmaf(S.d2[s][u], S.h1[s][k], g);
+        } else if (p < oW3) {                // b2[u]
+            const int u = p - oB2;
+            for (int s = 0; s < kMB; ++s) g += S.d2[s][u];
+        } else if (p < oB3) {                // W3[k] = sum dy * h2[k]
+            const int k = p - oW3;
+            for (int s = 0; s < kMB; ++s) g = fmaf(S.dy[s], S.h2[s][k], g);
+        } else {                             // b3
+            for (int s = 0; s < kMB; ++s) g += S.dy[s];
+        }
+        atomicAdd(&grad[p], g);
+    }
+    // block loss
+    float l = loss;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) l += __shfl_down_sync(0xffffffffu, l, o);
+    if ((t & 31) == 0 && loss_sum) atomicAdd(loss_sum, l);
+}
+
+// Adam on FP32 master weights; writes the BF16 copy used by forward/backward.
+__global__ void band_adam_kernel(float *__restrict__ w, __nv_bfloat16 *__restrict__ wbf, float *__restrict__ m,
+                                 float *__restrict__ v, const float *__restrict__ grad, float lr, float b1, float b2,
+                                 float eps, float bc1, float bc2)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= kNParams) return;
+    const float g = grad[p];
+    const float mp = b1 * m[p] + (1.f - b1) * g;
+    const float vp = b2 * v[p] + (1.f - b2) * g * g;
+    m[p] = mp;
+    v[p] = vp;
+    const float upd = lr * (mp / bc1) / (sqrtf(vp / bc2) + eps);
+    const float wn = w[p] - upd;
+    w[p] = wn;
+    wbf[p] = __float2bfloat16_rn(wn);
+}
+
+size_t band_bwd_smem_bytes() { return sizeof(BwdSmem); }
+
+static NormConsts norm_of(const float *mean, const float *std_) {
+    NormConsts nc;
+    for (int k = 0; k < kIn; ++k) {
+        nc.mean[k] = mean[k];
+        nc.inv_std[k] = std_[k] > 1e-12f ? 1.f / std_[k] : 1.f;
+    }
+    return nc;
+}
+
+cudaError_t launch_band_predict(const __nv_bfloat16 *d_wbf, const float *mean, const float *std_, const float *d_x,
+                                const fa_job *d_jobs, uint32_t n, float margin, int w_min, float *d_y,
+                                int32_t *d_w, cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    band_predict_kernel<<<(n + 127) / 128, 128, 0, s>>>(d_wbf, norm_of(mean, std_), d_x, d_jobs, n, margin, w_min,
+                                                        d_y, d_w);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_band_backward(const __nv_bfloat16 *d_wbf, const float *mean, const float *std_, const float *d_x,
+                                 const float *d_target, uint32_t n, float tau, float inv_total, float *d_grad,
+                                 float *d_loss, cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    const size_t smem = band_bwd_smem_bytes();
+    cudaError_t e = cudaFuncSetAttribute(band_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    band_backward_kernel<<<(n + kMB - 1) / kMB, kMB, smem, s>>>(d_wbf, norm_of(mean, std_), d_x, d_target, n, tau,
+                                                                inv_total, d_grad, d_loss);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_band_adam(float *d_w, __nv_bfloat16 *d_wbf, float *d_m, float *d_v, const float *d_grad, float lr,
+                             int step, cudaStream_t s)
+{
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float bc1 = 1.f - powf(b1, (float)step), bc2 = 1.f - powf(b2, (float)step);
+    band_adam_kernel<<<(kNParams + 255) / 256, 256, 0, s>>>(d_w, d_wbf, d_m, d_v, d_grad, lr, b1, b2, 1e-8f, bc1, bc2);
+    return cudaGetLastError();
+}
+
+}  // namespace fa

@@ -77,7 +77,7 @@ struct fa_ctx {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     DevBuf jobs, order, qseq, tseq, out, clamped, cells_job, misc;
-    DevBuf w_first, w_cur, prev, kk, w_final, tries, missed, list_a, list_b, hist;
+    DevBuf w_first, w_cur, prev, kk, w_final, tries, missed, list_a, list_b, hist, feat, wbf, part_n, part_w;
     uint32_t last_launches = 0;
     bool timing = false;
     int kernel = FA_KERNEL_AUTO;
@@ -85,17 +85,21 @@ struct fa_ctx {
     cudaEvent_t kev0 = nullptr, kev1 = nullptr;   // bracket the extension kernels of a device call
 };
 
+int fa::fa_ctx_device(const fa_ctx *c) { return c->device; }
+
 namespace {
 
-// misc buffer layout: [0] status u32, [2] cells u64, [4] count A u32, [5] count B u32
+// misc buffer layout (bytes): [0] status u32, [8] cells u64, [16] count A, [20] count B,
+// [24] narrow count, [28] wide count
 struct Misc {
     uint32_t *status;
     unsigned long long *cells;
-    uint32_t *cnt_a, *cnt_b;
+    uint32_t *cnt_a, *cnt_b, *cnt_narrow, *cnt_wide;
 };
 Misc misc_of(fa_ctx *c) {
     char *b = c->misc.as<char>();
-    return Misc{(uint32_t *)b, (unsigned long long *)(b + 8), (uint32_t *)(b + 16), (uint32_t *)(b + 20)};
+    return Misc{(uint32_t *)b, (unsigned long long *)(b + 8), (uint32_t *)(b + 16), (uint32_t *)(b + 20),
+                (uint32_t *)(b + 24), (uint32_t *)(b + 28)};
 }
 
 // Extension launch: the int32 one-job-per-thread kernel, or on request the int16x2
@@ -206,6 +210,8 @@ int ensure_policy_buffers(fa_ctx *c, uint32_t n) {
     FA_CUDA(c->missed.ensure(n));
     FA_CUDA(c->list_a.ensure(b));
     FA_CUDA(c->list_b.ensure(b));
+    FA_CUDA(c->part_n.ensure(b));
+    FA_CUDA(c->part_w.ensure(b));
     return FA_OK;
 }
 
@@ -254,7 +260,7 @@ int run_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n,
         uint32_t *next = c->list_a.as<uint32_t>(), *next_cnt = m.cnt_a;
         uint32_t *spare = c->list_b.as<uint32_t>(), *spare_cnt = m.cnt_b;
         for (int r = 0; r < max_rounds; ++r) {
-            if (r == 0) {
+            if (r == 0 && !learned) {
                 uint32_t b = 0;
                 for (auto &sg : segs) {
                     FA_CUDA(launch_ext(c->kernel, d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp, sg.second,
@@ -263,6 +269,14 @@ int run_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n,
                     ++launches;
                     b = sg.first;
                 }
+            } else if (learned) {
+                // full-band warps first, narrow-band warps after, one launch
+                FA_CUDA(launch_band_partition(d_jobs, list, cnt, n, st.w_cur, c->part_n.as<uint32_t>(), m.cnt_wide,
+                                              m.cnt_narrow, s));
+                FA_CUDA(launch_ext(c->kernel, d_jobs, c->part_n.as<uint32_t>(), n, cnt, d_q, d_t, kp, qcap_all,
+                                   st.w_cur, d_out, c->clamped.as<uint8_t>(), c->cells_job.as<uint32_t>(), m.cells,
+                                   m.status, s));
+                launches += 2;
             } else {
                 FA_CUDA(launch_ext(c->kernel, d_jobs, list, n, cnt, d_q, d_t, kp, qcap_all, st.w_cur, d_out,
                                    c->clamped.as<uint8_t>(), c->cells_job.as<uint32_t>(), m.cells, m.status, s));
@@ -348,7 +362,8 @@ void fa_ctx_destroy(fa_ctx *c) {
     cudaSetDevice(c->device);
     for (DevBuf *b : {&c->jobs, &c->order, &c->qseq, &c->tseq, &c->out, &c->clamped, &c->cells_job,
                       &c->misc, &c->w_first, &c->w_cur, &c->prev, &c->kk, &c->w_final, &c->tries,
-                      &c->missed, &c->list_a, &c->list_b, &c->hist})
+                      &c->missed, &c->list_a, &c->list_b, &c->hist, &c->feat, &c->wbf, &c->part_n,
+                      &c->part_w})
         b->release();
     if (c->kev0) cudaEventDestroy(c->kev0);
     if (c->kev1) cudaEventDestroy(c->kev1);
@@ -424,6 +439,64 @@ int fa_ext_batch_policy(fa_ctx *c, const fa_params *p, const fa_policy *pol, con
         for (uint32_t i = 0; i < n; ++i) w_final[i] = jobs[i].w;
     if (stats)
         stats->total_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return FA_OK;
+}
+
+int fa_ext_batch_learned(fa_ctx *c, const fa_params *p, const fa_policy *pol, const fa_band_model *model,
+                         float margin, const fa_job *jobs, uint32_t n, const uint8_t *qseq, uint64_t qseq_len,
+                         const uint8_t *tseq, uint64_t tseq_len, const fa_band_hint *hints, fa_ext_result *out,
+                         int32_t *w_first_out, int32_t *w_final, fa_ext_stats *stats) {
+    auto t0 = std::chrono::steady_clock::now();
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    if (!model) return fail(FA_ERR_STATE, "no band model");
+    if (!pol || pol->mode != FA_POLICY_LEARNED) return fail(FA_ERR_ARG, "fa_ext_batch_learned needs FA_POLICY_LEARNED");
+    if (int rc = check_params(p)) return rc;
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (n == 0) return FA_OK;
+    if (!jobs || !out || !qseq || !tseq) return fail(FA_ERR_ARG, "null buffer");
+    FA_CUDA(cudaSetDevice(c->device));
+    const ExtParams kp = ext_params_of(p);
+    int max_q = 0;
+    if (int rc = check_jobs(jobs, n, qseq_len, tseq_len, kp, packed_qcap_limit(c->smem_optin), &max_q)) return rc;
+    std::vector<uint32_t> order;
+    std::vector<std::pair<uint32_t, int>> segs;
+    length_order(jobs, n, order, segs);
+    if (int rc = ensure_ext_buffers(c, n, qseq_len, tseq_len)) return rc;
+    if (int rc = ensure_policy_buffers(c, n)) return rc;
+    FA_CUDA(c->feat.ensure(sizeof(float) * 16 * (size_t)n + sizeof(fa_band_hint) * (size_t)n));
+    FA_CUDA(c->wbf.ensure(sizeof(__nv_bfloat16) * FA_BAND_NPARAMS));
+    cudaStream_t s = c->stream;
+    FA_CUDA(cudaMemcpyAsync(c->jobs.p, jobs, sizeof(fa_job) * (size_t)n, cudaMemcpyHostToDevice, s));
+    FA_CUDA(cudaMemcpyAsync(c->order.p, order.data(), 4ull * n, cudaMemcpyHostToDevice, s));
+    FA_CUDA(cudaMemcpyAsync(c->qseq.p, qseq, qseq_len, cudaMemcpyHostToDevice, s));
+    FA_CUDA(cudaMemcpyAsync(c->tseq.p, tseq, tseq_len, cudaMemcpyHostToDevice, s));
+    float *d_x = c->feat.as<float>();
+    fa_band_hint *d_h = hints ? reinterpret_cast<fa_band_hint *>(d_x + 16 * (size_t)n) : nullptr;
+    if (hints) FA_CUDA(cudaMemcpyAsync(d_h, hints, sizeof(fa_band_hint) * (size_t)n, cudaMemcpyHostToDevice, s));
+    std::vector<__nv_bfloat16> wbf;
+    float mean[16], sd[16];
+    band_model_export(model, wbf, mean, sd);
+    FA_CUDA(cudaMemcpyAsync(c->wbf.p, wbf.data(), sizeof(__nv_bfloat16) * FA_BAND_NPARAMS, cudaMemcpyHostToDevice, s));
+    FA_CUDA(cudaEventRecord(c->ev0, s));
+    FA_CUDA(launch_band_features(c->jobs.as<fa_job>(), n, c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(), d_h,
+                                 kp.max_score, d_x, s));
+    FA_CUDA(launch_band_predict(c->wbf.as<__nv_bfloat16>(), mean, sd, d_x, c->jobs.as<fa_job>(), n, margin, pol->w_min,
+                                nullptr, c->w_first.as<int32_t>(), s));
+    FA_CUDA(cudaEventRecord(c->ev1, s));
+    float pred_ms = 0.f;
+    FA_CUDA(cudaEventSynchronize(c->ev1));
+    cudaEventElapsedTime(&pred_ms, c->ev0, c->ev1);
+    if (w_first_out) FA_CUDA(cudaMemcpy(w_first_out, c->w_first.p, 4ull * n, cudaMemcpyDeviceToHost));
+    int rc = run_ext(c, kp, pol, n, segs, max_q, c->jobs.as<fa_job>(), c->order.as<uint32_t>(), c->qseq.as<uint8_t>(),
+                     c->tseq.as<uint8_t>(), c->w_first.as<int32_t>(), c->out.as<fa_ext_result>(), s, stats, w_final);
+    if (rc) return rc;
+    FA_CUDA(cudaMemcpyAsync(out, c->out.p, sizeof(fa_ext_result) * (size_t)n, cudaMemcpyDeviceToHost, s));
+    FA_CUDA(cudaStreamSynchronize(s));
+    if (stats) {
+        stats->kernel_ms += pred_ms;
+        stats->kernel_launches += 2;
+        stats->total_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
     return FA_OK;
 }
 

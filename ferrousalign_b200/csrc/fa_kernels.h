@@ -4,6 +4,8 @@
 #include <cstddef>
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <vector>
 
 #include "fa_device.cuh"
 
@@ -44,6 +46,9 @@ cudaError_t launch_policy_step(const fa_job *d_jobs, const uint32_t *d_list, con
                                uint32_t n_max, const fa_ext_result *d_out, const uint8_t *d_clamped,
                                PolicyState st, int max_tries, int judge, uint32_t *d_next,
                                uint32_t *d_next_count, cudaStream_t stream);
+cudaError_t launch_band_partition(const fa_job *d_jobs, const uint32_t *d_list, const uint32_t *d_count,
+                                  uint32_t n_max, const int32_t *d_w_cur, uint32_t *d_out, uint32_t *d_n_wide,
+                                  uint32_t *d_n_narrow, cudaStream_t stream);
 cudaError_t launch_policy_init(const fa_job *d_jobs, uint32_t n, const int32_t *d_w_first, int w_min,
                                int learned, PolicyState st, cudaStream_t stream);
 
@@ -58,6 +63,22 @@ cudaError_t launch_mate_sw(bool byte_lanes, const fa_mate_job *d_jobs, const uin
 cudaError_t launch_qlen_hist(const fa_job *d_jobs, uint32_t n, uint32_t *d_hist, int sm_count, cudaStream_t s);
 cudaError_t launch_qlen_scatter(const fa_job *d_jobs, uint32_t n, uint32_t *d_cursor, uint32_t *d_order,
                                 cudaStream_t s);
+
+// Learned band predictor (band_model.cu).
+cudaError_t launch_band_features(const fa_job *d_jobs, uint32_t n, const uint8_t *d_q, const uint8_t *d_t,
+                                 const fa_band_hint *d_hints, int max_score, float *d_x, cudaStream_t s);
+cudaError_t launch_band_predict(const __nv_bfloat16 *d_wbf, const float *mean, const float *std_, const float *d_x,
+                                const fa_job *d_jobs, uint32_t n, float margin, int w_min, float *d_y,
+                                int32_t *d_w, cudaStream_t s);
+cudaError_t launch_band_backward(const __nv_bfloat16 *d_wbf, const float *mean, const float *std_, const float *d_x,
+                                 const float *d_target, uint32_t n, float tau, float inv_total, float *d_grad,
+                                 float *d_loss, cudaStream_t s);
+cudaError_t launch_band_adam(float *d_w, __nv_bfloat16 *d_wbf, float *d_m, float *d_v, const float *d_grad, float lr,
+                             int step, cudaStream_t s);
+// BF16 weights and normalisation of a model, for device-side prediction (band_api.cu).
+void band_model_export(const fa_band_model *m, std::vector<__nv_bfloat16> &wbf, float *mean, float *std_);
+// Device of a context (fa_api.cu).
+int fa_ctx_device(const fa_ctx *ctx);
 
 // Records the calling thread's fa_last_error() message and returns `code` (fa_api.cu).
 int set_last_error(int code, const char *msg);

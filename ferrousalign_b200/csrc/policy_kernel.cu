@@ -9,8 +9,10 @@
 // Learned policy: start at a predicted narrow band and double it while it is below
 // the configured band.  A narrow run is accepted when its band clamp never bound
 // (then every wider band reproduces it exactly) or, with FA_JUDGE_MAXOFF, when it
-// also passes the bwa-mem2 max_off test; otherwise the job continues on the ladder
-// and finally falls back to the plain policy at the configured band.
+// passes the bwa-mem2 max_off test (with FA_JUDGE_GLOBAL also requiring that its best
+// score is its end-to-end score); otherwise the band doubles -- or, when only the
+// end-to-end test failed, goes straight to the configured band -- and at the
+// configured band the plain policy takes over.
 //
 // The decisions compact the jobs that need another run into a list whose length
 // stays on the device, so a retry round needs no host round trip.
@@ -60,11 +62,19 @@ __global__ void policy_step_kernel(const fa_job *__restrict__ jobs, const uint32
         st.w_final[jid] = w;
         if (k < 0) {   // learned narrow ladder
             bool ok = !clamped[jid];
-            if (!ok && (judge & FA_JUDGE_MAXOFF)) ok = r.max_off < (w >> 1) + (w >> 2);
+            bool jump = false;
+            if (!ok && (judge & FA_JUDGE_MAXOFF)) {
+                const bool off_ok = r.max_off < (w >> 1) + (w >> 2);
+                const bool global = r.gscore == r.score;
+                ok = off_ok && (!(judge & FA_JUDGE_GLOBAL) || global);
+                // rejected only because the best score is not end-to-end: a wider
+                // narrow band would not change that, so go to the configured band
+                jump = off_ok && !ok;
+            }
             if (!ok) {
                 if (st.missed && st.tries[jid] == 1) st.missed[jid] = 1;
                 w <<= 1;
-                if (w >= jb.w) { w = jb.w; k = 0; }
+                if (jump || w >= jb.w) { w = jb.w; k = 0; }
                 st.w_cur[jid] = w;
                 st.k[jid] = k;
                 again = true;
@@ -88,6 +98,54 @@ __global__ void policy_step_kernel(const fa_job *__restrict__ jobs, const uint32
         base = __shfl_sync(0xffffffffu, base, __ffs(mask) - 1);
         if (again) next[base + __popc(mask & ((1u << lane) - 1u))] = jid;
     }
+}
+
+// Reorders a round's job list so that jobs running at their configured band come
+// first and jobs running below it (narrow) fill the list from the back: every warp then
+// holds jobs of one kind (a warp runs as long as its widest job), and the long jobs
+// start first, which balances the end of the launch.  The output has the same length
+// as the input; order inside each part follows the input in runs of up to one warp.
+__global__ void band_partition_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ list,
+                                      const uint32_t *__restrict__ count, uint32_t n_max,
+                                      const int32_t *__restrict__ w_cur, uint32_t *__restrict__ out,
+                                      uint32_t *__restrict__ n_wide, uint32_t *__restrict__ n_narrow)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t n = count ? min(*count, n_max) : n_max;
+    const bool live = t < n;
+    uint32_t jid = 0;
+    bool nar = false;
+    if (live) {
+        jid = list[t];
+        nar = w_cur[jid] < jobs[jid].w;
+    }
+    const unsigned mn = __ballot_sync(0xffffffffu, live && nar);
+    const unsigned mw = __ballot_sync(0xffffffffu, live && !nar);
+    const int lane = threadIdx.x & 31;
+    uint32_t bn = 0, bw = 0;
+    if (lane == 0) {
+        if (mn) bn = atomicAdd(n_narrow, (uint32_t)__popc(mn));
+        if (mw) bw = atomicAdd(n_wide, (uint32_t)__popc(mw));
+    }
+    bn = __shfl_sync(0xffffffffu, bn, 0);
+    bw = __shfl_sync(0xffffffffu, bw, 0);
+    if (!live) return;
+    const unsigned below = (1u << lane) - 1u;
+    if (nar) out[n - 1 - (bn + __popc(mn & below))] = jid;
+    else out[bw + __popc(mw & below)] = jid;
+}
+
+cudaError_t launch_band_partition(const fa_job *d_jobs, const uint32_t *d_list, const uint32_t *d_count,
+                                  uint32_t n_max, const int32_t *d_w_cur, uint32_t *d_out, uint32_t *d_n_wide,
+                                  uint32_t *d_n_narrow, cudaStream_t stream)
+{
+    if (n_max == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(d_n_wide, 0, 4, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_n_narrow, 0, 4, stream);
+    if (e != cudaSuccess) return e;
+    band_partition_kernel<<<(n_max + 255) / 256, 256, 0, stream>>>(d_jobs, d_list, d_count, n_max, d_w_cur, d_out,
+                                                                   d_n_wide, d_n_narrow);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_policy_init(const fa_job *d_jobs, uint32_t n, const int32_t *d_w_first, int w_min,

@@ -79,6 +79,7 @@ typedef struct {
 
 #define FA_JUDGE_CERT    1  /* accept a narrow run only when its band clamp never bound (sound) */
 #define FA_JUDGE_MAXOFF  2  /* also accept when max_off < (w>>1)+(w>>2) (the bwa-mem2 test)    */
+#define FA_JUDGE_GLOBAL  4  /* with MAXOFF: additionally require gscore == score              */
 
 typedef struct {
     int32_t mode;
@@ -220,6 +221,48 @@ int fa_mate_sw_batch(fa_ctx *ctx, const fa_mate_params *p, const fa_mate_job *jo
                      const uint8_t *qseq, uint64_t qseq_len,
                      const uint8_t *tseq, uint64_t tseq_len,
                      fa_kswr *out, fa_ext_stats *stats);
+
+/* ---- learned band (no reference counterpart) ----------------------------
+ * A 16-64-32-1 MLP (BF16 weights, FP32 accumulation) predicts log2 of the band each
+ * extension needs from 16 features of the job (seed length, lengths, h0, the chain's
+ * seed-diagonal spread, mismatch counts on the seed diagonal and its neighbours).
+ * Trained on the GPU by this library's own forward/backward/Adam kernels. */
+#define FA_BAND_NPARAMS 3201
+typedef struct {
+    int32_t diag_spread;   /* |diagonal difference| between the seed and its chain partner */
+    int32_t has_partner;   /* 1 if the chain has a second seed                             */
+} fa_band_hint;
+typedef struct fa_band_model fa_band_model;
+
+int  fa_band_model_create(uint64_t seed, fa_band_model **out);
+void fa_band_model_destroy(fa_band_model *m);
+int  fa_band_model_get(const fa_band_model *m, float *weights, float *mean16, float *std16);
+int  fa_band_model_set(fa_band_model *m, const float *weights, const float *mean16, const float *std16);
+int  fa_band_model_save(const fa_band_model *m, const char *path);   /* versioned, checksummed */
+int  fa_band_model_load(const char *path, fa_band_model **out);
+/* feature normalisation constants from a training feature matrix (n x 16) */
+int  fa_band_model_fit_norm(fa_band_model *m, const float *x, uint32_t n);
+/* x[n*16] raw features of host jobs (hints may be NULL) */
+int  fa_band_features(fa_ctx *ctx, const fa_params *p, const fa_job *jobs, uint32_t n,
+                      const uint8_t *qseq, uint64_t qseq_len, const uint8_t *tseq, uint64_t tseq_len,
+                      const fa_band_hint *hints, float *x);
+/* y[n] = MLP(x) (log2 band); w_out[n] = ceil(2^(y+margin)) raised to w_min, or job.w when
+ * that exceeds 2*w_min (such jobs are better started at the configured band) */
+int  fa_band_predict(fa_ctx *ctx, const fa_band_model *m, const float *x, const fa_job *jobs, uint32_t n,
+                     float margin, int w_min, float *y_out, int32_t *w_out);
+/* mean gradient and loss of the pinball(tau) loss on (x, target = log2 band) */
+int  fa_band_grad(fa_ctx *ctx, const fa_band_model *m, const float *x, const float *target, uint32_t n,
+                  float tau, float *grad, float *loss);
+/* Adam training on the GPU; epoch_loss[epochs] may be NULL */
+int  fa_band_train(fa_ctx *ctx, fa_band_model *m, const float *x, const float *target, uint32_t n, int epochs,
+                   uint32_t batch, float lr, float tau, uint64_t seed, float *epoch_loss);
+/* Learned-band extension: features and prediction on the GPU give each job its first
+ * band (w_first_out, may be NULL), then FA_POLICY_LEARNED runs as in fa_ext_batch_policy. */
+int  fa_ext_batch_learned(fa_ctx *ctx, const fa_params *p, const fa_policy *pol, const fa_band_model *model,
+                          float margin, const fa_job *jobs, uint32_t n,
+                          const uint8_t *qseq, uint64_t qseq_len, const uint8_t *tseq, uint64_t tseq_len,
+                          const fa_band_hint *hints, fa_ext_result *out, int32_t *w_first_out,
+                          int32_t *w_final, fa_ext_stats *stats);
 
 /* Device-resident variant (no reference counterpart): device pointers, kernels
  * asynchronous on `stream` after one small synchronous read of the batch's job

@@ -457,10 +457,15 @@ static int policy_one(const batch_t *B, uint32_t i)
             rc = run_ext(B->p, jb, B->qseq, B->tseq, w, &B->out[i], &tr);
             if (rc) break;
             cx += tr.cells; ntries += 1;
-            int ok = !tr.clamped;
-            if (!ok && (pol->judge & FA_JUDGE_MAXOFF))
-                ok = B->out[i].max_off < (w >> 1) + (w >> 2);
+            int ok = !tr.clamped, jump = 0;
+            if (!ok && (pol->judge & FA_JUDGE_MAXOFF)) {
+                int off_ok = B->out[i].max_off < (w >> 1) + (w >> 2);
+                int global = B->out[i].gscore == B->out[i].score;
+                ok = off_ok && (!(pol->judge & FA_JUDGE_GLOBAL) || global);
+                jump = off_ok && !ok;
+            }
             if (ok) { accepted = 1; wfin = w; break; }
+            if (jump) break;   /* straight to the configured band */
             w <<= 1;
         }
         if (!rc && !accepted)
