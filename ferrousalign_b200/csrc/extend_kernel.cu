@@ -29,6 +29,65 @@ __device__ __forceinline__ int32_t prmt_s8(uint32_t lo, uint32_t hi, uint32_t se
     return static_cast<int32_t>(r);
 }
 
+// Exit-bound certificate (CERT = true).  A path that leaves the run's computed
+// region first steps onto a gap cell the run itself evaluates: the F value just past
+// a row's end, the E value of a column the band drops on the left, the first column
+// when the band leaves it, or the first row beyond the band.  From such an exit of
+// value x at (ix, jx) the path reaches row i with a score of at most
+//     min(x + a*(i-ix), x + a*D - e_del*(i-ix-D)),   D = qlen-1-jx,  a = max(mat),
+// a tent in i.  P1/P3 hold, per side (right exits, left exits), the maxima of the
+// two lines' intercepts.  The run's outputs are those of every wider run when:
+//   * every row up to the last max / gscore event has its row max above the bound
+//     (so row maxima, their first columns and the z-drop decisions agree),
+//   * the bound stays below min(score, gscore) on every processed row, and on the
+//     rows a wider run could still process after a zero row,
+//   * a z-drop break row passes the first test too (a wider run breaks there),
+//   * the run never read a column no earlier row wrote (a first-row value standing in
+//     for a later row), and the wider band's first row covers every positive
+//     first-row value (so neither run does).
+// Widening is monotone in every cell, so the wider run sees the same values inside
+// this run's region, raised only by exiting paths, which the tents bound.
+struct ExitBound {
+    static constexpr int NEG = -(1 << 29);
+    int p1[2], p3[2];
+    __device__ __forceinline__ void init() { p1[0] = p1[1] = p3[0] = p3[1] = NEG; }
+    __device__ __forceinline__ void add(int side, int x, int ix, int jx, int qlen, int a, int e_del) {
+        if (x > 0) {
+            const int D = qlen - 1 - jx;
+            p1[side] = max(p1[side], x - a * ix);
+            p3[side] = max(p3[side], x + (a + e_del) * D + e_del * ix);
+        }
+    }
+    __device__ __forceinline__ int at(int i, int a, int e_del) const {
+        int b = NEG;
+#pragma unroll
+        for (int s = 0; s < 2; ++s)
+            if (p1[s] != NEG) b = max(b, min(p1[s] + a * i, p3[s] - e_del * i));
+        return b;
+    }
+    // max over integer rows i0..i1 of at(i): each tent is concave, so its maximum over
+    // the interval sits at the integer rows beside the crossing of its two lines
+    __device__ __forceinline__ int max_over(int i0, int i1, int a, int e_del) const {
+        int b = NEG;
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            if (p1[s] == NEG) continue;
+            int c = i1;
+            if (a + e_del > 0) {
+                const int num = p3[s] - p1[s], den = a + e_del;
+                c = num >= 0 ? num / den : -((-num + den - 1) / den);   // floor
+            }
+#pragma unroll
+            for (int d = 0; d < 2; ++d) {
+                const int k = min(max(c + d, i0), i1);
+                b = max(b, min(p1[s] + a * k, p3[s] - e_del * k));
+            }
+        }
+        return b;
+    }
+};
+
+template <bool CERT>
 __global__ void __launch_bounds__(kExtThreads)
 ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ order,
                   uint32_t n, const uint32_t *__restrict__ n_dev, const uint8_t *__restrict__ qseq,
@@ -70,7 +129,7 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
             // Query codes and the first row: eh[0]=h0, eh[1]=h0-oe_ins, then -e_ins
             // while the previous value exceeds e_ins (ksw_affine_gap.rs:1017-1025).
             uint32_t bad = 0;
-            int hp = h0;
+            int hp = h0, init_reach = 0;
             bool filling = true;
             for (int j = 0; j <= qlen; ++j) {
                 uint32_t q = 0;
@@ -85,11 +144,17 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
                 else if (filling && hp > e_ins) h = hp - e_ins;
                 else { filling = false; h = 0; }
                 hp = h;
+                if (CERT && j > 0 && h > 0) init_reach = j;
                 col[j * T] = (uint32_t)h << 16 | q;
             }
 
             int best = h0, max_i = -1, max_j = -1, max_ie = -1, gscore = -1, max_off = 0;
             int beg = 0, end = qlen, clamped = 0;
+            const int a = p.max_score;
+            ExitBound xb;
+            int bmax = ExitBound::NEG, first_fail = INT32_MAX, max_written = -1, rows = 0;
+            bool row_ok = true, stale = false, broke = false, zbreak = false;
+            if (CERT) xb.init();
             for (int i = 0; i < tlen; ++i) {
                 const uint32_t tb = Tg[i];
                 if (tb >= (uint32_t)p.m) { bad = 1; break; }
@@ -103,6 +168,19 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
                 if (end > i + w + 1) end = i + w + 1;
                 if (end > qlen) end = qlen;
                 clamped |= (beg != beg_a) | (end != end_a);
+                if (CERT) {
+                    ++rows;
+                    if (i == 0) {
+                        if (end < qlen) xb.add(0, (int)(col[end * T] >> 16), -1, end - 1, qlen, a, e_del);
+                    } else {
+                        for (int j = beg_a; j < beg && j < qlen; ++j)          // columns the band drops
+                            xb.add(1, (int)((col[j * T] >> 3) & 0x1FFFu), i, j, qlen, a, e_del);
+                        if (beg_a == 0 && beg > 0)                            // the first column leaves
+                            xb.add(1, h0 - (p.o_del + e_del * i), i - 1, -1, qlen, a, e_del);
+                        const int lo = max(beg, max_written + 1), hi = min(end - 1, init_reach);
+                        stale |= lo <= hi;                                    // a never-written column
+                    }
+                }
 
                 int h1 = 0;
                 if (beg == 0) {
@@ -133,7 +211,15 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
                 if (end == qlen && gscore < h1) { gscore = h1; max_ie = i; }
                 const int m_row = key >> 12;
                 const int mj = 4095 - (key & 4095);
-                if (m_row == 0) break;
+                if (CERT) {
+                    max_written = max(max_written, end);
+                    if (end < qlen) xb.add(0, f, i, end, qlen, a, e_del);   // F past the row's end
+                    const int b = xb.at(i, a, e_del);
+                    row_ok = m_row > 0 ? b < m_row : b <= 0;
+                    if (!row_ok && first_fail == INT32_MAX) first_fail = i;
+                    bmax = max(bmax, b);
+                }
+                if (m_row == 0) { broke = true; break; }
                 if (m_row > best) {
                     best = m_row; max_i = i; max_j = mj;
                     const int off = mj > i ? mj - i : i - mj;
@@ -141,8 +227,9 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
                 } else if (p.zdrop > 0) {
                     const int di = i - max_i, dj = mj - max_j;
                     if (di > dj) {
-                        if (best - m_row - (di - dj) * e_del > p.zdrop) break;
+                        if (best - m_row - (di - dj) * e_del > p.zdrop) { broke = zbreak = true; break; }
                     } else if (best - m_row - (dj - di) * e_ins > p.zdrop) {
+                        broke = zbreak = true;
                         break;
                     }
                 }
@@ -162,7 +249,18 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
             r.gscore = gscore;
             r.max_off = max_off;
             out[jid] = r;
-            if (clamped_out) clamped_out[jid] = (uint8_t)clamped;
+            uint8_t flags = (uint8_t)clamped;
+            if (CERT) {
+                const int i_ev = max(max_i, max_ie), lim = min(best, gscore);
+                // after a zero row every live path has left the region: a wider run's
+                // remaining rows are bounded by the tents over [last row, tlen-1]
+                const bool tail_ok = !broke || (zbreak ? row_ok : xb.max_over(rows - 1, tlen - 1, a, e_del) < lim);
+                const int W = ext_band_clamp(qlen, jb.w, p);
+                const bool wide_clean = init_reach <= min(W + 1, qlen);
+                const bool cert = !stale && gscore > 0 && first_fail > i_ev && tail_ok && bmax < lim && wide_clean;
+                flags |= (uint8_t)cert << 1;
+            }
+            if (clamped_out) clamped_out[jid] = flags;
             if (cells_job) cells_job[jid] = cells;
         }
     }
@@ -187,13 +285,13 @@ cudaError_t launch_ext_packed(const fa_job *d_jobs, const uint32_t *d_order, uin
 {
     if (n == 0) return cudaSuccess;
     const size_t smem = ext_packed_smem_bytes(qcap);
-    cudaError_t err = cudaFuncSetAttribute(ext_packed_kernel,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // the certificate variant runs whenever per-job flags are asked for
+    auto kern = d_clamped ? ext_packed_kernel<true> : ext_packed_kernel<false>;
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return err;
     const uint32_t blocks = (n + kExtThreads - 1) / kExtThreads;
-    ext_packed_kernel<<<blocks, kExtThreads, smem, stream>>>(d_jobs, d_order, n, d_n, d_qseq, d_tseq, p,
-                                                             qcap, d_w_try, d_out, d_clamped,
-                                                             d_cells_job, d_cells, d_status);
+    kern<<<blocks, kExtThreads, smem, stream>>>(d_jobs, d_order, n, d_n, d_qseq, d_tseq, p, qcap, d_w_try,
+                                                d_out, d_clamped, d_cells_job, d_cells, d_status);
     return cudaGetLastError();
 }
 

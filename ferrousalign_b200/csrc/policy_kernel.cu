@@ -8,7 +8,10 @@
 //
 // Learned policy: start at a predicted narrow band and double it while it is below
 // the configured band.  A narrow run is accepted when its band clamp never bound
-// (then every wider band reproduces it exactly) or, with FA_JUDGE_MAXOFF, when it
+// (then every wider band reproduces it exactly), with FA_JUDGE_BOUND when its
+// exit-bound certificate holds (it then equals the configured-band run, proven; see
+// extend_kernel.cu) and that run would also end the plain ladder, or, with
+// FA_JUDGE_MAXOFF (empirical, not exact), when it
 // passes the bwa-mem2 max_off test (with FA_JUDGE_GLOBAL also requiring that its best
 // score is its end-to-end score); otherwise the band doubles -- or, when only the
 // end-to-end test failed, goes straight to the configured band -- and at the
@@ -61,7 +64,11 @@ __global__ void policy_step_kernel(const fa_job *__restrict__ jobs, const uint32
         st.tries[jid] += 1;
         st.w_final[jid] = w;
         if (k < 0) {   // learned narrow ladder
-            bool ok = !clamped[jid];
+            const uint8_t fl = clamped[jid];   // bit 0: band clamp bound, bit 1: exit-bound certificate
+            bool ok = !(fl & 1);
+            if (!ok && (judge & FA_JUDGE_BOUND))
+                // certified equal to the configured-band run, which the plain policy keeps
+                ok = (fl & 2) && (r.score == st.prev[jid] || r.max_off < (jb.w >> 1) + (jb.w >> 2));
             bool jump = false;
             if (!ok && (judge & FA_JUDGE_MAXOFF)) {
                 const bool off_ok = r.max_off < (w >> 1) + (w >> 2);

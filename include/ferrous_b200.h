@@ -80,6 +80,8 @@ typedef struct {
 #define FA_JUDGE_CERT    1  /* accept a narrow run only when its band clamp never bound (sound) */
 #define FA_JUDGE_MAXOFF  2  /* also accept when max_off < (w>>1)+(w>>2) (the bwa-mem2 test)    */
 #define FA_JUDGE_GLOBAL  4  /* with MAXOFF: additionally require gscore == score              */
+#define FA_JUDGE_BOUND   8  /* accept when the exit-bound certificate holds (sound): no path
+                               leaving the narrow run's region can reach any output statistic */
 
 typedef struct {
     int32_t mode;

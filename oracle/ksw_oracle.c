@@ -49,6 +49,13 @@ static int ext_band_clamp(int qlen, int m, const int8_t *mat, int o_del, int e_d
 
 typedef struct { int32_t h, e; } eh_t;
 
+int ora_wide_clean(const fa_params *p, int qlen, int W, int init_reach)
+{
+    W = ext_band_clamp(qlen, p->m, p->mat, p->o_del, p->e_del, p->o_ins, p->e_ins, W, p->end_bonus);
+    const int end0 = W + 1 < qlen ? W + 1 : qlen;
+    return init_reach <= end0;
+}
+
 int ora_ksw_extend2(int qlen, const uint8_t *query, int tlen, const uint8_t *target,
                     int m, const int8_t *mat, int o_del, int e_del, int o_ins, int e_ins,
                     int w, int end_bonus, int zdrop, int h0,
@@ -71,6 +78,8 @@ int ora_ksw_extend2(int qlen, const uint8_t *query, int tlen, const uint8_t *tar
     eh[0].h = h0;
     eh[1].h = h0 > oe_ins ? h0 - oe_ins : 0;
     for (int j = 2; j <= qlen && eh[j - 1].h > e_ins; ++j) eh[j].h = eh[j - 1].h - e_ins;
+    int init_reach = 0;
+    for (int j = 1; j <= qlen; ++j) if (eh[j].h > 0) init_reach = j;
 
     w = ext_band_clamp(qlen, m, mat, o_del, e_del, o_ins, e_ins, w, end_bonus);
 
@@ -78,6 +87,24 @@ int ora_ksw_extend2(int qlen, const uint8_t *query, int tlen, const uint8_t *tar
     int beg = 0, end = qlen;
     int64_t cells = 0;
     int rows = 0, clamped = 0, label = 0;
+
+    /* Exit-bound certificate.  Every path that leaves the computed region does so
+     * through a gap cell the run itself computes (the F value past a row's end,
+     * the E value of a column the band drops on the left, the first column or the
+     * first row beyond the band).  From such an exit x at (ix, jx) the path can
+     * reach row i with at most  min(x + a*(i-ix), x + a*D - e_del*(i-ix-D)),
+     * D = qlen-1-jx.  P1 and P3 keep the maxima of the two lines' intercepts. */
+    int a = 0;
+    for (int k = 0; k < m * m; ++k) if (mat[k] > a) a = mat[k];
+    const int NEG = -(1 << 29);
+    /* [0]: exits on the right (F past the row end, first row), [1]: on the left
+     * (dropped columns, first column); each side's tents peak near one row */
+    int P1[2] = {NEG, NEG}, P3[2] = {NEG, NEG};
+    int bmax = NEG, first_fail = INT32_MAX, row_ok = 1, stale = 0;
+    int max_written = -1, broke = 0, zbreak = 0;
+#define ORA_EXIT(side, x, ix, jx) do { const int x_ = (x), ix_ = (ix), D_ = qlen - 1 - (jx); \
+        if (x_ > 0) { if (x_ - a * ix_ > P1[side]) P1[side] = x_ - a * ix_;                 \
+            const int t_ = x_ + (a + e_del) * D_ + e_del * ix_; if (t_ > P3[side]) P3[side] = t_; } } while (0)
 
     for (int i = 0; i < tlen; ++i) {
         int f = 0, m_row = 0, mj = -1;
@@ -93,6 +120,18 @@ int ora_ksw_extend2(int qlen, const uint8_t *query, int tlen, const uint8_t *tar
         if (i - beg > label) label = i - beg;
         if (end - 1 - i > label) label = end - 1 - i;
         if (end > beg) cells += end - beg;
+        if (i == 0) {
+            if (end < qlen) ORA_EXIT(0, eh[end].h, -1, end - 1);       /* first row past the band */
+        } else {
+            for (int j = beg_a; j < beg && j < qlen; ++j) ORA_EXIT(1, eh[j].e, i, j);  /* dropped column */
+            if (beg_a == 0 && beg > 0) {                               /* first column leaves */
+                const int x = h0 - (o_del + e_del * i);
+                ORA_EXIT(1, x, i - 1, -1);
+            }
+            const int lo = beg > max_written + 1 ? beg : max_written + 1;
+            const int hi = end - 1 < init_reach ? end - 1 : init_reach;
+            if (lo <= hi) stale = 1;                                   /* reads a never-written cell */
+        }
 
         /* first column */
         int h1;
@@ -125,7 +164,21 @@ int ora_ksw_extend2(int qlen, const uint8_t *query, int tlen, const uint8_t *tar
             int h_end = end == qlen ? h1 : eh[qlen - 1].h;
             if (gscore < h_end) { gscore = h_end; max_ie = i; }   /* earliest row wins ties */
         }
-        if (m_row == 0) break;
+        if (end > max_written) max_written = end;
+        if (end < qlen) ORA_EXIT(0, f, i, end);                        /* F past the row's end */
+        {
+            int b = NEG;
+            for (int sd = 0; sd < 2; ++sd) {
+                if (P1[sd] == NEG) continue;
+                const int b1 = P1[sd] + a * i, b3 = P3[sd] - e_del * i;
+                const int bs = b1 < b3 ? b1 : b3;
+                if (bs > b) b = bs;
+            }
+            row_ok = m_row > 0 ? b < m_row : b <= 0;
+            if (!row_ok && first_fail == INT32_MAX) first_fail = i;
+            if (b > bmax) bmax = b;
+        }
+        if (m_row == 0) { broke = 1; break; }
         if (m_row > max) {
             max = m_row; max_i = i; max_j = mj;
             int off = mj - i; if (off < 0) off = -off;
@@ -133,8 +186,9 @@ int ora_ksw_extend2(int qlen, const uint8_t *query, int tlen, const uint8_t *tar
         } else if (zdrop > 0) {
             int di = i - max_i, dj = mj - max_j;
             if (di > dj) {
-                if (max - m_row - (di - dj) * e_del > zdrop) break;
+                if (max - m_row - (di - dj) * e_del > zdrop) { broke = zbreak = 1; break; }
             } else if (max - m_row - (dj - di) * e_ins > zdrop) {
+                broke = zbreak = 1;
                 break;
             }
         }
@@ -159,7 +213,38 @@ int ora_ksw_extend2(int qlen, const uint8_t *query, int tlen, const uint8_t *tar
         trace->clamped = clamped;
         trace->label = label < 0 ? 0 : label;
         trace->w_eff = w;
+        /* outputs are fixed by the rows up to the last max or gscore event; the
+         * break row must match too, so the wider run stops at the same row */
+        const int i_ev = max_i > max_ie ? max_i : max_ie;
+        const int lim = max < gscore ? max : gscore;
+        /* after a zero row every live path has left the region: the rows a wider
+         * run may still process are bounded by the tents over [rows-1, tlen-1] */
+        int fut = NEG;
+        if (broke && !zbreak) {
+            const int i0 = rows - 1, i1 = tlen - 1;
+            for (int sd = 0; sd < 2; ++sd) {
+                if (P1[sd] == NEG) continue;
+                /* tent peak where the two lines meet; its max over [i0, i1] */
+                int lo = i0, hi = i1;
+                while (lo < hi) {            /* first row where the falling line is lower */
+                    const int mid = lo + (hi - lo) / 2;
+                    if (P3[sd] - e_del * mid <= P1[sd] + a * mid) hi = mid; else lo = mid + 1;
+                }
+                int best_t = NEG;
+                for (int k = lo - 1; k <= lo; ++k) {
+                    if (k < i0 || k > i1) continue;
+                    const int b1 = P1[sd] + a * k, b3 = P3[sd] - e_del * k;
+                    const int v = b1 < b3 ? b1 : b3;
+                    if (v > best_t) best_t = v;
+                }
+                if (best_t > fut) fut = best_t;
+            }
+        }
+        const int tail_ok = !broke || (zbreak ? row_ok : fut < lim);
+        trace->bound_ok = !stale && gscore > 0 && first_fail > i_ev && tail_ok && bmax < lim;
+        trace->init_reach = init_reach;
     }
+#undef ORA_EXIT
     free(qp);
     free(eh);
     return FA_OK;
@@ -458,6 +543,11 @@ static int policy_one(const batch_t *B, uint32_t i)
             if (rc) break;
             cx += tr.cells; ntries += 1;
             int ok = !tr.clamped, jump = 0;
+            if (!ok && (pol->judge & FA_JUDGE_BOUND)) {
+                const int prev0 = jb->dir == FA_DIR_RIGHT ? jb->h0 : 0;
+                ok = tr.bound_ok && ora_wide_clean(B->p, jb->qlen, jb->w, tr.init_reach) &&
+                     (B->out[i].score == prev0 || B->out[i].max_off < (jb->w >> 1) + (jb->w >> 2));
+            }
             if (!ok && (pol->judge & FA_JUDGE_MAXOFF)) {
                 int off_ok = B->out[i].max_off < (w >> 1) + (w >> 2);
                 int global = B->out[i].gscore == B->out[i].score;

@@ -28,7 +28,15 @@ typedef struct {
     int32_t label;     /* max over rows of max(i-beg, end-1-i, 0): the
                           smallest band that reproduces this run exactly    */
     int32_t w_eff;     /* band after the max_ins / max_del clamp             */
+    int32_t bound_ok;  /* exit-bound certificate: no path that leaves this
+                          run's computed region can change any output       */
+    int32_t init_reach;/* last column whose first-row value is positive     */
 } ora_ext_trace;
+
+/* The exit-bound certificate of a narrow run at band w transfers to a run at
+ * configured band W >= w when W's first row covers every positive first-row
+ * cell (so W never reads an unwritten column).  Returns 1 if so. */
+int ora_wide_clean(const fa_params *p, int qlen, int W, int init_reach);
 
 /* ksw_extend2 (ksw_affine_gap.rs:952-1169).  Returns FA_OK, or FA_ERR_ARG
  * where the reference panics (h0 <= 0, qlen <= 0, code >= m). */

@@ -14,7 +14,7 @@ HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libksw_oracle.so"
 
 TRACE_DT = np.dtype([("cells", "<i8"), ("rows", "<i4"), ("clamped", "<i4"), ("label", "<i4"),
-                     ("w_eff", "<i4")])
+                     ("w_eff", "<i4"), ("bound_ok", "<i4"), ("init_reach", "<i4")])
 EXT_RESULT_DT = np.dtype([("score", "<i4"), ("qle", "<i4"), ("tle", "<i4"), ("gtle", "<i4"),
                           ("gscore", "<i4"), ("max_off", "<i4")])
 KSWR_DT = np.dtype([("score", "<i4"), ("te", "<i4"), ("qe", "<i4"), ("score2", "<i4"),
@@ -39,6 +39,8 @@ def load() -> C.CDLL:
         lib.ora_ext_batch.argtypes = [P, P, C.c_uint32, P, P, P, P, C.c_int]
         lib.ora_ext_batch_policy.restype = C.c_int
         lib.ora_ext_batch_policy.argtypes = [P, P, P, C.c_uint32, P, P, P, P, P, P, P, C.c_int]
+        lib.ora_wide_clean.restype = C.c_int
+        lib.ora_wide_clean.argtypes = [P, C.c_int, C.c_int, C.c_int]
         lib.ora_mate_batch.restype = C.c_int
         lib.ora_mate_batch.argtypes = [P, P, C.c_uint32, P, P, P, P, C.c_int]
         _lib = lib
@@ -65,6 +67,11 @@ def ksw_extend2(query, target, mat, o_del, e_del, o_ins, e_ins, w, end_bonus, zd
     if rc:
         raise ValueError(f"oracle ksw_extend2 rejected the input ({rc})")
     return out[0], tr[0]
+
+
+def wide_clean(params, qlen: int, w: int, init_reach: int) -> bool:
+    """Whether band w's first row covers every positive first-row cell."""
+    return bool(load().ora_wide_clean(_p(params), qlen, w, init_reach))
 
 
 def ksw_align2(query, target, mat, o_del, e_del, o_ins, e_ins, xtra):

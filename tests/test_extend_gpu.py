@@ -124,12 +124,33 @@ def test_policies_match_oracle(ctx):
     assert st["retries"] == (rtries - 1).sum()
     rng = np.random.default_rng(5)
     wf = rng.choice([5, 10, 20, 40], size=len(b.jobs)).astype(np.int32)
-    for judge in (N.FA_JUDGE_CERT, N.FA_JUDGE_CERT | N.FA_JUDGE_MAXOFF):
+    for judge in (N.FA_JUDGE_CERT, N.FA_JUDGE_CERT | N.FA_JUDGE_MAXOFF, N.FA_JUDGE_BOUND):
         pol = fa.make_policy(N.FA_POLICY_LEARNED, 2, judge, 1)
         out, st, wfin = fa.extend_batch(p, b.jobs, b.qseq, b.tseq, policy=pol, w_first=wf, ctx=ctx)
         ref, rwfin, rtries, _ = O.ext_batch_policy(p, pol, b.jobs, b.qseq, b.tseq, wf)
         assert np.array_equal(out, ref), diff_report(out, ref)
-        assert np.array_equal(wfin, rwfin)
+        assert np.array_equal(wfin, rwfin)     # same acceptance decisions, so the same certificates
+
+
+@pytest.mark.parametrize("workload", ["mixture", "uneven"])
+def test_bound_judge_is_exact_and_matches_oracle(ctx, workload):
+    """Narrow bands accepted by the exit-bound certificate reproduce the plain
+    policy bit for bit; the GPU takes the same decisions as the oracle."""
+    if workload == "mixture":
+        b = synth.workload_ext_1m(100_000, seed=23)
+    else:
+        b = synth.workload_ext_uneven(50_000, seed=24, ref_len=5_000_000)
+    p = fa.BandedPairWiseSW().to_struct()
+    plain, pst, _ = fa.extend_batch(p, b.jobs, b.qseq, b.tseq, policy=fa.make_policy(N.FA_POLICY_BWA, 2), ctx=ctx)
+    rng = np.random.default_rng(7)
+    wf = rng.choice([2, 4, 8, 16, 32], size=len(b.jobs)).astype(np.int32)
+    pol = fa.make_policy(N.FA_POLICY_LEARNED, 2, N.FA_JUDGE_BOUND, 1)
+    out, st, wfin = fa.extend_batch(p, b.jobs, b.qseq, b.tseq, policy=pol, w_first=wf, ctx=ctx)
+    assert np.array_equal(out, plain), diff_report(out, plain)
+    ref, rwfin, rtries, rcells = O.ext_batch_policy(p, pol, b.jobs, b.qseq, b.tseq, wf)
+    assert np.array_equal(wfin, rwfin)
+    assert st["cells_executed"] == rcells.sum()
+    assert st["cells_executed"] < pst["cells_executed"]
 
 
 def test_reference_style_interface(ctx):
