@@ -1,10 +1,10 @@
 """Learned band predictor: Python side of the band-model C ABI.
 
 A 16-64-32-1 MLP (BF16 weights, FP32 accumulation) maps 16 features of an extension job
-to log2 of the narrowest band that still reproduces the full-band result and passes the
-acceptance judge.  Features, prediction and training (forward, backward, Adam) run in
-this library's own CUDA kernels; `make_labels` derives training labels from the plain
-extension itself, run at a ladder of bands.
+to log2 of the narrowest band whose run the exit-bound certificate proves equal to the
+configured-band run.  Features, prediction and training (forward, backward, Adam) run in
+this library's own CUDA kernels; `make_labels` derives training labels from the
+extension itself, run along band ladders with the certificate as the judge.
 """
 from __future__ import annotations
 
@@ -15,9 +15,14 @@ import numpy as np
 
 from . import _native as N
 
-LADDER = (4, 6, 8, 12, 16, 24, 32, 48, 64)
+LADDER_STARTS = (2, 3)          # doubling ladders 2,4,8,..,64 and 3,6,12,..,96
 HINT_DT = np.dtype([("diag_spread", "<i4"), ("has_partner", "<i4")])
 DEFAULT_MODEL = Path(__file__).resolve().parent / "band_model_151bp.bin"
+# exact: a narrow run is accepted only with a proof that it equals the configured band's
+JUDGE_EXACT = N.FA_JUDGE_CERT | N.FA_JUDGE_BOUND
+# the learned path's default: exact judge, one narrow try, then the configured band
+JUDGE_LEARNED = JUDGE_EXACT | N.FA_JUDGE_ONCE
+# empirical: also accept on the bwa-mem2 max_off test plus an end-to-end check (not exact)
 JUDGE_FAST = N.FA_JUDGE_CERT | N.FA_JUDGE_MAXOFF | N.FA_JUDGE_GLOBAL
 
 
@@ -120,41 +125,27 @@ def hints_from_info(info: np.ndarray) -> np.ndarray:
     return h
 
 
-def judge_accepts(out: np.ndarray, w: int, judge: int = JUDGE_FAST) -> np.ndarray:
-    """The policy's acceptance test for a narrow run at band w (without the clamp
-    certificate, which never fires on the 151-bp workload)."""
-    ok = np.zeros(len(out), bool)
-    if judge & N.FA_JUDGE_MAXOFF:
-        ok = out["max_off"] < (w >> 1) + (w >> 2)
-        if judge & N.FA_JUDGE_GLOBAL:
-            ok &= out["gscore"] == out["score"]
-    return ok
-
-
-def make_labels(params: np.ndarray, jobs: np.ndarray, qseq: np.ndarray, tseq: np.ndarray, plain: np.ndarray,
-                judge: int = JUDGE_FAST, ladder=LADDER, ctx: N.Context | None = None):
-    """Smallest ladder band whose single run equals the plain result and passes the
-    judge; the configured band (job.w) when none does.  Returns (labels, cells per band)."""
-    from .batch_extension import extend_batch
-    n = len(jobs)
+def make_labels(params: np.ndarray, jobs: np.ndarray, qseq: np.ndarray, tseq: np.ndarray,
+                starts=LADDER_STARTS, ctx: N.Context | None = None):
+    """Smallest band of the doubling ladders from `starts` whose run is certified equal
+    to the configured-band run (the learned policy's w_final with every job starting
+    at the ladder's first rung); the configured band when no rung certifies.
+    Returns (labels, executed cells per ladder)."""
+    from .batch_extension import extend_batch, make_policy
     label = jobs["w"].astype(np.int32).copy()
-    done = np.zeros(n, bool)
     cells = {}
-    for w in ladder:
-        j = jobs.copy()
-        j["w"] = np.minimum(j["w"], w)
-        out, st, _ = extend_batch(params, j, qseq, tseq, ctx=ctx)
-        cells[w] = int(st["cells"])
-        good = (out == plain) & judge_accepts(out, w, judge)
-        newly = good & ~done
-        label[newly] = np.minimum(w, jobs["w"][newly])
-        done |= good
+    for w0 in starts:
+        wf = np.full(len(jobs), w0, np.int32)
+        _, st, wfin = extend_batch(params, jobs, qseq, tseq, policy=make_policy(N.FA_POLICY_LEARNED, 2, JUDGE_EXACT, 1),
+                                   w_first=wf, ctx=ctx)
+        label = np.minimum(label, np.minimum(wfin, jobs["w"]))
+        cells[w0] = int(st["cells_executed"])
     return label, cells
 
 
 def extend_batch_learned(params: np.ndarray, jobs: np.ndarray, qseq: np.ndarray, tseq: np.ndarray,
-                         model: BandModel, hints: np.ndarray | None = None, judge: int = JUDGE_FAST,
-                         margin: float = 0.0, w_min: int = 16, max_tries: int = 2, ctx: N.Context | None = None):
+                         model: BandModel, hints: np.ndarray | None = None, judge: int = JUDGE_LEARNED,
+                         margin: float = 0.0, w_min: int = 2, max_tries: int = 2, ctx: N.Context | None = None):
     """fa_ext_batch_learned: predicted first band, judge, doubling up to job.w, then the
     bwa-mem2 policy.  Returns (results, stats, w_first, w_final)."""
     from .batch_extension import make_policy

@@ -176,9 +176,12 @@ __device__ __forceinline__ void load_norm(const float *__restrict__ xr, const No
 }
 
 // Inference: y = MLP(x) in log2(band) units; band = ceil(2^(y + margin)) raised to
-// w_min.  A band above 2*w_min starts at the configured band: such jobs are mostly
-// rejected by the acceptance judge at any narrow band, and a rejected mid-size first
-// run costs more than starting wide.
+// w_min and rounded up to the ladder 2, 3, 4, 6, 8, 12, ... (bands of one launch fall
+// into few classes, which the band partition turns into uniform warps; doubling after a
+// rejection stays on the ladder).  A band above half the configured band starts at the
+// configured band: its
+// narrow run would save less than half the cells, and a rejected one costs more than
+// starting wide.
 __global__ void __launch_bounds__(128) band_predict_kernel(const __nv_bfloat16 *__restrict__ wbf, NormConsts nc,
                                                            const float *__restrict__ x, const fa_job *__restrict__ jobs,
                                                            uint32_t n, float margin, int w_min,
@@ -198,7 +201,11 @@ __global__ void __launch_bounds__(128) band_predict_kernel(const __nv_bfloat16 *
         const float e = fminf(fmaxf(y + margin, 0.f), 16.f);
         int band = (int)ceilf(exp2f(e));
         band = max(band, w_min);
-        if (band > 2 * w_min) band = wj;
+        if (band > 2) {                 // up to the ladder 2^k, 3*2^(k-1): few distinct bands per launch
+            const int p2 = 1 << (32 - __clz(band - 1));
+            band = 3 * p2 / 4 >= band ? 3 * p2 / 4 : p2;
+        }
+        if (2 * band > wj) band = wj;   // a narrow run above half the configured band saves too little
         band = min(band, wj);
         w_out[i] = band;
     }

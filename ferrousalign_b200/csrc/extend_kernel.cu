@@ -131,21 +131,30 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
             uint32_t bad = 0;
             int hp = h0, init_reach = 0;
             bool filling = true;
-            for (int j = 0; j <= qlen; ++j) {
-                uint32_t q = 0;
-                if (j < qlen) {
-                    q = Q[j];
-                    bad |= q >= (uint32_t)p.m;
-                    q &= 7u;
+            // eight independent byte loads in flight per thread before their first use
+            for (int j0 = 0; j0 <= qlen; j0 += 8) {
+                uint32_t qb[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) qb[u] = j0 + u < qlen ? (uint32_t)Q[j0 + u] : 0u;
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int j = j0 + u;
+                    if (j <= qlen) {
+                        uint32_t q = qb[u];
+                        if (j < qlen) {
+                            bad |= q >= (uint32_t)p.m;
+                            q &= 7u;
+                        }
+                        int h;
+                        if (j == 0) h = h0;
+                        else if (j == 1) h = h0 > oe_ins ? h0 - oe_ins : 0;
+                        else if (filling && hp > e_ins) h = hp - e_ins;
+                        else { filling = false; h = 0; }
+                        hp = h;
+                        if (CERT && j > 0 && h > 0) init_reach = j;
+                        col[j * T] = (uint32_t)h << 16 | q;
+                    }
                 }
-                int h;
-                if (j == 0) h = h0;
-                else if (j == 1) h = h0 > oe_ins ? h0 - oe_ins : 0;
-                else if (filling && hp > e_ins) h = hp - e_ins;
-                else { filling = false; h = 0; }
-                hp = h;
-                if (CERT && j > 0 && h > 0) init_reach = j;
-                col[j * T] = (uint32_t)h << 16 | q;
             }
 
             int best = h0, max_i = -1, max_j = -1, max_ie = -1, gscore = -1, max_off = 0;
@@ -155,8 +164,24 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
             int bmax = ExitBound::NEG, first_fail = INT32_MAX, max_written = -1, rows = 0;
             bool row_ok = true, stale = false, broke = false, zbreak = false;
             if (CERT) xb.init();
+            // target bases arrive 5 to 8 rows ahead of their row: tq0 holds the current
+            // group of four, tq1 the next, loaded when tq0 is used up
+            uint32_t tq0 = 0, tq1 = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (k < tlen) tq0 |= (uint32_t)Tg[k] << (8 * k);
+                if (4 + k < tlen) tq1 |= (uint32_t)Tg[4 + k] << (8 * k);
+            }
             for (int i = 0; i < tlen; ++i) {
-                const uint32_t tb = Tg[i];
+                const uint32_t tb = tq0 & 0xFFu;
+                tq0 >>= 8;
+                if ((i & 3) == 3) {
+                    tq0 = tq1;
+                    tq1 = 0;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        if (i + 5 + k < tlen) tq1 |= (uint32_t)Tg[i + 5 + k] << (8 * k);
+                }
                 if (tb >= (uint32_t)p.m) { bad = 1; break; }
                 uint32_t row_lo = rlo[0], row_hi = rhi[0];
 #pragma unroll

@@ -90,16 +90,17 @@ int fa::fa_ctx_device(const fa_ctx *c) { return c->device; }
 namespace {
 
 // misc buffer layout (bytes): [0] status u32, [8] cells u64, [16] count A, [20] count B,
-// [24] narrow count, [28] wide count
+// [64] band-bucket histogram u32[kBandBuckets], [128] band-bucket cursors u32[kBandBuckets]
+constexpr size_t kMiscBytes = 256;
 struct Misc {
     uint32_t *status;
     unsigned long long *cells;
-    uint32_t *cnt_a, *cnt_b, *cnt_narrow, *cnt_wide;
+    uint32_t *cnt_a, *cnt_b, *bucket_hist, *bucket_cursor;
 };
 Misc misc_of(fa_ctx *c) {
     char *b = c->misc.as<char>();
     return Misc{(uint32_t *)b, (unsigned long long *)(b + 8), (uint32_t *)(b + 16), (uint32_t *)(b + 20),
-                (uint32_t *)(b + 24), (uint32_t *)(b + 28)};
+                (uint32_t *)(b + 64), (uint32_t *)(b + 128)};
 }
 
 // Extension launch: the int32 one-job-per-thread kernel, or on request the int16x2
@@ -195,7 +196,7 @@ int ensure_ext_buffers(fa_ctx *c, uint32_t n, uint64_t qb, uint64_t tb) {
     FA_CUDA(c->out.ensure(sizeof(fa_ext_result) * (size_t)n));
     FA_CUDA(c->clamped.ensure(n));
     FA_CUDA(c->cells_job.ensure(sizeof(uint32_t) * (size_t)n));
-    FA_CUDA(c->misc.ensure(64));
+    FA_CUDA(c->misc.ensure(kMiscBytes));
     return FA_OK;
 }
 
@@ -270,13 +271,13 @@ int run_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n,
                     b = sg.first;
                 }
             } else if (learned) {
-                // full-band warps first, narrow-band warps after, one launch
-                FA_CUDA(launch_band_partition(d_jobs, list, cnt, n, st.w_cur, c->part_n.as<uint32_t>(), m.cnt_wide,
-                                              m.cnt_narrow, s));
+                // band buckets (configured band first, then narrow bands decreasing), one launch
+                FA_CUDA(launch_band_partition(d_jobs, list, cnt, n, st.w_cur, c->part_n.as<uint32_t>(),
+                                              m.bucket_hist, m.bucket_cursor, s));
                 FA_CUDA(launch_ext(c->kernel, d_jobs, c->part_n.as<uint32_t>(), n, cnt, d_q, d_t, kp, qcap_all,
                                    st.w_cur, d_out, c->clamped.as<uint8_t>(), c->cells_job.as<uint32_t>(), m.cells,
                                    m.status, s));
-                launches += 2;
+                launches += 3;
             } else {
                 FA_CUDA(launch_ext(c->kernel, d_jobs, list, n, cnt, d_q, d_t, kp, qcap_all, st.w_cur, d_out,
                                    c->clamped.as<uint8_t>(), c->cells_job.as<uint32_t>(), m.cells, m.status, s));
@@ -517,7 +518,7 @@ int fa_ext_batch_device(fa_ctx *c, const fa_params *p, const fa_job *d_jobs, uin
     FA_CUDA(cudaSetDevice(c->device));
     const ExtParams kp = ext_params_of(p);
     cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
-    FA_CUDA(c->misc.ensure(64));
+    FA_CUDA(c->misc.ensure(kMiscBytes));
     FA_CUDA(c->hist.ensure(sizeof(uint32_t) * (FA_MAX_QLEN + 1)));
     Misc m = misc_of(c);
     FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
@@ -623,7 +624,7 @@ int fa_mate_sw_batch_device(fa_ctx *c, const fa_mate_params *p, const fa_mate_jo
     mp.max = mx;
     FA_CUDA(cudaSetDevice(c->device));
     cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
-    FA_CUDA(c->misc.ensure(64));
+    FA_CUDA(c->misc.ensure(kMiscBytes));
     FA_CUDA(c->order.ensure(4ull * n));
     FA_CUDA(c->list_a.ensure(4ull * n));
     FA_CUDA(c->hist.ensure(sizeof(uint32_t) * (FA_MAX_QLEN + 1)));
@@ -704,7 +705,7 @@ int fa_mate_sw_batch(fa_ctx *c, const fa_mate_params *p, const fa_mate_job *jobs
     FA_CUDA(c->qseq.ensure(qseq_len));
     FA_CUDA(c->tseq.ensure(tseq_len));
     FA_CUDA(c->out.ensure(sizeof(fa_kswr) * (size_t)n));
-    FA_CUDA(c->misc.ensure(64));
+    FA_CUDA(c->misc.ensure(kMiscBytes));
     Misc m = misc_of(c);
     FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
     std::vector<uint32_t> order(byte_list);

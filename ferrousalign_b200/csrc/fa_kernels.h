@@ -13,6 +13,7 @@ namespace fa {
 
 constexpr int kExtThreads = 128;     // threads (= jobs) per extension block
 constexpr int kPackedHMax = 8191;    // largest H/E the packed column word holds
+constexpr int kBandBuckets = 13;   // configured band + 12 narrow band classes
 constexpr int kPairThreads = 32;     // threads per int16x2 extension block (2 jobs each)
 
 size_t ext_packed_smem_bytes(int qcap);
@@ -47,8 +48,8 @@ cudaError_t launch_policy_step(const fa_job *d_jobs, const uint32_t *d_list, con
                                PolicyState st, int max_tries, int judge, uint32_t *d_next,
                                uint32_t *d_next_count, cudaStream_t stream);
 cudaError_t launch_band_partition(const fa_job *d_jobs, const uint32_t *d_list, const uint32_t *d_count,
-                                  uint32_t n_max, const int32_t *d_w_cur, uint32_t *d_out, uint32_t *d_n_wide,
-                                  uint32_t *d_n_narrow, cudaStream_t stream);
+                                  uint32_t n_max, const int32_t *d_w_cur, uint32_t *d_out, uint32_t *d_hist,
+                                  uint32_t *d_cursor, cudaStream_t stream);
 cudaError_t launch_policy_init(const fa_job *d_jobs, uint32_t n, const int32_t *d_w_first, int w_min,
                                int learned, PolicyState st, cudaStream_t stream);
 

@@ -13,9 +13,9 @@
 // extend_kernel.cu) and that run would also end the plain ladder, or, with
 // FA_JUDGE_MAXOFF (empirical, not exact), when it
 // passes the bwa-mem2 max_off test (with FA_JUDGE_GLOBAL also requiring that its best
-// score is its end-to-end score); otherwise the band doubles -- or, when only the
-// end-to-end test failed, goes straight to the configured band -- and at the
-// configured band the plain policy takes over.
+// score is its end-to-end score); otherwise the band doubles -- or goes straight to
+// the configured band with FA_JUDGE_ONCE, or when only the end-to-end test failed --
+// and at the configured band the plain policy takes over.
 //
 // The decisions compact the jobs that need another run into a list whose length
 // stays on the device, so a retry round needs no host round trip.
@@ -80,6 +80,7 @@ __global__ void policy_step_kernel(const fa_job *__restrict__ jobs, const uint32
             }
             if (!ok) {
                 if (st.missed && st.tries[jid] == 1) st.missed[jid] = 1;
+                jump |= (judge & FA_JUDGE_ONCE) != 0;
                 w <<= 1;
                 if (jump || w >= jb.w) { w = jb.w; k = 0; }
                 st.w_cur[jid] = w;
@@ -107,51 +108,79 @@ __global__ void policy_step_kernel(const fa_job *__restrict__ jobs, const uint32
     }
 }
 
-// Reorders a round's job list so that jobs running at their configured band come
-// first and jobs running below it (narrow) fill the list from the back: every warp then
-// holds jobs of one kind (a warp runs as long as its widest job), and the long jobs
-// start first, which balances the end of the launch.  The output has the same length
-// as the input; order inside each part follows the input in runs of up to one warp.
-__global__ void band_partition_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ list,
-                                      const uint32_t *__restrict__ count, uint32_t n_max,
-                                      const int32_t *__restrict__ w_cur, uint32_t *__restrict__ out,
-                                      uint32_t *__restrict__ n_wide, uint32_t *__restrict__ n_narrow)
+// Reorders a round's job list into band buckets so that every warp holds jobs of one
+// band (a warp runs as long as its widest job): jobs at their configured band first,
+// then narrow jobs by decreasing band, so the longest jobs start first and balance the
+// end of the launch.  Order inside a bucket follows the input list in runs of up to one
+// warp.  Two passes: a histogram of the buckets, then a scatter behind their prefix.
+__device__ __forceinline__ int band_bucket(int w, int wj) {
+    if (w >= wj) return 0;
+    // descending narrow classes: >64, 49-64, 33-48, 25-32, 17-24, 13-16, 9-12, 7-8, 5-6, 4, 3, <=2
+    constexpr int lo[kBandBuckets - 1] = {65, 49, 33, 25, 17, 13, 9, 7, 5, 4, 3, 0};
+    int b = kBandBuckets - 1;
+#pragma unroll
+    for (int k = kBandBuckets - 2; k >= 0; --k)
+        if (w >= lo[k]) b = k + 1;
+    return b;
+}
+
+__global__ void band_hist_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ list,
+                                 const uint32_t *__restrict__ count, uint32_t n_max, const int32_t *__restrict__ w_cur,
+                                 uint32_t *__restrict__ hist)
 {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t n = count ? min(*count, n_max) : n_max;
     const bool live = t < n;
+    int b = -1;
+    if (live) {
+        const uint32_t jid = list[t];
+        b = band_bucket(w_cur[jid], jobs[jid].w);
+    }
+    const unsigned peers = __match_any_sync(0xffffffffu, b);
+    const int lane = threadIdx.x & 31;
+    if (live && lane == __ffs(peers) - 1) atomicAdd(&hist[b], (uint32_t)__popc(peers));
+}
+
+__global__ void band_scatter_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ list,
+                                    const uint32_t *__restrict__ count, uint32_t n_max,
+                                    const int32_t *__restrict__ w_cur, const uint32_t *__restrict__ hist,
+                                    uint32_t *__restrict__ cursor, uint32_t *__restrict__ out)
+{
+    __shared__ uint32_t base[kBandBuckets];
+    if (threadIdx.x == 0) {
+        uint32_t acc = 0;
+        for (int k = 0; k < kBandBuckets; ++k) { base[k] = acc; acc += hist[k]; }
+    }
+    __syncthreads();
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t n = count ? min(*count, n_max) : n_max;
+    const bool live = t < n;
     uint32_t jid = 0;
-    bool nar = false;
+    int b = -1;
     if (live) {
         jid = list[t];
-        nar = w_cur[jid] < jobs[jid].w;
+        b = band_bucket(w_cur[jid], jobs[jid].w);
     }
-    const unsigned mn = __ballot_sync(0xffffffffu, live && nar);
-    const unsigned mw = __ballot_sync(0xffffffffu, live && !nar);
+    const unsigned peers = __match_any_sync(0xffffffffu, b);
     const int lane = threadIdx.x & 31;
-    uint32_t bn = 0, bw = 0;
-    if (lane == 0) {
-        if (mn) bn = atomicAdd(n_narrow, (uint32_t)__popc(mn));
-        if (mw) bw = atomicAdd(n_wide, (uint32_t)__popc(mw));
-    }
-    bn = __shfl_sync(0xffffffffu, bn, 0);
-    bw = __shfl_sync(0xffffffffu, bw, 0);
-    if (!live) return;
-    const unsigned below = (1u << lane) - 1u;
-    if (nar) out[n - 1 - (bn + __popc(mn & below))] = jid;
-    else out[bw + __popc(mw & below)] = jid;
+    const int leader = __ffs(peers) - 1;
+    uint32_t pos = 0;
+    if (live && lane == leader) pos = atomicAdd(&cursor[b], (uint32_t)__popc(peers));
+    pos = __shfl_sync(0xffffffffu, pos, leader);
+    if (live) out[base[b] + pos + __popc(peers & ((1u << lane) - 1u))] = jid;
 }
 
 cudaError_t launch_band_partition(const fa_job *d_jobs, const uint32_t *d_list, const uint32_t *d_count,
-                                  uint32_t n_max, const int32_t *d_w_cur, uint32_t *d_out, uint32_t *d_n_wide,
-                                  uint32_t *d_n_narrow, cudaStream_t stream)
+                                  uint32_t n_max, const int32_t *d_w_cur, uint32_t *d_out, uint32_t *d_hist,
+                                  uint32_t *d_cursor, cudaStream_t stream)
 {
     if (n_max == 0) return cudaSuccess;
-    cudaError_t e = cudaMemsetAsync(d_n_wide, 0, 4, stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(d_n_narrow, 0, 4, stream);
+    cudaError_t e = cudaMemsetAsync(d_hist, 0, sizeof(uint32_t) * kBandBuckets, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_cursor, 0, sizeof(uint32_t) * kBandBuckets, stream);
     if (e != cudaSuccess) return e;
-    band_partition_kernel<<<(n_max + 255) / 256, 256, 0, stream>>>(d_jobs, d_list, d_count, n_max, d_w_cur, d_out,
-                                                                   d_n_wide, d_n_narrow);
+    const uint32_t blocks = (n_max + 255) / 256;
+    band_hist_kernel<<<blocks, 256, 0, stream>>>(d_jobs, d_list, d_count, n_max, d_w_cur, d_hist);
+    band_scatter_kernel<<<blocks, 256, 0, stream>>>(d_jobs, d_list, d_count, n_max, d_w_cur, d_hist, d_cursor, d_out);
     return cudaGetLastError();
 }
 

@@ -1,6 +1,8 @@
 """One device-resident extension batch of the bench workload, for ncu captures.
 
 Usage: python -m ferrousalign_b200.profile_run [n_jobs] [probe|-] [kernel: 0 auto, 1 int32, 2 int16x2] [reps]
+       python -m ferrousalign_b200.profile_run learned [n_jobs] [reps]   (learned-band path)
+       python -m ferrousalign_b200.profile_run bands [n_jobs]            (single runs at fixed bands)
 """
 import ctypes
 import sys
@@ -10,6 +12,30 @@ import torch
 
 import ferrousalign_b200 as fa
 from ferrousalign_b200 import _native as N, synth
+
+if len(sys.argv) > 1 and sys.argv[1] in ("learned", "bands"):
+    from ferrousalign_b200 import band_model as B
+    mode = sys.argv[1]
+    n = int(sys.argv[2]) if len(sys.argv) > 2 else 1_000_000
+    b = synth.workload_ext_1m(n)
+    p = fa.BandedPairWiseSW().to_struct()
+    ctx = fa.Context(0)
+    if mode == "learned":
+        m = B.BandModel.load()
+        hints = B.hints_from_info(b.info)
+        for r in range(int(sys.argv[3]) if len(sys.argv) > 3 else 1):
+            out, st, wf, wfin = B.extend_batch_learned(p, b.jobs, b.qseq, b.tseq, m, hints=hints, ctx=ctx)
+            print("learned kernel ms", float(st["kernel_ms"]), "cells", int(st["cells_executed"]),
+                  "launches", int(st["kernel_launches"]), "retries", int(st["retries"]))
+    else:
+        for w in (1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 64, 100):
+            j = b.jobs.copy()
+            j["w"] = np.minimum(j["w"], w)
+            for r in range(2):
+                out, st, _ = fa.extend_batch(p, j, b.qseq, b.tseq, ctx=ctx)
+            print(f"band {w}: kernel ms {float(st['kernel_ms']):.3f} cells {int(st['cells_executed'])} "
+                  f"Gcell/s {int(st['cells_executed']) / float(st['kernel_ms']) / 1e6:.1f}")
+    sys.exit(0)
 
 n = int(sys.argv[1]) if len(sys.argv) > 1 else 1_000_000
 b = synth.workload_ext_1m(n)

@@ -82,6 +82,8 @@ typedef struct {
 #define FA_JUDGE_GLOBAL  4  /* with MAXOFF: additionally require gscore == score              */
 #define FA_JUDGE_BOUND   8  /* accept when the exit-bound certificate holds (sound): no path
                                leaving the narrow run's region can reach any output statistic */
+#define FA_JUDGE_ONCE   16  /* retry rule: a rejected narrow run goes straight to the configured
+                               band instead of doubling (one narrow try per job)            */
 
 typedef struct {
     int32_t mode;
@@ -248,8 +250,9 @@ int  fa_band_model_fit_norm(fa_band_model *m, const float *x, uint32_t n);
 int  fa_band_features(fa_ctx *ctx, const fa_params *p, const fa_job *jobs, uint32_t n,
                       const uint8_t *qseq, uint64_t qseq_len, const uint8_t *tseq, uint64_t tseq_len,
                       const fa_band_hint *hints, float *x);
-/* y[n] = MLP(x) (log2 band); w_out[n] = ceil(2^(y+margin)) raised to w_min, or job.w when
- * that exceeds 2*w_min (such jobs are better started at the configured band) */
+/* y[n] = MLP(x) (log2 band); w_out[n] = ceil(2^(y+margin)) raised to w_min and rounded up
+ * to the ladder 2, 3, 4, 6, 8, 12, 16, ... (2^k and 3*2^k), or job.w when twice that
+ * exceeds job.w (such jobs are better started at the configured band) */
 int  fa_band_predict(fa_ctx *ctx, const fa_band_model *m, const float *x, const fa_job *jobs, uint32_t n,
                      float margin, int w_min, float *y_out, int32_t *w_out);
 /* mean gradient and loss of the pinball(tau) loss on (x, target = log2 band) */

@@ -55,3 +55,18 @@ def grad(w, mean, std, x, target, tau):
     g[O_W1:O_B1] = (d1.T @ xn).reshape(-1)
     g[O_B1:O_W2] = d1.sum(0)
     return g, loss
+
+
+def first_band(y, margin: float, w_min: int, wj):
+    """The predicted first band of a job from the network output y (log2 band):
+    ceil(2^(y + margin)) with the exponent clamped to [0, 16], raised to w_min, rounded
+    up to the ladder 2^k / 3*2^(k-1), and the configured band wj when twice that
+    exceeds wj."""
+    e = np.clip(np.asarray(y, np.float64) + margin, 0.0, 16.0)
+    band = np.maximum(np.ceil(np.exp2(e)).astype(np.int64), w_min)
+    p2 = np.where(band > 2, 1 << np.ceil(np.log2(np.maximum(band, 2))).astype(np.int64), band)
+    three = 3 * p2 // 4
+    band = np.where(band > 2, np.where(three >= band, three, p2), band)
+    wj = np.asarray(wj, np.int64)
+    band = np.where(2 * band > wj, wj, band)
+    return np.minimum(band, wj).astype(np.int32)

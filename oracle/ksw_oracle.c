@@ -555,7 +555,7 @@ static int policy_one(const batch_t *B, uint32_t i)
                 jump = off_ok && !ok;
             }
             if (ok) { accepted = 1; wfin = w; break; }
-            if (jump) break;   /* straight to the configured band */
+            if (jump || (pol->judge & FA_JUDGE_ONCE)) break;   /* straight to the configured band */
             w <<= 1;
         }
         if (!rc && !accepted)
