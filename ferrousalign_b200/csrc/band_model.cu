@@ -92,14 +92,16 @@ __global__ void __launch_bounds__(128) band_features_kernel(const fa_job *__rest
     mm = __reduce_add_sync(0xffffffffu, mm);
     nq = __reduce_add_sync(0xffffffffu, nq);
     last_mm = __reduce_max_sync(0xffffffffu, last_mm);
-    int best_s = 0, best_c = 1 << 30, best_n = 1, best_last = -1;
+    // shifted diagonal with the lowest mismatch fraction (ties: the smaller shift)
+    int best_s = 0, best_c = -1, best_n = 1, best_last = -1;
 #pragma unroll
     for (int s = 0; s < 9; ++s) {
         const int cs = __reduce_add_sync(0xffffffffu, c[s]);
         const int ns = __reduce_add_sync(0xffffffffu, cnt[s]);
         const int ls = __reduce_max_sync(0xffffffffu, last_s[s]);
         const int sh = s - 4;
-        if (ns > 0 && (cs * best_n < best_c * ns || (cs * best_n == best_c * ns && abs(sh) < abs(best_s)))) {
+        const long long lhs = (long long)cs * best_n, rhs = (long long)best_c * ns;
+        if (ns > 0 && (best_c < 0 || lhs < rhs || (lhs == rhs && abs(sh) < abs(best_s)))) {
             best_c = cs; best_n = ns; best_s = sh; best_last = ls;
         }
     }
@@ -121,7 +123,7 @@ __global__ void __launch_bounds__(128) band_features_kernel(const fa_job *__rest
     o[12] = (float)nq;
     o[13] = (float)(tlen - qlen);
     o[14] = (float)abs(best_s);
-    o[15] = best_c >= (1 << 30) ? 1.f : (float)best_c / (float)best_n;
+    o[15] = best_c < 0 ? 1.f : (float)best_c / (float)best_n;
 }
 
 cudaError_t launch_band_features(const fa_job *d_jobs, uint32_t n, const uint8_t *d_q, const uint8_t *d_t,

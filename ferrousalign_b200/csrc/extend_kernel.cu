@@ -87,18 +87,26 @@ struct ExitBound {
     }
 };
 
-template <bool CERT>
+// RING = 0: one shared-memory word per query column (any band).  RING = R > 0: only R
+// column words, column j in slot j mod R, plus the query packed 8 codes per word -- for
+// bands w <= R/2 - 1, whose rows span at most 2w+2 columns, so a slot is never reused
+// while the recurrence can still read it; far less shared memory per job, so several
+// times the resident warps.  Columns entering the ring get their query code explicitly,
+// and a column the rows grow into after a trim gets the value the full array would
+// hold there: 0 once written (trimmed cells are zero), its first-row value if never.
+template <bool CERT, int RING>
 __global__ void __launch_bounds__(kExtThreads)
 ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ order,
-                  uint32_t n, const uint32_t *__restrict__ n_dev, const uint8_t *__restrict__ qseq,
-                  const uint8_t *__restrict__ tseq, const ExtParams p, int qcap,
+                  uint32_t n, const uint32_t *__restrict__ first_dev, const uint32_t *__restrict__ n_dev,
+                  const uint8_t *__restrict__ qseq, const uint8_t *__restrict__ tseq, const ExtParams p, int qcap,
                   const int32_t *__restrict__ w_try, fa_ext_result *__restrict__ out,
                   uint8_t *__restrict__ clamped_out, uint32_t *__restrict__ cells_job,
                   unsigned long long *__restrict__ cells_out, uint32_t *__restrict__ status)
 {
     extern __shared__ uint32_t smem[];
     constexpr int T = kExtThreads;
-    const uint32_t gi = blockIdx.x * T + threadIdx.x;
+    const uint32_t first = first_dev ? *first_dev : 0u;   // device-side sub-range of the order
+    const uint32_t gi = first + blockIdx.x * T + threadIdx.x;
     uint32_t cells = 0;
     if (n_dev) n = min(n, *n_dev);   // device-side job count (retry rounds)
 
@@ -106,13 +114,14 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
         const uint32_t jid = order ? order[gi] : gi;
         const fa_job jb = jobs[jid];
         uint32_t *col = smem + threadIdx.x;
+        uint32_t *qw = smem + RING * T + threadIdx.x;     // RING: packed query codes
         const int qlen = jb.qlen, tlen = jb.tlen, h0 = jb.h0;
+        const int w = ext_band_clamp(qlen, w_try ? w_try[jid] : jb.w, p);
         if (h0 <= 0 || qlen <= 0 || tlen < 0) {
             atomicOr(status, ST_ARG);
-        } else if (qlen > qcap || h0 + p.max_score * qlen > kPackedHMax) {
+        } else if (qlen > qcap || h0 + p.max_score * qlen > kPackedHMax || (RING > 0 && 2 * w + 2 > RING)) {
             atomicOr(status, ST_CAPACITY);
         } else {
-            const int w = ext_band_clamp(qlen, w_try ? w_try[jid] : jb.w, p);
             const int oe_del = p.o_del + p.e_del, oe_ins = p.o_ins + p.e_ins;
             const int e_del = p.e_del, e_ins = p.e_ins;
             const uint8_t *Q = qseq + jb.q_off;
@@ -131,8 +140,28 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
             uint32_t bad = 0;
             int hp = h0, init_reach = 0;
             bool filling = true;
+            // first-row value of column j >= 1 (positive exactly up to init_reach)
+            auto init_h = [&](int j) { return j == 0 ? h0 : (j <= init_reach ? h0 - oe_ins - (j - 1) * e_ins : 0); };
+            if (RING > 0) {
+                init_reach = h0 <= oe_ins ? 0 : (e_ins == 0 ? qlen : min(qlen, 1 + (h0 - oe_ins - 1) / e_ins));
+                for (int j0 = 0; j0 < qlen; j0 += 8) {
+                    uint32_t qb[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) qb[u] = j0 + u < qlen ? (uint32_t)Q[j0 + u] : 0u;
+                    uint32_t word = 0;
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        bad |= qb[u] >= (uint32_t)p.m;
+                        word |= (qb[u] & 7u) << (4 * u);
+                        const int j = j0 + u;
+                        if (j < RING && j < qlen) col[j * T] = (uint32_t)init_h(j) << 16 | (qb[u] & 7u);
+                    }
+                    qw[(j0 >> 3) * T] = word;
+                }
+                if (qlen < RING) col[qlen * T] = (uint32_t)init_h(qlen) << 16;
+            }
             // eight independent byte loads in flight per thread before their first use
-            for (int j0 = 0; j0 <= qlen; j0 += 8) {
+            for (int j0 = 0; RING == 0 && j0 <= qlen; j0 += 8) {
                 uint32_t qb[8];
 #pragma unroll
                 for (int u = 0; u < 8; ++u) qb[u] = j0 + u < qlen ? (uint32_t)Q[j0 + u] : 0u;
@@ -161,8 +190,10 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
             int beg = 0, end = qlen, clamped = 0;
             const int a = p.max_score;
             ExitBound xb;
-            int bmax = ExitBound::NEG, first_fail = INT32_MAX, max_written = -1, rows = 0;
+            int bmax = ExitBound::NEG, first_fail = INT32_MAX, max_written = -1, rows = 0, prev_end = 0;
             bool row_ok = true, stale = false, broke = false, zbreak = false;
+            auto slot = [](int j) { return RING > 0 ? (j & (RING - 1)) : j; };
+            auto qcode = [&](int j) { return (qw[(j >> 3) * T] >> (4 * (j & 7))) & 7u; };
             if (CERT) xb.init();
             // target bases arrive 5 to 8 rows ahead of their row: tq0 holds the current
             // group of four, tq1 the next, loaded when tq0 is used up
@@ -196,10 +227,10 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
                 if (CERT) {
                     ++rows;
                     if (i == 0) {
-                        if (end < qlen) xb.add(0, (int)(col[end * T] >> 16), -1, end - 1, qlen, a, e_del);
+                        if (end < qlen) xb.add(0, (int)(col[slot(end) * T] >> 16), -1, end - 1, qlen, a, e_del);
                     } else {
                         for (int j = beg_a; j < beg && j < qlen; ++j)          // columns the band drops
-                            xb.add(1, (int)((col[j * T] >> 3) & 0x1FFFu), i, j, qlen, a, e_del);
+                            xb.add(1, (int)((col[slot(j) * T] >> 3) & 0x1FFFu), i, j, qlen, a, e_del);
                         if (beg_a == 0 && beg > 0)                            // the first column leaves
                             xb.add(1, h0 - (p.o_del + e_del * i), i - 1, -1, qlen, a, e_del);
                         const int lo = max(beg, max_written + 1), hi = min(end - 1, init_reach);
@@ -212,10 +243,18 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
                     h1 = h0 - (p.o_del + e_del * (i + 1));
                     if (h1 < 0) h1 = 0;
                 }
+                if (RING > 0) {
+                    // a column grown into after a trim: the full array's value there
+                    if (i > 0 && end > prev_end + 1) {
+                        const int j = prev_end + 1;
+                        const int hv = j > max_written ? init_h(j) : 0;
+                        col[slot(j) * T] = (uint32_t)hv << 16 | qcode(j);
+                    }
+                }
                 int f = 0, key = 0;
 #pragma unroll 4
                 for (int j = beg; j < end; ++j) {
-                    const uint32_t wd = col[j * T];
+                    const uint32_t wd = col[slot(j) * T];
                     const int M = (int)(wd >> 16);
                     const int e = (int)((wd >> 3) & 0x1FFFu);
                     const uint32_t q = wd & 7u;
@@ -225,10 +264,14 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
                     const int e_new = __viaddmax_s32_relu(e, -e_del, Mp - oe_del);
                     f = __viaddmax_s32_relu(f, -e_ins, Mp - oe_ins);
                     key = max(key, (h << 12) | (4095 - j));   // first column of the row max
-                    col[j * T] = (uint32_t)h1 << 16 | (uint32_t)e_new << 3 | q;
+                    col[slot(j) * T] = (uint32_t)h1 << 16 | (uint32_t)e_new << 3 | q;
                     h1 = h;
                 }
-                {
+                if (RING > 0) {
+                    col[slot(end) * T] = (uint32_t)h1 << 16 | (end < qlen ? qcode(end) : 0u);
+                    max_written = max(max_written, end);
+                    prev_end = end;
+                } else {
                     const uint32_t wd = col[end * T];
                     col[end * T] = (uint32_t)h1 << 16 | (wd & 7u);
                 }
@@ -237,7 +280,7 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
                 const int m_row = key >> 12;
                 const int mj = 4095 - (key & 4095);
                 if (CERT) {
-                    max_written = max(max_written, end);
+                    if (RING == 0) max_written = max(max_written, end);
                     if (end < qlen) xb.add(0, f, i, end, qlen, a, e_del);   // F past the row's end
                     const int b = xb.at(i, a, e_del);
                     row_ok = m_row > 0 ? b < m_row : b <= 0;
@@ -259,10 +302,10 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
                     }
                 }
                 int nb = beg;
-                while (nb < end && (col[nb * T] >> 3) == 0) ++nb;
+                while (nb < end && (col[slot(nb) * T] >> 3) == 0) ++nb;
                 beg = nb;
                 int ne = end;
-                while (ne > beg && (col[ne * T] >> 3) == 0) --ne;
+                while (ne > beg && (col[slot(ne) * T] >> 3) == 0) --ne;
                 end = ne + 2 < qlen ? ne + 2 : qlen;
             }
             if (bad) atomicOr(status, ST_BAD_CODE);
@@ -297,27 +340,49 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
     }
 }
 
-size_t ext_packed_smem_bytes(int qcap) {
-    return (size_t)(qcap + 1) * kExtThreads * sizeof(uint32_t);
+size_t ext_packed_smem_bytes(int qcap, int ring) {
+    const size_t words = ring > 0 ? (size_t)ring + (size_t)(qcap + 7) / 8 : (size_t)qcap + 1;
+    return words * kExtThreads * sizeof(uint32_t);
 }
 
+namespace {
+template <bool CERT, int RING>
+cudaError_t launch_variant(uint32_t blocks, size_t smem, cudaStream_t stream, const fa_job *d_jobs,
+                           const uint32_t *d_order, uint32_t n, const uint32_t *d_first, const uint32_t *d_n,
+                           const uint8_t *d_qseq, const uint8_t *d_tseq, const ExtParams &p, int qcap,
+                           const int32_t *d_w_try, fa_ext_result *d_out, uint8_t *d_clamped, uint32_t *d_cells_job,
+                           unsigned long long *d_cells, uint32_t *d_status)
+{
+    cudaError_t err = cudaFuncSetAttribute(ext_packed_kernel<CERT, RING>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return err;
+    ext_packed_kernel<CERT, RING><<<blocks, kExtThreads, smem, stream>>>(
+        d_jobs, d_order, n, d_first, d_n, d_qseq, d_tseq, p, qcap, d_w_try, d_out, d_clamped, d_cells_job,
+        d_cells, d_status);
+    return cudaGetLastError();
+}
+}  // namespace
+
 cudaError_t launch_ext_packed(const fa_job *d_jobs, const uint32_t *d_order, uint32_t n,
-                              const uint32_t *d_n, const uint8_t *d_qseq, const uint8_t *d_tseq,
-                              const ExtParams &p, int qcap, const int32_t *d_w_try,
-                              fa_ext_result *d_out, uint8_t *d_clamped, uint32_t *d_cells_job,
-                              unsigned long long *d_cells, uint32_t *d_status,
+                              const uint32_t *d_first, const uint32_t *d_n, const uint8_t *d_qseq,
+                              const uint8_t *d_tseq, const ExtParams &p, int qcap, int ring,
+                              const int32_t *d_w_try, fa_ext_result *d_out, uint8_t *d_clamped, bool cert,
+                              uint32_t *d_cells_job, unsigned long long *d_cells, uint32_t *d_status,
                               cudaStream_t stream)
 {
     if (n == 0) return cudaSuccess;
-    const size_t smem = ext_packed_smem_bytes(qcap);
-    // the certificate variant runs whenever per-job flags are asked for
-    auto kern = d_clamped ? ext_packed_kernel<true> : ext_packed_kernel<false>;
-    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (err != cudaSuccess) return err;
+    if (ring != 0 && ring != 32 && ring != 64) return cudaErrorInvalidValue;
+    const size_t smem = ext_packed_smem_bytes(qcap, ring);
     const uint32_t blocks = (n + kExtThreads - 1) / kExtThreads;
-    kern<<<blocks, kExtThreads, smem, stream>>>(d_jobs, d_order, n, d_n, d_qseq, d_tseq, p, qcap, d_w_try,
-                                                d_out, d_clamped, d_cells_job, d_cells, d_status);
-    return cudaGetLastError();
+    // the certificate variant only where a judge reads it (it adds work to every row)
+    const bool c = cert && d_clamped;
+#define FA_EXT_LAUNCH(CV, RV) launch_variant<CV, RV>(blocks, smem, stream, d_jobs, d_order, n, d_first, d_n, d_qseq, \
+                                                     d_tseq, p, qcap, d_w_try, d_out, d_clamped, d_cells_job,        \
+                                                     d_cells, d_status)
+    if (ring == 32) return c ? FA_EXT_LAUNCH(true, 32) : FA_EXT_LAUNCH(false, 32);
+    if (ring == 64) return c ? FA_EXT_LAUNCH(true, 64) : FA_EXT_LAUNCH(false, 64);
+    return c ? FA_EXT_LAUNCH(true, 0) : FA_EXT_LAUNCH(false, 0);
+#undef FA_EXT_LAUNCH
 }
 
 }  // namespace fa

@@ -83,6 +83,9 @@ struct fa_ctx {
     int kernel = FA_KERNEL_AUTO;
     cudaStream_t last_stream = nullptr;   // stream of the last device-resident call
     cudaEvent_t kev0 = nullptr, kev1 = nullptr;   // bracket the extension kernels of a device call
+    // learned rounds run their band groups on forked streams: fork on `stream`, join back
+    cudaStream_t aux[2] = {nullptr, nullptr};
+    cudaEvent_t fork_ev = nullptr, join_ev[2] = {nullptr, nullptr};
 };
 
 int fa::fa_ctx_device(const fa_ctx *c) { return c->device; }
@@ -90,32 +93,68 @@ int fa::fa_ctx_device(const fa_ctx *c) { return c->device; }
 namespace {
 
 // misc buffer layout (bytes): [0] status u32, [8] cells u64, [16] count A, [20] count B,
-// [64] band-bucket histogram u32[kBandBuckets], [128] band-bucket cursors u32[kBandBuckets]
+// [64] band-bucket histogram u32[kBandBuckets], [128] band-bucket cursors u32[kBandBuckets],
+// [192] band-group bounds u32[3]
 constexpr size_t kMiscBytes = 256;
 struct Misc {
     uint32_t *status;
     unsigned long long *cells;
-    uint32_t *cnt_a, *cnt_b, *bucket_hist, *bucket_cursor;
+    uint32_t *cnt_a, *cnt_b, *bucket_hist, *bucket_cursor, *group_bounds;
 };
 Misc misc_of(fa_ctx *c) {
     char *b = c->misc.as<char>();
     return Misc{(uint32_t *)b, (unsigned long long *)(b + 8), (uint32_t *)(b + 16), (uint32_t *)(b + 20),
-                (uint32_t *)(b + 64), (uint32_t *)(b + 128)};
+                (uint32_t *)(b + 64), (uint32_t *)(b + 128), (uint32_t *)(b + 192)};
+}
+
+int ensure_aux_streams(fa_ctx *c) {
+    if (c->fork_ev) return FA_OK;
+    for (int k = 0; k < 2; ++k) {
+        FA_CUDA(cudaStreamCreateWithFlags(&c->aux[k], cudaStreamNonBlocking));
+        FA_CUDA(cudaEventCreateWithFlags(&c->join_ev[k], cudaEventDisableTiming));
+    }
+    FA_CUDA(cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming));
+    return FA_OK;
 }
 
 // Extension launch: the int32 one-job-per-thread kernel, or on request the int16x2
 // two-jobs-per-thread kernel for bwa-form matrices.  Both are exact; the int32 kernel
 // is faster on B200 (the int16x2 one holds twice the shared memory per thread, so
 // half the warps), hence the default.
+// With `cert` the int32 kernel also evaluates the exit-bound certificate (flag bit 1),
+// which only the int32 kernel implements.
 cudaError_t launch_ext(int kernel, const fa_job *d_jobs, const uint32_t *d_order, uint32_t n,
                        const uint32_t *d_n, const uint8_t *d_q, const uint8_t *d_t, const ExtParams &kp, int qcap,
-                       const int32_t *d_w_try, fa_ext_result *d_out, uint8_t *d_clamped, uint32_t *d_cells_job,
-                       unsigned long long *d_cells, uint32_t *d_status, cudaStream_t s) {
-    if (kernel == FA_KERNEL_INT16X2 && ext_pair_eligible(kp))
+                       const int32_t *d_w_try, fa_ext_result *d_out, uint8_t *d_clamped, bool cert,
+                       uint32_t *d_cells_job, unsigned long long *d_cells, uint32_t *d_status, cudaStream_t s) {
+    if (kernel == FA_KERNEL_INT16X2 && ext_pair_eligible(kp) && !cert)
         return launch_ext_pair(d_jobs, d_order, n, d_n, d_q, d_t, kp, qcap, d_w_try, d_out, d_clamped,
                                d_cells_job, d_cells, d_status, s);
-    return launch_ext_packed(d_jobs, d_order, n, d_n, d_q, d_t, kp, qcap, d_w_try, d_out, d_clamped,
-                             d_cells_job, d_cells, d_status, s);
+    return launch_ext_packed(d_jobs, d_order, n, nullptr, d_n, d_q, d_t, kp, qcap, 0, d_w_try, d_out, d_clamped,
+                             cert, d_cells_job, d_cells, d_status, s);
+}
+
+// One learned round over a band-partitioned list: configured-band and wide narrow jobs
+// in the full-row kernel, bands 13-24 in the 64-column ring kernel, bands <= 12 in the
+// 32-column ring kernel; the three run concurrently on forked streams.
+int launch_learned_round(fa_ctx *c, const fa_job *d_jobs, const uint32_t *d_list, uint32_t n_max,
+                         const uint8_t *d_q, const uint8_t *d_t, const ExtParams &kp, int qcap,
+                         const int32_t *d_w_cur, fa_ext_result *d_out, uint8_t *d_flags, bool cert, Misc &m,
+                         cudaStream_t s) {
+    if (int rc = ensure_aux_streams(c)) return rc;
+    const uint32_t *g = m.group_bounds;
+    FA_CUDA(cudaEventRecord(c->fork_ev, s));
+    FA_CUDA(launch_ext_packed(d_jobs, d_list, n_max, nullptr, g + 0, d_q, d_t, kp, qcap, 0, d_w_cur, d_out, d_flags,
+                              cert, c->cells_job.as<uint32_t>(), m.cells, m.status, s));
+    const int rings[2] = {64, 32};
+    for (int k = 0; k < 2; ++k) {
+        FA_CUDA(cudaStreamWaitEvent(c->aux[k], c->fork_ev, 0));
+        FA_CUDA(launch_ext_packed(d_jobs, d_list, n_max, g + k, g + k + 1, d_q, d_t, kp, qcap, rings[k], d_w_cur,
+                                  d_out, d_flags, cert, c->cells_job.as<uint32_t>(), m.cells, m.status, c->aux[k]));
+        FA_CUDA(cudaEventRecord(c->join_ev[k], c->aux[k]));
+        FA_CUDA(cudaStreamWaitEvent(s, c->join_ev[k], 0));
+    }
+    return FA_OK;
 }
 
 int check_params(const fa_params *p) {
@@ -242,7 +281,7 @@ int run_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n,
         uint32_t b = 0;
         for (auto &sg : segs) {
             FA_CUDA(launch_ext(c->kernel, d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp, sg.second,
-                               nullptr, d_out, nullptr, c->cells_job.as<uint32_t>(), m.cells, m.status, s));
+                               nullptr, d_out, nullptr, false, c->cells_job.as<uint32_t>(), m.cells, m.status, s));
             ++launches;
             b = sg.first;
         }
@@ -251,6 +290,9 @@ int run_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n,
         PolicyState st{c->w_cur.as<int32_t>(), c->prev.as<int32_t>(), c->kk.as<int32_t>(),
                        c->w_final.as<int32_t>(), c->tries.as<int32_t>(), c->missed.as<uint8_t>()};
         const int learned = mode == FA_POLICY_LEARNED;
+        // flags feed the learned judge only; the certificate only its BOUND test
+        uint8_t *d_flags = learned ? c->clamped.as<uint8_t>() : nullptr;
+        const bool cert = learned && (pol->judge & FA_JUDGE_BOUND);
         FA_CUDA(launch_policy_init(d_jobs, n, d_wfirst, pol->w_min, learned, st, s));
         ++launches;
         const int max_tries = std::max(1, pol->max_tries);
@@ -265,26 +307,34 @@ int run_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n,
                 uint32_t b = 0;
                 for (auto &sg : segs) {
                     FA_CUDA(launch_ext(c->kernel, d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp, sg.second,
-                                       st.w_cur, d_out, c->clamped.as<uint8_t>(), c->cells_job.as<uint32_t>(),
+                                       st.w_cur, d_out, d_flags, cert, c->cells_job.as<uint32_t>(),
                                        m.cells, m.status, s));
                     ++launches;
                     b = sg.first;
                 }
             } else if (learned) {
-                // band buckets (configured band first, then narrow bands decreasing), one launch
+                // band buckets (configured band first, then narrow bands decreasing), then the
+                // three band groups concurrently
                 FA_CUDA(launch_band_partition(d_jobs, list, cnt, n, st.w_cur, c->part_n.as<uint32_t>(),
-                                              m.bucket_hist, m.bucket_cursor, s));
-                FA_CUDA(launch_ext(c->kernel, d_jobs, c->part_n.as<uint32_t>(), n, cnt, d_q, d_t, kp, qcap_all,
-                                   st.w_cur, d_out, c->clamped.as<uint8_t>(), c->cells_job.as<uint32_t>(), m.cells,
-                                   m.status, s));
-                launches += 3;
+                                              m.bucket_hist, m.bucket_cursor, m.group_bounds, s));
+                if (c->kernel == FA_KERNEL_INT16X2) {
+                    FA_CUDA(launch_ext(c->kernel, d_jobs, c->part_n.as<uint32_t>(), n, cnt, d_q, d_t, kp, qcap_all,
+                                       st.w_cur, d_out, d_flags, cert, c->cells_job.as<uint32_t>(), m.cells,
+                                       m.status, s));
+                    launches += 3;
+                } else {
+                    if (int rc = launch_learned_round(c, d_jobs, c->part_n.as<uint32_t>(), n, d_q, d_t, kp, qcap_all,
+                                                      st.w_cur, d_out, d_flags, cert, m, s))
+                        return rc;
+                    launches += 5;
+                }
             } else {
                 FA_CUDA(launch_ext(c->kernel, d_jobs, list, n, cnt, d_q, d_t, kp, qcap_all, st.w_cur, d_out,
-                                   c->clamped.as<uint8_t>(), c->cells_job.as<uint32_t>(), m.cells, m.status, s));
+                                   d_flags, cert, c->cells_job.as<uint32_t>(), m.cells, m.status, s));
                 ++launches;
             }
             FA_CUDA(cudaMemsetAsync(next_cnt, 0, 4, s));
-            FA_CUDA(launch_policy_step(d_jobs, list, cnt, n, d_out, c->clamped.as<uint8_t>(), st, max_tries,
+            FA_CUDA(launch_policy_step(d_jobs, list, cnt, n, d_out, d_flags, st, max_tries,
                                        pol->judge, next, next_cnt, s));
             ++launches;
             uint32_t h_cnt = 0;
@@ -366,6 +416,11 @@ void fa_ctx_destroy(fa_ctx *c) {
                       &c->missed, &c->list_a, &c->list_b, &c->hist, &c->feat, &c->wbf, &c->part_n,
                       &c->part_w})
         b->release();
+    for (int k = 0; k < 2; ++k) {
+        if (c->join_ev[k]) cudaEventDestroy(c->join_ev[k]);
+        if (c->aux[k]) cudaStreamDestroy(c->aux[k]);
+    }
+    if (c->fork_ev) cudaEventDestroy(c->fork_ev);
     if (c->kev0) cudaEventDestroy(c->kev0);
     if (c->kev1) cudaEventDestroy(c->kev1);
     if (c->ev0) cudaEventDestroy(c->ev0);
@@ -557,7 +612,7 @@ int fa_ext_batch_device(fa_ctx *c, const fa_params *p, const fa_job *d_jobs, uin
     if (c->timing) FA_CUDA(cudaEventRecord(c->kev0, s));
     for (auto &sg : segs) {
         FA_CUDA(launch_ext(c->kernel, d_jobs, order + b, sg.first - b, nullptr, d_qseq, d_tseq, kp, sg.second,
-                           nullptr, d_out, nullptr, nullptr, nullptr, m.status, s));
+                           nullptr, d_out, nullptr, false, nullptr, nullptr, m.status, s));
         b = sg.first;
     }
     if (c->timing) FA_CUDA(cudaEventRecord(c->kev1, s));

@@ -16,12 +16,12 @@ constexpr int kPackedHMax = 8191;    // largest H/E the packed column word holds
 constexpr int kBandBuckets = 13;   // configured band + 12 narrow band classes
 constexpr int kPairThreads = 32;     // threads per int16x2 extension block (2 jobs each)
 
-size_t ext_packed_smem_bytes(int qcap);
+size_t ext_packed_smem_bytes(int qcap, int ring);
 cudaError_t launch_ext_packed(const fa_job *d_jobs, const uint32_t *d_order, uint32_t n,
-                              const uint32_t *d_n, const uint8_t *d_qseq, const uint8_t *d_tseq,
-                              const ExtParams &p, int qcap, const int32_t *d_w_try,
-                              fa_ext_result *d_out, uint8_t *d_clamped, uint32_t *d_cells_job,
-                              unsigned long long *d_cells, uint32_t *d_status,
+                              const uint32_t *d_first, const uint32_t *d_n, const uint8_t *d_qseq,
+                              const uint8_t *d_tseq, const ExtParams &p, int qcap, int ring,
+                              const int32_t *d_w_try, fa_ext_result *d_out, uint8_t *d_clamped, bool cert,
+                              uint32_t *d_cells_job, unsigned long long *d_cells, uint32_t *d_status,
                               cudaStream_t stream);
 
 // int16x2 variant: two jobs per thread (extend_pair_kernel.cu).  Eligible for
@@ -49,7 +49,7 @@ cudaError_t launch_policy_step(const fa_job *d_jobs, const uint32_t *d_list, con
                                uint32_t *d_next_count, cudaStream_t stream);
 cudaError_t launch_band_partition(const fa_job *d_jobs, const uint32_t *d_list, const uint32_t *d_count,
                                   uint32_t n_max, const int32_t *d_w_cur, uint32_t *d_out, uint32_t *d_hist,
-                                  uint32_t *d_cursor, cudaStream_t stream);
+                                  uint32_t *d_cursor, uint32_t *d_bounds, cudaStream_t stream);
 cudaError_t launch_policy_init(const fa_job *d_jobs, uint32_t n, const int32_t *d_w_first, int w_min,
                                int learned, PolicyState st, cudaStream_t stream);
 

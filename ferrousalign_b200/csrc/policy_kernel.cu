@@ -144,12 +144,19 @@ __global__ void band_hist_kernel(const fa_job *__restrict__ jobs, const uint32_t
 __global__ void band_scatter_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ list,
                                     const uint32_t *__restrict__ count, uint32_t n_max,
                                     const int32_t *__restrict__ w_cur, const uint32_t *__restrict__ hist,
-                                    uint32_t *__restrict__ cursor, uint32_t *__restrict__ out)
+                                    uint32_t *__restrict__ cursor, uint32_t *__restrict__ out,
+                                    uint32_t *__restrict__ bounds)
 {
     __shared__ uint32_t base[kBandBuckets];
     if (threadIdx.x == 0) {
         uint32_t acc = 0;
         for (int k = 0; k < kBandBuckets; ++k) { base[k] = acc; acc += hist[k]; }
+        if (bounds && blockIdx.x == 0) {
+            // band groups: buckets 0-4 (configured band, bands > 24), 5-6 (13-24), 7-12 (<= 12)
+            bounds[0] = base[5];
+            bounds[1] = base[7];
+            bounds[2] = acc;
+        }
     }
     __syncthreads();
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -172,7 +179,7 @@ __global__ void band_scatter_kernel(const fa_job *__restrict__ jobs, const uint3
 
 cudaError_t launch_band_partition(const fa_job *d_jobs, const uint32_t *d_list, const uint32_t *d_count,
                                   uint32_t n_max, const int32_t *d_w_cur, uint32_t *d_out, uint32_t *d_hist,
-                                  uint32_t *d_cursor, cudaStream_t stream)
+                                  uint32_t *d_cursor, uint32_t *d_bounds, cudaStream_t stream)
 {
     if (n_max == 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(d_hist, 0, sizeof(uint32_t) * kBandBuckets, stream);
@@ -180,7 +187,8 @@ cudaError_t launch_band_partition(const fa_job *d_jobs, const uint32_t *d_list, 
     if (e != cudaSuccess) return e;
     const uint32_t blocks = (n_max + 255) / 256;
     band_hist_kernel<<<blocks, 256, 0, stream>>>(d_jobs, d_list, d_count, n_max, d_w_cur, d_hist);
-    band_scatter_kernel<<<blocks, 256, 0, stream>>>(d_jobs, d_list, d_count, n_max, d_w_cur, d_hist, d_cursor, d_out);
+    band_scatter_kernel<<<blocks, 256, 0, stream>>>(d_jobs, d_list, d_count, n_max, d_w_cur, d_hist, d_cursor, d_out,
+                                                    d_bounds);
     return cudaGetLastError();
 }
 

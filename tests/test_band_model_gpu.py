@@ -31,6 +31,37 @@ def test_gradients_match_cpu_oracle(ctx):
     assert np.max(np.abs(y - yr)) <= 1e-4 * max(1.0, np.max(np.abs(yr)))
 
 
+def test_features_match_restatement(ctx):
+    b = synth.workload_ext_1m(3000, seed=406)
+    b2 = synth.workload_ext_uneven(1000, seed=407, ref_len=2_000_000)
+    p = fa.BandedPairWiseSW().to_struct()
+    for batch in (b, b2):
+        hints = B.hints_from_info(batch.info)
+        x = B.features(p, batch.jobs, batch.qseq, batch.tseq, hints, ctx=ctx)
+        xr = M.features(1, batch.jobs, batch.qseq, batch.tseq, hints)
+        bad = np.argwhere(x != xr)
+        assert len(bad) == 0, f"{len(bad)} feature values differ, first {bad[:3].tolist()}"
+        assert len(np.unique(x[:, 14])) > 1 and len(np.unique(x[:, 15])) > 1
+
+
+def test_first_band_rule(ctx):
+    rng = np.random.default_rng(9)
+    x = rng.normal(0.0, 1.0, size=(5000, 16)).astype(np.float32)
+    w = rng.normal(0.0, 0.3, M.NPARAMS).astype(np.float32)
+    w[M.O_B3] = 3.0                           # outputs spread over bands 1..2^9
+    m = B.BandModel.create(seed=3)
+    m.set(w=w, mean=x.mean(0), std=x.std(0))
+    jobs = np.zeros(len(x), N.JOB_DT)
+    jobs["w"] = rng.choice([20, 50, 100, 200], len(x))
+    for margin, w_min in ((0.0, 2), (0.5, 4), (-0.3, 1)):
+        y, band = m.predict(x, jobs=jobs, margin=margin, w_min=w_min, ctx=ctx)
+        ref = M.first_band(y, margin, w_min, jobs["w"])
+        e = np.clip(y.astype(np.float64) + margin, 0, 16)
+        clear = np.abs(np.exp2(e) - np.round(np.exp2(e))) > 1e-3     # away from integer boundaries
+        assert clear.mean() > 0.9
+        assert np.array_equal(band[clear], ref[clear])
+
+
 def test_first_band_rule(ctx):
     rng = np.random.default_rng(9)
     x = rng.normal(0.0, 1.0, size=(5000, 16)).astype(np.float32)
