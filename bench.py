@@ -131,31 +131,51 @@ def cpu_oracle_rate(b, p, sample: int):
 
 def bench_learned(args, ctx, b, p):
     """Learned band vs plain band on the same 1M batch: the plain bwa-mem2 retry policy at
-    w=100 against the learned path (GPU features + MLP first band, judge, retry), both
-    through the host ABI; rates from the device time of their kernels; outputs compared."""
+    w=100 against the learned path (GPU features + MLP first band, exit-bound certificate
+    as the judge, one narrow try then the configured band), and the same policy without
+    the network (every job starting at one fixed band); all through the host ABI, rates
+    from the device time of their kernels, outputs compared with the plain path's."""
     import ferrousalign_b200 as fa
     from ferrousalign_b200 import _native as N
     from ferrousalign_b200 import band_model as B
     bwa = fa.make_policy(N.FA_POLICY_BWA, 2)
     model = B.BandModel.load()
     hints = B.hints_from_info(b.info)
-    plain_ms, learned_ms = [], []
-    plain = learned = None
-    for _ in range(max(2, args.steps // 10)):
+    n = len(b.jobs)
+    fixed_w = 24
+    nonet_pol = fa.make_policy(N.FA_POLICY_LEARNED, 2, B.JUDGE_LEARNED, 1)
+    wf_fixed = np.full(n, fixed_w, np.int32)
+    plain_ms, learned_ms, nonet_ms = [], [], []
+    plain = learned = nonet = None
+    for _ in range(max(3, args.steps // 10)):
         plain, pst, _ = fa.extend_batch(p, b.jobs, b.qseq, b.tseq, policy=bwa, ctx=ctx)
         plain_ms.append(float(pst["kernel_ms"]))
         learned, lst, wf, _ = B.extend_batch_learned(p, b.jobs, b.qseq, b.tseq, model, hints=hints, ctx=ctx)
         learned_ms.append(float(lst["kernel_ms"]))
-    n = len(b.jobs)
-    pm, lm = float(np.median(plain_ms)), float(np.median(learned_ms))
+        nonet, nst, _ = fa.extend_batch(p, b.jobs, b.qseq, b.tseq, policy=nonet_pol, w_first=wf_fixed, ctx=ctx)
+        nonet_ms.append(float(nst["kernel_ms"]))
+    pm, lm, fm = float(np.median(plain_ms)), float(np.median(learned_ms)), float(np.median(nonet_ms))
     return {"plain": {"policy": "bwa-mem2 w=100 then 200", "value": n / (pm * 1e-3), "unit": "alignments/s",
+                      "gcups": float(pst["cells_executed"]) / (pm * 1e-3) / 1e9,
                       "kernel_ms": pm, "cells_executed": int(pst["cells_executed"])},
-            "learned": {"policy": "MLP first band (>= 16), max_off + end-to-end judge, doubling / full-band retry",
+            "learned": {"policy": "MLP first band (ladder 2,3,4,6,8,12,..; >= 2), exit-bound certificate judge "
+                                  "(exact), one narrow try then w=100 plain policy",
                         "value": n / (lm * 1e-3), "unit": "alignments/s", "kernel_ms": lm,
+                        "kernel_launches": int(lst["kernel_launches"]),
                         "cells_executed": int(lst["cells_executed"]),
                         "cells_saved_frac": 1.0 - float(lst["cells_executed"]) / float(pst["cells_executed"]),
-                        "miss_rate": float(lst["misses"]) / n, "first_band_median": float(np.median(wf))},
-            "speedup": pm / lm, "identical_outputs": bool(np.array_equal(plain, learned)),
+                        "miss_rate": float(lst["misses"]) / n,
+                        "wasted_cells": int(lst["cells_executed"]) - int(lst["cells"]),
+                        "wasted_frac_of_executed": (float(lst["cells_executed"]) - float(lst["cells"]))
+                        / float(lst["cells_executed"]),
+                        "first_band_median": float(np.median(wf))},
+            "no_network": {"policy": f"same policy, every job first at w={fixed_w} (best fixed first band on the "
+                                     "held-out evaluation batch)",
+                           "value": n / (fm * 1e-3), "unit": "alignments/s", "kernel_ms": fm,
+                           "cells_executed": int(nst["cells_executed"]),
+                           "identical_outputs": bool(np.array_equal(plain, nonet))},
+            "speedup": pm / lm, "network_gain": fm / lm,
+            "identical_outputs": bool(np.array_equal(plain, learned)),
             "identical_frac": float(np.mean(plain == learned))}
 
 
