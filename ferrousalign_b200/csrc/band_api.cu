@@ -161,7 +161,7 @@ int fa_band_features(fa_ctx *ctx, const fa_params *p, const fa_job *jobs, uint32
     int ms = 0;
     for (int i = 0; i < 25; ++i) if (p->mat[i] > ms) ms = p->mat[i];
     BA_CUDA(cudaSetDevice(fa_ctx_device(ctx)));
-    DBuf dj(sizeof(fa_job) * (size_t)n), dq(qseq_len ? qseq_len : 1), dt(tseq_len ? tseq_len : 1),
+    DBuf dj(sizeof(fa_job) * (size_t)n), dq(qseq_len + kSeqPad), dt(tseq_len + kSeqPad),
         dh(hints ? sizeof(fa_band_hint) * (size_t)n : 0), dx(sizeof(float) * 16 * (size_t)n);
     if (!dj.ok() || !dq.ok() || !dt.ok() || !dx.ok() || (hints && !dh.ok()))
         return err(FA_ERR_CAPACITY, "device allocation failed");
@@ -169,7 +169,7 @@ int fa_band_features(fa_ctx *ctx, const fa_params *p, const fa_job *jobs, uint32
     BA_CUDA(cudaMemcpy(dq.p, qseq, qseq_len, cudaMemcpyHostToDevice));
     BA_CUDA(cudaMemcpy(dt.p, tseq, tseq_len, cudaMemcpyHostToDevice));
     if (hints) BA_CUDA(cudaMemcpy(dh.p, hints, sizeof(fa_band_hint) * (size_t)n, cudaMemcpyHostToDevice));
-    BA_CUDA(launch_band_features(dj.as<fa_job>(), n, dq.as<uint8_t>(), dt.as<uint8_t>(),
+    BA_CUDA(launch_band_features(dj.as<fa_job>(), n, dq.as<uint8_t>(), qseq_len, dt.as<uint8_t>(), tseq_len,
                                  hints ? dh.as<fa_band_hint>() : nullptr, ms, dx.as<float>(), 0));
     BA_CUDA(cudaMemcpy(x, dx.p, sizeof(float) * 16 * (size_t)n, cudaMemcpyDeviceToHost));
     return FA_OK;

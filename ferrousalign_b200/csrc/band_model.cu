@@ -29,84 +29,126 @@ namespace fa {
 // 11 longest matching block run / blocks              12 N bases in the query
 // 13 tlen - qlen                    14 |best shift| of the second half (diagonals -4..4)
 // 15 mismatch fraction of the second half on that best shifted diagonal
-// One warp per job, one pass over the query: lane l takes positions l, l+32, ...; every
-// load instruction of the warp touches consecutive bytes, and counts and extremes are
-// warp reductions (redux.sync).
+// One thread per job, 16 positions per step as four 32-bit words: the query bytes and a
+// 28-byte target window are read as aligned words and realigned with funnel shifts;
+// byte-wise SIMD compares (__vcmpne4, __vcmpgtu4) give one 0xFF byte per mismatching
+// position, masked to the valid position range, and counts / last positions come from
+// popc / clz.  The valid range of each shifted diagonal is known in closed form, so only
+// its mismatches are counted.  Sequence buffers carry kSeqPad bytes of padding, so the
+// word holding a buffer's last byte is always inside the allocation.
+__device__ __forceinline__ uint32_t byte_range_mask(int p0, int lo, int hi)
+{
+    const int a = min(max(lo - p0, 0), 4), b = min(max(hi - p0, 0), 4);
+    const uint32_t hm = b >= 4 ? 0xFFFFFFFFu : (1u << (8 * b)) - 1u;
+    const uint32_t lm = a >= 4 ? 0xFFFFFFFFu : (1u << (8 * a)) - 1u;
+    return hm & ~lm;
+}
+
+__device__ __forceinline__ uint32_t word_at(const uint8_t *__restrict__ base, long long byte_addr, uint64_t bytes)
+{
+    return (byte_addr >= 0 && (uint64_t)byte_addr < bytes)
+               ? __ldg(reinterpret_cast<const uint32_t *>(base + byte_addr)) : 0u;
+}
+
+__device__ __forceinline__ int last_byte(uint32_t m) { return (31 - __clz(m)) >> 3; }
+
 __global__ void __launch_bounds__(128) band_features_kernel(const fa_job *__restrict__ jobs, uint32_t n,
-                                                            const uint8_t *__restrict__ qseq,
-                                                            const uint8_t *__restrict__ tseq,
+                                                            const uint8_t *__restrict__ qseq, uint64_t qbytes,
+                                                            const uint8_t *__restrict__ tseq, uint64_t tbytes,
                                                             const fa_band_hint *__restrict__ hints, int max_score,
                                                             float *__restrict__ x)
 {
-    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (i >= n) return;                       // whole warps exit together
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
     const fa_job jb = jobs[i];
-    const uint8_t *Q = qseq + jb.q_off, *T = tseq + jb.t_off;
     const int qlen = jb.qlen, tlen = jb.tlen;
     const int L = min(qlen, tlen);
     const int nblk = (L + 7) / 8;
     const int half = qlen / 2;
-    int mm = 0, last_mm = -1, nq = 0;
-    int c[9], cnt[9], last_s[9];
+    int lo[9], hi[9], c[9], last_s[9];
 #pragma unroll
-    for (int s = 0; s < 9; ++s) { c[s] = 0; cnt[s] = 0; last_s[s] = -1; }
-    int mmblk = 0, first = -1, lastq = 0, best_run = 0, run = 0;
-    for (int k0 = 0; k0 < qlen; k0 += 32) {
-        const int k = k0 + lane;
-        uint32_t q = 5;
-        if (k < qlen) {
-            q = Q[k];
-            nq += q > 3;
+    for (int s = 0; s < 9; ++s) {
+        const int sh = s - 4;
+        lo[s] = max(half, -sh);
+        hi[s] = min(qlen, tlen - sh);
+        c[s] = 0;
+        last_s[s] = -1;
+    }
+    int mm = 0, last_mm = -1, nq = 0, mmblk = 0, first = -1, lastq = 0, best_run = 0, run = 0;
+    for (int k0 = 0; k0 < qlen; k0 += 16) {
+        uint32_t q4[4], nm[4], t7[7];
+        {
+            const long long a = (long long)jb.q_off + k0, a0 = a & ~3LL;
+            const int sh = (int)(a - a0) * 8;
+            uint32_t w[5];
+#pragma unroll
+            for (int m = 0; m < 5; ++m) w[m] = word_at(qseq, a0 + 4 * m, qbytes);
+#pragma unroll
+            for (int m = 0; m < 4; ++m) q4[m] = __funnelshift_r(w[m], w[m + 1], sh);
         }
-        const int d = (k < L) ? (q != T[k] || q > 3) : 0;
-        mm += d;
-        if (d) last_mm = k;
-        if (k < qlen && k >= half) {
+        {
+            const long long a = (long long)jb.t_off + k0 - 4, a0 = a & ~3LL;   // target bytes k0-4 .. k0+23
+            const int sh = (int)(a - a0) * 8;
+            uint32_t w[8];
 #pragma unroll
-            for (int s = 0; s < 9; ++s) {
-                const int t = k + s - 4;
-                if (t >= 0 && t < tlen) {
-                    const int dd = q != T[t] || q > 3;
-                    c[s] += dd;
-                    ++cnt[s];
-                    if (dd) last_s[s] = k;
+            for (int m = 0; m < 8; ++m) w[m] = word_at(tseq, a0 + 4 * m, tbytes);
+#pragma unroll
+            for (int m = 0; m < 7; ++m) t7[m] = __funnelshift_r(w[m], w[m + 1], sh);
+        }
+        uint32_t dmask[4];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const int p0 = k0 + 4 * m;
+            nm[m] = __vcmpgtu4(q4[m], 0x03030303u);                     // N in the query
+            nq += __popc(nm[m] & byte_range_mask(p0, 0, qlen)) >> 3;
+            const uint32_t d = (__vcmpne4(q4[m], t7[m + 1]) | nm[m]) & byte_range_mask(p0, 0, L);
+            dmask[m] = d;
+            mm += __popc(d) >> 3;
+            if (d) last_mm = p0 + last_byte(d);
+        }
+#pragma unroll
+        for (int bb = 0; bb < 2; ++bb) {                                // 8-position blocks
+            const int bidx = k0 / 8 + bb;
+            if (bidx < nblk) {
+                if (dmask[2 * bb] | dmask[2 * bb + 1]) {
+                    ++mmblk;
+                    if (first < 0) first = bidx;
+                    if (bidx * 4 >= nblk * 3) ++lastq;
+                    run = 0;
+                } else {
+                    best_run = max(best_run, ++run);
                 }
             }
         }
-        // 8-position blocks of this 32-position step (steps are block aligned)
-        const unsigned bal = __ballot_sync(0xffffffffu, d);
-        for (int qb = 0; qb < 4; ++qb) {
-            const int bidx = k0 / 8 + qb;
-            if (bidx >= nblk) break;
-            if ((bal >> (8 * qb)) & 0xffu) {
-                ++mmblk;
-                if (first < 0) first = bidx;
-                if (bidx * 4 >= nblk * 3) ++lastq;
-                run = 0;
-            } else {
-                best_run = max(best_run, ++run);
+        if (k0 + 16 > half) {
+#pragma unroll
+            for (int s = 0; s < 9; ++s) {                               // target shifted by s - 4
+#pragma unroll
+                for (int m = 0; m < 4; ++m) {
+                    const int p0 = k0 + 4 * m;
+                    const uint32_t rm = byte_range_mask(p0, lo[s], hi[s]);
+                    // bytes T[p0 + s - 4 ..]: offset 4m + s in the window
+                    const int wi = m + s / 4;
+                    const uint32_t tw = __funnelshift_r(t7[wi], t7[wi + 1], 8 * (s % 4));
+                    const uint32_t dd = (__vcmpne4(q4[m], tw) | nm[m]) & rm;
+                    c[s] += __popc(dd) >> 3;
+                    if (dd) last_s[s] = p0 + last_byte(dd);
+                }
             }
         }
     }
-    mm = __reduce_add_sync(0xffffffffu, mm);
-    nq = __reduce_add_sync(0xffffffffu, nq);
-    last_mm = __reduce_max_sync(0xffffffffu, last_mm);
     // shifted diagonal with the lowest mismatch fraction (ties: the smaller shift)
     int best_s = 0, best_c = -1, best_n = 1, best_last = -1;
 #pragma unroll
     for (int s = 0; s < 9; ++s) {
-        const int cs = __reduce_add_sync(0xffffffffu, c[s]);
-        const int ns = __reduce_add_sync(0xffffffffu, cnt[s]);
-        const int ls = __reduce_max_sync(0xffffffffu, last_s[s]);
+        const int ns = max(0, hi[s] - lo[s]);
         const int sh = s - 4;
-        const long long lhs = (long long)cs * best_n, rhs = (long long)best_c * ns;
+        const long long lhs = (long long)c[s] * best_n, rhs = (long long)best_c * ns;
         if (ns > 0 && (best_c < 0 || lhs < rhs || (lhs == rhs && abs(sh) < abs(best_s)))) {
-            best_c = cs; best_n = ns; best_s = sh; best_last = ls;
+            best_c = c[s]; best_n = ns; best_s = sh; best_last = last_s[s];
         }
     }
-    if (lane != 0) return;
-    float *o = x + (size_t)i * 16;
+    float o[16];
     const float fb = (float)max(nblk, 1);
     o[0] = max_score > 0 ? (float)jb.h0 / (float)max_score : (float)jb.h0;
     o[1] = (float)qlen;
@@ -124,15 +166,18 @@ __global__ void __launch_bounds__(128) band_features_kernel(const fa_job *__rest
     o[13] = (float)(tlen - qlen);
     o[14] = (float)abs(best_s);
     o[15] = best_c < 0 ? 1.f : (float)best_c / (float)best_n;
+    float4 *xo = reinterpret_cast<float4 *>(x + (size_t)i * 16);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) xo[k] = make_float4(o[4 * k], o[4 * k + 1], o[4 * k + 2], o[4 * k + 3]);
 }
 
-cudaError_t launch_band_features(const fa_job *d_jobs, uint32_t n, const uint8_t *d_q, const uint8_t *d_t,
-                                 const fa_band_hint *d_hints, int max_score, float *d_x, cudaStream_t s)
+cudaError_t launch_band_features(const fa_job *d_jobs, uint32_t n, const uint8_t *d_q, uint64_t qbytes,
+                                 const uint8_t *d_t, uint64_t tbytes, const fa_band_hint *d_hints, int max_score,
+                                 float *d_x, cudaStream_t s)
 {
     if (n == 0) return cudaSuccess;
-    const uint64_t threads = (uint64_t)n * 32;
-    band_features_kernel<<<(uint32_t)((threads + 127) / 128), 128, 0, s>>>(d_jobs, n, d_q, d_t, d_hints, max_score,
-                                                                           d_x);
+    band_features_kernel<<<(n + 127) / 128, 128, 0, s>>>(d_jobs, n, d_q, qbytes, d_t, tbytes, d_hints, max_score,
+                                                         d_x);
     return cudaGetLastError();
 }
 

@@ -230,8 +230,8 @@ void length_order(const fa_job *jobs, uint32_t n, std::vector<uint32_t> &order,
 int ensure_ext_buffers(fa_ctx *c, uint32_t n, uint64_t qb, uint64_t tb) {
     FA_CUDA(c->jobs.ensure(sizeof(fa_job) * (size_t)n));
     FA_CUDA(c->order.ensure(sizeof(uint32_t) * (size_t)n));
-    FA_CUDA(c->qseq.ensure(qb));
-    FA_CUDA(c->tseq.ensure(tb));
+    FA_CUDA(c->qseq.ensure(qb + kSeqPad));
+    FA_CUDA(c->tseq.ensure(tb + kSeqPad));
     FA_CUDA(c->out.ensure(sizeof(fa_ext_result) * (size_t)n));
     FA_CUDA(c->clamped.ensure(n));
     FA_CUDA(c->cells_job.ensure(sizeof(uint32_t) * (size_t)n));
@@ -534,8 +534,8 @@ int fa_ext_batch_learned(fa_ctx *c, const fa_params *p, const fa_policy *pol, co
     band_model_export(model, wbf, mean, sd);
     FA_CUDA(cudaMemcpyAsync(c->wbf.p, wbf.data(), sizeof(__nv_bfloat16) * FA_BAND_NPARAMS, cudaMemcpyHostToDevice, s));
     FA_CUDA(cudaEventRecord(c->ev0, s));
-    FA_CUDA(launch_band_features(c->jobs.as<fa_job>(), n, c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(), d_h,
-                                 kp.max_score, d_x, s));
+    FA_CUDA(launch_band_features(c->jobs.as<fa_job>(), n, c->qseq.as<uint8_t>(), qseq_len, c->tseq.as<uint8_t>(),
+                                 tseq_len, d_h, kp.max_score, d_x, s));
     FA_CUDA(launch_band_predict(c->wbf.as<__nv_bfloat16>(), mean, sd, d_x, c->jobs.as<fa_job>(), n, margin, pol->w_min,
                                 nullptr, c->w_first.as<int32_t>(), s));
     FA_CUDA(cudaEventRecord(c->ev1, s));
