@@ -27,6 +27,8 @@ if len(sys.argv) > 1 and sys.argv[1] in ("learned", "bands"):
             out, st, wf, wfin = B.extend_batch_learned(p, b.jobs, b.qseq, b.tseq, m, hints=hints, ctx=ctx)
             print("learned kernel ms", float(st["kernel_ms"]), "cells", int(st["cells_executed"]),
                   "launches", int(st["kernel_launches"]), "retries", int(st["retries"]))
+        vals, cnts = np.unique(wf, return_counts=True)
+        print("first bands", {int(v): int(c) for v, c in zip(vals, cnts)})
     else:
         for w in (1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 64, 100):
             j = b.jobs.copy()
