@@ -255,16 +255,38 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
 #pragma unroll 4
                 for (int j = beg; j < end; ++j) {
                     const uint32_t wd = col[slot(j) * T];
-                    const int M = (int)(wd >> 16);
-                    const int e = (int)((wd >> 3) & 0x1FFFu);
-                    const uint32_t q = wd & 7u;
-                    const int s = prmt_s8(row_lo, row_hi, q * 0x1111u + 0x8880u);
-                    const int Mp = M ? M + s : 0;
-                    const int h = __vimax3_s32(Mp, e, f);
-                    const int e_new = __viaddmax_s32_relu(e, -e_del, Mp - oe_del);
-                    f = __viaddmax_s32_relu(f, -e_ins, Mp - oe_ins);
-                    key = max(key, (h << 12) | (4095 - j));   // first column of the row max
-                    col[slot(j) * T] = (uint32_t)h1 << 16 | (uint32_t)e_new << 3 | q;
+                    int h;
+                    if constexpr (!CERT) {
+                        // Unpacking, the key and the repacking as multiplies and high
+                        // multiplies, which can issue on the FMA pipe beside the DPX max/add
+                        // work on the integer pipe (measured faster for this variant; the
+                        // certificate variants keep the shift form, which needs fewer
+                        // registers there).
+                        const int M = (int)__umulhi(wd, 1u << 16);                  // bits 16..31
+                        const int e = (int)__umulhi(wd * (1u << 16), 1u << 13);     // bits 3..15
+                        const uint32_t q = wd & 7u;
+                        const int s = prmt_s8(row_lo, row_hi, q * 0x1111u + 0x8880u);
+                        // M == 0 leaves no diagonal term (ksw_extend2's `M ? M + s : 0`); any
+                        // value <= 0 acts exactly like 0 in every max below, and for M > 0
+                        // M * 8192 exceeds M + s
+                        const int Mp = __viaddmin_s32(M, s, M * 8192);
+                        h = __vimax3_s32(Mp, e, f);
+                        const int e_new = __viaddmax_s32_relu(e, -e_del, Mp - oe_del);
+                        f = __viaddmax_s32_relu(f, -e_ins, Mp - oe_ins);
+                        key = max(key, h * 4096 + (4095 - j));   // first column of the row max
+                        col[slot(j) * T] = (uint32_t)h1 * 65536u + (uint32_t)e_new * 8u + q;
+                    } else {
+                        const int M = (int)(wd >> 16);
+                        const int e = (int)((wd >> 3) & 0x1FFFu);
+                        const uint32_t q = wd & 7u;
+                        const int s = prmt_s8(row_lo, row_hi, q * 0x1111u + 0x8880u);
+                        const int Mp = M ? M + s : 0;
+                        h = __vimax3_s32(Mp, e, f);
+                        const int e_new = __viaddmax_s32_relu(e, -e_del, Mp - oe_del);
+                        f = __viaddmax_s32_relu(f, -e_ins, Mp - oe_ins);
+                        key = max(key, (h << 12) | (4095 - j));   // first column of the row max
+                        col[slot(j) * T] = (uint32_t)h1 << 16 | (uint32_t)e_new << 3 | q;
+                    }
                     h1 = h;
                 }
                 if (RING > 0) {

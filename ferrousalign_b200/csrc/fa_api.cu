@@ -302,7 +302,10 @@ int run_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n,
         const uint32_t *cnt = nullptr;
         uint32_t *next = c->list_a.as<uint32_t>(), *next_cnt = m.cnt_a;
         uint32_t *spare = c->list_b.as<uint32_t>(), *spare_cnt = m.cnt_b;
+        const bool once = learned && (pol->judge & FA_JUDGE_ONCE);
         for (int r = 0; r < max_rounds; ++r) {
+            // with one narrow try, rounds after the first hold only plain-policy runs
+            const bool cert_r = cert && !(once && r > 0);
             if (r == 0 && !learned) {
                 uint32_t b = 0;
                 for (auto &sg : segs) {
@@ -319,12 +322,12 @@ int run_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n,
                                               m.bucket_hist, m.bucket_cursor, m.group_bounds, s));
                 if (c->kernel == FA_KERNEL_INT16X2) {
                     FA_CUDA(launch_ext(c->kernel, d_jobs, c->part_n.as<uint32_t>(), n, cnt, d_q, d_t, kp, qcap_all,
-                                       st.w_cur, d_out, d_flags, cert, c->cells_job.as<uint32_t>(), m.cells,
+                                       st.w_cur, d_out, d_flags, cert_r, c->cells_job.as<uint32_t>(), m.cells,
                                        m.status, s));
                     launches += 3;
                 } else {
                     if (int rc = launch_learned_round(c, d_jobs, c->part_n.as<uint32_t>(), n, d_q, d_t, kp, qcap_all,
-                                                      st.w_cur, d_out, d_flags, cert, m, s))
+                                                      st.w_cur, d_out, d_flags, cert_r, m, s))
                         return rc;
                     launches += 5;
                 }
@@ -334,7 +337,7 @@ int run_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n,
                 ++launches;
             }
             FA_CUDA(cudaMemsetAsync(next_cnt, 0, 4, s));
-            FA_CUDA(launch_policy_step(d_jobs, list, cnt, n, d_out, d_flags, st, max_tries,
+            FA_CUDA(launch_policy_step(d_jobs, list, nullptr, cnt, n, d_out, d_flags, st, max_tries,
                                        pol->judge, next, next_cnt, s));
             ++launches;
             uint32_t h_cnt = 0;

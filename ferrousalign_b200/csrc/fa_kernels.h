@@ -43,10 +43,10 @@ struct PolicyState {
     int32_t *tries;      // runs per job
     uint8_t *missed;     // learned path: first narrow run not accepted
 };
-cudaError_t launch_policy_step(const fa_job *d_jobs, const uint32_t *d_list, const uint32_t *d_count,
-                               uint32_t n_max, const fa_ext_result *d_out, const uint8_t *d_clamped,
-                               PolicyState st, int max_tries, int judge, uint32_t *d_next,
-                               uint32_t *d_next_count, cudaStream_t stream);
+cudaError_t launch_policy_step(const fa_job *d_jobs, const uint32_t *d_list, const uint32_t *d_first,
+                               const uint32_t *d_count, uint32_t n_max, const fa_ext_result *d_out,
+                               const uint8_t *d_clamped, PolicyState st, int max_tries, int judge,
+                               uint32_t *d_next, uint32_t *d_next_count, cudaStream_t stream);
 cudaError_t launch_band_partition(const fa_job *d_jobs, const uint32_t *d_list, const uint32_t *d_count,
                                   uint32_t n_max, const int32_t *d_w_cur, uint32_t *d_out, uint32_t *d_hist,
                                   uint32_t *d_cursor, uint32_t *d_bounds, cudaStream_t stream);

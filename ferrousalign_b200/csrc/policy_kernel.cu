@@ -47,12 +47,13 @@ __global__ void policy_init_kernel(const fa_job *__restrict__ jobs, uint32_t n,
 }
 
 __global__ void policy_step_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ list,
-                                   const uint32_t *__restrict__ count, uint32_t n_max,
-                                   const fa_ext_result *__restrict__ out,
+                                   const uint32_t *__restrict__ first, const uint32_t *__restrict__ count,
+                                   uint32_t n_max, const fa_ext_result *__restrict__ out,
                                    const uint8_t *__restrict__ clamped, PolicyState st, int max_tries,
                                    int judge, uint32_t *__restrict__ next, uint32_t *__restrict__ next_count)
 {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    // list entries [*first, *count) (device-side bounds; 0 and n_max when null)
+    const uint32_t t = (first ? *first : 0u) + blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t n = count ? min(*count, n_max) : n_max;
     bool again = false;
     uint32_t jid = 0;
@@ -200,13 +201,13 @@ cudaError_t launch_policy_init(const fa_job *d_jobs, uint32_t n, const int32_t *
     return cudaGetLastError();
 }
 
-cudaError_t launch_policy_step(const fa_job *d_jobs, const uint32_t *d_list, const uint32_t *d_count,
-                               uint32_t n_max, const fa_ext_result *d_out, const uint8_t *d_clamped,
-                               PolicyState st, int max_tries, int judge, uint32_t *d_next,
-                               uint32_t *d_next_count, cudaStream_t stream)
+cudaError_t launch_policy_step(const fa_job *d_jobs, const uint32_t *d_list, const uint32_t *d_first,
+                               const uint32_t *d_count, uint32_t n_max, const fa_ext_result *d_out,
+                               const uint8_t *d_clamped, PolicyState st, int max_tries, int judge,
+                               uint32_t *d_next, uint32_t *d_next_count, cudaStream_t stream)
 {
     if (n_max == 0) return cudaSuccess;
-    policy_step_kernel<<<(n_max + 255) / 256, 256, 0, stream>>>(d_jobs, d_list, d_count, n_max, d_out,
+    policy_step_kernel<<<(n_max + 255) / 256, 256, 0, stream>>>(d_jobs, d_list, d_first, d_count, n_max, d_out,
                                                                d_clamped, st, max_tries, judge, d_next,
                                                                d_next_count);
     return cudaGetLastError();
