@@ -63,6 +63,7 @@ SIGNATURES = {
     "fa_ctx_sync": (C.c_int, [_P]),
     "fa_ctx_set_timing": (C.c_int, [_P, C.c_int]),
     "fa_ctx_set_kernel": (C.c_int, [_P, C.c_int]),
+    "fa_ctx_set_graph": (C.c_int, [_P, C.c_int]),
     "fa_ctx_last_timing": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_int)]),
     "fa_ext_batch_device_noalloc": (C.c_int, [_P, _P, C.c_uint32, _P, _P, _P, _P]),
     "fa_mate_sw_batch_device": (C.c_int, [_P, _P, _P, C.c_uint32, _P, _P, _P, _P]),
@@ -144,6 +145,10 @@ class Context:
 
     def set_kernel(self, kernel: int) -> None:
         check(load().fa_ctx_set_kernel(self.handle, kernel))
+
+    def set_graph(self, enable: bool) -> None:
+        """Run policy / learned batches as one recorded CUDA graph per batch shape."""
+        check(load().fa_ctx_set_graph(self.handle, int(enable)))
 
     def close(self) -> None:
         if self._h is not None:

@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <functional>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -86,6 +87,12 @@ struct fa_ctx {
     // learned rounds run their band groups on forked streams: fork on `stream`, join back
     cudaStream_t aux[2] = {nullptr, nullptr};
     cudaEvent_t fork_ev = nullptr, join_ev[2] = {nullptr, nullptr};
+    // graph mode: the rounds of a call recorded once as a CUDA graph and replayed while the
+    // call's shape (key) stays the same
+    bool graph = false;
+    cudaGraphExec_t gexec = nullptr;
+    std::vector<uint64_t> gkey;
+    uint32_t glaunches = 0;
 };
 
 int fa::fa_ctx_device(const fa_ctx *c) { return c->device; }
@@ -167,6 +174,7 @@ int check_params(const fa_params *p) {
 
 ExtParams ext_params_of(const fa_params *p) {
     ExtParams k;
+    memset(&k, 0, sizeof(k));   // padding too: graph keys compare the raw words
     memcpy(k.mat, p->mat, 25);
     k.m = p->m;
     k.o_del = p->o_del; k.e_del = p->e_del; k.o_ins = p->o_ins; k.e_ins = p->e_ins;
@@ -268,89 +276,117 @@ int read_status(fa_ctx *c, cudaStream_t s) {
 
 // Runs the extension rounds on device data.  order/segs describe the first round;
 // retry rounds reuse the widest capacity class.
-int run_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n,
-            const std::vector<std::pair<uint32_t, int>> &segs, int qcap_all, const fa_job *d_jobs,
-            const uint32_t *d_order, const uint8_t *d_q, const uint8_t *d_t, const int32_t *d_wfirst,
-            fa_ext_result *d_out, cudaStream_t s, fa_ext_stats *stats, int32_t *h_wfinal) {
+// Number of extension rounds a call may need: narrow rounds of the learned ladder
+// (doubling from w_min up to the widest configured band, or one with FA_JUDGE_ONCE)
+// plus the bwa-mem2 tries.
+int max_rounds_of(const fa_policy *pol, int max_w) {
+    const int mode = pol ? pol->mode : FA_POLICY_SINGLE;
+    if (mode == FA_POLICY_SINGLE) return 1;
+    const int max_tries = std::max(1, pol->max_tries);
+    if (mode != FA_POLICY_LEARNED) return max_tries;
+    int narrow = 1;
+    if (!(pol->judge & FA_JUDGE_ONCE))
+        for (long long w = std::max(1, pol->w_min); w * 2 < max_w && narrow < 13; w *= 2) ++narrow;
+    return narrow + max_tries;
+}
+
+// Enqueues the extension rounds of one call on stream s.  Without `capture` the host
+// reads each round's retry count and stops early when nothing is left; with `capture`
+// (recording a CUDA graph) the rounds run a fixed number of times with every count on
+// the device, so no round needs the host, and the first round is one launch over the
+// length-sorted order instead of one per shared-memory class.
+int enqueue_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n,
+                const std::vector<std::pair<uint32_t, int>> &segs, int qcap_all, int max_w, const fa_job *d_jobs,
+                const uint32_t *d_order, const uint8_t *d_q, const uint8_t *d_t, const int32_t *d_wfirst,
+                fa_ext_result *d_out, cudaStream_t s, bool capture, uint32_t *launches, uint32_t *retries) {
     Misc m = misc_of(c);
     FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
     const int mode = pol ? pol->mode : FA_POLICY_SINGLE;
-    uint32_t launches = 0;
-    FA_CUDA(cudaEventRecord(c->ev0, s));
+    const std::vector<std::pair<uint32_t, int>> one_seg{{n, qcap_all}};
+    const auto &segs0 = capture ? one_seg : segs;
     if (mode == FA_POLICY_SINGLE) {
         uint32_t b = 0;
-        for (auto &sg : segs) {
+        for (auto &sg : segs0) {
             FA_CUDA(launch_ext(c->kernel, d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp, sg.second,
                                nullptr, d_out, nullptr, false, c->cells_job.as<uint32_t>(), m.cells, m.status, s));
-            ++launches;
+            ++*launches;
             b = sg.first;
         }
-    } else {
-        if (int rc = ensure_policy_buffers(c, n)) return rc;
-        PolicyState st{c->w_cur.as<int32_t>(), c->prev.as<int32_t>(), c->kk.as<int32_t>(),
-                       c->w_final.as<int32_t>(), c->tries.as<int32_t>(), c->missed.as<uint8_t>()};
-        const int learned = mode == FA_POLICY_LEARNED;
-        // flags feed the learned judge only; the certificate only its BOUND test
-        uint8_t *d_flags = learned ? c->clamped.as<uint8_t>() : nullptr;
-        const bool cert = learned && (pol->judge & FA_JUDGE_BOUND);
-        FA_CUDA(launch_policy_init(d_jobs, n, d_wfirst, pol->w_min, learned, st, s));
-        ++launches;
-        const int max_tries = std::max(1, pol->max_tries);
-        // worst case rounds: narrow ladder (<= 12 doublings) + bwa tries
-        const int max_rounds = (learned ? 13 : 0) + max_tries;
-        const uint32_t *list = d_order;
-        const uint32_t *cnt = nullptr;
-        uint32_t *next = c->list_a.as<uint32_t>(), *next_cnt = m.cnt_a;
-        uint32_t *spare = c->list_b.as<uint32_t>(), *spare_cnt = m.cnt_b;
-        const bool once = learned && (pol->judge & FA_JUDGE_ONCE);
-        for (int r = 0; r < max_rounds; ++r) {
-            // with one narrow try, rounds after the first hold only plain-policy runs
-            const bool cert_r = cert && !(once && r > 0);
-            if (r == 0 && !learned) {
-                uint32_t b = 0;
-                for (auto &sg : segs) {
-                    FA_CUDA(launch_ext(c->kernel, d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp, sg.second,
-                                       st.w_cur, d_out, d_flags, cert, c->cells_job.as<uint32_t>(),
-                                       m.cells, m.status, s));
-                    ++launches;
-                    b = sg.first;
-                }
-            } else if (learned) {
-                // band buckets (configured band first, then narrow bands decreasing), then the
-                // three band groups concurrently
-                FA_CUDA(launch_band_partition(d_jobs, list, cnt, n, st.w_cur, c->part_n.as<uint32_t>(),
-                                              m.bucket_hist, m.bucket_cursor, m.group_bounds, s));
-                if (c->kernel == FA_KERNEL_INT16X2) {
-                    FA_CUDA(launch_ext(c->kernel, d_jobs, c->part_n.as<uint32_t>(), n, cnt, d_q, d_t, kp, qcap_all,
-                                       st.w_cur, d_out, d_flags, cert_r, c->cells_job.as<uint32_t>(), m.cells,
-                                       m.status, s));
-                    launches += 3;
-                } else {
-                    if (int rc = launch_learned_round(c, d_jobs, c->part_n.as<uint32_t>(), n, d_q, d_t, kp, qcap_all,
-                                                      st.w_cur, d_out, d_flags, cert_r, m, s))
-                        return rc;
-                    launches += 5;
-                }
-            } else {
-                FA_CUDA(launch_ext(c->kernel, d_jobs, list, n, cnt, d_q, d_t, kp, qcap_all, st.w_cur, d_out,
-                                   d_flags, cert, c->cells_job.as<uint32_t>(), m.cells, m.status, s));
-                ++launches;
+        return FA_OK;
+    }
+    PolicyState st{c->w_cur.as<int32_t>(), c->prev.as<int32_t>(), c->kk.as<int32_t>(),
+                   c->w_final.as<int32_t>(), c->tries.as<int32_t>(), c->missed.as<uint8_t>()};
+    const int learned = mode == FA_POLICY_LEARNED;
+    // flags feed the learned judge only; the certificate only its BOUND test
+    uint8_t *d_flags = learned ? c->clamped.as<uint8_t>() : nullptr;
+    const bool cert = learned && (pol->judge & FA_JUDGE_BOUND);
+    FA_CUDA(launch_policy_init(d_jobs, n, d_wfirst, pol->w_min, learned, st, s));
+    ++*launches;
+    const int max_tries = std::max(1, pol->max_tries);
+    const int max_rounds = capture ? max_rounds_of(pol, max_w) : (learned ? 13 : 0) + max_tries;
+    const bool once = learned && (pol->judge & FA_JUDGE_ONCE);
+    const uint32_t *list = d_order;
+    const uint32_t *cnt = nullptr;
+    uint32_t *next = c->list_a.as<uint32_t>(), *next_cnt = m.cnt_a;
+    uint32_t *spare = c->list_b.as<uint32_t>(), *spare_cnt = m.cnt_b;
+    for (int r = 0; r < max_rounds; ++r) {
+        // with one narrow try, rounds after the first hold only plain-policy runs
+        const bool cert_r = cert && !(once && r > 0);
+        if (r == 0 && !learned) {
+            uint32_t b = 0;
+            for (auto &sg : segs0) {
+                FA_CUDA(launch_ext(c->kernel, d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp, sg.second,
+                                   st.w_cur, d_out, d_flags, cert_r, c->cells_job.as<uint32_t>(), m.cells, m.status,
+                                   s));
+                ++*launches;
+                b = sg.first;
             }
-            FA_CUDA(cudaMemsetAsync(next_cnt, 0, 4, s));
-            FA_CUDA(launch_policy_step(d_jobs, list, nullptr, cnt, n, d_out, d_flags, st, max_tries,
-                                       pol->judge, next, next_cnt, s));
-            ++launches;
+        } else if (learned) {
+            // band buckets (configured band first, then narrow bands decreasing), then the
+            // three band groups concurrently
+            FA_CUDA(launch_band_partition(d_jobs, list, cnt, n, st.w_cur, c->part_n.as<uint32_t>(),
+                                          m.bucket_hist, m.bucket_cursor, m.group_bounds, s));
+            if (c->kernel == FA_KERNEL_INT16X2) {
+                FA_CUDA(launch_ext(c->kernel, d_jobs, c->part_n.as<uint32_t>(), n, cnt, d_q, d_t, kp, qcap_all,
+                                   st.w_cur, d_out, d_flags, cert_r, c->cells_job.as<uint32_t>(), m.cells,
+                                   m.status, s));
+                *launches += 3;
+            } else {
+                if (int rc = launch_learned_round(c, d_jobs, c->part_n.as<uint32_t>(), n, d_q, d_t, kp, qcap_all,
+                                                  st.w_cur, d_out, d_flags, cert_r, m, s))
+                    return rc;
+                *launches += 5;
+            }
+        } else {
+            FA_CUDA(launch_ext(c->kernel, d_jobs, list, n, cnt, d_q, d_t, kp, qcap_all, st.w_cur, d_out,
+                               d_flags, cert_r, c->cells_job.as<uint32_t>(), m.cells, m.status, s));
+            ++*launches;
+        }
+        FA_CUDA(cudaMemsetAsync(next_cnt, 0, 4, s));
+        FA_CUDA(launch_policy_step(d_jobs, list, nullptr, cnt, n, d_out, d_flags, st, max_tries,
+                                   pol->judge, next, next_cnt, s));
+        ++*launches;
+        if (!capture) {
             uint32_t h_cnt = 0;
             FA_CUDA(cudaMemcpyAsync(&h_cnt, next_cnt, 4, cudaMemcpyDeviceToHost, s));
             FA_CUDA(cudaStreamSynchronize(s));
             if (h_cnt == 0) break;
-            if (stats) stats->retries += h_cnt;
-            list = next; cnt = next_cnt;
-            std::swap(next, spare);
-            std::swap(next_cnt, spare_cnt);
+            if (retries) *retries += h_cnt;
         }
+        list = next; cnt = next_cnt;
+        std::swap(next, spare);
+        std::swap(next_cnt, spare_cnt);
     }
-    FA_CUDA(cudaEventRecord(c->ev1, s));
+    return FA_OK;
+}
+
+// Status word, statistics and final bands of the call whose work ev0..ev1 bracket.
+// `retries_from_tries`: count retries from the per-job run counts (graph replays, where
+// the host saw no round).
+int finish_ext(fa_ctx *c, const fa_policy *pol, uint32_t n, cudaStream_t s, fa_ext_stats *stats,
+               int32_t *h_wfinal, uint32_t launches, uint32_t retries, bool retries_from_tries) {
+    Misc m = misc_of(c);
+    const int mode = pol ? pol->mode : FA_POLICY_SINGLE;
     if (int rc = read_status(c, s)) return rc;
     if (stats) {
         float ms = 0.f;
@@ -366,6 +402,14 @@ int run_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n,
         uint64_t acc = 0;
         for (uint32_t i = 0; i < n; ++i) acc += cj[i];
         stats->cells = acc;
+        stats->retries = retries;
+        if (retries_from_tries && mode != FA_POLICY_SINGLE) {
+            std::vector<int32_t> tr(n);
+            FA_CUDA(cudaMemcpy(tr.data(), c->tries.p, 4ull * n, cudaMemcpyDeviceToHost));
+            uint64_t t = 0;
+            for (uint32_t i = 0; i < n; ++i) t += (uint32_t)tr[i];
+            stats->retries = (uint32_t)(t - n);
+        }
         if (mode == FA_POLICY_LEARNED) {
             std::vector<uint8_t> ms_(n);
             FA_CUDA(cudaMemcpy(ms_.data(), c->missed.p, n, cudaMemcpyDeviceToHost));
@@ -377,6 +421,87 @@ int run_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n,
     if (h_wfinal && mode != FA_POLICY_SINGLE)
         FA_CUDA(cudaMemcpy(h_wfinal, c->w_final.p, 4ull * n, cudaMemcpyDeviceToHost));
     return FA_OK;
+}
+
+// Runs the extension rounds on device data.  order/segs describe the first round;
+// retry rounds reuse the widest capacity class.
+int run_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n,
+            const std::vector<std::pair<uint32_t, int>> &segs, int qcap_all, const fa_job *d_jobs,
+            const uint32_t *d_order, const uint8_t *d_q, const uint8_t *d_t, const int32_t *d_wfirst,
+            fa_ext_result *d_out, cudaStream_t s, fa_ext_stats *stats, int32_t *h_wfinal) {
+    uint32_t launches = 0, retries = 0;
+    if (pol && pol->mode != FA_POLICY_SINGLE)
+        if (int rc = ensure_policy_buffers(c, n)) return rc;
+    FA_CUDA(cudaEventRecord(c->ev0, s));
+    if (int rc = enqueue_ext(c, kp, pol, n, segs, qcap_all, 0, d_jobs, d_order, d_q, d_t, d_wfirst, d_out, s, false,
+                             &launches, &retries))
+        return rc;
+    FA_CUDA(cudaEventRecord(c->ev1, s));
+    return finish_ext(c, pol, n, s, stats, h_wfinal, launches, retries, false);
+}
+
+// Everything a recorded graph bakes in: the launch sequence's shape, every scalar passed
+// by value, and every buffer address.
+std::vector<uint64_t> graph_key(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n, int qcap, int max_w,
+                                const std::vector<uint64_t> &extra) {
+    std::vector<uint64_t> k{(uint64_t)(pol ? pol->mode : -1), (uint64_t)(pol ? pol->judge : 0),
+                            (uint64_t)(pol ? pol->max_tries : 0), (uint64_t)(pol ? pol->w_min : 0), n,
+                            (uint64_t)qcap, (uint64_t)max_w, (uint64_t)c->kernel};
+    const uint32_t *kw = reinterpret_cast<const uint32_t *>(&kp);
+    for (size_t i = 0; i < sizeof(ExtParams) / 4; ++i) k.push_back(kw[i]);
+    for (DevBuf *b : {&c->jobs, &c->order, &c->qseq, &c->tseq, &c->out, &c->clamped, &c->cells_job, &c->misc,
+                      &c->w_first, &c->w_cur, &c->prev, &c->kk, &c->w_final, &c->tries, &c->missed, &c->list_a,
+                      &c->list_b, &c->feat, &c->wbf, &c->part_n})
+        k.push_back((uint64_t)(uintptr_t)b->p);
+    k.insert(k.end(), extra.begin(), extra.end());
+    return k;
+}
+
+// Graph mode: records `prologue` (if any) and the call's rounds as one CUDA graph the
+// first time a key is seen, then replays it; ev0..ev1 bracket the replay.
+int run_ext_graph(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n, int qcap, int max_w,
+                  const std::vector<uint64_t> &extra, const std::function<int(cudaStream_t, uint32_t *)> &prologue,
+                  const int32_t *d_wfirst, cudaStream_t s, fa_ext_stats *stats, int32_t *h_wfinal) {
+    if (pol && pol->mode != FA_POLICY_SINGLE)
+        if (int rc = ensure_policy_buffers(c, n)) return rc;
+    if (int rc = ensure_aux_streams(c)) return rc;
+    std::vector<uint64_t> key = graph_key(c, kp, pol, n, qcap, max_w, extra);
+    if (!c->gexec || key != c->gkey) {
+        if (c->gexec) {
+            cudaGraphExecDestroy(c->gexec);
+            c->gexec = nullptr;
+        }
+        const std::vector<std::pair<uint32_t, int>> segs{{n, qcap}};
+        uint32_t launches = 0;
+        FA_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+        int rc = prologue ? prologue(s, &launches) : FA_OK;
+        if (!rc)
+            rc = enqueue_ext(c, kp, pol, n, segs, qcap, max_w, c->jobs.as<fa_job>(), c->order.as<uint32_t>(),
+                             c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(), d_wfirst, c->out.as<fa_ext_result>(), s,
+                             true, &launches, nullptr);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(s, &g);
+        if (rc || ec != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            if (rc) return rc;
+            FA_CUDA(ec);
+        }
+        const cudaError_t ei = cudaGraphInstantiate(&c->gexec, g, 0);
+        cudaGraphDestroy(g);
+        FA_CUDA(ei);
+        c->gkey = key;
+        c->glaunches = launches;
+    }
+    FA_CUDA(cudaEventRecord(c->ev0, s));
+    FA_CUDA(cudaGraphLaunch(c->gexec, s));
+    FA_CUDA(cudaEventRecord(c->ev1, s));
+    return finish_ext(c, pol, n, s, stats, h_wfinal, c->glaunches, 0, true);
+}
+
+int max_band_of(const fa_job *jobs, uint32_t n) {
+    int w = 0;
+    for (uint32_t i = 0; i < n; ++i) w = std::max(w, jobs[i].w);
+    return w;
 }
 
 }  // namespace
@@ -424,6 +549,7 @@ void fa_ctx_destroy(fa_ctx *c) {
         if (c->aux[k]) cudaStreamDestroy(c->aux[k]);
     }
     if (c->fork_ev) cudaEventDestroy(c->fork_ev);
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
     if (c->kev0) cudaEventDestroy(c->kev0);
     if (c->kev1) cudaEventDestroy(c->kev1);
     if (c->ev0) cudaEventDestroy(c->ev0);
@@ -487,10 +613,12 @@ int fa_ext_batch_policy(fa_ctx *c, const fa_params *p, const fa_policy *pol, con
         if (int rc = ensure_policy_buffers(c, n)) return rc;
         FA_CUDA(cudaMemcpyAsync(c->w_first.p, w_first, 4ull * n, cudaMemcpyHostToDevice, s));
     }
-    int rc = run_ext(c, kp, pol, n, segs, max_q, c->jobs.as<fa_job>(), c->order.as<uint32_t>(),
-                     c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(),
-                     (pol && pol->mode == FA_POLICY_LEARNED) ? c->w_first.as<int32_t>() : nullptr,
-                     c->out.as<fa_ext_result>(), s, stats, w_final);
+    const int32_t *d_wf = (pol && pol->mode == FA_POLICY_LEARNED) ? c->w_first.as<int32_t>() : nullptr;
+    int rc = c->graph
+                 ? run_ext_graph(c, kp, pol, n, max_q, max_band_of(jobs, n), {}, nullptr, d_wf, s, stats, w_final)
+                 : run_ext(c, kp, pol, n, segs, max_q, c->jobs.as<fa_job>(), c->order.as<uint32_t>(),
+                           c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(), d_wf, c->out.as<fa_ext_result>(), s, stats,
+                           w_final);
     if (rc) return rc;
     FA_CUDA(cudaMemcpyAsync(out, c->out.p, sizeof(fa_ext_result) * (size_t)n, cudaMemcpyDeviceToHost, s));
     FA_CUDA(cudaStreamSynchronize(s));
@@ -536,11 +664,41 @@ int fa_ext_batch_learned(fa_ctx *c, const fa_params *p, const fa_policy *pol, co
     float mean[16], sd[16];
     band_model_export(model, wbf, mean, sd);
     FA_CUDA(cudaMemcpyAsync(c->wbf.p, wbf.data(), sizeof(__nv_bfloat16) * FA_BAND_NPARAMS, cudaMemcpyHostToDevice, s));
+    auto predict = [&](cudaStream_t st, uint32_t *launches) -> int {
+        FA_CUDA(launch_band_features(c->jobs.as<fa_job>(), n, c->qseq.as<uint8_t>(), qseq_len, c->tseq.as<uint8_t>(),
+                                     tseq_len, d_h, kp.max_score, d_x, st));
+        FA_CUDA(launch_band_predict(c->wbf.as<__nv_bfloat16>(), mean, sd, d_x, c->jobs.as<fa_job>(), n, margin,
+                                    pol->w_min, nullptr, c->w_first.as<int32_t>(), st));
+        *launches += 2;
+        return FA_OK;
+    };
+    if (c->graph) {
+        // features, prediction and every round in one graph
+        std::vector<uint64_t> extra{qseq_len, tseq_len, (uint64_t)(uintptr_t)d_h};
+        uint32_t mb;
+        memcpy(&mb, &margin, 4);
+        extra.push_back(mb);
+        for (int k = 0; k < 16; ++k) {
+            uint32_t a, b;
+            memcpy(&a, &mean[k], 4);
+            memcpy(&b, &sd[k], 4);
+            extra.push_back((uint64_t)a << 32 | b);
+        }
+        int rc = run_ext_graph(c, kp, pol, n, max_q, max_band_of(jobs, n), extra, predict, c->w_first.as<int32_t>(),
+                               s, stats, w_final);
+        if (rc) return rc;
+        if (w_first_out) FA_CUDA(cudaMemcpy(w_first_out, c->w_first.p, 4ull * n, cudaMemcpyDeviceToHost));
+        FA_CUDA(cudaMemcpyAsync(out, c->out.p, sizeof(fa_ext_result) * (size_t)n, cudaMemcpyDeviceToHost, s));
+        FA_CUDA(cudaStreamSynchronize(s));
+        if (stats)
+            stats->total_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        return FA_OK;
+    }
     FA_CUDA(cudaEventRecord(c->ev0, s));
-    FA_CUDA(launch_band_features(c->jobs.as<fa_job>(), n, c->qseq.as<uint8_t>(), qseq_len, c->tseq.as<uint8_t>(),
-                                 tseq_len, d_h, kp.max_score, d_x, s));
-    FA_CUDA(launch_band_predict(c->wbf.as<__nv_bfloat16>(), mean, sd, d_x, c->jobs.as<fa_job>(), n, margin, pol->w_min,
-                                nullptr, c->w_first.as<int32_t>(), s));
+    {
+        uint32_t pl = 0;
+        if (int rc = predict(s, &pl)) return rc;
+    }
     FA_CUDA(cudaEventRecord(c->ev1, s));
     float pred_ms = 0.f;
     FA_CUDA(cudaEventSynchronize(c->ev1));
@@ -629,6 +787,18 @@ int fa_ctx_set_kernel(fa_ctx *c, int kernel) {
     if (kernel < FA_KERNEL_AUTO || kernel > FA_KERNEL_INT16X2)
         return fail(FA_ERR_ARG, "unknown kernel choice %d", kernel);
     c->kernel = kernel;
+    return FA_OK;
+}
+
+int fa_ctx_set_graph(fa_ctx *c, int enable) {
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    FA_CUDA(cudaSetDevice(c->device));
+    c->graph = enable != 0;
+    if (!c->graph && c->gexec) {
+        cudaGraphExecDestroy(c->gexec);
+        c->gexec = nullptr;
+        c->gkey.clear();
+    }
     return FA_OK;
 }
 

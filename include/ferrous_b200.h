@@ -193,6 +193,15 @@ int fa_ctx_sync(fa_ctx *ctx);
 #define FA_KERNEL_INT16X2 2
 int fa_ctx_set_kernel(fa_ctx *ctx, int kernel);
 
+/* Graph mode (no reference counterpart): with it on, fa_ext_batch_policy and
+ * fa_ext_batch_learned run their device work -- band features and prediction, every
+ * extension round, band check and retry -- as one CUDA graph: recorded at the first call
+ * of a shape (job count, longest query, widest band, policy, scoring, model constants,
+ * buffer addresses) and replayed by later calls of the same shape, with no host round
+ * trip between rounds.  Results are identical either way.  The host-side copies stay
+ * outside the graph.  Turning it off releases the recorded graph. */
+int fa_ctx_set_graph(fa_ctx *ctx, int enable);
+
 /* Kernel timing of device-resident calls (no reference counterpart): with timing on,
  * fa_ext_batch_device brackets its extension kernels with CUDA events on the call's
  * stream; fa_ctx_last_timing waits for them and returns their device time and the
