@@ -87,6 +87,10 @@ struct fa_ctx {
     // learned rounds run their band groups on forked streams: fork on `stream`, join back
     cudaStream_t aux[2] = {nullptr, nullptr};
     cudaEvent_t fork_ev = nullptr, join_ev[2] = {nullptr, nullptr};
+    // pipelined host batches: slice uploads on their own stream, one event per slice
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t slice_ev[8] = {};
+    DevBuf chunk_scratch;
     // graph mode: the rounds of a call recorded once as a CUDA graph and replayed while the
     // call's shape (key) stays the same
     bool graph = false;
@@ -498,6 +502,75 @@ int run_ext_graph(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t
     return finish_ext(c, pol, n, s, stats, h_wfinal, c->glaunches, 0, true);
 }
 
+// Single-band host batch with the uploads pipelined under the kernels: the job records go
+// first, the GPU validates them and orders them by (upload slice, query length) while the
+// query and target buffers stream up in kSlices byte slices on a copy stream, and the
+// jobs of each slice start as soon as that slice has arrived.  Same results, statistics
+// and errors as the serial path (a rejected batch reports the first bad job through the
+// host-side checks); with pageable host buffers the copies simply do not overlap.
+constexpr int kSlices = 8;
+constexpr uint32_t kPipeMinJobs = 32768;
+
+int ext_batch_pipelined(fa_ctx *c, const ExtParams &kp, const fa_job *jobs, uint32_t n, const uint8_t *qseq,
+                        uint64_t qseq_len, const uint8_t *tseq, uint64_t tseq_len, fa_ext_result *out,
+                        fa_ext_stats *stats) {
+    if (int rc = ensure_ext_buffers(c, n, qseq_len, tseq_len)) return rc;
+    FA_CUDA(c->chunk_scratch.ensure(chunk_scratch_bytes(kSlices)));
+    if (!c->copy_stream) {
+        FA_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+        for (auto &e : c->slice_ev) FA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    cudaStream_t s = c->stream, cs = c->copy_stream;
+    const uint64_t qs = std::max<uint64_t>(1, (qseq_len + kSlices - 1) / kSlices);
+    const uint64_t ts = std::max<uint64_t>(1, (tseq_len + kSlices - 1) / kSlices);
+    Misc m = misc_of(c);
+    uint32_t *scratch = c->chunk_scratch.as<uint32_t>();
+    const size_t nbins = (size_t)kSlices * (FA_MAX_QLEN + 1);
+    uint32_t *info = scratch + 3 * nbins;
+    FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
+    FA_CUDA(cudaMemcpyAsync(c->jobs.p, jobs, sizeof(fa_job) * (size_t)n, cudaMemcpyHostToDevice, s));
+    // the sequence slices stream up meanwhile
+    for (int k = 0; k < kSlices; ++k) {
+        const uint64_t q0 = std::min(qseq_len, k * qs), q1 = std::min(qseq_len, (k + 1) * qs);
+        const uint64_t t0 = std::min(tseq_len, k * ts), t1 = std::min(tseq_len, (k + 1) * ts);
+        if (q1 > q0) FA_CUDA(cudaMemcpyAsync(c->qseq.as<uint8_t>() + q0, qseq + q0, q1 - q0, cudaMemcpyHostToDevice, cs));
+        if (t1 > t0) FA_CUDA(cudaMemcpyAsync(c->tseq.as<uint8_t>() + t0, tseq + t0, t1 - t0, cudaMemcpyHostToDevice, cs));
+        FA_CUDA(cudaEventRecord(c->slice_ev[k], cs));
+    }
+    FA_CUDA(launch_chunk_prep(c->jobs.as<fa_job>(), n, qseq_len, tseq_len, qs, ts, kSlices, kp.max_score,
+                              packed_qcap_limit(c->smem_optin), scratch, s));
+    uint32_t h_info[4 + kSlices + 1];
+    FA_CUDA(cudaMemcpyAsync(h_info, info, sizeof(h_info), cudaMemcpyDeviceToHost, s));
+    FA_CUDA(cudaStreamSynchronize(s));
+    if (h_info[0]) {
+        FA_CUDA(cudaStreamSynchronize(cs));   // the caller's buffers stay in use until then
+        const uint32_t bad = h_info[1] < n ? h_info[1] : 0;
+        int mq = 0;
+        const int rc = check_jobs(jobs + bad, 1, qseq_len, tseq_len, kp, packed_qcap_limit(c->smem_optin), &mq);
+        if (rc) return fail(rc, "job %u: %s", bad, g_err.c_str() + (g_err.compare(0, 7, "job 0: ") == 0 ? 7 : 0));
+        return fail(FA_ERR_ARG, "job %u is invalid", bad);
+    }
+    const int max_q = (int)h_info[2];
+    FA_CUDA(launch_chunk_scatter(c->jobs.as<fa_job>(), n, qs, ts, kSlices, scratch, c->order.as<uint32_t>(), s));
+    uint32_t launches = 2;
+    FA_CUDA(cudaEventRecord(c->ev0, s));
+    for (int k = 0; k < kSlices; ++k) {
+        const uint32_t cnt = h_info[4 + k + 1] - h_info[4 + k];
+        FA_CUDA(cudaStreamWaitEvent(s, c->slice_ev[k], 0));
+        if (cnt == 0) continue;
+        FA_CUDA(launch_ext_packed(c->jobs.as<fa_job>(), c->order.as<uint32_t>() + h_info[4 + k], cnt, nullptr,
+                                  nullptr, c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(), kp, max_q, 0, nullptr,
+                                  c->out.as<fa_ext_result>(), nullptr, false, c->cells_job.as<uint32_t>(), m.cells,
+                                  m.status, s));
+        ++launches;
+    }
+    FA_CUDA(cudaEventRecord(c->ev1, s));
+    FA_CUDA(cudaMemcpyAsync(out, c->out.p, sizeof(fa_ext_result) * (size_t)n, cudaMemcpyDeviceToHost, s));
+    if (int rc = finish_ext(c, nullptr, n, s, stats, nullptr, launches, 0, false)) return rc;
+    FA_CUDA(cudaStreamSynchronize(s));
+    return FA_OK;
+}
+
 int max_band_of(const fa_job *jobs, uint32_t n) {
     int w = 0;
     for (uint32_t i = 0; i < n; ++i) w = std::max(w, jobs[i].w);
@@ -550,6 +623,10 @@ void fa_ctx_destroy(fa_ctx *c) {
     }
     if (c->fork_ev) cudaEventDestroy(c->fork_ev);
     if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    for (auto &e : c->slice_ev)
+        if (e) cudaEventDestroy(e);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+    c->chunk_scratch.release();
     if (c->kev0) cudaEventDestroy(c->kev0);
     if (c->kev1) cudaEventDestroy(c->kev1);
     if (c->ev0) cudaEventDestroy(c->ev0);
@@ -597,6 +674,15 @@ int fa_ext_batch_policy(fa_ctx *c, const fa_params *p, const fa_policy *pol, con
         return fail(FA_ERR_STATE, "learned policy needs w_first (or a loaded band model)");
     FA_CUDA(cudaSetDevice(c->device));
     const ExtParams kp = ext_params_of(p);
+    if ((!pol || pol->mode == FA_POLICY_SINGLE) && !c->graph && n >= kPipeMinJobs && c->kernel != FA_KERNEL_INT16X2) {
+        int rc = ext_batch_pipelined(c, kp, jobs, n, qseq, qseq_len, tseq, tseq_len, out, stats);
+        if (rc) return rc;
+        if (w_final)
+            for (uint32_t i = 0; i < n; ++i) w_final[i] = jobs[i].w;
+        if (stats)
+            stats->total_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        return FA_OK;
+    }
     int max_q = 0;
     if (int rc = check_jobs(jobs, n, qseq_len, tseq_len, kp, packed_qcap_limit(c->smem_optin), &max_q))
         return rc;

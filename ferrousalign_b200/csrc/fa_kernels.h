@@ -61,6 +61,15 @@ cudaError_t launch_mate_sw(bool byte_lanes, const fa_mate_job *d_jobs, const uin
                            unsigned long long *d_cells, uint32_t *d_status, cudaStream_t stream);
 
 // Device-side longest-first ordering by query length (order_kernel.cu).
+// Pipelined host batches: validation + (chunk, length) histogram + prefix, then scatter.
+// Scratch layout: hist | base | cursor (nchunks * (FA_MAX_QLEN+1) each) | info[4] =
+// {status bits, first bad job, longest query, 0} | bounds[nchunks+1].
+size_t chunk_scratch_bytes(int nchunks);
+cudaError_t launch_chunk_prep(const fa_job *d_jobs, uint32_t n, uint64_t qbytes, uint64_t tbytes, uint64_t qslice,
+                              uint64_t tslice, int nchunks, int max_score, int qcap_limit, uint32_t *d_scratch,
+                              cudaStream_t s);
+cudaError_t launch_chunk_scatter(const fa_job *d_jobs, uint32_t n, uint64_t qslice, uint64_t tslice, int nchunks,
+                                 uint32_t *d_scratch, uint32_t *d_order, cudaStream_t s);
 cudaError_t launch_qlen_hist(const fa_job *d_jobs, uint32_t n, uint32_t *d_hist, int sm_count, cudaStream_t s);
 cudaError_t launch_qlen_scatter(const fa_job *d_jobs, uint32_t n, uint32_t *d_cursor, uint32_t *d_order,
                                 cudaStream_t s);

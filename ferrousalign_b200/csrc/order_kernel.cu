@@ -109,3 +109,137 @@ cudaError_t launch_mate_split(const fa_mate_job *d_jobs, uint32_t n, uint32_t *d
 }
 
 }  // namespace fa
+
+namespace fa {
+
+// ------------------------------------------------------------- pipelined host batches
+// A host batch is uploaded in K byte slices of the query and target buffers; a job can
+// run once the slices holding its sequences have arrived, so jobs are grouped by that
+// slice ("chunk", the larger of the query's and the target's last slice) and, inside a
+// chunk, by decreasing query length.  Bin = chunk * (FA_MAX_QLEN + 1) + (FA_MAX_QLEN - qlen).
+// The prep kernel also validates every job against the buffer lengths and the kernel
+// limits (the same rules as the host-side checks), keeping the first bad job's index,
+// and reduces the longest query.  info = {status, first bad job, longest query}.
+
+constexpr int kChunkBins = FA_MAX_QLEN + 1;
+
+__global__ void chunk_prep_kernel(const fa_job *__restrict__ jobs, uint32_t n, uint64_t qbytes, uint64_t tbytes,
+                                  uint64_t qslice, uint64_t tslice, int nchunks, int max_score, int qcap_limit,
+                                  uint32_t *__restrict__ hist, uint32_t *__restrict__ info)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = i < n;
+    int bin = -1, qlen = 0;
+    if (live) {
+        const fa_job jb = jobs[i];
+        qlen = jb.qlen;
+        uint32_t st = 0;
+        if (jb.qlen <= 0 || jb.tlen < 0 || jb.h0 <= 0) st |= ST_ARG;
+        else if (jb.qlen > FA_MAX_QLEN || jb.tlen > FA_MAX_TLEN) st |= ST_CAPACITY;
+        else if (jb.q_off + (uint64_t)jb.qlen > qbytes || jb.t_off + (uint64_t)jb.tlen > tbytes) st |= ST_ARG;
+        else if ((int64_t)jb.h0 + (int64_t)max_score * jb.qlen > kPackedHMax || jb.qlen > qcap_limit)
+            st |= ST_CAPACITY;
+        if (st) {
+            atomicOr(&info[0], st);
+            atomicMin(&info[1], i);
+            qlen = 0;
+        } else {
+            const uint64_t cq = (jb.q_off + (uint64_t)jb.qlen - 1) / qslice;
+            const uint64_t ct = jb.tlen > 0 ? (jb.t_off + (uint64_t)jb.tlen - 1) / tslice : 0;
+            const uint64_t c = cq > ct ? cq : ct;
+            const int chunk = c < (uint64_t)nchunks ? (int)c : nchunks - 1;
+            bin = chunk * kChunkBins + (FA_MAX_QLEN - jb.qlen);
+        }
+    }
+    const int mq = __reduce_max_sync(0xffffffffu, qlen);
+    if ((threadIdx.x & 31) == 0 && mq > 0) atomicMax(&info[2], (uint32_t)mq);
+    const unsigned peers = __match_any_sync(0xffffffffu, bin);
+    if (bin >= 0 && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&hist[bin], (uint32_t)__popc(peers));
+}
+
+// Exclusive prefix over the bins (one block), and the chunk bounds: bounds[k] = first
+// order position of chunk k, bounds[nchunks] = the number of valid jobs.
+__global__ void __launch_bounds__(1024) chunk_scan_kernel(const uint32_t *__restrict__ hist, int nbins,
+                                                          uint32_t *__restrict__ base, int nchunks,
+                                                          uint32_t *__restrict__ bounds)
+{
+    __shared__ uint32_t part[1024];
+    const int per = (nbins + 1023) / 1024;
+    const int b0 = threadIdx.x * per;
+    uint32_t s = 0;
+    for (int b = b0; b < min(b0 + per, nbins); ++b) s += hist[b];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {      // inclusive Hillis-Steele scan
+        const uint32_t v = threadIdx.x >= off ? part[threadIdx.x - off] : 0u;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    uint32_t acc = threadIdx.x ? part[threadIdx.x - 1] : 0u;
+    for (int b = b0; b < min(b0 + per, nbins); ++b) {
+        base[b] = acc;
+        acc += hist[b];
+    }
+    __syncthreads();
+    if (threadIdx.x <= nchunks) {
+        const int b = threadIdx.x * kChunkBins;
+        bounds[threadIdx.x] = threadIdx.x == nchunks ? part[1023] : base[b];
+    }
+}
+
+__global__ void chunk_scatter_kernel(const fa_job *__restrict__ jobs, uint32_t n, uint64_t qslice, uint64_t tslice,
+                                     int nchunks, const uint32_t *__restrict__ base, uint32_t *__restrict__ cursor,
+                                     uint32_t *__restrict__ order)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    int bin = -1;
+    if (i < n) {
+        const fa_job jb = jobs[i];
+        const uint64_t cq = (jb.q_off + (uint64_t)jb.qlen - 1) / qslice;
+        const uint64_t ct = jb.tlen > 0 ? (jb.t_off + (uint64_t)jb.tlen - 1) / tslice : 0;
+        const uint64_t c = cq > ct ? cq : ct;
+        const int chunk = c < (uint64_t)nchunks ? (int)c : nchunks - 1;
+        bin = chunk * kChunkBins + (FA_MAX_QLEN - jb.qlen);
+    }
+    const unsigned peers = __match_any_sync(0xffffffffu, bin);
+    if (bin < 0) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    uint32_t pos = 0;
+    if (lane == leader) pos = atomicAdd(&cursor[bin], (uint32_t)__popc(peers));
+    pos = __shfl_sync(peers, pos, leader);
+    order[base[bin] + pos + __popc(peers & ((1u << lane) - 1u))] = i;
+}
+
+size_t chunk_scratch_bytes(int nchunks) { return sizeof(uint32_t) * (3 * (size_t)nchunks * kChunkBins + 64); }
+
+// scratch layout: hist[nbins] | base[nbins] | cursor[nbins] | info[4] | bounds[nchunks+1]
+cudaError_t launch_chunk_prep(const fa_job *d_jobs, uint32_t n, uint64_t qbytes, uint64_t tbytes, uint64_t qslice,
+                              uint64_t tslice, int nchunks, int max_score, int qcap_limit, uint32_t *d_scratch,
+                              cudaStream_t s)
+{
+    const size_t nbins = (size_t)nchunks * kChunkBins;
+    uint32_t *hist = d_scratch, *cursor = d_scratch + 2 * nbins, *info = d_scratch + 3 * nbins;
+    cudaError_t e = cudaMemsetAsync(hist, 0, sizeof(uint32_t) * nbins, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(cursor, 0, sizeof(uint32_t) * nbins, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(info, 0, sizeof(uint32_t) * 4, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(info + 1, 0xFF, sizeof(uint32_t), s);   // first bad job: none
+    if (e != cudaSuccess || n == 0) return e;
+    chunk_prep_kernel<<<(n + 255) / 256, 256, 0, s>>>(d_jobs, n, qbytes, tbytes, qslice, tslice, nchunks, max_score,
+                                                      qcap_limit, hist, info);
+    chunk_scan_kernel<<<1, 1024, 0, s>>>(hist, (int)nbins, d_scratch + nbins, nchunks, info + 4);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_chunk_scatter(const fa_job *d_jobs, uint32_t n, uint64_t qslice, uint64_t tslice, int nchunks,
+                                 uint32_t *d_scratch, uint32_t *d_order, cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    const size_t nbins = (size_t)nchunks * kChunkBins;
+    chunk_scatter_kernel<<<(n + 255) / 256, 256, 0, s>>>(d_jobs, n, qslice, tslice, nchunks, d_scratch + nbins,
+                                                         d_scratch + 2 * nbins, d_order);
+    return cudaGetLastError();
+}
+
+}  // namespace fa

@@ -193,3 +193,28 @@ def test_errors_are_reported(ctx):
     jobs, q, t = one_job_arrays([0, 1, 2, 3], [0, 1, 2, 3], 10, 50)
     out, _, _ = fa.extend_batch(p, jobs, q, t, ctx=ctx)
     assert out[0]["qle"] == 4 and out[0]["tle"] == 4
+
+
+def test_large_batch_errors_and_pinned_pipeline(ctx):
+    """Batches large enough for the sliced-upload path: the first bad job is reported with
+    the same code and message as on the serial path, nothing runs, the context stays
+    usable, and pinned host buffers give the serial path's results."""
+    import torch
+    p = fa.BandedPairWiseSW().to_struct()
+    b = synth.workload_ext_1m(60_000, seed=31)
+    for field, value, code in (("q_off", 10 ** 12, N.FA_ERR_ARG), ("h0", 0, N.FA_ERR_ARG),
+                               ("qlen", 5000, N.FA_ERR_CAPACITY)):
+        jobs = b.jobs.copy()
+        jobs[40_001][field] = value
+        jobs[51_234][field] = value
+        with pytest.raises(N.NativeError) as e:
+            fa.extend_batch(p, jobs, b.qseq, b.tseq, ctx=ctx)
+        assert e.value.code == code and "job 40001" in str(e.value)
+    ref, tr = O.ext_batch(p, b.jobs, b.qseq, b.tseq)
+    pin_q = torch.from_numpy(b.qseq).pin_memory().numpy()
+    pin_t = torch.from_numpy(b.tseq).pin_memory().numpy()
+    pin_j = torch.from_numpy(b.jobs.view(np.uint8)).pin_memory().numpy().view(N.JOB_DT)
+    for _ in range(2):
+        out, st, _ = fa.extend_batch(p, pin_j, pin_q, pin_t, ctx=ctx)
+        assert np.array_equal(out, ref), diff_report(out, ref)
+        assert st["cells"] == tr["cells"].sum()
