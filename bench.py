@@ -179,6 +179,68 @@ def bench_learned(args, ctx, b, p):
             "identical_frac": float(np.mean(plain == learned))}
 
 
+def bench_mixed(args, b, p):
+    """Mixed batch: 500,000 mate-rescue pairs and the 1,000,000 seed extensions of one
+    batch, submitted together through the host ABI (two contexts on two host threads, so
+    the mate SW and the extensions run concurrently on the GPU), inputs in pinned host
+    memory, copies included.  Plain (bwa-mem2 policy) and learned-band forms; latency
+    percentiles over the batches."""
+    import threading
+    import torch
+    import ferrousalign_b200 as fa
+    from ferrousalign_b200 import _native as N
+    from ferrousalign_b200 import band_model as B
+    from ferrousalign_b200 import synth
+    m = synth.workload_mate(MATE_JOBS)
+    mp = fa.make_mate_params()
+
+    def pin(a, dt=None):
+        t = torch.from_numpy(np.ascontiguousarray(a).view(np.uint8)).pin_memory().numpy()
+        return t.view(dt if dt is not None else a.dtype)
+
+    mj, mq, mt = pin(m.jobs, N.MATE_JOB_DT), pin(m.qseq), pin(m.tseq)
+    ej, eq, et = pin(b.jobs, N.JOB_DT), pin(b.qseq), pin(b.tseq)
+    hints = B.hints_from_info(b.info)
+    model = B.BandModel.load()
+    bwa = fa.make_policy(N.FA_POLICY_BWA, 2)
+    ctx_e, ctx_m = N.Context(0), N.Context(0)
+    res = {"workload": f"{MATE_JOBS} mate-rescue SW jobs (2x151 bp pairs, 551 bp windows) + {len(b.jobs)} "
+                       "151-bp seed extensions per batch, host ABI, pinned buffers, two concurrent contexts"}
+    outs = {}
+    try:
+        for form in ("plain", "learned"):
+            lat = []
+            for it in range(args.warmup + max(5, args.steps // 3)):
+                box = {}
+
+                def mate():
+                    box["mate"] = fa.mate_sw_batch(mp, mj, mq, mt, ctx=ctx_m)[0]
+
+                t0 = time.perf_counter()
+                th = threading.Thread(target=mate)
+                th.start()
+                if form == "plain":
+                    ext, _, _ = fa.extend_batch(p, ej, eq, et, policy=bwa, ctx=ctx_e)
+                else:
+                    ext, _, _, _ = B.extend_batch_learned(p, ej, eq, et, model, hints=hints, ctx=ctx_e)
+                th.join()
+                dt = (time.perf_counter() - t0) * 1e3
+                if it >= args.warmup:
+                    lat.append(dt)
+            outs[form] = (ext, box["mate"])
+            lat = np.array(lat)
+            res[form] = {"batches": len(lat), "p50_ms": float(np.percentile(lat, 50)),
+                         "p95_ms": float(np.percentile(lat, 95)), "p99_ms": float(np.percentile(lat, 99)),
+                         "max_ms": float(lat.max()),
+                         "alignments_per_s": (MATE_JOBS + len(b.jobs)) / (float(np.median(lat)) * 1e-3)}
+        res["identical_outputs"] = bool(np.array_equal(outs["plain"][0], outs["learned"][0]) and
+                                        np.array_equal(outs["plain"][1], outs["learned"][1]))
+    finally:
+        ctx_e.close()
+        ctx_m.close()
+    return res
+
+
 def bench_mate(args, ctx, lib, dev, stream, flush, skip_cpu=False):
     """Mate-rescue local SW on 500,000 2x151 bp pairs (insert ~ N(400, 50), window 551 bp),
     device-resident, same step/warm-up counts as the extension line."""
@@ -288,6 +350,7 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true", help="omit the CPU baseline leg")
     ap.add_argument("--skip-mate", action="store_true", help="omit the mate-rescue section")
     ap.add_argument("--skip-learned", action="store_true", help="omit the learned-band section")
+    ap.add_argument("--skip-mixed", action="store_true", help="omit the mixed mate + extension batch section")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -450,6 +513,8 @@ def main():
         line["learned_band"] = bench_learned(args, ctx, b, p)
     if not args.skip_mate:
         line["mate_rescue"] = bench_mate(args, ctx, lib, dev, stream, flush, skip_cpu=args.skip_cpu)
+    if not args.skip_mate and not args.skip_learned and not args.skip_mixed:
+        line["mixed_batch"] = bench_mixed(args, b, p)
     if not args.skip_cpu:
         ref2, tr2, dt, threads = cpu_oracle_rate(b, p, min(CPU_SAMPLE, n))
         line["cpu_baseline"] = {"value": min(CPU_SAMPLE, n) / dt, "unit": "alignments/s", "cores": threads,
