@@ -47,7 +47,7 @@ __device__ fa_kswr sw_pass(SeqView Q, int qlen, SeqView Tg, int tlen, uint32_t x
                            int bcap, unsigned long long &cells, uint32_t &status)
 {
     constexpr bool U8 = (P == 16);
-    constexpr int NQW = SMAX / 8;
+    constexpr int NQW = (SMAX + 7) / 8;
     const int slen = (qlen + P - 1) / P;
     const int off = SMAX - slen;   // segment j lives at register index j + off
     const uint32_t minsc = (xtra & FA_KSW_XSUBO) ? (xtra & 0xffffu) : 0x10000u;
@@ -293,14 +293,23 @@ cudaError_t launch_mate_sw(bool byte_lanes, const fa_mate_job *d_jobs, const uin
 {
     if (n == 0) return cudaSuccess;
     const int bcap = (max_tlen + 1) / 2 + 2;   // consecutive list rows differ by >= 2
+    // the smallest register depth (segments per lane) that holds the longest query: slots
+    // beyond a job's segment count are predicated off but still issue, so the depth tracks
+    // the batch's query length (151-bp mates: 10 u8 segments, 19 i16 segments)
+#define FA_MATE(PP, SS) launch_mate_t<PP, SS>(d_jobs, d_order, n, d_qseq, d_tseq, p, bcap, d_out, d_cells, d_status, \
+                                              stream)
     if (byte_lanes) {
-        if (max_qlen <= 16 * 16)
-            return launch_mate_t<16, 16>(d_jobs, d_order, n, d_qseq, d_tseq, p, bcap, d_out, d_cells, d_status, stream);
-        return launch_mate_t<16, 32>(d_jobs, d_order, n, d_qseq, d_tseq, p, bcap, d_out, d_cells, d_status, stream);
+        if (max_qlen <= 16 * 10) return FA_MATE(16, 10);
+        if (max_qlen <= 16 * 12) return FA_MATE(16, 12);
+        if (max_qlen <= 16 * 16) return FA_MATE(16, 16);
+        if (max_qlen <= 16 * 24) return FA_MATE(16, 24);
+        return FA_MATE(16, 32);
     }
-    if (max_qlen <= 8 * 16)
-        return launch_mate_t<8, 16>(d_jobs, d_order, n, d_qseq, d_tseq, p, bcap, d_out, d_cells, d_status, stream);
-    return launch_mate_t<8, 32>(d_jobs, d_order, n, d_qseq, d_tseq, p, bcap, d_out, d_cells, d_status, stream);
+    if (max_qlen <= 8 * 16) return FA_MATE(8, 16);
+    if (max_qlen <= 8 * 20) return FA_MATE(8, 20);
+    if (max_qlen <= 8 * 24) return FA_MATE(8, 24);
+    return FA_MATE(8, 32);
+#undef FA_MATE
 }
 
 }  // namespace fa
