@@ -438,6 +438,7 @@ def main():
     ref_out, ref_tr = O.ext_batch(p, sub, b.qseq, b.tseq)
     exact = bool(np.array_equal(out[chk], ref_out))
 
+    tune_dev = ctx.kernel_choice()   # autotuned kernel of the device-resident runs above
     # per-batch stats (cells, kernel time) from the host API run, also the e2e timing
     pin_jobs = torch.from_numpy(b.jobs.view(np.uint8)).pin_memory().numpy().view(N.JOB_DT)
     pin_q = torch.from_numpy(b.qseq).pin_memory().numpy()
@@ -508,6 +509,7 @@ def main():
                 "h2d_bytes_per_step": bytes_in + n * 4, "d2h_bytes_per_step": bytes_out},
         "gpu_launches": launches,
         "clocks": clocks,
+        "autotune": tune_dev,
     }
     if not args.skip_learned:
         line["learned_band"] = bench_learned(args, ctx, b, p)

@@ -64,6 +64,9 @@ SIGNATURES = {
     "fa_ctx_set_timing": (C.c_int, [_P, C.c_int]),
     "fa_ctx_set_kernel": (C.c_int, [_P, C.c_int]),
     "fa_ctx_set_graph": (C.c_int, [_P, C.c_int]),
+    "fa_ctx_set_threads": (C.c_int, [_P, C.c_int]),
+    "fa_ctx_kernel_choice": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int, _P, _P, _P,
+                                       C.POINTER(C.c_int)]),
     "fa_ctx_last_timing": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_int)]),
     "fa_ext_batch_device_noalloc": (C.c_int, [_P, _P, C.c_uint32, _P, _P, _P, _P]),
     "fa_mate_sw_batch_device": (C.c_int, [_P, _P, _P, C.c_uint32, _P, _P, _P, _P]),
@@ -145,6 +148,21 @@ class Context:
 
     def set_kernel(self, kernel: int) -> None:
         check(load().fa_ctx_set_kernel(self.handle, kernel))
+
+    def set_threads(self, threads_per_block: int) -> None:
+        check(load().fa_ctx_set_threads(self.handle, threads_per_block))
+
+    def kernel_choice(self) -> dict:
+        """Kernel and threads per block of the last call, and the last autotuning table."""
+        k, t, nc = C.c_int(), C.c_int(), C.c_int()
+        ck = (C.c_int * 8)()
+        ct = (C.c_int * 8)()
+        cm = (C.c_float * 8)()
+        check(load().fa_ctx_kernel_choice(self.handle, C.byref(k), C.byref(t), 8, ck, ct, cm, C.byref(nc)))
+        names = {FA_KERNEL_INT32: "int32", FA_KERNEL_INT16X2: "int16x2"}
+        return {"kernel": names.get(k.value, str(k.value)), "threads_per_block": t.value,
+                "candidates": [{"kernel": names.get(ck[i], str(ck[i])), "threads_per_block": ct[i],
+                                "sample_ms": float(cm[i])} for i in range(min(nc.value, 8))]}
 
     def set_graph(self, enable: bool) -> None:
         """Run policy / learned batches as one recorded CUDA graph per batch shape."""

@@ -94,8 +94,8 @@ struct ExitBound {
 // times the resident warps.  Columns entering the ring get their query code explicitly,
 // and a column the rows grow into after a trim gets the value the full array would
 // hold there: 0 once written (trimmed cells are zero), its first-row value if never.
-template <bool CERT, int RING>
-__global__ void __launch_bounds__(kExtThreads)
+template <bool CERT, int RING, int TPB>
+__global__ void __launch_bounds__(TPB)
 ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ order,
                   uint32_t n, const uint32_t *__restrict__ first_dev, const uint32_t *__restrict__ n_dev,
                   const uint8_t *__restrict__ qseq, const uint8_t *__restrict__ tseq, const ExtParams p, int qcap,
@@ -104,7 +104,7 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
                   unsigned long long *__restrict__ cells_out, uint32_t *__restrict__ status)
 {
     extern __shared__ uint32_t smem[];
-    constexpr int T = kExtThreads;
+    constexpr int T = TPB;   // threads (= jobs) per block; also the stride of the column words
     const uint32_t first = first_dev ? *first_dev : 0u;   // device-side sub-range of the order
     const uint32_t gi = first + blockIdx.x * T + threadIdx.x;
     uint32_t cells = 0;
@@ -362,23 +362,24 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
     }
 }
 
-size_t ext_packed_smem_bytes(int qcap, int ring) {
+size_t ext_packed_smem_bytes(int qcap, int ring, int tpb) {
     const size_t words = ring > 0 ? (size_t)ring + (size_t)(qcap + 7) / 8 : (size_t)qcap + 1;
-    return words * kExtThreads * sizeof(uint32_t);
+    return words * (size_t)tpb * sizeof(uint32_t);
 }
 
 namespace {
-template <bool CERT, int RING>
-cudaError_t launch_variant(uint32_t blocks, size_t smem, cudaStream_t stream, const fa_job *d_jobs,
-                           const uint32_t *d_order, uint32_t n, const uint32_t *d_first, const uint32_t *d_n,
-                           const uint8_t *d_qseq, const uint8_t *d_tseq, const ExtParams &p, int qcap,
-                           const int32_t *d_w_try, fa_ext_result *d_out, uint8_t *d_clamped, uint32_t *d_cells_job,
+template <bool CERT, int RING, int TPB>
+cudaError_t launch_variant(size_t smem, cudaStream_t stream, const fa_job *d_jobs, const uint32_t *d_order,
+                           uint32_t n, const uint32_t *d_first, const uint32_t *d_n, const uint8_t *d_qseq,
+                           const uint8_t *d_tseq, const ExtParams &p, int qcap, const int32_t *d_w_try,
+                           fa_ext_result *d_out, uint8_t *d_clamped, uint32_t *d_cells_job,
                            unsigned long long *d_cells, uint32_t *d_status)
 {
-    cudaError_t err = cudaFuncSetAttribute(ext_packed_kernel<CERT, RING>,
+    cudaError_t err = cudaFuncSetAttribute(ext_packed_kernel<CERT, RING, TPB>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return err;
-    ext_packed_kernel<CERT, RING><<<blocks, kExtThreads, smem, stream>>>(
+    const uint32_t blocks = (n + TPB - 1) / TPB;
+    ext_packed_kernel<CERT, RING, TPB><<<blocks, TPB, smem, stream>>>(
         d_jobs, d_order, n, d_first, d_n, d_qseq, d_tseq, p, qcap, d_w_try, d_out, d_clamped, d_cells_job,
         d_cells, d_status);
     return cudaGetLastError();
@@ -390,20 +391,31 @@ cudaError_t launch_ext_packed(const fa_job *d_jobs, const uint32_t *d_order, uin
                               const uint8_t *d_tseq, const ExtParams &p, int qcap, int ring,
                               const int32_t *d_w_try, fa_ext_result *d_out, uint8_t *d_clamped, bool cert,
                               uint32_t *d_cells_job, unsigned long long *d_cells, uint32_t *d_status,
-                              cudaStream_t stream)
+                              cudaStream_t stream, int tpb)
 {
     if (n == 0) return cudaSuccess;
     if (ring != 0 && ring != 32 && ring != 64) return cudaErrorInvalidValue;
-    const size_t smem = ext_packed_smem_bytes(qcap, ring);
-    const uint32_t blocks = (n + kExtThreads - 1) / kExtThreads;
-    // the certificate variant only where a judge reads it (it adds work to every row)
+    // the certificate variant only where a judge reads it (it adds work to every row);
+    // block sizes other than the default only for the plain full-row kernel
     const bool c = cert && d_clamped;
-#define FA_EXT_LAUNCH(CV, RV) launch_variant<CV, RV>(blocks, smem, stream, d_jobs, d_order, n, d_first, d_n, d_qseq, \
-                                                     d_tseq, p, qcap, d_w_try, d_out, d_clamped, d_cells_job,        \
-                                                     d_cells, d_status)
-    if (ring == 32) return c ? FA_EXT_LAUNCH(true, 32) : FA_EXT_LAUNCH(false, 32);
-    if (ring == 64) return c ? FA_EXT_LAUNCH(true, 64) : FA_EXT_LAUNCH(false, 64);
-    return c ? FA_EXT_LAUNCH(true, 0) : FA_EXT_LAUNCH(false, 0);
+    if (c || ring != 0 || (tpb != 64 && tpb != 256)) tpb = kExtThreads;
+    if (tpb == 256) {   // a block of 256 jobs holds twice the shared memory: fall back when it does not fit
+        int dev = 0, optin = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess &&
+            ext_packed_smem_bytes(qcap, ring, 256) > (size_t)optin)
+            tpb = kExtThreads;
+    }
+    const size_t smem = ext_packed_smem_bytes(qcap, ring, tpb);
+#define FA_EXT_LAUNCH(CV, RV, TV) launch_variant<CV, RV, TV>(smem, stream, d_jobs, d_order, n, d_first, d_n, d_qseq, \
+                                                             d_tseq, p, qcap, d_w_try, d_out, d_clamped, d_cells_job, \
+                                                             d_cells, d_status)
+    if (ring == 32) return c ? FA_EXT_LAUNCH(true, 32, kExtThreads) : FA_EXT_LAUNCH(false, 32, kExtThreads);
+    if (ring == 64) return c ? FA_EXT_LAUNCH(true, 64, kExtThreads) : FA_EXT_LAUNCH(false, 64, kExtThreads);
+    if (c) return FA_EXT_LAUNCH(true, 0, kExtThreads);
+    if (tpb == 64) return FA_EXT_LAUNCH(false, 0, 64);
+    if (tpb == 256) return FA_EXT_LAUNCH(false, 0, 256);
+    return FA_EXT_LAUNCH(false, 0, kExtThreads);
 #undef FA_EXT_LAUNCH
 }
 

@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <chrono>
 #include <functional>
+#include <map>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -91,6 +92,12 @@ struct fa_ctx {
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t slice_ev[8] = {};
     DevBuf chunk_scratch;
+    // kernel choice: fixed, or (FA_KERNEL_AUTO) tuned per (query capacity class, band)
+    struct Choice { int kernel; int tpb; };
+    int threads = kExtThreads;   // threads per block of the int32 kernel when fixed
+    std::map<std::pair<int, int>, Choice> tuned;
+    Choice last_choice{FA_KERNEL_INT32, kExtThreads};
+    std::vector<std::pair<Choice, float>> last_tuning;
     // graph mode: the rounds of a call recorded once as a CUDA graph and replayed while the
     // call's shape (key) stays the same
     bool graph = false;
@@ -134,15 +141,71 @@ int ensure_aux_streams(fa_ctx *c) {
 // half the warps), hence the default.
 // With `cert` the int32 kernel also evaluates the exit-bound certificate (flag bit 1),
 // which only the int32 kernel implements.
-cudaError_t launch_ext(int kernel, const fa_job *d_jobs, const uint32_t *d_order, uint32_t n,
+using Choice = fa_ctx::Choice;
+
+cudaError_t launch_ext(Choice kc, const fa_job *d_jobs, const uint32_t *d_order, uint32_t n,
                        const uint32_t *d_n, const uint8_t *d_q, const uint8_t *d_t, const ExtParams &kp, int qcap,
                        const int32_t *d_w_try, fa_ext_result *d_out, uint8_t *d_clamped, bool cert,
                        uint32_t *d_cells_job, unsigned long long *d_cells, uint32_t *d_status, cudaStream_t s) {
-    if (kernel == FA_KERNEL_INT16X2 && ext_pair_eligible(kp) && !cert)
+    if (kc.kernel == FA_KERNEL_INT16X2 && ext_pair_eligible(kp) && !cert)
         return launch_ext_pair(d_jobs, d_order, n, d_n, d_q, d_t, kp, qcap, d_w_try, d_out, d_clamped,
                                d_cells_job, d_cells, d_status, s);
     return launch_ext_packed(d_jobs, d_order, n, nullptr, d_n, d_q, d_t, kp, qcap, 0, d_w_try, d_out, d_clamped,
-                             cert, d_cells_job, d_cells, d_status, s);
+                             cert, d_cells_job, d_cells, d_status, s, kc.tpb);
+}
+
+// The kernel a call runs.  A fixed setting is used as is.  FA_KERNEL_AUTO is an
+// autotuner: the first time a (query capacity class of 32 columns, configured band) pair
+// is seen, every exact candidate -- the int32 one-job-per-thread kernel with 64, 128 or
+// 256 threads per block, and the int16x2 two-jobs-per-thread kernel where the scoring
+// allows it -- runs twice on the first (longest) jobs of the call's order, and the
+// fastest is kept for that pair.  All candidates give identical results.
+Choice resolve_choice(fa_ctx *c, const ExtParams &kp, const fa_job *d_jobs, const uint32_t *d_order, uint32_t n,
+                      const uint8_t *d_q, const uint8_t *d_t, int qcap, int band, fa_ext_result *d_out,
+                      uint32_t *d_status, cudaStream_t s, int *rc) {
+    *rc = FA_OK;
+    if (c->kernel == FA_KERNEL_INT16X2) return c->last_choice = Choice{FA_KERNEL_INT16X2, kPairThreads};
+    if (c->kernel == FA_KERNEL_INT32) return c->last_choice = Choice{FA_KERNEL_INT32, c->threads};
+    const std::pair<int, int> key{(qcap + 31) / 32, band};
+    auto it = c->tuned.find(key);
+    if (it != c->tuned.end()) return c->last_choice = it->second;
+    std::vector<Choice> cands{{FA_KERNEL_INT32, 64}, {FA_KERNEL_INT32, kExtThreads}, {FA_KERNEL_INT32, 256}};
+    if (ext_pair_eligible(kp)) cands.push_back({FA_KERNEL_INT16X2, kPairThreads});
+    const uint32_t ns = std::min<uint32_t>(n, 131072);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    Choice best{FA_KERNEL_INT32, kExtThreads};
+    float best_ms = 1e30f;
+    c->last_tuning.clear();
+    auto bail = [&](cudaError_t e) {
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        *rc = fail(FA_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
+        return best;
+    };
+    cudaError_t e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    if (e != cudaSuccess) return bail(e);
+    for (const Choice &kc : cands) {
+        if (kc.kernel == FA_KERNEL_INT32 && ext_packed_smem_bytes(qcap, 0, kc.tpb) > c->smem_optin) continue;
+        if (kc.kernel == FA_KERNEL_INT16X2 && ext_pair_smem_bytes(qcap) > c->smem_optin) continue;
+        for (int rep = 0; rep < 3; ++rep) {           // one warm-up, two timed
+            if (rep == 1 && (e = cudaEventRecord(e0, s)) != cudaSuccess) return bail(e);
+            e = launch_ext(kc, d_jobs, d_order, ns, nullptr, d_q, d_t, kp, qcap, nullptr, d_out, nullptr, false,
+                           nullptr, nullptr, d_status, s);
+            if (e != cudaSuccess) return bail(e);
+        }
+        if ((e = cudaEventRecord(e1, s)) != cudaSuccess || (e = cudaEventSynchronize(e1)) != cudaSuccess)
+            return bail(e);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms *= 0.5f;
+        c->last_tuning.push_back({kc, ms});
+        if (ms < best_ms) { best_ms = ms; best = kc; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->tuned[key] = best;
+    return c->last_choice = best;
 }
 
 // One learned round over a band-partitioned list: configured-band and wide narrow jobs
@@ -302,7 +365,8 @@ int max_rounds_of(const fa_policy *pol, int max_w) {
 int enqueue_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n,
                 const std::vector<std::pair<uint32_t, int>> &segs, int qcap_all, int max_w, const fa_job *d_jobs,
                 const uint32_t *d_order, const uint8_t *d_q, const uint8_t *d_t, const int32_t *d_wfirst,
-                fa_ext_result *d_out, cudaStream_t s, bool capture, uint32_t *launches, uint32_t *retries) {
+                fa_ext_result *d_out, cudaStream_t s, bool capture, uint32_t *launches, uint32_t *retries,
+                Choice kc) {
     Misc m = misc_of(c);
     FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
     const int mode = pol ? pol->mode : FA_POLICY_SINGLE;
@@ -311,7 +375,7 @@ int enqueue_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n
     if (mode == FA_POLICY_SINGLE) {
         uint32_t b = 0;
         for (auto &sg : segs0) {
-            FA_CUDA(launch_ext(c->kernel, d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp, sg.second,
+            FA_CUDA(launch_ext(kc, d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp, sg.second,
                                nullptr, d_out, nullptr, false, c->cells_job.as<uint32_t>(), m.cells, m.status, s));
             ++*launches;
             b = sg.first;
@@ -339,7 +403,7 @@ int enqueue_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n
         if (r == 0 && !learned) {
             uint32_t b = 0;
             for (auto &sg : segs0) {
-                FA_CUDA(launch_ext(c->kernel, d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp, sg.second,
+                FA_CUDA(launch_ext(kc, d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp, sg.second,
                                    st.w_cur, d_out, d_flags, cert_r, c->cells_job.as<uint32_t>(), m.cells, m.status,
                                    s));
                 ++*launches;
@@ -351,7 +415,7 @@ int enqueue_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n
             FA_CUDA(launch_band_partition(d_jobs, list, cnt, n, st.w_cur, c->part_n.as<uint32_t>(),
                                           m.bucket_hist, m.bucket_cursor, m.group_bounds, s));
             if (c->kernel == FA_KERNEL_INT16X2) {
-                FA_CUDA(launch_ext(c->kernel, d_jobs, c->part_n.as<uint32_t>(), n, cnt, d_q, d_t, kp, qcap_all,
+                FA_CUDA(launch_ext(kc, d_jobs, c->part_n.as<uint32_t>(), n, cnt, d_q, d_t, kp, qcap_all,
                                    st.w_cur, d_out, d_flags, cert_r, c->cells_job.as<uint32_t>(), m.cells,
                                    m.status, s));
                 *launches += 3;
@@ -362,7 +426,7 @@ int enqueue_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n
                 *launches += 5;
             }
         } else {
-            FA_CUDA(launch_ext(c->kernel, d_jobs, list, n, cnt, d_q, d_t, kp, qcap_all, st.w_cur, d_out,
+            FA_CUDA(launch_ext(kc, d_jobs, list, n, cnt, d_q, d_t, kp, qcap_all, st.w_cur, d_out,
                                d_flags, cert_r, c->cells_job.as<uint32_t>(), m.cells, m.status, s));
             ++*launches;
         }
@@ -430,15 +494,19 @@ int finish_ext(fa_ctx *c, const fa_policy *pol, uint32_t n, cudaStream_t s, fa_e
 // Runs the extension rounds on device data.  order/segs describe the first round;
 // retry rounds reuse the widest capacity class.
 int run_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n,
-            const std::vector<std::pair<uint32_t, int>> &segs, int qcap_all, const fa_job *d_jobs,
+            const std::vector<std::pair<uint32_t, int>> &segs, int qcap_all, int band, const fa_job *d_jobs,
             const uint32_t *d_order, const uint8_t *d_q, const uint8_t *d_t, const int32_t *d_wfirst,
             fa_ext_result *d_out, cudaStream_t s, fa_ext_stats *stats, int32_t *h_wfinal) {
     uint32_t launches = 0, retries = 0;
     if (pol && pol->mode != FA_POLICY_SINGLE)
         if (int rc = ensure_policy_buffers(c, n)) return rc;
+    int rc0 = FA_OK;
+    const Choice kc = resolve_choice(c, kp, d_jobs, d_order, n, d_q, d_t, qcap_all, band, d_out, misc_of(c).status, s,
+                                     &rc0);
+    if (rc0) return rc0;
     FA_CUDA(cudaEventRecord(c->ev0, s));
     if (int rc = enqueue_ext(c, kp, pol, n, segs, qcap_all, 0, d_jobs, d_order, d_q, d_t, d_wfirst, d_out, s, false,
-                             &launches, &retries))
+                             &launches, &retries, kc))
         return rc;
     FA_CUDA(cudaEventRecord(c->ev1, s));
     return finish_ext(c, pol, n, s, stats, h_wfinal, launches, retries, false);
@@ -469,7 +537,14 @@ int run_ext_graph(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t
     if (pol && pol->mode != FA_POLICY_SINGLE)
         if (int rc = ensure_policy_buffers(c, n)) return rc;
     if (int rc = ensure_aux_streams(c)) return rc;
-    std::vector<uint64_t> key = graph_key(c, kp, pol, n, qcap, max_w, extra);
+    int rc0 = FA_OK;
+    const Choice kc = resolve_choice(c, kp, c->jobs.as<fa_job>(), c->order.as<uint32_t>(), n, c->qseq.as<uint8_t>(),
+                                     c->tseq.as<uint8_t>(), qcap, max_w, c->out.as<fa_ext_result>(),
+                                     misc_of(c).status, s, &rc0);
+    if (rc0) return rc0;
+    std::vector<uint64_t> extra2 = extra;
+    extra2.push_back((uint64_t)kc.kernel << 32 | (uint32_t)kc.tpb);
+    std::vector<uint64_t> key = graph_key(c, kp, pol, n, qcap, max_w, extra2);
     if (!c->gexec || key != c->gkey) {
         if (c->gexec) {
             cudaGraphExecDestroy(c->gexec);
@@ -482,7 +557,7 @@ int run_ext_graph(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t
         if (!rc)
             rc = enqueue_ext(c, kp, pol, n, segs, qcap, max_w, c->jobs.as<fa_job>(), c->order.as<uint32_t>(),
                              c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(), d_wfirst, c->out.as<fa_ext_result>(), s,
-                             true, &launches, nullptr);
+                             true, &launches, nullptr, kc);
         cudaGraph_t g = nullptr;
         const cudaError_t ec = cudaStreamEndCapture(s, &g);
         if (rc || ec != cudaSuccess) {
@@ -500,6 +575,12 @@ int run_ext_graph(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t
     FA_CUDA(cudaGraphLaunch(c->gexec, s));
     FA_CUDA(cudaEventRecord(c->ev1, s));
     return finish_ext(c, pol, n, s, stats, h_wfinal, c->glaunches, 0, true);
+}
+
+int max_band_of(const fa_job *jobs, uint32_t n) {
+    int w = 0;
+    for (uint32_t i = 0; i < n; ++i) w = std::max(w, jobs[i].w);
+    return w;
 }
 
 // Single-band host batch with the uploads pipelined under the kernels: the job records go
@@ -552,16 +633,22 @@ int ext_batch_pipelined(fa_ctx *c, const ExtParams &kp, const fa_job *jobs, uint
     }
     const int max_q = (int)h_info[2];
     FA_CUDA(launch_chunk_scatter(c->jobs.as<fa_job>(), n, qs, ts, kSlices, scratch, c->order.as<uint32_t>(), s));
+    const int band = max_band_of(jobs, n);
+    if (c->kernel == FA_KERNEL_AUTO && !c->tuned.count({(max_q + 31) / 32, band}))
+        FA_CUDA(cudaStreamWaitEvent(s, c->slice_ev[kSlices - 1], 0));   // tuning reads every slice
+    int rc0 = FA_OK;
+    const Choice kc = resolve_choice(c, kp, c->jobs.as<fa_job>(), c->order.as<uint32_t>(), n, c->qseq.as<uint8_t>(),
+                                     c->tseq.as<uint8_t>(), max_q, band, c->out.as<fa_ext_result>(), m.status, s, &rc0);
+    if (rc0) return rc0;
     uint32_t launches = 2;
     FA_CUDA(cudaEventRecord(c->ev0, s));
     for (int k = 0; k < kSlices; ++k) {
         const uint32_t cnt = h_info[4 + k + 1] - h_info[4 + k];
         FA_CUDA(cudaStreamWaitEvent(s, c->slice_ev[k], 0));
         if (cnt == 0) continue;
-        FA_CUDA(launch_ext_packed(c->jobs.as<fa_job>(), c->order.as<uint32_t>() + h_info[4 + k], cnt, nullptr,
-                                  nullptr, c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(), kp, max_q, 0, nullptr,
-                                  c->out.as<fa_ext_result>(), nullptr, false, c->cells_job.as<uint32_t>(), m.cells,
-                                  m.status, s));
+        FA_CUDA(launch_ext(kc, c->jobs.as<fa_job>(), c->order.as<uint32_t>() + h_info[4 + k], cnt, nullptr,
+                           c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(), kp, max_q, nullptr, c->out.as<fa_ext_result>(),
+                           nullptr, false, c->cells_job.as<uint32_t>(), m.cells, m.status, s));
         ++launches;
     }
     FA_CUDA(cudaEventRecord(c->ev1, s));
@@ -569,12 +656,6 @@ int ext_batch_pipelined(fa_ctx *c, const ExtParams &kp, const fa_job *jobs, uint
     if (int rc = finish_ext(c, nullptr, n, s, stats, nullptr, launches, 0, false)) return rc;
     FA_CUDA(cudaStreamSynchronize(s));
     return FA_OK;
-}
-
-int max_band_of(const fa_job *jobs, uint32_t n) {
-    int w = 0;
-    for (uint32_t i = 0; i < n; ++i) w = std::max(w, jobs[i].w);
-    return w;
 }
 
 }  // namespace
@@ -674,7 +755,7 @@ int fa_ext_batch_policy(fa_ctx *c, const fa_params *p, const fa_policy *pol, con
         return fail(FA_ERR_STATE, "learned policy needs w_first (or a loaded band model)");
     FA_CUDA(cudaSetDevice(c->device));
     const ExtParams kp = ext_params_of(p);
-    if ((!pol || pol->mode == FA_POLICY_SINGLE) && !c->graph && n >= kPipeMinJobs && c->kernel != FA_KERNEL_INT16X2) {
+    if ((!pol || pol->mode == FA_POLICY_SINGLE) && !c->graph && n >= kPipeMinJobs) {
         int rc = ext_batch_pipelined(c, kp, jobs, n, qseq, qseq_len, tseq, tseq_len, out, stats);
         if (rc) return rc;
         if (w_final)
@@ -702,7 +783,7 @@ int fa_ext_batch_policy(fa_ctx *c, const fa_params *p, const fa_policy *pol, con
     const int32_t *d_wf = (pol && pol->mode == FA_POLICY_LEARNED) ? c->w_first.as<int32_t>() : nullptr;
     int rc = c->graph
                  ? run_ext_graph(c, kp, pol, n, max_q, max_band_of(jobs, n), {}, nullptr, d_wf, s, stats, w_final)
-                 : run_ext(c, kp, pol, n, segs, max_q, c->jobs.as<fa_job>(), c->order.as<uint32_t>(),
+                 : run_ext(c, kp, pol, n, segs, max_q, max_band_of(jobs, n), c->jobs.as<fa_job>(), c->order.as<uint32_t>(),
                            c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(), d_wf, c->out.as<fa_ext_result>(), s, stats,
                            w_final);
     if (rc) return rc;
@@ -790,7 +871,7 @@ int fa_ext_batch_learned(fa_ctx *c, const fa_params *p, const fa_policy *pol, co
     FA_CUDA(cudaEventSynchronize(c->ev1));
     cudaEventElapsedTime(&pred_ms, c->ev0, c->ev1);
     if (w_first_out) FA_CUDA(cudaMemcpy(w_first_out, c->w_first.p, 4ull * n, cudaMemcpyDeviceToHost));
-    int rc = run_ext(c, kp, pol, n, segs, max_q, c->jobs.as<fa_job>(), c->order.as<uint32_t>(), c->qseq.as<uint8_t>(),
+    int rc = run_ext(c, kp, pol, n, segs, max_q, max_band_of(jobs, n), c->jobs.as<fa_job>(), c->order.as<uint32_t>(), c->qseq.as<uint8_t>(),
                      c->tseq.as<uint8_t>(), c->w_first.as<int32_t>(), c->out.as<fa_ext_result>(), s, stats, w_final);
     if (rc) return rc;
     FA_CUDA(cudaMemcpyAsync(out, c->out.p, sizeof(fa_ext_result) * (size_t)n, cudaMemcpyDeviceToHost, s));
@@ -855,10 +936,14 @@ int fa_ext_batch_device(fa_ctx *c, const fa_params *p, const fa_job *d_jobs, uin
     } else {
         segs.assign(1, {n, std::max(0, segs.empty() ? 0 : segs.front().second)});
     }
+    int rc0 = FA_OK;
+    const Choice kc = resolve_choice(c, kp, d_jobs, order, n, d_qseq, d_tseq, segs.empty() ? 0 : segs.front().second,
+                                     -1, d_out, m.status, s, &rc0);
+    if (rc0) return rc0;
     uint32_t b = 0;
     if (c->timing) FA_CUDA(cudaEventRecord(c->kev0, s));
     for (auto &sg : segs) {
-        FA_CUDA(launch_ext(c->kernel, d_jobs, order + b, sg.first - b, nullptr, d_qseq, d_tseq, kp, sg.second,
+        FA_CUDA(launch_ext(kc, d_jobs, order + b, sg.first - b, nullptr, d_qseq, d_tseq, kp, sg.second,
                            nullptr, d_out, nullptr, false, nullptr, nullptr, m.status, s));
         b = sg.first;
     }
@@ -873,6 +958,30 @@ int fa_ctx_set_kernel(fa_ctx *c, int kernel) {
     if (kernel < FA_KERNEL_AUTO || kernel > FA_KERNEL_INT16X2)
         return fail(FA_ERR_ARG, "unknown kernel choice %d", kernel);
     c->kernel = kernel;
+    c->tuned.clear();
+    return FA_OK;
+}
+
+int fa_ctx_set_threads(fa_ctx *c, int threads_per_block) {
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    if (threads_per_block != 64 && threads_per_block != 128 && threads_per_block != 256)
+        return fail(FA_ERR_ARG, "threads per block must be 64, 128 or 256 (got %d)", threads_per_block);
+    c->threads = threads_per_block;
+    return FA_OK;
+}
+
+int fa_ctx_kernel_choice(fa_ctx *c, int *kernel, int *threads_per_block, int cap, int *cand_kernel,
+                         int *cand_threads, float *cand_ms, int *n_cand) {
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    if (kernel) *kernel = c->last_choice.kernel;
+    if (threads_per_block) *threads_per_block = c->last_choice.tpb;
+    const int nc = (int)c->last_tuning.size();
+    for (int k = 0; k < nc && k < cap; ++k) {
+        if (cand_kernel) cand_kernel[k] = c->last_tuning[k].first.kernel;
+        if (cand_threads) cand_threads[k] = c->last_tuning[k].first.tpb;
+        if (cand_ms) cand_ms[k] = c->last_tuning[k].second;
+    }
+    if (n_cand) *n_cand = nc;
     return FA_OK;
 }
 

@@ -16,13 +16,13 @@ constexpr int kPackedHMax = 8191;    // largest H/E the packed column word holds
 constexpr int kBandBuckets = 13;   // configured band + 12 narrow band classes
 constexpr int kPairThreads = 32;     // threads per int16x2 extension block (2 jobs each)
 
-size_t ext_packed_smem_bytes(int qcap, int ring);
+size_t ext_packed_smem_bytes(int qcap, int ring, int tpb);
 cudaError_t launch_ext_packed(const fa_job *d_jobs, const uint32_t *d_order, uint32_t n,
                               const uint32_t *d_first, const uint32_t *d_n, const uint8_t *d_qseq,
                               const uint8_t *d_tseq, const ExtParams &p, int qcap, int ring,
                               const int32_t *d_w_try, fa_ext_result *d_out, uint8_t *d_clamped, bool cert,
                               uint32_t *d_cells_job, unsigned long long *d_cells, uint32_t *d_status,
-                              cudaStream_t stream);
+                              cudaStream_t stream, int tpb = kExtThreads);
 
 // int16x2 variant: two jobs per thread (extend_pair_kernel.cu).  Eligible for
 // bwa-form scoring matrices; same arguments and results as launch_ext_packed.

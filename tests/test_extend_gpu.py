@@ -92,12 +92,15 @@ def test_parameter_sweep_bit_exact(ctx, a, b_, n, gaps, w, zdrop, eb):
     assert np.array_equal(out, ref), diff_report(out, ref)
 
 
-@pytest.mark.parametrize("kernel", [N.FA_KERNEL_INT32, N.FA_KERNEL_INT16X2])
-def test_kernel_variants_bit_exact(ctx, kernel):
-    """Both extension kernels (int32 one job per thread, int16x2 two jobs per thread)."""
+@pytest.mark.parametrize("kernel,threads", [(N.FA_KERNEL_INT32, 64), (N.FA_KERNEL_INT32, 128),
+                                            (N.FA_KERNEL_INT32, 256), (N.FA_KERNEL_INT16X2, 128)])
+def test_kernel_variants_bit_exact(ctx, kernel, threads):
+    """Every autotuning candidate (int32 one job per thread at 64/128/256 threads per
+    block, int16x2 two jobs per thread) gives the oracle's results."""
     b = synth.workload_ext_1m(100_000, seed=31)
     p = fa.BandedPairWiseSW().to_struct()
     ctx.set_kernel(kernel)
+    ctx.set_threads(threads)
     try:
         out, stats, ref, tr = run_both(ctx, p, b)
         ref_seq = synth.reference(5_000_000, seed=6, n_rate=0.01, repeat_frac=0.05)
@@ -105,8 +108,11 @@ def test_kernel_variants_bit_exact(ctx, kernel):
         out2, _, ref2, _ = run_both(ctx, p, u)
         sw = fa.BandedPairWiseSW(o_del=5, e_del=2, o_ins=3, e_ins=1, mat=fa.bwa_fill_scmat(3, 2, 0), zdrop=30)
         out3, _, ref3, _ = run_both(ctx, sw.to_struct(), u)
+        choice = ctx.kernel_choice()
     finally:
         ctx.set_kernel(N.FA_KERNEL_AUTO)
+        ctx.set_threads(128)
+    assert choice["kernel"] == ("int32" if kernel == N.FA_KERNEL_INT32 else "int16x2")
     assert np.array_equal(out, ref), diff_report(out, ref)
     assert stats["cells"] == tr["cells"].sum()
     assert np.array_equal(out2, ref2), diff_report(out2, ref2)
@@ -218,3 +224,24 @@ def test_large_batch_errors_and_pinned_pipeline(ctx):
         out, st, _ = fa.extend_batch(p, pin_j, pin_q, pin_t, ctx=ctx)
         assert np.array_equal(out, ref), diff_report(out, ref)
         assert st["cells"] == tr["cells"].sum()
+
+
+def test_autotuner_picks_a_measured_candidate():
+    """FA_KERNEL_AUTO times every candidate once per shape and runs the fastest; the
+    results equal the oracle's whichever wins."""
+    b = synth.workload_ext_1m(150_000, seed=33)
+    p = fa.BandedPairWiseSW().to_struct()
+    c = N.Context(0)
+    try:
+        out, _, _ = fa.extend_batch(p, b.jobs, b.qseq, b.tseq, ctx=c)
+        ch = c.kernel_choice()
+        cands = ch["candidates"]
+        assert len(cands) >= 3
+        best = min(cands, key=lambda x: x["sample_ms"])
+        assert (best["kernel"], best["threads_per_block"]) == (ch["kernel"], ch["threads_per_block"])
+        out2, _, _ = fa.extend_batch(p, b.jobs, b.qseq, b.tseq, ctx=c)   # cached choice, no new table
+        assert c.kernel_choice()["kernel"] == ch["kernel"]
+    finally:
+        c.close()
+    ref, _ = O.ext_batch(p, b.jobs, b.qseq, b.tseq)
+    assert np.array_equal(out, ref) and np.array_equal(out2, ref)
