@@ -38,6 +38,7 @@ METRIC = "GCUPS & alignments/s @151bp, learned-band vs plain-band on B200, bit-e
 N_JOBS = 1_000_000
 CPU_SAMPLE = 200_000
 MATE_JOBS = 500_000
+UNEVEN_JOBS = 2_000_000
 MATE_CPU_SAMPLE = 20_000
 DPX_OPS_PER_CELL_PAIR = 9   # int16x2 ops per packed cell pair in the roofline model
 
@@ -177,6 +178,41 @@ def bench_learned(args, ctx, b, p):
             "speedup": pm / lm, "network_gain": fm / lm,
             "identical_outputs": bool(np.array_equal(plain, learned)),
             "identical_frac": float(np.mean(plain == learned))}
+
+
+def bench_uneven(args, ctx, p):
+    """Uneven-length batch: 2,000,000 mixed left and right extensions, reads 50-300 bp,
+    seeds anywhere in the read, targets from a 100 Mbp reference with 5% low-complexity
+    repeats.  Plain bwa-mem2 policy against the learned path (the 151-bp model; results
+    stay exact whatever it predicts), both through the host ABI, device time of their
+    kernels; outputs compared."""
+    import ferrousalign_b200 as fa
+    from ferrousalign_b200 import _native as N
+    from ferrousalign_b200 import band_model as B
+    from ferrousalign_b200 import synth
+    t0 = time.time()
+    u = synth.workload_ext_uneven(UNEVEN_JOBS)
+    log(f"uneven workload: {UNEVEN_JOBS} jobs in {time.time() - t0:.1f}s")
+    n = len(u.jobs)
+    bwa = fa.make_policy(N.FA_POLICY_BWA, 2)
+    model = B.BandModel.load()
+    hints = B.hints_from_info(u.info)
+    pm, lm = [], []
+    for _ in range(max(2, args.steps // 10)):
+        plain, pst, _ = fa.extend_batch(p, u.jobs, u.qseq, u.tseq, policy=bwa, ctx=ctx)
+        pm.append(float(pst["kernel_ms"]))
+        learned, lst, wf, _ = B.extend_batch_learned(p, u.jobs, u.qseq, u.tseq, model, hints=hints, ctx=ctx)
+        lm.append(float(lst["kernel_ms"]))
+    pms, lms = float(np.median(pm)), float(np.median(lm))
+    ql = u.jobs["qlen"]
+    return {"workload": f"{n} mixed left/right extensions, reads 50-300 bp, 100 Mbp reference with 5% repeats",
+            "qlen_mean": float(ql.mean()), "qlen_max": int(ql.max()),
+            "plain": {"value": n / (pms * 1e-3), "unit": "alignments/s", "kernel_ms": pms,
+                      "gcups": float(pst["cells_executed"]) / (pms * 1e-3) / 1e9},
+            "learned": {"value": n / (lms * 1e-3), "unit": "alignments/s", "kernel_ms": lms,
+                        "cells_saved_frac": 1.0 - float(lst["cells_executed"]) / float(pst["cells_executed"]),
+                        "miss_rate": float(lst["misses"]) / n},
+            "speedup": pms / lms, "identical_outputs": bool(np.array_equal(plain, learned))}
 
 
 def bench_mixed(args, b, p):
@@ -351,6 +387,7 @@ def main():
     ap.add_argument("--skip-mate", action="store_true", help="omit the mate-rescue section")
     ap.add_argument("--skip-learned", action="store_true", help="omit the learned-band section")
     ap.add_argument("--skip-mixed", action="store_true", help="omit the mixed mate + extension batch section")
+    ap.add_argument("--skip-uneven", action="store_true", help="omit the uneven-length batch section")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -517,6 +554,8 @@ def main():
         line["mate_rescue"] = bench_mate(args, ctx, lib, dev, stream, flush, skip_cpu=args.skip_cpu)
     if not args.skip_mate and not args.skip_learned and not args.skip_mixed:
         line["mixed_batch"] = bench_mixed(args, b, p)
+    if not args.skip_learned and not args.skip_uneven:
+        line["uneven"] = bench_uneven(args, ctx, p)
     if not args.skip_cpu:
         ref2, tr2, dt, threads = cpu_oracle_rate(b, p, min(CPU_SAMPLE, n))
         line["cpu_baseline"] = {"value": min(CPU_SAMPLE, n) / dt, "unit": "alignments/s", "cores": threads,

@@ -6,13 +6,13 @@
 // H values before the lazy-F correction, F is restarted at every stripe boundary and
 // the lazy-F loop stops after the first pass that changes nothing, padding columns
 // score 0 and take part in the row maxima, and the query end is searched over
-// sign-interpreted lanes.  This kernel reproduces the striped machine exactly by
-// giving every SIMD lane of the reference its own GPU lane: a group of P = 16 (u8)
-// or 8 (i16) lanes owns one job, lane l holds stripe l (query positions
-// j + l*slen) in registers, the diagonal crosses stripes with one shuffle per row,
-// lazy-F passes move the F carry one lane per pass, and row maxima, the query-end
-// search and the second-best scan are group reductions.  The forward pass and the
-// KSW_XSTART reverse pass share the same code.
+// sign-interpreted lanes.  These kernels reproduce the striped machine exactly: a
+// group of 8 GPU lanes owns one job; for i16 jobs each GPU lane holds one SIMD lane of
+// the reference (stripe l: query positions j + l*slen) in registers, for u8 jobs each
+// holds two (sw_pass_u8x2, 16-bit halves, DPX 16x2 instructions).  The diagonal crosses
+// stripes with one shuffle per row, lazy-F passes move the F carry one SIMD lane per
+// pass, and row maxima, the query-end search and the second-best scan are group
+// reductions.  The forward pass and the KSW_XSTART reverse pass share the same code.
 
 #include <climits>
 
@@ -222,6 +222,198 @@ __device__ fa_kswr sw_pass(SeqView Q, int qlen, SeqView Tg, int tlen, uint32_t x
     return r;
 }
 
+// The u8 engine with two SIMD lanes per GPU lane: thread l of an 8-thread group holds
+// the reference's lanes 2l (low 16 bits) and 2l+1 (high 16 bits) of every segment, so
+// each DPX instruction updates two cells.  Values stay within 0..255, so the 16-bit
+// halves never carry; the u8 saturations are explicit: min(hd + s, 255) as
+// __viaddmin_u16x2, the -shift with a zero floor and the gap updates as
+// __viaddmax_s16x2_relu.  Moving a register one lane up (the diagonal between segments,
+// F between lazy-F passes) is one shuffle of the group plus one PRMT.  Same results as
+// sw_pass<16, SMAX>.
+__device__ __forceinline__ uint32_t lane_up_u16x2(uint32_t v, uint32_t gmask, int l) {
+    uint32_t prev = __shfl_up_sync(gmask, v, 1, 8);
+    if (l == 0) prev = 0;
+    return prmt(v, prev, 0x1076u);   // low <- previous thread's high, high <- own low
+}
+
+template <int SMAX>
+__device__ fa_kswr sw_pass_u8x2(SeqView Q, int qlen, SeqView Tg, int tlen, uint32_t xtra, const MateParams &p,
+                                uint32_t gmask, int l, uint32_t *blist, int bcap, unsigned long long &cells,
+                                uint32_t &status)
+{
+    constexpr int P = 16;                      // lanes of the reference's u8 vector
+    const int slen = (qlen + P - 1) / P;
+    const int off = SMAX - slen;               // segment j lives at register index j + off
+    const uint32_t minsc = (xtra & FA_KSW_XSUBO) ? (xtra & 0xffffu) : 0x10000u;
+    const uint32_t endsc = (xtra & FA_KSW_XSTOP) ? (xtra & 0xffffu) : 0x10000u;
+    const uint32_t shift = (uint32_t)p.shift;
+    const uint32_t neg_shift2 = (uint32_t)(uint16_t)(-(int)shift) * 0x10001u;
+    const uint32_t neg_oedel2 = (uint32_t)(uint16_t)(-(p.o_del + p.e_del)) * 0x10001u;
+    const uint32_t neg_edel2 = (uint32_t)(uint16_t)(-p.e_del) * 0x10001u;
+    const uint32_t neg_oeins2 = (uint32_t)(uint16_t)(-(p.o_ins + p.e_ins)) * 0x10001u;
+    const uint32_t neg_eins2 = (uint32_t)(uint16_t)(-p.e_ins) * 0x10001u;
+    const uint32_t cap255 = 0x00FF00FFu, neg2 = 0x80008000u;
+
+    // PRMT selectors of both lanes' query codes per segment (byte 5 of the table pair is
+    // zero: code 5 marks padding, whose profile score is `shift`, held in byte 5's place
+    // by the row table below)
+    uint32_t sel[SMAX];
+    uint32_t bad = 0;
+#pragma unroll
+    for (int a = 0; a < SMAX; ++a) {
+        uint32_t c2[2] = {5u, 5u};
+        if (a >= off) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int k = (a - off) + (2 * l + h) * slen;
+                if (k < qlen) {
+                    uint32_t c = Q.at(k);
+                    bad |= c > 4u;
+                    c2[h] = c > 4u ? 4u : c;
+                }
+            }
+        }
+        // result bytes: [c_lo, zero, c_hi, zero] with the zero from byte 7 of the table
+        sel[a] = c2[0] | 0x70u | c2[1] << 8 | 0x7000u;
+    }
+
+    uint32_t H0[SMAX], H1[SMAX], E[SMAX], Hm[SMAX];
+#pragma unroll
+    for (int a = 0; a < SMAX; ++a) { H0[a] = 0; H1[a] = 0; E[a] = 0; Hm[a] = 0; }
+
+    // profile rows (mat + shift mod 256 for codes 0..4, shift for padding code 5, 0 in byte 7)
+    uint32_t rlo[5], rhi[5];
+#pragma unroll
+    for (int t = 0; t < 5; ++t) {
+        rlo[t] = (uint8_t)(p.mat[t * 5] + shift) | (uint32_t)(uint8_t)(p.mat[t * 5 + 1] + shift) << 8 |
+                 (uint32_t)(uint8_t)(p.mat[t * 5 + 2] + shift) << 16 |
+                 (uint32_t)(uint8_t)(p.mat[t * 5 + 3] + shift) << 24;
+        rhi[t] = (uint8_t)(p.mat[t * 5 + 4] + shift) | (uint32_t)(uint8_t)shift << 8;
+    }
+
+    int gmax = 0, te = -1;
+    int nb = 0, last_row = -2, last_sc = 0;
+
+    for (int i = 0; i < tlen; ++i) {
+        const uint32_t tb = Tg.at(i);
+        if (tb > 4u) { bad = 1; break; }
+        uint32_t lo = rlo[0], hi = rhi[0];
+#pragma unroll
+        for (int t = 1; t < 5; ++t)
+            if (tb == (uint32_t)t) { lo = rlo[t]; hi = rhi[t]; }
+        cells += (unsigned long long)qlen;
+
+        uint32_t hd = lane_up_u16x2(H0[SMAX - 1], gmask, l);
+        uint32_t f = 0, mx = 0;
+#pragma unroll
+        for (int a = 0; a < SMAX; ++a) {
+            if (a >= off) {
+                const uint32_t s = prmt(lo, hi, sel[a]);
+                uint32_t h = __viaddmin_u16x2(hd, s, cap255);          // adds_epu8
+                h = __viaddmax_s16x2_relu(h, neg_shift2, 0u);          // subs_epu8(., shift)
+                const uint32_t e = E[a];
+                h = __vimax3_s16x2(h, e, f);
+                mx = __vimax3_s16x2(mx, h, h);
+                H1[a] = h;
+                const uint32_t tdel = __viaddmax_s16x2(h, neg_oedel2, neg2);
+                E[a] = __viaddmax_s16x2_relu(e, neg_edel2, tdel);
+                const uint32_t tins = __viaddmax_s16x2(h, neg_oeins2, neg2);
+                f = __viaddmax_s16x2_relu(f, neg_eins2, tins);
+                hd = H0[a];
+            }
+        }
+        // lazy-F: one lane further per pass, stop after a pass that changed nothing
+        for (int pass = 0; pass < P; ++pass) {
+            f = lane_up_u16x2(f, gmask, l);
+            uint32_t changed = 0;
+#pragma unroll
+            for (int a = 0; a < SMAX; ++a) {
+                if (a >= off) {
+                    const uint32_t hb = H1[a];
+                    const uint32_t hn = __vimax3_s16x2(hb, f, f);
+                    changed |= hn ^ hb;
+                    H1[a] = hn;
+                    f = __viaddmax_s16x2_relu(f, neg_eins2, 0u);
+                }
+            }
+            if (!__any_sync(gmask, changed != 0)) break;
+        }
+        const uint32_t mx1 = max(mx & 0xffffu, mx >> 16);
+        const int imax = (int)__reduce_max_sync(gmask, mx1);
+        if ((uint32_t)imax >= minsc) {
+            if (nb == 0 || last_row + 1 != i) {
+                if (nb < bcap) {
+                    if (l == 0) blist[nb] = (uint32_t)imax << 16 | (uint32_t)i;
+                } else {
+                    status |= ST_BLIST;
+                }
+                ++nb;
+                last_row = i;
+                last_sc = imax;
+            } else if (last_sc < imax) {
+                if (l == 0 && nb - 1 < bcap) blist[nb - 1] = (uint32_t)imax << 16 | (uint32_t)i;
+                last_row = i;
+                last_sc = imax;
+            }
+        }
+        if (imax > gmax) {
+            gmax = imax;
+            te = i;
+#pragma unroll
+            for (int a = 0; a < SMAX; ++a) Hm[a] = H1[a];
+            if (gmax + (int)shift >= 255 || (uint32_t)gmax >= endsc) break;
+        }
+#pragma unroll
+        for (int a = 0; a < SMAX; ++a) H0[a] = H1[a];
+    }
+    if (bad) status |= ST_BAD_CODE;
+
+    fa_kswr r;
+    r.score = gmax + (int)shift < 255 ? gmax : 255;
+    r.te = te;
+    r.qe = -1; r.score2 = -1; r.te2 = -1; r.tb = -1; r.qb = -1;
+    if (r.score != 255) {
+        // query end: smallest position holding the largest sign-interpreted lane value
+        int bv = -1, bk = -1;
+#pragma unroll
+        for (int a = 0; a < SMAX; ++a) {
+            if (a >= off) {
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int k = (a - off) + (2 * l + h) * slen;
+                    if (k < qlen) {
+                        const int v = (int)(int8_t)(uint8_t)(h ? (Hm[a] >> 16) : (Hm[a] & 0xffffu));
+                        if (v > bv || (v == bv && k < bk)) { bv = v; bk = k; }
+                    }
+                }
+            }
+        }
+        const int gv = __reduce_max_sync(gmask, bv);
+        r.qe = __reduce_min_sync(gmask, bv == gv ? bk : INT_MAX);
+        if (r.qe == INT_MAX) r.qe = -1;
+        if (nb > 0) {
+            __syncwarp(gmask);
+            const int iv = (r.score + p.max - 1) / p.max;
+            const int low = te - iv, high = te + iv;
+            const int cnt = nb < bcap ? nb : bcap;
+            int s2 = -1, e2 = INT_MAX;
+            for (int e = l; e < cnt; e += 8) {
+                const uint32_t b = blist[e];
+                const int row = (int)(b & 0xffffu), sc = (int)(b >> 16);
+                if ((row < low || row > high) && sc > s2) { s2 = sc; e2 = e; }
+            }
+            const int gs2 = __reduce_max_sync(gmask, s2);
+            const int ge2 = __reduce_min_sync(gmask, s2 == gs2 ? e2 : INT_MAX);
+            if (gs2 >= 0 && ge2 != INT_MAX) {
+                r.score2 = gs2;
+                r.te2 = (int)(blist[ge2] & 0xffffu);
+            }
+            __syncwarp(gmask);
+        }
+    }
+    return r;
+}
+
 template <int P, int SMAX>
 __global__ void __launch_bounds__(kMateThreads)
 mate_sw_kernel(const fa_mate_job *__restrict__ jobs, const uint32_t *__restrict__ order, uint32_t n,
@@ -269,6 +461,70 @@ mate_sw_kernel(const fa_mate_job *__restrict__ jobs, const uint32_t *__restrict_
     }
 }
 
+// u8 jobs: one 8-thread group per job, two reference lanes per thread (sw_pass_u8x2).
+template <int SMAX>
+__global__ void __launch_bounds__(kMateThreads)
+mate_sw_kernel_u8x2(const fa_mate_job *__restrict__ jobs, const uint32_t *__restrict__ order, uint32_t n,
+                    const uint8_t *__restrict__ qseq, const uint8_t *__restrict__ tseq, const MateParams p,
+                    int bcap, fa_kswr *__restrict__ out, unsigned long long *__restrict__ cells_out,
+                    uint32_t *__restrict__ status)
+{
+    constexpr int G = 8;
+    extern __shared__ uint32_t bsm[];
+    const uint32_t gtid = blockIdx.x * kMateThreads + threadIdx.x;
+    const uint32_t gidx = gtid / G;
+    const int lane = threadIdx.x & 31;
+    const int l = lane % G;
+    const uint32_t gmask = ((1u << G) - 1u) << (lane - l);
+    unsigned long long cells = 0;
+    uint32_t st = 0;
+    if (gidx < n) {
+        const uint32_t jid = order ? order[gidx] : gidx;
+        const fa_mate_job jb = jobs[jid];
+        uint32_t *blist = bsm + (threadIdx.x / G) * bcap;
+        SeqView Q{qseq + jb.q_off, -1}, Tg{tseq + jb.t_off, -1};
+        fa_kswr r = sw_pass_u8x2<SMAX>(Q, jb.qlen, Tg, jb.tlen, jb.xtra, p, gmask, l, blist, bcap, cells, st);
+        const uint32_t xtra = jb.xtra;
+        const bool find_start = (xtra & FA_KSW_XSTART) &&
+                                !((xtra & FA_KSW_XSUBO) && r.score < (int)(xtra & 0xffffu));
+        if (find_start && r.qe >= 0 && r.te >= 0) {
+            SeqView Q2{qseq + jb.q_off, r.qe}, T2{tseq + jb.t_off, r.te};
+            const fa_kswr rr = sw_pass_u8x2<SMAX>(Q2, r.qe + 1, T2, jb.tlen, FA_KSW_XSTOP | (uint32_t)r.score, p,
+                                                  gmask, l, blist, bcap, cells, st);
+            if (rr.score >= r.score) { r.tb = r.te - rr.te; r.qb = r.qe - rr.qe; }
+        }
+        st = __reduce_or_sync(gmask, st);
+        if (l == 0) {
+            out[jid] = r;
+            if (st) atomicOr(status, st);
+        } else {
+            cells = 0;
+        }
+    }
+    if (cells_out) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) cells += __shfl_down_sync(0xffffffffu, cells, o);
+        if (lane == 0 && cells) atomicAdd(cells_out, cells);
+    }
+}
+
+template <int SMAX>
+static cudaError_t launch_mate_u8x2(const fa_mate_job *d_jobs, const uint32_t *d_order, uint32_t n,
+                                    const uint8_t *d_qseq, const uint8_t *d_tseq, const MateParams &p, int bcap,
+                                    fa_kswr *d_out, unsigned long long *d_cells, uint32_t *d_status,
+                                    cudaStream_t stream)
+{
+    const size_t smem = (size_t)(kMateThreads / 8) * bcap * sizeof(uint32_t);
+    cudaError_t err = cudaFuncSetAttribute(mate_sw_kernel_u8x2<SMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem);
+    if (err != cudaSuccess) return err;
+    const uint64_t threads = (uint64_t)n * 8;
+    const uint32_t blocks = (uint32_t)((threads + kMateThreads - 1) / kMateThreads);
+    mate_sw_kernel_u8x2<SMAX><<<blocks, kMateThreads, smem, stream>>>(d_jobs, d_order, n, d_qseq, d_tseq, p, bcap,
+                                                                      d_out, d_cells, d_status);
+    return cudaGetLastError();
+}
+
 template <int P, int SMAX>
 static cudaError_t launch_mate_t(const fa_mate_job *d_jobs, const uint32_t *d_order, uint32_t n,
                                  const uint8_t *d_qseq, const uint8_t *d_tseq, const MateParams &p,
@@ -298,13 +554,15 @@ cudaError_t launch_mate_sw(bool byte_lanes, const fa_mate_job *d_jobs, const uin
     // the batch's query length (151-bp mates: 10 u8 segments, 19 i16 segments)
 #define FA_MATE(PP, SS) launch_mate_t<PP, SS>(d_jobs, d_order, n, d_qseq, d_tseq, p, bcap, d_out, d_cells, d_status, \
                                               stream)
+#define FA_MATE2(SS) launch_mate_u8x2<SS>(d_jobs, d_order, n, d_qseq, d_tseq, p, bcap, d_out, d_cells, d_status, stream)
     if (byte_lanes) {
-        if (max_qlen <= 16 * 10) return FA_MATE(16, 10);
-        if (max_qlen <= 16 * 12) return FA_MATE(16, 12);
-        if (max_qlen <= 16 * 16) return FA_MATE(16, 16);
-        if (max_qlen <= 16 * 24) return FA_MATE(16, 24);
-        return FA_MATE(16, 32);
+        if (max_qlen <= 16 * 10) return FA_MATE2(10);
+        if (max_qlen <= 16 * 12) return FA_MATE2(12);
+        if (max_qlen <= 16 * 16) return FA_MATE2(16);
+        if (max_qlen <= 16 * 24) return FA_MATE2(24);
+        return FA_MATE2(32);
     }
+#undef FA_MATE2
     if (max_qlen <= 8 * 16) return FA_MATE(8, 16);
     if (max_qlen <= 8 * 20) return FA_MATE(8, 20);
     if (max_qlen <= 8 * 24) return FA_MATE(8, 24);
