@@ -38,6 +38,9 @@ METRIC = "GCUPS & alignments/s @151bp, learned-band vs plain-band on B200, bit-e
 N_JOBS = 1_000_000
 CPU_SAMPLE = 200_000
 MATE_JOBS = 500_000
+# ncu: ext_packed_kernel<0,0,128> on 439,186 jobs of the 151-bp workload read 248.1 MB and
+# wrote 11.2 MB of DRAM (the algorithmic bytes are about 372 B per job)
+EXT_DRAM_BYTES_PER_JOB = (248.106e6 + 11.161e6) / 439_186
 UNEVEN_JOBS = 2_000_000
 MATE_CPU_SAMPLE = 20_000
 DPX_OPS_PER_CELL_PAIR = 9   # int16x2 ops per packed cell pair in the roofline model
@@ -537,7 +540,12 @@ def main():
         "roofline": {"bound": "dpx", "achieved": achieved_gcups, "peak": peak_gcups, "unit": "Gcell/s",
                      "kernel": "ext_packed_kernel", "kernel_ms_per_step": kernel_ms,
                      "launches_per_step": 2,
-                     "frac": achieved_gcups / peak_gcups, "traffic": None,
+                     "frac": achieved_gcups / peak_gcups,
+                     # DRAM bytes of one step's extension launches: the per-job read + write
+                     # traffic of one ncu capture of ext_packed_kernel (500k-job launch,
+                     # profiles/ext_packed_kernel_1M_151bp.md) times the step's jobs
+                     "traffic": EXT_DRAM_BYTES_PER_JOB * n,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per job, scaled",
                      "peak_source": f"measured __viaddmax_s16x2_relu rate {peak_ops / 1e12:.2f} Tops/s x2/"
                                     f"{DPX_OPS_PER_CELL_PAIR}; s32 DPX {peak_s32 / 1e12:.2f} Tops/s",
                      "hbm": {"achieved_gbs": (bytes_in + bytes_out) / (kernel_ms * 1e-3) / 1e9,

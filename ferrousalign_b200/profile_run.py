@@ -3,6 +3,7 @@
 Usage: python -m ferrousalign_b200.profile_run [n_jobs] [probe|-] [kernel: 0 auto, 1 int32, 2 int16x2] [reps]
        python -m ferrousalign_b200.profile_run learned [n_jobs] [reps]   (learned-band path)
        python -m ferrousalign_b200.profile_run bands [n_jobs]            (single runs at fixed bands)
+       python -m ferrousalign_b200.profile_run mate [n_jobs] [reps]      (mate-rescue SW, device-resident)
 """
 import ctypes
 import sys
@@ -12,6 +13,30 @@ import torch
 
 import ferrousalign_b200 as fa
 from ferrousalign_b200 import _native as N, synth
+
+if len(sys.argv) > 1 and sys.argv[1] == "mate":
+    n = int(sys.argv[2]) if len(sys.argv) > 2 else 500_000
+    m = synth.workload_mate(n)
+    mp = fa.make_mate_params()
+    ctx = fa.Context(0)
+    lib = N.load()
+    dev = torch.device("cuda", 0)
+    st = torch.cuda.Stream(dev)
+    with torch.cuda.stream(st):
+        d_jobs = torch.from_numpy(m.jobs.view(np.uint8)).to(dev)
+        d_q = torch.from_numpy(m.qseq).to(dev)
+        d_t = torch.from_numpy(m.tseq).to(dev)
+        d_out = torch.empty(n * 7, dtype=torch.int32, device=dev)
+        for r in range(int(sys.argv[3]) if len(sys.argv) > 3 else 1):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            N.check(lib.fa_mate_sw_batch_device(ctx.handle, N.ptr(mp), d_jobs.data_ptr(), n, d_q.data_ptr(),
+                                                d_t.data_ptr(), d_out.data_ptr(), ctypes.c_void_p(st.cuda_stream)))
+            e1.record(st)
+            st.synchronize()
+            N.check(lib.fa_ctx_sync(ctx.handle))
+            print("mate batch ms", e0.elapsed_time(e1))
+    sys.exit(0)
 
 if len(sys.argv) > 1 and sys.argv[1] in ("learned", "bands"):
     from ferrousalign_b200 import band_model as B
