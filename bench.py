@@ -107,16 +107,15 @@ class ClockSampler:
 
 
 def dist_env():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    from ferrousalign_b200.replicas import dist_env as env
+    return env()
 
 
 def make_workload(rank: int, n: int):
     from ferrousalign_b200 import synth
+    from ferrousalign_b200.replicas import shard_seed
     t0 = time.time()
-    b = synth.workload_ext_1m(n, seed=2 + 1000 * rank)
+    b = synth.workload_ext_1m(n, seed=shard_seed(2, rank))
     log(f"[rank {rank}] generated {n} jobs in {time.time() - t0:.1f}s "
         f"(query {b.qseq.nbytes / 1e6:.0f} MB, target {b.tseq.nbytes / 1e6:.0f} MB)")
     return b
@@ -463,12 +462,9 @@ def main():
             torch.distributed.barrier()
     N.check(lib.fa_ctx_sync(ctx.handle))
     clocks = clk.summary()
-    ms_step = float(np.mean(times))
+    from ferrousalign_b200.replicas import max_over_ranks
+    ms_step = max_over_ranks(float(np.mean(times)), dev)
     kernel_ms = float(np.mean(ktimes))
-    if ws > 1:
-        t = torch.tensor([ms_step], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_step = float(t.item())
 
     # correctness on the timed outputs: a sample against the oracle, plus the cell count
     out = d_out.view(torch.int32).cpu().numpy().view(N.EXT_RESULT_DT).reshape(-1)
@@ -500,11 +496,7 @@ def main():
         t0 = time.perf_counter()
         step_host()
         e2e_times.append((time.perf_counter() - t0) * 1e3)
-    e2e_ms = float(np.mean(e2e_times))
-    if ws > 1:
-        t = torch.tensor([e2e_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(float(np.mean(e2e_times)), dev)
     cells = int(stats[0]["cells"])
     exact = exact and np.array_equal(out_h[chk], ref_out)
 
