@@ -16,7 +16,7 @@ LIB_PATH = PKG / "libferrous_b200.so"
 
 FA_OK, FA_ERR_ARG, FA_ERR_CAPACITY, FA_ERR_CUDA, FA_ERR_TIMEOUT, FA_ERR_STATE = range(6)
 FA_POLICY_SINGLE, FA_POLICY_BWA, FA_POLICY_LEARNED = 0, 1, 2
-FA_JUDGE_CERT, FA_JUDGE_MAXOFF, FA_JUDGE_GLOBAL, FA_JUDGE_BOUND, FA_JUDGE_ONCE = 1, 2, 4, 8, 16
+FA_JUDGE_CERT, FA_JUDGE_MAXOFF, FA_JUDGE_GLOBAL, FA_JUDGE_BOUND, FA_JUDGE_ONCE, FA_JUDGE_HINT = 1, 2, 4, 8, 16, 32
 FA_DIR_LEFT, FA_DIR_RIGHT = 0, 1
 FA_KERNEL_AUTO, FA_KERNEL_INT32, FA_KERNEL_INT16X2 = 0, 1, 2
 KSW_XBYTE, KSW_XSTOP, KSW_XSUBO, KSW_XSTART = 0x10000, 0x20000, 0x40000, 0x80000

@@ -191,6 +191,7 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
             const int a = p.max_score;
             ExitBound xb;
             int bmax = ExitBound::NEG, first_fail = INT32_MAX, max_written = -1, rows = 0, prev_end = 0;
+            int srun = 0, sev = 0, slast = 0;   // bound shortfall: running max, at the last event, last row
             bool row_ok = true, stale = false, broke = false, zbreak = false;
             auto slot = [](int j) { return RING > 0 ? (j & (RING - 1)) : j; };
             auto qcode = [&](int j) { return (qw[(j >> 3) * T] >> (4 * (j & 7))) & 7u; };
@@ -307,11 +308,15 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
                     const int b = xb.at(i, a, e_del);
                     row_ok = m_row > 0 ? b < m_row : b <= 0;
                     if (!row_ok && first_fail == INT32_MAX) first_fail = i;
+                    slast = row_ok ? 0 : b - m_row + 1;
+                    srun = max(srun, slast);
+                    if (max_ie == i) sev = srun;
                     bmax = max(bmax, b);
                 }
                 if (m_row == 0) { broke = true; break; }
                 if (m_row > best) {
                     best = m_row; max_i = i; max_j = mj;
+                    if (CERT) sev = srun;
                     const int off = mj > i ? mj - i : i - mj;
                     if (max_off < off) max_off = off;
                 } else if (p.zdrop > 0) {
@@ -344,11 +349,23 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
                 const int i_ev = max(max_i, max_ie), lim = min(best, gscore);
                 // after a zero row every live path has left the region: a wider run's
                 // remaining rows are bounded by the tents over [last row, tlen-1]
-                const bool tail_ok = !broke || (zbreak ? row_ok : xb.max_over(rows - 1, tlen - 1, a, e_del) < lim);
+                const int fut = (broke && !zbreak) ? xb.max_over(rows - 1, tlen - 1, a, e_del) : ExitBound::NEG;
+                const bool tail_ok = !broke || (zbreak ? row_ok : fut < lim);
                 const int W = ext_band_clamp(qlen, jb.w, p);
                 const bool wide_clean = init_reach <= min(W + 1, qlen);
                 const bool cert = !stale && gscore > 0 && first_fail > i_ev && tail_ok && bmax < lim && wide_clean;
                 flags |= (uint8_t)cert << 1;
+                // bits 2-7: extra band columns the certificate's shortfall asks for (63: none);
+                // widening the band moves every exit at least one gap extension further away
+                int slack = sev;                            // rows up to the last event count
+                if (broke && zbreak) slack = max(slack, slast);
+                if (bmax >= lim) slack = max(slack, bmax - lim + 1);
+                if (broke && !zbreak && fut >= lim) slack = max(slack, fut - lim + 1);
+                const int e_min = min(e_del, e_ins);
+                int hint = kBandHintNone;
+                if (!stale && gscore > 0 && e_min > 0 && wide_clean)
+                    hint = min(kBandHintNone, (max(slack, 1) + e_min - 1) / e_min);
+                flags |= (uint8_t)(hint << 2);
             }
             if (clamped_out) clamped_out[jid] = flags;
             if (cells_job) cells_job[jid] = cells;

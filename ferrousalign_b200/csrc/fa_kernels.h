@@ -13,6 +13,7 @@ namespace fa {
 
 constexpr int kExtThreads = 128;     // threads (= jobs) per extension block
 constexpr int kPackedHMax = 8191;    // largest H/E the packed column word holds
+constexpr int kBandHintNone = 63;    // flags bits 2-7: no band suggested by the certificate
 constexpr int kBandBuckets = 13;   // configured band + 12 narrow band classes
 constexpr int kPairThreads = 32;     // threads per int16x2 extension block (2 jobs each)
 

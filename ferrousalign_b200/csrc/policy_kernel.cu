@@ -81,9 +81,24 @@ __global__ void policy_step_kernel(const fa_job *__restrict__ jobs, const uint32
             }
             if (!ok) {
                 if (st.missed && st.tries[jid] == 1) st.missed[jid] = 1;
-                jump |= (judge & FA_JUDGE_ONCE) != 0;
-                w <<= 1;
-                if (jump || w >= jb.w) { w = jb.w; k = 0; }
+                const int hint = fl >> 2;
+                int nw = 0;
+                if (!jump && (judge & FA_JUDGE_BOUND) && (judge & FA_JUDGE_ONCE) && (judge & FA_JUDGE_HINT) &&
+                    st.tries[jid] == 1 && hint < kBandHintNone) {
+                    nw = w + hint;                      // up to the band ladder 2^k, 3*2^(k-1)
+                    if (nw > 2) {
+                        const int p2 = 1 << (32 - __clz(nw - 1));
+                        nw = 3 * p2 / 4 >= nw ? 3 * p2 / 4 : p2;
+                    }
+                    if (2 * nw > jb.w) nw = 0;
+                }
+                if (nw > 0) {
+                    w = nw;                             // one retry at the suggested band
+                } else {
+                    jump |= (judge & FA_JUDGE_ONCE) != 0;
+                    w <<= 1;
+                    if (jump || w >= jb.w) { w = jb.w; k = 0; }
+                }
                 st.w_cur[jid] = w;
                 st.k[jid] = k;
                 again = true;

@@ -4,7 +4,9 @@ Training set: 5,000,000 right extensions of the 151-bp generator with per-read i
 rates {0, 0.1, 1, 3}% (seed 4).  Label: the smallest band of the doubling ladders from 2
 and 3 whose run the exit-bound certificate proves equal to the configured-band run (the
 configured band when none does).  One model is trained per pinball quantile tau and
-evaluated with both retry rules (doubling, or one narrow try then the configured band);
+evaluated with three retry rules (doubling; one narrow try then the configured band; one
+narrow try, one retry at the band the certificate's shortfall suggests, then the configured
+band);
 the pair with the shortest extension time on a validation batch (seed 6) is kept.  Evaluation on
 a fresh 1,000,000-job batch from disjoint generator seeds: the plain bwa-mem2 policy
 against the learned path (outputs must be identical), miss rate, executed and saved
@@ -93,7 +95,8 @@ def main(argv=None) -> dict:
         model.fit_norm(x)
         t0 = time.time()
         losses = model.train(x, target, epochs=args.epochs, batch=8192, lr=args.lr, tau=tau, ctx=ctx)
-        for rule, judge in (("double", B.JUDGE_EXACT), ("once", B.JUDGE_EXACT | N.FA_JUDGE_ONCE)):
+        for rule, judge in (("double", B.JUDGE_EXACT), ("once", B.JUDGE_EXACT | N.FA_JUDGE_ONCE),
+                            ("hint", B.JUDGE_EXACT | N.FA_JUDGE_ONCE | N.FA_JUDGE_HINT)):
             out, st, wf, _ = run_learned(p, val, model, args.w_min, ctx, judge=judge)
             if not np.array_equal(out, val_plain):
                 raise RuntimeError(f"tau {tau}: learned path differs from the plain path on the validation batch")

@@ -84,6 +84,10 @@ typedef struct {
                                leaving the narrow run's region can reach any output statistic */
 #define FA_JUDGE_ONCE   16  /* retry rule: a rejected narrow run goes straight to the configured
                                band instead of doubling (one narrow try per job)            */
+#define FA_JUDGE_HINT   32  /* with ONCE and BOUND: a rejected first narrow run retries once
+                               at the band its certificate's shortfall suggests (rounded up
+                               to the band ladder) when that is at most half the configured
+                               band; then the configured band                                */
 
 typedef struct {
     int32_t mode;

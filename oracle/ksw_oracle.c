@@ -101,6 +101,7 @@ int ora_ksw_extend2(int qlen, const uint8_t *query, int tlen, const uint8_t *tar
      * (dropped columns, first column); each side's tents peak near one row */
     int P1[2] = {NEG, NEG}, P3[2] = {NEG, NEG};
     int bmax = NEG, first_fail = INT32_MAX, row_ok = 1, stale = 0;
+    int srun = 0, sev = 0, slast = 0;   /* bound shortfall: running max, at the last event, last row */
     int max_written = -1, broke = 0, zbreak = 0;
 #define ORA_EXIT(side, x, ix, jx) do { const int x_ = (x), ix_ = (ix), D_ = qlen - 1 - (jx); \
         if (x_ > 0) { if (x_ - a * ix_ > P1[side]) P1[side] = x_ - a * ix_;                 \
@@ -176,11 +177,15 @@ int ora_ksw_extend2(int qlen, const uint8_t *query, int tlen, const uint8_t *tar
             }
             row_ok = m_row > 0 ? b < m_row : b <= 0;
             if (!row_ok && first_fail == INT32_MAX) first_fail = i;
+            slast = row_ok ? 0 : b - m_row + 1;
+            if (slast > srun) srun = slast;
+            if (max_ie == i) sev = srun;
             if (b > bmax) bmax = b;
         }
         if (m_row == 0) { broke = 1; break; }
         if (m_row > max) {
             max = m_row; max_i = i; max_j = mj;
+            sev = srun;
             int off = mj - i; if (off < 0) off = -off;
             if (max_off < off) max_off = off;
         } else if (zdrop > 0) {
@@ -242,6 +247,20 @@ int ora_ksw_extend2(int qlen, const uint8_t *query, int tlen, const uint8_t *tar
         }
         const int tail_ok = !broke || (zbreak ? row_ok : fut < lim);
         trace->bound_ok = !stale && gscore > 0 && first_fail > i_ev && tail_ok && bmax < lim;
+        /* how far the bound missed, in columns of extra band: widening the band moves
+         * every exit at least one more gap extension away */
+        int slack = sev;                                 /* rows up to the last event count */
+        if (broke && zbreak && slast > slack) slack = slast;
+        if (bmax >= lim && bmax - lim + 1 > slack) slack = bmax - lim + 1;
+        if (broke && !zbreak && fut >= lim && fut - lim + 1 > slack) slack = fut - lim + 1;
+        const int e_min = e_del < e_ins ? e_del : e_ins;
+        int delta = ORA_HINT_NONE;
+        if (!stale && gscore > 0 && e_min > 0) {
+            const int sl = slack > 1 ? slack : 1;
+            delta = (sl + e_min - 1) / e_min;
+            if (delta > ORA_HINT_NONE) delta = ORA_HINT_NONE;
+        }
+        trace->hint = delta;
         trace->init_reach = init_reach;
     }
 #undef ORA_EXIT
@@ -501,6 +520,15 @@ static int run_ext(const fa_params *p, const fa_job *jb, const uint8_t *qseq, co
                            jb->h0, o, tr);
 }
 
+/* Smallest band of the ladder 1, 2, 3, 4, 6, 8, 12, 16, ... (2^k, 3*2^(k-1)) >= b. */
+static int ladder_ceil(int b)
+{
+    if (b <= 2) return b;
+    int p2 = 1;
+    while (p2 < b) p2 <<= 1;
+    return 3 * p2 / 4 >= b ? 3 * p2 / 4 : p2;
+}
+
 /* bwa-mem2 mem_chain2aln retry loop, starting from try k0 with `prev` given. */
 static int policy_bwa(const fa_params *p, const fa_job *jb, const uint8_t *qs, const uint8_t *ts,
                       int max_tries, fa_ext_result *o, int32_t *wfin, int32_t *ntries, int64_t *cx)
@@ -555,6 +583,12 @@ static int policy_one(const batch_t *B, uint32_t i)
                 jump = off_ok && !ok;
             }
             if (ok) { accepted = 1; wfin = w; break; }
+            if (!jump && (pol->judge & FA_JUDGE_BOUND) && (pol->judge & FA_JUDGE_ONCE) &&
+                (pol->judge & FA_JUDGE_HINT) && ntries == 1 &&
+                tr.hint < ORA_HINT_NONE && ora_wide_clean(B->p, jb->qlen, jb->w, tr.init_reach)) {
+                const int nw = ladder_ceil(w + tr.hint);     /* one retry at the suggested band */
+                if (2 * nw <= jb->w) { w = nw; continue; }
+            }
             if (jump || (pol->judge & FA_JUDGE_ONCE)) break;   /* straight to the configured band */
             w <<= 1;
         }

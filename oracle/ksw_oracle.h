@@ -31,7 +31,12 @@ typedef struct {
     int32_t bound_ok;  /* exit-bound certificate: no path that leaves this
                           run's computed region can change any output       */
     int32_t init_reach;/* last column whose first-row value is positive     */
+    int32_t hint;      /* extra band columns the certificate asks for when it
+                          fails (ORA_HINT_NONE: none suggested)            */
+    int32_t _pad;
 } ora_ext_trace;
+
+#define ORA_HINT_NONE 63
 
 /* The exit-bound certificate of a narrow run at band w transfers to a run at
  * configured band W >= w when W's first row covers every positive first-row

@@ -14,7 +14,7 @@ HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libksw_oracle.so"
 
 TRACE_DT = np.dtype([("cells", "<i8"), ("rows", "<i4"), ("clamped", "<i4"), ("label", "<i4"),
-                     ("w_eff", "<i4"), ("bound_ok", "<i4"), ("init_reach", "<i4")])
+                     ("w_eff", "<i4"), ("bound_ok", "<i4"), ("init_reach", "<i4"), ("hint", "<i4"), ("_pad", "<i4")])
 EXT_RESULT_DT = np.dtype([("score", "<i4"), ("qle", "<i4"), ("tle", "<i4"), ("gtle", "<i4"),
                           ("gscore", "<i4"), ("max_off", "<i4")])
 KSWR_DT = np.dtype([("score", "<i4"), ("te", "<i4"), ("qe", "<i4"), ("score2", "<i4"),

@@ -150,13 +150,14 @@ def test_bound_judge_is_exact_and_matches_oracle(ctx, workload):
     plain, pst, _ = fa.extend_batch(p, b.jobs, b.qseq, b.tseq, policy=fa.make_policy(N.FA_POLICY_BWA, 2), ctx=ctx)
     rng = np.random.default_rng(7)
     wf = rng.choice([2, 4, 8, 16, 32], size=len(b.jobs)).astype(np.int32)
-    pol = fa.make_policy(N.FA_POLICY_LEARNED, 2, N.FA_JUDGE_BOUND, 1)
-    out, st, wfin = fa.extend_batch(p, b.jobs, b.qseq, b.tseq, policy=pol, w_first=wf, ctx=ctx)
-    assert np.array_equal(out, plain), diff_report(out, plain)
-    ref, rwfin, rtries, rcells = O.ext_batch_policy(p, pol, b.jobs, b.qseq, b.tseq, wf)
-    assert np.array_equal(wfin, rwfin)
-    assert st["cells_executed"] == rcells.sum()
-    assert st["cells_executed"] < pst["cells_executed"]
+    for judge in (N.FA_JUDGE_BOUND, N.FA_JUDGE_BOUND | N.FA_JUDGE_ONCE | N.FA_JUDGE_HINT):
+        pol = fa.make_policy(N.FA_POLICY_LEARNED, 2, judge, 1)
+        out, st, wfin = fa.extend_batch(p, b.jobs, b.qseq, b.tseq, policy=pol, w_first=wf, ctx=ctx)
+        assert np.array_equal(out, plain), diff_report(out, plain)
+        ref, rwfin, rtries, rcells = O.ext_batch_policy(p, pol, b.jobs, b.qseq, b.tseq, wf)
+        assert np.array_equal(wfin, rwfin)          # same certificates and the same hints
+        assert st["cells_executed"] == rcells.sum()
+        assert st["cells_executed"] < pst["cells_executed"]
 
 
 def test_reference_style_interface(ctx):

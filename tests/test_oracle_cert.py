@@ -71,11 +71,15 @@ def test_bound_policy_equals_plain_policy(name):
     plain, _, _, pc = O.ext_batch_policy(p, fa.make_policy(N.FA_POLICY_BWA, 2), b.jobs, b.qseq, b.tseq)
     rng = np.random.default_rng(5)
     wf = rng.choice([1, 2, 4, 8, 16, 32], len(b.jobs)).astype(np.int32)
-    pol = fa.make_policy(N.FA_POLICY_LEARNED, 2, N.FA_JUDGE_BOUND, 1)
-    out, wfin, tries, cells = O.ext_batch_policy(p, pol, b.jobs, b.qseq, b.tseq, wf)
-    assert np.array_equal(out, plain)
-    assert (wfin < b.jobs["w"]).mean() > 0.3          # most jobs stop at a narrow band
-    assert cells.sum() < pc.sum()
+    for judge in (N.FA_JUDGE_BOUND, N.FA_JUDGE_BOUND | N.FA_JUDGE_ONCE,
+                  N.FA_JUDGE_BOUND | N.FA_JUDGE_ONCE | N.FA_JUDGE_HINT):
+        pol = fa.make_policy(N.FA_POLICY_LEARNED, 2, judge, 1)
+        out, wfin, tries, cells = O.ext_batch_policy(p, pol, b.jobs, b.qseq, b.tseq, wf)
+        assert np.array_equal(out, plain)
+        assert (wfin < b.jobs["w"]).mean() > 0.3          # most jobs stop at a narrow band
+        assert cells.sum() < pc.sum()
+        if judge & N.FA_JUDGE_HINT:                       # some rejected runs retried narrow
+            assert ((tries == 2) & (wfin < b.jobs["w"])).any()
 
 
 def test_certificate_examples():
