@@ -351,7 +351,7 @@ int max_rounds_of(const fa_policy *pol, int max_w) {
     if (mode == FA_POLICY_SINGLE) return 1;
     const int max_tries = std::max(1, pol->max_tries);
     if (mode != FA_POLICY_LEARNED) return max_tries;
-    int narrow = 1;
+    int narrow = (pol->judge & FA_JUDGE_HINT) && (pol->judge & FA_JUDGE_BOUND) ? 2 : 1;
     if (!(pol->judge & FA_JUDGE_ONCE))
         for (long long w = std::max(1, pol->w_min); w * 2 < max_w && narrow < 13; w *= 2) ++narrow;
     return narrow + max_tries;
@@ -393,13 +393,15 @@ int enqueue_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n
     const int max_tries = std::max(1, pol->max_tries);
     const int max_rounds = capture ? max_rounds_of(pol, max_w) : (learned ? 13 : 0) + max_tries;
     const bool once = learned && (pol->judge & FA_JUDGE_ONCE);
+    // rounds that can hold narrow runs: the first, and with hints also the second
+    const int narrow_rounds = (learned && (pol->judge & FA_JUDGE_HINT) && (pol->judge & FA_JUDGE_BOUND)) ? 2 : 1;
     const uint32_t *list = d_order;
     const uint32_t *cnt = nullptr;
     uint32_t *next = c->list_a.as<uint32_t>(), *next_cnt = m.cnt_a;
     uint32_t *spare = c->list_b.as<uint32_t>(), *spare_cnt = m.cnt_b;
     for (int r = 0; r < max_rounds; ++r) {
-        // with one narrow try, rounds after the first hold only plain-policy runs
-        const bool cert_r = cert && !(once && r > 0);
+        // with one narrow try, rounds after the narrow ones hold only plain-policy runs
+        const bool cert_r = cert && !(once && r >= narrow_rounds);
         if (r == 0 && !learned) {
             uint32_t b = 0;
             for (auto &sg : segs0) {
