@@ -18,7 +18,7 @@ FA_OK, FA_ERR_ARG, FA_ERR_CAPACITY, FA_ERR_CUDA, FA_ERR_TIMEOUT, FA_ERR_STATE = 
 FA_POLICY_SINGLE, FA_POLICY_BWA, FA_POLICY_LEARNED = 0, 1, 2
 FA_JUDGE_CERT, FA_JUDGE_MAXOFF, FA_JUDGE_GLOBAL, FA_JUDGE_BOUND, FA_JUDGE_ONCE, FA_JUDGE_HINT = 1, 2, 4, 8, 16, 32
 FA_DIR_LEFT, FA_DIR_RIGHT = 0, 1
-FA_KERNEL_AUTO, FA_KERNEL_INT32, FA_KERNEL_INT16X2 = 0, 1, 2
+FA_KERNEL_AUTO, FA_KERNEL_INT32, FA_KERNEL_INT16X2, FA_KERNEL_ROWS2 = 0, 1, 2, 3
 KSW_XBYTE, KSW_XSTOP, KSW_XSUBO, KSW_XSTART = 0x10000, 0x20000, 0x40000, 0x80000
 FA_MAX_QLEN, FA_MAX_TLEN = 4096, 65535
 FA_NOALLOC_MAX_JOBS = 1 << 18
@@ -159,7 +159,7 @@ class Context:
         ct = (C.c_int * 8)()
         cm = (C.c_float * 8)()
         check(load().fa_ctx_kernel_choice(self.handle, C.byref(k), C.byref(t), 8, ck, ct, cm, C.byref(nc)))
-        names = {FA_KERNEL_INT32: "int32", FA_KERNEL_INT16X2: "int16x2"}
+        names = {FA_KERNEL_INT32: "int32", FA_KERNEL_INT16X2: "int16x2", FA_KERNEL_ROWS2: "rows2"}
         return {"kernel": names.get(k.value, str(k.value)), "threads_per_block": t.value,
                 "candidates": [{"kernel": names.get(ck[i], str(ck[i])), "threads_per_block": ct[i],
                                 "sample_ms": float(cm[i])} for i in range(min(nc.value, 8))]}

@@ -1,0 +1,429 @@
+// extend_rows2_kernel.cu -- banded seed extension, two target rows per thread (sm_100a).
+//
+// Same recurrence, band rescans, stale-cell semantics and outputs as ext_packed_kernel
+// (ksw_extend2, src/core/alignment/ksw_affine_gap.rs:952-1169).  One thread owns one job
+// and computes rows i and i+1 together in int16x2 registers: the low half holds row i at
+// column j, the high half row i+1 at column j-1.  Row i+1's inputs at column j-1 (row i's
+// H at column j-2 and its E for column j-1) are the low half's results of the two previous
+// steps, so they never pass through shared memory, and every DPX instruction updates two
+// cells.  Shared memory is read once (row i-1's column word) and written once (row i+1's)
+// per two cells.
+//
+// Column words are 16 bits, H in the low byte and E in the high byte: exact while
+// h0 + max(mat) * qlen <= 255, which bounds every H and E the recurrence produces.  Other
+// jobs go to an overflow list that the int32 kernel runs next.  Query codes are stored as
+// PRMT selector bytes; the score is byte (t XOR q) of the table [a, -b, -b, -b, n, n, n, n]
+// with the sign replicated into the high byte, so the kernel serves bwa-form matrices
+// (ext_pair_eligible): a on the diagonal, -b off it, n (0 or -1) for N.
+//
+// Row i+1's band follows from row i's final words: its first column is row i's first
+// non-zero word (found while the first steps run), its end from row i's last positive H
+// (tracked every step).  Until row i has ended the high half runs on; cells past row i+1's
+// true end see only zero inputs, so their H is row i+1's decaying F (below its row max,
+// never a first argmax) and their E is zero, and their words are cleared after the pair,
+// which leaves shared memory as the one-row recurrence leaves it on every column a later
+// row can read.
+
+#include "fa_device.cuh"
+#include "fa_kernels.h"
+
+namespace fa {
+
+namespace {
+
+// PRMT, generic mode (byte select, nibble bit 3 replicates the selected byte's sign); the
+// host branch states those semantics so the thread body also runs on the CPU (tests).
+__host__ __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
+#ifdef __CUDA_ARCH__
+    uint32_t r;
+    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(sel));
+    return r;
+#else
+    const uint64_t src = (uint64_t)b << 32 | a;
+    uint32_t r = 0;
+    for (int k = 0; k < 4; ++k) {
+        const uint32_t nib = (sel >> (4 * k)) & 0xFu;
+        uint32_t byte = (uint32_t)(src >> (8 * (nib & 7u))) & 0xFFu;
+        if (nib & 8u) byte = (byte & 0x80u) ? 0xFFu : 0x00u;
+        r |= byte << (8 * k);
+    }
+    return r;
+#endif
+}
+
+__host__ __device__ __forceinline__ void or_status(uint32_t *st, uint32_t v) {
+#ifdef __CUDA_ARCH__
+    atomicOr(st, v);
+#else
+    *st |= v;
+#endif
+}
+
+__host__ __device__ __forceinline__ uint32_t take_slot(uint32_t *cnt) {
+#ifdef __CUDA_ARCH__
+    return atomicAdd(cnt, 1u);
+#else
+    return (*cnt)++;
+#endif
+}
+
+__host__ __device__ inline uint32_t dup16(int v) { return (uint32_t)(v & 0xFFFF) * 0x10001u; }
+
+}  // namespace
+
+constexpr int kRows2MaxQ = 254;   // u8 column words: h0 >= 1 and a >= 1 leave qlen <= 254
+
+// One job.  eh[c * T]: column word of column c (H | E << 8), c in [0, qcap]; sw[k * T]:
+// the selector bytes of columns 4k..4k+3.  Returns the cells the recurrence evaluated.
+template <int T>
+__host__ __device__ __forceinline__ uint32_t rows2_thread(
+    uint32_t jid, uint16_t *__restrict__ eh, uint32_t *__restrict__ sw, const fa_job *__restrict__ jobs,
+    const uint8_t *__restrict__ qseq, const uint8_t *__restrict__ tseq, const ExtParams &p, int qcap,
+    const int32_t *__restrict__ w_try, fa_ext_result *__restrict__ out, uint8_t *__restrict__ clamped_out,
+    uint32_t *__restrict__ cells_job, uint32_t *__restrict__ status, uint32_t *__restrict__ ovf,
+    uint32_t *__restrict__ ovf_n)
+{
+    uint32_t cells = 0;
+    {
+        const fa_job jb = jobs[jid];
+        const int qlen = jb.qlen, tlen = jb.tlen, h0 = jb.h0;
+        const int a = p.max_score;
+        if (h0 <= 0 || qlen <= 0 || tlen < 0) {
+            or_status(status, ST_ARG);
+        } else if (qlen > qcap) {
+            or_status(status, ST_CAPACITY);
+        } else if (h0 > 255 || a * qlen > 255 - h0) {
+            ovf[take_slot(ovf_n)] = jid;              // needs wider cells: the int32 kernel
+        } else {
+            const int w = ext_band_clamp(qlen, w_try ? w_try[jid] : jb.w, p);
+            const int oe_del = p.o_del + p.e_del, oe_ins = p.o_ins + p.e_ins;
+            const int e_del = p.e_del, e_ins = p.e_ins;
+            const uint32_t NOED = dup16(-oe_del), NED = dup16(-e_del), NOEI = dup16(-oe_ins), NEI = dup16(-e_ins);
+            const uint32_t TAB = (uint32_t)(uint8_t)p.mat[0] | (uint32_t)(uint8_t)p.mat[1] * 0x01010100u;
+            const uint32_t TABN = (uint32_t)(uint8_t)p.mat[4] * 0x01010101u;
+            const uint32_t kmul = a <= 1 ? 2u : 4u;   // kmul * M >= M + a for every M >= 1
+            // selector nibble of a query N: lands on bytes 4-7 (n) for t < 4 and, for a
+            // target N, on a byte whose sign is n's (n = -1: -b; n = 0: a)
+            const uint32_t qn = p.mat[4] < 0 ? 13u : 12u;
+            const uint8_t *Q = qseq + jb.q_off;
+            const uint8_t *Tg = tseq + jb.t_off;
+
+            uint32_t bad = 0;
+            for (int j0 = 0; j0 < qlen; j0 += 8) {
+                uint32_t qb[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) qb[u] = j0 + u < qlen ? (uint32_t)Q[j0 + u] : 0u;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    uint32_t word = 0;
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const uint32_t q = qb[4 * h + u];
+                        if (j0 + 4 * h + u < qlen) bad |= q >= (uint32_t)p.m;
+                        word |= (q < 4u ? q * 0x11u + 0x80u : qn * 0x11u) << (8 * u);
+                    }
+                    if (j0 + 4 * h < qlen) sw[((j0 >> 2) + h) * T] = word;
+                }
+            }
+            // first row (ksw_affine_gap.rs:1017-1025): h0, h0-oe_ins, then -e_ins while the
+            // previous value exceeds e_ins; E = 0
+            {
+                int hv = h0;
+                bool filling = true;
+                for (int j = 0; j <= qlen; ++j) {
+                    int h;
+                    if (j == 0) h = h0;
+                    else if (j == 1) h = h0 > oe_ins ? h0 - oe_ins : 0;
+                    else if (filling && hv > e_ins) h = hv - e_ins;
+                    else { filling = false; h = 0; }
+                    hv = h;
+                    eh[j * T] = (uint16_t)h;
+                }
+            }
+            auto sbyte = [&](int c) -> uint32_t { return (sw[(c >> 2) * T] >> (8 * (c & 3))) & 0xFFu; };
+            auto score1 = [&](uint32_t t, int c) -> int {   // one cell of row t at column c
+                return (int)(int16_t)(prmt(TAB, TABN, sbyte(c) ^ (t * 0x11u)) & 0xFFFFu);
+            };
+
+            // pair state, int16x2: low half row i, high half row i+1 (one column behind)
+            uint32_t hpp = 0, hp = 0, ep = 0, f2 = 0, km = 0, lpk = 0, tsel = 0;
+            // one step: low half column j, high half column j-1; ow = row i+1's word for
+            // column j-1.  km: max over cells of H << 8 | (255 - column) (row max, first
+            // column); lpk (low half): last column with H > 0.
+            auto step = [&](uint32_t wd, uint32_t qsel, uint32_t jk, uint32_t jpos, uint32_t &ow) {
+                const uint32_t M2 = prmt(wd, hpp, 0x5420u);     // (H of row i-1 at j-1, H of row i at j-2)
+                const uint32_t e2 = prmt(wd, ep, 0x5421u);      // (E at j, row i's E for j-1)
+                const uint32_t s2 = prmt(TAB, TABN, qsel ^ tsel);
+                // ksw_extend2's `M ? M + s : 0`: for M > 0, kmul * M >= M + s; for M == 0 the
+                // result is <= 0, which acts as 0 in every max below (halves stay apart:
+                // 4 * 255 < 2^15)
+                const uint32_t Mp = __viaddmin_s16x2(M2, s2, M2 * kmul);
+                const uint32_t h2 = __vimax3_s16x2(Mp, e2, f2);
+                const uint32_t en2 = __viaddmax_s16x2(e2, NED, __viaddmax_s16x2_relu(Mp, NOED, 0u));
+                f2 = __viaddmax_s16x2(f2, NEI, __viaddmax_s16x2_relu(Mp, NOEI, 0u));
+                const uint32_t hs = h2 << 8;
+                km = __viaddmax_u16x2(hs, jk, km);
+                lpk = __viaddmax_u16x2(__viaddmin_u16x2(hs, 0u, jpos), 0u, lpk);
+                ow = prmt(hp, en2, 0x62u);                      // (H of row i+1 at j-2, its E for j-1)
+                hpp = hp;
+                hp = h2;
+                ep = en2;
+            };
+            auto jk_of = [](int j) { return (uint32_t)(255 - j) | (uint32_t)((256 - j) & 0xFFFF) << 16; };
+            auto generic = [&](int j, uint32_t &ow) {
+                const uint32_t qsel = sbyte(j) | (j > 0 ? sbyte(j - 1) << 8 : 0u);
+                step((uint32_t)eh[j * T], qsel, jk_of(j), (uint32_t)j, ow);
+            };
+
+            int best = h0, max_i = -1, max_j = -1, max_ie = -1, gscore = -1, max_off = 0;
+            int beg = 0, end = qlen, clamped = 0;
+            // row-end rules of ksw_extend2 for row r with max m at column mj; false = stop
+            auto row_end = [&](int r, int m, int mj) -> bool {
+                if (m == 0) return false;
+                if (m > best) {
+                    best = m; max_i = r; max_j = mj;
+                    const int off = mj > r ? mj - r : r - mj;
+                    if (max_off < off) max_off = off;
+                } else if (p.zdrop > 0) {
+                    const int di = r - max_i, dj = mj - max_j;
+                    if (di > dj) {
+                        if (best - m - (di - dj) * e_del > p.zdrop) return false;
+                    } else if (best - m - (dj - di) * e_ins > p.zdrop) {
+                        return false;
+                    }
+                }
+                return true;
+            };
+            // target bases: tq0 holds the current four rows, tq1 the next four
+            uint32_t tq0 = 0, tq1 = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (k < tlen) tq0 |= (uint32_t)Tg[k] << (8 * k);
+                if (4 + k < tlen) tq1 |= (uint32_t)Tg[4 + k] << (8 * k);
+            }
+            for (int i = 0; i < tlen; i += 2) {
+                const bool two = i + 1 < tlen;
+                const uint32_t t0 = tq0 & 0xFFu, t1 = two ? (tq0 >> 8) & 0xFFu : 0u;
+                tq0 >>= 16;
+                if ((i & 3) == 2) {
+                    tq0 = tq1;
+                    tq1 = 0;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        if (i + 6 + k < tlen) tq1 |= (uint32_t)Tg[i + 6 + k] << (8 * k);
+                }
+                if (t0 >= (uint32_t)p.m || t1 >= (uint32_t)p.m) { bad = 1; break; }
+                tsel = t0 * 0x11u | t1 * 0x1100u;
+
+                // ---- row i: band
+                {
+                    const int beg_a = beg, end_a = end < qlen ? end : qlen;
+                    if (beg < i - w) beg = i - w;
+                    if (end > i + w + 1) end = i + w + 1;
+                    if (end > qlen) end = qlen;
+                    clamped |= (beg != beg_a) | (end != end_a);
+                }
+                const int b0 = beg, e0 = end;
+                const int h1lo = b0 == 0 ? max(h0 - (p.o_del + e_del * (i + 1)), 0) : 0;
+                hpp = 0; hp = (uint32_t)h1lo; ep = 0; f2 = 0; km = 0; lpk = 0;
+
+                // ---- phase A: row i alone until row i+1's first column is known
+                int j = b0, hs_trim = -1, c0 = -1;
+                uint32_t ow;
+                while (j < e0) {
+                    const uint32_t hprev = hp;
+                    generic(j, ow);
+                    // row i's word for column j: (its H at j-1, its E for j)
+                    if (two && hs_trim < 0 && ((hprev | ep) & 0xFFFFu)) hs_trim = j;
+                    ++j;
+                    if (hs_trim >= 0 && j - 1 >= i + 1 - w) { c0 = j - 1; break; }
+                }
+                if (c0 >= 0) {
+                    const int h1hi = c0 == 0 ? max(h0 - (p.o_del + e_del * (i + 2)), 0) : 0;
+                    hp = (hp & 0xFFFFu) | (uint32_t)h1hi << 16;
+                    f2 &= 0xFFFFu;
+                    km &= 0xFFFFu;
+                    // ---- phase B: both rows; row i+1's word for column j-1 stored each step
+                    while (j < e0 && (j & 3)) {
+                        generic(j, ow);
+                        eh[(j - 1) * T] = (uint16_t)ow;
+                        ++j;
+                    }
+                    if (j + 3 < e0) {
+                        uint32_t swp = sw[((j >> 2) - 1) * T];
+                        uint32_t jk = jk_of(j);
+                        for (; j + 3 < e0; j += 4) {
+                            const uint32_t swc = sw[(j >> 2) * T];
+                            const uint32_t w0 = eh[j * T], w1 = eh[(j + 1) * T], w2 = eh[(j + 2) * T],
+                                           w3 = eh[(j + 3) * T];
+                            uint32_t o0, o1, o2, o3;
+                            step(w0, prmt(swc, swp, 0x70u), jk, (uint32_t)j, o0);
+                            step(w1, prmt(swc, swc, 0x01u), jk - 0x10001u, (uint32_t)(j + 1), o1);
+                            step(w2, prmt(swc, swc, 0x12u), jk - 0x20002u, (uint32_t)(j + 2), o2);
+                            step(w3, prmt(swc, swc, 0x23u), jk - 0x30003u, (uint32_t)(j + 3), o3);
+                            eh[(j - 1) * T] = (uint16_t)o0;
+                            eh[j * T] = (uint16_t)o1;
+                            eh[(j + 1) * T] = (uint16_t)o2;
+                            eh[(j + 2) * T] = (uint16_t)o3;
+                            swp = swc;
+                            jk -= 0x40004u;
+                        }
+                    }
+                    while (j < e0) {
+                        generic(j, ow);
+                        eh[(j - 1) * T] = (uint16_t)ow;
+                        ++j;
+                    }
+                }
+
+                // ---- row i ends (hp's low half: H at e0-1, or the row's h1 when empty)
+                const int hlast = (int)(hp & 0xFFFFu);
+                if (e0 > b0) cells += e0 - b0;
+                if (e0 == qlen && gscore < hlast) { gscore = hlast; max_ie = i; }
+                if (!row_end(i, (int)((km & 0xFFFFu) >> 8), 255 - (int)(km & 0xFFu))) break;
+                if (!two) break;
+
+                // ---- row i+1: band from row i's words
+                const int lp = (int)(lpk & 0xFFFFu);   // row i's last column with H > 0
+                int b1 = hs_trim >= 0 ? hs_trim : e0;
+                int e1 = lp + 3 < qlen ? lp + 3 : qlen;
+                {
+                    const int beg_a = b1, end_a = e1;
+                    if (b1 < i + 1 - w) b1 = i + 1 - w;
+                    if (e1 > i + w + 2) e1 = i + w + 2;
+                    clamped |= (b1 != beg_a) | (e1 != end_a);
+                }
+                int h1h, fh, kh;
+                if (c0 >= 0) {
+                    h1h = (int)(hp >> 16); fh = (int)(f2 >> 16); kh = (int)(km >> 16);
+                } else {
+                    h1h = b1 == 0 ? max(h0 - (p.o_del + e_del * (i + 2)), 0) : 0; fh = 0; kh = 0;
+                }
+                if (c0 >= 0 && e1 <= e0 - 1) {
+                    // row i+1 already ran past its end: its word at e1 holds (H at e1-1, 0)
+                    // unless e1 is the column the last step did not reach
+                    if (e1 == e0 - 1) eh[e1 * T] = (uint16_t)h1h;
+                } else {
+                    // ---- phase C: row i+1's columns from max(c0, e0-1) on, one at a time
+                    for (int c = c0 >= 0 ? e0 - 1 : b1; c < e1; ++c) {
+                        int M, e;
+                        if (c < e0) { M = (int)(hpp & 0xFFFFu); e = (int)(ep & 0xFFFFu); }   // c == e0-1
+                        else if (c == e0) { M = (int)(hp & 0xFFFFu); e = 0; }               // row i's end word
+                        else { const uint32_t wd = eh[c * T]; M = (int)(wd & 0xFFu); e = (int)(wd >> 8); }
+                        const int s = score1(t1, c);
+                        const int Mp = M ? M + s : 0;
+                        const int h = max(max(Mp, e), fh);
+                        const int en = max(max(e - e_del, Mp - oe_del), 0);
+                        fh = max(max(fh - e_ins, Mp - oe_ins), 0);
+                        kh = max(kh, h << 8 | (255 - c));
+                        eh[c * T] = (uint16_t)(h1h | en << 8);
+                        h1h = h;
+                    }
+                    eh[e1 * T] = (uint16_t)h1h;
+                }
+                for (int c = e1 + 1; c <= e0; ++c) eh[c * T] = 0;   // row i's zero words
+                if (e1 > b1) cells += e1 - b1;
+                if (e1 == qlen && gscore < h1h) { gscore = h1h; max_ie = i + 1; }
+                if (!row_end(i + 1, kh >> 8, 255 - (kh & 0xFF))) break;
+                // rescans for the next pair (ksw_affine_gap.rs:1155-1166) on row i+1's words
+                int nb = b1;
+                while (nb < e1 && eh[nb * T] == 0) ++nb;
+                beg = nb;
+                int ne = e1;
+                while (ne > beg && eh[ne * T] == 0) --ne;
+                end = ne + 2 < qlen ? ne + 2 : qlen;
+            }
+            if (bad) or_status(status, ST_BAD_CODE);
+            fa_ext_result r;
+            r.score = best;
+            r.qle = max_j + 1;
+            r.tle = max_i + 1;
+            r.gtle = max_ie + 1;
+            r.gscore = gscore;
+            r.max_off = max_off;
+            out[jid] = r;
+            if (clamped_out) clamped_out[jid] = (uint8_t)clamped;
+            if (cells_job) cells_job[jid] = cells;
+        }
+    }
+    return cells;
+}
+
+template <int TPB>
+__global__ void __launch_bounds__(TPB)
+ext_rows2_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ order, uint32_t n,
+                 const uint32_t *__restrict__ n_dev, const uint8_t *__restrict__ qseq,
+                 const uint8_t *__restrict__ tseq, const ExtParams p, int qcap,
+                 const int32_t *__restrict__ w_try, fa_ext_result *__restrict__ out,
+                 uint8_t *__restrict__ clamped_out, uint32_t *__restrict__ cells_job,
+                 unsigned long long *__restrict__ cells_out, uint32_t *__restrict__ status,
+                 uint32_t *__restrict__ ovf, uint32_t *__restrict__ ovf_n)
+{
+    extern __shared__ uint32_t smem[];
+    const uint32_t gi = blockIdx.x * TPB + threadIdx.x;
+    uint32_t cells = 0;
+    if (n_dev) n = min(n, *n_dev);
+    if (gi < n) {
+        uint16_t *eh = reinterpret_cast<uint16_t *>(smem) + threadIdx.x;
+        uint32_t *sw = smem + (qcap + 1) * (TPB / 2) + threadIdx.x;
+        cells = rows2_thread<TPB>(order ? order[gi] : gi, eh, sw, jobs, qseq, tseq, p, qcap, w_try, out,
+                                  clamped_out, cells_job, status, ovf, ovf_n);
+    }
+    if (cells_out) {
+        unsigned long long c = cells;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+        if ((threadIdx.x & 31) == 0 && c) atomicAdd(cells_out, c);
+    }
+}
+
+size_t ext_rows2_smem_bytes(int qcap, int tpb) {
+    return (size_t)(qcap + 1) * tpb * sizeof(uint16_t) + (size_t)((qcap + 3) / 4) * tpb * sizeof(uint32_t);
+}
+
+bool ext_rows2_eligible(const ExtParams &p, int qcap) {
+    return qcap <= kRows2MaxQ && ext_pair_eligible(p);
+}
+
+namespace {
+template <int TPB>
+cudaError_t launch_rows2_variant(size_t smem, cudaStream_t stream, const fa_job *d_jobs, const uint32_t *d_order,
+                                 uint32_t n, const uint32_t *d_n, const uint8_t *d_qseq, const uint8_t *d_tseq,
+                                 const ExtParams &p, int qcap, const int32_t *d_w_try, fa_ext_result *d_out,
+                                 uint8_t *d_clamped, uint32_t *d_cells_job, unsigned long long *d_cells,
+                                 uint32_t *d_status, uint32_t *d_ovf, uint32_t *d_ovf_n)
+{
+    cudaError_t err = cudaFuncSetAttribute(ext_rows2_kernel<TPB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem);
+    if (err != cudaSuccess) return err;
+    const uint32_t blocks = (n + TPB - 1) / TPB;
+    ext_rows2_kernel<TPB><<<blocks, TPB, smem, stream>>>(d_jobs, d_order, n, d_n, d_qseq, d_tseq, p, qcap, d_w_try,
+                                                         d_out, d_clamped, d_cells_job, d_cells, d_status, d_ovf,
+                                                         d_ovf_n);
+    return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_ext_rows2(const fa_job *d_jobs, const uint32_t *d_order, uint32_t n, const uint32_t *d_n,
+                             const uint8_t *d_qseq, const uint8_t *d_tseq, const ExtParams &p, int qcap,
+                             const int32_t *d_w_try, fa_ext_result *d_out, uint8_t *d_clamped,
+                             uint32_t *d_cells_job, unsigned long long *d_cells, uint32_t *d_status,
+                             uint32_t *d_ovf, uint32_t *d_ovf_n, cudaStream_t stream, int tpb)
+{
+    if (n == 0) return cudaSuccess;
+    if (!ext_rows2_eligible(p, qcap) || !d_ovf || !d_ovf_n) return cudaErrorInvalidValue;
+    cudaError_t err = cudaMemsetAsync(d_ovf_n, 0, sizeof(uint32_t), stream);
+    if (err != cudaSuccess) return err;
+    const int t = tpb == 128 ? 128 : 64;
+    const size_t smem = ext_rows2_smem_bytes(qcap, t);
+    err = t == 128 ? launch_rows2_variant<128>(smem, stream, d_jobs, d_order, n, d_n, d_qseq, d_tseq, p, qcap, d_w_try,
+                                               d_out, d_clamped, d_cells_job, d_cells, d_status, d_ovf, d_ovf_n)
+                   : launch_rows2_variant<64>(smem, stream, d_jobs, d_order, n, d_n, d_qseq, d_tseq, p, qcap, d_w_try,
+                                              d_out, d_clamped, d_cells_job, d_cells, d_status, d_ovf, d_ovf_n);
+    if (err != cudaSuccess) return err;
+    // jobs whose scores can pass 255: the int32 kernel over the overflow list
+    return launch_ext_packed(d_jobs, d_ovf, n, nullptr, d_ovf_n, d_qseq, d_tseq, p, qcap, 0, d_w_try, d_out,
+                             d_clamped, false, d_cells_job, d_cells, d_status, stream);
+}
+
+}  // namespace fa

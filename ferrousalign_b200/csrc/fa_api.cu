@@ -79,6 +79,7 @@ struct fa_ctx {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     DevBuf jobs, order, qseq, tseq, out, clamped, cells_job, misc;
+    DevBuf ovf;   // two-row kernel: jobs handed on to the int32 kernel
     DevBuf w_first, w_cur, prev, kk, w_final, tries, missed, list_a, list_b, hist, feat, wbf, part_n, part_w;
     uint32_t last_launches = 0;
     bool timing = false;
@@ -111,18 +112,18 @@ int fa::fa_ctx_device(const fa_ctx *c) { return c->device; }
 namespace {
 
 // misc buffer layout (bytes): [0] status u32, [8] cells u64, [16] count A, [20] count B,
-// [64] band-bucket histogram u32[kBandBuckets], [128] band-bucket cursors u32[kBandBuckets],
-// [192] band-group bounds u32[3]
+// [24] two-row kernel overflow count, [64] band-bucket histogram u32[kBandBuckets],
+// [128] band-bucket cursors u32[kBandBuckets], [192] band-group bounds u32[3]
 constexpr size_t kMiscBytes = 256;
 struct Misc {
     uint32_t *status;
     unsigned long long *cells;
-    uint32_t *cnt_a, *cnt_b, *bucket_hist, *bucket_cursor, *group_bounds;
+    uint32_t *cnt_a, *cnt_b, *ovf_n, *bucket_hist, *bucket_cursor, *group_bounds;
 };
 Misc misc_of(fa_ctx *c) {
     char *b = c->misc.as<char>();
     return Misc{(uint32_t *)b, (unsigned long long *)(b + 8), (uint32_t *)(b + 16), (uint32_t *)(b + 20),
-                (uint32_t *)(b + 64), (uint32_t *)(b + 128), (uint32_t *)(b + 192)};
+                (uint32_t *)(b + 24), (uint32_t *)(b + 64), (uint32_t *)(b + 128), (uint32_t *)(b + 192)};
 }
 
 int ensure_aux_streams(fa_ctx *c) {
@@ -135,18 +136,21 @@ int ensure_aux_streams(fa_ctx *c) {
     return FA_OK;
 }
 
-// Extension launch: the int32 one-job-per-thread kernel, or on request the int16x2
-// two-jobs-per-thread kernel for bwa-form matrices.  Both are exact; the int32 kernel
-// is faster on B200 (the int16x2 one holds twice the shared memory per thread, so
-// half the warps), hence the default.
-// With `cert` the int32 kernel also evaluates the exit-bound certificate (flag bit 1),
-// which only the int32 kernel implements.
+// Extension launch: the int32 one-job-per-thread kernel, the two-rows-per-thread
+// int16x2 kernel (bwa-form matrices, queries up to 254 columns; jobs whose scores can pass
+// 255 go on to the int32 kernel in the same call), or the two-jobs-per-thread int16x2
+// kernel.  All are exact.  With `cert` the int32 kernel also evaluates the exit-bound
+// certificate (flag bit 1), which only the int32 kernel implements.
 using Choice = fa_ctx::Choice;
 
-cudaError_t launch_ext(Choice kc, const fa_job *d_jobs, const uint32_t *d_order, uint32_t n,
+cudaError_t launch_ext(fa_ctx *c, Choice kc, const fa_job *d_jobs, const uint32_t *d_order, uint32_t n,
                        const uint32_t *d_n, const uint8_t *d_q, const uint8_t *d_t, const ExtParams &kp, int qcap,
                        const int32_t *d_w_try, fa_ext_result *d_out, uint8_t *d_clamped, bool cert,
                        uint32_t *d_cells_job, unsigned long long *d_cells, uint32_t *d_status, cudaStream_t s) {
+    if (kc.kernel == FA_KERNEL_ROWS2 && !cert && ext_rows2_eligible(kp, qcap) &&
+        c->ovf.cap >= sizeof(uint32_t) * (size_t)n && c->misc.p)
+        return launch_ext_rows2(d_jobs, d_order, n, d_n, d_q, d_t, kp, qcap, d_w_try, d_out, d_clamped, d_cells_job,
+                                d_cells, d_status, c->ovf.as<uint32_t>(), misc_of(c).ovf_n, s, kc.tpb);
     if (kc.kernel == FA_KERNEL_INT16X2 && ext_pair_eligible(kp) && !cert)
         return launch_ext_pair(d_jobs, d_order, n, d_n, d_q, d_t, kp, qcap, d_w_try, d_out, d_clamped,
                                d_cells_job, d_cells, d_status, s);
@@ -157,19 +161,25 @@ cudaError_t launch_ext(Choice kc, const fa_job *d_jobs, const uint32_t *d_order,
 // The kernel a call runs.  A fixed setting is used as is.  FA_KERNEL_AUTO is an
 // autotuner: the first time a (query capacity class of 32 columns, configured band) pair
 // is seen, every exact candidate -- the int32 one-job-per-thread kernel with 64, 128 or
-// 256 threads per block, and the int16x2 two-jobs-per-thread kernel where the scoring
-// allows it -- runs twice on the first (longest) jobs of the call's order, and the
-// fastest is kept for that pair.  All candidates give identical results.
+// 256 threads per block, and where the scoring allows them the two-rows-per-thread
+// kernel with 64 or 128 and the two-jobs-per-thread kernel -- runs twice on the first
+// (longest) jobs of the call's order, and the fastest is kept for that pair.  All
+// candidates give identical results.
 Choice resolve_choice(fa_ctx *c, const ExtParams &kp, const fa_job *d_jobs, const uint32_t *d_order, uint32_t n,
                       const uint8_t *d_q, const uint8_t *d_t, int qcap, int band, fa_ext_result *d_out,
                       uint32_t *d_status, cudaStream_t s, int *rc) {
     *rc = FA_OK;
     if (c->kernel == FA_KERNEL_INT16X2) return c->last_choice = Choice{FA_KERNEL_INT16X2, kPairThreads};
     if (c->kernel == FA_KERNEL_INT32) return c->last_choice = Choice{FA_KERNEL_INT32, c->threads};
+    if (c->kernel == FA_KERNEL_ROWS2) return c->last_choice = Choice{FA_KERNEL_ROWS2, c->threads == 128 ? 128 : 64};
     const std::pair<int, int> key{(qcap + 31) / 32, band};
     auto it = c->tuned.find(key);
     if (it != c->tuned.end()) return c->last_choice = it->second;
     std::vector<Choice> cands{{FA_KERNEL_INT32, 64}, {FA_KERNEL_INT32, kExtThreads}, {FA_KERNEL_INT32, 256}};
+    if (ext_rows2_eligible(kp, qcap)) {
+        cands.push_back({FA_KERNEL_ROWS2, 64});
+        cands.push_back({FA_KERNEL_ROWS2, 128});
+    }
     if (ext_pair_eligible(kp)) cands.push_back({FA_KERNEL_INT16X2, kPairThreads});
     const uint32_t ns = std::min<uint32_t>(n, 131072);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -188,9 +198,12 @@ Choice resolve_choice(fa_ctx *c, const ExtParams &kp, const fa_job *d_jobs, cons
     for (const Choice &kc : cands) {
         if (kc.kernel == FA_KERNEL_INT32 && ext_packed_smem_bytes(qcap, 0, kc.tpb) > c->smem_optin) continue;
         if (kc.kernel == FA_KERNEL_INT16X2 && ext_pair_smem_bytes(qcap) > c->smem_optin) continue;
+        if (kc.kernel == FA_KERNEL_ROWS2 && (ext_rows2_smem_bytes(qcap, kc.tpb) > c->smem_optin ||
+                                             c->ovf.cap < sizeof(uint32_t) * (size_t)ns))
+            continue;
         for (int rep = 0; rep < 3; ++rep) {           // one warm-up, two timed
             if (rep == 1 && (e = cudaEventRecord(e0, s)) != cudaSuccess) return bail(e);
-            e = launch_ext(kc, d_jobs, d_order, ns, nullptr, d_q, d_t, kp, qcap, nullptr, d_out, nullptr, false,
+            e = launch_ext(c, kc, d_jobs, d_order, ns, nullptr, d_q, d_t, kp, qcap, nullptr, d_out, nullptr, false,
                            nullptr, nullptr, d_status, s);
             if (e != cudaSuccess) return bail(e);
         }
@@ -310,6 +323,7 @@ int ensure_ext_buffers(fa_ctx *c, uint32_t n, uint64_t qb, uint64_t tb) {
     FA_CUDA(c->out.ensure(sizeof(fa_ext_result) * (size_t)n));
     FA_CUDA(c->clamped.ensure(n));
     FA_CUDA(c->cells_job.ensure(sizeof(uint32_t) * (size_t)n));
+    FA_CUDA(c->ovf.ensure(sizeof(uint32_t) * (size_t)n));
     FA_CUDA(c->misc.ensure(kMiscBytes));
     return FA_OK;
 }
@@ -375,7 +389,7 @@ int enqueue_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n
     if (mode == FA_POLICY_SINGLE) {
         uint32_t b = 0;
         for (auto &sg : segs0) {
-            FA_CUDA(launch_ext(kc, d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp, sg.second,
+            FA_CUDA(launch_ext(c, kc, d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp, sg.second,
                                nullptr, d_out, nullptr, false, c->cells_job.as<uint32_t>(), m.cells, m.status, s));
             ++*launches;
             b = sg.first;
@@ -405,7 +419,7 @@ int enqueue_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n
         if (r == 0 && !learned) {
             uint32_t b = 0;
             for (auto &sg : segs0) {
-                FA_CUDA(launch_ext(kc, d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp, sg.second,
+                FA_CUDA(launch_ext(c, kc, d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp, sg.second,
                                    st.w_cur, d_out, d_flags, cert_r, c->cells_job.as<uint32_t>(), m.cells, m.status,
                                    s));
                 ++*launches;
@@ -417,7 +431,7 @@ int enqueue_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n
             FA_CUDA(launch_band_partition(d_jobs, list, cnt, n, st.w_cur, c->part_n.as<uint32_t>(),
                                           m.bucket_hist, m.bucket_cursor, m.group_bounds, s));
             if (c->kernel == FA_KERNEL_INT16X2) {
-                FA_CUDA(launch_ext(kc, d_jobs, c->part_n.as<uint32_t>(), n, cnt, d_q, d_t, kp, qcap_all,
+                FA_CUDA(launch_ext(c, kc, d_jobs, c->part_n.as<uint32_t>(), n, cnt, d_q, d_t, kp, qcap_all,
                                    st.w_cur, d_out, d_flags, cert_r, c->cells_job.as<uint32_t>(), m.cells,
                                    m.status, s));
                 *launches += 3;
@@ -428,7 +442,7 @@ int enqueue_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n
                 *launches += 5;
             }
         } else {
-            FA_CUDA(launch_ext(kc, d_jobs, list, n, cnt, d_q, d_t, kp, qcap_all, st.w_cur, d_out,
+            FA_CUDA(launch_ext(c, kc, d_jobs, list, n, cnt, d_q, d_t, kp, qcap_all, st.w_cur, d_out,
                                d_flags, cert_r, c->cells_job.as<uint32_t>(), m.cells, m.status, s));
             ++*launches;
         }
@@ -525,7 +539,7 @@ std::vector<uint64_t> graph_key(fa_ctx *c, const ExtParams &kp, const fa_policy 
     for (size_t i = 0; i < sizeof(ExtParams) / 4; ++i) k.push_back(kw[i]);
     for (DevBuf *b : {&c->jobs, &c->order, &c->qseq, &c->tseq, &c->out, &c->clamped, &c->cells_job, &c->misc,
                       &c->w_first, &c->w_cur, &c->prev, &c->kk, &c->w_final, &c->tries, &c->missed, &c->list_a,
-                      &c->list_b, &c->feat, &c->wbf, &c->part_n})
+                      &c->list_b, &c->feat, &c->wbf, &c->part_n, &c->ovf})
         k.push_back((uint64_t)(uintptr_t)b->p);
     k.insert(k.end(), extra.begin(), extra.end());
     return k;
@@ -648,7 +662,7 @@ int ext_batch_pipelined(fa_ctx *c, const ExtParams &kp, const fa_job *jobs, uint
         const uint32_t cnt = h_info[4 + k + 1] - h_info[4 + k];
         FA_CUDA(cudaStreamWaitEvent(s, c->slice_ev[k], 0));
         if (cnt == 0) continue;
-        FA_CUDA(launch_ext(kc, c->jobs.as<fa_job>(), c->order.as<uint32_t>() + h_info[4 + k], cnt, nullptr,
+        FA_CUDA(launch_ext(c, kc, c->jobs.as<fa_job>(), c->order.as<uint32_t>() + h_info[4 + k], cnt, nullptr,
                            c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(), kp, max_q, nullptr, c->out.as<fa_ext_result>(),
                            nullptr, false, c->cells_job.as<uint32_t>(), m.cells, m.status, s));
         ++launches;
@@ -698,7 +712,7 @@ void fa_ctx_destroy(fa_ctx *c) {
     for (DevBuf *b : {&c->jobs, &c->order, &c->qseq, &c->tseq, &c->out, &c->clamped, &c->cells_job,
                       &c->misc, &c->w_first, &c->w_cur, &c->prev, &c->kk, &c->w_final, &c->tries,
                       &c->missed, &c->list_a, &c->list_b, &c->hist, &c->feat, &c->wbf, &c->part_n,
-                      &c->part_w})
+                      &c->part_w, &c->ovf})
         b->release();
     for (int k = 0; k < 2; ++k) {
         if (c->join_ev[k]) cudaEventDestroy(c->join_ev[k]);
@@ -904,6 +918,7 @@ int fa_ext_batch_device(fa_ctx *c, const fa_params *p, const fa_job *d_jobs, uin
     const ExtParams kp = ext_params_of(p);
     cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
     FA_CUDA(c->misc.ensure(kMiscBytes));
+    FA_CUDA(c->ovf.ensure(sizeof(uint32_t) * (size_t)n));
     FA_CUDA(c->hist.ensure(sizeof(uint32_t) * (FA_MAX_QLEN + 1)));
     Misc m = misc_of(c);
     FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
@@ -945,7 +960,7 @@ int fa_ext_batch_device(fa_ctx *c, const fa_params *p, const fa_job *d_jobs, uin
     uint32_t b = 0;
     if (c->timing) FA_CUDA(cudaEventRecord(c->kev0, s));
     for (auto &sg : segs) {
-        FA_CUDA(launch_ext(kc, d_jobs, order + b, sg.first - b, nullptr, d_qseq, d_tseq, kp, sg.second,
+        FA_CUDA(launch_ext(c, kc, d_jobs, order + b, sg.first - b, nullptr, d_qseq, d_tseq, kp, sg.second,
                            nullptr, d_out, nullptr, false, nullptr, nullptr, m.status, s));
         b = sg.first;
     }
@@ -957,7 +972,7 @@ int fa_ext_batch_device(fa_ctx *c, const fa_params *p, const fa_job *d_jobs, uin
 
 int fa_ctx_set_kernel(fa_ctx *c, int kernel) {
     if (!c) return fail(FA_ERR_ARG, "null context");
-    if (kernel < FA_KERNEL_AUTO || kernel > FA_KERNEL_INT16X2)
+    if (kernel < FA_KERNEL_AUTO || kernel > FA_KERNEL_ROWS2)
         return fail(FA_ERR_ARG, "unknown kernel choice %d", kernel);
     c->kernel = kernel;
     c->tuned.clear();

@@ -190,20 +190,25 @@ int fa_ctx_sync(fa_ctx *ctx);
  * FA_KERNEL_AUTO     autotuned: the fastest exact candidate measured on the call's data;
  * FA_KERNEL_INT32    int32 cells, one job per thread;
  * FA_KERNEL_INT16X2  int16x2 cells, two jobs per thread, for bwa-form scoring matrices
- *                    (a on the diagonal with 1 <= a <= 3, -b off it, N = -1 or 0; else int32).
+ *                    (a on the diagonal with 1 <= a <= 3, -b off it, N = -1 or 0; else int32);
+ * FA_KERNEL_ROWS2    int16x2 cells, two target rows per thread with 8-bit column state,
+ *                    for bwa-form matrices and queries up to 254 bases; a job whose
+ *                    h0 + a * qlen exceeds 255 runs in the int32 kernel within the same call.
  * Every choice gives identical results. */
 #define FA_KERNEL_AUTO    0
 #define FA_KERNEL_INT32   1
 #define FA_KERNEL_INT16X2 2
+#define FA_KERNEL_ROWS2   3
 int fa_ctx_set_kernel(fa_ctx *ctx, int kernel);
-/* The kernel the last call ran (FA_KERNEL_INT32 / FA_KERNEL_INT16X2) and its threads per
+/* The kernel the last call ran (FA_KERNEL_INT32 / _INT16X2 / _ROWS2) and its threads per
  * block, and the last autotuning table (up to cap candidates: kernel, threads per block,
  * ms per sample run); *n_cand = 0 when no tuning has run.  With FA_KERNEL_AUTO (the
  * default) the first call of each (query capacity class, configured band) times every
  * exact candidate on its longest jobs and keeps the fastest. */
 int fa_ctx_kernel_choice(fa_ctx *ctx, int *kernel, int *threads_per_block, int cap, int *cand_kernel,
                          int *cand_threads, float *cand_ms, int *n_cand);
-/* Threads per block (64, 128 or 256) of the int32 kernel when FA_KERNEL_INT32 is set. */
+/* Threads per block (64, 128 or 256) of the int32 kernel when FA_KERNEL_INT32 is set;
+ * with FA_KERNEL_ROWS2, 128 selects 128 threads per block and any other value 64. */
 int fa_ctx_set_threads(fa_ctx *ctx, int threads_per_block);
 
 /* Graph mode (no reference counterpart): with it on, fa_ext_batch_policy and

@@ -1,22 +1,27 @@
-"""Builds tests/kernel_host/libpair_host.so: the extension kernels' thread bodies
-compiled for the host (nvcc, no GPU needed)."""
+"""Builds the test harnesses that compile extension kernels' thread bodies for the host
+(nvcc, no GPU needed): libpair_host.so (two jobs per thread) and librows2_host.so (two
+target rows per thread)."""
 import subprocess
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-SRC = HERE / "pair_host.cu"
-LIB = HERE / "libpair_host.so"
-DEPS = [SRC, HERE.parent.parent / "ferrousalign_b200" / "csrc" / "extend_pair_kernel.cu",
-        HERE.parent.parent / "ferrousalign_b200" / "csrc" / "fa_kernels.h",
-        HERE.parent.parent / "ferrousalign_b200" / "csrc" / "fa_device.cuh"]
+CSRC = HERE.parent.parent / "ferrousalign_b200" / "csrc"
+COMMON = [CSRC / "fa_kernels.h", CSRC / "fa_device.cuh"]
+HARNESSES = {
+    "pair": (HERE / "pair_host.cu", [CSRC / "extend_pair_kernel.cu"]),
+    "rows2": (HERE / "rows2_host.cu",
+              [CSRC / "extend_kernel.cu", CSRC / "extend_pair_kernel.cu", CSRC / "extend_rows2_kernel.cu"]),
+}
 
 
-def build() -> Path:
-    if LIB.exists() and all(d.stat().st_mtime <= LIB.stat().st_mtime for d in DEPS):
-        return LIB
+def build(name: str = "pair") -> Path:
+    src, deps = HARNESSES[name]
+    lib = HERE / f"lib{name}_host.so"
+    if lib.exists() and all(d.stat().st_mtime <= lib.stat().st_mtime for d in [src, *deps, *COMMON]):
+        return lib
     nvcc = "/usr/local/cuda/bin/nvcc" if Path("/usr/local/cuda/bin/nvcc").exists() else "nvcc"
-    tmp = LIB.with_suffix(".so.tmp")
+    tmp = lib.with_suffix(".so.tmp")
     subprocess.run([nvcc, "-std=c++17", "-O2", "-Xcompiler", "-fPIC", "-shared",
-                    "-gencode", "arch=compute_100a,code=sm_100a", "-o", str(tmp), str(SRC)], check=True)
-    tmp.replace(LIB)
-    return LIB
+                    "-gencode", "arch=compute_100a,code=sm_100a", "-o", str(tmp), str(src)], check=True)
+    tmp.replace(lib)
+    return lib

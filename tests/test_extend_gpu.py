@@ -93,10 +93,13 @@ def test_parameter_sweep_bit_exact(ctx, a, b_, n, gaps, w, zdrop, eb):
 
 
 @pytest.mark.parametrize("kernel,threads", [(N.FA_KERNEL_INT32, 64), (N.FA_KERNEL_INT32, 128),
-                                            (N.FA_KERNEL_INT32, 256), (N.FA_KERNEL_INT16X2, 128)])
+                                            (N.FA_KERNEL_INT32, 256), (N.FA_KERNEL_INT16X2, 128),
+                                            (N.FA_KERNEL_ROWS2, 64), (N.FA_KERNEL_ROWS2, 128)])
 def test_kernel_variants_bit_exact(ctx, kernel, threads):
     """Every autotuning candidate (int32 one job per thread at 64/128/256 threads per
-    block, int16x2 two jobs per thread) gives the oracle's results."""
+    block, int16x2 two jobs per thread, int16x2 two target rows per thread at 64/128)
+    gives the oracle's results, including reads past 254 bases and a = 3 scoring, where
+    the two-row kernel hands jobs on to the int32 kernel."""
     b = synth.workload_ext_1m(100_000, seed=31)
     p = fa.BandedPairWiseSW().to_struct()
     ctx.set_kernel(kernel)
@@ -112,7 +115,8 @@ def test_kernel_variants_bit_exact(ctx, kernel, threads):
     finally:
         ctx.set_kernel(N.FA_KERNEL_AUTO)
         ctx.set_threads(128)
-    assert choice["kernel"] == ("int32" if kernel == N.FA_KERNEL_INT32 else "int16x2")
+    assert choice["kernel"] == {N.FA_KERNEL_INT32: "int32", N.FA_KERNEL_INT16X2: "int16x2",
+                                N.FA_KERNEL_ROWS2: "rows2"}[kernel]
     assert np.array_equal(out, ref), diff_report(out, ref)
     assert stats["cells"] == tr["cells"].sum()
     assert np.array_equal(out2, ref2), diff_report(out2, ref2)
@@ -246,3 +250,26 @@ def test_autotuner_picks_a_measured_candidate():
         c.close()
     ref, _ = O.ext_batch(p, b.jobs, b.qseq, b.tseq)
     assert np.array_equal(out, ref) and np.array_equal(out2, ref)
+
+
+@pytest.mark.gpu
+def test_rows2_under_retry_policy_and_graph():
+    """The two-row kernel inside the bwa-mem2 retry rounds (device job counts, per-job
+    bands) and as a recorded CUDA graph: the oracle's results and bands."""
+    b = synth.workload_ext_1m(40_000, seed=35)
+    p = fa.BandedPairWiseSW(zdrop=40).to_struct()
+    pol = fa.make_policy(N.FA_POLICY_BWA, 2)
+    ref, rwfin, _, _ = O.ext_batch_policy(p, pol, b.jobs, b.qseq, b.tseq)
+    c = N.Context(0)
+    try:
+        c.set_kernel(N.FA_KERNEL_ROWS2)
+        out, _, wfin = fa.extend_batch(p, b.jobs, b.qseq, b.tseq, policy=pol, ctx=c)
+        c.set_graph(True)
+        outg, _, wfing = fa.extend_batch(p, b.jobs, b.qseq, b.tseq, policy=pol, ctx=c)
+        outg2, _, _ = fa.extend_batch(p, b.jobs, b.qseq, b.tseq, policy=pol, ctx=c)
+        assert c.kernel_choice()["kernel"] == "rows2"
+    finally:
+        c.close()
+    for o, wf in ((out, wfin), (outg, wfing), (outg2, wfing)):
+        assert np.array_equal(o, ref), diff_report(o, ref)
+        assert np.array_equal(wf, rwfin)

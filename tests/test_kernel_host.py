@@ -96,3 +96,96 @@ def test_golden_cases_as_pairs(host_lib):
         out, st = run_host(host_lib, p, jobs, qs, ts)
         ref, _ = O.ext_batch(p, jobs, qs, ts)
         assert np.array_equal(out, ref), (c0["name"], c1["name"], out, ref)
+
+
+# ---- two target rows per thread (extend_rows2_kernel.cu), same oracle
+
+
+@pytest.fixture(scope="module")
+def rows2_lib(built):
+    import build_host
+    lib = C.CDLL(str(build_host.build("rows2")))
+    lib.rows2_host_run.restype = C.c_int
+    lib.rows2_host_run.argtypes = [C.c_void_p] * 3 + [C.c_uint32, C.c_void_p, C.c_void_p, C.c_int] + [C.c_void_p] * 5
+    return lib
+
+
+def run_rows2(lib, p, jobs, qseq, tseq):
+    """Longest-first order in 32-column capacity classes; returns results, per-job cells,
+    status and the overflow jobs (the ones the kernel hands to the int32 kernel)."""
+    q = jobs["qlen"]
+    n = len(q)
+    order = np.array(sorted(range(n), key=lambda i: (-int(q[i]), i)), np.uint32)
+    out = np.zeros(n, N.EXT_RESULT_DT)
+    cells = np.zeros(n, np.uint32)
+    st = np.zeros(1, np.uint32)
+    ovf = np.zeros(n, np.uint32)
+    ovf_n = np.zeros(1, np.uint32)
+    s0 = 0
+    while s0 < n:
+        cap = (int(q[order[s0]]) + 31) // 32 * 32
+        e0 = s0
+        while e0 < n and q[order[e0]] > cap - 32:
+            e0 += 1
+        sub = np.ascontiguousarray(order[s0:e0])
+        rc = lib.rows2_host_run(p.ctypes.data, jobs.ctypes.data, sub.ctypes.data, len(sub), qseq.ctypes.data,
+                                tseq.ctypes.data, int(q[order[s0]]), out.ctypes.data, cells.ctypes.data,
+                                st.ctypes.data, ovf.ctypes.data, ovf_n.ctypes.data)
+        assert rc == 0
+        s0 = e0
+    return out, cells, int(st[0]), np.sort(ovf[:int(ovf_n[0])])
+
+
+def check_rows2(lib, p, jobs, qseq, tseq):
+    out, cells, st, ovf = run_rows2(lib, p, jobs, qseq, tseq)
+    ref, tr = O.ext_batch(p, jobs, qseq, tseq)
+    a = int(max(0, p["mat"][0].max()))
+    wide = np.nonzero(jobs["h0"].astype(np.int64) + a * jobs["qlen"].astype(np.int64) > 255)[0]
+    assert st == 0
+    assert np.array_equal(ovf, wide.astype(np.uint32))
+    keep = np.ones(len(jobs), bool)
+    keep[wide] = False
+    bad = np.nonzero(keep & (out != ref))[0]
+    assert len(bad) == 0, (bad[:10], out[bad[:3]], ref[bad[:3]])
+    assert np.array_equal(cells[keep], tr["cells"][keep].astype(np.uint32))
+    return int(keep.sum())
+
+
+def test_rows2_151bp_jobs(rows2_lib):
+    b = synth.workload_ext_plain(3000)
+    p = fa.BandedPairWiseSW().to_struct()
+    assert check_rows2(rows2_lib, p, b.jobs, b.qseq, b.tseq) == 3000
+
+
+@pytest.mark.parametrize("a,b_,n,gaps,w,zdrop", [(1, 4, -1, (6, 1, 6, 1), 100, 100), (2, 3, 0, (5, 2, 3, 1), 20, 30),
+                                                 (3, 1, -1, (0, 1, 2, 2), 7, 0), (1, 2, -1, (3, 3, 1, 1), 3, 5),
+                                                 (1, 4, 0, (6, 1, 6, 1), 1, 100)])
+def test_rows2_uneven_jobs_and_parameters(rows2_lib, a, b_, n, gaps, w, zdrop):
+    ref_seq = synth.reference(400_000, seed=12, n_rate=0.02, repeat_frac=0.05)
+    b = synth.ext_jobs(ref_seq, 2000, seed=19, read_len=(10, 160), seed_len=(3, 30), seed_at_start=False, w=w,
+                       indel_rates=(0.0, 0.02, 0.06), sub_rate=0.04)
+    sw = fa.BandedPairWiseSW(o_del=gaps[0], e_del=gaps[1], o_ins=gaps[2], e_ins=gaps[3], zdrop=zdrop,
+                             mat=fa.bwa_fill_scmat(a, b_, n))
+    assert check_rows2(rows2_lib, sw.to_struct(), b.jobs, b.qseq, b.tseq) > 200
+
+
+def test_rows2_golden_cases(rows2_lib):
+    """Every golden case with a bwa-form matrix, one job at a time."""
+    cases = [c for c in json.loads((HERE / "golden" / "ext_cases.json").read_text())
+             if c["mat"][0] in (1, 2, 3) and c["mat"][4] in (-1, 0) and all(
+                 c["mat"][t * 5 + q] == (c["mat"][4] if 4 in (t, q) else (c["mat"][0] if t == q else c["mat"][1]))
+                 for t in range(5) for q in range(5)) and (c["mat"][4] == 0 or c["mat"][1] <= -1)]
+    assert len(cases) > 10
+    for c in cases:
+        p = np.zeros(1, N.PARAMS_DT)
+        p["mat"][0] = np.array(c["mat"], np.int8)
+        p["m"] = 5
+        for k in ("o_del", "e_del", "o_ins", "e_ins", "zdrop", "end_bonus"):
+            p[k] = c[k]
+        qs = np.array(c["query"], np.uint8)
+        ts = np.array(c["target"] + [0], np.uint8)
+        jobs = np.zeros(1, N.JOB_DT)
+        jobs[0] = (0, 0, len(c["query"]), len(c["target"]), c["h0"], c["w"], 1, 0)
+        if len(c["query"]) > 254:
+            continue
+        check_rows2(rows2_lib, p, jobs, qs, ts)
