@@ -67,17 +67,26 @@ __host__ __device__ __forceinline__ uint32_t take_slot(uint32_t *cnt) {
 #endif
 }
 
+__host__ __device__ __forceinline__ uint32_t mulhi(uint32_t a, uint32_t b) {
+#ifdef __CUDA_ARCH__
+    return __umulhi(a, b);
+#else
+    return (uint32_t)(((uint64_t)a * b) >> 32);
+#endif
+}
+
 __host__ __device__ inline uint32_t dup16(int v) { return (uint32_t)(v & 0xFFFF) * 0x10001u; }
 
 }  // namespace
 
 constexpr int kRows2MaxQ = 254;   // u8 column words: h0 >= 1 and a >= 1 leave qlen <= 254
 
-// One job.  eh[c * T]: column word of column c (H | E << 8), c in [0, qcap]; sw[k * T]:
-// the selector bytes of columns 4k..4k+3.  Returns the cells the recurrence evaluated.
-template <int T>
+// One job.  eh[c * T]: column word of column c (H | E << 8), c in [0, qcap]; sb[c * T]: the
+// selector byte of query column c.  SYM: o_del + e_del == o_ins + e_ins and e_del == e_ins,
+// so E and F open from one shared term.  Returns the cells the recurrence evaluated.
+template <int T, bool SYM>
 __host__ __device__ __forceinline__ uint32_t rows2_thread(
-    uint32_t jid, uint16_t *__restrict__ eh, uint32_t *__restrict__ sw, const fa_job *__restrict__ jobs,
+    uint32_t jid, uint16_t *__restrict__ eh, uint8_t *__restrict__ sb, const fa_job *__restrict__ jobs,
     const uint8_t *__restrict__ qseq, const uint8_t *__restrict__ tseq, const ExtParams &p, int qcap,
     const int32_t *__restrict__ w_try, fa_ext_result *__restrict__ out, uint8_t *__restrict__ clamped_out,
     uint32_t *__restrict__ cells_job, uint32_t *__restrict__ status, uint32_t *__restrict__ ovf,
@@ -114,15 +123,11 @@ __host__ __device__ __forceinline__ uint32_t rows2_thread(
 #pragma unroll
                 for (int u = 0; u < 8; ++u) qb[u] = j0 + u < qlen ? (uint32_t)Q[j0 + u] : 0u;
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    uint32_t word = 0;
-#pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        const uint32_t q = qb[4 * h + u];
-                        if (j0 + 4 * h + u < qlen) bad |= q >= (uint32_t)p.m;
-                        word |= (q < 4u ? q * 0x11u + 0x80u : qn * 0x11u) << (8 * u);
+                for (int u = 0; u < 8; ++u) {
+                    if (j0 + u < qlen) {
+                        bad |= qb[u] >= (uint32_t)p.m;
+                        sb[(j0 + u) * T] = (uint8_t)(qb[u] < 4u ? qb[u] * 0x11u + 0x80u : qn * 0x11u);
                     }
-                    if (j0 + 4 * h < qlen) sw[((j0 >> 2) + h) * T] = word;
                 }
             }
             // first row (ksw_affine_gap.rs:1017-1025): h0, h0-oe_ins, then -e_ins while the
@@ -140,39 +145,53 @@ __host__ __device__ __forceinline__ uint32_t rows2_thread(
                     eh[j * T] = (uint16_t)h;
                 }
             }
-            auto sbyte = [&](int c) -> uint32_t { return (sw[(c >> 2) * T] >> (8 * (c & 3))) & 0xFFu; };
             auto score1 = [&](uint32_t t, int c) -> int {   // one cell of row t at column c
-                return (int)(int16_t)(prmt(TAB, TABN, sbyte(c) ^ (t * 0x11u)) & 0xFFFFu);
+                return (int)(int16_t)(prmt(TAB, TABN, (uint32_t)sb[c * T] ^ (t * 0x11u)) & 0xFFFFu);
             };
 
-            // pair state, int16x2: low half row i, high half row i+1 (one column behind)
-            uint32_t hpp = 0, hp = 0, ep = 0, f2 = 0, km = 0, lpk = 0, tsel = 0;
-            // one step: low half column j, high half column j-1; ow = row i+1's word for
-            // column j-1.  km: max over cells of H << 8 | (255 - column) (row max, first
-            // column); lpk (low half): last column with H > 0.
-            auto step = [&](uint32_t wd, uint32_t qsel, uint32_t jk, uint32_t jpos, uint32_t &ow) {
-                const uint32_t M2 = prmt(wd, hpp, 0x5420u);     // (H of row i-1 at j-1, H of row i at j-2)
-                const uint32_t e2 = prmt(wd, ep, 0x5421u);      // (E at j, row i's E for j-1)
+            // pair state, int16x2: low half row i, high half row i+1 (one column behind);
+            // sprev: the previous step's selector byte (the high half's query column)
+            uint32_t hpp = 0, hp = 0, ep = 0, f2 = 0, km = 0, lpk = 0, tsel = 0, sprev = 0;
+            // One step: low half column j, high half column j-1, from wd = eh[j] and sbj = sb[j].
+            // ow = row i+1's word for column j-1.  key = H << 8 | ck: the row max with its first
+            // column (ck counts down with the column); lpv = min(H << 8 + kk, 256 + kk): 256 + kk
+            // where the low row's H > 0 (its last such column).  Unpacking and the selector pair
+            // are multiply-adds, so they issue beside the DPX work.
+            auto core = [&](uint32_t wd, uint32_t sbj, uint32_t ck, uint32_t kk, uint32_t kk256, uint32_t &key,
+                            uint32_t &lpv, uint32_t &ow) {
+                const uint32_t E = mulhi(wd, 1u << 24);                   // row i-1's E byte
+                const uint32_t M2 = (hpp * 65536u + wd) - E * 256u;          // (H at j-1, row i's H at j-2)
+                const uint32_t e2 = ep * 65536u + E;                         // (E at j, row i's E for j-1)
+                const uint32_t qsel = sprev * 256u + sbj;
+                sprev = sbj;
                 const uint32_t s2 = prmt(TAB, TABN, qsel ^ tsel);
                 // ksw_extend2's `M ? M + s : 0`: for M > 0, kmul * M >= M + s; for M == 0 the
                 // result is <= 0, which acts as 0 in every max below (halves stay apart:
                 // 4 * 255 < 2^15)
                 const uint32_t Mp = __viaddmin_s16x2(M2, s2, M2 * kmul);
                 const uint32_t h2 = __vimax3_s16x2(Mp, e2, f2);
-                const uint32_t en2 = __viaddmax_s16x2(e2, NED, __viaddmax_s16x2_relu(Mp, NOED, 0u));
-                f2 = __viaddmax_s16x2(f2, NEI, __viaddmax_s16x2_relu(Mp, NOEI, 0u));
-                const uint32_t hs = h2 << 8;
-                km = __viaddmax_u16x2(hs, jk, km);
-                lpk = __viaddmax_u16x2(__viaddmin_u16x2(hs, 0u, jpos), 0u, lpk);
+                uint32_t en2;
+                if (SYM) {
+                    const uint32_t t = __viaddmax_s16x2_relu(Mp, NOED, 0u);
+                    en2 = __viaddmax_s16x2(e2, NED, t);
+                    f2 = __viaddmax_s16x2(f2, NED, t);
+                } else {
+                    en2 = __viaddmax_s16x2(e2, NED, __viaddmax_s16x2_relu(Mp, NOED, 0u));
+                    f2 = __viaddmax_s16x2(f2, NEI, __viaddmax_s16x2_relu(Mp, NOEI, 0u));
+                }
+                key = h2 * 256u + ck;
+                lpv = __viaddmin_u16x2(h2 * 256u, kk, kk256);
                 ow = prmt(hp, en2, 0x62u);                      // (H of row i+1 at j-2, its E for j-1)
                 hpp = hp;
                 hp = h2;
                 ep = en2;
             };
-            auto jk_of = [](int j) { return (uint32_t)(255 - j) | (uint32_t)((256 - j) & 0xFFFF) << 16; };
-            auto generic = [&](int j, uint32_t &ow) {
-                const uint32_t qsel = sbyte(j) | (j > 0 ? sbyte(j - 1) << 8 : 0u);
-                step((uint32_t)eh[j * T], qsel, jk_of(j), (uint32_t)j, ow);
+            // a single step at column j, folded into km / lpk at once
+            auto step1 = [&](int j, uint32_t &ow) {
+                uint32_t key, lpv;
+                core((uint32_t)eh[j * T], (uint32_t)sb[j * T], 0u, 0u, 256u, key, lpv, ow);
+                km = __viaddmax_u16x2(key, (uint32_t)(255 - j) | (uint32_t)((256 - j) & 0xFFFF) << 16, km);
+                lpk = __viaddmax_u16x2(lpv, (uint32_t)j, lpk);
             };
 
             int best = h0, max_i = -1, max_j = -1, max_ie = -1, gscore = -1, max_off = 0;
@@ -226,57 +245,61 @@ __host__ __device__ __forceinline__ uint32_t rows2_thread(
                 const int b0 = beg, e0 = end;
                 const int h1lo = b0 == 0 ? max(h0 - (p.o_del + e_del * (i + 1)), 0) : 0;
                 hpp = 0; hp = (uint32_t)h1lo; ep = 0; f2 = 0; km = 0; lpk = 0;
+                sprev = b0 > 0 ? (uint32_t)sb[(b0 - 1) * T] : 0u;
 
-                // ---- phase A: row i alone until row i+1's first column is known
+                // ---- phase A: row i alone until row i+1's first column is known (for the
+                // last row of an odd count the high half just runs along, unread).  A loop
+                // condition rather than a break, so the warp's threads reconverge after it
+                // (the break form ran 1.8x slower: threads in different phases interleaved).
                 int j = b0, hs_trim = -1, c0 = -1;
                 uint32_t ow;
-                while (j < e0) {
+                bool go = j < e0;
+                while (go) {
                     const uint32_t hprev = hp;
-                    generic(j, ow);
+                    step1(j, ow);
                     // row i's word for column j: (its H at j-1, its E for j)
-                    if (two && hs_trim < 0 && ((hprev | ep) & 0xFFFFu)) hs_trim = j;
+                    if (hs_trim < 0 && ((hprev | ep) & 0xFFFFu)) hs_trim = j;
+                    const bool start = !two || (hs_trim >= 0 && j >= i + 1 - w);
+                    c0 = start ? j : c0;
                     ++j;
-                    if (hs_trim >= 0 && j - 1 >= i + 1 - w) { c0 = j - 1; break; }
+                    go = !start && j < e0;
                 }
                 if (c0 >= 0) {
                     const int h1hi = c0 == 0 ? max(h0 - (p.o_del + e_del * (i + 2)), 0) : 0;
                     hp = (hp & 0xFFFFu) | (uint32_t)h1hi << 16;
                     f2 &= 0xFFFFu;
                     km &= 0xFFFFu;
-                    // ---- phase B: both rows; row i+1's word for column j-1 stored each step
-                    while (j < e0 && (j & 3)) {
-                        generic(j, ow);
-                        eh[(j - 1) * T] = (uint16_t)ow;
-                        ++j;
-                    }
-                    if (j + 3 < e0) {
-                        uint32_t swp = sw[((j >> 2) - 1) * T];
-                        uint32_t jk = jk_of(j);
-                        for (; j + 3 < e0; j += 4) {
-                            const uint32_t swc = sw[(j >> 2) * T];
-                            const uint32_t w0 = eh[j * T], w1 = eh[(j + 1) * T], w2 = eh[(j + 2) * T],
-                                           w3 = eh[(j + 3) * T];
-                            uint32_t o0, o1, o2, o3;
-                            step(w0, prmt(swc, swp, 0x70u), jk, (uint32_t)j, o0);
-                            step(w1, prmt(swc, swc, 0x01u), jk - 0x10001u, (uint32_t)(j + 1), o1);
-                            step(w2, prmt(swc, swc, 0x12u), jk - 0x20002u, (uint32_t)(j + 2), o2);
-                            step(w3, prmt(swc, swc, 0x23u), jk - 0x30003u, (uint32_t)(j + 3), o3);
-                            eh[(j - 1) * T] = (uint16_t)o0;
-                            eh[j * T] = (uint16_t)o1;
-                            eh[(j + 1) * T] = (uint16_t)o2;
-                            eh[(j + 2) * T] = (uint16_t)o3;
-                            swp = swc;
-                            jk -= 0x40004u;
-                        }
+                    // ---- phase B: both rows, four steps a group; row i+1's word for column
+                    // j-1 stored each step.  Group keys carry 3-k / k and are folded with the
+                    // group's first column.
+                    uint32_t kb = (uint32_t)(252 - j) | (uint32_t)((253 - j) & 0xFFFF) << 16;
+                    for (; j + 3 < e0; j += 4) {
+                        const uint32_t w0 = eh[j * T], w1 = eh[(j + 1) * T], w2 = eh[(j + 2) * T],
+                                       w3 = eh[(j + 3) * T];
+                        const uint32_t s0 = sb[j * T], s1 = sb[(j + 1) * T], s2 = sb[(j + 2) * T],
+                                       s3 = sb[(j + 3) * T];
+                        uint32_t k0, k1, k2, k3, l0, l1, l2, l3, o0, o1, o2, o3;
+                        core(w0, s0, 0x30003u, 0u, 256u, k0, l0, o0);
+                        core(w1, s1, 0x20002u, 1u, 257u, k1, l1, o1);
+                        core(w2, s2, 0x10001u, 2u, 258u, k2, l2, o2);
+                        core(w3, s3, 0u, 3u, 259u, k3, l3, o3);
+                        eh[(j - 1) * T] = (uint16_t)o0;
+                        eh[j * T] = (uint16_t)o1;
+                        eh[(j + 1) * T] = (uint16_t)o2;
+                        eh[(j + 2) * T] = (uint16_t)o3;
+                        km = __viaddmax_u16x2(__viaddmax_u16x2(k3, 0u, __vimax3_u16x2(k0, k1, k2)), kb, km);
+                        lpk = __viaddmax_u16x2(__viaddmax_u16x2(l3, 0u, __vimax3_u16x2(l0, l1, l2)), (uint32_t)j,
+                                               lpk);
+                        kb -= 0x40004u;
                     }
                     while (j < e0) {
-                        generic(j, ow);
+                        step1(j, ow);
                         eh[(j - 1) * T] = (uint16_t)ow;
                         ++j;
                     }
                 }
 
-                // ---- row i ends (hp's low half: H at e0-1, or the row's h1 when empty)
+            // ---- row i ends (hp's low half: H at e0-1, or the row's h1 when empty)
                 const int hlast = (int)(hp & 0xFFFFu);
                 if (e0 > b0) cells += e0 - b0;
                 if (e0 == qlen && gscore < hlast) { gscore = hlast; max_ie = i; }
@@ -284,7 +307,7 @@ __host__ __device__ __forceinline__ uint32_t rows2_thread(
                 if (!two) break;
 
                 // ---- row i+1: band from row i's words
-                const int lp = (int)(lpk & 0xFFFFu);   // row i's last column with H > 0
+                const int lp = (int)(lpk & 0xFFFFu) - 256;   // row i's last column with H > 0
                 int b1 = hs_trim >= 0 ? hs_trim : e0;
                 int e1 = lp + 3 < qlen ? lp + 3 : qlen;
                 {
@@ -349,7 +372,7 @@ __host__ __device__ __forceinline__ uint32_t rows2_thread(
     return cells;
 }
 
-template <int TPB>
+template <int TPB, bool SYM>
 __global__ void __launch_bounds__(TPB)
 ext_rows2_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ order, uint32_t n,
                  const uint32_t *__restrict__ n_dev, const uint8_t *__restrict__ qseq,
@@ -365,9 +388,9 @@ ext_rows2_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ o
     if (n_dev) n = min(n, *n_dev);
     if (gi < n) {
         uint16_t *eh = reinterpret_cast<uint16_t *>(smem) + threadIdx.x;
-        uint32_t *sw = smem + (qcap + 1) * (TPB / 2) + threadIdx.x;
-        cells = rows2_thread<TPB>(order ? order[gi] : gi, eh, sw, jobs, qseq, tseq, p, qcap, w_try, out,
-                                  clamped_out, cells_job, status, ovf, ovf_n);
+        uint8_t *sb = reinterpret_cast<uint8_t *>(smem) + (size_t)(qcap + 1) * TPB * 2 + threadIdx.x;
+        cells = rows2_thread<TPB, SYM>(order ? order[gi] : gi, eh, sb, jobs, qseq, tseq, p, qcap, w_try, out,
+                                       clamped_out, cells_job, status, ovf, ovf_n);
     }
     if (cells_out) {
         unsigned long long c = cells;
@@ -377,8 +400,12 @@ ext_rows2_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ o
     }
 }
 
+bool ext_rows2_sym(const ExtParams &p) {
+    return p.o_del + p.e_del == p.o_ins + p.e_ins && p.e_del == p.e_ins;
+}
+
 size_t ext_rows2_smem_bytes(int qcap, int tpb) {
-    return (size_t)(qcap + 1) * tpb * sizeof(uint16_t) + (size_t)((qcap + 3) / 4) * tpb * sizeof(uint32_t);
+    return (size_t)(qcap + 1) * tpb * sizeof(uint16_t) + (size_t)(qcap + 3) / 4 * 4 * tpb;
 }
 
 bool ext_rows2_eligible(const ExtParams &p, int qcap) {
@@ -386,18 +413,18 @@ bool ext_rows2_eligible(const ExtParams &p, int qcap) {
 }
 
 namespace {
-template <int TPB>
+template <int TPB, bool SYM>
 cudaError_t launch_rows2_variant(size_t smem, cudaStream_t stream, const fa_job *d_jobs, const uint32_t *d_order,
                                  uint32_t n, const uint32_t *d_n, const uint8_t *d_qseq, const uint8_t *d_tseq,
                                  const ExtParams &p, int qcap, const int32_t *d_w_try, fa_ext_result *d_out,
                                  uint8_t *d_clamped, uint32_t *d_cells_job, unsigned long long *d_cells,
                                  uint32_t *d_status, uint32_t *d_ovf, uint32_t *d_ovf_n)
 {
-    cudaError_t err = cudaFuncSetAttribute(ext_rows2_kernel<TPB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t err = cudaFuncSetAttribute(ext_rows2_kernel<TPB, SYM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)smem);
     if (err != cudaSuccess) return err;
     const uint32_t blocks = (n + TPB - 1) / TPB;
-    ext_rows2_kernel<TPB><<<blocks, TPB, smem, stream>>>(d_jobs, d_order, n, d_n, d_qseq, d_tseq, p, qcap, d_w_try,
+    ext_rows2_kernel<TPB, SYM><<<blocks, TPB, smem, stream>>>(d_jobs, d_order, n, d_n, d_qseq, d_tseq, p, qcap, d_w_try,
                                                          d_out, d_clamped, d_cells_job, d_cells, d_status, d_ovf,
                                                          d_ovf_n);
     return cudaGetLastError();
@@ -416,10 +443,13 @@ cudaError_t launch_ext_rows2(const fa_job *d_jobs, const uint32_t *d_order, uint
     if (err != cudaSuccess) return err;
     const int t = tpb == 128 ? 128 : 64;
     const size_t smem = ext_rows2_smem_bytes(qcap, t);
-    err = t == 128 ? launch_rows2_variant<128>(smem, stream, d_jobs, d_order, n, d_n, d_qseq, d_tseq, p, qcap, d_w_try,
-                                               d_out, d_clamped, d_cells_job, d_cells, d_status, d_ovf, d_ovf_n)
-                   : launch_rows2_variant<64>(smem, stream, d_jobs, d_order, n, d_n, d_qseq, d_tseq, p, qcap, d_w_try,
-                                              d_out, d_clamped, d_cells_job, d_cells, d_status, d_ovf, d_ovf_n);
+#define FA_ROWS2(TV, SV) launch_rows2_variant<TV, SV>(smem, stream, d_jobs, d_order, n, d_n, d_qseq, d_tseq, p, qcap, \
+                                                     d_w_try, d_out, d_clamped, d_cells_job, d_cells, d_status, d_ovf, \
+                                                     d_ovf_n)
+    const bool sym = ext_rows2_sym(p);
+    if (t == 128) err = sym ? FA_ROWS2(128, true) : FA_ROWS2(128, false);
+    else err = sym ? FA_ROWS2(64, true) : FA_ROWS2(64, false);
+#undef FA_ROWS2
     if (err != cudaSuccess) return err;
     // jobs whose scores can pass 255: the int32 kernel over the overflow list
     return launch_ext_packed(d_jobs, d_ovf, n, nullptr, d_ovf_n, d_qseq, d_tseq, p, qcap, 0, d_w_try, d_out,

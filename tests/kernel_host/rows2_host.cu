@@ -20,9 +20,12 @@ extern "C" int rows2_host_run(const fa_params *prm, const fa_job *jobs, const ui
     k.max_score = ms;
     if (!fa::ext_rows2_eligible(k, qcap)) return -1;
     std::vector<uint16_t> eh((size_t)qcap + 1);
-    std::vector<uint32_t> sw((size_t)(qcap + 3) / 4);
+    std::vector<uint8_t> sb((size_t)qcap + 1);
+    const bool sym = fa::ext_rows2_sym(k);
     for (uint32_t g = 0; g < n; ++g)
-        cells[order[g]] = fa::rows2_thread<1>(order[g], eh.data(), sw.data(), jobs, qseq, tseq, k, qcap, nullptr,
-                                              out, nullptr, nullptr, status, ovf, ovf_n);
+        cells[order[g]] = sym ? fa::rows2_thread<1, true>(order[g], eh.data(), sb.data(), jobs, qseq, tseq, k, qcap,
+                                                          nullptr, out, nullptr, nullptr, status, ovf, ovf_n)
+                              : fa::rows2_thread<1, false>(order[g], eh.data(), sb.data(), jobs, qseq, tseq, k, qcap,
+                                                           nullptr, out, nullptr, nullptr, status, ovf, ovf_n);
     return 0;
 }
