@@ -38,9 +38,13 @@ METRIC = "GCUPS & alignments/s @151bp, learned-band vs plain-band on B200, bit-e
 N_JOBS = 1_000_000
 CPU_SAMPLE = 200_000
 MATE_JOBS = 500_000
-# ncu: ext_packed_kernel<0,0,128> on 439,186 jobs of the 151-bp workload read 248.1 MB and
-# wrote 11.2 MB of DRAM (the algorithmic bytes are about 372 B per job)
-EXT_DRAM_BYTES_PER_JOB = (248.106e6 + 11.161e6) / 439_186
+# DRAM bytes per job of the extension kernels (ncu dram__bytes_read.sum + write.sum of one
+# launch on the 151-bp workload; the algorithmic bytes are about 372 B per job):
+# ext_packed_kernel (int32, 439,186 jobs): 248.1 MB + 11.2 MB;
+# ext_rows2_kernel (two rows per thread, 175,709 jobs): 72.3 MB + 2.5 MB
+EXT_KERNELS = {"int32": ("ext_packed_kernel", (248.106e6 + 11.161e6) / 439_186, "int32"),
+               "rows2": ("ext_rows2_kernel", (72.319e6 + 2.543e6) / 175_709, "int16x2"),
+               "int16x2": ("ext_pair_kernel", None, "int16x2")}
 UNEVEN_JOBS = 2_000_000
 MATE_CPU_SAMPLE = 20_000
 DPX_OPS_PER_CELL_PAIR = 9   # int16x2 ops per packed cell pair in the roofline model
@@ -519,10 +523,11 @@ def main():
     gcups_step = cells * ws / (ms_step * 1e-3) / 1e9
     bytes_in = int(b.jobs.nbytes + b.qseq.nbytes + b.tseq.nbytes)
     bytes_out = n * 24
+    kname, kbytes, kdtype = EXT_KERNELS.get(tune_dev["kernel"], ("ext_packed_kernel", None, "int32"))
     line = {
         "metric": METRIC, "value": value, "unit": "alignments/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "vs_baseline": None, "dtype": kdtype, "data": "synthetic",
         "config": {"workload": "1M right extensions, 151 bp reads, indel rate {0,0.1,1,3}%, w=100",
                    "jobs_per_gpu": n, "w": 100, "zdrop": 100, "end_bonus": 5, "scoring": "A1 B4 N-1 O6 E1",
                    "l2": "inputs (%d MB) larger than L2; 256 MB flush between steps" % (bytes_in // 10**6),
@@ -530,13 +535,12 @@ def main():
         "gcups": gcups_step,
         "bit_exact_sample": exact,
         "roofline": {"bound": "dpx", "achieved": achieved_gcups, "peak": peak_gcups, "unit": "Gcell/s",
-                     "kernel": "ext_packed_kernel", "kernel_ms_per_step": kernel_ms,
-                     "launches_per_step": 2,
+                     "kernel": kname, "kernel_ms_per_step": kernel_ms,
+                     "launches_per_step": launches / max(1, args.steps),
                      "frac": achieved_gcups / peak_gcups,
                      # DRAM bytes of one step's extension launches: the per-job read + write
-                     # traffic of one ncu capture of ext_packed_kernel (500k-job launch,
-                     # profiles/ext_packed_kernel_1M_151bp.md) times the step's jobs
-                     "traffic": EXT_DRAM_BYTES_PER_JOB * n,
+                     # traffic of one ncu capture of that kernel (profiles/) times the step's jobs
+                     "traffic": kbytes * n if kbytes else None,
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per job, scaled",
                      "peak_source": f"measured __viaddmax_s16x2_relu rate {peak_ops / 1e12:.2f} Tops/s x2/"
                                     f"{DPX_OPS_PER_CELL_PAIR}; s32 DPX {peak_s32 / 1e12:.2f} Tops/s",

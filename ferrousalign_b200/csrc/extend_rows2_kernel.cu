@@ -269,11 +269,31 @@ __host__ __device__ __forceinline__ uint32_t rows2_thread(
                     hp = (hp & 0xFFFFu) | (uint32_t)h1hi << 16;
                     f2 &= 0xFFFFu;
                     km &= 0xFFFFu;
-                    // ---- phase B: both rows, four steps a group; row i+1's word for column
-                    // j-1 stored each step.  Group keys carry 3-k / k and are folded with the
-                    // group's first column.
-                    uint32_t kb = (uint32_t)(252 - j) | (uint32_t)((253 - j) & 0xFFFF) << 16;
-                    for (; j + 3 < e0; j += 4) {
+                    // ---- phase B: both rows, eight steps a group (then one of four); row
+                    // i+1's word for column j-1 stored each step.  Group keys carry (size-1-k) and
+                    // k and are folded with the group's first column.
+                    for (; j + 7 < e0; j += 8) {
+                        uint32_t wv[8], sv[8], kv[8], lv[8], ov[8];
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) { wv[k] = eh[(j + k) * T]; sv[k] = sb[(j + k) * T]; }
+#pragma unroll
+                        for (int k = 0; k < 8; ++k)
+                            core(wv[k], sv[k], (uint32_t)(7 - k) * 0x10001u, (uint32_t)k, 256u + k, kv[k], lv[k],
+                                 ov[k]);
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) eh[(j - 1 + k) * T] = (uint16_t)ov[k];
+                        const uint32_t kb8 = (uint32_t)(248 - j) | (uint32_t)((249 - j) & 0xFFFF) << 16;
+                        const uint32_t kg = __vimax3_u16x2(__vimax3_u16x2(kv[0], kv[1], kv[2]),
+                                                           __vimax3_u16x2(kv[3], kv[4], kv[5]),
+                                                           __vimax3_u16x2(kv[6], kv[7], kv[7]));
+                        const uint32_t lg = __vimax3_u16x2(__vimax3_u16x2(lv[0], lv[1], lv[2]),
+                                                           __vimax3_u16x2(lv[3], lv[4], lv[5]),
+                                                           __vimax3_u16x2(lv[6], lv[7], lv[7]));
+                        km = __viaddmax_u16x2(kg, kb8, km);
+                        lpk = __viaddmax_u16x2(lg, (uint32_t)j, lpk);
+                    }
+                    if (j + 3 < e0) {
+                        const uint32_t kb = (uint32_t)(252 - j) | (uint32_t)((253 - j) & 0xFFFF) << 16;
                         const uint32_t w0 = eh[j * T], w1 = eh[(j + 1) * T], w2 = eh[(j + 2) * T],
                                        w3 = eh[(j + 3) * T];
                         const uint32_t s0 = sb[j * T], s1 = sb[(j + 1) * T], s2 = sb[(j + 2) * T],
@@ -290,7 +310,7 @@ __host__ __device__ __forceinline__ uint32_t rows2_thread(
                         km = __viaddmax_u16x2(__viaddmax_u16x2(k3, 0u, __vimax3_u16x2(k0, k1, k2)), kb, km);
                         lpk = __viaddmax_u16x2(__viaddmax_u16x2(l3, 0u, __vimax3_u16x2(l0, l1, l2)), (uint32_t)j,
                                                lpk);
-                        kb -= 0x40004u;
+                        j += 4;
                     }
                     while (j < e0) {
                         step1(j, ow);

@@ -158,6 +158,11 @@ cudaError_t launch_ext(fa_ctx *c, Choice kc, const fa_job *d_jobs, const uint32_
                              cert, d_cells_job, d_cells, d_status, s, kc.tpb);
 }
 
+// Kernel launches one launch_ext call makes (the two-row kernel adds its overflow pass).
+uint32_t ext_kernels_of(Choice kc, const ExtParams &kp, int qcap) {
+    return kc.kernel == FA_KERNEL_ROWS2 && ext_rows2_eligible(kp, qcap) ? 2u : 1u;
+}
+
 // The kernel a call runs.  A fixed setting is used as is.  FA_KERNEL_AUTO is an
 // autotuner: the first time a (query capacity class of 32 columns, configured band) pair
 // is seen, every exact candidate -- the int32 one-job-per-thread kernel with 64, 128 or
@@ -380,18 +385,21 @@ int enqueue_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n
                 const std::vector<std::pair<uint32_t, int>> &segs, int qcap_all, int max_w, const fa_job *d_jobs,
                 const uint32_t *d_order, const uint8_t *d_q, const uint8_t *d_t, const int32_t *d_wfirst,
                 fa_ext_result *d_out, cudaStream_t s, bool capture, uint32_t *launches, uint32_t *retries,
-                Choice kc) {
+                Choice kc, const std::vector<Choice> *seg_kc = nullptr) {
     Misc m = misc_of(c);
     FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
     const int mode = pol ? pol->mode : FA_POLICY_SINGLE;
     const std::vector<std::pair<uint32_t, int>> one_seg{{n, qcap_all}};
     const auto &segs0 = capture ? one_seg : segs;
+    // first-round kernel of each capacity class (tuned per class); retries use kc
+    auto kc_of = [&](size_t k) { return !capture && seg_kc && k < seg_kc->size() ? (*seg_kc)[k] : kc; };
     if (mode == FA_POLICY_SINGLE) {
         uint32_t b = 0;
-        for (auto &sg : segs0) {
-            FA_CUDA(launch_ext(c, kc, d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp, sg.second,
+        for (size_t k = 0; k < segs0.size(); ++k) {
+            const auto &sg = segs0[k];
+            FA_CUDA(launch_ext(c, kc_of(k), d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp, sg.second,
                                nullptr, d_out, nullptr, false, c->cells_job.as<uint32_t>(), m.cells, m.status, s));
-            ++*launches;
+            *launches += ext_kernels_of(kc_of(k), kp, sg.second);
             b = sg.first;
         }
         return FA_OK;
@@ -418,13 +426,20 @@ int enqueue_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n
         const bool cert_r = cert && !(once && r >= narrow_rounds);
         if (r == 0 && !learned) {
             uint32_t b = 0;
-            for (auto &sg : segs0) {
-                FA_CUDA(launch_ext(c, kc, d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp, sg.second,
+            for (size_t k = 0; k < segs0.size(); ++k) {
+                const auto &sg = segs0[k];
+                FA_CUDA(launch_ext(c, kc_of(k), d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp, sg.second,
                                    st.w_cur, d_out, d_flags, cert_r, c->cells_job.as<uint32_t>(), m.cells, m.status,
                                    s));
-                ++*launches;
+                *launches += ext_kernels_of(kc_of(k), kp, sg.second);
                 b = sg.first;
             }
+        } else if (learned && !cert_r && c->kernel != FA_KERNEL_INT16X2) {
+            // after the narrow tries every job left runs the plain policy: one launch of the
+            // call's autotuned kernel over the compacted list
+            FA_CUDA(launch_ext(c, kc, d_jobs, list, n, cnt, d_q, d_t, kp, qcap_all, st.w_cur, d_out, d_flags, false,
+                               c->cells_job.as<uint32_t>(), m.cells, m.status, s));
+            *launches += ext_kernels_of(kc, kp, qcap_all);
         } else if (learned) {
             // band buckets (configured band first, then narrow bands decreasing), then the
             // three band groups concurrently
@@ -444,7 +459,7 @@ int enqueue_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n
         } else {
             FA_CUDA(launch_ext(c, kc, d_jobs, list, n, cnt, d_q, d_t, kp, qcap_all, st.w_cur, d_out,
                                d_flags, cert_r, c->cells_job.as<uint32_t>(), m.cells, m.status, s));
-            ++*launches;
+            *launches += cert_r ? 1u : ext_kernels_of(kc, kp, qcap_all);
         }
         FA_CUDA(cudaMemsetAsync(next_cnt, 0, 4, s));
         FA_CUDA(launch_policy_step(d_jobs, list, nullptr, cnt, n, d_out, d_flags, st, max_tries,
@@ -520,9 +535,22 @@ int run_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n,
     const Choice kc = resolve_choice(c, kp, d_jobs, d_order, n, d_q, d_t, qcap_all, band, d_out, misc_of(c).status, s,
                                      &rc0);
     if (rc0) return rc0;
+    // each capacity class gets its own tuned choice (a class the two-row kernel cannot hold
+    // does not decide for the others)
+    std::vector<Choice> seg_kc;
+    {
+        uint32_t b = 0;
+        for (auto &sg : segs) {
+            seg_kc.push_back(resolve_choice(c, kp, d_jobs, d_order + b, sg.first - b, d_q, d_t, sg.second, band, d_out,
+                                            misc_of(c).status, s, &rc0));
+            if (rc0) return rc0;
+            b = sg.first;
+        }
+        c->last_choice = kc;
+    }
     FA_CUDA(cudaEventRecord(c->ev0, s));
     if (int rc = enqueue_ext(c, kp, pol, n, segs, qcap_all, 0, d_jobs, d_order, d_q, d_t, d_wfirst, d_out, s, false,
-                             &launches, &retries, kc))
+                             &launches, &retries, kc, &seg_kc))
         return rc;
     FA_CUDA(cudaEventRecord(c->ev1, s));
     return finish_ext(c, pol, n, s, stats, h_wfinal, launches, retries, false);
@@ -957,15 +985,28 @@ int fa_ext_batch_device(fa_ctx *c, const fa_params *p, const fa_job *d_jobs, uin
     const Choice kc = resolve_choice(c, kp, d_jobs, order, n, d_qseq, d_tseq, segs.empty() ? 0 : segs.front().second,
                                      -1, d_out, m.status, s, &rc0);
     if (rc0) return rc0;
+    std::vector<Choice> seg_kc;
+    {
+        uint32_t b = 0;
+        for (auto &sg : segs) {
+            seg_kc.push_back(resolve_choice(c, kp, d_jobs, order + b, sg.first - b, d_qseq, d_tseq, sg.second, -1,
+                                            d_out, m.status, s, &rc0));
+            if (rc0) return rc0;
+            b = sg.first;
+        }
+        c->last_choice = kc;
+    }
     uint32_t b = 0;
     if (c->timing) FA_CUDA(cudaEventRecord(c->kev0, s));
-    for (auto &sg : segs) {
-        FA_CUDA(launch_ext(c, kc, d_jobs, order + b, sg.first - b, nullptr, d_qseq, d_tseq, kp, sg.second,
+    for (size_t k = 0; k < segs.size(); ++k) {
+        const auto &sg = segs[k];
+        FA_CUDA(launch_ext(c, seg_kc[k], d_jobs, order + b, sg.first - b, nullptr, d_qseq, d_tseq, kp, sg.second,
                            nullptr, d_out, nullptr, false, nullptr, nullptr, m.status, s));
         b = sg.first;
     }
     if (c->timing) FA_CUDA(cudaEventRecord(c->kev1, s));
-    c->last_launches = (uint32_t)segs.size() + (d_order ? 1u : 2u);
+    c->last_launches = d_order ? 1u : 2u;
+    for (size_t k = 0; k < segs.size(); ++k) c->last_launches += ext_kernels_of(seg_kc[k], kp, segs[k].second);
     c->last_stream = s;
     return FA_OK;
 }
