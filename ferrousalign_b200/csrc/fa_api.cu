@@ -112,7 +112,8 @@ int fa::fa_ctx_device(const fa_ctx *c) { return c->device; }
 namespace {
 
 // misc buffer layout (bytes): [0] status u32, [8] cells u64, [16] count A, [20] count B,
-// [24] two-row kernel overflow count, [64] band-bucket histogram u32[kBandBuckets],
+// [24..35] two-row kernel overflow counts (one per concurrent band group), [64] band-bucket
+// histogram u32[kBandBuckets],
 // [128] band-bucket cursors u32[kBandBuckets], [192] band-group bounds u32[3]
 constexpr size_t kMiscBytes = 256;
 struct Misc {
@@ -149,8 +150,9 @@ cudaError_t launch_ext(fa_ctx *c, Choice kc, const fa_job *d_jobs, const uint32_
                        uint32_t *d_cells_job, unsigned long long *d_cells, uint32_t *d_status, cudaStream_t s) {
     if (kc.kernel == FA_KERNEL_ROWS2 && !cert && ext_rows2_eligible(kp, qcap) &&
         c->ovf.cap >= sizeof(uint32_t) * (size_t)n && c->misc.p)
-        return launch_ext_rows2(d_jobs, d_order, n, d_n, d_q, d_t, kp, qcap, d_w_try, d_out, d_clamped, d_cells_job,
-                                d_cells, d_status, c->ovf.as<uint32_t>(), misc_of(c).ovf_n, s, kc.tpb);
+        return launch_ext_rows2(d_jobs, d_order, n, nullptr, d_n, d_q, d_t, kp, qcap, 0, false, d_w_try, d_out,
+                                d_clamped, d_cells_job, d_cells, d_status, c->ovf.as<uint32_t>(), misc_of(c).ovf_n, s,
+                                kc.tpb);
     if (kc.kernel == FA_KERNEL_INT16X2 && ext_pair_eligible(kp) && !cert)
         return launch_ext_pair(d_jobs, d_order, n, d_n, d_q, d_t, kp, qcap, d_w_try, d_out, d_clamped,
                                d_cells_job, d_cells, d_status, s);
@@ -203,7 +205,7 @@ Choice resolve_choice(fa_ctx *c, const ExtParams &kp, const fa_job *d_jobs, cons
     for (const Choice &kc : cands) {
         if (kc.kernel == FA_KERNEL_INT32 && ext_packed_smem_bytes(qcap, 0, kc.tpb) > c->smem_optin) continue;
         if (kc.kernel == FA_KERNEL_INT16X2 && ext_pair_smem_bytes(qcap) > c->smem_optin) continue;
-        if (kc.kernel == FA_KERNEL_ROWS2 && (ext_rows2_smem_bytes(qcap, kc.tpb) > c->smem_optin ||
+        if (kc.kernel == FA_KERNEL_ROWS2 && (ext_rows2_smem_bytes(qcap, kc.tpb, 0) > c->smem_optin ||
                                              c->ovf.cap < sizeof(uint32_t) * (size_t)ns))
             continue;
         for (int rep = 0; rep < 3; ++rep) {           // one warm-up, two timed
@@ -228,21 +230,32 @@ Choice resolve_choice(fa_ctx *c, const ExtParams &kp, const fa_job *d_jobs, cons
 
 // One learned round over a band-partitioned list: configured-band and wide narrow jobs
 // in the full-row kernel, bands 13-24 in the 64-column ring kernel, bands <= 12 in the
-// 32-column ring kernel; the three run concurrently on forked streams.
+// 32-column ring kernel; the three run concurrently on forked streams.  The two-row
+// kernels run them where the scoring allows (each group with its own overflow list), the
+// int32 kernels otherwise or when int32 is the fixed choice.
 int launch_learned_round(fa_ctx *c, const fa_job *d_jobs, const uint32_t *d_list, uint32_t n_max,
                          const uint8_t *d_q, const uint8_t *d_t, const ExtParams &kp, int qcap,
                          const int32_t *d_w_cur, fa_ext_result *d_out, uint8_t *d_flags, bool cert, Misc &m,
                          cudaStream_t s) {
     if (int rc = ensure_aux_streams(c)) return rc;
     const uint32_t *g = m.group_bounds;
+    const bool rows2 = c->kernel != FA_KERNEL_INT32 && ext_rows2_eligible(kp, qcap) &&
+                       c->ovf.cap >= 3 * sizeof(uint32_t) * (size_t)n_max;
+    auto group = [&](int k, int ring, cudaStream_t st) -> cudaError_t {
+        const uint32_t *first = k == 0 ? nullptr : g + k - 1;
+        if (rows2)
+            return launch_ext_rows2(d_jobs, d_list, n_max, first, g + k, d_q, d_t, kp, qcap, ring, cert, d_w_cur,
+                                    d_out, d_flags, c->cells_job.as<uint32_t>(), m.cells, m.status,
+                                    c->ovf.as<uint32_t>() + (size_t)k * n_max, m.ovf_n + k, st, 64);
+        return launch_ext_packed(d_jobs, d_list, n_max, first, g + k, d_q, d_t, kp, qcap, ring, d_w_cur, d_out,
+                                 d_flags, cert, c->cells_job.as<uint32_t>(), m.cells, m.status, st);
+    };
     FA_CUDA(cudaEventRecord(c->fork_ev, s));
-    FA_CUDA(launch_ext_packed(d_jobs, d_list, n_max, nullptr, g + 0, d_q, d_t, kp, qcap, 0, d_w_cur, d_out, d_flags,
-                              cert, c->cells_job.as<uint32_t>(), m.cells, m.status, s));
+    FA_CUDA(group(0, 0, s));
     const int rings[2] = {64, 32};
     for (int k = 0; k < 2; ++k) {
         FA_CUDA(cudaStreamWaitEvent(c->aux[k], c->fork_ev, 0));
-        FA_CUDA(launch_ext_packed(d_jobs, d_list, n_max, g + k, g + k + 1, d_q, d_t, kp, qcap, rings[k], d_w_cur,
-                                  d_out, d_flags, cert, c->cells_job.as<uint32_t>(), m.cells, m.status, c->aux[k]));
+        FA_CUDA(group(k + 1, rings[k], c->aux[k]));
         FA_CUDA(cudaEventRecord(c->join_ev[k], c->aux[k]));
         FA_CUDA(cudaStreamWaitEvent(s, c->join_ev[k], 0));
     }
@@ -328,7 +341,7 @@ int ensure_ext_buffers(fa_ctx *c, uint32_t n, uint64_t qb, uint64_t tb) {
     FA_CUDA(c->out.ensure(sizeof(fa_ext_result) * (size_t)n));
     FA_CUDA(c->clamped.ensure(n));
     FA_CUDA(c->cells_job.ensure(sizeof(uint32_t) * (size_t)n));
-    FA_CUDA(c->ovf.ensure(sizeof(uint32_t) * (size_t)n));
+    FA_CUDA(c->ovf.ensure(3 * sizeof(uint32_t) * (size_t)n));
     FA_CUDA(c->misc.ensure(kMiscBytes));
     return FA_OK;
 }

@@ -5,11 +5,24 @@
 #include "../../ferrousalign_b200/csrc/extend_pair_kernel.cu"
 #include "../../ferrousalign_b200/csrc/extend_rows2_kernel.cu"
 
+namespace {
+template <bool SYM, bool CERT, int RING>
+uint32_t run_one(uint32_t jid, uint16_t *eh, uint8_t *sb, const fa_job *jobs, const uint8_t *qseq,
+                 const uint8_t *tseq, const fa::ExtParams &k, int qcap, const int32_t *w_try, fa_ext_result *out,
+                 uint8_t *flags, uint32_t *status, uint32_t *ovf, uint32_t *ovf_n) {
+    return fa::rows2_thread<1, SYM, CERT, RING>(jid, eh, sb, jobs, qseq, tseq, k, qcap, w_try, out, flags, nullptr,
+                                                status, ovf, ovf_n);
+}
+}  // namespace
+
 // Runs every job of `order` through rows2_thread (shared-memory stride 1).  Jobs whose
 // scores can pass 255 are listed in ovf[0..*ovf_n) instead, as the kernel hands them on.
+// cert: evaluate the certificate into flags[jid]; ring: 0, 32 or 64 column slots.
+// w_try (optional): per-job band of this run, as the learned rounds pass it.
 extern "C" int rows2_host_run(const fa_params *prm, const fa_job *jobs, const uint32_t *order, uint32_t n,
-                              const uint8_t *qseq, const uint8_t *tseq, int qcap, fa_ext_result *out,
-                              uint32_t *cells, uint32_t *status, uint32_t *ovf, uint32_t *ovf_n) {
+                              const uint8_t *qseq, const uint8_t *tseq, int qcap, int cert, int ring,
+                              const int32_t *w_try, fa_ext_result *out, uint8_t *flags, uint32_t *cells,
+                              uint32_t *status, uint32_t *ovf, uint32_t *ovf_n) {
     fa::ExtParams k;
     for (int i = 0; i < 25; ++i) k.mat[i] = prm->mat[i];
     k.m = prm->m;
@@ -18,14 +31,26 @@ extern "C" int rows2_host_run(const fa_params *prm, const fa_job *jobs, const ui
     int ms = 0;
     for (int i = 0; i < 25; ++i) if (prm->mat[i] > ms) ms = prm->mat[i];
     k.max_score = ms;
-    if (!fa::ext_rows2_eligible(k, qcap)) return -1;
-    std::vector<uint16_t> eh((size_t)qcap + 1);
+    if (!fa::ext_rows2_eligible(k, qcap) || (ring != 0 && ring != 32 && ring != 64)) return -1;
+    std::vector<uint16_t> eh((size_t)(ring > 0 ? ring : qcap + 1));
     std::vector<uint8_t> sb((size_t)qcap + 1);
     const bool sym = fa::ext_rows2_sym(k);
-    for (uint32_t g = 0; g < n; ++g)
-        cells[order[g]] = sym ? fa::rows2_thread<1, true>(order[g], eh.data(), sb.data(), jobs, qseq, tseq, k, qcap,
-                                                          nullptr, out, nullptr, nullptr, status, ovf, ovf_n)
-                              : fa::rows2_thread<1, false>(order[g], eh.data(), sb.data(), jobs, qseq, tseq, k, qcap,
-                                                           nullptr, out, nullptr, nullptr, status, ovf, ovf_n);
+    for (uint32_t g = 0; g < n; ++g) {
+        const uint32_t j = order[g];
+        uint32_t c = 0;
+#define RUN(S, C, R) c = run_one<S, C, R>(j, eh.data(), sb.data(), jobs, qseq, tseq, k, qcap, w_try, out, flags, \
+                                          status, ovf, ovf_n)
+        if (cert) {
+            if (ring == 32) { if (sym) RUN(true, true, 32); else RUN(false, true, 32); }
+            else if (ring == 64) { if (sym) RUN(true, true, 64); else RUN(false, true, 64); }
+            else { if (sym) RUN(true, true, 0); else RUN(false, true, 0); }
+        } else {
+            if (ring == 32) { if (sym) RUN(true, false, 32); else RUN(false, false, 32); }
+            else if (ring == 64) { if (sym) RUN(true, false, 64); else RUN(false, false, 64); }
+            else { if (sym) RUN(true, false, 0); else RUN(false, false, 0); }
+        }
+#undef RUN
+        cells[j] = c;
+    }
     return 0;
 }

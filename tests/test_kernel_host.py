@@ -106,21 +106,24 @@ def rows2_lib(built):
     import build_host
     lib = C.CDLL(str(build_host.build("rows2")))
     lib.rows2_host_run.restype = C.c_int
-    lib.rows2_host_run.argtypes = [C.c_void_p] * 3 + [C.c_uint32, C.c_void_p, C.c_void_p, C.c_int] + [C.c_void_p] * 5
+    lib.rows2_host_run.argtypes = ([C.c_void_p] * 3 + [C.c_uint32, C.c_void_p, C.c_void_p] + [C.c_int] * 3
+                                   + [C.c_void_p] * 7)
     return lib
 
 
-def run_rows2(lib, p, jobs, qseq, tseq):
+def run_rows2(lib, p, jobs, qseq, tseq, cert=0, ring=0, w_try=None):
     """Longest-first order in 32-column capacity classes; returns results, per-job cells,
-    status and the overflow jobs (the ones the kernel hands to the int32 kernel)."""
+    status, the overflow jobs (the ones the kernel hands to the int32 kernel) and flags."""
     q = jobs["qlen"]
     n = len(q)
     order = np.array(sorted(range(n), key=lambda i: (-int(q[i]), i)), np.uint32)
     out = np.zeros(n, N.EXT_RESULT_DT)
     cells = np.zeros(n, np.uint32)
+    flags = np.zeros(n, np.uint8)
     st = np.zeros(1, np.uint32)
     ovf = np.zeros(n, np.uint32)
     ovf_n = np.zeros(1, np.uint32)
+    wt = None if w_try is None else np.ascontiguousarray(w_try, np.int32)
     s0 = 0
     while s0 < n:
         cap = (int(q[order[s0]]) + 31) // 32 * 32
@@ -129,15 +132,16 @@ def run_rows2(lib, p, jobs, qseq, tseq):
             e0 += 1
         sub = np.ascontiguousarray(order[s0:e0])
         rc = lib.rows2_host_run(p.ctypes.data, jobs.ctypes.data, sub.ctypes.data, len(sub), qseq.ctypes.data,
-                                tseq.ctypes.data, int(q[order[s0]]), out.ctypes.data, cells.ctypes.data,
-                                st.ctypes.data, ovf.ctypes.data, ovf_n.ctypes.data)
+                                tseq.ctypes.data, int(q[order[s0]]), cert, ring,
+                                None if wt is None else wt.ctypes.data, out.ctypes.data, flags.ctypes.data,
+                                cells.ctypes.data, st.ctypes.data, ovf.ctypes.data, ovf_n.ctypes.data)
         assert rc == 0
         s0 = e0
-    return out, cells, int(st[0]), np.sort(ovf[:int(ovf_n[0])])
+    return out, cells, int(st[0]), np.sort(ovf[:int(ovf_n[0])]), flags
 
 
 def check_rows2(lib, p, jobs, qseq, tseq):
-    out, cells, st, ovf = run_rows2(lib, p, jobs, qseq, tseq)
+    out, cells, st, ovf, _ = run_rows2(lib, p, jobs, qseq, tseq)
     ref, tr = O.ext_batch(p, jobs, qseq, tseq)
     a = int(max(0, p["mat"][0].max()))
     wide = np.nonzero(jobs["h0"].astype(np.int64) + a * jobs["qlen"].astype(np.int64) > 255)[0]
@@ -189,3 +193,56 @@ def test_rows2_golden_cases(rows2_lib):
         if len(c["query"]) > 254:
             continue
         check_rows2(rows2_lib, p, jobs, qs, ts)
+
+
+def check_rows2_cert(lib, p, jobs, qseq, tseq, w_try, ring):
+    """Narrow runs at per-job bands w_try with the certificate: results and cells equal the
+    oracle's run at that band, certificate bit and hint equal the oracle's trace (bit 1 =
+    bound_ok and the configured band covers the first row's positive cells)."""
+    jw = jobs.copy()
+    jw["w"] = w_try
+    out, cells, st, ovf, flags = run_rows2(lib, p, jobs, qseq, tseq, cert=1, ring=ring, w_try=w_try)
+    ref, tr = O.ext_batch(p, jw, qseq, tseq)
+    a = int(max(0, p["mat"][0].max()))
+    wide = np.nonzero(jobs["h0"].astype(np.int64) + a * jobs["qlen"].astype(np.int64) > 255)[0]
+    assert st == 0
+    assert np.array_equal(ovf, wide.astype(np.uint32))
+    keep = np.ones(len(jobs), bool)
+    keep[wide] = False
+    bad = np.nonzero(keep & (out != ref))[0]
+    assert len(bad) == 0, (bad[:10], out[bad[:3]], ref[bad[:3]])
+    assert np.array_equal(cells[keep], tr["cells"][keep].astype(np.uint32))
+    clean = np.array([O.wide_clean(p, int(jobs["qlen"][k]), int(jobs["w"][k]), int(tr["init_reach"][k]))
+                      for k in range(len(jobs))], bool)
+    want_cert = (tr["bound_ok"] != 0) & clean
+    want_hint = np.where(clean, tr["hint"], 63)
+    assert np.array_equal((flags[keep] >> 1) & 1, want_cert[keep].astype(np.uint8)), \
+        np.nonzero(((flags >> 1) & 1) != want_cert)[0][:10]
+    assert np.array_equal(flags[keep] >> 2, want_hint[keep].astype(np.uint8))
+    assert np.array_equal(flags[keep] & 1, (tr["clamped"][keep] != 0).astype(np.uint8))
+    return int(keep.sum()), int(want_cert[keep].sum())
+
+
+@pytest.mark.parametrize("ring", [0, 32, 64])
+def test_rows2_certificate_matches_oracle(rows2_lib, ring):
+    b = synth.workload_ext_1m(4000, seed=41)
+    p = fa.BandedPairWiseSW().to_struct()
+    rng = np.random.default_rng(ring + 1)
+    cap = {0: 100, 32: 14, 64: 30}[ring]
+    w_try = rng.integers(1, cap + 1, size=len(b.jobs)).astype(np.int32)
+    n, ncert = check_rows2_cert(rows2_lib, p, b.jobs, b.qseq, b.tseq, w_try, ring)
+    assert n == 4000 and 0 < ncert < n
+
+
+@pytest.mark.parametrize("a,b_,n,gaps,zdrop", [(2, 3, 0, (5, 2, 3, 1), 30), (1, 2, -1, (3, 3, 1, 1), 5),
+                                               (3, 1, -1, (0, 1, 2, 2), 0)])
+def test_rows2_certificate_uneven_parameters(rows2_lib, a, b_, n, gaps, zdrop):
+    ref_seq = synth.reference(400_000, seed=13, n_rate=0.02, repeat_frac=0.05)
+    bt = synth.ext_jobs(ref_seq, 2000, seed=23, read_len=(10, 160), seed_len=(3, 30), seed_at_start=False, w=100,
+                        indel_rates=(0.0, 0.02, 0.06), sub_rate=0.04)
+    sw = fa.BandedPairWiseSW(o_del=gaps[0], e_del=gaps[1], o_ins=gaps[2], e_ins=gaps[3], zdrop=zdrop,
+                             mat=fa.bwa_fill_scmat(a, b_, n))
+    rng = np.random.default_rng(7)
+    for ring, cap in ((0, 100), (32, 14), (64, 30)):
+        w_try = rng.integers(1, cap + 1, size=len(bt.jobs)).astype(np.int32)
+        check_rows2_cert(rows2_lib, sw.to_struct(), bt.jobs, bt.qseq, bt.tseq, w_try, ring)
