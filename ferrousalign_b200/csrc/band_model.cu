@@ -222,40 +222,90 @@ __device__ __forceinline__ void load_norm(const float *__restrict__ xr, const No
     for (int k = 0; k < kIn; ++k) x[k] = (xr[k] - nc.mean[k]) * nc.inv_std[k];
 }
 
+// Forward of two samples at once: every weight comes from shared memory once for both, and
+// layer 2 accumulates as each layer-1 unit is done (W2 transposed in w2t, so its reads are
+// contiguous).  Each sum runs in the same order as mlp_forward's, so the outputs are the same.
+__device__ __forceinline__ void mlp_forward2(const float *__restrict__ w, const float *__restrict__ w2t,
+                                             const float *x0, const float *x1, float &y0, float &y1)
+{
+    float a0[kH2], a1[kH2];
+#pragma unroll
+    for (int v = 0; v < kH2; ++v) a0[v] = a1[v] = w[oB2 + v];
+#pragma unroll 2
+    for (int u = 0; u < kH1; ++u) {
+        float s0 = w[oB1 + u], s1 = s0;
+#pragma unroll
+        for (int k = 0; k < kIn; ++k) {
+            const float wk = w[oW1 + u * kIn + k];
+            s0 = fmaf(wk, x0[k], s0);
+            s1 = fmaf(wk, x1[k], s1);
+        }
+        s0 = fmaxf(s0, 0.f);
+        s1 = fmaxf(s1, 0.f);
+#pragma unroll
+        for (int v = 0; v < kH2; ++v) {
+            const float wv = w2t[u * kH2 + v];
+            a0[v] = fmaf(wv, s0, a0[v]);
+            a1[v] = fmaf(wv, s1, a1[v]);
+        }
+    }
+    y0 = y1 = w[oB3];
+#pragma unroll
+    for (int k = 0; k < kH2; ++k) {
+        const float wk = w[oW3 + k];
+        y0 = fmaf(wk, fmaxf(a0[k], 0.f), y0);
+        y1 = fmaf(wk, fmaxf(a1[k], 0.f), y1);
+    }
+}
+
 // Inference: y = MLP(x) in log2(band) units; band = ceil(2^(y + margin)) raised to
 // w_min and rounded up to the ladder 2, 3, 4, 6, 8, 12, ... (bands of one launch fall
 // into few classes, which the band partition turns into uniform warps; doubling after a
 // rejection stays on the ladder).  A band above half the configured band starts at the
-// configured band: its
-// narrow run would save less than half the cells, and a rejected one costs more than
-// starting wide.
-__global__ void __launch_bounds__(128) band_predict_kernel(const __nv_bfloat16 *__restrict__ wbf, NormConsts nc,
-                                                           const float *__restrict__ x, const fa_job *__restrict__ jobs,
-                                                           uint32_t n, float margin, int w_min,
-                                                           float *__restrict__ y_out, int32_t *__restrict__ w_out)
+// configured band: its narrow run would save less than half the cells, and a rejected one
+// costs more than starting wide.  Each thread predicts two jobs, i and i + blockDim.x.
+constexpr int kPredThreads = 128;
+__global__ void __launch_bounds__(kPredThreads) band_predict_kernel(
+    const __nv_bfloat16 *__restrict__ wbf, NormConsts nc, const float *__restrict__ x,
+    const fa_job *__restrict__ jobs, uint32_t n, float margin, int w_min, float *__restrict__ y_out,
+    int32_t *__restrict__ w_out)
 {
-    __shared__ float w[kNParams];
+    __shared__ __align__(16) float w[kNParams];
+    __shared__ __align__(16) float w2t[kH1 * kH2];
     for (int k = threadIdx.x; k < kNParams; k += blockDim.x) w[k] = __bfloat162float(wbf[k]);
-    __syncthreads();
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    float xi[kIn], h1[kH1], h2[kH2];
-    load_norm(x + (size_t)i * kIn, nc, xi);
-    const float y = mlp_forward(w, xi, h1, h2);
-    if (y_out) y_out[i] = y;
-    if (w_out) {
-        const int wj = jobs ? jobs[i].w : 100;
-        const float e = fminf(fmaxf(y + margin, 0.f), 16.f);
-        int band = (int)ceilf(exp2f(e));
-        band = max(band, w_min);
-        if (band > 2) {                 // up to the ladder 2^k, 3*2^(k-1): few distinct bands per launch
-            const int p2 = 1 << (32 - __clz(band - 1));
-            band = 3 * p2 / 4 >= band ? 3 * p2 / 4 : p2;
-        }
-        if (2 * band > wj) band = wj;   // a narrow run above half the configured band saves too little
-        band = min(band, wj);
-        w_out[i] = band;
+    for (int k = threadIdx.x; k < kH1 * kH2; k += blockDim.x) {
+        const int u = k / kH2, v = k % kH2;
+        w2t[k] = __bfloat162float(wbf[oW2 + v * kH1 + u]);
     }
+    __syncthreads();
+    const uint32_t i0 = blockIdx.x * (2 * kPredThreads) + threadIdx.x, i1 = i0 + kPredThreads;
+    if (i0 >= n) return;
+    float x0[kIn], x1[kIn];
+    load_norm(x + (size_t)i0 * kIn, nc, x0);
+    if (i1 < n) load_norm(x + (size_t)i1 * kIn, nc, x1);
+    else
+#pragma unroll
+        for (int k = 0; k < kIn; ++k) x1[k] = 0.f;
+    float y0, y1;
+    mlp_forward2(w, w2t, x0, x1, y0, y1);
+    auto put = [&](uint32_t i, float y) {
+        if (y_out) y_out[i] = y;
+        if (w_out) {
+            const int wj = jobs ? jobs[i].w : 100;
+            const float e = fminf(fmaxf(y + margin, 0.f), 16.f);
+            int band = (int)ceilf(exp2f(e));
+            band = max(band, w_min);
+            if (band > 2) {                 // up to the ladder 2^k, 3*2^(k-1): few distinct bands per launch
+                const int p2 = 1 << (32 - __clz(band - 1));
+                band = 3 * p2 / 4 >= band ? 3 * p2 / 4 : p2;
+            }
+            if (2 * band > wj) band = wj;   // a narrow run above half the configured band saves too little
+            band = min(band, wj);
+            w_out[i] = band;
+        }
+    };
+    put(i0, y0);
+    if (i1 < n) put(i1, y1);
 }
 
 // Backward over one minibatch of up to kMB samples per block: activations in shared
@@ -384,7 +434,8 @@ cudaError_t launch_band_predict(const __nv_bfloat16 *d_wbf, const float *mean, c
                                 int32_t *d_w, cudaStream_t s)
 {
     if (n == 0) return cudaSuccess;
-    band_predict_kernel<<<(n + 127) / 128, 128, 0, s>>>(d_wbf, norm_of(mean, std_), d_x, d_jobs, n, margin, w_min,
+    const uint32_t blocks = (n + 2 * kPredThreads - 1) / (2 * kPredThreads);
+    band_predict_kernel<<<blocks, kPredThreads, 0, s>>>(d_wbf, norm_of(mean, std_), d_x, d_jobs, n, margin, w_min,
                                                         d_y, d_w);
     return cudaGetLastError();
 }

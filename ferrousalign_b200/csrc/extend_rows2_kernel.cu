@@ -529,8 +529,10 @@ size_t ext_rows2_smem_bytes(int qcap, int tpb, int ring) {
     return words * tpb * sizeof(uint16_t) + (size_t)(qcap + 3) / 4 * 4 * tpb;
 }
 
+// Any capacity whose shared memory fits: jobs past kRows2MaxQ columns always exceed the 8-bit
+// bound and go to the int32 kernel through the overflow list.
 bool ext_rows2_eligible(const ExtParams &p, int qcap) {
-    return qcap <= kRows2MaxQ && ext_pair_eligible(p);
+    return qcap >= 1 && qcap <= FA_MAX_QLEN && ext_pair_eligible(p);
 }
 
 namespace {

@@ -149,7 +149,8 @@ cudaError_t launch_ext(fa_ctx *c, Choice kc, const fa_job *d_jobs, const uint32_
                        const int32_t *d_w_try, fa_ext_result *d_out, uint8_t *d_clamped, bool cert,
                        uint32_t *d_cells_job, unsigned long long *d_cells, uint32_t *d_status, cudaStream_t s) {
     if (kc.kernel == FA_KERNEL_ROWS2 && !cert && ext_rows2_eligible(kp, qcap) &&
-        c->ovf.cap >= sizeof(uint32_t) * (size_t)n && c->misc.p)
+        ext_rows2_smem_bytes(qcap, kc.tpb, 0) <= c->smem_optin && c->ovf.cap >= sizeof(uint32_t) * (size_t)n &&
+        c->misc.p)
         return launch_ext_rows2(d_jobs, d_order, n, nullptr, d_n, d_q, d_t, kp, qcap, 0, false, d_w_try, d_out,
                                 d_clamped, d_cells_job, d_cells, d_status, c->ovf.as<uint32_t>(), misc_of(c).ovf_n, s,
                                 kc.tpb);
@@ -161,8 +162,9 @@ cudaError_t launch_ext(fa_ctx *c, Choice kc, const fa_job *d_jobs, const uint32_
 }
 
 // Kernel launches one launch_ext call makes (the two-row kernel adds its overflow pass).
-uint32_t ext_kernels_of(Choice kc, const ExtParams &kp, int qcap) {
-    return kc.kernel == FA_KERNEL_ROWS2 && ext_rows2_eligible(kp, qcap) ? 2u : 1u;
+uint32_t ext_kernels_of(fa_ctx *c, Choice kc, const ExtParams &kp, int qcap) {
+    return kc.kernel == FA_KERNEL_ROWS2 && ext_rows2_eligible(kp, qcap) &&
+                   ext_rows2_smem_bytes(qcap, kc.tpb, 0) <= c->smem_optin ? 2u : 1u;
 }
 
 // The kernel a call runs.  A fixed setting is used as is.  FA_KERNEL_AUTO is an
@@ -236,10 +238,11 @@ Choice resolve_choice(fa_ctx *c, const ExtParams &kp, const fa_job *d_jobs, cons
 int launch_learned_round(fa_ctx *c, const fa_job *d_jobs, const uint32_t *d_list, uint32_t n_max,
                          const uint8_t *d_q, const uint8_t *d_t, const ExtParams &kp, int qcap,
                          const int32_t *d_w_cur, fa_ext_result *d_out, uint8_t *d_flags, bool cert, Misc &m,
-                         cudaStream_t s) {
+                         cudaStream_t s, uint32_t *launches) {
     if (int rc = ensure_aux_streams(c)) return rc;
     const uint32_t *g = m.group_bounds;
     const bool rows2 = c->kernel != FA_KERNEL_INT32 && ext_rows2_eligible(kp, qcap) &&
+                       ext_rows2_smem_bytes(qcap, 64, 0) <= c->smem_optin &&
                        c->ovf.cap >= 3 * sizeof(uint32_t) * (size_t)n_max;
     auto group = [&](int k, int ring, cudaStream_t st) -> cudaError_t {
         const uint32_t *first = k == 0 ? nullptr : g + k - 1;
@@ -259,6 +262,7 @@ int launch_learned_round(fa_ctx *c, const fa_job *d_jobs, const uint32_t *d_list
         FA_CUDA(cudaEventRecord(c->join_ev[k], c->aux[k]));
         FA_CUDA(cudaStreamWaitEvent(s, c->join_ev[k], 0));
     }
+    *launches += rows2 ? 6 : 3;
     return FA_OK;
 }
 
@@ -412,7 +416,7 @@ int enqueue_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n
             const auto &sg = segs0[k];
             FA_CUDA(launch_ext(c, kc_of(k), d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp, sg.second,
                                nullptr, d_out, nullptr, false, c->cells_job.as<uint32_t>(), m.cells, m.status, s));
-            *launches += ext_kernels_of(kc_of(k), kp, sg.second);
+            *launches += ext_kernels_of(c, kc_of(k), kp, sg.second);
             b = sg.first;
         }
         return FA_OK;
@@ -444,7 +448,7 @@ int enqueue_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n
                 FA_CUDA(launch_ext(c, kc_of(k), d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp, sg.second,
                                    st.w_cur, d_out, d_flags, cert_r, c->cells_job.as<uint32_t>(), m.cells, m.status,
                                    s));
-                *launches += ext_kernels_of(kc_of(k), kp, sg.second);
+                *launches += ext_kernels_of(c, kc_of(k), kp, sg.second);
                 b = sg.first;
             }
         } else if (learned && !cert_r && c->kernel != FA_KERNEL_INT16X2) {
@@ -452,7 +456,7 @@ int enqueue_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n
             // call's autotuned kernel over the compacted list
             FA_CUDA(launch_ext(c, kc, d_jobs, list, n, cnt, d_q, d_t, kp, qcap_all, st.w_cur, d_out, d_flags, false,
                                c->cells_job.as<uint32_t>(), m.cells, m.status, s));
-            *launches += ext_kernels_of(kc, kp, qcap_all);
+            *launches += ext_kernels_of(c, kc, kp, qcap_all);
         } else if (learned) {
             // band buckets (configured band first, then narrow bands decreasing), then the
             // three band groups concurrently
@@ -465,14 +469,14 @@ int enqueue_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n
                 *launches += 3;
             } else {
                 if (int rc = launch_learned_round(c, d_jobs, c->part_n.as<uint32_t>(), n, d_q, d_t, kp, qcap_all,
-                                                  st.w_cur, d_out, d_flags, cert_r, m, s))
+                                                  st.w_cur, d_out, d_flags, cert_r, m, s, launches))
                     return rc;
-                *launches += 5;
+                *launches += 2;   // band histogram and scatter
             }
         } else {
             FA_CUDA(launch_ext(c, kc, d_jobs, list, n, cnt, d_q, d_t, kp, qcap_all, st.w_cur, d_out,
                                d_flags, cert_r, c->cells_job.as<uint32_t>(), m.cells, m.status, s));
-            *launches += cert_r ? 1u : ext_kernels_of(kc, kp, qcap_all);
+            *launches += cert_r ? 1u : ext_kernels_of(c, kc, kp, qcap_all);
         }
         FA_CUDA(cudaMemsetAsync(next_cnt, 0, 4, s));
         FA_CUDA(launch_policy_step(d_jobs, list, nullptr, cnt, n, d_out, d_flags, st, max_tries,
@@ -1019,7 +1023,7 @@ int fa_ext_batch_device(fa_ctx *c, const fa_params *p, const fa_job *d_jobs, uin
     }
     if (c->timing) FA_CUDA(cudaEventRecord(c->kev1, s));
     c->last_launches = d_order ? 1u : 2u;
-    for (size_t k = 0; k < segs.size(); ++k) c->last_launches += ext_kernels_of(seg_kc[k], kp, segs[k].second);
+    for (size_t k = 0; k < segs.size(); ++k) c->last_launches += ext_kernels_of(c, seg_kc[k], kp, segs[k].second);
     c->last_stream = s;
     return FA_OK;
 }

@@ -36,9 +36,9 @@ cudaError_t launch_ext_pair(const fa_job *d_jobs, const uint32_t *d_order, uint3
                             unsigned long long *d_cells, uint32_t *d_status, cudaStream_t stream);
 
 // Two target rows per thread in int16x2 cells with 8-bit column state (extend_rows2_kernel.cu).
-// Eligible for bwa-form matrices and queries up to 254 columns; jobs whose scores can pass
-// 255 are appended to d_ovf (count in *d_ovf_n) and run by the int32 kernel in the same call
-// with the same settings.  ring 32/64 keeps only that many column words (bands with
+// Eligible for bwa-form matrices (any capacity whose shared memory fits); jobs whose scores
+// can pass 255 -- every job past 254 query columns among them -- are appended to d_ovf (count
+// in *d_ovf_n) and run by the int32 kernel in the same call with the same settings.  ring 32/64 keeps only that many column words (bands with
 // 2w + 3 <= ring); cert evaluates the exit-bound certificate and hint into d_clamped.
 // d_first (optional): device-side first index into d_order, as for launch_ext_packed.
 bool ext_rows2_eligible(const ExtParams &p, int qcap);
