@@ -45,6 +45,8 @@ if len(sys.argv) > 1 and sys.argv[1] in ("learned", "bands"):
     b = synth.workload_ext_1m(n)
     p = fa.BandedPairWiseSW().to_struct()
     ctx = fa.Context(0)
+    if len(sys.argv) > 4:               # fixed kernel choice (autotuning timings mean nothing under ncu)
+        ctx.set_kernel(int(sys.argv[4]))
     if mode == "learned":
         m = B.BandModel.load()
         hints = B.hints_from_info(b.info)
