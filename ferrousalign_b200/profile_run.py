@@ -1,7 +1,7 @@
 """One device-resident extension batch of the bench workload, for ncu captures.
 
-Usage: python -m ferrousalign_b200.profile_run [n_jobs] [probe|-] [kernel: 0 auto, 1 int32, 2 int16x2] [reps]
-       python -m ferrousalign_b200.profile_run learned [n_jobs] [reps]   (learned-band path)
+Usage: python -m ferrousalign_b200.profile_run [n_jobs] [probe|-] [kernel: 0 auto, 1 int32, 2 int16x2, 3 rows2] [reps]
+       python -m ferrousalign_b200.profile_run learned [n_jobs] [reps] [kernel]   (learned-band path)
        python -m ferrousalign_b200.profile_run bands [n_jobs]            (single runs at fixed bands)
        python -m ferrousalign_b200.profile_run mate [n_jobs] [reps]      (mate-rescue SW, device-resident)
 """
