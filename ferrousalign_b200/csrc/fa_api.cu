@@ -144,16 +144,19 @@ int ensure_aux_streams(fa_ctx *c) {
 // certificate (flag bit 1), which only the int32 kernel implements.
 using Choice = fa_ctx::Choice;
 
+// `slot` (0-2) picks the two-row kernel's overflow list and count, so launches that may run
+// concurrently use different ones; each list holds a third of the buffer.
 cudaError_t launch_ext(fa_ctx *c, Choice kc, const fa_job *d_jobs, const uint32_t *d_order, uint32_t n,
                        const uint32_t *d_n, const uint8_t *d_q, const uint8_t *d_t, const ExtParams &kp, int qcap,
                        const int32_t *d_w_try, fa_ext_result *d_out, uint8_t *d_clamped, bool cert,
-                       uint32_t *d_cells_job, unsigned long long *d_cells, uint32_t *d_status, cudaStream_t s) {
+                       uint32_t *d_cells_job, unsigned long long *d_cells, uint32_t *d_status, cudaStream_t s,
+                       int slot = 0) {
+    const size_t ovf_words = c->ovf.cap / (3 * sizeof(uint32_t));
     if (kc.kernel == FA_KERNEL_ROWS2 && !cert && ext_rows2_eligible(kp, qcap) &&
-        ext_rows2_smem_bytes(qcap, kc.tpb, 0) <= c->smem_optin && c->ovf.cap >= sizeof(uint32_t) * (size_t)n &&
-        c->misc.p)
+        ext_rows2_smem_bytes(qcap, kc.tpb, 0) <= c->smem_optin && ovf_words >= (size_t)n && c->misc.p)
         return launch_ext_rows2(d_jobs, d_order, n, nullptr, d_n, d_q, d_t, kp, qcap, 0, false, d_w_try, d_out,
-                                d_clamped, d_cells_job, d_cells, d_status, c->ovf.as<uint32_t>(), misc_of(c).ovf_n, s,
-                                kc.tpb);
+                                d_clamped, d_cells_job, d_cells, d_status, c->ovf.as<uint32_t>() + slot * ovf_words,
+                                misc_of(c).ovf_n + slot, s, kc.tpb);
     if (kc.kernel == FA_KERNEL_INT16X2 && ext_pair_eligible(kp) && !cert)
         return launch_ext_pair(d_jobs, d_order, n, d_n, d_q, d_t, kp, qcap, d_w_try, d_out, d_clamped,
                                d_cells_job, d_cells, d_status, s);
@@ -208,7 +211,7 @@ Choice resolve_choice(fa_ctx *c, const ExtParams &kp, const fa_job *d_jobs, cons
         if (kc.kernel == FA_KERNEL_INT32 && ext_packed_smem_bytes(qcap, 0, kc.tpb) > c->smem_optin) continue;
         if (kc.kernel == FA_KERNEL_INT16X2 && ext_pair_smem_bytes(qcap) > c->smem_optin) continue;
         if (kc.kernel == FA_KERNEL_ROWS2 && (ext_rows2_smem_bytes(qcap, kc.tpb, 0) > c->smem_optin ||
-                                             c->ovf.cap < sizeof(uint32_t) * (size_t)ns))
+                                             c->ovf.cap < 3 * sizeof(uint32_t) * (size_t)ns))
             continue;
         for (int rep = 0; rep < 3; ++rep) {           // one warm-up, two timed
             if (rep == 1 && (e = cudaEventRecord(e0, s)) != cudaSuccess) return bail(e);
@@ -694,7 +697,7 @@ int ext_batch_pipelined(fa_ctx *c, const ExtParams &kp, const fa_job *jobs, uint
     }
     const int max_q = (int)h_info[2];
     FA_CUDA(launch_chunk_scatter(c->jobs.as<fa_job>(), n, qs, ts, kSlices, scratch, c->order.as<uint32_t>(), s));
-    const int band = max_band_of(jobs, n);
+    const int band = (int)h_info[3];   // widest configured band, reduced on the device
     if (c->kernel == FA_KERNEL_AUTO && !c->tuned.count({(max_q + 31) / 32, band}))
         FA_CUDA(cudaStreamWaitEvent(s, c->slice_ev[kSlices - 1], 0));   // tuning reads every slice
     int rc0 = FA_OK;
@@ -702,16 +705,25 @@ int ext_batch_pipelined(fa_ctx *c, const ExtParams &kp, const fa_job *jobs, uint
                                      c->tseq.as<uint8_t>(), max_q, band, c->out.as<fa_ext_result>(), m.status, s, &rc0);
     if (rc0) return rc0;
     uint32_t launches = 2;
+    // slices alternate between the main stream and an auxiliary one (each with its own
+    // overflow list), so one slice's last, partly filled wave overlaps the next slice's start
+    if (int rc = ensure_aux_streams(c)) return rc;
+    cudaStream_t sk[2] = {s, c->aux[0]};
     FA_CUDA(cudaEventRecord(c->ev0, s));
+    FA_CUDA(cudaEventRecord(c->fork_ev, s));
+    FA_CUDA(cudaStreamWaitEvent(sk[1], c->fork_ev, 0));
     for (int k = 0; k < kSlices; ++k) {
         const uint32_t cnt = h_info[4 + k + 1] - h_info[4 + k];
-        FA_CUDA(cudaStreamWaitEvent(s, c->slice_ev[k], 0));
+        cudaStream_t st = sk[k & 1];
+        FA_CUDA(cudaStreamWaitEvent(st, c->slice_ev[k], 0));
         if (cnt == 0) continue;
         FA_CUDA(launch_ext(c, kc, c->jobs.as<fa_job>(), c->order.as<uint32_t>() + h_info[4 + k], cnt, nullptr,
                            c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(), kp, max_q, nullptr, c->out.as<fa_ext_result>(),
-                           nullptr, false, c->cells_job.as<uint32_t>(), m.cells, m.status, s));
-        ++launches;
+                           nullptr, false, c->cells_job.as<uint32_t>(), m.cells, m.status, st, k & 1));
+        launches += ext_kernels_of(c, kc, kp, max_q);
     }
+    FA_CUDA(cudaEventRecord(c->join_ev[0], sk[1]));
+    FA_CUDA(cudaStreamWaitEvent(s, c->join_ev[0], 0));
     FA_CUDA(cudaEventRecord(c->ev1, s));
     FA_CUDA(cudaMemcpyAsync(out, c->out.p, sizeof(fa_ext_result) * (size_t)n, cudaMemcpyDeviceToHost, s));
     if (int rc = finish_ext(c, nullptr, n, s, stats, nullptr, launches, 0, false)) return rc;
@@ -963,7 +975,7 @@ int fa_ext_batch_device(fa_ctx *c, const fa_params *p, const fa_job *d_jobs, uin
     const ExtParams kp = ext_params_of(p);
     cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
     FA_CUDA(c->misc.ensure(kMiscBytes));
-    FA_CUDA(c->ovf.ensure(sizeof(uint32_t) * (size_t)n));
+    FA_CUDA(c->ovf.ensure(3 * sizeof(uint32_t) * (size_t)n));
     FA_CUDA(c->hist.ensure(sizeof(uint32_t) * (FA_MAX_QLEN + 1)));
     Misc m = misc_of(c);
     FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));

@@ -38,8 +38,9 @@ cudaError_t launch_ext_pair(const fa_job *d_jobs, const uint32_t *d_order, uint3
 // Two target rows per thread in int16x2 cells with 8-bit column state (extend_rows2_kernel.cu).
 // Eligible for bwa-form matrices (any capacity whose shared memory fits); jobs whose scores
 // can pass 255 -- every job past 254 query columns among them -- are appended to d_ovf (count
-// in *d_ovf_n) and run by the int32 kernel in the same call with the same settings.  ring 32/64 keeps only that many column words (bands with
-// 2w + 3 <= ring); cert evaluates the exit-bound certificate and hint into d_clamped.
+// in *d_ovf_n) and run by the int32 kernel in the same call with the same settings.  ring
+// 32/64 keeps only that many column words (bands with 2w + 3 <= ring); cert evaluates the
+// exit-bound certificate and hint into d_clamped.
 // d_first (optional): device-side first index into d_order, as for launch_ext_packed.
 bool ext_rows2_eligible(const ExtParams &p, int qcap);
 size_t ext_rows2_smem_bytes(int qcap, int tpb, int ring);
@@ -78,7 +79,7 @@ cudaError_t launch_mate_sw(bool byte_lanes, const fa_mate_job *d_jobs, const uin
 // Device-side longest-first ordering by query length (order_kernel.cu).
 // Pipelined host batches: validation + (chunk, length) histogram + prefix, then scatter.
 // Scratch layout: hist | base | cursor (nchunks * (FA_MAX_QLEN+1) each) | info[4] =
-// {status bits, first bad job, longest query, 0} | bounds[nchunks+1].
+// {status bits, first bad job, longest query, widest configured band} | bounds[nchunks+1].
 size_t chunk_scratch_bytes(int nchunks);
 cudaError_t launch_chunk_prep(const fa_job *d_jobs, uint32_t n, uint64_t qbytes, uint64_t tbytes, uint64_t qslice,
                               uint64_t tslice, int nchunks, int max_score, int qcap_limit, uint32_t *d_scratch,

@@ -119,7 +119,8 @@ namespace fa {
 // chunk, by decreasing query length.  Bin = chunk * (FA_MAX_QLEN + 1) + (FA_MAX_QLEN - qlen).
 // The prep kernel also validates every job against the buffer lengths and the kernel
 // limits (the same rules as the host-side checks), keeping the first bad job's index,
-// and reduces the longest query.  info = {status, first bad job, longest query}.
+// and reduces the longest query and the widest configured band.  info = {status, first bad
+// job, longest query, widest band}.
 
 constexpr int kChunkBins = FA_MAX_QLEN + 1;
 
@@ -129,10 +130,11 @@ __global__ void chunk_prep_kernel(const fa_job *__restrict__ jobs, uint32_t n, u
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool live = i < n;
-    int bin = -1, qlen = 0;
+    int bin = -1, qlen = 0, band = 0;
     if (live) {
         const fa_job jb = jobs[i];
         qlen = jb.qlen;
+        band = max(jb.w, 0);
         uint32_t st = 0;
         if (jb.qlen <= 0 || jb.tlen < 0 || jb.h0 <= 0) st |= ST_ARG;
         else if (jb.qlen > FA_MAX_QLEN || jb.tlen > FA_MAX_TLEN) st |= ST_CAPACITY;
@@ -153,6 +155,8 @@ __global__ void chunk_prep_kernel(const fa_job *__restrict__ jobs, uint32_t n, u
     }
     const int mq = __reduce_max_sync(0xffffffffu, qlen);
     if ((threadIdx.x & 31) == 0 && mq > 0) atomicMax(&info[2], (uint32_t)mq);
+    const int mw = __reduce_max_sync(0xffffffffu, band);
+    if ((threadIdx.x & 31) == 0 && mw > 0) atomicMax(&info[3], (uint32_t)mw);
     const unsigned peers = __match_any_sync(0xffffffffu, bin);
     if (bin >= 0 && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&hist[bin], (uint32_t)__popc(peers));
 }
