@@ -507,8 +507,17 @@ ext_rows2_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ o
     if (gi < n) {
         constexpr int slots = RING > 0 ? RING : 0;
         const int words = slots > 0 ? slots : qcap + 1;
-        uint16_t *eh = reinterpret_cast<uint16_t *>(smem) + threadIdx.x;
-        uint8_t *sb = reinterpret_cast<uint8_t *>(smem) + (size_t)words * TPB * 2 + threadIdx.x;
+        // Per-thread slots within a column: the 32 lanes of a warp get 32 different 32-bit
+        // words of every column (two warps share a word of 16-bit column words, four a word
+        // of selector bytes at 128 threads per block), so lanes at different columns never
+        // meet in one bank; the column stride stays TPB entries.
+        static_assert(TPB == 64 || TPB == 128, "the slot maps cover 64 or 128 threads per block");
+        const int t = threadIdx.x;
+        const int e_off = 2 * (((t >> 6) << 5) + (t & 31)) + ((t >> 5) & 1);
+        const int s_off = TPB >= 128 ? 4 * (((t >> 7) << 5) + (t & 31)) + ((t >> 5) & 3)
+                                     : 4 * ((t & 31) >> 1) + 2 * (t & 1) + ((t >> 5) & 1);
+        uint16_t *eh = reinterpret_cast<uint16_t *>(smem) + e_off;
+        uint8_t *sb = reinterpret_cast<uint8_t *>(smem) + (size_t)words * TPB * 2 + s_off;
         cells = rows2_thread<TPB, SYM, CERT, RING>(order ? order[gi] : gi, eh, sb, jobs, qseq, tseq, p, qcap, w_try,
                                                    out, clamped_out, cells_job, status, ovf, ovf_n);
     }
