@@ -210,6 +210,23 @@ def bench_uneven(args, ctx, p):
         learned, lst, wf, _ = B.extend_batch_learned(p, u.jobs, u.qseq, u.tseq, model, hints=hints, ctx=ctx)
         lm.append(float(lst["kernel_ms"]))
     pms, lms = float(np.median(pm)), float(np.median(lm))
+    # the same two calls with the whole extend / check / retry loop recorded as one CUDA graph
+    # per context (replayed after the first call of the shape)
+    gp, gl = N.Context(0), N.Context(0)
+    try:
+        gp.set_graph(True)
+        gl.set_graph(True)
+        gpm, glm = [], []
+        for r in range(1 + max(2, args.steps // 10)):
+            gplain, gst, _ = fa.extend_batch(p, u.jobs, u.qseq, u.tseq, policy=bwa, ctx=gp)
+            glearned, glst, _, _ = B.extend_batch_learned(p, u.jobs, u.qseq, u.tseq, model, hints=hints, ctx=gl)
+            if r:
+                gpm.append(float(gst["kernel_ms"]))
+                glm.append(float(glst["kernel_ms"]))
+    finally:
+        gp.close()
+        gl.close()
+    gpms, glms = float(np.median(gpm)), float(np.median(glm))
     ql = u.jobs["qlen"]
     return {"workload": f"{n} mixed left/right extensions, reads 50-300 bp, 100 Mbp reference with 5% repeats",
             "qlen_mean": float(ql.mean()), "qlen_max": int(ql.max()),
@@ -218,7 +235,10 @@ def bench_uneven(args, ctx, p):
             "learned": {"value": n / (lms * 1e-3), "unit": "alignments/s", "kernel_ms": lms,
                         "cells_saved_frac": 1.0 - float(lst["cells_executed"]) / float(pst["cells_executed"]),
                         "miss_rate": float(lst["misses"]) / n},
-            "speedup": pms / lms, "identical_outputs": bool(np.array_equal(plain, learned))}
+            "speedup": pms / lms, "identical_outputs": bool(np.array_equal(plain, learned)),
+            "graph": {"plain_kernel_ms": gpms, "learned_kernel_ms": glms,
+                      "plain_value": n / (gpms * 1e-3), "learned_value": n / (glms * 1e-3),
+                      "identical_outputs": bool(np.array_equal(gplain, plain) and np.array_equal(glearned, plain))}}
 
 
 def bench_mixed(args, b, p):

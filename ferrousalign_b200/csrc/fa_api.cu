@@ -399,8 +399,8 @@ int max_rounds_of(const fa_policy *pol, int max_w) {
 // Enqueues the extension rounds of one call on stream s.  Without `capture` the host
 // reads each round's retry count and stops early when nothing is left; with `capture`
 // (recording a CUDA graph) the rounds run a fixed number of times with every count on
-// the device, so no round needs the host, and the first round is one launch over the
-// length-sorted order instead of one per shared-memory class.
+// the device, so no round needs the host.  The first round launches once per capacity
+// class of the length-sorted order either way.
 int enqueue_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n,
                 const std::vector<std::pair<uint32_t, int>> &segs, int qcap_all, int max_w, const fa_job *d_jobs,
                 const uint32_t *d_order, const uint8_t *d_q, const uint8_t *d_t, const int32_t *d_wfirst,
@@ -410,9 +410,9 @@ int enqueue_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n
     FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
     const int mode = pol ? pol->mode : FA_POLICY_SINGLE;
     const std::vector<std::pair<uint32_t, int>> one_seg{{n, qcap_all}};
-    const auto &segs0 = capture ? one_seg : segs;
+    const auto &segs0 = segs.empty() ? one_seg : segs;
     // first-round kernel of each capacity class (tuned per class); retries use kc
-    auto kc_of = [&](size_t k) { return !capture && seg_kc && k < seg_kc->size() ? (*seg_kc)[k] : kc; };
+    auto kc_of = [&](size_t k) { return seg_kc && k < seg_kc->size() ? (*seg_kc)[k] : kc; };
     if (mode == FA_POLICY_SINGLE) {
         uint32_t b = 0;
         for (size_t k = 0; k < segs0.size(); ++k) {
@@ -595,7 +595,8 @@ std::vector<uint64_t> graph_key(fa_ctx *c, const ExtParams &kp, const fa_policy 
 
 // Graph mode: records `prologue` (if any) and the call's rounds as one CUDA graph the
 // first time a key is seen, then replays it; ev0..ev1 bracket the replay.
-int run_ext_graph(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n, int qcap, int max_w,
+int run_ext_graph(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n,
+                  const std::vector<std::pair<uint32_t, int>> &segs, int qcap, int max_w,
                   const std::vector<uint64_t> &extra, const std::function<int(cudaStream_t, uint32_t *)> &prologue,
                   const int32_t *d_wfirst, cudaStream_t s, fa_ext_stats *stats, int32_t *h_wfinal) {
     if (pol && pol->mode != FA_POLICY_SINGLE)
@@ -606,22 +607,39 @@ int run_ext_graph(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t
                                      c->tseq.as<uint8_t>(), qcap, max_w, c->out.as<fa_ext_result>(),
                                      misc_of(c).status, s, &rc0);
     if (rc0) return rc0;
+    // each capacity class's kernel, tuned before recording (tuning cannot run in a capture);
+    // the classes and their choices are part of the key, so a replay has the same ones
+    std::vector<Choice> seg_kc;
+    {
+        uint32_t b = 0;
+        for (auto &sg : segs) {
+            seg_kc.push_back(resolve_choice(c, kp, c->jobs.as<fa_job>(), c->order.as<uint32_t>() + b, sg.first - b,
+                                            c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(), sg.second, max_w,
+                                            c->out.as<fa_ext_result>(), misc_of(c).status, s, &rc0));
+            if (rc0) return rc0;
+            b = sg.first;
+        }
+        c->last_choice = kc;
+    }
     std::vector<uint64_t> extra2 = extra;
     extra2.push_back((uint64_t)kc.kernel << 32 | (uint32_t)kc.tpb);
+    for (size_t k = 0; k < segs.size(); ++k) {
+        extra2.push_back((uint64_t)segs[k].first << 32 | (uint32_t)segs[k].second);
+        extra2.push_back((uint64_t)seg_kc[k].kernel << 32 | (uint32_t)seg_kc[k].tpb);
+    }
     std::vector<uint64_t> key = graph_key(c, kp, pol, n, qcap, max_w, extra2);
     if (!c->gexec || key != c->gkey) {
         if (c->gexec) {
             cudaGraphExecDestroy(c->gexec);
             c->gexec = nullptr;
         }
-        const std::vector<std::pair<uint32_t, int>> segs{{n, qcap}};
         uint32_t launches = 0;
         FA_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
         int rc = prologue ? prologue(s, &launches) : FA_OK;
         if (!rc)
             rc = enqueue_ext(c, kp, pol, n, segs, qcap, max_w, c->jobs.as<fa_job>(), c->order.as<uint32_t>(),
                              c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(), d_wfirst, c->out.as<fa_ext_result>(), s,
-                             true, &launches, nullptr, kc);
+                             true, &launches, nullptr, kc, &seg_kc);
         cudaGraph_t g = nullptr;
         const cudaError_t ec = cudaStreamEndCapture(s, &g);
         if (rc || ec != cudaSuccess) {
@@ -855,7 +873,8 @@ int fa_ext_batch_policy(fa_ctx *c, const fa_params *p, const fa_policy *pol, con
     }
     const int32_t *d_wf = (pol && pol->mode == FA_POLICY_LEARNED) ? c->w_first.as<int32_t>() : nullptr;
     int rc = c->graph
-                 ? run_ext_graph(c, kp, pol, n, max_q, max_band_of(jobs, n), {}, nullptr, d_wf, s, stats, w_final)
+                 ? run_ext_graph(c, kp, pol, n, segs, max_q, max_band_of(jobs, n), {}, nullptr, d_wf, s, stats,
+                                 w_final)
                  : run_ext(c, kp, pol, n, segs, max_q, max_band_of(jobs, n), c->jobs.as<fa_job>(), c->order.as<uint32_t>(),
                            c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(), d_wf, c->out.as<fa_ext_result>(), s, stats,
                            w_final);
@@ -924,7 +943,8 @@ int fa_ext_batch_learned(fa_ctx *c, const fa_params *p, const fa_policy *pol, co
             memcpy(&b, &sd[k], 4);
             extra.push_back((uint64_t)a << 32 | b);
         }
-        int rc = run_ext_graph(c, kp, pol, n, max_q, max_band_of(jobs, n), extra, predict, c->w_first.as<int32_t>(),
+        int rc = run_ext_graph(c, kp, pol, n, segs, max_q, max_band_of(jobs, n), extra, predict,
+                               c->w_first.as<int32_t>(),
                                s, stats, w_final);
         if (rc) return rc;
         if (w_first_out) FA_CUDA(cudaMemcpy(w_first_out, c->w_first.p, 4ull * n, cudaMemcpyDeviceToHost));
