@@ -369,6 +369,58 @@ def bench_mate(args, ctx, lib, dev, stream, flush, skip_cpu=False):
     return res
 
 
+def bench_regions(args, ctx, lib, dev, stream, flush):
+    """Region merge (merge_scores_to_regions) over the results of an extension batch:
+    2M chains of 1-8 seeds (9M seeds, one left and one right result each), device
+    resident, timed with CUDA events; HBM-bound, so reported against the measured copy
+    bandwidth.  Algorithmic bytes per chain: its bounds and read length (8 B), its seed
+    records (24 B each), the left and right results they index (2 x 24 B each) and the
+    region written (48 B)."""
+    import ctypes
+    import torch
+    import ferrousalign_b200 as fa
+    from ferrousalign_b200 import _native as N
+    from oracle import region_oracle as R
+    from ferrousalign_b200 import synth
+    first, qlen, seeds, left, right = synth.workload_regions(2_000_000)
+    n_chains, ns = len(qlen), len(seeds)
+    res = [left, right]
+    opt = fa.region_opts()
+    t = lambda a: torch.from_numpy(a.view(np.uint8)).to(dev)  # noqa: E731
+    d_first, d_qlen, d_seeds, d_left, d_right = t(first), t(qlen), t(seeds), t(res[0]), t(res[1])
+    d_out = torch.empty(n_chains * N.REGION_DT.itemsize, dtype=torch.uint8, device=dev)
+
+    def step():
+        N.check(lib.fa_merge_regions_device(ctx.handle, N.ptr(opt), d_first.data_ptr(), n_chains, d_qlen.data_ptr(),
+                                            d_seeds.data_ptr(), ns, d_left.data_ptr(), ns, d_right.data_ptr(), ns,
+                                            d_out.data_ptr(), ctypes.c_void_p(stream.cuda_stream)))
+
+    times = []
+    with torch.cuda.stream(stream):
+        for it in range(args.warmup + 10):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            e1.synchronize()
+            if it >= args.warmup:
+                times.append(e0.elapsed_time(e1))
+    N.check(lib.fa_ctx_sync(ctx.handle))
+    ms = float(np.median(times))
+    out = d_out.cpu().numpy().view(N.REGION_DT)
+    k = 3000
+    o = {f: int(opt[f][0]) for f in ("a", "pen_clip5", "pen_clip3", "w")}
+    ref = R.merge_regions(o, first[:k + 1], qlen[:k], seeds, res[0], res[1])
+    algo = n_chains * (8 + 48) + ns * (24 + 2 * 24)
+    return {"workload": f"{n_chains} chains, {ns} seeds (1-8 per chain), one left and one right result per seed",
+            "kernel": "merge_regions_kernel", "kernel_ms": ms, "chains_per_s": n_chains / (ms * 1e-3),
+            "roofline": {"bound": "hbm", "achieved": algo / (ms * 1e-3) / 1e9, "peak": 6546.6, "unit": "GB/s",
+                         "frac": algo / (ms * 1e-3) / 1e9 / 6546.6, "algorithmic_bytes": algo,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs"},
+            "bit_exact_sample": bool(np.array_equal(out[:k], ref)), "sample": f"first {k} chains against the oracle"}
+
+
 def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
@@ -414,6 +466,7 @@ def main():
     ap.add_argument("--skip-learned", action="store_true", help="omit the learned-band section")
     ap.add_argument("--skip-mixed", action="store_true", help="omit the mixed mate + extension batch section")
     ap.add_argument("--skip-uneven", action="store_true", help="omit the uneven-length batch section")
+    ap.add_argument("--skip-regions", action="store_true", help="omit the region-merge section")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -580,6 +633,8 @@ def main():
         line["mixed_batch"] = bench_mixed(args, b, p)
     if not args.skip_learned and not args.skip_uneven:
         line["uneven"] = bench_uneven(args, ctx, p)
+    if not args.skip_regions:
+        line["region_merge"] = bench_regions(args, ctx, lib, dev, stream, flush)
     if not args.skip_cpu:
         ref2, tr2, dt, threads = cpu_oracle_rate(b, p, min(CPU_SAMPLE, n))
         line["cpu_baseline"] = {"value": min(CPU_SAMPLE, n) / dt, "unit": "alignments/s", "cores": threads,

@@ -1,8 +1,9 @@
 """B200-native batched banded seed extension and mate-rescue Smith-Waterman.
 
-A drop-in for FerrousAlign's batch-extension call (execute_batch_simd_scoring) and
-its mate-rescue ksw_align2 calls, computed by hand-written sm_100a CUDA kernels behind
-the C ABI in include/ferrous_b200.h.
+A drop-in for FerrousAlign's batch-extension call (execute_batch_simd_scoring), the
+region merge that consumes its results (merge_scores_to_regions) and its mate-rescue
+ksw_align2 calls, computed by hand-written sm_100a CUDA kernels behind the C ABI in
+include/ferrous_b200.h.
 """
 from ._native import Context, NativeError, default_context, load  # noqa: F401
 from .batch_extension import (BandedPairWiseSW, BatchedExtensionJob, BatchExtensionResult,  # noqa: F401
@@ -11,5 +12,6 @@ from .batch_extension import (BandedPairWiseSW, BatchedExtensionJob, BatchExtens
 from .mate_rescue import (MATE_RESCUE_SCORING_MATRIX, Kswr, MateRescueJob, MateRescueResult,  # noqa: F401
                           execute_mate_rescue_batch_with_engine, make_mate_params, mate_sw_batch,
                           mate_xtra)
+from .region import chain_seed_table, merge_scores_to_regions, region_opts  # noqa: F401
 
 __version__ = "0.1.0"

@@ -41,10 +41,16 @@ MATE_JOB_DT = np.dtype([("q_off", "<u8"), ("t_off", "<u8"), ("qlen", "<i4"), ("t
                         ("xtra", "<u4"), ("_pad", "<i4")])
 KSWR_DT = np.dtype([("score", "<i4"), ("te", "<i4"), ("qe", "<i4"), ("score2", "<i4"),
                     ("te2", "<i4"), ("tb", "<i4"), ("qb", "<i4")])
+REGION_OPTS_DT = np.dtype([("a", "<i4"), ("pen_clip5", "<i4"), ("pen_clip3", "<i4"), ("w", "<i4")])
+SEED_EXT_DT = np.dtype([("ref_pos", "<u8"), ("query_pos", "<i4"), ("len", "<i4"), ("left_job", "<i4"),
+                        ("right_job", "<i4")])
+REGION_DT = np.dtype([("rb", "<u8"), ("re", "<u8"), ("qb", "<i4"), ("qe", "<i4"), ("score", "<i4"),
+                      ("truesc", "<i4"), ("seedcov", "<i4"), ("seedlen0", "<i4"), ("w", "<i4"), ("seed", "<i4")])
 
 assert PARAMS_DT.itemsize == 64 and JOB_DT.itemsize == 40 and EXT_RESULT_DT.itemsize == 24
 assert STATS_DT.itemsize == 40 and MATE_PARAMS_DT.itemsize == 48 and MATE_JOB_DT.itemsize == 32
 assert KSWR_DT.itemsize == 28
+assert REGION_OPTS_DT.itemsize == 16 and SEED_EXT_DT.itemsize == 24 and REGION_DT.itemsize == 48
 
 # Every symbol the header declares, with its ctypes signature.
 _P = C.c_void_p
@@ -85,6 +91,10 @@ SIGNATURES = {
     "fa_ext_batch_learned": (C.c_int, [_P, _P, _P, _P, C.c_float, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64,
                                        _P, _P, _P, _P, _P]),
     "fa_mate_sw_batch": (C.c_int, [_P, _P, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64, _P, _P]),
+    "fa_merge_regions": (C.c_int, [_P, _P, _P, C.c_uint32, _P, _P, C.c_uint32, _P, C.c_uint32, _P, C.c_uint32,
+                                   _P]),
+    "fa_merge_regions_device": (C.c_int, [_P, _P, _P, C.c_uint32, _P, _P, C.c_uint32, _P, C.c_uint32, _P,
+                                          C.c_uint32, _P, _P]),
 }
 
 

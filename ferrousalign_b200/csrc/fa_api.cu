@@ -80,6 +80,7 @@ struct fa_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     DevBuf jobs, order, qseq, tseq, out, clamped, cells_job, misc;
     DevBuf ovf;   // two-row kernel: jobs handed on to the int32 kernel
+    DevBuf reg_in, reg_out;   // region merge of host buffers: inputs, regions
     DevBuf w_first, w_cur, prev, kk, w_final, tries, missed, list_a, list_b, hist, feat, wbf, part_n, part_w;
     uint32_t last_launches = 0;
     bool timing = false;
@@ -377,6 +378,7 @@ int read_status(fa_ctx *c, cudaStream_t s) {
     if (st & ST_CAPACITY) return fail(FA_ERR_CAPACITY, "a job exceeded the launch capacity");
     if (st & ST_BLIST) return fail(FA_ERR_CAPACITY, "mate-SW run list overflow");
     if (st & ST_ARG) return fail(FA_ERR_ARG, "a job has h0 <= 0, qlen <= 0 or tlen < 0");
+    if (st & ST_RANGE) return fail(FA_ERR_ARG, "a chain's seed range is malformed");
     return FA_OK;
 }
 
@@ -787,7 +789,7 @@ void fa_ctx_destroy(fa_ctx *c) {
     for (DevBuf *b : {&c->jobs, &c->order, &c->qseq, &c->tseq, &c->out, &c->clamped, &c->cells_job,
                       &c->misc, &c->w_first, &c->w_cur, &c->prev, &c->kk, &c->w_final, &c->tries,
                       &c->missed, &c->list_a, &c->list_b, &c->hist, &c->feat, &c->wbf, &c->part_n,
-                      &c->part_w, &c->ovf})
+                      &c->part_w, &c->ovf, &c->reg_in, &c->reg_out})
         b->release();
     for (int k = 0; k < 2; ++k) {
         if (c->join_ev[k]) cudaEventDestroy(c->join_ev[k]);
@@ -1184,6 +1186,70 @@ int fa_mate_sw_batch_device(fa_ctx *c, const fa_mate_params *p, const fa_mate_jo
     c->last_launches = launches;
     c->last_stream = s;
     return FA_OK;
+}
+
+int fa_merge_regions_device(fa_ctx *c, const fa_region_opts *opt, const uint32_t *d_chain_first, uint32_t n_chains,
+                            const int32_t *d_query_len, const fa_seed_ext *d_seeds, uint32_t n_seeds,
+                            const fa_ext_result *d_left, uint32_t n_left, const fa_ext_result *d_right,
+                            uint32_t n_right, fa_region *d_out, void *stream) {
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    if (!opt) return fail(FA_ERR_ARG, "null options");
+    if (n_chains == 0) return FA_OK;
+    if (!d_chain_first || !d_query_len || !d_out || (n_seeds && !d_seeds) || (n_left && !d_left) ||
+        (n_right && !d_right))
+        return fail(FA_ERR_ARG, "null buffer");
+    FA_CUDA(cudaSetDevice(c->device));
+    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    FA_CUDA(c->misc.ensure(kMiscBytes));
+    FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
+    if (c->timing) FA_CUDA(cudaEventRecord(c->kev0, s));
+    FA_CUDA(launch_merge_regions(*opt, d_chain_first, n_chains, d_query_len, d_seeds, n_seeds, d_left, n_left, d_right,
+                                 n_right, d_out, misc_of(c).status, s));
+    if (c->timing) FA_CUDA(cudaEventRecord(c->kev1, s));
+    c->last_launches = 1;
+    c->last_stream = s;
+    return FA_OK;
+}
+
+int fa_merge_regions(fa_ctx *c, const fa_region_opts *opt, const uint32_t *chain_first, uint32_t n_chains,
+                     const int32_t *query_len, const fa_seed_ext *seeds, uint32_t n_seeds,
+                     const fa_ext_result *left, uint32_t n_left, const fa_ext_result *right, uint32_t n_right,
+                     fa_region *out) {
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    if (!opt) return fail(FA_ERR_ARG, "null options");
+    if (n_chains == 0) return FA_OK;
+    if (!chain_first || !query_len || !out || (n_seeds && !seeds) || (n_left && !left) || (n_right && !right))
+        return fail(FA_ERR_ARG, "null buffer");
+    for (uint32_t k = 0; k < n_chains; ++k)
+        if (chain_first[k + 1] < chain_first[k]) return fail(FA_ERR_ARG, "chain_first is not ascending");
+    if (chain_first[n_chains] > n_seeds) return fail(FA_ERR_ARG, "a chain's seeds run past the seed array");
+    FA_CUDA(cudaSetDevice(c->device));
+    cudaStream_t s = c->stream;
+    // one input buffer: chain bounds | query lengths | seeds | left results | right results
+    auto up16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
+    const size_t b_first = up16(4ull * (n_chains + 1)), b_qlen = up16(4ull * n_chains);
+    const size_t b_seeds = up16(sizeof(fa_seed_ext) * n_seeds), b_left = up16(sizeof(fa_ext_result) * n_left);
+    const size_t b_right = up16(sizeof(fa_ext_result) * n_right);
+    FA_CUDA(c->reg_in.ensure(b_first + b_qlen + b_seeds + b_left + b_right));
+    FA_CUDA(c->reg_out.ensure(sizeof(fa_region) * n_chains));
+    char *d = c->reg_in.as<char>();
+    uint32_t *d_first = reinterpret_cast<uint32_t *>(d);
+    int32_t *d_qlen = reinterpret_cast<int32_t *>(d + b_first);
+    fa_seed_ext *d_seeds = reinterpret_cast<fa_seed_ext *>(d + b_first + b_qlen);
+    fa_ext_result *d_left = reinterpret_cast<fa_ext_result *>(d + b_first + b_qlen + b_seeds);
+    fa_ext_result *d_right = reinterpret_cast<fa_ext_result *>(d + b_first + b_qlen + b_seeds + b_left);
+    FA_CUDA(cudaMemcpyAsync(d_first, chain_first, 4ull * (n_chains + 1), cudaMemcpyHostToDevice, s));
+    FA_CUDA(cudaMemcpyAsync(d_qlen, query_len, 4ull * n_chains, cudaMemcpyHostToDevice, s));
+    if (n_seeds) FA_CUDA(cudaMemcpyAsync(d_seeds, seeds, sizeof(fa_seed_ext) * n_seeds, cudaMemcpyHostToDevice, s));
+    if (n_left) FA_CUDA(cudaMemcpyAsync(d_left, left, sizeof(fa_ext_result) * n_left, cudaMemcpyHostToDevice, s));
+    if (n_right)
+        FA_CUDA(cudaMemcpyAsync(d_right, right, sizeof(fa_ext_result) * n_right, cudaMemcpyHostToDevice, s));
+    if (int rc = fa_merge_regions_device(c, opt, d_first, n_chains, d_qlen, n_seeds ? d_seeds : nullptr, n_seeds,
+                                         n_left ? d_left : nullptr, n_left, n_right ? d_right : nullptr, n_right,
+                                         c->reg_out.as<fa_region>(), s))
+        return rc;
+    FA_CUDA(cudaMemcpyAsync(out, c->reg_out.p, sizeof(fa_region) * n_chains, cudaMemcpyDeviceToHost, s));
+    return read_status(c, s);
 }
 
 int fa_ctx_last_cells(fa_ctx *c, unsigned long long *cells) {

@@ -14,6 +14,7 @@ enum : uint32_t {
     ST_CAPACITY = 1u << 1,   // a job exceeded the launch's length limit
     ST_BLIST    = 1u << 2,   // mate-SW run list overflowed its buffer
     ST_ARG      = 1u << 3,   // a job violates an argument rule (h0 <= 0, qlen <= 0, tlen < 0)
+    ST_RANGE    = 1u << 4,   // a chain's seed range is malformed (region merge)
 };
 
 // Scoring parameters in the form the extension kernel consumes.

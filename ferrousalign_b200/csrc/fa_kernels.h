@@ -118,6 +118,12 @@ int set_last_error(int code, const char *msg);
 cudaError_t launch_mate_split(const fa_mate_job *d_jobs, uint32_t n, uint32_t *d_order_b, uint32_t *d_order_w,
                               uint32_t *d_info, cudaStream_t s);
 
+// Alignment regions from left/right extension results, one thread per chain (region_kernel.cu).
+cudaError_t launch_merge_regions(const fa_region_opts &opt, const uint32_t *d_chain_first, uint32_t n_chains,
+                                 const int32_t *d_query_len, const fa_seed_ext *d_seeds, uint32_t n_seeds,
+                                 const fa_ext_result *d_left, uint32_t n_left, const fa_ext_result *d_right,
+                                 uint32_t n_right, fa_region *d_out, uint32_t *d_status, cudaStream_t s);
+
 // Integer / DPX instruction throughput (ops per second) for the roofline denominator.
 double probe_int_peak(int kind, int sm_count, cudaStream_t s, float *ms_out);
 

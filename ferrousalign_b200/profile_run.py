@@ -4,6 +4,7 @@ Usage: python -m ferrousalign_b200.profile_run [n_jobs] [probe|-] [kernel: 0 aut
        python -m ferrousalign_b200.profile_run learned [n_jobs] [reps] [kernel]   (learned-band path)
        python -m ferrousalign_b200.profile_run bands [n_jobs]            (single runs at fixed bands)
        python -m ferrousalign_b200.profile_run mate [n_jobs] [reps]      (mate-rescue SW, device-resident)
+       python -m ferrousalign_b200.profile_run regions [n_chains] [reps] (region merge, device-resident)
 """
 import ctypes
 import sys
@@ -36,6 +37,29 @@ if len(sys.argv) > 1 and sys.argv[1] == "mate":
             st.synchronize()
             N.check(lib.fa_ctx_sync(ctx.handle))
             print("mate batch ms", e0.elapsed_time(e1))
+    sys.exit(0)
+
+if len(sys.argv) > 1 and sys.argv[1] == "regions":
+    n = int(sys.argv[2]) if len(sys.argv) > 2 else 2_000_000
+    first, qlen, seeds, left, right = synth.workload_regions(n)
+    ctx = fa.Context(0)
+    lib = N.load()
+    dev = torch.device("cuda", 0)
+    st = torch.cuda.Stream(dev)
+    opt = fa.region_opts()
+    t = lambda a: torch.from_numpy(a.view(np.uint8)).to(dev)  # noqa: E731
+    d = [t(first), t(qlen), t(seeds), t(left), t(right)]
+    d_out = torch.empty(n * N.REGION_DT.itemsize, dtype=torch.uint8, device=dev)
+    for r in range(int(sys.argv[3]) if len(sys.argv) > 3 else 1):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        N.check(lib.fa_merge_regions_device(ctx.handle, N.ptr(opt), d[0].data_ptr(), n, d[1].data_ptr(),
+                                            d[2].data_ptr(), len(seeds), d[3].data_ptr(), len(left), d[4].data_ptr(),
+                                            len(right), d_out.data_ptr(), ctypes.c_void_p(st.cuda_stream)))
+        e1.record(st)
+        st.synchronize()
+        N.check(lib.fa_ctx_sync(ctx.handle))
+        print("region merge ms", e0.elapsed_time(e1))
     sys.exit(0)
 
 if len(sys.argv) > 1 and sys.argv[1] in ("learned", "bands"):

@@ -158,3 +158,31 @@ def workload_ext_train(n: int = 5_000_000, seed: int = 4) -> ExtBatch:
 def workload_mate(n: int = 500_000, seed: int = 5, ref_len: int = 10_000_000) -> MateBatch:
     ref = reference(ref_len, seed=seed, n_rate=0.001)
     return mate_jobs(ref, n, seed=seed + 100)
+
+
+def workload_regions(n_chains: int = 2_000_000, seed: int = 17):
+    """Region-merge input shaped like an extension batch's consumer: chains of 1-8 seeds
+    (19-51 bp, nearby reference positions per chain, so seeds cover one another), one left
+    and one right result per seed with scores, ends and end-to-end scores around the clip
+    threshold.  Returns (chain_first, query_len, seeds, left_results, right_results)."""
+    rng = np.random.default_rng(seed)
+    counts = rng.integers(1, 9, n_chains)
+    first = np.concatenate([[0], np.cumsum(counts)]).astype(np.uint32)
+    ns = int(first[-1])
+    seeds = np.zeros(ns, N.SEED_EXT_DT)
+    ci = np.repeat(np.arange(n_chains, dtype=np.uint64), counts)
+    seeds["ref_pos"] = np.uint64(1 << 20) + ci * np.uint64(4096) + rng.integers(0, 200, ns).astype(np.uint64)
+    seeds["query_pos"] = rng.integers(0, 100, ns)
+    seeds["len"] = rng.integers(19, 52, ns)
+    seeds["left_job"] = np.arange(ns)
+    seeds["right_job"] = np.arange(ns)
+    res = []
+    for _ in range(2):
+        r = np.zeros(ns, N.EXT_RESULT_DT)
+        r["score"] = rng.integers(20, 160, ns)
+        r["qle"] = rng.integers(0, 100, ns)
+        r["tle"] = rng.integers(0, 120, ns)
+        r["gtle"] = rng.integers(0, 120, ns)
+        r["gscore"] = r["score"] - rng.integers(-3, 30, ns)
+        res.append(r)
+    return first, np.full(n_chains, 151, np.int32), seeds, res[0], res[1]

@@ -245,6 +245,59 @@ int fa_ext_batch_device_noalloc(const fa_params *p, const fa_job *d_jobs, uint32
                                 const uint8_t *d_qseq, const uint8_t *d_tseq,
                                 fa_ext_result *d_out, void *stream);
 
+/* ---- alignment regions from extension results --------------------------
+ * Replaces merge_scores_to_regions (src/pipelines/linear/region.rs:737-890), the consumer
+ * of the left/right extension batches: for each seed of a chain, the region its
+ * extensions reach -- per side the local bounds (qle/tle) unless gscore > 0 and
+ * gscore > score - pen_clip, then the query end and gtle (bwa-mem2's clip decision,
+ * region.rs:792-835) -- its total score, true score and seed coverage, and per chain
+ * the region of the first seed with the strictly highest total score.  Reference
+ * coordinates stay in FM-index space: the conversion to chromosome coordinates
+ * (coordinates.rs, needs the index) and the chain's frac_rep stay with the caller. */
+typedef struct {
+    int32_t a;           /* match score: a seed alone scores len * a (MemOpt.a) */
+    int32_t pen_clip5;   /* clipping penalty of left extensions (MemOpt.pen_clip5) */
+    int32_t pen_clip3;   /* clipping penalty of right extensions (MemOpt.pen_clip3) */
+    int32_t w;           /* band width recorded in every region (MemOpt.w) */
+} fa_region_opts;
+
+/* One seed of a chain with its extension jobs: Seed + SeedExtensionMapping (region.rs:230-235). */
+typedef struct {
+    uint64_t ref_pos;     /* seed.ref_pos (FM-index space) */
+    int32_t  query_pos;   /* seed.query_pos */
+    int32_t  len;         /* seed.len */
+    int32_t  left_job;    /* index into the left results, -1 = none (an index past them is ignored) */
+    int32_t  right_job;   /* index into the right results, -1 = none */
+} fa_seed_ext;
+
+/* The AlignmentRegion fields (region.rs:47-100) this step sets. */
+typedef struct {
+    uint64_t rb, re;      /* reference bounds [rb, re), FM-index space */
+    int32_t  qb, qe;      /* query bounds [qb, qe) */
+    int32_t  score;       /* total score: left result's score (or len * a) + right result's score */
+    int32_t  truesc;
+    int32_t  seedcov;     /* summed length of the chain's seeds inside the region */
+    int32_t  seedlen0;    /* length of the chosen seed */
+    int32_t  w;
+    int32_t  seed;        /* index into seeds of the chosen seed; -1 = the chain gives no region */
+} fa_region;
+
+/* Chain c owns seeds[chain_first[c] .. chain_first[c+1]) in the reference's mapping order
+ * (the chain's seeds last to first, region.rs:397) and its read has query_len[c] bases;
+ * chain_first has n_chains + 1 entries.  left/right are the results of the left and right
+ * extension batches the jobs index.  out[c] for every chain (seed = -1 for an empty chain). */
+int fa_merge_regions(fa_ctx *ctx, const fa_region_opts *opt, const uint32_t *chain_first, uint32_t n_chains,
+                     const int32_t *query_len, const fa_seed_ext *seeds, uint32_t n_seeds,
+                     const fa_ext_result *left, uint32_t n_left, const fa_ext_result *right, uint32_t n_right,
+                     fa_region *out);
+/* Device-resident variant (no reference counterpart): device pointers, asynchronous on
+ * `stream` (NULL = the context's stream); a malformed chain range is reported by the next
+ * fa_ctx_sync(). */
+int fa_merge_regions_device(fa_ctx *ctx, const fa_region_opts *opt, const uint32_t *d_chain_first,
+                            uint32_t n_chains, const int32_t *d_query_len, const fa_seed_ext *d_seeds,
+                            uint32_t n_seeds, const fa_ext_result *d_left, uint32_t n_left,
+                            const fa_ext_result *d_right, uint32_t n_right, fa_region *d_out, void *stream);
+
 /* ---- mate rescue -------------------------------------------------------
  * Replaces the ksw_align2 calls of execute_mate_rescue_batch_with_engine
  * (src/pipelines/linear/paired/mate_rescue.rs:595-685). */
