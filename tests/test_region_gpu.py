@@ -109,6 +109,15 @@ def test_device_entry_and_argument_checks(built):
     N.check(lib.fa_ctx_sync(ctx.handle))
     got = d_out.cpu().numpy().view(N.REGION_DT)
     assert np.array_equal(got, ref)
+    # result arrays only 4-byte aligned: the field-by-field loads, same regions
+    pad = lambda a: torch.from_numpy(np.concatenate([np.zeros(4, np.uint8), a.view(np.uint8)])).to(dev)  # noqa: E731
+    d_left4, d_right4 = pad(left), pad(right)
+    d_out.zero_()
+    N.check(lib.fa_merge_regions_device(ctx.handle, N.ptr(opt), d_first.data_ptr(), len(qlen), d_qlen.data_ptr(),
+                                        d_seeds.data_ptr(), len(seeds), d_left4.data_ptr() + 4, len(left),
+                                        d_right4.data_ptr() + 4, len(right), d_out.data_ptr(), None))
+    N.check(lib.fa_ctx_sync(ctx.handle))
+    assert np.array_equal(d_out.cpu().numpy().view(N.REGION_DT), ref)
     # a chain range past the seed array: reported by the kernel, no region for it
     bad_first = first.copy()
     bad_first[-1] = len(seeds) + 4
