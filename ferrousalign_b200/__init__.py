@@ -13,5 +13,6 @@ from .mate_rescue import (MATE_RESCUE_SCORING_MATRIX, Kswr, MateRescueJob, MateR
                           execute_mate_rescue_batch_with_engine, make_mate_params, mate_sw_batch,
                           mate_xtra)
 from .region import chain_seed_table, merge_scores_to_regions, region_opts  # noqa: F401
+from .collect import CollectedJobs, collect_extension_jobs, collect_opts, pack_reference  # noqa: F401
 
 __version__ = "0.1.0"

@@ -46,11 +46,19 @@ SEED_EXT_DT = np.dtype([("ref_pos", "<u8"), ("query_pos", "<i4"), ("len", "<i4")
                         ("right_job", "<i4")])
 REGION_DT = np.dtype([("rb", "<u8"), ("re", "<u8"), ("qb", "<i4"), ("qe", "<i4"), ("score", "<i4"),
                       ("truesc", "<i4"), ("seedcov", "<i4"), ("seedlen0", "<i4"), ("w", "<i4"), ("seed", "<i4")])
+COLLECT_OPTS_DT = np.dtype([("a", "<i4"), ("o_del", "<i4"), ("e_del", "<i4"), ("o_ins", "<i4"), ("e_ins", "<i4"),
+                            ("w", "<i4")])
+CHAIN_DT = np.dtype([("read", "<u4"), ("seed_first", "<u4"), ("n_seeds", "<u4"), ("kept", "<i4")])
+SEED_DT = np.dtype([("ref_pos", "<u8"), ("query_pos", "<i4"), ("len", "<i4")])
+COLLECT_COUNTS_DT = np.dtype([("n_left", "<u4"), ("n_right", "<u4"), ("n_seed_ext", "<u4"), ("_pad", "<u4"),
+                              ("qbuf_len", "<u8"), ("tbuf_len", "<u8")])
 
 assert PARAMS_DT.itemsize == 64 and JOB_DT.itemsize == 40 and EXT_RESULT_DT.itemsize == 24
 assert STATS_DT.itemsize == 40 and MATE_PARAMS_DT.itemsize == 48 and MATE_JOB_DT.itemsize == 32
 assert KSWR_DT.itemsize == 28
 assert REGION_OPTS_DT.itemsize == 16 and SEED_EXT_DT.itemsize == 24 and REGION_DT.itemsize == 48
+assert COLLECT_OPTS_DT.itemsize == 24 and CHAIN_DT.itemsize == 16 and SEED_DT.itemsize == 16
+assert COLLECT_COUNTS_DT.itemsize == 32
 
 # Every symbol the header declares, with its ctypes signature.
 _P = C.c_void_p
@@ -91,6 +99,8 @@ SIGNATURES = {
     "fa_ext_batch_learned": (C.c_int, [_P, _P, _P, _P, C.c_float, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64,
                                        _P, _P, _P, _P, _P]),
     "fa_mate_sw_batch": (C.c_int, [_P, _P, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64, _P, _P]),
+    "fa_collect_ext_jobs": (C.c_int, [_P, _P, _P, C.c_uint64, _P, _P, C.c_uint32, _P, C.c_uint32, _P, C.c_uint32,
+                                      _P, _P, _P, _P, C.c_uint64, _P, _P, _P, _P]),
     "fa_merge_regions": (C.c_int, [_P, _P, _P, C.c_uint32, _P, _P, C.c_uint32, _P, C.c_uint32, _P, C.c_uint32,
                                    _P]),
     "fa_merge_regions_device": (C.c_int, [_P, _P, _P, C.c_uint32, _P, _P, C.c_uint32, _P, C.c_uint32, _P,

@@ -81,6 +81,7 @@ struct fa_ctx {
     DevBuf jobs, order, qseq, tseq, out, clamped, cells_job, misc;
     DevBuf ovf;   // two-row kernel: jobs handed on to the int32 kernel
     DevBuf reg_in, reg_out;   // region merge of host buffers: inputs, regions
+    DevBuf col_in, col_plan, col_out;   // job collection: inputs, chain plans + scan sums, outputs
     DevBuf w_first, w_cur, prev, kk, w_final, tries, missed, list_a, list_b, hist, feat, wbf, part_n, part_w;
     uint32_t last_launches = 0;
     bool timing = false;
@@ -789,7 +790,7 @@ void fa_ctx_destroy(fa_ctx *c) {
     for (DevBuf *b : {&c->jobs, &c->order, &c->qseq, &c->tseq, &c->out, &c->clamped, &c->cells_job,
                       &c->misc, &c->w_first, &c->w_cur, &c->prev, &c->kk, &c->w_final, &c->tries,
                       &c->missed, &c->list_a, &c->list_b, &c->hist, &c->feat, &c->wbf, &c->part_n,
-                      &c->part_w, &c->ovf, &c->reg_in, &c->reg_out})
+                      &c->part_w, &c->ovf, &c->reg_in, &c->reg_out, &c->col_in, &c->col_plan, &c->col_out})
         b->release();
     for (int k = 0; k < 2; ++k) {
         if (c->join_ev[k]) cudaEventDestroy(c->join_ev[k]);
@@ -1250,6 +1251,104 @@ int fa_merge_regions(fa_ctx *c, const fa_region_opts *opt, const uint32_t *chain
         return rc;
     FA_CUDA(cudaMemcpyAsync(out, c->reg_out.p, sizeof(fa_region) * n_chains, cudaMemcpyDeviceToHost, s));
     return read_status(c, s);
+}
+
+int fa_collect_ext_jobs(fa_ctx *c, const fa_collect_opts *opt, const uint8_t *pac, uint64_t l_pac,
+                        const uint8_t *reads, const uint64_t *read_off, uint32_t n_reads,
+                        const fa_chain *chains, uint32_t n_chains, const fa_seed *seeds, uint32_t n_seeds,
+                        fa_job *left_jobs, fa_job *right_jobs, uint8_t *qbuf, uint8_t *tbuf, uint64_t tbuf_cap,
+                        fa_seed_ext *seed_ext, uint32_t *chain_first, uint64_t *chain_win,
+                        fa_collect_counts *counts) {
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    if (!opt || !counts || !chain_first) return fail(FA_ERR_ARG, "null argument");
+    *counts = fa_collect_counts{};
+    if (n_chains && (!chains || !chain_win)) return fail(FA_ERR_ARG, "null chain buffer");
+    if (n_reads && (!read_off || !reads)) return fail(FA_ERR_ARG, "null read buffer");
+    if (n_seeds && !seeds) return fail(FA_ERR_ARG, "null seed buffer");
+    if (l_pac == 0 || !pac) return fail(FA_ERR_ARG, "empty packed reference");
+    if (l_pac > (1ull << 62)) return fail(FA_ERR_ARG, "packed reference too long");
+    // the reference's slices and windows would panic on these (collect_soa.rs:150-209)
+    for (uint32_t r = 0; r < n_reads; ++r) {
+        if (read_off[r + 1] < read_off[r]) return fail(FA_ERR_ARG, "read_off is not ascending");
+        if (read_off[r + 1] - read_off[r] > (uint64_t)INT32_MAX) return fail(FA_ERR_ARG, "a read is too long");
+    }
+    for (uint32_t k = 0; k < n_chains; ++k) {
+        const fa_chain &ch = chains[k];
+        if (ch.read >= n_reads) return fail(FA_ERR_ARG, "a chain's read index is out of range");
+        if ((uint64_t)ch.seed_first + ch.n_seeds > n_seeds) return fail(FA_ERR_ARG, "a chain's seeds run past the seed array");
+        if (!ch.kept) continue;
+        const int64_t qlen = (int64_t)(read_off[ch.read + 1] - read_off[ch.read]);
+        for (uint32_t s = 0; s < ch.n_seeds; ++s) {
+            const fa_seed &sd = seeds[ch.seed_first + s];
+            if (sd.query_pos < 0 || sd.len < 0 || (int64_t)sd.query_pos + sd.len > qlen)
+                return fail(FA_ERR_ARG, "a seed lies outside its read");
+            if (sd.ref_pos >= (l_pac << 1) || sd.ref_pos + (uint64_t)sd.len > (l_pac << 1))
+                return fail(FA_ERR_ARG, "a seed lies outside the reference");
+        }
+    }
+    chain_first[0] = 0;
+    if (n_chains == 0) return FA_OK;
+    FA_CUDA(cudaSetDevice(c->device));
+    cudaStream_t s = c->stream;
+    auto up16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
+    const uint64_t read_bytes = read_off[n_reads];   // reads[0 .. read_off[n_reads]) travel
+    const size_t b_pac = up16((size_t)((l_pac + 3) / 4)), b_reads = up16(read_bytes + 1);
+    const size_t b_off = up16(8ull * (n_reads + 1)), b_chains = up16(sizeof(fa_chain) * n_chains);
+    const size_t b_seeds = up16(sizeof(fa_seed) * n_seeds);
+    FA_CUDA(c->col_in.ensure(b_pac + b_reads + b_off + b_chains + b_seeds));
+    char *in = c->col_in.as<char>();
+    uint8_t *d_pac = reinterpret_cast<uint8_t *>(in);
+    uint8_t *d_reads = reinterpret_cast<uint8_t *>(in + b_pac);
+    uint64_t *d_off = reinterpret_cast<uint64_t *>(in + b_pac + b_reads);
+    fa_chain *d_chains = reinterpret_cast<fa_chain *>(in + b_pac + b_reads + b_off);
+    fa_seed *d_seeds = reinterpret_cast<fa_seed *>(in + b_pac + b_reads + b_off + b_chains);
+    FA_CUDA(cudaMemcpyAsync(d_pac, pac, (size_t)((l_pac + 3) / 4), cudaMemcpyHostToDevice, s));
+    if (read_bytes) FA_CUDA(cudaMemcpyAsync(d_reads, reads, read_bytes, cudaMemcpyHostToDevice, s));
+    FA_CUDA(cudaMemcpyAsync(d_off, read_off, 8ull * (n_reads + 1), cudaMemcpyHostToDevice, s));
+    FA_CUDA(cudaMemcpyAsync(d_chains, chains, sizeof(fa_chain) * n_chains, cudaMemcpyHostToDevice, s));
+    if (n_seeds) FA_CUDA(cudaMemcpyAsync(d_seeds, seeds, sizeof(fa_seed) * n_seeds, cudaMemcpyHostToDevice, s));
+    const size_t nb = collect_scan_blocks(n_chains);
+    const size_t b_plan = up16(sizeof(CollectPlan) * n_chains);
+    FA_CUDA(c->col_plan.ensure(b_plan + sizeof(ulonglong4) * (nb + 1)));
+    CollectPlan *d_plan = c->col_plan.as<CollectPlan>();
+    ulonglong4 *d_sums = reinterpret_cast<ulonglong4 *>(c->col_plan.as<char>() + b_plan);
+    FA_CUDA(launch_collect_plan(*opt, l_pac, d_off, d_chains, n_chains, d_seeds, d_plan, d_sums, s));
+    ulonglong4 tot;
+    FA_CUDA(cudaMemcpyAsync(&tot, d_sums + nb, sizeof(tot), cudaMemcpyDeviceToHost, s));
+    FA_CUDA(cudaStreamSynchronize(s));
+    counts->n_left = (uint32_t)tot.y;
+    counts->n_right = (uint32_t)tot.z;
+    counts->n_seed_ext = (uint32_t)tot.w;
+    counts->qbuf_len = 2 * read_bytes;
+    counts->tbuf_len = tot.x;
+    if (tot.x > tbuf_cap) return fail(FA_ERR_CAPACITY, "tbuf_cap is below the windows' bytes (counts->tbuf_len)");
+    if ((tot.y && !left_jobs) || (tot.z && !right_jobs) || (tot.w && !seed_ext) || (read_bytes && !qbuf) ||
+        (tot.x && !tbuf))
+        return fail(FA_ERR_ARG, "null output buffer");
+    const size_t b_left = up16(sizeof(fa_job) * tot.y), b_right = up16(sizeof(fa_job) * tot.z);
+    const size_t b_q = up16(2 * read_bytes + 1), b_t = up16(tot.x + 1), b_ext = up16(sizeof(fa_seed_ext) * tot.w);
+    const size_t b_first = up16(4ull * (n_chains + 1)), b_win = up16(16ull * n_chains);
+    FA_CUDA(c->col_out.ensure(b_left + b_right + b_q + b_t + b_ext + b_first + b_win));
+    char *o = c->col_out.as<char>();
+    fa_job *d_left = reinterpret_cast<fa_job *>(o);
+    fa_job *d_right = reinterpret_cast<fa_job *>(o + b_left);
+    uint8_t *d_q = reinterpret_cast<uint8_t *>(o + b_left + b_right);
+    uint8_t *d_t = reinterpret_cast<uint8_t *>(o + b_left + b_right + b_q);
+    fa_seed_ext *d_ext = reinterpret_cast<fa_seed_ext *>(o + b_left + b_right + b_q + b_t);
+    uint32_t *d_first = reinterpret_cast<uint32_t *>(o + b_left + b_right + b_q + b_t + b_ext);
+    uint64_t *d_win = reinterpret_cast<uint64_t *>(o + b_left + b_right + b_q + b_t + b_ext + b_first);
+    FA_CUDA(launch_collect_fill(*opt, d_pac, l_pac, d_reads, d_off, n_reads, d_chains, n_chains, d_seeds, d_plan,
+                                d_left, d_right, d_q, d_t, d_ext, d_first, d_win, s));
+    if (tot.y) FA_CUDA(cudaMemcpyAsync(left_jobs, d_left, sizeof(fa_job) * tot.y, cudaMemcpyDeviceToHost, s));
+    if (tot.z) FA_CUDA(cudaMemcpyAsync(right_jobs, d_right, sizeof(fa_job) * tot.z, cudaMemcpyDeviceToHost, s));
+    if (read_bytes) FA_CUDA(cudaMemcpyAsync(qbuf, d_q, 2 * read_bytes, cudaMemcpyDeviceToHost, s));
+    if (tot.x) FA_CUDA(cudaMemcpyAsync(tbuf, d_t, tot.x, cudaMemcpyDeviceToHost, s));
+    if (tot.w) FA_CUDA(cudaMemcpyAsync(seed_ext, d_ext, sizeof(fa_seed_ext) * tot.w, cudaMemcpyDeviceToHost, s));
+    FA_CUDA(cudaMemcpyAsync(chain_first, d_first, 4ull * n_chains, cudaMemcpyDeviceToHost, s));
+    FA_CUDA(cudaMemcpyAsync(chain_win, d_win, 16ull * n_chains, cudaMemcpyDeviceToHost, s));
+    FA_CUDA(cudaStreamSynchronize(s));
+    chain_first[n_chains] = (uint32_t)tot.w;
+    return FA_OK;
 }
 
 int fa_ctx_last_cells(fa_ctx *c, unsigned long long *cells) {

@@ -124,6 +124,27 @@ cudaError_t launch_merge_regions(const fa_region_opts &opt, const uint32_t *d_ch
                                  const fa_ext_result *d_left, uint32_t n_left, const fa_ext_result *d_right,
                                  uint32_t n_right, fa_region *d_out, uint32_t *d_status, cudaStream_t s);
 
+// Extension jobs from chains and a packed reference (collect_kernel.cu).  Per chain: its
+// window [r0, r1), counters v = {window bytes (forward + reversed), left jobs, right jobs,
+// seed-table entries} and their exclusive prefix sums off over the chains.
+struct CollectPlan {
+    uint64_t r0, r1;
+    unsigned long long v[4];
+    unsigned long long off[4];
+};
+int collect_max_gap(const fa_collect_opts &o, int qlen);
+size_t collect_scan_blocks(uint32_t n_chains);   // entries of the scan's block-sum array, less one
+// plan + scan; d_sums holds collect_scan_blocks(n) + 1 entries, the last one the totals
+cudaError_t launch_collect_plan(const fa_collect_opts &opt, uint64_t l_pac, const uint64_t *d_read_off,
+                                const fa_chain *d_chains, uint32_t n_chains, const fa_seed *d_seeds,
+                                CollectPlan *d_plan, ulonglong4 *d_sums, cudaStream_t s);
+cudaError_t launch_collect_fill(const fa_collect_opts &opt, const uint8_t *d_pac, uint64_t l_pac,
+                                const uint8_t *d_reads, const uint64_t *d_read_off, uint32_t n_reads,
+                                const fa_chain *d_chains, uint32_t n_chains, const fa_seed *d_seeds,
+                                const CollectPlan *d_plan, fa_job *d_left, fa_job *d_right, uint8_t *d_qbuf,
+                                uint8_t *d_tbuf, fa_seed_ext *d_seed_ext, uint32_t *d_chain_first,
+                                uint64_t *d_chain_win, cudaStream_t s);
+
 // Integer / DPX instruction throughput (ops per second) for the roofline denominator.
 double probe_int_peak(int kind, int sm_count, cudaStream_t s, float *ms_out);
 

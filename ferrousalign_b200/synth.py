@@ -186,3 +186,57 @@ def workload_regions(n_chains: int = 2_000_000, seed: int = 17):
         r["gscore"] = r["score"] - rng.integers(-3, 30, ns)
         res.append(r)
     return first, np.full(n_chains, 151, np.int32), seeds, res[0], res[1]
+
+
+def workload_chains(n_reads: int = 100_000, seed: int = 21, ref_len: int = 10_000_000, read_len: int = 151,
+                    w: int = 100):
+    """Chains of seeds for the job collection: reads sampled from either strand of a seeded
+    reference (1% substitutions), 1-3 chains per read, each of 1-4 exact seeds of 19-40 bp
+    along the read's true diagonal (occasionally shifted by a small indel-like offset), a
+    tenth of the chains placed at a random position instead, and one chain in twenty marked
+    as not kept.  Positions are in FM-index space: forward [0, l_pac), reverse strand
+    [l_pac, 2 l_pac).  Returns (ref_codes, reads, read_off, chains, seeds)."""
+    rng = np.random.default_rng(seed)
+    ref = reference(ref_len, seed=seed, n_rate=0.0, repeat_frac=0.02)
+    l_pac = len(ref)
+    reads = np.empty(n_reads * read_len, np.uint8)
+    read_off = np.arange(n_reads + 1, dtype=np.uint64) * read_len
+    starts = rng.integers(0, l_pac - read_len, n_reads)
+    strand = rng.random(n_reads) < 0.5
+    for r in range(n_reads):
+        s = ref[starts[r]:starts[r] + read_len] & 3
+        if strand[r]:
+            s = (3 - s)[::-1]
+        reads[r * read_len:(r + 1) * read_len] = s
+    sub = rng.random(len(reads)) < 0.01
+    reads[sub] = (reads[sub] + rng.integers(1, 4, int(sub.sum()))) & 3
+    # FM coordinate of read position 0: forward start, or the reverse-strand image
+    origin = np.where(strand, 2 * l_pac - (starts + read_len), starts).astype(np.int64)
+    n_ch = rng.integers(1, 4, n_reads)
+    chain_read = np.repeat(np.arange(n_reads), n_ch)
+    nc = len(chain_read)
+    n_sd = rng.integers(1, 5, nc)
+    chains = np.zeros(nc, N.CHAIN_DT)
+    chains["read"] = chain_read
+    chains["n_seeds"] = n_sd
+    chains["seed_first"] = np.concatenate([[0], np.cumsum(n_sd)[:-1]])
+    chains["kept"] = (rng.random(nc) >= 0.05).astype(np.int32)
+    ns = int(n_sd.sum())
+    seeds = np.zeros(ns, N.SEED_DT)
+    ci = np.repeat(np.arange(nc), n_sd)
+    ln = rng.integers(19, 41, ns)
+    qp = rng.integers(0, read_len - ln + 1)
+    base = origin[chain_read[ci]]
+    rand_chain = rng.random(nc) < 0.1
+    strand_c = strand[chain_read]
+    rand_origin = np.where(strand_c, l_pac + rng.integers(0, l_pac - 2 * read_len, nc),
+                           rng.integers(0, l_pac - 2 * read_len, nc))
+    base = np.where(rand_chain[ci], rand_origin[ci], base)
+    shift = np.where(rng.random(ns) < 0.1, rng.integers(-3, 4, ns), 0)
+    rp = base + qp + shift
+    lo = np.where(base >= l_pac, l_pac, 0)
+    hi = np.where(base >= l_pac, 2 * l_pac, l_pac) - ln
+    seeds["ref_pos"] = np.clip(rp, lo, hi).astype(np.uint64)
+    seeds["query_pos"] = qp
+    seeds["len"] = ln
+    return ref, reads, read_off, chains, seeds

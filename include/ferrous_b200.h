@@ -298,6 +298,58 @@ int fa_merge_regions_device(fa_ctx *ctx, const fa_region_opts *opt, const uint32
                             uint32_t n_seeds, const fa_ext_result *d_left, uint32_t n_left,
                             const fa_ext_result *d_right, uint32_t n_right, fa_region *d_out, void *stream);
 
+/* ---- extension jobs from chains ----------------------------------------
+ * Replaces collect_extension_jobs_batch_soa (src/pipelines/linear/batch_extension/
+ * collect_soa.rs:28-230): per kept chain with seeds, the reference window
+ * [rmax0, rmax1) its seeds can reach (cal_max_gap margins, chaining.rs:1108-1116, kept on
+ * one strand), fetched from the 2-bit packed reference (bntseq.rs:451-535: the reverse
+ * strand is the reverse complement of the forward one), and for each seed, last to first,
+ * a left job (reversed read prefix against the reversed window before the seed, h0 =
+ * len * a) and a right job (read suffix against the window after the seed, h0 = 0), with
+ * the seed table the region merge reads.  Sequences are written once per read (forward |
+ * reversed) and once per chain window (forward | reversed); jobs address slices of them. */
+typedef struct {
+    int32_t a;                  /* match score */
+    int32_t o_del, e_del, o_ins, e_ins;
+    int32_t w;                  /* band width given to every job (MemOpt.w) */
+} fa_collect_opts;
+
+typedef struct {                /* one chain of a read (SoA chain batch entry) */
+    uint32_t read;              /* index of its read */
+    uint32_t seed_first;        /* its seeds: seeds[seed_first .. seed_first + n_seeds), chain order */
+    uint32_t n_seeds;
+    int32_t  kept;              /* 0: filtered out, no jobs (collect_soa.rs:74-80) */
+} fa_chain;
+
+typedef struct {                /* one seed (SoA seed batch entry) */
+    uint64_t ref_pos;           /* FM-index space: [0, l_pac) forward, [l_pac, 2 l_pac) reverse */
+    int32_t  query_pos;
+    int32_t  len;
+} fa_seed;
+
+typedef struct {
+    uint32_t n_left, n_right;   /* jobs written */
+    uint32_t n_seed_ext;        /* seed-table entries written */
+    uint32_t _pad;
+    uint64_t qbuf_len, tbuf_len;   /* bytes of query / target sequence the jobs address */
+} fa_collect_counts;
+
+/* reads: read r is reads[read_off[r] .. read_off[r+1]) (codes 0-4); pac: the .pac layout,
+ * base k in bits 7-6 of byte k/4 for k % 4 == 0, down to bits 1-0 for k % 4 == 3.
+ * Outputs (caller-allocated): left_jobs/right_jobs hold up to n_seeds jobs each, in the
+ * reference's order; their q_off/t_off address qbuf (2 x the reads' bytes) and tbuf
+ * (tbuf_cap bytes); seed_ext + chain_first (n_chains + 1) are the region-merge seed table,
+ * seed_ext's left_job/right_job being indices into left_jobs/right_jobs (the reference
+ * numbers them per read; here across the batch); chain_win gets each chain's [rmax0,
+ * rmax1) (two u64 per chain; 0,0 for a chain without jobs).  When tbuf_cap is too small
+ * nothing is written except counts (with the bytes needed) and FA_ERR_CAPACITY returns. */
+int fa_collect_ext_jobs(fa_ctx *ctx, const fa_collect_opts *opt, const uint8_t *pac, uint64_t l_pac,
+                        const uint8_t *reads, const uint64_t *read_off, uint32_t n_reads,
+                        const fa_chain *chains, uint32_t n_chains, const fa_seed *seeds, uint32_t n_seeds,
+                        fa_job *left_jobs, fa_job *right_jobs, uint8_t *qbuf, uint8_t *tbuf, uint64_t tbuf_cap,
+                        fa_seed_ext *seed_ext, uint32_t *chain_first, uint64_t *chain_win,
+                        fa_collect_counts *counts);
+
 /* ---- mate rescue -------------------------------------------------------
  * Replaces the ksw_align2 calls of execute_mate_rescue_batch_with_engine
  * (src/pipelines/linear/paired/mate_rescue.rs:595-685). */

@@ -1,0 +1,110 @@
+"""The job-collection kernels (csrc/collect_kernel.cu) against the CPU restatement of
+collect_extension_jobs_batch_soa (oracle/collect_oracle.py): every job's query and target
+bases, h0, band and direction, the seed table, the chain windows; then the whole
+chain -> jobs -> extension -> region path against the oracle's.  Bit-exact."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle_collect(opts, pac, l_pac, reads, read_off, chains, seeds):
+    from oracle import collect_oracle as C
+    o = {k: int(opts[k][0]) for k in ("a", "o_del", "e_del", "o_ins", "e_ins", "w")}
+    rl = [list(reads[int(read_off[r]):int(read_off[r + 1])]) for r in range(len(read_off) - 1)]
+    ch = [{k: int(c[k]) for k in ("read", "seed_first", "n_seeds", "kept")} for c in chains]
+    sd = [{"ref_pos": int(s["ref_pos"]), "query_pos": int(s["query_pos"]), "len": int(s["len"])} for s in seeds]
+    return C.collect(o, pac, l_pac, rl, ch, sd)
+
+
+def check_same(got, want):
+    for side, jobs in (("left", got.left_jobs), ("right", got.right_jobs)):
+        ref = want[side]
+        assert len(jobs) == len(ref), side
+        for j, (q, t, h0, w, d) in zip(jobs, ref):
+            assert (int(j["h0"]), int(j["w"]), int(j["dir"])) == (h0, w, d)
+            assert list(got.qbuf[int(j["q_off"]):int(j["q_off"]) + int(j["qlen"])]) == q
+            assert list(got.tbuf[int(j["t_off"]):int(j["t_off"]) + int(j["tlen"])]) == t
+    ext = want["seed_ext"]
+    assert len(got.seed_ext) == len(ext)
+    for e, r in zip(got.seed_ext, ext):
+        assert tuple(int(e[k]) for k in ("ref_pos", "query_pos", "len", "left_job", "right_job")) == \
+            tuple(r[k] for k in ("ref_pos", "query_pos", "len", "left_job", "right_job"))
+    assert list(got.chain_first) == want["chain_first"]
+    assert [tuple(int(x) for x in w) for w in got.chain_win] == want["chain_win"]
+
+
+def test_chains_of_both_strands_match_oracle(built):
+    from ferrousalign_b200 import collect as K, synth
+    ref, reads, off, chains, seeds = synth.workload_chains(3000, ref_len=2_000_000)
+    pac, l_pac = K.pack_reference(ref)
+    for opts in (K.collect_opts(), K.collect_opts(a=2, o_del=5, e_del=2, o_ins=4, e_ins=0, w=30)):
+        got = K.collect_extension_jobs(pac, l_pac, reads, off, chains, seeds, opts=opts)
+        want = oracle_collect(opts, pac, l_pac, reads, off, chains, seeds)
+        assert len(want["left"]) > 1000 and len(want["right"]) > 1000
+        check_same(got, want)
+
+
+def test_chain_to_region_path(built):
+    """Collected jobs through the extension kernels (right jobs with the seed's score as h0,
+    the bwa-mem2 form: h0 = 0 is outside ksw_extend2's contract) and the region merge, the
+    same jobs through the oracle's extension and merge."""
+    import ferrousalign_b200 as fa
+    from ferrousalign_b200 import collect as K, synth
+    from oracle import ksw_oracle as O, region_oracle as R
+    ref, reads, off, chains, seeds = synth.workload_chains(4000, ref_len=2_000_000)
+    pac, l_pac = K.pack_reference(ref)
+    got = K.collect_extension_jobs(pac, l_pac, reads, off, chains, seeds)
+    p = fa.BandedPairWiseSW().to_struct()
+    right = got.right_jobs.copy()
+    owner = np.full(len(right), -1)
+    for e in got.seed_ext:
+        if e["right_job"] >= 0:
+            owner[e["right_job"]] = e["len"]
+    right["h0"] = owner
+    assert (right["h0"] > 0).all()
+    lres, _, _ = fa.extend_batch(p, got.left_jobs, got.qbuf, got.tbuf)
+    rres, _, _ = fa.extend_batch(p, right, got.qbuf, got.tbuf)
+    lref, _ = O.ext_batch(p, got.left_jobs, got.qbuf, got.tbuf)
+    rref, _ = O.ext_batch(p, right, got.qbuf, got.tbuf)
+    assert np.array_equal(lres, lref) and np.array_equal(rres, rref)
+    qlen = np.diff(off.astype(np.int64))[chains["read"]].astype(np.int32)
+    regions = fa.merge_scores_to_regions(got.chain_first, qlen, got.seed_ext, lres, rres)
+    want = R.merge_regions({"a": 1, "pen_clip5": 5, "pen_clip3": 5, "w": 100}, got.chain_first, qlen,
+                           got.seed_ext, lref, rref)
+    assert np.array_equal(regions, want)
+    assert (regions["seed"] >= 0).sum() > 0.9 * len(chains)
+
+
+def test_argument_checks_and_capacity(built):
+    from ferrousalign_b200 import _native as N, collect as K, synth
+    ref, reads, off, chains, seeds = synth.workload_chains(200, ref_len=200_000)
+    pac, l_pac = K.pack_reference(ref)
+    lib = N.load()
+    ctx = N.Context(0)
+    opts = K.collect_opts()
+    n = len(seeds)
+    left, right = np.zeros(n, N.JOB_DT), np.zeros(n, N.JOB_DT)
+    qbuf = np.zeros(2 * len(reads), np.uint8)
+    tbuf = np.zeros(16, np.uint8)
+    ext = np.zeros(n, N.SEED_EXT_DT)
+    first = np.zeros(len(chains) + 1, np.uint32)
+    win = np.zeros((len(chains), 2), np.uint64)
+    counts = np.zeros(1, N.COLLECT_COUNTS_DT)
+
+    def call(ch=chains, sd=seeds, cap=len(tbuf)):
+        return lib.fa_collect_ext_jobs(ctx.handle, N.ptr(opts), N.ptr(pac), l_pac, N.ptr(reads), N.ptr(off),
+                                       len(off) - 1, N.ptr(ch), len(ch), N.ptr(sd), len(sd), N.ptr(left),
+                                       N.ptr(right), N.ptr(qbuf), N.ptr(tbuf), cap, N.ptr(ext), N.ptr(first),
+                                       N.ptr(win), N.ptr(counts))
+    assert call() == N.FA_ERR_CAPACITY and counts["tbuf_len"][0] > 16    # the bytes needed come back
+    bad = seeds.copy()
+    bad["query_pos"][0] = 200                                          # past its read
+    assert call(sd=bad) == N.FA_ERR_ARG
+    bad = seeds.copy()
+    bad["ref_pos"][0] = 2 * l_pac                                      # past the reference
+    assert call(sd=bad) == N.FA_ERR_ARG
+    badc = chains.copy()
+    badc["read"][0] = 10**6
+    assert call(ch=badc) == N.FA_ERR_ARG
+    ctx.close()
