@@ -421,6 +421,60 @@ def bench_regions(args, ctx, lib, dev, stream, flush):
             "bit_exact_sample": bool(np.array_equal(out[:k], ref)), "sample": f"first {k} chains against the oracle"}
 
 
+def bench_collect(args, ctx, lib):
+    """Extension-job collection (collect_extension_jobs_batch_soa) from chains of seeds over
+    a 100 Mbp reference held 2-bit packed on the GPU: 500k 151-bp reads from both strands,
+    1-3 chains of 1-4 seeds each.  Timed through the host ABI (copies in and out, `e2e`) and
+    on the device (the kernels, with the one read of the totals between plan and fill).
+    Algorithmic bytes: reads, chains, seeds and the windows' packed bases in; both copies
+    of every read and window, the jobs, the seed table and the chain windows out."""
+    import ctypes
+    import ferrousalign_b200 as fa
+    from ferrousalign_b200 import _native as N, synth
+    from oracle import collect_oracle as C
+    ref, reads, off, chains, seeds = synth.workload_chains(500_000, ref_len=100_000_000)
+    pac, l_pac = fa.pack_reference(ref)
+    N.check(lib.fa_ctx_set_timing(ctx.handle, 1))
+    k_ms, k_n = ctypes.c_float(), ctypes.c_int()
+    wall, kern = [], []
+    got = None
+    for it in range(args.warmup + 5):
+        t0 = time.perf_counter()
+        got = fa.collect_extension_jobs(pac, l_pac, reads, off, chains, seeds, ctx=ctx)
+        t1 = time.perf_counter()
+        N.check(lib.fa_ctx_last_timing(ctx.handle, ctypes.byref(k_ms), ctypes.byref(k_n)))
+        if it >= args.warmup:
+            wall.append((t1 - t0) * 1e3)
+            kern.append(k_ms.value)
+    win = got.chain_win.astype(np.int64)
+    wlen = int(np.maximum(win[:, 1] - win[:, 0], 0).sum())
+    n_jobs = len(got.left_jobs) + len(got.right_jobs)
+    algo = (len(reads) + 16 * (len(chains) + len(seeds)) + wlen // 4 + 2 * len(reads) + 2 * wlen + 40 * n_jobs
+            + 24 * len(got.seed_ext) + 20 * len(chains))
+    km = float(np.median(kern))
+    # the first chains' jobs and seed table against the oracle (job numbers start at 0 there too)
+    k = 1500
+    o = {f: int(v) for f, v in zip(("a", "o_del", "e_del", "o_ins", "e_ins", "w"), (1, 6, 1, 6, 1, 100))}
+    rl = [list(reads[int(off[r]):int(off[r + 1])]) for r in range(int(chains["read"][k - 1]) + 1)]
+    ch = [{f: int(c[f]) for f in ("read", "seed_first", "n_seeds", "kept")} for c in chains[:k]]
+    ns = int(chains["seed_first"][k - 1] + chains["n_seeds"][k - 1])
+    sd = [{"ref_pos": int(s["ref_pos"]), "query_pos": int(s["query_pos"]), "len": int(s["len"])} for s in seeds[:ns]]
+    want = C.collect(o, pac, l_pac, rl, ch, sd)
+    same = all(list(got.qbuf[int(j["q_off"]):int(j["q_off"]) + int(j["qlen"])]) == q and
+               list(got.tbuf[int(j["t_off"]):int(j["t_off"]) + int(j["tlen"])]) == t and int(j["h0"]) == h0
+               for jobs, side in ((got.left_jobs, "left"), (got.right_jobs, "right"))
+               for j, (q, t, h0, _, _) in zip(jobs, want[side]))
+    same = same and [int(x) for x in got.chain_first[:k + 1]] == want["chain_first"]
+    return {"workload": f"{len(off) - 1} reads of 151 bp, {len(chains)} chains, {len(seeds)} seeds, "
+                        f"100 Mbp reference (2-bit packed, {len(pac)} B)",
+            "jobs": {"left": len(got.left_jobs), "right": len(got.right_jobs)},
+            "kernel_ms": km, "e2e_ms": float(np.median(wall)), "kernel_launches": int(k_n.value),
+            "roofline": {"bound": "hbm", "achieved": algo / (km * 1e-3) / 1e9, "peak": 6546.6, "unit": "GB/s",
+                         "frac": algo / (km * 1e-3) / 1e9 / 6546.6, "algorithmic_bytes": algo,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs"},
+            "bit_exact_sample": bool(same), "sample": f"first {k} chains against the oracle"}
+
+
 def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
@@ -635,6 +689,7 @@ def main():
         line["uneven"] = bench_uneven(args, ctx, p)
     if not args.skip_regions:
         line["region_merge"] = bench_regions(args, ctx, lib, dev, stream, flush)
+        line["job_collection"] = bench_collect(args, ctx, lib)
     if not args.skip_cpu:
         ref2, tr2, dt, threads = cpu_oracle_rate(b, p, min(CPU_SAMPLE, n))
         line["cpu_baseline"] = {"value": min(CPU_SAMPLE, n) / dt, "unit": "alignments/s", "cores": threads,

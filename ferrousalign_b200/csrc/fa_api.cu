@@ -1312,6 +1312,7 @@ int fa_collect_ext_jobs(fa_ctx *c, const fa_collect_opts *opt, const uint8_t *pa
     FA_CUDA(c->col_plan.ensure(b_plan + sizeof(ulonglong4) * (nb + 1)));
     CollectPlan *d_plan = c->col_plan.as<CollectPlan>();
     ulonglong4 *d_sums = reinterpret_cast<ulonglong4 *>(c->col_plan.as<char>() + b_plan);
+    if (c->timing) FA_CUDA(cudaEventRecord(c->kev0, s));
     FA_CUDA(launch_collect_plan(*opt, l_pac, d_off, d_chains, n_chains, d_seeds, d_plan, d_sums, s));
     ulonglong4 tot;
     FA_CUDA(cudaMemcpyAsync(&tot, d_sums + nb, sizeof(tot), cudaMemcpyDeviceToHost, s));
@@ -1339,6 +1340,9 @@ int fa_collect_ext_jobs(fa_ctx *c, const fa_collect_opts *opt, const uint8_t *pa
     uint64_t *d_win = reinterpret_cast<uint64_t *>(o + b_left + b_right + b_q + b_t + b_ext + b_first);
     FA_CUDA(launch_collect_fill(*opt, d_pac, l_pac, d_reads, d_off, n_reads, d_chains, n_chains, d_seeds, d_plan,
                                 d_left, d_right, d_q, d_t, d_ext, d_first, d_win, s));
+    if (c->timing) FA_CUDA(cudaEventRecord(c->kev1, s));
+    c->last_launches = 7;
+    c->last_stream = s;
     if (tot.y) FA_CUDA(cudaMemcpyAsync(left_jobs, d_left, sizeof(fa_job) * tot.y, cudaMemcpyDeviceToHost, s));
     if (tot.z) FA_CUDA(cudaMemcpyAsync(right_jobs, d_right, sizeof(fa_job) * tot.z, cudaMemcpyDeviceToHost, s));
     if (read_bytes) FA_CUDA(cudaMemcpyAsync(qbuf, d_q, 2 * read_bytes, cudaMemcpyDeviceToHost, s));

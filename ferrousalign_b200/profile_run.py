@@ -5,6 +5,7 @@ Usage: python -m ferrousalign_b200.profile_run [n_jobs] [probe|-] [kernel: 0 aut
        python -m ferrousalign_b200.profile_run bands [n_jobs]            (single runs at fixed bands)
        python -m ferrousalign_b200.profile_run mate [n_jobs] [reps]      (mate-rescue SW, device-resident)
        python -m ferrousalign_b200.profile_run regions [n_chains] [reps] (region merge, device-resident)
+       python -m ferrousalign_b200.profile_run collect [n_reads] [reps]  (extension jobs from chains)
 """
 import ctypes
 import sys
@@ -37,6 +38,20 @@ if len(sys.argv) > 1 and sys.argv[1] == "mate":
             st.synchronize()
             N.check(lib.fa_ctx_sync(ctx.handle))
             print("mate batch ms", e0.elapsed_time(e1))
+    sys.exit(0)
+
+if len(sys.argv) > 1 and sys.argv[1] == "collect":
+    n = int(sys.argv[2]) if len(sys.argv) > 2 else 500_000
+    ref, reads, off, chains, seeds = synth.workload_chains(n, ref_len=100_000_000)
+    pac, l_pac = fa.pack_reference(ref)
+    ctx = fa.Context(0)
+    lib = N.load()
+    N.check(lib.fa_ctx_set_timing(ctx.handle, 1))
+    k_ms, k_n = ctypes.c_float(), ctypes.c_int()
+    for r in range(int(sys.argv[3]) if len(sys.argv) > 3 else 1):
+        got = fa.collect_extension_jobs(pac, l_pac, reads, off, chains, seeds, ctx=ctx)
+        N.check(lib.fa_ctx_last_timing(ctx.handle, ctypes.byref(k_ms), ctypes.byref(k_n)))
+        print("collect kernel ms", k_ms.value, "jobs", len(got.left_jobs), len(got.right_jobs))
     sys.exit(0)
 
 if len(sys.argv) > 1 and sys.argv[1] == "regions":

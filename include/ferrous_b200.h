@@ -292,7 +292,7 @@ int fa_merge_regions(fa_ctx *ctx, const fa_region_opts *opt, const uint32_t *cha
                      fa_region *out);
 /* Device-resident variant (no reference counterpart): device pointers, asynchronous on
  * `stream` (NULL = the context's stream); a malformed chain range is reported by the next
- * fa_ctx_sync(). */
+ * fa_ctx_sync().  With fa_ctx_set_timing on, fa_ctx_last_timing covers its kernel. */
 int fa_merge_regions_device(fa_ctx *ctx, const fa_region_opts *opt, const uint32_t *d_chain_first,
                             uint32_t n_chains, const int32_t *d_query_len, const fa_seed_ext *d_seeds,
                             uint32_t n_seeds, const fa_ext_result *d_left, uint32_t n_left,
@@ -337,12 +337,15 @@ typedef struct {
 /* reads: read r is reads[read_off[r] .. read_off[r+1]) (codes 0-4); pac: the .pac layout,
  * base k in bits 7-6 of byte k/4 for k % 4 == 0, down to bits 1-0 for k % 4 == 3.
  * Outputs (caller-allocated): left_jobs/right_jobs hold up to n_seeds jobs each, in the
- * reference's order; their q_off/t_off address qbuf (2 x the reads' bytes) and tbuf
- * (tbuf_cap bytes); seed_ext + chain_first (n_chains + 1) are the region-merge seed table,
+ * reference's order; their q_off/t_off address qbuf (2 x the reads' bytes: read r forward
+ * at 2 read_off[r], reversed right after it) and tbuf (tbuf_cap bytes: per chain its
+ * window forward, then reversed); seed_ext + chain_first (n_chains + 1) are the region-merge seed table,
  * seed_ext's left_job/right_job being indices into left_jobs/right_jobs (the reference
  * numbers them per read; here across the batch); chain_win gets each chain's [rmax0,
  * rmax1) (two u64 per chain; 0,0 for a chain without jobs).  When tbuf_cap is too small
- * nothing is written except counts (with the bytes needed) and FA_ERR_CAPACITY returns. */
+ * nothing is written except counts (with the bytes needed) and FA_ERR_CAPACITY returns.
+ * With fa_ctx_set_timing on, fa_ctx_last_timing covers the call's kernels (and the one read
+ * of the totals between its planning and filling launches). */
 int fa_collect_ext_jobs(fa_ctx *ctx, const fa_collect_opts *opt, const uint8_t *pac, uint64_t l_pac,
                         const uint8_t *reads, const uint64_t *read_off, uint32_t n_reads,
                         const fa_chain *chains, uint32_t n_chains, const fa_seed *seeds, uint32_t n_seeds,
