@@ -475,6 +475,57 @@ def bench_collect(args, ctx, lib):
             "bit_exact_sample": bool(same), "sample": f"first {k} chains against the oracle"}
 
 
+def bench_cigar(args, ctx, lib):
+    """CIGAR regeneration (scalar_banded_swa, h0 = 0) for 200k regions of 151-bp reads (the
+    read against its reference span, bands of the length difference plus 5-30): kernel time
+    with CUDA events, cells from the kernel's own count.  One thread per alignment runs the
+    scalar int32 recurrence with a two-bit traceback written to HBM and read back along the
+    path; reported against the copy bandwidth for its bytes (sequences in, traceback out
+    and back, results out) and as cells per second."""
+    import ctypes
+    import ferrousalign_b200 as fa
+    from ferrousalign_b200 import _native as N, synth
+    from oracle import cigar_oracle as C
+    jobs, qseq, tseq = synth.workload_cigar(200_000)
+    p = fa.BandedPairWiseSW().to_struct()
+    N.check(lib.fa_ctx_set_timing(ctx.handle, 1))
+    k_ms, k_n = ctypes.c_float(), ctypes.c_int()
+    kern, wall = [], []
+    got = None
+    for it in range(args.warmup + 5):
+        t0 = time.perf_counter()
+        got = fa.scalar_banded_swa_batch(p, jobs, qseq, tseq, ctx=ctx)
+        t1 = time.perf_counter()
+        N.check(lib.fa_ctx_last_timing(ctx.handle, ctypes.byref(k_ms), ctypes.byref(k_n)))
+        if it >= args.warmup:
+            kern.append(k_ms.value)
+            wall.append((t1 - t0) * 1e3)
+    km = float(np.median(kern))
+    n = len(jobs)
+    cells = int(got.results["cells"].sum())
+    seq_bytes = int(jobs["qlen"].sum() + jobs["tlen"].sum())
+    out_bytes = n * 40 + 4 * int(got.results["n_cigar"].sum()) + int(got.results["n_ref"].sum() +
+                                                                         got.results["n_query"].sum())
+    algo = seq_bytes + cells // 4 + out_bytes + n * 32
+    op = {"mat": [int(x) for x in p["mat"][0]], "o_del": 6, "e_del": 1, "o_ins": 6, "e_ins": 1, "zdrop": 100,
+          "pen_clip3": 5}
+    k = 300
+    same = True
+    for i in range(k):
+        j = jobs[i]
+        q = list(qseq[int(j["q_off"]):int(j["q_off"]) + int(j["qlen"])])
+        t = list(tseq[int(j["t_off"]):int(j["t_off"]) + int(j["tlen"])])
+        out, cig, ra, qa = C.banded_swa(op, q, t, int(j["w"]), int(j["h0"]))
+        same = same and {f: int(got.results[i][f]) for f in out} == out and got.cigar_of(i) == cig
+    return {"workload": f"{n} regions of 151-bp reads (read vs its reference span, h0 = 0, bands |dlen| + 5-30)",
+            "kernel": "cigar_kernel", "kernel_ms": km, "alignments_per_s": n / (km * 1e-3),
+            "gcups": cells / (km * 1e-3) / 1e9, "cells": cells, "e2e_ms": float(np.median(wall)),
+            "roofline": {"bound": "alu", "hbm_achieved_gbs": algo / (km * 1e-3) / 1e9, "hbm_peak_gbs": 6546.6,
+                         "hbm_frac": algo / (km * 1e-3) / 1e9 / 6546.6, "algorithmic_bytes": algo,
+                         "note": "scalar int32 cells with a 2-bit traceback; one thread per alignment"},
+            "bit_exact_sample": bool(same), "sample": f"first {k} alignments against the oracle"}
+
+
 def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
@@ -690,6 +741,7 @@ def main():
     if not args.skip_regions:
         line["region_merge"] = bench_regions(args, ctx, lib, dev, stream, flush)
         line["job_collection"] = bench_collect(args, ctx, lib)
+        line["cigar"] = bench_cigar(args, ctx, lib)
     if not args.skip_cpu:
         ref2, tr2, dt, threads = cpu_oracle_rate(b, p, min(CPU_SAMPLE, n))
         line["cpu_baseline"] = {"value": min(CPU_SAMPLE, n) / dt, "unit": "alignments/s", "cores": threads,

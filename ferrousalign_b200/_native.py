@@ -52,6 +52,11 @@ CHAIN_DT = np.dtype([("read", "<u4"), ("seed_first", "<u4"), ("n_seeds", "<u4"),
 SEED_DT = np.dtype([("ref_pos", "<u8"), ("query_pos", "<i4"), ("len", "<i4")])
 COLLECT_COUNTS_DT = np.dtype([("n_left", "<u4"), ("n_right", "<u4"), ("n_seed_ext", "<u4"), ("_pad", "<u4"),
                               ("qbuf_len", "<u8"), ("tbuf_len", "<u8")])
+CIGAR_JOB_DT = np.dtype([("q_off", "<u8"), ("t_off", "<u8"), ("qlen", "<i4"), ("tlen", "<i4"), ("w", "<i4"),
+                         ("h0", "<i4")])
+CIGAR_RESULT_DT = np.dtype([("score", "<i4"), ("qle", "<i4"), ("tle", "<i4"), ("gtle", "<i4"), ("gscore", "<i4"),
+                            ("max_off", "<i4"), ("n_cigar", "<i4"), ("n_ref", "<i4"), ("n_query", "<i4"),
+                            ("cells", "<i4")])
 
 assert PARAMS_DT.itemsize == 64 and JOB_DT.itemsize == 40 and EXT_RESULT_DT.itemsize == 24
 assert STATS_DT.itemsize == 40 and MATE_PARAMS_DT.itemsize == 48 and MATE_JOB_DT.itemsize == 32
@@ -59,6 +64,7 @@ assert KSWR_DT.itemsize == 28
 assert REGION_OPTS_DT.itemsize == 16 and SEED_EXT_DT.itemsize == 24 and REGION_DT.itemsize == 48
 assert COLLECT_OPTS_DT.itemsize == 24 and CHAIN_DT.itemsize == 16 and SEED_DT.itemsize == 16
 assert COLLECT_COUNTS_DT.itemsize == 32
+assert CIGAR_JOB_DT.itemsize == 32 and CIGAR_RESULT_DT.itemsize == 40
 
 # Every symbol the header declares, with its ctypes signature.
 _P = C.c_void_p
@@ -101,6 +107,7 @@ SIGNATURES = {
     "fa_mate_sw_batch": (C.c_int, [_P, _P, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64, _P, _P]),
     "fa_collect_ext_jobs": (C.c_int, [_P, _P, _P, C.c_uint64, _P, _P, C.c_uint32, _P, C.c_uint32, _P, C.c_uint32,
                                       _P, _P, _P, _P, C.c_uint64, _P, _P, _P, _P]),
+    "fa_cigar_batch": (C.c_int, [_P, _P, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64, _P, _P, _P, _P]),
     "fa_merge_regions": (C.c_int, [_P, _P, _P, C.c_uint32, _P, _P, C.c_uint32, _P, C.c_uint32, _P, C.c_uint32,
                                    _P]),
     "fa_merge_regions_device": (C.c_int, [_P, _P, _P, C.c_uint32, _P, _P, C.c_uint32, _P, C.c_uint32, _P,

@@ -1,0 +1,82 @@
+"""CIGAR regeneration: the host mirror of scalar_banded_swa
+(src/core/alignment/banded_swa/scalar/implementation.rs:5-440) as a batch on the GPU
+(csrc/cigar_kernel.cu), and infer_band_width (src/pipelines/linear/region.rs:1277-1316),
+which picks each job's band.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as N
+
+CIGAR_JOB_DT = N.CIGAR_JOB_DT
+CIGAR_RESULT_DT = N.CIGAR_RESULT_DT
+CIGAR_OPS = "MIDNS"   # op codes 0-4 of the packed CIGAR words (len << 4 | op)
+
+
+def infer_band_width(l_query: int, l_ref: int, score: int, a: int, o_del: int, e_del: int, o_ins: int,
+                     e_ins: int, cmd_w: int, region_w: int) -> int:
+    """Band for regenerating a region's CIGAR (bwamem.cpp:1752-1756 in the reference's
+    port): from the score lost to gaps on either axis, at least the length difference,
+    the region's own band when above the command-line one, at most four times that."""
+    def side(o: int, e: int) -> int:
+        if l_query == l_ref and l_query * a - score < (o + e - a) * 2:
+            return 0
+        x = float(min(l_query, l_ref) * a - score - o)
+        q = x / e if e else (math.inf if x > 0 else -math.inf if x < 0 else math.nan)
+        q += 2.0
+        v = 0 if math.isnan(q) else (2**31 - 1 if q >= 2**31 - 1 else -2**31 if q <= -2**31 else int(q))
+        return max(v, abs(l_query - l_ref))
+    w = max(side(o_del, e_del), side(o_ins, e_ins))
+    if w > cmd_w:
+        w = min(w, region_w)
+    return min(w, cmd_w * 4)
+
+
+@dataclass
+class CigarBatch:
+    results: np.ndarray        # CIGAR_RESULT_DT: OutScore fields and output lengths
+    cigar: np.ndarray          # u32 words, job k's at cigar_off[k]
+    ref_aligned: np.ndarray    # u8, job k's at ref_off[k]
+    query_aligned: np.ndarray  # u8, job k's at qry_off[k]
+    cigar_off: np.ndarray
+    ref_off: np.ndarray
+    qry_off: np.ndarray
+
+    def cigar_of(self, k: int) -> list[tuple[str, int]]:
+        n = int(self.results["n_cigar"][k])
+        words = self.cigar[int(self.cigar_off[k]):int(self.cigar_off[k]) + n]
+        return [(CIGAR_OPS[int(x) & 15], int(x) >> 4) for x in words]
+
+    def ref_aligned_of(self, k: int) -> np.ndarray:
+        return self.ref_aligned[int(self.ref_off[k]):int(self.ref_off[k]) + int(self.results["n_ref"][k])]
+
+    def query_aligned_of(self, k: int) -> np.ndarray:
+        return self.query_aligned[int(self.qry_off[k]):int(self.qry_off[k]) + int(self.results["n_query"][k])]
+
+
+def scalar_banded_swa_batch(params: np.ndarray, jobs: np.ndarray, qseq: np.ndarray, tseq: np.ndarray,
+                            ctx: N.Context | None = None) -> CigarBatch:
+    """scalar_banded_swa for every job (CIGAR_JOB_DT: offsets, lengths, band, h0)."""
+    lib = N.load()
+    ctx = ctx or N.default_context()
+    jobs = np.ascontiguousarray(jobs, CIGAR_JOB_DT)
+    qseq = np.ascontiguousarray(qseq, np.uint8)
+    tseq = np.ascontiguousarray(tseq, np.uint8)
+    n = len(jobs)
+    q = jobs["qlen"].astype(np.int64)
+    t = jobs["tlen"].astype(np.int64)
+    cig_off = np.concatenate([[0], np.cumsum(q + t + 2)])
+    ref_off = np.concatenate([[0], np.cumsum(t)])
+    qry_off = np.concatenate([[0], np.cumsum(q)])
+    res = np.zeros(n, CIGAR_RESULT_DT)
+    cig = np.zeros(max(int(cig_off[-1]), 1), np.uint32)
+    ra = np.zeros(max(int(ref_off[-1]), 1), np.uint8)
+    qa = np.zeros(max(int(qry_off[-1]), 1), np.uint8)
+    if n:
+        N.check(lib.fa_cigar_batch(ctx.handle, N.ptr(params), N.ptr(jobs), n, N.ptr(qseq), len(qseq), N.ptr(tseq),
+                                   len(tseq), N.ptr(res), N.ptr(cig), N.ptr(ra), N.ptr(qa)))
+    return CigarBatch(res, cig, ra, qa, cig_off[:-1], ref_off[:-1], qry_off[:-1])

@@ -1,0 +1,253 @@
+// cigar_kernel.cu -- banded Smith-Waterman with traceback for CIGAR regeneration (sm_100a).
+//
+// scalar_banded_swa (src/core/alignment/banded_swa/scalar/implementation.rs:5-440), the
+// alignment the region step runs to turn a region's bounds back into a CIGAR
+// (src/pipelines/linear/region.rs:1029-1070): the banded row recurrence of ksw_extend2
+// with three differences -- the match term is clamped at zero (H(i-1,j-1) + s, then 0
+// if negative) rather than gated on H(i-1,j-1) > 0, the band is used as given, and every
+// cell records which of M, E (deletion) and F (insertion) it took (ties to M, then E) --
+// followed by a traceback from the best cell to the matrix edge that emits run-length
+// M / D / I operations and the aligned reference and query bases, a 5' soft clip for the
+// query left over, and at the 3' end either a soft clip or an M run to the query end by
+// bwa-mem2's clip rule (gscore <= 0 or gscore <= score - pen_clip3: clip).
+//
+// One thread per alignment.  The traceback codes take two bits per cell in a band of
+// min(2w + 1, qlen) columns per row, kept in HBM per job (about 12 KB for a 151-bp read
+// against a 250-base window at w = 100); cells never written read as M, as the
+// reference's zero-initialised matrix does.  The row state (H, E per column) sits in a
+// per-job HBM scratch that stays in L1/L2 while the row loop runs.
+
+#include "fa_device.cuh"
+#include "fa_kernels.h"
+
+namespace fa {
+
+namespace {
+
+constexpr int kCigarThreads = 64;
+constexpr uint8_t TB_M = 0, TB_D = 1, TB_I = 2;   // types.rs:101-103
+constexpr int kMaxTraceSteps = 10000;             // implementation.rs:253
+
+struct CigarCtx {
+    const uint32_t *tb;
+    int w, wpr;
+    __device__ __forceinline__ uint32_t at(int ii, int jj) const {   // tb[ii][jj] of the reference
+        if (ii == 0) return jj == 0 ? TB_M : TB_I;
+        if (jj == 0) return TB_D;
+        const int i = ii - 1, j = jj - 1;
+        const int lo = i - w > 0 ? i - w : 0;
+        const int k = j - lo;
+        if (k < 0 || k >= wpr * 16) return TB_M;
+        return (tb[(size_t)i * wpr + (k >> 4)] >> ((k & 15) * 2)) & 3u;
+    }
+};
+
+__device__ __forceinline__ uint32_t cigar_op(uint32_t op, uint32_t len) { return len << 4 | op; }
+
+__global__ void __launch_bounds__(kCigarThreads)
+cigar_kernel(const fa_cigar_job *__restrict__ jobs, const CigarPlan *__restrict__ plan, uint32_t n,
+             const uint8_t *__restrict__ qseq, const uint8_t *__restrict__ tseq, const ExtParams p, int pen_clip3,
+             int2 *__restrict__ eh_all, uint32_t *__restrict__ tb_all, fa_cigar_result *__restrict__ out,
+             uint32_t *__restrict__ cigar, uint8_t *__restrict__ ref_al, uint8_t *__restrict__ qry_al)
+{
+    const uint32_t k = blockIdx.x * kCigarThreads + threadIdx.x;
+    if (k >= n) return;
+    const fa_cigar_job J = jobs[k];
+    const CigarPlan P = plan[k];
+    fa_cigar_result r;
+    r.score = r.qle = r.tle = r.gtle = r.gscore = r.max_off = 0;
+    r.n_cigar = r.n_ref = r.n_query = 0;
+    r.cells = 0;
+    const int qlen = J.qlen, tlen = J.tlen, w = J.w, h0 = J.h0;
+    if (qlen <= 0 || tlen <= 0) {   // implementation.rs:17-30
+        out[k] = r;
+        return;
+    }
+    const uint8_t *Q = qseq + J.q_off;
+    const uint8_t *T = tseq + J.t_off;
+    int2 *eh = eh_all + P.eh;
+    uint32_t *tb = tb_all + P.tb;
+    const int oe_del = p.o_del + p.e_del, oe_ins = p.o_ins + p.e_ins;
+    // first row (implementation.rs:67-75)
+    eh[0] = make_int2(h0, 0);
+    int hp = h0 > oe_ins ? h0 - oe_ins : 0;
+    eh[1] = make_int2(hp, 0);
+    for (int j = 2; j <= qlen; ++j) {
+        hp = hp > p.e_ins ? hp - p.e_ins : 0;
+        eh[j] = make_int2(hp, 0);
+    }
+    int max_score = h0, max_i = -1, max_j = -1, max_ie = -1, gscore = -1, max_off = 0;
+    int beg = 0, end = qlen, cells = 0;
+    for (int i = 0; i < tlen; ++i) {
+        const int tbase = T[i] < 4 ? T[i] : 4;
+        const int8_t *row = p.mat + tbase * 5;
+        int cb = beg, ce = end;
+        if (cb < i - w) cb = i - w;
+        if (ce > i + w + 1) ce = i + w + 1;
+        if (ce > qlen) ce = qlen;
+        int h1 = 0;
+        if (cb == 0) {
+            h1 = h0 - (p.o_del + p.e_del * (i + 1));
+            if (h1 < 0) h1 = 0;
+        }
+        int f = 0, m_val = 0, mj = -1;
+        const int lo = i - w > 0 ? i - w : 0;
+        uint32_t *rowtb = tb + (size_t)i * P.wpr;
+        uint32_t acc = 0;
+        int widx = -1;
+        for (int j = cb; j < ce; ++j) {
+            const int2 ej = eh[j];
+            int m = ej.x;
+            int e = ej.y;
+            const int qb = Q[j] < 4 ? Q[j] : 4;
+            m += row[qb];
+            if (m < 0) m = 0;
+            int h;
+            uint32_t code;
+            if (m >= e && m >= f) { h = m; code = TB_M; }
+            else if (e >= f) { h = e; code = TB_D; }
+            else { h = f; code = TB_I; }
+            const int kk = j - lo, wi = kk >> 4;
+            if (wi != widx) {
+                if (widx >= 0) rowtb[widx] = acc;
+                acc = 0;
+                widx = wi;
+            }
+            acc |= code << ((kk & 15) * 2);
+            if (m_val < h) { m_val = h; mj = j; }
+            int t = m - oe_del;
+            t = t > 0 ? t : 0;
+            e -= p.e_del;
+            e = e > t ? e : t;
+            eh[j] = make_int2(h1, e);   // H of the previous row's cell, E for the next row
+            t = m - oe_ins;
+            t = t > 0 ? t : 0;
+            f -= p.e_ins;
+            f = f > t ? f : t;
+            h1 = h;
+        }
+        if (widx >= 0) rowtb[widx] = acc;
+        if (ce > cb) cells += ce - cb;
+        eh[ce] = make_int2(h1, 0);
+        if (ce == qlen && gscore < h1) { gscore = h1; max_ie = i; }
+        if (m_val == 0) break;
+        if (m_val > max_score) {
+            max_score = m_val;
+            max_i = i;
+            max_j = mj;
+            const int off = mj > i ? mj - i : i - mj;
+            max_off = max_off > off ? max_off : off;
+        } else if (p.zdrop > 0) {
+            const int di = i - max_i, dj = mj - max_j;
+            if (di > dj) {
+                if (max_score - m_val - (di - dj) * p.e_del > p.zdrop) break;
+            } else if (max_score - m_val - (dj - di) * p.e_ins > p.zdrop) {
+                break;
+            }
+        }
+        int nb = cb;
+        while (nb < ce && eh[nb].x == 0 && eh[nb].y == 0) ++nb;
+        beg = nb;
+        int ne = ce;
+        while (ne >= beg && eh[ne].x == 0 && eh[ne].y == 0) --ne;
+        end = ne + 2 < qlen ? ne + 2 : qlen;
+    }
+
+    // traceback from the best cell (implementation.rs:239-321); operations and bases come
+    // out last to first and are reversed afterwards.  Slot 0 is kept for a 5' clip.
+    const CigarCtx tbx{tb, w, P.wpr};
+    uint32_t *ops = cigar + P.cig;
+    uint8_t *ra = ref_al + P.ref, *qa = qry_al + P.qry;
+    int ci = max_i + 1, cj = max_j + 1, nops = 0, nr = 0, nq = 0;
+    for (int it = 0; (ci > 0 || cj > 0) && it < kMaxTraceSteps; ++it) {
+        const int pi = ci, pj = cj;
+        const uint32_t code = tbx.at(ci, cj);
+        int cnt = 0;
+        if (code == TB_M) {
+            while (ci > 0 && cj > 0 && tbx.at(ci, cj) == TB_M) {
+                ra[nr++] = T[ci - 1];
+                qa[nq++] = Q[cj - 1];
+                --ci;
+                --cj;
+                ++cnt;
+            }
+            if (cnt) ops[1 + nops++] = cigar_op(0, cnt);
+        } else if (code == TB_D) {
+            while (ci > 0 && tbx.at(ci, cj) == TB_D) {
+                ra[nr++] = T[ci - 1];
+                --ci;
+                ++cnt;
+            }
+            if (cnt) ops[1 + nops++] = cigar_op(2, cnt);
+        } else if (code == TB_I) {
+            while (cj > 0 && tbx.at(ci, cj) == TB_I) {
+                qa[nq++] = Q[cj - 1];
+                --cj;
+                ++cnt;
+            }
+            if (cnt) ops[1 + nops++] = cigar_op(1, cnt);
+        } else {
+            break;
+        }
+        if (ci == pi && cj == pj) break;
+    }
+    for (int a = 0, b = nops - 1; a < b; ++a, --b) {
+        const uint32_t t = ops[1 + a];
+        ops[1 + a] = ops[1 + b];
+        ops[1 + b] = t;
+    }
+    for (int a = 0, b = nr - 1; a < b; ++a, --b) {
+        const uint8_t t = ra[a];
+        ra[a] = ra[b];
+        ra[b] = t;
+    }
+    for (int a = 0, b = nq - 1; a < b; ++a, --b) {
+        const uint8_t t = qa[a];
+        qa[a] = qa[b];
+        qa[b] = t;
+    }
+    // clips (implementation.rs:340-412)
+    const int qs = cj, qe = max_j + 1;
+    int total = nops;
+    if (qs > 0) {
+        ops[0] = cigar_op(4, qs);
+        ++total;
+    } else {
+        for (int a = 0; a < nops; ++a) ops[a] = ops[a + 1];
+    }
+    if (qe < qlen) {
+        const bool clip = gscore <= 0 || gscore <= max_score - pen_clip3;
+        ops[total++] = cigar_op(clip ? 4 : 0, qlen - qe);
+    }
+    r.score = max_score;
+    r.qle = max_j + 1;
+    r.tle = max_i + 1;
+    r.gtle = max_ie + 1;
+    r.gscore = gscore;
+    r.max_off = max_off;
+    r.n_cigar = total;
+    r.n_ref = nr;
+    r.n_query = nq;
+    r.cells = cells;
+    out[k] = r;
+}
+
+}  // namespace
+
+int cigar_band_words(int qlen, int w) {
+    const long long cols = 2ll * w + 1 < qlen ? 2ll * w + 1 : qlen;
+    return cols <= 0 ? 0 : (int)((cols + 15) / 16);
+}
+
+cudaError_t launch_cigar(const fa_cigar_job *d_jobs, const CigarPlan *d_plan, uint32_t n, const uint8_t *d_qseq,
+                         const uint8_t *d_tseq, const ExtParams &p, int pen_clip3, int2 *d_eh, uint32_t *d_tb,
+                         fa_cigar_result *d_out, uint32_t *d_cigar, uint8_t *d_ref_al, uint8_t *d_qry_al,
+                         cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    cigar_kernel<<<(n + kCigarThreads - 1) / kCigarThreads, kCigarThreads, 0, s>>>(
+        d_jobs, d_plan, n, d_qseq, d_tseq, p, pen_clip3, d_eh, d_tb, d_out, d_cigar, d_ref_al, d_qry_al);
+    return cudaGetLastError();
+}
+
+}  // namespace fa

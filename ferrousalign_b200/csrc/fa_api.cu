@@ -82,6 +82,7 @@ struct fa_ctx {
     DevBuf ovf;   // two-row kernel: jobs handed on to the int32 kernel
     DevBuf reg_in, reg_out;   // region merge of host buffers: inputs, regions
     DevBuf col_in, col_plan, col_out;   // job collection: inputs, chain plans + scan sums, outputs
+    DevBuf cg_in, cg_scratch, cg_out;   // CIGAR regeneration: inputs, row state + traceback, outputs
     DevBuf w_first, w_cur, prev, kk, w_final, tries, missed, list_a, list_b, hist, feat, wbf, part_n, part_w;
     uint32_t last_launches = 0;
     bool timing = false;
@@ -790,7 +791,8 @@ void fa_ctx_destroy(fa_ctx *c) {
     for (DevBuf *b : {&c->jobs, &c->order, &c->qseq, &c->tseq, &c->out, &c->clamped, &c->cells_job,
                       &c->misc, &c->w_first, &c->w_cur, &c->prev, &c->kk, &c->w_final, &c->tries,
                       &c->missed, &c->list_a, &c->list_b, &c->hist, &c->feat, &c->wbf, &c->part_n,
-                      &c->part_w, &c->ovf, &c->reg_in, &c->reg_out, &c->col_in, &c->col_plan, &c->col_out})
+                      &c->part_w, &c->ovf, &c->reg_in, &c->reg_out, &c->col_in, &c->col_plan, &c->col_out,
+                      &c->cg_in, &c->cg_scratch, &c->cg_out})
         b->release();
     for (int k = 0; k < 2; ++k) {
         if (c->join_ev[k]) cudaEventDestroy(c->join_ev[k]);
@@ -1352,6 +1354,74 @@ int fa_collect_ext_jobs(fa_ctx *c, const fa_collect_opts *opt, const uint8_t *pa
     FA_CUDA(cudaMemcpyAsync(chain_win, d_win, 16ull * n_chains, cudaMemcpyDeviceToHost, s));
     FA_CUDA(cudaStreamSynchronize(s));
     chain_first[n_chains] = (uint32_t)tot.w;
+    return FA_OK;
+}
+
+int fa_cigar_batch(fa_ctx *c, const fa_params *p, const fa_cigar_job *jobs, uint32_t n, const uint8_t *qseq,
+                   uint64_t qseq_len, const uint8_t *tseq, uint64_t tseq_len, fa_cigar_result *out, uint32_t *cigar,
+                   uint8_t *ref_aligned, uint8_t *query_aligned) {
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    if (int rc = check_params(p)) return rc;
+    if (n == 0) return FA_OK;
+    if (!jobs || !out || !cigar || !ref_aligned || !query_aligned) return fail(FA_ERR_ARG, "null buffer");
+    // output and scratch offsets per job (the reference would panic on a range past its slices)
+    std::vector<CigarPlan> plan(n);
+    uint64_t cig = 0, ref = 0, qry = 0, eh = 0, tb = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        const fa_cigar_job &j = jobs[k];
+        if (j.qlen < 0 || j.tlen < 0 || j.w < 0) return fail(FA_ERR_ARG, "cigar job %u: negative length or band", k);
+        if (j.qlen > FA_MAX_QLEN || j.tlen > FA_MAX_TLEN) return fail(FA_ERR_CAPACITY, "cigar job %u too long", k);
+        if (j.q_off + (uint64_t)j.qlen > qseq_len || j.t_off + (uint64_t)j.tlen > tseq_len)
+            return fail(FA_ERR_ARG, "cigar job %u: range outside the sequence buffers", k);
+        CigarPlan &pl = plan[k];
+        pl.cig = cig; pl.ref = ref; pl.qry = qry; pl.eh = eh; pl.tb = tb;
+        pl.wpr = cigar_band_words(j.qlen, j.w);
+        pl._pad = 0;
+        cig += (uint64_t)j.qlen + j.tlen + 2;
+        ref += (uint64_t)j.tlen;
+        qry += (uint64_t)j.qlen;
+        eh += (uint64_t)j.qlen + 1;
+        tb += (uint64_t)j.tlen * pl.wpr;
+    }
+    FA_CUDA(cudaSetDevice(c->device));
+    cudaStream_t s = c->stream;
+    auto up16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
+    const size_t b_jobs = up16(sizeof(fa_cigar_job) * n), b_plan = up16(sizeof(CigarPlan) * n);
+    const size_t b_q = up16(qseq_len + 1), b_t = up16(tseq_len + 1);
+    FA_CUDA(c->cg_in.ensure(b_jobs + b_plan + b_q + b_t));
+    char *in = c->cg_in.as<char>();
+    fa_cigar_job *d_jobs = reinterpret_cast<fa_cigar_job *>(in);
+    CigarPlan *d_plan = reinterpret_cast<CigarPlan *>(in + b_jobs);
+    uint8_t *d_q = reinterpret_cast<uint8_t *>(in + b_jobs + b_plan);
+    uint8_t *d_t = reinterpret_cast<uint8_t *>(in + b_jobs + b_plan + b_q);
+    const size_t b_eh = up16(sizeof(int2) * eh), b_tb = up16(4 * tb);
+    FA_CUDA(c->cg_scratch.ensure(b_eh + b_tb));
+    int2 *d_eh = c->cg_scratch.as<int2>();
+    uint32_t *d_tb = reinterpret_cast<uint32_t *>(c->cg_scratch.as<char>() + b_eh);
+    const size_t b_out = up16(sizeof(fa_cigar_result) * n), b_cig = up16(4 * cig);
+    const size_t b_ref = up16(ref + 1), b_qry = up16(qry + 1);
+    FA_CUDA(c->cg_out.ensure(b_out + b_cig + b_ref + b_qry));
+    char *o = c->cg_out.as<char>();
+    fa_cigar_result *d_out = reinterpret_cast<fa_cigar_result *>(o);
+    uint32_t *d_cig = reinterpret_cast<uint32_t *>(o + b_out);
+    uint8_t *d_ref = reinterpret_cast<uint8_t *>(o + b_out + b_cig);
+    uint8_t *d_qry = reinterpret_cast<uint8_t *>(o + b_out + b_cig + b_ref);
+    FA_CUDA(cudaMemcpyAsync(d_jobs, jobs, sizeof(fa_cigar_job) * n, cudaMemcpyHostToDevice, s));
+    FA_CUDA(cudaMemcpyAsync(d_plan, plan.data(), sizeof(CigarPlan) * n, cudaMemcpyHostToDevice, s));
+    if (qseq_len) FA_CUDA(cudaMemcpyAsync(d_q, qseq, qseq_len, cudaMemcpyHostToDevice, s));
+    if (tseq_len) FA_CUDA(cudaMemcpyAsync(d_t, tseq, tseq_len, cudaMemcpyHostToDevice, s));
+    if (tb) FA_CUDA(cudaMemsetAsync(d_tb, 0, 4 * tb, s));   // unwritten cells read as M, as the reference's
+    const ExtParams kp = ext_params_of(p);
+    if (c->timing) FA_CUDA(cudaEventRecord(c->kev0, s));
+    FA_CUDA(launch_cigar(d_jobs, d_plan, n, d_q, d_t, kp, p->pen_clip3, d_eh, d_tb, d_out, d_cig, d_ref, d_qry, s));
+    if (c->timing) FA_CUDA(cudaEventRecord(c->kev1, s));
+    c->last_launches = 1;
+    c->last_stream = s;
+    FA_CUDA(cudaMemcpyAsync(out, d_out, sizeof(fa_cigar_result) * n, cudaMemcpyDeviceToHost, s));
+    FA_CUDA(cudaMemcpyAsync(cigar, d_cig, 4 * cig, cudaMemcpyDeviceToHost, s));
+    if (ref) FA_CUDA(cudaMemcpyAsync(ref_aligned, d_ref, ref, cudaMemcpyDeviceToHost, s));
+    if (qry) FA_CUDA(cudaMemcpyAsync(query_aligned, d_qry, qry, cudaMemcpyDeviceToHost, s));
+    FA_CUDA(cudaStreamSynchronize(s));
     return FA_OK;
 }
 

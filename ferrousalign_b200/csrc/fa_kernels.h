@@ -145,6 +145,19 @@ cudaError_t launch_collect_fill(const fa_collect_opts &opt, const uint8_t *d_pac
                                 uint8_t *d_tbuf, fa_seed_ext *d_seed_ext, uint32_t *d_chain_first,
                                 uint64_t *d_chain_win, cudaStream_t s);
 
+// CIGAR regeneration (cigar_kernel.cu): per job the offsets of its outputs (cigar words,
+// aligned reference / query bases) and of its scratch (row state in int2 units, traceback
+// in words), and its traceback words per row.
+struct CigarPlan {
+    uint64_t cig, ref, qry, eh, tb;
+    int32_t wpr, _pad;
+};
+int cigar_band_words(int qlen, int w);
+cudaError_t launch_cigar(const fa_cigar_job *d_jobs, const CigarPlan *d_plan, uint32_t n, const uint8_t *d_qseq,
+                         const uint8_t *d_tseq, const ExtParams &p, int pen_clip3, int2 *d_eh, uint32_t *d_tb,
+                         fa_cigar_result *d_out, uint32_t *d_cigar, uint8_t *d_ref_al, uint8_t *d_qry_al,
+                         cudaStream_t s);
+
 // Integer / DPX instruction throughput (ops per second) for the roofline denominator.
 double probe_int_peak(int kind, int sm_count, cudaStream_t s, float *ms_out);
 

@@ -6,6 +6,7 @@ Usage: python -m ferrousalign_b200.profile_run [n_jobs] [probe|-] [kernel: 0 aut
        python -m ferrousalign_b200.profile_run mate [n_jobs] [reps]      (mate-rescue SW, device-resident)
        python -m ferrousalign_b200.profile_run regions [n_chains] [reps] (region merge, device-resident)
        python -m ferrousalign_b200.profile_run collect [n_reads] [reps]  (extension jobs from chains)
+       python -m ferrousalign_b200.profile_run cigar [n_jobs] [reps]     (CIGAR regeneration)
 """
 import ctypes
 import sys
@@ -38,6 +39,20 @@ if len(sys.argv) > 1 and sys.argv[1] == "mate":
             st.synchronize()
             N.check(lib.fa_ctx_sync(ctx.handle))
             print("mate batch ms", e0.elapsed_time(e1))
+    sys.exit(0)
+
+if len(sys.argv) > 1 and sys.argv[1] == "cigar":
+    n = int(sys.argv[2]) if len(sys.argv) > 2 else 200_000
+    jobs, qseq, tseq = synth.workload_cigar(n)
+    ctx = fa.Context(0)
+    lib = N.load()
+    N.check(lib.fa_ctx_set_timing(ctx.handle, 1))
+    k_ms, k_n = ctypes.c_float(), ctypes.c_int()
+    p = fa.BandedPairWiseSW().to_struct()
+    for r in range(int(sys.argv[3]) if len(sys.argv) > 3 else 1):
+        got = fa.scalar_banded_swa_batch(p, jobs, qseq, tseq, ctx=ctx)
+        N.check(lib.fa_ctx_last_timing(ctx.handle, ctypes.byref(k_ms), ctypes.byref(k_n)))
+        print("cigar kernel ms", k_ms.value, "cells", int(got.results["cells"].sum()))
     sys.exit(0)
 
 if len(sys.argv) > 1 and sys.argv[1] == "collect":

@@ -240,3 +240,21 @@ def workload_chains(n_reads: int = 100_000, seed: int = 21, ref_len: int = 10_00
     seeds["query_pos"] = qp
     seeds["len"] = ln
     return ref, reads, read_off, chains, seeds
+
+
+def workload_cigar(n: int = 200_000, seed: int = 31, ref_len: int = 10_000_000, read_len: int = 151):
+    """CIGAR-regeneration jobs shaped like the regions of 151-bp reads: the whole read
+    against the reference span it came from (1% substitutions, per-read indel rate drawn
+    from {0, 0.1, 1, 3}%, so the span is the read length give or take the indels), h0 = 0,
+    and a band of the length difference plus 5-30 (the range infer_band_width gives such
+    regions).  Returns (jobs, qseq, tseq) with CIGAR_JOB_DT jobs."""
+    rng = np.random.default_rng(seed)
+    ref = reference(ref_len, seed=seed, n_rate=0.001)
+    b = ext_jobs(ref, n, seed=seed + 100, read_len=(read_len, read_len), seed_len=(1, 1),
+                 indel_rates=(0.0, 0.001, 0.01, 0.03), w=100)
+    jobs = np.zeros(n, N.CIGAR_JOB_DT)
+    jobs["q_off"], jobs["t_off"] = b.jobs["q_off"], b.jobs["t_off"]
+    jobs["qlen"] = b.jobs["qlen"]
+    jobs["tlen"] = np.minimum(b.jobs["tlen"], b.jobs["qlen"] + rng.integers(-3, 4, n))
+    jobs["w"] = np.abs(jobs["qlen"] - jobs["tlen"]) + rng.integers(5, 31, n)
+    return jobs, b.qseq, b.tseq

@@ -353,6 +353,38 @@ int fa_collect_ext_jobs(fa_ctx *ctx, const fa_collect_opts *opt, const uint8_t *
                         fa_seed_ext *seed_ext, uint32_t *chain_first, uint64_t *chain_win,
                         fa_collect_counts *counts);
 
+/* ---- CIGAR regeneration ------------------------------------------------
+ * Replaces scalar_banded_swa (src/core/alignment/banded_swa/scalar/implementation.rs:5-440),
+ * the banded alignment with traceback that turns a region's bounds back into a CIGAR
+ * (src/pipelines/linear/region.rs:1029-1070, there with h0 = 0 and end_bonus 0): the
+ * banded recurrence with the match term clamped at zero, a traceback from the best cell
+ * (ties M, then deletion, then insertion), a 5' soft clip for the query left over, and at
+ * the 3' end a soft clip or an M run to the query end (clip when gscore <= 0 or
+ * gscore <= score - pen_clip3).  Codes above 4 count as N, as the reference clamps them. */
+typedef struct {
+    uint64_t q_off, t_off;   /* query / target offsets in the sequence buffers */
+    int32_t  qlen, tlen;
+    int32_t  w;              /* band, as given (>= 0; the reference's infer_band_width at region.rs:1277) */
+    int32_t  h0;             /* initial score (0 for CIGAR regeneration) */
+} fa_cigar_job;
+
+/* OutScore (banded_swa/types.rs:77-85) and the lengths of the three outputs. */
+typedef struct {
+    int32_t score, qle, tle, gtle, gscore, max_off;   /* qle = query_end_pos, tle = target_end_pos, gtle = gtarget_end_pos */
+    int32_t n_cigar;   /* CIGAR operations: len << 4 | op, op 0 = M, 1 = I, 2 = D, 4 = S */
+    int32_t n_ref;     /* aligned reference bases (ref_aligned) */
+    int32_t n_query;   /* aligned query bases (query_aligned) */
+    int32_t cells;     /* cells the recurrence evaluated */
+} fa_cigar_result;
+
+/* Job k's outputs start at cigar[sum over earlier jobs of (qlen + tlen + 2)],
+ * ref_aligned[sum of earlier tlen] and query_aligned[sum of earlier qlen] (each job's
+ * capacity).  p supplies the scoring matrix, gaps, zdrop and pen_clip3 (end_bonus unused).
+ * With fa_ctx_set_timing on, fa_ctx_last_timing covers the kernel. */
+int fa_cigar_batch(fa_ctx *ctx, const fa_params *p, const fa_cigar_job *jobs, uint32_t n,
+                   const uint8_t *qseq, uint64_t qseq_len, const uint8_t *tseq, uint64_t tseq_len,
+                   fa_cigar_result *out, uint32_t *cigar, uint8_t *ref_aligned, uint8_t *query_aligned);
+
 /* ---- mate rescue -------------------------------------------------------
  * Replaces the ksw_align2 calls of execute_mate_rescue_batch_with_engine
  * (src/pipelines/linear/paired/mate_rescue.rs:595-685). */

@@ -1,0 +1,87 @@
+"""The CIGAR kernel (csrc/cigar_kernel.cu) against the CPU restatement of scalar_banded_swa
+(oracle/cigar_oracle.py): scores and ends, every CIGAR operation and both aligned base
+strings, on extension-shaped jobs at several bands, uneven jobs with N bases and repeats,
+codes above 4, empty sequences and a zero band.  Bit-exact."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle_params(p):
+    return {"mat": [int(x) for x in p["mat"][0]], "o_del": int(p["o_del"][0]), "e_del": int(p["e_del"][0]),
+            "o_ins": int(p["o_ins"][0]), "e_ins": int(p["e_ins"][0]), "zdrop": int(p["zdrop"][0]),
+            "pen_clip3": int(p["pen_clip3"][0])}
+
+
+def check(p, jobs, qseq, tseq):
+    from ferrousalign_b200 import cigar as G
+    from oracle import cigar_oracle as C
+    got = G.scalar_banded_swa_batch(p, jobs, qseq, tseq)
+    op = oracle_params(p)
+    for k, j in enumerate(jobs):
+        q = qseq[int(j["q_off"]):int(j["q_off"]) + int(j["qlen"])]
+        t = tseq[int(j["t_off"]):int(j["t_off"]) + int(j["tlen"])]
+        out, cig, ra, qa = C.banded_swa(op, list(q), list(t), int(j["w"]), int(j["h0"]))
+        r = got.results[k]
+        assert {f: int(r[f]) for f in out} == out, (k, r, out)
+        assert got.cigar_of(k) == cig, (k, got.cigar_of(k), cig)
+        assert list(got.ref_aligned_of(k)) == ra and list(got.query_aligned_of(k)) == qa, k
+    return got
+
+
+def jobs_from(batch, rng, bands=(0, 5, 20, 100), h0s=(0,)):
+    from ferrousalign_b200 import cigar as G
+    j = np.zeros(len(batch.jobs), G.CIGAR_JOB_DT)
+    j["q_off"], j["t_off"] = batch.jobs["q_off"], batch.jobs["t_off"]
+    j["qlen"], j["tlen"] = batch.jobs["qlen"], batch.jobs["tlen"]
+    j["w"] = rng.choice(bands, len(j))
+    j["h0"] = rng.choice(h0s, len(j))
+    return j
+
+
+def test_extension_shaped_jobs(built):
+    import ferrousalign_b200 as fa
+    from ferrousalign_b200 import synth
+    rng = np.random.default_rng(1)
+    b = synth.workload_ext_1m(600)
+    p = fa.BandedPairWiseSW().to_struct()
+    got = check(p, jobs_from(b, rng, h0s=(0, 0, 19, 40)), b.qseq, b.tseq)
+    assert (got.results["n_cigar"] > 0).all()
+
+
+def test_uneven_jobs_other_scoring(built):
+    import ferrousalign_b200 as fa
+    from ferrousalign_b200 import synth
+    rng = np.random.default_rng(2)
+    b = synth.workload_ext_uneven(500, ref_len=2_000_000)
+    sw = fa.BandedPairWiseSW(o_del=5, e_del=2, o_ins=3, e_ins=1, zdrop=40, mat=fa.bwa_fill_scmat(2, 3, 0))
+    p = sw.to_struct()
+    p["pen_clip3"] = 9
+    check(p, jobs_from(b, rng, bands=(3, 17, 60)), b.qseq, b.tseq)
+
+
+def test_edges_codes_and_empty(built):
+    import ferrousalign_b200 as fa
+    from ferrousalign_b200 import cigar as G
+    rng = np.random.default_rng(3)
+    n = 200
+    ql = rng.integers(0, 60, n)
+    tl = rng.integers(0, 70, n)
+    ql[:5] = 0
+    tl[5:10] = 0
+    qseq = rng.integers(0, 8, int(ql.sum()) + 1).astype(np.uint8)    # codes 5-7 count as N
+    tseq = rng.integers(0, 8, int(tl.sum()) + 1).astype(np.uint8)
+    jobs = np.zeros(n, G.CIGAR_JOB_DT)
+    jobs["q_off"] = np.concatenate([[0], np.cumsum(ql)[:-1]])
+    jobs["t_off"] = np.concatenate([[0], np.cumsum(tl)[:-1]])
+    jobs["qlen"], jobs["tlen"] = ql, tl
+    jobs["w"] = rng.integers(0, 40, n)
+    jobs["h0"] = rng.integers(0, 30, n)
+    # similar pairs too: the target a mutated copy of the query
+    for k in range(100, n):
+        q = qseq[int(jobs["q_off"][k]):int(jobs["q_off"][k]) + int(ql[k])]
+        m = min(int(ql[k]), int(tl[k]))
+        tseq[int(jobs["t_off"][k]):int(jobs["t_off"][k]) + m] = q[:m]
+    got = check(fa.BandedPairWiseSW().to_struct(), jobs, qseq, tseq)
+    assert (got.results["n_cigar"][:10] == 0).all()
