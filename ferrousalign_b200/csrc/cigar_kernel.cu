@@ -95,36 +95,50 @@ cigar_kernel(const fa_cigar_job *__restrict__ jobs, const CigarPlan *__restrict_
         uint32_t *rowtb = tb + (size_t)i * P.wpr;
         uint32_t acc = 0;
         int widx = -1;
-        for (int j = cb; j < ce; ++j) {
-            const int2 ej = eh[j];
-            int m = ej.x;
-            int e = ej.y;
-            const int qb = Q[j] < 4 ? Q[j] : 4;
-            m += row[qb];
-            if (m < 0) m = 0;
-            int h;
-            uint32_t code;
-            if (m >= e && m >= f) { h = m; code = TB_M; }
-            else if (e >= f) { h = e; code = TB_D; }
-            else { h = f; code = TB_I; }
-            const int kk = j - lo, wi = kk >> 4;
-            if (wi != widx) {
-                if (widx >= 0) rowtb[widx] = acc;
-                acc = 0;
-                widx = wi;
+        // eight columns a step: their row-state words and query bases are loaded together
+        // (each is overwritten only at its own column, so the loads may run ahead)
+        for (int j0 = cb; j0 < ce; j0 += 8) {
+            int2 ev[8];
+            int qv[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                if (j0 + u < ce) {
+                    ev[u] = eh[j0 + u];
+                    qv[u] = Q[j0 + u];
+                }
             }
-            acc |= code << ((kk & 15) * 2);
-            if (m_val < h) { m_val = h; mj = j; }
-            int t = m - oe_del;
-            t = t > 0 ? t : 0;
-            e -= p.e_del;
-            e = e > t ? e : t;
-            eh[j] = make_int2(h1, e);   // H of the previous row's cell, E for the next row
-            t = m - oe_ins;
-            t = t > 0 ? t : 0;
-            f -= p.e_ins;
-            f = f > t ? f : t;
-            h1 = h;
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int j = j0 + u;
+                if (j >= ce) break;
+                int m = ev[u].x;
+                int e = ev[u].y;
+                m += row[qv[u] < 4 ? qv[u] : 4];
+                if (m < 0) m = 0;
+                int h;
+                uint32_t code;
+                if (m >= e && m >= f) { h = m; code = TB_M; }
+                else if (e >= f) { h = e; code = TB_D; }
+                else { h = f; code = TB_I; }
+                const int kk = j - lo, wi = kk >> 4;
+                if (wi != widx) {
+                    if (widx >= 0) rowtb[widx] = acc;
+                    acc = 0;
+                    widx = wi;
+                }
+                acc |= code << ((kk & 15) * 2);
+                if (m_val < h) { m_val = h; mj = j; }
+                int t = m - oe_del;
+                t = t > 0 ? t : 0;
+                e -= p.e_del;
+                e = e > t ? e : t;
+                eh[j] = make_int2(h1, e);   // H of the previous row's cell, E for the next row
+                t = m - oe_ins;
+                t = t > 0 ? t : 0;
+                f -= p.e_ins;
+                f = f > t ? f : t;
+                h1 = h;
+            }
         }
         if (widx >= 0) rowtb[widx] = acc;
         if (ce > cb) cells += ce - cb;
