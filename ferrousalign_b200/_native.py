@@ -57,6 +57,14 @@ CIGAR_JOB_DT = np.dtype([("q_off", "<u8"), ("t_off", "<u8"), ("qlen", "<i4"), ("
 CIGAR_RESULT_DT = np.dtype([("score", "<i4"), ("qle", "<i4"), ("tle", "<i4"), ("gtle", "<i4"), ("gscore", "<i4"),
                             ("max_off", "<i4"), ("n_cigar", "<i4"), ("n_ref", "<i4"), ("n_query", "<i4"),
                             ("cells", "<i4")])
+INSERT_BOUNDS_DT = np.dtype([("low", "<i4"), ("high", "<i4"), ("failed", "<i4"), ("_pad", "<i4")])
+RESCUE_ALN_DT = np.dtype([("pos", "<i8"), ("ref_id", "<i4"), ("is_rev", "<i4"), ("ref_len", "<i4"), ("score", "<i4")])
+RESCUE_CAND_DT = np.dtype([("read", "<u4"), ("aln_first", "<u4"), ("aln_count", "<u4"), ("primary", "<u4"),
+                           ("anchor", RESCUE_ALN_DT)])
+RESCUE_OPTS_DT = np.dtype([("pen_unpaired", "<i4"), ("max_matesw", "<i4"), ("min_seed_len", "<i4"),
+                           ("match_score", "<i4")])
+RESCUE_JOB_INFO_DT = np.dtype([("cand", "<u4"), ("orientation", "<i4"), ("is_rev", "<i4"), ("rid", "<i4"),
+                               ("adj_rb", "<i8"), ("adj_re", "<i8")])
 
 assert PARAMS_DT.itemsize == 64 and JOB_DT.itemsize == 40 and EXT_RESULT_DT.itemsize == 24
 assert STATS_DT.itemsize == 40 and MATE_PARAMS_DT.itemsize == 48 and MATE_JOB_DT.itemsize == 32
@@ -65,6 +73,8 @@ assert REGION_OPTS_DT.itemsize == 16 and SEED_EXT_DT.itemsize == 24 and REGION_D
 assert COLLECT_OPTS_DT.itemsize == 24 and CHAIN_DT.itemsize == 16 and SEED_DT.itemsize == 16
 assert COLLECT_COUNTS_DT.itemsize == 32
 assert CIGAR_JOB_DT.itemsize == 32 and CIGAR_RESULT_DT.itemsize == 40
+assert INSERT_BOUNDS_DT.itemsize == 16 and RESCUE_ALN_DT.itemsize == 24 and RESCUE_CAND_DT.itemsize == 40
+assert RESCUE_OPTS_DT.itemsize == 16 and RESCUE_JOB_INFO_DT.itemsize == 32
 
 # Every symbol the header declares, with its ctypes signature.
 _P = C.c_void_p
@@ -108,6 +118,8 @@ SIGNATURES = {
     "fa_collect_ext_jobs": (C.c_int, [_P, _P, _P, C.c_uint64, _P, _P, C.c_uint32, _P, C.c_uint32, _P, C.c_uint32,
                                       _P, _P, _P, _P, C.c_uint64, _P, _P, _P, _P]),
     "fa_cigar_batch": (C.c_int, [_P, _P, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64, _P, _P, _P, _P]),
+    "fa_collect_mate_jobs": (C.c_int, [_P, _P, _P, _P, C.c_uint64, _P, _P, C.c_uint32, _P, _P, C.c_uint32, _P,
+                                       C.c_uint32, _P, C.c_uint32, _P, _P, _P, C.c_uint64, _P, C.c_uint64, _P]),
     "fa_merge_regions": (C.c_int, [_P, _P, _P, C.c_uint32, _P, _P, C.c_uint32, _P, C.c_uint32, _P, C.c_uint32,
                                    _P]),
     "fa_merge_regions_device": (C.c_int, [_P, _P, _P, C.c_uint32, _P, _P, C.c_uint32, _P, C.c_uint32, _P,

@@ -44,14 +44,6 @@ namespace {
 constexpr int kCollectThreads = 128;
 constexpr int kScanThreads = 1024;
 
-// base of FM-index position x (x < 2 l_pac)
-__device__ __forceinline__ uint8_t pac_base(const uint8_t *__restrict__ pac, uint64_t l_pac, uint64_t x) {
-    const bool rev = x >= l_pac;
-    const uint64_t f = rev ? (l_pac << 1) - 1 - x : x;
-    const uint8_t b = (pac[f >> 2] >> ((~(uint32_t)f & 3u) << 1)) & 3u;
-    return rev ? (uint8_t)(3u - b) : b;
-}
-
 __global__ void __launch_bounds__(kCollectThreads)
 collect_plan_kernel(fa_collect_opts opt, uint64_t l_pac, const uint64_t *__restrict__ read_off,
                     const fa_chain *__restrict__ chains, uint32_t n_chains, const fa_seed *__restrict__ seeds,
@@ -312,10 +304,16 @@ cudaError_t launch_collect_plan(const fa_collect_opts &opt, uint64_t l_pac, cons
     if (n_chains == 0) return cudaSuccess;
     collect_plan_kernel<<<(n_chains + kCollectThreads - 1) / kCollectThreads, kCollectThreads, 0, s>>>(
         opt, l_pac, d_read_off, d_chains, n_chains, d_seeds, d_plan);
-    const uint32_t nb = (uint32_t)collect_scan_blocks(n_chains);
-    collect_scan_sums_kernel<<<nb, kScanThreads, 0, s>>>(d_plan, n_chains, d_sums);
+    return launch_plan_scan(d_plan, n_chains, d_sums, s);
+}
+
+cudaError_t launch_plan_scan(CollectPlan *d_plan, uint32_t n, ulonglong4 *d_sums, cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    const uint32_t nb = (uint32_t)collect_scan_blocks(n);
+    collect_scan_sums_kernel<<<nb, kScanThreads, 0, s>>>(d_plan, n, d_sums);
     collect_scan_top_kernel<<<1, kScanThreads, 0, s>>>(d_sums, nb);
-    collect_scan_apply_kernel<<<nb, kScanThreads, 0, s>>>(d_plan, n_chains, d_sums);
+    collect_scan_apply_kernel<<<nb, kScanThreads, 0, s>>>(d_plan, n, d_sums);
     return cudaGetLastError();
 }
 

@@ -83,6 +83,7 @@ struct fa_ctx {
     DevBuf reg_in, reg_out;   // region merge of host buffers: inputs, regions
     DevBuf col_in, col_plan, col_out;   // job collection: inputs, chain plans + scan sums, outputs
     DevBuf cg_in, cg_scratch, cg_out;   // CIGAR regeneration: inputs, row state + traceback, outputs
+    DevBuf mc_in, mc_plan, mc_out;      // mate-rescue jobs: inputs, plans + scan sums, outputs
     DevBuf w_first, w_cur, prev, kk, w_final, tries, missed, list_a, list_b, hist, feat, wbf, part_n, part_w;
     uint32_t last_launches = 0;
     bool timing = false;
@@ -792,7 +793,7 @@ void fa_ctx_destroy(fa_ctx *c) {
                       &c->misc, &c->w_first, &c->w_cur, &c->prev, &c->kk, &c->w_final, &c->tries,
                       &c->missed, &c->list_a, &c->list_b, &c->hist, &c->feat, &c->wbf, &c->part_n,
                       &c->part_w, &c->ovf, &c->reg_in, &c->reg_out, &c->col_in, &c->col_plan, &c->col_out,
-                      &c->cg_in, &c->cg_scratch, &c->cg_out})
+                      &c->cg_in, &c->cg_scratch, &c->cg_out, &c->mc_in, &c->mc_plan, &c->mc_out})
         b->release();
     for (int k = 0; k < 2; ++k) {
         if (c->join_ev[k]) cudaEventDestroy(c->join_ev[k]);
@@ -1421,6 +1422,99 @@ int fa_cigar_batch(fa_ctx *c, const fa_params *p, const fa_cigar_job *jobs, uint
     FA_CUDA(cudaMemcpyAsync(cigar, d_cig, 4 * cig, cudaMemcpyDeviceToHost, s));
     if (ref) FA_CUDA(cudaMemcpyAsync(ref_aligned, d_ref, ref, cudaMemcpyDeviceToHost, s));
     if (qry) FA_CUDA(cudaMemcpyAsync(query_aligned, d_qry, qry, cudaMemcpyDeviceToHost, s));
+    FA_CUDA(cudaStreamSynchronize(s));
+    return FA_OK;
+}
+
+int fa_collect_mate_jobs(fa_ctx *c, const fa_rescue_opts *opt, const fa_insert_bounds *bounds4, const uint8_t *pac,
+                         uint64_t l_pac, const uint64_t *chr_off, const uint64_t *chr_len, uint32_t n_chr,
+                         const uint8_t *reads, const uint64_t *read_off, uint32_t n_reads, const fa_rescue_aln *alns,
+                         uint32_t n_alns, const fa_rescue_cand *cands, uint32_t n_cand, fa_mate_job *jobs,
+                         fa_rescue_job_info *info, uint8_t *qbuf, uint64_t qbuf_cap, uint8_t *tbuf,
+                         uint64_t tbuf_cap, fa_collect_counts *counts) {
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    if (!opt || !bounds4 || !counts) return fail(FA_ERR_ARG, "null argument");
+    *counts = fa_collect_counts{};
+    if (n_cand == 0) return FA_OK;
+    if (!cands || !jobs || !info || !read_off || !reads || (n_alns && !alns)) return fail(FA_ERR_ARG, "null buffer");
+    if (l_pac == 0 || !pac || l_pac > (1ull << 62)) return fail(FA_ERR_ARG, "empty or oversized packed reference");
+    if (n_chr == 0 || !chr_off || !chr_len) return fail(FA_ERR_ARG, "no reference sequences");
+    for (uint32_t k = 0; k < n_chr; ++k) {
+        if (chr_off[k] + chr_len[k] > l_pac) return fail(FA_ERR_ARG, "a reference sequence runs past l_pac");
+        if (k && chr_off[k] < chr_off[k - 1]) return fail(FA_ERR_ARG, "reference offsets are not ascending");
+    }
+    for (uint32_t r = 0; r < n_reads; ++r)
+        if (read_off[r + 1] < read_off[r] || read_off[r + 1] - read_off[r] > FA_MAX_QLEN)
+            return fail(FA_ERR_ARG, "read %u: bad offsets or longer than FA_MAX_QLEN", r);
+    for (uint32_t k = 0; k < n_cand; ++k) {
+        const fa_rescue_cand &q = cands[k];
+        if (q.read >= n_reads || (uint64_t)q.aln_first + q.aln_count > n_alns || q.primary >= n_alns)
+            return fail(FA_ERR_ARG, "rescue attempt %u: index out of range", k);
+        if (q.anchor.ref_id < 0 || (uint32_t)q.anchor.ref_id >= n_chr)
+            return fail(FA_ERR_ARG, "rescue attempt %u: anchor reference out of range", k);
+    }
+    FA_CUDA(cudaSetDevice(c->device));
+    cudaStream_t s = c->stream;
+    auto up16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
+    const uint64_t read_bytes = read_off[n_reads];
+    const size_t b_pac = up16((size_t)((l_pac + 3) / 4)), b_chr = up16(8ull * n_chr);
+    const size_t b_reads = up16(read_bytes + 1), b_off = up16(8ull * (n_reads + 1));
+    const size_t b_alns = up16(sizeof(fa_rescue_aln) * n_alns), b_cands = up16(sizeof(fa_rescue_cand) * n_cand);
+    FA_CUDA(c->mc_in.ensure(b_pac + 2 * b_chr + b_reads + b_off + b_alns + b_cands));
+    char *in = c->mc_in.as<char>();
+    size_t o = 0;
+    auto take = [&](size_t b) { char *p = in + o; o += b; return p; };
+    uint8_t *d_pac = reinterpret_cast<uint8_t *>(take(b_pac));
+    uint64_t *d_coff = reinterpret_cast<uint64_t *>(take(b_chr));
+    uint64_t *d_clen = reinterpret_cast<uint64_t *>(take(b_chr));
+    uint8_t *d_reads = reinterpret_cast<uint8_t *>(take(b_reads));
+    uint64_t *d_off = reinterpret_cast<uint64_t *>(take(b_off));
+    fa_rescue_aln *d_alns = reinterpret_cast<fa_rescue_aln *>(take(b_alns));
+    fa_rescue_cand *d_cands = reinterpret_cast<fa_rescue_cand *>(take(b_cands));
+    FA_CUDA(cudaMemcpyAsync(d_pac, pac, (size_t)((l_pac + 3) / 4), cudaMemcpyHostToDevice, s));
+    FA_CUDA(cudaMemcpyAsync(d_coff, chr_off, 8ull * n_chr, cudaMemcpyHostToDevice, s));
+    FA_CUDA(cudaMemcpyAsync(d_clen, chr_len, 8ull * n_chr, cudaMemcpyHostToDevice, s));
+    if (read_bytes) FA_CUDA(cudaMemcpyAsync(d_reads, reads, read_bytes, cudaMemcpyHostToDevice, s));
+    FA_CUDA(cudaMemcpyAsync(d_off, read_off, 8ull * (n_reads + 1), cudaMemcpyHostToDevice, s));
+    if (n_alns) FA_CUDA(cudaMemcpyAsync(d_alns, alns, sizeof(fa_rescue_aln) * n_alns, cudaMemcpyHostToDevice, s));
+    FA_CUDA(cudaMemcpyAsync(d_cands, cands, sizeof(fa_rescue_cand) * n_cand, cudaMemcpyHostToDevice, s));
+    const size_t nb = collect_scan_blocks(n_cand);
+    const size_t b_plan = up16(sizeof(CollectPlan) * n_cand);
+    FA_CUDA(c->mc_plan.ensure(b_plan + sizeof(ulonglong4) * (nb + 1)));
+    CollectPlan *d_plan = c->mc_plan.as<CollectPlan>();
+    ulonglong4 *d_sums = reinterpret_cast<ulonglong4 *>(c->mc_plan.as<char>() + b_plan);
+    const RescueRef ref{l_pac, d_pac, d_coff, d_clen, n_chr};
+    if (c->timing) FA_CUDA(cudaEventRecord(c->kev0, s));
+    FA_CUDA(launch_mate_collect_plan(*opt, bounds4, ref, d_off, d_alns, d_cands, n_cand, d_plan, s));
+    FA_CUDA(launch_plan_scan(d_plan, n_cand, d_sums, s));
+    ulonglong4 tot;
+    FA_CUDA(cudaMemcpyAsync(&tot, d_sums + nb, sizeof(tot), cudaMemcpyDeviceToHost, s));
+    FA_CUDA(cudaStreamSynchronize(s));
+    counts->n_left = (uint32_t)tot.y;
+    counts->qbuf_len = tot.z;
+    counts->tbuf_len = tot.x;
+    if (tot.x > tbuf_cap || tot.z > qbuf_cap)
+        return fail(FA_ERR_CAPACITY, "qbuf_cap or tbuf_cap below the jobs' bytes (counts->qbuf_len, tbuf_len)");
+    if ((tot.z && !qbuf) || (tot.x && !tbuf)) return fail(FA_ERR_ARG, "null sequence buffer");
+    const size_t b_jobs = up16(sizeof(fa_mate_job) * tot.y), b_info = up16(sizeof(fa_rescue_job_info) * tot.y);
+    const size_t b_q = up16(tot.z + 1), b_t = up16(tot.x + 1);
+    FA_CUDA(c->mc_out.ensure(b_jobs + b_info + b_q + b_t));
+    char *out = c->mc_out.as<char>();
+    fa_mate_job *d_jobs = reinterpret_cast<fa_mate_job *>(out);
+    fa_rescue_job_info *d_info = reinterpret_cast<fa_rescue_job_info *>(out + b_jobs);
+    uint8_t *d_q = reinterpret_cast<uint8_t *>(out + b_jobs + b_info);
+    uint8_t *d_t = reinterpret_cast<uint8_t *>(out + b_jobs + b_info + b_q);
+    FA_CUDA(launch_mate_collect_fill(*opt, bounds4, ref, d_reads, d_off, d_alns, d_cands, n_cand, d_plan, d_jobs,
+                                     d_info, d_q, d_t, s));
+    if (c->timing) FA_CUDA(cudaEventRecord(c->kev1, s));
+    c->last_launches = 5;
+    c->last_stream = s;
+    if (tot.y) {
+        FA_CUDA(cudaMemcpyAsync(jobs, d_jobs, sizeof(fa_mate_job) * tot.y, cudaMemcpyDeviceToHost, s));
+        FA_CUDA(cudaMemcpyAsync(info, d_info, sizeof(fa_rescue_job_info) * tot.y, cudaMemcpyDeviceToHost, s));
+    }
+    if (tot.z) FA_CUDA(cudaMemcpyAsync(qbuf, d_q, tot.z, cudaMemcpyDeviceToHost, s));
+    if (tot.x) FA_CUDA(cudaMemcpyAsync(tbuf, d_t, tot.x, cudaMemcpyDeviceToHost, s));
     FA_CUDA(cudaStreamSynchronize(s));
     return FA_OK;
 }

@@ -17,6 +17,16 @@ enum : uint32_t {
     ST_RANGE    = 1u << 4,   // a chain's seed range is malformed (region merge)
 };
 
+// Base (0-3) of FM-index position x < 2 l_pac in a 2-bit packed reference (the .pac layout:
+// base k in bits 7-6 of byte k/4 when k % 4 == 0 down to bits 1-0 when k % 4 == 3; positions
+// at or past l_pac are the reverse complement of forward position 2 l_pac - 1 - x).
+__device__ __forceinline__ uint8_t pac_base(const uint8_t *__restrict__ pac, uint64_t l_pac, uint64_t x) {
+    const bool rev = x >= l_pac;
+    const uint64_t f = rev ? (l_pac << 1) - 1 - x : x;
+    const uint8_t b = (pac[f >> 2] >> ((~(uint32_t)f & 3u) << 1)) & 3u;
+    return rev ? (uint8_t)(3u - b) : b;
+}
+
 // Scoring parameters in the form the extension kernel consumes.
 struct ExtParams {
     int8_t  mat[25];

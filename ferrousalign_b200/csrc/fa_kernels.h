@@ -138,12 +138,33 @@ size_t collect_scan_blocks(uint32_t n_chains);   // entries of the scan's block-
 cudaError_t launch_collect_plan(const fa_collect_opts &opt, uint64_t l_pac, const uint64_t *d_read_off,
                                 const fa_chain *d_chains, uint32_t n_chains, const fa_seed *d_seeds,
                                 CollectPlan *d_plan, ulonglong4 *d_sums, cudaStream_t s);
+// the scan alone: plan[i].off = exclusive prefix sums of plan[].v; d_sums[collect_scan_blocks(n)]
+// gets the totals
+cudaError_t launch_plan_scan(CollectPlan *d_plan, uint32_t n, ulonglong4 *d_sums, cudaStream_t s);
 cudaError_t launch_collect_fill(const fa_collect_opts &opt, const uint8_t *d_pac, uint64_t l_pac,
                                 const uint8_t *d_reads, const uint64_t *d_read_off, uint32_t n_reads,
                                 const fa_chain *d_chains, uint32_t n_chains, const fa_seed *d_seeds,
                                 const CollectPlan *d_plan, fa_job *d_left, fa_job *d_right, uint8_t *d_qbuf,
                                 uint8_t *d_tbuf, fa_seed_ext *d_seed_ext, uint32_t *d_chain_first,
                                 uint64_t *d_chain_win, cudaStream_t s);
+
+// Mate-rescue jobs (mate_collect_kernel.cu): per attempt a plan (v = {target bytes, jobs,
+// query bytes, 0}), scanned with launch_plan_scan, then the fill.
+struct RescueRef {
+    uint64_t l_pac;
+    const uint8_t *pac;
+    const uint64_t *chr_off, *chr_len;
+    uint32_t n_chr;
+};
+cudaError_t launch_mate_collect_plan(const fa_rescue_opts &opt, const fa_insert_bounds *bounds4, RescueRef ref,
+                                     const uint64_t *d_read_off, const fa_rescue_aln *d_alns,
+                                     const fa_rescue_cand *d_cands, uint32_t n_cand, CollectPlan *d_plan,
+                                     cudaStream_t s);
+cudaError_t launch_mate_collect_fill(const fa_rescue_opts &opt, const fa_insert_bounds *bounds4, RescueRef ref,
+                                     const uint8_t *d_reads, const uint64_t *d_read_off, const fa_rescue_aln *d_alns,
+                                     const fa_rescue_cand *d_cands, uint32_t n_cand, const CollectPlan *d_plan,
+                                     fa_mate_job *d_jobs, fa_rescue_job_info *d_info, uint8_t *d_qbuf,
+                                     uint8_t *d_tbuf, cudaStream_t s);
 
 // CIGAR regeneration (cigar_kernel.cu): per job the offsets of its outputs (cigar words,
 // aligned reference / query bases) and of its scratch (row state in int2 units, traceback

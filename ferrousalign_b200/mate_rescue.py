@@ -98,3 +98,65 @@ def execute_mate_rescue_batch_with_engine(jobs: list[MateRescueJob], engine=None
     t = np.frombuffer(bytes(tb), dtype=np.uint8) if tb else np.zeros(1, np.uint8)
     out, _ = mate_sw_batch(make_mate_params(), arr, q, t)
     return [MateRescueResult(i, Kswr(*(int(v) for v in o))) for i, o in enumerate(out)]
+
+
+# ---- rescue jobs from anchors (collect_rescue_jobs_for_read_soa, mate_rescue.rs:1804-2045)
+
+def rescue_opts(pen_unpaired: int = 17, max_matesw: int = 50, min_seed_len: int = 19,
+                match_score: int = 1) -> np.ndarray:
+    """MemOpt's pen_unpaired and max_matesw, the index's min_seed_len, the match score."""
+    o = np.zeros(1, N.RESCUE_OPTS_DT)
+    o["pen_unpaired"], o["max_matesw"], o["min_seed_len"], o["match_score"] = (pen_unpaired, max_matesw,
+                                                                               min_seed_len, match_score)
+    return o
+
+
+@dataclass
+class RescueJobs:
+    jobs: np.ndarray     # MATE_JOB_DT, for mate_sw_batch with qbuf / tbuf
+    info: np.ndarray     # RESCUE_JOB_INFO_DT: attempt, orientation, strand, window
+    qbuf: np.ndarray
+    tbuf: np.ndarray
+
+
+def collect_rescue_jobs(pac: np.ndarray, l_pac: int, chr_off: np.ndarray, chr_len: np.ndarray,
+                        reads: np.ndarray, read_off: np.ndarray, alns: np.ndarray, cands: np.ndarray,
+                        bounds: np.ndarray, opts: np.ndarray | None = None,
+                        ctx: N.Context | None = None) -> RescueJobs:
+    """Mate-rescue jobs of every attempt (RESCUE_CAND_DT) on the GPU; bounds is
+    INSERT_BOUNDS_DT[4] (FF, FR, RF, RR: low, high, failed)."""
+    lib = N.load()
+    ctx = ctx or N.default_context()
+    opts = rescue_opts() if opts is None else opts
+    pac = np.ascontiguousarray(pac, np.uint8)
+    chr_off = np.ascontiguousarray(chr_off, np.uint64)
+    chr_len = np.ascontiguousarray(chr_len, np.uint64)
+    reads = np.ascontiguousarray(reads, np.uint8)
+    read_off = np.ascontiguousarray(read_off, np.uint64)
+    alns = np.ascontiguousarray(alns, N.RESCUE_ALN_DT)
+    cands = np.ascontiguousarray(cands, N.RESCUE_CAND_DT)
+    bounds = np.ascontiguousarray(bounds, N.INSERT_BOUNDS_DT)
+    n = len(cands)
+    jobs = np.zeros(4 * n, N.MATE_JOB_DT)
+    info = np.zeros(4 * n, N.RESCUE_JOB_INFO_DT)
+    counts = np.zeros(1, N.COLLECT_COUNTS_DT)
+    qlen = np.diff(read_off.astype(np.int64))
+    qcap = int(4 * qlen[cands["read"]].sum()) if n else 0
+    span = int(np.maximum(bounds["high"] - bounds["low"], 0).max()) if len(bounds) else 0
+    tcap = int(4 * (qlen[cands["read"]] + span + 1).sum()) if n else 0
+    for _ in range(2):
+        qbuf = np.zeros(max(qcap, 1), np.uint8)
+        tbuf = np.zeros(max(tcap, 1), np.uint8)
+        rc = lib.fa_collect_mate_jobs(ctx.handle, N.ptr(opts), N.ptr(bounds), N.ptr(pac), l_pac, N.ptr(chr_off),
+                                      N.ptr(chr_len), len(chr_off), N.ptr(reads), N.ptr(read_off),
+                                      len(read_off) - 1, N.ptr(alns), len(alns), N.ptr(cands), n, N.ptr(jobs),
+                                      N.ptr(info), N.ptr(qbuf), qcap, N.ptr(tbuf), tcap, N.ptr(counts))
+        c = counts[0]
+        if rc == N.FA_ERR_CAPACITY and (int(c["qbuf_len"]) > qcap or int(c["tbuf_len"]) > tcap):
+            qcap, tcap = max(qcap, int(c["qbuf_len"])), max(tcap, int(c["tbuf_len"]))
+            continue
+        N.check(rc)
+        break
+    k = int(counts[0]["n_left"])
+    return RescueJobs(jobs[:k].copy(), info[:k].copy(), qbuf[:int(counts[0]["qbuf_len"])],
+                      tbuf[:int(counts[0]["tbuf_len"])])

@@ -258,3 +258,50 @@ def workload_cigar(n: int = 200_000, seed: int = 31, ref_len: int = 10_000_000, 
     jobs["tlen"] = np.minimum(b.jobs["tlen"], b.jobs["qlen"] + rng.integers(-3, 4, n))
     jobs["w"] = np.abs(jobs["qlen"] - jobs["tlen"]) + rng.integers(5, 31, n)
     return jobs, b.qseq, b.tseq
+
+
+def workload_rescue(n_pairs: int = 100_000, seed: int = 41, ref_len: int = 20_000_000, n_chr: int = 6,
+                    read_len: int = 151):
+    """Mate-rescue attempts shaped like paired-end data: a reference cut into n_chr sequences,
+    fragments of N(400, 50) bases, read 1 (the anchor) at one end of a fragment and read 2 at
+    the other, either strand; read 2 carries 1-3 alignments of its own, half the time one of
+    them at its true place (so that orientation is already paired) and the others anywhere.
+    Returns (ref_codes, chr_off, chr_len, reads, read_off, alns, cands) with reads the
+    rescued reads' codes."""
+    rng = np.random.default_rng(seed)
+    ref = reference(ref_len, seed=seed, n_rate=0.001)
+    cuts = np.sort(rng.choice(np.arange(1, n_chr * 8) * (ref_len // (n_chr * 8)), n_chr - 1, replace=False))
+    chr_off = np.concatenate([[0], cuts]).astype(np.uint64)
+    chr_len = (np.concatenate([cuts, [ref_len]]) - chr_off.astype(np.int64)).astype(np.uint64)
+    ins = np.clip(rng.normal(400, 50, n_pairs).astype(np.int64), read_len, 1000)
+    rid = rng.integers(0, n_chr, n_pairs)
+    span = chr_len[rid].astype(np.int64) - ins - 1
+    p1 = chr_off[rid].astype(np.int64) + (rng.random(n_pairs) * span).astype(np.int64)
+    flip = rng.random(n_pairs) < 0.5
+    reads = np.empty(n_pairs * read_len, np.uint8)
+    read_off = np.arange(n_pairs + 1, dtype=np.uint64) * read_len
+    alns_l, cands = [], np.zeros(n_pairs, N.RESCUE_CAND_DT)
+    for i in range(n_pairs):
+        a_pos, m_pos = int(p1[i]), int(p1[i] + ins[i] - read_len)
+        if flip[i]:
+            a_pos, m_pos = m_pos, a_pos
+        seg = ref[m_pos:m_pos + read_len] & 3
+        # read 2 lies on the other strand from the anchor (FR pairs)
+        mate_rev = not flip[i]
+        reads[i * read_len:(i + 1) * read_len] = (3 - seg)[::-1] if mate_rev else seg
+        off = int(chr_off[rid[i]])
+        own = []
+        if rng.random() < 0.5:
+            own.append((m_pos - off, int(rid[i]), int(mate_rev), read_len, int(rng.integers(100, 152))))
+        for _ in range(int(rng.integers(1 if not own else 0, 3))):
+            r2 = int(rng.integers(0, n_chr))
+            own.append((int(rng.integers(0, int(chr_len[r2]) - read_len)), r2, int(rng.integers(0, 2)), read_len,
+                        int(rng.integers(20, 152))))
+        first = len(alns_l)
+        alns_l.extend(own)
+        best = max(range(len(own)), key=lambda k: own[k][4])
+        cands[i] = (i, first, len(own), first + best,
+                    (a_pos - off, int(rid[i]), int(flip[i]), read_len, int(rng.integers(120, 152))))
+    alns = np.array(alns_l, dtype=[("pos", "<i8"), ("ref_id", "<i4"), ("is_rev", "<i4"), ("ref_len", "<i4"),
+                                   ("score", "<i4")]).astype(N.RESCUE_ALN_DT)
+    return ref, chr_off, chr_len, reads, read_off, alns, cands

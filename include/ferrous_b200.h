@@ -393,6 +393,58 @@ int fa_mate_sw_batch(fa_ctx *ctx, const fa_mate_params *p, const fa_mate_job *jo
                      const uint8_t *tseq, uint64_t tseq_len,
                      fa_kswr *out, fa_ext_stats *stats);
 
+/* Mate-rescue jobs (collect_rescue_jobs_for_read_soa, mate_rescue.rs:1804-2045): per rescue
+ * candidate -- a read whose mate (the anchor) aligned -- nothing unless its primary
+ * alignment scores at least best - pen_unpaired; then the orientations not yet failed
+ * (insert-size statistics) nor covered by one of the read's own alignments at a consistent
+ * distance (mem_infer_dir, mate_rescue.rs:537-551), and for each a reference window
+ * [anchor +/- insert-size bounds, plus the read length] cut to the anchor's chromosome
+ * (bns_fetch_seq, bntseq.rs:700-739); a window on that chromosome of at least min_seed_len
+ * bases gives a job: the read (reverse complemented for the reverse orientations) against
+ * the window, read from the 2-bit packed reference. */
+typedef struct { int32_t low, high, failed, _pad; } fa_insert_bounds;   /* InsertSizeStats per orientation */
+
+typedef struct {                /* one alignment of a read (SoAAlignmentResult entry) */
+    int64_t pos;                /* 0-based position on its chromosome */
+    int32_t ref_id;
+    int32_t is_rev;             /* flag & REVERSE */
+    int32_t ref_len;            /* reference bases its CIGAR covers */
+    int32_t score;
+} fa_rescue_aln;
+
+typedef struct {                /* one rescue attempt */
+    uint32_t read;              /* the read to rescue: reads[read_off[read] .. read_off[read+1]) */
+    uint32_t aln_first;         /* its alignments: alns[aln_first .. aln_first + aln_count) */
+    uint32_t aln_count;
+    uint32_t primary;           /* index into alns of its primary alignment */
+    fa_rescue_aln anchor;       /* the mate's primary alignment */
+} fa_rescue_cand;
+
+typedef struct {
+    int32_t pen_unpaired, max_matesw, min_seed_len, match_score;
+} fa_rescue_opts;
+
+typedef struct {                /* per job: which attempt, orientation and window it came from */
+    uint32_t cand;
+    int32_t  orientation;       /* 0 FF, 1 FR, 2 RF, 3 RR */
+    int32_t  is_rev;
+    int32_t  rid;
+    int64_t  adj_rb, adj_re;
+} fa_rescue_job_info;
+
+/* chr_off/chr_len: the reference sequences (annotations: offset and length, n_chr of them)
+ * of the packed reference (pac, l_pac as for fa_collect_ext_jobs).  Outputs: up to
+ * 4 n_cand jobs and infos, in the reference's order (attempts in order, orientations 0-3);
+ * jobs' q_off/t_off address qbuf (qbuf_cap bytes) and tbuf (tbuf_cap bytes); their xtra is
+ * fa_mate_xtra(read length, match_score, min_seed_len).  With too small a buffer nothing is
+ * written except counts (n_left = jobs, qbuf_len, tbuf_len) and FA_ERR_CAPACITY returns. */
+int fa_collect_mate_jobs(fa_ctx *ctx, const fa_rescue_opts *opt, const fa_insert_bounds *bounds4,
+                         const uint8_t *pac, uint64_t l_pac, const uint64_t *chr_off, const uint64_t *chr_len,
+                         uint32_t n_chr, const uint8_t *reads, const uint64_t *read_off, uint32_t n_reads,
+                         const fa_rescue_aln *alns, uint32_t n_alns, const fa_rescue_cand *cands, uint32_t n_cand,
+                         fa_mate_job *jobs, fa_rescue_job_info *info, uint8_t *qbuf, uint64_t qbuf_cap,
+                         uint8_t *tbuf, uint64_t tbuf_cap, fa_collect_counts *counts);
+
 /* ---- learned band (no reference counterpart) ----------------------------
  * A 16-64-32-1 MLP (BF16 weights, FP32 accumulation) predicts log2 of the band each
  * extension needs from 16 features of the job (seed length, lengths, h0, the chain's
