@@ -11,9 +11,10 @@
 // :535-559); a window on that sequence of at least min_seed_len bases is a job: the read
 // (reverse complemented for orientations 1 and 2) against the window's bases.
 //
-// One thread per attempt computes its (at most four) windows twice: once to size its
+// Each attempt's (at most four) windows are computed twice: by one thread to size its
 // output (target bytes, jobs, query bytes, scanned over the attempts with the job
-// collection's scan) and once to write the jobs, their sequences and their origin.
+// collection's scan), then by one warp whose lanes write the read and window bases of its
+// jobs side by side.
 
 #include "fa_device.cuh"
 #include "fa_kernels.h"
@@ -159,7 +160,8 @@ mate_collect_fill_kernel(fa_rescue_opts opt, fa_insert_bounds b0, fa_insert_boun
                          fa_rescue_job_info *__restrict__ info, uint8_t *__restrict__ qbuf,
                          uint8_t *__restrict__ tbuf)
 {
-    const uint32_t i = blockIdx.x * kMateCollectThreads + threadIdx.x;
+    const uint32_t i = (blockIdx.x * kMateCollectThreads + threadIdx.x) >> 5;   // one warp per attempt
+    const int lane = threadIdx.x & 31;
     if (i >= n_cand) return;
     const CollectPlan pl = plan[i];
     if (pl.v[1] == 0) return;
@@ -168,7 +170,7 @@ mate_collect_fill_kernel(fa_rescue_opts opt, fa_insert_bounds b0, fa_insert_boun
     const uint64_t ro = read_off[c.read];
     const int qlen = (int)(read_off[c.read + 1] - ro);
     Win w[4];
-    rescue_windows(opt, bd, R, alns, c, qlen, w);
+    rescue_windows(opt, bd, R, alns, c, qlen, w);   // every lane: the same windows
     uint64_t ji = pl.off[1], qo = pl.off[2], to = pl.off[0];
     // mate_rescue.rs:314-321: the xtra word of every job of this read
     uint32_t xtra = 0x40000u | 0x80000u | (uint32_t)(opt.min_seed_len * opt.match_score);
@@ -176,28 +178,30 @@ mate_collect_fill_kernel(fa_rescue_opts opt, fa_insert_bounds b0, fa_insert_boun
     for (int r = 0; r < 4; ++r) {
         if (!w[r].ok) continue;
         const bool is_rev = (r >> 1) != (r & 1);
-        for (int k = 0; k < qlen; ++k) {   // the read, reverse complemented for 1 and 2
+        for (int k = lane; k < qlen; k += 32) {   // the read, reverse complemented for 1 and 2
             const uint8_t b = is_rev ? reads[ro + qlen - 1 - k] : reads[ro + k];
             qbuf[qo + k] = is_rev ? (uint8_t)(b < 4 ? 3 - b : 4) : b;
         }
         const uint64_t L = (uint64_t)(w[r].end - w[r].beg);
-        for (uint64_t p = 0; p < L; ++p) tbuf[to + p] = pac_base(R.pac, R.l_pac, (uint64_t)w[r].beg + p);
-        fa_mate_job j;
-        j.q_off = qo;
-        j.t_off = to;
-        j.qlen = qlen;
-        j.tlen = (int32_t)L;
-        j.xtra = xtra;
-        j._pad = 0;
-        jobs[ji] = j;
-        fa_rescue_job_info f;
-        f.cand = i;
-        f.orientation = r;
-        f.is_rev = is_rev;
-        f.rid = w[r].rid;
-        f.adj_rb = w[r].beg;
-        f.adj_re = w[r].end;
-        info[ji] = f;
+        for (uint64_t p = lane; p < L; p += 32) tbuf[to + p] = pac_base(R.pac, R.l_pac, (uint64_t)w[r].beg + p);
+        if (lane == 0) {
+            fa_mate_job j;
+            j.q_off = qo;
+            j.t_off = to;
+            j.qlen = qlen;
+            j.tlen = (int32_t)L;
+            j.xtra = xtra;
+            j._pad = 0;
+            jobs[ji] = j;
+            fa_rescue_job_info f;
+            f.cand = i;
+            f.orientation = r;
+            f.is_rev = is_rev;
+            f.rid = w[r].rid;
+            f.adj_rb = w[r].beg;
+            f.adj_re = w[r].end;
+            info[ji] = f;
+        }
         ++ji;
         qo += (uint64_t)qlen;
         to += L;
@@ -225,8 +229,9 @@ cudaError_t launch_mate_collect_fill(const fa_rescue_opts &opt, const fa_insert_
                                      uint8_t *d_tbuf, cudaStream_t s)
 {
     if (n_cand == 0) return cudaSuccess;
-    mate_collect_fill_kernel<<<(n_cand + kMateCollectThreads - 1) / kMateCollectThreads, kMateCollectThreads, 0,
-                               s>>>(opt, bd[0], bd[1], bd[2], bd[3], ref, d_reads, d_read_off, d_alns, d_cands,
+    const uint64_t threads = 32ull * n_cand;
+    mate_collect_fill_kernel<<<(unsigned)((threads + kMateCollectThreads - 1) / kMateCollectThreads),
+                               kMateCollectThreads, 0, s>>>(opt, bd[0], bd[1], bd[2], bd[3], ref, d_reads, d_read_off, d_alns, d_cands,
                                     n_cand, d_plan, d_jobs, d_info, d_qbuf, d_tbuf);
     return cudaGetLastError();
 }

@@ -7,6 +7,7 @@ Usage: python -m ferrousalign_b200.profile_run [n_jobs] [probe|-] [kernel: 0 aut
        python -m ferrousalign_b200.profile_run regions [n_chains] [reps] (region merge, device-resident)
        python -m ferrousalign_b200.profile_run collect [n_reads] [reps]  (extension jobs from chains)
        python -m ferrousalign_b200.profile_run cigar [n_jobs] [reps]     (CIGAR regeneration)
+       python -m ferrousalign_b200.profile_run rescue [n_pairs] [reps]   (mate-rescue jobs from anchors)
 """
 import ctypes
 import sys
@@ -39,6 +40,23 @@ if len(sys.argv) > 1 and sys.argv[1] == "mate":
             st.synchronize()
             N.check(lib.fa_ctx_sync(ctx.handle))
             print("mate batch ms", e0.elapsed_time(e1))
+    sys.exit(0)
+
+if len(sys.argv) > 1 and sys.argv[1] == "rescue":
+    from ferrousalign_b200 import mate_rescue as R
+    n = int(sys.argv[2]) if len(sys.argv) > 2 else 200_000
+    ref, chr_off, chr_len, reads, off, alns, cands = synth.workload_rescue(n)
+    pac, l_pac = fa.pack_reference(ref)
+    bounds = np.zeros(4, N.INSERT_BOUNDS_DT)
+    bounds[:] = [(0, 0, 1, 0), (200, 600, 0, 0), (0, 0, 1, 0), (0, 0, 1, 0)]
+    ctx = fa.Context(0)
+    lib = N.load()
+    N.check(lib.fa_ctx_set_timing(ctx.handle, 1))
+    k_ms, k_n = ctypes.c_float(), ctypes.c_int()
+    for r in range(int(sys.argv[3]) if len(sys.argv) > 3 else 1):
+        got = R.collect_rescue_jobs(pac, l_pac, chr_off, chr_len, reads, off, alns, cands, bounds, ctx=ctx)
+        N.check(lib.fa_ctx_last_timing(ctx.handle, ctypes.byref(k_ms), ctypes.byref(k_n)))
+        print("rescue collection kernel ms", k_ms.value, "jobs", len(got.jobs))
     sys.exit(0)
 
 if len(sys.argv) > 1 and sys.argv[1] == "cigar":
