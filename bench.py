@@ -553,6 +553,18 @@ def bench_rescue_collect(args, ctx, lib):
             kern.append(k_ms.value)
             wall.append((t1 - t0) * 1e3)
     km = float(np.median(kern))
+    # insert-size statistics of the attempts' pairs (anchor, the read's first alignment)
+    l2 = np.int64(l_pac) * 2
+    def fm(a):   # noqa: E306
+        g = chr_off[a["ref_id"]].astype(np.int64) + a["pos"]
+        return np.where(a["is_rev"] != 0, l2 - 1 - (g + a["ref_len"] - 1), g)
+    pairs = np.stack([fm(cands["anchor"]), fm(alns[cands["aln_first"]])], 1).astype(np.int64)
+    st_ms = []
+    for it in range(args.warmup + 5):
+        stats = R.calculate_insert_size_stats(l_pac, pairs, ctx=ctx)
+        N.check(lib.fa_ctx_last_timing(ctx.handle, ctypes.byref(k_ms), ctypes.byref(k_n)))
+        if it >= args.warmup:
+            st_ms.append(k_ms.value)
     wl = int(got.info["adj_re"].sum() - got.info["adj_rb"].sum())
     algo = (cands.nbytes + alns.nbytes + len(reads) + wl // 4 + got.jobs.nbytes + got.info.nbytes +
             len(got.qbuf) + len(got.tbuf))
@@ -573,7 +585,9 @@ def bench_rescue_collect(args, ctx, lib):
             "roofline": {"bound": "hbm", "achieved": algo / (km * 1e-3) / 1e9, "peak": 6546.6, "unit": "GB/s",
                          "frac": algo / (km * 1e-3) / 1e9 / 6546.6, "algorithmic_bytes": algo,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs"},
-            "bit_exact_sample": bool(same), "sample": f"first {k} attempts against the oracle"}
+            "bit_exact_sample": bool(same), "sample": f"first {k} attempts against the oracle",
+            "insert_size_stats": {"pairs": len(pairs), "kernel_ms": float(np.median(st_ms)),
+                                  "fr": {f: float(stats[1][f]) for f in ("avg", "std", "low", "high", "failed")}}}
 
 
 def run_reference(args):

@@ -58,6 +58,8 @@ CIGAR_RESULT_DT = np.dtype([("score", "<i4"), ("qle", "<i4"), ("tle", "<i4"), ("
                             ("max_off", "<i4"), ("n_cigar", "<i4"), ("n_ref", "<i4"), ("n_query", "<i4"),
                             ("cells", "<i4")])
 INSERT_BOUNDS_DT = np.dtype([("low", "<i4"), ("high", "<i4"), ("failed", "<i4"), ("_pad", "<i4")])
+INSERT_STATS_DT = np.dtype([("avg", "<f8"), ("std", "<f8"), ("low", "<i4"), ("high", "<i4"), ("failed", "<i4"),
+                            ("_pad", "<i4")])
 RESCUE_ALN_DT = np.dtype([("pos", "<i8"), ("ref_id", "<i4"), ("is_rev", "<i4"), ("ref_len", "<i4"), ("score", "<i4")])
 RESCUE_CAND_DT = np.dtype([("read", "<u4"), ("aln_first", "<u4"), ("aln_count", "<u4"), ("primary", "<u4"),
                            ("anchor", RESCUE_ALN_DT)])
@@ -75,6 +77,7 @@ assert COLLECT_COUNTS_DT.itemsize == 32
 assert CIGAR_JOB_DT.itemsize == 32 and CIGAR_RESULT_DT.itemsize == 40
 assert INSERT_BOUNDS_DT.itemsize == 16 and RESCUE_ALN_DT.itemsize == 24 and RESCUE_CAND_DT.itemsize == 40
 assert RESCUE_OPTS_DT.itemsize == 16 and RESCUE_JOB_INFO_DT.itemsize == 32
+assert INSERT_STATS_DT.itemsize == 32
 
 # Every symbol the header declares, with its ctypes signature.
 _P = C.c_void_p
@@ -120,6 +123,7 @@ SIGNATURES = {
     "fa_cigar_batch": (C.c_int, [_P, _P, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64, _P, _P, _P, _P]),
     "fa_collect_mate_jobs": (C.c_int, [_P, _P, _P, _P, C.c_uint64, _P, _P, C.c_uint32, _P, _P, C.c_uint32, _P,
                                        C.c_uint32, _P, C.c_uint32, _P, _P, _P, C.c_uint64, _P, C.c_uint64, _P]),
+    "fa_insert_size_stats": (C.c_int, [_P, C.c_uint64, _P, C.c_uint32, _P]),
     "fa_merge_regions": (C.c_int, [_P, _P, _P, C.c_uint32, _P, _P, C.c_uint32, _P, C.c_uint32, _P, C.c_uint32,
                                    _P]),
     "fa_merge_regions_device": (C.c_int, [_P, _P, _P, C.c_uint32, _P, _P, C.c_uint32, _P, C.c_uint32, _P,

@@ -84,6 +84,7 @@ struct fa_ctx {
     DevBuf col_in, col_plan, col_out;   // job collection: inputs, chain plans + scan sums, outputs
     DevBuf cg_in, cg_scratch, cg_out;   // CIGAR regeneration: inputs, row state + traceback, outputs
     DevBuf mc_in, mc_plan, mc_out;      // mate-rescue jobs: inputs, plans + scan sums, outputs
+    DevBuf is_buf;                      // insert-size statistics: pairs, histogram, results
     DevBuf w_first, w_cur, prev, kk, w_final, tries, missed, list_a, list_b, hist, feat, wbf, part_n, part_w;
     uint32_t last_launches = 0;
     bool timing = false;
@@ -793,7 +794,7 @@ void fa_ctx_destroy(fa_ctx *c) {
                       &c->misc, &c->w_first, &c->w_cur, &c->prev, &c->kk, &c->w_final, &c->tries,
                       &c->missed, &c->list_a, &c->list_b, &c->hist, &c->feat, &c->wbf, &c->part_n,
                       &c->part_w, &c->ovf, &c->reg_in, &c->reg_out, &c->col_in, &c->col_plan, &c->col_out,
-                      &c->cg_in, &c->cg_scratch, &c->cg_out, &c->mc_in, &c->mc_plan, &c->mc_out})
+                      &c->cg_in, &c->cg_scratch, &c->cg_out, &c->mc_in, &c->mc_plan, &c->mc_out, &c->is_buf})
         b->release();
     for (int k = 0; k < 2; ++k) {
         if (c->join_ev[k]) cudaEventDestroy(c->join_ev[k]);
@@ -1515,6 +1516,30 @@ int fa_collect_mate_jobs(fa_ctx *c, const fa_rescue_opts *opt, const fa_insert_b
     }
     if (tot.z) FA_CUDA(cudaMemcpyAsync(qbuf, d_q, tot.z, cudaMemcpyDeviceToHost, s));
     if (tot.x) FA_CUDA(cudaMemcpyAsync(tbuf, d_t, tot.x, cudaMemcpyDeviceToHost, s));
+    FA_CUDA(cudaStreamSynchronize(s));
+    return FA_OK;
+}
+
+int fa_insert_size_stats(fa_ctx *c, uint64_t l_pac, const int64_t *pairs, uint32_t n, fa_insert_stats *out4) {
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    if (!out4 || (n && !pairs)) return fail(FA_ERR_ARG, "null buffer");
+    if (l_pac == 0 || l_pac > (1ull << 62)) return fail(FA_ERR_ARG, "l_pac out of range");
+    FA_CUDA(cudaSetDevice(c->device));
+    cudaStream_t s = c->stream;
+    auto up16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
+    const size_t b_pairs = up16(16ull * n), b_hist = up16(insert_hist_bytes());
+    FA_CUDA(c->is_buf.ensure(b_pairs + b_hist + sizeof(fa_insert_stats) * 4));
+    char *b = c->is_buf.as<char>();
+    int64_t *d_pairs = reinterpret_cast<int64_t *>(b);
+    uint32_t *d_hist = reinterpret_cast<uint32_t *>(b + b_pairs);
+    fa_insert_stats *d_out = reinterpret_cast<fa_insert_stats *>(b + b_pairs + b_hist);
+    if (n) FA_CUDA(cudaMemcpyAsync(d_pairs, pairs, 16ull * n, cudaMemcpyHostToDevice, s));
+    if (c->timing) FA_CUDA(cudaEventRecord(c->kev0, s));
+    FA_CUDA(launch_insert_stats((int64_t)l_pac, d_pairs, n, d_hist, d_out, s));
+    if (c->timing) FA_CUDA(cudaEventRecord(c->kev1, s));
+    c->last_launches = n ? 2 : 1;
+    c->last_stream = s;
+    FA_CUDA(cudaMemcpyAsync(out4, d_out, sizeof(fa_insert_stats) * 4, cudaMemcpyDeviceToHost, s));
     FA_CUDA(cudaStreamSynchronize(s));
     return FA_OK;
 }

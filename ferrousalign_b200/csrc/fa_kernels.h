@@ -166,6 +166,11 @@ cudaError_t launch_mate_collect_fill(const fa_rescue_opts &opt, const fa_insert_
                                      fa_mate_job *d_jobs, fa_rescue_job_info *d_info, uint8_t *d_qbuf,
                                      uint8_t *d_tbuf, cudaStream_t s);
 
+// Insert-size statistics (insert_size_kernel.cu): d_hist holds insert_hist_bytes().
+size_t insert_hist_bytes();
+cudaError_t launch_insert_stats(int64_t l_pac, const int64_t *d_pairs, uint32_t n, uint32_t *d_hist,
+                                fa_insert_stats *d_out, cudaStream_t s);
+
 // CIGAR regeneration (cigar_kernel.cu): per job the offsets of its outputs (cigar words,
 // aligned reference / query bases) and of its scratch (row state in int2 units, traceback
 // in words), and its traceback words per row.

@@ -160,3 +160,22 @@ def collect_rescue_jobs(pac: np.ndarray, l_pac: int, chr_off: np.ndarray, chr_le
     k = int(counts[0]["n_left"])
     return RescueJobs(jobs[:k].copy(), info[:k].copy(), qbuf[:int(counts[0]["qbuf_len"])],
                       tbuf[:int(counts[0]["tbuf_len"])])
+
+
+def calculate_insert_size_stats(l_pac: int, pairs: np.ndarray, ctx: N.Context | None = None) -> np.ndarray:
+    """InsertSizeStats of the four orientations (FF, FR, RF, RR) from pairs of FM-index
+    positions (n x 2 int64: read 1, read 2), on the GPU (insert_size.rs:73-243)."""
+    lib = N.load()
+    ctx = ctx or N.default_context()
+    pairs = np.ascontiguousarray(pairs, np.int64).reshape(-1, 2)
+    out = np.zeros(4, N.INSERT_STATS_DT)
+    N.check(lib.fa_insert_size_stats(ctx.handle, l_pac, N.ptr(pairs) if len(pairs) else None, len(pairs),
+                                     N.ptr(out)))
+    return out
+
+
+def insert_bounds(stats: np.ndarray) -> np.ndarray:
+    """The bounds the rescue-job collection reads, from InsertSizeStats."""
+    b = np.zeros(4, N.INSERT_BOUNDS_DT)
+    b["low"], b["high"], b["failed"] = stats["low"], stats["high"], stats["failed"]
+    return b

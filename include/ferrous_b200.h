@@ -404,6 +404,21 @@ int fa_mate_sw_batch(fa_ctx *ctx, const fa_mate_params *p, const fa_mate_job *jo
  * the window, read from the 2-bit packed reference. */
 typedef struct { int32_t low, high, failed, _pad; } fa_insert_bounds;   /* InsertSizeStats per orientation */
 
+/* InsertSizeStats (insert_size.rs:23-29). */
+typedef struct {
+    double  avg, std;
+    int32_t low, high;   /* proper-pair bounds */
+    int32_t failed;
+    int32_t _pad;
+} fa_insert_stats;
+
+/* Replaces calculate_insert_size_stats (insert_size.rs:73-243): the four orientations'
+ * statistics (FF, FR, RF, RR) of n pairs given as FM-index positions (pairs[2k] = read 1,
+ * pairs[2k+1] = read 2, as the reference's (pos1, pos2)), bit-identical to the reference's
+ * double arithmetic.  out4[r].low / high / failed are the fa_insert_bounds of the job
+ * collection below. */
+int fa_insert_size_stats(fa_ctx *ctx, uint64_t l_pac, const int64_t *pairs, uint32_t n, fa_insert_stats *out4);
+
 typedef struct {                /* one alignment of a read (SoAAlignmentResult entry) */
     int64_t pos;                /* 0-based position on its chromosome */
     int32_t ref_id;
