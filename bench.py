@@ -43,7 +43,7 @@ MATE_JOBS = 500_000
 # ext_packed_kernel (int32, 439,186 jobs): 248.1 MB + 11.2 MB;
 # ext_rows2_kernel (two rows per thread, 175,709 jobs): 72.3 MB + 2.5 MB
 EXT_KERNELS = {"int32": ("ext_packed_kernel", (248.106e6 + 11.161e6) / 439_186, "int32"),
-               "rows2": ("ext_rows2_kernel", (72.319e6 + 2.543e6) / 175_709, "int16x2"),
+               "rows2": ("ext_rows2_persist_kernel", (72.319e6 + 2.543e6) / 175_709, "int16x2"),
                "int16x2": ("ext_pair_kernel", None, "int16x2")}
 UNEVEN_JOBS = 2_000_000
 MATE_CPU_SAMPLE = 20_000

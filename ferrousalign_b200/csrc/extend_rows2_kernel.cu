@@ -529,6 +529,50 @@ ext_rows2_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ o
     }
 }
 
+// Persistent form of the plain kernel: as many blocks as stay resident, each warp taking
+// the next 32 jobs of the (longest-first) order from a device counter until none are left,
+// so the batch runs as one launch without a tail of partly filled last waves and SMs that
+// finish their share early take over the rest.  The claim is warp-uniform (lane 0 takes it,
+// a shuffle hands it round), so the warp's lanes stay together between jobs.
+template <int TPB, bool SYM>
+__global__ void __launch_bounds__(TPB, 1)
+ext_rows2_persist_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ order, uint32_t n,
+                         const uint32_t *__restrict__ n_dev, uint32_t *__restrict__ work,
+                         const uint8_t *__restrict__ qseq, const uint8_t *__restrict__ tseq, const ExtParams p,
+                         int qcap, const int32_t *__restrict__ w_try, fa_ext_result *__restrict__ out,
+                         uint8_t *__restrict__ clamped_out, uint32_t *__restrict__ cells_job,
+                         unsigned long long *__restrict__ cells_out, uint32_t *__restrict__ status,
+                         uint32_t *__restrict__ ovf, uint32_t *__restrict__ ovf_n)
+{
+    extern __shared__ uint32_t smem[];
+    if (n_dev) n = min(n, *n_dev);
+    const int t = threadIdx.x, lane = t & 31;
+    const int words = qcap + 1;
+    static_assert(TPB == 64 || TPB == 128, "the slot maps cover 64 or 128 threads per block");
+    const int e_off = 2 * (((t >> 6) << 5) + (t & 31)) + ((t >> 5) & 1);
+    const int s_off = TPB >= 128 ? 4 * (((t >> 7) << 5) + (t & 31)) + ((t >> 5) & 3)
+                                 : 4 * ((t & 31) >> 1) + 2 * (t & 1) + ((t >> 5) & 1);
+    uint16_t *eh = reinterpret_cast<uint16_t *>(smem) + e_off;
+    uint8_t *sb = reinterpret_cast<uint8_t *>(smem) + (size_t)words * TPB * 2 + s_off;
+    uint32_t cells = 0;
+    for (;;) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(work, 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n) break;
+        const uint32_t gi = base + lane;
+        if (gi < n)
+            cells += rows2_thread<TPB, SYM, false, 0>(order ? order[gi] : gi, eh, sb, jobs, qseq, tseq, p, qcap,
+                                                      w_try, out, clamped_out, cells_job, status, ovf, ovf_n);
+    }
+    if (cells_out) {
+        unsigned long long c = cells;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+        if (lane == 0 && c) atomicAdd(cells_out, c);
+    }
+}
+
 bool ext_rows2_sym(const ExtParams &p) {
     return p.o_del + p.e_del == p.o_ins + p.e_ins && p.e_del == p.e_ins;
 }
@@ -567,7 +611,8 @@ cudaError_t launch_ext_rows2(const fa_job *d_jobs, const uint32_t *d_order, uint
                              const uint32_t *d_n, const uint8_t *d_qseq, const uint8_t *d_tseq, const ExtParams &p,
                              int qcap, int ring, bool cert, const int32_t *d_w_try, fa_ext_result *d_out,
                              uint8_t *d_clamped, uint32_t *d_cells_job, unsigned long long *d_cells,
-                             uint32_t *d_status, uint32_t *d_ovf, uint32_t *d_ovf_n, cudaStream_t stream, int tpb)
+                             uint32_t *d_status, uint32_t *d_ovf, uint32_t *d_ovf_n, cudaStream_t stream, int tpb,
+                             uint32_t *d_work)
 {
     if (n == 0) return cudaSuccess;
     if (!ext_rows2_eligible(p, qcap) || !d_ovf || !d_ovf_n) return cudaErrorInvalidValue;
@@ -591,6 +636,26 @@ cudaError_t launch_ext_rows2(const fa_job *d_jobs, const uint32_t *d_order, uint
         err = sym ? FA_ROWS2(64, true, false, 32) : FA_ROWS2(64, false, false, 32);
     } else if (ring == 64) {
         err = sym ? FA_ROWS2(64, true, false, 64) : FA_ROWS2(64, false, false, 64);
+    } else if (d_work && !d_first) {
+        // persistent: one block per resident slot, warps claiming jobs from d_work
+        err = cudaMemsetAsync(d_work, 0, sizeof(uint32_t), stream);
+        auto go = [&](auto kernel, int tv) -> cudaError_t {
+            cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            int per_sm = 0, dev = 0, sms = 0;
+            if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, tv, smem)) != cudaSuccess) return e;
+            if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+            if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+            const uint32_t want = (n + tv - 1) / tv, cap = (uint32_t)(per_sm > 0 ? per_sm : 1) * (uint32_t)sms;
+            kernel<<<want < cap ? want : cap, tv, smem, stream>>>(d_jobs, d_order, n, d_n, d_work, d_qseq, d_tseq, p,
+                                                                qcap, d_w_try, d_out, d_clamped, d_cells_job, d_cells,
+                                                                d_status, d_ovf, d_ovf_n);
+            return cudaGetLastError();
+        };
+        if (err == cudaSuccess) {
+            if (t == 128) err = sym ? go(ext_rows2_persist_kernel<128, true>, 128) : go(ext_rows2_persist_kernel<128, false>, 128);
+            else err = sym ? go(ext_rows2_persist_kernel<64, true>, 64) : go(ext_rows2_persist_kernel<64, false>, 64);
+        }
     } else if (t == 128) {
         err = sym ? FA_ROWS2(128, true, false, 0) : FA_ROWS2(128, false, false, 0);
     } else {

@@ -117,7 +117,8 @@ int fa::fa_ctx_device(const fa_ctx *c) { return c->device; }
 namespace {
 
 // misc buffer layout (bytes): [0] status u32, [8] cells u64, [16] count A, [20] count B,
-// [24..35] two-row kernel overflow counts (one per concurrent band group), [64] band-bucket
+// [24..35] two-row kernel overflow counts (one per concurrent band group), [40..51] persistent
+// two-row launches' job counters (one per overflow slot), [64] band-bucket
 // histogram u32[kBandBuckets],
 // [128] band-bucket cursors u32[kBandBuckets], [192] band-group bounds u32[3]
 constexpr size_t kMiscBytes = 256;
@@ -125,11 +126,13 @@ struct Misc {
     uint32_t *status;
     unsigned long long *cells;
     uint32_t *cnt_a, *cnt_b, *ovf_n, *bucket_hist, *bucket_cursor, *group_bounds;
+    uint32_t *work;   // persistent two-row launches' job counters, one per overflow slot
 };
 Misc misc_of(fa_ctx *c) {
     char *b = c->misc.as<char>();
     return Misc{(uint32_t *)b, (unsigned long long *)(b + 8), (uint32_t *)(b + 16), (uint32_t *)(b + 20),
-                (uint32_t *)(b + 24), (uint32_t *)(b + 64), (uint32_t *)(b + 128), (uint32_t *)(b + 192)};
+                (uint32_t *)(b + 24), (uint32_t *)(b + 64), (uint32_t *)(b + 128), (uint32_t *)(b + 192),
+                (uint32_t *)(b + 40)};
 }
 
 int ensure_aux_streams(fa_ctx *c) {
@@ -161,7 +164,7 @@ cudaError_t launch_ext(fa_ctx *c, Choice kc, const fa_job *d_jobs, const uint32_
         ext_rows2_smem_bytes(qcap, kc.tpb, 0) <= c->smem_optin && ovf_words >= (size_t)n && c->misc.p)
         return launch_ext_rows2(d_jobs, d_order, n, nullptr, d_n, d_q, d_t, kp, qcap, 0, false, d_w_try, d_out,
                                 d_clamped, d_cells_job, d_cells, d_status, c->ovf.as<uint32_t>() + slot * ovf_words,
-                                misc_of(c).ovf_n + slot, s, kc.tpb);
+                                misc_of(c).ovf_n + slot, s, kc.tpb, misc_of(c).work + slot);
     if (kc.kernel == FA_KERNEL_INT16X2 && ext_pair_eligible(kp) && !cert)
         return launch_ext_pair(d_jobs, d_order, n, d_n, d_q, d_t, kp, qcap, d_w_try, d_out, d_clamped,
                                d_cells_job, d_cells, d_status, s);

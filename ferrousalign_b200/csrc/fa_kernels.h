@@ -42,13 +42,16 @@ cudaError_t launch_ext_pair(const fa_job *d_jobs, const uint32_t *d_order, uint3
 // 32/64 keeps only that many column words (bands with 2w + 3 <= ring); cert evaluates the
 // exit-bound certificate and hint into d_clamped.
 // d_first (optional): device-side first index into d_order, as for launch_ext_packed.
+// d_work (optional, plain full-row form without d_first): a device counter that makes the
+// launch persistent, warps claiming 32 jobs at a time until the order is used up.
 bool ext_rows2_eligible(const ExtParams &p, int qcap);
 size_t ext_rows2_smem_bytes(int qcap, int tpb, int ring);
 cudaError_t launch_ext_rows2(const fa_job *d_jobs, const uint32_t *d_order, uint32_t n, const uint32_t *d_first,
                              const uint32_t *d_n, const uint8_t *d_qseq, const uint8_t *d_tseq, const ExtParams &p,
                              int qcap, int ring, bool cert, const int32_t *d_w_try, fa_ext_result *d_out,
                              uint8_t *d_clamped, uint32_t *d_cells_job, unsigned long long *d_cells,
-                             uint32_t *d_status, uint32_t *d_ovf, uint32_t *d_ovf_n, cudaStream_t stream, int tpb);
+                             uint32_t *d_status, uint32_t *d_ovf, uint32_t *d_ovf_n, cudaStream_t stream, int tpb,
+                             uint32_t *d_work = nullptr);
 
 // Band-retry policy step over the jobs of the last extension round (see policy_kernel.cu).
 struct PolicyState {
