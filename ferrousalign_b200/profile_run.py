@@ -1,6 +1,7 @@
 """One device-resident extension batch of the bench workload, for ncu captures.
 
 Usage: python -m ferrousalign_b200.profile_run [n_jobs] [probe|-] [kernel: 0 auto, 1 int32, 2 int16x2, 3 rows2] [reps]
+       [threads per block]
        python -m ferrousalign_b200.profile_run learned [n_jobs] [reps] [kernel]   (learned-band path)
        python -m ferrousalign_b200.profile_run bands [n_jobs]            (single runs at fixed bands)
        python -m ferrousalign_b200.profile_run mate [n_jobs] [reps]      (mate-rescue SW, device-resident)
@@ -145,6 +146,8 @@ ctx = fa.Context(0)
 lib = N.load()
 if len(sys.argv) > 3:
     ctx.set_kernel(int(sys.argv[3]))
+if len(sys.argv) > 5:
+    ctx.set_threads(int(sys.argv[5]))
 reps = int(sys.argv[4]) if len(sys.argv) > 4 else 1
 dev = torch.device("cuda", 0)
 st = torch.cuda.Stream(dev)
