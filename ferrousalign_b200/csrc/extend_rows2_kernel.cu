@@ -534,20 +534,23 @@ ext_rows2_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ o
 // so the batch runs as one launch without a tail of partly filled last waves and SMs that
 // finish their share early take over the rest.  The claim is warp-uniform (lane 0 takes it,
 // a shuffle hands it round), so the warp's lanes stay together between jobs.
-template <int TPB, bool SYM>
+template <int TPB, bool SYM, bool CERT, int RING>
 __global__ void __launch_bounds__(TPB, 1)
 ext_rows2_persist_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ order, uint32_t n,
-                         const uint32_t *__restrict__ n_dev, uint32_t *__restrict__ work,
-                         const uint8_t *__restrict__ qseq, const uint8_t *__restrict__ tseq, const ExtParams p,
-                         int qcap, const int32_t *__restrict__ w_try, fa_ext_result *__restrict__ out,
+                         const uint32_t *__restrict__ first_dev, const uint32_t *__restrict__ n_dev,
+                         uint32_t *__restrict__ work, const uint8_t *__restrict__ qseq,
+                         const uint8_t *__restrict__ tseq, const ExtParams p, int qcap,
+                         const int32_t *__restrict__ w_try, fa_ext_result *__restrict__ out,
                          uint8_t *__restrict__ clamped_out, uint32_t *__restrict__ cells_job,
                          unsigned long long *__restrict__ cells_out, uint32_t *__restrict__ status,
                          uint32_t *__restrict__ ovf, uint32_t *__restrict__ ovf_n)
 {
     extern __shared__ uint32_t smem[];
+    const uint32_t first = first_dev ? *first_dev : 0u;   // device-side sub-range of the order
     if (n_dev) n = min(n, *n_dev);
+    const uint32_t count = n > first ? n - first : 0u;
     const int t = threadIdx.x, lane = t & 31;
-    const int words = qcap + 1;
+    const int words = RING > 0 ? RING : qcap + 1;
     static_assert(TPB == 64 || TPB == 128, "the slot maps cover 64 or 128 threads per block");
     const int e_off = 2 * (((t >> 6) << 5) + (t & 31)) + ((t >> 5) & 1);
     const int s_off = TPB >= 128 ? 4 * (((t >> 7) << 5) + (t & 31)) + ((t >> 5) & 3)
@@ -559,11 +562,13 @@ ext_rows2_persist_kernel(const fa_job *__restrict__ jobs, const uint32_t *__rest
         uint32_t base = 0;
         if (lane == 0) base = atomicAdd(work, 32u);
         base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= n) break;
-        const uint32_t gi = base + lane;
-        if (gi < n)
-            cells += rows2_thread<TPB, SYM, false, 0>(order ? order[gi] : gi, eh, sb, jobs, qseq, tseq, p, qcap,
-                                                      w_try, out, clamped_out, cells_job, status, ovf, ovf_n);
+        if (base >= count) break;
+        const uint32_t k = base + lane;
+        if (k < count) {
+            const uint32_t gi = first + k;
+            cells += rows2_thread<TPB, SYM, CERT, RING>(order ? order[gi] : gi, eh, sb, jobs, qseq, tseq, p, qcap,
+                                                        w_try, out, clamped_out, cells_job, status, ovf, ovf_n);
+        }
     }
     if (cells_out) {
         unsigned long long c = cells;
@@ -628,7 +633,38 @@ cudaError_t launch_ext_rows2(const fa_job *d_jobs, const uint32_t *d_order, uint
                                                                       d_qseq, d_tseq, p, qcap, d_w_try, d_out,    \
                                                                       d_clamped, d_cells_job, d_cells, d_status,  \
                                                                       d_ovf, d_ovf_n)
-    if (c) {
+    // persistent: one block per resident slot, warps claiming jobs from d_work
+    auto go = [&](auto kernel, int tv) -> cudaError_t {
+        cudaError_t e = cudaMemsetAsync(d_work, 0, sizeof(uint32_t), stream);
+        if (e != cudaSuccess) return e;
+        if ((e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
+            return e;
+        int per_sm = 0, dev = 0, sms = 0;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, tv, smem)) != cudaSuccess) return e;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+        if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+        const uint32_t want = (n + tv - 1) / tv, cap = (uint32_t)(per_sm > 0 ? per_sm : 1) * (uint32_t)sms;
+        kernel<<<want < cap ? want : cap, tv, smem, stream>>>(d_jobs, d_order, n, d_first, d_n, d_work, d_qseq,
+                                                            d_tseq, p, qcap, d_w_try, d_out, d_clamped, d_cells_job,
+                                                            d_cells, d_status, d_ovf, d_ovf_n);
+        return cudaGetLastError();
+    };
+#define FA_PERSIST(TV, SV, CV, RV) go(ext_rows2_persist_kernel<TV, SV, CV, RV>, TV)
+    if (d_work) {
+        if (c) {
+            if (ring == 32) err = sym ? FA_PERSIST(64, true, true, 32) : FA_PERSIST(64, false, true, 32);
+            else if (ring == 64) err = sym ? FA_PERSIST(64, true, true, 64) : FA_PERSIST(64, false, true, 64);
+            else err = sym ? FA_PERSIST(64, true, true, 0) : FA_PERSIST(64, false, true, 0);
+        } else if (ring == 32) {
+            err = sym ? FA_PERSIST(64, true, false, 32) : FA_PERSIST(64, false, false, 32);
+        } else if (ring == 64) {
+            err = sym ? FA_PERSIST(64, true, false, 64) : FA_PERSIST(64, false, false, 64);
+        } else if (t == 128) {
+            err = sym ? FA_PERSIST(128, true, false, 0) : FA_PERSIST(128, false, false, 0);
+        } else {
+            err = sym ? FA_PERSIST(64, true, false, 0) : FA_PERSIST(64, false, false, 0);
+        }
+    } else if (c) {
         if (ring == 32) err = sym ? FA_ROWS2(64, true, true, 32) : FA_ROWS2(64, false, true, 32);
         else if (ring == 64) err = sym ? FA_ROWS2(64, true, true, 64) : FA_ROWS2(64, false, true, 64);
         else err = sym ? FA_ROWS2(64, true, true, 0) : FA_ROWS2(64, false, true, 0);
@@ -636,32 +672,13 @@ cudaError_t launch_ext_rows2(const fa_job *d_jobs, const uint32_t *d_order, uint
         err = sym ? FA_ROWS2(64, true, false, 32) : FA_ROWS2(64, false, false, 32);
     } else if (ring == 64) {
         err = sym ? FA_ROWS2(64, true, false, 64) : FA_ROWS2(64, false, false, 64);
-    } else if (d_work && !d_first) {
-        // persistent: one block per resident slot, warps claiming jobs from d_work
-        err = cudaMemsetAsync(d_work, 0, sizeof(uint32_t), stream);
-        auto go = [&](auto kernel, int tv) -> cudaError_t {
-            cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) return e;
-            int per_sm = 0, dev = 0, sms = 0;
-            if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, tv, smem)) != cudaSuccess) return e;
-            if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
-            if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-            const uint32_t want = (n + tv - 1) / tv, cap = (uint32_t)(per_sm > 0 ? per_sm : 1) * (uint32_t)sms;
-            kernel<<<want < cap ? want : cap, tv, smem, stream>>>(d_jobs, d_order, n, d_n, d_work, d_qseq, d_tseq, p,
-                                                                qcap, d_w_try, d_out, d_clamped, d_cells_job, d_cells,
-                                                                d_status, d_ovf, d_ovf_n);
-            return cudaGetLastError();
-        };
-        if (err == cudaSuccess) {
-            if (t == 128) err = sym ? go(ext_rows2_persist_kernel<128, true>, 128) : go(ext_rows2_persist_kernel<128, false>, 128);
-            else err = sym ? go(ext_rows2_persist_kernel<64, true>, 64) : go(ext_rows2_persist_kernel<64, false>, 64);
-        }
     } else if (t == 128) {
         err = sym ? FA_ROWS2(128, true, false, 0) : FA_ROWS2(128, false, false, 0);
     } else {
         err = sym ? FA_ROWS2(64, true, false, 0) : FA_ROWS2(64, false, false, 0);
     }
 #undef FA_ROWS2
+#undef FA_PERSIST
     if (err != cudaSuccess) return err;
     // jobs whose scores can pass 255: the int32 kernel over the overflow list, same settings
     return launch_ext_packed(d_jobs, d_ovf, n, nullptr, d_ovf_n, d_qseq, d_tseq, p, qcap, ring, d_w_try, d_out,

@@ -42,8 +42,8 @@ cudaError_t launch_ext_pair(const fa_job *d_jobs, const uint32_t *d_order, uint3
 // 32/64 keeps only that many column words (bands with 2w + 3 <= ring); cert evaluates the
 // exit-bound certificate and hint into d_clamped.
 // d_first (optional): device-side first index into d_order, as for launch_ext_packed.
-// d_work (optional, plain full-row form without d_first): a device counter that makes the
-// launch persistent, warps claiming 32 jobs at a time until the order is used up.
+// d_work (optional): a device counter that makes the launch persistent, warps claiming 32
+// jobs at a time until the order (from d_first on) is used up.
 bool ext_rows2_eligible(const ExtParams &p, int qcap);
 size_t ext_rows2_smem_bytes(int qcap, int tpb, int ring);
 cudaError_t launch_ext_rows2(const fa_job *d_jobs, const uint32_t *d_order, uint32_t n, const uint32_t *d_first,
