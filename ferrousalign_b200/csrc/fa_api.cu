@@ -183,7 +183,7 @@ uint32_t ext_kernels_of(fa_ctx *c, Choice kc, const ExtParams &kp, int qcap) {
 // is seen, every exact candidate -- the int32 one-job-per-thread kernel with 64, 128 or
 // 256 threads per block, and where the scoring allows them the two-rows-per-thread
 // kernel with 64 or 128 and the two-jobs-per-thread kernel -- runs twice on the first
-// (longest) jobs of the call's order, and the fastest is kept for that pair.  All
+// (longest) 393,216 jobs of the call's order, and the fastest is kept for that pair.  All
 // candidates give identical results.
 Choice resolve_choice(fa_ctx *c, const ExtParams &kp, const fa_job *d_jobs, const uint32_t *d_order, uint32_t n,
                       const uint8_t *d_q, const uint8_t *d_t, int qcap, int band, fa_ext_result *d_out,
@@ -201,7 +201,9 @@ Choice resolve_choice(fa_ctx *c, const ExtParams &kp, const fa_job *d_jobs, cons
         cands.push_back({FA_KERNEL_ROWS2, 128});
     }
     if (ext_pair_eligible(kp)) cands.push_back({FA_KERNEL_INT16X2, kPairThreads});
-    const uint32_t ns = std::min<uint32_t>(n, 131072);
+    // a sample of several claim rounds of the persistent launch (about 2,700 resident warps of
+    // 32 jobs), so the partly used last round does not decide between 64 and 128 threads
+    const uint32_t ns = std::min<uint32_t>(n, 393216);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     Choice best{FA_KERNEL_INT32, kExtThreads};
     float best_ms = 1e30f;
