@@ -121,6 +121,8 @@ SIGNATURES = {
     "fa_collect_ext_jobs": (C.c_int, [_P, _P, _P, C.c_uint64, _P, _P, C.c_uint32, _P, C.c_uint32, _P, C.c_uint32,
                                       _P, _P, _P, _P, C.c_uint64, _P, _P, _P, _P]),
     "fa_cigar_batch": (C.c_int, [_P, _P, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64, _P, _P, _P, _P]),
+    "fa_cigar_batch_packed": (C.c_int, [_P, _P, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64, _P, _P, C.c_uint64,
+                                        _P, _P, _P]),
     "fa_collect_mate_jobs": (C.c_int, [_P, _P, _P, _P, C.c_uint64, _P, _P, C.c_uint32, _P, _P, C.c_uint32, _P,
                                        C.c_uint32, _P, C.c_uint32, _P, _P, _P, C.c_uint64, _P, C.c_uint64, _P]),
     "fa_insert_size_stats": (C.c_int, [_P, C.c_uint64, _P, C.c_uint32, _P]),

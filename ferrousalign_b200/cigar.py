@@ -59,8 +59,10 @@ class CigarBatch:
 
 
 def scalar_banded_swa_batch(params: np.ndarray, jobs: np.ndarray, qseq: np.ndarray, tseq: np.ndarray,
-                            ctx: N.Context | None = None) -> CigarBatch:
-    """scalar_banded_swa for every job (CIGAR_JOB_DT: offsets, lengths, band, h0)."""
+                            ctx: N.Context | None = None, packed: bool = True) -> CigarBatch:
+    """scalar_banded_swa for every job (CIGAR_JOB_DT: offsets, lengths, band, h0).  packed:
+    the CIGAR words come back back to back (fa_cigar_batch_packed), otherwise in slots of
+    qlen + tlen + 2 words per job (fa_cigar_batch)."""
     lib = N.load()
     ctx = ctx or N.default_context()
     jobs = np.ascontiguousarray(jobs, CIGAR_JOB_DT)
@@ -73,9 +75,19 @@ def scalar_banded_swa_batch(params: np.ndarray, jobs: np.ndarray, qseq: np.ndarr
     ref_off = np.concatenate([[0], np.cumsum(t)])
     qry_off = np.concatenate([[0], np.cumsum(q)])
     res = np.zeros(n, CIGAR_RESULT_DT)
+    ra = np.empty(max(int(ref_off[-1]), 1), np.uint8)
+    qa = np.empty(max(int(qry_off[-1]), 1), np.uint8)
+    if packed:
+        # capacity for every slot, of which only the used words' pages are ever touched
+        cig = np.empty(max(int(cig_off[-1]), 1), np.uint32)
+        first = np.zeros(max(n, 1), np.uint64)
+        if n:
+            N.check(lib.fa_cigar_batch_packed(ctx.handle, N.ptr(params), N.ptr(jobs), n, N.ptr(qseq), len(qseq),
+                                              N.ptr(tseq), len(tseq), N.ptr(res), N.ptr(cig), len(cig),
+                                              N.ptr(first), N.ptr(ra), N.ptr(qa)))
+        total = int(res["n_cigar"].sum()) if n else 0
+        return CigarBatch(res, cig[:total], ra, qa, first[:n], ref_off[:-1], qry_off[:-1])
     cig = np.zeros(max(int(cig_off[-1]), 1), np.uint32)
-    ra = np.zeros(max(int(ref_off[-1]), 1), np.uint8)
-    qa = np.zeros(max(int(qry_off[-1]), 1), np.uint8)
     if n:
         N.check(lib.fa_cigar_batch(ctx.handle, N.ptr(params), N.ptr(jobs), n, N.ptr(qseq), len(qseq), N.ptr(tseq),
                                    len(tseq), N.ptr(res), N.ptr(cig), N.ptr(ra), N.ptr(qa)))

@@ -246,6 +246,21 @@ cigar_kernel(const fa_cigar_job *__restrict__ jobs, const CigarPlan *__restrict_
     out[k] = r;
 }
 
+// Packs the jobs' CIGAR words back to back: job k's n_cigar words from its capacity slot
+// to first[k] (one warp per job; a job has a handful of operations).
+__global__ void __launch_bounds__(256)
+cigar_pack_kernel(const CigarPlan *__restrict__ plan, const fa_cigar_result *__restrict__ res,
+                  const uint64_t *__restrict__ first, uint32_t n, const uint32_t *__restrict__ cigar,
+                  uint32_t *__restrict__ packed)
+{
+    const uint32_t k = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (k >= n) return;
+    const uint32_t *src = cigar + plan[k].cig;
+    uint32_t *dst = packed + first[k];
+    const int m = res[k].n_cigar;
+    for (int i = threadIdx.x & 31; i < m; i += 32) dst[i] = src[i];
+}
+
 }  // namespace
 
 int cigar_band_words(int qlen, int w) {
@@ -261,6 +276,14 @@ cudaError_t launch_cigar(const fa_cigar_job *d_jobs, const CigarPlan *d_plan, ui
     if (n == 0) return cudaSuccess;
     cigar_kernel<<<(n + kCigarThreads - 1) / kCigarThreads, kCigarThreads, 0, s>>>(
         d_jobs, d_plan, n, d_qseq, d_tseq, p, pen_clip3, d_eh, d_tb, d_out, d_cigar, d_ref_al, d_qry_al);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cigar_pack(const CigarPlan *d_plan, const fa_cigar_result *d_res, const uint64_t *d_first,
+                              uint32_t n, const uint32_t *d_cigar, uint32_t *d_packed, cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    cigar_pack_kernel<<<(n + 7) / 8, 256, 0, s>>>(d_plan, d_res, d_first, n, d_cigar, d_packed);
     return cudaGetLastError();
 }
 

@@ -1366,13 +1366,21 @@ int fa_collect_ext_jobs(fa_ctx *c, const fa_collect_opts *opt, const uint8_t *pa
     return FA_OK;
 }
 
-int fa_cigar_batch(fa_ctx *c, const fa_params *p, const fa_cigar_job *jobs, uint32_t n, const uint8_t *qseq,
-                   uint64_t qseq_len, const uint8_t *tseq, uint64_t tseq_len, fa_cigar_result *out, uint32_t *cigar,
-                   uint8_t *ref_aligned, uint8_t *query_aligned) {
-    if (!c) return fail(FA_ERR_ARG, "null context");
-    if (int rc = check_params(p)) return rc;
-    if (n == 0) return FA_OK;
-    if (!jobs || !out || !cigar || !ref_aligned || !query_aligned) return fail(FA_ERR_ARG, "null buffer");
+namespace {
+
+// Device side of one CIGAR batch: the outputs in their capacity slots.
+struct CigarRun {
+    CigarPlan *plan = nullptr;
+    fa_cigar_result *out = nullptr;
+    uint32_t *cig = nullptr;
+    uint8_t *ref = nullptr, *qry = nullptr;
+    uint64_t n_cig = 0, n_ref = 0, n_qry = 0;
+};
+
+// Validates the jobs, uploads them with the sequences and launches the kernel on the
+// context's stream.
+int cigar_launch(fa_ctx *c, const fa_params *p, const fa_cigar_job *jobs, uint32_t n, const uint8_t *qseq,
+                 uint64_t qseq_len, const uint8_t *tseq, uint64_t tseq_len, CigarRun *r) {
     // output and scratch offsets per job (the reference would panic on a range past its slices)
     std::vector<CigarPlan> plan(n);
     uint64_t cig = 0, ref = 0, qry = 0, eh = 0, tb = 0;
@@ -1411,10 +1419,14 @@ int fa_cigar_batch(fa_ctx *c, const fa_params *p, const fa_cigar_job *jobs, uint
     const size_t b_ref = up16(ref + 1), b_qry = up16(qry + 1);
     FA_CUDA(c->cg_out.ensure(b_out + b_cig + b_ref + b_qry));
     char *o = c->cg_out.as<char>();
-    fa_cigar_result *d_out = reinterpret_cast<fa_cigar_result *>(o);
-    uint32_t *d_cig = reinterpret_cast<uint32_t *>(o + b_out);
-    uint8_t *d_ref = reinterpret_cast<uint8_t *>(o + b_out + b_cig);
-    uint8_t *d_qry = reinterpret_cast<uint8_t *>(o + b_out + b_cig + b_ref);
+    r->plan = d_plan;
+    r->out = reinterpret_cast<fa_cigar_result *>(o);
+    r->cig = reinterpret_cast<uint32_t *>(o + b_out);
+    r->ref = reinterpret_cast<uint8_t *>(o + b_out + b_cig);
+    r->qry = reinterpret_cast<uint8_t *>(o + b_out + b_cig + b_ref);
+    r->n_cig = cig;
+    r->n_ref = ref;
+    r->n_qry = qry;
     FA_CUDA(cudaMemcpyAsync(d_jobs, jobs, sizeof(fa_cigar_job) * n, cudaMemcpyHostToDevice, s));
     FA_CUDA(cudaMemcpyAsync(d_plan, plan.data(), sizeof(CigarPlan) * n, cudaMemcpyHostToDevice, s));
     if (qseq_len) FA_CUDA(cudaMemcpyAsync(d_q, qseq, qseq_len, cudaMemcpyHostToDevice, s));
@@ -1422,14 +1434,68 @@ int fa_cigar_batch(fa_ctx *c, const fa_params *p, const fa_cigar_job *jobs, uint
     if (tb) FA_CUDA(cudaMemsetAsync(d_tb, 0, 4 * tb, s));   // unwritten cells read as M, as the reference's
     const ExtParams kp = ext_params_of(p);
     if (c->timing) FA_CUDA(cudaEventRecord(c->kev0, s));
-    FA_CUDA(launch_cigar(d_jobs, d_plan, n, d_q, d_t, kp, p->pen_clip3, d_eh, d_tb, d_out, d_cig, d_ref, d_qry, s));
+    FA_CUDA(launch_cigar(d_jobs, d_plan, n, d_q, d_t, kp, p->pen_clip3, d_eh, d_tb, r->out, r->cig, r->ref, r->qry,
+                         s));
     if (c->timing) FA_CUDA(cudaEventRecord(c->kev1, s));
     c->last_launches = 1;
     c->last_stream = s;
-    FA_CUDA(cudaMemcpyAsync(out, d_out, sizeof(fa_cigar_result) * n, cudaMemcpyDeviceToHost, s));
-    FA_CUDA(cudaMemcpyAsync(cigar, d_cig, 4 * cig, cudaMemcpyDeviceToHost, s));
-    if (ref) FA_CUDA(cudaMemcpyAsync(ref_aligned, d_ref, ref, cudaMemcpyDeviceToHost, s));
-    if (qry) FA_CUDA(cudaMemcpyAsync(query_aligned, d_qry, qry, cudaMemcpyDeviceToHost, s));
+    return FA_OK;
+}
+
+}  // namespace
+
+int fa_cigar_batch(fa_ctx *c, const fa_params *p, const fa_cigar_job *jobs, uint32_t n, const uint8_t *qseq,
+                   uint64_t qseq_len, const uint8_t *tseq, uint64_t tseq_len, fa_cigar_result *out, uint32_t *cigar,
+                   uint8_t *ref_aligned, uint8_t *query_aligned) {
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    if (int rc = check_params(p)) return rc;
+    if (n == 0) return FA_OK;
+    if (!jobs || !out || !cigar || !ref_aligned || !query_aligned) return fail(FA_ERR_ARG, "null buffer");
+    CigarRun r;
+    if (int rc = cigar_launch(c, p, jobs, n, qseq, qseq_len, tseq, tseq_len, &r)) return rc;
+    cudaStream_t s = c->stream;
+    FA_CUDA(cudaMemcpyAsync(out, r.out, sizeof(fa_cigar_result) * n, cudaMemcpyDeviceToHost, s));
+    FA_CUDA(cudaMemcpyAsync(cigar, r.cig, 4 * r.n_cig, cudaMemcpyDeviceToHost, s));
+    if (r.n_ref) FA_CUDA(cudaMemcpyAsync(ref_aligned, r.ref, r.n_ref, cudaMemcpyDeviceToHost, s));
+    if (r.n_qry) FA_CUDA(cudaMemcpyAsync(query_aligned, r.qry, r.n_qry, cudaMemcpyDeviceToHost, s));
+    FA_CUDA(cudaStreamSynchronize(s));
+    return FA_OK;
+}
+
+int fa_cigar_batch_packed(fa_ctx *c, const fa_params *p, const fa_cigar_job *jobs, uint32_t n, const uint8_t *qseq,
+                          uint64_t qseq_len, const uint8_t *tseq, uint64_t tseq_len, fa_cigar_result *out,
+                          uint32_t *cigar, uint64_t cigar_cap, uint64_t *cigar_first, uint8_t *ref_aligned,
+                          uint8_t *query_aligned) {
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    if (int rc = check_params(p)) return rc;
+    if (n == 0) return FA_OK;
+    if (!jobs || !out || !cigar_first || !ref_aligned || !query_aligned) return fail(FA_ERR_ARG, "null buffer");
+    CigarRun r;
+    if (int rc = cigar_launch(c, p, jobs, n, qseq, qseq_len, tseq, tseq_len, &r)) return rc;
+    cudaStream_t s = c->stream;
+    FA_CUDA(cudaMemcpyAsync(out, r.out, sizeof(fa_cigar_result) * n, cudaMemcpyDeviceToHost, s));
+    if (r.n_ref) FA_CUDA(cudaMemcpyAsync(ref_aligned, r.ref, r.n_ref, cudaMemcpyDeviceToHost, s));
+    if (r.n_qry) FA_CUDA(cudaMemcpyAsync(query_aligned, r.qry, r.n_qry, cudaMemcpyDeviceToHost, s));
+    FA_CUDA(cudaStreamSynchronize(s));
+    uint64_t total = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        cigar_first[k] = total;
+        total += (uint64_t)out[k].n_cigar;
+    }
+    if (total > cigar_cap)
+        return fail(FA_ERR_CAPACITY, "cigar buffer holds %llu words, the batch has %llu", (unsigned long long)cigar_cap,
+                    (unsigned long long)total);
+    if (total == 0) return FA_OK;
+    if (!cigar) return fail(FA_ERR_ARG, "null buffer");
+    // the packed words and their offsets go to the scratch, which the kernel no longer needs
+    const size_t b_first = (sizeof(uint64_t) * n + 15) & ~(size_t)15;
+    FA_CUDA(c->cg_scratch.ensure(b_first + 4 * total));
+    uint64_t *d_first = c->cg_scratch.as<uint64_t>();
+    uint32_t *d_packed = reinterpret_cast<uint32_t *>(c->cg_scratch.as<char>() + b_first);
+    FA_CUDA(cudaMemcpyAsync(d_first, cigar_first, sizeof(uint64_t) * n, cudaMemcpyHostToDevice, s));
+    FA_CUDA(launch_cigar_pack(r.plan, r.out, d_first, n, r.cig, d_packed, s));
+    c->last_launches = 2;
+    FA_CUDA(cudaMemcpyAsync(cigar, d_packed, 4 * total, cudaMemcpyDeviceToHost, s));
     FA_CUDA(cudaStreamSynchronize(s));
     return FA_OK;
 }

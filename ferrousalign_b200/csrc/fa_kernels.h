@@ -186,6 +186,9 @@ cudaError_t launch_cigar(const fa_cigar_job *d_jobs, const CigarPlan *d_plan, ui
                          const uint8_t *d_tseq, const ExtParams &p, int pen_clip3, int2 *d_eh, uint32_t *d_tb,
                          fa_cigar_result *d_out, uint32_t *d_cigar, uint8_t *d_ref_al, uint8_t *d_qry_al,
                          cudaStream_t s);
+// job k's n_cigar words from its slot at plan[k].cig to d_packed[d_first[k]]
+cudaError_t launch_cigar_pack(const CigarPlan *d_plan, const fa_cigar_result *d_res, const uint64_t *d_first,
+                              uint32_t n, const uint32_t *d_cigar, uint32_t *d_packed, cudaStream_t s);
 
 // Integer / DPX instruction throughput (ops per second) for the roofline denominator.
 double probe_int_peak(int kind, int sm_count, cudaStream_t s, float *ms_out);

@@ -385,6 +385,17 @@ int fa_cigar_batch(fa_ctx *ctx, const fa_params *p, const fa_cigar_job *jobs, ui
                    const uint8_t *qseq, uint64_t qseq_len, const uint8_t *tseq, uint64_t tseq_len,
                    fa_cigar_result *out, uint32_t *cigar, uint8_t *ref_aligned, uint8_t *query_aligned);
 
+/* fa_cigar_batch with the CIGAR words packed: job k's n_cigar words start at
+ * cigar[cigar_first[k]], cigar_first[k] being the sum of the earlier jobs' n_cigar (the
+ * reference returns one operation vector per alignment; a batch of 151-bp regions has a few
+ * words per job against the qlen + tlen + 2 capacity slots above).  ref_aligned and
+ * query_aligned keep their slots.  A batch with more than cigar_cap words returns
+ * FA_ERR_CAPACITY with out and cigar_first filled, so the caller can size the buffer. */
+int fa_cigar_batch_packed(fa_ctx *ctx, const fa_params *p, const fa_cigar_job *jobs, uint32_t n,
+                          const uint8_t *qseq, uint64_t qseq_len, const uint8_t *tseq, uint64_t tseq_len,
+                          fa_cigar_result *out, uint32_t *cigar, uint64_t cigar_cap, uint64_t *cigar_first,
+                          uint8_t *ref_aligned, uint8_t *query_aligned);
+
 /* ---- mate rescue -------------------------------------------------------
  * Replaces the ksw_align2 calls of execute_mate_rescue_batch_with_engine
  * (src/pipelines/linear/paired/mate_rescue.rs:595-685). */

@@ -85,3 +85,40 @@ def test_edges_codes_and_empty(built):
         tseq[int(jobs["t_off"][k]):int(jobs["t_off"][k]) + m] = q[:m]
     got = check(fa.BandedPairWiseSW().to_struct(), jobs, qseq, tseq)
     assert (got.results["n_cigar"][:10] == 0).all()
+
+
+def test_packed_and_slotted_layouts_agree(built):
+    """fa_cigar_batch_packed gives the slotted call's words back to back (offsets = running
+    sums of n_cigar); a buffer one word short returns FA_ERR_CAPACITY with the results and
+    offsets filled."""
+    import ctypes
+    import ferrousalign_b200 as fa
+    from ferrousalign_b200 import _native as N, cigar as G, synth
+    rng = np.random.default_rng(5)
+    b = synth.workload_ext_uneven(3000, ref_len=2_000_000)
+    jobs = jobs_from(b, rng, bands=(0, 3, 17, 60))
+    p = fa.BandedPairWiseSW().to_struct()
+    pk = G.scalar_banded_swa_batch(p, jobs, b.qseq, b.tseq, packed=True)
+    sl = G.scalar_banded_swa_batch(p, jobs, b.qseq, b.tseq, packed=False)
+    assert np.array_equal(pk.results, sl.results)
+    n_cig = sl.results["n_cigar"].astype(np.uint64)
+    assert np.array_equal(pk.cigar_off, np.concatenate([[0], np.cumsum(n_cig)[:-1]]).astype(np.uint64))
+    assert len(pk.cigar) == int(n_cig.sum())
+    for k in range(len(jobs)):
+        assert pk.cigar_of(k) == sl.cigar_of(k), k
+        assert np.array_equal(pk.ref_aligned_of(k), sl.ref_aligned_of(k))
+        assert np.array_equal(pk.query_aligned_of(k), sl.query_aligned_of(k))
+    lib = N.load()
+    ctx = N.default_context()
+    n = len(jobs)
+    res = np.zeros(n, G.CIGAR_RESULT_DT)
+    first = np.zeros(n, np.uint64)
+    cap = int(n_cig.sum()) - 1
+    cig = np.zeros(cap, np.uint32)
+    ra = np.zeros(int(jobs["tlen"].sum()) + 1, np.uint8)
+    qa = np.zeros(int(jobs["qlen"].sum()) + 1, np.uint8)
+    rc = lib.fa_cigar_batch_packed(ctx.handle, N.ptr(p), N.ptr(jobs), n, N.ptr(b.qseq), len(b.qseq), N.ptr(b.tseq),
+                                   len(b.tseq), N.ptr(res), N.ptr(cig), ctypes.c_uint64(cap), N.ptr(first),
+                                   N.ptr(ra), N.ptr(qa))
+    assert rc == N.FA_ERR_CAPACITY
+    assert np.array_equal(res, sl.results) and np.array_equal(first, pk.cigar_off)
