@@ -64,10 +64,12 @@ def collect_extension_jobs(pac: np.ndarray, l_pac: int, reads: np.ndarray, read_
     seeds = np.ascontiguousarray(seeds, SEED_DT)
     n_reads, n_chains, n_seeds = len(read_off) - 1, len(chains), len(seeds)
     read_bytes = int(read_off[-1]) if n_reads >= 0 and len(read_off) else 0
-    left = np.zeros(n_seeds, N.JOB_DT)
-    right = np.zeros(n_seeds, N.JOB_DT)
-    qbuf = np.zeros(max(2 * read_bytes, 1), np.uint8)
-    ext = np.zeros(n_seeds, N.SEED_EXT_DT)
+    # outputs the library writes in full up to the returned counts: left uninitialised, so
+    # only the pages the copies reach are ever touched
+    left = np.empty(n_seeds, N.JOB_DT)
+    right = np.empty(n_seeds, N.JOB_DT)
+    qbuf = np.empty(max(2 * read_bytes, 1), np.uint8)
+    ext = np.empty(n_seeds, N.SEED_EXT_DT)
     first = np.zeros(n_chains + 1, np.uint32)
     win = np.zeros((n_chains, 2), np.uint64)
     counts = np.zeros(1, N.COLLECT_COUNTS_DT)
@@ -75,7 +77,7 @@ def collect_extension_jobs(pac: np.ndarray, l_pac: int, reads: np.ndarray, read_
     w = int(opts["w"][0])
     cap = int(2 * (qlen[chains["read"]] + 4 * w + 64).sum()) if n_chains else 0
     for _ in range(2):
-        tbuf = np.zeros(max(cap, 1), np.uint8)
+        tbuf = np.empty(max(cap, 1), np.uint8)
         rc = lib.fa_collect_ext_jobs(ctx.handle, N.ptr(opts), N.ptr(pac), l_pac, N.ptr(reads), N.ptr(read_off),
                                      n_reads, N.ptr(chains), n_chains, N.ptr(seeds), n_seeds, N.ptr(left),
                                      N.ptr(right), N.ptr(qbuf), N.ptr(tbuf), cap, N.ptr(ext), N.ptr(first),
@@ -86,5 +88,5 @@ def collect_extension_jobs(pac: np.ndarray, l_pac: int, reads: np.ndarray, read_
         N.check(rc)
         break
     c = counts[0]
-    return CollectedJobs(left[:c["n_left"]].copy(), right[:c["n_right"]].copy(), qbuf[:c["qbuf_len"]],
-                         tbuf[:c["tbuf_len"]], ext[:c["n_seed_ext"]].copy(), first, win)
+    return CollectedJobs(left[:c["n_left"]], right[:c["n_right"]], qbuf[:c["qbuf_len"]],
+                         tbuf[:c["tbuf_len"]], ext[:c["n_seed_ext"]], first, win)

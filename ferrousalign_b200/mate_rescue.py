@@ -137,16 +137,17 @@ def collect_rescue_jobs(pac: np.ndarray, l_pac: int, chr_off: np.ndarray, chr_le
     cands = np.ascontiguousarray(cands, N.RESCUE_CAND_DT)
     bounds = np.ascontiguousarray(bounds, N.INSERT_BOUNDS_DT)
     n = len(cands)
-    jobs = np.zeros(4 * n, N.MATE_JOB_DT)
-    info = np.zeros(4 * n, N.RESCUE_JOB_INFO_DT)
+    # written in full up to the returned counts; uninitialised, so untouched pages stay unmapped
+    jobs = np.empty(4 * n, N.MATE_JOB_DT)
+    info = np.empty(4 * n, N.RESCUE_JOB_INFO_DT)
     counts = np.zeros(1, N.COLLECT_COUNTS_DT)
     qlen = np.diff(read_off.astype(np.int64))
     qcap = int(4 * qlen[cands["read"]].sum()) if n else 0
     span = int(np.maximum(bounds["high"] - bounds["low"], 0).max()) if len(bounds) else 0
     tcap = int(4 * (qlen[cands["read"]] + span + 1).sum()) if n else 0
     for _ in range(2):
-        qbuf = np.zeros(max(qcap, 1), np.uint8)
-        tbuf = np.zeros(max(tcap, 1), np.uint8)
+        qbuf = np.empty(max(qcap, 1), np.uint8)
+        tbuf = np.empty(max(tcap, 1), np.uint8)
         rc = lib.fa_collect_mate_jobs(ctx.handle, N.ptr(opts), N.ptr(bounds), N.ptr(pac), l_pac, N.ptr(chr_off),
                                       N.ptr(chr_len), len(chr_off), N.ptr(reads), N.ptr(read_off),
                                       len(read_off) - 1, N.ptr(alns), len(alns), N.ptr(cands), n, N.ptr(jobs),
@@ -158,7 +159,7 @@ def collect_rescue_jobs(pac: np.ndarray, l_pac: int, chr_off: np.ndarray, chr_le
         N.check(rc)
         break
     k = int(counts[0]["n_left"])
-    return RescueJobs(jobs[:k].copy(), info[:k].copy(), qbuf[:int(counts[0]["qbuf_len"])],
+    return RescueJobs(jobs[:k], info[:k], qbuf[:int(counts[0]["qbuf_len"])],
                       tbuf[:int(counts[0]["tbuf_len"])])
 
 
