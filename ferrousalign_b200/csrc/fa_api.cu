@@ -94,9 +94,10 @@ struct fa_ctx {
     // learned rounds run their band groups on forked streams: fork on `stream`, join back
     cudaStream_t aux[2] = {nullptr, nullptr};
     cudaEvent_t fork_ev = nullptr, join_ev[2] = {nullptr, nullptr};
-    // pipelined host batches: slice uploads on their own stream, one event per slice
+    // pipelined host batches: slice uploads on their own stream, one event per slice; the
+    // same stream then returns each finished slice's results, after its done event
     cudaStream_t copy_stream = nullptr;
-    cudaEvent_t slice_ev[8] = {};
+    cudaEvent_t slice_ev[8] = {}, done_ev[8] = {};
     DevBuf chunk_scratch;
     // kernel choice: fixed, or (FA_KERNEL_AUTO) tuned per (query capacity class, band)
     struct Choice { int kernel; int tpb; };
@@ -695,6 +696,7 @@ int ext_batch_pipelined(fa_ctx *c, const ExtParams &kp, const fa_job *jobs, uint
     if (!c->copy_stream) {
         FA_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
         for (auto &e : c->slice_ev) FA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        for (auto &e : c->done_ev) FA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
     cudaStream_t s = c->stream, cs = c->copy_stream;
     const uint64_t qs = std::max<uint64_t>(1, (qseq_len + kSlices - 1) / kSlices);
@@ -715,7 +717,9 @@ int ext_batch_pipelined(fa_ctx *c, const ExtParams &kp, const fa_job *jobs, uint
     }
     FA_CUDA(launch_chunk_prep(c->jobs.as<fa_job>(), n, qseq_len, tseq_len, qs, ts, kSlices, kp.max_score,
                               packed_qcap_limit(c->smem_optin), scratch, s));
-    uint32_t h_info[4 + kSlices + 1];
+    // info: status, first bad job, longest query, widest band | slice bounds in the order |
+    // each slice's lowest and highest job index
+    uint32_t h_info[4 + kSlices + 1 + 2 * kSlices];
     FA_CUDA(cudaMemcpyAsync(h_info, info, sizeof(h_info), cudaMemcpyDeviceToHost, s));
     FA_CUDA(cudaStreamSynchronize(s));
     if (h_info[0]) {
@@ -743,6 +747,24 @@ int ext_batch_pipelined(fa_ctx *c, const ExtParams &kp, const fa_job *jobs, uint
     FA_CUDA(cudaEventRecord(c->ev0, s));
     FA_CUDA(cudaEventRecord(c->fork_ev, s));
     FA_CUDA(cudaStreamWaitEvent(sk[1], c->fork_ev, 0));
+    // Results come back slice by slice on the upload stream, behind the uploads, each once
+    // its kernels have run, when every slice's jobs form one index range (sequences laid
+    // out in job order) and `out` is pinned (an asynchronous copy into pageable memory would
+    // hold the host thread): only the last slice's results are left for the end.
+    bool early = false;
+    {
+        cudaPointerAttributes pa;
+        early = cudaPointerGetAttributes(&pa, out) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+        cudaGetLastError();
+        uint32_t covered = 0;
+        for (int k = 0; k < kSlices && early; ++k) {
+            const uint32_t cnt = h_info[4 + k + 1] - h_info[4 + k];
+            const uint32_t lo = h_info[4 + kSlices + 1 + k], hi = h_info[4 + 2 * kSlices + 1 + k];
+            if (cnt && hi - lo + 1 != cnt) early = false;
+            covered += cnt;
+        }
+        early = early && covered == n;
+    }
     for (int k = 0; k < kSlices; ++k) {
         const uint32_t cnt = h_info[4 + k + 1] - h_info[4 + k];
         cudaStream_t st = sk[k & 1];
@@ -752,11 +774,23 @@ int ext_batch_pipelined(fa_ctx *c, const ExtParams &kp, const fa_job *jobs, uint
                            c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(), kp, max_q, nullptr, c->out.as<fa_ext_result>(),
                            nullptr, false, c->cells_job.as<uint32_t>(), m.cells, m.status, st, k & 1));
         launches += ext_kernels_of(c, kc, kp, max_q);
+        if (early) {
+            const uint32_t lo = h_info[4 + kSlices + 1 + k];
+            FA_CUDA(cudaEventRecord(c->done_ev[k], st));
+            FA_CUDA(cudaStreamWaitEvent(cs, c->done_ev[k], 0));
+            FA_CUDA(cudaMemcpyAsync(out + lo, c->out.as<fa_ext_result>() + lo, sizeof(fa_ext_result) * (size_t)cnt,
+                                    cudaMemcpyDeviceToHost, cs));
+        }
     }
     FA_CUDA(cudaEventRecord(c->join_ev[0], sk[1]));
     FA_CUDA(cudaStreamWaitEvent(s, c->join_ev[0], 0));
     FA_CUDA(cudaEventRecord(c->ev1, s));
-    FA_CUDA(cudaMemcpyAsync(out, c->out.p, sizeof(fa_ext_result) * (size_t)n, cudaMemcpyDeviceToHost, s));
+    if (early) {
+        FA_CUDA(cudaEventRecord(c->join_ev[1], cs));
+        FA_CUDA(cudaStreamWaitEvent(s, c->join_ev[1], 0));
+    } else {
+        FA_CUDA(cudaMemcpyAsync(out, c->out.p, sizeof(fa_ext_result) * (size_t)n, cudaMemcpyDeviceToHost, s));
+    }
     if (int rc = finish_ext(c, nullptr, n, s, stats, nullptr, launches, 0, false)) return rc;
     FA_CUDA(cudaStreamSynchronize(s));
     return FA_OK;
@@ -810,6 +844,8 @@ void fa_ctx_destroy(fa_ctx *c) {
     if (c->fork_ev) cudaEventDestroy(c->fork_ev);
     if (c->gexec) cudaGraphExecDestroy(c->gexec);
     for (auto &e : c->slice_ev)
+        if (e) cudaEventDestroy(e);
+    for (auto &e : c->done_ev)
         if (e) cudaEventDestroy(e);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     c->chunk_scratch.release();

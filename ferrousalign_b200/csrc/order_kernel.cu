@@ -153,6 +153,17 @@ __global__ void chunk_prep_kernel(const fa_job *__restrict__ jobs, uint32_t n, u
             bin = chunk * kChunkBins + (FA_MAX_QLEN - jb.qlen);
         }
     }
+    {
+        // each chunk's lowest and highest job index (a chunk whose jobs form one index range
+        // can return its results as soon as it has run)
+        const int chunk = bin >= 0 ? bin / kChunkBins : -1;
+        const unsigned same = __match_any_sync(0xffffffffu, chunk);
+        const int lane = threadIdx.x & 31, lo_lane = __ffs(same) - 1, hi_lane = 31 - __clz(same);
+        if (chunk >= 0 && lane == lo_lane) {
+            atomicMin(&info[4 + nchunks + 1 + chunk], i);
+            atomicMax(&info[4 + 2 * nchunks + 1 + chunk], i - lane + hi_lane);
+        }
+    }
     const int mq = __reduce_max_sync(0xffffffffu, qlen);
     if ((threadIdx.x & 31) == 0 && mq > 0) atomicMax(&info[2], (uint32_t)mq);
     const int mw = __reduce_max_sync(0xffffffffu, band);
@@ -218,17 +229,21 @@ __global__ void chunk_scatter_kernel(const fa_job *__restrict__ jobs, uint32_t n
 
 size_t chunk_scratch_bytes(int nchunks) { return sizeof(uint32_t) * (3 * (size_t)nchunks * kChunkBins + 64); }
 
-// scratch layout: hist[nbins] | base[nbins] | cursor[nbins] | info[4] | bounds[nchunks+1]
+// scratch layout: hist[nbins] | base[nbins] | cursor[nbins] | info[4] | bounds[nchunks+1] |
+// lowest job index per chunk[nchunks] | highest[nchunks]
 cudaError_t launch_chunk_prep(const fa_job *d_jobs, uint32_t n, uint64_t qbytes, uint64_t tbytes, uint64_t qslice,
                               uint64_t tslice, int nchunks, int max_score, int qcap_limit, uint32_t *d_scratch,
                               cudaStream_t s)
 {
     const size_t nbins = (size_t)nchunks * kChunkBins;
     uint32_t *hist = d_scratch, *cursor = d_scratch + 2 * nbins, *info = d_scratch + 3 * nbins;
+    if (4 + 3 * (size_t)nchunks + 1 > 64) return cudaErrorInvalidValue;   // the 64 words past the bins
     cudaError_t e = cudaMemsetAsync(hist, 0, sizeof(uint32_t) * nbins, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(cursor, 0, sizeof(uint32_t) * nbins, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(info, 0, sizeof(uint32_t) * 4, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(info + 1, 0xFF, sizeof(uint32_t), s);   // first bad job: none
+    if (e == cudaSuccess) e = cudaMemsetAsync(info + 4 + nchunks + 1, 0xFF, sizeof(uint32_t) * nchunks, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(info + 4 + 2 * nchunks + 1, 0, sizeof(uint32_t) * nchunks, s);
     if (e != cudaSuccess || n == 0) return e;
     chunk_prep_kernel<<<(n + 255) / 256, 256, 0, s>>>(d_jobs, n, qbytes, tbytes, qslice, tslice, nchunks, max_score,
                                                       qcap_limit, hist, info);
