@@ -97,7 +97,7 @@ struct fa_ctx {
     // pipelined host batches: slice uploads on their own stream, one event per slice; the
     // same stream then returns each finished slice's results, after its done event
     cudaStream_t copy_stream = nullptr;
-    cudaEvent_t slice_ev[8] = {}, done_ev[8] = {};
+    cudaEvent_t slice_ev[8] = {}, done_ev[8] = {}, jobs_ev = nullptr;
     DevBuf chunk_scratch;
     // kernel choice: fixed, or (FA_KERNEL_AUTO) tuned per (query capacity class, band)
     struct Choice { int kernel; int tpb; };
@@ -697,25 +697,41 @@ int ext_batch_pipelined(fa_ctx *c, const ExtParams &kp, const fa_job *jobs, uint
         FA_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
         for (auto &e : c->slice_ev) FA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         for (auto &e : c->done_ev) FA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        FA_CUDA(cudaEventCreateWithFlags(&c->jobs_ev, cudaEventDisableTiming));
     }
     cudaStream_t s = c->stream, cs = c->copy_stream;
-    const uint64_t qs = std::max<uint64_t>(1, (qseq_len + kSlices - 1) / kSlices);
-    const uint64_t ts = std::max<uint64_t>(1, (tseq_len + kSlices - 1) / kSlices);
+    // graded slices (1, 1, 2, 4, 6, 6, 6, 6 thirty-seconds of each buffer): the first jobs
+    // start after a small upload, and the uploads, faster than the kernels, stay ahead
+    ChunkEnds ends;
+    {
+        static constexpr int kCum[kSlices] = {1, 2, 4, 8, 14, 20, 26, 32};
+        static_assert(kSlices <= kMaxChunks, "slice count");
+        for (int k = 0; k < kSlices; ++k) {
+            ends.q[k] = k == kSlices - 1 ? qseq_len : qseq_len / 32 * kCum[k];
+            ends.t[k] = k == kSlices - 1 ? tseq_len : tseq_len / 32 * kCum[k];
+        }
+    }
     Misc m = misc_of(c);
     uint32_t *scratch = c->chunk_scratch.as<uint32_t>();
     const size_t nbins = (size_t)kSlices * (FA_MAX_QLEN + 1);
     uint32_t *info = scratch + 3 * nbins;
     FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
-    FA_CUDA(cudaMemcpyAsync(c->jobs.p, jobs, sizeof(fa_job) * (size_t)n, cudaMemcpyHostToDevice, s));
-    // the sequence slices stream up meanwhile
+    // the job records first, then the sequence slices, all on the copy stream (one after
+    // another, so the records arrive at full bandwidth)
+    if (int rc = ensure_aux_streams(c)) return rc;
+    FA_CUDA(cudaEventRecord(c->fork_ev, s));      // after all earlier work on the main stream
+    FA_CUDA(cudaStreamWaitEvent(cs, c->fork_ev, 0));
+    FA_CUDA(cudaMemcpyAsync(c->jobs.p, jobs, sizeof(fa_job) * (size_t)n, cudaMemcpyHostToDevice, cs));
+    FA_CUDA(cudaEventRecord(c->jobs_ev, cs));
+    FA_CUDA(cudaStreamWaitEvent(s, c->jobs_ev, 0));
     for (int k = 0; k < kSlices; ++k) {
-        const uint64_t q0 = std::min(qseq_len, k * qs), q1 = std::min(qseq_len, (k + 1) * qs);
-        const uint64_t t0 = std::min(tseq_len, k * ts), t1 = std::min(tseq_len, (k + 1) * ts);
+        const uint64_t q0 = k ? ends.q[k - 1] : 0, q1 = ends.q[k];
+        const uint64_t t0 = k ? ends.t[k - 1] : 0, t1 = ends.t[k];
         if (q1 > q0) FA_CUDA(cudaMemcpyAsync(c->qseq.as<uint8_t>() + q0, qseq + q0, q1 - q0, cudaMemcpyHostToDevice, cs));
         if (t1 > t0) FA_CUDA(cudaMemcpyAsync(c->tseq.as<uint8_t>() + t0, tseq + t0, t1 - t0, cudaMemcpyHostToDevice, cs));
         FA_CUDA(cudaEventRecord(c->slice_ev[k], cs));
     }
-    FA_CUDA(launch_chunk_prep(c->jobs.as<fa_job>(), n, qseq_len, tseq_len, qs, ts, kSlices, kp.max_score,
+    FA_CUDA(launch_chunk_prep(c->jobs.as<fa_job>(), n, qseq_len, tseq_len, ends, kSlices, kp.max_score,
                               packed_qcap_limit(c->smem_optin), scratch, s));
     // info: status, first bad job, longest query, widest band | slice bounds in the order |
     // each slice's lowest and highest job index
@@ -731,7 +747,7 @@ int ext_batch_pipelined(fa_ctx *c, const ExtParams &kp, const fa_job *jobs, uint
         return fail(FA_ERR_ARG, "job %u is invalid", bad);
     }
     const int max_q = (int)h_info[2];
-    FA_CUDA(launch_chunk_scatter(c->jobs.as<fa_job>(), n, qs, ts, kSlices, scratch, c->order.as<uint32_t>(), s));
+    FA_CUDA(launch_chunk_scatter(c->jobs.as<fa_job>(), n, ends, kSlices, scratch, c->order.as<uint32_t>(), s));
     const int band = (int)h_info[3];   // widest configured band, reduced on the device
     if (c->kernel == FA_KERNEL_AUTO && !c->tuned.count({(max_q + 31) / 32, band}))
         FA_CUDA(cudaStreamWaitEvent(s, c->slice_ev[kSlices - 1], 0));   // tuning reads every slice
@@ -847,6 +863,7 @@ void fa_ctx_destroy(fa_ctx *c) {
         if (e) cudaEventDestroy(e);
     for (auto &e : c->done_ev)
         if (e) cudaEventDestroy(e);
+    if (c->jobs_ev) cudaEventDestroy(c->jobs_ev);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     c->chunk_scratch.release();
     if (c->kev0) cudaEventDestroy(c->kev0);

@@ -82,12 +82,18 @@ cudaError_t launch_mate_sw(bool byte_lanes, const fa_mate_job *d_jobs, const uin
 // Device-side longest-first ordering by query length (order_kernel.cu).
 // Pipelined host batches: validation + (chunk, length) histogram + prefix, then scatter.
 // Scratch layout: hist | base | cursor (nchunks * (FA_MAX_QLEN+1) each) | info[4] =
-// {status bits, first bad job, longest query, widest configured band} | bounds[nchunks+1].
+// {status bits, first bad job, longest query, widest configured band} | bounds[nchunks+1] |
+// each chunk's lowest and highest job index.  A job belongs to the chunk that holds the
+// last byte of its query or of its target, whichever comes later; chunk k of a buffer ends
+// at byte end[k] (exclusive; the last end is the buffer's length).
+constexpr int kMaxChunks = 8;
+struct ChunkEnds {
+    uint64_t q[kMaxChunks], t[kMaxChunks];
+};
 size_t chunk_scratch_bytes(int nchunks);
-cudaError_t launch_chunk_prep(const fa_job *d_jobs, uint32_t n, uint64_t qbytes, uint64_t tbytes, uint64_t qslice,
-                              uint64_t tslice, int nchunks, int max_score, int qcap_limit, uint32_t *d_scratch,
-                              cudaStream_t s);
-cudaError_t launch_chunk_scatter(const fa_job *d_jobs, uint32_t n, uint64_t qslice, uint64_t tslice, int nchunks,
+cudaError_t launch_chunk_prep(const fa_job *d_jobs, uint32_t n, uint64_t qbytes, uint64_t tbytes, const ChunkEnds &ends,
+                              int nchunks, int max_score, int qcap_limit, uint32_t *d_scratch, cudaStream_t s);
+cudaError_t launch_chunk_scatter(const fa_job *d_jobs, uint32_t n, const ChunkEnds &ends, int nchunks,
                                  uint32_t *d_scratch, uint32_t *d_order, cudaStream_t s);
 cudaError_t launch_qlen_hist(const fa_job *d_jobs, uint32_t n, uint32_t *d_hist, int sm_count, cudaStream_t s);
 cudaError_t launch_qlen_scatter(const fa_job *d_jobs, uint32_t n, uint32_t *d_cursor, uint32_t *d_order,

@@ -124,8 +124,22 @@ namespace fa {
 
 constexpr int kChunkBins = FA_MAX_QLEN + 1;
 
+// the chunk of a job: the one holding the later of its query's and its target's last byte
+__device__ __forceinline__ int chunk_of(const fa_job &jb, const ChunkEnds &ends, int nchunks) {
+    const uint64_t lq = jb.q_off + (uint64_t)jb.qlen - 1;
+    const uint64_t lt = jb.tlen > 0 ? jb.t_off + (uint64_t)jb.tlen - 1 : 0;
+    // the ends are increasing, so the count of ends at or below a byte is its chunk; the
+    // later of the two chunks is the larger count
+    int cq = 0, ct = 0;
+    for (int k = 0; k < nchunks - 1; ++k) {
+        cq += ends.q[k] <= lq;
+        ct += ends.t[k] <= lt;
+    }
+    return cq > ct ? cq : ct;
+}
+
 __global__ void chunk_prep_kernel(const fa_job *__restrict__ jobs, uint32_t n, uint64_t qbytes, uint64_t tbytes,
-                                  uint64_t qslice, uint64_t tslice, int nchunks, int max_score, int qcap_limit,
+                                  const ChunkEnds ends, int nchunks, int max_score, int qcap_limit,
                                   uint32_t *__restrict__ hist, uint32_t *__restrict__ info)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -146,11 +160,7 @@ __global__ void chunk_prep_kernel(const fa_job *__restrict__ jobs, uint32_t n, u
             atomicMin(&info[1], i);
             qlen = 0;
         } else {
-            const uint64_t cq = (jb.q_off + (uint64_t)jb.qlen - 1) / qslice;
-            const uint64_t ct = jb.tlen > 0 ? (jb.t_off + (uint64_t)jb.tlen - 1) / tslice : 0;
-            const uint64_t c = cq > ct ? cq : ct;
-            const int chunk = c < (uint64_t)nchunks ? (int)c : nchunks - 1;
-            bin = chunk * kChunkBins + (FA_MAX_QLEN - jb.qlen);
+            bin = chunk_of(jb, ends, nchunks) * kChunkBins + (FA_MAX_QLEN - jb.qlen);
         }
     }
     {
@@ -203,7 +213,7 @@ __global__ void __launch_bounds__(1024) chunk_scan_kernel(const uint32_t *__rest
     }
 }
 
-__global__ void chunk_scatter_kernel(const fa_job *__restrict__ jobs, uint32_t n, uint64_t qslice, uint64_t tslice,
+__global__ void chunk_scatter_kernel(const fa_job *__restrict__ jobs, uint32_t n, const ChunkEnds ends,
                                      int nchunks, const uint32_t *__restrict__ base, uint32_t *__restrict__ cursor,
                                      uint32_t *__restrict__ order)
 {
@@ -211,11 +221,7 @@ __global__ void chunk_scatter_kernel(const fa_job *__restrict__ jobs, uint32_t n
     int bin = -1;
     if (i < n) {
         const fa_job jb = jobs[i];
-        const uint64_t cq = (jb.q_off + (uint64_t)jb.qlen - 1) / qslice;
-        const uint64_t ct = jb.tlen > 0 ? (jb.t_off + (uint64_t)jb.tlen - 1) / tslice : 0;
-        const uint64_t c = cq > ct ? cq : ct;
-        const int chunk = c < (uint64_t)nchunks ? (int)c : nchunks - 1;
-        bin = chunk * kChunkBins + (FA_MAX_QLEN - jb.qlen);
+        bin = chunk_of(jb, ends, nchunks) * kChunkBins + (FA_MAX_QLEN - jb.qlen);
     }
     const unsigned peers = __match_any_sync(0xffffffffu, bin);
     if (bin < 0) return;
@@ -231,10 +237,10 @@ size_t chunk_scratch_bytes(int nchunks) { return sizeof(uint32_t) * (3 * (size_t
 
 // scratch layout: hist[nbins] | base[nbins] | cursor[nbins] | info[4] | bounds[nchunks+1] |
 // lowest job index per chunk[nchunks] | highest[nchunks]
-cudaError_t launch_chunk_prep(const fa_job *d_jobs, uint32_t n, uint64_t qbytes, uint64_t tbytes, uint64_t qslice,
-                              uint64_t tslice, int nchunks, int max_score, int qcap_limit, uint32_t *d_scratch,
-                              cudaStream_t s)
+cudaError_t launch_chunk_prep(const fa_job *d_jobs, uint32_t n, uint64_t qbytes, uint64_t tbytes, const ChunkEnds &ends,
+                              int nchunks, int max_score, int qcap_limit, uint32_t *d_scratch, cudaStream_t s)
 {
+    if (nchunks < 1 || nchunks > kMaxChunks) return cudaErrorInvalidValue;
     const size_t nbins = (size_t)nchunks * kChunkBins;
     uint32_t *hist = d_scratch, *cursor = d_scratch + 2 * nbins, *info = d_scratch + 3 * nbins;
     if (4 + 3 * (size_t)nchunks + 1 > 64) return cudaErrorInvalidValue;   // the 64 words past the bins
@@ -245,18 +251,19 @@ cudaError_t launch_chunk_prep(const fa_job *d_jobs, uint32_t n, uint64_t qbytes,
     if (e == cudaSuccess) e = cudaMemsetAsync(info + 4 + nchunks + 1, 0xFF, sizeof(uint32_t) * nchunks, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(info + 4 + 2 * nchunks + 1, 0, sizeof(uint32_t) * nchunks, s);
     if (e != cudaSuccess || n == 0) return e;
-    chunk_prep_kernel<<<(n + 255) / 256, 256, 0, s>>>(d_jobs, n, qbytes, tbytes, qslice, tslice, nchunks, max_score,
+    chunk_prep_kernel<<<(n + 255) / 256, 256, 0, s>>>(d_jobs, n, qbytes, tbytes, ends, nchunks, max_score,
                                                       qcap_limit, hist, info);
     chunk_scan_kernel<<<1, 1024, 0, s>>>(hist, (int)nbins, d_scratch + nbins, nchunks, info + 4);
     return cudaGetLastError();
 }
 
-cudaError_t launch_chunk_scatter(const fa_job *d_jobs, uint32_t n, uint64_t qslice, uint64_t tslice, int nchunks,
+cudaError_t launch_chunk_scatter(const fa_job *d_jobs, uint32_t n, const ChunkEnds &ends, int nchunks,
                                  uint32_t *d_scratch, uint32_t *d_order, cudaStream_t s)
 {
     if (n == 0) return cudaSuccess;
     const size_t nbins = (size_t)nchunks * kChunkBins;
-    chunk_scatter_kernel<<<(n + 255) / 256, 256, 0, s>>>(d_jobs, n, qslice, tslice, nchunks, d_scratch + nbins,
+    if (nchunks < 1 || nchunks > kMaxChunks) return cudaErrorInvalidValue;
+    chunk_scatter_kernel<<<(n + 255) / 256, 256, 0, s>>>(d_jobs, n, ends, nchunks, d_scratch + nbins,
                                                          d_scratch + 2 * nbins, d_order);
     return cudaGetLastError();
 }
