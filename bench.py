@@ -14,8 +14,10 @@ e2e     : alignments/s through the host C ABI call fa_ext_batch from pinned host
           results inside the timed region.
 GCUPS   : cells = sum over rows of the adaptive band width (end - beg), the oracle's count.
 
---impl reference times the CPU oracle (a restatement of the reference's ksw_extend2;
-the Rust reference cannot be built here) on all host cores over a bounded sample.
+--impl reference times the reference's own CPU path for this step -- its SIMD batch kernels
+(sw_kernel_i16, AVX-512BW or AVX2), restated in C++ because the Rust crate cannot be built
+here -- on all host cores over the whole batch.  The line's cpu_baselines also time that path
+in every width the CPU runs and the exact-semantics scalar port of ksw_extend2.
 """
 from __future__ import annotations
 
@@ -52,6 +54,20 @@ DPX_OPS_PER_CELL_PAIR = 9   # int16x2 ops per packed cell pair in the roofline m
 
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
+
+
+def hbm_peak() -> tuple[float, str]:
+    """HBM copy bandwidth (GB/s) for the HBM rooflines: the measured figure of this GPU pool
+    (MEASURED_PEAKS.json hbm_gbs) when the file is there, else the pool's earlier measured
+    6,650 GB/s."""
+    try:
+        v = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"])
+        return v, f"of measured (MEASURED_PEAKS.json hbm_gbs = {v})"
+    except (OSError, ValueError, KeyError, TypeError):
+        return 6650.0, "of fallback (6.65 TB/s, earlier measurement on this GPU pool)"
+
+
+HBM_GBS, HBM_SOURCE = hbm_peak()
 
 
 class ClockSampler:
@@ -134,6 +150,53 @@ def cpu_oracle_rate(b, p, sample: int):
     out, tr = O.ext_batch(p, jobs, b.qseq, b.tseq, threads=threads)
     dt = time.perf_counter() - t0
     return out, tr, dt, threads
+
+
+SIMD_PATH = {"avx512": "sw_kernel_i16 (banded_swa/kernel_i16.rs:44-272) with AVX-512BW, 32 int16 lanes",
+             "avx2": "sw_kernel_i16 (banded_swa/kernel_i16.rs:44-272) with AVX2, 16 int16 lanes"}
+KSWV_PATH = {"avx512": "batch_ksw_align (kswv_avx2.rs:93-641) with AVX-512BW, 64 u8 lanes",
+             "avx2": "batch_ksw_align_avx2 (kswv_avx2.rs:93-641), 32 u8 lanes"}
+
+
+def cpu_simd_rate(b, p, isa: str, reps: int = 1):
+    """The reference's SIMD CPU path restated (oracle/simd_baseline.cpp): every job of the
+    batch in chunks of the vector width, SoA transposes included, on all host threads.
+    Returns (seconds per pass, threads)."""
+    from oracle import simd_baseline as S
+    threads = os.cpu_count() or 1
+    best = None
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        S.ext_batch(p, b.jobs, b.qseq, b.tseq, isa=isa, threads=threads)
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    return best, threads
+
+
+def cpu_baselines(b, p, cells: int | None):
+    """CPU baselines on the host cores: the reference's SIMD path (every width the CPU runs)
+    over the whole batch, and the exact-semantics scalar port over a 200k-job sample.
+    `cells`: the batch's algorithmic cells (the GCUPS numerator of every line)."""
+    from oracle import simd_baseline as S
+    n = len(b.jobs)
+    res = {}
+    for isa in S.ISAS:
+        if not S.cpu_has(isa):
+            res[f"simd_{isa}"] = {"unavailable": f"host CPU lacks {isa}"}
+            continue
+        dt, threads = cpu_simd_rate(b, p, isa, reps=2)
+        res[f"simd_{isa}"] = {"value": n / dt, "unit": "alignments/s", "cores": threads, "kind": "port",
+                              "restates": SIMD_PATH[isa], "gcups": (cells / dt / 1e9) if cells else None,
+                              "sample": f"all {n} jobs of the batch (chunks of the vector width), all host threads"}
+    sample = min(CPU_SAMPLE, n)
+    _, tr, dt, threads = cpu_oracle_rate(b, p, sample)
+    res["scalar_ksw_extend2"] = {"value": sample / dt, "unit": "alignments/s", "cores": threads, "kind": "port",
+                                 "restates": "ksw_extend2 (ksw_affine_gap.rs:952-1169), exact outputs",
+                                 "gcups": float(tr["cells"].sum()) / dt / 1e9,
+                                 "sample": f"first {sample} jobs of the batch, all host threads"}
+    isa = S.best_isa()
+    head = dict(res[f"simd_{isa}"])
+    return head, res
 
 
 def bench_learned(args, ctx, b, p):
@@ -359,13 +422,30 @@ def bench_mate(args, ctx, lib, dev, stream, flush, skip_cpu=False):
            "cells_per_step": int(cells.value), "bit_exact_sample": bool(np.array_equal(out[chk], ref)),
            "gpu_launches": launches}
     if not skip_cpu:
+        from oracle import simd_baseline as S
+        base = {}
+        for isa in S.ISAS:
+            if not S.cpu_has(isa):
+                continue
+            t0 = time.perf_counter()
+            S.kswv_batch(m.jobs, m.qseq, m.tseq, isa=isa, threads=os.cpu_count() or 1)
+            dt = time.perf_counter() - t0
+            base[f"kswv_{isa}"] = {"value": MATE_JOBS / dt, "unit": "alignments/s", "cores": os.cpu_count(),
+                                   "kind": "port", "restates": KSWV_PATH[isa],
+                                   "gcups": cells.value / dt / 1e9,
+                                   "sample": f"all {MATE_JOBS} jobs, all host threads (score/te exact; tb/qb "
+                                             "estimated and score2 on every other lane, as the reference's kernel)"}
         sample = m.jobs[:MATE_CPU_SAMPLE]
         t0 = time.perf_counter()
         _, cc = O.mate_batch(mp, sample, m.qseq, m.tseq, threads=os.cpu_count() or 1)
         dt = time.perf_counter() - t0
-        res["cpu_baseline"] = {"value": MATE_CPU_SAMPLE / dt, "unit": "alignments/s", "cores": os.cpu_count(),
-                               "kind": "port", "gcups": float(cc.sum()) / dt / 1e9,
-                               "sample": f"first {MATE_CPU_SAMPLE} jobs, oracle on all host threads"}
+        base["scalar_ksw_align2"] = {"value": MATE_CPU_SAMPLE / dt, "unit": "alignments/s",
+                                     "cores": os.cpu_count(), "kind": "port",
+                                     "restates": "ksw_align2 (ksw_affine_gap.rs:773-861), exact outputs",
+                                     "gcups": float(cc.sum()) / dt / 1e9,
+                                     "sample": f"first {MATE_CPU_SAMPLE} jobs, all host threads"}
+        res["cpu_baseline"] = dict(base.get(f"kswv_{S.best_isa()}", base["scalar_ksw_align2"]))
+        res["cpu_baselines"] = base
     return res
 
 
@@ -415,9 +495,9 @@ def bench_regions(args, ctx, lib, dev, stream, flush):
     algo = n_chains * (8 + 48) + ns * (24 + 2 * 24)
     return {"workload": f"{n_chains} chains, {ns} seeds (1-8 per chain), one left and one right result per seed",
             "kernel": "merge_regions_kernel", "kernel_ms": ms, "chains_per_s": n_chains / (ms * 1e-3),
-            "roofline": {"bound": "hbm", "achieved": algo / (ms * 1e-3) / 1e9, "peak": 6546.6, "unit": "GB/s",
-                         "frac": algo / (ms * 1e-3) / 1e9 / 6546.6, "algorithmic_bytes": algo,
-                         "peak_source": "MEASURED_PEAKS.json hbm_gbs"},
+            "roofline": {"bound": "hbm", "achieved": algo / (ms * 1e-3) / 1e9, "peak": HBM_GBS, "unit": "GB/s",
+                         "frac": algo / (ms * 1e-3) / 1e9 / HBM_GBS, "algorithmic_bytes": algo,
+                         "peak_source": HBM_SOURCE},
             "bit_exact_sample": bool(np.array_equal(out[:k], ref)), "sample": f"first {k} chains against the oracle"}
 
 
@@ -469,9 +549,9 @@ def bench_collect(args, ctx, lib):
                         f"100 Mbp reference (2-bit packed, {len(pac)} B)",
             "jobs": {"left": len(got.left_jobs), "right": len(got.right_jobs)},
             "kernel_ms": km, "e2e_ms": float(np.median(wall)), "kernel_launches": int(k_n.value),
-            "roofline": {"bound": "hbm", "achieved": algo / (km * 1e-3) / 1e9, "peak": 6546.6, "unit": "GB/s",
-                         "frac": algo / (km * 1e-3) / 1e9 / 6546.6, "algorithmic_bytes": algo,
-                         "peak_source": "MEASURED_PEAKS.json hbm_gbs"},
+            "roofline": {"bound": "hbm", "achieved": algo / (km * 1e-3) / 1e9, "peak": HBM_GBS, "unit": "GB/s",
+                         "frac": algo / (km * 1e-3) / 1e9 / HBM_GBS, "algorithmic_bytes": algo,
+                         "peak_source": HBM_SOURCE},
             "bit_exact_sample": bool(same), "sample": f"first {k} chains against the oracle"}
 
 
@@ -520,8 +600,8 @@ def bench_cigar(args, ctx, lib):
     return {"workload": f"{n} regions of 151-bp reads (read vs its reference span, h0 = 0, bands |dlen| + 5-30)",
             "kernel": "cigar_kernel", "kernel_ms": km, "alignments_per_s": n / (km * 1e-3),
             "gcups": cells / (km * 1e-3) / 1e9, "cells": cells, "e2e_ms": float(np.median(wall)),
-            "roofline": {"bound": "alu", "hbm_achieved_gbs": algo / (km * 1e-3) / 1e9, "hbm_peak_gbs": 6546.6,
-                         "hbm_frac": algo / (km * 1e-3) / 1e9 / 6546.6, "algorithmic_bytes": algo,
+            "roofline": {"bound": "alu", "hbm_achieved_gbs": algo / (km * 1e-3) / 1e9, "hbm_peak_gbs": HBM_GBS,
+                         "hbm_frac": algo / (km * 1e-3) / 1e9 / HBM_GBS, "algorithmic_bytes": algo,
                          "note": "scalar int32 cells with a 2-bit traceback; one thread per alignment"},
             "bit_exact_sample": bool(same), "sample": f"first {k} alignments against the oracle"}
 
@@ -582,40 +662,50 @@ def bench_rescue_collect(args, ctx, lib):
     return {"workload": f"{len(cands)} rescue attempts of 2x151-bp pairs, 20 Mbp reference (6 sequences, 2-bit packed)",
             "jobs": len(got.jobs), "kernel_ms": km, "e2e_ms": float(np.median(wall)),
             "kernel_launches": int(k_n.value),
-            "roofline": {"bound": "hbm", "achieved": algo / (km * 1e-3) / 1e9, "peak": 6546.6, "unit": "GB/s",
-                         "frac": algo / (km * 1e-3) / 1e9 / 6546.6, "algorithmic_bytes": algo,
-                         "peak_source": "MEASURED_PEAKS.json hbm_gbs"},
+            "roofline": {"bound": "hbm", "achieved": algo / (km * 1e-3) / 1e9, "peak": HBM_GBS, "unit": "GB/s",
+                         "frac": algo / (km * 1e-3) / 1e9 / HBM_GBS, "algorithmic_bytes": algo,
+                         "peak_source": HBM_SOURCE},
             "bit_exact_sample": bool(same), "sample": f"first {k} attempts against the oracle",
             "insert_size_stats": {"pairs": len(pairs), "kernel_ms": float(np.median(st_ms)),
                                   "fr": {f: float(stats[1][f]) for f in ("avg", "std", "low", "high", "failed")}}}
 
 
 def run_reference(args):
+    """The reference's own CPU implementation of the path, on the host cores: its SIMD batch
+    kernels (sw_kernel_i16 in the widest vector width the CPU runs, fed chunk by chunk as the
+    reference's dispatcher intends), restated in C++ in oracle/simd_baseline.cpp because the
+    Rust crate cannot be built here.  One step = the whole 1M-job batch."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
     import ferrousalign_b200 as fa
+    from oracle import ksw_oracle as O
+    from oracle import simd_baseline as S
     b = make_workload(0, N_JOBS)
     p = fa.BandedPairWiseSW().to_struct()
-    sample = min(CPU_SAMPLE, N_JOBS)
+    isa = S.best_isa()
     for _ in range(args.warmup):
-        cpu_oracle_rate(b, p, min(sample, 20_000))
-    times, cells = [], 0
+        cpu_simd_rate(b, p, isa)
+    times = []
+    threads = os.cpu_count() or 1
     for _ in range(args.steps):
-        _, tr, dt, threads = cpu_oracle_rate(b, p, sample)
+        dt, threads = cpu_simd_rate(b, p, isa)
         times.append(dt)
-        cells = int(tr["cells"].sum())
     dt = sum(times) / len(times)
-    aln = sample / dt
+    aln = N_JOBS / dt
+    # GCUPS numerator: the batch's algorithmic cells (the scalar port's count, untimed)
+    _, tr = O.ext_batch(p, b.jobs, b.qseq, b.tseq, threads=threads)
+    cells = int(tr["cells"].sum())
     line = {
         "impl": "reference", "metric": METRIC, "value": aln, "unit": "alignments/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": {"workload": "1M right extensions, 151 bp reads (sample of the batch per step)",
-                   "sample_jobs": sample, "w": 100, "zdrop": 100, "end_bonus": 5},
+        "scaling": "weak", "vs_baseline": None, "dtype": "int16", "data": "synthetic",
+        "config": {"workload": "1M right extensions, 151 bp reads, indel rate {0,0.1,1,3}%, w=100",
+                   "jobs_per_step": N_JOBS, "w": 100, "zdrop": 100, "end_bonus": 5},
         "gcups": cells / dt / 1e9,
         "cpu_baseline": {"value": aln, "unit": "alignments/s", "cores": threads, "kind": "port",
-                         "sample": f"first {sample} of the 1M jobs, all host threads"},
+                         "restates": SIMD_PATH[isa],
+                         "sample": f"all {N_JOBS} jobs per step, chunks of the vector width, all host threads"},
         "e2e": {"value": aln, "unit": "alignments/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "gpu_launches": 0,
     }
@@ -787,7 +877,7 @@ def main():
                      "peak_source": f"measured __viaddmax_s16x2_relu rate {peak_ops / 1e12:.2f} Tops/s x2/"
                                     f"{DPX_OPS_PER_CELL_PAIR}; s32 DPX {peak_s32 / 1e12:.2f} Tops/s",
                      "hbm": {"achieved_gbs": (bytes_in + bytes_out) / (kernel_ms * 1e-3) / 1e9,
-                             "peak_gbs": 6546.6, "peak_source": "MEASURED_PEAKS.json hbm_gbs"}},
+                             "peak_gbs": HBM_GBS, "peak_source": HBM_SOURCE}},
         "e2e": {"value": total_aln / (e2e_ms * 1e-3), "unit": "alignments/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": bytes_in + n * 4, "d2h_bytes_per_step": bytes_out},
         "gpu_launches": launches,
@@ -808,10 +898,7 @@ def main():
         line["cigar"] = bench_cigar(args, ctx, lib)
         line["rescue_collection"] = bench_rescue_collect(args, ctx, lib)
     if not args.skip_cpu:
-        ref2, tr2, dt, threads = cpu_oracle_rate(b, p, min(CPU_SAMPLE, n))
-        line["cpu_baseline"] = {"value": min(CPU_SAMPLE, n) / dt, "unit": "alignments/s", "cores": threads,
-                                "kind": "port", "gcups": float(tr2["cells"].sum()) / dt / 1e9,
-                                "sample": f"first {min(CPU_SAMPLE, n)} jobs of the batch, oracle on all host threads"}
+        line["cpu_baseline"], line["cpu_baselines"] = cpu_baselines(b, p, cells)
     print(json.dumps(line), flush=True)
     if ws > 1:
         torch.distributed.destroy_process_group()

@@ -22,9 +22,10 @@ FA_KERNEL_AUTO, FA_KERNEL_INT32, FA_KERNEL_INT16X2, FA_KERNEL_ROWS2 = 0, 1, 2, 3
 KSW_XBYTE, KSW_XSTOP, KSW_XSUBO, KSW_XSTART = 0x10000, 0x20000, 0x40000, 0x80000
 FA_MAX_QLEN, FA_MAX_TLEN = 4096, 65535
 FA_NOALLOC_MAX_JOBS = 1 << 18
+FA_PARAM_H0_ZERO = 1
 FA_BAND_NPARAMS = 3201
 
-PARAMS_DT = np.dtype([("mat", "i1", 25), ("_pad", "i1", 3), ("m", "<i4"), ("o_del", "<i4"),
+PARAMS_DT = np.dtype([("mat", "i1", 25), ("flags", "u1"), ("_pad", "i1", 2), ("m", "<i4"), ("o_del", "<i4"),
                       ("e_del", "<i4"), ("o_ins", "<i4"), ("e_ins", "<i4"), ("zdrop", "<i4"),
                       ("end_bonus", "<i4"), ("pen_clip5", "<i4"), ("pen_clip3", "<i4")])
 JOB_DT = np.dtype([("q_off", "<u8"), ("t_off", "<u8"), ("qlen", "<i4"), ("tlen", "<i4"),
@@ -35,7 +36,7 @@ POLICY_DT = np.dtype([("mode", "<i4"), ("max_tries", "<i4"), ("judge", "<i4"), (
 STATS_DT = np.dtype([("cells", "<u8"), ("cells_executed", "<u8"), ("jobs", "<u4"), ("retries", "<u4"),
                      ("misses", "<u4"), ("kernel_launches", "<u4"), ("kernel_ms", "<f4"),
                      ("total_ms", "<f4")])
-MATE_PARAMS_DT = np.dtype([("mat", "i1", 25), ("_pad", "i1", 3), ("m", "<i4"), ("o_del", "<i4"),
+MATE_PARAMS_DT = np.dtype([("mat", "i1", 25), ("flags", "u1"), ("_pad", "i1", 2), ("m", "<i4"), ("o_del", "<i4"),
                            ("e_del", "<i4"), ("o_ins", "<i4"), ("e_ins", "<i4")])
 MATE_JOB_DT = np.dtype([("q_off", "<u8"), ("t_off", "<u8"), ("qlen", "<i4"), ("tlen", "<i4"),
                         ("xtra", "<u4"), ("_pad", "<i4")])

@@ -7,7 +7,8 @@ them and returns one ``BatchExtensionResult`` per job in job order.  Scores foll
 ``ksw_extend2`` (src/core/alignment/ksw_affine_gap.rs:952-1169) exactly.
 
 Errors: the reference panics where ksw_extend2 asserts (h0 <= 0) or a slice is out of
-range; here those raise ``NativeError`` with code FA_ERR_ARG.  An empty batch returns
+range; here those raise ``NativeError`` with code FA_ERR_ARG.  With
+``BandedPairWiseSW(allow_h0_zero=True)`` jobs with h0 == 0 run the recurrence as written.  An empty batch returns
 an empty list (dispatch.rs:36-38).
 """
 from __future__ import annotations
@@ -49,6 +50,9 @@ class BandedPairWiseSW:
     mat: np.ndarray | None = None
     w_match: int = 1
     w_mismatch: int = -4
+    # FA_PARAM_H0_ZERO: jobs with h0 == 0 (the reference's right jobs, collect_soa.rs:206)
+    # run the recurrence as written instead of failing like ksw_extend2's assert
+    allow_h0_zero: bool = False
 
     def __post_init__(self):
         if self.mat is None:
@@ -61,6 +65,7 @@ class BandedPairWiseSW:
         p["m"] = 5
         for k in ("o_del", "e_del", "o_ins", "e_ins", "zdrop", "end_bonus", "pen_clip5", "pen_clip3"):
             p[k] = getattr(self, k)
+        p["flags"] = N.FA_PARAM_H0_ZERO if self.allow_h0_zero else 0
         return p
 
 

@@ -50,11 +50,13 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
     if force or _stale(LIB, deps):
         objdir = PKG / "_build"
         objdir.mkdir(exist_ok=True)
-        objs = []
-        for src in cu:
-            obj = objdir / (src.stem + ".o")
-            _run([_nvcc(), *NVCC_FLAGS, "-c", str(src), "-o", str(obj)], verbose)
-            objs.append(str(obj))
+        objs = [str(objdir / (src.stem + ".o")) for src in cu]
+        # one nvcc per translation unit, run side by side
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(max_workers=min(len(cu), os.cpu_count() or 1)) as ex:
+            for f in [ex.submit(_run, [_nvcc(), *NVCC_FLAGS, "-c", str(src), "-o", o], verbose)
+                      for src, o in zip(cu, objs)]:
+                f.result()
         tmp = LIB.with_suffix(".so.tmp")
         _run([_nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", str(tmp), *objs,
               "-lcudart"], verbose)

@@ -60,8 +60,16 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
         uint32_t *qw = smem + RING * T + threadIdx.x;     // RING: packed query codes
         const int qlen = jb.qlen, tlen = jb.tlen, h0 = jb.h0;
         const int w = ext_band_clamp(qlen, w_try ? w_try[jid] : jb.w, p);
-        if (h0 <= 0 || qlen <= 0 || tlen < 0) {
+        if (h0 < 0 || (h0 == 0 && !(p.flags & FA_PARAM_H0_ZERO)) || qlen <= 0 || tlen < 0) {
             atomicOr(status, ST_ARG);
+        } else if (h0 == 0) {
+            // FA_PARAM_H0_ZERO: the recurrence as written is all zero after row 0
+            fa_ext_result r;
+            cells = ext_h0_zero_result(qlen, tlen, w, &r);
+            out[jid] = r;
+            if (clamped_out)
+                clamped_out[jid] = (uint8_t)((tlen > 0 && qlen > w + 1 ? 1 : 0) | (CERT ? kBandHintNone << 2 : 0));
+            if (cells_job) cells_job[jid] = cells;
         } else if (qlen > qcap || h0 + p.max_score * qlen > kPackedHMax || (RING > 0 && 2 * w + 2 > RING)) {
             atomicOr(status, ST_CAPACITY);
         } else {

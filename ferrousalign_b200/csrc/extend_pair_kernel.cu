@@ -175,7 +175,20 @@ __host__ __device__ __forceinline__ unsigned long long ext_pair_thread(
             s.cells = 0; s.clamped = 0;
             s.best = jb.h0; s.max_i = s.max_j = s.max_ie = -1; s.gscore = -1; s.max_off = 0;
             s.beg = 0; s.end = jb.qlen;
-            if (s.live && (jb.h0 <= 0 || jb.qlen <= 0 || jb.tlen < 0)) { status_or(status, ST_ARG); s.live = 0; }
+            if (s.live && (jb.h0 < 0 || (jb.h0 == 0 && !(p.flags & FA_PARAM_H0_ZERO)) || jb.qlen <= 0 || jb.tlen < 0)) {
+                status_or(status, ST_ARG);
+                s.live = 0;
+            } else if (s.live && jb.h0 == 0) {
+                // FA_PARAM_H0_ZERO: the recurrence as written is all zero after row 0; the job's
+                // final state is set here and written out with the others at the end
+                const int w0 = ext_band_clamp(jb.qlen, w_try ? w_try[s.jid] : jb.w, p);
+                fa_ext_result r;
+                s.cells = ext_h0_zero_result(jb.qlen, jb.tlen, w0, &r);
+                s.best = r.score; s.max_j = r.qle - 1; s.max_i = r.tle - 1; s.max_ie = r.gtle - 1;
+                s.gscore = r.gscore; s.max_off = r.max_off;
+                s.clamped = jb.tlen > 0 && jb.qlen > w0 + 1 ? 1 : 0;
+                s.live = 0;
+            }
             else if (s.live && (jb.qlen > qcap || jb.h0 + p.max_score * jb.qlen > kPackedHMax)) {
                 status_or(status, ST_CAPACITY); s.live = 0;
             }

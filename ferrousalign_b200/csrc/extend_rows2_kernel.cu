@@ -100,13 +100,23 @@ __host__ __device__ __forceinline__ uint32_t rows2_thread(
     const fa_job jb = jobs[jid];
     const int qlen = jb.qlen, tlen = jb.tlen, h0 = jb.h0;
     const int a = p.max_score;
-    if (h0 <= 0 || qlen <= 0 || tlen < 0) {
+    if (h0 < 0 || (h0 == 0 && !(p.flags & FA_PARAM_H0_ZERO)) || qlen <= 0 || tlen < 0) {
         or_status(status, ST_ARG);
         return 0;
     }
     if (qlen > qcap) {
         or_status(status, ST_CAPACITY);
         return 0;
+    }
+    if (h0 == 0) {   // FA_PARAM_H0_ZERO: the recurrence as written is all zero after row 0
+        const int w0 = ext_band_clamp(qlen, w_try ? w_try[jid] : jb.w, p);
+        fa_ext_result r;
+        const uint32_t c = ext_h0_zero_result(qlen, tlen, w0, &r);
+        out[jid] = r;
+        if (clamped_out)
+            clamped_out[jid] = (uint8_t)((tlen > 0 && qlen > w0 + 1 ? 1 : 0) | (CERT ? kBandHintNone << 2 : 0));
+        if (cells_job) cells_job[jid] = c;
+        return c;
     }
     if (h0 > 255 || a * qlen > 255 - h0) {
         ovf[take_slot(ovf_n)] = jid;                  // needs wider cells: the int32 kernel

@@ -300,11 +300,13 @@ ExtParams ext_params_of(const fa_params *p) {
     int ms = 0;
     for (int i = 0; i < 25; ++i) if (p->mat[i] > (int8_t)ms) ms = p->mat[i];
     k.max_score = ms;
+    k.flags = p->flags;
     return k;
 }
 
 // Validation mirrors the reference's panics (h0 <= 0 asserts at ksw_affine_gap.rs:968,
-// out-of-range slices) and this library's limits.
+// unless FA_PARAM_H0_ZERO lifts the assert for h0 == 0; out-of-range slices) and this
+// library's limits.
 int check_jobs(const fa_job *jobs, uint32_t n, uint64_t qlen_buf, uint64_t tlen_buf,
                const ExtParams &k, int qcap_limit, int *max_qlen) {
     int mq = 0;
@@ -312,7 +314,8 @@ int check_jobs(const fa_job *jobs, uint32_t n, uint64_t qlen_buf, uint64_t tlen_
         const fa_job &j = jobs[i];
         if (j.qlen <= 0) return fail(FA_ERR_ARG, "job %u: qlen=%d must be > 0", i, j.qlen);
         if (j.tlen < 0) return fail(FA_ERR_ARG, "job %u: tlen=%d must be >= 0", i, j.tlen);
-        if (j.h0 <= 0) return fail(FA_ERR_ARG, "job %u: h0=%d must be > 0", i, j.h0);
+        if (j.h0 < 0 || (j.h0 == 0 && !(k.flags & FA_PARAM_H0_ZERO)))
+            return fail(FA_ERR_ARG, "job %u: h0=%d must be > 0 (or 0 with FA_PARAM_H0_ZERO)", i, j.h0);
         if (j.qlen > FA_MAX_QLEN || j.tlen > FA_MAX_TLEN)
             return fail(FA_ERR_CAPACITY, "job %u: lengths %d/%d exceed %d/%d", i, j.qlen, j.tlen,
                         FA_MAX_QLEN, FA_MAX_TLEN);
@@ -389,7 +392,7 @@ int read_status(fa_ctx *c, cudaStream_t s) {
     if (st & ST_BAD_CODE) return fail(FA_ERR_ARG, "a sequence byte is outside the alphabet (codes 0-4)");
     if (st & ST_CAPACITY) return fail(FA_ERR_CAPACITY, "a job exceeded the launch capacity");
     if (st & ST_BLIST) return fail(FA_ERR_CAPACITY, "mate-SW run list overflow");
-    if (st & ST_ARG) return fail(FA_ERR_ARG, "a job has h0 <= 0, qlen <= 0 or tlen < 0");
+    if (st & ST_ARG) return fail(FA_ERR_ARG, "a job has h0 <= 0 (h0 < 0 with FA_PARAM_H0_ZERO), qlen <= 0 or tlen < 0");
     if (st & ST_RANGE) return fail(FA_ERR_ARG, "a chain's seed range is malformed");
     return FA_OK;
 }
@@ -732,7 +735,7 @@ int ext_batch_pipelined(fa_ctx *c, const ExtParams &kp, const fa_job *jobs, uint
         FA_CUDA(cudaEventRecord(c->slice_ev[k], cs));
     }
     FA_CUDA(launch_chunk_prep(c->jobs.as<fa_job>(), n, qseq_len, tseq_len, ends, kSlices, kp.max_score,
-                              packed_qcap_limit(c->smem_optin), scratch, s));
+                              (kp.flags & FA_PARAM_H0_ZERO) ? 0 : 1, packed_qcap_limit(c->smem_optin), scratch, s));
     // info: status, first bad job, longest query, widest band | slice bounds in the order |
     // each slice's lowest and highest job index
     uint32_t h_info[4 + kSlices + 1 + 2 * kSlices];

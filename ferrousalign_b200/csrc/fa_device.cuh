@@ -34,6 +34,7 @@ struct ExtParams {
     int32_t o_del, e_del, o_ins, e_ins;
     int32_t zdrop, end_bonus;
     int32_t max_score;      // max(0, max(mat))  (ksw_affine_gap.rs:1000-1005)
+    int32_t flags;          // fa_params.flags (FA_PARAM_*)
 };
 
 struct MateParams {
@@ -63,6 +64,29 @@ __host__ __device__ inline int32_t ext_band_clamp(int32_t qlen, int32_t w, const
     if (max_del < 1) max_del = 1;
     if (w > max_del) w = max_del;
     return w;
+}
+
+// ksw_extend2 run as written on a job with h0 == 0 (FA_PARAM_H0_ZERO; the reference asserts
+// h0 > 0 at ksw_affine_gap.rs:968).  The first row is then all zero (eh[0].h = h0 = 0 and
+// eh[1].h = 0, :1017-1025), so every M is 0 (`M ? M + s : 0`, :1066-1071) and every H, E
+// and F of row 0 is 0: the row maximum is 0 and the loop breaks after row 0 (:1122), which
+// sets gscore = 0 and max_ie = 0 only when row 0's band reaches the query end (:1109-1120,
+// end = min(qlen, w + 1) with the clamped band w).  `w` is the band after ext_band_clamp.
+// Returns the cells row 0 visited (end - beg), 0 when tlen == 0 (no row runs).
+__host__ __device__ inline uint32_t ext_h0_zero_result(int32_t qlen, int32_t tlen, int32_t w, fa_ext_result *r) {
+    r->score = 0;
+    r->qle = 0;
+    r->tle = 0;
+    r->max_off = 0;
+    r->gscore = -1;
+    r->gtle = 0;
+    if (tlen <= 0) return 0;
+    const int32_t end = qlen < w + 1 ? qlen : w + 1;
+    if (end == qlen) {
+        r->gscore = 0;
+        r->gtle = 1;
+    }
+    return (uint32_t)end;
 }
 
 }  // namespace fa

@@ -91,8 +91,10 @@ struct ChunkEnds {
     uint64_t q[kMaxChunks], t[kMaxChunks];
 };
 size_t chunk_scratch_bytes(int nchunks);
+// h0_min: the smallest valid h0 (1, or 0 with FA_PARAM_H0_ZERO)
 cudaError_t launch_chunk_prep(const fa_job *d_jobs, uint32_t n, uint64_t qbytes, uint64_t tbytes, const ChunkEnds &ends,
-                              int nchunks, int max_score, int qcap_limit, uint32_t *d_scratch, cudaStream_t s);
+                              int nchunks, int max_score, int h0_min, int qcap_limit, uint32_t *d_scratch,
+                              cudaStream_t s);
 cudaError_t launch_chunk_scatter(const fa_job *d_jobs, uint32_t n, const ChunkEnds &ends, int nchunks,
                                  uint32_t *d_scratch, uint32_t *d_order, cudaStream_t s);
 cudaError_t launch_qlen_hist(const fa_job *d_jobs, uint32_t n, uint32_t *d_hist, int sm_count, cudaStream_t s);

@@ -112,9 +112,12 @@ extern "C" int fa_ext_batch_device_noalloc(const fa_params *p, const fa_job *d_j
     int ms = 0;
     for (int i = 0; i < 25; ++i) if (p->mat[i] > (int8_t)ms) ms = p->mat[i];
     kp.max_score = ms;
+    kp.flags = p->flags;
 
-    // Every call reuses the array: clear the status word (the histogram is cleared by
-    // its launcher and the order is fully rewritten by the scatter).
+    // Every call reuses the array: clear the status word.  The histogram is cleared by its
+    // launcher, and the scatter rewrites the first n order slots, each exactly once: the
+    // histogram and the scatter put every job in the same bin (qlen_bin, invalid lengths
+    // included), so no slot keeps an index left by an earlier, larger call.
     NA_CUDA(cudaMemsetAsync(sc->status, 0, sizeof(uint32_t), s));
     NA_CUDA(launch_qlen_hist(d_jobs, n, sc->hist, sm_count, s));
     uint32_t hist[kHistWords];
@@ -156,7 +159,8 @@ extern "C" int fa_ext_batch_device_noalloc(const fa_params *p, const fa_job *d_j
     NA_CUDA(cudaMemcpyAsync(&st, sc->status, sizeof(st), cudaMemcpyDeviceToHost, s));
     NA_CUDA(cudaStreamSynchronize(s));
     if (st & ST_BAD_CODE) return set_last_error(FA_ERR_ARG, "a sequence byte is outside the alphabet (codes 0-4)");
-    if (st & ST_ARG) return set_last_error(FA_ERR_ARG, "a job has h0 <= 0, qlen <= 0 or tlen < 0");
+    if (st & ST_ARG)
+        return set_last_error(FA_ERR_ARG, "a job has h0 <= 0 (h0 < 0 with FA_PARAM_H0_ZERO), qlen <= 0 or tlen < 0");
     if (st & ST_CAPACITY) return set_last_error(FA_ERR_CAPACITY, "a job exceeded the kernel capacity");
     return FA_OK;
 }

@@ -11,16 +11,20 @@ namespace fa {
 
 constexpr int kHistBins = FA_MAX_QLEN + 1;
 
+// Histogram bin of a job's query length: [0, FA_MAX_QLEN], lengths outside clamped to the
+// nearer end.  The histogram and the scatter both use it, so every job has the same bin in
+// both and each order slot is written exactly once.
+__host__ __device__ __forceinline__ int qlen_bin(int qlen) {
+    return qlen < 0 ? 0 : (qlen > FA_MAX_QLEN ? FA_MAX_QLEN : qlen);
+}
+
 __global__ void qlen_hist_kernel(const fa_job *__restrict__ jobs, uint32_t n, uint32_t *__restrict__ hist)
 {
     __shared__ uint32_t h[kHistBins];
     for (int b = threadIdx.x; b < kHistBins; b += blockDim.x) h[b] = 0;
     __syncthreads();
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        int q = jobs[i].qlen;
-        q = q < 0 ? 0 : (q > FA_MAX_QLEN ? FA_MAX_QLEN : q);
-        atomicAdd(&h[q], 1u);
-    }
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        atomicAdd(&h[qlen_bin(jobs[i].qlen)], 1u);
     __syncthreads();
     for (int b = threadIdx.x; b < kHistBins; b += blockDim.x)
         if (h[b]) atomicAdd(&hist[b], h[b]);
@@ -31,8 +35,9 @@ __global__ void qlen_scatter_kernel(const fa_job *__restrict__ jobs, uint32_t n,
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool live = i < n;
-    int q = live ? jobs[i].qlen : -1;
-    q = q < -1 ? 0 : (q > FA_MAX_QLEN ? FA_MAX_QLEN : q);
+    // a live job lands in the same bin as in qlen_hist_kernel (negative lengths in bin 0);
+    // -1 marks only the lanes past n, which leave before touching the cursors
+    const int q = live ? qlen_bin(jobs[i].qlen) : -1;
     const unsigned peers = __match_any_sync(0xffffffffu, q);
     if (!live) return;
     const int lane = threadIdx.x & 31;
@@ -139,7 +144,7 @@ __device__ __forceinline__ int chunk_of(const fa_job &jb, const ChunkEnds &ends,
 }
 
 __global__ void chunk_prep_kernel(const fa_job *__restrict__ jobs, uint32_t n, uint64_t qbytes, uint64_t tbytes,
-                                  const ChunkEnds ends, int nchunks, int max_score, int qcap_limit,
+                                  const ChunkEnds ends, int nchunks, int max_score, int h0_min, int qcap_limit,
                                   uint32_t *__restrict__ hist, uint32_t *__restrict__ info)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -150,7 +155,7 @@ __global__ void chunk_prep_kernel(const fa_job *__restrict__ jobs, uint32_t n, u
         qlen = jb.qlen;
         band = max(jb.w, 0);
         uint32_t st = 0;
-        if (jb.qlen <= 0 || jb.tlen < 0 || jb.h0 <= 0) st |= ST_ARG;
+        if (jb.qlen <= 0 || jb.tlen < 0 || jb.h0 < h0_min) st |= ST_ARG;
         else if (jb.qlen > FA_MAX_QLEN || jb.tlen > FA_MAX_TLEN) st |= ST_CAPACITY;
         else if (jb.q_off + (uint64_t)jb.qlen > qbytes || jb.t_off + (uint64_t)jb.tlen > tbytes) st |= ST_ARG;
         else if ((int64_t)jb.h0 + (int64_t)max_score * jb.qlen > kPackedHMax || jb.qlen > qcap_limit)
@@ -238,7 +243,8 @@ size_t chunk_scratch_bytes(int nchunks) { return sizeof(uint32_t) * (3 * (size_t
 // scratch layout: hist[nbins] | base[nbins] | cursor[nbins] | info[4] | bounds[nchunks+1] |
 // lowest job index per chunk[nchunks] | highest[nchunks]
 cudaError_t launch_chunk_prep(const fa_job *d_jobs, uint32_t n, uint64_t qbytes, uint64_t tbytes, const ChunkEnds &ends,
-                              int nchunks, int max_score, int qcap_limit, uint32_t *d_scratch, cudaStream_t s)
+                              int nchunks, int max_score, int h0_min, int qcap_limit, uint32_t *d_scratch,
+                              cudaStream_t s)
 {
     if (nchunks < 1 || nchunks > kMaxChunks) return cudaErrorInvalidValue;
     const size_t nbins = (size_t)nchunks * kChunkBins;
@@ -252,7 +258,7 @@ cudaError_t launch_chunk_prep(const fa_job *d_jobs, uint32_t n, uint64_t qbytes,
     if (e == cudaSuccess) e = cudaMemsetAsync(info + 4 + 2 * nchunks + 1, 0, sizeof(uint32_t) * nchunks, s);
     if (e != cudaSuccess || n == 0) return e;
     chunk_prep_kernel<<<(n + 255) / 256, 256, 0, s>>>(d_jobs, n, qbytes, tbytes, ends, nchunks, max_score,
-                                                      qcap_limit, hist, info);
+                                                      h0_min, qcap_limit, hist, info);
     chunk_scan_kernel<<<1, 1024, 0, s>>>(hist, (int)nbins, d_scratch + nbins, nchunks, info + 4);
     return cudaGetLastError();
 }

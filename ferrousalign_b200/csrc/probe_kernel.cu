@@ -1,9 +1,11 @@
 // probe_kernel.cu -- integer / DPX instruction-throughput probe.
 //
 // The roofline of the DP kernels is the SM integer pipe, for which no measured peak
-// exists on this hardware; this probe measures it.  Each thread keeps 8 independent
-// accumulator chains and applies one instruction kind per step, so the issue rate,
-// not latency, bounds the run.
+// exists on this hardware; this probe measures it.  Each thread keeps 32 independent
+// accumulator chains and applies one instruction kind to all of them four times per loop
+// iteration (128 instructions of the measured kind against one add, compare and branch
+// of loop control), with no other ALU work in the loop, so the issue rate of that one
+// instruction kind, not latency or bookkeeping, bounds the run.
 
 #include <cstdio>
 
@@ -11,26 +13,32 @@
 
 namespace fa {
 
+constexpr int kProbeChains = 32;
+constexpr int kProbeUnroll = 4;
+
 template <int KIND>
 __global__ void __launch_bounds__(256) probe_kernel(uint32_t b, uint32_t c, int iters, uint32_t *sink)
 {
-    uint32_t acc[8];
+    uint32_t acc[kProbeChains];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) acc[k] = threadIdx.x * 2654435761u + k * 40503u + blockIdx.x;
+    for (int k = 0; k < kProbeChains; ++k) acc[k] = threadIdx.x * 2654435761u + k * 40503u + blockIdx.x;
+#pragma unroll 1
     for (int it = 0; it < iters; ++it) {
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            if (KIND == 0) acc[k] = __viaddmax_s16x2_relu(acc[k], b, c);
-            else if (KIND == 1) acc[k] = __vimax3_s16x2_relu(acc[k], b, c);
-            else if (KIND == 2) acc[k] = (uint32_t)__viaddmax_s32_relu((int)acc[k], (int)b, (int)c);
-            else if (KIND == 3) acc[k] = (uint32_t)__vimax3_s32((int)acc[k], (int)b, (int)c);
-            else acc[k] = (uint32_t)max((int)acc[k] + (int)b, (int)c);
+        for (int u = 0; u < kProbeUnroll; ++u) {
+#pragma unroll
+            for (int k = 0; k < kProbeChains; ++k) {
+                if (KIND == 0) acc[k] = __viaddmax_s16x2_relu(acc[k], b, c);
+                else if (KIND == 1) acc[k] = __vimax3_s16x2_relu(acc[k], b, c);
+                else if (KIND == 2) acc[k] = (uint32_t)__viaddmax_s32_relu((int)acc[k], (int)b, (int)c);
+                else if (KIND == 3) acc[k] = (uint32_t)__vimax3_s32((int)acc[k], (int)b, (int)c);
+                else acc[k] = (uint32_t)max((int)acc[k] + (int)b, (int)c);
+            }
         }
-        b ^= acc[it & 7] & 1u;   // keeps the operands live without a long dependency
     }
     uint32_t x = 0;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) x ^= acc[k];
+    for (int k = 0; k < kProbeChains; ++k) x ^= acc[k];
     if (x == 0x9e3779b9u) sink[0] = x;
 }
 
@@ -40,7 +48,7 @@ double probe_int_peak(int kind, int sm_count, cudaStream_t s, float *ms_out)
 {
     uint32_t *sink = nullptr;
     if (cudaMalloc(&sink, 4) != cudaSuccess) return -1.0;
-    const int iters = 4096, threads = 256, blocks = sm_count * 8;
+    const int iters = 1024, threads = 256, blocks = sm_count * 8;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -69,7 +77,7 @@ double probe_int_peak(int kind, int sm_count, cudaStream_t s, float *ms_out)
     cudaFree(sink);
     if (cudaGetLastError() != cudaSuccess) return -1.0;
     if (ms_out) *ms_out = best;
-    const double ops = (double)blocks * threads * iters * 8.0 * (kind == 4 ? 2.0 : 1.0);
+    const double ops = (double)blocks * threads * iters * (kProbeChains * kProbeUnroll) * (kind == 4 ? 2.0 : 1.0);
     return ops / (best * 1e-3);
 }
 

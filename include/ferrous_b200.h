@@ -36,13 +36,25 @@ extern "C" {
  * (ksw_affine_gap.rs:990-997, 1042). */
 typedef struct {
     int8_t  mat[25];
-    int8_t  _pad[3];
+    uint8_t flags;      /* FA_PARAM_* (0 = ksw_extend2's own argument rules) */
+    int8_t  _pad[2];
     int32_t m;          /* alphabet size; must be 5 */
     int32_t o_del, e_del, o_ins, e_ins;
     int32_t zdrop;
     int32_t end_bonus;
     int32_t pen_clip5, pen_clip3;   /* carried for the region merge; unused by the DP */
 } fa_params;
+
+/* fa_params.flags.
+ * FA_PARAM_H0_ZERO: accept jobs with h0 == 0 and run the ksw_extend2 recurrence on them as
+ *   written, without its `assert!(h0 > 0)` (ksw_affine_gap.rs:968).  The reference's job
+ *   collection gives every right job h0 = 0 (collect_soa.rs:206), so a caller that hands
+ *   those batches over unchanged sets this flag.  With h0 = 0 the first row is all zero, so
+ *   every cell is 0 and the first row ends the run: score 0, qle = tle = 0, max_off 0, and
+ *   gscore = 0, gtle = 1 when the first row's band reaches the query end (qlen <= w + 1 after
+ *   the max_ins/max_del clamp), else gscore = -1, gtle = 0.  Without the flag h0 <= 0 is
+ *   FA_ERR_ARG, where ksw_extend2 panics.  Negative h0 is FA_ERR_ARG either way. */
+#define FA_PARAM_H0_ZERO 1u
 
 #define FA_DIR_LEFT  0
 #define FA_DIR_RIGHT 1
@@ -55,7 +67,7 @@ typedef struct {
     uint64_t t_off;     /* offset of the target in the target buffer */
     int32_t  qlen;      /* query_len                                  */
     int32_t  tlen;      /* ref_len                                    */
-    int32_t  h0;        /* initial score; must be > 0 (ksw_affine_gap.rs:968) */
+    int32_t  h0;        /* initial score; > 0 (ksw_affine_gap.rs:968), or 0 with FA_PARAM_H0_ZERO */
     int32_t  w;         /* band_width                                 */
     int32_t  dir;       /* FA_DIR_LEFT / FA_DIR_RIGHT                 */
     int32_t  _pad;
@@ -237,8 +249,9 @@ int fa_ctx_last_timing(fa_ctx *ctx, float *kernel_ms, int *launches);
  * It runs on the current device and on `stream` (a cudaStream_t; NULL = legacy default
  * stream) and returns once the results are in d_out, reporting kernel-detected
  * argument errors.  The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress) and caches it; make that first call before any stream
- * capture.  All calls share the one array: calls that overlap on the GPU (from several
+ * (cudaGetSymbolAddress) and caches it for the life of the process, which assumes the
+ * device's primary context (the runtime API's default) and no cudaDeviceReset between
+ * calls; make that first call before any stream capture.  All calls share the one array: calls that overlap on the GPU (from several
  * host threads or streams at once) race and must be serialised by the caller. */
 #define FA_NOALLOC_MAX_JOBS (1u << 18)
 int fa_ext_batch_device_noalloc(const fa_params *p, const fa_job *d_jobs, uint32_t n,

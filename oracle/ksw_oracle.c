@@ -61,7 +61,19 @@ int ora_ksw_extend2(int qlen, const uint8_t *query, int tlen, const uint8_t *tar
                     int w, int end_bonus, int zdrop, int h0,
                     fa_ext_result *out, ora_ext_trace *trace)
 {
-    if (h0 <= 0 || qlen <= 0 || tlen < 0 || m <= 0 || m > 5) return FA_ERR_ARG;
+    return ora_ksw_extend2_flags(qlen, query, tlen, target, m, mat, o_del, e_del, o_ins, e_ins, w, end_bonus,
+                                 zdrop, h0, 0, out, trace);
+}
+
+int ora_ksw_extend2_flags(int qlen, const uint8_t *query, int tlen, const uint8_t *target,
+                          int m, const int8_t *mat, int o_del, int e_del, int o_ins, int e_ins,
+                          int w, int end_bonus, int zdrop, int h0, unsigned flags,
+                          fa_ext_result *out, ora_ext_trace *trace)
+{
+    /* ksw_affine_gap.rs:968 asserts h0 > 0; FA_PARAM_H0_ZERO lifts that for h0 == 0 and the
+     * recurrence below then runs on h0 = 0 exactly as written */
+    if (h0 < 0 || (h0 == 0 && !(flags & FA_PARAM_H0_ZERO))) return FA_ERR_ARG;
+    if (qlen <= 0 || tlen < 0 || m <= 0 || m > 5) return FA_ERR_ARG;
     for (int j = 0; j < qlen; ++j) if (query[j] >= m) return FA_ERR_ARG;
     for (int i = 0; i < tlen; ++i) if (target[i] >= m) return FA_ERR_ARG;
 
@@ -515,9 +527,9 @@ typedef struct {
 static int run_ext(const fa_params *p, const fa_job *jb, const uint8_t *qseq, const uint8_t *tseq,
                    int w, fa_ext_result *o, ora_ext_trace *tr)
 {
-    return ora_ksw_extend2(jb->qlen, qseq + jb->q_off, jb->tlen, tseq + jb->t_off, p->m, p->mat,
-                           p->o_del, p->e_del, p->o_ins, p->e_ins, w, p->end_bonus, p->zdrop,
-                           jb->h0, o, tr);
+    return ora_ksw_extend2_flags(jb->qlen, qseq + jb->q_off, jb->tlen, tseq + jb->t_off, p->m, p->mat,
+                                 p->o_del, p->e_del, p->o_ins, p->e_ins, w, p->end_bonus, p->zdrop,
+                                 jb->h0, p->flags, o, tr);
 }
 
 /* Smallest band of the ladder 1, 2, 3, 4, 6, 8, 12, 16, ... (2^k, 3*2^(k-1)) >= b. */

@@ -49,6 +49,12 @@ int ora_ksw_extend2(int qlen, const uint8_t *query, int tlen, const uint8_t *tar
                     int m, const int8_t *mat, int o_del, int e_del, int o_ins, int e_ins,
                     int w, int end_bonus, int zdrop, int h0,
                     fa_ext_result *out, ora_ext_trace *trace);
+/* Same, with fa_params.flags: FA_PARAM_H0_ZERO accepts h0 == 0 and runs the recurrence on it
+ * as written (the reference's assert at ksw_affine_gap.rs:968 lifted). */
+int ora_ksw_extend2_flags(int qlen, const uint8_t *query, int tlen, const uint8_t *target,
+                          int m, const int8_t *mat, int o_del, int e_del, int o_ins, int e_ins,
+                          int w, int end_bonus, int zdrop, int h0, unsigned flags,
+                          fa_ext_result *out, ora_ext_trace *trace);
 
 /* ksw_align2 (ksw_affine_gap.rs:773-861) with the 128-bit striped engine the
  * reference instantiates it with (16 u8 lanes, 8 i16 lanes). */

@@ -33,6 +33,8 @@ def load() -> C.CDLL:
         P = C.c_void_p
         lib.ora_ksw_extend2.restype = C.c_int
         lib.ora_ksw_extend2.argtypes = [C.c_int, P, C.c_int, P, C.c_int, P] + [C.c_int] * 8 + [P, P]
+        lib.ora_ksw_extend2_flags.restype = C.c_int
+        lib.ora_ksw_extend2_flags.argtypes = [C.c_int, P, C.c_int, P, C.c_int, P] + [C.c_int] * 8 + [C.c_uint, P, P]
         lib.ora_ksw_align2.restype = C.c_int
         lib.ora_ksw_align2.argtypes = [C.c_int, P, C.c_int, P, C.c_int, P] + [C.c_int] * 4 + [C.c_uint32, P, P]
         lib.ora_ext_batch.restype = C.c_int
@@ -57,13 +59,14 @@ def _codes(x):
     return np.ascontiguousarray(x, dtype=np.uint8)
 
 
-def ksw_extend2(query, target, mat, o_del, e_del, o_ins, e_ins, w, end_bonus, zdrop, h0):
+def ksw_extend2(query, target, mat, o_del, e_del, o_ins, e_ins, w, end_bonus, zdrop, h0, flags: int = 0):
+    """flags: fa_params.flags (1 = FA_PARAM_H0_ZERO: h0 == 0 runs as written)."""
     q, t = _codes(query), _codes(target)
     m = np.ascontiguousarray(mat, dtype=np.int8)
     out = np.zeros(1, EXT_RESULT_DT)
     tr = np.zeros(1, TRACE_DT)
-    rc = load().ora_ksw_extend2(len(q), _p(q), len(t), _p(t), 5, _p(m), o_del, e_del, o_ins, e_ins, w,
-                                end_bonus, zdrop, h0, _p(out), _p(tr))
+    rc = load().ora_ksw_extend2_flags(len(q), _p(q), len(t), _p(t), 5, _p(m), o_del, e_del, o_ins, e_ins, w,
+                                      end_bonus, zdrop, h0, flags, _p(out), _p(tr))
     if rc:
         raise ValueError(f"oracle ksw_extend2 rejected the input ({rc})")
     return out[0], tr[0]

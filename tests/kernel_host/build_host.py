@@ -1,6 +1,6 @@
 """Builds the test harnesses that compile extension kernels' thread bodies for the host
-(nvcc, no GPU needed): libpair_host.so (two jobs per thread) and librows2_host.so (two
-target rows per thread)."""
+(nvcc, no GPU needed): libpair_host.so (two jobs per thread), librows2_host.so (two
+target rows per thread) and liborder_host.so (the job-ordering bin mapping)."""
 import subprocess
 from pathlib import Path
 
@@ -11,6 +11,7 @@ HARNESSES = {
     "pair": (HERE / "pair_host.cu", [CSRC / "extend_pair_kernel.cu"]),
     "rows2": (HERE / "rows2_host.cu",
               [CSRC / "extend_kernel.cu", CSRC / "extend_pair_kernel.cu", CSRC / "extend_rows2_kernel.cu"]),
+    "order": (HERE / "order_host.cu", [CSRC / "order_kernel.cu"]),
 }
 
 

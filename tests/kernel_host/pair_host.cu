@@ -18,6 +18,7 @@ extern "C" int pair_host_run(const fa_params *prm, const fa_job *jobs, const uin
     int ms = 0;
     for (int i = 0; i < 25; ++i) if (prm->mat[i] > ms) ms = prm->mat[i];
     k.max_score = ms;
+    k.flags = prm->flags;
     if (!fa::ext_pair_eligible(k)) return -1;
     return fa::ext_pair_host(jobs, order, n, qseq, tseq, k, qcap, out, status);
 }

@@ -31,6 +31,7 @@ extern "C" int rows2_host_run(const fa_params *prm, const fa_job *jobs, const ui
     int ms = 0;
     for (int i = 0; i < 25; ++i) if (prm->mat[i] > ms) ms = prm->mat[i];
     k.max_score = ms;
+    k.flags = prm->flags;
     if (!fa::ext_rows2_eligible(k, qcap) || (ring != 0 && ring != 32 && ring != 64)) return -1;
     std::vector<uint16_t> eh((size_t)(ring > 0 ? ring : qcap + 1));
     std::vector<uint8_t> sb((size_t)qcap + 1);

@@ -62,24 +62,6 @@ def test_first_band_rule(ctx):
         assert np.array_equal(band[clear], ref[clear])
 
 
-def test_first_band_rule(ctx):
-    rng = np.random.default_rng(9)
-    x = rng.normal(0.0, 1.0, size=(5000, 16)).astype(np.float32)
-    w = rng.normal(0.0, 0.3, M.NPARAMS).astype(np.float32)
-    w[M.O_B3] = 3.0                           # outputs spread over bands 1..2^9
-    m = B.BandModel.create(seed=3)
-    m.set(w=w, mean=x.mean(0), std=x.std(0))
-    jobs = np.zeros(len(x), N.JOB_DT)
-    jobs["w"] = rng.choice([20, 50, 100, 200], len(x))
-    for margin, w_min in ((0.0, 2), (0.5, 4), (-0.3, 1)):
-        y, band = m.predict(x, jobs=jobs, margin=margin, w_min=w_min, ctx=ctx)
-        ref = M.first_band(y, margin, w_min, jobs["w"])
-        e = np.clip(y.astype(np.float64) + margin, 0, 16)
-        clear = np.abs(np.exp2(e) - np.round(np.exp2(e))) > 1e-3     # away from integer boundaries
-        assert clear.mean() > 0.9
-        assert np.array_equal(band[clear], ref[clear])
-
-
 def test_training_reduces_loss_and_file_round_trip(ctx, tmp_path):
     rng = np.random.default_rng(5)
     x = rng.normal(0.0, 1.0, size=(20000, 16)).astype(np.float32)

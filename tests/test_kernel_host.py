@@ -246,3 +246,80 @@ def test_rows2_certificate_uneven_parameters(rows2_lib, a, b_, n, gaps, zdrop):
     for ring, cap in ((0, 100), (32, 14), (64, 30)):
         w_try = rng.integers(1, cap + 1, size=len(bt.jobs)).astype(np.int32)
         check_rows2_cert(rows2_lib, sw.to_struct(), bt.jobs, bt.qseq, bt.tseq, w_try, ring)
+
+
+# ---- job ordering (order_kernel.cu): the bin mapping shared by histogram and scatter
+
+
+@pytest.fixture(scope="module")
+def order_lib(built):
+    import build_host
+    lib = C.CDLL(str(build_host.build("order")))
+    lib.order_host_bin.restype = C.c_int
+    lib.order_host_bin.argtypes = [C.c_int]
+    lib.order_host_run.restype = C.c_int
+    lib.order_host_run.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
+    return lib
+
+
+def test_order_bins_clamp_invalid_lengths(order_lib):
+    """A live job with a negative query length lands in bin 0 (never bin -1, which would
+    step a cursor before the histogram), an oversized one in the last bin."""
+    assert order_lib.order_host_bin(-1) == 0
+    assert order_lib.order_host_bin(-(2 ** 31)) == 0
+    assert order_lib.order_host_bin(0) == 0
+    assert order_lib.order_host_bin(151) == 151
+    assert order_lib.order_host_bin(N.FA_MAX_QLEN) == N.FA_MAX_QLEN
+    assert order_lib.order_host_bin(N.FA_MAX_QLEN + 1) == N.FA_MAX_QLEN
+    assert order_lib.order_host_bin(2 ** 31 - 1) == N.FA_MAX_QLEN
+
+
+def test_order_scatter_writes_every_slot_once(order_lib):
+    rng = np.random.default_rng(5)
+    q = rng.integers(1, 300, 5000).astype(np.int32)
+    q[rng.choice(5000, 60, replace=False)] = rng.choice([-1, 0, -7, N.FA_MAX_QLEN + 5, -(2 ** 31)], 60)
+    order = np.full(len(q), 0xFFFFFFFF, np.uint32)
+    assert order_lib.order_host_run(q.ctypes.data, len(q), order.ctypes.data) == 0
+    assert sorted(order.tolist()) == list(range(len(q)))
+    b = np.clip(q[order], 0, N.FA_MAX_QLEN)
+    assert np.all(b[:-1] >= b[1:])            # longest first
+
+
+# ---- h0 = 0 under FA_PARAM_H0_ZERO: the kernels' closed form against the recurrence
+
+
+def test_h0_zero_closed_form_matches_recurrence(rows2_lib, host_lib):
+    """The oracle runs ksw_extend2's recurrence on h0 = 0 as written; the two-row kernel's
+    thread body writes the closed form (all cells zero after row 0).  Same six fields and
+    cell counts, over lengths and bands where row 0 does and does not reach the query end."""
+    rng = np.random.default_rng(11)
+    n = 400
+    qlen = rng.integers(1, 200, n).astype(np.int32)
+    tlen = rng.integers(0, 260, n).astype(np.int32)
+    w = rng.integers(0, 150, n).astype(np.int32)
+    qs = rng.integers(0, 5, int(qlen.sum())).astype(np.uint8)
+    ts = rng.integers(0, 5, int(tlen.sum()) + 1).astype(np.uint8)
+    jobs = np.zeros(n, N.JOB_DT)
+    jobs["q_off"] = np.concatenate([[0], np.cumsum(qlen)[:-1]])
+    jobs["t_off"] = np.concatenate([[0], np.cumsum(tlen)[:-1]])
+    jobs["qlen"], jobs["tlen"], jobs["w"], jobs["dir"] = qlen, tlen, w, N.FA_DIR_RIGHT
+    jobs["h0"] = np.where(rng.random(n) < 0.7, 0, rng.integers(1, 40, n))
+    p = fa.BandedPairWiseSW(allow_h0_zero=True).to_struct()
+    ref, tr = O.ext_batch(p, jobs, qs, ts)
+    out, cells, st, ovf, flags = run_rows2(rows2_lib, p, jobs, qs, ts)
+    assert st == 0 and len(ovf) == 0
+    assert np.array_equal(out, ref), np.nonzero(out != ref)[0][:10]
+    assert np.array_equal(cells.astype(np.int64), tr["cells"])
+    pout, pst = run_host(host_lib, p, jobs, qs, ts)          # two jobs per thread
+    assert pst == 0 and np.array_equal(pout, ref), np.nonzero(pout != ref)[0][:10]
+    z = jobs["h0"] == 0
+    assert np.all(out["score"][z] == 0) and np.all(out["max_off"][z] == 0)
+    assert set(out["gscore"][z].tolist()) == {-1, 0}
+
+
+def test_h0_zero_rejected_without_the_flag():
+    p = fa.BandedPairWiseSW().to_struct()
+    with pytest.raises(ValueError):
+        O.ksw_extend2([0, 1, 2], [0, 1, 2], p["mat"][0], 6, 1, 6, 1, 100, 5, 100, 0)
+    r, _ = O.ksw_extend2([0, 1, 2], [0, 1, 2], p["mat"][0], 6, 1, 6, 1, 100, 5, 100, 0, flags=N.FA_PARAM_H0_ZERO)
+    assert (int(r["score"]), int(r["qle"]), int(r["tle"]), int(r["gtle"]), int(r["gscore"])) == (0, 0, 0, 1, 0)
