@@ -249,6 +249,66 @@ def bench_learned(args, ctx, b, p):
             "identical_frac": float(np.mean(plain == learned))}
 
 
+def pin_array(a):
+    """A page-locked copy of a numpy array (same dtype and shape)."""
+    import torch
+    a = np.ascontiguousarray(a)
+    return torch.from_numpy(a.view(np.uint8).reshape(-1)).pin_memory().numpy().view(a.dtype).reshape(a.shape)
+
+
+def bench_e2e_forms(args, ctx, b, p):
+    """End to end through the host ABI, on the 1M-job batch: the call a user makes, from
+    page-locked host buffers (jobs, sequences, hints) into a page-locked result buffer, with
+    every copy inside the timed call, in wall-clock milliseconds (median over the steps).
+    Forms: byte-code buffers (the drop-in for execute_batch_simd_scoring) and 2-bit packed
+    buffers; the single-band call, the bwa-mem2 retry policy and the learned band.  Host-side
+    packing is not timed (a packed caller holds packed sequences, as the reference's index
+    holds its .pac)."""
+    import ferrousalign_b200 as fa
+    from ferrousalign_b200 import _native as N
+    from ferrousalign_b200 import band_model as B
+    n = len(b.jobs)
+    bwa = fa.make_policy(N.FA_POLICY_BWA, 2)
+    model = B.BandModel.load()
+    hints = pin_array(B.hints_from_info(b.info))
+    pj, pq, pt = pin_array(b.jobs), pin_array(b.qseq), pin_array(b.tseq)
+    qp, tp = fa.pack(b.qseq).pinned(), fa.pack(b.tseq).pinned()
+    out_h = pin_array(np.zeros(n, N.EXT_RESULT_DT))
+    byte_in = int(pj.nbytes + pq.nbytes + pt.nbytes)
+    pack_in = int(pj.nbytes + qp.nbytes + tp.nbytes)
+    hint_in = int(hints.nbytes)
+    forms = {
+        "bytes_single": (lambda: fa.extend_batch(p, pj, pq, pt, ctx=ctx, out=out_h), byte_in),
+        "packed_single": (lambda: fa.extend_batch_packed(p, pj, qp, tp, ctx=ctx, out=out_h), pack_in),
+        "bytes_bwa": (lambda: fa.extend_batch(p, pj, pq, pt, policy=bwa, ctx=ctx, out=out_h), byte_in),
+        "packed_bwa": (lambda: fa.extend_batch_packed(p, pj, qp, tp, policy=bwa, ctx=ctx, out=out_h), pack_in),
+        "bytes_learned": (lambda: B.extend_batch_learned(p, pj, pq, pt, model, hints=hints, ctx=ctx, out=out_h),
+                          byte_in + hint_in),
+        "packed_learned": (lambda: fa.extend_batch_learned_packed(p, pj, qp, tp, model, hints=hints, ctx=ctx,
+                                                                  out=out_h), pack_in + hint_in),
+    }
+    res, outs = {}, {}
+    for name, (fn, h2d) in forms.items():
+        for _ in range(max(2, args.warmup)):
+            fn()
+        t = []
+        for _ in range(max(5, args.steps // 2)):
+            t0 = time.perf_counter()
+            fn()
+            t.append((time.perf_counter() - t0) * 1e3)
+        outs[name] = out_h.copy()
+        ms = float(np.median(t))
+        res[name] = {"value": n / (ms * 1e-3), "unit": "alignments/s", "ms_per_step": ms,
+                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": n * 24}
+    res["identical_outputs"] = bool(all(np.array_equal(outs[k], outs["bytes_bwa"])
+                                        for k in ("packed_bwa", "bytes_learned", "packed_learned")) and
+                                    np.array_equal(outs["packed_single"], outs["bytes_single"]))
+    res["learned_vs_bwa_packed"] = res["packed_bwa"]["ms_per_step"] / res["packed_learned"]["ms_per_step"]
+    res["learned_vs_single_packed"] = res["packed_single"]["ms_per_step"] / res["packed_learned"]["ms_per_step"]
+    res["learned_vs_bwa_bytes"] = res["bytes_bwa"]["ms_per_step"] / res["bytes_learned"]["ms_per_step"]
+    return res
+
+
 def bench_uneven(args, ctx, p):
     """Uneven-length batch: 2,000,000 mixed left and right extensions, reads 50-300 bp,
     seeds anywhere in the read, targets from a 100 Mbp reference with 5% low-complexity
@@ -886,6 +946,9 @@ def main():
     }
     if not args.skip_learned:
         line["learned_band"] = bench_learned(args, ctx, b, p)
+        forms = bench_e2e_forms(args, ctx, b, p)
+        line["learned_band"]["e2e"] = forms
+        line["e2e_packed"] = dict(forms["packed_single"], entry="fa_ext_batch_packed (2-bit packed host buffers)")
     if not args.skip_mate:
         line["mate_rescue"] = bench_mate(args, ctx, lib, dev, stream, flush, skip_cpu=args.skip_cpu)
     if not args.skip_mate and not args.skip_learned and not args.skip_mixed:

@@ -69,6 +69,10 @@ RESCUE_OPTS_DT = np.dtype([("pen_unpaired", "<i4"), ("max_matesw", "<i4"), ("min
 RESCUE_JOB_INFO_DT = np.dtype([("cand", "<u4"), ("orientation", "<i4"), ("is_rev", "<i4"), ("rid", "<i4"),
                                ("adj_rb", "<i8"), ("adj_re", "<i8")])
 
+NRUN_DT = np.dtype([("pos", "<u8"), ("len", "<u8")])
+PACKED_SEQ_DT = np.dtype([("bases", "<u8"), ("n_bases", "<u8"), ("n_runs", "<u8"), ("n_nruns", "<u8")])
+
+assert NRUN_DT.itemsize == 16 and PACKED_SEQ_DT.itemsize == 32
 assert PARAMS_DT.itemsize == 64 and JOB_DT.itemsize == 40 and EXT_RESULT_DT.itemsize == 24
 assert STATS_DT.itemsize == 40 and MATE_PARAMS_DT.itemsize == 48 and MATE_JOB_DT.itemsize == 32
 assert KSWR_DT.itemsize == 28
@@ -94,6 +98,8 @@ SIGNATURES = {
     "fa_ext_batch_policy": (C.c_int, [_P, _P, _P, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64,
                                       _P, _P, _P, _P]),
     "fa_ext_batch_device": (C.c_int, [_P, _P, _P, C.c_uint32, _P, _P, _P, _P, _P]),
+    "fa_ext_batch_packed": (C.c_int, [_P, _P, _P, _P, C.c_uint32, _P, _P, _P, _P, _P, _P]),
+    "fa_ext_batch_packed_device": (C.c_int, [_P, _P, _P, C.c_uint32, _P, _P, _P, _P, _P]),
     "fa_ctx_sync": (C.c_int, [_P]),
     "fa_ctx_set_timing": (C.c_int, [_P, C.c_int]),
     "fa_ctx_set_kernel": (C.c_int, [_P, C.c_int]),
@@ -118,6 +124,8 @@ SIGNATURES = {
     "fa_band_train": (C.c_int, [_P, _P, _P, _P, C.c_uint32, C.c_int, C.c_uint32, C.c_float, C.c_float, C.c_uint64, _P]),
     "fa_ext_batch_learned": (C.c_int, [_P, _P, _P, _P, C.c_float, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64,
                                        _P, _P, _P, _P, _P]),
+    "fa_ext_batch_learned_packed": (C.c_int, [_P, _P, _P, _P, C.c_float, _P, C.c_uint32, _P, _P, _P, _P, _P, _P,
+                                              _P]),
     "fa_mate_sw_batch": (C.c_int, [_P, _P, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64, _P, _P]),
     "fa_collect_ext_jobs": (C.c_int, [_P, _P, _P, C.c_uint64, _P, _P, C.c_uint32, _P, C.c_uint32, _P, C.c_uint32,
                                       _P, _P, _P, _P, C.c_uint64, _P, _P, _P, _P]),

@@ -148,14 +148,16 @@ def make_labels(params: np.ndarray, jobs: np.ndarray, qseq: np.ndarray, tseq: np
 
 def extend_batch_learned(params: np.ndarray, jobs: np.ndarray, qseq: np.ndarray, tseq: np.ndarray,
                          model: BandModel, hints: np.ndarray | None = None, judge: int = JUDGE_LEARNED,
-                         margin: float = 0.0, w_min: int = 2, max_tries: int = 2, ctx: N.Context | None = None):
+                         margin: float = 0.0, w_min: int = 2, max_tries: int = 2, ctx: N.Context | None = None,
+                         out: np.ndarray | None = None):
     """fa_ext_batch_learned: predicted first band, judge, doubling up to job.w, then the
-    bwa-mem2 policy.  Returns (results, stats, w_first, w_final)."""
+    bwa-mem2 policy.  Returns (results, stats, w_first, w_final); `out` may be a (pinned)
+    result buffer to fill."""
     from .batch_extension import make_policy
     ctx = ctx or N.default_context()
     jobs = np.ascontiguousarray(jobs, N.JOB_DT)
     n = len(jobs)
-    out = np.zeros(n, N.EXT_RESULT_DT)
+    out = np.zeros(n, N.EXT_RESULT_DT) if out is None else out
     stats = np.zeros(1, N.STATS_DT)
     wf = np.zeros(n, np.int32)
     wfin = np.zeros(n, np.int32)

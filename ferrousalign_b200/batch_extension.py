@@ -156,15 +156,16 @@ def make_policy(mode: int = N.FA_POLICY_SINGLE, max_tries: int = 2, judge: int =
 
 def extend_batch(params: np.ndarray, jobs: np.ndarray, qseq: np.ndarray, tseq: np.ndarray,
                  policy: np.ndarray | None = None, w_first: np.ndarray | None = None,
-                 ctx: N.Context | None = None):
-    """Array-level call of fa_ext_batch_policy.  Returns (results, stats, w_final)."""
+                 ctx: N.Context | None = None, out: np.ndarray | None = None):
+    """Array-level call of fa_ext_batch_policy.  Returns (results, stats, w_final); `out`
+    may be a (pinned) result buffer to fill."""
     lib = N.load()
     ctx = ctx or N.default_context()
     jobs = np.ascontiguousarray(jobs, dtype=N.JOB_DT)
     qseq = np.ascontiguousarray(qseq, dtype=np.uint8)
     tseq = np.ascontiguousarray(tseq, dtype=np.uint8)
     n = len(jobs)
-    out = np.zeros(n, dtype=N.EXT_RESULT_DT)
+    out = np.zeros(n, dtype=N.EXT_RESULT_DT) if out is None else out
     stats = np.zeros(1, dtype=N.STATS_DT)
     w_final = np.zeros(n, dtype=np.int32)
     wf = None if w_first is None else np.ascontiguousarray(w_first, dtype=np.int32)

@@ -169,7 +169,8 @@ int fa_band_features(fa_ctx *ctx, const fa_params *p, const fa_job *jobs, uint32
     BA_CUDA(cudaMemcpy(dq.p, qseq, qseq_len, cudaMemcpyHostToDevice));
     BA_CUDA(cudaMemcpy(dt.p, tseq, tseq_len, cudaMemcpyHostToDevice));
     if (hints) BA_CUDA(cudaMemcpy(dh.p, hints, sizeof(fa_band_hint) * (size_t)n, cudaMemcpyHostToDevice));
-    BA_CUDA(launch_band_features(dj.as<fa_job>(), n, dq.as<uint8_t>(), qseq_len, dt.as<uint8_t>(), tseq_len,
+    BA_CUDA(launch_band_features(dj.as<fa_job>(), n, SeqBuf{dq.as<uint8_t>(), qseq_len, nullptr, 0, 0},
+                                 SeqBuf{dt.as<uint8_t>(), tseq_len, nullptr, 0, 0},
                                  hints ? dh.as<fa_band_hint>() : nullptr, ms, dx.as<float>(), 0));
     BA_CUDA(cudaMemcpy(x, dx.p, sizeof(float) * 16 * (size_t)n, cudaMemcpyDeviceToHost));
     return FA_OK;

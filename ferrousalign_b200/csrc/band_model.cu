@@ -52,12 +52,18 @@ __device__ __forceinline__ uint32_t word_at(const uint8_t *__restrict__ base, lo
 
 __device__ __forceinline__ int last_byte(uint32_t m) { return (31 - __clz(m)) >> 3; }
 
+// PK: 2-bit packed sequences, read through PackedReader (positions outside the job come
+// back as 0 there, where the byte form reads the neighbouring bytes; every use below masks
+// them, so the features are the same).
+template <bool PK>
 __global__ void __launch_bounds__(128) band_features_kernel(const fa_job *__restrict__ jobs, uint32_t n,
-                                                            const uint8_t *__restrict__ qseq, uint64_t qbytes,
-                                                            const uint8_t *__restrict__ tseq, uint64_t tbytes,
+                                                            const SeqBuf qs, const SeqBuf ts,
                                                             const fa_band_hint *__restrict__ hints, int max_score,
                                                             float *__restrict__ x)
 {
+    const uint8_t *__restrict__ qseq = qs.p;
+    const uint8_t *__restrict__ tseq = ts.p;
+    const uint64_t qbytes = qs.nbytes, tbytes = ts.nbytes;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const fa_job jb = jobs[i];
@@ -75,25 +81,37 @@ __global__ void __launch_bounds__(128) band_features_kernel(const fa_job *__rest
         last_s[s] = -1;
     }
     int mm = 0, last_mm = -1, nq = 0, mmblk = 0, first = -1, lastq = 0, best_run = 0, run = 0;
+    PackedReader qr, tr;
+    if (PK) {
+        qr.init(qs, jb.q_off, qlen);
+        tr.init(ts, jb.t_off, tlen);
+    }
     for (int k0 = 0; k0 < qlen; k0 += 16) {
         uint32_t q4[4], nm[4], t7[7];
-        {
-            const long long a = (long long)jb.q_off + k0, a0 = a & ~3LL;
-            const int sh = (int)(a - a0) * 8;
-            uint32_t w[5];
+        if (PK) {
 #pragma unroll
-            for (int m = 0; m < 5; ++m) w[m] = word_at(qseq, a0 + 4 * m, qbytes);
+            for (int m = 0; m < 4; ++m) q4[m] = qr.get4(k0 + 4 * m);
 #pragma unroll
-            for (int m = 0; m < 4; ++m) q4[m] = __funnelshift_r(w[m], w[m + 1], sh);
-        }
-        {
-            const long long a = (long long)jb.t_off + k0 - 4, a0 = a & ~3LL;   // target bytes k0-4 .. k0+23
-            const int sh = (int)(a - a0) * 8;
-            uint32_t w[8];
+            for (int m = 0; m < 7; ++m) t7[m] = tr.get4(k0 - 4 + 4 * m);   // target positions k0-4 .. k0+23
+        } else {
+            {
+                const long long a = (long long)jb.q_off + k0, a0 = a & ~3LL;
+                const int sh = (int)(a - a0) * 8;
+                uint32_t w[5];
 #pragma unroll
-            for (int m = 0; m < 8; ++m) w[m] = word_at(tseq, a0 + 4 * m, tbytes);
+                for (int m = 0; m < 5; ++m) w[m] = word_at(qseq, a0 + 4 * m, qbytes);
 #pragma unroll
-            for (int m = 0; m < 7; ++m) t7[m] = __funnelshift_r(w[m], w[m + 1], sh);
+                for (int m = 0; m < 4; ++m) q4[m] = __funnelshift_r(w[m], w[m + 1], sh);
+            }
+            {
+                const long long a = (long long)jb.t_off + k0 - 4, a0 = a & ~3LL;   // target bytes k0-4 .. k0+23
+                const int sh = (int)(a - a0) * 8;
+                uint32_t w[8];
+#pragma unroll
+                for (int m = 0; m < 8; ++m) w[m] = word_at(tseq, a0 + 4 * m, tbytes);
+#pragma unroll
+                for (int m = 0; m < 7; ++m) t7[m] = __funnelshift_r(w[m], w[m + 1], sh);
+            }
         }
         uint32_t dmask[4];
 #pragma unroll
@@ -171,13 +189,14 @@ __global__ void __launch_bounds__(128) band_features_kernel(const fa_job *__rest
     for (int k = 0; k < 4; ++k) xo[k] = make_float4(o[4 * k], o[4 * k + 1], o[4 * k + 2], o[4 * k + 3]);
 }
 
-cudaError_t launch_band_features(const fa_job *d_jobs, uint32_t n, const uint8_t *d_q, uint64_t qbytes,
-                                 const uint8_t *d_t, uint64_t tbytes, const fa_band_hint *d_hints, int max_score,
-                                 float *d_x, cudaStream_t s)
+cudaError_t launch_band_features(const fa_job *d_jobs, uint32_t n, const SeqBuf &d_q, const SeqBuf &d_t,
+                                 const fa_band_hint *d_hints, int max_score, float *d_x, cudaStream_t s)
 {
     if (n == 0) return cudaSuccess;
-    band_features_kernel<<<(n + 127) / 128, 128, 0, s>>>(d_jobs, n, d_q, qbytes, d_t, tbytes, d_hints, max_score,
-                                                         d_x);
+    if (d_q.packed)
+        band_features_kernel<true><<<(n + 127) / 128, 128, 0, s>>>(d_jobs, n, d_q, d_t, d_hints, max_score, d_x);
+    else
+        band_features_kernel<false><<<(n + 127) / 128, 128, 0, s>>>(d_jobs, n, d_q, d_t, d_hints, max_score, d_x);
     return cudaGetLastError();
 }
 

@@ -19,6 +19,7 @@
 #include "fa_cert.cuh"
 #include "fa_device.cuh"
 #include "fa_kernels.h"
+#include "fa_packed.cuh"
 
 namespace fa {
 
@@ -37,11 +38,12 @@ __device__ __forceinline__ int32_t prmt_s8(uint32_t lo, uint32_t hi, uint32_t se
 // times the resident warps.  Columns entering the ring get their query code explicitly,
 // and a column the rows grow into after a trim gets the value the full array would
 // hold there: 0 once written (trimmed cells are zero), its first-row value if never.
-template <bool CERT, int RING, int TPB>
+// PK: the sequences are 2-bit packed (SeqBuf.packed), read 16 bases per word load.
+template <bool CERT, int RING, int TPB, bool PK>
 __global__ void __launch_bounds__(TPB)
 ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ order,
                   uint32_t n, const uint32_t *__restrict__ first_dev, const uint32_t *__restrict__ n_dev,
-                  const uint8_t *__restrict__ qseq, const uint8_t *__restrict__ tseq, const ExtParams p, int qcap,
+                  const SeqBuf qs, const SeqBuf ts, const ExtParams p, int qcap,
                   const int32_t *__restrict__ w_try, fa_ext_result *__restrict__ out,
                   uint8_t *__restrict__ clamped_out, uint32_t *__restrict__ cells_job,
                   unsigned long long *__restrict__ cells_out, uint32_t *__restrict__ status)
@@ -75,8 +77,24 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
         } else {
             const int oe_del = p.o_del + p.e_del, oe_ins = p.o_ins + p.e_ins;
             const int e_del = p.e_del, e_ins = p.e_ins;
-            const uint8_t *Q = qseq + jb.q_off;
-            const uint8_t *Tg = tseq + jb.t_off;
+            const uint8_t *Q = qs.p + jb.q_off;    // byte codes (PK false)
+            const uint8_t *Tg = ts.p + jb.t_off;
+            PackedReader qr, tr;                    // packed bases (PK true)
+            if (PK) {
+                qr.init(qs, jb.q_off, qlen);
+                tr.init(ts, jb.t_off, tlen);
+            }
+            // eight query codes from column j0 on (0 past the query)
+            auto load8 = [&](int j0, uint32_t *qb) {
+                if (PK) {
+                    const uint32_t lo = qr.get4(j0), hi = qr.get4(j0 + 4);
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) qb[u] = ((u < 4 ? lo : hi) >> (8 * (u & 3))) & 0xFFu;
+                } else {
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) qb[u] = j0 + u < qlen ? (uint32_t)Q[j0 + u] : 0u;
+                }
+            };
             // scoring rows as PRMT tables, indexed only with constants
             uint32_t rlo[5], rhi[5];
 #pragma unroll
@@ -97,8 +115,7 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
                 init_reach = h0 <= oe_ins ? 0 : (e_ins == 0 ? qlen : min(qlen, 1 + (h0 - oe_ins - 1) / e_ins));
                 for (int j0 = 0; j0 < qlen; j0 += 8) {
                     uint32_t qb[8];
-#pragma unroll
-                    for (int u = 0; u < 8; ++u) qb[u] = j0 + u < qlen ? (uint32_t)Q[j0 + u] : 0u;
+                    load8(j0, qb);
                     uint32_t word = 0;
 #pragma unroll
                     for (int u = 0; u < 8; ++u) {
@@ -114,8 +131,7 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
             // eight independent byte loads in flight per thread before their first use
             for (int j0 = 0; RING == 0 && j0 <= qlen; j0 += 8) {
                 uint32_t qb[8];
-#pragma unroll
-                for (int u = 0; u < 8; ++u) qb[u] = j0 + u < qlen ? (uint32_t)Q[j0 + u] : 0u;
+                load8(j0, qb);
 #pragma unroll
                 for (int u = 0; u < 8; ++u) {
                     const int j = j0 + u;
@@ -150,10 +166,15 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
             // target bases arrive 5 to 8 rows ahead of their row: tq0 holds the current
             // group of four, tq1 the next, loaded when tq0 is used up
             uint32_t tq0 = 0, tq1 = 0;
+            if (PK) {
+                tq0 = tr.get4(0);
+                tq1 = tr.get4(4);
+            } else {
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                if (k < tlen) tq0 |= (uint32_t)Tg[k] << (8 * k);
-                if (4 + k < tlen) tq1 |= (uint32_t)Tg[4 + k] << (8 * k);
+                for (int k = 0; k < 4; ++k) {
+                    if (k < tlen) tq0 |= (uint32_t)Tg[k] << (8 * k);
+                    if (4 + k < tlen) tq1 |= (uint32_t)Tg[4 + k] << (8 * k);
+                }
             }
             for (int i = 0; i < tlen; ++i) {
                 const uint32_t tb = tq0 & 0xFFu;
@@ -161,9 +182,13 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
                 if ((i & 3) == 3) {
                     tq0 = tq1;
                     tq1 = 0;
+                    if (PK) {
+                        tq1 = tr.get4(i + 5);
+                    } else {
 #pragma unroll
-                    for (int k = 0; k < 4; ++k)
-                        if (i + 5 + k < tlen) tq1 |= (uint32_t)Tg[i + 5 + k] << (8 * k);
+                        for (int k = 0; k < 4; ++k)
+                            if (i + 5 + k < tlen) tq1 |= (uint32_t)Tg[i + 5 + k] << (8 * k);
+                    }
                 }
                 if (tb >= (uint32_t)p.m) { bad = 1; break; }
                 uint32_t row_lo = rlo[0], row_hi = rhi[0];
@@ -338,16 +363,25 @@ size_t ext_packed_smem_bytes(int qcap, int ring, int tpb) {
 namespace {
 template <bool CERT, int RING, int TPB>
 cudaError_t launch_variant(size_t smem, cudaStream_t stream, const fa_job *d_jobs, const uint32_t *d_order,
-                           uint32_t n, const uint32_t *d_first, const uint32_t *d_n, const uint8_t *d_qseq,
-                           const uint8_t *d_tseq, const ExtParams &p, int qcap, const int32_t *d_w_try,
+                           uint32_t n, const uint32_t *d_first, const uint32_t *d_n, const SeqBuf &d_qseq,
+                           const SeqBuf &d_tseq, const ExtParams &p, int qcap, const int32_t *d_w_try,
                            fa_ext_result *d_out, uint8_t *d_clamped, uint32_t *d_cells_job,
                            unsigned long long *d_cells, uint32_t *d_status)
 {
-    cudaError_t err = cudaFuncSetAttribute(ext_packed_kernel<CERT, RING, TPB>,
+    if (d_qseq.packed) {
+        cudaError_t err = cudaFuncSetAttribute(ext_packed_kernel<CERT, RING, TPB, true>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (err != cudaSuccess) return err;
+        ext_packed_kernel<CERT, RING, TPB, true><<<(n + TPB - 1) / TPB, TPB, smem, stream>>>(
+            d_jobs, d_order, n, d_first, d_n, d_qseq, d_tseq, p, qcap, d_w_try, d_out, d_clamped, d_cells_job,
+            d_cells, d_status);
+        return cudaGetLastError();
+    }
+    cudaError_t err = cudaFuncSetAttribute(ext_packed_kernel<CERT, RING, TPB, false>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return err;
     const uint32_t blocks = (n + TPB - 1) / TPB;
-    ext_packed_kernel<CERT, RING, TPB><<<blocks, TPB, smem, stream>>>(
+    ext_packed_kernel<CERT, RING, TPB, false><<<blocks, TPB, smem, stream>>>(
         d_jobs, d_order, n, d_first, d_n, d_qseq, d_tseq, p, qcap, d_w_try, d_out, d_clamped, d_cells_job,
         d_cells, d_status);
     return cudaGetLastError();
@@ -355,8 +389,8 @@ cudaError_t launch_variant(size_t smem, cudaStream_t stream, const fa_job *d_job
 }  // namespace
 
 cudaError_t launch_ext_packed(const fa_job *d_jobs, const uint32_t *d_order, uint32_t n,
-                              const uint32_t *d_first, const uint32_t *d_n, const uint8_t *d_qseq,
-                              const uint8_t *d_tseq, const ExtParams &p, int qcap, int ring,
+                              const uint32_t *d_first, const uint32_t *d_n, const SeqBuf &d_qseq,
+                              const SeqBuf &d_tseq, const ExtParams &p, int qcap, int ring,
                               const int32_t *d_w_try, fa_ext_result *d_out, uint8_t *d_clamped, bool cert,
                               uint32_t *d_cells_job, unsigned long long *d_cells, uint32_t *d_status,
                               cudaStream_t stream, int tpb)

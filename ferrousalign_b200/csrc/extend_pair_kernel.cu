@@ -25,6 +25,7 @@
 
 #include "fa_device.cuh"
 #include "fa_kernels.h"
+#include "fa_packed.cuh"
 
 namespace fa {
 
@@ -458,11 +459,12 @@ bool ext_pair_eligible(const ExtParams &p) {
 }
 
 cudaError_t launch_ext_pair(const fa_job *d_jobs, const uint32_t *d_order, uint32_t n, const uint32_t *d_n,
-                            const uint8_t *d_qseq,
-                            const uint8_t *d_tseq, const ExtParams &p, int qcap, const int32_t *d_w_try,
+                            const SeqBuf &q, const SeqBuf &t, const ExtParams &p, int qcap, const int32_t *d_w_try,
                             fa_ext_result *d_out, uint8_t *d_clamped, uint32_t *d_cells_job,
                             unsigned long long *d_cells, uint32_t *d_status, cudaStream_t stream)
 {
+    if (q.packed || t.packed) return cudaErrorNotSupported;   // byte codes only
+    const uint8_t *d_qseq = q.p, *d_tseq = t.p;
     if (n == 0) return cudaSuccess;
     int n_code_t = 0;
     bool sym = false;

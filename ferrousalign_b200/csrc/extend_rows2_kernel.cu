@@ -27,6 +27,7 @@
 #include "fa_cert.cuh"
 #include "fa_device.cuh"
 #include "fa_kernels.h"
+#include "fa_packed.cuh"
 
 namespace fa {
 
@@ -89,10 +90,11 @@ constexpr int kRows2MaxQ = 254;   // u8 column words: h0 >= 1 and a >= 1 leave q
 // e_del == e_ins, so E and F open from one shared term.  CERT: also evaluates the exit-bound
 // certificate (flags bit 1) and its band hint (bits 2-7) exactly as the int32 kernel does.
 // Returns the cells the recurrence evaluated.
-template <int T, bool SYM, bool CERT, int RING>
+// PK: the sequences are 2-bit packed (SeqBuf.packed), read 16 bases per word load.
+template <int T, bool SYM, bool CERT, int RING, bool PK = false>
 __host__ __device__ __forceinline__ uint32_t rows2_thread(
     uint32_t jid, uint16_t *__restrict__ eh, uint8_t *__restrict__ sb, const fa_job *__restrict__ jobs,
-    const uint8_t *__restrict__ qseq, const uint8_t *__restrict__ tseq, const ExtParams &p, int qcap,
+    const SeqBuf &qs, const SeqBuf &ts, const ExtParams &p, int qcap,
     const int32_t *__restrict__ w_try, fa_ext_result *__restrict__ out, uint8_t *__restrict__ clamped_out,
     uint32_t *__restrict__ cells_job, uint32_t *__restrict__ status, uint32_t *__restrict__ ovf,
     uint32_t *__restrict__ ovf_n)
@@ -137,8 +139,13 @@ __host__ __device__ __forceinline__ uint32_t rows2_thread(
     // selector nibble of a query N: lands on bytes 4-7 (n) for t < 4 and, for a target N, on
     // a byte whose sign is n's (n = -1: -b; n = 0: a)
     const uint32_t qn = p.mat[4] < 0 ? 13u : 12u;
-    const uint8_t *Q = qseq + jb.q_off;
-    const uint8_t *Tg = tseq + jb.t_off;
+    const uint8_t *Q = qs.p + jb.q_off;    // byte codes (PK false)
+    const uint8_t *Tg = ts.p + jb.t_off;
+    PackedReader qr, tr;                    // packed bases (PK true)
+    if (PK) {
+        qr.init(qs, jb.q_off, qlen);
+        tr.init(ts, jb.t_off, tlen);
+    }
     auto slot = [](int c) { return RING > 0 ? (c & (RING - 1)) : c; };
     // first row (ksw_affine_gap.rs:1017-1025): h0, h0-oe_ins, then -e_ins while the previous
     // value exceeds e_ins, so positive exactly up to init_reach; E = 0
@@ -148,8 +155,14 @@ __host__ __device__ __forceinline__ uint32_t rows2_thread(
     uint32_t bad = 0;
     for (int j0 = 0; j0 < qlen; j0 += 8) {
         uint32_t qb[8];
+        if (PK) {
+            const uint32_t lo = qr.get4(j0), hi = qr.get4(j0 + 4);
 #pragma unroll
-        for (int u = 0; u < 8; ++u) qb[u] = j0 + u < qlen ? (uint32_t)Q[j0 + u] : 0u;
+            for (int u = 0; u < 8; ++u) qb[u] = ((u < 4 ? lo : hi) >> (8 * (u & 3))) & 0xFFu;
+        } else {
+#pragma unroll
+            for (int u = 0; u < 8; ++u) qb[u] = j0 + u < qlen ? (uint32_t)Q[j0 + u] : 0u;
+        }
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
             if (j0 + u < qlen) {
@@ -254,10 +267,15 @@ __host__ __device__ __forceinline__ uint32_t rows2_thread(
     };
     // target bases: tq0 holds the current four rows, tq1 the next four
     uint32_t tq0 = 0, tq1 = 0;
+    if (PK) {
+        tq0 = tr.get4(0);
+        tq1 = tr.get4(4);
+    } else {
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        if (k < tlen) tq0 |= (uint32_t)Tg[k] << (8 * k);
-        if (4 + k < tlen) tq1 |= (uint32_t)Tg[4 + k] << (8 * k);
+        for (int k = 0; k < 4; ++k) {
+            if (k < tlen) tq0 |= (uint32_t)Tg[k] << (8 * k);
+            if (4 + k < tlen) tq1 |= (uint32_t)Tg[4 + k] << (8 * k);
+        }
     }
     for (int i = 0; i < tlen; i += 2) {
         const bool two = i + 1 < tlen;
@@ -266,9 +284,13 @@ __host__ __device__ __forceinline__ uint32_t rows2_thread(
         if ((i & 3) == 2) {
             tq0 = tq1;
             tq1 = 0;
+            if (PK) {
+                tq1 = tr.get4(i + 6);
+            } else {
 #pragma unroll
-            for (int k = 0; k < 4; ++k)
-                if (i + 6 + k < tlen) tq1 |= (uint32_t)Tg[i + 6 + k] << (8 * k);
+                for (int k = 0; k < 4; ++k)
+                    if (i + 6 + k < tlen) tq1 |= (uint32_t)Tg[i + 6 + k] << (8 * k);
+            }
         }
         if (t0 >= (uint32_t)p.m || t1 >= (uint32_t)p.m) { bad = 1; break; }
         tsel = t0 * 0x11u | t1 * 0x1100u;
@@ -499,11 +521,11 @@ __host__ __device__ __forceinline__ uint32_t rows2_thread(
     return cells;
 }
 
-template <int TPB, bool SYM, bool CERT, int RING>
+template <int TPB, bool SYM, bool CERT, int RING, bool PK>
 __global__ void __launch_bounds__(TPB)
 ext_rows2_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ order, uint32_t n,
                  const uint32_t *__restrict__ first_dev, const uint32_t *__restrict__ n_dev,
-                 const uint8_t *__restrict__ qseq, const uint8_t *__restrict__ tseq, const ExtParams p, int qcap,
+                 const SeqBuf qs, const SeqBuf ts, const ExtParams p, int qcap,
                  const int32_t *__restrict__ w_try, fa_ext_result *__restrict__ out,
                  uint8_t *__restrict__ clamped_out, uint32_t *__restrict__ cells_job,
                  unsigned long long *__restrict__ cells_out, uint32_t *__restrict__ status,
@@ -528,8 +550,8 @@ ext_rows2_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ o
                                      : 4 * ((t & 31) >> 1) + 2 * (t & 1) + ((t >> 5) & 1);
         uint16_t *eh = reinterpret_cast<uint16_t *>(smem) + e_off;
         uint8_t *sb = reinterpret_cast<uint8_t *>(smem) + (size_t)words * TPB * 2 + s_off;
-        cells = rows2_thread<TPB, SYM, CERT, RING>(order ? order[gi] : gi, eh, sb, jobs, qseq, tseq, p, qcap, w_try,
-                                                   out, clamped_out, cells_job, status, ovf, ovf_n);
+        cells = rows2_thread<TPB, SYM, CERT, RING, PK>(order ? order[gi] : gi, eh, sb, jobs, qs, ts, p, qcap, w_try,
+                                                       out, clamped_out, cells_job, status, ovf, ovf_n);
     }
     if (cells_out) {
         unsigned long long c = cells;
@@ -544,12 +566,12 @@ ext_rows2_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ o
 // so the batch runs as one launch without a tail of partly filled last waves and SMs that
 // finish their share early take over the rest.  The claim is warp-uniform (lane 0 takes it,
 // a shuffle hands it round), so the warp's lanes stay together between jobs.
-template <int TPB, bool SYM, bool CERT, int RING>
+template <int TPB, bool SYM, bool CERT, int RING, bool PK>
 __global__ void __launch_bounds__(TPB, 1)
 ext_rows2_persist_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ order, uint32_t n,
                          const uint32_t *__restrict__ first_dev, const uint32_t *__restrict__ n_dev,
-                         uint32_t *__restrict__ work, const uint8_t *__restrict__ qseq,
-                         const uint8_t *__restrict__ tseq, const ExtParams p, int qcap,
+                         uint32_t *__restrict__ work, const SeqBuf qs, const SeqBuf ts, const ExtParams p,
+                         int qcap,
                          const int32_t *__restrict__ w_try, fa_ext_result *__restrict__ out,
                          uint8_t *__restrict__ clamped_out, uint32_t *__restrict__ cells_job,
                          unsigned long long *__restrict__ cells_out, uint32_t *__restrict__ status,
@@ -576,7 +598,7 @@ ext_rows2_persist_kernel(const fa_job *__restrict__ jobs, const uint32_t *__rest
         const uint32_t k = base + lane;
         if (k < count) {
             const uint32_t gi = first + k;
-            cells += rows2_thread<TPB, SYM, CERT, RING>(order ? order[gi] : gi, eh, sb, jobs, qseq, tseq, p, qcap,
+            cells += rows2_thread<TPB, SYM, CERT, RING, PK>(order ? order[gi] : gi, eh, sb, jobs, qs, ts, p, qcap,
                                                         w_try, out, clamped_out, cells_job, status, ovf, ovf_n);
         }
     }
@@ -604,26 +626,28 @@ bool ext_rows2_eligible(const ExtParams &p, int qcap) {
 }
 
 namespace {
-template <int TPB, bool SYM, bool CERT, int RING>
+template <int TPB, bool SYM, bool CERT, int RING, bool PK>
 cudaError_t launch_rows2_variant(size_t smem, cudaStream_t stream, const fa_job *d_jobs, const uint32_t *d_order,
-                                 uint32_t n, const uint32_t *d_first, const uint32_t *d_n, const uint8_t *d_qseq,
-                                 const uint8_t *d_tseq, const ExtParams &p, int qcap, const int32_t *d_w_try,
+                                 uint32_t n, const uint32_t *d_first, const uint32_t *d_n, const SeqBuf &d_qseq,
+                                 const SeqBuf &d_tseq, const ExtParams &p, int qcap, const int32_t *d_w_try,
                                  fa_ext_result *d_out, uint8_t *d_clamped, uint32_t *d_cells_job,
                                  unsigned long long *d_cells, uint32_t *d_status, uint32_t *d_ovf, uint32_t *d_ovf_n)
 {
-    cudaError_t err = cudaFuncSetAttribute(ext_rows2_kernel<TPB, SYM, CERT, RING>,
+    cudaError_t err = cudaFuncSetAttribute(ext_rows2_kernel<TPB, SYM, CERT, RING, PK>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return err;
     const uint32_t blocks = (n + TPB - 1) / TPB;
-    ext_rows2_kernel<TPB, SYM, CERT, RING><<<blocks, TPB, smem, stream>>>(
+    ext_rows2_kernel<TPB, SYM, CERT, RING, PK><<<blocks, TPB, smem, stream>>>(
         d_jobs, d_order, n, d_first, d_n, d_qseq, d_tseq, p, qcap, d_w_try, d_out, d_clamped, d_cells_job, d_cells,
         d_status, d_ovf, d_ovf_n);
     return cudaGetLastError();
 }
 }  // namespace
 
-cudaError_t launch_ext_rows2(const fa_job *d_jobs, const uint32_t *d_order, uint32_t n, const uint32_t *d_first,
-                             const uint32_t *d_n, const uint8_t *d_qseq, const uint8_t *d_tseq, const ExtParams &p,
+namespace {
+template <bool PK>
+cudaError_t launch_rows2_seq(const fa_job *d_jobs, const uint32_t *d_order, uint32_t n, const uint32_t *d_first,
+                             const uint32_t *d_n, const SeqBuf &d_qseq, const SeqBuf &d_tseq, const ExtParams &p,
                              int qcap, int ring, bool cert, const int32_t *d_w_try, fa_ext_result *d_out,
                              uint8_t *d_clamped, uint32_t *d_cells_job, unsigned long long *d_cells,
                              uint32_t *d_status, uint32_t *d_ovf, uint32_t *d_ovf_n, cudaStream_t stream, int tpb,
@@ -639,7 +663,7 @@ cudaError_t launch_ext_rows2(const fa_job *d_jobs, const uint32_t *d_order, uint
     const int t = (c || ring != 0) ? 64 : (tpb == 128 ? 128 : 64);
     const size_t smem = ext_rows2_smem_bytes(qcap, t, ring);
     const bool sym = ext_rows2_sym(p);
-#define FA_ROWS2(TV, SV, CV, RV) launch_rows2_variant<TV, SV, CV, RV>(smem, stream, d_jobs, d_order, n, d_first, d_n, \
+#define FA_ROWS2(TV, SV, CV, RV) launch_rows2_variant<TV, SV, CV, RV, PK>(smem, stream, d_jobs, d_order, n, d_first, d_n, \
                                                                       d_qseq, d_tseq, p, qcap, d_w_try, d_out,    \
                                                                       d_clamped, d_cells_job, d_cells, d_status,  \
                                                                       d_ovf, d_ovf_n)
@@ -659,7 +683,7 @@ cudaError_t launch_ext_rows2(const fa_job *d_jobs, const uint32_t *d_order, uint
                                                             d_cells, d_status, d_ovf, d_ovf_n);
         return cudaGetLastError();
     };
-#define FA_PERSIST(TV, SV, CV, RV) go(ext_rows2_persist_kernel<TV, SV, CV, RV>, TV)
+#define FA_PERSIST(TV, SV, CV, RV) go(ext_rows2_persist_kernel<TV, SV, CV, RV, PK>, TV)
     if (d_work) {
         if (c) {
             if (ring == 32) err = sym ? FA_PERSIST(64, true, true, 32) : FA_PERSIST(64, false, true, 32);
@@ -693,6 +717,23 @@ cudaError_t launch_ext_rows2(const fa_job *d_jobs, const uint32_t *d_order, uint
     // jobs whose scores can pass 255: the int32 kernel over the overflow list, same settings
     return launch_ext_packed(d_jobs, d_ovf, n, nullptr, d_ovf_n, d_qseq, d_tseq, p, qcap, ring, d_w_try, d_out,
                              d_clamped, c, d_cells_job, d_cells, d_status, stream);
+}
+}  // namespace
+
+cudaError_t launch_ext_rows2(const fa_job *d_jobs, const uint32_t *d_order, uint32_t n, const uint32_t *d_first,
+                             const uint32_t *d_n, const SeqBuf &d_qseq, const SeqBuf &d_tseq, const ExtParams &p,
+                             int qcap, int ring, bool cert, const int32_t *d_w_try, fa_ext_result *d_out,
+                             uint8_t *d_clamped, uint32_t *d_cells_job, unsigned long long *d_cells,
+                             uint32_t *d_status, uint32_t *d_ovf, uint32_t *d_ovf_n, cudaStream_t stream, int tpb,
+                             uint32_t *d_work)
+{
+    return d_qseq.packed
+               ? launch_rows2_seq<true>(d_jobs, d_order, n, d_first, d_n, d_qseq, d_tseq, p, qcap, ring, cert, d_w_try,
+                                        d_out, d_clamped, d_cells_job, d_cells, d_status, d_ovf, d_ovf_n, stream, tpb,
+                                        d_work)
+               : launch_rows2_seq<false>(d_jobs, d_order, n, d_first, d_n, d_qseq, d_tseq, p, qcap, ring, cert,
+                                         d_w_try, d_out, d_clamped, d_cells_job, d_cells, d_status, d_ovf, d_ovf_n,
+                                         stream, tpb, d_work);
 }
 
 }  // namespace fa

@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "fa_kernels.h"
@@ -86,6 +87,9 @@ struct fa_ctx {
     DevBuf mc_in, mc_plan, mc_out;      // mate-rescue jobs: inputs, plans + scan sums, outputs
     DevBuf is_buf;                      // insert-size statistics: pairs, histogram, results
     DevBuf w_first, w_cur, prev, kk, w_final, tries, missed, list_a, list_b, hist, feat, wbf, part_n, part_w;
+    DevBuf qruns, truns;                // N runs of packed host batches
+    // the sequences of the current host call on the device (byte codes or packed bases)
+    SeqBuf cq{}, ct{};
     uint32_t last_launches = 0;
     bool timing = false;
     int kernel = FA_KERNEL_AUTO;
@@ -98,11 +102,12 @@ struct fa_ctx {
     // same stream then returns each finished slice's results, after its done event
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t slice_ev[8] = {}, done_ev[8] = {}, jobs_ev = nullptr;
+    cudaEvent_t span_ev[8][2] = {};   // sliced rounds: each slice's kernels, start and end
     DevBuf chunk_scratch;
     // kernel choice: fixed, or (FA_KERNEL_AUTO) tuned per (query capacity class, band)
     struct Choice { int kernel; int tpb; };
     int threads = kExtThreads;   // threads per block of the int32 kernel when fixed
-    std::map<std::pair<int, int>, Choice> tuned;
+    std::map<std::tuple<int, int, int>, Choice> tuned;   // (capacity class, band, packed)
     Choice last_choice{FA_KERNEL_INT32, kExtThreads};
     std::vector<std::pair<Choice, float>> last_tuning;
     // graph mode: the rounds of a call recorded once as a CUDA graph and replayed while the
@@ -156,7 +161,7 @@ using Choice = fa_ctx::Choice;
 // `slot` (0-2) picks the two-row kernel's overflow list and count, so launches that may run
 // concurrently use different ones; each list holds a third of the buffer.
 cudaError_t launch_ext(fa_ctx *c, Choice kc, const fa_job *d_jobs, const uint32_t *d_order, uint32_t n,
-                       const uint32_t *d_n, const uint8_t *d_q, const uint8_t *d_t, const ExtParams &kp, int qcap,
+                       const uint32_t *d_n, const SeqBuf &d_q, const SeqBuf &d_t, const ExtParams &kp, int qcap,
                        const int32_t *d_w_try, fa_ext_result *d_out, uint8_t *d_clamped, bool cert,
                        uint32_t *d_cells_job, unsigned long long *d_cells, uint32_t *d_status, cudaStream_t s,
                        int slot = 0) {
@@ -166,7 +171,7 @@ cudaError_t launch_ext(fa_ctx *c, Choice kc, const fa_job *d_jobs, const uint32_
         return launch_ext_rows2(d_jobs, d_order, n, nullptr, d_n, d_q, d_t, kp, qcap, 0, false, d_w_try, d_out,
                                 d_clamped, d_cells_job, d_cells, d_status, c->ovf.as<uint32_t>() + slot * ovf_words,
                                 misc_of(c).ovf_n + slot, s, kc.tpb, misc_of(c).work + slot);
-    if (kc.kernel == FA_KERNEL_INT16X2 && ext_pair_eligible(kp) && !cert)
+    if (kc.kernel == FA_KERNEL_INT16X2 && ext_pair_eligible(kp) && !cert && !d_q.packed)
         return launch_ext_pair(d_jobs, d_order, n, d_n, d_q, d_t, kp, qcap, d_w_try, d_out, d_clamped,
                                d_cells_job, d_cells, d_status, s);
     return launch_ext_packed(d_jobs, d_order, n, nullptr, d_n, d_q, d_t, kp, qcap, 0, d_w_try, d_out, d_clamped,
@@ -187,13 +192,13 @@ uint32_t ext_kernels_of(fa_ctx *c, Choice kc, const ExtParams &kp, int qcap) {
 // (longest) 393,216 jobs of the call's order, and the fastest is kept for that pair.  All
 // candidates give identical results.
 Choice resolve_choice(fa_ctx *c, const ExtParams &kp, const fa_job *d_jobs, const uint32_t *d_order, uint32_t n,
-                      const uint8_t *d_q, const uint8_t *d_t, int qcap, int band, fa_ext_result *d_out,
+                      const SeqBuf &d_q, const SeqBuf &d_t, int qcap, int band, fa_ext_result *d_out,
                       uint32_t *d_status, cudaStream_t s, int *rc) {
     *rc = FA_OK;
     if (c->kernel == FA_KERNEL_INT16X2) return c->last_choice = Choice{FA_KERNEL_INT16X2, kPairThreads};
     if (c->kernel == FA_KERNEL_INT32) return c->last_choice = Choice{FA_KERNEL_INT32, c->threads};
     if (c->kernel == FA_KERNEL_ROWS2) return c->last_choice = Choice{FA_KERNEL_ROWS2, c->threads == 128 ? 128 : 64};
-    const std::pair<int, int> key{(qcap + 31) / 32, band};
+    const std::tuple<int, int, int> key{(qcap + 31) / 32, band, (int)d_q.packed};
     auto it = c->tuned.find(key);
     if (it != c->tuned.end()) return c->last_choice = it->second;
     std::vector<Choice> cands{{FA_KERNEL_INT32, 64}, {FA_KERNEL_INT32, kExtThreads}, {FA_KERNEL_INT32, 256}};
@@ -201,7 +206,7 @@ Choice resolve_choice(fa_ctx *c, const ExtParams &kp, const fa_job *d_jobs, cons
         cands.push_back({FA_KERNEL_ROWS2, 64});
         cands.push_back({FA_KERNEL_ROWS2, 128});
     }
-    if (ext_pair_eligible(kp)) cands.push_back({FA_KERNEL_INT16X2, kPairThreads});
+    if (ext_pair_eligible(kp) && !d_q.packed) cands.push_back({FA_KERNEL_INT16X2, kPairThreads});
     // a sample of several claim rounds of the persistent launch (about 2,700 resident warps of
     // 32 jobs), so the partly used last round does not decide between 64 and 128 threads
     const uint32_t ns = std::min<uint32_t>(n, 393216);
@@ -252,7 +257,7 @@ Choice resolve_choice(fa_ctx *c, const ExtParams &kp, const fa_job *d_jobs, cons
 // kernels run them where the scoring allows (each group with its own overflow list), the
 // int32 kernels otherwise or when int32 is the fixed choice.
 int launch_learned_round(fa_ctx *c, const fa_job *d_jobs, const uint32_t *d_list, uint32_t n_max,
-                         const uint8_t *d_q, const uint8_t *d_t, const ExtParams &kp, int qcap,
+                         const SeqBuf &d_q, const SeqBuf &d_t, const ExtParams &kp, int qcap,
                          const int32_t *d_w_cur, fa_ext_result *d_out, uint8_t *d_flags, bool cert, Misc &m,
                          cudaStream_t s, uint32_t *launches) {
     if (int rc = ensure_aux_streams(c)) return rc;
@@ -420,11 +425,14 @@ int max_rounds_of(const fa_policy *pol, int max_w) {
 // class of the length-sorted order either way.
 int enqueue_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n,
                 const std::vector<std::pair<uint32_t, int>> &segs, int qcap_all, int max_w, const fa_job *d_jobs,
-                const uint32_t *d_order, const uint8_t *d_q, const uint8_t *d_t, const int32_t *d_wfirst,
+                const uint32_t *d_order, const SeqBuf &d_q, const SeqBuf &d_t, const int32_t *d_wfirst,
                 fa_ext_result *d_out, cudaStream_t s, bool capture, uint32_t *launches, uint32_t *retries,
-                Choice kc, const std::vector<Choice> *seg_kc = nullptr) {
+                Choice kc, const std::vector<Choice> *seg_kc = nullptr, int r_first = 0,
+                const uint32_t *list0 = nullptr, const uint32_t *cnt0 = nullptr) {
+    // r_first > 0: the rounds before it have run (policy state initialised, their retry list
+    // in list0 / *cnt0, which is list_a / cnt_a); go on from round r_first
     Misc m = misc_of(c);
-    FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
+    if (r_first == 0) FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
     const int mode = pol ? pol->mode : FA_POLICY_SINGLE;
     const std::vector<std::pair<uint32_t, int>> one_seg{{n, qcap_all}};
     const auto &segs0 = segs.empty() ? one_seg : segs;
@@ -447,18 +455,24 @@ int enqueue_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n
     // flags feed the learned judge only; the certificate only its BOUND test
     uint8_t *d_flags = learned ? c->clamped.as<uint8_t>() : nullptr;
     const bool cert = learned && (pol->judge & FA_JUDGE_BOUND);
-    FA_CUDA(launch_policy_init(d_jobs, n, d_wfirst, pol->w_min, learned, st, s));
-    ++*launches;
+    if (r_first == 0) {
+        FA_CUDA(launch_policy_init(d_jobs, n, d_wfirst, pol->w_min, learned, st, s));
+        ++*launches;
+    }
     const int max_tries = std::max(1, pol->max_tries);
     const int max_rounds = capture ? max_rounds_of(pol, max_w) : (learned ? 13 : 0) + max_tries;
     const bool once = learned && (pol->judge & FA_JUDGE_ONCE);
     // rounds that can hold narrow runs: the first, and with hints also the second
     const int narrow_rounds = (learned && (pol->judge & FA_JUDGE_HINT) && (pol->judge & FA_JUDGE_BOUND)) ? 2 : 1;
-    const uint32_t *list = d_order;
-    const uint32_t *cnt = nullptr;
+    const uint32_t *list = r_first ? list0 : d_order;
+    const uint32_t *cnt = r_first ? cnt0 : nullptr;
     uint32_t *next = c->list_a.as<uint32_t>(), *next_cnt = m.cnt_a;
     uint32_t *spare = c->list_b.as<uint32_t>(), *spare_cnt = m.cnt_b;
-    for (int r = 0; r < max_rounds; ++r) {
+    if (r_first) {
+        std::swap(next, spare);
+        std::swap(next_cnt, spare_cnt);
+    }
+    for (int r = r_first; r < max_rounds; ++r) {
         // with one narrow try, rounds after the narrow ones hold only plain-policy runs
         const bool cert_r = cert && !(once && r >= narrow_rounds);
         if (r == 0 && !learned) {
@@ -563,7 +577,7 @@ int finish_ext(fa_ctx *c, const fa_policy *pol, uint32_t n, cudaStream_t s, fa_e
 // retry rounds reuse the widest capacity class.
 int run_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n,
             const std::vector<std::pair<uint32_t, int>> &segs, int qcap_all, int band, const fa_job *d_jobs,
-            const uint32_t *d_order, const uint8_t *d_q, const uint8_t *d_t, const int32_t *d_wfirst,
+            const uint32_t *d_order, const SeqBuf &d_q, const SeqBuf &d_t, const int32_t *d_wfirst,
             fa_ext_result *d_out, cudaStream_t s, fa_ext_stats *stats, int32_t *h_wfinal) {
     uint32_t launches = 0, retries = 0;
     if (pol && pol->mode != FA_POLICY_SINGLE)
@@ -606,6 +620,12 @@ std::vector<uint64_t> graph_key(fa_ctx *c, const ExtParams &kp, const fa_policy 
                       &c->w_first, &c->w_cur, &c->prev, &c->kk, &c->w_final, &c->tries, &c->missed, &c->list_a,
                       &c->list_b, &c->feat, &c->wbf, &c->part_n, &c->ovf})
         k.push_back((uint64_t)(uintptr_t)b->p);
+    for (const SeqBuf *b : {&c->cq, &c->ct}) {
+        k.push_back(b->packed);
+        k.push_back(b->nbytes);
+        k.push_back(b->n_runs);
+        k.push_back((uint64_t)(uintptr_t)b->runs);
+    }
     k.insert(k.end(), extra.begin(), extra.end());
     return k;
 }
@@ -620,8 +640,8 @@ int run_ext_graph(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t
         if (int rc = ensure_policy_buffers(c, n)) return rc;
     if (int rc = ensure_aux_streams(c)) return rc;
     int rc0 = FA_OK;
-    const Choice kc = resolve_choice(c, kp, c->jobs.as<fa_job>(), c->order.as<uint32_t>(), n, c->qseq.as<uint8_t>(),
-                                     c->tseq.as<uint8_t>(), qcap, max_w, c->out.as<fa_ext_result>(),
+    const Choice kc = resolve_choice(c, kp, c->jobs.as<fa_job>(), c->order.as<uint32_t>(), n, c->cq, c->ct, qcap,
+                                     max_w, c->out.as<fa_ext_result>(),
                                      misc_of(c).status, s, &rc0);
     if (rc0) return rc0;
     // each capacity class's kernel, tuned before recording (tuning cannot run in a capture);
@@ -631,7 +651,7 @@ int run_ext_graph(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t
         uint32_t b = 0;
         for (auto &sg : segs) {
             seg_kc.push_back(resolve_choice(c, kp, c->jobs.as<fa_job>(), c->order.as<uint32_t>() + b, sg.first - b,
-                                            c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(), sg.second, max_w,
+                                            c->cq, c->ct, sg.second, max_w,
                                             c->out.as<fa_ext_result>(), misc_of(c).status, s, &rc0));
             if (rc0) return rc0;
             b = sg.first;
@@ -655,7 +675,7 @@ int run_ext_graph(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t
         int rc = prologue ? prologue(s, &launches) : FA_OK;
         if (!rc)
             rc = enqueue_ext(c, kp, pol, n, segs, qcap, max_w, c->jobs.as<fa_job>(), c->order.as<uint32_t>(),
-                             c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(), d_wfirst, c->out.as<fa_ext_result>(), s,
+                             c->cq, c->ct, d_wfirst, c->out.as<fa_ext_result>(), s,
                              true, &launches, nullptr, kc, &seg_kc);
         cudaGraph_t g = nullptr;
         const cudaError_t ec = cudaStreamEndCapture(s, &g);
@@ -682,86 +702,182 @@ int max_band_of(const fa_job *jobs, uint32_t n) {
     return w;
 }
 
+// One host sequence buffer as a call receives it: byte codes, or 2-bit packed bases with
+// their N runs.  npos: the positions jobs may address (bytes, or bases when packed).
+struct HostSeq {
+    const uint8_t *p;
+    uint64_t nbytes;
+    uint64_t npos;
+    const fa_nrun *runs;
+    uint64_t n_runs;
+    bool packed;
+};
+
+HostSeq host_bytes(const uint8_t *p, uint64_t len) { return HostSeq{p, len, len, nullptr, 0, false}; }
+
+// A packed host buffer, checked: bases present, N runs sorted, non-overlapping, non-empty and
+// inside the buffer.
+int host_packed(const fa_packed_seq *ps, const char *what, HostSeq *out) {
+    if (!ps) return fail(FA_ERR_ARG, "null packed %s buffer", what);
+    if (ps->n_bases && !ps->bases) return fail(FA_ERR_ARG, "packed %s buffer has no bases", what);
+    if (ps->n_nruns && !ps->n_runs) return fail(FA_ERR_ARG, "packed %s buffer has no run array", what);
+    if (ps->n_nruns >= (1ull << 32)) return fail(FA_ERR_CAPACITY, "packed %s buffer: too many N runs", what);
+    uint64_t end = 0;
+    for (uint64_t k = 0; k < ps->n_nruns; ++k) {
+        const fa_nrun &r = ps->n_runs[k];
+        if (r.len == 0 || r.pos < end || r.pos > ps->n_bases || r.len > ps->n_bases - r.pos)
+            return fail(FA_ERR_ARG, "packed %s buffer: N run %llu is empty, unsorted, overlapping or outside "
+                        "the bases", what, (unsigned long long)k);
+        end = r.pos + r.len;
+    }
+    *out = HostSeq{ps->bases, (ps->n_bases + 3) / 4, ps->n_bases, ps->n_runs, ps->n_nruns, true};
+    return FA_OK;
+}
+
+// Device copies of a call's sequences (kSeqPad bytes of slack) and N runs, and the SeqBufs
+// the kernels read them through.
+int ensure_seq_buffers(fa_ctx *c, const HostSeq &q, const HostSeq &t) {
+    FA_CUDA(c->qseq.ensure(q.nbytes + kSeqPad));
+    FA_CUDA(c->tseq.ensure(t.nbytes + kSeqPad));
+    if (q.n_runs) FA_CUDA(c->qruns.ensure(sizeof(fa_nrun) * q.n_runs));
+    if (t.n_runs) FA_CUDA(c->truns.ensure(sizeof(fa_nrun) * t.n_runs));
+    c->cq = SeqBuf{c->qseq.as<uint8_t>(), q.nbytes, q.n_runs ? c->qruns.as<fa_nrun>() : nullptr,
+                   (uint32_t)q.n_runs, q.packed ? 1u : 0u};
+    c->ct = SeqBuf{c->tseq.as<uint8_t>(), t.nbytes, t.n_runs ? c->truns.as<fa_nrun>() : nullptr,
+                   (uint32_t)t.n_runs, t.packed ? 1u : 0u};
+    return FA_OK;
+}
+
+int upload_runs(fa_ctx *c, const HostSeq &q, const HostSeq &t, cudaStream_t s) {
+    if (q.n_runs) FA_CUDA(cudaMemcpyAsync(c->qruns.p, q.runs, sizeof(fa_nrun) * q.n_runs, cudaMemcpyHostToDevice, s));
+    if (t.n_runs) FA_CUDA(cudaMemcpyAsync(c->truns.p, t.runs, sizeof(fa_nrun) * t.n_runs, cudaMemcpyHostToDevice, s));
+    return FA_OK;
+}
+
 // Single-band host batch with the uploads pipelined under the kernels: the job records go
 // first, the GPU validates them and orders them by (upload slice, query length) while the
 // query and target buffers stream up in kSlices byte slices on a copy stream, and the
 // jobs of each slice start as soon as that slice has arrived.  Same results, statistics
 // and errors as the serial path (a rejected batch reports the first bad job through the
-// host-side checks); with pageable host buffers the copies simply do not overlap.
+// host-side checks); with pageable host buffers the copies simply do not overlap.  Byte
+// codes and packed bases alike: slices are cut in bytes, jobs placed by the byte holding
+// their last base.
 constexpr int kSlices = 8;
 constexpr uint32_t kPipeMinJobs = 32768;
 
-int ext_batch_pipelined(fa_ctx *c, const ExtParams &kp, const fa_job *jobs, uint32_t n, const uint8_t *qseq,
-                        uint64_t qseq_len, const uint8_t *tseq, uint64_t tseq_len, fa_ext_result *out,
-                        fa_ext_stats *stats) {
-    if (int rc = ensure_ext_buffers(c, n, qseq_len, tseq_len)) return rc;
+int ensure_pipe_streams(fa_ctx *c) {
     FA_CUDA(c->chunk_scratch.ensure(chunk_scratch_bytes(kSlices)));
     if (!c->copy_stream) {
         FA_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
         for (auto &e : c->slice_ev) FA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         for (auto &e : c->done_ev) FA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         FA_CUDA(cudaEventCreateWithFlags(&c->jobs_ev, cudaEventDisableTiming));
-    }
-    cudaStream_t s = c->stream, cs = c->copy_stream;
-    // graded slices (1, 1, 2, 4, 6, 6, 6, 6 thirty-seconds of each buffer): the first jobs
-    // start after a small upload, and the uploads, faster than the kernels, stay ahead
-    ChunkEnds ends;
-    {
-        static constexpr int kCum[kSlices] = {1, 2, 4, 8, 14, 20, 26, 32};
-        static_assert(kSlices <= kMaxChunks, "slice count");
         for (int k = 0; k < kSlices; ++k) {
-            ends.q[k] = k == kSlices - 1 ? qseq_len : qseq_len / 32 * kCum[k];
-            ends.t[k] = k == kSlices - 1 ? tseq_len : tseq_len / 32 * kCum[k];
+            FA_CUDA(cudaEventCreate(&c->span_ev[k][0]));
+            FA_CUDA(cudaEventCreate(&c->span_ev[k][1]));
         }
     }
-    Misc m = misc_of(c);
-    uint32_t *scratch = c->chunk_scratch.as<uint32_t>();
-    const size_t nbins = (size_t)kSlices * (FA_MAX_QLEN + 1);
-    uint32_t *info = scratch + 3 * nbins;
-    FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
-    // the job records first, then the sequence slices, all on the copy stream (one after
-    // another, so the records arrive at full bandwidth)
-    if (int rc = ensure_aux_streams(c)) return rc;
-    FA_CUDA(cudaEventRecord(c->fork_ev, s));      // after all earlier work on the main stream
-    FA_CUDA(cudaStreamWaitEvent(cs, c->fork_ev, 0));
-    FA_CUDA(cudaMemcpyAsync(c->jobs.p, jobs, sizeof(fa_job) * (size_t)n, cudaMemcpyHostToDevice, cs));
-    FA_CUDA(cudaEventRecord(c->jobs_ev, cs));
-    FA_CUDA(cudaStreamWaitEvent(s, c->jobs_ev, 0));
+    return ensure_aux_streams(c);
+}
+
+// graded slices (1, 1, 2, 4, 6, 6, 6, 6 thirty-seconds of each buffer): the first jobs start
+// after a small upload, and the uploads, faster than the kernels, stay ahead
+ChunkEnds graded_ends(const HostSeq &q, const HostSeq &t) {
+    ChunkEnds ends;
+    static constexpr int kCum[kSlices] = {1, 2, 4, 8, 14, 20, 26, 32};
+    static_assert(kSlices <= kMaxChunks, "slice count");
+    for (int k = 0; k < kSlices; ++k) {
+        ends.q[k] = k == kSlices - 1 ? q.nbytes : q.nbytes / 32 * kCum[k];
+        ends.t[k] = k == kSlices - 1 ? t.nbytes : t.nbytes / 32 * kCum[k];
+    }
+    ends.shift = q.packed ? 2 : 0;
+    return ends;
+}
+
+// The sequence slices on the copy stream, one event per slice.
+int upload_slices(fa_ctx *c, const HostSeq &q, const HostSeq &t, const ChunkEnds &ends) {
+    cudaStream_t cs = c->copy_stream;
     for (int k = 0; k < kSlices; ++k) {
         const uint64_t q0 = k ? ends.q[k - 1] : 0, q1 = ends.q[k];
         const uint64_t t0 = k ? ends.t[k - 1] : 0, t1 = ends.t[k];
-        if (q1 > q0) FA_CUDA(cudaMemcpyAsync(c->qseq.as<uint8_t>() + q0, qseq + q0, q1 - q0, cudaMemcpyHostToDevice, cs));
-        if (t1 > t0) FA_CUDA(cudaMemcpyAsync(c->tseq.as<uint8_t>() + t0, tseq + t0, t1 - t0, cudaMemcpyHostToDevice, cs));
+        if (q1 > q0) FA_CUDA(cudaMemcpyAsync(c->qseq.as<uint8_t>() + q0, q.p + q0, q1 - q0, cudaMemcpyHostToDevice, cs));
+        if (t1 > t0) FA_CUDA(cudaMemcpyAsync(c->tseq.as<uint8_t>() + t0, t.p + t0, t1 - t0, cudaMemcpyHostToDevice, cs));
         FA_CUDA(cudaEventRecord(c->slice_ev[k], cs));
     }
-    FA_CUDA(launch_chunk_prep(c->jobs.as<fa_job>(), n, qseq_len, tseq_len, ends, kSlices, kp.max_score,
+    return FA_OK;
+}
+
+// Validation and (slice, length) histogram of the uploaded jobs; h_info as launch_chunk_prep
+// lays it out: status, first bad job, longest query, widest band | slice bounds in the order |
+// each slice's lowest and highest job index.  A rejected batch reports its first bad job
+// with the host-side checks' message.
+constexpr int kInfoWords = 4 + kSlices + 1 + 2 * kSlices;
+int prep_slices(fa_ctx *c, const ExtParams &kp, const fa_job *jobs, uint32_t n, const HostSeq &q, const HostSeq &t,
+                const ChunkEnds &ends, uint32_t *h_info) {
+    cudaStream_t s = c->stream;
+    uint32_t *scratch = c->chunk_scratch.as<uint32_t>();
+    const size_t nbins = (size_t)kSlices * (FA_MAX_QLEN + 1);
+    FA_CUDA(launch_chunk_prep(c->jobs.as<fa_job>(), n, q.npos, t.npos, ends, kSlices, kp.max_score,
                               (kp.flags & FA_PARAM_H0_ZERO) ? 0 : 1, packed_qcap_limit(c->smem_optin), scratch, s));
-    // info: status, first bad job, longest query, widest band | slice bounds in the order |
-    // each slice's lowest and highest job index
-    uint32_t h_info[4 + kSlices + 1 + 2 * kSlices];
-    FA_CUDA(cudaMemcpyAsync(h_info, info, sizeof(h_info), cudaMemcpyDeviceToHost, s));
+    FA_CUDA(cudaMemcpyAsync(h_info, scratch + 3 * nbins, sizeof(uint32_t) * kInfoWords, cudaMemcpyDeviceToHost, s));
     FA_CUDA(cudaStreamSynchronize(s));
     if (h_info[0]) {
-        FA_CUDA(cudaStreamSynchronize(cs));   // the caller's buffers stay in use until then
+        FA_CUDA(cudaStreamSynchronize(c->copy_stream));   // the caller's buffers stay in use until then
         const uint32_t bad = h_info[1] < n ? h_info[1] : 0;
         int mq = 0;
-        const int rc = check_jobs(jobs + bad, 1, qseq_len, tseq_len, kp, packed_qcap_limit(c->smem_optin), &mq);
+        const int rc = check_jobs(jobs + bad, 1, q.npos, t.npos, kp, packed_qcap_limit(c->smem_optin), &mq);
         if (rc) return fail(rc, "job %u: %s", bad, g_err.c_str() + (g_err.compare(0, 7, "job 0: ") == 0 ? 7 : 0));
         return fail(FA_ERR_ARG, "job %u is invalid", bad);
     }
+    return FA_OK;
+}
+
+// Whether every slice's jobs form one index range, together covering all n jobs (the
+// sequences lie in job order).
+bool slices_in_order(const uint32_t *h_info, uint32_t n) {
+    uint32_t covered = 0;
+    for (int k = 0; k < kSlices; ++k) {
+        const uint32_t cnt = h_info[4 + k + 1] - h_info[4 + k];
+        const uint32_t lo = h_info[4 + kSlices + 1 + k], hi = h_info[4 + 2 * kSlices + 1 + k];
+        if (cnt && hi - lo + 1 != cnt) return false;
+        covered += cnt;
+    }
+    return covered == n;
+}
+
+int ext_batch_pipelined(fa_ctx *c, const ExtParams &kp, const fa_job *jobs, uint32_t n, const HostSeq &hq,
+                        const HostSeq &ht, fa_ext_result *out, fa_ext_stats *stats) {
+    if (int rc = ensure_ext_buffers(c, n, 0, 0)) return rc;
+    if (int rc = ensure_seq_buffers(c, hq, ht)) return rc;
+    if (int rc = ensure_pipe_streams(c)) return rc;
+    cudaStream_t s = c->stream, cs = c->copy_stream;
+    const ChunkEnds ends = graded_ends(hq, ht);
+    Misc m = misc_of(c);
+    FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
+    // the job records and N runs first, then the sequence slices, all on the copy stream
+    // (one after another, so the records arrive at full bandwidth)
+    FA_CUDA(cudaEventRecord(c->fork_ev, s));      // after all earlier work on the main stream
+    FA_CUDA(cudaStreamWaitEvent(cs, c->fork_ev, 0));
+    FA_CUDA(cudaMemcpyAsync(c->jobs.p, jobs, sizeof(fa_job) * (size_t)n, cudaMemcpyHostToDevice, cs));
+    if (int rc = upload_runs(c, hq, ht, cs)) return rc;
+    FA_CUDA(cudaEventRecord(c->jobs_ev, cs));
+    FA_CUDA(cudaStreamWaitEvent(s, c->jobs_ev, 0));
+    if (int rc = upload_slices(c, hq, ht, ends)) return rc;
+    uint32_t h_info[kInfoWords];
+    if (int rc = prep_slices(c, kp, jobs, n, hq, ht, ends, h_info)) return rc;
     const int max_q = (int)h_info[2];
-    FA_CUDA(launch_chunk_scatter(c->jobs.as<fa_job>(), n, ends, kSlices, scratch, c->order.as<uint32_t>(), s));
+    FA_CUDA(launch_chunk_scatter(c->jobs.as<fa_job>(), n, ends, kSlices, c->chunk_scratch.as<uint32_t>(),
+                                 c->order.as<uint32_t>(), s));
     const int band = (int)h_info[3];   // widest configured band, reduced on the device
-    if (c->kernel == FA_KERNEL_AUTO && !c->tuned.count({(max_q + 31) / 32, band}))
+    if (c->kernel == FA_KERNEL_AUTO && !c->tuned.count({(max_q + 31) / 32, band, (int)hq.packed}))
         FA_CUDA(cudaStreamWaitEvent(s, c->slice_ev[kSlices - 1], 0));   // tuning reads every slice
     int rc0 = FA_OK;
-    const Choice kc = resolve_choice(c, kp, c->jobs.as<fa_job>(), c->order.as<uint32_t>(), n, c->qseq.as<uint8_t>(),
-                                     c->tseq.as<uint8_t>(), max_q, band, c->out.as<fa_ext_result>(), m.status, s, &rc0);
+    const Choice kc = resolve_choice(c, kp, c->jobs.as<fa_job>(), c->order.as<uint32_t>(), n, c->cq, c->ct, max_q,
+                                     band, c->out.as<fa_ext_result>(), m.status, s, &rc0);
     if (rc0) return rc0;
     uint32_t launches = 2;
     // slices alternate between the main stream and an auxiliary one (each with its own
     // overflow list), so one slice's last, partly filled wave overlaps the next slice's start
-    if (int rc = ensure_aux_streams(c)) return rc;
     cudaStream_t sk[2] = {s, c->aux[0]};
     FA_CUDA(cudaEventRecord(c->ev0, s));
     FA_CUDA(cudaEventRecord(c->fork_ev, s));
@@ -775,23 +891,16 @@ int ext_batch_pipelined(fa_ctx *c, const ExtParams &kp, const fa_job *jobs, uint
         cudaPointerAttributes pa;
         early = cudaPointerGetAttributes(&pa, out) == cudaSuccess && pa.type == cudaMemoryTypeHost;
         cudaGetLastError();
-        uint32_t covered = 0;
-        for (int k = 0; k < kSlices && early; ++k) {
-            const uint32_t cnt = h_info[4 + k + 1] - h_info[4 + k];
-            const uint32_t lo = h_info[4 + kSlices + 1 + k], hi = h_info[4 + 2 * kSlices + 1 + k];
-            if (cnt && hi - lo + 1 != cnt) early = false;
-            covered += cnt;
-        }
-        early = early && covered == n;
+        early = early && slices_in_order(h_info, n);
     }
     for (int k = 0; k < kSlices; ++k) {
         const uint32_t cnt = h_info[4 + k + 1] - h_info[4 + k];
         cudaStream_t st = sk[k & 1];
         FA_CUDA(cudaStreamWaitEvent(st, c->slice_ev[k], 0));
         if (cnt == 0) continue;
-        FA_CUDA(launch_ext(c, kc, c->jobs.as<fa_job>(), c->order.as<uint32_t>() + h_info[4 + k], cnt, nullptr,
-                           c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(), kp, max_q, nullptr, c->out.as<fa_ext_result>(),
-                           nullptr, false, c->cells_job.as<uint32_t>(), m.cells, m.status, st, k & 1));
+        FA_CUDA(launch_ext(c, kc, c->jobs.as<fa_job>(), c->order.as<uint32_t>() + h_info[4 + k], cnt, nullptr, c->cq,
+                           c->ct, kp, max_q, nullptr, c->out.as<fa_ext_result>(), nullptr, false,
+                           c->cells_job.as<uint32_t>(), m.cells, m.status, st, k & 1));
         launches += ext_kernels_of(c, kc, kp, max_q);
         if (early) {
             const uint32_t lo = h_info[4 + kSlices + 1 + k];
@@ -815,177 +924,239 @@ int ext_batch_pipelined(fa_ctx *c, const ExtParams &kp, const fa_job *jobs, uint
     return FA_OK;
 }
 
-}  // namespace
-
-extern "C" {
-
-const char *fa_last_error(void) { return g_err.c_str(); }
-const char *fa_version(void) { return "ferrous_b200 0.1 (sm_100a)"; }
-
-int fa_ctx_create(int device, fa_ctx **out) {
-    if (!out) return fail(FA_ERR_ARG, "null out");
-    *out = nullptr;
-    int ndev = 0;
-    FA_CUDA(cudaGetDeviceCount(&ndev));
-    if (device < 0 || device >= ndev) return fail(FA_ERR_ARG, "device %d not present (%d)", device, ndev);
-    FA_CUDA(cudaSetDevice(device));
-    fa_ctx *c = new fa_ctx();
-    c->device = device;
-    cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major < 10) {
-        delete c;
-        return fail(FA_ERR_CUDA, "device %d is not sm_100-class", device);
+// A retry policy's rounds on a host batch whose jobs address their sequences in job order
+// (FA_POLICY_BWA, or FA_POLICY_LEARNED with first bands from w_first or, given a model, from
+// the band features and MLP on the device): the job records, hints, first bands and N runs
+// go up first, then the sequences in kSlices graded slices on the copy stream.  As each
+// slice arrives its jobs run prediction, policy set-up and the first extension round; the
+// jobs that round rejects collect in one retry list across the slices, and the later rounds
+// run over that list.  Results, bands and statistics are those of the serial path; the
+// device time reported is the kernels' busy time (the waits for uploads left out).
+// *done = false (nothing run) when the jobs' sequences are not in job order.
+int ext_batch_sliced(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, const fa_band_model *model, float margin,
+                     const fa_job *jobs, uint32_t n, const HostSeq &hq, const HostSeq &ht, const fa_band_hint *hints,
+                     const int32_t *w_first, fa_ext_result *out, int32_t *w_first_out, int32_t *w_final,
+                     fa_ext_stats *stats, bool *done) {
+    *done = false;
+    const bool learned = pol->mode == FA_POLICY_LEARNED;
+    if (int rc = ensure_ext_buffers(c, n, 0, 0)) return rc;
+    if (int rc = ensure_seq_buffers(c, hq, ht)) return rc;
+    if (int rc = ensure_policy_buffers(c, n)) return rc;
+    if (int rc = ensure_pipe_streams(c)) return rc;
+    float *d_x = nullptr;
+    fa_band_hint *d_h = nullptr;
+    std::vector<__nv_bfloat16> wbf;
+    float mean[16], sd[16];
+    if (model) {
+        FA_CUDA(c->feat.ensure(sizeof(float) * 16 * (size_t)n + sizeof(fa_band_hint) * (size_t)n));
+        FA_CUDA(c->wbf.ensure(sizeof(__nv_bfloat16) * FA_BAND_NPARAMS));
+        d_x = c->feat.as<float>();
+        d_h = hints ? reinterpret_cast<fa_band_hint *>(d_x + 16 * (size_t)n) : nullptr;
+        band_model_export(model, wbf, mean, sd);
     }
-    c->sm_count = prop.multiProcessorCount;
-    c->smem_optin = prop.sharedMemPerBlockOptin;
-    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
-        delete c;
-        return fail(FA_ERR_CUDA, "stream/event creation failed");
+    cudaStream_t s = c->stream, cs = c->copy_stream;
+    const ChunkEnds ends = graded_ends(hq, ht);
+    Misc m = misc_of(c);
+    FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
+    FA_CUDA(cudaEventRecord(c->fork_ev, s));
+    FA_CUDA(cudaStreamWaitEvent(cs, c->fork_ev, 0));
+    FA_CUDA(cudaMemcpyAsync(c->jobs.p, jobs, sizeof(fa_job) * (size_t)n, cudaMemcpyHostToDevice, cs));
+    if (int rc = upload_runs(c, hq, ht, cs)) return rc;
+    if (model) {
+        if (d_h) FA_CUDA(cudaMemcpyAsync(d_h, hints, sizeof(fa_band_hint) * (size_t)n, cudaMemcpyHostToDevice, cs));
+        FA_CUDA(cudaMemcpyAsync(c->wbf.p, wbf.data(), sizeof(__nv_bfloat16) * FA_BAND_NPARAMS,
+                                cudaMemcpyHostToDevice, cs));
+    } else if (learned) {
+        FA_CUDA(cudaMemcpyAsync(c->w_first.p, w_first, 4ull * n, cudaMemcpyHostToDevice, cs));
     }
-    *out = c;
+    FA_CUDA(cudaEventRecord(c->jobs_ev, cs));
+    FA_CUDA(cudaStreamWaitEvent(s, c->jobs_ev, 0));
+    if (int rc = upload_slices(c, hq, ht, ends)) return rc;
+    uint32_t h_info[kInfoWords];
+    if (int rc = prep_slices(c, kp, jobs, n, hq, ht, ends, h_info)) return rc;
+    if (!slices_in_order(h_info, n)) {
+        FA_CUDA(cudaStreamSynchronize(cs));
+        return FA_OK;
+    }
+    *done = true;
+    const int max_q = (int)h_info[2];
+    const int band = (int)h_info[3];
+    FA_CUDA(launch_chunk_scatter(c->jobs.as<fa_job>(), n, ends, kSlices, c->chunk_scratch.as<uint32_t>(),
+                                 c->order.as<uint32_t>(), s));
+    if (c->kernel == FA_KERNEL_AUTO && !c->tuned.count({(max_q + 31) / 32, band, (int)hq.packed}))
+        FA_CUDA(cudaStreamWaitEvent(s, c->slice_ev[kSlices - 1], 0));   // tuning reads every slice
+    int rc0 = FA_OK;
+    const Choice kc = resolve_choice(c, kp, c->jobs.as<fa_job>(), c->order.as<uint32_t>(), n, c->cq, c->ct, max_q,
+                                     band, c->out.as<fa_ext_result>(), m.status, s, &rc0);
+    if (rc0) return rc0;
+    FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));   // the tuner's runs leave their cells and status
+    const fa_job *d_jobs = c->jobs.as<fa_job>();
+    const uint32_t *order = c->order.as<uint32_t>();
+    int32_t *d_wf = c->w_first.as<int32_t>();
+    PolicyState st{c->w_cur.as<int32_t>(), c->prev.as<int32_t>(), c->kk.as<int32_t>(),
+                   c->w_final.as<int32_t>(), c->tries.as<int32_t>(), c->missed.as<uint8_t>()};
+    uint8_t *d_flags = learned ? c->clamped.as<uint8_t>() : nullptr;
+    const bool cert = learned && (pol->judge & FA_JUDGE_BOUND);
+    const int max_tries = std::max(1, pol->max_tries);
+    uint32_t launches = 0, retries = 0;
+    int spans = 0;
+    for (int k = 0; k < kSlices; ++k) {
+        const uint32_t b = h_info[4 + k], cnt = h_info[4 + k + 1] - b;
+        FA_CUDA(cudaStreamWaitEvent(s, c->slice_ev[k], 0));
+        if (cnt == 0) continue;
+        const uint32_t lo = h_info[4 + kSlices + 1 + k];
+        FA_CUDA(cudaEventRecord(c->span_ev[k][0], s));
+        if (model) {
+            FA_CUDA(launch_band_features(d_jobs + lo, cnt, c->cq, c->ct, d_h ? d_h + lo : nullptr, kp.max_score,
+                                         d_x + 16 * (size_t)lo, s));
+            FA_CUDA(launch_band_predict(c->wbf.as<__nv_bfloat16>(), mean, sd, d_x + 16 * (size_t)lo, d_jobs + lo, cnt,
+                                        margin, pol->w_min, nullptr, d_wf + lo, s));
+            launches += 2;
+        }
+        const PolicyState sl{st.w_cur + lo, st.prev + lo, st.k + lo, st.w_final + lo, st.tries + lo,
+                             st.missed + lo};
+        FA_CUDA(launch_policy_init(d_jobs + lo, cnt, learned ? d_wf + lo : nullptr, pol->w_min, learned, sl, s));
+        const uint32_t *list = order + b;
+        if (learned) {
+            FA_CUDA(launch_band_partition(d_jobs, list, nullptr, cnt, st.w_cur, c->part_n.as<uint32_t>() + b,
+                                          m.bucket_hist, m.bucket_cursor, m.group_bounds, s));
+            if (int rc = launch_learned_round(c, d_jobs, c->part_n.as<uint32_t>() + b, cnt, c->cq, c->ct, kp, max_q,
+                                              st.w_cur, c->out.as<fa_ext_result>(), d_flags, cert, m, s, &launches))
+                return rc;
+            launches += 2;
+        } else {
+            FA_CUDA(launch_ext(c, kc, d_jobs, list, cnt, nullptr, c->cq, c->ct, kp, max_q, st.w_cur,
+                               c->out.as<fa_ext_result>(), d_flags, false, c->cells_job.as<uint32_t>(), m.cells,
+                               m.status, s));
+            launches += ext_kernels_of(c, kc, kp, max_q);
+        }
+        // the round's rejected jobs join one retry list (cnt_a counts across the slices)
+        FA_CUDA(launch_policy_step(d_jobs, list, nullptr, nullptr, cnt, c->out.as<fa_ext_result>(), d_flags, st,
+                                   max_tries, pol->judge, c->list_a.as<uint32_t>(), m.cnt_a, s));
+        launches += 2;
+        FA_CUDA(cudaEventRecord(c->span_ev[k][1], s));
+        spans |= 1 << k;
+    }
+    FA_CUDA(cudaEventRecord(c->ev0, s));
+    std::vector<std::pair<uint32_t, int>> segs{{n, max_q}};
+    if (int rc = enqueue_ext(c, kp, pol, n, segs, max_q, band, d_jobs, order, c->cq, c->ct, d_wf,
+                             c->out.as<fa_ext_result>(), s, false, &launches, &retries, kc, nullptr, 1,
+                             c->list_a.as<uint32_t>(), m.cnt_a))
+        return rc;
+    FA_CUDA(cudaEventRecord(c->ev1, s));
+    FA_CUDA(cudaMemcpyAsync(out, c->out.p, sizeof(fa_ext_result) * (size_t)n, cudaMemcpyDeviceToHost, s));
+    if (w_first_out && model) FA_CUDA(cudaMemcpyAsync(w_first_out, d_wf, 4ull * n, cudaMemcpyDeviceToHost, s));
+    if (int rc = finish_ext(c, pol, n, s, stats, w_final, launches, retries, true)) return rc;
+    if (stats) {   // busy time: the slices' spans plus the later rounds
+        for (int k = 0; k < kSlices; ++k) {
+            if (!(spans & (1 << k))) continue;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, c->span_ev[k][0], c->span_ev[k][1]);
+            stats->kernel_ms += ms;
+        }
+    }
+    FA_CUDA(cudaStreamSynchronize(s));
     return FA_OK;
 }
 
-void fa_ctx_destroy(fa_ctx *c) {
-    if (!c) return;
-    cudaSetDevice(c->device);
-    for (DevBuf *b : {&c->jobs, &c->order, &c->qseq, &c->tseq, &c->out, &c->clamped, &c->cells_job,
-                      &c->misc, &c->w_first, &c->w_cur, &c->prev, &c->kk, &c->w_final, &c->tries,
-                      &c->missed, &c->list_a, &c->list_b, &c->hist, &c->feat, &c->wbf, &c->part_n,
-                      &c->part_w, &c->ovf, &c->reg_in, &c->reg_out, &c->col_in, &c->col_plan, &c->col_out,
-                      &c->cg_in, &c->cg_scratch, &c->cg_out, &c->mc_in, &c->mc_plan, &c->mc_out, &c->is_buf})
-        b->release();
-    for (int k = 0; k < 2; ++k) {
-        if (c->join_ev[k]) cudaEventDestroy(c->join_ev[k]);
-        if (c->aux[k]) cudaStreamDestroy(c->aux[k]);
-    }
-    if (c->fork_ev) cudaEventDestroy(c->fork_ev);
-    if (c->gexec) cudaGraphExecDestroy(c->gexec);
-    for (auto &e : c->slice_ev)
-        if (e) cudaEventDestroy(e);
-    for (auto &e : c->done_ev)
-        if (e) cudaEventDestroy(e);
-    if (c->jobs_ev) cudaEventDestroy(c->jobs_ev);
-    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
-    c->chunk_scratch.release();
-    if (c->kev0) cudaEventDestroy(c->kev0);
-    if (c->kev1) cudaEventDestroy(c->kev1);
-    if (c->ev0) cudaEventDestroy(c->ev0);
-    if (c->ev1) cudaEventDestroy(c->ev1);
-    if (c->stream) cudaStreamDestroy(c->stream);
-    delete c;
-}
-
-int fa_probe_int_peak(fa_ctx *c, int kind, double *ops_per_s, float *ms) {
-    if (!c || !ops_per_s) return fail(FA_ERR_ARG, "null argument");
-    if (kind < 0 || kind > 4) return fail(FA_ERR_ARG, "unknown probe kind %d", kind);
-    FA_CUDA(cudaSetDevice(c->device));
-    const double r = probe_int_peak(kind, c->sm_count, c->stream, ms);
-    if (r <= 0) return fail(FA_ERR_CUDA, "probe kernel failed");
-    *ops_per_s = r;
-    return FA_OK;
-}
-
-int fa_device_info(fa_ctx *c, int *sm_count, int *smem_optin_bytes) {
-    if (!c) return fail(FA_ERR_ARG, "null context");
-    if (sm_count) *sm_count = c->sm_count;
-    if (smem_optin_bytes) *smem_optin_bytes = (int)c->smem_optin;
-    return FA_OK;
-}
-
-uint32_t fa_mate_xtra(int32_t mate_len, int32_t match_score, int32_t min_seed_len) {
-    uint32_t x = FA_KSW_XSUBO | FA_KSW_XSTART;
-    if (mate_len * match_score < 250) x |= FA_KSW_XBYTE;
-    return x | (uint32_t)(min_seed_len * match_score);
-}
-
-int fa_ext_batch_policy(fa_ctx *c, const fa_params *p, const fa_policy *pol, const fa_job *jobs,
-                        uint32_t n, const uint8_t *qseq, uint64_t qseq_len, const uint8_t *tseq,
-                        uint64_t tseq_len, const int32_t *w_first, fa_ext_result *out,
-                        int32_t *w_final, fa_ext_stats *stats) {
+// fa_ext_batch_policy / fa_ext_batch_packed on host buffers of either form.
+int ext_batch_host(fa_ctx *c, const fa_params *p, const fa_policy *pol, const fa_job *jobs, uint32_t n,
+                   const HostSeq &hq, const HostSeq &ht, const int32_t *w_first, fa_ext_result *out,
+                   int32_t *w_final, fa_ext_stats *stats) {
     auto t0 = std::chrono::steady_clock::now();
-    if (!c) return fail(FA_ERR_ARG, "null context");
-    if (int rc = check_params(p)) return rc;
-    if (stats) memset(stats, 0, sizeof(*stats));
-    if (n == 0) return FA_OK;
-    if (!jobs || !out || !qseq || !tseq) return fail(FA_ERR_ARG, "null buffer");
-    if (pol && (pol->mode < FA_POLICY_SINGLE || pol->mode > FA_POLICY_LEARNED))
-        return fail(FA_ERR_ARG, "unknown policy mode %d", pol->mode);
-    if (pol && pol->mode == FA_POLICY_LEARNED && !w_first)
-        return fail(FA_ERR_STATE, "learned policy needs w_first (or a loaded band model)");
-    FA_CUDA(cudaSetDevice(c->device));
     const ExtParams kp = ext_params_of(p);
-    if ((!pol || pol->mode == FA_POLICY_SINGLE) && !c->graph && n >= kPipeMinJobs) {
-        int rc = ext_batch_pipelined(c, kp, jobs, n, qseq, qseq_len, tseq, tseq_len, out, stats);
+    auto total = [&]() {
+        if (stats)
+            stats->total_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    };
+    const int mode = pol ? pol->mode : FA_POLICY_SINGLE;
+    if (mode == FA_POLICY_SINGLE && !c->graph && n >= kPipeMinJobs) {
+        int rc = ext_batch_pipelined(c, kp, jobs, n, hq, ht, out, stats);
         if (rc) return rc;
         if (w_final)
             for (uint32_t i = 0; i < n; ++i) w_final[i] = jobs[i].w;
-        if (stats)
-            stats->total_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        total();
         return FA_OK;
     }
+    if (mode != FA_POLICY_SINGLE && !c->graph && n >= kPipeMinJobs) {
+        bool done = false;
+        int rc = ext_batch_sliced(c, kp, pol, nullptr, 0.f, jobs, n, hq, ht, nullptr, w_first, out, nullptr, w_final,
+                                  stats, &done);
+        if (rc) return rc;
+        if (done) {
+            total();
+            return FA_OK;
+        }
+    }
     int max_q = 0;
-    if (int rc = check_jobs(jobs, n, qseq_len, tseq_len, kp, packed_qcap_limit(c->smem_optin), &max_q))
-        return rc;
+    if (int rc = check_jobs(jobs, n, hq.npos, ht.npos, kp, packed_qcap_limit(c->smem_optin), &max_q)) return rc;
     std::vector<uint32_t> order;
     std::vector<std::pair<uint32_t, int>> segs;
     length_order(jobs, n, order, segs);
-    if (int rc = ensure_ext_buffers(c, n, qseq_len, tseq_len)) return rc;
+    if (int rc = ensure_ext_buffers(c, n, 0, 0)) return rc;
+    if (int rc = ensure_seq_buffers(c, hq, ht)) return rc;
     cudaStream_t s = c->stream;
     FA_CUDA(cudaMemcpyAsync(c->jobs.p, jobs, sizeof(fa_job) * (size_t)n, cudaMemcpyHostToDevice, s));
     FA_CUDA(cudaMemcpyAsync(c->order.p, order.data(), 4ull * n, cudaMemcpyHostToDevice, s));
-    FA_CUDA(cudaMemcpyAsync(c->qseq.p, qseq, qseq_len, cudaMemcpyHostToDevice, s));
-    FA_CUDA(cudaMemcpyAsync(c->tseq.p, tseq, tseq_len, cudaMemcpyHostToDevice, s));
-    if (pol && pol->mode == FA_POLICY_LEARNED) {
+    FA_CUDA(cudaMemcpyAsync(c->qseq.p, hq.p, hq.nbytes, cudaMemcpyHostToDevice, s));
+    FA_CUDA(cudaMemcpyAsync(c->tseq.p, ht.p, ht.nbytes, cudaMemcpyHostToDevice, s));
+    if (int rc = upload_runs(c, hq, ht, s)) return rc;
+    if (mode == FA_POLICY_LEARNED) {
         if (int rc = ensure_policy_buffers(c, n)) return rc;
         FA_CUDA(cudaMemcpyAsync(c->w_first.p, w_first, 4ull * n, cudaMemcpyHostToDevice, s));
     }
-    const int32_t *d_wf = (pol && pol->mode == FA_POLICY_LEARNED) ? c->w_first.as<int32_t>() : nullptr;
+    const int32_t *d_wf = mode == FA_POLICY_LEARNED ? c->w_first.as<int32_t>() : nullptr;
     int rc = c->graph
                  ? run_ext_graph(c, kp, pol, n, segs, max_q, max_band_of(jobs, n), {}, nullptr, d_wf, s, stats,
                                  w_final)
-                 : run_ext(c, kp, pol, n, segs, max_q, max_band_of(jobs, n), c->jobs.as<fa_job>(), c->order.as<uint32_t>(),
-                           c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(), d_wf, c->out.as<fa_ext_result>(), s, stats,
+                 : run_ext(c, kp, pol, n, segs, max_q, max_band_of(jobs, n), c->jobs.as<fa_job>(),
+                           c->order.as<uint32_t>(), c->cq, c->ct, d_wf, c->out.as<fa_ext_result>(), s, stats,
                            w_final);
     if (rc) return rc;
     FA_CUDA(cudaMemcpyAsync(out, c->out.p, sizeof(fa_ext_result) * (size_t)n, cudaMemcpyDeviceToHost, s));
     FA_CUDA(cudaStreamSynchronize(s));
-    if (w_final && (!pol || pol->mode == FA_POLICY_SINGLE))
+    if (w_final && mode == FA_POLICY_SINGLE)
         for (uint32_t i = 0; i < n; ++i) w_final[i] = jobs[i].w;
-    if (stats)
-        stats->total_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    total();
     return FA_OK;
 }
 
-int fa_ext_batch_learned(fa_ctx *c, const fa_params *p, const fa_policy *pol, const fa_band_model *model,
-                         float margin, const fa_job *jobs, uint32_t n, const uint8_t *qseq, uint64_t qseq_len,
-                         const uint8_t *tseq, uint64_t tseq_len, const fa_band_hint *hints, fa_ext_result *out,
-                         int32_t *w_first_out, int32_t *w_final, fa_ext_stats *stats) {
+// fa_ext_batch_learned / fa_ext_batch_learned_packed on host buffers of either form.
+int ext_learned_host(fa_ctx *c, const fa_params *p, const fa_policy *pol, const fa_band_model *model, float margin,
+                     const fa_job *jobs, uint32_t n, const HostSeq &hq, const HostSeq &ht, const fa_band_hint *hints,
+                     fa_ext_result *out, int32_t *w_first_out, int32_t *w_final, fa_ext_stats *stats) {
     auto t0 = std::chrono::steady_clock::now();
-    if (!c) return fail(FA_ERR_ARG, "null context");
-    if (!model) return fail(FA_ERR_STATE, "no band model");
-    if (!pol || pol->mode != FA_POLICY_LEARNED) return fail(FA_ERR_ARG, "fa_ext_batch_learned needs FA_POLICY_LEARNED");
-    if (int rc = check_params(p)) return rc;
-    if (stats) memset(stats, 0, sizeof(*stats));
-    if (n == 0) return FA_OK;
-    if (!jobs || !out || !qseq || !tseq) return fail(FA_ERR_ARG, "null buffer");
-    FA_CUDA(cudaSetDevice(c->device));
     const ExtParams kp = ext_params_of(p);
+    auto total = [&]() {
+        if (stats)
+            stats->total_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    };
+    if (!c->graph && n >= kPipeMinJobs) {
+        bool done = false;
+        int rc = ext_batch_sliced(c, kp, pol, model, margin, jobs, n, hq, ht, hints, nullptr, out, w_first_out,
+                                  w_final, stats, &done);
+        if (rc) return rc;
+        if (done) {
+            total();
+            return FA_OK;
+        }
+    }
     int max_q = 0;
-    if (int rc = check_jobs(jobs, n, qseq_len, tseq_len, kp, packed_qcap_limit(c->smem_optin), &max_q)) return rc;
+    if (int rc = check_jobs(jobs, n, hq.npos, ht.npos, kp, packed_qcap_limit(c->smem_optin), &max_q)) return rc;
     std::vector<uint32_t> order;
     std::vector<std::pair<uint32_t, int>> segs;
     length_order(jobs, n, order, segs);
-    if (int rc = ensure_ext_buffers(c, n, qseq_len, tseq_len)) return rc;
+    if (int rc = ensure_ext_buffers(c, n, 0, 0)) return rc;
+    if (int rc = ensure_seq_buffers(c, hq, ht)) return rc;
     if (int rc = ensure_policy_buffers(c, n)) return rc;
     FA_CUDA(c->feat.ensure(sizeof(float) * 16 * (size_t)n + sizeof(fa_band_hint) * (size_t)n));
     FA_CUDA(c->wbf.ensure(sizeof(__nv_bfloat16) * FA_BAND_NPARAMS));
     cudaStream_t s = c->stream;
     FA_CUDA(cudaMemcpyAsync(c->jobs.p, jobs, sizeof(fa_job) * (size_t)n, cudaMemcpyHostToDevice, s));
     FA_CUDA(cudaMemcpyAsync(c->order.p, order.data(), 4ull * n, cudaMemcpyHostToDevice, s));
-    FA_CUDA(cudaMemcpyAsync(c->qseq.p, qseq, qseq_len, cudaMemcpyHostToDevice, s));
-    FA_CUDA(cudaMemcpyAsync(c->tseq.p, tseq, tseq_len, cudaMemcpyHostToDevice, s));
+    FA_CUDA(cudaMemcpyAsync(c->qseq.p, hq.p, hq.nbytes, cudaMemcpyHostToDevice, s));
+    FA_CUDA(cudaMemcpyAsync(c->tseq.p, ht.p, ht.nbytes, cudaMemcpyHostToDevice, s));
+    if (int rc = upload_runs(c, hq, ht, s)) return rc;
     float *d_x = c->feat.as<float>();
     fa_band_hint *d_h = hints ? reinterpret_cast<fa_band_hint *>(d_x + 16 * (size_t)n) : nullptr;
     if (hints) FA_CUDA(cudaMemcpyAsync(d_h, hints, sizeof(fa_band_hint) * (size_t)n, cudaMemcpyHostToDevice, s));
@@ -994,8 +1165,7 @@ int fa_ext_batch_learned(fa_ctx *c, const fa_params *p, const fa_policy *pol, co
     band_model_export(model, wbf, mean, sd);
     FA_CUDA(cudaMemcpyAsync(c->wbf.p, wbf.data(), sizeof(__nv_bfloat16) * FA_BAND_NPARAMS, cudaMemcpyHostToDevice, s));
     auto predict = [&](cudaStream_t st, uint32_t *launches) -> int {
-        FA_CUDA(launch_band_features(c->jobs.as<fa_job>(), n, c->qseq.as<uint8_t>(), qseq_len, c->tseq.as<uint8_t>(),
-                                     tseq_len, d_h, kp.max_score, d_x, st));
+        FA_CUDA(launch_band_features(c->jobs.as<fa_job>(), n, c->cq, c->ct, d_h, kp.max_score, d_x, st));
         FA_CUDA(launch_band_predict(c->wbf.as<__nv_bfloat16>(), mean, sd, d_x, c->jobs.as<fa_job>(), n, margin,
                                     pol->w_min, nullptr, c->w_first.as<int32_t>(), st));
         *launches += 2;
@@ -1003,7 +1173,7 @@ int fa_ext_batch_learned(fa_ctx *c, const fa_params *p, const fa_policy *pol, co
     };
     if (c->graph) {
         // features, prediction and every round in one graph
-        std::vector<uint64_t> extra{qseq_len, tseq_len, (uint64_t)(uintptr_t)d_h};
+        std::vector<uint64_t> extra{hq.nbytes, ht.nbytes, (uint64_t)(uintptr_t)d_h};
         uint32_t mb;
         memcpy(&mb, &margin, 4);
         extra.push_back(mb);
@@ -1014,14 +1184,12 @@ int fa_ext_batch_learned(fa_ctx *c, const fa_params *p, const fa_policy *pol, co
             extra.push_back((uint64_t)a << 32 | b);
         }
         int rc = run_ext_graph(c, kp, pol, n, segs, max_q, max_band_of(jobs, n), extra, predict,
-                               c->w_first.as<int32_t>(),
-                               s, stats, w_final);
+                               c->w_first.as<int32_t>(), s, stats, w_final);
         if (rc) return rc;
         if (w_first_out) FA_CUDA(cudaMemcpy(w_first_out, c->w_first.p, 4ull * n, cudaMemcpyDeviceToHost));
         FA_CUDA(cudaMemcpyAsync(out, c->out.p, sizeof(fa_ext_result) * (size_t)n, cudaMemcpyDeviceToHost, s));
         FA_CUDA(cudaStreamSynchronize(s));
-        if (stats)
-            stats->total_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        total();
         return FA_OK;
     }
     FA_CUDA(cudaEventRecord(c->ev0, s));
@@ -1034,33 +1202,33 @@ int fa_ext_batch_learned(fa_ctx *c, const fa_params *p, const fa_policy *pol, co
     FA_CUDA(cudaEventSynchronize(c->ev1));
     cudaEventElapsedTime(&pred_ms, c->ev0, c->ev1);
     if (w_first_out) FA_CUDA(cudaMemcpy(w_first_out, c->w_first.p, 4ull * n, cudaMemcpyDeviceToHost));
-    int rc = run_ext(c, kp, pol, n, segs, max_q, max_band_of(jobs, n), c->jobs.as<fa_job>(), c->order.as<uint32_t>(), c->qseq.as<uint8_t>(),
-                     c->tseq.as<uint8_t>(), c->w_first.as<int32_t>(), c->out.as<fa_ext_result>(), s, stats, w_final);
+    int rc = run_ext(c, kp, pol, n, segs, max_q, max_band_of(jobs, n), c->jobs.as<fa_job>(), c->order.as<uint32_t>(),
+                     c->cq, c->ct, c->w_first.as<int32_t>(), c->out.as<fa_ext_result>(), s, stats, w_final);
     if (rc) return rc;
     FA_CUDA(cudaMemcpyAsync(out, c->out.p, sizeof(fa_ext_result) * (size_t)n, cudaMemcpyDeviceToHost, s));
     FA_CUDA(cudaStreamSynchronize(s));
     if (stats) {
         stats->kernel_ms += pred_ms;
         stats->kernel_launches += 2;
-        stats->total_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
+    total();
     return FA_OK;
 }
 
-int fa_ext_batch(fa_ctx *c, const fa_params *p, const fa_job *jobs, uint32_t n, const uint8_t *qseq,
-                 uint64_t qseq_len, const uint8_t *tseq, uint64_t tseq_len, fa_ext_result *out,
-                 fa_ext_stats *stats) {
-    return fa_ext_batch_policy(c, p, nullptr, jobs, n, qseq, qseq_len, tseq, tseq_len, nullptr, out,
-                               nullptr, stats);
-}
-
-int fa_ext_batch_device(fa_ctx *c, const fa_params *p, const fa_job *d_jobs, uint32_t n,
-                        const uint8_t *d_qseq, const uint8_t *d_tseq, const uint32_t *d_order,
-                        fa_ext_result *d_out, void *stream) {
+// Argument checks shared by the host extension entry points.
+int check_host_call(fa_ctx *c, const fa_params *p, const fa_policy *pol, const fa_job *jobs, uint32_t n,
+                    const void *out) {
     if (!c) return fail(FA_ERR_ARG, "null context");
     if (int rc = check_params(p)) return rc;
     if (n == 0) return FA_OK;
-    if (!d_jobs || !d_qseq || !d_tseq || !d_out) return fail(FA_ERR_ARG, "null buffer");
+    if (!jobs || !out) return fail(FA_ERR_ARG, "null buffer");
+    if (pol && (pol->mode < FA_POLICY_SINGLE || pol->mode > FA_POLICY_LEARNED))
+        return fail(FA_ERR_ARG, "unknown policy mode %d", pol->mode);
+    return FA_OK;
+}
+
+int ext_batch_device(fa_ctx *c, const fa_params *p, const fa_job *d_jobs, uint32_t n, const SeqBuf &d_qseq,
+                     const SeqBuf &d_tseq, const uint32_t *d_order, fa_ext_result *d_out, void *stream) {
     FA_CUDA(cudaSetDevice(c->device));
     const ExtParams kp = ext_params_of(p);
     cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
@@ -1128,6 +1296,195 @@ int fa_ext_batch_device(fa_ctx *c, const fa_params *p, const fa_job *d_jobs, uin
     for (size_t k = 0; k < segs.size(); ++k) c->last_launches += ext_kernels_of(c, seg_kc[k], kp, segs[k].second);
     c->last_stream = s;
     return FA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *fa_last_error(void) { return g_err.c_str(); }
+const char *fa_version(void) { return "ferrous_b200 0.1 (sm_100a)"; }
+
+int fa_ctx_create(int device, fa_ctx **out) {
+    if (!out) return fail(FA_ERR_ARG, "null out");
+    *out = nullptr;
+    int ndev = 0;
+    FA_CUDA(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) return fail(FA_ERR_ARG, "device %d not present (%d)", device, ndev);
+    FA_CUDA(cudaSetDevice(device));
+    fa_ctx *c = new fa_ctx();
+    c->device = device;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major < 10) {
+        delete c;
+        return fail(FA_ERR_CUDA, "device %d is not sm_100-class", device);
+    }
+    c->sm_count = prop.multiProcessorCount;
+    c->smem_optin = prop.sharedMemPerBlockOptin;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+        delete c;
+        return fail(FA_ERR_CUDA, "stream/event creation failed");
+    }
+    *out = c;
+    return FA_OK;
+}
+
+void fa_ctx_destroy(fa_ctx *c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    for (DevBuf *b : {&c->jobs, &c->order, &c->qseq, &c->tseq, &c->out, &c->clamped, &c->cells_job,
+                      &c->misc, &c->w_first, &c->w_cur, &c->prev, &c->kk, &c->w_final, &c->tries,
+                      &c->missed, &c->list_a, &c->list_b, &c->hist, &c->feat, &c->wbf, &c->part_n,
+                      &c->part_w, &c->ovf, &c->reg_in, &c->reg_out, &c->col_in, &c->col_plan, &c->col_out,
+                      &c->cg_in, &c->cg_scratch, &c->cg_out, &c->mc_in, &c->mc_plan, &c->mc_out, &c->is_buf,
+                      &c->qruns, &c->truns})
+        b->release();
+    for (auto &pr : c->span_ev)
+        for (auto &e : pr)
+            if (e) cudaEventDestroy(e);
+    for (int k = 0; k < 2; ++k) {
+        if (c->join_ev[k]) cudaEventDestroy(c->join_ev[k]);
+        if (c->aux[k]) cudaStreamDestroy(c->aux[k]);
+    }
+    if (c->fork_ev) cudaEventDestroy(c->fork_ev);
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    for (auto &e : c->slice_ev)
+        if (e) cudaEventDestroy(e);
+    for (auto &e : c->done_ev)
+        if (e) cudaEventDestroy(e);
+    if (c->jobs_ev) cudaEventDestroy(c->jobs_ev);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+    c->chunk_scratch.release();
+    if (c->kev0) cudaEventDestroy(c->kev0);
+    if (c->kev1) cudaEventDestroy(c->kev1);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+int fa_probe_int_peak(fa_ctx *c, int kind, double *ops_per_s, float *ms) {
+    if (!c || !ops_per_s) return fail(FA_ERR_ARG, "null argument");
+    if (kind < 0 || kind > 4) return fail(FA_ERR_ARG, "unknown probe kind %d", kind);
+    FA_CUDA(cudaSetDevice(c->device));
+    const double r = probe_int_peak(kind, c->sm_count, c->stream, ms);
+    if (r <= 0) return fail(FA_ERR_CUDA, "probe kernel failed");
+    *ops_per_s = r;
+    return FA_OK;
+}
+
+int fa_device_info(fa_ctx *c, int *sm_count, int *smem_optin_bytes) {
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    if (sm_count) *sm_count = c->sm_count;
+    if (smem_optin_bytes) *smem_optin_bytes = (int)c->smem_optin;
+    return FA_OK;
+}
+
+uint32_t fa_mate_xtra(int32_t mate_len, int32_t match_score, int32_t min_seed_len) {
+    uint32_t x = FA_KSW_XSUBO | FA_KSW_XSTART;
+    if (mate_len * match_score < 250) x |= FA_KSW_XBYTE;
+    return x | (uint32_t)(min_seed_len * match_score);
+}
+
+int fa_ext_batch_policy(fa_ctx *c, const fa_params *p, const fa_policy *pol, const fa_job *jobs,
+                        uint32_t n, const uint8_t *qseq, uint64_t qseq_len, const uint8_t *tseq,
+                        uint64_t tseq_len, const int32_t *w_first, fa_ext_result *out,
+                        int32_t *w_final, fa_ext_stats *stats) {
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (int rc = check_host_call(c, p, pol, jobs, n, out)) return rc;
+    if (n == 0) return FA_OK;
+    if (!qseq || !tseq) return fail(FA_ERR_ARG, "null buffer");
+    if (pol && pol->mode == FA_POLICY_LEARNED && !w_first)
+        return fail(FA_ERR_STATE, "learned policy needs w_first (or a loaded band model)");
+    FA_CUDA(cudaSetDevice(c->device));
+    return ext_batch_host(c, p, pol, jobs, n, host_bytes(qseq, qseq_len), host_bytes(tseq, tseq_len), w_first, out,
+                          w_final, stats);
+}
+
+int fa_ext_batch_packed(fa_ctx *c, const fa_params *p, const fa_policy *pol, const fa_job *jobs, uint32_t n,
+                        const fa_packed_seq *qseq, const fa_packed_seq *tseq, const int32_t *w_first,
+                        fa_ext_result *out, int32_t *w_final, fa_ext_stats *stats) {
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (int rc = check_host_call(c, p, pol, jobs, n, out)) return rc;
+    if (n == 0) return FA_OK;
+    HostSeq hq, ht;
+    if (int rc = host_packed(qseq, "query", &hq)) return rc;
+    if (int rc = host_packed(tseq, "target", &ht)) return rc;
+    if (pol && pol->mode == FA_POLICY_LEARNED && !w_first)
+        return fail(FA_ERR_STATE, "learned policy needs w_first (or a band model: fa_ext_batch_learned_packed)");
+    FA_CUDA(cudaSetDevice(c->device));
+    return ext_batch_host(c, p, pol, jobs, n, hq, ht, w_first, out, w_final, stats);
+}
+
+int fa_ext_batch_learned(fa_ctx *c, const fa_params *p, const fa_policy *pol, const fa_band_model *model,
+                         float margin, const fa_job *jobs, uint32_t n, const uint8_t *qseq, uint64_t qseq_len,
+                         const uint8_t *tseq, uint64_t tseq_len, const fa_band_hint *hints, fa_ext_result *out,
+                         int32_t *w_first_out, int32_t *w_final, fa_ext_stats *stats) {
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    if (!model) return fail(FA_ERR_STATE, "no band model");
+    if (!pol || pol->mode != FA_POLICY_LEARNED) return fail(FA_ERR_ARG, "fa_ext_batch_learned needs FA_POLICY_LEARNED");
+    if (int rc = check_host_call(c, p, pol, jobs, n, out)) return rc;
+    if (n == 0) return FA_OK;
+    if (!qseq || !tseq) return fail(FA_ERR_ARG, "null buffer");
+    FA_CUDA(cudaSetDevice(c->device));
+    return ext_learned_host(c, p, pol, model, margin, jobs, n, host_bytes(qseq, qseq_len), host_bytes(tseq, tseq_len),
+                            hints, out, w_first_out, w_final, stats);
+}
+
+int fa_ext_batch_learned_packed(fa_ctx *c, const fa_params *p, const fa_policy *pol, const fa_band_model *model,
+                                float margin, const fa_job *jobs, uint32_t n, const fa_packed_seq *qseq,
+                                const fa_packed_seq *tseq, const fa_band_hint *hints, fa_ext_result *out,
+                                int32_t *w_first_out, int32_t *w_final, fa_ext_stats *stats) {
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    if (!model) return fail(FA_ERR_STATE, "no band model");
+    if (!pol || pol->mode != FA_POLICY_LEARNED)
+        return fail(FA_ERR_ARG, "fa_ext_batch_learned_packed needs FA_POLICY_LEARNED");
+    if (int rc = check_host_call(c, p, pol, jobs, n, out)) return rc;
+    if (n == 0) return FA_OK;
+    HostSeq hq, ht;
+    if (int rc = host_packed(qseq, "query", &hq)) return rc;
+    if (int rc = host_packed(tseq, "target", &ht)) return rc;
+    FA_CUDA(cudaSetDevice(c->device));
+    return ext_learned_host(c, p, pol, model, margin, jobs, n, hq, ht, hints, out, w_first_out, w_final, stats);
+}
+
+int fa_ext_batch(fa_ctx *c, const fa_params *p, const fa_job *jobs, uint32_t n, const uint8_t *qseq,
+                 uint64_t qseq_len, const uint8_t *tseq, uint64_t tseq_len, fa_ext_result *out,
+                 fa_ext_stats *stats) {
+    return fa_ext_batch_policy(c, p, nullptr, jobs, n, qseq, qseq_len, tseq, tseq_len, nullptr, out,
+                               nullptr, stats);
+}
+
+int fa_ext_batch_device(fa_ctx *c, const fa_params *p, const fa_job *d_jobs, uint32_t n,
+                        const uint8_t *d_qseq, const uint8_t *d_tseq, const uint32_t *d_order,
+                        fa_ext_result *d_out, void *stream) {
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    if (int rc = check_params(p)) return rc;
+    if (n == 0) return FA_OK;
+    if (!d_jobs || !d_qseq || !d_tseq || !d_out) return fail(FA_ERR_ARG, "null buffer");
+    // byte codes: the kernels take the caller's word that every job lies inside the buffers
+    return ext_batch_device(c, p, d_jobs, n, SeqBuf{d_qseq, ~0ull, nullptr, 0, 0}, SeqBuf{d_tseq, ~0ull, nullptr, 0, 0},
+                            d_order, d_out, stream);
+}
+
+int fa_ext_batch_packed_device(fa_ctx *c, const fa_params *p, const fa_job *d_jobs, uint32_t n,
+                               const fa_packed_seq *d_qseq, const fa_packed_seq *d_tseq, const uint32_t *d_order,
+                               fa_ext_result *d_out, void *stream) {
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    if (int rc = check_params(p)) return rc;
+    if (n == 0) return FA_OK;
+    if (!d_jobs || !d_qseq || !d_tseq || !d_out) return fail(FA_ERR_ARG, "null buffer");
+    SeqBuf q, t;
+    for (auto [src, dst, what] : {std::tuple{d_qseq, &q, "query"}, std::tuple{d_tseq, &t, "target"}}) {
+        if (!src->bases || (src->n_nruns && !src->n_runs)) return fail(FA_ERR_ARG, "null packed %s buffer", what);
+        if ((uintptr_t)src->bases % 4) return fail(FA_ERR_ARG, "packed %s bases must be 4-byte aligned", what);
+        if (src->n_nruns >= (1ull << 32)) return fail(FA_ERR_CAPACITY, "packed %s buffer: too many N runs", what);
+        *dst = SeqBuf{src->bases, (src->n_bases + 3) / 4, src->n_runs, (uint32_t)src->n_nruns, 1};
+    }
+    return ext_batch_device(c, p, d_jobs, n, q, t, d_order, d_out, stream);
 }
 
 int fa_ctx_set_kernel(fa_ctx *c, int kernel) {

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "fa_device.cuh"
+#include "fa_packed.cuh"
 
 namespace fa {
 
@@ -19,8 +20,8 @@ constexpr int kPairThreads = 32;     // threads per int16x2 extension block (2 j
 
 size_t ext_packed_smem_bytes(int qcap, int ring, int tpb);
 cudaError_t launch_ext_packed(const fa_job *d_jobs, const uint32_t *d_order, uint32_t n,
-                              const uint32_t *d_first, const uint32_t *d_n, const uint8_t *d_qseq,
-                              const uint8_t *d_tseq, const ExtParams &p, int qcap, int ring,
+                              const uint32_t *d_first, const uint32_t *d_n, const SeqBuf &d_qseq,
+                              const SeqBuf &d_tseq, const ExtParams &p, int qcap, int ring,
                               const int32_t *d_w_try, fa_ext_result *d_out, uint8_t *d_clamped, bool cert,
                               uint32_t *d_cells_job, unsigned long long *d_cells, uint32_t *d_status,
                               cudaStream_t stream, int tpb = kExtThreads);
@@ -29,9 +30,10 @@ cudaError_t launch_ext_packed(const fa_job *d_jobs, const uint32_t *d_order, uin
 // bwa-form scoring matrices; same arguments and results as launch_ext_packed.
 bool ext_pair_eligible(const ExtParams &p);
 size_t ext_pair_smem_bytes(int qcap);
+// Byte-code sequences only (cudaErrorNotSupported for packed ones).
 cudaError_t launch_ext_pair(const fa_job *d_jobs, const uint32_t *d_order, uint32_t n, const uint32_t *d_n,
-                            const uint8_t *d_qseq,
-                            const uint8_t *d_tseq, const ExtParams &p, int qcap, const int32_t *d_w_try,
+                            const SeqBuf &d_qseq, const SeqBuf &d_tseq, const ExtParams &p, int qcap,
+                            const int32_t *d_w_try,
                             fa_ext_result *d_out, uint8_t *d_clamped, uint32_t *d_cells_job,
                             unsigned long long *d_cells, uint32_t *d_status, cudaStream_t stream);
 
@@ -47,7 +49,7 @@ cudaError_t launch_ext_pair(const fa_job *d_jobs, const uint32_t *d_order, uint3
 bool ext_rows2_eligible(const ExtParams &p, int qcap);
 size_t ext_rows2_smem_bytes(int qcap, int tpb, int ring);
 cudaError_t launch_ext_rows2(const fa_job *d_jobs, const uint32_t *d_order, uint32_t n, const uint32_t *d_first,
-                             const uint32_t *d_n, const uint8_t *d_qseq, const uint8_t *d_tseq, const ExtParams &p,
+                             const uint32_t *d_n, const SeqBuf &d_qseq, const SeqBuf &d_tseq, const ExtParams &p,
                              int qcap, int ring, bool cert, const int32_t *d_w_try, fa_ext_result *d_out,
                              uint8_t *d_clamped, uint32_t *d_cells_job, unsigned long long *d_cells,
                              uint32_t *d_status, uint32_t *d_ovf, uint32_t *d_ovf_n, cudaStream_t stream, int tpb,
@@ -85,10 +87,13 @@ cudaError_t launch_mate_sw(bool byte_lanes, const fa_mate_job *d_jobs, const uin
 // {status bits, first bad job, longest query, widest configured band} | bounds[nchunks+1] |
 // each chunk's lowest and highest job index.  A job belongs to the chunk that holds the
 // last byte of its query or of its target, whichever comes later; chunk k of a buffer ends
-// at byte end[k] (exclusive; the last end is the buffer's length).
+// at byte end[k] (exclusive; the last end is the buffer's length).  shift: log2 of the
+// positions per byte (0 for byte codes, 2 for packed bases); qbytes / tbytes of the prep
+// are then the buffers' lengths in positions.
 constexpr int kMaxChunks = 8;
 struct ChunkEnds {
     uint64_t q[kMaxChunks], t[kMaxChunks];
+    int shift;
 };
 size_t chunk_scratch_bytes(int nchunks);
 // h0_min: the smallest valid h0 (1, or 0 with FA_PARAM_H0_ZERO)
@@ -105,9 +110,8 @@ cudaError_t launch_qlen_scatter(const fa_job *d_jobs, uint32_t n, uint32_t *d_cu
 // Device copies of the query / target byte arrays are allocated kSeqPad bytes longer than
 // their contents, so readers of aligned 32-bit words never leave the allocation.
 constexpr uint64_t kSeqPad = 16;
-cudaError_t launch_band_features(const fa_job *d_jobs, uint32_t n, const uint8_t *d_q, uint64_t qbytes,
-                                 const uint8_t *d_t, uint64_t tbytes, const fa_band_hint *d_hints, int max_score,
-                                 float *d_x, cudaStream_t s);
+cudaError_t launch_band_features(const fa_job *d_jobs, uint32_t n, const SeqBuf &d_q, const SeqBuf &d_t,
+                                 const fa_band_hint *d_hints, int max_score, float *d_x, cudaStream_t s);
 cudaError_t launch_band_predict(const __nv_bfloat16 *d_wbf, const float *mean, const float *std_, const float *d_x,
                                 const fa_job *d_jobs, uint32_t n, float margin, int w_min, float *d_y,
                                 int32_t *d_w, cudaStream_t s);

@@ -151,7 +151,8 @@ extern "C" int fa_ext_batch_device_noalloc(const fa_params *p, const fa_job *d_j
     NA_CUDA(launch_qlen_scatter(d_jobs, n, sc->hist, sc->order, s));
     uint32_t b = 0;
     for (int k = 0; k < nseg; ++k) {
-        NA_CUDA(launch_ext_packed(d_jobs, sc->order + b, seg_end[k] - b, nullptr, nullptr, d_qseq, d_tseq, kp,
+        NA_CUDA(launch_ext_packed(d_jobs, sc->order + b, seg_end[k] - b, nullptr, nullptr,
+                                  SeqBuf{d_qseq, ~0ull, nullptr, 0, 0}, SeqBuf{d_tseq, ~0ull, nullptr, 0, 0}, kp,
                                   seg_cap[k], 0, nullptr, d_out, nullptr, false, nullptr, nullptr, sc->status, s));
         b = seg_end[k];
     }

@@ -131,8 +131,8 @@ constexpr int kChunkBins = FA_MAX_QLEN + 1;
 
 // the chunk of a job: the one holding the later of its query's and its target's last byte
 __device__ __forceinline__ int chunk_of(const fa_job &jb, const ChunkEnds &ends, int nchunks) {
-    const uint64_t lq = jb.q_off + (uint64_t)jb.qlen - 1;
-    const uint64_t lt = jb.tlen > 0 ? jb.t_off + (uint64_t)jb.tlen - 1 : 0;
+    const uint64_t lq = (jb.q_off + (uint64_t)jb.qlen - 1) >> ends.shift;
+    const uint64_t lt = jb.tlen > 0 ? (jb.t_off + (uint64_t)jb.tlen - 1) >> ends.shift : 0;
     // the ends are increasing, so the count of ends at or below a byte is its chunk; the
     // later of the two chunks is the larger count
     int cq = 0, ct = 0;

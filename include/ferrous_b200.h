@@ -198,6 +198,43 @@ int fa_ext_batch_device(fa_ctx *ctx, const fa_params *p, const fa_job *d_jobs, u
  * kernels detected. */
 int fa_ctx_sync(fa_ctx *ctx);
 
+/* ---- 2-bit packed sequences (no reference counterpart) ------------------
+ * The same extension on sequences held 2 bits per base, a quarter of the bytes to move and
+ * read: base k is bits 2*(k % 4) .. 2*(k % 4) + 1 of byte k / 4 (A=0 C=1 G=2 T=3), and the N
+ * bases (code 4, which 2 bits cannot hold) are listed as sorted, non-overlapping runs -- the
+ * way the reference's index keeps a 2-bit .pac beside its ambiguous stretches
+ * (src/pipelines/linear/index/bntseq.rs:451-535).  The packed value stored at an N position
+ * is ignored.  Job offsets q_off / t_off and lengths count bases; left jobs are reversed by
+ * the caller as with byte codes.  Results are identical to the byte-code entry points on the
+ * same bases. */
+typedef struct {
+    uint64_t pos;               /* first base of the run */
+    uint64_t len;               /* bases; pos + len <= n_bases */
+} fa_nrun;
+
+typedef struct {
+    const uint8_t *bases;       /* (n_bases + 3) / 4 bytes; device pointers must be 4-byte aligned */
+    uint64_t n_bases;
+    const fa_nrun *n_runs;      /* sorted by pos, non-overlapping; NULL when n_nruns == 0 */
+    uint64_t n_nruns;           /* at most 2^32 - 1 */
+} fa_packed_seq;
+
+/* fa_ext_batch_policy on packed host buffers: same policies, results, statistics and
+ * errors.  Batches of 32,768 jobs or more upload the packed bases in slices under the kernels
+ * (job records first); with every job's sequences at increasing offsets in job order and a
+ * pinned `out`, results return slice by slice behind the uploads.  FA_POLICY_BWA and
+ * FA_POLICY_LEARNED batches (w_first given) run their rounds slice by slice as each slice
+ * arrives. */
+int fa_ext_batch_packed(fa_ctx *ctx, const fa_params *p, const fa_policy *pol, const fa_job *jobs, uint32_t n,
+                        const fa_packed_seq *qseq, const fa_packed_seq *tseq, const int32_t *w_first,
+                        fa_ext_result *out, int32_t *w_final, fa_ext_stats *stats);
+
+/* fa_ext_batch_device on packed device buffers (the fa_packed_seq structs themselves are host
+ * memory holding device pointers). */
+int fa_ext_batch_packed_device(fa_ctx *ctx, const fa_params *p, const fa_job *d_jobs, uint32_t n,
+                               const fa_packed_seq *d_qseq, const fa_packed_seq *d_tseq, const uint32_t *d_order,
+                               fa_ext_result *d_out, void *stream);
+
 /* Extension kernel choice for this context (no reference counterpart):
  * FA_KERNEL_AUTO     autotuned: the fastest exact candidate measured on the call's data;
  * FA_KERNEL_INT32    int32 cells, one job per thread;
@@ -526,6 +563,17 @@ int  fa_ext_batch_learned(fa_ctx *ctx, const fa_params *p, const fa_policy *pol,
                           const uint8_t *qseq, uint64_t qseq_len, const uint8_t *tseq, uint64_t tseq_len,
                           const fa_band_hint *hints, fa_ext_result *out, int32_t *w_first_out,
                           int32_t *w_final, fa_ext_stats *stats);
+/* Learned-band extension on 2-bit packed host buffers (fa_packed_seq above): same results,
+ * bands and statistics as fa_ext_batch_learned on the same bases.  Batches of 32,768 jobs or
+ * more whose jobs address their sequences at increasing offsets in job order run slice by
+ * slice: each slice's job records, hints and bases go up on a copy stream while the slices
+ * before it run features, prediction and every extension round on the device, and each
+ * slice's results come back as soon as its rounds are done (into a pinned `out`). */
+int  fa_ext_batch_learned_packed(fa_ctx *ctx, const fa_params *p, const fa_policy *pol,
+                                 const fa_band_model *model, float margin, const fa_job *jobs, uint32_t n,
+                                 const fa_packed_seq *qseq, const fa_packed_seq *tseq,
+                                 const fa_band_hint *hints, fa_ext_result *out, int32_t *w_first_out,
+                                 int32_t *w_final, fa_ext_stats *stats);
 
 /* Device-resident variant (no reference counterpart): device pointers, kernels
  * asynchronous on `stream` after one small synchronous read of the batch's job

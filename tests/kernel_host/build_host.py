@@ -6,7 +6,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 CSRC = HERE.parent.parent / "ferrousalign_b200" / "csrc"
-COMMON = [CSRC / "fa_kernels.h", CSRC / "fa_device.cuh"]
+COMMON = [CSRC / "fa_kernels.h", CSRC / "fa_device.cuh", CSRC / "fa_packed.cuh"]
 HARNESSES = {
     "pair": (HERE / "pair_host.cu", [CSRC / "extend_pair_kernel.cu"]),
     "rows2": (HERE / "rows2_host.cu",

@@ -7,11 +7,14 @@
 
 namespace {
 template <bool SYM, bool CERT, int RING>
-uint32_t run_one(uint32_t jid, uint16_t *eh, uint8_t *sb, const fa_job *jobs, const uint8_t *qseq,
-                 const uint8_t *tseq, const fa::ExtParams &k, int qcap, const int32_t *w_try, fa_ext_result *out,
+uint32_t run_one(uint32_t jid, uint16_t *eh, uint8_t *sb, const fa_job *jobs, const fa::SeqBuf &qs,
+                 const fa::SeqBuf &ts, const fa::ExtParams &k, int qcap, const int32_t *w_try, fa_ext_result *out,
                  uint8_t *flags, uint32_t *status, uint32_t *ovf, uint32_t *ovf_n) {
-    return fa::rows2_thread<1, SYM, CERT, RING>(jid, eh, sb, jobs, qseq, tseq, k, qcap, w_try, out, flags, nullptr,
-                                                status, ovf, ovf_n);
+    if (qs.packed)
+        return fa::rows2_thread<1, SYM, CERT, RING, true>(jid, eh, sb, jobs, qs, ts, k, qcap, w_try, out, flags,
+                                                          nullptr, status, ovf, ovf_n);
+    return fa::rows2_thread<1, SYM, CERT, RING, false>(jid, eh, sb, jobs, qs, ts, k, qcap, w_try, out, flags, nullptr,
+                                                       status, ovf, ovf_n);
 }
 }  // namespace
 
@@ -19,10 +22,18 @@ uint32_t run_one(uint32_t jid, uint16_t *eh, uint8_t *sb, const fa_job *jobs, co
 // scores can pass 255 are listed in ovf[0..*ovf_n) instead, as the kernel hands them on.
 // cert: evaluate the certificate into flags[jid]; ring: 0, 32 or 64 column slots.
 // w_try (optional): per-job band of this run, as the learned rounds pass it.
+// Sequences: byte codes (qpk / tpk NULL), or 2-bit packed buffers (fa_packed_seq, host
+// memory) read through the kernels' packed reader.
 extern "C" int rows2_host_run(const fa_params *prm, const fa_job *jobs, const uint32_t *order, uint32_t n,
                               const uint8_t *qseq, const uint8_t *tseq, int qcap, int cert, int ring,
                               const int32_t *w_try, fa_ext_result *out, uint8_t *flags, uint32_t *cells,
-                              uint32_t *status, uint32_t *ovf, uint32_t *ovf_n) {
+                              uint32_t *status, uint32_t *ovf, uint32_t *ovf_n, const fa_packed_seq *qpk,
+                              const fa_packed_seq *tpk) {
+    fa::SeqBuf qs{qseq, ~0ull, nullptr, 0, 0}, ts{tseq, ~0ull, nullptr, 0, 0};
+    if (qpk && tpk) {
+        qs = fa::SeqBuf{qpk->bases, (qpk->n_bases + 3) / 4, qpk->n_runs, (uint32_t)qpk->n_nruns, 1};
+        ts = fa::SeqBuf{tpk->bases, (tpk->n_bases + 3) / 4, tpk->n_runs, (uint32_t)tpk->n_nruns, 1};
+    }
     fa::ExtParams k;
     for (int i = 0; i < 25; ++i) k.mat[i] = prm->mat[i];
     k.m = prm->m;
@@ -39,7 +50,7 @@ extern "C" int rows2_host_run(const fa_params *prm, const fa_job *jobs, const ui
     for (uint32_t g = 0; g < n; ++g) {
         const uint32_t j = order[g];
         uint32_t c = 0;
-#define RUN(S, C, R) c = run_one<S, C, R>(j, eh.data(), sb.data(), jobs, qseq, tseq, k, qcap, w_try, out, flags, \
+#define RUN(S, C, R) c = run_one<S, C, R>(j, eh.data(), sb.data(), jobs, qs, ts, k, qcap, w_try, out, flags, \
                                           status, ovf, ovf_n)
         if (cert) {
             if (ring == 32) { if (sym) RUN(true, true, 32); else RUN(false, true, 32); }

@@ -107,11 +107,11 @@ def rows2_lib(built):
     lib = C.CDLL(str(build_host.build("rows2")))
     lib.rows2_host_run.restype = C.c_int
     lib.rows2_host_run.argtypes = ([C.c_void_p] * 3 + [C.c_uint32, C.c_void_p, C.c_void_p] + [C.c_int] * 3
-                                   + [C.c_void_p] * 7)
+                                   + [C.c_void_p] * 9)
     return lib
 
 
-def run_rows2(lib, p, jobs, qseq, tseq, cert=0, ring=0, w_try=None):
+def run_rows2(lib, p, jobs, qseq, tseq, cert=0, ring=0, w_try=None, packed=None):
     """Longest-first order in 32-column capacity classes; returns results, per-job cells,
     status, the overflow jobs (the ones the kernel hands to the int32 kernel) and flags."""
     q = jobs["qlen"]
@@ -124,6 +124,7 @@ def run_rows2(lib, p, jobs, qseq, tseq, cert=0, ring=0, w_try=None):
     ovf = np.zeros(n, np.uint32)
     ovf_n = np.zeros(1, np.uint32)
     wt = None if w_try is None else np.ascontiguousarray(w_try, np.int32)
+    ps = None if packed is None else [packed[0].struct(), packed[1].struct()]
     s0 = 0
     while s0 < n:
         cap = (int(q[order[s0]]) + 31) // 32 * 32
@@ -134,14 +135,16 @@ def run_rows2(lib, p, jobs, qseq, tseq, cert=0, ring=0, w_try=None):
         rc = lib.rows2_host_run(p.ctypes.data, jobs.ctypes.data, sub.ctypes.data, len(sub), qseq.ctypes.data,
                                 tseq.ctypes.data, int(q[order[s0]]), cert, ring,
                                 None if wt is None else wt.ctypes.data, out.ctypes.data, flags.ctypes.data,
-                                cells.ctypes.data, st.ctypes.data, ovf.ctypes.data, ovf_n.ctypes.data)
+                                cells.ctypes.data, st.ctypes.data, ovf.ctypes.data, ovf_n.ctypes.data,
+                                None if packed is None else ps[0].ctypes.data,
+                                None if packed is None else ps[1].ctypes.data)
         assert rc == 0
         s0 = e0
     return out, cells, int(st[0]), np.sort(ovf[:int(ovf_n[0])]), flags
 
 
-def check_rows2(lib, p, jobs, qseq, tseq):
-    out, cells, st, ovf, _ = run_rows2(lib, p, jobs, qseq, tseq)
+def check_rows2(lib, p, jobs, qseq, tseq, packed=None):
+    out, cells, st, ovf, _ = run_rows2(lib, p, jobs, qseq, tseq, packed=packed)
     ref, tr = O.ext_batch(p, jobs, qseq, tseq)
     a = int(max(0, p["mat"][0].max()))
     wide = np.nonzero(jobs["h0"].astype(np.int64) + a * jobs["qlen"].astype(np.int64) > 255)[0]
@@ -323,3 +326,37 @@ def test_h0_zero_rejected_without_the_flag():
         O.ksw_extend2([0, 1, 2], [0, 1, 2], p["mat"][0], 6, 1, 6, 1, 100, 5, 100, 0)
     r, _ = O.ksw_extend2([0, 1, 2], [0, 1, 2], p["mat"][0], 6, 1, 6, 1, 100, 5, 100, 0, flags=N.FA_PARAM_H0_ZERO)
     assert (int(r["score"]), int(r["qle"]), int(r["tle"]), int(r["gtle"]), int(r["gscore"])) == (0, 0, 0, 1, 0)
+
+
+# ---- 2-bit packed sequences: the same thread body reading packed bases and N runs
+
+
+def test_pack_round_trip_and_runs():
+    rng = np.random.default_rng(3)
+    c = rng.integers(0, 4, 1001).astype(np.uint8)
+    c[[0, 5, 6, 7, 500, 1000]] = 4
+    ps = fa.pack(c)
+    assert ps.n_bases == 1001 and len(ps.runs) == 4
+    assert [tuple(int(x) for x in r) for r in ps.runs] == [(0, 1), (5, 3), (500, 1), (1000, 1)]
+    assert np.array_equal(fa.unpack(ps), c)
+
+
+@pytest.mark.parametrize("ring,cert", [(0, 0), (0, 1), (32, 1)])
+def test_rows2_packed_reads_match_oracle(rows2_lib, ring, cert):
+    """Uneven jobs with N-rich sequences (2% N, runs at job edges) through the two-row thread
+    body reading 2-bit packed buffers: results, cells and certificate flags equal the byte-code
+    run's and the oracle's."""
+    ref_seq = synth.reference(400_000, seed=12, n_rate=0.02, repeat_frac=0.05)
+    b = synth.ext_jobs(ref_seq, 1500, seed=23, read_len=(10, 160), seed_len=(3, 30), seed_at_start=False, w=20,
+                       indel_rates=(0.0, 0.02, 0.06), sub_rate=0.04)
+    p = fa.BandedPairWiseSW().to_struct()
+    qp, tp = fa.pack(b.qseq), fa.pack(b.tseq)
+    assert len(qp.runs) > 50 and len(tp.runs) > 50
+    w_try = np.full(len(b.jobs), 12 if ring else 20, np.int32)
+    got = run_rows2(rows2_lib, p, b.jobs, b.qseq, b.tseq, cert=cert, ring=ring, w_try=w_try, packed=(qp, tp))
+    byt = run_rows2(rows2_lib, p, b.jobs, b.qseq, b.tseq, cert=cert, ring=ring, w_try=w_try)
+    for a_, b_ in zip(got[:2] + got[3:], byt[:2] + byt[3:]):
+        assert np.array_equal(a_, b_)
+    assert got[2] == 0
+    if not cert:
+        check_rows2(rows2_lib, p, b.jobs, b.qseq, b.tseq, packed=(qp, tp))
