@@ -277,15 +277,15 @@ def bench_e2e_forms(args, ctx, b, p):
     byte_in = int(pj.nbytes + pq.nbytes + pt.nbytes)
     pack_in = int(pj.nbytes + qp.nbytes + tp.nbytes)
     hint_in = int(hints.nbytes)
+    o = {"ctx": ctx, "out": out_h, "bands": False}
     forms = {
-        "bytes_single": (lambda: fa.extend_batch(p, pj, pq, pt, ctx=ctx, out=out_h), byte_in),
-        "packed_single": (lambda: fa.extend_batch_packed(p, pj, qp, tp, ctx=ctx, out=out_h), pack_in),
-        "bytes_bwa": (lambda: fa.extend_batch(p, pj, pq, pt, policy=bwa, ctx=ctx, out=out_h), byte_in),
-        "packed_bwa": (lambda: fa.extend_batch_packed(p, pj, qp, tp, policy=bwa, ctx=ctx, out=out_h), pack_in),
-        "bytes_learned": (lambda: B.extend_batch_learned(p, pj, pq, pt, model, hints=hints, ctx=ctx, out=out_h),
-                          byte_in + hint_in),
-        "packed_learned": (lambda: fa.extend_batch_learned_packed(p, pj, qp, tp, model, hints=hints, ctx=ctx,
-                                                                  out=out_h), pack_in + hint_in),
+        "bytes_single": (lambda: fa.extend_batch(p, pj, pq, pt, **o), byte_in),
+        "packed_single": (lambda: fa.extend_batch_packed(p, pj, qp, tp, **o), pack_in),
+        "bytes_bwa": (lambda: fa.extend_batch(p, pj, pq, pt, policy=bwa, **o), byte_in),
+        "packed_bwa": (lambda: fa.extend_batch_packed(p, pj, qp, tp, policy=bwa, **o), pack_in),
+        "bytes_learned": (lambda: B.extend_batch_learned(p, pj, pq, pt, model, hints=hints, **o), byte_in + hint_in),
+        "packed_learned": (lambda: fa.extend_batch_learned_packed(p, pj, qp, tp, model, hints=hints, **o),
+                           pack_in + hint_in),
     }
     res, outs = {}, {}
     for name, (fn, h2d) in forms.items():
@@ -366,63 +366,54 @@ def bench_uneven(args, ctx, p):
 
 def bench_mixed(args, b, p):
     """Mixed batch: 500,000 mate-rescue pairs and the 1,000,000 seed extensions of one
-    batch, submitted together through the host ABI (two contexts on two host threads, so
-    the mate SW and the extensions run concurrently on the GPU), inputs in pinned host
+    batch, submitted together through one host ABI call (fa_pair_batch: the mate SW runs on
+    its own stream while the extension rounds run), inputs and results in pinned host
     memory, copies included.  Plain (bwa-mem2 policy) and learned-band forms; latency
     percentiles over the batches."""
-    import threading
-    import torch
     import ferrousalign_b200 as fa
     from ferrousalign_b200 import _native as N
     from ferrousalign_b200 import band_model as B
     from ferrousalign_b200 import synth
     m = synth.workload_mate(MATE_JOBS)
     mp = fa.make_mate_params()
-
-    def pin(a, dt=None):
-        t = torch.from_numpy(np.ascontiguousarray(a).view(np.uint8)).pin_memory().numpy()
-        return t.view(dt if dt is not None else a.dtype)
-
-    mj, mq, mt = pin(m.jobs, N.MATE_JOB_DT), pin(m.qseq), pin(m.tseq)
-    ej, eq, et = pin(b.jobs, N.JOB_DT), pin(b.qseq), pin(b.tseq)
-    hints = B.hints_from_info(b.info)
+    mj, mq, mt = pin_array(m.jobs), pin_array(m.qseq), pin_array(m.tseq)
+    ej, eq, et = pin_array(b.jobs), pin_array(b.qseq), pin_array(b.tseq)
+    hints = pin_array(B.hints_from_info(b.info))
     model = B.BandModel.load()
     bwa = fa.make_policy(N.FA_POLICY_BWA, 2)
-    ctx_e, ctx_m = N.Context(0), N.Context(0)
+    ctx = N.Context(0)
     res = {"workload": f"{MATE_JOBS} mate-rescue SW jobs (2x151 bp pairs, 551 bp windows) + {len(b.jobs)} "
-                       "151-bp seed extensions per batch, host ABI, pinned buffers, two concurrent contexts"}
+                       "151-bp seed extensions per batch, one fa_pair_batch call, pinned buffers"}
     outs = {}
     try:
         for form in ("plain", "learned"):
-            lat = []
+            eo = pin_array(np.zeros(len(b.jobs), N.EXT_RESULT_DT))
+            mo = pin_array(np.zeros(MATE_JOBS, N.KSWR_DT))
+            lat, kern, mkern = [], [], []
             for it in range(args.warmup + max(5, args.steps // 3)):
-                box = {}
-
-                def mate():
-                    box["mate"] = fa.mate_sw_batch(mp, mj, mq, mt, ctx=ctx_m)[0]
-
                 t0 = time.perf_counter()
-                th = threading.Thread(target=mate)
-                th.start()
                 if form == "plain":
-                    ext, _, _ = fa.extend_batch(p, ej, eq, et, policy=bwa, ctx=ctx_e)
+                    _, _, st, mst = fa.pair_batch(p, ej, eq, et, mp, mj, mq, mt, policy=bwa, ctx=ctx, out=eo,
+                                                  mate_out=mo)
                 else:
-                    ext, _, _, _ = B.extend_batch_learned(p, ej, eq, et, model, hints=hints, ctx=ctx_e)
-                th.join()
+                    _, _, st, mst = fa.pair_batch(p, ej, eq, et, mp, mj, mq, mt, model=model, hints=hints,
+                                                  ctx=ctx, out=eo, mate_out=mo)
                 dt = (time.perf_counter() - t0) * 1e3
                 if it >= args.warmup:
                     lat.append(dt)
-            outs[form] = (ext, box["mate"])
+                    kern.append(float(st["kernel_ms"]))
+                    mkern.append(float(mst["kernel_ms"]))
+            outs[form] = (eo.copy(), mo.copy())
             lat = np.array(lat)
             res[form] = {"batches": len(lat), "p50_ms": float(np.percentile(lat, 50)),
                          "p95_ms": float(np.percentile(lat, 95)), "p99_ms": float(np.percentile(lat, 99)),
                          "max_ms": float(lat.max()),
+                         "ext_kernel_ms_p50": float(np.median(kern)), "mate_kernel_ms_p50": float(np.median(mkern)),
                          "alignments_per_s": (MATE_JOBS + len(b.jobs)) / (float(np.median(lat)) * 1e-3)}
         res["identical_outputs"] = bool(np.array_equal(outs["plain"][0], outs["learned"][0]) and
                                         np.array_equal(outs["plain"][1], outs["learned"][1]))
     finally:
-        ctx_e.close()
-        ctx_m.close()
+        ctx.close()
     return res
 
 

@@ -15,6 +15,7 @@ from .mate_rescue import (MATE_RESCUE_SCORING_MATRIX, Kswr, MateRescueJob, MateR
 from .region import chain_seed_table, merge_scores_to_regions, region_opts  # noqa: F401
 from .collect import CollectedJobs, collect_extension_jobs, collect_opts, pack_reference  # noqa: F401
 from .cigar import CigarBatch, infer_band_width, scalar_banded_swa_batch  # noqa: F401
+from .pair_batch import pair_batch  # noqa: F401
 from .packed import PackedSeq, extend_batch_learned_packed, extend_batch_packed, pack, unpack  # noqa: F401
 
 __version__ = "0.1.0"

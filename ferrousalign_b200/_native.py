@@ -104,6 +104,7 @@ SIGNATURES = {
     "fa_ctx_set_timing": (C.c_int, [_P, C.c_int]),
     "fa_ctx_set_kernel": (C.c_int, [_P, C.c_int]),
     "fa_ctx_set_graph": (C.c_int, [_P, C.c_int]),
+    "fa_ctx_set_slices": (C.c_int, [_P, C.c_int, C.c_int]),
     "fa_ctx_set_threads": (C.c_int, [_P, C.c_int]),
     "fa_ctx_kernel_choice": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int, _P, _P, _P,
                                        C.POINTER(C.c_int)]),
@@ -127,6 +128,8 @@ SIGNATURES = {
     "fa_ext_batch_learned_packed": (C.c_int, [_P, _P, _P, _P, C.c_float, _P, C.c_uint32, _P, _P, _P, _P, _P, _P,
                                               _P]),
     "fa_mate_sw_batch": (C.c_int, [_P, _P, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64, _P, _P]),
+    "fa_pair_batch": (C.c_int, [_P, _P, _P, _P, C.c_float, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64, _P, _P,
+                                _P, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64, _P, _P, _P]),
     "fa_collect_ext_jobs": (C.c_int, [_P, _P, _P, C.c_uint64, _P, _P, C.c_uint32, _P, C.c_uint32, _P, C.c_uint32,
                                       _P, _P, _P, _P, C.c_uint64, _P, _P, _P, _P]),
     "fa_cigar_batch": (C.c_int, [_P, _P, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64, _P, _P, _P, _P]),
@@ -217,6 +220,10 @@ class Context:
         return {"kernel": names.get(k.value, str(k.value)), "threads_per_block": t.value,
                 "candidates": [{"kernel": names.get(ck[i], str(ck[i])), "threads_per_block": ct[i],
                                 "sample_ms": float(cm[i])} for i in range(min(nc.value, 8))]}
+
+    def set_slices(self, single_band: int = 0, policy_rounds: int = 0) -> None:
+        """Upload slices of large host batches (2..8; 0 keeps the current value)."""
+        check(load().fa_ctx_set_slices(self.handle, single_band, policy_rounds))
 
     def set_graph(self, enable: bool) -> None:
         """Run policy / learned batches as one recorded CUDA graph per batch shape."""

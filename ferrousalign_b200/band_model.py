@@ -149,22 +149,21 @@ def make_labels(params: np.ndarray, jobs: np.ndarray, qseq: np.ndarray, tseq: np
 def extend_batch_learned(params: np.ndarray, jobs: np.ndarray, qseq: np.ndarray, tseq: np.ndarray,
                          model: BandModel, hints: np.ndarray | None = None, judge: int = JUDGE_LEARNED,
                          margin: float = 0.0, w_min: int = 2, max_tries: int = 2, ctx: N.Context | None = None,
-                         out: np.ndarray | None = None):
+                         out: np.ndarray | None = None, bands: bool = True):
     """fa_ext_batch_learned: predicted first band, judge, doubling up to job.w, then the
     bwa-mem2 policy.  Returns (results, stats, w_first, w_final); `out` may be a (pinned)
-    result buffer to fill."""
+    result buffer to fill; bands=False asks for neither band array (None, None)."""
     from .batch_extension import make_policy
     ctx = ctx or N.default_context()
     jobs = np.ascontiguousarray(jobs, N.JOB_DT)
     n = len(jobs)
     out = np.zeros(n, N.EXT_RESULT_DT) if out is None else out
     stats = np.zeros(1, N.STATS_DT)
-    wf = np.zeros(n, np.int32)
-    wfin = np.zeros(n, np.int32)
+    wf = np.zeros(n, np.int32) if bands else None
+    wfin = np.zeros(n, np.int32) if bands else None
     pol = make_policy(N.FA_POLICY_LEARNED, max_tries, judge, w_min)
     h = None if hints is None else np.ascontiguousarray(hints, HINT_DT)
     N.check(N.load().fa_ext_batch_learned(ctx.handle, N.ptr(params), N.ptr(pol), model.handle, margin,
                                           jobs.ctypes.data, n, N.ptr(qseq), qseq.nbytes, N.ptr(tseq), tseq.nbytes,
-                                          N.ptr(h), out.ctypes.data, wf.ctypes.data, wfin.ctypes.data,
-                                          stats.ctypes.data))
+                                          N.ptr(h), out.ctypes.data, N.ptr(wf), N.ptr(wfin), stats.ctypes.data))
     return out, stats[0], wf, wfin

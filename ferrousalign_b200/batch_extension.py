@@ -156,9 +156,9 @@ def make_policy(mode: int = N.FA_POLICY_SINGLE, max_tries: int = 2, judge: int =
 
 def extend_batch(params: np.ndarray, jobs: np.ndarray, qseq: np.ndarray, tseq: np.ndarray,
                  policy: np.ndarray | None = None, w_first: np.ndarray | None = None,
-                 ctx: N.Context | None = None, out: np.ndarray | None = None):
+                 ctx: N.Context | None = None, out: np.ndarray | None = None, bands: bool = True):
     """Array-level call of fa_ext_batch_policy.  Returns (results, stats, w_final); `out`
-    may be a (pinned) result buffer to fill."""
+    may be a (pinned) result buffer to fill; bands=False asks for no final bands (None)."""
     lib = N.load()
     ctx = ctx or N.default_context()
     jobs = np.ascontiguousarray(jobs, dtype=N.JOB_DT)
@@ -167,7 +167,7 @@ def extend_batch(params: np.ndarray, jobs: np.ndarray, qseq: np.ndarray, tseq: n
     n = len(jobs)
     out = np.zeros(n, dtype=N.EXT_RESULT_DT) if out is None else out
     stats = np.zeros(1, dtype=N.STATS_DT)
-    w_final = np.zeros(n, dtype=np.int32)
+    w_final = np.zeros(n, dtype=np.int32) if bands else None
     wf = None if w_first is None else np.ascontiguousarray(w_first, dtype=np.int32)
     N.check(lib.fa_ext_batch_policy(ctx.handle, N.ptr(params), N.ptr(policy), N.ptr(jobs), n,
                                     N.ptr(qseq), qseq.nbytes, N.ptr(tseq), tseq.nbytes, N.ptr(wf),

@@ -98,11 +98,22 @@ struct fa_ctx {
     // learned rounds run their band groups on forked streams: fork on `stream`, join back
     cudaStream_t aux[2] = {nullptr, nullptr};
     cudaEvent_t fork_ev = nullptr, join_ev[2] = {nullptr, nullptr};
+    // a second lane for sliced host batches (alternate slices run concurrently): its own
+    // stream, band-group streams and events, and scratch counters
+    cudaStream_t lane1 = nullptr, aux1[2] = {nullptr, nullptr};
+    cudaEvent_t fork_ev1 = nullptr, join_ev1[2] = {nullptr, nullptr}, lane_ev[2] = {nullptr, nullptr};
+    DevBuf misc1;
+    // paired batches: the mate-rescue half's own buffers, stream and events
+    DevBuf pm_jobs, pm_order, pm_q, pm_t, pm_out, pm_misc, pm_rev;
+    DevBuf mate_rev;   // the mate SW reverse-pass list (launch_mate_sw)
+    cudaStream_t pm_stream = nullptr;
+    cudaEvent_t pm_ev0 = nullptr, pm_ev1 = nullptr;
     // pipelined host batches: slice uploads on their own stream, one event per slice; the
     // same stream then returns each finished slice's results, after its done event
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t slice_ev[8] = {}, done_ev[8] = {}, jobs_ev = nullptr;
     cudaEvent_t span_ev[8][2] = {};   // sliced rounds: each slice's kernels, start and end
+    int slices_single = 8, slices_rounds = 8;   // upload slices of pipelined / sliced host batches
     DevBuf chunk_scratch;
     // kernel choice: fixed, or (FA_KERNEL_AUTO) tuned per (query capacity class, band)
     struct Choice { int kernel; int tpb; };
@@ -123,22 +134,47 @@ int fa::fa_ctx_device(const fa_ctx *c) { return c->device; }
 namespace {
 
 // misc buffer layout (bytes): [0] status u32, [8] cells u64, [16] count A, [20] count B,
+// [232] three u64 statistics sums (kStatsOff),
 // [24..35] two-row kernel overflow counts (one per concurrent band group), [40..51] persistent
 // two-row launches' job counters (one per overflow slot), [64] band-bucket
 // histogram u32[kBandBuckets],
-// [128] band-bucket cursors u32[kBandBuckets], [192] band-group bounds u32[3]
+// [128] band-bucket cursors u32[kBandBuckets], [192] band-group bounds u32[3] and the end of
+// the configured-band bucket u32
 constexpr size_t kMiscBytes = 256;
+constexpr size_t kStatsOff = 232;   // 3 x u64, after the band-group bounds at [192, 208)
 struct Misc {
     uint32_t *status;
     unsigned long long *cells;
     uint32_t *cnt_a, *cnt_b, *ovf_n, *bucket_hist, *bucket_cursor, *group_bounds;
     uint32_t *work;   // persistent two-row launches' job counters, one per overflow slot
 };
+Misc misc_at(char *b, char *shared) {
+    return Misc{(uint32_t *)shared, (unsigned long long *)(shared + 8), (uint32_t *)(b + 16), (uint32_t *)(b + 20),
+                (uint32_t *)(b + 24), (uint32_t *)(b + 64), (uint32_t *)(b + 128), (uint32_t *)(b + 192),
+                (uint32_t *)(b + 40)};
+}
 Misc misc_of(fa_ctx *c) {
     char *b = c->misc.as<char>();
     return Misc{(uint32_t *)b, (unsigned long long *)(b + 8), (uint32_t *)(b + 16), (uint32_t *)(b + 20),
                 (uint32_t *)(b + 24), (uint32_t *)(b + 64), (uint32_t *)(b + 128), (uint32_t *)(b + 192),
                 (uint32_t *)(b + 40)};
+}
+
+// The second lane of sliced host batches: its misc block shares the status word and the
+// cell counter of the first (misc_of), the rest is its own.
+int ensure_lane1(fa_ctx *c, Misc *m1) {
+    if (!c->lane1) {
+        FA_CUDA(cudaStreamCreateWithFlags(&c->lane1, cudaStreamNonBlocking));
+        for (int k = 0; k < 2; ++k) {
+            FA_CUDA(cudaStreamCreateWithFlags(&c->aux1[k], cudaStreamNonBlocking));
+            FA_CUDA(cudaEventCreateWithFlags(&c->join_ev1[k], cudaEventDisableTiming));
+            FA_CUDA(cudaEventCreateWithFlags(&c->lane_ev[k], cudaEventDisableTiming));
+        }
+        FA_CUDA(cudaEventCreateWithFlags(&c->fork_ev1, cudaEventDisableTiming));
+    }
+    FA_CUDA(c->misc1.ensure(kMiscBytes));
+    *m1 = misc_at(c->misc1.as<char>(), c->misc.as<char>());
+    return FA_OK;
 }
 
 int ensure_aux_streams(fa_ctx *c) {
@@ -256,32 +292,39 @@ Choice resolve_choice(fa_ctx *c, const ExtParams &kp, const fa_job *d_jobs, cons
 // after the other (measured 5.69 against 5.59 ms for the learned bench batch).  The two-row
 // kernels run them where the scoring allows (each group with its own overflow list), the
 // int32 kernels otherwise or when int32 is the fixed choice.
+// lane 1 (sliced host batches): the second lane's group streams and events, and the overflow
+// lists from ovf_off words on.
 int launch_learned_round(fa_ctx *c, const fa_job *d_jobs, const uint32_t *d_list, uint32_t n_max,
                          const SeqBuf &d_q, const SeqBuf &d_t, const ExtParams &kp, int qcap,
                          const int32_t *d_w_cur, fa_ext_result *d_out, uint8_t *d_flags, bool cert, Misc &m,
-                         cudaStream_t s, uint32_t *launches) {
+                         cudaStream_t s, uint32_t *launches, int lane = 0, size_t ovf_off = 0,
+                         bool narrow_only = false) {
+    // narrow_only: the configured-band bucket is left out (its jobs run in a later round)
     if (int rc = ensure_aux_streams(c)) return rc;
+    cudaStream_t *aux = lane ? c->aux1 : c->aux;
+    cudaEvent_t fork_ev = lane ? c->fork_ev1 : c->fork_ev, *join_ev = lane ? c->join_ev1 : c->join_ev;
     const uint32_t *g = m.group_bounds;
     const bool rows2 = c->kernel != FA_KERNEL_INT32 && ext_rows2_eligible(kp, qcap) &&
                        ext_rows2_smem_bytes(qcap, 64, 0) <= c->smem_optin &&
-                       c->ovf.cap >= 3 * sizeof(uint32_t) * (size_t)n_max;
+                       c->ovf.cap >= sizeof(uint32_t) * (ovf_off + 3 * (size_t)n_max);
     auto group = [&](int k, int ring, cudaStream_t st) -> cudaError_t {
-        const uint32_t *first = k == 0 ? nullptr : g + k - 1;
+        // narrow_only: group 0 starts after the configured-band bucket (g[3])
+        const uint32_t *first = k == 0 ? (narrow_only ? g + 3 : nullptr) : g + k - 1;
         if (rows2)
             return launch_ext_rows2(d_jobs, d_list, n_max, first, g + k, d_q, d_t, kp, qcap, ring, cert, d_w_cur,
                                     d_out, d_flags, c->cells_job.as<uint32_t>(), m.cells, m.status,
-                                    c->ovf.as<uint32_t>() + (size_t)k * n_max, m.ovf_n + k, st, 64);
+                                    c->ovf.as<uint32_t>() + ovf_off + (size_t)k * n_max, m.ovf_n + k, st, 64);
         return launch_ext_packed(d_jobs, d_list, n_max, first, g + k, d_q, d_t, kp, qcap, ring, d_w_cur, d_out,
                                  d_flags, cert, c->cells_job.as<uint32_t>(), m.cells, m.status, st);
     };
-    FA_CUDA(cudaEventRecord(c->fork_ev, s));
+    FA_CUDA(cudaEventRecord(fork_ev, s));
     FA_CUDA(group(0, 0, s));
     const int rings[2] = {64, 32};
     for (int k = 0; k < 2; ++k) {
-        FA_CUDA(cudaStreamWaitEvent(c->aux[k], c->fork_ev, 0));
-        FA_CUDA(group(k + 1, rings[k], c->aux[k]));
-        FA_CUDA(cudaEventRecord(c->join_ev[k], c->aux[k]));
-        FA_CUDA(cudaStreamWaitEvent(s, c->join_ev[k], 0));
+        FA_CUDA(cudaStreamWaitEvent(aux[k], fork_ev, 0));
+        FA_CUDA(group(k + 1, rings[k], aux[k]));
+        FA_CUDA(cudaEventRecord(join_ev[k], aux[k]));
+        FA_CUDA(cudaStreamWaitEvent(s, join_ev[k], 0));
     }
     *launches += rows2 ? 6 : 3;
     return FA_OK;
@@ -541,32 +584,23 @@ int finish_ext(fa_ctx *c, const fa_policy *pol, uint32_t n, cudaStream_t s, fa_e
     if (stats) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-        unsigned long long cells = 0;
-        FA_CUDA(cudaMemcpy(&cells, m.cells, 8, cudaMemcpyDeviceToHost));
-        stats->cells_executed = cells;
+        // the per-job counts summed on the device: one read of four words
+        const bool tries = retries_from_tries && mode != FA_POLICY_SINGLE;
+        const bool missed = mode == FA_POLICY_LEARNED;
+        unsigned long long *d_sums = reinterpret_cast<unsigned long long *>(c->misc.as<char>() + kStatsOff);
+        FA_CUDA(launch_stats_sum(c->cells_job.as<uint32_t>(), tries ? c->tries.as<int32_t>() : nullptr,
+                                 missed ? c->missed.as<uint8_t>() : nullptr, n, d_sums, c->sm_count, s));
+        unsigned long long h[4];
+        FA_CUDA(cudaMemcpyAsync(h, m.cells, 8, cudaMemcpyDeviceToHost, s));
+        FA_CUDA(cudaMemcpyAsync(h + 1, d_sums, 24, cudaMemcpyDeviceToHost, s));
+        FA_CUDA(cudaStreamSynchronize(s));
+        stats->cells_executed = h[0];
         stats->kernel_ms = ms;
         stats->kernel_launches = launches;
         stats->jobs = n;
-        std::vector<uint32_t> cj(n);
-        FA_CUDA(cudaMemcpy(cj.data(), c->cells_job.p, 4ull * n, cudaMemcpyDeviceToHost));
-        uint64_t acc = 0;
-        for (uint32_t i = 0; i < n; ++i) acc += cj[i];
-        stats->cells = acc;
-        stats->retries = retries;
-        if (retries_from_tries && mode != FA_POLICY_SINGLE) {
-            std::vector<int32_t> tr(n);
-            FA_CUDA(cudaMemcpy(tr.data(), c->tries.p, 4ull * n, cudaMemcpyDeviceToHost));
-            uint64_t t = 0;
-            for (uint32_t i = 0; i < n; ++i) t += (uint32_t)tr[i];
-            stats->retries = (uint32_t)(t - n);
-        }
-        if (mode == FA_POLICY_LEARNED) {
-            std::vector<uint8_t> ms_(n);
-            FA_CUDA(cudaMemcpy(ms_.data(), c->missed.p, n, cudaMemcpyDeviceToHost));
-            uint32_t miss = 0;
-            for (uint32_t i = 0; i < n; ++i) miss += ms_[i];
-            stats->misses = miss;
-        }
+        stats->cells = h[1];
+        stats->retries = tries ? (uint32_t)(h[2] - n) : retries;
+        if (missed) stats->misses = (uint32_t)h[3];
     }
     if (h_wfinal && mode != FA_POLICY_SINGLE)
         FA_CUDA(cudaMemcpy(h_wfinal, c->w_final.p, 4ull * n, cudaMemcpyDeviceToHost));
@@ -762,7 +796,7 @@ int upload_runs(fa_ctx *c, const HostSeq &q, const HostSeq &t, cudaStream_t s) {
 // host-side checks); with pageable host buffers the copies simply do not overlap.  Byte
 // codes and packed bases alike: slices are cut in bytes, jobs placed by the byte holding
 // their last base.
-constexpr int kSlices = 8;
+constexpr int kSlices = 8;   // at most this many upload slices (the event and scratch arrays)
 constexpr uint32_t kPipeMinJobs = 32768;
 
 int ensure_pipe_streams(fa_ctx *c) {
@@ -780,24 +814,26 @@ int ensure_pipe_streams(fa_ctx *c) {
     return ensure_aux_streams(c);
 }
 
-// graded slices (1, 1, 2, 4, 6, 6, 6, 6 thirty-seconds of each buffer): the first jobs start
-// after a small upload, and the uploads, faster than the kernels, stay ahead
-ChunkEnds graded_ends(const HostSeq &q, const HostSeq &t) {
+// graded slices (for 8: 1, 1, 2, 4, 6, 6, 6, 6 thirty-seconds of each buffer): the first jobs
+// start after a small upload, and the uploads, faster than the kernels, stay ahead
+ChunkEnds graded_ends(const HostSeq &q, const HostSeq &t, int ns) {
     ChunkEnds ends;
-    static constexpr int kCum[kSlices] = {1, 2, 4, 8, 14, 20, 26, 32};
+    static constexpr int kCum[kSlices + 1][kSlices] = {
+        {32}, {32}, {4, 32}, {2, 10, 32}, {1, 4, 14, 32}, {1, 2, 6, 16, 32}, {1, 2, 4, 10, 20, 32},
+        {1, 2, 4, 8, 14, 22, 32}, {1, 2, 4, 8, 14, 20, 26, 32}};
     static_assert(kSlices <= kMaxChunks, "slice count");
-    for (int k = 0; k < kSlices; ++k) {
-        ends.q[k] = k == kSlices - 1 ? q.nbytes : q.nbytes / 32 * kCum[k];
-        ends.t[k] = k == kSlices - 1 ? t.nbytes : t.nbytes / 32 * kCum[k];
+    for (int k = 0; k < ns; ++k) {
+        ends.q[k] = k == ns - 1 ? q.nbytes : q.nbytes / 32 * kCum[ns][k];
+        ends.t[k] = k == ns - 1 ? t.nbytes : t.nbytes / 32 * kCum[ns][k];
     }
     ends.shift = q.packed ? 2 : 0;
     return ends;
 }
 
 // The sequence slices on the copy stream, one event per slice.
-int upload_slices(fa_ctx *c, const HostSeq &q, const HostSeq &t, const ChunkEnds &ends) {
+int upload_slices(fa_ctx *c, const HostSeq &q, const HostSeq &t, const ChunkEnds &ends, int ns) {
     cudaStream_t cs = c->copy_stream;
-    for (int k = 0; k < kSlices; ++k) {
+    for (int k = 0; k < ns; ++k) {
         const uint64_t q0 = k ? ends.q[k - 1] : 0, q1 = ends.q[k];
         const uint64_t t0 = k ? ends.t[k - 1] : 0, t1 = ends.t[k];
         if (q1 > q0) FA_CUDA(cudaMemcpyAsync(c->qseq.as<uint8_t>() + q0, q.p + q0, q1 - q0, cudaMemcpyHostToDevice, cs));
@@ -812,14 +848,16 @@ int upload_slices(fa_ctx *c, const HostSeq &q, const HostSeq &t, const ChunkEnds
 // each slice's lowest and highest job index.  A rejected batch reports its first bad job
 // with the host-side checks' message.
 constexpr int kInfoWords = 4 + kSlices + 1 + 2 * kSlices;
+inline int info_words(int ns) { return 4 + ns + 1 + 2 * ns; }
 int prep_slices(fa_ctx *c, const ExtParams &kp, const fa_job *jobs, uint32_t n, const HostSeq &q, const HostSeq &t,
-                const ChunkEnds &ends, uint32_t *h_info) {
+                const ChunkEnds &ends, int ns, uint32_t *h_info) {
     cudaStream_t s = c->stream;
     uint32_t *scratch = c->chunk_scratch.as<uint32_t>();
-    const size_t nbins = (size_t)kSlices * (FA_MAX_QLEN + 1);
-    FA_CUDA(launch_chunk_prep(c->jobs.as<fa_job>(), n, q.npos, t.npos, ends, kSlices, kp.max_score,
+    const size_t nbins = (size_t)ns * (FA_MAX_QLEN + 1);
+    FA_CUDA(launch_chunk_prep(c->jobs.as<fa_job>(), n, q.npos, t.npos, ends, ns, kp.max_score,
                               (kp.flags & FA_PARAM_H0_ZERO) ? 0 : 1, packed_qcap_limit(c->smem_optin), scratch, s));
-    FA_CUDA(cudaMemcpyAsync(h_info, scratch + 3 * nbins, sizeof(uint32_t) * kInfoWords, cudaMemcpyDeviceToHost, s));
+    FA_CUDA(cudaMemcpyAsync(h_info, scratch + 3 * nbins, sizeof(uint32_t) * info_words(ns), cudaMemcpyDeviceToHost,
+                            s));
     FA_CUDA(cudaStreamSynchronize(s));
     if (h_info[0]) {
         FA_CUDA(cudaStreamSynchronize(c->copy_stream));   // the caller's buffers stay in use until then
@@ -834,11 +872,11 @@ int prep_slices(fa_ctx *c, const ExtParams &kp, const fa_job *jobs, uint32_t n, 
 
 // Whether every slice's jobs form one index range, together covering all n jobs (the
 // sequences lie in job order).
-bool slices_in_order(const uint32_t *h_info, uint32_t n) {
+bool slices_in_order(const uint32_t *h_info, uint32_t n, int ns) {
     uint32_t covered = 0;
-    for (int k = 0; k < kSlices; ++k) {
+    for (int k = 0; k < ns; ++k) {
         const uint32_t cnt = h_info[4 + k + 1] - h_info[4 + k];
-        const uint32_t lo = h_info[4 + kSlices + 1 + k], hi = h_info[4 + 2 * kSlices + 1 + k];
+        const uint32_t lo = h_info[4 + ns + 1 + k], hi = h_info[4 + 2 * ns + 1 + k];
         if (cnt && hi - lo + 1 != cnt) return false;
         covered += cnt;
     }
@@ -851,7 +889,8 @@ int ext_batch_pipelined(fa_ctx *c, const ExtParams &kp, const fa_job *jobs, uint
     if (int rc = ensure_seq_buffers(c, hq, ht)) return rc;
     if (int rc = ensure_pipe_streams(c)) return rc;
     cudaStream_t s = c->stream, cs = c->copy_stream;
-    const ChunkEnds ends = graded_ends(hq, ht);
+    const int ns = c->slices_single;
+    const ChunkEnds ends = graded_ends(hq, ht, ns);
     Misc m = misc_of(c);
     FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
     // the job records and N runs first, then the sequence slices, all on the copy stream
@@ -862,15 +901,15 @@ int ext_batch_pipelined(fa_ctx *c, const ExtParams &kp, const fa_job *jobs, uint
     if (int rc = upload_runs(c, hq, ht, cs)) return rc;
     FA_CUDA(cudaEventRecord(c->jobs_ev, cs));
     FA_CUDA(cudaStreamWaitEvent(s, c->jobs_ev, 0));
-    if (int rc = upload_slices(c, hq, ht, ends)) return rc;
+    if (int rc = upload_slices(c, hq, ht, ends, ns)) return rc;
     uint32_t h_info[kInfoWords];
-    if (int rc = prep_slices(c, kp, jobs, n, hq, ht, ends, h_info)) return rc;
+    if (int rc = prep_slices(c, kp, jobs, n, hq, ht, ends, ns, h_info)) return rc;
     const int max_q = (int)h_info[2];
-    FA_CUDA(launch_chunk_scatter(c->jobs.as<fa_job>(), n, ends, kSlices, c->chunk_scratch.as<uint32_t>(),
+    FA_CUDA(launch_chunk_scatter(c->jobs.as<fa_job>(), n, ends, ns, c->chunk_scratch.as<uint32_t>(),
                                  c->order.as<uint32_t>(), s));
     const int band = (int)h_info[3];   // widest configured band, reduced on the device
     if (c->kernel == FA_KERNEL_AUTO && !c->tuned.count({(max_q + 31) / 32, band, (int)hq.packed}))
-        FA_CUDA(cudaStreamWaitEvent(s, c->slice_ev[kSlices - 1], 0));   // tuning reads every slice
+        FA_CUDA(cudaStreamWaitEvent(s, c->slice_ev[ns - 1], 0));   // tuning reads every slice
     int rc0 = FA_OK;
     const Choice kc = resolve_choice(c, kp, c->jobs.as<fa_job>(), c->order.as<uint32_t>(), n, c->cq, c->ct, max_q,
                                      band, c->out.as<fa_ext_result>(), m.status, s, &rc0);
@@ -891,9 +930,9 @@ int ext_batch_pipelined(fa_ctx *c, const ExtParams &kp, const fa_job *jobs, uint
         cudaPointerAttributes pa;
         early = cudaPointerGetAttributes(&pa, out) == cudaSuccess && pa.type == cudaMemoryTypeHost;
         cudaGetLastError();
-        early = early && slices_in_order(h_info, n);
+        early = early && slices_in_order(h_info, n, ns);
     }
-    for (int k = 0; k < kSlices; ++k) {
+    for (int k = 0; k < ns; ++k) {
         const uint32_t cnt = h_info[4 + k + 1] - h_info[4 + k];
         cudaStream_t st = sk[k & 1];
         FA_CUDA(cudaStreamWaitEvent(st, c->slice_ev[k], 0));
@@ -903,7 +942,7 @@ int ext_batch_pipelined(fa_ctx *c, const ExtParams &kp, const fa_job *jobs, uint
                            c->cells_job.as<uint32_t>(), m.cells, m.status, st, k & 1));
         launches += ext_kernels_of(c, kc, kp, max_q);
         if (early) {
-            const uint32_t lo = h_info[4 + kSlices + 1 + k];
+            const uint32_t lo = h_info[4 + ns + 1 + k];
             FA_CUDA(cudaEventRecord(c->done_ev[k], st));
             FA_CUDA(cudaStreamWaitEvent(cs, c->done_ev[k], 0));
             FA_CUDA(cudaMemcpyAsync(out + lo, c->out.as<fa_ext_result>() + lo, sizeof(fa_ext_result) * (size_t)cnt,
@@ -955,7 +994,8 @@ int ext_batch_sliced(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, const
         band_model_export(model, wbf, mean, sd);
     }
     cudaStream_t s = c->stream, cs = c->copy_stream;
-    const ChunkEnds ends = graded_ends(hq, ht);
+    const int ns = c->slices_rounds;
+    const ChunkEnds ends = graded_ends(hq, ht, ns);
     Misc m = misc_of(c);
     FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
     FA_CUDA(cudaEventRecord(c->fork_ev, s));
@@ -971,20 +1011,20 @@ int ext_batch_sliced(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, const
     }
     FA_CUDA(cudaEventRecord(c->jobs_ev, cs));
     FA_CUDA(cudaStreamWaitEvent(s, c->jobs_ev, 0));
-    if (int rc = upload_slices(c, hq, ht, ends)) return rc;
+    if (int rc = upload_slices(c, hq, ht, ends, ns)) return rc;
     uint32_t h_info[kInfoWords];
-    if (int rc = prep_slices(c, kp, jobs, n, hq, ht, ends, h_info)) return rc;
-    if (!slices_in_order(h_info, n)) {
+    if (int rc = prep_slices(c, kp, jobs, n, hq, ht, ends, ns, h_info)) return rc;
+    if (!slices_in_order(h_info, n, ns)) {
         FA_CUDA(cudaStreamSynchronize(cs));
         return FA_OK;
     }
     *done = true;
     const int max_q = (int)h_info[2];
     const int band = (int)h_info[3];
-    FA_CUDA(launch_chunk_scatter(c->jobs.as<fa_job>(), n, ends, kSlices, c->chunk_scratch.as<uint32_t>(),
+    FA_CUDA(launch_chunk_scatter(c->jobs.as<fa_job>(), n, ends, ns, c->chunk_scratch.as<uint32_t>(),
                                  c->order.as<uint32_t>(), s));
     if (c->kernel == FA_KERNEL_AUTO && !c->tuned.count({(max_q + 31) / 32, band, (int)hq.packed}))
-        FA_CUDA(cudaStreamWaitEvent(s, c->slice_ev[kSlices - 1], 0));   // tuning reads every slice
+        FA_CUDA(cudaStreamWaitEvent(s, c->slice_ev[ns - 1], 0));   // tuning reads every slice
     int rc0 = FA_OK;
     const Choice kc = resolve_choice(c, kp, c->jobs.as<fa_job>(), c->order.as<uint32_t>(), n, c->cq, c->ct, max_q,
                                      band, c->out.as<fa_ext_result>(), m.status, s, &rc0);
@@ -1000,43 +1040,68 @@ int ext_batch_sliced(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, const
     const int max_tries = std::max(1, pol->max_tries);
     uint32_t launches = 0, retries = 0;
     int spans = 0;
-    for (int k = 0; k < kSlices; ++k) {
+    // Alternate slices run on two lanes, so one slice's last, longest jobs overlap the next
+    // slice's start: lane 0 is the main stream with misc_of(c), lane 1 its own stream, band-
+    // group streams and counters (status, cells and the retry list's count are shared).
+    Misc m1;
+    if (int rc = ensure_lane1(c, &m1)) return rc;
+    uint32_t max_cnt = 0;
+    for (int k = 0; k < ns; ++k) max_cnt = std::max(max_cnt, h_info[4 + k + 1] - h_info[4 + k]);
+    FA_CUDA(c->ovf.ensure(sizeof(uint32_t) * std::max<size_t>(3 * (size_t)n, 6 * (size_t)max_cnt)));
+    FA_CUDA(cudaMemsetAsync(c->misc1.p, 0, 64, s));
+    FA_CUDA(cudaEventRecord(c->lane_ev[0], s));
+    FA_CUDA(cudaStreamWaitEvent(c->lane1, c->lane_ev[0], 0));
+    for (int k = 0; k < ns; ++k) {
         const uint32_t b = h_info[4 + k], cnt = h_info[4 + k + 1] - b;
-        FA_CUDA(cudaStreamWaitEvent(s, c->slice_ev[k], 0));
+        const int lane = k & 1;
+        cudaStream_t ls = lane ? c->lane1 : s;
+        Misc &ml = lane ? m1 : m;
+        FA_CUDA(cudaStreamWaitEvent(ls, c->slice_ev[k], 0));
         if (cnt == 0) continue;
-        const uint32_t lo = h_info[4 + kSlices + 1 + k];
-        FA_CUDA(cudaEventRecord(c->span_ev[k][0], s));
+        const uint32_t lo = h_info[4 + ns + 1 + k];
+        FA_CUDA(cudaEventRecord(c->span_ev[k][0], ls));
         if (model) {
             FA_CUDA(launch_band_features(d_jobs + lo, cnt, c->cq, c->ct, d_h ? d_h + lo : nullptr, kp.max_score,
-                                         d_x + 16 * (size_t)lo, s));
+                                         d_x + 16 * (size_t)lo, ls));
             FA_CUDA(launch_band_predict(c->wbf.as<__nv_bfloat16>(), mean, sd, d_x + 16 * (size_t)lo, d_jobs + lo, cnt,
-                                        margin, pol->w_min, nullptr, d_wf + lo, s));
+                                        margin, pol->w_min, nullptr, d_wf + lo, ls));
             launches += 2;
         }
         const PolicyState sl{st.w_cur + lo, st.prev + lo, st.k + lo, st.w_final + lo, st.tries + lo,
                              st.missed + lo};
-        FA_CUDA(launch_policy_init(d_jobs + lo, cnt, learned ? d_wf + lo : nullptr, pol->w_min, learned, sl, s));
+        FA_CUDA(launch_policy_init(d_jobs + lo, cnt, learned ? d_wf + lo : nullptr, pol->w_min, learned, sl, ls));
         const uint32_t *list = order + b;
         if (learned) {
-            FA_CUDA(launch_band_partition(d_jobs, list, nullptr, cnt, st.w_cur, c->part_n.as<uint32_t>() + b,
-                                          m.bucket_hist, m.bucket_cursor, m.group_bounds, s));
-            if (int rc = launch_learned_round(c, d_jobs, c->part_n.as<uint32_t>() + b, cnt, c->cq, c->ct, kp, max_q,
-                                              st.w_cur, c->out.as<fa_ext_result>(), d_flags, cert, m, s, &launches))
+            // the narrow bands now, each slice as it arrives; jobs whose first band is the
+            // configured one join the retry list and run with the later round (same runs, same
+            // policy state: the configured band goes straight to the bwa-mem2 rule either way)
+            uint32_t *part = c->part_n.as<uint32_t>() + b;
+            FA_CUDA(launch_band_partition(d_jobs, list, nullptr, cnt, st.w_cur, part, ml.bucket_hist,
+                                          ml.bucket_cursor, ml.group_bounds, ls));
+            if (int rc = launch_learned_round(c, d_jobs, part, cnt, c->cq, c->ct, kp, max_q, st.w_cur,
+                                              c->out.as<fa_ext_result>(), d_flags, cert, ml, ls, &launches, lane,
+                                              (size_t)lane * 3 * max_cnt, true))
                 return rc;
-            launches += 2;
+            FA_CUDA(launch_list_append(part, ml.group_bounds + 3, cnt, c->list_a.as<uint32_t>(), m.cnt_a, ls));
+            FA_CUDA(launch_policy_step(d_jobs, part, ml.group_bounds + 3, ml.group_bounds + 2, cnt,
+                                       c->out.as<fa_ext_result>(), d_flags, st, max_tries, pol->judge,
+                                       c->list_a.as<uint32_t>(), m.cnt_a, ls));
+            launches += 4;
         } else {
             FA_CUDA(launch_ext(c, kc, d_jobs, list, cnt, nullptr, c->cq, c->ct, kp, max_q, st.w_cur,
                                c->out.as<fa_ext_result>(), d_flags, false, c->cells_job.as<uint32_t>(), m.cells,
-                               m.status, s));
+                               m.status, ls, lane));
             launches += ext_kernels_of(c, kc, kp, max_q);
+            // the round's rejected jobs join one retry list (cnt_a counts across the slices)
+            FA_CUDA(launch_policy_step(d_jobs, list, nullptr, nullptr, cnt, c->out.as<fa_ext_result>(), d_flags, st,
+                                       max_tries, pol->judge, c->list_a.as<uint32_t>(), m.cnt_a, ls));
+            launches += 2;
         }
-        // the round's rejected jobs join one retry list (cnt_a counts across the slices)
-        FA_CUDA(launch_policy_step(d_jobs, list, nullptr, nullptr, cnt, c->out.as<fa_ext_result>(), d_flags, st,
-                                   max_tries, pol->judge, c->list_a.as<uint32_t>(), m.cnt_a, s));
-        launches += 2;
-        FA_CUDA(cudaEventRecord(c->span_ev[k][1], s));
+        FA_CUDA(cudaEventRecord(c->span_ev[k][1], ls));
         spans |= 1 << k;
     }
+    FA_CUDA(cudaEventRecord(c->lane_ev[1], c->lane1));
+    FA_CUDA(cudaStreamWaitEvent(s, c->lane_ev[1], 0));
     FA_CUDA(cudaEventRecord(c->ev0, s));
     std::vector<std::pair<uint32_t, int>> segs{{n, max_q}};
     if (int rc = enqueue_ext(c, kp, pol, n, segs, max_q, band, d_jobs, order, c->cq, c->ct, d_wf,
@@ -1047,13 +1112,27 @@ int ext_batch_sliced(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, const
     FA_CUDA(cudaMemcpyAsync(out, c->out.p, sizeof(fa_ext_result) * (size_t)n, cudaMemcpyDeviceToHost, s));
     if (w_first_out && model) FA_CUDA(cudaMemcpyAsync(w_first_out, d_wf, 4ull * n, cudaMemcpyDeviceToHost, s));
     if (int rc = finish_ext(c, pol, n, s, stats, w_final, launches, retries, true)) return rc;
-    if (stats) {   // busy time: the slices' spans plus the later rounds
-        for (int k = 0; k < kSlices; ++k) {
+    if (stats && spans) {   // busy time: the union of the slices' spans, plus the later rounds
+        int k0 = 0;
+        while (!(spans & (1 << k0))) ++k0;
+        std::vector<std::pair<float, float>> iv;
+        for (int k = k0; k < ns; ++k) {
             if (!(spans & (1 << k))) continue;
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, c->span_ev[k][0], c->span_ev[k][1]);
-            stats->kernel_ms += ms;
+            float a = 0.f, b = 0.f;
+            cudaEventElapsedTime(&a, c->span_ev[k0][0], c->span_ev[k][0]);
+            cudaEventElapsedTime(&b, c->span_ev[k0][0], c->span_ev[k][1]);
+            iv.push_back({a, b});
         }
+        std::sort(iv.begin(), iv.end());
+        float busy = 0.f, lo = iv[0].first, hi = iv[0].second;
+        for (size_t i = 1; i < iv.size(); ++i) {
+            if (iv[i].first > hi) {
+                busy += hi - lo;
+                lo = iv[i].first;
+            }
+            hi = std::max(hi, iv[i].second);
+        }
+        stats->kernel_ms += busy + (hi - lo);
     }
     FA_CUDA(cudaStreamSynchronize(s));
     return FA_OK;
@@ -1215,6 +1294,66 @@ int ext_learned_host(fa_ctx *c, const fa_params *p, const fa_policy *pol, const 
     return FA_OK;
 }
 
+// Mate-rescue host batch: parameters, validation and the u8 / i16 lane split (the jobs of
+// each kind in job order), as fa_mate_sw_batch and fa_pair_batch take them.
+struct MateHostPlan {
+    MateParams mp;
+    std::vector<uint32_t> order;   // u8 jobs, then i16 jobs
+    uint32_t n_byte = 0;
+    int mq_b = 0, mq_w = 0, mt = 0;
+};
+
+int plan_mate_host(const fa_mate_params *p, const fa_mate_job *jobs, uint32_t n, uint64_t qseq_len,
+                   uint64_t tseq_len, MateHostPlan *pl) {
+    int mn = 127, mx = 0;
+    for (int i = 0; i < 25; ++i) { mn = std::min<int>(mn, p->mat[i]); mx = std::max<int>(mx, p->mat[i]); }
+    if (mx <= 0) return fail(FA_ERR_ARG, "scoring matrix needs a positive entry");
+    MateParams &mp = pl->mp;
+    memcpy(mp.mat, p->mat, 25);
+    mp.m = 5;
+    mp.o_del = p->o_del; mp.e_del = p->e_del; mp.o_ins = p->o_ins; mp.e_ins = p->e_ins;
+    mp.shift = (uint8_t)(256 - mn);
+    mp.max = mx;
+    std::vector<uint32_t> word_list;
+    pl->order.clear();
+    for (uint32_t i = 0; i < n; ++i) {
+        const fa_mate_job &j = jobs[i];
+        if (j.qlen <= 0 || j.tlen < 0) return fail(FA_ERR_ARG, "mate job %u: bad lengths", i);
+        if (j.tlen > FA_MAX_TLEN) return fail(FA_ERR_CAPACITY, "mate job %u: tlen too long", i);
+        if (j.q_off + (uint64_t)j.qlen > qseq_len || j.t_off + (uint64_t)j.tlen > tseq_len)
+            return fail(FA_ERR_ARG, "mate job %u: sequence range outside the buffers", i);
+        const bool byte = (j.xtra & FA_KSW_XBYTE) != 0;
+        if (byte ? j.qlen > 16 * 32 : j.qlen > 8 * 32)
+            return fail(FA_ERR_CAPACITY, "mate job %u: qlen=%d exceeds the %s-lane limit", i, j.qlen,
+                        byte ? "u8" : "i16");
+        (byte ? pl->order : word_list).push_back(i);
+        if (byte) pl->mq_b = std::max(pl->mq_b, j.qlen); else pl->mq_w = std::max(pl->mq_w, j.qlen);
+        pl->mt = std::max(pl->mt, j.tlen);
+    }
+    pl->n_byte = (uint32_t)pl->order.size();
+    pl->order.insert(pl->order.end(), word_list.begin(), word_list.end());
+    return FA_OK;
+}
+
+// The mate SW kernels of a planned batch on device copies (jobs, order, sequences in d_*).
+cudaError_t launch_mate_plan(const MateHostPlan &pl, const fa_mate_job *d_jobs, const uint32_t *d_order, uint32_t n,
+                             const uint8_t *d_q, const uint8_t *d_t, fa_kswr *d_out, unsigned long long *d_cells,
+                             uint32_t *d_status, uint32_t *d_rev, cudaStream_t s, uint32_t *launches) {
+    if (pl.n_byte) {
+        cudaError_t e = launch_mate_sw(true, d_jobs, d_order, pl.n_byte, d_q, d_t, pl.mp, pl.mq_b, pl.mt, d_out,
+                                       d_cells, d_status, d_rev, s);
+        if (e != cudaSuccess) return e;
+        *launches += 2;
+    }
+    if (n > pl.n_byte) {
+        cudaError_t e = launch_mate_sw(false, d_jobs, d_order + pl.n_byte, n - pl.n_byte, d_q, d_t, pl.mp, pl.mq_w,
+                                       pl.mt, d_out, d_cells, d_status, nullptr, s);
+        if (e != cudaSuccess) return e;
+        ++*launches;
+    }
+    return cudaSuccess;
+}
+
 // Argument checks shared by the host extension entry points.
 int check_host_call(fa_ctx *c, const fa_params *p, const fa_policy *pol, const fa_job *jobs, uint32_t n,
                     const void *out) {
@@ -1344,6 +1483,19 @@ void fa_ctx_destroy(fa_ctx *c) {
         for (auto &e : pr)
             if (e) cudaEventDestroy(e);
     for (int k = 0; k < 2; ++k) {
+        if (c->aux1[k]) cudaStreamDestroy(c->aux1[k]);
+        if (c->join_ev1[k]) cudaEventDestroy(c->join_ev1[k]);
+        if (c->lane_ev[k]) cudaEventDestroy(c->lane_ev[k]);
+    }
+    if (c->fork_ev1) cudaEventDestroy(c->fork_ev1);
+    for (DevBuf *b : {&c->pm_jobs, &c->pm_order, &c->pm_q, &c->pm_t, &c->pm_out, &c->pm_misc, &c->pm_rev, &c->mate_rev})
+        b->release();
+    if (c->pm_ev0) cudaEventDestroy(c->pm_ev0);
+    if (c->pm_ev1) cudaEventDestroy(c->pm_ev1);
+    if (c->pm_stream) cudaStreamDestroy(c->pm_stream);
+    if (c->lane1) cudaStreamDestroy(c->lane1);
+    c->misc1.release();
+    for (int k = 0; k < 2; ++k) {
         if (c->join_ev[k]) cudaEventDestroy(c->join_ev[k]);
         if (c->aux[k]) cudaStreamDestroy(c->aux[k]);
     }
@@ -1366,7 +1518,7 @@ void fa_ctx_destroy(fa_ctx *c) {
 
 int fa_probe_int_peak(fa_ctx *c, int kind, double *ops_per_s, float *ms) {
     if (!c || !ops_per_s) return fail(FA_ERR_ARG, "null argument");
-    if (kind < 0 || kind > 4) return fail(FA_ERR_ARG, "unknown probe kind %d", kind);
+    if (kind < 0 || kind > 9) return fail(FA_ERR_ARG, "unknown probe kind %d", kind);
     FA_CUDA(cudaSetDevice(c->device));
     const double r = probe_int_peak(kind, c->sm_count, c->stream, ms);
     if (r <= 0) return fail(FA_ERR_CUDA, "probe kernel failed");
@@ -1519,6 +1671,15 @@ int fa_ctx_kernel_choice(fa_ctx *c, int *kernel, int *threads_per_block, int cap
     return FA_OK;
 }
 
+int fa_ctx_set_slices(fa_ctx *c, int single_band, int policy_rounds) {
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    for (int v : {single_band, policy_rounds})
+        if (v != 0 && (v < 2 || v > kSlices)) return fail(FA_ERR_ARG, "slice count %d outside 2..%d", v, kSlices);
+    if (single_band) c->slices_single = single_band;
+    if (policy_rounds) c->slices_rounds = policy_rounds;
+    return FA_OK;
+}
+
 int fa_ctx_set_graph(fa_ctx *c, int enable) {
     if (!c) return fail(FA_ERR_ARG, "null context");
     FA_CUDA(cudaSetDevice(c->device));
@@ -1584,6 +1745,7 @@ int fa_mate_sw_batch_device(fa_ctx *c, const fa_mate_params *p, const fa_mate_jo
     FA_CUDA(c->misc.ensure(kMiscBytes));
     FA_CUDA(c->order.ensure(4ull * n));
     FA_CUDA(c->list_a.ensure(4ull * n));
+    FA_CUDA(c->mate_rev.ensure(4ull * (2 + (size_t)n)));
     FA_CUDA(c->hist.ensure(sizeof(uint32_t) * (FA_MAX_QLEN + 1)));
     Misc m = misc_of(c);
     FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
@@ -1599,12 +1761,12 @@ int fa_mate_sw_batch_device(fa_ctx *c, const fa_mate_params *p, const fa_mate_jo
     if (c->timing) FA_CUDA(cudaEventRecord(c->kev0, s));
     if (h[0]) {
         FA_CUDA(launch_mate_sw(true, d_jobs, c->order.as<uint32_t>(), h[0], d_qseq, d_tseq, mp, (int)h[2], (int)h[4],
-                               d_out, m.cells, m.status, s));
-        ++launches;
+                               d_out, m.cells, m.status, c->mate_rev.as<uint32_t>(), s));
+        launches += 2;
     }
     if (h[1]) {
         FA_CUDA(launch_mate_sw(false, d_jobs, c->list_a.as<uint32_t>(), h[1], d_qseq, d_tseq, mp, (int)h[3],
-                               (int)h[4], d_out, m.cells, m.status, s));
+                               (int)h[4], d_out, m.cells, m.status, nullptr, s));
         ++launches;
     }
     if (c->timing) FA_CUDA(cudaEventRecord(c->kev1, s));
@@ -2038,6 +2200,92 @@ int fa_ctx_last_cells(fa_ctx *c, unsigned long long *cells) {
     return FA_OK;
 }
 
+int fa_pair_batch(fa_ctx *c, const fa_params *p, const fa_policy *pol, const fa_band_model *model, float margin,
+                  const fa_job *jobs, uint32_t n, const uint8_t *qseq, uint64_t qseq_len, const uint8_t *tseq,
+                  uint64_t tseq_len, const fa_band_hint *hints, fa_ext_result *out, const fa_mate_params *mp,
+                  const fa_mate_job *mjobs, uint32_t mn, const uint8_t *mqseq, uint64_t mqseq_len,
+                  const uint8_t *mtseq, uint64_t mtseq_len, fa_kswr *mout, fa_ext_stats *stats,
+                  fa_ext_stats *mate_stats) {
+    auto t0 = std::chrono::steady_clock::now();
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (mate_stats) memset(mate_stats, 0, sizeof(*mate_stats));
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    if (model && (!pol || pol->mode != FA_POLICY_LEARNED))
+        return fail(FA_ERR_ARG, "a band model needs FA_POLICY_LEARNED");
+    if (!model && pol && pol->mode == FA_POLICY_LEARNED)
+        return fail(FA_ERR_STATE, "FA_POLICY_LEARNED needs a band model");
+    if (int rc = check_host_call(c, p, pol, jobs, n, out)) return rc;
+    if (n && (!qseq || !tseq)) return fail(FA_ERR_ARG, "null buffer");
+    if (!mp || mp->m != 5) return fail(FA_ERR_ARG, "mate alphabet size must be 5");
+    if (mn && (!mjobs || !mout || !mqseq || !mtseq)) return fail(FA_ERR_ARG, "null mate buffer");
+    MateHostPlan pl;
+    if (mn)
+        if (int rc = plan_mate_host(mp, mjobs, mn, mqseq_len, mtseq_len, &pl)) return rc;
+    FA_CUDA(cudaSetDevice(c->device));
+    // the mate half, asynchronous on its own stream: uploads, kernels, results back
+    if (!c->pm_stream) {
+        FA_CUDA(cudaStreamCreateWithFlags(&c->pm_stream, cudaStreamNonBlocking));
+        FA_CUDA(cudaEventCreate(&c->pm_ev0));
+        FA_CUDA(cudaEventCreate(&c->pm_ev1));
+    }
+    cudaStream_t ms = c->pm_stream;
+    uint32_t mlaunches = 0;
+    if (mn) {
+        FA_CUDA(c->pm_jobs.ensure(sizeof(fa_mate_job) * (size_t)mn));
+        FA_CUDA(c->pm_order.ensure(4ull * mn));
+        FA_CUDA(c->pm_q.ensure(mqseq_len));
+        FA_CUDA(c->pm_t.ensure(mtseq_len));
+        FA_CUDA(c->pm_out.ensure(sizeof(fa_kswr) * (size_t)mn));
+        FA_CUDA(c->pm_misc.ensure(64));
+        FA_CUDA(c->pm_rev.ensure(4ull * (2 + (size_t)pl.n_byte)));
+        FA_CUDA(cudaMemsetAsync(c->pm_misc.p, 0, 64, ms));
+        FA_CUDA(cudaMemcpyAsync(c->pm_jobs.p, mjobs, sizeof(fa_mate_job) * (size_t)mn, cudaMemcpyHostToDevice, ms));
+        FA_CUDA(cudaMemcpyAsync(c->pm_order.p, pl.order.data(), 4ull * mn, cudaMemcpyHostToDevice, ms));
+        FA_CUDA(cudaMemcpyAsync(c->pm_q.p, mqseq, mqseq_len, cudaMemcpyHostToDevice, ms));
+        FA_CUDA(cudaMemcpyAsync(c->pm_t.p, mtseq, mtseq_len, cudaMemcpyHostToDevice, ms));
+        FA_CUDA(cudaEventRecord(c->pm_ev0, ms));
+        uint32_t *st = c->pm_misc.as<uint32_t>();
+        unsigned long long *cells = reinterpret_cast<unsigned long long *>(c->pm_misc.as<char>() + 8);
+        FA_CUDA(launch_mate_plan(pl, c->pm_jobs.as<fa_mate_job>(), c->pm_order.as<uint32_t>(), mn,
+                                 c->pm_q.as<uint8_t>(), c->pm_t.as<uint8_t>(), c->pm_out.as<fa_kswr>(), cells, st,
+                                 c->pm_rev.as<uint32_t>(), ms, &mlaunches));
+        FA_CUDA(cudaEventRecord(c->pm_ev1, ms));
+        FA_CUDA(cudaMemcpyAsync(mout, c->pm_out.p, sizeof(fa_kswr) * (size_t)mn, cudaMemcpyDeviceToHost, ms));
+    }
+    // the extension half on the main stream, meanwhile
+    int rc = FA_OK;
+    if (n) {
+        rc = model ? ext_learned_host(c, p, pol, model, margin, jobs, n, host_bytes(qseq, qseq_len),
+                                      host_bytes(tseq, tseq_len), hints, out, nullptr, nullptr, stats)
+                   : ext_batch_host(c, p, pol, jobs, n, host_bytes(qseq, qseq_len), host_bytes(tseq, tseq_len),
+                                    nullptr, out, nullptr, stats);
+    }
+    // the mate half's end (also on an extension error, so the caller's buffers are free)
+    const cudaError_t es = cudaStreamSynchronize(ms);
+    if (rc) return rc;
+    FA_CUDA(es);
+    if (mn) {
+        uint32_t h[4];
+        FA_CUDA(cudaMemcpy(h, c->pm_misc.p, 16, cudaMemcpyDeviceToHost));
+        if (h[0] & ST_BAD_CODE) return fail(FA_ERR_ARG, "a mate sequence byte is outside the alphabet (codes 0-4)");
+        if (h[0] & ST_BLIST) return fail(FA_ERR_CAPACITY, "mate-SW run list overflow");
+        if (h[0]) return fail(FA_ERR_ARG, "a mate job was rejected by the kernels");
+        if (mate_stats) {
+            float k_ms = 0.f;
+            cudaEventElapsedTime(&k_ms, c->pm_ev0, c->pm_ev1);
+            unsigned long long cells = (unsigned long long)h[2] | (unsigned long long)h[3] << 32;
+            mate_stats->cells = mate_stats->cells_executed = cells;
+            mate_stats->kernel_ms = k_ms;
+            mate_stats->kernel_launches = mlaunches;
+            mate_stats->jobs = mn;
+        }
+    }
+    const float total = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    if (stats) stats->total_ms = total;
+    if (mate_stats) mate_stats->total_ms = total;
+    return FA_OK;
+}
+
 int fa_mate_sw_batch(fa_ctx *c, const fa_mate_params *p, const fa_mate_job *jobs, uint32_t n,
                      const uint8_t *qseq, uint64_t qseq_len, const uint8_t *tseq, uint64_t tseq_len,
                      fa_kswr *out, fa_ext_stats *stats) {
@@ -2047,31 +2295,8 @@ int fa_mate_sw_batch(fa_ctx *c, const fa_mate_params *p, const fa_mate_job *jobs
     if (stats) memset(stats, 0, sizeof(*stats));
     if (n == 0) return FA_OK;
     if (!jobs || !out || !qseq || !tseq) return fail(FA_ERR_ARG, "null buffer");
-    int mn = 127, mx = 0;
-    for (int i = 0; i < 25; ++i) { mn = std::min<int>(mn, p->mat[i]); mx = std::max<int>(mx, p->mat[i]); }
-    if (mx <= 0) return fail(FA_ERR_ARG, "scoring matrix needs a positive entry");
-    MateParams mp;
-    memcpy(mp.mat, p->mat, 25);
-    mp.m = 5;
-    mp.o_del = p->o_del; mp.e_del = p->e_del; mp.o_ins = p->o_ins; mp.e_ins = p->e_ins;
-    mp.shift = (uint8_t)(256 - mn);
-    mp.max = mx;
-    std::vector<uint32_t> byte_list, word_list;
-    int mq_b = 0, mq_w = 0, mt = 0;
-    for (uint32_t i = 0; i < n; ++i) {
-        const fa_mate_job &j = jobs[i];
-        if (j.qlen <= 0 || j.tlen < 0) return fail(FA_ERR_ARG, "mate job %u: bad lengths", i);
-        if (j.tlen > FA_MAX_TLEN) return fail(FA_ERR_CAPACITY, "mate job %u: tlen too long", i);
-        if (j.q_off + (uint64_t)j.qlen > qseq_len || j.t_off + (uint64_t)j.tlen > tseq_len)
-            return fail(FA_ERR_ARG, "mate job %u: sequence range outside the buffers", i);
-        const bool byte = (j.xtra & FA_KSW_XBYTE) != 0;
-        if (byte ? j.qlen > 16 * 32 : j.qlen > 8 * 32)
-            return fail(FA_ERR_CAPACITY, "mate job %u: qlen=%d exceeds the %s-lane limit", i, j.qlen,
-                        byte ? "u8" : "i16");
-        (byte ? byte_list : word_list).push_back(i);
-        if (byte) mq_b = std::max(mq_b, j.qlen); else mq_w = std::max(mq_w, j.qlen);
-        mt = std::max(mt, j.tlen);
-    }
+    MateHostPlan pl;
+    if (int rc = plan_mate_host(p, jobs, n, qseq_len, tseq_len, &pl)) return rc;
     FA_CUDA(cudaSetDevice(c->device));
     cudaStream_t s = c->stream;
     FA_CUDA(c->jobs.ensure(sizeof(fa_mate_job) * (size_t)n));
@@ -2082,26 +2307,16 @@ int fa_mate_sw_batch(fa_ctx *c, const fa_mate_params *p, const fa_mate_job *jobs
     FA_CUDA(c->misc.ensure(kMiscBytes));
     Misc m = misc_of(c);
     FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
-    std::vector<uint32_t> order(byte_list);
-    order.insert(order.end(), word_list.begin(), word_list.end());
     FA_CUDA(cudaMemcpyAsync(c->jobs.p, jobs, sizeof(fa_mate_job) * (size_t)n, cudaMemcpyHostToDevice, s));
-    FA_CUDA(cudaMemcpyAsync(c->order.p, order.data(), 4ull * n, cudaMemcpyHostToDevice, s));
+    FA_CUDA(cudaMemcpyAsync(c->order.p, pl.order.data(), 4ull * n, cudaMemcpyHostToDevice, s));
     FA_CUDA(cudaMemcpyAsync(c->qseq.p, qseq, qseq_len, cudaMemcpyHostToDevice, s));
     FA_CUDA(cudaMemcpyAsync(c->tseq.p, tseq, tseq_len, cudaMemcpyHostToDevice, s));
     FA_CUDA(cudaEventRecord(c->ev0, s));
     uint32_t launches = 0;
-    if (!byte_list.empty()) {
-        FA_CUDA(launch_mate_sw(true, c->jobs.as<fa_mate_job>(), c->order.as<uint32_t>(),
-                               (uint32_t)byte_list.size(), c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(), mp,
-                               mq_b, mt, c->out.as<fa_kswr>(), m.cells, m.status, s));
-        ++launches;
-    }
-    if (!word_list.empty()) {
-        FA_CUDA(launch_mate_sw(false, c->jobs.as<fa_mate_job>(), c->order.as<uint32_t>() + byte_list.size(),
-                               (uint32_t)word_list.size(), c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(), mp,
-                               mq_w, mt, c->out.as<fa_kswr>(), m.cells, m.status, s));
-        ++launches;
-    }
+    FA_CUDA(c->mate_rev.ensure(4ull * (2 + (size_t)pl.n_byte)));
+    FA_CUDA(launch_mate_plan(pl, c->jobs.as<fa_mate_job>(), c->order.as<uint32_t>(), n, c->qseq.as<uint8_t>(),
+                             c->tseq.as<uint8_t>(), c->out.as<fa_kswr>(), m.cells, m.status,
+                             c->mate_rev.as<uint32_t>(), s, &launches));
     FA_CUDA(cudaEventRecord(c->ev1, s));
     if (int rc = read_status(c, s)) return rc;
     FA_CUDA(cudaMemcpyAsync(out, c->out.p, sizeof(fa_kswr) * (size_t)n, cudaMemcpyDeviceToHost, s));

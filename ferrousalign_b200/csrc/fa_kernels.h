@@ -71,15 +71,24 @@ cudaError_t launch_policy_step(const fa_job *d_jobs, const uint32_t *d_list, con
 cudaError_t launch_band_partition(const fa_job *d_jobs, const uint32_t *d_list, const uint32_t *d_count,
                                   uint32_t n_max, const int32_t *d_w_cur, uint32_t *d_out, uint32_t *d_hist,
                                   uint32_t *d_cursor, uint32_t *d_bounds, cudaStream_t stream);
+// dst[atomic positions] = src[0 .. *d_end), *d_end <= n_max (a device-side count)
+cudaError_t launch_list_append(const uint32_t *d_src, const uint32_t *d_end, uint32_t n_max, uint32_t *d_dst,
+                               uint32_t *d_dst_count, cudaStream_t stream);
+// sums[0..2] = {sum of cells_job, sum of tries (d_tries may be NULL), sum of missed (may be NULL)}
+cudaError_t launch_stats_sum(const uint32_t *d_cells_job, const int32_t *d_tries, const uint8_t *d_missed, uint32_t n,
+                             unsigned long long *d_sums, int sm_count, cudaStream_t stream);
 cudaError_t launch_policy_init(const fa_job *d_jobs, uint32_t n, const int32_t *d_w_first, int w_min,
                                int learned, PolicyState st, cudaStream_t stream);
 
 // Mate-rescue local SW.  `byte_lanes` selects the u8 (16-lane) or i16 (8-lane)
 // emulation of the reference's striped kernels; d_order lists the jobs of that kind.
+// d_rev (2 + n words; needed for u8 jobs, unused for i16 jobs): the list of KSW_XSTART
+// reverse passes that a second kernel runs after the forward passes.
 cudaError_t launch_mate_sw(bool byte_lanes, const fa_mate_job *d_jobs, const uint32_t *d_order,
                            uint32_t n, const uint8_t *d_qseq, const uint8_t *d_tseq,
                            const MateParams &p, int max_qlen, int max_tlen, fa_kswr *d_out,
-                           unsigned long long *d_cells, uint32_t *d_status, cudaStream_t stream);
+                           unsigned long long *d_cells, uint32_t *d_status, uint32_t *d_rev,
+                           cudaStream_t stream);
 
 // Device-side longest-first ordering by query length (order_kernel.cu).
 // Pipelined host batches: validation + (chunk, length) histogram + prefix, then scatter.

@@ -14,6 +14,7 @@
 // pass, and row maxima, the query-end search and the second-best scan are group
 // reductions.  The forward pass and the KSW_XSTART reverse pass share the same code.
 
+#include <algorithm>
 #include <climits>
 
 #include "fa_device.cuh"
@@ -236,10 +237,21 @@ __device__ __forceinline__ uint32_t lane_up_u16x2(uint32_t v, uint32_t gmask, in
     return prmt(v, prev, 0x1076u);   // low <- previous thread's high, high <- own low
 }
 
-template <int SMAX>
+// hm: this group's SMAX x 8 words of shared memory for the row snapshot at the best score
+// (slot a * 8 + l), kept out of registers so more groups fit on an SM.
+// rt: the block's profile rows in shared memory, rt[t] / rt[5 + t] the low / high table of
+// target base t (mate_row_tables).
+// REV: the KSW_XSTART reverse pass (KSW_XSTOP, no KSW_XSUBO), which keeps no run list.
+// FAST: the batch's jobs satisfy (qlen + 1) * max + shift <= 255 and the two gap penalties are
+// equal.  Every value is the score of an alignment of at most qlen query bases, so
+// hd + (mat + shift) stays below 256 and adds_epu8 never saturates: the profile byte is the
+// signed matrix entry (PRMT sign-extends it to 16 bits), one __viaddmax_s16x2_relu gives
+// max(hd + mat, E, 0), and the insertion and deletion terms share one subtraction.  Same
+// results as the general form.
+template <int SMAX, bool REV, bool FAST>
 __device__ fa_kswr sw_pass_u8x2(SeqView Q, int qlen, SeqView Tg, int tlen, uint32_t xtra, const MateParams &p,
-                                uint32_t gmask, int l, uint32_t *blist, int bcap, unsigned long long &cells,
-                                uint32_t &status)
+                                uint32_t gmask, int l, uint32_t *blist, int bcap, uint32_t *hm, const uint32_t *rt,
+                                unsigned long long &cells, uint32_t &status)
 {
     constexpr int P = 16;                      // lanes of the reference's u8 vector
     const int slen = (qlen + P - 1) / P;
@@ -273,74 +285,81 @@ __device__ fa_kswr sw_pass_u8x2(SeqView Q, int qlen, SeqView Tg, int tlen, uint3
                 }
             }
         }
-        // result bytes: [c_lo, zero, c_hi, zero] with the zero from byte 7 of the table
-        sel[a] = c2[0] | 0x70u | c2[1] << 8 | 0x7000u;
+        // result bytes: [c_lo, zero, c_hi, zero] with the zero from byte 7 of the table, or
+        // (FAST) [c_lo, sign of c_lo, c_hi, sign of c_hi]
+        sel[a] = FAST ? (c2[0] | (c2[0] | 8u) << 4 | c2[1] << 8 | (c2[1] | 8u) << 12)
+                      : (c2[0] | 0x70u | c2[1] << 8 | 0x7000u);
     }
 
-    uint32_t H0[SMAX], H1[SMAX], E[SMAX], Hm[SMAX];
+    // H: the previous row until a segment is updated, then the current one (in place)
+    uint32_t H[SMAX], E[SMAX];
 #pragma unroll
-    for (int a = 0; a < SMAX; ++a) { H0[a] = 0; H1[a] = 0; E[a] = 0; Hm[a] = 0; }
-
-    // profile rows (mat + shift mod 256 for codes 0..4, shift for padding code 5, 0 in byte 7)
-    uint32_t rlo[5], rhi[5];
-#pragma unroll
-    for (int t = 0; t < 5; ++t) {
-        rlo[t] = (uint8_t)(p.mat[t * 5] + shift) | (uint32_t)(uint8_t)(p.mat[t * 5 + 1] + shift) << 8 |
-                 (uint32_t)(uint8_t)(p.mat[t * 5 + 2] + shift) << 16 |
-                 (uint32_t)(uint8_t)(p.mat[t * 5 + 3] + shift) << 24;
-        rhi[t] = (uint8_t)(p.mat[t * 5 + 4] + shift) | (uint32_t)(uint8_t)shift << 8;
-    }
+    for (int a = 0; a < SMAX; ++a) { H[a] = 0; E[a] = 0; hm[a * 8 + l] = 0; }
 
     int gmax = 0, te = -1;
     int nb = 0, last_row = -2, last_sc = 0;
 
+    int rows = tlen;   // rows computed (cell count)
+    uint32_t tb_next = tlen > 0 ? Tg.at(0) : 0u;
     for (int i = 0; i < tlen; ++i) {
-        const uint32_t tb = Tg.at(i);
-        if (tb > 4u) { bad = 1; break; }
-        uint32_t lo = rlo[0], hi = rhi[0];
-#pragma unroll
-        for (int t = 1; t < 5; ++t)
-            if (tb == (uint32_t)t) { lo = rlo[t]; hi = rhi[t]; }
-        cells += (unsigned long long)qlen;
+        const uint32_t tb = tb_next;
+        if (i + 1 < tlen) tb_next = Tg.at(i + 1);   // the next row's base, in flight during this row
+        if (tb > 4u) { bad = 1; rows = i; break; }
+        const uint32_t lo = rt[tb], hi = rt[5 + tb];
 
-        uint32_t hd = lane_up_u16x2(H0[SMAX - 1], gmask, l);
-        uint32_t f = 0, mx = 0;
+        uint32_t hd = lane_up_u16x2(H[SMAX - 1], gmask, l);
+        uint32_t f = 0;
 #pragma unroll
         for (int a = 0; a < SMAX; ++a) {
             if (a >= off) {
                 const uint32_t s = prmt(lo, hi, sel[a]);
-                uint32_t h = __viaddmin_u16x2(hd, s, cap255);          // adds_epu8
-                h = __viaddmax_s16x2_relu(h, neg_shift2, 0u);          // subs_epu8(., shift)
                 const uint32_t e = E[a];
-                h = __vimax3_s16x2(h, e, f);
-                mx = __vimax3_s16x2(mx, h, h);
-                H1[a] = h;
+                uint32_t h;
+                if (FAST) {
+                    h = __viaddmax_s16x2_relu(hd, s, e);               // max(hd + mat, E, 0)
+                    h = __vimax_s16x2_relu(h, f);
+                } else {
+                    h = __viaddmin_u16x2(hd, s, cap255);               // adds_epu8
+                    h = __viaddmax_s16x2_relu(h, neg_shift2, 0u);      // subs_epu8(., shift)
+                    h = __vimax3_s16x2(h, e, f);
+                }
+                hd = H[a];                                             // the next segment's diagonal
+                H[a] = h;
                 const uint32_t tdel = __viaddmax_s16x2(h, neg_oedel2, neg2);
                 E[a] = __viaddmax_s16x2_relu(e, neg_edel2, tdel);
-                const uint32_t tins = __viaddmax_s16x2(h, neg_oeins2, neg2);
+                const uint32_t tins = FAST ? tdel : __viaddmax_s16x2(h, neg_oeins2, neg2);
                 f = __viaddmax_s16x2_relu(f, neg_eins2, tins);
-                hd = H0[a];
             }
         }
-        // lazy-F: one lane further per pass, stop after a pass that changed nothing
+        // the row maximum before the lazy-F correction (the reference's max_epu8 in the
+        // segment loop): slots below `off` still hold their initial zero
+        uint32_t mx = 0;
+#pragma unroll
+        for (int a = 0; a < SMAX; a += 2)
+            mx = a + 1 < SMAX ? __vimax3_s16x2(mx, H[a], H[a + 1]) : __vimax_s16x2_relu(mx, H[a]);
+        // lazy-F: one lane further per pass, stop after a pass that changed nothing.  Every
+        // value is >= 0, so a lane whose incoming F is zero in both halves changes nothing in
+        // this pass (max(H, 0) = H, and F stays 0): it skips the segments.
         for (int pass = 0; pass < P; ++pass) {
             f = lane_up_u16x2(f, gmask, l);
             uint32_t changed = 0;
+            if (f != 0u) {
 #pragma unroll
-            for (int a = 0; a < SMAX; ++a) {
-                if (a >= off) {
-                    const uint32_t hb = H1[a];
-                    const uint32_t hn = __vimax3_s16x2(hb, f, f);
-                    changed |= hn ^ hb;
-                    H1[a] = hn;
-                    f = __viaddmax_s16x2_relu(f, neg_eins2, 0u);
+                for (int a = 0; a < SMAX; ++a) {
+                    if (a >= off) {
+                        const uint32_t hb = H[a];
+                        const uint32_t hn = __vimax3_s16x2(hb, f, f);
+                        changed |= hn ^ hb;
+                        H[a] = hn;
+                        f = __viaddmax_s16x2_relu(f, neg_eins2, 0u);
+                    }
                 }
             }
             if (!__any_sync(gmask, changed != 0)) break;
         }
         const uint32_t mx1 = max(mx & 0xffffu, mx >> 16);
         const int imax = (int)__reduce_max_sync(gmask, mx1);
-        if ((uint32_t)imax >= minsc) {
+        if (!REV && (uint32_t)imax >= minsc) {
             if (nb == 0 || last_row + 1 != i) {
                 if (nb < bcap) {
                     if (l == 0) blist[nb] = (uint32_t)imax << 16 | (uint32_t)i;
@@ -360,12 +379,11 @@ __device__ fa_kswr sw_pass_u8x2(SeqView Q, int qlen, SeqView Tg, int tlen, uint3
             gmax = imax;
             te = i;
 #pragma unroll
-            for (int a = 0; a < SMAX; ++a) Hm[a] = H1[a];
-            if (gmax + (int)shift >= 255 || (uint32_t)gmax >= endsc) break;
+            for (int a = 0; a < SMAX; ++a) hm[a * 8 + l] = H[a];
+            if (gmax + (int)shift >= 255 || (uint32_t)gmax >= endsc) { rows = i + 1; break; }
         }
-#pragma unroll
-        for (int a = 0; a < SMAX; ++a) H0[a] = H1[a];
     }
+    cells += (unsigned long long)rows * (unsigned)qlen;
     if (bad) status |= ST_BAD_CODE;
 
     fa_kswr r;
@@ -382,7 +400,8 @@ __device__ fa_kswr sw_pass_u8x2(SeqView Q, int qlen, SeqView Tg, int tlen, uint3
                 for (int h = 0; h < 2; ++h) {
                     const int k = (a - off) + (2 * l + h) * slen;
                     if (k < qlen) {
-                        const int v = (int)(int8_t)(uint8_t)(h ? (Hm[a] >> 16) : (Hm[a] & 0xffffu));
+                        const uint32_t w = hm[a * 8 + l];
+                        const int v = (int)(int8_t)(uint8_t)(h ? (w >> 16) : (w & 0xffffu));
                         if (v > bv || (v == bv && k < bk)) { bv = v; bk = k; }
                     }
                 }
@@ -391,7 +410,7 @@ __device__ fa_kswr sw_pass_u8x2(SeqView Q, int qlen, SeqView Tg, int tlen, uint3
         const int gv = __reduce_max_sync(gmask, bv);
         r.qe = __reduce_min_sync(gmask, bv == gv ? bk : INT_MAX);
         if (r.qe == INT_MAX) r.qe = -1;
-        if (nb > 0) {
+        if (!REV && nb > 0) {
             __syncwarp(gmask);
             const int iv = (r.score + p.max - 1) / p.max;
             const int low = te - iv, high = te + iv;
@@ -412,6 +431,20 @@ __device__ fa_kswr sw_pass_u8x2(SeqView Q, int qlen, SeqView Tg, int tlen, uint3
         }
     }
     return r;
+}
+
+// Whether ksw_align2's KSW_XSTART reverse pass (ksw_affine_gap.rs, ksw_align2) runs for a
+// forward result, and whether it can change the result.  Every value of the reverse pass is
+// the score of an alignment of the reversed query prefix 0..qe, so it is at most
+// (qe + 1) * max: below the forward score the pass can neither stop early (KSW_XSTOP at the
+// forward score, u8 saturation above it) nor set tb / qb -- it runs all tlen rows for
+// nothing, and only its cell count is kept.
+__device__ __forceinline__ bool mate_needs_start(const fa_kswr &r, uint32_t xtra) {
+    return (xtra & FA_KSW_XSTART) && !((xtra & FA_KSW_XSUBO) && r.score < (int)(xtra & 0xffffu)) && r.qe >= 0 &&
+           r.te >= 0;
+}
+__device__ __forceinline__ bool mate_start_reachable(const fa_kswr &r, const MateParams &p) {
+    return (r.qe + 1) * p.max >= r.score;
 }
 
 template <int P, int SMAX>
@@ -436,10 +469,9 @@ mate_sw_kernel(const fa_mate_job *__restrict__ jobs, const uint32_t *__restrict_
         SeqView Q{qseq + jb.q_off, -1}, Tg{tseq + jb.t_off, -1};
         fa_kswr r = sw_pass<P, SMAX>(Q, jb.qlen, Tg, jb.tlen, jb.xtra, p, gmask, l, blist, bcap,
                                      cells, st);
-        const uint32_t xtra = jb.xtra;
-        const bool find_start = (xtra & FA_KSW_XSTART) &&
-                                !((xtra & FA_KSW_XSUBO) && r.score < (int)(xtra & 0xffffu));
-        if (find_start && r.qe >= 0 && r.te >= 0) {
+        if (mate_needs_start(r, jb.xtra) && !mate_start_reachable(r, p)) {
+            cells += (unsigned long long)(r.qe + 1) * (unsigned)jb.tlen;
+        } else if (mate_needs_start(r, jb.xtra)) {
             SeqView Q2{qseq + jb.q_off, r.qe}, T2{tseq + jb.t_off, r.te};
             const fa_kswr rr = sw_pass<P, SMAX>(Q2, r.qe + 1, T2, jb.tlen,
                                                 FA_KSW_XSTOP | (uint32_t)r.score, p, gmask, l,
@@ -461,16 +493,36 @@ mate_sw_kernel(const fa_mate_job *__restrict__ jobs, const uint32_t *__restrict_
     }
 }
 
-// u8 jobs: one 8-thread group per job, two reference lanes per thread (sw_pass_u8x2).
-template <int SMAX>
+// The profile row tables of the u8 engine in shared memory (mat + shift mod 256 for codes
+// 0..4, shift for padding code 5, 0 in byte 7): rt[t] the low and rt[5 + t] the high word of
+// target base t's table.  Threads 0-4 write them; the caller synchronises.
+// With FAST (sw_pass_u8x2) the bytes are the signed matrix entries and padding scores 0.
+template <bool FAST>
+__device__ __forceinline__ void mate_row_tables(uint32_t *rt, const MateParams &p) {
+    if (threadIdx.x < 5) {
+        const int t = threadIdx.x;
+        const uint32_t sh = FAST ? 0u : (uint32_t)p.shift;
+        rt[t] = (uint8_t)(p.mat[t * 5] + sh) | (uint32_t)(uint8_t)(p.mat[t * 5 + 1] + sh) << 8 |
+                (uint32_t)(uint8_t)(p.mat[t * 5 + 2] + sh) << 16 | (uint32_t)(uint8_t)(p.mat[t * 5 + 3] + sh) << 24;
+        rt[5 + t] = (uint8_t)(p.mat[t * 5 + 4] + sh) | (uint32_t)(uint8_t)sh << 8;
+    }
+}
+
+// u8 jobs: one 8-thread group per job, two reference lanes per thread (sw_pass_u8x2): the
+// forward pass of every job.  A reverse pass that can reach the forward score is appended to
+// `rev` (rev[0] the count, the job ids from rev[2]) for mate_rev_kernel_u8x2, which keeps
+// all its groups busy with listed jobs.
+template <int SMAX, bool FAST>
 __global__ void __launch_bounds__(kMateThreads)
 mate_sw_kernel_u8x2(const fa_mate_job *__restrict__ jobs, const uint32_t *__restrict__ order, uint32_t n,
                     const uint8_t *__restrict__ qseq, const uint8_t *__restrict__ tseq, const MateParams p,
                     int bcap, fa_kswr *__restrict__ out, unsigned long long *__restrict__ cells_out,
-                    uint32_t *__restrict__ status)
+                    uint32_t *__restrict__ status, uint32_t *__restrict__ rev)
 {
     constexpr int G = 8;
     extern __shared__ uint32_t bsm[];
+    mate_row_tables<FAST>(bsm, p);
+    __syncthreads();
     const uint32_t gtid = blockIdx.x * kMateThreads + threadIdx.x;
     const uint32_t gidx = gtid / G;
     const int lane = threadIdx.x & 31;
@@ -481,17 +533,18 @@ mate_sw_kernel_u8x2(const fa_mate_job *__restrict__ jobs, const uint32_t *__rest
     if (gidx < n) {
         const uint32_t jid = order ? order[gidx] : gidx;
         const fa_mate_job jb = jobs[jid];
-        uint32_t *blist = bsm + (threadIdx.x / G) * bcap;
+        // this group's run list, then its row snapshot (the block's lists come first)
+        uint32_t *blist = bsm + 16 + (threadIdx.x / G) * bcap;
+        uint32_t *hm = bsm + 16 + (kMateThreads / G) * bcap + (threadIdx.x / G) * (SMAX * G);
         SeqView Q{qseq + jb.q_off, -1}, Tg{tseq + jb.t_off, -1};
-        fa_kswr r = sw_pass_u8x2<SMAX>(Q, jb.qlen, Tg, jb.tlen, jb.xtra, p, gmask, l, blist, bcap, cells, st);
-        const uint32_t xtra = jb.xtra;
-        const bool find_start = (xtra & FA_KSW_XSTART) &&
-                                !((xtra & FA_KSW_XSUBO) && r.score < (int)(xtra & 0xffffu));
-        if (find_start && r.qe >= 0 && r.te >= 0) {
-            SeqView Q2{qseq + jb.q_off, r.qe}, T2{tseq + jb.t_off, r.te};
-            const fa_kswr rr = sw_pass_u8x2<SMAX>(Q2, r.qe + 1, T2, jb.tlen, FA_KSW_XSTOP | (uint32_t)r.score, p,
-                                                  gmask, l, blist, bcap, cells, st);
-            if (rr.score >= r.score) { r.tb = r.te - rr.te; r.qb = r.qe - rr.qe; }
+        fa_kswr r = sw_pass_u8x2<SMAX, false, FAST>(Q, jb.qlen, Tg, jb.tlen, jb.xtra, p, gmask, l, blist, bcap, hm, bsm,
+                                              cells, st);
+        if (mate_needs_start(r, jb.xtra)) {
+            if (!mate_start_reachable(r, p)) {
+                cells += (unsigned long long)(r.qe + 1) * (unsigned)jb.tlen;
+            } else if (l == 0) {
+                rev[2 + atomicAdd(rev, 1u)] = jid;
+            }
         }
         st = __reduce_or_sync(gmask, st);
         if (l == 0) {
@@ -508,20 +561,89 @@ mate_sw_kernel_u8x2(const fa_mate_job *__restrict__ jobs, const uint32_t *__rest
     }
 }
 
-template <int SMAX>
+// The reverse passes listed by mate_sw_kernel_u8x2, four jobs per warp taken from a shared
+// counter (rev[1]) as warps finish, the forward result read back from `out`.
+template <int SMAX, bool FAST>
+__global__ void __launch_bounds__(kMateThreads, 7)
+mate_rev_kernel_u8x2(const fa_mate_job *__restrict__ jobs, const uint8_t *__restrict__ qseq,
+                     const uint8_t *__restrict__ tseq, const MateParams p, fa_kswr *__restrict__ out,
+                     unsigned long long *__restrict__ cells_out, uint32_t *__restrict__ status,
+                     uint32_t *__restrict__ rev)
+{
+    constexpr int G = 8;
+    extern __shared__ uint32_t bsm[];
+    mate_row_tables<FAST>(bsm, p);
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int l = lane % G;
+    const uint32_t gmask = ((1u << G) - 1u) << (lane - l);
+    uint32_t *hm = bsm + 16 + (threadIdx.x / G) * (SMAX * G);
+    const uint32_t count = *(volatile uint32_t *)rev;
+    unsigned long long cells = 0;
+    uint32_t st = 0;
+    for (;;) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(rev + 1, 32u / G);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= count) break;
+        const uint32_t idx = base + lane / G;
+        if (idx < count) {
+            const uint32_t jid = rev[2 + idx];
+            const fa_mate_job jb = jobs[jid];
+            const fa_kswr r = out[jid];
+            SeqView Q2{qseq + jb.q_off, r.qe}, T2{tseq + jb.t_off, r.te};
+            const fa_kswr rr = sw_pass_u8x2<SMAX, true, FAST>(Q2, r.qe + 1, T2, jb.tlen, FA_KSW_XSTOP | (uint32_t)r.score, p,
+                                                        gmask, l, nullptr, 0, hm, bsm, cells, st);
+            if (l == 0 && rr.score >= r.score) {
+                out[jid].tb = r.te - rr.te;
+                out[jid].qb = r.qe - rr.qe;
+            }
+        }
+        __syncwarp();
+    }
+    st = __reduce_or_sync(0xffffffffu, st);
+    if (lane == 0 && st) atomicOr(status, st);
+    if (l != 0) cells = 0;
+    if (cells_out) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) cells += __shfl_down_sync(0xffffffffu, cells, o);
+        if (lane == 0 && cells) atomicAdd(cells_out, cells);
+    }
+}
+
+template <int SMAX, bool FAST>
 static cudaError_t launch_mate_u8x2(const fa_mate_job *d_jobs, const uint32_t *d_order, uint32_t n,
                                     const uint8_t *d_qseq, const uint8_t *d_tseq, const MateParams &p, int bcap,
-                                    fa_kswr *d_out, unsigned long long *d_cells, uint32_t *d_status,
+                                    fa_kswr *d_out, unsigned long long *d_cells, uint32_t *d_status, uint32_t *d_rev,
                                     cudaStream_t stream)
 {
-    const size_t smem = (size_t)(kMateThreads / 8) * bcap * sizeof(uint32_t);
-    cudaError_t err = cudaFuncSetAttribute(mate_sw_kernel_u8x2<SMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    const size_t smem = (16 + (size_t)(kMateThreads / 8) * (bcap + SMAX * 8)) * sizeof(uint32_t);
+    cudaError_t err = cudaFuncSetAttribute(mate_sw_kernel_u8x2<SMAX, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)smem);
+    if (err != cudaSuccess) return err;
+    if (!d_rev) return cudaErrorInvalidValue;
+    err = cudaMemsetAsync(d_rev, 0, 2 * sizeof(uint32_t), stream);
     if (err != cudaSuccess) return err;
     const uint64_t threads = (uint64_t)n * 8;
     const uint32_t blocks = (uint32_t)((threads + kMateThreads - 1) / kMateThreads);
-    mate_sw_kernel_u8x2<SMAX><<<blocks, kMateThreads, smem, stream>>>(d_jobs, d_order, n, d_qseq, d_tseq, p, bcap,
-                                                                      d_out, d_cells, d_status);
+    mate_sw_kernel_u8x2<SMAX, FAST><<<blocks, kMateThreads, smem, stream>>>(d_jobs, d_order, n, d_qseq, d_tseq, p, bcap,
+                                                                      d_out, d_cells, d_status, d_rev);
+    err = cudaGetLastError();
+    if (err != cudaSuccess) return err;
+    // reverse passes: as many blocks as are resident at once (or as the jobs need), each warp
+    // taking four listed jobs at a time until the list is done
+    const size_t rsmem = (16 + (size_t)(kMateThreads / 8) * SMAX * 8) * sizeof(uint32_t);
+    err = cudaFuncSetAttribute(mate_rev_kernel_u8x2<SMAX, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsmem);
+    if (err != cudaSuccess) return err;
+    int dev = 0, sms = 0, per_sm = 0;
+    if ((err = cudaGetDevice(&dev)) != cudaSuccess) return err;
+    if ((err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return err;
+    if ((err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mate_rev_kernel_u8x2<SMAX, FAST>, kMateThreads,
+                                                             rsmem)) != cudaSuccess)
+        return err;
+    const uint32_t rblocks = std::min<uint32_t>(blocks, (uint32_t)std::max(1, sms * std::max(per_sm, 1)));
+    mate_rev_kernel_u8x2<SMAX, FAST><<<rblocks, kMateThreads, rsmem, stream>>>(d_jobs, d_qseq, d_tseq, p, d_out, d_cells,
+                                                                         d_status, d_rev);
     return cudaGetLastError();
 }
 
@@ -545,7 +667,8 @@ static cudaError_t launch_mate_t(const fa_mate_job *d_jobs, const uint32_t *d_or
 cudaError_t launch_mate_sw(bool byte_lanes, const fa_mate_job *d_jobs, const uint32_t *d_order,
                            uint32_t n, const uint8_t *d_qseq, const uint8_t *d_tseq,
                            const MateParams &p, int max_qlen, int max_tlen, fa_kswr *d_out,
-                           unsigned long long *d_cells, uint32_t *d_status, cudaStream_t stream)
+                           unsigned long long *d_cells, uint32_t *d_status, uint32_t *d_rev,
+                           cudaStream_t stream)
 {
     if (n == 0) return cudaSuccess;
     const int bcap = (max_tlen + 1) / 2 + 2;   // consecutive list rows differ by >= 2
@@ -554,7 +677,12 @@ cudaError_t launch_mate_sw(bool byte_lanes, const fa_mate_job *d_jobs, const uin
     // the batch's query length (151-bp mates: 10 u8 segments, 19 i16 segments)
 #define FA_MATE(PP, SS) launch_mate_t<PP, SS>(d_jobs, d_order, n, d_qseq, d_tseq, p, bcap, d_out, d_cells, d_status, \
                                               stream)
-#define FA_MATE2(SS) launch_mate_u8x2<SS>(d_jobs, d_order, n, d_qseq, d_tseq, p, bcap, d_out, d_cells, d_status, stream)
+#define FA_MATE2(SS) (fast ? launch_mate_u8x2<SS, true>(d_jobs, d_order, n, d_qseq, d_tseq, p, bcap, d_out, d_cells, \
+                                                      d_status, d_rev, stream)                                      \
+                  : launch_mate_u8x2<SS, false>(d_jobs, d_order, n, d_qseq, d_tseq, p, bcap, d_out, d_cells,       \
+                                                d_status, d_rev, stream))
+    // sw_pass_u8x2's FAST form: no u8 saturation possible below the score cap, equal gap penalties
+    const bool fast = (max_qlen + 1) * p.max + (p.shift & 0xff) <= 255 && p.o_del == p.o_ins && p.e_del == p.e_ins;
     if (byte_lanes) {
         if (max_qlen <= 16 * 10) return FA_MATE2(10);
         if (max_qlen <= 16 * 12) return FA_MATE2(12);

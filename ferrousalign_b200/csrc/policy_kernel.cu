@@ -168,10 +168,12 @@ __global__ void band_scatter_kernel(const fa_job *__restrict__ jobs, const uint3
         uint32_t acc = 0;
         for (int k = 0; k < kBandBuckets; ++k) { base[k] = acc; acc += hist[k]; }
         if (bounds && blockIdx.x == 0) {
-            // band groups: buckets 0-4 (configured band, bands > 24), 5-6 (13-24), 7-12 (<= 12)
+            // band groups: buckets 0-4 (configured band, bands > 24), 5-6 (13-24), 7-12 (<= 12);
+            // bounds[3]: the end of bucket 0 (the jobs at their configured band)
             bounds[0] = base[5];
             bounds[1] = base[7];
             bounds[2] = acc;
+            bounds[3] = base[1];
         }
     }
     __syncthreads();
@@ -205,6 +207,65 @@ cudaError_t launch_band_partition(const fa_job *d_jobs, const uint32_t *d_list, 
     band_hist_kernel<<<blocks, 256, 0, stream>>>(d_jobs, d_list, d_count, n_max, d_w_cur, d_hist);
     band_scatter_kernel<<<blocks, 256, 0, stream>>>(d_jobs, d_list, d_count, n_max, d_w_cur, d_hist, d_cursor, d_out,
                                                     d_bounds);
+    return cudaGetLastError();
+}
+
+// A batch's statistics summed on the device: sums = {cells of the accepted runs, runs per
+// job (tries, when given), missed narrow tries (when given)}, so a call reads back three words
+// instead of its per-job arrays.
+__global__ void __launch_bounds__(256) stats_sum_kernel(const uint32_t *__restrict__ cells_job,
+                                                        const int32_t *__restrict__ tries,
+                                                        const uint8_t *__restrict__ missed, uint32_t n,
+                                                        unsigned long long *__restrict__ sums)
+{
+    unsigned long long v[3] = {0, 0, 0};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        v[0] += cells_job[i];
+        if (tries) v[1] += (uint32_t)tries[i];
+        if (missed) v[2] += missed[i];
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+        if ((threadIdx.x & 31) == 0 && v[k]) atomicAdd(&sums[k], v[k]);
+    }
+}
+
+cudaError_t launch_stats_sum(const uint32_t *d_cells_job, const int32_t *d_tries, const uint8_t *d_missed, uint32_t n,
+                             unsigned long long *d_sums, int sm_count, cudaStream_t stream)
+{
+    cudaError_t e = cudaMemsetAsync(d_sums, 0, 3 * sizeof(unsigned long long), stream);
+    if (e != cudaSuccess || n == 0) return e;
+    uint32_t blocks = (n + 255) / 256;
+    if (blocks > (uint32_t)sm_count * 8) blocks = sm_count * 8;
+    stats_sum_kernel<<<blocks, 256, 0, stream>>>(d_cells_job, d_tries, d_missed, n, d_sums);
+    return cudaGetLastError();
+}
+
+// Appends src[0 .. *d_end) (a device-side count, at most n_max) to dst at the positions an
+// atomic counter hands out, one claim per warp; the order inside dst is not kept.
+__global__ void __launch_bounds__(256) list_append_kernel(const uint32_t *__restrict__ src,
+                                                          const uint32_t *__restrict__ d_end, uint32_t n_max,
+                                                          uint32_t *__restrict__ dst, uint32_t *__restrict__ dst_count)
+{
+    const uint32_t n = min(*d_end, n_max);
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = i < n;
+    const unsigned mask = __ballot_sync(0xffffffffu, live);
+    if (!mask) return;
+    const int lane = threadIdx.x & 31;
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(dst_count, (uint32_t)__popc(mask));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (live) dst[base + __popc(mask & ((1u << lane) - 1u))] = src[i];
+}
+
+cudaError_t launch_list_append(const uint32_t *d_src, const uint32_t *d_end, uint32_t n_max, uint32_t *d_dst,
+                               uint32_t *d_dst_count, cudaStream_t stream)
+{
+    if (n_max == 0) return cudaSuccess;
+    list_append_kernel<<<(n_max + 255) / 256, 256, 0, stream>>>(d_src, d_end, n_max, d_dst, d_dst_count);
     return cudaGetLastError();
 }
 

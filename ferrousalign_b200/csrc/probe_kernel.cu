@@ -8,12 +8,24 @@
 // instruction kind, not latency or bookkeeping, bounds the run.
 
 #include <cstdio>
+#include <cuda_fp16.h>
 
 #include "fa_kernels.h"
 
 namespace fa {
 
 constexpr int kProbeChains = 32;
+
+__device__ __forceinline__ __half2 u2h(uint32_t x) {
+    __half2 h;
+    memcpy(&h, &x, 4);
+    return h;
+}
+__device__ __forceinline__ uint32_t h2u(__half2 h) {
+    uint32_t x;
+    memcpy(&x, &h, 4);
+    return x;
+}
 constexpr int kProbeUnroll = 4;
 
 template <int KIND>
@@ -32,7 +44,17 @@ __global__ void __launch_bounds__(256) probe_kernel(uint32_t b, uint32_t c, int 
                 else if (KIND == 1) acc[k] = __vimax3_s16x2_relu(acc[k], b, c);
                 else if (KIND == 2) acc[k] = (uint32_t)__viaddmax_s32_relu((int)acc[k], (int)b, (int)c);
                 else if (KIND == 3) acc[k] = (uint32_t)__vimax3_s32((int)acc[k], (int)b, (int)c);
-                else acc[k] = (uint32_t)max((int)acc[k] + (int)b, (int)c);
+                else if (KIND == 4) acc[k] = (uint32_t)max((int)acc[k] + (int)b, (int)c);
+                else if (KIND == 5) acc[k] = h2u(__hmax2(u2h(acc[k]), u2h(b)));
+                else if (KIND == 6) acc[k] = h2u(__hadd2(u2h(acc[k]), u2h(b)));
+                else if (KIND == 7) acc[k] = acc[k] * b + c;                         // IMAD
+                else if (KIND == 8) {   // half the chains on DPX, half on half2 max: shared pipe or not
+                    if (k & 1) acc[k] = h2u(__hmax2(u2h(acc[k]), u2h(b)));
+                    else acc[k] = __viaddmax_s16x2_relu(acc[k], b, c);
+                } else {                // KIND 9: DPX and IMAD interleaved
+                    if (k & 1) acc[k] = acc[k] * b + c;
+                    else acc[k] = __viaddmax_s16x2_relu(acc[k], b, c);
+                }
             }
         }
     }
@@ -43,7 +65,9 @@ __global__ void __launch_bounds__(256) probe_kernel(uint32_t b, uint32_t c, int 
 }
 
 // ops/s for one instruction kind (0: viaddmax_s16x2_relu, 1: vimax3_s16x2_relu,
-// 2: viaddmax_s32_relu, 3: vimax3_s32, 4: add+max as two plain instructions).
+// 2: viaddmax_s32_relu, 3: vimax3_s32, 4: add+max as two plain instructions, 5: half2 max,
+// 6: half2 add, 7: integer multiply-add, 8: DPX and half2 max on alternate chains, 9: DPX and
+// integer multiply-add on alternate chains -- the last two tell whether the kinds share a pipe).
 double probe_int_peak(int kind, int sm_count, cudaStream_t s, float *ms_out)
 {
     uint32_t *sink = nullptr;
@@ -58,6 +82,11 @@ double probe_int_peak(int kind, int sm_count, cudaStream_t s, float *ms_out)
             case 1: probe_kernel<1><<<blocks, threads, 0, s>>>(0x00010001u, 0x00020002u, iters, sink); break;
             case 2: probe_kernel<2><<<blocks, threads, 0, s>>>(1u, 2u, iters, sink); break;
             case 3: probe_kernel<3><<<blocks, threads, 0, s>>>(1u, 2u, iters, sink); break;
+            case 5: probe_kernel<5><<<blocks, threads, 0, s>>>(0x64006400u, 0x64016401u, iters, sink); break;
+            case 6: probe_kernel<6><<<blocks, threads, 0, s>>>(0x00010001u, 0u, iters, sink); break;
+            case 7: probe_kernel<7><<<blocks, threads, 0, s>>>(3u, 1u, iters, sink); break;
+            case 8: probe_kernel<8><<<blocks, threads, 0, s>>>(0x00010001u, 0x00020002u, iters, sink); break;
+            case 9: probe_kernel<9><<<blocks, threads, 0, s>>>(0x00010001u, 0x00020002u, iters, sink); break;
             default: probe_kernel<4><<<blocks, threads, 0, s>>>(1u, 2u, iters, sink); break;
         }
     };

@@ -87,16 +87,16 @@ def unpack(ps: PackedSeq) -> np.ndarray:
 
 def extend_batch_packed(params: np.ndarray, jobs: np.ndarray, qseq: PackedSeq, tseq: PackedSeq,
                         policy: np.ndarray | None = None, w_first: np.ndarray | None = None,
-                        ctx: N.Context | None = None, out: np.ndarray | None = None):
+                        ctx: N.Context | None = None, out: np.ndarray | None = None, bands: bool = True):
     """fa_ext_batch_packed.  Returns (results, stats, w_final); `out` may be a (pinned)
-    result buffer to fill."""
+    result buffer to fill; bands=False asks for no final bands (None)."""
     lib = N.load()
     ctx = ctx or N.default_context()
     jobs = np.ascontiguousarray(jobs, N.JOB_DT)
     n = len(jobs)
     out = np.zeros(n, N.EXT_RESULT_DT) if out is None else out
     stats = np.zeros(1, N.STATS_DT)
-    w_final = np.zeros(n, np.int32)
+    w_final = np.zeros(n, np.int32) if bands else None
     wf = None if w_first is None else np.ascontiguousarray(w_first, np.int32)
     qs, ts = qseq.struct(), tseq.struct()
     N.check(lib.fa_ext_batch_packed(ctx.handle, N.ptr(params), N.ptr(policy), N.ptr(jobs), n, N.ptr(qs), N.ptr(ts),
@@ -107,8 +107,9 @@ def extend_batch_packed(params: np.ndarray, jobs: np.ndarray, qseq: PackedSeq, t
 def extend_batch_learned_packed(params: np.ndarray, jobs: np.ndarray, qseq: PackedSeq, tseq: PackedSeq, model,
                                 hints: np.ndarray | None = None, judge: int | None = None, margin: float = 0.0,
                                 w_min: int = 2, max_tries: int = 2, ctx: N.Context | None = None,
-                                out: np.ndarray | None = None):
-    """fa_ext_batch_learned_packed.  Returns (results, stats, w_first, w_final)."""
+                                out: np.ndarray | None = None, bands: bool = True):
+    """fa_ext_batch_learned_packed.  Returns (results, stats, w_first, w_final); bands=False
+    asks for neither band array (None, None)."""
     from .band_model import HINT_DT, JUDGE_LEARNED
     from .batch_extension import make_policy
     ctx = ctx or N.default_context()
@@ -116,13 +117,12 @@ def extend_batch_learned_packed(params: np.ndarray, jobs: np.ndarray, qseq: Pack
     n = len(jobs)
     out = np.zeros(n, N.EXT_RESULT_DT) if out is None else out
     stats = np.zeros(1, N.STATS_DT)
-    wf = np.zeros(n, np.int32)
-    wfin = np.zeros(n, np.int32)
+    wf = np.zeros(n, np.int32) if bands else None
+    wfin = np.zeros(n, np.int32) if bands else None
     pol = make_policy(N.FA_POLICY_LEARNED, max_tries, JUDGE_LEARNED if judge is None else judge, w_min)
     h = None if hints is None else np.ascontiguousarray(hints, HINT_DT)
     qs, ts = qseq.struct(), tseq.struct()
     N.check(N.load().fa_ext_batch_learned_packed(ctx.handle, N.ptr(params), N.ptr(pol), model.handle, margin,
                                                  jobs.ctypes.data, n, N.ptr(qs), N.ptr(ts), N.ptr(h),
-                                                 out.ctypes.data, wf.ctypes.data, wfin.ctypes.data,
-                                                 stats.ctypes.data))
+                                                 out.ctypes.data, N.ptr(wf), N.ptr(wfin), stats.ctypes.data))
     return out, stats[0], wf, wfin

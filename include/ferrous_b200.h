@@ -155,7 +155,9 @@ const char *fa_version(void);
 /* Diagnostics (no reference counterpart): SM count / opt-in shared memory of the
  * context's device, and the measured throughput of one integer instruction kind
  * (0: __viaddmax_s16x2_relu, 1: __vimax3_s16x2_relu, 2: __viaddmax_s32_relu,
- *  3: __vimax3_s32, 4: add + max as two instructions), used as the roofline peak. */
+ *  3: __vimax3_s32, 4: add + max as two instructions, 5: half2 max, 6: half2 add,
+ *  7: integer multiply-add, 8 / 9: kind 0 and kind 5 / 7 on alternate chains), used as the
+ * roofline peak (kind 0) and to tell which instruction kinds share an issue pipe. */
 int fa_device_info(fa_ctx *ctx, int *sm_count, int *smem_optin_bytes);
 int fa_probe_int_peak(fa_ctx *ctx, int kind, double *ops_per_s, float *ms);
 
@@ -268,6 +270,12 @@ int fa_ctx_set_threads(fa_ctx *ctx, int threads_per_block);
  * trip between rounds.  Results are identical either way.  The host-side copies stay
  * outside the graph.  Turning it off releases the recorded graph. */
 int fa_ctx_set_graph(fa_ctx *ctx, int enable);
+
+/* Upload slices of host batches of 32,768 jobs or more (no reference counterpart): the
+ * sequences of a single-band batch, and of a retry-policy or learned batch that runs its rounds
+ * slice by slice, go up in this many graded slices (2..8, default 8 for both; 0 keeps a value).
+ * Results are identical for every setting; only the overlap of copies and kernels changes. */
+int fa_ctx_set_slices(fa_ctx *ctx, int single_band, int policy_rounds);
 
 /* Kernel timing of device-resident calls (no reference counterpart): with timing on,
  * fa_ext_batch_device brackets its extension kernels with CUDA events on the call's
@@ -574,6 +582,24 @@ int  fa_ext_batch_learned_packed(fa_ctx *ctx, const fa_params *p, const fa_polic
                                  const fa_packed_seq *qseq, const fa_packed_seq *tseq,
                                  const fa_band_hint *hints, fa_ext_result *out, int32_t *w_first_out,
                                  int32_t *w_final, fa_ext_stats *stats);
+
+/* ---- paired-end batch (no reference counterpart) -------------------------
+ * One submission of a paired-end batch's two kinds of work on one context: the seed
+ * extensions of execute_batch_simd_scoring (src/pipelines/linear/batch_extension/
+ * dispatch.rs:31-86) and the mate-rescue ksw_align2 jobs of
+ * execute_mate_rescue_batch_with_engine (src/pipelines/linear/paired/mate_rescue.rs:595-685).
+ * Both job sets go up at once; the mate SW kernels run on the context's mate stream while
+ * the extension rounds -- fa_ext_batch_policy's, or fa_ext_batch_learned's when `model` is
+ * given (pol must then be FA_POLICY_LEARNED) -- run on its main stream, so the GPU's block
+ * scheduler works on both kinds of blocks at once; the call returns when both result sets are
+ * back.  Results are those of the separate calls.  stats / mate_stats (may be NULL) get
+ * each half's statistics and the call's wall time. */
+int fa_pair_batch(fa_ctx *ctx, const fa_params *p, const fa_policy *pol, const fa_band_model *model, float margin,
+                  const fa_job *jobs, uint32_t n, const uint8_t *qseq, uint64_t qseq_len, const uint8_t *tseq,
+                  uint64_t tseq_len, const fa_band_hint *hints, fa_ext_result *out, const fa_mate_params *mp,
+                  const fa_mate_job *mjobs, uint32_t mn, const uint8_t *mqseq, uint64_t mqseq_len,
+                  const uint8_t *mtseq, uint64_t mtseq_len, fa_kswr *mout, fa_ext_stats *stats,
+                  fa_ext_stats *mate_stats);
 
 /* Device-resident variant (no reference counterpart): device pointers, kernels
  * asynchronous on `stream` after one small synchronous read of the batch's job

@@ -53,6 +53,32 @@ def test_i16_lanes_and_random_flags_bit_exact(ctx):
         assert np.array_equal(out, ref), diff_report(out, ref)
 
 
+@pytest.mark.parametrize("qlen", [125, 126])
+def test_short_form_boundary_bit_exact(ctx, qlen):
+    """Match 2 / mismatch -3 (shift 3): 125-base queries keep (qlen + 1) * 2 + 3 <= 255, the
+    batch takes the unsaturated u8 form; 126-base queries do not, and an exact copy of the
+    query in the window scores 252, which saturates (score 255) in the u8 engine."""
+    rng = np.random.default_rng(qlen)
+    qs, ts, jobs = [], [], np.zeros(600, N.MATE_JOB_DT)
+    qo = to = 0
+    for k in range(len(jobs)):
+        q = rng.integers(0, 4, qlen).astype(np.uint8)
+        t = rng.integers(0, 5, 400).astype(np.uint8)
+        if k % 3 == 0:
+            pos = int(rng.integers(0, 400 - qlen))
+            t[pos:pos + qlen] = q
+            if k % 2 == 0:
+                t[pos + qlen // 2] = (q[qlen // 2] + 1) % 4
+        jobs[k] = (qo, to, qlen, len(t), N.KSW_XBYTE | N.KSW_XSTART | N.KSW_XSUBO | 30, 0)
+        qs.append(q); ts.append(t); qo += qlen; to += len(t)
+    qseq, tseq = np.concatenate(qs), np.concatenate(ts)
+    p = fa.make_mate_params(fa.bwa_fill_scmat(2, 3, -1), 6, 1, 6, 1)
+    out, _ = fa.mate_sw_batch(p, jobs, qseq, tseq, ctx=ctx)
+    ref, _ = O.mate_batch(p, jobs, qseq, tseq)
+    assert np.array_equal(out, ref), diff_report(out, ref)
+    assert (ref["score"] == 255).any() == (qlen == 126)
+
+
 def test_reference_style_interface(ctx):
     rng = np.random.default_rng(2)
     jobs = []
