@@ -89,10 +89,8 @@ __global__ void __launch_bounds__(128) band_features_kernel(const fa_job *__rest
     for (int k0 = 0; k0 < qlen; k0 += 16) {
         uint32_t q4[4], nm[4], t7[7];
         if (PK) {
-#pragma unroll
-            for (int m = 0; m < 4; ++m) q4[m] = qr.get4(k0 + 4 * m);
-#pragma unroll
-            for (int m = 0; m < 7; ++m) t7[m] = tr.get4(k0 - 4 + 4 * m);   // target positions k0-4 .. k0+23
+            qr.getw<4>(k0, q4);
+            tr.getw<7>(k0 - 4, t7);   // target positions k0-4 .. k0+23
         } else {
             {
                 const long long a = (long long)jb.q_off + k0, a0 = a & ~3LL;

@@ -87,9 +87,10 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
             // eight query codes from column j0 on (0 past the query)
             auto load8 = [&](int j0, uint32_t *qb) {
                 if (PK) {
-                    const uint32_t lo = qr.get4(j0), hi = qr.get4(j0 + 4);
+                    uint32_t v[2];
+                    qr.getw<2>(j0, v);
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) qb[u] = ((u < 4 ? lo : hi) >> (8 * (u & 3))) & 0xFFu;
+                    for (int u = 0; u < 8; ++u) qb[u] = (v[u / 4] >> (8 * (u & 3))) & 0xFFu;
                 } else {
 #pragma unroll
                     for (int u = 0; u < 8; ++u) qb[u] = j0 + u < qlen ? (uint32_t)Q[j0 + u] : 0u;
@@ -166,9 +167,11 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
             // target bases arrive 5 to 8 rows ahead of their row: tq0 holds the current
             // group of four, tq1 the next, loaded when tq0 is used up
             uint32_t tq0 = 0, tq1 = 0;
+            PackedStream4 tstream;   // PK: target positions 0, 4, 8, ...
             if (PK) {
-                tq0 = tr.get4(0);
-                tq1 = tr.get4(4);
+                tstream.start(0);
+                tq0 = tstream.next4(tr);
+                tq1 = tstream.next4(tr);
             } else {
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
@@ -183,7 +186,7 @@ ext_packed_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ 
                     tq0 = tq1;
                     tq1 = 0;
                     if (PK) {
-                        tq1 = tr.get4(i + 5);
+                        tq1 = tstream.next4(tr);   // positions i + 5 .. i + 8
                     } else {
 #pragma unroll
                         for (int k = 0; k < 4; ++k)

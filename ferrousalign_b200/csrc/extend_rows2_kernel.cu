@@ -153,18 +153,19 @@ __host__ __device__ __forceinline__ uint32_t rows2_thread(
     auto init_h = [&](int c) { return c == 0 ? h0 : (c <= init_reach ? h0 - oe_ins - (c - 1) * e_ins : 0); };
 
     uint32_t bad = 0;
-    for (int j0 = 0; j0 < qlen; j0 += 8) {
-        uint32_t qb[8];
+    for (int j0 = 0; j0 < qlen; j0 += 16) {
+        uint32_t qb[16];
         if (PK) {
-            const uint32_t lo = qr.get4(j0), hi = qr.get4(j0 + 4);
+            uint32_t v[4];
+            qr.getw<4>(j0, v);
 #pragma unroll
-            for (int u = 0; u < 8; ++u) qb[u] = ((u < 4 ? lo : hi) >> (8 * (u & 3))) & 0xFFu;
+            for (int u = 0; u < 16; ++u) qb[u] = (v[u / 4] >> (8 * (u & 3))) & 0xFFu;
         } else {
 #pragma unroll
-            for (int u = 0; u < 8; ++u) qb[u] = j0 + u < qlen ? (uint32_t)Q[j0 + u] : 0u;
+            for (int u = 0; u < 16; ++u) qb[u] = j0 + u < qlen ? (uint32_t)Q[j0 + u] : 0u;
         }
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
+        for (int u = 0; u < 16; ++u) {
             if (j0 + u < qlen) {
                 bad |= qb[u] >= (uint32_t)p.m;
                 sb[(j0 + u) * T] = (uint8_t)(qb[u] < 4u ? qb[u] * 0x11u + 0x80u : qn * 0x11u);
@@ -267,9 +268,11 @@ __host__ __device__ __forceinline__ uint32_t rows2_thread(
     };
     // target bases: tq0 holds the current four rows, tq1 the next four
     uint32_t tq0 = 0, tq1 = 0;
+    PackedStream4 tstream;   // PK: target positions 0, 4, 8, ...
     if (PK) {
-        tq0 = tr.get4(0);
-        tq1 = tr.get4(4);
+        tstream.start(0);
+        tq0 = tstream.next4(tr);
+        tq1 = tstream.next4(tr);
     } else {
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
@@ -285,7 +288,7 @@ __host__ __device__ __forceinline__ uint32_t rows2_thread(
             tq0 = tq1;
             tq1 = 0;
             if (PK) {
-                tq1 = tr.get4(i + 6);
+                tq1 = tstream.next4(tr);   // positions i + 6 .. i + 9
             } else {
 #pragma unroll
                 for (int k = 0; k < 4; ++k)

@@ -94,11 +94,85 @@ struct PackedReader {
         return v;
     }
 
+    // word at a signed index: 0 outside the buffer
+    __host__ __device__ __forceinline__ uint32_t word_s(int64_t i) const {
+        return i >= 0 && (uint64_t)i < nwords ? w[i] : 0u;
+    }
+
+    // codes of positions r .. r + 4*NW - 1 of the job, four per word (same bytes as NW calls
+    // of get4): ceil(NW / 4) + 1 word loads, one funnel shift per 16 bases
+    template <int NW>
+    __host__ __device__ __forceinline__ void getw(int r, uint32_t (&out)[NW]) {
+        constexpr int NA = (NW + 3) / 4;   // aligned 16-base words
+        const int64_t pos = (int64_t)base + r;
+        const int64_t wi = pos >> 4;       // floor, also below zero
+        const uint32_t sh = (uint32_t)(pos & 15) * 2u;
+        uint32_t wv[NA + 1];
+#pragma unroll
+        for (int m = 0; m <= NA; ++m) wv[m] = word_s(wi + m);
+#pragma unroll
+        for (int m = 0; m < NA; ++m) wv[m] = funnel_r(wv[m], wv[m + 1], sh);
+#pragma unroll
+        for (int m = 0; m < NW; ++m) out[m] = spread4((wv[m / 4] >> (8 * (m % 4))) & 0xFFu);
+        const int64_t end = pos + 4 * NW;
+        if (end > 0 && nxt < (uint64_t)end) {   // an N run starts before the end of the span: rare
+            for (uint32_t j = k; j < nr && (int64_t)runs[j].pos < end; ++j) {
+                const int64_t a = (int64_t)runs[j].pos, e = a + (int64_t)runs[j].len;
+#pragma unroll
+                for (int m = 0; m < NW; ++m) {
+                    const int64_t p0 = pos + 4 * m;
+                    const int lo = (int)(a > p0 ? (a - p0 < 4 ? a - p0 : 4) : 0);
+                    const int hi = (int)(e > p0 ? (e - p0 < 4 ? e - p0 : 4) : 0);
+                    if (hi > lo) {
+                        const uint32_t bm = (hi >= 4 ? 0xFFFFFFFFu : (1u << (8 * hi)) - 1u) & ~((1u << (8 * lo)) - 1u);
+                        out[m] = (out[m] & ~bm) | (0x04040404u & bm);
+                    }
+                }
+            }
+            while (k < nr && (int64_t)(runs[k].pos + runs[k].len) + kBack <= pos) ++k;
+            nxt = k < nr ? runs[k].pos : ~0ull;
+        }
+        // zero outside [0, len)
+#pragma unroll
+        for (int m = 0; m < NW; ++m) {
+            const int p0 = r + 4 * m;
+            if (p0 < 0 || p0 + 4 > len) {
+                const int lo = p0 >= 0 ? 0 : (-p0 < 4 ? -p0 : 4);
+                const int hi = len - p0 <= 0 ? 0 : (len - p0 < 4 ? len - p0 : 4);
+                const uint32_t bm = (hi >= 4 ? 0xFFFFFFFFu : (1u << (8 * hi)) - 1u) & ~(lo >= 4 ? 0xFFFFFFFFu : (1u << (8 * lo)) - 1u);
+                out[m] &= bm;
+            }
+        }
+    }
+
     __host__ __device__ __forceinline__ uint32_t get4(int r) {
         if (r >= len || r + 4 <= 0) return 0u;
         // -3 <= r < 0: the bytes of positions r .. -1 are 0, the rest come from position 0 on
         uint32_t v = r < 0 ? raw4(base) << (8u * (uint32_t)(-r)) : raw4(base + (uint64_t)r);
         if (r + 4 > len) v &= 0xFFFFFFFFu >> (8 * (uint32_t)(r + 4 - len));
+        return v;
+    }
+};
+
+// Sequential four-base reads of positions p, p + 4, p + 8, ... through a PackedReader: one
+// 16-base span read per four calls.
+struct PackedStream4 {
+    uint32_t b[4];
+    int left, next;
+
+    __host__ __device__ __forceinline__ void start(int pos) { next = pos; left = 0; }
+
+    __host__ __device__ __forceinline__ uint32_t next4(PackedReader &r) {
+        if (left == 0) {
+            r.getw<4>(next, b);
+            next += 16;
+            left = 4;
+        }
+        const uint32_t v = b[0];
+        b[0] = b[1];
+        b[1] = b[2];
+        b[2] = b[3];
+        --left;
         return v;
     }
 };

@@ -1,6 +1,7 @@
 """Builds the test harnesses that compile extension kernels' thread bodies for the host
 (nvcc, no GPU needed): libpair_host.so (two jobs per thread), librows2_host.so (two
-target rows per thread) and liborder_host.so (the job-ordering bin mapping)."""
+target rows per thread), liborder_host.so (the job-ordering bin mapping) and
+libpacked_host.so (the packed-sequence reader)."""
 import subprocess
 from pathlib import Path
 
@@ -12,6 +13,7 @@ HARNESSES = {
     "rows2": (HERE / "rows2_host.cu",
               [CSRC / "extend_kernel.cu", CSRC / "extend_pair_kernel.cu", CSRC / "extend_rows2_kernel.cu"]),
     "order": (HERE / "order_host.cu", [CSRC / "order_kernel.cu"]),
+    "packed": (HERE / "packed_host.cu", []),
 }
 
 

@@ -360,3 +360,41 @@ def test_rows2_packed_reads_match_oracle(rows2_lib, ring, cert):
     assert got[2] == 0
     if not cert:
         check_rows2(rows2_lib, p, b.jobs, b.qseq, b.tseq, packed=(qp, tp))
+
+
+@pytest.fixture(scope="module")
+def packed_lib(built):
+    import build_host
+    lib = C.CDLL(str(build_host.build("packed")))
+    lib.packed_host_read.restype = C.c_int
+    lib.packed_host_read.argtypes = [C.c_void_p, C.c_uint64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                     C.c_void_p, C.c_void_p]
+    return lib
+
+
+@pytest.mark.parametrize("nw,r0,step", [(4, 0, 16), (7, -4, 16), (4, 8, 16), (2, 0, 8)])
+def test_packed_span_reads_equal_four_base_reads(packed_lib, nw, r0, step):
+    """The packed reader's multi-word spans (the band-feature windows, the query and target
+    streams of the two-row kernel) give the bytes of the four-base reads and of the byte
+    codes: N runs applied (runs at job edges, long and single), zero outside the job."""
+    rng = np.random.default_rng(nw * 100 + r0)
+    codes = rng.integers(0, 4, 60_000).astype(np.uint8)
+    for _ in range(300):
+        a = int(rng.integers(0, len(codes) - 40))
+        codes[a:a + int(rng.integers(1, 40))] = 4
+    codes[:3] = 4
+    codes[-2:] = 4
+    ps = fa.pack(codes)
+    st = ps.struct()
+    for off, ln in [(0, 151), (1, 77), (len(codes) - 151, 151), (len(codes) - 3, 3), (5, 0), (2, 1)] + \
+            [(int(rng.integers(0, len(codes) - 300)), int(rng.integers(1, 300))) for _ in range(200)]:
+        nsteps = max(1, (ln + step - 1) // step + 1)
+        ow = np.zeros(nsteps * nw, np.uint32)
+        o4 = np.zeros(nsteps * nw, np.uint32)
+        assert packed_lib.packed_host_read(st.ctypes.data, off, ln, r0, step, nsteps, nw, ow.ctypes.data,
+                                           o4.ctypes.data) == 0
+        assert np.array_equal(ow, o4), (off, ln)
+        pos = (r0 + np.arange(nsteps)[:, None] * step + np.arange(nw * 4)[None, :]).reshape(-1)
+        ok = (pos >= 0) & (pos < ln)
+        want = np.where(ok, codes[np.clip(off + pos, 0, len(codes) - 1)], 0).astype(np.uint8)
+        assert np.array_equal(ow.view(np.uint8), want), (off, ln)
