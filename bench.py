@@ -50,6 +50,14 @@ EXT_KERNELS = {"int32": ("ext_packed_kernel", (248.106e6 + 11.161e6) / 439_186, 
 UNEVEN_JOBS = 2_000_000
 MATE_CPU_SAMPLE = 20_000
 DPX_OPS_PER_CELL_PAIR = 9   # int16x2 ops per packed cell pair in the roofline model
+# mate SW (u8 engine, unsaturated form): PRMT profile byte, max(hd + s, E, 0), max(., F), the
+# shared gap term, E and F updates -- DPX 16x2 instructions per two cells of a segment
+MATE_DPX_OPS_PER_CELL_PAIR = 6
+# mate SW bytes per job: the algorithmic reads and writes (job record 32 B, query 151 B,
+# window 551 B, result 28 B) and the DRAM traffic of one ncu capture of both kernels on
+# 200,000 jobs of the same workload, per job
+MATE_ALGO_PER_JOB = 32 + 151 + 551 + 28
+MATE_DRAM_PER_JOB = None
 
 
 def log(*a):
@@ -203,8 +211,10 @@ def bench_learned(args, ctx, b, p):
     """Learned band vs plain band on the same 1M batch: the plain bwa-mem2 retry policy at
     w=100 against the learned path (GPU features + MLP first band, exit-bound certificate
     as the judge, one narrow try then the configured band), and the same policy without
-    the network (every job starting at one fixed band); all through the host ABI, rates
-    from the device time of their kernels, outputs compared with the plain path's."""
+    the network (every job starting at one fixed band); all through the host ABI with the
+    whole batch uploaded before its kernels (slice count 1, so each kernel runs over the full
+    batch), rates from the device time of their kernels, outputs compared with the plain
+    path's.  The overlapped end-to-end forms are in the e2e_packed section."""
     import ferrousalign_b200 as fa
     from ferrousalign_b200 import _native as N
     from ferrousalign_b200 import band_model as B
@@ -217,6 +227,7 @@ def bench_learned(args, ctx, b, p):
     wf_fixed = np.full(n, fixed_w, np.int32)
     plain_ms, learned_ms, nonet_ms = [], [], []
     plain = learned = nonet = None
+    ctx.set_slices(1, 1)
     for _ in range(max(3, args.steps // 10)):
         plain, pst, _ = fa.extend_batch(p, b.jobs, b.qseq, b.tseq, policy=bwa, ctx=ctx)
         plain_ms.append(float(pst["kernel_ms"]))
@@ -224,6 +235,7 @@ def bench_learned(args, ctx, b, p):
         learned_ms.append(float(lst["kernel_ms"]))
         nonet, nst, _ = fa.extend_batch(p, b.jobs, b.qseq, b.tseq, policy=nonet_pol, w_first=wf_fixed, ctx=ctx)
         nonet_ms.append(float(nst["kernel_ms"]))
+    ctx.set_slices(-1, -1)
     pm, lm, fm = float(np.median(plain_ms)), float(np.median(learned_ms)), float(np.median(nonet_ms))
     return {"plain": {"policy": "bwa-mem2 w=100 then 200", "value": n / (pm * 1e-3), "unit": "alignments/s",
                       "gcups": float(pst["cells_executed"]) / (pm * 1e-3) / 1e9,
@@ -467,11 +479,27 @@ def bench_mate(args, ctx, lib, dev, stream, flush, skip_cpu=False):
     from oracle import ksw_oracle as O
     chk = np.arange(0, MATE_JOBS, max(1, MATE_JOBS // 2000))
     ref, _ = O.mate_batch(mp, m.jobs[chk], m.qseq, m.tseq)
+    # roofline: the u8 engine's unsaturated form issues MATE_DPX_OPS_PER_CELL_PAIR DPX 16x2
+    # instructions per two cells of a segment update; the peak is the measured DPX issue rate
+    v, pms = ctypes.c_double(), ctypes.c_float()
+    N.check(lib.fa_probe_int_peak(ctx.handle, 0, ctypes.byref(v), ctypes.byref(pms)))
+    peak_gcups = v.value * 2 / MATE_DPX_OPS_PER_CELL_PAIR / 1e9
+    achieved = cells.value / (kms * 1e-3) / 1e9
     res = {"workload": "500k 2x151bp pairs, insert N(400,50), 551 bp window, ksw_align2 u8 + XSTART",
            "value": MATE_JOBS / (ms * 1e-3), "unit": "alignments/s", "ms_per_step": ms,
-           "gcups": cells.value / (kms * 1e-3) / 1e9, "kernel_ms_per_step": kms,
+           "gcups": achieved, "kernel_ms_per_step": kms,
            "cells_per_step": int(cells.value), "bit_exact_sample": bool(np.array_equal(out[chk], ref)),
-           "gpu_launches": launches}
+           "gpu_launches": launches,
+           "roofline": {"bound": "dpx", "achieved": achieved, "peak": peak_gcups, "unit": "Gcell/s",
+                        "frac": achieved / peak_gcups, "kernel": "mate_sw_kernel_u8x2 + mate_rev_kernel_u8x2",
+                        "cells": "ksw_align2's cells (forward pass and every KSW_XSTART pass it runs, those "
+                                 "skipped as unable to reach the score included)",
+                        "traffic": None if MATE_DRAM_PER_JOB is None else MATE_DRAM_PER_JOB * MATE_JOBS,
+                        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per job of both "
+                                          "kernels, scaled",
+                        "algorithmic_bytes": MATE_ALGO_PER_JOB * MATE_JOBS,
+                        "peak_source": f"measured __viaddmax_s16x2_relu rate {v.value / 1e12:.2f} Tops/s x2/"
+                                       f"{MATE_DPX_OPS_PER_CELL_PAIR}"}}
     if not skip_cpu:
         from oracle import simd_baseline as S
         base = {}

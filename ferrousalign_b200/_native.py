@@ -222,7 +222,9 @@ class Context:
                                 "sample_ms": float(cm[i])} for i in range(min(nc.value, 8))]}
 
     def set_slices(self, single_band: int = 0, policy_rounds: int = 0) -> None:
-        """Upload slices of large host batches (2..8; 0 keeps the current value)."""
+        """Upload slices of large host batches (2..8; 1 uploads the whole batch before one run
+        of the kernels; 0 keeps the current value, -1 restores the default: 8, or 2 for the
+        rounds of a packed batch)."""
         check(load().fa_ctx_set_slices(self.handle, single_band, policy_rounds))
 
     def set_graph(self, enable: bool) -> None:

@@ -106,6 +106,7 @@ struct fa_ctx {
     // paired batches: the mate-rescue half's own buffers, stream and events
     DevBuf pm_jobs, pm_order, pm_q, pm_t, pm_out, pm_misc, pm_rev;
     DevBuf mate_rev;   // the mate SW reverse-pass list (launch_mate_sw)
+    uint64_t q_bases = 0, t_bases = 0;   // bases of the host call's sequence buffers (cq / ct)
     cudaStream_t pm_stream = nullptr;
     cudaEvent_t pm_ev0 = nullptr, pm_ev1 = nullptr;
     // pipelined host batches: slice uploads on their own stream, one event per slice; the
@@ -113,7 +114,8 @@ struct fa_ctx {
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t slice_ev[8] = {}, done_ev[8] = {}, jobs_ev = nullptr;
     cudaEvent_t span_ev[8][2] = {};   // sliced rounds: each slice's kernels, start and end
-    int slices_single = 8, slices_rounds = 8;   // upload slices of pipelined / sliced host batches
+    // upload slices of pipelined / sliced host batches (0: chosen per batch, auto_slices)
+    int slices_single = 0, slices_rounds = 0;
     DevBuf chunk_scratch;
     // kernel choice: fixed, or (FA_KERNEL_AUTO) tuned per (query capacity class, band)
     struct Choice { int kernel; int tpb; };
@@ -442,6 +444,8 @@ int read_status(fa_ctx *c, cudaStream_t s) {
     if (st & ST_BLIST) return fail(FA_ERR_CAPACITY, "mate-SW run list overflow");
     if (st & ST_ARG) return fail(FA_ERR_ARG, "a job has h0 <= 0 (h0 < 0 with FA_PARAM_H0_ZERO), qlen <= 0 or tlen < 0");
     if (st & ST_RANGE) return fail(FA_ERR_ARG, "a chain's seed range is malformed");
+    if (st & ST_RUNS)
+        return fail(FA_ERR_ARG, "a packed buffer's N runs are empty, unsorted, overlapping or outside the bases");
     return FA_OK;
 }
 
@@ -580,6 +584,10 @@ int finish_ext(fa_ctx *c, const fa_policy *pol, uint32_t n, cudaStream_t s, fa_e
                int32_t *h_wfinal, uint32_t launches, uint32_t retries, bool retries_from_tries) {
     Misc m = misc_of(c);
     const int mode = pol ? pol->mode : FA_POLICY_SINGLE;
+    // the N runs of packed host buffers are checked on the device, after the rounds (which
+    // read them without faulting whatever they hold): a bad list fails the call
+    for (const auto &[buf, nb] : {std::pair<const SeqBuf *, uint64_t>{&c->cq, c->q_bases}, {&c->ct, c->t_bases}})
+        if (buf->packed && buf->n_runs) FA_CUDA(launch_runs_check(buf->runs, buf->n_runs, nb, m.status, s));
     if (int rc = read_status(c, s)) return rc;
     if (stats) {
         float ms = 0.f;
@@ -756,14 +764,7 @@ int host_packed(const fa_packed_seq *ps, const char *what, HostSeq *out) {
     if (ps->n_bases && !ps->bases) return fail(FA_ERR_ARG, "packed %s buffer has no bases", what);
     if (ps->n_nruns && !ps->n_runs) return fail(FA_ERR_ARG, "packed %s buffer has no run array", what);
     if (ps->n_nruns >= (1ull << 32)) return fail(FA_ERR_CAPACITY, "packed %s buffer: too many N runs", what);
-    uint64_t end = 0;
-    for (uint64_t k = 0; k < ps->n_nruns; ++k) {
-        const fa_nrun &r = ps->n_runs[k];
-        if (r.len == 0 || r.pos < end || r.pos > ps->n_bases || r.len > ps->n_bases - r.pos)
-            return fail(FA_ERR_ARG, "packed %s buffer: N run %llu is empty, unsorted, overlapping or outside "
-                        "the bases", what, (unsigned long long)k);
-        end = r.pos + r.len;
-    }
+    // the runs themselves are checked on the device (finish_ext)
     *out = HostSeq{ps->bases, (ps->n_bases + 3) / 4, ps->n_bases, ps->n_runs, ps->n_nruns, true};
     return FA_OK;
 }
@@ -779,6 +780,8 @@ int ensure_seq_buffers(fa_ctx *c, const HostSeq &q, const HostSeq &t) {
                    (uint32_t)q.n_runs, q.packed ? 1u : 0u};
     c->ct = SeqBuf{c->tseq.as<uint8_t>(), t.nbytes, t.n_runs ? c->truns.as<fa_nrun>() : nullptr,
                    (uint32_t)t.n_runs, t.packed ? 1u : 0u};
+    c->q_bases = q.npos;
+    c->t_bases = t.npos;
     return FA_OK;
 }
 
@@ -883,13 +886,20 @@ bool slices_in_order(const uint32_t *h_info, uint32_t n, int ns) {
     return covered == n;
 }
 
+// Slice counts when the caller set none.  Byte-code batches are upload-bound (the
+// sequences take longer to copy than the rounds to run), so eight slices let the kernels follow
+// the copies closely; packed batches upload a quarter of the bytes, and the per-slice rounds
+// then cost more than the overlap gains past two slices.  A single-band batch runs one kernel
+// per slice and takes eight either way.
+int auto_slices(bool rounds, const HostSeq &hq) { return rounds && hq.packed ? 2 : 8; }
+
 int ext_batch_pipelined(fa_ctx *c, const ExtParams &kp, const fa_job *jobs, uint32_t n, const HostSeq &hq,
                         const HostSeq &ht, fa_ext_result *out, fa_ext_stats *stats) {
     if (int rc = ensure_ext_buffers(c, n, 0, 0)) return rc;
     if (int rc = ensure_seq_buffers(c, hq, ht)) return rc;
     if (int rc = ensure_pipe_streams(c)) return rc;
     cudaStream_t s = c->stream, cs = c->copy_stream;
-    const int ns = c->slices_single;
+    const int ns = c->slices_single ? c->slices_single : auto_slices(false, hq);
     const ChunkEnds ends = graded_ends(hq, ht, ns);
     Misc m = misc_of(c);
     FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
@@ -994,7 +1004,7 @@ int ext_batch_sliced(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, const
         band_model_export(model, wbf, mean, sd);
     }
     cudaStream_t s = c->stream, cs = c->copy_stream;
-    const int ns = c->slices_rounds;
+    const int ns = c->slices_rounds ? c->slices_rounds : auto_slices(true, hq);
     const ChunkEnds ends = graded_ends(hq, ht, ns);
     Misc m = misc_of(c);
     FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
@@ -1149,7 +1159,7 @@ int ext_batch_host(fa_ctx *c, const fa_params *p, const fa_policy *pol, const fa
             stats->total_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
     };
     const int mode = pol ? pol->mode : FA_POLICY_SINGLE;
-    if (mode == FA_POLICY_SINGLE && !c->graph && n >= kPipeMinJobs) {
+    if (mode == FA_POLICY_SINGLE && !c->graph && n >= kPipeMinJobs && c->slices_single != 1) {
         int rc = ext_batch_pipelined(c, kp, jobs, n, hq, ht, out, stats);
         if (rc) return rc;
         if (w_final)
@@ -1157,7 +1167,7 @@ int ext_batch_host(fa_ctx *c, const fa_params *p, const fa_policy *pol, const fa
         total();
         return FA_OK;
     }
-    if (mode != FA_POLICY_SINGLE && !c->graph && n >= kPipeMinJobs) {
+    if (mode != FA_POLICY_SINGLE && !c->graph && n >= kPipeMinJobs && c->slices_rounds != 1) {
         bool done = false;
         int rc = ext_batch_sliced(c, kp, pol, nullptr, 0.f, jobs, n, hq, ht, nullptr, w_first, out, nullptr, w_final,
                                   stats, &done);
@@ -1210,7 +1220,7 @@ int ext_learned_host(fa_ctx *c, const fa_params *p, const fa_policy *pol, const 
         if (stats)
             stats->total_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
     };
-    if (!c->graph && n >= kPipeMinJobs) {
+    if (!c->graph && n >= kPipeMinJobs && c->slices_rounds != 1) {
         bool done = false;
         int rc = ext_batch_sliced(c, kp, pol, model, margin, jobs, n, hq, ht, hints, nullptr, out, w_first_out,
                                   w_final, stats, &done);
@@ -1674,9 +1684,9 @@ int fa_ctx_kernel_choice(fa_ctx *c, int *kernel, int *threads_per_block, int cap
 int fa_ctx_set_slices(fa_ctx *c, int single_band, int policy_rounds) {
     if (!c) return fail(FA_ERR_ARG, "null context");
     for (int v : {single_band, policy_rounds})
-        if (v != 0 && (v < 2 || v > kSlices)) return fail(FA_ERR_ARG, "slice count %d outside 2..%d", v, kSlices);
-    if (single_band) c->slices_single = single_band;
-    if (policy_rounds) c->slices_rounds = policy_rounds;
+        if (v < -1 || v > kSlices) return fail(FA_ERR_ARG, "slice count %d outside 1..%d", v, kSlices);
+    if (single_band) c->slices_single = single_band < 0 ? 0 : single_band;
+    if (policy_rounds) c->slices_rounds = policy_rounds < 0 ? 0 : policy_rounds;
     return FA_OK;
 }
 

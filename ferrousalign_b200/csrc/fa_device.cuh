@@ -15,6 +15,7 @@ enum : uint32_t {
     ST_BLIST    = 1u << 2,   // mate-SW run list overflowed its buffer
     ST_ARG      = 1u << 3,   // a job violates an argument rule (h0 <= 0, qlen <= 0, tlen < 0)
     ST_RANGE    = 1u << 4,   // a chain's seed range is malformed (region merge)
+    ST_RUNS     = 1u << 5,   // a packed buffer's N runs are empty, unsorted, overlapping or past its bases
 };
 
 // Base (0-3) of FM-index position x < 2 l_pac in a 2-bit packed reference (the .pac layout:

@@ -74,6 +74,10 @@ cudaError_t launch_band_partition(const fa_job *d_jobs, const uint32_t *d_list, 
 // dst[atomic positions] = src[0 .. *d_end), *d_end <= n_max (a device-side count)
 cudaError_t launch_list_append(const uint32_t *d_src, const uint32_t *d_end, uint32_t n_max, uint32_t *d_dst,
                                uint32_t *d_dst_count, cudaStream_t stream);
+// ST_RUNS into *d_status when a packed buffer's N runs are not sorted, disjoint, non-empty
+// runs inside its n_bases bases
+cudaError_t launch_runs_check(const fa_nrun *d_runs, uint32_t n, uint64_t n_bases, uint32_t *d_status,
+                              cudaStream_t stream);
 // sums[0..2] = {sum of cells_job, sum of tries (d_tries may be NULL), sum of missed (may be NULL)}
 cudaError_t launch_stats_sum(const uint32_t *d_cells_job, const int32_t *d_tries, const uint8_t *d_missed, uint32_t n,
                              unsigned long long *d_sums, int sm_count, cudaStream_t stream);

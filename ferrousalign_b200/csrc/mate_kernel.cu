@@ -348,7 +348,7 @@ __device__ fa_kswr sw_pass_u8x2(SeqView Q, int qlen, SeqView Tg, int tlen, uint3
                 for (int a = 0; a < SMAX; ++a) {
                     if (a >= off) {
                         const uint32_t hb = H[a];
-                        const uint32_t hn = __vimax3_s16x2(hb, f, f);
+                        const uint32_t hn = __vimax_s16x2_relu(hb, f);
                         changed |= hn ^ hb;
                         H[a] = hn;
                         f = __viaddmax_s16x2_relu(f, neg_eins2, 0u);

@@ -269,6 +269,30 @@ cudaError_t launch_list_append(const uint32_t *d_src, const uint32_t *d_end, uin
     return cudaGetLastError();
 }
 
+// One thread per N run of a packed buffer: ST_RUNS when the run is empty, reaches past the
+// buffer's bases or starts before the previous run's end.
+__global__ void __launch_bounds__(256) runs_check_kernel(const fa_nrun *__restrict__ runs, uint32_t n,
+                                                         uint64_t n_bases, uint32_t *__restrict__ status)
+{
+    const uint32_t k = blockIdx.x * 256 + threadIdx.x;
+    if (k >= n) return;
+    const fa_nrun r = runs[k];
+    bool bad = r.len == 0 || r.pos > n_bases || r.len > n_bases - r.pos;
+    if (k > 0) {
+        const fa_nrun q = runs[k - 1];
+        bad = bad || r.pos < q.pos + q.len;
+    }
+    if (bad) atomicOr(status, ST_RUNS);
+}
+
+cudaError_t launch_runs_check(const fa_nrun *d_runs, uint32_t n, uint64_t n_bases, uint32_t *d_status,
+                              cudaStream_t stream)
+{
+    if (n == 0) return cudaSuccess;
+    runs_check_kernel<<<(n + 255) / 256, 256, 0, stream>>>(d_runs, n, n_bases, d_status);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_policy_init(const fa_job *d_jobs, uint32_t n, const int32_t *d_w_first, int w_min,
                                int learned, PolicyState st, cudaStream_t stream)
 {

@@ -273,8 +273,10 @@ int fa_ctx_set_graph(fa_ctx *ctx, int enable);
 
 /* Upload slices of host batches of 32,768 jobs or more (no reference counterpart): the
  * sequences of a single-band batch, and of a retry-policy or learned batch that runs its rounds
- * slice by slice, go up in this many graded slices (2..8, default 8 for both; 0 keeps a value).
- * Results are identical for every setting; only the overlap of copies and kernels changes. */
+ * slice by slice, go up in this many graded slices (2..8; 1: the whole batch goes up before
+ * one run of the kernels over all of it; 0 keeps a value, -1 restores the default: 8, except 2
+ * for the rounds of a packed batch).  Results are identical for every setting; only the
+ * overlap of copies and kernels changes. */
 int fa_ctx_set_slices(fa_ctx *ctx, int single_band, int policy_rounds);
 
 /* Kernel timing of device-resident calls (no reference counterpart): with timing on,

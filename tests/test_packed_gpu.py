@@ -90,6 +90,31 @@ def test_learned_packed_matches_learned_bytes(big):
     assert int(sp["misses"]) == int(sb["misses"]) and int(sp["cells_executed"]) == int(sb["cells_executed"])
 
 
+@pytest.mark.parametrize("slices", [(2, 3), (5, 8), (1, 1), (-1, -1)])
+def test_slice_counts_give_identical_results(big, slices):
+    """fa_ctx_set_slices changes only how copies and kernels overlap: single-band, retry and
+    learned results and cell counts are the same for every slice count."""
+    b = big
+    p = fa.BandedPairWiseSW().to_struct()
+    qp, tp = fa.pack(b.qseq), fa.pack(b.tseq)
+    model = B.BandModel.load()
+    hints = B.hints_from_info(b.info)
+    bwa = fa.make_policy(N.FA_POLICY_BWA, 2)
+    with fa.Context(0) as ctx:
+        want = [fa.extend_batch_packed(p, b.jobs, qp, tp, ctx=ctx),
+                fa.extend_batch_packed(p, b.jobs, qp, tp, policy=bwa, ctx=ctx),
+                fa.extend_batch_learned_packed(p, b.jobs, qp, tp, model, hints=hints, ctx=ctx)]
+        ctx.set_slices(*slices)
+        got = [fa.extend_batch_packed(p, b.jobs, qp, tp, ctx=ctx),
+               fa.extend_batch_packed(p, b.jobs, qp, tp, policy=bwa, ctx=ctx),
+               fa.extend_batch_learned_packed(p, b.jobs, qp, tp, model, hints=hints, ctx=ctx)]
+        with pytest.raises(N.NativeError):
+            ctx.set_slices(9, 0)
+    for g, w in zip(got, want):
+        assert np.array_equal(g[0], w[0])
+        assert int(g[1]["cells_executed"]) == int(w[1]["cells_executed"])
+
+
 def test_out_of_order_jobs_fall_back(big):
     """Jobs whose sequences are not in job order cannot be sliced: the serial path runs."""
     b = big
