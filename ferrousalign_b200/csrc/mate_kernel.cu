@@ -264,6 +264,8 @@ __device__ fa_kswr sw_pass_u8x2(SeqView Q, int qlen, SeqView Tg, int tlen, uint3
     const uint32_t neg_edel2 = (uint32_t)(uint16_t)(-p.e_del) * 0x10001u;
     const uint32_t neg_oeins2 = (uint32_t)(uint16_t)(-(p.o_ins + p.e_ins)) * 0x10001u;
     const uint32_t neg_eins2 = (uint32_t)(uint16_t)(-p.e_ins) * 0x10001u;
+    const uint32_t eins2 = (uint32_t)(uint16_t)p.e_ins * 0x10001u;
+    const uint32_t neg_pass2 = (uint32_t)(uint16_t)(-(slen * p.e_ins)) * 0x10001u;   // F decay over a pass
     const uint32_t cap255 = 0x00FF00FFu, neg2 = 0x80008000u;
 
     // PRMT selectors of both lanes' query codes per segment (byte 5 of the table pair is
@@ -337,25 +339,39 @@ __device__ fa_kswr sw_pass_u8x2(SeqView Q, int qlen, SeqView Tg, int tlen, uint3
 #pragma unroll
         for (int a = 0; a < SMAX; a += 2)
             mx = a + 1 < SMAX ? __vimax3_s16x2(mx, H[a], H[a + 1]) : __vimax_s16x2_relu(mx, H[a]);
-        // lazy-F: one lane further per pass, stop after a pass that changed nothing.  Every
-        // value is >= 0, so a lane whose incoming F is zero in both halves changes nothing in
-        // this pass (max(H, 0) = H, and F stays 0): it skips the segments.
-        for (int pass = 0; pass < P; ++pass) {
-            f = lane_up_u16x2(f, gmask, l);
-            uint32_t changed = 0;
-            if (f != 0u) {
+        // lazy-F (the reference's loop: F moves one lane further per pass, H = max(H, F) along
+        // the segments while F decays by e_ins, and the loop stops after the first pass that
+        // changes nothing), in closed form.  Within the loop F never reads H, so the value a
+        // lane receives at the start of pass p, g_p, follows from the main loop's final F
+        // alone: g_1 = F of the lane below, g_p = that lane's relu(g_(p-1) - slen * e_ins).
+        // Segment j then sees relu(g_p - j * e_ins).  Pass p changes a lane exactly when g_p
+        // exceeds both every earlier g of that lane and T - 1 = min_j(H_j + j * e_ins), so the
+        // loop runs on one carried value per lane (U = max(T - 1, g_1 .. g_p), G = max of the
+        // g), and H takes max(H_j, relu(G - j * e_ins)) once at the end: the same H.
+        {
+            // T - 1 by the backward recurrence m = min(H_j, m + e_ins)
+            uint32_t u = H[SMAX - 1];
+#pragma unroll
+            for (int a = SMAX - 2; a >= 0; --a)
+                if (a >= off) u = __viaddmin_s16x2(u, eins2, H[a]);
+            uint32_t g = 0, gs = lane_up_u16x2(f, gmask, l);
+            for (int pass = 0; pass < P; ++pass) {
+                const uint32_t un = __vimax_s16x2_relu(u, gs);
+                const uint32_t changed = un ^ u;
+                u = un;
+                g = __vimax_s16x2_relu(g, gs);
+                if (!__any_sync(gmask, changed != 0)) break;
+                gs = lane_up_u16x2(__viaddmax_s16x2_relu(gs, neg_pass2, 0u), gmask, l);
+            }
+            if (g != 0u) {
 #pragma unroll
                 for (int a = 0; a < SMAX; ++a) {
                     if (a >= off) {
-                        const uint32_t hb = H[a];
-                        const uint32_t hn = __vimax_s16x2_relu(hb, f);
-                        changed |= hn ^ hb;
-                        H[a] = hn;
-                        f = __viaddmax_s16x2_relu(f, neg_eins2, 0u);
+                        H[a] = __vimax_s16x2_relu(H[a], g);
+                        g = __viaddmax_s16x2_relu(g, neg_eins2, 0u);
                     }
                 }
             }
-            if (!__any_sync(gmask, changed != 0)) break;
         }
         const uint32_t mx1 = max(mx & 0xffffu, mx >> 16);
         const int imax = (int)__reduce_max_sync(gmask, mx1);
