@@ -25,6 +25,7 @@ namespace fa {
 namespace {
 
 constexpr int kCigarThreads = 64;
+constexpr size_t kCigarSmemMax = 96 * 1024;   // shared row state per block, at most
 constexpr uint8_t TB_M = 0, TB_D = 1, TB_I = 2;   // types.rs:101-103
 constexpr int kMaxTraceSteps = 10000;             // implementation.rs:253
 
@@ -44,16 +45,47 @@ struct CigarCtx {
 
 __device__ __forceinline__ uint32_t cigar_op(uint32_t op, uint32_t len) { return len << 4 | op; }
 
-__global__ void __launch_bounds__(kCigarThreads)
-cigar_kernel(const fa_cigar_job *__restrict__ jobs, const CigarPlan *__restrict__ plan, uint32_t n,
-             const uint8_t *__restrict__ qseq, const uint8_t *__restrict__ tseq, const ExtParams p, int pen_clip3,
-             int2 *__restrict__ eh_all, uint32_t *__restrict__ tb_all, fa_cigar_result *__restrict__ out,
-             uint32_t *__restrict__ cigar, uint8_t *__restrict__ ref_al, uint8_t *__restrict__ qry_al)
+// Row state of one job (H of the previous row's cell and E, per query column 0..qlen): int32
+// pairs in a per-job global scratch, or 16-bit pairs in shared memory (one word per column,
+// the block's jobs interleaved so that each thread's accesses hit its own bank).
+struct EhGlobal {
+    int2 *eh;
+    __device__ __forceinline__ int2 ld(int j) const { return eh[j]; }
+    __device__ __forceinline__ void st(int j, int h, int e) const { eh[j] = make_int2(h, e); }
+};
+struct EhShared {
+    uint32_t *w;   // w[j * stride]
+    int stride;
+    __device__ __forceinline__ int2 ld(int j) const {
+        const uint32_t v = w[j * stride];
+        return make_int2((int)(v & 0xFFFFu), (int)(v >> 16));
+    }
+    __device__ __forceinline__ void st(int j, int h, int e) const { w[j * stride] = (uint32_t)h | (uint32_t)e << 16; }
+};
+
+// One alignment: the banded rows into the row state and the traceback words, then the
+// traceback, clips and result of job k.
+// The scoring matrix rows as PRMT tables: rt[t] holds mat[t][0..3], rt[5 + t] mat[t][4]
+// (one signed byte per query code), for target code t.  Threads 0-4 write them; the caller
+// synchronises before use.
+__device__ __forceinline__ void cigar_row_tables(uint32_t *rt, const ExtParams &p) {
+    if (threadIdx.x < 5) {
+        const int t = threadIdx.x;
+        rt[t] = (uint32_t)(uint8_t)p.mat[t * 5] | (uint32_t)(uint8_t)p.mat[t * 5 + 1] << 8 |
+                (uint32_t)(uint8_t)p.mat[t * 5 + 2] << 16 | (uint32_t)(uint8_t)p.mat[t * 5 + 3] << 24;
+        rt[5 + t] = (uint32_t)(uint8_t)p.mat[t * 5 + 4];
+    }
+}
+
+// rt: the scoring matrix as PRMT tables in shared memory (cigar_row_tables).
+template <class EH>
+__device__ __forceinline__ void cigar_job(uint32_t k, const fa_cigar_job &J, const CigarPlan &P,
+                                          const uint8_t *__restrict__ qseq, const uint8_t *__restrict__ tseq,
+                                          const ExtParams &p, int pen_clip3, const EH eh, const uint32_t *rt,
+                                          uint32_t *__restrict__ tb_all, fa_cigar_result *__restrict__ out,
+                                          uint32_t *__restrict__ cigar, uint8_t *__restrict__ ref_al,
+                                          uint8_t *__restrict__ qry_al)
 {
-    const uint32_t k = blockIdx.x * kCigarThreads + threadIdx.x;
-    if (k >= n) return;
-    const fa_cigar_job J = jobs[k];
-    const CigarPlan P = plan[k];
     fa_cigar_result r;
     r.score = r.qle = r.tle = r.gtle = r.gscore = r.max_off = 0;
     r.n_cigar = r.n_ref = r.n_query = 0;
@@ -65,22 +97,21 @@ cigar_kernel(const fa_cigar_job *__restrict__ jobs, const CigarPlan *__restrict_
     }
     const uint8_t *Q = qseq + J.q_off;
     const uint8_t *T = tseq + J.t_off;
-    int2 *eh = eh_all + P.eh;
     uint32_t *tb = tb_all + P.tb;
     const int oe_del = p.o_del + p.e_del, oe_ins = p.o_ins + p.e_ins;
     // first row (implementation.rs:67-75)
-    eh[0] = make_int2(h0, 0);
+    eh.st(0, h0, 0);
     int hp = h0 > oe_ins ? h0 - oe_ins : 0;
-    eh[1] = make_int2(hp, 0);
+    eh.st(1, hp, 0);
     for (int j = 2; j <= qlen; ++j) {
         hp = hp > p.e_ins ? hp - p.e_ins : 0;
-        eh[j] = make_int2(hp, 0);
+        eh.st(j, hp, 0);
     }
     int max_score = h0, max_i = -1, max_j = -1, max_ie = -1, gscore = -1, max_off = 0;
     int beg = 0, end = qlen, cells = 0;
     for (int i = 0; i < tlen; ++i) {
         const int tbase = T[i] < 4 ? T[i] : 4;
-        const int8_t *row = p.mat + tbase * 5;
+        const uint32_t rlo = rt[tbase], rhi = rt[5 + tbase];   // this row's scores, one byte per query code
         int cb = beg, ce = end;
         if (cb < i - w) cb = i - w;
         if (ce > i + w + 1) ce = i + w + 1;
@@ -103,7 +134,7 @@ cigar_kernel(const fa_cigar_job *__restrict__ jobs, const CigarPlan *__restrict_
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
                 if (j0 + u < ce) {
-                    ev[u] = eh[j0 + u];
+                    ev[u] = eh.ld(j0 + u);
                     qv[u] = Q[j0 + u];
                 }
             }
@@ -113,7 +144,12 @@ cigar_kernel(const fa_cigar_job *__restrict__ jobs, const CigarPlan *__restrict_
                 if (j >= ce) break;
                 int m = ev[u].x;
                 int e = ev[u].y;
-                m += row[qv[u] < 4 ? qv[u] : 4];
+                {
+                    const uint32_t q = qv[u] < 4 ? (uint32_t)qv[u] : 4u;
+                    uint32_t sv;
+                    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(sv) : "r"(rlo), "r"(rhi), "r"(q | (q | 8u) << 4));
+                    m += (int)(int16_t)(sv & 0xFFFFu);   // the byte, sign-extended by the selector
+                }
                 if (m < 0) m = 0;
                 int h;
                 uint32_t code;
@@ -132,7 +168,7 @@ cigar_kernel(const fa_cigar_job *__restrict__ jobs, const CigarPlan *__restrict_
                 t = t > 0 ? t : 0;
                 e -= p.e_del;
                 e = e > t ? e : t;
-                eh[j] = make_int2(h1, e);   // H of the previous row's cell, E for the next row
+                eh.st(j, h1, e);   // H of the previous row's cell, E for the next row
                 t = m - oe_ins;
                 t = t > 0 ? t : 0;
                 f -= p.e_ins;
@@ -142,7 +178,7 @@ cigar_kernel(const fa_cigar_job *__restrict__ jobs, const CigarPlan *__restrict_
         }
         if (widx >= 0) rowtb[widx] = acc;
         if (ce > cb) cells += ce - cb;
-        eh[ce] = make_int2(h1, 0);
+        eh.st(ce, h1, 0);
         if (ce == qlen && gscore < h1) { gscore = h1; max_ie = i; }
         if (m_val == 0) break;
         if (m_val > max_score) {
@@ -160,10 +196,18 @@ cigar_kernel(const fa_cigar_job *__restrict__ jobs, const CigarPlan *__restrict_
             }
         }
         int nb = cb;
-        while (nb < ce && eh[nb].x == 0 && eh[nb].y == 0) ++nb;
+        while (nb < ce) {
+            const int2 v = eh.ld(nb);
+            if (v.x != 0 || v.y != 0) break;
+            ++nb;
+        }
         beg = nb;
         int ne = ce;
-        while (ne >= beg && eh[ne].x == 0 && eh[ne].y == 0) --ne;
+        while (ne >= beg) {
+            const int2 v = eh.ld(ne);
+            if (v.x != 0 || v.y != 0) break;
+            --ne;
+        }
         end = ne + 2 < qlen ? ne + 2 : qlen;
     }
 
@@ -246,6 +290,42 @@ cigar_kernel(const fa_cigar_job *__restrict__ jobs, const CigarPlan *__restrict_
     out[k] = r;
 }
 
+__global__ void __launch_bounds__(kCigarThreads)
+cigar_kernel(const fa_cigar_job *__restrict__ jobs, const CigarPlan *__restrict__ plan, uint32_t n,
+             const uint8_t *__restrict__ qseq, const uint8_t *__restrict__ tseq, const ExtParams p, int pen_clip3,
+             int2 *__restrict__ eh_all, uint32_t *__restrict__ tb_all, fa_cigar_result *__restrict__ out,
+             uint32_t *__restrict__ cigar, uint8_t *__restrict__ ref_al, uint8_t *__restrict__ qry_al)
+{
+    __shared__ uint32_t rt[10];
+    cigar_row_tables(rt, p);
+    __syncthreads();
+    const uint32_t k = blockIdx.x * kCigarThreads + threadIdx.x;
+    if (k >= n) return;
+    const CigarPlan P = plan[k];
+    cigar_job(k, jobs[k], P, qseq, tseq, p, pen_clip3, EhGlobal{eh_all + P.eh}, rt, tb_all, out, cigar, ref_al,
+              qry_al);
+}
+
+// The row state in shared memory as 16-bit pairs (every score of the batch fits: the host
+// checks h0 + qlen * max <= 32767), jobs taken in `order` (similar bands side by side in a
+// warp), (qcap + 1) words per thread.
+__global__ void __launch_bounds__(kCigarThreads)
+cigar_smem_kernel(const fa_cigar_job *__restrict__ jobs, const CigarPlan *__restrict__ plan,
+                  const uint32_t *__restrict__ order, uint32_t n, const uint8_t *__restrict__ qseq,
+                  const uint8_t *__restrict__ tseq, const ExtParams p, int pen_clip3, uint32_t *__restrict__ tb_all,
+                  fa_cigar_result *__restrict__ out, uint32_t *__restrict__ cigar, uint8_t *__restrict__ ref_al,
+                  uint8_t *__restrict__ qry_al)
+{
+    extern __shared__ uint32_t ehs[];   // 16 words of tables, then the row state
+    cigar_row_tables(ehs, p);
+    __syncthreads();
+    const uint32_t t = blockIdx.x * kCigarThreads + threadIdx.x;
+    if (t >= n) return;
+    const uint32_t k = order[t];
+    cigar_job(k, jobs[k], plan[k], qseq, tseq, p, pen_clip3, EhShared{ehs + 16 + threadIdx.x, kCigarThreads}, ehs,
+              tb_all, out, cigar, ref_al, qry_al);
+}
+
 // Packs the jobs' CIGAR words back to back: job k's n_cigar words from its capacity slot
 // to first[k] (one warp per job; a job has a handful of operations).
 __global__ void __launch_bounds__(256)
@@ -278,6 +358,22 @@ cudaError_t launch_cigar(const fa_cigar_job *d_jobs, const CigarPlan *d_plan, ui
         d_jobs, d_plan, n, d_qseq, d_tseq, p, pen_clip3, d_eh, d_tb, d_out, d_cigar, d_ref_al, d_qry_al);
     return cudaGetLastError();
 }
+
+cudaError_t launch_cigar_smem(const fa_cigar_job *d_jobs, const CigarPlan *d_plan, const uint32_t *d_order,
+                              uint32_t n, int qcap, const uint8_t *d_qseq, const uint8_t *d_tseq, const ExtParams &p,
+                              int pen_clip3, uint32_t *d_tb, fa_cigar_result *d_out, uint32_t *d_cigar,
+                              uint8_t *d_ref_al, uint8_t *d_qry_al, cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    const size_t smem = sizeof(uint32_t) * (16 + kCigarThreads * (size_t)(qcap + 1));
+    cudaError_t err = cudaFuncSetAttribute(cigar_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return err;
+    cigar_smem_kernel<<<(n + kCigarThreads - 1) / kCigarThreads, kCigarThreads, smem, s>>>(
+        d_jobs, d_plan, d_order, n, d_qseq, d_tseq, p, pen_clip3, d_tb, d_out, d_cigar, d_ref_al, d_qry_al);
+    return cudaGetLastError();
+}
+
+int cigar_smem_qcap() { return (int)((kCigarSmemMax - 64) / (sizeof(uint32_t) * kCigarThreads)) - 1; }
 
 cudaError_t launch_cigar_pack(const CigarPlan *d_plan, const fa_cigar_result *d_res, const uint64_t *d_first,
                               uint32_t n, const uint32_t *d_cigar, uint32_t *d_packed, cudaStream_t s)

@@ -1969,6 +1969,9 @@ int cigar_launch(fa_ctx *c, const fa_params *p, const fa_cigar_job *jobs, uint32
     // output and scratch offsets per job (the reference would panic on a range past its slices)
     std::vector<CigarPlan> plan(n);
     uint64_t cig = 0, ref = 0, qry = 0, eh = 0, tb = 0;
+    int max_mat = 0, qmax = 0;
+    for (int i = 0; i < 25; ++i) max_mat = std::max<int>(max_mat, p->mat[i]);
+    bool narrow = true;   // every score fits the shared-memory kernel's 16-bit row state
     for (uint32_t k = 0; k < n; ++k) {
         const fa_cigar_job &j = jobs[k];
         if (j.qlen < 0 || j.tlen < 0 || j.w < 0) return fail(FA_ERR_ARG, "cigar job %u: negative length or band", k);
@@ -1984,19 +1987,35 @@ int cigar_launch(fa_ctx *c, const fa_params *p, const fa_cigar_job *jobs, uint32
         qry += (uint64_t)j.qlen;
         eh += (uint64_t)j.qlen + 1;
         tb += (uint64_t)j.tlen * pl.wpr;
+        qmax = std::max(qmax, j.qlen);
+        narrow = narrow && j.h0 >= 0 && (long long)j.h0 + (long long)j.qlen * max_mat <= 32767;
+    }
+    const bool smem = narrow && qmax <= cigar_smem_qcap();
+    // shared-memory kernel: jobs ordered by band, widest first (a counting sort), so that a
+    // warp's jobs run rows of similar length
+    std::vector<uint32_t> order;
+    if (smem) {
+        constexpr int kBins = 1024;
+        std::vector<uint32_t> cnt(kBins + 1, 0);
+        auto bin = [&](uint32_t k) { return kBins - 1 - std::min(jobs[k].w, kBins - 1); };
+        for (uint32_t k = 0; k < n; ++k) ++cnt[bin(k) + 1];
+        for (int b = 0; b < kBins; ++b) cnt[b + 1] += cnt[b];
+        order.resize(n);
+        for (uint32_t k = 0; k < n; ++k) order[cnt[bin(k)]++] = k;
     }
     FA_CUDA(cudaSetDevice(c->device));
     cudaStream_t s = c->stream;
     auto up16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
     const size_t b_jobs = up16(sizeof(fa_cigar_job) * n), b_plan = up16(sizeof(CigarPlan) * n);
-    const size_t b_q = up16(qseq_len + 1), b_t = up16(tseq_len + 1);
-    FA_CUDA(c->cg_in.ensure(b_jobs + b_plan + b_q + b_t));
+    const size_t b_q = up16(qseq_len + 1), b_t = up16(tseq_len + 1), b_ord = up16(4ull * order.size());
+    FA_CUDA(c->cg_in.ensure(b_jobs + b_plan + b_q + b_t + b_ord));
     char *in = c->cg_in.as<char>();
     fa_cigar_job *d_jobs = reinterpret_cast<fa_cigar_job *>(in);
     CigarPlan *d_plan = reinterpret_cast<CigarPlan *>(in + b_jobs);
     uint8_t *d_q = reinterpret_cast<uint8_t *>(in + b_jobs + b_plan);
     uint8_t *d_t = reinterpret_cast<uint8_t *>(in + b_jobs + b_plan + b_q);
-    const size_t b_eh = up16(sizeof(int2) * eh), b_tb = up16(4 * tb);
+    uint32_t *d_order = reinterpret_cast<uint32_t *>(in + b_jobs + b_plan + b_q + b_t);
+    const size_t b_eh = smem ? 0 : up16(sizeof(int2) * eh), b_tb = up16(4 * tb);
     FA_CUDA(c->cg_scratch.ensure(b_eh + b_tb));
     int2 *d_eh = c->cg_scratch.as<int2>();
     uint32_t *d_tb = reinterpret_cast<uint32_t *>(c->cg_scratch.as<char>() + b_eh);
@@ -2014,13 +2033,18 @@ int cigar_launch(fa_ctx *c, const fa_params *p, const fa_cigar_job *jobs, uint32
     r->n_qry = qry;
     FA_CUDA(cudaMemcpyAsync(d_jobs, jobs, sizeof(fa_cigar_job) * n, cudaMemcpyHostToDevice, s));
     FA_CUDA(cudaMemcpyAsync(d_plan, plan.data(), sizeof(CigarPlan) * n, cudaMemcpyHostToDevice, s));
+    if (smem) FA_CUDA(cudaMemcpyAsync(d_order, order.data(), 4ull * n, cudaMemcpyHostToDevice, s));
     if (qseq_len) FA_CUDA(cudaMemcpyAsync(d_q, qseq, qseq_len, cudaMemcpyHostToDevice, s));
     if (tseq_len) FA_CUDA(cudaMemcpyAsync(d_t, tseq, tseq_len, cudaMemcpyHostToDevice, s));
     if (tb) FA_CUDA(cudaMemsetAsync(d_tb, 0, 4 * tb, s));   // unwritten cells read as M, as the reference's
     const ExtParams kp = ext_params_of(p);
     if (c->timing) FA_CUDA(cudaEventRecord(c->kev0, s));
-    FA_CUDA(launch_cigar(d_jobs, d_plan, n, d_q, d_t, kp, p->pen_clip3, d_eh, d_tb, r->out, r->cig, r->ref, r->qry,
-                         s));
+    if (smem)
+        FA_CUDA(launch_cigar_smem(d_jobs, d_plan, d_order, n, qmax, d_q, d_t, kp, p->pen_clip3, d_tb, r->out, r->cig,
+                                  r->ref, r->qry, s));
+    else
+        FA_CUDA(launch_cigar(d_jobs, d_plan, n, d_q, d_t, kp, p->pen_clip3, d_eh, d_tb, r->out, r->cig, r->ref,
+                             r->qry, s));
     if (c->timing) FA_CUDA(cudaEventRecord(c->kev1, s));
     c->last_launches = 1;
     c->last_stream = s;

@@ -61,6 +61,27 @@ def test_uneven_jobs_other_scoring(built):
     check(p, jobs_from(b, rng, bands=(3, 17, 60)), b.qseq, b.tseq)
 
 
+def test_wide_scores_and_long_reads_take_the_int32_row_state(built):
+    """A batch whose scores could pass 16 bits (h0 near 32767), or with a query longer than
+    the shared row state holds, runs the int32 global-memory form: same results."""
+    import ferrousalign_b200 as fa
+    from ferrousalign_b200 import synth
+    rng = np.random.default_rng(4)
+    b = synth.workload_ext_1m(300)
+    p = fa.BandedPairWiseSW().to_struct()
+    j = jobs_from(b, rng, bands=(5, 20))
+    j["h0"][::7] = 32700
+    check(p, j, b.qseq, b.tseq)
+    ub = synth.workload_ext_uneven(200, ref_len=2_000_000)
+    long_q = rng.integers(0, 4, 450).astype(np.uint8)
+    qseq = np.concatenate([ub.qseq, long_q])
+    tseq = np.concatenate([ub.tseq, long_q, rng.integers(0, 4, 40).astype(np.uint8)])
+    j2 = jobs_from(ub, rng, bands=(3, 17))
+    extra = np.zeros(1, j2.dtype)
+    extra[0] = (len(ub.qseq), len(ub.tseq), 450, 490, 30, 0)
+    check(p, np.concatenate([j2, extra]), qseq, tseq)
+
+
 def test_edges_codes_and_empty(built):
     import ferrousalign_b200 as fa
     from ferrousalign_b200 import cigar as G
