@@ -11,11 +11,13 @@
 // query left over, and at the 3' end either a soft clip or an M run to the query end by
 // bwa-mem2's clip rule (gscore <= 0 or gscore <= score - pen_clip3: clip).
 //
-// One thread per alignment.  The traceback codes take two bits per cell in a band of
-// min(2w + 1, qlen) columns per row, kept in HBM per job (about 12 KB for a 151-bp read
-// against a 250-base window at w = 100); cells never written read as M, as the
-// reference's zero-initialised matrix does.  The row state (H, E per column) sits in a
-// per-job HBM scratch that stays in L1/L2 while the row loop runs.
+// One thread per alignment, jobs ordered by band so that a warp's rows have similar
+// lengths.  The row state (H, E per query column) sits in shared memory as 16-bit pairs
+// when every score of the batch fits (otherwise in a per-job int32 global scratch); each
+// row's cells run eight at a time in straight-line code.  The traceback codes take two
+// bits per cell of the row's band [cb, ce) behind a header word naming it (at most
+// min(2w + 1, qlen) columns), kept per job in global memory; cells outside a row's band
+// were never written and read as M, as the reference's zero-initialised matrix does.
 
 #include "fa_device.cuh"
 #include "fa_kernels.h"
@@ -29,17 +31,20 @@ constexpr size_t kCigarSmemMax = 96 * 1024;   // shared row state per block, at 
 constexpr uint8_t TB_M = 0, TB_D = 1, TB_I = 2;   // types.rs:101-103
 constexpr int kMaxTraceSteps = 10000;             // implementation.rs:253
 
+// Traceback codes: row i holds a header word (its first coded column cb, and the count
+// ce - cb) and then two bits per column from cb on; a cell outside [cb, ce) was never
+// written and reads as M, as the reference's zero-initialised matrix does.
 struct CigarCtx {
     const uint32_t *tb;
-    int w, wpr;
+    int wpr;
     __device__ __forceinline__ uint32_t at(int ii, int jj) const {   // tb[ii][jj] of the reference
         if (ii == 0) return jj == 0 ? TB_M : TB_I;
         if (jj == 0) return TB_D;
-        const int i = ii - 1, j = jj - 1;
-        const int lo = i - w > 0 ? i - w : 0;
-        const int k = j - lo;
-        if (k < 0 || k >= wpr * 16) return TB_M;
-        return (tb[(size_t)i * wpr + (k >> 4)] >> ((k & 15) * 2)) & 3u;
+        const uint32_t *row = tb + (size_t)(ii - 1) * (wpr + 1);
+        const uint32_t hdr = row[0];
+        const int k = jj - 1 - (int)(hdr & 0xFFFFu);
+        if (k < 0 || k >= (int)(hdr >> 16)) return TB_M;
+        return (row[1 + (k >> 4)] >> ((k & 15) * 2)) & 3u;
     }
 };
 
@@ -49,11 +54,13 @@ __device__ __forceinline__ uint32_t cigar_op(uint32_t op, uint32_t len) { return
 // pairs in a per-job global scratch, or 16-bit pairs in shared memory (one word per column,
 // the block's jobs interleaved so that each thread's accesses hit its own bank).
 struct EhGlobal {
+    static constexpr bool kNarrow = false;   // scores may pass 16 bits
     int2 *eh;
     __device__ __forceinline__ int2 ld(int j) const { return eh[j]; }
     __device__ __forceinline__ void st(int j, int h, int e) const { eh[j] = make_int2(h, e); }
 };
 struct EhShared {
+    static constexpr bool kNarrow = true;    // every score < 32768
     uint32_t *w;   // w[j * stride]
     int stride;
     __device__ __forceinline__ int2 ld(int j) const {
@@ -121,62 +128,63 @@ __device__ __forceinline__ void cigar_job(uint32_t k, const fa_cigar_job &J, con
             h1 = h0 - (p.o_del + p.e_del * (i + 1));
             if (h1 < 0) h1 = 0;
         }
-        int f = 0, m_val = 0, mj = -1;
-        const int lo = i - w > 0 ? i - w : 0;
-        uint32_t *rowtb = tb + (size_t)i * P.wpr;
+        int f = 0;
+        // row maximum and its first column: packed h << 16 | (0xFFFF - j) for 16-bit scores,
+        // else as a pair
+        int best = 0, m_val = 0, mj = -1;
+        uint32_t *rowtb = tb + (size_t)i * (P.wpr + 1);
+        rowtb[0] = (uint32_t)cb | (uint32_t)(ce > cb ? ce - cb : 0) << 16;   // the columns this row codes
         uint32_t acc = 0;
-        int widx = -1;
         // eight columns a step: their row-state words and query bases are loaded together
         // (each is overwritten only at its own column, so the loads may run ahead)
-        for (int j0 = cb; j0 < ce; j0 += 8) {
+        for (int j0 = cb, st = 0; j0 < ce; j0 += 8, ++st) {
             int2 ev[8];
-            int qv[8];
+            uint32_t qv[8];
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
+                ev[u] = make_int2(0, 0);
+                qv[u] = 0;
                 if (j0 + u < ce) {
                     ev[u] = eh.ld(j0 + u);
                     qv[u] = Q[j0 + u];
                 }
             }
+            uint32_t chunk = 0;
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
                 const int j = j0 + u;
                 if (j >= ce) break;
-                int m = ev[u].x;
-                int e = ev[u].y;
-                {
-                    const uint32_t q = qv[u] < 4 ? (uint32_t)qv[u] : 4u;
-                    uint32_t sv;
-                    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(sv) : "r"(rlo), "r"(rhi), "r"(q | (q | 8u) << 4));
-                    m += (int)(int16_t)(sv & 0xFFFFu);   // the byte, sign-extended by the selector
+                const uint32_t q = min(qv[u], 4u);
+                uint32_t sv;
+                asm("prmt.b32 %0, %1, %2, %3;" : "=r"(sv) : "r"(rlo), "r"(rhi), "r"(q | (q | 8u) << 4));
+                const int m = __viaddmax_s32_relu(ev[u].x, (int)(int16_t)(sv & 0xFFFFu), 0);   // clamped at zero
+                const int e = ev[u].y;
+                const int ef = max(e, f);
+                const int h = max(m, ef);
+                const uint32_t code = m >= ef ? TB_M : (e >= f ? TB_D : TB_I);
+                chunk |= code << (2 * u);
+                if (EH::kNarrow) {
+                    best = max(best, h << 16 | (0xFFFF - j));
+                } else if (m_val < h) {
+                    m_val = h;
+                    mj = j;
                 }
-                if (m < 0) m = 0;
-                int h;
-                uint32_t code;
-                if (m >= e && m >= f) { h = m; code = TB_M; }
-                else if (e >= f) { h = e; code = TB_D; }
-                else { h = f; code = TB_I; }
-                const int kk = j - lo, wi = kk >> 4;
-                if (wi != widx) {
-                    if (widx >= 0) rowtb[widx] = acc;
-                    acc = 0;
-                    widx = wi;
-                }
-                acc |= code << ((kk & 15) * 2);
-                if (m_val < h) { m_val = h; mj = j; }
-                int t = m - oe_del;
-                t = t > 0 ? t : 0;
-                e -= p.e_del;
-                e = e > t ? e : t;
-                eh.st(j, h1, e);   // H of the previous row's cell, E for the next row
-                t = m - oe_ins;
-                t = t > 0 ? t : 0;
-                f -= p.e_ins;
-                f = f > t ? f : t;
+                const int en = __viaddmax_s32_relu(e, -p.e_del, m - oe_del);
+                eh.st(j, h1, en);   // H of the previous row's cell, E for the next row
+                f = __viaddmax_s32_relu(f, -p.e_ins, m - oe_ins);
                 h1 = h;
             }
+            if (st & 1) {
+                rowtb[1 + (st >> 1)] = acc | chunk << 16;
+            } else {
+                acc = chunk;
+                if (j0 + 8 >= ce) rowtb[1 + (st >> 1)] = acc;
+            }
         }
-        if (widx >= 0) rowtb[widx] = acc;
+        if (EH::kNarrow) {
+            m_val = best >> 16;
+            mj = 0xFFFF - (best & 0xFFFF);
+        }
         if (ce > cb) cells += ce - cb;
         eh.st(ce, h1, 0);
         if (ce == qlen && gscore < h1) { gscore = h1; max_ie = i; }
@@ -213,7 +221,7 @@ __device__ __forceinline__ void cigar_job(uint32_t k, const fa_cigar_job &J, con
 
     // traceback from the best cell (implementation.rs:239-321); operations and bases come
     // out last to first and are reversed afterwards.  Slot 0 is kept for a 5' clip.
-    const CigarCtx tbx{tb, w, P.wpr};
+    const CigarCtx tbx{tb, P.wpr};
     uint32_t *ops = cigar + P.cig;
     uint8_t *ra = ref_al + P.ref, *qa = qry_al + P.qry;
     int ci = max_i + 1, cj = max_j + 1, nops = 0, nr = 0, nq = 0;

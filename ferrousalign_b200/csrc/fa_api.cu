@@ -1986,7 +1986,7 @@ int cigar_launch(fa_ctx *c, const fa_params *p, const fa_cigar_job *jobs, uint32
         ref += (uint64_t)j.tlen;
         qry += (uint64_t)j.qlen;
         eh += (uint64_t)j.qlen + 1;
-        tb += (uint64_t)j.tlen * pl.wpr;
+        tb += (uint64_t)j.tlen * (pl.wpr + 1);   // per row: a header word, then the codes
         qmax = std::max(qmax, j.qlen);
         narrow = narrow && j.h0 >= 0 && (long long)j.h0 + (long long)j.qlen * max_mat <= 32767;
     }
@@ -2007,7 +2007,8 @@ int cigar_launch(fa_ctx *c, const fa_params *p, const fa_cigar_job *jobs, uint32
     cudaStream_t s = c->stream;
     auto up16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
     const size_t b_jobs = up16(sizeof(fa_cigar_job) * n), b_plan = up16(sizeof(CigarPlan) * n);
-    const size_t b_q = up16(qseq_len + 1), b_t = up16(tseq_len + 1), b_ord = up16(4ull * order.size());
+    // (the kernel loads a step's eight query bases together, up to seven past a job's end)
+    const size_t b_q = up16(qseq_len + 8), b_t = up16(tseq_len + 1), b_ord = up16(4ull * order.size());
     FA_CUDA(c->cg_in.ensure(b_jobs + b_plan + b_q + b_t + b_ord));
     char *in = c->cg_in.as<char>();
     fa_cigar_job *d_jobs = reinterpret_cast<fa_cigar_job *>(in);
@@ -2036,7 +2037,6 @@ int cigar_launch(fa_ctx *c, const fa_params *p, const fa_cigar_job *jobs, uint32
     if (smem) FA_CUDA(cudaMemcpyAsync(d_order, order.data(), 4ull * n, cudaMemcpyHostToDevice, s));
     if (qseq_len) FA_CUDA(cudaMemcpyAsync(d_q, qseq, qseq_len, cudaMemcpyHostToDevice, s));
     if (tseq_len) FA_CUDA(cudaMemcpyAsync(d_t, tseq, tseq_len, cudaMemcpyHostToDevice, s));
-    if (tb) FA_CUDA(cudaMemsetAsync(d_tb, 0, 4 * tb, s));   // unwritten cells read as M, as the reference's
     const ExtParams kp = ext_params_of(p);
     if (c->timing) FA_CUDA(cudaEventRecord(c->kev0, s));
     if (smem)
