@@ -611,6 +611,19 @@ def bench_collect(args, ctx, lib):
     algo = (len(reads) + 16 * (len(chains) + len(seeds)) + wlen // 4 + 2 * len(reads) + 2 * wlen + 40 * n_jobs
             + 24 * len(got.seed_ext) + 20 * len(chains))
     km = float(np.median(kern))
+    # the packed form: same jobs, qbuf / tbuf packed on the device (a quarter of their bytes back)
+    pwall, pkern = [], []
+    pk = None
+    for it in range(args.warmup + 5):
+        t0 = time.perf_counter()
+        pk = fa.collect_extension_jobs_packed(pac, l_pac, reads, off, chains, seeds, ctx=ctx)
+        t1 = time.perf_counter()
+        N.check(lib.fa_ctx_last_timing(ctx.handle, ctypes.byref(k_ms), ctypes.byref(k_n)))
+        if it >= args.warmup:
+            pwall.append((t1 - t0) * 1e3)
+            pkern.append(k_ms.value)
+    packed_same = bool(np.array_equal(pk.left_jobs, got.left_jobs) and np.array_equal(pk.right_jobs, got.right_jobs)
+                       and np.array_equal(fa.unpack(pk.tbuf)[:1 << 20], got.tbuf[:1 << 20]))
     # the first chains' jobs and seed table against the oracle (job numbers start at 0 there too)
     k = 1500
     o = {f: int(v) for f, v in zip(("a", "o_del", "e_del", "o_ins", "e_ins", "w"), (1, 6, 1, 6, 1, 100))}
@@ -631,7 +644,11 @@ def bench_collect(args, ctx, lib):
             "roofline": {"bound": "hbm", "achieved": algo / (km * 1e-3) / 1e9, "peak": HBM_GBS, "unit": "GB/s",
                          "frac": algo / (km * 1e-3) / 1e9 / HBM_GBS, "algorithmic_bytes": algo,
                          "peak_source": HBM_SOURCE},
-            "bit_exact_sample": bool(same), "sample": f"first {k} chains against the oracle"}
+            "bit_exact_sample": bool(same), "sample": f"first {k} chains against the oracle",
+            "packed": {"e2e_ms": float(np.median(pwall)), "kernel_ms": float(np.median(pkern)),
+                       "d2h_sequence_bytes": int(pk.qbuf.nbytes + pk.tbuf.nbytes),
+                       "byte_form_sequence_bytes": int(len(got.qbuf) + len(got.tbuf)),
+                       "same_jobs_and_bases": packed_same}}
 
 
 def bench_cigar(args, ctx, lib):

@@ -132,6 +132,9 @@ SIGNATURES = {
                                 _P, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64, _P, _P, _P]),
     "fa_collect_ext_jobs": (C.c_int, [_P, _P, _P, C.c_uint64, _P, _P, C.c_uint32, _P, C.c_uint32, _P, C.c_uint32,
                                       _P, _P, _P, _P, C.c_uint64, _P, _P, _P, _P]),
+    "fa_collect_ext_jobs_packed": (C.c_int, [_P, _P, _P, C.c_uint64, _P, _P, C.c_uint32, _P, C.c_uint32, _P,
+                                             C.c_uint32, _P, _P, _P, _P, C.c_uint64, _P, C.c_uint64, _P,
+                                             C.c_uint64, _P, _P, _P, _P, _P]),
     "fa_cigar_batch": (C.c_int, [_P, _P, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64, _P, _P, _P, _P]),
     "fa_cigar_batch_packed": (C.c_int, [_P, _P, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64, _P, _P, C.c_uint64,
                                         _P, _P, _P]),

@@ -90,3 +90,53 @@ def collect_extension_jobs(pac: np.ndarray, l_pac: int, reads: np.ndarray, read_
     c = counts[0]
     return CollectedJobs(left[:c["n_left"]], right[:c["n_right"]], qbuf[:c["qbuf_len"]],
                          tbuf[:c["tbuf_len"]], ext[:c["n_seed_ext"]], first, win)
+
+
+def collect_extension_jobs_packed(pac: np.ndarray, l_pac: int, reads: np.ndarray, read_off: np.ndarray,
+                                  chains: np.ndarray, seeds: np.ndarray, opts: np.ndarray | None = None,
+                                  ctx: N.Context | None = None) -> CollectedJobs:
+    """fa_collect_ext_jobs_packed: the same jobs and seed table, with `qbuf` and `tbuf` as
+    2-bit packed buffers (PackedSeq, N runs listed), packed on the device -- ready for
+    extend_batch_packed."""
+    from .packed import PackedSeq
+    lib = N.load()
+    ctx = ctx or N.default_context()
+    opts = collect_opts() if opts is None else opts
+    pac = np.ascontiguousarray(pac, np.uint8)
+    reads = np.ascontiguousarray(reads, np.uint8)
+    read_off = np.ascontiguousarray(read_off, np.uint64)
+    chains = np.ascontiguousarray(chains, CHAIN_DT)
+    seeds = np.ascontiguousarray(seeds, SEED_DT)
+    n_reads, n_chains, n_seeds = len(read_off) - 1, len(chains), len(seeds)
+    read_bytes = int(read_off[-1]) if len(read_off) else 0
+    left = np.empty(n_seeds, N.JOB_DT)
+    right = np.empty(n_seeds, N.JOB_DT)
+    qb = np.zeros((2 * read_bytes + 3) // 4 + 4, np.uint8)   # 4 bytes of slack, as pack() leaves
+    ext = np.empty(n_seeds, N.SEED_EXT_DT)
+    first = np.zeros(n_chains + 1, np.uint32)
+    win = np.zeros((n_chains, 2), np.uint64)
+    counts = np.zeros(1, N.COLLECT_COUNTS_DT)
+    n_runs = np.zeros(2, np.uint64)
+    qlen = np.diff(read_off.astype(np.int64))
+    w = int(opts["w"][0])
+    cap = int(2 * (qlen[chains["read"]] + 4 * w + 64).sum()) if n_chains else 0
+    qcap, tcap = max(1024, 2 * read_bytes // 64), max(1024, cap // 256)
+    for _ in range(3):
+        tb = np.zeros((cap + 3) // 4 + 4, np.uint8)
+        qr = np.empty(qcap, N.NRUN_DT)
+        tr = np.empty(tcap, N.NRUN_DT)
+        rc = lib.fa_collect_ext_jobs_packed(ctx.handle, N.ptr(opts), N.ptr(pac), l_pac, N.ptr(reads),
+                                            N.ptr(read_off), n_reads, N.ptr(chains), n_chains, N.ptr(seeds),
+                                            n_seeds, N.ptr(left), N.ptr(right), N.ptr(qb), N.ptr(qr), qcap,
+                                            N.ptr(tb), len(tb) - 4, N.ptr(tr), tcap, N.ptr(ext), N.ptr(first),
+                                            N.ptr(win), N.ptr(counts), N.ptr(n_runs))
+        if rc == N.FA_ERR_CAPACITY:
+            cap = max(cap, int(counts["tbuf_len"][0]))
+            qcap, tcap = max(qcap, int(n_runs[0])), max(tcap, int(n_runs[1]))
+            continue
+        N.check(rc)
+        break
+    c = counts[0]
+    qs = PackedSeq(qb, int(c["qbuf_len"]), qr[:int(n_runs[0])].copy())
+    ts = PackedSeq(tb, int(c["tbuf_len"]), tr[:int(n_runs[1])].copy())
+    return CollectedJobs(left[:c["n_left"]], right[:c["n_right"]], qs, ts, ext[:c["n_seed_ext"]], first, win)

@@ -83,6 +83,7 @@ struct fa_ctx {
     DevBuf ovf;   // two-row kernel: jobs handed on to the int32 kernel
     DevBuf reg_in, reg_out;   // region merge of host buffers: inputs, regions
     DevBuf col_in, col_plan, col_out;   // job collection: inputs, chain plans + scan sums, outputs
+    DevBuf col_pk;                      // packed collection outputs: bases, N runs, run-scan scratch
     DevBuf cg_in, cg_scratch, cg_out;   // CIGAR regeneration: inputs, row state + traceback, outputs
     DevBuf mc_in, mc_plan, mc_out;      // mate-rescue jobs: inputs, plans + scan sums, outputs
     DevBuf is_buf;                      // insert-size statistics: pairs, histogram, results
@@ -1485,7 +1486,7 @@ void fa_ctx_destroy(fa_ctx *c) {
     for (DevBuf *b : {&c->jobs, &c->order, &c->qseq, &c->tseq, &c->out, &c->clamped, &c->cells_job,
                       &c->misc, &c->w_first, &c->w_cur, &c->prev, &c->kk, &c->w_final, &c->tries,
                       &c->missed, &c->list_a, &c->list_b, &c->hist, &c->feat, &c->wbf, &c->part_n,
-                      &c->part_w, &c->ovf, &c->reg_in, &c->reg_out, &c->col_in, &c->col_plan, &c->col_out,
+                      &c->part_w, &c->ovf, &c->reg_in, &c->reg_out, &c->col_in, &c->col_plan, &c->col_out, &c->col_pk,
                       &c->cg_in, &c->cg_scratch, &c->cg_out, &c->mc_in, &c->mc_plan, &c->mc_out, &c->is_buf,
                       &c->qruns, &c->truns})
         b->release();
@@ -1849,12 +1850,30 @@ int fa_merge_regions(fa_ctx *c, const fa_region_opts *opt, const uint32_t *chain
     return read_status(c, s);
 }
 
-int fa_collect_ext_jobs(fa_ctx *c, const fa_collect_opts *opt, const uint8_t *pac, uint64_t l_pac,
-                        const uint8_t *reads, const uint64_t *read_off, uint32_t n_reads,
-                        const fa_chain *chains, uint32_t n_chains, const fa_seed *seeds, uint32_t n_seeds,
-                        fa_job *left_jobs, fa_job *right_jobs, uint8_t *qbuf, uint8_t *tbuf, uint64_t tbuf_cap,
-                        fa_seed_ext *seed_ext, uint32_t *chain_first, uint64_t *chain_win,
-                        fa_collect_counts *counts) {
+}  // extern "C"
+
+namespace {
+
+// Device side of one job collection: the outputs on the device and the totals (x: window
+// bytes, y / z: left / right jobs, w: seed-table entries).
+struct CollectDev {
+    fa_job *left = nullptr, *right = nullptr;
+    uint8_t *q = nullptr, *t = nullptr;
+    fa_seed_ext *ext = nullptr;
+    uint32_t *first = nullptr;
+    uint64_t *win = nullptr;
+    ulonglong4 tot{};
+    uint64_t read_bytes = 0;
+};
+
+// Validates, uploads, plans and fills one job collection on the context's stream.  `check`
+// sees the totals (counts already filled) before the fill and may refuse the call (output
+// capacity, null buffers).  d->left == nullptr on return: no chains, nothing launched.
+template <class Check>
+int collect_ext_run(fa_ctx *c, const fa_collect_opts *opt, const uint8_t *pac, uint64_t l_pac, const uint8_t *reads,
+                    const uint64_t *read_off, uint32_t n_reads, const fa_chain *chains, uint32_t n_chains,
+                    const fa_seed *seeds, uint32_t n_seeds, uint32_t *chain_first, uint64_t *chain_win,
+                    fa_collect_counts *counts, Check check, CollectDev *d) {
     if (!c) return fail(FA_ERR_ARG, "null context");
     if (!opt || !counts || !chain_first) return fail(FA_ERR_ARG, "null argument");
     *counts = fa_collect_counts{};
@@ -1918,10 +1937,7 @@ int fa_collect_ext_jobs(fa_ctx *c, const fa_collect_opts *opt, const uint8_t *pa
     counts->n_seed_ext = (uint32_t)tot.w;
     counts->qbuf_len = 2 * read_bytes;
     counts->tbuf_len = tot.x;
-    if (tot.x > tbuf_cap) return fail(FA_ERR_CAPACITY, "tbuf_cap is below the windows' bytes (counts->tbuf_len)");
-    if ((tot.y && !left_jobs) || (tot.z && !right_jobs) || (tot.w && !seed_ext) || (read_bytes && !qbuf) ||
-        (tot.x && !tbuf))
-        return fail(FA_ERR_ARG, "null output buffer");
+    if (int rc = check(tot)) return rc;
     const size_t b_left = up16(sizeof(fa_job) * tot.y), b_right = up16(sizeof(fa_job) * tot.z);
     const size_t b_q = up16(2 * read_bytes + 1), b_t = up16(tot.x + 1), b_ext = up16(sizeof(fa_seed_ext) * tot.w);
     const size_t b_first = up16(4ull * (n_chains + 1)), b_win = up16(16ull * n_chains);
@@ -1936,18 +1952,116 @@ int fa_collect_ext_jobs(fa_ctx *c, const fa_collect_opts *opt, const uint8_t *pa
     uint64_t *d_win = reinterpret_cast<uint64_t *>(o + b_left + b_right + b_q + b_t + b_ext + b_first);
     FA_CUDA(launch_collect_fill(*opt, d_pac, l_pac, d_reads, d_off, n_reads, d_chains, n_chains, d_seeds, d_plan,
                                 d_left, d_right, d_q, d_t, d_ext, d_first, d_win, s));
-    if (c->timing) FA_CUDA(cudaEventRecord(c->kev1, s));
     c->last_launches = 7;
     c->last_stream = s;
-    if (tot.y) FA_CUDA(cudaMemcpyAsync(left_jobs, d_left, sizeof(fa_job) * tot.y, cudaMemcpyDeviceToHost, s));
-    if (tot.z) FA_CUDA(cudaMemcpyAsync(right_jobs, d_right, sizeof(fa_job) * tot.z, cudaMemcpyDeviceToHost, s));
-    if (read_bytes) FA_CUDA(cudaMemcpyAsync(qbuf, d_q, 2 * read_bytes, cudaMemcpyDeviceToHost, s));
-    if (tot.x) FA_CUDA(cudaMemcpyAsync(tbuf, d_t, tot.x, cudaMemcpyDeviceToHost, s));
-    if (tot.w) FA_CUDA(cudaMemcpyAsync(seed_ext, d_ext, sizeof(fa_seed_ext) * tot.w, cudaMemcpyDeviceToHost, s));
-    FA_CUDA(cudaMemcpyAsync(chain_first, d_first, 4ull * n_chains, cudaMemcpyDeviceToHost, s));
-    FA_CUDA(cudaMemcpyAsync(chain_win, d_win, 16ull * n_chains, cudaMemcpyDeviceToHost, s));
-    FA_CUDA(cudaStreamSynchronize(s));
+    *d = CollectDev{d_left, d_right, d_q, d_t, d_ext, d_first, d_win, tot, read_bytes};
+    return FA_OK;
+}
+
+// The host outputs common to both collection entries: jobs, seed table, chain bounds.
+int collect_ext_copy_common(fa_ctx *c, const CollectDev &d, uint32_t n_chains, fa_job *left_jobs,
+                            fa_job *right_jobs, fa_seed_ext *seed_ext, uint32_t *chain_first, uint64_t *chain_win) {
+    cudaStream_t s = c->stream;
+    const ulonglong4 &tot = d.tot;
+    if (tot.y) FA_CUDA(cudaMemcpyAsync(left_jobs, d.left, sizeof(fa_job) * tot.y, cudaMemcpyDeviceToHost, s));
+    if (tot.z) FA_CUDA(cudaMemcpyAsync(right_jobs, d.right, sizeof(fa_job) * tot.z, cudaMemcpyDeviceToHost, s));
+    if (tot.w) FA_CUDA(cudaMemcpyAsync(seed_ext, d.ext, sizeof(fa_seed_ext) * tot.w, cudaMemcpyDeviceToHost, s));
+    FA_CUDA(cudaMemcpyAsync(chain_first, d.first, 4ull * n_chains, cudaMemcpyDeviceToHost, s));
+    FA_CUDA(cudaMemcpyAsync(chain_win, d.win, 16ull * n_chains, cudaMemcpyDeviceToHost, s));
     chain_first[n_chains] = (uint32_t)tot.w;
+    return FA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fa_collect_ext_jobs(fa_ctx *c, const fa_collect_opts *opt, const uint8_t *pac, uint64_t l_pac,
+                        const uint8_t *reads, const uint64_t *read_off, uint32_t n_reads,
+                        const fa_chain *chains, uint32_t n_chains, const fa_seed *seeds, uint32_t n_seeds,
+                        fa_job *left_jobs, fa_job *right_jobs, uint8_t *qbuf, uint8_t *tbuf, uint64_t tbuf_cap,
+                        fa_seed_ext *seed_ext, uint32_t *chain_first, uint64_t *chain_win,
+                        fa_collect_counts *counts) {
+    CollectDev d;
+    auto check = [&](const ulonglong4 &tot) -> int {
+        if (tot.x > tbuf_cap) return fail(FA_ERR_CAPACITY, "tbuf_cap is below the windows' bytes (counts->tbuf_len)");
+        if ((tot.y && !left_jobs) || (tot.z && !right_jobs) || (tot.w && !seed_ext) || (counts->qbuf_len && !qbuf) ||
+            (tot.x && !tbuf))
+            return fail(FA_ERR_ARG, "null output buffer");
+        return FA_OK;
+    };
+    if (int rc = collect_ext_run(c, opt, pac, l_pac, reads, read_off, n_reads, chains, n_chains, seeds, n_seeds,
+                                 chain_first, chain_win, counts, check, &d))
+        return rc;
+    if (!d.left) return FA_OK;
+    cudaStream_t s = c->stream;
+    if (c->timing) FA_CUDA(cudaEventRecord(c->kev1, s));
+    if (d.read_bytes) FA_CUDA(cudaMemcpyAsync(qbuf, d.q, 2 * d.read_bytes, cudaMemcpyDeviceToHost, s));
+    if (d.tot.x) FA_CUDA(cudaMemcpyAsync(tbuf, d.t, d.tot.x, cudaMemcpyDeviceToHost, s));
+    if (int rc = collect_ext_copy_common(c, d, n_chains, left_jobs, right_jobs, seed_ext, chain_first, chain_win))
+        return rc;
+    FA_CUDA(cudaStreamSynchronize(s));
+    return FA_OK;
+}
+
+int fa_collect_ext_jobs_packed(fa_ctx *c, const fa_collect_opts *opt, const uint8_t *pac, uint64_t l_pac,
+                               const uint8_t *reads, const uint64_t *read_off, uint32_t n_reads,
+                               const fa_chain *chains, uint32_t n_chains, const fa_seed *seeds, uint32_t n_seeds,
+                               fa_job *left_jobs, fa_job *right_jobs, uint8_t *qbases, fa_nrun *qruns,
+                               uint64_t qruns_cap, uint8_t *tbases, uint64_t tbases_cap, fa_nrun *truns,
+                               uint64_t truns_cap, fa_seed_ext *seed_ext, uint32_t *chain_first,
+                               uint64_t *chain_win, fa_collect_counts *counts, uint64_t *n_runs) {
+    if (!n_runs) return fail(FA_ERR_ARG, "null argument");
+    n_runs[0] = n_runs[1] = 0;
+    CollectDev d;
+    auto check = [&](const ulonglong4 &tot) -> int {
+        if ((tot.x + 3) / 4 > tbases_cap)
+            return fail(FA_ERR_CAPACITY, "tbases_cap is below the packed windows' bytes ((counts->tbuf_len + 3) / 4)");
+        if ((tot.y && !left_jobs) || (tot.z && !right_jobs) || (tot.w && !seed_ext) || (counts->qbuf_len && !qbases) ||
+            (tot.x && !tbases) || (qruns_cap && !qruns) || (truns_cap && !truns))
+            return fail(FA_ERR_ARG, "null output buffer");
+        return FA_OK;
+    };
+    if (int rc = collect_ext_run(c, opt, pac, l_pac, reads, read_off, n_reads, chains, n_chains, seeds, n_seeds,
+                                 chain_first, chain_win, counts, check, &d))
+        return rc;
+    if (!d.left) return FA_OK;
+    cudaStream_t s = c->stream;
+    // pack both buffers and list their N runs on the device (the run lists hold at most one
+    // run per two bases), then bring back the packed bytes and the runs
+    const uint64_t nq = 2 * d.read_bytes, nt = d.tot.x;
+    auto up16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
+    const uint64_t rq_cap = std::min<uint64_t>(qruns_cap, nq / 2 + 1), rt_cap = std::min<uint64_t>(truns_cap, nt / 2 + 1);
+    const size_t b_pq = up16(4 * ((nq + 15) / 16) + 4), b_pt = up16(4 * ((nt + 15) / 16) + 4);
+    const size_t b_rq = up16(sizeof(fa_nrun) * rq_cap), b_rt = up16(sizeof(fa_nrun) * rt_cap);
+    const size_t wq = pack_runs_scratch_words(nq), wt = pack_runs_scratch_words(nt);
+    FA_CUDA(c->col_pk.ensure(b_pq + b_pt + b_rq + b_rt + 4 * (wq + wt)));
+    char *k = c->col_pk.as<char>();
+    uint8_t *d_pq = reinterpret_cast<uint8_t *>(k), *d_pt = reinterpret_cast<uint8_t *>(k + b_pq);
+    fa_nrun *d_rq = reinterpret_cast<fa_nrun *>(k + b_pq + b_pt);
+    fa_nrun *d_rt = reinterpret_cast<fa_nrun *>(k + b_pq + b_pt + b_rq);
+    uint32_t *d_sq = reinterpret_cast<uint32_t *>(k + b_pq + b_pt + b_rq + b_rt), *d_st = d_sq + wq;
+    FA_CUDA(launch_pack2(d.q, nq, d_pq, s));
+    FA_CUDA(launch_pack2(d.t, nt, d_pt, s));
+    FA_CUDA(launch_nruns(d.q, nq, d_rq, rq_cap, d_sq, s));
+    FA_CUDA(launch_nruns(d.t, nt, d_rt, rt_cap, d_st, s));
+    if (c->timing) FA_CUDA(cudaEventRecord(c->kev1, s));
+    c->last_launches += 8;
+    uint32_t cnt[2];
+    FA_CUDA(cudaMemcpyAsync(&cnt[0], d_sq + wq - 1, 4, cudaMemcpyDeviceToHost, s));
+    FA_CUDA(cudaMemcpyAsync(&cnt[1], d_st + wt - 1, 4, cudaMemcpyDeviceToHost, s));
+    FA_CUDA(cudaStreamSynchronize(s));
+    n_runs[0] = cnt[0];
+    n_runs[1] = cnt[1];
+    if (cnt[0] > qruns_cap || cnt[1] > truns_cap)
+        return fail(FA_ERR_CAPACITY, "an N-run buffer is too small (n_runs holds the counts)");
+    if (nq) FA_CUDA(cudaMemcpyAsync(qbases, d_pq, (nq + 3) / 4, cudaMemcpyDeviceToHost, s));
+    if (nt) FA_CUDA(cudaMemcpyAsync(tbases, d_pt, (nt + 3) / 4, cudaMemcpyDeviceToHost, s));
+    if (cnt[0]) FA_CUDA(cudaMemcpyAsync(qruns, d_rq, sizeof(fa_nrun) * cnt[0], cudaMemcpyDeviceToHost, s));
+    if (cnt[1]) FA_CUDA(cudaMemcpyAsync(truns, d_rt, sizeof(fa_nrun) * cnt[1], cudaMemcpyDeviceToHost, s));
+    if (int rc = collect_ext_copy_common(c, d, n_chains, left_jobs, right_jobs, seed_ext, chain_first, chain_win))
+        return rc;
+    FA_CUDA(cudaStreamSynchronize(s));
     return FA_OK;
 }
 

@@ -84,6 +84,16 @@ cudaError_t launch_stats_sum(const uint32_t *d_cells_job, const int32_t *d_tries
 cudaError_t launch_policy_init(const fa_job *d_jobs, uint32_t n, const int32_t *d_w_first, int w_min,
                                int learned, PolicyState st, cudaStream_t stream);
 
+// Byte codes to 2-bit packed bases (pack_kernel.cu): d_dst gets (n + 3) / 4 bytes, written as
+// whole 32-bit words (room for ceil(n / 16) words); d_src 16-byte aligned and readable up to
+// a multiple of 16 bytes past n.
+cudaError_t launch_pack2(const uint8_t *d_src, uint64_t n, uint8_t *d_dst, cudaStream_t s);
+// The N (code 4) runs of n byte codes, sorted: at most cap written to d_runs; the count at
+// d_scratch[pack_runs_scratch_words(n) - 1] after the launches (d_scratch: that many words).
+cudaError_t launch_nruns(const uint8_t *d_src, uint64_t n, fa_nrun *d_runs, uint64_t cap, uint32_t *d_scratch,
+                         cudaStream_t s);
+size_t pack_runs_scratch_words(uint64_t n);
+
 // Mate-rescue local SW.  `byte_lanes` selects the u8 (16-lane) or i16 (8-lane)
 // emulation of the reference's striped kernels; d_order lists the jobs of that kind.
 // d_rev (2 + n words; needed for u8 jobs, unused for i16 jobs): the list of KSW_XSTART

@@ -413,6 +413,22 @@ int fa_collect_ext_jobs(fa_ctx *ctx, const fa_collect_opts *opt, const uint8_t *
                         fa_seed_ext *seed_ext, uint32_t *chain_first, uint64_t *chain_win,
                         fa_collect_counts *counts);
 
+/* fa_collect_ext_jobs with the query and target buffers 2-bit packed (no reference
+ * counterpart; the fa_packed_seq layout, so the jobs go straight to fa_ext_batch_packed):
+ * qbases gets (counts->qbuf_len + 3) / 4 bytes and tbases (counts->tbuf_len + 3) / 4 bytes
+ * (at most tbases_cap), qruns / truns the sorted N runs of each buffer (at most qruns_cap /
+ * truns_cap; n_runs[0] / n_runs[1] their counts).  The jobs, seed table and chain bounds are
+ * those of fa_collect_ext_jobs.  The packing runs on the device, so a quarter of the bases'
+ * bytes come back.  FA_ERR_CAPACITY with counts (and, for the runs, n_runs) filled when a
+ * buffer is too small; nothing else is written then. */
+int fa_collect_ext_jobs_packed(fa_ctx *ctx, const fa_collect_opts *opt, const uint8_t *pac, uint64_t l_pac,
+                               const uint8_t *reads, const uint64_t *read_off, uint32_t n_reads,
+                               const fa_chain *chains, uint32_t n_chains, const fa_seed *seeds, uint32_t n_seeds,
+                               fa_job *left_jobs, fa_job *right_jobs, uint8_t *qbases, fa_nrun *qruns,
+                               uint64_t qruns_cap, uint8_t *tbases, uint64_t tbases_cap, fa_nrun *truns,
+                               uint64_t truns_cap, fa_seed_ext *seed_ext, uint32_t *chain_first,
+                               uint64_t *chain_win, fa_collect_counts *counts, uint64_t *n_runs);
+
 /* ---- CIGAR regeneration ------------------------------------------------
  * Replaces scalar_banded_swa (src/core/alignment/banded_swa/scalar/implementation.rs:5-440),
  * the banded alignment with traceback that turns a region's bounds back into a CIGAR

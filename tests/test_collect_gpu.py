@@ -108,3 +108,33 @@ def test_argument_checks_and_capacity(built):
     badc["read"][0] = 10**6
     assert call(ch=badc) == N.FA_ERR_ARG
     ctx.close()
+
+
+def test_packed_collection_equals_byte_collection(built):
+    """fa_collect_ext_jobs_packed: the same jobs, seed table and chain windows as the byte
+    form; its packed buffers unpack to the byte form's qbuf / tbuf (reads carrying N runs,
+    at read edges too), and the jobs extend to the same results through the packed entry."""
+    import ferrousalign_b200 as fa
+    from ferrousalign_b200 import collect as K, synth
+    ref, reads, off, chains, seeds = synth.workload_chains(3000, ref_len=2_000_000)
+    reads = reads.copy()
+    rng = np.random.default_rng(11)
+    for r in rng.choice(len(off) - 1, 200, replace=False):
+        a, b = int(off[r]), int(off[r + 1])
+        k = int(rng.integers(a, b))
+        reads[k:min(b, k + int(rng.integers(1, 6)))] = 4
+    reads[int(off[0])] = 4
+    reads[int(off[-1]) - 1] = 4
+    pac, l_pac = K.pack_reference(ref)
+    byt = K.collect_extension_jobs(pac, l_pac, reads, off, chains, seeds)
+    pk = K.collect_extension_jobs_packed(pac, l_pac, reads, off, chains, seeds)
+    for f in ("left_jobs", "right_jobs", "seed_ext", "chain_first", "chain_win"):
+        assert np.array_equal(getattr(pk, f), getattr(byt, f)), f
+    assert np.array_equal(fa.unpack(pk.qbuf), byt.qbuf)
+    assert np.array_equal(fa.unpack(pk.tbuf), byt.tbuf)
+    assert len(pk.qbuf.runs) >= 200
+    assert np.array_equal(pk.qbuf.runs, fa.packed.n_runs_of(byt.qbuf))
+    p = fa.BandedPairWiseSW().to_struct()
+    got, _, _ = fa.extend_batch_packed(p, pk.left_jobs, pk.qbuf, pk.tbuf)
+    want, _, _ = fa.extend_batch(p, byt.left_jobs, byt.qbuf, byt.tbuf)
+    assert np.array_equal(got, want)
