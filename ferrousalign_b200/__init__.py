@@ -11,6 +11,7 @@ from .batch_extension import (BandedPairWiseSW, BatchedExtensionJob, BatchExtens
                               execute_batch_simd_scoring, extend_batch, make_policy)
 from .mate_rescue import (MATE_RESCUE_SCORING_MATRIX, Kswr, MateRescueJob, MateRescueResult,  # noqa: F401
                           execute_mate_rescue_batch_with_engine, make_mate_params, mate_sw_batch,
+                          mate_sw_batch_packed,
                           mate_xtra)
 from .region import chain_seed_table, merge_scores_to_regions, region_opts  # noqa: F401
 from .collect import (CollectedJobs, collect_extension_jobs, collect_extension_jobs_packed,  # noqa: F401

@@ -128,6 +128,7 @@ SIGNATURES = {
     "fa_ext_batch_learned_packed": (C.c_int, [_P, _P, _P, _P, C.c_float, _P, C.c_uint32, _P, _P, _P, _P, _P, _P,
                                               _P]),
     "fa_mate_sw_batch": (C.c_int, [_P, _P, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64, _P, _P]),
+    "fa_mate_sw_batch_packed": (C.c_int, [_P, _P, _P, C.c_uint32, _P, _P, _P, _P]),
     "fa_pair_batch": (C.c_int, [_P, _P, _P, _P, C.c_float, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64, _P, _P,
                                 _P, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64, _P, _P, _P]),
     "fa_collect_ext_jobs": (C.c_int, [_P, _P, _P, C.c_uint64, _P, _P, C.c_uint32, _P, C.c_uint32, _P, C.c_uint32,

@@ -107,6 +107,7 @@ struct fa_ctx {
     // paired batches: the mate-rescue half's own buffers, stream and events
     DevBuf pm_jobs, pm_order, pm_q, pm_t, pm_out, pm_misc, pm_rev;
     DevBuf mate_rev;   // the mate SW reverse-pass list (launch_mate_sw)
+    DevBuf mate_pk;    // packed mate input: bases and N runs before the unpack
     uint64_t q_bases = 0, t_bases = 0;   // bases of the host call's sequence buffers (cq / ct)
     cudaStream_t pm_stream = nullptr;
     cudaEvent_t pm_ev0 = nullptr, pm_ev1 = nullptr;
@@ -1450,6 +1451,54 @@ int ext_batch_device(fa_ctx *c, const fa_params *p, const fa_job *d_jobs, uint32
 
 }  // namespace
 
+// One host mate-SW batch: job checks and plan, the job upload, `upload` for the sequences
+// (byte codes into c->qseq / c->tseq on stream s, after the status word is cleared), the SW
+// kernels, the results and statistics.
+template <class Upload>
+int mate_host_batch(fa_ctx *c, const fa_mate_params *p, const fa_mate_job *jobs, uint32_t n, uint64_t qseq_len,
+                    uint64_t tseq_len, Upload upload, fa_kswr *out, fa_ext_stats *stats,
+                    std::chrono::steady_clock::time_point t0) {
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    if (!p || p->m != 5) return fail(FA_ERR_ARG, "alphabet size must be 5");
+    if (n == 0) return FA_OK;
+    if (!jobs || !out) return fail(FA_ERR_ARG, "null buffer");
+    MateHostPlan pl;
+    if (int rc = plan_mate_host(p, jobs, n, qseq_len, tseq_len, &pl)) return rc;
+    FA_CUDA(cudaSetDevice(c->device));
+    cudaStream_t s = c->stream;
+    FA_CUDA(c->jobs.ensure(sizeof(fa_mate_job) * (size_t)n));
+    FA_CUDA(c->order.ensure(4ull * n));
+    FA_CUDA(c->out.ensure(sizeof(fa_kswr) * (size_t)n));
+    FA_CUDA(c->misc.ensure(kMiscBytes));
+    Misc m = misc_of(c);
+    FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
+    FA_CUDA(cudaMemcpyAsync(c->jobs.p, jobs, sizeof(fa_mate_job) * (size_t)n, cudaMemcpyHostToDevice, s));
+    FA_CUDA(cudaMemcpyAsync(c->order.p, pl.order.data(), 4ull * n, cudaMemcpyHostToDevice, s));
+    if (int rc = upload(s)) return rc;
+    FA_CUDA(cudaEventRecord(c->ev0, s));
+    uint32_t launches = 0;
+    FA_CUDA(c->mate_rev.ensure(4ull * (2 + (size_t)pl.n_byte)));
+    FA_CUDA(launch_mate_plan(pl, c->jobs.as<fa_mate_job>(), c->order.as<uint32_t>(), n, c->qseq.as<uint8_t>(),
+                             c->tseq.as<uint8_t>(), c->out.as<fa_kswr>(), m.cells, m.status,
+                             c->mate_rev.as<uint32_t>(), s, &launches));
+    FA_CUDA(cudaEventRecord(c->ev1, s));
+    if (int rc = read_status(c, s)) return rc;
+    FA_CUDA(cudaMemcpyAsync(out, c->out.p, sizeof(fa_kswr) * (size_t)n, cudaMemcpyDeviceToHost, s));
+    FA_CUDA(cudaStreamSynchronize(s));
+    if (stats) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        unsigned long long cells = 0;
+        FA_CUDA(cudaMemcpy(&cells, m.cells, 8, cudaMemcpyDeviceToHost));
+        stats->cells = stats->cells_executed = cells;
+        stats->kernel_ms = ms;
+        stats->kernel_launches = launches;
+        stats->jobs = n;
+        stats->total_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return FA_OK;
+}
+
 extern "C" {
 
 const char *fa_last_error(void) { return g_err.c_str(); }
@@ -1499,7 +1548,8 @@ void fa_ctx_destroy(fa_ctx *c) {
         if (c->lane_ev[k]) cudaEventDestroy(c->lane_ev[k]);
     }
     if (c->fork_ev1) cudaEventDestroy(c->fork_ev1);
-    for (DevBuf *b : {&c->pm_jobs, &c->pm_order, &c->pm_q, &c->pm_t, &c->pm_out, &c->pm_misc, &c->pm_rev, &c->mate_rev})
+    for (DevBuf *b : {&c->pm_jobs, &c->pm_order, &c->pm_q, &c->pm_t, &c->pm_out, &c->pm_misc, &c->pm_rev,
+                      &c->mate_rev, &c->mate_pk})
         b->release();
     if (c->pm_ev0) cudaEventDestroy(c->pm_ev0);
     if (c->pm_ev1) cudaEventDestroy(c->pm_ev1);
@@ -2438,49 +2488,50 @@ int fa_mate_sw_batch(fa_ctx *c, const fa_mate_params *p, const fa_mate_job *jobs
                      const uint8_t *qseq, uint64_t qseq_len, const uint8_t *tseq, uint64_t tseq_len,
                      fa_kswr *out, fa_ext_stats *stats) {
     auto t0 = std::chrono::steady_clock::now();
-    if (!c) return fail(FA_ERR_ARG, "null context");
-    if (!p || p->m != 5) return fail(FA_ERR_ARG, "alphabet size must be 5");
     if (stats) memset(stats, 0, sizeof(*stats));
-    if (n == 0) return FA_OK;
-    if (!jobs || !out || !qseq || !tseq) return fail(FA_ERR_ARG, "null buffer");
-    MateHostPlan pl;
-    if (int rc = plan_mate_host(p, jobs, n, qseq_len, tseq_len, &pl)) return rc;
-    FA_CUDA(cudaSetDevice(c->device));
-    cudaStream_t s = c->stream;
-    FA_CUDA(c->jobs.ensure(sizeof(fa_mate_job) * (size_t)n));
-    FA_CUDA(c->order.ensure(4ull * n));
-    FA_CUDA(c->qseq.ensure(qseq_len));
-    FA_CUDA(c->tseq.ensure(tseq_len));
-    FA_CUDA(c->out.ensure(sizeof(fa_kswr) * (size_t)n));
-    FA_CUDA(c->misc.ensure(kMiscBytes));
-    Misc m = misc_of(c);
-    FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
-    FA_CUDA(cudaMemcpyAsync(c->jobs.p, jobs, sizeof(fa_mate_job) * (size_t)n, cudaMemcpyHostToDevice, s));
-    FA_CUDA(cudaMemcpyAsync(c->order.p, pl.order.data(), 4ull * n, cudaMemcpyHostToDevice, s));
-    FA_CUDA(cudaMemcpyAsync(c->qseq.p, qseq, qseq_len, cudaMemcpyHostToDevice, s));
-    FA_CUDA(cudaMemcpyAsync(c->tseq.p, tseq, tseq_len, cudaMemcpyHostToDevice, s));
-    FA_CUDA(cudaEventRecord(c->ev0, s));
-    uint32_t launches = 0;
-    FA_CUDA(c->mate_rev.ensure(4ull * (2 + (size_t)pl.n_byte)));
-    FA_CUDA(launch_mate_plan(pl, c->jobs.as<fa_mate_job>(), c->order.as<uint32_t>(), n, c->qseq.as<uint8_t>(),
-                             c->tseq.as<uint8_t>(), c->out.as<fa_kswr>(), m.cells, m.status,
-                             c->mate_rev.as<uint32_t>(), s, &launches));
-    FA_CUDA(cudaEventRecord(c->ev1, s));
-    if (int rc = read_status(c, s)) return rc;
-    FA_CUDA(cudaMemcpyAsync(out, c->out.p, sizeof(fa_kswr) * (size_t)n, cudaMemcpyDeviceToHost, s));
-    FA_CUDA(cudaStreamSynchronize(s));
-    if (stats) {
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-        unsigned long long cells = 0;
-        FA_CUDA(cudaMemcpy(&cells, m.cells, 8, cudaMemcpyDeviceToHost));
-        stats->cells = stats->cells_executed = cells;
-        stats->kernel_ms = ms;
-        stats->kernel_launches = launches;
-        stats->jobs = n;
-        stats->total_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    }
-    return FA_OK;
+    if (n && (!qseq || !tseq)) return fail(FA_ERR_ARG, "null buffer");
+    auto upload = [&](cudaStream_t s) -> int {
+        FA_CUDA(c->qseq.ensure(qseq_len));
+        FA_CUDA(c->tseq.ensure(tseq_len));
+        FA_CUDA(cudaMemcpyAsync(c->qseq.p, qseq, qseq_len, cudaMemcpyHostToDevice, s));
+        FA_CUDA(cudaMemcpyAsync(c->tseq.p, tseq, tseq_len, cudaMemcpyHostToDevice, s));
+        return FA_OK;
+    };
+    return mate_host_batch(c, p, jobs, n, qseq_len, tseq_len, upload, out, stats, t0);
+}
+
+int fa_mate_sw_batch_packed(fa_ctx *c, const fa_mate_params *p, const fa_mate_job *jobs, uint32_t n,
+                            const fa_packed_seq *qseq, const fa_packed_seq *tseq, fa_kswr *out, fa_ext_stats *stats) {
+    auto t0 = std::chrono::steady_clock::now();
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (n == 0) return c ? FA_OK : fail(FA_ERR_ARG, "null context");
+    HostSeq hq, ht;
+    if (int rc = host_packed(qseq, "query", &hq)) return rc;
+    if (int rc = host_packed(tseq, "target", &ht)) return rc;
+    // the packed bases and N runs go up, and the device unpacks them to byte codes for the
+    // SW kernels (which read each base many times, from cache); the runs are checked there
+    auto upload = [&](cudaStream_t s) -> int {
+        auto up16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
+        FA_CUDA(c->qseq.ensure(up16(hq.npos) + 16));
+        FA_CUDA(c->tseq.ensure(up16(ht.npos) + 16));
+        const size_t bq = up16(hq.nbytes) + 16, bt = up16(ht.nbytes) + 16;
+        const size_t brq = up16(sizeof(fa_nrun) * hq.n_runs), brt = up16(sizeof(fa_nrun) * ht.n_runs);
+        FA_CUDA(c->mate_pk.ensure(bq + bt + brq + brt));
+        char *k = c->mate_pk.as<char>();
+        uint8_t *pq = reinterpret_cast<uint8_t *>(k), *pt = reinterpret_cast<uint8_t *>(k + bq);
+        fa_nrun *rq = reinterpret_cast<fa_nrun *>(k + bq + bt), *rt = reinterpret_cast<fa_nrun *>(k + bq + bt + brq);
+        FA_CUDA(cudaMemcpyAsync(pq, hq.p, hq.nbytes, cudaMemcpyHostToDevice, s));
+        FA_CUDA(cudaMemcpyAsync(pt, ht.p, ht.nbytes, cudaMemcpyHostToDevice, s));
+        if (hq.n_runs) FA_CUDA(cudaMemcpyAsync(rq, hq.runs, sizeof(fa_nrun) * hq.n_runs, cudaMemcpyHostToDevice, s));
+        if (ht.n_runs) FA_CUDA(cudaMemcpyAsync(rt, ht.runs, sizeof(fa_nrun) * ht.n_runs, cudaMemcpyHostToDevice, s));
+        Misc m = misc_of(c);
+        FA_CUDA(launch_runs_check(rq, (uint32_t)hq.n_runs, hq.npos, m.status, s));
+        FA_CUDA(launch_runs_check(rt, (uint32_t)ht.n_runs, ht.npos, m.status, s));
+        FA_CUDA(launch_unpack2(pq, hq.npos, rq, (uint32_t)hq.n_runs, c->qseq.as<uint8_t>(), s));
+        FA_CUDA(launch_unpack2(pt, ht.npos, rt, (uint32_t)ht.n_runs, c->tseq.as<uint8_t>(), s));
+        return FA_OK;
+    };
+    return mate_host_batch(c, p, jobs, n, hq.npos, ht.npos, upload, out, stats, t0);
 }
 
 }  // extern "C"

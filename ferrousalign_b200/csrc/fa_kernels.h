@@ -93,6 +93,10 @@ cudaError_t launch_pack2(const uint8_t *d_src, uint64_t n, uint8_t *d_dst, cudaS
 cudaError_t launch_nruns(const uint8_t *d_src, uint64_t n, fa_nrun *d_runs, uint64_t cap, uint32_t *d_scratch,
                          cudaStream_t s);
 size_t pack_runs_scratch_words(uint64_t n);
+// 2-bit packed bases (16-byte readable past (n + 3) / 4, word aligned) to n byte codes with
+// the N runs applied; d_dst 16-byte aligned with room for a multiple of 16 bytes past n.
+cudaError_t launch_unpack2(const uint8_t *d_src, uint64_t n, const fa_nrun *d_runs, uint32_t n_runs, uint8_t *d_dst,
+                           cudaStream_t s);
 
 // Mate-rescue local SW.  `byte_lanes` selects the u8 (16-lane) or i16 (8-lane)
 // emulation of the reference's striped kernels; d_order lists the jobs of that kind.

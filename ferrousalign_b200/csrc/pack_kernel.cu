@@ -9,6 +9,7 @@
 
 #include "fa_device.cuh"
 #include "fa_kernels.h"
+#include "fa_packed.cuh"
 
 namespace fa {
 
@@ -152,7 +153,45 @@ runs_write_kernel(const uint8_t *__restrict__ src, uint64_t n, const uint32_t *_
     }
 }
 
+// 2-bit packed -> byte codes, one thread per 16 bases (one 32-bit load, one 16-byte store)
+__global__ void __launch_bounds__(kPackThreads)
+unpack2_kernel(const uint32_t *__restrict__ src, uint64_t n, uint8_t *__restrict__ dst)
+{
+    const uint64_t w = (uint64_t)blockIdx.x * kPackThreads + threadIdx.x;
+    if (w * 16 >= n) return;
+    const uint32_t x = src[w];
+    uint4 o;
+    o.x = spread4(x & 0xFFu);
+    o.y = spread4((x >> 8) & 0xFFu);
+    o.z = spread4((x >> 16) & 0xFFu);
+    o.w = spread4(x >> 24);
+    *reinterpret_cast<uint4 *>(dst + w * 16) = o;   // the destination is padded to 16 bytes
+}
+
+// one thread per N run: its bases back to code 4
+__global__ void __launch_bounds__(kPackThreads)
+apply_runs_kernel(const fa_nrun *__restrict__ runs, uint32_t nr, uint64_t n, uint8_t *__restrict__ dst)
+{
+    const uint32_t k = blockIdx.x * kPackThreads + threadIdx.x;
+    if (k >= nr) return;
+    const fa_nrun r = runs[k];
+    const uint64_t e = r.pos + r.len < n ? r.pos + r.len : n;
+    for (uint64_t q = r.pos; q < e; ++q) dst[q] = 4;
+}
+
 }  // namespace
+
+cudaError_t launch_unpack2(const uint8_t *d_src, uint64_t n, const fa_nrun *d_runs, uint32_t n_runs, uint8_t *d_dst,
+                           cudaStream_t s)
+{
+    if (n == 0) return cudaSuccess;
+    const uint64_t words = (n + 15) / 16;
+    unpack2_kernel<<<(unsigned)((words + kPackThreads - 1) / kPackThreads), kPackThreads, 0, s>>>(
+        reinterpret_cast<const uint32_t *>(d_src), n, d_dst);
+    if (n_runs)
+        apply_runs_kernel<<<(n_runs + kPackThreads - 1) / kPackThreads, kPackThreads, 0, s>>>(d_runs, n_runs, n, d_dst);
+    return cudaGetLastError();
+}
 
 size_t pack_runs_scratch_words(uint64_t n) { return (n + kRunBlockBytes - 1) / kRunBlockBytes + 1; }
 

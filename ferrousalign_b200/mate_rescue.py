@@ -83,6 +83,20 @@ def mate_sw_batch(params: np.ndarray, jobs: np.ndarray, qseq: np.ndarray, tseq: 
     return out, stats[0]
 
 
+def mate_sw_batch_packed(params: np.ndarray, jobs: np.ndarray, qseq, tseq, ctx: N.Context | None = None):
+    """fa_mate_sw_batch_packed on PackedSeq buffers (packed.pack).  Returns (kswr records,
+    stats), those of mate_sw_batch on the same bases."""
+    lib = N.load()
+    ctx = ctx or N.default_context()
+    jobs = np.ascontiguousarray(jobs, dtype=N.MATE_JOB_DT)
+    out = np.zeros(len(jobs), dtype=N.KSWR_DT)
+    stats = np.zeros(1, dtype=N.STATS_DT)
+    qs, ts = qseq.struct(), tseq.struct()
+    N.check(lib.fa_mate_sw_batch_packed(ctx.handle, N.ptr(params), N.ptr(jobs), len(jobs), N.ptr(qs), N.ptr(ts),
+                                        N.ptr(out), N.ptr(stats)))
+    return out, stats[0]
+
+
 def execute_mate_rescue_batch_with_engine(jobs: list[MateRescueJob], engine=None) -> list[MateRescueResult]:
     """mate_rescue.rs:595-637.  ``engine`` is accepted for signature compatibility."""
     if not jobs:

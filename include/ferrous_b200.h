@@ -480,6 +480,14 @@ int fa_mate_sw_batch(fa_ctx *ctx, const fa_mate_params *p, const fa_mate_job *jo
                      const uint8_t *tseq, uint64_t tseq_len,
                      fa_kswr *out, fa_ext_stats *stats);
 
+/* fa_mate_sw_batch on 2-bit packed host buffers (fa_packed_seq; no reference counterpart):
+ * jobs address bases by position.  A quarter of the sequence bytes go up; the device
+ * unpacks them (N runs applied) before the SW kernels, so the results and statistics are
+ * fa_mate_sw_batch's on the same bases.  Bad N run lists fail the call with FA_ERR_ARG. */
+int fa_mate_sw_batch_packed(fa_ctx *ctx, const fa_mate_params *p, const fa_mate_job *jobs, uint32_t n,
+                            const fa_packed_seq *qseq, const fa_packed_seq *tseq, fa_kswr *out,
+                            fa_ext_stats *stats);
+
 /* Mate-rescue jobs (collect_rescue_jobs_for_read_soa, mate_rescue.rs:1804-2045): per rescue
  * candidate -- a read whose mate (the anchor) aligned -- nothing unless its primary
  * alignment scores at least best - pen_unpaired; then the orientations not yet failed

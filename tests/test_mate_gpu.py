@@ -120,3 +120,24 @@ def test_device_entry_point_matches_host_entry_point(ctx):
     out = d_out.cpu().numpy().view(N.KSWR_DT).reshape(-1)
     assert np.array_equal(out, ref), diff_report(out, ref)
     assert cells.value == st["cells"]
+
+
+def test_packed_input_equals_byte_input(ctx):
+    """fa_mate_sw_batch_packed: the same records and cells as the byte form on the same
+    bases (a reference with N runs, so reads and windows carry them); a bad run list fails."""
+    ref_seq = synth.reference(3_000_000, seed=21, n_rate=0.01)
+    b = synth.mate_jobs(ref_seq, 6000, seed=22, read_len=151, insert_sd=50.0, sub_rate=0.02, indel_rate=0.005)
+    p = fa.make_mate_params()
+    qp, tp = fa.pack(b.qseq), fa.pack(b.tseq)
+    assert len(tp.runs) > 10
+    got, st = fa.mate_sw_batch_packed(p, b.jobs, qp, tp, ctx=ctx)
+    want, sw = fa.mate_sw_batch(p, b.jobs, b.qseq, b.tseq, ctx=ctx)
+    assert np.array_equal(got, want), diff_report(got, want)
+    assert int(st["cells"]) == int(sw["cells"])
+    r = tp.runs.copy()
+    r[[0, 1]] = r[[1, 0]]
+    with pytest.raises(N.NativeError) as e:
+        fa.mate_sw_batch_packed(p, b.jobs, qp, fa.PackedSeq(tp.bases, tp.n_bases, r), ctx=ctx)
+    assert e.value.code == N.FA_ERR_ARG
+    again, _ = fa.mate_sw_batch_packed(p, b.jobs[:100], qp, tp, ctx=ctx)
+    assert np.array_equal(again, want[:100])
