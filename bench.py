@@ -500,6 +500,25 @@ def bench_mate(args, ctx, lib, dev, stream, flush, skip_cpu=False):
                         "algorithmic_bytes": MATE_ALGO_PER_JOB * MATE_JOBS,
                         "peak_source": f"measured __viaddmax_s16x2_relu rate {v.value / 1e12:.2f} Tops/s x2/"
                                        f"{MATE_DPX_OPS_PER_CELL_PAIR}"}}
+    # end to end through the host entries, pinned buffers, copies in the timed call: byte codes
+    # and 2-bit packed bases
+    mj, mq, mt = pin_array(m.jobs), pin_array(m.qseq), pin_array(m.tseq)
+    qp, tp = fa.pack(m.qseq).pinned(), fa.pack(m.tseq).pinned()
+    forms = {"bytes": (lambda: fa.mate_sw_batch(mp, mj, mq, mt, ctx=ctx), int(mj.nbytes + mq.nbytes + mt.nbytes)),
+             "packed": (lambda: fa.mate_sw_batch_packed(mp, mj, qp, tp, ctx=ctx),
+                        int(mj.nbytes + qp.nbytes + tp.nbytes))}
+    e2e = {}
+    for name, (fn, h2d) in forms.items():
+        fn()
+        wall = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            o, _ = fn()
+            wall.append((time.perf_counter() - t0) * 1e3)
+        e2e[name] = {"value": MATE_JOBS / (float(np.median(wall)) * 1e-3), "unit": "alignments/s",
+                     "ms_per_step": float(np.median(wall)), "h2d_bytes_per_step": h2d,
+                     "d2h_bytes_per_step": MATE_JOBS * 28, "identical": bool(np.array_equal(o[chk], ref))}
+    res["e2e"] = e2e
     if not skip_cpu:
         from oracle import simd_baseline as S
         base = {}
