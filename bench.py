@@ -57,7 +57,7 @@ MATE_DPX_OPS_PER_CELL_PAIR = 6
 # window 551 B, result 28 B) and the DRAM traffic of one ncu capture of both kernels on
 # 200,000 jobs of the same workload, per job
 MATE_ALGO_PER_JOB = 32 + 151 + 551 + 28
-MATE_DRAM_PER_JOB = None
+MATE_DRAM_PER_JOB = (6.405e6 + 148.886e6 + 3.509e6 + 100.364e6 + 7.430e6) / 200_000
 
 
 def log(*a):
