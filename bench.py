@@ -324,9 +324,10 @@ def bench_e2e_forms(args, ctx, b, p):
 def bench_uneven(args, ctx, p):
     """Uneven-length batch: 2,000,000 mixed left and right extensions, reads 50-300 bp,
     seeds anywhere in the read, targets from a 100 Mbp reference with 5% low-complexity
-    repeats.  Plain bwa-mem2 policy against the learned path (the 151-bp model; results
-    stay exact whatever it predicts), both through the host ABI, device time of their
-    kernels; outputs compared."""
+    repeats.  Plain bwa-mem2 policy against the learned path (the model trained on this
+    shape, band_model_uneven.bin, when present, else the 151-bp model; results stay exact
+    whatever it predicts), both through the host ABI with whole-batch kernels (slice count
+    1), device time of their kernels; outputs compared."""
     import ferrousalign_b200 as fa
     from ferrousalign_b200 import _native as N
     from ferrousalign_b200 import band_model as B
@@ -336,14 +337,17 @@ def bench_uneven(args, ctx, p):
     log(f"uneven workload: {UNEVEN_JOBS} jobs in {time.time() - t0:.1f}s")
     n = len(u.jobs)
     bwa = fa.make_policy(N.FA_POLICY_BWA, 2)
-    model = B.BandModel.load()
+    model_path = B.UNEVEN_MODEL if B.UNEVEN_MODEL.exists() else B.DEFAULT_MODEL
+    model = B.BandModel.load(model_path)
     hints = B.hints_from_info(u.info)
     pm, lm = [], []
+    ctx.set_slices(1, 1)
     for _ in range(max(2, args.steps // 10)):
         plain, pst, _ = fa.extend_batch(p, u.jobs, u.qseq, u.tseq, policy=bwa, ctx=ctx)
         pm.append(float(pst["kernel_ms"]))
         learned, lst, wf, _ = B.extend_batch_learned(p, u.jobs, u.qseq, u.tseq, model, hints=hints, ctx=ctx)
         lm.append(float(lst["kernel_ms"]))
+    ctx.set_slices(-1, -1)
     pms, lms = float(np.median(pm)), float(np.median(lm))
     # the same two calls with the whole extend / check / retry loop recorded as one CUDA graph
     # per context (replayed after the first call of the shape)
@@ -364,7 +368,7 @@ def bench_uneven(args, ctx, p):
     gpms, glms = float(np.median(gpm)), float(np.median(glm))
     ql = u.jobs["qlen"]
     return {"workload": f"{n} mixed left/right extensions, reads 50-300 bp, 100 Mbp reference with 5% repeats",
-            "qlen_mean": float(ql.mean()), "qlen_max": int(ql.max()),
+            "qlen_mean": float(ql.mean()), "qlen_max": int(ql.max()), "model": model_path.name,
             "plain": {"value": n / (pms * 1e-3), "unit": "alignments/s", "kernel_ms": pms,
                       "gcups": float(pst["cells_executed"]) / (pms * 1e-3) / 1e9},
             "learned": {"value": n / (lms * 1e-3), "unit": "alignments/s", "kernel_ms": lms,

@@ -18,6 +18,8 @@ from . import _native as N
 LADDER_STARTS = (2, 3)          # doubling ladders 2,4,8,..,64 and 3,6,12,..,96
 HINT_DT = np.dtype([("diag_spread", "<i4"), ("has_partner", "<i4")])
 DEFAULT_MODEL = Path(__file__).resolve().parent / "band_model_151bp.bin"
+# trained on mixed left/right extensions of 50-300 bp reads (train_band_model --shape uneven)
+UNEVEN_MODEL = Path(__file__).resolve().parent / "band_model_uneven.bin"
 # exact: a narrow run is accepted only with a proof that it equals the configured band's
 JUDGE_EXACT = N.FA_JUDGE_CERT | N.FA_JUDGE_BOUND
 # the learned path's default: exact judge, one narrow try, then the configured band.  With

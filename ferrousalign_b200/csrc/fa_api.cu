@@ -88,6 +88,7 @@ struct fa_ctx {
     DevBuf mc_in, mc_plan, mc_out;      // mate-rescue jobs: inputs, plans + scan sums, outputs
     DevBuf is_buf;                      // insert-size statistics: pairs, histogram, results
     DevBuf w_first, w_cur, prev, kk, w_final, tries, missed, list_a, list_b, hist, feat, wbf, part_n, part_w;
+    DevBuf part_blk[2];   // band partition scratch (per-block bucket offsets), one per lane
     DevBuf qruns, truns;                // N runs of packed host batches
     // the sequences of the current host call on the device (byte codes or packed bases)
     SeqBuf cq{}, ct{};
@@ -149,19 +150,17 @@ constexpr size_t kStatsOff = 232;   // 3 x u64, after the band-group bounds at [
 struct Misc {
     uint32_t *status;
     unsigned long long *cells;
-    uint32_t *cnt_a, *cnt_b, *ovf_n, *bucket_hist, *bucket_cursor, *group_bounds;
+    uint32_t *cnt_a, *cnt_b, *ovf_n, *bucket_hist, *group_bounds;
     uint32_t *work;   // persistent two-row launches' job counters, one per overflow slot
 };
 Misc misc_at(char *b, char *shared) {
     return Misc{(uint32_t *)shared, (unsigned long long *)(shared + 8), (uint32_t *)(b + 16), (uint32_t *)(b + 20),
-                (uint32_t *)(b + 24), (uint32_t *)(b + 64), (uint32_t *)(b + 128), (uint32_t *)(b + 192),
-                (uint32_t *)(b + 40)};
+                (uint32_t *)(b + 24), (uint32_t *)(b + 64), (uint32_t *)(b + 192), (uint32_t *)(b + 40)};
 }
 Misc misc_of(fa_ctx *c) {
     char *b = c->misc.as<char>();
     return Misc{(uint32_t *)b, (unsigned long long *)(b + 8), (uint32_t *)(b + 16), (uint32_t *)(b + 20),
-                (uint32_t *)(b + 24), (uint32_t *)(b + 64), (uint32_t *)(b + 128), (uint32_t *)(b + 192),
-                (uint32_t *)(b + 40)};
+                (uint32_t *)(b + 24), (uint32_t *)(b + 64), (uint32_t *)(b + 192), (uint32_t *)(b + 40)};
 }
 
 // The second lane of sliced host batches: its misc block shares the status word and the
@@ -434,6 +433,7 @@ int ensure_policy_buffers(fa_ctx *c, uint32_t n) {
     FA_CUDA(c->list_b.ensure(b));
     FA_CUDA(c->part_n.ensure(b));
     FA_CUDA(c->part_w.ensure(b));
+    for (DevBuf &pb : c->part_blk) FA_CUDA(pb.ensure(sizeof(uint32_t) * band_partition_scratch_words(n)));
     return FA_OK;
 }
 
@@ -544,7 +544,7 @@ int enqueue_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n
             // band buckets (configured band first, then narrow bands decreasing), then the
             // three band groups concurrently
             FA_CUDA(launch_band_partition(d_jobs, list, cnt, n, st.w_cur, c->part_n.as<uint32_t>(),
-                                          m.bucket_hist, m.bucket_cursor, m.group_bounds, s));
+                                          m.bucket_hist, c->part_blk[0].as<uint32_t>(), m.group_bounds, s));
             if (c->kernel == FA_KERNEL_INT16X2) {
                 FA_CUDA(launch_ext(c, kc, d_jobs, c->part_n.as<uint32_t>(), n, cnt, d_q, d_t, kp, qcap_all,
                                    st.w_cur, d_out, d_flags, cert_r, c->cells_job.as<uint32_t>(), m.cells,
@@ -1089,7 +1089,7 @@ int ext_batch_sliced(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, const
             // policy state: the configured band goes straight to the bwa-mem2 rule either way)
             uint32_t *part = c->part_n.as<uint32_t>() + b;
             FA_CUDA(launch_band_partition(d_jobs, list, nullptr, cnt, st.w_cur, part, ml.bucket_hist,
-                                          ml.bucket_cursor, ml.group_bounds, ls));
+                                          c->part_blk[lane].as<uint32_t>(), ml.group_bounds, ls));
             if (int rc = launch_learned_round(c, d_jobs, part, cnt, c->cq, c->ct, kp, max_q, st.w_cur,
                                               c->out.as<fa_ext_result>(), d_flags, cert, ml, ls, &launches, lane,
                                               (size_t)lane * 3 * max_cnt, true))
@@ -1535,7 +1535,7 @@ void fa_ctx_destroy(fa_ctx *c) {
     for (DevBuf *b : {&c->jobs, &c->order, &c->qseq, &c->tseq, &c->out, &c->clamped, &c->cells_job,
                       &c->misc, &c->w_first, &c->w_cur, &c->prev, &c->kk, &c->w_final, &c->tries,
                       &c->missed, &c->list_a, &c->list_b, &c->hist, &c->feat, &c->wbf, &c->part_n,
-                      &c->part_w, &c->ovf, &c->reg_in, &c->reg_out, &c->col_in, &c->col_plan, &c->col_out, &c->col_pk,
+                      &c->part_w, &c->ovf, &c->reg_in, &c->reg_out, &c->col_in, &c->col_plan, &c->col_out, &c->col_pk, &c->part_blk[0], &c->part_blk[1],
                       &c->cg_in, &c->cg_scratch, &c->cg_out, &c->mc_in, &c->mc_plan, &c->mc_out, &c->is_buf,
                       &c->qruns, &c->truns})
         b->release();

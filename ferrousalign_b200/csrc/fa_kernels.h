@@ -68,9 +68,13 @@ cudaError_t launch_policy_step(const fa_job *d_jobs, const uint32_t *d_list, con
                                const uint32_t *d_count, uint32_t n_max, const fa_ext_result *d_out,
                                const uint8_t *d_clamped, PolicyState st, int max_tries, int judge,
                                uint32_t *d_next, uint32_t *d_next_count, cudaStream_t stream);
+// The list reordered into band buckets (the input order kept inside a bucket): d_base gets
+// the kBandBuckets bucket starts, d_bounds (may be null) the band-group bounds; d_blk is
+// scratch of band_partition_scratch_words(n_max) words.
 cudaError_t launch_band_partition(const fa_job *d_jobs, const uint32_t *d_list, const uint32_t *d_count,
-                                  uint32_t n_max, const int32_t *d_w_cur, uint32_t *d_out, uint32_t *d_hist,
-                                  uint32_t *d_cursor, uint32_t *d_bounds, cudaStream_t stream);
+                                  uint32_t n_max, const int32_t *d_w_cur, uint32_t *d_out, uint32_t *d_base,
+                                  uint32_t *d_blk, uint32_t *d_bounds, cudaStream_t stream);
+size_t band_partition_scratch_words(uint32_t n_max);
 // dst[atomic positions] = src[0 .. *d_end), *d_end <= n_max (a device-side count)
 cudaError_t launch_list_append(const uint32_t *d_src, const uint32_t *d_end, uint32_t n_max, uint32_t *d_dst,
                                uint32_t *d_dst_count, cudaStream_t stream);

@@ -127,8 +127,10 @@ __global__ void policy_step_kernel(const fa_job *__restrict__ jobs, const uint32
 // Reorders a round's job list into band buckets so that every warp holds jobs of one
 // band (a warp runs as long as its widest job): jobs at their configured band first,
 // then narrow jobs by decreasing band, so the longest jobs start first and balance the
-// end of the launch.  Order inside a bucket follows the input list in runs of up to one
-// warp.  Two passes: a histogram of the buckets, then a scatter behind their prefix.
+// end of the launch.  Order inside a bucket is the input list's (the longest-first order
+// of the first round), so a warp's jobs also have similar lengths.  Three passes: per-block
+// bucket counts, one block scanning them per bucket, then each job written at its bucket's
+// base + its block's offset + its rank among the block's jobs of that bucket.
 __device__ __forceinline__ int band_bucket(int w, int wj) {
     if (w >= wj) return 0;
     // descending narrow classes: >64, 49-64, 33-48, 25-32, 17-24, 13-16, 9-12, 7-8, 5-6, 4, 3, <=2
@@ -140,73 +142,105 @@ __device__ __forceinline__ int band_bucket(int w, int wj) {
     return b;
 }
 
-__global__ void band_hist_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ list,
-                                 const uint32_t *__restrict__ count, uint32_t n_max, const int32_t *__restrict__ w_cur,
-                                 uint32_t *__restrict__ hist)
-{
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t n = count ? min(*count, n_max) : n_max;
-    const bool live = t < n;
-    int b = -1;
-    if (live) {
-        const uint32_t jid = list[t];
-        b = band_bucket(w_cur[jid], jobs[jid].w);
-    }
-    const unsigned peers = __match_any_sync(0xffffffffu, b);
-    const int lane = threadIdx.x & 31;
-    if (live && lane == __ffs(peers) - 1) atomicAdd(&hist[b], (uint32_t)__popc(peers));
+constexpr int kPartThreads = 256;
+
+__device__ __forceinline__ int job_bucket(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ list,
+                                          uint32_t t, uint32_t n, const int32_t *__restrict__ w_cur, uint32_t *jid) {
+    if (t >= n) return -1;
+    *jid = list[t];
+    return band_bucket(w_cur[*jid], jobs[*jid].w);
 }
 
-__global__ void band_scatter_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ list,
-                                    const uint32_t *__restrict__ count, uint32_t n_max,
-                                    const int32_t *__restrict__ w_cur, const uint32_t *__restrict__ hist,
-                                    uint32_t *__restrict__ cursor, uint32_t *__restrict__ out,
-                                    uint32_t *__restrict__ bounds)
+__global__ void __launch_bounds__(kPartThreads)
+band_count_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ list,
+                  const uint32_t *__restrict__ count, uint32_t n_max, const int32_t *__restrict__ w_cur,
+                  uint32_t *__restrict__ blk)
 {
-    __shared__ uint32_t base[kBandBuckets];
+    __shared__ uint32_t cnt[kBandBuckets];
+    if (threadIdx.x < kBandBuckets) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    const uint32_t n = count ? min(*count, n_max) : n_max;
+    uint32_t jid = 0;
+    const int b = job_bucket(jobs, list, blockIdx.x * kPartThreads + threadIdx.x, n, w_cur, &jid);
+    const unsigned peers = __match_any_sync(0xffffffffu, b);
+    if (b >= 0 && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&cnt[b], (uint32_t)__popc(peers));
+    __syncthreads();
+    if (threadIdx.x < kBandBuckets) blk[blockIdx.x * kBandBuckets + threadIdx.x] = cnt[threadIdx.x];
+}
+
+// one warp per bucket: the per-block counts become exclusive offsets inside the bucket;
+// base[b] = the bucket's first slot, and the band-group bounds
+__global__ void __launch_bounds__(32 * kBandBuckets)
+band_scan_kernel(uint32_t *__restrict__ blk, uint32_t nblk, uint32_t *__restrict__ base,
+                 uint32_t *__restrict__ bounds)
+{
+    __shared__ uint32_t tot[kBandBuckets];
+    const int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t run = 0;
+    for (uint32_t i0 = 0; i0 < nblk; i0 += 32) {
+        const uint32_t i = i0 + lane;
+        const uint32_t v = i < nblk ? blk[i * kBandBuckets + k] : 0u;
+        uint32_t x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (i < nblk) blk[i * kBandBuckets + k] = run + x - v;
+        run += __shfl_sync(0xffffffffu, x, 31);
+    }
+    if (lane == 0) tot[k] = run;
+    __syncthreads();
     if (threadIdx.x == 0) {
-        uint32_t acc = 0;
-        for (int k = 0; k < kBandBuckets; ++k) { base[k] = acc; acc += hist[k]; }
-        if (bounds && blockIdx.x == 0) {
+        uint32_t acc = 0, bs[kBandBuckets];
+        for (int q = 0; q < kBandBuckets; ++q) { bs[q] = acc; base[q] = acc; acc += tot[q]; }
+        if (bounds) {
             // band groups: buckets 0-4 (configured band, bands > 24), 5-6 (13-24), 7-12 (<= 12);
             // bounds[3]: the end of bucket 0 (the jobs at their configured band)
-            bounds[0] = base[5];
-            bounds[1] = base[7];
+            bounds[0] = bs[5];
+            bounds[1] = bs[7];
             bounds[2] = acc;
-            bounds[3] = base[1];
+            bounds[3] = bs[1];
         }
     }
+}
+
+__global__ void __launch_bounds__(kPartThreads)
+band_place_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ list,
+                  const uint32_t *__restrict__ count, uint32_t n_max, const int32_t *__restrict__ w_cur,
+                  const uint32_t *__restrict__ blk, const uint32_t *__restrict__ base, uint32_t *__restrict__ out)
+{
+    constexpr int W = kPartThreads / 32;
+    __shared__ uint32_t wcnt[W][kBandBuckets];
+    for (int i = threadIdx.x; i < W * kBandBuckets; i += kPartThreads) (&wcnt[0][0])[i] = 0;
     __syncthreads();
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t n = count ? min(*count, n_max) : n_max;
-    const bool live = t < n;
     uint32_t jid = 0;
-    int b = -1;
-    if (live) {
-        jid = list[t];
-        b = band_bucket(w_cur[jid], jobs[jid].w);
-    }
+    const int b = job_bucket(jobs, list, blockIdx.x * kPartThreads + threadIdx.x, n, w_cur, &jid);
     const unsigned peers = __match_any_sync(0xffffffffu, b);
-    const int lane = threadIdx.x & 31;
-    const int leader = __ffs(peers) - 1;
-    uint32_t pos = 0;
-    if (live && lane == leader) pos = atomicAdd(&cursor[b], (uint32_t)__popc(peers));
-    pos = __shfl_sync(0xffffffffu, pos, leader);
-    if (live) out[base[b] + pos + __popc(peers & ((1u << lane) - 1u))] = jid;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (b >= 0 && lane == __ffs(peers) - 1) wcnt[w][b] = (uint32_t)__popc(peers);
+    __syncthreads();
+    if (b < 0) return;
+    uint32_t pos = base[b] + blk[blockIdx.x * kBandBuckets + b] + __popc(peers & ((1u << lane) - 1u));
+    for (int v = 0; v < w; ++v) pos += wcnt[v][b];
+    out[pos] = jid;
+}
+
+size_t band_partition_scratch_words(uint32_t n_max) {
+    return (size_t)((n_max + kPartThreads - 1) / kPartThreads) * kBandBuckets;
 }
 
 cudaError_t launch_band_partition(const fa_job *d_jobs, const uint32_t *d_list, const uint32_t *d_count,
-                                  uint32_t n_max, const int32_t *d_w_cur, uint32_t *d_out, uint32_t *d_hist,
-                                  uint32_t *d_cursor, uint32_t *d_bounds, cudaStream_t stream)
+                                  uint32_t n_max, const int32_t *d_w_cur, uint32_t *d_out, uint32_t *d_base,
+                                  uint32_t *d_blk, uint32_t *d_bounds, cudaStream_t stream)
 {
     if (n_max == 0) return cudaSuccess;
-    cudaError_t e = cudaMemsetAsync(d_hist, 0, sizeof(uint32_t) * kBandBuckets, stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(d_cursor, 0, sizeof(uint32_t) * kBandBuckets, stream);
-    if (e != cudaSuccess) return e;
-    const uint32_t blocks = (n_max + 255) / 256;
-    band_hist_kernel<<<blocks, 256, 0, stream>>>(d_jobs, d_list, d_count, n_max, d_w_cur, d_hist);
-    band_scatter_kernel<<<blocks, 256, 0, stream>>>(d_jobs, d_list, d_count, n_max, d_w_cur, d_hist, d_cursor, d_out,
-                                                    d_bounds);
+    const uint32_t blocks = (n_max + kPartThreads - 1) / kPartThreads;
+    band_count_kernel<<<blocks, kPartThreads, 0, stream>>>(d_jobs, d_list, d_count, n_max, d_w_cur, d_blk);
+    band_scan_kernel<<<1, 32 * kBandBuckets, 0, stream>>>(d_blk, blocks, d_base, d_bounds);
+    band_place_kernel<<<blocks, kPartThreads, 0, stream>>>(d_jobs, d_list, d_count, n_max, d_w_cur, d_blk, d_base,
+                                                           d_out);
     return cudaGetLastError();
 }
 

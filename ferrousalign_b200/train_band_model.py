@@ -14,6 +14,11 @@ cells, kernel time, and the same policy without the network (every job starting 
 fixed band).
 
     python -m ferrousalign_b200.train_band_model --out band_model_151bp.bin [--train N] [--eval N]
+
+With --shape uneven the three batches come from the uneven generator instead: mixed left and
+right extensions of 50-300 bp reads, seeds anywhere in the read, a reference with 5%
+low-complexity repeats (training seed 14, validation 16, evaluation 19; the bench's uneven
+batch uses seed 3), and the model goes to band_model_uneven.bin.
 """
 from __future__ import annotations
 
@@ -30,6 +35,20 @@ from . import band_model as B
 from . import synth
 
 FIXED_FIRST = (2, 3, 4, 6, 8, 12, 16, 24, 32)
+
+
+def uneven_batch(n: int, seed: int) -> synth.ExtBatch:
+    """The uneven shape (synth.workload_ext_uneven) on a 20 Mbp reference of its own seed."""
+    ref = synth.reference(20_000_000, seed=seed, n_rate=0.001, repeat_frac=0.05)
+    return synth.ext_jobs(ref, n, seed=seed + 100, read_len=(50, 300), seed_at_start=False, indel_rates=(0.001,))
+
+
+# generators per shape: (training, validation, evaluation) batches
+SHAPES = {
+    "151": (lambda n: synth.workload_ext_train(n, seed=4), lambda n: synth.workload_ext_1m(n, seed=6),
+            lambda n: synth.workload_ext_1m(n, seed=2 + 7919)),
+    "uneven": (lambda n: uneven_batch(n, 14), lambda n: uneven_batch(n, 16), lambda n: uneven_batch(n, 19)),
+}
 
 
 def log(*a):
@@ -62,7 +81,8 @@ def run_fixed(p, batch, w0, ctx, reps=2, judge=None):
 
 def main(argv=None) -> dict:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=str(B.DEFAULT_MODEL))
+    ap.add_argument("--out", default=None)
+    ap.add_argument("--shape", choices=sorted(SHAPES), default="151")
     ap.add_argument("--train", type=int, default=5_000_000)
     ap.add_argument("--val", type=int, default=500_000)
     ap.add_argument("--eval", type=int, default=1_000_000)
@@ -71,12 +91,16 @@ def main(argv=None) -> dict:
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--w-min", type=int, default=2)
     args = ap.parse_args(argv)
+    if args.out is None:
+        args.out = str(B.DEFAULT_MODEL if args.shape == "151" else B.UNEVEN_MODEL)
+    gen_train, gen_val, gen_eval = SHAPES[args.shape]
     ctx = N.default_context()
+    ctx.set_slices(1, 1)   # kernel times of whole-batch runs
     p = fa.BandedPairWiseSW().to_struct()
     bwa = fa.make_policy(N.FA_POLICY_BWA, 2)
 
     t0 = time.time()
-    tr = synth.workload_ext_train(args.train, seed=4)
+    tr = gen_train(args.train)
     log(f"train set {args.train} jobs in {time.time() - t0:.1f}s")
     t0 = time.time()
     label, ladder_cells = B.make_labels(p, tr.jobs, tr.qseq, tr.tseq, ctx=ctx)
@@ -86,7 +110,7 @@ def main(argv=None) -> dict:
     target = np.log2(label.astype(np.float32))
     del tr
 
-    val = synth.workload_ext_1m(args.val, seed=6)
+    val = gen_val(args.val)
     val_plain, _, _ = fa.extend_batch(p, val.jobs, val.qseq, val.tseq, policy=bwa, ctx=ctx)
     best = None
     sweep = {}
@@ -111,10 +135,10 @@ def main(argv=None) -> dict:
     del x, val
 
     # held-out evaluation (disjoint generator seeds)
-    ev = synth.workload_ext_1m(args.eval, seed=2 + 7919)
+    ev = gen_eval(args.eval)
     plain, pst, _ = fa.extend_batch(p, ev.jobs, ev.qseq, ev.tseq, policy=bwa, ctx=ctx)
     out, st, wf, wfin = run_learned(p, ev, model, args.w_min, ctx, judge=judge)
-    res = {"w_min": args.w_min, "train_jobs": args.train, "eval_jobs": args.eval, "epochs": args.epochs,
+    res = {"shape": args.shape, "w_min": args.w_min, "train_jobs": args.train, "eval_jobs": args.eval, "epochs": args.epochs,
            "tau": tau, "retry_rule": rule, "judge": judge, "tau_sweep": sweep, "train_loss": [float(v) for v in losses], "label_hist": hist,
            "plain": {"cells_executed": int(pst["cells_executed"]), "kernel_ms": float(pst["kernel_ms"])},
            "learned": {"identical_all": bool(np.array_equal(out, plain)),
