@@ -82,6 +82,23 @@ def test_wide_scores_and_long_reads_take_the_int32_row_state(built):
     check(p, np.concatenate([j2, extra]), qseq, tseq)
 
 
+def test_wide_band_over_long_targets(built):
+    """w = 100 over 1000-base targets (the row state's full band, rows far past the query's
+    length): same results as the oracle."""
+    import ferrousalign_b200 as fa
+    from ferrousalign_b200 import cigar as G
+    rng = np.random.default_rng(5)
+    qs, ts, jobs = [], [], np.zeros(3, G.CIGAR_JOB_DT)
+    qo = to = 0
+    for k in range(3):
+        t = rng.integers(0, 4, 1000).astype(np.uint8)
+        q = t[300 + 50 * k:500 + 50 * k].copy()
+        q[rng.integers(0, 200, 6)] = rng.integers(0, 4, 6)
+        jobs[k] = (qo, to, len(q), len(t), 100, 0)
+        qs.append(q); ts.append(t); qo += len(q); to += len(t)
+    check(fa.BandedPairWiseSW().to_struct(), jobs, np.concatenate(qs), np.concatenate(ts))
+
+
 def test_edges_codes_and_empty(built):
     import ferrousalign_b200 as fa
     from ferrousalign_b200 import cigar as G
