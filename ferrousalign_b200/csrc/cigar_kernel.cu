@@ -53,11 +53,16 @@ __device__ __forceinline__ uint32_t cigar_op(uint32_t op, uint32_t len) { return
 // Row state of one job (H of the previous row's cell and E, per query column 0..qlen): int32
 // pairs in a per-job global scratch, or 16-bit pairs in shared memory (one word per column,
 // the block's jobs interleaved so that each thread's accesses hit its own bank).
+// ldq(j, Q, q): the column's (H, E) and its query code (raw, as the sequence holds it);
+// st(j, h, e, q) stores a column the row computed, st_end(j, h) the row's end word (E = 0).
 struct EhGlobal {
     static constexpr bool kNarrow = false;   // scores may pass 16 bits
     int2 *eh;
     __device__ __forceinline__ int2 ld(int j) const { return eh[j]; }
-    __device__ __forceinline__ void st(int j, int h, int e) const { eh[j] = make_int2(h, e); }
+    __device__ __forceinline__ int2 ldq(int j, const uint8_t *Q, uint32_t &q) const { q = Q[j]; return eh[j]; }
+    __device__ __forceinline__ void init(int j, int h, const uint8_t *) const { eh[j] = make_int2(h, 0); }
+    __device__ __forceinline__ void st(int j, int h, int e, uint32_t) const { eh[j] = make_int2(h, e); }
+    __device__ __forceinline__ void st_end(int j, int h) const { eh[j] = make_int2(h, 0); }
 };
 struct EhShared {
     static constexpr bool kNarrow = true;    // every score < 32768
@@ -67,7 +72,40 @@ struct EhShared {
         const uint32_t v = w[j * stride];
         return make_int2((int)(v & 0xFFFFu), (int)(v >> 16));
     }
-    __device__ __forceinline__ void st(int j, int h, int e) const { w[j * stride] = (uint32_t)h | (uint32_t)e << 16; }
+    __device__ __forceinline__ int2 ldq(int j, const uint8_t *Q, uint32_t &q) const { q = Q[j]; return ld(j); }
+    __device__ __forceinline__ void init(int j, int h, const uint8_t *) const { w[j * stride] = (uint32_t)h; }
+    __device__ __forceinline__ void st(int j, int h, int e, uint32_t) const {
+        w[j * stride] = (uint32_t)h | (uint32_t)e << 16;
+    }
+    __device__ __forceinline__ void st_end(int j, int h) const { w[j * stride] = (uint32_t)h; }
+};
+// The same with the column's query code in the word (H in bits 0-12, E in 13-25, the code
+// clamped to 4 in 26-28): every score < 8192, and a step reads no query byte from global
+// memory (the traceback reads the raw bases).
+struct EhSharedQ {
+    static constexpr bool kNarrow = true;
+    uint32_t *w;
+    int stride;
+    __device__ __forceinline__ int2 ld(int j) const {
+        const uint32_t v = w[j * stride];
+        return make_int2((int)(v & 0x1FFFu), (int)((v >> 13) & 0x1FFFu));
+    }
+    __device__ __forceinline__ int2 ldq(int j, const uint8_t *, uint32_t &q) const {
+        const uint32_t v = w[j * stride];
+        q = v >> 26;
+        return make_int2((int)(v & 0x1FFFu), (int)((v >> 13) & 0x1FFFu));
+    }
+    __device__ __forceinline__ void init(int j, int h, const uint8_t *Q) const {
+        const uint32_t q = Q ? min((uint32_t)Q[j], 4u) : 0u;
+        w[j * stride] = (uint32_t)h | q << 26;
+    }
+    __device__ __forceinline__ void st(int j, int h, int e, uint32_t q) const {
+        w[j * stride] = (uint32_t)h | (uint32_t)e << 13 | q << 26;
+    }
+    __device__ __forceinline__ void st_end(int j, int h) const {
+        uint32_t *x = &w[j * stride];
+        *x = (*x & 0xFC000000u) | (uint32_t)h;
+    }
 };
 
 // One alignment: the banded rows into the row state and the traceback words, then the
@@ -107,12 +145,13 @@ __device__ __forceinline__ void cigar_job(uint32_t k, const fa_cigar_job &J, con
     uint32_t *tb = tb_all + P.tb;
     const int oe_del = p.o_del + p.e_del, oe_ins = p.o_ins + p.e_ins;
     // first row (implementation.rs:67-75)
-    eh.st(0, h0, 0);
+    // (a row state that carries the query codes gets them here, column qlen none)
+    eh.init(0, h0, Q);   // qlen >= 1 here
     int hp = h0 > oe_ins ? h0 - oe_ins : 0;
-    eh.st(1, hp, 0);
+    eh.init(1, hp, qlen > 1 ? Q : nullptr);
     for (int j = 2; j <= qlen; ++j) {
         hp = hp > p.e_ins ? hp - p.e_ins : 0;
-        eh.st(j, hp, 0);
+        eh.init(j, hp, j < qlen ? Q : nullptr);
     }
     int max_score = h0, max_i = -1, max_j = -1, max_ie = -1, gscore = -1, max_off = 0;
     int beg = 0, end = qlen, cells = 0;
@@ -144,10 +183,7 @@ __device__ __forceinline__ void cigar_job(uint32_t k, const fa_cigar_job &J, con
             for (int u = 0; u < 8; ++u) {
                 ev[u] = make_int2(0, 0);
                 qv[u] = 0;
-                if (j0 + u < ce) {
-                    ev[u] = eh.ld(j0 + u);
-                    qv[u] = Q[j0 + u];
-                }
+                if (j0 + u < ce) ev[u] = eh.ldq(j0 + u, Q, qv[u]);
             }
             uint32_t chunk = 0;
 #pragma unroll
@@ -170,7 +206,7 @@ __device__ __forceinline__ void cigar_job(uint32_t k, const fa_cigar_job &J, con
                     mj = j;
                 }
                 const int en = __viaddmax_s32_relu(e, -p.e_del, m - oe_del);
-                eh.st(j, h1, en);   // H of the previous row's cell, E for the next row
+                eh.st(j, h1, en, q);   // H of the previous row's cell, E for the next row
                 f = __viaddmax_s32_relu(f, -p.e_ins, m - oe_ins);
                 h1 = h;
             }
@@ -186,7 +222,7 @@ __device__ __forceinline__ void cigar_job(uint32_t k, const fa_cigar_job &J, con
             mj = 0xFFFF - (best & 0xFFFF);
         }
         if (ce > cb) cells += ce - cb;
-        eh.st(ce, h1, 0);
+        eh.st_end(ce, h1);
         if (ce == qlen && gscore < h1) { gscore = h1; max_ie = i; }
         if (m_val == 0) break;
         if (m_val > max_score) {
@@ -317,6 +353,8 @@ cigar_kernel(const fa_cigar_job *__restrict__ jobs, const CigarPlan *__restrict_
 // The row state in shared memory as 16-bit pairs (every score of the batch fits: the host
 // checks h0 + qlen * max <= 32767), jobs taken in `order` (similar bands side by side in a
 // warp), (qcap + 1) words per thread.
+// QW: the row-state words also carry the query codes (EhSharedQ).
+template <bool QW>
 __global__ void __launch_bounds__(kCigarThreads)
 cigar_smem_kernel(const fa_cigar_job *__restrict__ jobs, const CigarPlan *__restrict__ plan,
                   const uint32_t *__restrict__ order, uint32_t n, const uint8_t *__restrict__ qseq,
@@ -330,8 +368,12 @@ cigar_smem_kernel(const fa_cigar_job *__restrict__ jobs, const CigarPlan *__rest
     const uint32_t t = blockIdx.x * kCigarThreads + threadIdx.x;
     if (t >= n) return;
     const uint32_t k = order[t];
-    cigar_job(k, jobs[k], plan[k], qseq, tseq, p, pen_clip3, EhShared{ehs + 16 + threadIdx.x, kCigarThreads}, ehs,
-              tb_all, out, cigar, ref_al, qry_al);
+    if (QW)
+        cigar_job(k, jobs[k], plan[k], qseq, tseq, p, pen_clip3, EhSharedQ{ehs + 16 + threadIdx.x, kCigarThreads},
+                  ehs, tb_all, out, cigar, ref_al, qry_al);
+    else
+        cigar_job(k, jobs[k], plan[k], qseq, tseq, p, pen_clip3, EhShared{ehs + 16 + threadIdx.x, kCigarThreads},
+                  ehs, tb_all, out, cigar, ref_al, qry_al);
 }
 
 // Packs the jobs' CIGAR words back to back: job k's n_cigar words from its capacity slot
@@ -368,17 +410,20 @@ cudaError_t launch_cigar(const fa_cigar_job *d_jobs, const CigarPlan *d_plan, ui
 }
 
 cudaError_t launch_cigar_smem(const fa_cigar_job *d_jobs, const CigarPlan *d_plan, const uint32_t *d_order,
-                              uint32_t n, int qcap, const uint8_t *d_qseq, const uint8_t *d_tseq, const ExtParams &p,
-                              int pen_clip3, uint32_t *d_tb, fa_cigar_result *d_out, uint32_t *d_cigar,
-                              uint8_t *d_ref_al, uint8_t *d_qry_al, cudaStream_t s)
+                              uint32_t n, int qcap, bool qwords, const uint8_t *d_qseq, const uint8_t *d_tseq,
+                              const ExtParams &p, int pen_clip3, uint32_t *d_tb, fa_cigar_result *d_out,
+                              uint32_t *d_cigar, uint8_t *d_ref_al, uint8_t *d_qry_al, cudaStream_t s)
 {
     if (n == 0) return cudaSuccess;
     const size_t smem = sizeof(uint32_t) * (16 + kCigarThreads * (size_t)(qcap + 1));
-    cudaError_t err = cudaFuncSetAttribute(cigar_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (err != cudaSuccess) return err;
-    cigar_smem_kernel<<<(n + kCigarThreads - 1) / kCigarThreads, kCigarThreads, smem, s>>>(
-        d_jobs, d_plan, d_order, n, d_qseq, d_tseq, p, pen_clip3, d_tb, d_out, d_cigar, d_ref_al, d_qry_al);
-    return cudaGetLastError();
+    auto go = [&](auto kernel) -> cudaError_t {
+        cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (err != cudaSuccess) return err;
+        kernel<<<(n + kCigarThreads - 1) / kCigarThreads, kCigarThreads, smem, s>>>(
+            d_jobs, d_plan, d_order, n, d_qseq, d_tseq, p, pen_clip3, d_tb, d_out, d_cigar, d_ref_al, d_qry_al);
+        return cudaGetLastError();
+    };
+    return qwords ? go(cigar_smem_kernel<true>) : go(cigar_smem_kernel<false>);
 }
 
 int cigar_smem_qcap() { return (int)((kCigarSmemMax - 64) / (sizeof(uint32_t) * kCigarThreads)) - 1; }

@@ -2135,7 +2135,8 @@ int cigar_launch(fa_ctx *c, const fa_params *p, const fa_cigar_job *jobs, uint32
     uint64_t cig = 0, ref = 0, qry = 0, eh = 0, tb = 0;
     int max_mat = 0, qmax = 0;
     for (int i = 0; i < 25; ++i) max_mat = std::max<int>(max_mat, p->mat[i]);
-    bool narrow = true;   // every score fits the shared-memory kernel's 16-bit row state
+    bool narrow = true;     // every score fits the shared-memory kernel's 16-bit row state
+    bool narrow13 = true;   // ... and 13 bits, leaving room for the query codes in the words
     for (uint32_t k = 0; k < n; ++k) {
         const fa_cigar_job &j = jobs[k];
         if (j.qlen < 0 || j.tlen < 0 || j.w < 0) return fail(FA_ERR_ARG, "cigar job %u: negative length or band", k);
@@ -2153,6 +2154,7 @@ int cigar_launch(fa_ctx *c, const fa_params *p, const fa_cigar_job *jobs, uint32
         tb += (uint64_t)j.tlen * (pl.wpr + 1);   // per row: a header word, then the codes
         qmax = std::max(qmax, j.qlen);
         narrow = narrow && j.h0 >= 0 && (long long)j.h0 + (long long)j.qlen * max_mat <= 32767;
+        narrow13 = narrow13 && j.h0 >= 0 && (long long)j.h0 + (long long)j.qlen * max_mat <= 8191;
     }
     const bool smem = narrow && qmax <= cigar_smem_qcap();
     // shared-memory kernel: jobs ordered by band, widest first (a counting sort), so that a
@@ -2204,8 +2206,8 @@ int cigar_launch(fa_ctx *c, const fa_params *p, const fa_cigar_job *jobs, uint32
     const ExtParams kp = ext_params_of(p);
     if (c->timing) FA_CUDA(cudaEventRecord(c->kev0, s));
     if (smem)
-        FA_CUDA(launch_cigar_smem(d_jobs, d_plan, d_order, n, qmax, d_q, d_t, kp, p->pen_clip3, d_tb, r->out, r->cig,
-                                  r->ref, r->qry, s));
+        FA_CUDA(launch_cigar_smem(d_jobs, d_plan, d_order, n, qmax, narrow13, d_q, d_t, kp, p->pen_clip3, d_tb, r->out,
+                                  r->cig, r->ref, r->qry, s));
     else
         FA_CUDA(launch_cigar(d_jobs, d_plan, n, d_q, d_t, kp, p->pen_clip3, d_eh, d_tb, r->out, r->cig, r->ref,
                              r->qry, s));

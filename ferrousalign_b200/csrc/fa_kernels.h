@@ -230,11 +230,12 @@ cudaError_t launch_cigar(const fa_cigar_job *d_jobs, const CigarPlan *d_plan, ui
                          fa_cigar_result *d_out, uint32_t *d_cigar, uint8_t *d_ref_al, uint8_t *d_qry_al,
                          cudaStream_t s);
 // The same with the row state in shared memory as 16-bit pairs: every job's qlen <= qcap <=
-// cigar_smem_qcap() and h0 + qlen * max(mat) <= 32767; jobs run in d_order.
+// cigar_smem_qcap() and h0 + qlen * max(mat) <= 32767; jobs run in d_order.  qwords: the
+// words also carry the query codes (13-bit H and E: h0 + qlen * max(mat) <= 8191).
 cudaError_t launch_cigar_smem(const fa_cigar_job *d_jobs, const CigarPlan *d_plan, const uint32_t *d_order,
-                              uint32_t n, int qcap, const uint8_t *d_qseq, const uint8_t *d_tseq, const ExtParams &p,
-                              int pen_clip3, uint32_t *d_tb, fa_cigar_result *d_out, uint32_t *d_cigar,
-                              uint8_t *d_ref_al, uint8_t *d_qry_al, cudaStream_t s);
+                              uint32_t n, int qcap, bool qwords, const uint8_t *d_qseq, const uint8_t *d_tseq,
+                              const ExtParams &p, int pen_clip3, uint32_t *d_tb, fa_cigar_result *d_out,
+                              uint32_t *d_cigar, uint8_t *d_ref_al, uint8_t *d_qry_al, cudaStream_t s);
 int cigar_smem_qcap();
 // job k's n_cigar words from its slot at plan[k].cig to d_packed[d_first[k]]
 cudaError_t launch_cigar_pack(const CigarPlan *d_plan, const fa_cigar_result *d_res, const uint64_t *d_first,

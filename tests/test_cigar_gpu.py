@@ -62,15 +62,18 @@ def test_uneven_jobs_other_scoring(built):
 
 
 def test_wide_scores_and_long_reads_take_the_int32_row_state(built):
-    """A batch whose scores could pass 16 bits (h0 near 32767), or with a query longer than
-    the shared row state holds, runs the int32 global-memory form: same results."""
+    """A batch whose scores could pass 13 bits runs the 16-bit row state without query codes,
+    one whose scores could pass 16 bits (h0 near 32767), or with a query longer than the
+    shared row state holds, the int32 global-memory form: same results."""
     import ferrousalign_b200 as fa
     from ferrousalign_b200 import synth
     rng = np.random.default_rng(4)
     b = synth.workload_ext_1m(300)
     p = fa.BandedPairWiseSW().to_struct()
     j = jobs_from(b, rng, bands=(5, 20))
-    j["h0"][::7] = 32700
+    j["h0"][::7] = 10000           # past 13 bits: 16-bit row state without the query codes
+    check(p, j, b.qseq, b.tseq)
+    j["h0"][::7] = 32700           # past 16 bits: the int32 global row state
     check(p, j, b.qseq, b.tseq)
     ub = synth.workload_ext_uneven(200, ref_len=2_000_000)
     long_q = rng.integers(0, 4, 450).astype(np.uint8)
