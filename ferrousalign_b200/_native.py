@@ -221,9 +221,16 @@ class Context:
         cm = (C.c_float * 8)()
         check(load().fa_ctx_kernel_choice(self.handle, C.byref(k), C.byref(t), 8, ck, ct, cm, C.byref(nc)))
         names = {FA_KERNEL_INT32: "int32", FA_KERNEL_INT16X2: "int16x2", FA_KERNEL_ROWS2: "rows2"}
-        return {"kernel": names.get(k.value, str(k.value)), "threads_per_block": t.value,
-                "candidates": [{"kernel": names.get(ck[i], str(ck[i])), "threads_per_block": ct[i],
-                                "sample_ms": float(cm[i])} for i in range(min(nc.value, 8))]}
+        # the tiling each kernel kind stands for: jobs per thread and target rows per step
+        shape = {FA_KERNEL_INT32: (1, 1), FA_KERNEL_INT16X2: (2, 1), FA_KERNEL_ROWS2: (1, 2)}
+
+        def entry(kind: int, tpb: int) -> dict:
+            jobs, rows = shape.get(kind, (1, 1))
+            return {"kernel": names.get(kind, str(kind)), "threads_per_block": tpb, "jobs_per_thread": jobs,
+                    "rows_per_thread": rows, "jobs_per_warp": 32 * jobs}
+        out = entry(k.value, t.value)
+        out["candidates"] = [dict(entry(ck[i], ct[i]), sample_ms=float(cm[i])) for i in range(min(nc.value, 8))]
+        return out
 
     def set_slices(self, single_band: int = 0, policy_rounds: int = 0) -> None:
         """Upload slices of large host batches (2..8; 1 uploads the whole batch before one run
