@@ -1312,7 +1312,7 @@ struct MateHostPlan {
     MateParams mp;
     std::vector<uint32_t> order;   // u8 jobs, then i16 jobs
     uint32_t n_byte = 0;
-    int mq_b = 0, mq_w = 0, mt = 0;
+    int mq_b = 0, mq_w = 0, mt = 0, mn_b = INT_MAX;
 };
 
 int plan_mate_host(const fa_mate_params *p, const fa_mate_job *jobs, uint32_t n, uint64_t qseq_len,
@@ -1339,7 +1339,12 @@ int plan_mate_host(const fa_mate_params *p, const fa_mate_job *jobs, uint32_t n,
             return fail(FA_ERR_CAPACITY, "mate job %u: qlen=%d exceeds the %s-lane limit", i, j.qlen,
                         byte ? "u8" : "i16");
         (byte ? pl->order : word_list).push_back(i);
-        if (byte) pl->mq_b = std::max(pl->mq_b, j.qlen); else pl->mq_w = std::max(pl->mq_w, j.qlen);
+        if (byte) {
+            pl->mq_b = std::max(pl->mq_b, j.qlen);
+            pl->mn_b = std::min(pl->mn_b, j.qlen);
+        } else {
+            pl->mq_w = std::max(pl->mq_w, j.qlen);
+        }
         pl->mt = std::max(pl->mt, j.tlen);
     }
     pl->n_byte = (uint32_t)pl->order.size();
@@ -1352,13 +1357,14 @@ cudaError_t launch_mate_plan(const MateHostPlan &pl, const fa_mate_job *d_jobs, 
                              const uint8_t *d_q, const uint8_t *d_t, fa_kswr *d_out, unsigned long long *d_cells,
                              uint32_t *d_status, uint32_t *d_rev, cudaStream_t s, uint32_t *launches) {
     if (pl.n_byte) {
-        cudaError_t e = launch_mate_sw(true, d_jobs, d_order, pl.n_byte, d_q, d_t, pl.mp, pl.mq_b, pl.mt, d_out,
+        cudaError_t e = launch_mate_sw(true, d_jobs, d_order, pl.n_byte, d_q, d_t, pl.mp, pl.mn_b, pl.mq_b, pl.mt,
+                                       d_out,
                                        d_cells, d_status, d_rev, s);
         if (e != cudaSuccess) return e;
         *launches += 2;
     }
     if (n > pl.n_byte) {
-        cudaError_t e = launch_mate_sw(false, d_jobs, d_order + pl.n_byte, n - pl.n_byte, d_q, d_t, pl.mp, pl.mq_w,
+        cudaError_t e = launch_mate_sw(false, d_jobs, d_order + pl.n_byte, n - pl.n_byte, d_q, d_t, pl.mp, 1, pl.mq_w,
                                        pl.mt, d_out, d_cells, d_status, nullptr, s);
         if (e != cudaSuccess) return e;
         ++*launches;
@@ -1821,12 +1827,13 @@ int fa_mate_sw_batch_device(fa_ctx *c, const fa_mate_params *p, const fa_mate_jo
     uint32_t launches = 1;
     if (c->timing) FA_CUDA(cudaEventRecord(c->kev0, s));
     if (h[0]) {
-        FA_CUDA(launch_mate_sw(true, d_jobs, c->order.as<uint32_t>(), h[0], d_qseq, d_tseq, mp, (int)h[2], (int)h[4],
+        FA_CUDA(launch_mate_sw(true, d_jobs, c->order.as<uint32_t>(), h[0], d_qseq, d_tseq, mp,
+                               (int)(0xFFFFFFFFu - h[6]), (int)h[2], (int)h[4],
                                d_out, m.cells, m.status, c->mate_rev.as<uint32_t>(), s));
         launches += 2;
     }
     if (h[1]) {
-        FA_CUDA(launch_mate_sw(false, d_jobs, c->list_a.as<uint32_t>(), h[1], d_qseq, d_tseq, mp, (int)h[3],
+        FA_CUDA(launch_mate_sw(false, d_jobs, c->list_a.as<uint32_t>(), h[1], d_qseq, d_tseq, mp, 1, (int)h[3],
                                (int)h[4], d_out, m.cells, m.status, nullptr, s));
         ++launches;
     }

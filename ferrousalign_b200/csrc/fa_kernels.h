@@ -106,9 +106,11 @@ cudaError_t launch_unpack2(const uint8_t *d_src, uint64_t n, const fa_nrun *d_ru
 // emulation of the reference's striped kernels; d_order lists the jobs of that kind.
 // d_rev (2 + n words; needed for u8 jobs, unused for i16 jobs): the list of KSW_XSTART
 // reverse passes that a second kernel runs after the forward passes.
+// min_qlen: the shortest query of the launch's jobs (u8 jobs whose segment counts all equal
+// the register depth run a form without per-segment range checks).
 cudaError_t launch_mate_sw(bool byte_lanes, const fa_mate_job *d_jobs, const uint32_t *d_order,
                            uint32_t n, const uint8_t *d_qseq, const uint8_t *d_tseq,
-                           const MateParams &p, int max_qlen, int max_tlen, fa_kswr *d_out,
+                           const MateParams &p, int min_qlen, int max_qlen, int max_tlen, fa_kswr *d_out,
                            unsigned long long *d_cells, uint32_t *d_status, uint32_t *d_rev,
                            cudaStream_t stream);
 
@@ -160,7 +162,7 @@ int fa_ctx_device(const fa_ctx *ctx);
 int set_last_error(int code, const char *msg);
 
 // Mate-rescue jobs split by lane width into two order lists; info (8 words) =
-// {n_byte, n_word, max_q_byte, max_q_word, max_t, bad_lengths, -, -}.
+// {n_byte, n_word, max_q_byte, max_q_word, max_t, bad_lengths, 0xFFFFFFFF - min_q_byte, -}.
 cudaError_t launch_mate_split(const fa_mate_job *d_jobs, uint32_t n, uint32_t *d_order_b, uint32_t *d_order_w,
                               uint32_t *d_info, cudaStream_t s);
 

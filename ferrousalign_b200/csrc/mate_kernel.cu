@@ -248,14 +248,15 @@ __device__ __forceinline__ uint32_t lane_up_u16x2(uint32_t v, uint32_t gmask, in
 // signed matrix entry (PRMT sign-extends it to 16 bits), one __viaddmax_s16x2_relu gives
 // max(hd + mat, E, 0), and the insertion and deletion terms share one subtraction.  Same
 // results as the general form.
-template <int SMAX, bool REV, bool FAST>
+// FULL: every job of the launch has exactly SMAX segments (no per-segment range checks).
+template <int SMAX, bool REV, bool FAST, bool FULL = false>
 __device__ fa_kswr sw_pass_u8x2(SeqView Q, int qlen, SeqView Tg, int tlen, uint32_t xtra, const MateParams &p,
                                 uint32_t gmask, int l, uint32_t *blist, int bcap, uint32_t *hm, const uint32_t *rt,
                                 unsigned long long &cells, uint32_t &status)
 {
     constexpr int P = 16;                      // lanes of the reference's u8 vector
     const int slen = (qlen + P - 1) / P;
-    const int off = SMAX - slen;               // segment j lives at register index j + off
+    const int off = FULL ? 0 : SMAX - slen;               // segment j lives at register index j + off
     const uint32_t minsc = (xtra & FA_KSW_XSUBO) ? (xtra & 0xffffu) : 0x10000u;
     const uint32_t endsc = (xtra & FA_KSW_XSTOP) ? (xtra & 0xffffu) : 0x10000u;
     const uint32_t shift = (uint32_t)p.shift;
@@ -528,7 +529,7 @@ __device__ __forceinline__ void mate_row_tables(uint32_t *rt, const MateParams &
 // forward pass of every job.  A reverse pass that can reach the forward score is appended to
 // `rev` (rev[0] the count, the job ids from rev[2]) for mate_rev_kernel_u8x2, which keeps
 // all its groups busy with listed jobs.
-template <int SMAX, bool FAST>
+template <int SMAX, bool FAST, bool FULL>
 __global__ void __launch_bounds__(kMateThreads)
 mate_sw_kernel_u8x2(const fa_mate_job *__restrict__ jobs, const uint32_t *__restrict__ order, uint32_t n,
                     const uint8_t *__restrict__ qseq, const uint8_t *__restrict__ tseq, const MateParams p,
@@ -553,7 +554,7 @@ mate_sw_kernel_u8x2(const fa_mate_job *__restrict__ jobs, const uint32_t *__rest
         uint32_t *blist = bsm + 16 + (threadIdx.x / G) * bcap;
         uint32_t *hm = bsm + 16 + (kMateThreads / G) * bcap + (threadIdx.x / G) * (SMAX * G);
         SeqView Q{qseq + jb.q_off, -1}, Tg{tseq + jb.t_off, -1};
-        fa_kswr r = sw_pass_u8x2<SMAX, false, FAST>(Q, jb.qlen, Tg, jb.tlen, jb.xtra, p, gmask, l, blist, bcap, hm, bsm,
+        fa_kswr r = sw_pass_u8x2<SMAX, false, FAST, FULL>(Q, jb.qlen, Tg, jb.tlen, jb.xtra, p, gmask, l, blist, bcap, hm, bsm,
                                               cells, st);
         if (mate_needs_start(r, jb.xtra)) {
             if (!mate_start_reachable(r, p)) {
@@ -627,14 +628,14 @@ mate_rev_kernel_u8x2(const fa_mate_job *__restrict__ jobs, const uint8_t *__rest
     }
 }
 
-template <int SMAX, bool FAST>
+template <int SMAX, bool FAST, bool FULL>
 static cudaError_t launch_mate_u8x2(const fa_mate_job *d_jobs, const uint32_t *d_order, uint32_t n,
                                     const uint8_t *d_qseq, const uint8_t *d_tseq, const MateParams &p, int bcap,
                                     fa_kswr *d_out, unsigned long long *d_cells, uint32_t *d_status, uint32_t *d_rev,
                                     cudaStream_t stream)
 {
     const size_t smem = (16 + (size_t)(kMateThreads / 8) * (bcap + SMAX * 8)) * sizeof(uint32_t);
-    cudaError_t err = cudaFuncSetAttribute(mate_sw_kernel_u8x2<SMAX, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t err = cudaFuncSetAttribute(mate_sw_kernel_u8x2<SMAX, FAST, FULL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)smem);
     if (err != cudaSuccess) return err;
     if (!d_rev) return cudaErrorInvalidValue;
@@ -642,7 +643,7 @@ static cudaError_t launch_mate_u8x2(const fa_mate_job *d_jobs, const uint32_t *d
     if (err != cudaSuccess) return err;
     const uint64_t threads = (uint64_t)n * 8;
     const uint32_t blocks = (uint32_t)((threads + kMateThreads - 1) / kMateThreads);
-    mate_sw_kernel_u8x2<SMAX, FAST><<<blocks, kMateThreads, smem, stream>>>(d_jobs, d_order, n, d_qseq, d_tseq, p, bcap,
+    mate_sw_kernel_u8x2<SMAX, FAST, FULL><<<blocks, kMateThreads, smem, stream>>>(d_jobs, d_order, n, d_qseq, d_tseq, p, bcap,
                                                                       d_out, d_cells, d_status, d_rev);
     err = cudaGetLastError();
     if (err != cudaSuccess) return err;
@@ -682,7 +683,7 @@ static cudaError_t launch_mate_t(const fa_mate_job *d_jobs, const uint32_t *d_or
 
 cudaError_t launch_mate_sw(bool byte_lanes, const fa_mate_job *d_jobs, const uint32_t *d_order,
                            uint32_t n, const uint8_t *d_qseq, const uint8_t *d_tseq,
-                           const MateParams &p, int max_qlen, int max_tlen, fa_kswr *d_out,
+                           const MateParams &p, int min_qlen, int max_qlen, int max_tlen, fa_kswr *d_out,
                            unsigned long long *d_cells, uint32_t *d_status, uint32_t *d_rev,
                            cudaStream_t stream)
 {
@@ -693,12 +694,15 @@ cudaError_t launch_mate_sw(bool byte_lanes, const fa_mate_job *d_jobs, const uin
     // the batch's query length (151-bp mates: 10 u8 segments, 19 i16 segments)
 #define FA_MATE(PP, SS) launch_mate_t<PP, SS>(d_jobs, d_order, n, d_qseq, d_tseq, p, bcap, d_out, d_cells, d_status, \
                                               stream)
-#define FA_MATE2(SS) (fast ? launch_mate_u8x2<SS, true>(d_jobs, d_order, n, d_qseq, d_tseq, p, bcap, d_out, d_cells, \
-                                                      d_status, d_rev, stream)                                      \
-                  : launch_mate_u8x2<SS, false>(d_jobs, d_order, n, d_qseq, d_tseq, p, bcap, d_out, d_cells,       \
-                                                d_status, d_rev, stream))
+#define FA_MATE2_(SS, FA, FU) launch_mate_u8x2<SS, FA, FU>(d_jobs, d_order, n, d_qseq, d_tseq, p, bcap, d_out, \
+                                                           d_cells, d_status, d_rev, stream)
+#define FA_MATE2(SS)                                                                                             \
+    (fast ? (full(SS) ? FA_MATE2_(SS, true, true) : FA_MATE2_(SS, true, false))                                 \
+          : (full(SS) ? FA_MATE2_(SS, false, true) : FA_MATE2_(SS, false, false)))
     // sw_pass_u8x2's FAST form: no u8 saturation possible below the score cap, equal gap penalties
     const bool fast = (max_qlen + 1) * p.max + (p.shift & 0xff) <= 255 && p.o_del == p.o_ins && p.e_del == p.e_ins;
+    // FULL form: every job's segment count equals the register depth
+    auto full = [&](int smax) { return min_qlen > 16 * (smax - 1); };
     if (byte_lanes) {
         if (max_qlen <= 16 * 10) return FA_MATE2(10);
         if (max_qlen <= 16 * 12) return FA_MATE2(12);
@@ -707,6 +711,7 @@ cudaError_t launch_mate_sw(bool byte_lanes, const fa_mate_job *d_jobs, const uin
         return FA_MATE2(32);
     }
 #undef FA_MATE2
+#undef FA_MATE2_
     if (max_qlen <= 8 * 16) return FA_MATE(8, 16);
     if (max_qlen <= 8 * 20) return FA_MATE(8, 20);
     if (max_qlen <= 8 * 24) return FA_MATE(8, 24);

@@ -72,7 +72,8 @@ namespace fa {
 
 // Splits mate-rescue jobs by lane width (KSW_XBYTE: 16 u8 lanes, else 8 i16 lanes) into
 // two order lists and records, per kind, the job count and the longest query, plus the
-// longest target: info = {n_byte, n_word, max_q_byte, max_q_word, max_t}.
+// longest target and the shortest u8 query: info = {n_byte, n_word, max_q_byte, max_q_word,
+// max_t, bad, ~min_q_byte}.
 __global__ void mate_split_kernel(const fa_mate_job *__restrict__ jobs, uint32_t n, uint32_t *__restrict__ order_b,
                                   uint32_t *__restrict__ order_w, uint32_t *__restrict__ info)
 {
@@ -96,6 +97,7 @@ __global__ void mate_split_kernel(const fa_mate_job *__restrict__ jobs, uint32_t
     if (byte) {
         order_b[base_b + __popc(mb & below)] = i;
         atomicMax(&info[2], (uint32_t)max(jb.qlen, 0));
+        atomicMax(&info[6], 0xFFFFFFFFu - (uint32_t)max(jb.qlen, 0));   // the shortest, complemented
     } else {
         order_w[base_w + __popc(mw & below)] = i;
         atomicMax(&info[3], (uint32_t)max(jb.qlen, 0));
