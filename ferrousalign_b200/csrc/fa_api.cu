@@ -88,7 +88,7 @@ struct fa_ctx {
     DevBuf mc_in, mc_plan, mc_out;      // mate-rescue jobs: inputs, plans + scan sums, outputs
     DevBuf is_buf;                      // insert-size statistics: pairs, histogram, results
     DevBuf w_first, w_cur, prev, kk, w_final, tries, missed, list_a, list_b, hist, feat, wbf, part_n, part_w;
-    DevBuf part_blk[2];   // band partition scratch (per-block bucket offsets), one per lane
+    DevBuf part_blk[4];   // band partition scratch (per-block bucket offsets), one per lane
     DevBuf qruns, truns;                // N runs of packed host batches
     // the sequences of the current host call on the device (byte codes or packed bases)
     SeqBuf cq{}, ct{};
@@ -102,9 +102,12 @@ struct fa_ctx {
     cudaEvent_t fork_ev = nullptr, join_ev[2] = {nullptr, nullptr};
     // a second lane for sliced host batches (alternate slices run concurrently): its own
     // stream, band-group streams and events, and scratch counters
-    cudaStream_t lane1 = nullptr, aux1[2] = {nullptr, nullptr};
-    cudaEvent_t fork_ev1 = nullptr, join_ev1[2] = {nullptr, nullptr}, lane_ev[2] = {nullptr, nullptr};
-    DevBuf misc1;
+    // (lane 0 is `stream` with misc, aux, fork_ev and join_ev; lanes 1 .. kLanes-1 here)
+    static constexpr int kLanes = 4;
+    cudaStream_t lane_s[kLanes] = {}, lane_aux[kLanes][2] = {};
+    cudaEvent_t lane_fork[kLanes] = {}, lane_join[kLanes][2] = {}, lane_done[kLanes] = {};
+    cudaEvent_t lane_ev[2] = {nullptr, nullptr};
+    DevBuf lane_misc;   // kMiscBytes per lane
     // paired batches: the mate-rescue half's own buffers, stream and events
     DevBuf pm_jobs, pm_order, pm_q, pm_t, pm_out, pm_misc, pm_rev;
     DevBuf mate_rev;   // the mate SW reverse-pass list (launch_mate_sw)
@@ -117,6 +120,11 @@ struct fa_ctx {
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t slice_ev[8] = {}, done_ev[8] = {}, jobs_ev = nullptr;
     cudaEvent_t span_ev[8][2] = {};   // sliced rounds: each slice's kernels, start and end
+    // streamed host batches: the slices' validation on their own stream, one event per slice
+    // for its job records uploaded and one for its summary back in pinned host words
+    cudaStream_t prep_stream = nullptr;
+    cudaEvent_t job_ev[8] = {}, info_ev[8] = {};
+    uint32_t *h_slice_info = nullptr;
     // upload slices of pipelined / sliced host batches (0: chosen per batch, auto_slices)
     int slices_single = 0, slices_rounds = 0;
     DevBuf chunk_scratch;
@@ -163,22 +171,29 @@ Misc misc_of(fa_ctx *c) {
                 (uint32_t *)(b + 24), (uint32_t *)(b + 64), (uint32_t *)(b + 192), (uint32_t *)(b + 40)};
 }
 
-// The second lane of sliced host batches: its misc block shares the status word and the
-// cell counter of the first (misc_of), the rest is its own.
-int ensure_lane1(fa_ctx *c, Misc *m1) {
-    if (!c->lane1) {
-        FA_CUDA(cudaStreamCreateWithFlags(&c->lane1, cudaStreamNonBlocking));
-        for (int k = 0; k < 2; ++k) {
-            FA_CUDA(cudaStreamCreateWithFlags(&c->aux1[k], cudaStreamNonBlocking));
-            FA_CUDA(cudaEventCreateWithFlags(&c->join_ev1[k], cudaEventDisableTiming));
-            FA_CUDA(cudaEventCreateWithFlags(&c->lane_ev[k], cudaEventDisableTiming));
+// Lanes 1 .. nl-1 of sliced and streamed host batches: their misc blocks share the status
+// word and the cell counter of lane 0 (misc_of), the rest is their own; ms[0] is lane 0's.
+int ensure_lanes(fa_ctx *c, int nl, Misc *ms) {
+    if (!c->lane_ev[0])
+        for (auto &e : c->lane_ev) FA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    FA_CUDA(c->lane_misc.ensure(kMiscBytes * fa_ctx::kLanes));
+    ms[0] = misc_of(c);
+    for (int l = 1; l < nl; ++l) {
+        if (!c->lane_s[l]) {
+            FA_CUDA(cudaStreamCreateWithFlags(&c->lane_s[l], cudaStreamNonBlocking));
+            for (int k = 0; k < 2; ++k) {
+                FA_CUDA(cudaStreamCreateWithFlags(&c->lane_aux[l][k], cudaStreamNonBlocking));
+                FA_CUDA(cudaEventCreateWithFlags(&c->lane_join[l][k], cudaEventDisableTiming));
+            }
+            FA_CUDA(cudaEventCreateWithFlags(&c->lane_fork[l], cudaEventDisableTiming));
+            FA_CUDA(cudaEventCreateWithFlags(&c->lane_done[l], cudaEventDisableTiming));
         }
-        FA_CUDA(cudaEventCreateWithFlags(&c->fork_ev1, cudaEventDisableTiming));
+        ms[l] = misc_at(c->lane_misc.as<char>() + l * kMiscBytes, c->misc.as<char>());
     }
-    FA_CUDA(c->misc1.ensure(kMiscBytes));
-    *m1 = misc_at(c->misc1.as<char>(), c->misc.as<char>());
     return FA_OK;
 }
+
+cudaStream_t lane_stream(fa_ctx *c, int l) { return l ? c->lane_s[l] : c->stream; }
 
 int ensure_aux_streams(fa_ctx *c) {
     if (c->fork_ev) return FA_OK;
@@ -197,6 +212,29 @@ int ensure_aux_streams(fa_ctx *c) {
 // certificate (flag bit 1), which only the int32 kernel implements.
 using Choice = fa_ctx::Choice;
 
+// The two-row kernel's overflow list (`words` entries), its count and the persistent
+// launch's job counter.
+struct OvfRes {
+    uint32_t *list, *count, *work;
+    size_t words;
+};
+
+cudaError_t launch_ext_res(fa_ctx *c, Choice kc, const fa_job *d_jobs, const uint32_t *d_order, uint32_t n,
+                           const uint32_t *d_n, const SeqBuf &d_q, const SeqBuf &d_t, const ExtParams &kp, int qcap,
+                           const int32_t *d_w_try, fa_ext_result *d_out, uint8_t *d_clamped, bool cert,
+                           uint32_t *d_cells_job, unsigned long long *d_cells, uint32_t *d_status, cudaStream_t s,
+                           const OvfRes &r) {
+    if (kc.kernel == FA_KERNEL_ROWS2 && !cert && ext_rows2_eligible(kp, qcap) &&
+        ext_rows2_smem_bytes(qcap, kc.tpb, 0) <= c->smem_optin && r.words >= (size_t)n && r.list)
+        return launch_ext_rows2(d_jobs, d_order, n, nullptr, d_n, d_q, d_t, kp, qcap, 0, false, d_w_try, d_out,
+                                d_clamped, d_cells_job, d_cells, d_status, r.list, r.count, s, kc.tpb, r.work);
+    if (kc.kernel == FA_KERNEL_INT16X2 && ext_pair_eligible(kp) && !cert && !d_q.packed)
+        return launch_ext_pair(d_jobs, d_order, n, d_n, d_q, d_t, kp, qcap, d_w_try, d_out, d_clamped,
+                               d_cells_job, d_cells, d_status, s);
+    return launch_ext_packed(d_jobs, d_order, n, nullptr, d_n, d_q, d_t, kp, qcap, 0, d_w_try, d_out, d_clamped,
+                             cert, d_cells_job, d_cells, d_status, s, kc.tpb);
+}
+
 // `slot` (0-2) picks the two-row kernel's overflow list and count, so launches that may run
 // concurrently use different ones; each list holds a third of the buffer.
 cudaError_t launch_ext(fa_ctx *c, Choice kc, const fa_job *d_jobs, const uint32_t *d_order, uint32_t n,
@@ -205,16 +243,11 @@ cudaError_t launch_ext(fa_ctx *c, Choice kc, const fa_job *d_jobs, const uint32_
                        uint32_t *d_cells_job, unsigned long long *d_cells, uint32_t *d_status, cudaStream_t s,
                        int slot = 0) {
     const size_t ovf_words = c->ovf.cap / (3 * sizeof(uint32_t));
-    if (kc.kernel == FA_KERNEL_ROWS2 && !cert && ext_rows2_eligible(kp, qcap) &&
-        ext_rows2_smem_bytes(qcap, kc.tpb, 0) <= c->smem_optin && ovf_words >= (size_t)n && c->misc.p)
-        return launch_ext_rows2(d_jobs, d_order, n, nullptr, d_n, d_q, d_t, kp, qcap, 0, false, d_w_try, d_out,
-                                d_clamped, d_cells_job, d_cells, d_status, c->ovf.as<uint32_t>() + slot * ovf_words,
-                                misc_of(c).ovf_n + slot, s, kc.tpb, misc_of(c).work + slot);
-    if (kc.kernel == FA_KERNEL_INT16X2 && ext_pair_eligible(kp) && !cert && !d_q.packed)
-        return launch_ext_pair(d_jobs, d_order, n, d_n, d_q, d_t, kp, qcap, d_w_try, d_out, d_clamped,
-                               d_cells_job, d_cells, d_status, s);
-    return launch_ext_packed(d_jobs, d_order, n, nullptr, d_n, d_q, d_t, kp, qcap, 0, d_w_try, d_out, d_clamped,
-                             cert, d_cells_job, d_cells, d_status, s, kc.tpb);
+    const OvfRes r{c->misc.p ? c->ovf.as<uint32_t>() + slot * ovf_words : nullptr,
+                   c->misc.p ? misc_of(c).ovf_n + slot : nullptr, c->misc.p ? misc_of(c).work + slot : nullptr,
+                   ovf_words};
+    return launch_ext_res(c, kc, d_jobs, d_order, n, d_n, d_q, d_t, kp, qcap, d_w_try, d_out, d_clamped, cert,
+                          d_cells_job, d_cells, d_status, s, r);
 }
 
 // Kernel launches one launch_ext call makes (the two-row kernel adds its overflow pass).
@@ -230,13 +263,22 @@ uint32_t ext_kernels_of(fa_ctx *c, Choice kc, const ExtParams &kp, int qcap) {
 // kernel with 64 or 128 and the two-jobs-per-thread kernel -- runs twice on the first
 // (longest) 393,216 jobs of the call's order, and the fastest is kept for that pair.  All
 // candidates give identical results.
+// The kernel a fixed setting names (false for FA_KERNEL_AUTO).
+bool fixed_choice(fa_ctx *c, Choice *kc) {
+    if (c->kernel == FA_KERNEL_INT16X2) *kc = Choice{FA_KERNEL_INT16X2, kPairThreads};
+    else if (c->kernel == FA_KERNEL_INT32) *kc = Choice{FA_KERNEL_INT32, c->threads};
+    else if (c->kernel == FA_KERNEL_ROWS2) *kc = Choice{FA_KERNEL_ROWS2, c->threads == 128 ? 128 : 64};
+    else return false;
+    c->last_choice = *kc;
+    return true;
+}
+
 Choice resolve_choice(fa_ctx *c, const ExtParams &kp, const fa_job *d_jobs, const uint32_t *d_order, uint32_t n,
                       const SeqBuf &d_q, const SeqBuf &d_t, int qcap, int band, fa_ext_result *d_out,
                       uint32_t *d_status, cudaStream_t s, int *rc) {
     *rc = FA_OK;
-    if (c->kernel == FA_KERNEL_INT16X2) return c->last_choice = Choice{FA_KERNEL_INT16X2, kPairThreads};
-    if (c->kernel == FA_KERNEL_INT32) return c->last_choice = Choice{FA_KERNEL_INT32, c->threads};
-    if (c->kernel == FA_KERNEL_ROWS2) return c->last_choice = Choice{FA_KERNEL_ROWS2, c->threads == 128 ? 128 : 64};
+    Choice fixed;
+    if (fixed_choice(c, &fixed)) return fixed;
     const std::tuple<int, int, int> key{(qcap + 31) / 32, band, (int)d_q.packed};
     auto it = c->tuned.find(key);
     if (it != c->tuned.end()) return c->last_choice = it->second;
@@ -288,6 +330,32 @@ Choice resolve_choice(fa_ctx *c, const ExtParams &kp, const fa_job *d_jobs, cons
     return c->last_choice = best;
 }
 
+// The kernel of one slice of a streamed host batch: the fixed one, the one tuned for the
+// slice's (capacity class, band, form), or one tuned for the same band and form -- the
+// nearest capacity class at or above the slice's, else the nearest below (every choice is
+// exact; launch_ext falls back where a kernel does not fit).  False when nothing is tuned
+// for that band and form.
+bool slice_choice(fa_ctx *c, int qcap, int band, bool packed, Choice *kc) {
+    if (fixed_choice(c, kc)) return true;
+    const int cls = (qcap + 31) / 32;
+    auto it = c->tuned.find({cls, band, (int)packed});
+    if (it == c->tuned.end()) {
+        int best = -1;
+        for (auto jt = c->tuned.begin(); jt != c->tuned.end(); ++jt) {
+            if (std::get<1>(jt->first) != band || std::get<2>(jt->first) != (int)packed) continue;
+            const int kcls = std::get<0>(jt->first);
+            const int d = kcls >= cls ? kcls - cls : 1000 + cls - kcls;
+            if (best < 0 || d < best) {
+                best = d;
+                it = jt;
+            }
+        }
+        if (best < 0) return false;
+    }
+    *kc = c->last_choice = it->second;
+    return true;
+}
+
 // One learned round over a band-partitioned list: configured-band and wide narrow jobs
 // in the full-row kernel, bands 13-24 in the 64-column ring kernel, bands <= 12 in the
 // 32-column ring kernel; the three run concurrently on forked streams.  Their launches are
@@ -301,24 +369,25 @@ int launch_learned_round(fa_ctx *c, const fa_job *d_jobs, const uint32_t *d_list
                          const SeqBuf &d_q, const SeqBuf &d_t, const ExtParams &kp, int qcap,
                          const int32_t *d_w_cur, fa_ext_result *d_out, uint8_t *d_flags, bool cert, Misc &m,
                          cudaStream_t s, uint32_t *launches, int lane = 0, size_t ovf_off = 0,
-                         bool narrow_only = false) {
+                         bool narrow_only = false, uint32_t *cells_job = nullptr) {
     // narrow_only: the configured-band bucket is left out (its jobs run in a later round)
     if (int rc = ensure_aux_streams(c)) return rc;
-    cudaStream_t *aux = lane ? c->aux1 : c->aux;
-    cudaEvent_t fork_ev = lane ? c->fork_ev1 : c->fork_ev, *join_ev = lane ? c->join_ev1 : c->join_ev;
+    cudaStream_t *aux = lane ? c->lane_aux[lane] : c->aux;
+    cudaEvent_t fork_ev = lane ? c->lane_fork[lane] : c->fork_ev, *join_ev = lane ? c->lane_join[lane] : c->join_ev;
     const uint32_t *g = m.group_bounds;
     const bool rows2 = c->kernel != FA_KERNEL_INT32 && ext_rows2_eligible(kp, qcap) &&
                        ext_rows2_smem_bytes(qcap, 64, 0) <= c->smem_optin &&
                        c->ovf.cap >= sizeof(uint32_t) * (ovf_off + 3 * (size_t)n_max);
+    if (!cells_job) cells_job = c->cells_job.as<uint32_t>();
     auto group = [&](int k, int ring, cudaStream_t st) -> cudaError_t {
         // narrow_only: group 0 starts after the configured-band bucket (g[3])
         const uint32_t *first = k == 0 ? (narrow_only ? g + 3 : nullptr) : g + k - 1;
         if (rows2)
             return launch_ext_rows2(d_jobs, d_list, n_max, first, g + k, d_q, d_t, kp, qcap, ring, cert, d_w_cur,
-                                    d_out, d_flags, c->cells_job.as<uint32_t>(), m.cells, m.status,
+                                    d_out, d_flags, cells_job, m.cells, m.status,
                                     c->ovf.as<uint32_t>() + ovf_off + (size_t)k * n_max, m.ovf_n + k, st, 64);
         return launch_ext_packed(d_jobs, d_list, n_max, first, g + k, d_q, d_t, kp, qcap, ring, d_w_cur, d_out,
-                                 d_flags, cert, c->cells_job.as<uint32_t>(), m.cells, m.status, st);
+                                 d_flags, cert, cells_job, m.cells, m.status, st);
     };
     FA_CUDA(cudaEventRecord(fork_ev, s));
     FA_CUDA(group(0, 0, s));
@@ -805,12 +874,17 @@ constexpr int kSlices = 8;   // at most this many upload slices (the event and s
 constexpr uint32_t kPipeMinJobs = 32768;
 
 int ensure_pipe_streams(fa_ctx *c) {
-    FA_CUDA(c->chunk_scratch.ensure(chunk_scratch_bytes(kSlices)));
+    FA_CUDA(c->chunk_scratch.ensure(std::max(chunk_scratch_bytes(kSlices),
+                                             sizeof(uint32_t) * slice_scratch_words(kSlices))));
     if (!c->copy_stream) {
         FA_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
         for (auto &e : c->slice_ev) FA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         for (auto &e : c->done_ev) FA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         FA_CUDA(cudaEventCreateWithFlags(&c->jobs_ev, cudaEventDisableTiming));
+        FA_CUDA(cudaStreamCreateWithFlags(&c->prep_stream, cudaStreamNonBlocking));
+        for (auto &e : c->job_ev) FA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        for (auto &e : c->info_ev) FA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        FA_CUDA(cudaMallocHost(&c->h_slice_info, sizeof(uint32_t) * kSliceInfoWords * kSlices));
         for (int k = 0; k < kSlices; ++k) {
             FA_CUDA(cudaEventCreate(&c->span_ev[k][0]));
             FA_CUDA(cudaEventCreate(&c->span_ev[k][1]));
@@ -821,15 +895,15 @@ int ensure_pipe_streams(fa_ctx *c) {
 
 // graded slices (for 8: 1, 1, 2, 4, 6, 6, 6, 6 thirty-seconds of each buffer): the first jobs
 // start after a small upload, and the uploads, faster than the kernels, stay ahead
+constexpr int kGradedCum[kSlices + 1][kSlices] = {
+    {32}, {32}, {4, 32}, {2, 10, 32}, {1, 4, 14, 32}, {1, 2, 6, 16, 32}, {1, 2, 4, 10, 20, 32},
+    {1, 2, 4, 8, 14, 22, 32}, {1, 2, 4, 8, 14, 20, 26, 32}};
 ChunkEnds graded_ends(const HostSeq &q, const HostSeq &t, int ns) {
     ChunkEnds ends;
-    static constexpr int kCum[kSlices + 1][kSlices] = {
-        {32}, {32}, {4, 32}, {2, 10, 32}, {1, 4, 14, 32}, {1, 2, 6, 16, 32}, {1, 2, 4, 10, 20, 32},
-        {1, 2, 4, 8, 14, 22, 32}, {1, 2, 4, 8, 14, 20, 26, 32}};
     static_assert(kSlices <= kMaxChunks, "slice count");
     for (int k = 0; k < ns; ++k) {
-        ends.q[k] = k == ns - 1 ? q.nbytes : q.nbytes / 32 * kCum[ns][k];
-        ends.t[k] = k == ns - 1 ? t.nbytes : t.nbytes / 32 * kCum[ns][k];
+        ends.q[k] = k == ns - 1 ? q.nbytes : q.nbytes / 32 * kGradedCum[ns][k];
+        ends.t[k] = k == ns - 1 ? t.nbytes : t.nbytes / 32 * kGradedCum[ns][k];
     }
     ends.shift = q.packed ? 2 : 0;
     return ends;
@@ -894,6 +968,12 @@ bool slices_in_order(const uint32_t *h_info, uint32_t n, int ns) {
 // then cost more than the overlap gains past two slices.  A single-band batch runs one kernel
 // per slice and takes eight either way.
 int auto_slices(bool rounds, const HostSeq &hq) { return rounds && hq.packed ? 2 : 8; }
+
+// Slice counts of streamed host batches when the caller set none (measured on 1M 151-bp
+// jobs): a retry policy's slices each end in a few long retries, so three; a single-band
+// batch runs one kernel per slice and follows its uploads more closely with more slices,
+// six for packed bases and eight for byte codes (four times the bytes to upload).
+int auto_slices_streamed(bool rounds, const HostSeq &hq) { return rounds ? 3 : hq.packed ? 6 : 8; }
 
 int ext_batch_pipelined(fa_ctx *c, const ExtParams &kp, const fa_job *jobs, uint32_t n, const HostSeq &hq,
                         const HostSeq &ht, fa_ext_result *out, fa_ext_stats *stats) {
@@ -973,6 +1053,30 @@ int ext_batch_pipelined(fa_ctx *c, const ExtParams &kp, const fa_job *jobs, uint
     if (int rc = finish_ext(c, nullptr, n, s, stats, nullptr, launches, 0, false)) return rc;
     FA_CUDA(cudaStreamSynchronize(s));
     return FA_OK;
+}
+
+// Busy time of the slices whose bits `spans` sets: the union of their [start, end] events.
+float busy_ms(fa_ctx *c, int spans, int ns) {
+    int k0 = 0;
+    while (!(spans & (1 << k0))) ++k0;
+    std::vector<std::pair<float, float>> iv;
+    for (int k = k0; k < ns; ++k) {
+        if (!(spans & (1 << k))) continue;
+        float a = 0.f, b = 0.f;
+        cudaEventElapsedTime(&a, c->span_ev[k0][0], c->span_ev[k][0]);
+        cudaEventElapsedTime(&b, c->span_ev[k0][0], c->span_ev[k][1]);
+        iv.push_back({a, b});
+    }
+    std::sort(iv.begin(), iv.end());
+    float busy = 0.f, lo = iv[0].first, hi = iv[0].second;
+    for (size_t i = 1; i < iv.size(); ++i) {
+        if (iv[i].first > hi) {
+            busy += hi - lo;
+            lo = iv[i].first;
+        }
+        hi = std::max(hi, iv[i].second);
+    }
+    return busy + (hi - lo);
 }
 
 // A retry policy's rounds on a host batch whose jobs address their sequences in job order
@@ -1055,18 +1159,19 @@ int ext_batch_sliced(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, const
     // Alternate slices run on two lanes, so one slice's last, longest jobs overlap the next
     // slice's start: lane 0 is the main stream with misc_of(c), lane 1 its own stream, band-
     // group streams and counters (status, cells and the retry list's count are shared).
-    Misc m1;
-    if (int rc = ensure_lane1(c, &m1)) return rc;
+    Misc ms[2];
+    if (int rc = ensure_lanes(c, 2, ms)) return rc;
+    Misc &m1 = ms[1];
     uint32_t max_cnt = 0;
     for (int k = 0; k < ns; ++k) max_cnt = std::max(max_cnt, h_info[4 + k + 1] - h_info[4 + k]);
     FA_CUDA(c->ovf.ensure(sizeof(uint32_t) * std::max<size_t>(3 * (size_t)n, 6 * (size_t)max_cnt)));
-    FA_CUDA(cudaMemsetAsync(c->misc1.p, 0, 64, s));
+    FA_CUDA(cudaMemsetAsync(c->lane_misc.as<char>() + kMiscBytes, 0, 64, s));
     FA_CUDA(cudaEventRecord(c->lane_ev[0], s));
-    FA_CUDA(cudaStreamWaitEvent(c->lane1, c->lane_ev[0], 0));
+    FA_CUDA(cudaStreamWaitEvent(c->lane_s[1], c->lane_ev[0], 0));
     for (int k = 0; k < ns; ++k) {
         const uint32_t b = h_info[4 + k], cnt = h_info[4 + k + 1] - b;
         const int lane = k & 1;
-        cudaStream_t ls = lane ? c->lane1 : s;
+        cudaStream_t ls = lane ? c->lane_s[1] : s;
         Misc &ml = lane ? m1 : m;
         FA_CUDA(cudaStreamWaitEvent(ls, c->slice_ev[k], 0));
         if (cnt == 0) continue;
@@ -1112,7 +1217,7 @@ int ext_batch_sliced(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, const
         FA_CUDA(cudaEventRecord(c->span_ev[k][1], ls));
         spans |= 1 << k;
     }
-    FA_CUDA(cudaEventRecord(c->lane_ev[1], c->lane1));
+    FA_CUDA(cudaEventRecord(c->lane_ev[1], c->lane_s[1]));
     FA_CUDA(cudaStreamWaitEvent(s, c->lane_ev[1], 0));
     FA_CUDA(cudaEventRecord(c->ev0, s));
     std::vector<std::pair<uint32_t, int>> segs{{n, max_q}};
@@ -1124,28 +1229,323 @@ int ext_batch_sliced(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, const
     FA_CUDA(cudaMemcpyAsync(out, c->out.p, sizeof(fa_ext_result) * (size_t)n, cudaMemcpyDeviceToHost, s));
     if (w_first_out && model) FA_CUDA(cudaMemcpyAsync(w_first_out, d_wf, 4ull * n, cudaMemcpyDeviceToHost, s));
     if (int rc = finish_ext(c, pol, n, s, stats, w_final, launches, retries, true)) return rc;
-    if (stats && spans) {   // busy time: the union of the slices' spans, plus the later rounds
-        int k0 = 0;
-        while (!(spans & (1 << k0))) ++k0;
-        std::vector<std::pair<float, float>> iv;
-        for (int k = k0; k < ns; ++k) {
-            if (!(spans & (1 << k))) continue;
-            float a = 0.f, b = 0.f;
-            cudaEventElapsedTime(&a, c->span_ev[k0][0], c->span_ev[k][0]);
-            cudaEventElapsedTime(&b, c->span_ev[k0][0], c->span_ev[k][1]);
-            iv.push_back({a, b});
-        }
-        std::sort(iv.begin(), iv.end());
-        float busy = 0.f, lo = iv[0].first, hi = iv[0].second;
-        for (size_t i = 1; i < iv.size(); ++i) {
-            if (iv[i].first > hi) {
-                busy += hi - lo;
-                lo = iv[i].first;
-            }
-            hi = std::max(hi, iv[i].second);
-        }
-        stats->kernel_ms += busy + (hi - lo);
+    if (stats && spans) stats->kernel_ms += busy_ms(c, spans, ns);   // plus the later rounds
+    FA_CUDA(cudaStreamSynchronize(s));
+    return FA_OK;
+}
+
+// Streamed host batch (every policy): the batch is cut by job index into graded slices, and
+// each slice's job records, hints or first bands, and the query and target bytes up to the
+// slice's resident ends go up back to back on the copy stream, so the first slice starts
+// after a small upload.  A prep stream validates each slice as its records arrive and
+// orders its resident jobs by query length; the host reads the slice's summary (longest
+// query, widest band, listed jobs), then enqueues the slice's whole work on one of two lanes
+// -- band prediction, policy set-up, the first round and every retry round over the slice's
+// own retry lists, with device-side counts -- and, into a pinned `out`, the copy of its
+// results, which runs while the other lane computes.  Results, bands, statistics and errors
+// are those of the serial path (a rejected batch reports its first bad job through the
+// host-side checks).  *done = false when the jobs do not address their sequences in job
+// order (nothing run, or, when a slice finds a job whose sequences lie past its resident
+// ends, everything drained): the caller takes another path.
+struct SliceSummary {
+    uint32_t status, bad, max_q, band, listed, away;
+};
+
+bool jobs_in_sequence_order(const fa_job *jobs, uint32_t n) {
+    constexpr uint32_t kProbes = 64;
+    uint64_t q = 0, t = 0;
+    for (uint32_t p = 0; p < kProbes; ++p) {
+        const fa_job &j = jobs[(uint64_t)p * (n - 1) / (kProbes - 1)];
+        if (j.q_off < q || j.t_off < t) return false;
+        q = j.q_off;
+        t = j.t_off;
     }
+    return true;
+}
+
+int ext_batch_streamed(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, const fa_band_model *model,
+                       float margin, const fa_job *jobs, uint32_t n, const HostSeq &hq, const HostSeq &ht,
+                       const fa_band_hint *hints, const int32_t *w_first, fa_ext_result *out, int32_t *w_first_out,
+                       int32_t *w_final, fa_ext_stats *stats, bool *done) {
+    *done = false;
+    const int mode = pol ? pol->mode : FA_POLICY_SINGLE;
+    const bool learned = mode == FA_POLICY_LEARNED;
+    const int ns = mode == FA_POLICY_SINGLE ? (c->slices_single ? c->slices_single : auto_slices_streamed(false, hq))
+                                            : (c->slices_rounds ? c->slices_rounds : auto_slices_streamed(true, hq));
+    if (ns < 2 || ns > kSlices || !jobs_in_sequence_order(jobs, n)) return FA_OK;
+    // slice bounds by job index, and each slice's resident ends (positions) and upload ends
+    // (bytes): the bytes up to the later of the next slice's first sequence and this slice's
+    // last job's end, never fewer than the slice before
+    const uint64_t ppb = hq.packed ? 4 : 1;
+    uint32_t J[kSlices + 1];
+    uint64_t qres[kSlices], tres[kSlices], qend[kSlices], tend[kSlices];
+    J[0] = 0;
+    J[ns] = n;
+    for (int k = 1; k < ns; ++k) J[k] = (uint32_t)((uint64_t)n * kGradedCum[ns][k - 1] / 32);
+    for (int k = 0; k < ns; ++k) {
+        if (k == ns - 1) {
+            qend[k] = hq.nbytes;
+            tend[k] = ht.nbytes;
+        } else {
+            const fa_job &a = jobs[J[k + 1]], &b = jobs[J[k + 1] - 1];
+            const uint64_t eq = std::min<uint64_t>(std::max<uint64_t>(a.q_off, b.q_off + (uint64_t)std::max(b.qlen, 0)), hq.npos);
+            const uint64_t et = std::min<uint64_t>(std::max<uint64_t>(a.t_off, b.t_off + (uint64_t)std::max(b.tlen, 0)), ht.npos);
+            qend[k] = std::min<uint64_t>((eq + ppb - 1) / ppb, hq.nbytes);
+            tend[k] = std::min<uint64_t>((et + ppb - 1) / ppb, ht.nbytes);
+        }
+        if (k) {
+            qend[k] = std::max(qend[k], qend[k - 1]);
+            tend[k] = std::max(tend[k], tend[k - 1]);
+        }
+        qres[k] = std::min<uint64_t>(qend[k] * ppb, hq.npos);
+        tres[k] = std::min<uint64_t>(tend[k] * ppb, ht.npos);
+    }
+    uint32_t max_cnt = 0;
+    for (int k = 0; k < ns; ++k) max_cnt = std::max(max_cnt, J[k + 1] - J[k]);
+    if (int rc = ensure_ext_buffers(c, n, 0, 0)) return rc;
+    if (int rc = ensure_seq_buffers(c, hq, ht)) return rc;
+    if (mode != FA_POLICY_SINGLE)
+        if (int rc = ensure_policy_buffers(c, n)) return rc;
+    if (int rc = ensure_pipe_streams(c)) return rc;
+    // one lane per slice, up to kLanes (slice k on lane k % nl), each with its own counters
+    // and a third-of-its-slice overflow region per band group
+    const int nl = std::min(ns, fa_ctx::kLanes);
+    Misc ms[fa_ctx::kLanes];
+    if (int rc = ensure_lanes(c, nl, ms)) return rc;
+    FA_CUDA(c->ovf.ensure(sizeof(uint32_t) * std::max<size_t>(3 * (size_t)n, 3 * (size_t)nl * max_cnt)));
+    float *d_x = nullptr;
+    fa_band_hint *d_h = nullptr;
+    std::vector<__nv_bfloat16> wbf;
+    float mean[16], sd[16];
+    if (model) {
+        FA_CUDA(c->feat.ensure(sizeof(float) * 16 * (size_t)n + sizeof(fa_band_hint) * (size_t)n));
+        FA_CUDA(c->wbf.ensure(sizeof(__nv_bfloat16) * FA_BAND_NPARAMS));
+        d_x = c->feat.as<float>();
+        d_h = hints ? reinterpret_cast<fa_band_hint *>(d_x + 16 * (size_t)n) : nullptr;
+        band_model_export(model, wbf, mean, sd);
+    }
+    cudaStream_t s = c->stream, cs = c->copy_stream, ps = c->prep_stream;
+    Misc &m = ms[0];
+    FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
+    FA_CUDA(cudaMemsetAsync(c->lane_misc.p, 0, kMiscBytes * fa_ctx::kLanes, s));
+    FA_CUDA(cudaEventRecord(c->fork_ev, s));
+    FA_CUDA(cudaStreamWaitEvent(cs, c->fork_ev, 0));
+    FA_CUDA(cudaStreamWaitEvent(ps, c->fork_ev, 0));
+    for (int l = 1; l < nl; ++l) FA_CUDA(cudaStreamWaitEvent(c->lane_s[l], c->fork_ev, 0));
+    // uploads: N runs and model weights, then per slice its records and its bytes
+    if (int rc = upload_runs(c, hq, ht, cs)) return rc;
+    if (model)
+        FA_CUDA(cudaMemcpyAsync(c->wbf.p, wbf.data(), sizeof(__nv_bfloat16) * FA_BAND_NPARAMS,
+                                cudaMemcpyHostToDevice, cs));
+    fa_job *d_jobs = c->jobs.as<fa_job>();
+    int32_t *d_wf = mode != FA_POLICY_SINGLE ? c->w_first.as<int32_t>() : nullptr;
+    for (int k = 0; k < ns; ++k) {
+        const uint32_t j0 = J[k], cnt = J[k + 1] - j0;
+        FA_CUDA(cudaMemcpyAsync(d_jobs + j0, jobs + j0, sizeof(fa_job) * (size_t)cnt, cudaMemcpyHostToDevice, cs));
+        if (d_h) FA_CUDA(cudaMemcpyAsync(d_h + j0, hints + j0, sizeof(fa_band_hint) * cnt, cudaMemcpyHostToDevice, cs));
+        if (learned && !model)
+            FA_CUDA(cudaMemcpyAsync(d_wf + j0, w_first + j0, 4ull * cnt, cudaMemcpyHostToDevice, cs));
+        FA_CUDA(cudaEventRecord(c->job_ev[k], cs));
+        const uint64_t q0 = k ? qend[k - 1] : 0, t0 = k ? tend[k - 1] : 0;
+        if (qend[k] > q0)
+            FA_CUDA(cudaMemcpyAsync(c->qseq.as<uint8_t>() + q0, hq.p + q0, qend[k] - q0, cudaMemcpyHostToDevice, cs));
+        if (tend[k] > t0)
+            FA_CUDA(cudaMemcpyAsync(c->tseq.as<uint8_t>() + t0, ht.p + t0, tend[k] - t0, cudaMemcpyHostToDevice, cs));
+        FA_CUDA(cudaEventRecord(c->slice_ev[k], cs));
+    }
+    // per slice: validation and length order as its records arrive, the summary to the host
+    uint32_t *scratch = c->chunk_scratch.as<uint32_t>();
+    uint32_t *order = c->order.as<uint32_t>();
+    const size_t sw = slice_scratch_words(1);
+    for (int k = 0; k < ns; ++k) {
+        const uint32_t j0 = J[k], cnt = J[k + 1] - j0;
+        FA_CUDA(cudaStreamWaitEvent(ps, c->job_ev[k], 0));
+        FA_CUDA(launch_slice_prep(d_jobs + j0, cnt, hq.npos, ht.npos, qres[k], tres[k], kp.max_score,
+                                  (kp.flags & FA_PARAM_H0_ZERO) ? 0 : 1, packed_qcap_limit(c->smem_optin),
+                                  scratch + k * sw, order + j0, ps));
+        FA_CUDA(cudaMemcpyAsync(c->h_slice_info + k * kSliceInfoWords, scratch + k * sw + 3 * (FA_MAX_QLEN + 1),
+                                sizeof(uint32_t) * kSliceInfoWords, cudaMemcpyDeviceToHost, ps));
+        FA_CUDA(cudaEventRecord(c->info_ev[k], ps));
+    }
+    auto drain = [&]() {
+        cudaStreamSynchronize(cs);
+        cudaStreamSynchronize(ps);
+        for (int l = 0; l < nl; ++l) cudaStreamSynchronize(lane_stream(c, l));
+    };
+    auto summary = [&](int k, SliceSummary *f) -> int {
+        FA_CUDA(cudaEventSynchronize(c->info_ev[k]));
+        const uint32_t *w = c->h_slice_info + k * kSliceInfoWords;
+        *f = SliceSummary{w[0], w[1], w[2], w[3], w[5], w[6]};
+        return FA_OK;
+    };
+    // a slice with a bad job ends the call with that job's error; one with a job whose
+    // sequences lie past its resident ends hands the batch to another path
+    auto refuse = [&](int k, const SliceSummary &f) -> int {
+        drain();
+        if (f.status) {
+            const uint32_t bad = J[k] + (f.bad < J[k + 1] - J[k] ? f.bad : 0);
+            int mq = 0;
+            const int rc = check_jobs(jobs + bad, 1, hq.npos, ht.npos, kp, packed_qcap_limit(c->smem_optin), &mq);
+            if (rc) return fail(rc, "job %u: %s", bad, g_err.c_str() + (g_err.compare(0, 7, "job 0: ") == 0 ? 7 : 0));
+            return fail(FA_ERR_ARG, "job %u is invalid", bad);
+        }
+        return FA_OK;   // *done stays false
+    };
+    SliceSummary f[kSlices];
+    if (int rc = summary(0, &f[0])) return rc;
+    if (f[0].status || f[0].away) return refuse(0, f[0]);
+    // the kernel of every slice: fixed, or tuned; the first call for a (band, form) waits for
+    // the whole batch and tunes on its largest slice
+    Choice kc;
+    if (!slice_choice(c, (int)f[0].max_q, (int)f[0].band, hq.packed, &kc)) {
+        int kt = 0;
+        for (int k = 1; k < ns; ++k) {
+            if (int rc = summary(k, &f[k])) return rc;
+            if (f[k].status || f[k].away) return refuse(k, f[k]);
+            if (f[k].listed > f[kt].listed) kt = k;
+        }
+        FA_CUDA(cudaStreamWaitEvent(s, c->slice_ev[ns - 1], 0));
+        FA_CUDA(cudaStreamWaitEvent(s, c->info_ev[ns - 1], 0));
+        int rc0 = FA_OK;
+        kc = resolve_choice(c, kp, d_jobs + J[kt], order + J[kt], f[kt].listed, c->cq, c->ct, (int)f[kt].max_q,
+                       (int)f[kt].band, c->out.as<fa_ext_result>() + J[kt], m.status, s, &rc0);
+        if (rc0) {
+            drain();
+            return rc0;
+        }
+        FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));   // the tuner's runs leave their cells and status
+        FA_CUDA(cudaEventRecord(c->lane_ev[0], s));
+        for (int l = 1; l < nl; ++l) FA_CUDA(cudaStreamWaitEvent(c->lane_s[l], c->lane_ev[0], 0));
+    }
+    // results back slice by slice only into page-locked memory (a copy into pageable memory
+    // would hold the host thread until the slice had run)
+    auto pinned = [](const void *p) {
+        cudaPointerAttributes pa;
+        const bool r = p && cudaPointerGetAttributes(&pa, p) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+        cudaGetLastError();
+        return r;
+    };
+    const bool early = pinned(out);
+    const bool wf_early = model && pinned(w_first_out);
+    PolicyState st{c->w_cur.as<int32_t>(), c->prev.as<int32_t>(), c->kk.as<int32_t>(),
+                   c->w_final.as<int32_t>(), c->tries.as<int32_t>(), c->missed.as<uint8_t>()};
+    uint8_t *d_flags = learned ? c->clamped.as<uint8_t>() : nullptr;
+    const bool cert = learned && (pol->judge & FA_JUDGE_BOUND);
+    const bool once = learned && (pol->judge & FA_JUDGE_ONCE);
+    const int narrow_rounds = learned && (pol->judge & FA_JUDGE_HINT) && (pol->judge & FA_JUDGE_BOUND) ? 2 : 1;
+    const int max_tries = mode != FA_POLICY_SINGLE ? std::max(1, pol->max_tries) : 1;
+    fa_ext_result *d_out = c->out.as<fa_ext_result>();
+    uint32_t launches = 0;
+    int spans = 0;
+    for (int k = 0; k < ns; ++k) {
+        if (k)
+            if (int rc = summary(k, &f[k])) return rc;
+        if (f[k].status || f[k].away) return refuse(k, f[k]);
+        const int lane = k % nl;
+        cudaStream_t ls = lane_stream(c, lane);
+        Misc &ml = ms[lane];
+        const uint32_t j0 = J[k], cnt = J[k + 1] - j0, listed = f[k].listed;
+        const int qcap = (int)f[k].max_q;
+        Choice kk = kc;
+        slice_choice(c, qcap, (int)f[k].band, hq.packed, &kk);
+        FA_CUDA(cudaStreamWaitEvent(ls, c->slice_ev[k], 0));
+        FA_CUDA(cudaStreamWaitEvent(ls, c->info_ev[k], 0));
+        FA_CUDA(cudaEventRecord(c->span_ev[k][0], ls));
+        spans |= 1 << k;
+        // the slice's views of the per-job arrays (its order and lists hold local indices)
+        const fa_job *jb = d_jobs + j0;
+        const uint32_t *ord = order + j0;
+        fa_ext_result *o = d_out + j0;
+        uint32_t *cj = c->cells_job.as<uint32_t>() + j0;
+        const OvfRes ovr{c->ovf.as<uint32_t>() + (size_t)lane * 3 * max_cnt, ml.ovf_n, ml.work, 3 * (size_t)max_cnt};
+        if (mode == FA_POLICY_SINGLE) {
+            FA_CUDA(launch_ext_res(c, kk, jb, ord, listed, nullptr, c->cq, c->ct, kp, qcap, nullptr, o, nullptr, false,
+                                   cj, ml.cells, ml.status, ls, ovr));
+            launches += ext_kernels_of(c, kk, kp, qcap);
+        } else {
+            const PolicyState sl{st.w_cur + j0, st.prev + j0, st.k + j0, st.w_final + j0, st.tries + j0,
+                                 st.missed + j0};
+            uint8_t *fl = d_flags ? d_flags + j0 : nullptr;
+            int32_t *wf = d_wf + j0;
+            if (model) {
+                FA_CUDA(launch_band_features(jb, cnt, c->cq, c->ct, d_h ? d_h + j0 : nullptr, kp.max_score,
+                                             d_x + 16 * (size_t)j0, ls));
+                FA_CUDA(launch_band_predict(c->wbf.as<__nv_bfloat16>(), mean, sd, d_x + 16 * (size_t)j0, jb, cnt,
+                                            margin, pol->w_min, nullptr, wf, ls));
+                launches += 2;
+            }
+            FA_CUDA(launch_policy_init(jb, cnt, learned ? wf : nullptr, pol->w_min, learned, sl, ls));
+            ++launches;
+            uint32_t *list = c->list_a.as<uint32_t>() + j0, *next = c->list_b.as<uint32_t>() + j0;
+            uint32_t *lcnt = ml.cnt_a, *ncnt = ml.cnt_b;
+            uint32_t *part = c->part_n.as<uint32_t>() + j0;
+            uint32_t *blk = c->part_blk[lane].as<uint32_t>();
+            const size_t ovf_off = (size_t)lane * 3 * max_cnt;
+            FA_CUDA(cudaMemsetAsync(lcnt, 0, 4, ls));
+            // first round: the narrow bands (the configured-band bucket joins the retry list),
+            // or the policy's first band
+            if (learned) {
+                FA_CUDA(launch_band_partition(jb, ord, nullptr, listed, sl.w_cur, part, ml.bucket_hist, blk,
+                                              ml.group_bounds, ls));
+                if (int rc = launch_learned_round(c, jb, part, listed, c->cq, c->ct, kp, qcap, sl.w_cur, o, fl, cert,
+                                                  ml, ls, &launches, lane, ovf_off, true, cj))
+                    return rc;
+                FA_CUDA(launch_list_append(part, ml.group_bounds + 3, listed, list, lcnt, ls));
+                FA_CUDA(launch_policy_step(jb, part, ml.group_bounds + 3, ml.group_bounds + 2, listed, o, fl, sl,
+                                           max_tries, pol->judge, list, lcnt, ls));
+                launches += 5;   // partition (3), list append, policy step
+            } else {
+                FA_CUDA(launch_ext_res(c, kk, jb, ord, listed, nullptr, c->cq, c->ct, kp, qcap, sl.w_cur, o, fl,
+                                       false, cj, ml.cells, ml.status, ls, ovr));
+                launches += ext_kernels_of(c, kk, kp, qcap);
+                FA_CUDA(launch_policy_step(jb, ord, nullptr, nullptr, listed, o, fl, sl, max_tries, pol->judge, list,
+                                           lcnt, ls));
+                ++launches;
+            }
+            // the later rounds over the slice's retry list, a fixed number with device-side
+            // counts (an empty round's launches leave at once)
+            const int rounds = max_rounds_of(pol, (int)f[k].band);
+            for (int r = 1; r < rounds; ++r) {
+                const bool cert_r = cert && !(once && r >= narrow_rounds);
+                if (learned && cert_r) {
+                    FA_CUDA(launch_band_partition(jb, list, lcnt, listed, sl.w_cur, part, ml.bucket_hist, blk,
+                                                  ml.group_bounds, ls));
+                    if (int rc = launch_learned_round(c, jb, part, listed, c->cq, c->ct, kp, qcap, sl.w_cur, o, fl,
+                                                      true, ml, ls, &launches, lane, ovf_off, false, cj))
+                        return rc;
+                    launches += 3;   // partition
+                } else {
+                    FA_CUDA(launch_ext_res(c, kk, jb, list, listed, lcnt, c->cq, c->ct, kp, qcap, sl.w_cur, o, fl,
+                                           cert_r, cj, ml.cells, ml.status, ls, ovr));
+                    launches += cert_r ? 1u : ext_kernels_of(c, kk, kp, qcap);
+                }
+                FA_CUDA(cudaMemsetAsync(ncnt, 0, 4, ls));
+                FA_CUDA(launch_policy_step(jb, list, nullptr, lcnt, listed, o, fl, sl, max_tries, pol->judge, next,
+                                           ncnt, ls));
+                ++launches;
+                std::swap(list, next);
+                std::swap(lcnt, ncnt);
+            }
+        }
+        FA_CUDA(cudaEventRecord(c->span_ev[k][1], ls));
+        if (early) FA_CUDA(cudaMemcpyAsync(out + j0, o, sizeof(fa_ext_result) * cnt, cudaMemcpyDeviceToHost, ls));
+        if (wf_early) FA_CUDA(cudaMemcpyAsync(w_first_out + j0, d_wf + j0, 4ull * cnt, cudaMemcpyDeviceToHost, ls));
+    }
+    for (int l = 1; l < nl; ++l) {
+        FA_CUDA(cudaEventRecord(c->lane_done[l], c->lane_s[l]));
+        FA_CUDA(cudaStreamWaitEvent(s, c->lane_done[l], 0));
+    }
+    FA_CUDA(cudaEventRecord(c->ev0, s));
+    FA_CUDA(cudaEventRecord(c->ev1, s));
+    if (!early) FA_CUDA(cudaMemcpyAsync(out, d_out, sizeof(fa_ext_result) * (size_t)n, cudaMemcpyDeviceToHost, s));
+    if (w_first_out && model && !wf_early)
+        FA_CUDA(cudaMemcpyAsync(w_first_out, d_wf, 4ull * n, cudaMemcpyDeviceToHost, s));
+    *done = true;
+    if (int rc = finish_ext(c, pol, n, s, stats, w_final, launches, 0, mode != FA_POLICY_SINGLE)) {
+        drain();
+        return rc;
+    }
+    if (stats) stats->kernel_ms = busy_ms(c, spans, ns);
     FA_CUDA(cudaStreamSynchronize(s));
     return FA_OK;
 }
@@ -1161,6 +1561,18 @@ int ext_batch_host(fa_ctx *c, const fa_params *p, const fa_policy *pol, const fa
             stats->total_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
     };
     const int mode = pol ? pol->mode : FA_POLICY_SINGLE;
+    if (!c->graph && n >= kPipeMinJobs && (mode == FA_POLICY_SINGLE ? c->slices_single : c->slices_rounds) != 1) {
+        bool done = false;
+        int rc = ext_batch_streamed(c, kp, pol, nullptr, 0.f, jobs, n, hq, ht, nullptr, w_first, out, nullptr,
+                                    w_final, stats, &done);
+        if (rc) return rc;
+        if (done) {
+            if (w_final && mode == FA_POLICY_SINGLE)
+                for (uint32_t i = 0; i < n; ++i) w_final[i] = jobs[i].w;
+            total();
+            return FA_OK;
+        }
+    }
     if (mode == FA_POLICY_SINGLE && !c->graph && n >= kPipeMinJobs && c->slices_single != 1) {
         int rc = ext_batch_pipelined(c, kp, jobs, n, hq, ht, out, stats);
         if (rc) return rc;
@@ -1224,8 +1636,15 @@ int ext_learned_host(fa_ctx *c, const fa_params *p, const fa_policy *pol, const 
     };
     if (!c->graph && n >= kPipeMinJobs && c->slices_rounds != 1) {
         bool done = false;
-        int rc = ext_batch_sliced(c, kp, pol, model, margin, jobs, n, hq, ht, hints, nullptr, out, w_first_out,
-                                  w_final, stats, &done);
+        int rc = ext_batch_streamed(c, kp, pol, model, margin, jobs, n, hq, ht, hints, nullptr, out, w_first_out,
+                                    w_final, stats, &done);
+        if (rc) return rc;
+        if (done) {
+            total();
+            return FA_OK;
+        }
+        rc = ext_batch_sliced(c, kp, pol, model, margin, jobs, n, hq, ht, hints, nullptr, out, w_first_out,
+                              w_final, stats, &done);
         if (rc) return rc;
         if (done) {
             total();
@@ -1541,27 +1960,32 @@ void fa_ctx_destroy(fa_ctx *c) {
     for (DevBuf *b : {&c->jobs, &c->order, &c->qseq, &c->tseq, &c->out, &c->clamped, &c->cells_job,
                       &c->misc, &c->w_first, &c->w_cur, &c->prev, &c->kk, &c->w_final, &c->tries,
                       &c->missed, &c->list_a, &c->list_b, &c->hist, &c->feat, &c->wbf, &c->part_n,
-                      &c->part_w, &c->ovf, &c->reg_in, &c->reg_out, &c->col_in, &c->col_plan, &c->col_out, &c->col_pk, &c->part_blk[0], &c->part_blk[1],
+                      &c->part_w, &c->ovf, &c->reg_in, &c->reg_out, &c->col_in, &c->col_plan, &c->col_out, &c->col_pk, &c->part_blk[0], &c->part_blk[1], &c->part_blk[2], &c->part_blk[3],
                       &c->cg_in, &c->cg_scratch, &c->cg_out, &c->mc_in, &c->mc_plan, &c->mc_out, &c->is_buf,
                       &c->qruns, &c->truns})
         b->release();
     for (auto &pr : c->span_ev)
         for (auto &e : pr)
             if (e) cudaEventDestroy(e);
-    for (int k = 0; k < 2; ++k) {
-        if (c->aux1[k]) cudaStreamDestroy(c->aux1[k]);
-        if (c->join_ev1[k]) cudaEventDestroy(c->join_ev1[k]);
-        if (c->lane_ev[k]) cudaEventDestroy(c->lane_ev[k]);
+    for (int l = 1; l < fa_ctx::kLanes; ++l) {
+        for (int k = 0; k < 2; ++k) {
+            if (c->lane_aux[l][k]) cudaStreamDestroy(c->lane_aux[l][k]);
+            if (c->lane_join[l][k]) cudaEventDestroy(c->lane_join[l][k]);
+        }
+        if (c->lane_fork[l]) cudaEventDestroy(c->lane_fork[l]);
+        if (c->lane_done[l]) cudaEventDestroy(c->lane_done[l]);
     }
-    if (c->fork_ev1) cudaEventDestroy(c->fork_ev1);
+    for (auto &e : c->lane_ev)
+        if (e) cudaEventDestroy(e);
     for (DevBuf *b : {&c->pm_jobs, &c->pm_order, &c->pm_q, &c->pm_t, &c->pm_out, &c->pm_misc, &c->pm_rev,
                       &c->mate_rev, &c->mate_pk})
         b->release();
     if (c->pm_ev0) cudaEventDestroy(c->pm_ev0);
     if (c->pm_ev1) cudaEventDestroy(c->pm_ev1);
     if (c->pm_stream) cudaStreamDestroy(c->pm_stream);
-    if (c->lane1) cudaStreamDestroy(c->lane1);
-    c->misc1.release();
+    for (int l = 1; l < fa_ctx::kLanes; ++l)
+        if (c->lane_s[l]) cudaStreamDestroy(c->lane_s[l]);
+    c->lane_misc.release();
     for (int k = 0; k < 2; ++k) {
         if (c->join_ev[k]) cudaEventDestroy(c->join_ev[k]);
         if (c->aux[k]) cudaStreamDestroy(c->aux[k]);
@@ -1573,6 +1997,12 @@ void fa_ctx_destroy(fa_ctx *c) {
     for (auto &e : c->done_ev)
         if (e) cudaEventDestroy(e);
     if (c->jobs_ev) cudaEventDestroy(c->jobs_ev);
+    for (int k = 0; k < kSlices; ++k) {
+        if (c->job_ev[k]) cudaEventDestroy(c->job_ev[k]);
+        if (c->info_ev[k]) cudaEventDestroy(c->info_ev[k]);
+    }
+    if (c->prep_stream) cudaStreamDestroy(c->prep_stream);
+    if (c->h_slice_info) cudaFreeHost(c->h_slice_info);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     c->chunk_scratch.release();
     if (c->kev0) cudaEventDestroy(c->kev0);

@@ -135,6 +135,16 @@ cudaError_t launch_chunk_prep(const fa_job *d_jobs, uint32_t n, uint64_t qbytes,
                               cudaStream_t s);
 cudaError_t launch_chunk_scatter(const fa_job *d_jobs, uint32_t n, const ChunkEnds &ends, int nchunks,
                                  uint32_t *d_scratch, uint32_t *d_order, cudaStream_t s);
+// Streamed host batches (order_kernel.cu): one slice of jobs validated against the whole
+// buffers (qpos / tpos positions) and the slice's resident ends (q_res / t_res), the valid
+// resident jobs ordered longest query first into d_order (local indices).  Scratch of
+// slice_scratch_words(1) words; its last 8 words: {status, first bad job, longest query,
+// widest band, 0, listed jobs, jobs not resident, 0}.
+size_t slice_scratch_words(int nslices);
+constexpr int kSliceInfoWords = 8;
+cudaError_t launch_slice_prep(const fa_job *d_jobs, uint32_t n, uint64_t qpos, uint64_t tpos, uint64_t q_res,
+                              uint64_t t_res, int max_score, int h0_min, int qcap_limit, uint32_t *d_scratch,
+                              uint32_t *d_order, cudaStream_t s);
 cudaError_t launch_qlen_hist(const fa_job *d_jobs, uint32_t n, uint32_t *d_hist, int sm_count, cudaStream_t s);
 cudaError_t launch_qlen_scatter(const fa_job *d_jobs, uint32_t n, uint32_t *d_cursor, uint32_t *d_order,
                                 cudaStream_t s);

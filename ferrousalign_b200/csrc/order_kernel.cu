@@ -277,3 +277,106 @@ cudaError_t launch_chunk_scatter(const fa_job *d_jobs, uint32_t n, const ChunkEn
 }
 
 }  // namespace fa
+
+namespace fa {
+
+// ------------------------------------------------------------- streamed host batches
+// A streamed host batch is cut by job index: slice k is jobs [J_k, J_k+1), uploaded with
+// the sequence bytes up to its resident ends, so a slice can start as soon as its own
+// records and bytes have arrived.  Per slice, on the device: every job validated (the rules
+// of chunk_prep_kernel), a valid job whose query or target ends past the resident ends
+// counted as not resident (the host then takes the batch to another path), the rest
+// ordered longest query first (local indices).  info = {status, first bad job (local),
+// longest query, widest band, 0, listed jobs, jobs not resident, 0}.
+
+// bin of a job in the slice's length order, or -1 (invalid, or not resident); *st gets the
+// job's status bits
+__device__ __forceinline__ int slice_bin(const fa_job &jb, uint64_t qpos, uint64_t tpos, uint64_t q_res,
+                                         uint64_t t_res, int max_score, int h0_min, int qcap_limit, uint32_t *st,
+                                         bool *resident) {
+    uint32_t s = 0;
+    if (jb.qlen <= 0 || jb.tlen < 0 || jb.h0 < h0_min) s |= ST_ARG;
+    else if (jb.qlen > FA_MAX_QLEN || jb.tlen > FA_MAX_TLEN) s |= ST_CAPACITY;
+    else if (jb.q_off + (uint64_t)jb.qlen > qpos || jb.t_off + (uint64_t)jb.tlen > tpos) s |= ST_ARG;
+    else if ((int64_t)jb.h0 + (int64_t)max_score * jb.qlen > kPackedHMax || jb.qlen > qcap_limit)
+        s |= ST_CAPACITY;
+    *st = s;
+    *resident = jb.q_off + (uint64_t)jb.qlen <= q_res && jb.t_off + (uint64_t)jb.tlen <= t_res;
+    return s || !*resident ? -1 : FA_MAX_QLEN - jb.qlen;
+}
+
+__global__ void slice_prep_kernel(const fa_job *__restrict__ jobs, uint32_t n, uint64_t qpos, uint64_t tpos,
+                                  uint64_t q_res, uint64_t t_res, int max_score, int h0_min, int qcap_limit,
+                                  uint32_t *__restrict__ hist, uint32_t *__restrict__ info)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    int bin = -1, qlen = 0, band = 0;
+    bool away = false;
+    if (i < n) {
+        const fa_job jb = jobs[i];
+        uint32_t st = 0;
+        bool resident = true;
+        bin = slice_bin(jb, qpos, tpos, q_res, t_res, max_score, h0_min, qcap_limit, &st, &resident);
+        if (st) {
+            atomicOr(&info[0], st);
+            atomicMin(&info[1], i);
+        } else {
+            qlen = jb.qlen;
+            band = max(jb.w, 0);
+            away = !resident;
+        }
+    }
+    const unsigned aw = __ballot_sync(0xffffffffu, away);
+    if ((threadIdx.x & 31) == 0 && aw) atomicAdd(&info[6], (uint32_t)__popc(aw));
+    const int mq = __reduce_max_sync(0xffffffffu, qlen);
+    if ((threadIdx.x & 31) == 0 && mq > 0) atomicMax(&info[2], (uint32_t)mq);
+    const int mw = __reduce_max_sync(0xffffffffu, band);
+    if ((threadIdx.x & 31) == 0 && mw > 0) atomicMax(&info[3], (uint32_t)mw);
+    const unsigned peers = __match_any_sync(0xffffffffu, bin);
+    if (bin >= 0 && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&hist[bin], (uint32_t)__popc(peers));
+}
+
+__global__ void slice_scatter_kernel(const fa_job *__restrict__ jobs, uint32_t n, uint64_t qpos, uint64_t tpos,
+                                     uint64_t q_res, uint64_t t_res, int max_score, int h0_min, int qcap_limit,
+                                     const uint32_t *__restrict__ base, uint32_t *__restrict__ cursor,
+                                     uint32_t *__restrict__ order)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    int bin = -1;
+    if (i < n) {
+        uint32_t st = 0;
+        bool resident = true;
+        bin = slice_bin(jobs[i], qpos, tpos, q_res, t_res, max_score, h0_min, qcap_limit, &st, &resident);
+    }
+    const unsigned peers = __match_any_sync(0xffffffffu, bin);
+    if (bin < 0) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    uint32_t pos = 0;
+    if (lane == leader) pos = atomicAdd(&cursor[bin], (uint32_t)__popc(peers));
+    pos = __shfl_sync(peers, pos, leader);
+    order[base[bin] + pos + __popc(peers & ((1u << lane) - 1u))] = i;
+}
+
+size_t slice_scratch_words(int nslices) { return (size_t)nslices * (3 * (size_t)kChunkBins + 8); }
+
+// scratch (slice_scratch_words(1) words): hist | base | cursor (kChunkBins each) | info[8]
+cudaError_t launch_slice_prep(const fa_job *d_jobs, uint32_t n, uint64_t qpos, uint64_t tpos, uint64_t q_res,
+                              uint64_t t_res, int max_score, int h0_min, int qcap_limit, uint32_t *d_scratch,
+                              uint32_t *d_order, cudaStream_t s)
+{
+    uint32_t *hist = d_scratch, *base = d_scratch + kChunkBins, *cursor = d_scratch + 2 * kChunkBins;
+    uint32_t *info = d_scratch + 3 * kChunkBins;
+    cudaError_t e = cudaMemsetAsync(d_scratch, 0, sizeof(uint32_t) * slice_scratch_words(1), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(info + 1, 0xFF, sizeof(uint32_t), s);   // first bad job: none
+    if (e != cudaSuccess || n == 0) return e;
+    slice_prep_kernel<<<(n + 255) / 256, 256, 0, s>>>(d_jobs, n, qpos, tpos, q_res, t_res, max_score, h0_min,
+                                                      qcap_limit, hist, info);
+    // one bin group: bounds = {0, listed jobs} at info[4], info[5]
+    chunk_scan_kernel<<<1, 1024, 0, s>>>(hist, kChunkBins, base, 1, info + 4);
+    slice_scatter_kernel<<<(n + 255) / 256, 256, 0, s>>>(d_jobs, n, qpos, tpos, q_res, t_res, max_score, h0_min,
+                                                         qcap_limit, base, cursor, d_order);
+    return cudaGetLastError();
+}
+
+}  // namespace fa
