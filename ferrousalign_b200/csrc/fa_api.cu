@@ -970,10 +970,19 @@ bool slices_in_order(const uint32_t *h_info, uint32_t n, int ns) {
 int auto_slices(bool rounds, const HostSeq &hq) { return rounds && hq.packed ? 2 : 8; }
 
 // Slice counts of streamed host batches when the caller set none (measured on 1M 151-bp
-// jobs): a retry policy's slices each end in a few long retries, so three; a single-band
-// batch runs one kernel per slice and follows its uploads more closely with more slices,
-// six for packed bases and eight for byte codes (four times the bytes to upload).
-int auto_slices_streamed(bool rounds, const HostSeq &hq) { return rounds ? 3 : hq.packed ? 6 : 8; }
+// jobs): byte codes are upload-bound (four times the bytes), so eight slices follow the
+// uploads; packed retry-policy slices each end in a few long retries, so three; packed
+// single-band slices run one kernel each, six.
+int auto_slices_streamed(bool rounds, const HostSeq &hq) { return !hq.packed ? 8 : rounds ? 3 : 6; }
+
+// Whether a host batch streams.  A learned batch of byte codes does not: its uploads end
+// after its kernels would, and a streamed slice's rounds -- the narrow round, then the
+// retries at the configured band, about 1 ms of one-thread-per-job latency whatever the
+// slice's size -- would follow the last upload; the pipelined path runs the retries of all
+// slices once after the last slice instead (9.9 against 10.0-12.1 ms per 1M jobs).
+bool streams(const fa_policy *pol, const HostSeq &hq) {
+    return hq.packed || !pol || pol->mode != FA_POLICY_LEARNED;
+}
 
 int ext_batch_pipelined(fa_ctx *c, const ExtParams &kp, const fa_job *jobs, uint32_t n, const HostSeq &hq,
                         const HostSeq &ht, fa_ext_result *out, fa_ext_stats *stats) {
@@ -1561,7 +1570,8 @@ int ext_batch_host(fa_ctx *c, const fa_params *p, const fa_policy *pol, const fa
             stats->total_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
     };
     const int mode = pol ? pol->mode : FA_POLICY_SINGLE;
-    if (!c->graph && n >= kPipeMinJobs && (mode == FA_POLICY_SINGLE ? c->slices_single : c->slices_rounds) != 1) {
+    if (!c->graph && n >= kPipeMinJobs && (mode == FA_POLICY_SINGLE ? c->slices_single : c->slices_rounds) != 1 &&
+        streams(pol, hq)) {
         bool done = false;
         int rc = ext_batch_streamed(c, kp, pol, nullptr, 0.f, jobs, n, hq, ht, nullptr, w_first, out, nullptr,
                                     w_final, stats, &done);
@@ -1636,12 +1646,15 @@ int ext_learned_host(fa_ctx *c, const fa_params *p, const fa_policy *pol, const 
     };
     if (!c->graph && n >= kPipeMinJobs && c->slices_rounds != 1) {
         bool done = false;
-        int rc = ext_batch_streamed(c, kp, pol, model, margin, jobs, n, hq, ht, hints, nullptr, out, w_first_out,
+        int rc = FA_OK;
+        if (streams(pol, hq)) {
+            rc = ext_batch_streamed(c, kp, pol, model, margin, jobs, n, hq, ht, hints, nullptr, out, w_first_out,
                                     w_final, stats, &done);
-        if (rc) return rc;
-        if (done) {
-            total();
-            return FA_OK;
+            if (rc) return rc;
+            if (done) {
+                total();
+                return FA_OK;
+            }
         }
         rc = ext_batch_sliced(c, kp, pol, model, margin, jobs, n, hq, ht, hints, nullptr, out, w_first_out,
                               w_final, stats, &done);
