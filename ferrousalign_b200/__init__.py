@@ -14,7 +14,8 @@ from .mate_rescue import (MATE_RESCUE_SCORING_MATRIX, Kswr, MateRescueJob, MateR
                           mate_sw_batch_packed,
                           mate_xtra)
 from .region import chain_seed_table, merge_scores_to_regions, region_opts  # noqa: F401
-from .collect import (CollectedJobs, collect_extension_jobs, collect_extension_jobs_packed,  # noqa: F401
+from .hostbuf import HostBuffers  # noqa: F401
+from .collect import (CollectBuffers, CollectedJobs, collect_extension_jobs, collect_extension_jobs_packed,  # noqa: F401
                       collect_opts, pack_reference)
 from .cigar import CigarBatch, infer_band_width, scalar_banded_swa_batch  # noqa: F401
 from .pair_batch import pair_batch  # noqa: F401

@@ -105,6 +105,7 @@ SIGNATURES = {
     "fa_ctx_set_kernel": (C.c_int, [_P, C.c_int]),
     "fa_ctx_set_graph": (C.c_int, [_P, C.c_int]),
     "fa_ctx_set_slices": (C.c_int, [_P, C.c_int, C.c_int]),
+    "fa_ctx_set_reference": (C.c_int, [_P, _P, C.c_uint64]),
     "fa_ctx_set_threads": (C.c_int, [_P, C.c_int]),
     "fa_ctx_kernel_choice": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int, _P, _P, _P,
                                        C.POINTER(C.c_int)]),
@@ -234,9 +235,18 @@ class Context:
 
     def set_slices(self, single_band: int = 0, policy_rounds: int = 0) -> None:
         """Upload slices of large host batches (2..8; 1 uploads the whole batch before one run
-        of the kernels; 0 keeps the current value, -1 restores the default: 8, or 2 for the
-        rounds of a packed batch)."""
+        of the kernels; 0 keeps the current value, -1 restores the defaults: 8 for byte codes,
+        3 for the rounds of a packed batch, 6 for a packed single-band batch)."""
         check(load().fa_ctx_set_slices(self.handle, single_band, policy_rounds))
+
+    def set_reference(self, pac, l_pac: int = 0) -> None:
+        """Keep the 2-bit packed reference (`pac`, l_pac bases) on the device: collection calls
+        given pac=None then read it instead of uploading it again.  None drops it."""
+        if pac is None:
+            check(load().fa_ctx_set_reference(self.handle, None, 0))
+            return
+        pac = np.ascontiguousarray(pac, np.uint8)
+        check(load().fa_ctx_set_reference(self.handle, pac.ctypes.data, int(l_pac)))
 
     def set_graph(self, enable: bool) -> None:
         """Run policy / learned batches as one recorded CUDA graph per batch shape."""

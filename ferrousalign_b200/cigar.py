@@ -11,6 +11,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _native as N
+from .hostbuf import HostBuffers, out_array
 
 CIGAR_JOB_DT = N.CIGAR_JOB_DT
 CIGAR_RESULT_DT = N.CIGAR_RESULT_DT
@@ -59,10 +60,12 @@ class CigarBatch:
 
 
 def scalar_banded_swa_batch(params: np.ndarray, jobs: np.ndarray, qseq: np.ndarray, tseq: np.ndarray,
-                            ctx: N.Context | None = None, packed: bool = True) -> CigarBatch:
+                            ctx: N.Context | None = None, packed: bool = True,
+                            bufs: HostBuffers | None = None) -> CigarBatch:
     """scalar_banded_swa for every job (CIGAR_JOB_DT: offsets, lengths, band, h0).  packed:
     the CIGAR words come back back to back (fa_cigar_batch_packed), otherwise in slots of
-    qlen + tlen + 2 words per job (fa_cigar_batch)."""
+    qlen + tlen + 2 words per job (fa_cigar_batch).  With `bufs` the outputs land in those
+    reusable (page-locked) buffers and the batch views them."""
     lib = N.load()
     ctx = ctx or N.default_context()
     jobs = np.ascontiguousarray(jobs, CIGAR_JOB_DT)
@@ -74,13 +77,13 @@ def scalar_banded_swa_batch(params: np.ndarray, jobs: np.ndarray, qseq: np.ndarr
     cig_off = np.concatenate([[0], np.cumsum(q + t + 2)])
     ref_off = np.concatenate([[0], np.cumsum(t)])
     qry_off = np.concatenate([[0], np.cumsum(q)])
-    res = np.zeros(n, CIGAR_RESULT_DT)
-    ra = np.empty(max(int(ref_off[-1]), 1), np.uint8)
-    qa = np.empty(max(int(qry_off[-1]), 1), np.uint8)
+    res = out_array(bufs, "res", n, CIGAR_RESULT_DT, zero=True)
+    ra = out_array(bufs, "ref_al", max(int(ref_off[-1]), 1), np.uint8)
+    qa = out_array(bufs, "qry_al", max(int(qry_off[-1]), 1), np.uint8)
     if packed:
         # capacity for every slot, of which only the used words' pages are ever touched
-        cig = np.empty(max(int(cig_off[-1]), 1), np.uint32)
-        first = np.zeros(max(n, 1), np.uint64)
+        cig = out_array(bufs, "cigar", max(int(cig_off[-1]), 1), np.uint32)
+        first = out_array(bufs, "first", max(n, 1), np.uint64, zero=True)
         if n:
             N.check(lib.fa_cigar_batch_packed(ctx.handle, N.ptr(params), N.ptr(jobs), n, N.ptr(qseq), len(qseq),
                                               N.ptr(tseq), len(tseq), N.ptr(res), N.ptr(cig), len(cig),

@@ -13,6 +13,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _native as N
+from .hostbuf import HostBuffers, capacity, out_array
 
 CHAIN_DT = N.CHAIN_DT
 SEED_DT = N.SEED_DT
@@ -40,6 +41,11 @@ def pack_reference(codes: np.ndarray) -> tuple[np.ndarray, int]:
     return pac.astype(np.uint8), n
 
 
+# Reusable output buffers of the collection calls (hostbuf.HostBuffers).
+CollectBuffers = HostBuffers
+_out = out_array
+
+
 @dataclass
 class CollectedJobs:
     left_jobs: np.ndarray      # JOB_DT, the reference's left batch order
@@ -53,11 +59,14 @@ class CollectedJobs:
 
 def collect_extension_jobs(pac: np.ndarray, l_pac: int, reads: np.ndarray, read_off: np.ndarray,
                            chains: np.ndarray, seeds: np.ndarray, opts: np.ndarray | None = None,
-                           ctx: N.Context | None = None) -> CollectedJobs:
+                           ctx: N.Context | None = None, bufs: HostBuffers | None = None) -> CollectedJobs:
+    """fa_collect_ext_jobs.  pac=None reads the reference the context keeps
+    (Context.set_reference).  With `bufs` the outputs land in those reusable (page-locked)
+    buffers and the result views them; without, in fresh arrays."""
     lib = N.load()
     ctx = ctx or N.default_context()
     opts = collect_opts() if opts is None else opts
-    pac = np.ascontiguousarray(pac, np.uint8)
+    pac = None if pac is None else np.ascontiguousarray(pac, np.uint8)   # None: the context's resident reference
     reads = np.ascontiguousarray(reads, np.uint8)
     read_off = np.ascontiguousarray(read_off, np.uint64)
     chains = np.ascontiguousarray(chains, CHAIN_DT)
@@ -66,18 +75,21 @@ def collect_extension_jobs(pac: np.ndarray, l_pac: int, reads: np.ndarray, read_
     read_bytes = int(read_off[-1]) if n_reads >= 0 and len(read_off) else 0
     # outputs the library writes in full up to the returned counts: left uninitialised, so
     # only the pages the copies reach are ever touched
-    left = np.empty(n_seeds, N.JOB_DT)
-    right = np.empty(n_seeds, N.JOB_DT)
-    qbuf = np.empty(max(2 * read_bytes, 1), np.uint8)
-    ext = np.empty(n_seeds, N.SEED_EXT_DT)
-    first = np.zeros(n_chains + 1, np.uint32)
-    win = np.zeros((n_chains, 2), np.uint64)
+    left = _out(bufs, "left", n_seeds, N.JOB_DT)
+    right = _out(bufs, "right", n_seeds, N.JOB_DT)
+    qbuf = _out(bufs, "qbuf", max(2 * read_bytes, 1), np.uint8)
+    ext = _out(bufs, "ext", n_seeds, N.SEED_EXT_DT)
+    first = _out(bufs, "first", n_chains + 1, np.uint32)
+    win = _out(bufs, "win", 2 * n_chains, np.uint64).reshape(n_chains, 2)
     counts = np.zeros(1, N.COLLECT_COUNTS_DT)
-    qlen = np.diff(read_off.astype(np.int64))
-    w = int(opts["w"][0])
-    cap = int(2 * (qlen[chains["read"]] + 4 * w + 64).sum()) if n_chains else 0
+    # target capacity: what reused buffers hold (the call reports the length it needs when
+    # that is short), else every chain's widest window
+    cap = capacity(bufs, "tbuf", np.uint8)
+    if cap == 0 and n_chains:
+        qlen = np.diff(read_off.astype(np.int64))
+        cap = int(2 * (qlen[chains["read"]] + 4 * int(opts["w"][0]) + 64).sum())
     for _ in range(2):
-        tbuf = np.empty(max(cap, 1), np.uint8)
+        tbuf = _out(bufs, "tbuf", max(cap, 1), np.uint8)
         rc = lib.fa_collect_ext_jobs(ctx.handle, N.ptr(opts), N.ptr(pac), l_pac, N.ptr(reads), N.ptr(read_off),
                                      n_reads, N.ptr(chains), n_chains, N.ptr(seeds), n_seeds, N.ptr(left),
                                      N.ptr(right), N.ptr(qbuf), N.ptr(tbuf), cap, N.ptr(ext), N.ptr(first),
@@ -94,37 +106,41 @@ def collect_extension_jobs(pac: np.ndarray, l_pac: int, reads: np.ndarray, read_
 
 def collect_extension_jobs_packed(pac: np.ndarray, l_pac: int, reads: np.ndarray, read_off: np.ndarray,
                                   chains: np.ndarray, seeds: np.ndarray, opts: np.ndarray | None = None,
-                                  ctx: N.Context | None = None) -> CollectedJobs:
+                                  ctx: N.Context | None = None, bufs: HostBuffers | None = None) -> CollectedJobs:
     """fa_collect_ext_jobs_packed: the same jobs and seed table, with `qbuf` and `tbuf` as
     2-bit packed buffers (PackedSeq, N runs listed), packed on the device -- ready for
-    extend_batch_packed."""
+    extend_batch_packed.  `bufs` as for collect_extension_jobs."""
     from .packed import PackedSeq
     lib = N.load()
     ctx = ctx or N.default_context()
     opts = collect_opts() if opts is None else opts
-    pac = np.ascontiguousarray(pac, np.uint8)
+    pac = None if pac is None else np.ascontiguousarray(pac, np.uint8)   # None: the context's resident reference
     reads = np.ascontiguousarray(reads, np.uint8)
     read_off = np.ascontiguousarray(read_off, np.uint64)
     chains = np.ascontiguousarray(chains, CHAIN_DT)
     seeds = np.ascontiguousarray(seeds, SEED_DT)
     n_reads, n_chains, n_seeds = len(read_off) - 1, len(chains), len(seeds)
     read_bytes = int(read_off[-1]) if len(read_off) else 0
-    left = np.empty(n_seeds, N.JOB_DT)
-    right = np.empty(n_seeds, N.JOB_DT)
-    qb = np.zeros((2 * read_bytes + 3) // 4 + 4, np.uint8)   # 4 bytes of slack, as pack() leaves
-    ext = np.empty(n_seeds, N.SEED_EXT_DT)
-    first = np.zeros(n_chains + 1, np.uint32)
-    win = np.zeros((n_chains, 2), np.uint64)
+    left = _out(bufs, "left", n_seeds, N.JOB_DT)
+    right = _out(bufs, "right", n_seeds, N.JOB_DT)
+    qb = _out(bufs, "qbuf", (2 * read_bytes + 3) // 4 + 4, np.uint8, zero=True)   # 4 bytes of slack, as pack() leaves
+    ext = _out(bufs, "ext", n_seeds, N.SEED_EXT_DT)
+    first = _out(bufs, "first", n_chains + 1, np.uint32)
+    win = _out(bufs, "win", 2 * n_chains, np.uint64).reshape(n_chains, 2)
     counts = np.zeros(1, N.COLLECT_COUNTS_DT)
     n_runs = np.zeros(2, np.uint64)
-    qlen = np.diff(read_off.astype(np.int64))
-    w = int(opts["w"][0])
-    cap = int(2 * (qlen[chains["read"]] + 4 * w + 64).sum()) if n_chains else 0
-    qcap, tcap = max(1024, 2 * read_bytes // 64), max(1024, cap // 256)
+    # capacities: what reused buffers hold (the call reports what it needs when that is
+    # short), else every chain's widest window and a run per 64 / 256 bases
+    cap = 4 * max(capacity(bufs, "tbuf", np.uint8) - 4, 0)
+    if cap == 0 and n_chains:
+        qlen = np.diff(read_off.astype(np.int64))
+        cap = int(2 * (qlen[chains["read"]] + 4 * int(opts["w"][0]) + 64).sum())
+    qcap = max(1024, 2 * read_bytes // 64, capacity(bufs, "qruns", N.NRUN_DT))
+    tcap = max(1024, cap // 256, capacity(bufs, "truns", N.NRUN_DT))
     for _ in range(3):
-        tb = np.zeros((cap + 3) // 4 + 4, np.uint8)
-        qr = np.empty(qcap, N.NRUN_DT)
-        tr = np.empty(tcap, N.NRUN_DT)
+        tb = _out(bufs, "tbuf", (cap + 3) // 4 + 4, np.uint8, zero=True)
+        qr = _out(bufs, "qruns", qcap, N.NRUN_DT)
+        tr = _out(bufs, "truns", tcap, N.NRUN_DT)
         rc = lib.fa_collect_ext_jobs_packed(ctx.handle, N.ptr(opts), N.ptr(pac), l_pac, N.ptr(reads),
                                             N.ptr(read_off), n_reads, N.ptr(chains), n_chains, N.ptr(seeds),
                                             n_seeds, N.ptr(left), N.ptr(right), N.ptr(qb), N.ptr(qr), qcap,
@@ -137,6 +153,6 @@ def collect_extension_jobs_packed(pac: np.ndarray, l_pac: int, reads: np.ndarray
         N.check(rc)
         break
     c = counts[0]
-    qs = PackedSeq(qb, int(c["qbuf_len"]), qr[:int(n_runs[0])].copy())
-    ts = PackedSeq(tb, int(c["tbuf_len"]), tr[:int(n_runs[1])].copy())
+    qs = PackedSeq(qb[:(int(c["qbuf_len"]) + 3) // 4 + 4], int(c["qbuf_len"]), qr[:int(n_runs[0])].copy())
+    ts = PackedSeq(tb[:(int(c["tbuf_len"]) + 3) // 4 + 4], int(c["tbuf_len"]), tr[:int(n_runs[1])].copy())
     return CollectedJobs(left[:c["n_left"]], right[:c["n_right"]], qs, ts, ext[:c["n_seed_ext"]], first, win)

@@ -44,16 +44,55 @@ namespace {
 constexpr int kCollectThreads = 128;
 constexpr int kScanThreads = 1024;
 
+// The argument rules the reference's slices and windows would panic on
+// (collect_soa.rs:150-209), one thread per read and per chain.  bad[0] gets the smallest
+// r << 8 | code over failing reads, bad[1] the smallest k << 8 | code over failing chains --
+// a chain's code is its first failure in the order the rules are listed: the first failing
+// read, else the first failing chain, is the one a serial check reports.  Codes: 1 read
+// offsets not ascending, 2 read too long, 3 read index out of range, 4 seeds past the seed
+// array, 5 a seed outside its read, 6 a seed outside the reference.
 __global__ void __launch_bounds__(kCollectThreads)
-collect_plan_kernel(fa_collect_opts opt, uint64_t l_pac, const uint64_t *__restrict__ read_off,
+collect_check_kernel(uint64_t l_pac, const uint64_t *__restrict__ read_off, uint32_t n_reads,
+                     const fa_chain *__restrict__ chains, uint32_t n_chains, const fa_seed *__restrict__ seeds,
+                     uint32_t n_seeds, unsigned long long *__restrict__ bad)
+{
+    const uint32_t i = blockIdx.x * kCollectThreads + threadIdx.x;
+    if (i < n_reads) {
+        const uint64_t a = read_off[i], b = read_off[i + 1];
+        const int code = b < a ? 1 : (b - a > (uint64_t)INT32_MAX ? 2 : 0);
+        if (code) atomicMin(&bad[0], (unsigned long long)i << 8 | code);
+    }
+    if (i < n_chains) {
+        const fa_chain ch = chains[i];
+        int code = 0;
+        if (ch.read >= n_reads) {
+            code = 3;
+        } else if ((uint64_t)ch.seed_first + ch.n_seeds > n_seeds) {
+            code = 4;
+        } else if (ch.kept) {
+            const int64_t qlen = (int64_t)(read_off[ch.read + 1] - read_off[ch.read]);
+            for (uint32_t k = 0; k < ch.n_seeds && !code; ++k) {
+                const fa_seed sd = seeds[ch.seed_first + k];
+                if (sd.query_pos < 0 || sd.len < 0 || (int64_t)sd.query_pos + sd.len > qlen) code = 5;
+                else if (sd.ref_pos >= (l_pac << 1) || sd.ref_pos + (uint64_t)sd.len > (l_pac << 1)) code = 6;
+            }
+        }
+        if (code) atomicMin(&bad[1], (unsigned long long)i << 8 | code);
+    }
+}
+
+// A chain whose read or seed range is out of bounds plans nothing (the check above fails
+// the call before anything reads its plan).
+__global__ void __launch_bounds__(kCollectThreads)
+collect_plan_kernel(fa_collect_opts opt, uint64_t l_pac, const uint64_t *__restrict__ read_off, uint32_t n_reads,
                     const fa_chain *__restrict__ chains, uint32_t n_chains, const fa_seed *__restrict__ seeds,
-                    CollectPlan *__restrict__ plan)
+                    uint32_t n_seeds, CollectPlan *__restrict__ plan)
 {
     const uint32_t c = blockIdx.x * kCollectThreads + threadIdx.x;
     if (c >= n_chains) return;
     const fa_chain ch = chains[c];
     CollectPlan pl{};
-    if (ch.kept != 0 && ch.n_seeds > 0) {
+    if (ch.kept != 0 && ch.n_seeds > 0 && ch.read < n_reads && (uint64_t)ch.seed_first + ch.n_seeds <= n_seeds) {
         const int qlen = (int)(read_off[ch.read + 1] - read_off[ch.read]);
         // collect_soa.rs:97-122: the window every seed's extensions can reach
         uint64_t r0 = l_pac << 1, r1 = 0;
@@ -298,12 +337,19 @@ int collect_max_gap(const fa_collect_opts &o, int qlen) { return max_gap(o, qlen
 size_t collect_scan_blocks(uint32_t n_chains) { return (n_chains + kScanThreads - 1) / kScanThreads; }
 
 cudaError_t launch_collect_plan(const fa_collect_opts &opt, uint64_t l_pac, const uint64_t *d_read_off,
-                                const fa_chain *d_chains, uint32_t n_chains, const fa_seed *d_seeds,
-                                CollectPlan *d_plan, ulonglong4 *d_sums, cudaStream_t s)
+                                uint32_t n_reads, const fa_chain *d_chains, uint32_t n_chains, const fa_seed *d_seeds,
+                                uint32_t n_seeds, CollectPlan *d_plan, ulonglong4 *d_sums, unsigned long long *d_bad,
+                                cudaStream_t s)
 {
-    if (n_chains == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(d_bad, 0xFF, 2 * sizeof(unsigned long long), s);
+    if (e != cudaSuccess) return e;
+    const uint32_t nc = n_reads > n_chains ? n_reads : n_chains;
+    if (nc)
+        collect_check_kernel<<<(nc + kCollectThreads - 1) / kCollectThreads, kCollectThreads, 0, s>>>(
+            l_pac, d_read_off, n_reads, d_chains, n_chains, d_seeds, n_seeds, d_bad);
+    if (n_chains == 0) return cudaGetLastError();
     collect_plan_kernel<<<(n_chains + kCollectThreads - 1) / kCollectThreads, kCollectThreads, 0, s>>>(
-        opt, l_pac, d_read_off, d_chains, n_chains, d_seeds, d_plan);
+        opt, l_pac, d_read_off, n_reads, d_chains, n_chains, d_seeds, n_seeds, d_plan);
     return launch_plan_scan(d_plan, n_chains, d_sums, s);
 }
 

@@ -90,6 +90,8 @@ struct fa_ctx {
     DevBuf w_first, w_cur, prev, kk, w_final, tries, missed, list_a, list_b, hist, feat, wbf, part_n, part_w;
     DevBuf part_blk[4];   // band partition scratch (per-block bucket offsets), one per lane
     DevBuf qruns, truns;                // N runs of packed host batches
+    DevBuf ref_pac;                     // the resident packed reference (fa_ctx_set_reference)
+    uint64_t ref_l_pac = 0;
     // the sequences of the current host call on the device (byte codes or packed bases)
     SeqBuf cq{}, ct{};
     uint32_t last_launches = 0;
@@ -1999,6 +2001,7 @@ void fa_ctx_destroy(fa_ctx *c) {
     for (int l = 1; l < fa_ctx::kLanes; ++l)
         if (c->lane_s[l]) cudaStreamDestroy(c->lane_s[l]);
     c->lane_misc.release();
+    c->ref_pac.release();
     for (int k = 0; k < 2; ++k) {
         if (c->join_ev[k]) cudaEventDestroy(c->join_ev[k]);
         if (c->aux[k]) cudaStreamDestroy(c->aux[k]);
@@ -2380,26 +2383,16 @@ int collect_ext_run(fa_ctx *c, const fa_collect_opts *opt, const uint8_t *pac, u
     if (n_chains && (!chains || !chain_win)) return fail(FA_ERR_ARG, "null chain buffer");
     if (n_reads && (!read_off || !reads)) return fail(FA_ERR_ARG, "null read buffer");
     if (n_seeds && !seeds) return fail(FA_ERR_ARG, "null seed buffer");
-    if (l_pac == 0 || !pac) return fail(FA_ERR_ARG, "empty packed reference");
+    if (l_pac == 0) return fail(FA_ERR_ARG, "empty packed reference");
+    if (!pac && c->ref_l_pac != l_pac)
+        return fail(FA_ERR_ARG, "no resident reference of %llu bases (fa_ctx_set_reference)", (unsigned long long)l_pac);
     if (l_pac > (1ull << 62)) return fail(FA_ERR_ARG, "packed reference too long");
-    // the reference's slices and windows would panic on these (collect_soa.rs:150-209)
+    // the rules the reference's slices and windows would panic on (collect_soa.rs:150-209):
+    // the read offsets here (they size the upload), the chains and seeds on the device
+    // (collect_check_kernel) before anything uses the plans
     for (uint32_t r = 0; r < n_reads; ++r) {
         if (read_off[r + 1] < read_off[r]) return fail(FA_ERR_ARG, "read_off is not ascending");
         if (read_off[r + 1] - read_off[r] > (uint64_t)INT32_MAX) return fail(FA_ERR_ARG, "a read is too long");
-    }
-    for (uint32_t k = 0; k < n_chains; ++k) {
-        const fa_chain &ch = chains[k];
-        if (ch.read >= n_reads) return fail(FA_ERR_ARG, "a chain's read index is out of range");
-        if ((uint64_t)ch.seed_first + ch.n_seeds > n_seeds) return fail(FA_ERR_ARG, "a chain's seeds run past the seed array");
-        if (!ch.kept) continue;
-        const int64_t qlen = (int64_t)(read_off[ch.read + 1] - read_off[ch.read]);
-        for (uint32_t s = 0; s < ch.n_seeds; ++s) {
-            const fa_seed &sd = seeds[ch.seed_first + s];
-            if (sd.query_pos < 0 || sd.len < 0 || (int64_t)sd.query_pos + sd.len > qlen)
-                return fail(FA_ERR_ARG, "a seed lies outside its read");
-            if (sd.ref_pos >= (l_pac << 1) || sd.ref_pos + (uint64_t)sd.len > (l_pac << 1))
-                return fail(FA_ERR_ARG, "a seed lies outside the reference");
-        }
     }
     chain_first[0] = 0;
     if (n_chains == 0) return FA_OK;
@@ -2407,31 +2400,43 @@ int collect_ext_run(fa_ctx *c, const fa_collect_opts *opt, const uint8_t *pac, u
     cudaStream_t s = c->stream;
     auto up16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
     const uint64_t read_bytes = read_off[n_reads];   // reads[0 .. read_off[n_reads]) travel
-    const size_t b_pac = up16((size_t)((l_pac + 3) / 4)), b_reads = up16(read_bytes + 1);
+    const size_t b_pac = pac ? up16((size_t)((l_pac + 3) / 4)) : 0, b_reads = up16(read_bytes + 1);
     const size_t b_off = up16(8ull * (n_reads + 1)), b_chains = up16(sizeof(fa_chain) * n_chains);
     const size_t b_seeds = up16(sizeof(fa_seed) * n_seeds);
     FA_CUDA(c->col_in.ensure(b_pac + b_reads + b_off + b_chains + b_seeds));
     char *in = c->col_in.as<char>();
-    uint8_t *d_pac = reinterpret_cast<uint8_t *>(in);
+    const uint8_t *d_pac = pac ? reinterpret_cast<uint8_t *>(in) : c->ref_pac.as<uint8_t>();
     uint8_t *d_reads = reinterpret_cast<uint8_t *>(in + b_pac);
     uint64_t *d_off = reinterpret_cast<uint64_t *>(in + b_pac + b_reads);
     fa_chain *d_chains = reinterpret_cast<fa_chain *>(in + b_pac + b_reads + b_off);
     fa_seed *d_seeds = reinterpret_cast<fa_seed *>(in + b_pac + b_reads + b_off + b_chains);
-    FA_CUDA(cudaMemcpyAsync(d_pac, pac, (size_t)((l_pac + 3) / 4), cudaMemcpyHostToDevice, s));
+    if (pac) FA_CUDA(cudaMemcpyAsync(in, pac, (size_t)((l_pac + 3) / 4), cudaMemcpyHostToDevice, s));
     if (read_bytes) FA_CUDA(cudaMemcpyAsync(d_reads, reads, read_bytes, cudaMemcpyHostToDevice, s));
     FA_CUDA(cudaMemcpyAsync(d_off, read_off, 8ull * (n_reads + 1), cudaMemcpyHostToDevice, s));
     FA_CUDA(cudaMemcpyAsync(d_chains, chains, sizeof(fa_chain) * n_chains, cudaMemcpyHostToDevice, s));
     if (n_seeds) FA_CUDA(cudaMemcpyAsync(d_seeds, seeds, sizeof(fa_seed) * n_seeds, cudaMemcpyHostToDevice, s));
     const size_t nb = collect_scan_blocks(n_chains);
     const size_t b_plan = up16(sizeof(CollectPlan) * n_chains);
-    FA_CUDA(c->col_plan.ensure(b_plan + sizeof(ulonglong4) * (nb + 1)));
+    FA_CUDA(c->col_plan.ensure(b_plan + sizeof(ulonglong4) * (nb + 2)));
     CollectPlan *d_plan = c->col_plan.as<CollectPlan>();
     ulonglong4 *d_sums = reinterpret_cast<ulonglong4 *>(c->col_plan.as<char>() + b_plan);
+    unsigned long long *d_bad = reinterpret_cast<unsigned long long *>(d_sums + nb + 1);
     if (c->timing) FA_CUDA(cudaEventRecord(c->kev0, s));
-    FA_CUDA(launch_collect_plan(*opt, l_pac, d_off, d_chains, n_chains, d_seeds, d_plan, d_sums, s));
+    FA_CUDA(launch_collect_plan(*opt, l_pac, d_off, n_reads, d_chains, n_chains, d_seeds, n_seeds, d_plan, d_sums,
+                                d_bad, s));
     ulonglong4 tot;
+    unsigned long long bad[2];
     FA_CUDA(cudaMemcpyAsync(&tot, d_sums + nb, sizeof(tot), cudaMemcpyDeviceToHost, s));
+    FA_CUDA(cudaMemcpyAsync(bad, d_bad, sizeof(bad), cudaMemcpyDeviceToHost, s));
     FA_CUDA(cudaStreamSynchronize(s));
+    for (const unsigned long long b : bad) {
+        static const char *const kWhy[] = {"", "read_off is not ascending", "a read is too long",
+                                           "a chain's read index is out of range",
+                                           "a chain's seeds run past the seed array", "a seed lies outside its read",
+                                           "a seed lies outside the reference"};
+        const unsigned code = (unsigned)(b & 0xFF);
+        if (b != ~0ull && code >= 1 && code <= 6) return fail(FA_ERR_ARG, "%s", kWhy[code]);
+    }
     counts->n_left = (uint32_t)tot.y;
     counts->n_right = (uint32_t)tot.z;
     counts->n_seed_ext = (uint32_t)tot.w;
@@ -2475,6 +2480,22 @@ int collect_ext_copy_common(fa_ctx *c, const CollectDev &d, uint32_t n_chains, f
 }  // namespace
 
 extern "C" {
+
+int fa_ctx_set_reference(fa_ctx *c, const uint8_t *pac, uint64_t l_pac) {
+    if (!c) return fail(FA_ERR_ARG, "null context");
+    FA_CUDA(cudaSetDevice(c->device));
+    c->ref_l_pac = 0;
+    if (!pac) {
+        c->ref_pac.release();
+        return FA_OK;
+    }
+    if (l_pac == 0 || l_pac > (1ull << 62)) return fail(FA_ERR_ARG, "empty or oversized packed reference");
+    const size_t b = (size_t)((l_pac + 3) / 4);
+    FA_CUDA(c->ref_pac.ensure(b + 16));
+    FA_CUDA(cudaMemcpy(c->ref_pac.p, pac, b, cudaMemcpyHostToDevice));
+    c->ref_l_pac = l_pac;
+    return FA_OK;
+}
 
 int fa_collect_ext_jobs(fa_ctx *c, const fa_collect_opts *opt, const uint8_t *pac, uint64_t l_pac,
                         const uint8_t *reads, const uint64_t *read_off, uint32_t n_reads,
@@ -2736,7 +2757,9 @@ int fa_collect_mate_jobs(fa_ctx *c, const fa_rescue_opts *opt, const fa_insert_b
     *counts = fa_collect_counts{};
     if (n_cand == 0) return FA_OK;
     if (!cands || !jobs || !info || !read_off || !reads || (n_alns && !alns)) return fail(FA_ERR_ARG, "null buffer");
-    if (l_pac == 0 || !pac || l_pac > (1ull << 62)) return fail(FA_ERR_ARG, "empty or oversized packed reference");
+    if (l_pac == 0 || l_pac > (1ull << 62)) return fail(FA_ERR_ARG, "empty or oversized packed reference");
+    if (!pac && c->ref_l_pac != l_pac)
+        return fail(FA_ERR_ARG, "no resident reference of %llu bases (fa_ctx_set_reference)", (unsigned long long)l_pac);
     if (n_chr == 0 || !chr_off || !chr_len) return fail(FA_ERR_ARG, "no reference sequences");
     for (uint32_t k = 0; k < n_chr; ++k) {
         if (chr_off[k] + chr_len[k] > l_pac) return fail(FA_ERR_ARG, "a reference sequence runs past l_pac");
@@ -2756,21 +2779,22 @@ int fa_collect_mate_jobs(fa_ctx *c, const fa_rescue_opts *opt, const fa_insert_b
     cudaStream_t s = c->stream;
     auto up16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
     const uint64_t read_bytes = read_off[n_reads];
-    const size_t b_pac = up16((size_t)((l_pac + 3) / 4)), b_chr = up16(8ull * n_chr);
+    const size_t b_pac = pac ? up16((size_t)((l_pac + 3) / 4)) : 0, b_chr = up16(8ull * n_chr);
     const size_t b_reads = up16(read_bytes + 1), b_off = up16(8ull * (n_reads + 1));
     const size_t b_alns = up16(sizeof(fa_rescue_aln) * n_alns), b_cands = up16(sizeof(fa_rescue_cand) * n_cand);
     FA_CUDA(c->mc_in.ensure(b_pac + 2 * b_chr + b_reads + b_off + b_alns + b_cands));
     char *in = c->mc_in.as<char>();
     size_t o = 0;
     auto take = [&](size_t b) { char *p = in + o; o += b; return p; };
-    uint8_t *d_pac = reinterpret_cast<uint8_t *>(take(b_pac));
+    uint8_t *d_pac_in = reinterpret_cast<uint8_t *>(take(b_pac));
+    const uint8_t *d_pac = pac ? d_pac_in : c->ref_pac.as<uint8_t>();
     uint64_t *d_coff = reinterpret_cast<uint64_t *>(take(b_chr));
     uint64_t *d_clen = reinterpret_cast<uint64_t *>(take(b_chr));
     uint8_t *d_reads = reinterpret_cast<uint8_t *>(take(b_reads));
     uint64_t *d_off = reinterpret_cast<uint64_t *>(take(b_off));
     fa_rescue_aln *d_alns = reinterpret_cast<fa_rescue_aln *>(take(b_alns));
     fa_rescue_cand *d_cands = reinterpret_cast<fa_rescue_cand *>(take(b_cands));
-    FA_CUDA(cudaMemcpyAsync(d_pac, pac, (size_t)((l_pac + 3) / 4), cudaMemcpyHostToDevice, s));
+    if (pac) FA_CUDA(cudaMemcpyAsync(d_pac_in, pac, (size_t)((l_pac + 3) / 4), cudaMemcpyHostToDevice, s));
     FA_CUDA(cudaMemcpyAsync(d_coff, chr_off, 8ull * n_chr, cudaMemcpyHostToDevice, s));
     FA_CUDA(cudaMemcpyAsync(d_clen, chr_len, 8ull * n_chr, cudaMemcpyHostToDevice, s));
     if (read_bytes) FA_CUDA(cudaMemcpyAsync(d_reads, reads, read_bytes, cudaMemcpyHostToDevice, s));

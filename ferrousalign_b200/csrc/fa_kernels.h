@@ -192,10 +192,13 @@ struct CollectPlan {
 };
 int collect_max_gap(const fa_collect_opts &o, int qlen);
 size_t collect_scan_blocks(uint32_t n_chains);   // entries of the scan's block-sum array, less one
-// plan + scan; d_sums holds collect_scan_blocks(n) + 1 entries, the last one the totals
+// argument check + plan + scan; d_sums holds collect_scan_blocks(n) + 1 entries, the last one
+// the totals; d_bad[2]: the first failing read and chain as index << 8 | code (all ones: none;
+// codes in collect_kernel.cu), known before any plan is used
 cudaError_t launch_collect_plan(const fa_collect_opts &opt, uint64_t l_pac, const uint64_t *d_read_off,
-                                const fa_chain *d_chains, uint32_t n_chains, const fa_seed *d_seeds,
-                                CollectPlan *d_plan, ulonglong4 *d_sums, cudaStream_t s);
+                                uint32_t n_reads, const fa_chain *d_chains, uint32_t n_chains, const fa_seed *d_seeds,
+                                uint32_t n_seeds, CollectPlan *d_plan, ulonglong4 *d_sums, unsigned long long *d_bad,
+                                cudaStream_t s);
 // the scan alone: plan[i].off = exclusive prefix sums of plan[].v; d_sums[collect_scan_blocks(n)]
 // gets the totals
 cudaError_t launch_plan_scan(CollectPlan *d_plan, uint32_t n, ulonglong4 *d_sums, cudaStream_t s);

@@ -14,6 +14,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _native as N
+from .hostbuf import HostBuffers, out_array
 
 MATE_RESCUE_SCORING_MATRIX = np.array([
     1, -4, -4, -4, 0,
@@ -136,13 +137,15 @@ class RescueJobs:
 def collect_rescue_jobs(pac: np.ndarray, l_pac: int, chr_off: np.ndarray, chr_len: np.ndarray,
                         reads: np.ndarray, read_off: np.ndarray, alns: np.ndarray, cands: np.ndarray,
                         bounds: np.ndarray, opts: np.ndarray | None = None,
-                        ctx: N.Context | None = None) -> RescueJobs:
+                        ctx: N.Context | None = None, bufs: HostBuffers | None = None) -> RescueJobs:
     """Mate-rescue jobs of every attempt (RESCUE_CAND_DT) on the GPU; bounds is
-    INSERT_BOUNDS_DT[4] (FF, FR, RF, RR: low, high, failed)."""
+    INSERT_BOUNDS_DT[4] (FF, FR, RF, RR: low, high, failed).  pac=None reads the reference the
+    context keeps (Context.set_reference).  With `bufs` the outputs land in those reusable
+    (page-locked) buffers and the result views them."""
     lib = N.load()
     ctx = ctx or N.default_context()
     opts = rescue_opts() if opts is None else opts
-    pac = np.ascontiguousarray(pac, np.uint8)
+    pac = None if pac is None else np.ascontiguousarray(pac, np.uint8)   # None: the context's resident reference
     chr_off = np.ascontiguousarray(chr_off, np.uint64)
     chr_len = np.ascontiguousarray(chr_len, np.uint64)
     reads = np.ascontiguousarray(reads, np.uint8)
@@ -152,16 +155,16 @@ def collect_rescue_jobs(pac: np.ndarray, l_pac: int, chr_off: np.ndarray, chr_le
     bounds = np.ascontiguousarray(bounds, N.INSERT_BOUNDS_DT)
     n = len(cands)
     # written in full up to the returned counts; uninitialised, so untouched pages stay unmapped
-    jobs = np.empty(4 * n, N.MATE_JOB_DT)
-    info = np.empty(4 * n, N.RESCUE_JOB_INFO_DT)
+    jobs = out_array(bufs, "jobs", 4 * n, N.MATE_JOB_DT)
+    info = out_array(bufs, "info", 4 * n, N.RESCUE_JOB_INFO_DT)
     counts = np.zeros(1, N.COLLECT_COUNTS_DT)
     qlen = np.diff(read_off.astype(np.int64))
     qcap = int(4 * qlen[cands["read"]].sum()) if n else 0
     span = int(np.maximum(bounds["high"] - bounds["low"], 0).max()) if len(bounds) else 0
     tcap = int(4 * (qlen[cands["read"]] + span + 1).sum()) if n else 0
     for _ in range(2):
-        qbuf = np.empty(max(qcap, 1), np.uint8)
-        tbuf = np.empty(max(tcap, 1), np.uint8)
+        qbuf = out_array(bufs, "qbuf", max(qcap, 1), np.uint8)
+        tbuf = out_array(bufs, "tbuf", max(tcap, 1), np.uint8)
         rc = lib.fa_collect_mate_jobs(ctx.handle, N.ptr(opts), N.ptr(bounds), N.ptr(pac), l_pac, N.ptr(chr_off),
                                       N.ptr(chr_len), len(chr_off), N.ptr(reads), N.ptr(read_off),
                                       len(read_off) - 1, N.ptr(alns), len(alns), N.ptr(cands), n, N.ptr(jobs),

@@ -271,12 +271,13 @@ int fa_ctx_set_threads(fa_ctx *ctx, int threads_per_block);
  * outside the graph.  Turning it off releases the recorded graph. */
 int fa_ctx_set_graph(fa_ctx *ctx, int enable);
 
-/* Upload slices of host batches of 32,768 jobs or more (no reference counterpart): the
- * sequences of a single-band batch, and of a retry-policy or learned batch that runs its rounds
- * slice by slice, go up in this many graded slices (2..8; 1: the whole batch goes up before
- * one run of the kernels over all of it; 0 keeps a value, -1 restores the default: 8, except 2
- * for the rounds of a packed batch).  Results are identical for every setting; only the
- * overlap of copies and kernels changes. */
+/* Upload slices of host batches of 32,768 jobs or more (no reference counterpart): the job
+ * records and sequences of a single-band batch, and of a retry-policy or learned batch that
+ * runs its rounds slice by slice, go up in this many graded slices (2..8; 1: the whole batch
+ * goes up before one run of the kernels over all of it; 0 keeps a value, -1 restores the
+ * defaults: 8 for byte codes, whose uploads are the bottleneck; 3 for the rounds of a packed
+ * batch; 6 for a packed single-band batch).  Results are identical for every setting; only
+ * the overlap of copies and kernels changes. */
 int fa_ctx_set_slices(fa_ctx *ctx, int single_band, int policy_rounds);
 
 /* Kernel timing of device-resident calls (no reference counterpart): with timing on,
@@ -393,6 +394,12 @@ typedef struct {
     uint32_t _pad;
     uint64_t qbuf_len, tbuf_len;   /* bytes of query / target sequence the jobs address */
 } fa_collect_counts;
+
+/* The 2-bit packed reference (l_pac bases, the .pac layout below) kept on the device for
+ * the collection calls of this context (no reference counterpart): a fa_collect_ext_jobs,
+ * fa_collect_ext_jobs_packed or fa_collect_mate_jobs call given pac == NULL and the same
+ * l_pac reads this copy instead of uploading the reference again.  pac == NULL drops it. */
+int fa_ctx_set_reference(fa_ctx *ctx, const uint8_t *pac, uint64_t l_pac);
 
 /* reads: read r is reads[read_off[r] .. read_off[r+1]) (codes 0-4); pac: the .pac layout,
  * base k in bits 7-6 of byte k/4 for k % 4 == 0, down to bits 1-0 for k % 4 == 3.

@@ -107,6 +107,26 @@ def test_argument_checks_and_capacity(built):
     badc = chains.copy()
     badc["read"][0] = 10**6
     assert call(ch=badc) == N.FA_ERR_ARG
+
+    def why(**kw):
+        with pytest.raises(N.NativeError) as e:
+            N.check(call(**kw))
+        assert e.value.code == N.FA_ERR_ARG
+        return str(e.value)
+    # the first failing chain's first failing rule is reported, as a serial walk finds it
+    kept = np.nonzero(chains["kept"] != 0)[0]
+    k1, k2 = int(kept[3]), int(kept[7])
+    badc = chains.copy()
+    badc["seed_first"][k2] = len(seeds)                                # seeds past the array
+    bad = seeds.copy()
+    bad["ref_pos"][int(chains["seed_first"][k1])] = 2 * l_pac          # an earlier chain's seed
+    assert "outside the reference" in why(ch=badc, sd=bad)
+    assert "run past the seed array" in why(ch=badc)
+    bad = seeds.copy()
+    j = int(chains["seed_first"][k1])
+    bad["ref_pos"][j] = 2 * l_pac
+    bad["query_pos"][j] = 500
+    assert "outside its read" in why(sd=bad)                           # the read rule is checked first
     ctx.close()
 
 
@@ -138,3 +158,55 @@ def test_packed_collection_equals_byte_collection(built):
     got, _, _ = fa.extend_batch_packed(p, pk.left_jobs, pk.qbuf, pk.tbuf)
     want, _, _ = fa.extend_batch(p, byt.left_jobs, byt.qbuf, byt.tbuf)
     assert np.array_equal(got, want)
+
+
+def test_reused_pinned_buffers_give_fresh_results(built):
+    """Collection and CIGAR regeneration into reused page-locked HostBuffers: two batches of
+    different sizes, one after the other through the same buffers, equal the calls into
+    fresh arrays (the outputs are written in full, so stale bytes of a larger earlier batch
+    never show)."""
+    import ferrousalign_b200 as fa
+    from ferrousalign_b200 import collect as K, synth
+    bufs, pbufs, cbufs = fa.HostBuffers(), fa.HostBuffers(), fa.HostBuffers()
+    p = fa.BandedPairWiseSW().to_struct()
+    for n, seed in ((4000, 5), (2500, 6)):
+        ref, reads, off, chains, seeds = synth.workload_chains(n, ref_len=2_000_000, seed=seed)
+        pac, l_pac = K.pack_reference(ref)
+        want = K.collect_extension_jobs(pac, l_pac, reads, off, chains, seeds)
+        got = K.collect_extension_jobs(pac, l_pac, reads, off, chains, seeds, bufs=bufs)
+        pk = K.collect_extension_jobs_packed(pac, l_pac, reads, off, chains, seeds, bufs=pbufs)
+        for f in ("left_jobs", "right_jobs", "seed_ext", "chain_first", "chain_win", "qbuf", "tbuf"):
+            assert np.array_equal(getattr(got, f), getattr(want, f)), f
+        for f in ("left_jobs", "right_jobs", "seed_ext", "chain_first", "chain_win"):
+            assert np.array_equal(getattr(pk, f), getattr(want, f)), f
+        assert np.array_equal(fa.unpack(pk.tbuf), want.tbuf)
+        cj, cq, ct = synth.workload_cigar(n, seed=seed)
+        cw = fa.scalar_banded_swa_batch(p, cj, cq, ct)
+        cg = fa.scalar_banded_swa_batch(p, cj, cq, ct, bufs=cbufs)
+        assert np.array_equal(cg.results, cw.results)
+        assert all(cg.cigar_of(i) == cw.cigar_of(i) for i in range(0, n, 97))
+
+
+def test_resident_reference(built):
+    """Context.set_reference keeps the packed reference on the device: collection calls given
+    pac=None read it and equal the calls that upload it; a call whose l_pac differs from the
+    resident copy's, or one after the copy is dropped, fails with FA_ERR_ARG."""
+    import ferrousalign_b200 as fa
+    from ferrousalign_b200 import _native as N, collect as K, synth
+    ref, reads, off, chains, seeds = synth.workload_chains(3000, ref_len=2_000_000, seed=9)
+    pac, l_pac = K.pack_reference(ref)
+    with fa.Context(0) as ctx:
+        want = K.collect_extension_jobs(pac, l_pac, reads, off, chains, seeds, ctx=ctx)
+        ctx.set_reference(pac, l_pac)
+        got = K.collect_extension_jobs(None, l_pac, reads, off, chains, seeds, ctx=ctx)
+        pk = K.collect_extension_jobs_packed(None, l_pac, reads, off, chains, seeds, ctx=ctx)
+        for f in ("left_jobs", "right_jobs", "seed_ext", "chain_first", "chain_win", "qbuf", "tbuf"):
+            assert np.array_equal(getattr(got, f), getattr(want, f)), f
+        assert np.array_equal(fa.unpack(pk.tbuf), want.tbuf)
+        with pytest.raises(N.NativeError) as e:
+            K.collect_extension_jobs(None, l_pac - 1, reads, off, chains, seeds, ctx=ctx)
+        assert e.value.code == N.FA_ERR_ARG
+        ctx.set_reference(None)
+        with pytest.raises(N.NativeError) as e:
+            K.collect_extension_jobs(None, l_pac, reads, off, chains, seeds, ctx=ctx)
+        assert e.value.code == N.FA_ERR_ARG

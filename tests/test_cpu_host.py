@@ -99,3 +99,20 @@ def test_oracle_policy_certificate_is_exact(built):
     wf = np.full(len(b.jobs), 4, np.int32)
     learned, wfin, tries, _ = O.ext_batch_policy(p, make_policy(2, 2, 1, 1), b.jobs, b.qseq, b.tseq, wf)
     assert np.array_equal(plain, learned)
+
+
+def test_host_buffers_reuse_and_grow():
+    """HostBuffers hands out views of one storage per name: reused while a request fits,
+    replaced by a larger one when it does not; dtypes and shapes as asked."""
+    from ferrousalign_b200.hostbuf import HostBuffers, out_array
+    b = HostBuffers(pinned=False)
+    a = b.get("x", 100, np.uint32)
+    a[:] = 7
+    c = b.get("x", 50, np.uint32)
+    assert c.shape == (50,) and c.dtype == np.uint32 and np.shares_memory(a, c) and (c == 7).all()
+    d = b.get("x", 400, np.uint64)
+    assert d.shape == (400,) and not np.shares_memory(a, d)
+    e = b.get("y", 3, np.dtype([("a", "<u4"), ("b", "<u8")]))
+    assert e.shape == (3,) and not np.shares_memory(d, e)
+    assert (out_array(None, "z", 5, np.int32, zero=True) == 0).all()
+    assert out_array(b, "x", 10, np.uint64).base is not None

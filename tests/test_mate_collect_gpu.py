@@ -87,3 +87,22 @@ def test_argument_checks(built):
         R.collect_rescue_jobs(pac, l_pac, chr_off, chr_len, reads, off, alns, bad, bounds)
     with pytest.raises(N.NativeError):
         R.collect_rescue_jobs(pac, l_pac, chr_off, chr_len + np.uint64(l_pac), reads, off, alns, cands, bounds)
+
+
+def test_resident_reference_and_reused_buffers(built):
+    """The rescue collection reading the context's resident reference (pac=None) into reused
+    page-locked HostBuffers equals the call that uploads the reference into fresh arrays."""
+    import ferrousalign_b200 as fa
+    from ferrousalign_b200 import mate_rescue as R, synth
+    ref, chr_off, chr_len, reads, off, alns, cands = synth.workload_rescue(1500, ref_len=3_000_000)
+    pac, l_pac = fa.pack_reference(ref)
+    bounds = bounds_of(((0, 0, 1), (200, 600, 0), (0, 0, 1), (0, 0, 1)))
+    bufs = fa.HostBuffers()
+    with fa.Context(0) as ctx:
+        want = R.collect_rescue_jobs(pac, l_pac, chr_off, chr_len, reads, off, alns, cands, bounds, ctx=ctx)
+        ctx.set_reference(pac, l_pac)
+        for _ in range(2):
+            got = R.collect_rescue_jobs(None, l_pac, chr_off, chr_len, reads, off, alns, cands, bounds, ctx=ctx,
+                                        bufs=bufs)
+            for f in ("jobs", "info", "qbuf", "tbuf"):
+                assert np.array_equal(getattr(got, f), getattr(want, f)), f
