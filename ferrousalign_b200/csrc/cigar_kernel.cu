@@ -155,8 +155,11 @@ __device__ __forceinline__ void cigar_job(uint32_t k, const fa_cigar_job &J, con
     }
     int max_score = h0, max_i = -1, max_j = -1, max_ie = -1, gscore = -1, max_off = 0;
     int beg = 0, end = qlen, cells = 0;
+    int t_next = T[0];   // the next row's target base, loaded a row ahead
     for (int i = 0; i < tlen; ++i) {
-        const int tbase = T[i] < 4 ? T[i] : 4;
+        const int t_cur = t_next;
+        if (i + 1 < tlen) t_next = T[i + 1];
+        const int tbase = t_cur < 4 ? t_cur : 4;
         const uint32_t rlo = rt[tbase], rhi = rt[5 + tbase];   // this row's scores, one byte per query code
         int cb = beg, ce = end;
         if (cb < i - w) cb = i - w;
