@@ -508,8 +508,10 @@ def bench_mate(args, ctx, lib, dev, stream, flush, skip_cpu=False):
     # and 2-bit packed bases
     mj, mq, mt = pin_array(m.jobs), pin_array(m.qseq), pin_array(m.tseq)
     qp, tp = fa.pack(m.qseq).pinned(), fa.pack(m.tseq).pinned()
-    forms = {"bytes": (lambda: fa.mate_sw_batch(mp, mj, mq, mt, ctx=ctx), int(mj.nbytes + mq.nbytes + mt.nbytes)),
-             "packed": (lambda: fa.mate_sw_batch_packed(mp, mj, qp, tp, ctx=ctx),
+    mo = pin_array(np.zeros(MATE_JOBS, N.KSWR_DT))
+    forms = {"bytes": (lambda: fa.mate_sw_batch(mp, mj, mq, mt, ctx=ctx, out=mo),
+                       int(mj.nbytes + mq.nbytes + mt.nbytes)),
+             "packed": (lambda: fa.mate_sw_batch_packed(mp, mj, qp, tp, ctx=ctx, out=mo),
                         int(mj.nbytes + qp.nbytes + tp.nbytes))}
     e2e = {}
     for name, (fn, h2d) in forms.items():

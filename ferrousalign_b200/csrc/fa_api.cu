@@ -127,6 +127,8 @@ struct fa_ctx {
     cudaStream_t prep_stream = nullptr;
     cudaEvent_t job_ev[8] = {}, info_ev[8] = {};
     uint32_t *h_slice_info = nullptr;
+    void *h_stage = nullptr;   // page-locked staging of host-built arrays (sliced mate orders)
+    size_t h_stage_cap = 0;
     // upload slices of pipelined / sliced host batches (0: chosen per batch, auto_slices)
     int slices_single = 0, slices_rounds = 0;
     DevBuf chunk_scratch;
@@ -1747,10 +1749,13 @@ struct MateHostPlan {
     std::vector<uint32_t> order;   // u8 jobs, then i16 jobs
     uint32_t n_byte = 0;
     int mq_b = 0, mq_w = 0, mt = 0, mn_b = INT_MAX;
+    uint64_t q_end = 0, t_end = 0;   // the jobs' furthest query and target bytes
 };
 
+// jobs[0 .. n) checked and split by lane width; `base` numbers them in messages (a slice of a
+// larger batch).
 int plan_mate_host(const fa_mate_params *p, const fa_mate_job *jobs, uint32_t n, uint64_t qseq_len,
-                   uint64_t tseq_len, MateHostPlan *pl) {
+                   uint64_t tseq_len, MateHostPlan *pl, uint32_t base = 0) {
     int mn = 127, mx = 0;
     for (int i = 0; i < 25; ++i) { mn = std::min<int>(mn, p->mat[i]); mx = std::max<int>(mx, p->mat[i]); }
     if (mx <= 0) return fail(FA_ERR_ARG, "scoring matrix needs a positive entry");
@@ -1764,14 +1769,16 @@ int plan_mate_host(const fa_mate_params *p, const fa_mate_job *jobs, uint32_t n,
     pl->order.clear();
     for (uint32_t i = 0; i < n; ++i) {
         const fa_mate_job &j = jobs[i];
-        if (j.qlen <= 0 || j.tlen < 0) return fail(FA_ERR_ARG, "mate job %u: bad lengths", i);
-        if (j.tlen > FA_MAX_TLEN) return fail(FA_ERR_CAPACITY, "mate job %u: tlen too long", i);
+        if (j.qlen <= 0 || j.tlen < 0) return fail(FA_ERR_ARG, "mate job %u: bad lengths", base + i);
+        if (j.tlen > FA_MAX_TLEN) return fail(FA_ERR_CAPACITY, "mate job %u: tlen too long", base + i);
         if (j.q_off + (uint64_t)j.qlen > qseq_len || j.t_off + (uint64_t)j.tlen > tseq_len)
-            return fail(FA_ERR_ARG, "mate job %u: sequence range outside the buffers", i);
+            return fail(FA_ERR_ARG, "mate job %u: sequence range outside the buffers", base + i);
         const bool byte = (j.xtra & FA_KSW_XBYTE) != 0;
         if (byte ? j.qlen > 16 * 32 : j.qlen > 8 * 32)
-            return fail(FA_ERR_CAPACITY, "mate job %u: qlen=%d exceeds the %s-lane limit", i, j.qlen,
+            return fail(FA_ERR_CAPACITY, "mate job %u: qlen=%d exceeds the %s-lane limit", base + i, j.qlen,
                         byte ? "u8" : "i16");
+        pl->q_end = std::max(pl->q_end, j.q_off + (uint64_t)j.qlen);
+        pl->t_end = std::max(pl->t_end, j.t_off + (uint64_t)j.tlen);
         (byte ? pl->order : word_list).push_back(i);
         if (byte) {
             pl->mq_b = std::max(pl->mq_b, j.qlen);
@@ -1939,6 +1946,122 @@ int mate_host_batch(fa_ctx *c, const fa_mate_params *p, const fa_mate_job *jobs,
     return FA_OK;
 }
 
+int ensure_host_stage(fa_ctx *c, size_t bytes) {
+    if (c->h_stage_cap >= bytes) return FA_OK;
+    if (c->h_stage) cudaFreeHost(c->h_stage);
+    c->h_stage = nullptr;
+    c->h_stage_cap = 0;
+    FA_CUDA(cudaMallocHost(&c->h_stage, bytes));
+    c->h_stage_cap = bytes;
+    return FA_OK;
+}
+
+bool host_pinned(const void *p) {
+    cudaPointerAttributes pa;
+    const bool r = p && cudaPointerGetAttributes(&pa, p) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    return r;
+}
+
+// A byte-code host mate-SW batch of kPipeMinJobs jobs or more in four graded job-index
+// slices: each slice is planned on the host (checks, lane split, its furthest query and target
+// bytes) while the GPU works on the earlier ones, then its job records, order and the sequence
+// bytes up to its furthest job go up on the copy stream, its kernels run on the main stream
+// and, into a page-locked `out`, its results come back on a third stream.  The kernels see a
+// slice through views of the job and result arrays, so jobs out of sequence order only widen
+// a slice's upload.  A bad job fails the call (after the earlier slices' work drains), named
+// by its index in the batch.  Results and statistics are those of one launch over the batch.
+int mate_host_sliced(fa_ctx *c, const fa_mate_params *p, const fa_mate_job *jobs, uint32_t n, const uint8_t *qseq,
+                     uint64_t qseq_len, const uint8_t *tseq, uint64_t tseq_len, fa_kswr *out, fa_ext_stats *stats,
+                     std::chrono::steady_clock::time_point t0, bool *done) {
+    *done = false;
+    constexpr int ns = 4;
+    if (!c || !p || p->m != 5 || !jobs || !out || n < kPipeMinJobs || c->slices_single == 1) return FA_OK;
+    uint32_t J[ns + 1];
+    J[0] = 0;
+    J[ns] = n;
+    for (int k = 1; k < ns; ++k) J[k] = (uint32_t)((uint64_t)n * kGradedCum[ns][k - 1] / 32);
+    uint32_t max_cnt = 0;
+    for (int k = 0; k < ns; ++k) max_cnt = std::max(max_cnt, J[k + 1] - J[k]);
+    FA_CUDA(cudaSetDevice(c->device));
+    FA_CUDA(c->jobs.ensure(sizeof(fa_mate_job) * (size_t)n));
+    FA_CUDA(c->order.ensure(4ull * n));
+    FA_CUDA(c->out.ensure(sizeof(fa_kswr) * (size_t)n));
+    FA_CUDA(c->misc.ensure(kMiscBytes));
+    FA_CUDA(c->qseq.ensure(qseq_len + 1));
+    FA_CUDA(c->tseq.ensure(tseq_len + 1));
+    FA_CUDA(c->mate_rev.ensure(4ull * (2 + (size_t)max_cnt)));
+    if (int rc = ensure_pipe_streams(c)) return rc;
+    if (int rc = ensure_host_stage(c, 4ull * n)) return rc;
+    uint32_t *h_order = static_cast<uint32_t *>(c->h_stage);
+    const bool early = host_pinned(out);
+    cudaStream_t s = c->stream, cs = c->copy_stream, ds = c->prep_stream;
+    auto drain = [&]() {
+        cudaStreamSynchronize(cs);
+        cudaStreamSynchronize(s);
+        cudaStreamSynchronize(ds);
+    };
+    Misc m = misc_of(c);
+    FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
+    FA_CUDA(cudaEventRecord(c->fork_ev, s));
+    FA_CUDA(cudaStreamWaitEvent(cs, c->fork_ev, 0));
+    FA_CUDA(cudaStreamWaitEvent(ds, c->fork_ev, 0));
+    fa_mate_job *d_jobs = c->jobs.as<fa_mate_job>();
+    uint32_t *d_order = c->order.as<uint32_t>();
+    fa_kswr *d_out = c->out.as<fa_kswr>();
+    uint32_t launches = 0;
+    uint64_t qe = 0, te = 0;
+    MateHostPlan pl;
+    for (int k = 0; k < ns; ++k) {
+        const uint32_t j0 = J[k], cnt = J[k + 1] - j0;
+        pl = MateHostPlan{};
+        if (int rc = plan_mate_host(p, jobs + j0, cnt, qseq_len, tseq_len, &pl, j0)) {
+            drain();
+            return rc;
+        }
+        memcpy(h_order + j0, pl.order.data(), 4ull * cnt);
+        FA_CUDA(cudaMemcpyAsync(d_jobs + j0, jobs + j0, sizeof(fa_mate_job) * cnt, cudaMemcpyHostToDevice, cs));
+        FA_CUDA(cudaMemcpyAsync(d_order + j0, h_order + j0, 4ull * cnt, cudaMemcpyHostToDevice, cs));
+        if (pl.q_end > qe) {
+            FA_CUDA(cudaMemcpyAsync(c->qseq.as<uint8_t>() + qe, qseq + qe, pl.q_end - qe, cudaMemcpyHostToDevice, cs));
+            qe = pl.q_end;
+        }
+        if (pl.t_end > te) {
+            FA_CUDA(cudaMemcpyAsync(c->tseq.as<uint8_t>() + te, tseq + te, pl.t_end - te, cudaMemcpyHostToDevice, cs));
+            te = pl.t_end;
+        }
+        FA_CUDA(cudaEventRecord(c->slice_ev[k], cs));
+        FA_CUDA(cudaStreamWaitEvent(s, c->slice_ev[k], 0));
+        if (k == 0) FA_CUDA(cudaEventRecord(c->ev0, s));
+        FA_CUDA(launch_mate_plan(pl, d_jobs + j0, d_order + j0, cnt, c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(),
+                                 d_out + j0, m.cells, m.status, c->mate_rev.as<uint32_t>(), s, &launches));
+        if (early) {
+            FA_CUDA(cudaEventRecord(c->done_ev[k], s));
+            FA_CUDA(cudaStreamWaitEvent(ds, c->done_ev[k], 0));
+            FA_CUDA(cudaMemcpyAsync(out + j0, d_out + j0, sizeof(fa_kswr) * cnt, cudaMemcpyDeviceToHost, ds));
+        }
+    }
+    FA_CUDA(cudaEventRecord(c->ev1, s));
+    *done = true;
+    const int rs = read_status(c, s);
+    FA_CUDA(cudaStreamSynchronize(ds));
+    FA_CUDA(cudaStreamSynchronize(cs));
+    if (rs) return rs;
+    if (!early) FA_CUDA(cudaMemcpy(out, d_out, sizeof(fa_kswr) * (size_t)n, cudaMemcpyDeviceToHost));
+    if (stats) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        unsigned long long cells = 0;
+        FA_CUDA(cudaMemcpy(&cells, m.cells, 8, cudaMemcpyDeviceToHost));
+        stats->cells = stats->cells_executed = cells;
+        stats->kernel_ms = ms;
+        stats->kernel_launches = launches;
+        stats->jobs = n;
+        stats->total_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return FA_OK;
+}
+
 extern "C" {
 
 const char *fa_last_error(void) { return g_err.c_str(); }
@@ -2019,6 +2142,7 @@ void fa_ctx_destroy(fa_ctx *c) {
     }
     if (c->prep_stream) cudaStreamDestroy(c->prep_stream);
     if (c->h_slice_info) cudaFreeHost(c->h_slice_info);
+    if (c->h_stage) cudaFreeHost(c->h_stage);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     c->chunk_scratch.release();
     if (c->kev0) cudaEventDestroy(c->kev0);
@@ -2966,6 +3090,9 @@ int fa_mate_sw_batch(fa_ctx *c, const fa_mate_params *p, const fa_mate_job *jobs
     auto t0 = std::chrono::steady_clock::now();
     if (stats) memset(stats, 0, sizeof(*stats));
     if (n && (!qseq || !tseq)) return fail(FA_ERR_ARG, "null buffer");
+    bool done = false;
+    if (int rc = mate_host_sliced(c, p, jobs, n, qseq, qseq_len, tseq, tseq_len, out, stats, t0, &done)) return rc;
+    if (done) return FA_OK;
     auto upload = [&](cudaStream_t s) -> int {
         FA_CUDA(c->qseq.ensure(qseq_len));
         FA_CUDA(c->tseq.ensure(tseq_len));

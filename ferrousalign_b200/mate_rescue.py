@@ -70,27 +70,29 @@ def make_mate_params(mat=MATE_RESCUE_SCORING_MATRIX, o_del=6, e_del=1, o_ins=6, 
 
 
 def mate_sw_batch(params: np.ndarray, jobs: np.ndarray, qseq: np.ndarray, tseq: np.ndarray,
-                  ctx: N.Context | None = None):
-    """Array-level call of fa_mate_sw_batch.  Returns (kswr records, stats)."""
+                  ctx: N.Context | None = None, out: np.ndarray | None = None):
+    """Array-level call of fa_mate_sw_batch.  Returns (kswr records, stats); `out` may be a
+    (page-locked) result buffer to fill."""
     lib = N.load()
     ctx = ctx or N.default_context()
     jobs = np.ascontiguousarray(jobs, dtype=N.MATE_JOB_DT)
     qseq = np.ascontiguousarray(qseq, dtype=np.uint8)
     tseq = np.ascontiguousarray(tseq, dtype=np.uint8)
-    out = np.zeros(len(jobs), dtype=N.KSWR_DT)
+    out = np.zeros(len(jobs), dtype=N.KSWR_DT) if out is None else out
     stats = np.zeros(1, dtype=N.STATS_DT)
     N.check(lib.fa_mate_sw_batch(ctx.handle, N.ptr(params), N.ptr(jobs), len(jobs), N.ptr(qseq), qseq.nbytes,
                                  N.ptr(tseq), tseq.nbytes, N.ptr(out), N.ptr(stats)))
     return out, stats[0]
 
 
-def mate_sw_batch_packed(params: np.ndarray, jobs: np.ndarray, qseq, tseq, ctx: N.Context | None = None):
+def mate_sw_batch_packed(params: np.ndarray, jobs: np.ndarray, qseq, tseq, ctx: N.Context | None = None,
+                         out: np.ndarray | None = None):
     """fa_mate_sw_batch_packed on PackedSeq buffers (packed.pack).  Returns (kswr records,
-    stats), those of mate_sw_batch on the same bases."""
+    stats), those of mate_sw_batch on the same bases; `out` as for mate_sw_batch."""
     lib = N.load()
     ctx = ctx or N.default_context()
     jobs = np.ascontiguousarray(jobs, dtype=N.MATE_JOB_DT)
-    out = np.zeros(len(jobs), dtype=N.KSWR_DT)
+    out = np.zeros(len(jobs), dtype=N.KSWR_DT) if out is None else out
     stats = np.zeros(1, dtype=N.STATS_DT)
     qs, ts = qseq.struct(), tseq.struct()
     N.check(lib.fa_mate_sw_batch_packed(ctx.handle, N.ptr(params), N.ptr(jobs), len(jobs), N.ptr(qs), N.ptr(ts),

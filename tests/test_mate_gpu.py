@@ -141,3 +141,32 @@ def test_packed_input_equals_byte_input(ctx):
     assert e.value.code == N.FA_ERR_ARG
     again, _ = fa.mate_sw_batch_packed(p, b.jobs[:100], qp, tp, ctx=ctx)
     assert np.array_equal(again, want[:100])
+
+
+def test_sliced_host_batch(ctx):
+    """A host batch of 32,768 jobs or more runs in job-index slices whose uploads overlap
+    the kernels: results into a page-locked and into a pageable buffer equal the unsliced
+    call's and the oracle's on a sample; a bad job in the last slice fails the call before
+    anything runs, named by its index in the batch."""
+    import torch
+    b = synth.workload_mate(100_000, seed=29)
+    mp = fa.make_mate_params()
+    c = fa.Context(0)
+    try:
+        c.set_slices(1, 1)
+        want, wst = fa.mate_sw_batch(mp, b.jobs, b.qseq, b.tseq, ctx=c)
+        c.set_slices(-1, -1)
+        pinned = torch.from_numpy(np.zeros(len(b.jobs), N.KSWR_DT).view(np.uint8)).pin_memory().numpy().view(N.KSWR_DT)
+        for out in (pinned, None):
+            got, st = fa.mate_sw_batch(mp, b.jobs, b.qseq, b.tseq, ctx=c, out=out)
+            assert np.array_equal(got, want)
+            assert int(st["cells"]) == int(wst["cells"])
+        ref, _ = O.mate_batch(mp, b.jobs[:3000], b.qseq, b.tseq)
+        assert np.array_equal(want[:3000], ref)
+        bad = b.jobs.copy()
+        bad["tlen"][97_123] = -1
+        with pytest.raises(N.NativeError) as e:
+            fa.mate_sw_batch(mp, bad, b.qseq, b.tseq, ctx=c)
+        assert e.value.code == N.FA_ERR_ARG and "97123" in str(e.value)
+    finally:
+        c.close()
