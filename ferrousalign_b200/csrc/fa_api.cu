@@ -115,8 +115,8 @@ struct fa_ctx {
     DevBuf mate_rev;   // the mate SW reverse-pass list (launch_mate_sw)
     DevBuf mate_pk;    // packed mate input: bases and N runs before the unpack
     uint64_t q_bases = 0, t_bases = 0;   // bases of the host call's sequence buffers (cq / ct)
-    cudaStream_t pm_stream = nullptr;
-    cudaEvent_t pm_ev0 = nullptr, pm_ev1 = nullptr;
+    cudaStream_t pm_stream = nullptr, pm_copy = nullptr;   // the mate half's kernels and uploads
+    cudaEvent_t pm_ev0 = nullptr, pm_ev1 = nullptr, pm_fork = nullptr, pm_slice_ev[4] = {};
     // pipelined host batches: slice uploads on their own stream, one event per slice; the
     // same stream then returns each finished slice's results, after its done event
     cudaStream_t copy_stream = nullptr;
@@ -1963,26 +1963,85 @@ bool host_pinned(const void *p) {
     return r;
 }
 
-// A byte-code host mate-SW batch of kPipeMinJobs jobs or more in four graded job-index
-// slices: each slice is planned on the host (checks, lane split, its furthest query and target
-// bytes) while the GPU works on the earlier ones, then its job records, order and the sequence
-// bytes up to its furthest job go up on the copy stream, its kernels run on the main stream
-// and, into a page-locked `out`, its results come back on a third stream.  The kernels see a
-// slice through views of the job and result arrays, so jobs out of sequence order only widen
-// a slice's upload.  A bad job fails the call (after the earlier slices' work drains), named
-// by its index in the batch.  Results and statistics are those of one launch over the batch.
+// Device buffers, streams and events a sliced mate-SW batch runs on: kernels on s, uploads
+// on cs, each slice's results (with an early-returned `out`) on ds.
+struct MateSliceRes {
+    cudaStream_t s, cs, ds;
+    cudaEvent_t *slice_ev, *done_ev, ev0;
+    fa_mate_job *jobs;
+    uint32_t *order;
+    uint8_t *q, *t;
+    fa_kswr *out;
+    unsigned long long *cells;
+    uint32_t *status, *rev;
+};
+constexpr int kMateSlices = 4;
+
+// Graded job-index slices of a host mate-SW batch (n >= kPipeMinJobs): each slice is planned on
+// the host (checks, lane split, its furthest query and target bytes) while the GPU works on the
+// earlier ones, then its job records, order (staged in the page-locked h_order) and the
+// sequence bytes up to its furthest job go up on r.cs and its kernels run on r.s, seeing the
+// slice through views of the job and result arrays, so jobs out of sequence order only widen a
+// slice's upload; with early_out its results go back on r.ds as soon as it has run.  A bad
+// job returns its error (named by its index in the batch) with the earlier slices enqueued:
+// the caller drains the streams.  r.rev holds 2 + the largest slice's job count.
+int enqueue_mate_sliced(const fa_mate_params *p, const fa_mate_job *jobs, uint32_t n, const uint8_t *qseq,
+                        uint64_t qseq_len, const uint8_t *tseq, uint64_t tseq_len, uint32_t *h_order,
+                        fa_kswr *early_out, const MateSliceRes &r, uint32_t *launches) {
+    uint32_t J[kMateSlices + 1];
+    J[0] = 0;
+    J[kMateSlices] = n;
+    for (int k = 1; k < kMateSlices; ++k) J[k] = (uint32_t)((uint64_t)n * kGradedCum[kMateSlices][k - 1] / 32);
+    uint64_t qe = 0, te = 0;
+    MateHostPlan pl;
+    for (int k = 0; k < kMateSlices; ++k) {
+        const uint32_t j0 = J[k], cnt = J[k + 1] - j0;
+        pl = MateHostPlan{};
+        if (int rc = plan_mate_host(p, jobs + j0, cnt, qseq_len, tseq_len, &pl, j0)) return rc;
+        memcpy(h_order + j0, pl.order.data(), 4ull * cnt);
+        FA_CUDA(cudaMemcpyAsync(r.jobs + j0, jobs + j0, sizeof(fa_mate_job) * cnt, cudaMemcpyHostToDevice, r.cs));
+        FA_CUDA(cudaMemcpyAsync(r.order + j0, h_order + j0, 4ull * cnt, cudaMemcpyHostToDevice, r.cs));
+        if (pl.q_end > qe) {
+            FA_CUDA(cudaMemcpyAsync(r.q + qe, qseq + qe, pl.q_end - qe, cudaMemcpyHostToDevice, r.cs));
+            qe = pl.q_end;
+        }
+        if (pl.t_end > te) {
+            FA_CUDA(cudaMemcpyAsync(r.t + te, tseq + te, pl.t_end - te, cudaMemcpyHostToDevice, r.cs));
+            te = pl.t_end;
+        }
+        FA_CUDA(cudaEventRecord(r.slice_ev[k], r.cs));
+        FA_CUDA(cudaStreamWaitEvent(r.s, r.slice_ev[k], 0));
+        if (k == 0) FA_CUDA(cudaEventRecord(r.ev0, r.s));
+        FA_CUDA(launch_mate_plan(pl, r.jobs + j0, r.order + j0, cnt, r.q, r.t, r.out + j0, r.cells, r.status, r.rev,
+                                 r.s, launches));
+        if (early_out) {
+            FA_CUDA(cudaEventRecord(r.done_ev[k], r.s));
+            FA_CUDA(cudaStreamWaitEvent(r.ds, r.done_ev[k], 0));
+            FA_CUDA(cudaMemcpyAsync(early_out + j0, r.out + j0, sizeof(fa_kswr) * cnt, cudaMemcpyDeviceToHost, r.ds));
+        }
+    }
+    return FA_OK;
+}
+
+// The largest slice enqueue_mate_sliced cuts from n jobs.
+uint32_t mate_max_slice(uint32_t n) {
+    uint32_t prev = 0, mx = 0;
+    for (int k = 1; k <= kMateSlices; ++k) {
+        const uint32_t e = k == kMateSlices ? n : (uint32_t)((uint64_t)n * kGradedCum[kMateSlices][k - 1] / 32);
+        mx = std::max(mx, e - prev);
+        prev = e;
+    }
+    return mx;
+}
+
+// A byte-code host mate-SW batch of kPipeMinJobs jobs or more, sliced (enqueue_mate_sliced)
+// on the context's main, copy and prep streams; results into a page-locked `out` come back
+// slice by slice.  Results and statistics are those of one launch over the batch.
 int mate_host_sliced(fa_ctx *c, const fa_mate_params *p, const fa_mate_job *jobs, uint32_t n, const uint8_t *qseq,
                      uint64_t qseq_len, const uint8_t *tseq, uint64_t tseq_len, fa_kswr *out, fa_ext_stats *stats,
                      std::chrono::steady_clock::time_point t0, bool *done) {
     *done = false;
-    constexpr int ns = 4;
     if (!c || !p || p->m != 5 || !jobs || !out || n < kPipeMinJobs || c->slices_single == 1) return FA_OK;
-    uint32_t J[ns + 1];
-    J[0] = 0;
-    J[ns] = n;
-    for (int k = 1; k < ns; ++k) J[k] = (uint32_t)((uint64_t)n * kGradedCum[ns][k - 1] / 32);
-    uint32_t max_cnt = 0;
-    for (int k = 0; k < ns; ++k) max_cnt = std::max(max_cnt, J[k + 1] - J[k]);
     FA_CUDA(cudaSetDevice(c->device));
     FA_CUDA(c->jobs.ensure(sizeof(fa_mate_job) * (size_t)n));
     FA_CUDA(c->order.ensure(4ull * n));
@@ -1990,56 +2049,27 @@ int mate_host_sliced(fa_ctx *c, const fa_mate_params *p, const fa_mate_job *jobs
     FA_CUDA(c->misc.ensure(kMiscBytes));
     FA_CUDA(c->qseq.ensure(qseq_len + 1));
     FA_CUDA(c->tseq.ensure(tseq_len + 1));
-    FA_CUDA(c->mate_rev.ensure(4ull * (2 + (size_t)max_cnt)));
+    FA_CUDA(c->mate_rev.ensure(4ull * (2 + (size_t)mate_max_slice(n))));
     if (int rc = ensure_pipe_streams(c)) return rc;
     if (int rc = ensure_host_stage(c, 4ull * n)) return rc;
-    uint32_t *h_order = static_cast<uint32_t *>(c->h_stage);
     const bool early = host_pinned(out);
     cudaStream_t s = c->stream, cs = c->copy_stream, ds = c->prep_stream;
-    auto drain = [&]() {
-        cudaStreamSynchronize(cs);
-        cudaStreamSynchronize(s);
-        cudaStreamSynchronize(ds);
-    };
     Misc m = misc_of(c);
     FA_CUDA(cudaMemsetAsync(c->misc.p, 0, 64, s));
     FA_CUDA(cudaEventRecord(c->fork_ev, s));
     FA_CUDA(cudaStreamWaitEvent(cs, c->fork_ev, 0));
     FA_CUDA(cudaStreamWaitEvent(ds, c->fork_ev, 0));
-    fa_mate_job *d_jobs = c->jobs.as<fa_mate_job>();
-    uint32_t *d_order = c->order.as<uint32_t>();
-    fa_kswr *d_out = c->out.as<fa_kswr>();
+    const MateSliceRes r{s, cs, ds, c->slice_ev, c->done_ev, c->ev0, c->jobs.as<fa_mate_job>(),
+                         c->order.as<uint32_t>(), c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(), c->out.as<fa_kswr>(),
+                         m.cells, m.status, c->mate_rev.as<uint32_t>()};
     uint32_t launches = 0;
-    uint64_t qe = 0, te = 0;
-    MateHostPlan pl;
-    for (int k = 0; k < ns; ++k) {
-        const uint32_t j0 = J[k], cnt = J[k + 1] - j0;
-        pl = MateHostPlan{};
-        if (int rc = plan_mate_host(p, jobs + j0, cnt, qseq_len, tseq_len, &pl, j0)) {
-            drain();
-            return rc;
-        }
-        memcpy(h_order + j0, pl.order.data(), 4ull * cnt);
-        FA_CUDA(cudaMemcpyAsync(d_jobs + j0, jobs + j0, sizeof(fa_mate_job) * cnt, cudaMemcpyHostToDevice, cs));
-        FA_CUDA(cudaMemcpyAsync(d_order + j0, h_order + j0, 4ull * cnt, cudaMemcpyHostToDevice, cs));
-        if (pl.q_end > qe) {
-            FA_CUDA(cudaMemcpyAsync(c->qseq.as<uint8_t>() + qe, qseq + qe, pl.q_end - qe, cudaMemcpyHostToDevice, cs));
-            qe = pl.q_end;
-        }
-        if (pl.t_end > te) {
-            FA_CUDA(cudaMemcpyAsync(c->tseq.as<uint8_t>() + te, tseq + te, pl.t_end - te, cudaMemcpyHostToDevice, cs));
-            te = pl.t_end;
-        }
-        FA_CUDA(cudaEventRecord(c->slice_ev[k], cs));
-        FA_CUDA(cudaStreamWaitEvent(s, c->slice_ev[k], 0));
-        if (k == 0) FA_CUDA(cudaEventRecord(c->ev0, s));
-        FA_CUDA(launch_mate_plan(pl, d_jobs + j0, d_order + j0, cnt, c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(),
-                                 d_out + j0, m.cells, m.status, c->mate_rev.as<uint32_t>(), s, &launches));
-        if (early) {
-            FA_CUDA(cudaEventRecord(c->done_ev[k], s));
-            FA_CUDA(cudaStreamWaitEvent(ds, c->done_ev[k], 0));
-            FA_CUDA(cudaMemcpyAsync(out + j0, d_out + j0, sizeof(fa_kswr) * cnt, cudaMemcpyDeviceToHost, ds));
-        }
+    const int rc = enqueue_mate_sliced(p, jobs, n, qseq, qseq_len, tseq, tseq_len, static_cast<uint32_t *>(c->h_stage),
+                                       early ? out : nullptr, r, &launches);
+    if (rc) {
+        cudaStreamSynchronize(cs);
+        cudaStreamSynchronize(s);
+        cudaStreamSynchronize(ds);
+        return rc;
     }
     FA_CUDA(cudaEventRecord(c->ev1, s));
     *done = true;
@@ -2047,7 +2077,7 @@ int mate_host_sliced(fa_ctx *c, const fa_mate_params *p, const fa_mate_job *jobs
     FA_CUDA(cudaStreamSynchronize(ds));
     FA_CUDA(cudaStreamSynchronize(cs));
     if (rs) return rs;
-    if (!early) FA_CUDA(cudaMemcpy(out, d_out, sizeof(fa_kswr) * (size_t)n, cudaMemcpyDeviceToHost));
+    if (!early) FA_CUDA(cudaMemcpy(out, c->out.p, sizeof(fa_kswr) * (size_t)n, cudaMemcpyDeviceToHost));
     if (stats) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, c->ev0, c->ev1);
@@ -2121,6 +2151,10 @@ void fa_ctx_destroy(fa_ctx *c) {
     if (c->pm_ev0) cudaEventDestroy(c->pm_ev0);
     if (c->pm_ev1) cudaEventDestroy(c->pm_ev1);
     if (c->pm_stream) cudaStreamDestroy(c->pm_stream);
+    if (c->pm_copy) cudaStreamDestroy(c->pm_copy);
+    if (c->pm_fork) cudaEventDestroy(c->pm_fork);
+    for (auto &e : c->pm_slice_ev)
+        if (e) cudaEventDestroy(e);
     for (int l = 1; l < fa_ctx::kLanes; ++l)
         if (c->lane_s[l]) cudaStreamDestroy(c->lane_s[l]);
     c->lane_misc.release();
@@ -3016,19 +3050,49 @@ int fa_pair_batch(fa_ctx *c, const fa_params *p, const fa_policy *pol, const fa_
     if (n && (!qseq || !tseq)) return fail(FA_ERR_ARG, "null buffer");
     if (!mp || mp->m != 5) return fail(FA_ERR_ARG, "mate alphabet size must be 5");
     if (mn && (!mjobs || !mout || !mqseq || !mtseq)) return fail(FA_ERR_ARG, "null mate buffer");
+    // a large mate half runs in job-index slices whose uploads overlap its kernels
+    const bool msliced = mn >= kPipeMinJobs && c->slices_single != 1;
     MateHostPlan pl;
-    if (mn)
+    if (mn && !msliced)
         if (int rc = plan_mate_host(mp, mjobs, mn, mqseq_len, mtseq_len, &pl)) return rc;
     FA_CUDA(cudaSetDevice(c->device));
     // the mate half, asynchronous on its own stream: uploads, kernels, results back
     if (!c->pm_stream) {
         FA_CUDA(cudaStreamCreateWithFlags(&c->pm_stream, cudaStreamNonBlocking));
+        FA_CUDA(cudaStreamCreateWithFlags(&c->pm_copy, cudaStreamNonBlocking));
         FA_CUDA(cudaEventCreate(&c->pm_ev0));
         FA_CUDA(cudaEventCreate(&c->pm_ev1));
+        FA_CUDA(cudaEventCreateWithFlags(&c->pm_fork, cudaEventDisableTiming));
+        for (auto &e : c->pm_slice_ev) FA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
     cudaStream_t ms = c->pm_stream;
     uint32_t mlaunches = 0;
-    if (mn) {
+    if (mn && msliced) {
+        FA_CUDA(c->pm_jobs.ensure(sizeof(fa_mate_job) * (size_t)mn));
+        FA_CUDA(c->pm_order.ensure(4ull * mn));
+        FA_CUDA(c->pm_q.ensure(mqseq_len + 1));
+        FA_CUDA(c->pm_t.ensure(mtseq_len + 1));
+        FA_CUDA(c->pm_out.ensure(sizeof(fa_kswr) * (size_t)mn));
+        FA_CUDA(c->pm_misc.ensure(64));
+        FA_CUDA(c->pm_rev.ensure(4ull * (2 + (size_t)mate_max_slice(mn))));
+        if (int rc = ensure_host_stage(c, 4ull * mn)) return rc;
+        FA_CUDA(cudaMemsetAsync(c->pm_misc.p, 0, 64, ms));
+        FA_CUDA(cudaEventRecord(c->pm_fork, ms));
+        FA_CUDA(cudaStreamWaitEvent(c->pm_copy, c->pm_fork, 0));
+        const MateSliceRes r{ms, c->pm_copy, nullptr, c->pm_slice_ev, nullptr, c->pm_ev0, c->pm_jobs.as<fa_mate_job>(),
+                             c->pm_order.as<uint32_t>(), c->pm_q.as<uint8_t>(), c->pm_t.as<uint8_t>(),
+                             c->pm_out.as<fa_kswr>(),
+                             reinterpret_cast<unsigned long long *>(c->pm_misc.as<char>() + 8),
+                             c->pm_misc.as<uint32_t>(), c->pm_rev.as<uint32_t>()};
+        if (int rc = enqueue_mate_sliced(mp, mjobs, mn, mqseq, mqseq_len, mtseq, mtseq_len,
+                                         static_cast<uint32_t *>(c->h_stage), nullptr, r, &mlaunches)) {
+            cudaStreamSynchronize(c->pm_copy);
+            cudaStreamSynchronize(ms);
+            return rc;
+        }
+        FA_CUDA(cudaEventRecord(c->pm_ev1, ms));
+        FA_CUDA(cudaMemcpyAsync(mout, c->pm_out.p, sizeof(fa_kswr) * (size_t)mn, cudaMemcpyDeviceToHost, ms));
+    } else if (mn) {
         FA_CUDA(c->pm_jobs.ensure(sizeof(fa_mate_job) * (size_t)mn));
         FA_CUDA(c->pm_order.ensure(4ull * mn));
         FA_CUDA(c->pm_q.ensure(mqseq_len));
@@ -3060,6 +3124,7 @@ int fa_pair_batch(fa_ctx *c, const fa_params *p, const fa_policy *pol, const fa_
     }
     // the mate half's end (also on an extension error, so the caller's buffers are free)
     const cudaError_t es = cudaStreamSynchronize(ms);
+    if (msliced) cudaStreamSynchronize(c->pm_copy);
     if (rc) return rc;
     FA_CUDA(es);
     if (mn) {

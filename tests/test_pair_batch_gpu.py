@@ -79,3 +79,25 @@ def test_empty_halves_and_policy_errors(ctx, work):
     # the context stays usable after the rejected call
     ext, _, _, _ = fa.pair_batch(p, b.jobs[:10], b.qseq, b.tseq, mp, m.jobs[:10], m.qseq, m.tseq, ctx=ctx)
     assert np.array_equal(ext, fa.extend_batch(p, b.jobs[:10], b.qseq, b.tseq, ctx=ctx)[0])
+
+
+def test_sliced_mate_half(ctx, work):
+    """A mate half of 32,768 jobs or more runs in job-index slices on its own streams: the
+    results and cell count equal the unsliced separate call's, and a bad mate job in the last
+    slice fails the call, named by its index."""
+    b, _ = work
+    m = synth.workload_mate(60_000, seed=16)
+    p = fa.BandedPairWiseSW().to_struct()
+    mp = fa.make_mate_params()
+    with fa.Context(0) as c1:
+        c1.set_slices(1, 1)
+        mate_ref, mst_ref = fa.mate_sw_batch(mp, m.jobs, m.qseq, m.tseq, ctx=c1)
+    ext, mate, _, mst = fa.pair_batch(p, b.jobs, b.qseq, b.tseq, mp, m.jobs, m.qseq, m.tseq, ctx=ctx)
+    assert np.array_equal(mate, mate_ref)
+    assert mst["cells"] == mst_ref["cells"]
+    assert np.array_equal(ext, fa.extend_batch(p, b.jobs, b.qseq, b.tseq, ctx=ctx)[0])
+    bad = m.jobs.copy()
+    bad["qlen"][59_001] = 0
+    with pytest.raises(N.NativeError) as e:
+        fa.pair_batch(p, b.jobs, b.qseq, b.tseq, mp, bad, m.qseq, m.tseq, ctx=ctx)
+    assert e.value.code == N.FA_ERR_ARG and "59001" in str(e.value)
