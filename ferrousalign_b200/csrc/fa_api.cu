@@ -1977,17 +1977,68 @@ struct MateSliceRes {
 };
 constexpr int kMateSlices = 4;
 
+// The byte-code sequences of a sliced mate batch: each slice's new query and target bytes
+// copied on the upload stream; nothing to prepare on the kernel stream.
+struct MateBytesUp {
+    const uint8_t *qseq, *tseq;
+    uint8_t *d_q, *d_t;
+    int upload(uint64_t qa, uint64_t qb, uint64_t ta, uint64_t tb, cudaStream_t cs) const {
+        if (qb > qa) FA_CUDA(cudaMemcpyAsync(d_q + qa, qseq + qa, qb - qa, cudaMemcpyHostToDevice, cs));
+        if (tb > ta) FA_CUDA(cudaMemcpyAsync(d_t + ta, tseq + ta, tb - ta, cudaMemcpyHostToDevice, cs));
+        return FA_OK;
+    }
+    int prepare(uint64_t, uint64_t, uint64_t, uint64_t, cudaStream_t) const { return FA_OK; }
+    int init(cudaStream_t, cudaStream_t, uint32_t *) const { return FA_OK; }
+};
+
+// The 2-bit packed sequences of a sliced mate batch: the N runs go up first and are checked on
+// the kernel stream; each slice's new packed words go up on the upload stream and are unpacked
+// to byte codes, its N runs applied, on the kernel stream before its kernels (the SW kernels
+// read each base many times, from cache).  Slices start on 16-position words, one packed
+// 32-bit word each.
+struct MatePackedUp {
+    HostSeq hq, ht;
+    uint8_t *pq, *pt, *d_q, *d_t;
+    fa_nrun *rq, *rt;
+    uint32_t *status;
+    int init(cudaStream_t cs, cudaStream_t, uint32_t *) const {
+        if (hq.n_runs) FA_CUDA(cudaMemcpyAsync(rq, hq.runs, sizeof(fa_nrun) * hq.n_runs, cudaMemcpyHostToDevice, cs));
+        if (ht.n_runs) FA_CUDA(cudaMemcpyAsync(rt, ht.runs, sizeof(fa_nrun) * ht.n_runs, cudaMemcpyHostToDevice, cs));
+        return FA_OK;
+    }
+    static int up_range(const HostSeq &h, uint8_t *dst, uint64_t a, uint64_t b, cudaStream_t cs) {
+        const uint64_t ba = a / 4, bb = std::min<uint64_t>((b + 3) / 4, h.nbytes);
+        if (bb > ba) FA_CUDA(cudaMemcpyAsync(dst + ba, h.p + ba, bb - ba, cudaMemcpyHostToDevice, cs));
+        return FA_OK;
+    }
+    int upload(uint64_t qa, uint64_t qb, uint64_t ta, uint64_t tb, cudaStream_t cs) const {
+        if (int rc = up_range(hq, pq, qa, qb, cs)) return rc;
+        return up_range(ht, pt, ta, tb, cs);
+    }
+    int prepare(uint64_t qa, uint64_t qb, uint64_t ta, uint64_t tb, cudaStream_t s) const {
+        if (qa == 0) {   // the first slice: the runs, uploaded before it, are checked once
+            FA_CUDA(launch_runs_check(rq, (uint32_t)hq.n_runs, hq.npos, status, s));
+            FA_CUDA(launch_runs_check(rt, (uint32_t)ht.n_runs, ht.npos, status, s));
+        }
+        FA_CUDA(launch_unpack2_range(pq, qa, qb, rq, (uint32_t)hq.n_runs, d_q, s));
+        FA_CUDA(launch_unpack2_range(pt, ta, tb, rt, (uint32_t)ht.n_runs, d_t, s));
+        return FA_OK;
+    }
+};
+
 // Graded job-index slices of a host mate-SW batch (n >= kPipeMinJobs): each slice is planned on
-// the host (checks, lane split, its furthest query and target bytes) while the GPU works on the
-// earlier ones, then its job records, order (staged in the page-locked h_order) and the
-// sequence bytes up to its furthest job go up on r.cs and its kernels run on r.s, seeing the
-// slice through views of the job and result arrays, so jobs out of sequence order only widen a
-// slice's upload; with early_out its results go back on r.ds as soon as it has run.  A bad
-// job returns its error (named by its index in the batch) with the earlier slices enqueued:
-// the caller drains the streams.  r.rev holds 2 + the largest slice's job count.
-int enqueue_mate_sliced(const fa_mate_params *p, const fa_mate_job *jobs, uint32_t n, const uint8_t *qseq,
-                        uint64_t qseq_len, const uint8_t *tseq, uint64_t tseq_len, uint32_t *h_order,
-                        fa_kswr *early_out, const MateSliceRes &r, uint32_t *launches) {
+// the host (checks, lane split, its furthest query and target positions) while the GPU works on
+// the earlier ones, then its job records and order (staged in the page-locked h_order) go up on
+// r.cs with up.upload of the sequence positions up to its furthest job (rounded up to 16, so
+// slices never share a 16-position word), up.prepare runs on r.s, and its kernels run on r.s,
+// seeing the slice through views of the job and result arrays, so jobs out of sequence order
+// only widen a slice's upload; with early_out its results go back on r.ds as soon as it has
+// run.  A bad job returns its error (named by its index in the batch) with the earlier slices
+// enqueued: the caller drains the streams.  r.rev holds 2 + the largest slice's job count.
+template <class SeqUp>
+int enqueue_mate_sliced(const fa_mate_params *p, const fa_mate_job *jobs, uint32_t n, uint64_t qseq_len,
+                        uint64_t tseq_len, const SeqUp &up, uint32_t *h_order, fa_kswr *early_out,
+                        const MateSliceRes &r, uint32_t *launches) {
     uint32_t J[kMateSlices + 1];
     J[0] = 0;
     J[kMateSlices] = n;
@@ -2001,17 +2052,15 @@ int enqueue_mate_sliced(const fa_mate_params *p, const fa_mate_job *jobs, uint32
         memcpy(h_order + j0, pl.order.data(), 4ull * cnt);
         FA_CUDA(cudaMemcpyAsync(r.jobs + j0, jobs + j0, sizeof(fa_mate_job) * cnt, cudaMemcpyHostToDevice, r.cs));
         FA_CUDA(cudaMemcpyAsync(r.order + j0, h_order + j0, 4ull * cnt, cudaMemcpyHostToDevice, r.cs));
-        if (pl.q_end > qe) {
-            FA_CUDA(cudaMemcpyAsync(r.q + qe, qseq + qe, pl.q_end - qe, cudaMemcpyHostToDevice, r.cs));
-            qe = pl.q_end;
-        }
-        if (pl.t_end > te) {
-            FA_CUDA(cudaMemcpyAsync(r.t + te, tseq + te, pl.t_end - te, cudaMemcpyHostToDevice, r.cs));
-            te = pl.t_end;
-        }
+        auto up16 = [](uint64_t x, uint64_t cap) { return std::min(cap, (x + 15) & ~(uint64_t)15); };
+        const uint64_t qn = std::max(qe, up16(pl.q_end, qseq_len)), tn = std::max(te, up16(pl.t_end, tseq_len));
+        if (int rc = up.upload(qe, qn, te, tn, r.cs)) return rc;
         FA_CUDA(cudaEventRecord(r.slice_ev[k], r.cs));
         FA_CUDA(cudaStreamWaitEvent(r.s, r.slice_ev[k], 0));
         if (k == 0) FA_CUDA(cudaEventRecord(r.ev0, r.s));
+        if (int rc = up.prepare(qe, qn, te, tn, r.s)) return rc;
+        qe = qn;
+        te = tn;
         FA_CUDA(launch_mate_plan(pl, r.jobs + j0, r.order + j0, cnt, r.q, r.t, r.out + j0, r.cells, r.status, r.rev,
                                  r.s, launches));
         if (early_out) {
@@ -2037,18 +2086,23 @@ uint32_t mate_max_slice(uint32_t n) {
 // A byte-code host mate-SW batch of kPipeMinJobs jobs or more, sliced (enqueue_mate_sliced)
 // on the context's main, copy and prep streams; results into a page-locked `out` come back
 // slice by slice.  Results and statistics are those of one launch over the batch.
-int mate_host_sliced(fa_ctx *c, const fa_mate_params *p, const fa_mate_job *jobs, uint32_t n, const uint8_t *qseq,
-                     uint64_t qseq_len, const uint8_t *tseq, uint64_t tseq_len, fa_kswr *out, fa_ext_stats *stats,
-                     std::chrono::steady_clock::time_point t0, bool *done) {
-    *done = false;
-    if (!c || !p || p->m != 5 || !jobs || !out || n < kPipeMinJobs || c->slices_single == 1) return FA_OK;
+// `make_up(qseq_dev, tseq_dev)` gives the sequence functor once the byte buffers exist; the
+// caller has checked that slicing applies (mate_sliceable).
+bool mate_sliceable(fa_ctx *c, const fa_mate_params *p, const fa_mate_job *jobs, uint32_t n, const fa_kswr *out) {
+    return c && p && p->m == 5 && jobs && out && n >= kPipeMinJobs && c->slices_single != 1;
+}
+
+template <class MakeUp>
+int mate_host_sliced(fa_ctx *c, const fa_mate_params *p, const fa_mate_job *jobs, uint32_t n, uint64_t qseq_len,
+                     uint64_t tseq_len, MakeUp make_up, fa_kswr *out, fa_ext_stats *stats,
+                     std::chrono::steady_clock::time_point t0) {
     FA_CUDA(cudaSetDevice(c->device));
     FA_CUDA(c->jobs.ensure(sizeof(fa_mate_job) * (size_t)n));
     FA_CUDA(c->order.ensure(4ull * n));
     FA_CUDA(c->out.ensure(sizeof(fa_kswr) * (size_t)n));
     FA_CUDA(c->misc.ensure(kMiscBytes));
-    FA_CUDA(c->qseq.ensure(qseq_len + 1));
-    FA_CUDA(c->tseq.ensure(tseq_len + 1));
+    FA_CUDA(c->qseq.ensure(((qseq_len + 15) & ~(uint64_t)15) + 16));   // unpacking writes whole 16-base words
+    FA_CUDA(c->tseq.ensure(((tseq_len + 15) & ~(uint64_t)15) + 16));
     FA_CUDA(c->mate_rev.ensure(4ull * (2 + (size_t)mate_max_slice(n))));
     if (int rc = ensure_pipe_streams(c)) return rc;
     if (int rc = ensure_host_stage(c, 4ull * n)) return rc;
@@ -2063,8 +2117,12 @@ int mate_host_sliced(fa_ctx *c, const fa_mate_params *p, const fa_mate_job *jobs
                          c->order.as<uint32_t>(), c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(), c->out.as<fa_kswr>(),
                          m.cells, m.status, c->mate_rev.as<uint32_t>()};
     uint32_t launches = 0;
-    const int rc = enqueue_mate_sliced(p, jobs, n, qseq, qseq_len, tseq, tseq_len, static_cast<uint32_t *>(c->h_stage),
-                                       early ? out : nullptr, r, &launches);
+    int rc = FA_OK;
+    const auto up = make_up(c->qseq.as<uint8_t>(), c->tseq.as<uint8_t>(), &rc);
+    if (rc == FA_OK) rc = up.init(cs, s, m.status);
+    if (rc == FA_OK)
+        rc = enqueue_mate_sliced(p, jobs, n, qseq_len, tseq_len, up, static_cast<uint32_t *>(c->h_stage),
+                                 early ? out : nullptr, r, &launches);
     if (rc) {
         cudaStreamSynchronize(cs);
         cudaStreamSynchronize(s);
@@ -2072,7 +2130,6 @@ int mate_host_sliced(fa_ctx *c, const fa_mate_params *p, const fa_mate_job *jobs
         return rc;
     }
     FA_CUDA(cudaEventRecord(c->ev1, s));
-    *done = true;
     const int rs = read_status(c, s);
     FA_CUDA(cudaStreamSynchronize(ds));
     FA_CUDA(cudaStreamSynchronize(cs));
@@ -3084,8 +3141,9 @@ int fa_pair_batch(fa_ctx *c, const fa_params *p, const fa_policy *pol, const fa_
                              c->pm_out.as<fa_kswr>(),
                              reinterpret_cast<unsigned long long *>(c->pm_misc.as<char>() + 8),
                              c->pm_misc.as<uint32_t>(), c->pm_rev.as<uint32_t>()};
-        if (int rc = enqueue_mate_sliced(mp, mjobs, mn, mqseq, mqseq_len, mtseq, mtseq_len,
-                                         static_cast<uint32_t *>(c->h_stage), nullptr, r, &mlaunches)) {
+        const MateBytesUp up{mqseq, mtseq, c->pm_q.as<uint8_t>(), c->pm_t.as<uint8_t>()};
+        if (int rc = enqueue_mate_sliced(mp, mjobs, mn, mqseq_len, mtseq_len, up, static_cast<uint32_t *>(c->h_stage),
+                                         nullptr, r, &mlaunches)) {
             cudaStreamSynchronize(c->pm_copy);
             cudaStreamSynchronize(ms);
             return rc;
@@ -3155,9 +3213,10 @@ int fa_mate_sw_batch(fa_ctx *c, const fa_mate_params *p, const fa_mate_job *jobs
     auto t0 = std::chrono::steady_clock::now();
     if (stats) memset(stats, 0, sizeof(*stats));
     if (n && (!qseq || !tseq)) return fail(FA_ERR_ARG, "null buffer");
-    bool done = false;
-    if (int rc = mate_host_sliced(c, p, jobs, n, qseq, qseq_len, tseq, tseq_len, out, stats, t0, &done)) return rc;
-    if (done) return FA_OK;
+    if (mate_sliceable(c, p, jobs, n, out))
+        return mate_host_sliced(c, p, jobs, n, qseq_len, tseq_len,
+                                [&](uint8_t *dq, uint8_t *dt, int *) { return MateBytesUp{qseq, tseq, dq, dt}; }, out,
+                                stats, t0);
     auto upload = [&](cudaStream_t s) -> int {
         FA_CUDA(c->qseq.ensure(qseq_len));
         FA_CUDA(c->tseq.ensure(tseq_len));
@@ -3176,10 +3235,29 @@ int fa_mate_sw_batch_packed(fa_ctx *c, const fa_mate_params *p, const fa_mate_jo
     HostSeq hq, ht;
     if (int rc = host_packed(qseq, "query", &hq)) return rc;
     if (int rc = host_packed(tseq, "target", &ht)) return rc;
+    auto up16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
+    if (mate_sliceable(c, p, jobs, n, out)) {
+        auto make_up = [&](uint8_t *dq, uint8_t *dt, int *rc) {
+            const size_t bq = up16(hq.nbytes) + 16, bt = up16(ht.nbytes) + 16;
+            const size_t brq = up16(sizeof(fa_nrun) * hq.n_runs), brt = up16(sizeof(fa_nrun) * ht.n_runs);
+            MatePackedUp up{hq, ht, nullptr, nullptr, dq, dt, nullptr, nullptr, misc_of(c).status};
+            const cudaError_t e = c->mate_pk.ensure(bq + bt + brq + brt);
+            if (e != cudaSuccess) {
+                *rc = fail(FA_ERR_CUDA, "%s", cudaGetErrorString(e));
+                return up;
+            }
+            char *k = c->mate_pk.as<char>();
+            up.pq = reinterpret_cast<uint8_t *>(k);
+            up.pt = reinterpret_cast<uint8_t *>(k + bq);
+            up.rq = reinterpret_cast<fa_nrun *>(k + bq + bt);
+            up.rt = reinterpret_cast<fa_nrun *>(k + bq + bt + brq);
+            return up;
+        };
+        return mate_host_sliced(c, p, jobs, n, hq.npos, ht.npos, make_up, out, stats, t0);
+    }
     // the packed bases and N runs go up, and the device unpacks them to byte codes for the
     // SW kernels (which read each base many times, from cache); the runs are checked there
     auto upload = [&](cudaStream_t s) -> int {
-        auto up16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
         FA_CUDA(c->qseq.ensure(up16(hq.npos) + 16));
         FA_CUDA(c->tseq.ensure(up16(ht.npos) + 16));
         const size_t bq = up16(hq.nbytes) + 16, bt = up16(ht.nbytes) + 16;

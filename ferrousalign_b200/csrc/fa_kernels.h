@@ -101,6 +101,10 @@ size_t pack_runs_scratch_words(uint64_t n);
 // the N runs applied; d_dst 16-byte aligned with room for a multiple of 16 bytes past n.
 cudaError_t launch_unpack2(const uint8_t *d_src, uint64_t n, const fa_nrun *d_runs, uint32_t n_runs, uint8_t *d_dst,
                            cudaStream_t s);
+// positions [p0, p1) only (p0 a multiple of 16; whole 16-base words are written, so p1 is a
+// multiple of 16 or the buffer's end), the N runs' bases inside the range back to code 4
+cudaError_t launch_unpack2_range(const uint8_t *d_src, uint64_t p0, uint64_t p1, const fa_nrun *d_runs,
+                                 uint32_t n_runs, uint8_t *d_dst, cudaStream_t s);
 
 // Mate-rescue local SW.  `byte_lanes` selects the u8 (16-lane) or i16 (8-lane)
 // emulation of the reference's striped kernels; d_order lists the jobs of that kind.

@@ -168,29 +168,37 @@ unpack2_kernel(const uint32_t *__restrict__ src, uint64_t n, uint8_t *__restrict
     *reinterpret_cast<uint4 *>(dst + w * 16) = o;   // the destination is padded to 16 bytes
 }
 
-// one thread per N run: its bases back to code 4
+// one thread per N run: its bases in [lo, hi) back to code 4
 __global__ void __launch_bounds__(kPackThreads)
-apply_runs_kernel(const fa_nrun *__restrict__ runs, uint32_t nr, uint64_t n, uint8_t *__restrict__ dst)
+apply_runs_kernel(const fa_nrun *__restrict__ runs, uint32_t nr, uint64_t lo, uint64_t hi, uint8_t *__restrict__ dst)
 {
     const uint32_t k = blockIdx.x * kPackThreads + threadIdx.x;
     if (k >= nr) return;
     const fa_nrun r = runs[k];
-    const uint64_t e = r.pos + r.len < n ? r.pos + r.len : n;
-    for (uint64_t q = r.pos; q < e; ++q) dst[q] = 4;
+    const uint64_t e = r.pos + r.len < hi ? r.pos + r.len : hi;
+    for (uint64_t q = r.pos > lo ? r.pos : lo; q < e; ++q) dst[q] = 4;
 }
 
 }  // namespace
 
+cudaError_t launch_unpack2_range(const uint8_t *d_src, uint64_t p0, uint64_t p1, const fa_nrun *d_runs,
+                                 uint32_t n_runs, uint8_t *d_dst, cudaStream_t s)
+{
+    if (p1 <= p0) return cudaSuccess;
+    if (p0 % 16) return cudaErrorInvalidValue;
+    const uint64_t words = (p1 - p0 + 15) / 16;
+    unpack2_kernel<<<(unsigned)((words + kPackThreads - 1) / kPackThreads), kPackThreads, 0, s>>>(
+        reinterpret_cast<const uint32_t *>(d_src) + p0 / 16, p1 - p0, d_dst + p0);
+    if (n_runs)
+        apply_runs_kernel<<<(n_runs + kPackThreads - 1) / kPackThreads, kPackThreads, 0, s>>>(d_runs, n_runs, p0, p1,
+                                                                                          d_dst);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_unpack2(const uint8_t *d_src, uint64_t n, const fa_nrun *d_runs, uint32_t n_runs, uint8_t *d_dst,
                            cudaStream_t s)
 {
-    if (n == 0) return cudaSuccess;
-    const uint64_t words = (n + 15) / 16;
-    unpack2_kernel<<<(unsigned)((words + kPackThreads - 1) / kPackThreads), kPackThreads, 0, s>>>(
-        reinterpret_cast<const uint32_t *>(d_src), n, d_dst);
-    if (n_runs)
-        apply_runs_kernel<<<(n_runs + kPackThreads - 1) / kPackThreads, kPackThreads, 0, s>>>(d_runs, n_runs, n, d_dst);
-    return cudaGetLastError();
+    return launch_unpack2_range(d_src, 0, n, d_runs, n_runs, d_dst, s);
 }
 
 size_t pack_runs_scratch_words(uint64_t n) { return (n + kRunBlockBytes - 1) / kRunBlockBytes + 1; }

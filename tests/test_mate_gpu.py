@@ -170,3 +170,25 @@ def test_sliced_host_batch(ctx):
         assert e.value.code == N.FA_ERR_ARG and "97123" in str(e.value)
     finally:
         c.close()
+
+
+def test_sliced_packed_batch_with_n_runs(ctx):
+    """The packed entry's sliced form (each slice's packed words uploaded, unpacked on the
+    device with its N runs) equals the byte entry on a 100k-job batch whose sequences carry N
+    bases and runs of N anywhere, slice boundaries included; bad runs are rejected."""
+    b = synth.workload_mate(100_000, seed=33)
+    q, t = b.qseq.copy(), b.tseq.copy()
+    rng = np.random.default_rng(7)
+    for buf in (q, t):
+        for k in rng.choice(len(buf) - 8, 3000, replace=False):
+            buf[k:k + int(rng.integers(1, 8))] = 4
+    mp = fa.make_mate_params()
+    want, wst = fa.mate_sw_batch(mp, b.jobs, q, t, ctx=ctx)
+    qp, tp = fa.pack(q), fa.pack(t)
+    got, st = fa.mate_sw_batch_packed(mp, b.jobs, qp, tp, ctx=ctx)
+    assert np.array_equal(got, want)
+    assert int(st["cells"]) == int(wst["cells"])
+    bad = fa.PackedSeq(qp.bases, qp.n_bases, qp.runs[::-1].copy())
+    with pytest.raises(N.NativeError) as e:
+        fa.mate_sw_batch_packed(mp, b.jobs, bad, tp, ctx=ctx)
+    assert e.value.code == N.FA_ERR_ARG
