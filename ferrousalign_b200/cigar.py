@@ -37,15 +37,41 @@ def infer_band_width(l_query: int, l_ref: int, score: int, a: int, o_del: int, e
     return min(w, cmd_w * 4)
 
 
+def _excl_cumsum(v: np.ndarray) -> np.ndarray:
+    o = np.zeros(len(v), np.int64)
+    if len(v) > 1:
+        np.cumsum(v[:-1], out=o[1:])
+    return o
+
+
 @dataclass
 class CigarBatch:
     results: np.ndarray        # CIGAR_RESULT_DT: OutScore fields and output lengths
     cigar: np.ndarray          # u32 words, job k's at cigar_off[k]
     ref_aligned: np.ndarray    # u8, job k's at ref_off[k]
     query_aligned: np.ndarray  # u8, job k's at qry_off[k]
-    cigar_off: np.ndarray
-    ref_off: np.ndarray
-    qry_off: np.ndarray
+    jobs: np.ndarray           # the batch's CIGAR_JOB_DT records: the offsets derive from them, so
+                               # they stay as they were while the offsets are read
+    first: np.ndarray | None = None   # the packed form's CIGAR offsets; slots of qlen + tlen + 2 without
+
+    # per-job offsets, computed on first use (a caller reading only the results never pays)
+    @property
+    def cigar_off(self) -> np.ndarray:
+        if self.first is None:
+            self.first = _excl_cumsum(self.jobs["qlen"].astype(np.int64) + self.jobs["tlen"] + 2)
+        return self.first
+
+    @property
+    def ref_off(self) -> np.ndarray:
+        if getattr(self, "_ref_off", None) is None:
+            self._ref_off = _excl_cumsum(self.jobs["tlen"])
+        return self._ref_off
+
+    @property
+    def qry_off(self) -> np.ndarray:
+        if getattr(self, "_qry_off", None) is None:
+            self._qry_off = _excl_cumsum(self.jobs["qlen"])
+        return self._qry_off
 
     def cigar_of(self, k: int) -> list[tuple[str, int]]:
         n = int(self.results["n_cigar"][k])
@@ -72,26 +98,24 @@ def scalar_banded_swa_batch(params: np.ndarray, jobs: np.ndarray, qseq: np.ndarr
     qseq = np.ascontiguousarray(qseq, np.uint8)
     tseq = np.ascontiguousarray(tseq, np.uint8)
     n = len(jobs)
-    q = jobs["qlen"].astype(np.int64)
-    t = jobs["tlen"].astype(np.int64)
-    cig_off = np.concatenate([[0], np.cumsum(q + t + 2)])
-    ref_off = np.concatenate([[0], np.cumsum(t)])
-    qry_off = np.concatenate([[0], np.cumsum(q)])
+    t_sum = int(jobs["tlen"].sum(dtype=np.int64))
+    q_sum = int(jobs["qlen"].sum(dtype=np.int64))
+    cig_total = q_sum + t_sum + 2 * n
     res = out_array(bufs, "res", n, CIGAR_RESULT_DT, zero=True)
-    ra = out_array(bufs, "ref_al", max(int(ref_off[-1]), 1), np.uint8)
-    qa = out_array(bufs, "qry_al", max(int(qry_off[-1]), 1), np.uint8)
+    ra = out_array(bufs, "ref_al", max(t_sum, 1), np.uint8)
+    qa = out_array(bufs, "qry_al", max(q_sum, 1), np.uint8)
     if packed:
         # capacity for every slot, of which only the used words' pages are ever touched
-        cig = out_array(bufs, "cigar", max(int(cig_off[-1]), 1), np.uint32)
+        cig = out_array(bufs, "cigar", max(cig_total, 1), np.uint32)
         first = out_array(bufs, "first", max(n, 1), np.uint64, zero=True)
         if n:
             N.check(lib.fa_cigar_batch_packed(ctx.handle, N.ptr(params), N.ptr(jobs), n, N.ptr(qseq), len(qseq),
                                               N.ptr(tseq), len(tseq), N.ptr(res), N.ptr(cig), len(cig),
                                               N.ptr(first), N.ptr(ra), N.ptr(qa)))
         total = int(res["n_cigar"].sum()) if n else 0
-        return CigarBatch(res, cig[:total], ra, qa, first[:n], ref_off[:-1], qry_off[:-1])
-    cig = np.zeros(max(int(cig_off[-1]), 1), np.uint32)
+        return CigarBatch(res, cig[:total], ra, qa, jobs, first[:n])
+    cig = np.zeros(max(cig_total, 1), np.uint32)
     if n:
         N.check(lib.fa_cigar_batch(ctx.handle, N.ptr(params), N.ptr(jobs), n, N.ptr(qseq), len(qseq), N.ptr(tseq),
                                    len(tseq), N.ptr(res), N.ptr(cig), N.ptr(ra), N.ptr(qa)))
-    return CigarBatch(res, cig, ra, qa, cig_off[:-1], ref_off[:-1], qry_off[:-1])
+    return CigarBatch(res, cig, ra, qa, jobs)

@@ -2816,8 +2816,11 @@ struct CigarRun {
 // context's stream.
 int cigar_launch(fa_ctx *c, const fa_params *p, const fa_cigar_job *jobs, uint32_t n, const uint8_t *qseq,
                  uint64_t qseq_len, const uint8_t *tseq, uint64_t tseq_len, CigarRun *r) {
-    // output and scratch offsets per job (the reference would panic on a range past its slices)
-    std::vector<CigarPlan> plan(n);
+    // output and scratch offsets per job (the reference would panic on a range past its slices),
+    // and the band order after them, built in page-locked staging so they go up asynchronously
+    if (int rc = ensure_host_stage(c, (sizeof(CigarPlan) + 4) * (size_t)n)) return rc;
+    CigarPlan *plan = static_cast<CigarPlan *>(c->h_stage);
+    uint32_t *order = reinterpret_cast<uint32_t *>(plan + n);
     uint64_t cig = 0, ref = 0, qry = 0, eh = 0, tb = 0;
     int max_mat = 0, qmax = 0;
     for (int i = 0; i < 25; ++i) max_mat = std::max<int>(max_mat, p->mat[i]);
@@ -2845,14 +2848,12 @@ int cigar_launch(fa_ctx *c, const fa_params *p, const fa_cigar_job *jobs, uint32
     const bool smem = narrow && qmax <= cigar_smem_qcap();
     // shared-memory kernel: jobs ordered by band, widest first (a counting sort), so that a
     // warp's jobs run rows of similar length
-    std::vector<uint32_t> order;
     if (smem) {
         constexpr int kBins = 1024;
         std::vector<uint32_t> cnt(kBins + 1, 0);
         auto bin = [&](uint32_t k) { return kBins - 1 - std::min(jobs[k].w, kBins - 1); };
         for (uint32_t k = 0; k < n; ++k) ++cnt[bin(k) + 1];
         for (int b = 0; b < kBins; ++b) cnt[b + 1] += cnt[b];
-        order.resize(n);
         for (uint32_t k = 0; k < n; ++k) order[cnt[bin(k)]++] = k;
     }
     FA_CUDA(cudaSetDevice(c->device));
@@ -2860,7 +2861,7 @@ int cigar_launch(fa_ctx *c, const fa_params *p, const fa_cigar_job *jobs, uint32
     auto up16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
     const size_t b_jobs = up16(sizeof(fa_cigar_job) * n), b_plan = up16(sizeof(CigarPlan) * n);
     // (the kernel loads a step's eight query bases together, up to seven past a job's end)
-    const size_t b_q = up16(qseq_len + 8), b_t = up16(tseq_len + 1), b_ord = up16(4ull * order.size());
+    const size_t b_q = up16(qseq_len + 8), b_t = up16(tseq_len + 1), b_ord = smem ? up16(4ull * n) : 0;
     FA_CUDA(c->cg_in.ensure(b_jobs + b_plan + b_q + b_t + b_ord));
     char *in = c->cg_in.as<char>();
     fa_cigar_job *d_jobs = reinterpret_cast<fa_cigar_job *>(in);
@@ -2885,8 +2886,8 @@ int cigar_launch(fa_ctx *c, const fa_params *p, const fa_cigar_job *jobs, uint32
     r->n_ref = ref;
     r->n_qry = qry;
     FA_CUDA(cudaMemcpyAsync(d_jobs, jobs, sizeof(fa_cigar_job) * n, cudaMemcpyHostToDevice, s));
-    FA_CUDA(cudaMemcpyAsync(d_plan, plan.data(), sizeof(CigarPlan) * n, cudaMemcpyHostToDevice, s));
-    if (smem) FA_CUDA(cudaMemcpyAsync(d_order, order.data(), 4ull * n, cudaMemcpyHostToDevice, s));
+    FA_CUDA(cudaMemcpyAsync(d_plan, plan, sizeof(CigarPlan) * n, cudaMemcpyHostToDevice, s));
+    if (smem) FA_CUDA(cudaMemcpyAsync(d_order, order, 4ull * n, cudaMemcpyHostToDevice, s));
     if (qseq_len) FA_CUDA(cudaMemcpyAsync(d_q, qseq, qseq_len, cudaMemcpyHostToDevice, s));
     if (tseq_len) FA_CUDA(cudaMemcpyAsync(d_t, tseq, tseq_len, cudaMemcpyHostToDevice, s));
     const ExtParams kp = ext_params_of(p);
