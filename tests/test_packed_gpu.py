@@ -168,3 +168,49 @@ def test_bad_runs_rejected(nrich):
         with pytest.raises(N.NativeError) as e:
             fa.extend_batch_packed(p, b.jobs[:100], q2, tp)
         assert e.value.code == N.FA_ERR_ARG
+
+
+def test_streamed_n_rich_batches_equal_unsliced(nrich):
+    """The streamed host path on the N-rich packed batch (N runs across slice boundaries, left
+    and right jobs of 30-300 bases): single band, bwa-mem2 policy and learned band give the
+    unsliced call's results, cells and bands."""
+    b = nrich
+    p = fa.BandedPairWiseSW().to_struct()
+    qp, tp = fa.pack(b.qseq), fa.pack(b.tseq)
+    model = B.BandModel.load()
+    bwa = fa.make_policy(N.FA_POLICY_BWA, 2)
+    with fa.Context(0) as ctx:
+        def run():
+            return [fa.extend_batch_packed(p, b.jobs, qp, tp, ctx=ctx),
+                    fa.extend_batch_packed(p, b.jobs, qp, tp, policy=bwa, ctx=ctx),
+                    fa.extend_batch_learned_packed(p, b.jobs, qp, tp, model, ctx=ctx)]
+        ctx.set_slices(1, 1)
+        want = run()
+        for slices in ((-1, -1), (8, 8), (2, 2)):
+            ctx.set_slices(*slices)
+            got = run()
+            for g, w in zip(got, want):
+                assert np.array_equal(g[0], w[0]), slices
+                assert int(g[1]["cells_executed"]) == int(w[1]["cells_executed"]), slices
+            assert np.array_equal(got[1][2], want[1][2]) and np.array_equal(got[2][3], want[2][3])
+
+
+def test_streamed_batch_at_the_threshold():
+    """Exactly 32,768 jobs in eight slices (the smallest about a thousand jobs): byte and packed
+    forms, single band and bwa-mem2 policy, equal to the unsliced call."""
+    b = synth.workload_ext_1m(32_768, seed=55)
+    p = fa.BandedPairWiseSW().to_struct()
+    qp, tp = fa.pack(b.qseq), fa.pack(b.tseq)
+    bwa = fa.make_policy(N.FA_POLICY_BWA, 2)
+    with fa.Context(0) as ctx:
+        def run():
+            return [fa.extend_batch(p, b.jobs, b.qseq, b.tseq, ctx=ctx)[0].copy(),
+                    fa.extend_batch(p, b.jobs, b.qseq, b.tseq, policy=bwa, ctx=ctx)[0].copy(),
+                    fa.extend_batch_packed(p, b.jobs, qp, tp, ctx=ctx)[0].copy(),
+                    fa.extend_batch_packed(p, b.jobs, qp, tp, policy=bwa, ctx=ctx)[0].copy()]
+        ctx.set_slices(1, 1)
+        want = run()
+        ctx.set_slices(8, 8)
+        got = run()
+    for g, w in zip(got, want):
+        assert np.array_equal(g, w)
