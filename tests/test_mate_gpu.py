@@ -192,3 +192,22 @@ def test_sliced_packed_batch_with_n_runs(ctx):
     with pytest.raises(N.NativeError) as e:
         fa.mate_sw_batch_packed(mp, b.jobs, bad, tp, ctx=ctx)
     assert e.value.code == N.FA_ERR_ARG
+
+
+def test_sliced_batch_out_of_sequence_order(ctx):
+    """Mate jobs in random order (a slice's jobs reach anywhere in the buffers): the sliced
+    host path, byte and packed forms, still equals the unsliced call."""
+    b = synth.workload_mate(60_000, seed=35)
+    jobs = b.jobs[np.random.default_rng(2).permutation(len(b.jobs))]
+    mp = fa.make_mate_params()
+    c = fa.Context(0)
+    try:
+        c.set_slices(1, 1)
+        want, _ = fa.mate_sw_batch(mp, jobs, b.qseq, b.tseq, ctx=c)
+        c.set_slices(-1, -1)
+        got, _ = fa.mate_sw_batch(mp, jobs, b.qseq, b.tseq, ctx=c)
+        assert np.array_equal(got, want)
+        got_p, _ = fa.mate_sw_batch_packed(mp, jobs, fa.pack(b.qseq), fa.pack(b.tseq), ctx=c)
+        assert np.array_equal(got_p, want)
+    finally:
+        c.close()
