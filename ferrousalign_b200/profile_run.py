@@ -1,7 +1,7 @@
 """One device-resident extension batch of the bench workload, for ncu captures.
 
-Usage: python -m ferrousalign_b200.profile_run [n_jobs] [probe|-] [kernel: 0 auto, 1 int32, 2 int16x2, 3 rows2] [reps]
-       [threads per block]
+Usage: python -m ferrousalign_b200.profile_run [n_jobs] [probe|uneven|-] [kernel: 0 auto, 1 int32, 2 int16x2, 3 rows2]
+       [reps] [threads per block]   (uneven: the 50-300 bp mixed left/right workload)
        python -m ferrousalign_b200.profile_run learned [n_jobs] [reps] [kernel]   (learned-band path)
        python -m ferrousalign_b200.profile_run bands [n_jobs]            (single runs at fixed bands)
        python -m ferrousalign_b200.profile_run mate [n_jobs] [reps]      (mate-rescue SW, device-resident)
@@ -140,7 +140,7 @@ if len(sys.argv) > 1 and sys.argv[1] in ("learned", "bands"):
     sys.exit(0)
 
 n = int(sys.argv[1]) if len(sys.argv) > 1 else 1_000_000
-b = synth.workload_ext_1m(n)
+b = synth.workload_ext_uneven(n) if len(sys.argv) > 2 and sys.argv[2] == "uneven" else synth.workload_ext_1m(n)
 p = fa.BandedPairWiseSW().to_struct()
 ctx = fa.Context(0)
 lib = N.load()
