@@ -81,7 +81,6 @@ __host__ __device__ inline uint32_t dup16(int v) { return (uint32_t)(v & 0xFFFF)
 
 }  // namespace
 
-constexpr int kRows2MaxQ = 254;   // u8 column words: h0 >= 1 and a >= 1 leave qlen <= 254
 
 // One job.  eh[slot(c) * T]: the column word of column c (H | E << 8); with RING = R > 0 only
 // R slots, column c in slot c mod R, for bands with 2w + 3 <= R (a row pair touches at most
@@ -654,7 +653,7 @@ cudaError_t launch_rows2_seq(const fa_job *d_jobs, const uint32_t *d_order, uint
                              int qcap, int ring, bool cert, const int32_t *d_w_try, fa_ext_result *d_out,
                              uint8_t *d_clamped, uint32_t *d_cells_job, unsigned long long *d_cells,
                              uint32_t *d_status, uint32_t *d_ovf, uint32_t *d_ovf_n, cudaStream_t stream, int tpb,
-                             uint32_t *d_work)
+                             uint32_t *d_work, cudaStream_t ovf_stream, cudaEvent_t ovf_ev)
 {
     if (n == 0) return cudaSuccess;
     if (!ext_rows2_eligible(p, qcap) || !d_ovf || !d_ovf_n) return cudaErrorInvalidValue;
@@ -717,6 +716,11 @@ cudaError_t launch_rows2_seq(const fa_job *d_jobs, const uint32_t *d_order, uint
 #undef FA_ROWS2
 #undef FA_PERSIST
     if (err != cudaSuccess) return err;
+    if (ovf_stream) {
+        if ((err = cudaEventRecord(ovf_ev, stream)) != cudaSuccess) return err;
+        if ((err = cudaStreamWaitEvent(ovf_stream, ovf_ev, 0)) != cudaSuccess) return err;
+        stream = ovf_stream;
+    }
     // jobs whose scores can pass 255: the int32 kernel over the overflow list, same settings
     return launch_ext_packed(d_jobs, d_ovf, n, nullptr, d_ovf_n, d_qseq, d_tseq, p, qcap, ring, d_w_try, d_out,
                              d_clamped, c, d_cells_job, d_cells, d_status, stream);
@@ -728,15 +732,16 @@ cudaError_t launch_ext_rows2(const fa_job *d_jobs, const uint32_t *d_order, uint
                              int qcap, int ring, bool cert, const int32_t *d_w_try, fa_ext_result *d_out,
                              uint8_t *d_clamped, uint32_t *d_cells_job, unsigned long long *d_cells,
                              uint32_t *d_status, uint32_t *d_ovf, uint32_t *d_ovf_n, cudaStream_t stream, int tpb,
-                             uint32_t *d_work)
+                             uint32_t *d_work, cudaStream_t ovf_stream, cudaEvent_t ovf_ev)
 {
+    if (ovf_stream && !ovf_ev) return cudaErrorInvalidValue;
     return d_qseq.packed
                ? launch_rows2_seq<true>(d_jobs, d_order, n, d_first, d_n, d_qseq, d_tseq, p, qcap, ring, cert, d_w_try,
                                         d_out, d_clamped, d_cells_job, d_cells, d_status, d_ovf, d_ovf_n, stream, tpb,
-                                        d_work)
+                                        d_work, ovf_stream, ovf_ev)
                : launch_rows2_seq<false>(d_jobs, d_order, n, d_first, d_n, d_qseq, d_tseq, p, qcap, ring, cert,
                                          d_w_try, d_out, d_clamped, d_cells_job, d_cells, d_status, d_ovf, d_ovf_n,
-                                         stream, tpb, d_work);
+                                         stream, tpb, d_work, ovf_stream, ovf_ev);
 }
 
 }  // namespace fa

@@ -102,6 +102,11 @@ struct fa_ctx {
     // learned rounds run their band groups on forked streams: fork on `stream`, join back
     cudaStream_t aux[2] = {nullptr, nullptr};
     cudaEvent_t fork_ev = nullptr, join_ev[2] = {nullptr, nullptr};
+    // multi-class launches: the int32 work (overflow passes, classes past the two-row
+    // kernel's columns) on its own stream, and one overflow count per class
+    cudaStream_t side = nullptr;
+    cudaEvent_t side_fork = nullptr, side_join = nullptr;
+    DevBuf class_ovf_n;
     // a second lane for sliced host batches (alternate slices run concurrently): its own
     // stream, band-group streams and events, and scratch counters
     // (lane 0 is `stream` with misc, aux, fork_ev and join_ev; lanes 1 .. kLanes-1 here)
@@ -218,9 +223,14 @@ using Choice = fa_ctx::Choice;
 
 // The two-row kernel's overflow list (`words` entries), its count and the persistent
 // launch's job counter.
+// side / side_ev (optional): the stream the int32 work runs on (the overflow pass, or the
+// whole launch when the capacity is past the two-row kernel's columns), forked from the
+// launch stream by side_ev.
 struct OvfRes {
     uint32_t *list, *count, *work;
     size_t words;
+    cudaStream_t side = nullptr;
+    cudaEvent_t side_ev = nullptr;
 };
 
 cudaError_t launch_ext_res(fa_ctx *c, Choice kc, const fa_job *d_jobs, const uint32_t *d_order, uint32_t n,
@@ -231,10 +241,17 @@ cudaError_t launch_ext_res(fa_ctx *c, Choice kc, const fa_job *d_jobs, const uin
     if (kc.kernel == FA_KERNEL_ROWS2 && !cert && ext_rows2_eligible(kp, qcap) &&
         ext_rows2_smem_bytes(qcap, kc.tpb, 0) <= c->smem_optin && r.words >= (size_t)n && r.list)
         return launch_ext_rows2(d_jobs, d_order, n, nullptr, d_n, d_q, d_t, kp, qcap, 0, false, d_w_try, d_out,
-                                d_clamped, d_cells_job, d_cells, d_status, r.list, r.count, s, kc.tpb, r.work);
+                                d_clamped, d_cells_job, d_cells, d_status, r.list, r.count, s, kc.tpb, r.work,
+                                r.side, r.side_ev);
     if (kc.kernel == FA_KERNEL_INT16X2 && ext_pair_eligible(kp) && !cert && !d_q.packed)
         return launch_ext_pair(d_jobs, d_order, n, d_n, d_q, d_t, kp, qcap, d_w_try, d_out, d_clamped,
                                d_cells_job, d_cells, d_status, s);
+    if (r.side && qcap > kRows2MaxQ) {
+        cudaError_t e = cudaEventRecord(r.side_ev, s);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(r.side, r.side_ev, 0);
+        if (e != cudaSuccess) return e;
+        s = r.side;
+    }
     return launch_ext_packed(d_jobs, d_order, n, nullptr, d_n, d_q, d_t, kp, qcap, 0, d_w_try, d_out, d_clamped,
                              cert, d_cells_job, d_cells, d_status, s, kc.tpb);
 }
@@ -258,6 +275,67 @@ cudaError_t launch_ext(fa_ctx *c, Choice kc, const fa_job *d_jobs, const uint32_
 uint32_t ext_kernels_of(fa_ctx *c, Choice kc, const ExtParams &kp, int qcap) {
     return kc.kernel == FA_KERNEL_ROWS2 && ext_rows2_eligible(kp, qcap) &&
                    ext_rows2_smem_bytes(qcap, kc.tpb, 0) <= c->smem_optin ? 2u : 1u;
+}
+
+// The side stream, its events and one overflow count per capacity class (outside any
+// capture: it may allocate).
+int ensure_side(fa_ctx *c, size_t classes) {
+    if (!c->side) {
+        FA_CUDA(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+        FA_CUDA(cudaEventCreateWithFlags(&c->side_fork, cudaEventDisableTiming));
+        FA_CUDA(cudaEventCreateWithFlags(&c->side_join, cudaEventDisableTiming));
+    }
+    FA_CUDA(c->class_ovf_n.ensure(sizeof(uint32_t) * std::max<size_t>(classes, 64)));
+    return FA_OK;
+}
+
+// The capacity classes of a length-sorted order (segs: each class's end and capacity, longest
+// first), one launch each on stream s.  With several classes the int32 work -- each two-row
+// launch's overflow pass (its own list in the overflow buffer at the class's offset, its own
+// count) and every class past the two-row kernel's columns -- runs on the side stream, so the
+// longest jobs, a few warps per SM whose time is set by their own latency, overlap the shorter
+// classes' launches instead of following each of them; the side stream joins s at the end.
+cudaError_t launch_classes(fa_ctx *c, const std::vector<std::pair<uint32_t, int>> &segs,
+                           const std::function<Choice(size_t)> &kc_of, const fa_job *d_jobs,
+                           const uint32_t *d_order, const SeqBuf &d_q, const SeqBuf &d_t, const ExtParams &kp,
+                           const int32_t *d_w_try, fa_ext_result *d_out, uint8_t *d_flags, bool cert,
+                           uint32_t *d_cells_job, unsigned long long *d_cells, uint32_t *d_status, cudaStream_t s,
+                           uint32_t *launches) {
+    const bool side = segs.size() > 1 && c->side && c->misc.p &&
+                      c->class_ovf_n.cap >= sizeof(uint32_t) * segs.size() &&
+                      c->ovf.cap >= sizeof(uint32_t) * (size_t)segs.back().first;
+    if (side) {
+        // the side stream joins the launch sequence (and any capture) from the start
+        cudaError_t e = cudaEventRecord(c->side_fork, s);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(c->side, c->side_fork, 0);
+        if (e != cudaSuccess) return e;
+    }
+    const size_t ovf_words = c->ovf.cap / (3 * sizeof(uint32_t));
+    uint32_t b = 0;
+    for (size_t k = 0; k < segs.size(); ++k) {
+        const auto &sg = segs[k];
+        const Choice kc = kc_of(k);
+        OvfRes r{c->misc.p ? c->ovf.as<uint32_t>() : nullptr, c->misc.p ? misc_of(c).ovf_n : nullptr,
+                 c->misc.p ? misc_of(c).work : nullptr, ovf_words};
+        if (side) {
+            r.list = c->ovf.as<uint32_t>() + b;
+            r.count = c->class_ovf_n.as<uint32_t>() + k;
+            r.words = sg.first - b;
+            r.side = c->side;
+            r.side_ev = c->side_fork;
+        }
+        cudaError_t e = launch_ext_res(c, kc, d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp, sg.second,
+                                       d_w_try, d_out, d_flags, cert, d_cells_job, d_cells, d_status, s, r);
+        if (e != cudaSuccess) return e;
+        if (launches) *launches += ext_kernels_of(c, kc, kp, sg.second);
+        b = sg.first;
+    }
+    if (side) {
+        cudaError_t e = cudaEventRecord(c->side_join, c->side);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s, c->side_join, 0);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 // The kernel a call runs.  A fixed setting is used as is.  FA_KERNEL_AUTO is an
@@ -561,14 +639,8 @@ int enqueue_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n
     // first-round kernel of each capacity class (tuned per class); retries use kc
     auto kc_of = [&](size_t k) { return seg_kc && k < seg_kc->size() ? (*seg_kc)[k] : kc; };
     if (mode == FA_POLICY_SINGLE) {
-        uint32_t b = 0;
-        for (size_t k = 0; k < segs0.size(); ++k) {
-            const auto &sg = segs0[k];
-            FA_CUDA(launch_ext(c, kc_of(k), d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp, sg.second,
-                               nullptr, d_out, nullptr, false, c->cells_job.as<uint32_t>(), m.cells, m.status, s));
-            *launches += ext_kernels_of(c, kc_of(k), kp, sg.second);
-            b = sg.first;
-        }
+        FA_CUDA(launch_classes(c, segs0, kc_of, d_jobs, d_order, d_q, d_t, kp, nullptr, d_out, nullptr, false,
+                               c->cells_job.as<uint32_t>(), m.cells, m.status, s, launches));
         return FA_OK;
     }
     PolicyState st{c->w_cur.as<int32_t>(), c->prev.as<int32_t>(), c->kk.as<int32_t>(),
@@ -598,15 +670,8 @@ int enqueue_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n
         // with one narrow try, rounds after the narrow ones hold only plain-policy runs
         const bool cert_r = cert && !(once && r >= narrow_rounds);
         if (r == 0 && !learned) {
-            uint32_t b = 0;
-            for (size_t k = 0; k < segs0.size(); ++k) {
-                const auto &sg = segs0[k];
-                FA_CUDA(launch_ext(c, kc_of(k), d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp, sg.second,
-                                   st.w_cur, d_out, d_flags, cert_r, c->cells_job.as<uint32_t>(), m.cells, m.status,
-                                   s));
-                *launches += ext_kernels_of(c, kc_of(k), kp, sg.second);
-                b = sg.first;
-            }
+            FA_CUDA(launch_classes(c, segs0, kc_of, d_jobs, d_order, d_q, d_t, kp, st.w_cur, d_out, d_flags, cert_r,
+                                   c->cells_job.as<uint32_t>(), m.cells, m.status, s, launches));
         } else if (learned && !cert_r && c->kernel != FA_KERNEL_INT16X2) {
             // after the narrow tries every job left runs the plain policy: one launch of the
             // call's autotuned kernel over the compacted list
@@ -699,6 +764,8 @@ int run_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n,
     uint32_t launches = 0, retries = 0;
     if (pol && pol->mode != FA_POLICY_SINGLE)
         if (int rc = ensure_policy_buffers(c, n)) return rc;
+    if (segs.size() > 1)
+        if (int rc = ensure_side(c, segs.size())) return rc;
     int rc0 = FA_OK;
     const Choice kc = resolve_choice(c, kp, d_jobs, d_order, n, d_q, d_t, qcap_all, band, d_out, misc_of(c).status, s,
                                      &rc0);
@@ -756,6 +823,8 @@ int run_ext_graph(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t
     if (pol && pol->mode != FA_POLICY_SINGLE)
         if (int rc = ensure_policy_buffers(c, n)) return rc;
     if (int rc = ensure_aux_streams(c)) return rc;
+    if (segs.size() > 1)
+        if (int rc = ensure_side(c, segs.size())) return rc;
     int rc0 = FA_OK;
     const Choice kc = resolve_choice(c, kp, c->jobs.as<fa_job>(), c->order.as<uint32_t>(), n, c->cq, c->ct, qcap,
                                      max_w, c->out.as<fa_ext_result>(),
@@ -1881,14 +1950,11 @@ int ext_batch_device(fa_ctx *c, const fa_params *p, const fa_job *d_jobs, uint32
         }
         c->last_choice = kc;
     }
-    uint32_t b = 0;
+    if (segs.size() > 1)
+        if (int rc = ensure_side(c, segs.size())) return rc;
     if (c->timing) FA_CUDA(cudaEventRecord(c->kev0, s));
-    for (size_t k = 0; k < segs.size(); ++k) {
-        const auto &sg = segs[k];
-        FA_CUDA(launch_ext(c, seg_kc[k], d_jobs, order + b, sg.first - b, nullptr, d_qseq, d_tseq, kp, sg.second,
-                           nullptr, d_out, nullptr, false, nullptr, nullptr, m.status, s));
-        b = sg.first;
-    }
+    FA_CUDA(launch_classes(c, segs, [&](size_t k) { return seg_kc[k]; }, d_jobs, order, d_qseq, d_tseq, kp, nullptr,
+                           d_out, nullptr, false, nullptr, nullptr, m.status, s, nullptr));
     if (c->timing) FA_CUDA(cudaEventRecord(c->kev1, s));
     c->last_launches = d_order ? 1u : 2u;
     for (size_t k = 0; k < segs.size(); ++k) c->last_launches += ext_kernels_of(c, seg_kc[k], kp, segs[k].second);
@@ -2221,6 +2287,10 @@ void fa_ctx_destroy(fa_ctx *c) {
         if (c->aux[k]) cudaStreamDestroy(c->aux[k]);
     }
     if (c->fork_ev) cudaEventDestroy(c->fork_ev);
+    if (c->side) cudaStreamDestroy(c->side);
+    if (c->side_fork) cudaEventDestroy(c->side_fork);
+    if (c->side_join) cudaEventDestroy(c->side_join);
+    c->class_ovf_n.release();
     if (c->gexec) cudaGraphExecDestroy(c->gexec);
     for (auto &e : c->slice_ev)
         if (e) cudaEventDestroy(e);
