@@ -120,7 +120,8 @@ __host__ __device__ __forceinline__ uint32_t rows2_thread(
         return c;
     }
     if (h0 > 255 || a * qlen > 255 - h0) {
-        ovf[take_slot(ovf_n)] = jid;                  // needs wider cells: the int32 kernel
+        // needs wider cells: the int32 kernel (ovf null: the job was listed before the launch)
+        if (ovf) ovf[take_slot(ovf_n)] = jid;
         return 0;
     }
     const int w = ext_band_clamp(qlen, w_try ? w_try[jid] : jb.w, p);
@@ -612,6 +613,25 @@ ext_rows2_persist_kernel(const fa_job *__restrict__ jobs, const uint32_t *__rest
     }
 }
 
+// The jobs of order[first .. n) that rows2_thread hands on to the int32 kernel (valid
+// arguments, within qcap, h0 >= 1 and h0 + a * qlen > 255), listed before the two-row launch
+// so their int32 pass can start at once; the two-row launch then runs with a null list and
+// skips them.  Same sub-range rules as the two-row kernels (first_dev, n_dev).
+__global__ void rows2_ovf_list_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ order,
+                                      uint32_t n, const uint32_t *__restrict__ first_dev,
+                                      const uint32_t *__restrict__ n_dev, int qcap, int a,
+                                      uint32_t *__restrict__ ovf, uint32_t *__restrict__ ovf_n)
+{
+    const uint32_t first = first_dev ? *first_dev : 0u;
+    if (n_dev) n = min(n, *n_dev);
+    for (uint32_t gi = first + blockIdx.x * blockDim.x + threadIdx.x; gi < n; gi += gridDim.x * blockDim.x) {
+        const uint32_t jid = order ? order[gi] : gi;
+        const fa_job jb = jobs[jid];
+        if (jb.h0 < 1 || jb.qlen <= 0 || jb.tlen < 0 || jb.qlen > qcap) continue;
+        if (jb.h0 > 255 || a * jb.qlen > 255 - jb.h0) ovf[atomicAdd(ovf_n, 1u)] = jid;
+    }
+}
+
 bool ext_rows2_sym(const ExtParams &p) {
     return p.o_del + p.e_del == p.o_ins + p.e_ins && p.e_del == p.e_ins;
 }
@@ -653,7 +673,7 @@ cudaError_t launch_rows2_seq(const fa_job *d_jobs, const uint32_t *d_order, uint
                              int qcap, int ring, bool cert, const int32_t *d_w_try, fa_ext_result *d_out,
                              uint8_t *d_clamped, uint32_t *d_cells_job, unsigned long long *d_cells,
                              uint32_t *d_status, uint32_t *d_ovf, uint32_t *d_ovf_n, cudaStream_t stream, int tpb,
-                             uint32_t *d_work, cudaStream_t ovf_stream, cudaEvent_t ovf_ev)
+                             uint32_t *d_work, cudaStream_t ovf_stream, cudaEvent_t ovf_ev, bool ovf_early)
 {
     if (n == 0) return cudaSuccess;
     if (!ext_rows2_eligible(p, qcap) || !d_ovf || !d_ovf_n) return cudaErrorInvalidValue;
@@ -665,6 +685,24 @@ cudaError_t launch_rows2_seq(const fa_job *d_jobs, const uint32_t *d_order, uint
     const int t = (c || ring != 0) ? 64 : (tpb == 128 ? 128 : 64);
     const size_t smem = ext_rows2_smem_bytes(qcap, t, ring);
     const bool sym = ext_rows2_sym(p);
+    // early: the overflow jobs are listed first and their int32 pass starts on the side
+    // stream before the two-row launch, which then skips them (a null list)
+    uint32_t *const d_ovf_all = d_ovf;
+    if (ovf_stream && ovf_early) {
+        int dev = 0, sms = 0;
+        if ((err = cudaGetDevice(&dev)) != cudaSuccess) return err;
+        if ((err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return err;
+        const uint32_t blocks = std::min<uint32_t>((n + 255) / 256, (uint32_t)sms * 8);
+        rows2_ovf_list_kernel<<<blocks, 256, 0, stream>>>(d_jobs, d_order, n, d_first, d_n, qcap, p.max_score, d_ovf,
+                                                          d_ovf_n);
+        if ((err = cudaGetLastError()) != cudaSuccess) return err;
+        if ((err = cudaEventRecord(ovf_ev, stream)) != cudaSuccess) return err;
+        if ((err = cudaStreamWaitEvent(ovf_stream, ovf_ev, 0)) != cudaSuccess) return err;
+        if ((err = launch_ext_packed(d_jobs, d_ovf, n, nullptr, d_ovf_n, d_qseq, d_tseq, p, qcap, ring, d_w_try, d_out,
+                                     d_clamped, c, d_cells_job, d_cells, d_status, ovf_stream)) != cudaSuccess)
+            return err;
+        d_ovf = nullptr;
+    }
 #define FA_ROWS2(TV, SV, CV, RV) launch_rows2_variant<TV, SV, CV, RV, PK>(smem, stream, d_jobs, d_order, n, d_first, d_n, \
                                                                       d_qseq, d_tseq, p, qcap, d_w_try, d_out,    \
                                                                       d_clamped, d_cells_job, d_cells, d_status,  \
@@ -715,14 +753,14 @@ cudaError_t launch_rows2_seq(const fa_job *d_jobs, const uint32_t *d_order, uint
     }
 #undef FA_ROWS2
 #undef FA_PERSIST
-    if (err != cudaSuccess) return err;
+    if (err != cudaSuccess || (ovf_stream && ovf_early)) return err;
     if (ovf_stream) {
         if ((err = cudaEventRecord(ovf_ev, stream)) != cudaSuccess) return err;
         if ((err = cudaStreamWaitEvent(ovf_stream, ovf_ev, 0)) != cudaSuccess) return err;
         stream = ovf_stream;
     }
     // jobs whose scores can pass 255: the int32 kernel over the overflow list, same settings
-    return launch_ext_packed(d_jobs, d_ovf, n, nullptr, d_ovf_n, d_qseq, d_tseq, p, qcap, ring, d_w_try, d_out,
+    return launch_ext_packed(d_jobs, d_ovf_all, n, nullptr, d_ovf_n, d_qseq, d_tseq, p, qcap, ring, d_w_try, d_out,
                              d_clamped, c, d_cells_job, d_cells, d_status, stream);
 }
 }  // namespace
@@ -732,16 +770,16 @@ cudaError_t launch_ext_rows2(const fa_job *d_jobs, const uint32_t *d_order, uint
                              int qcap, int ring, bool cert, const int32_t *d_w_try, fa_ext_result *d_out,
                              uint8_t *d_clamped, uint32_t *d_cells_job, unsigned long long *d_cells,
                              uint32_t *d_status, uint32_t *d_ovf, uint32_t *d_ovf_n, cudaStream_t stream, int tpb,
-                             uint32_t *d_work, cudaStream_t ovf_stream, cudaEvent_t ovf_ev)
+                             uint32_t *d_work, cudaStream_t ovf_stream, cudaEvent_t ovf_ev, bool ovf_early)
 {
     if (ovf_stream && !ovf_ev) return cudaErrorInvalidValue;
     return d_qseq.packed
                ? launch_rows2_seq<true>(d_jobs, d_order, n, d_first, d_n, d_qseq, d_tseq, p, qcap, ring, cert, d_w_try,
                                         d_out, d_clamped, d_cells_job, d_cells, d_status, d_ovf, d_ovf_n, stream, tpb,
-                                        d_work, ovf_stream, ovf_ev)
+                                        d_work, ovf_stream, ovf_ev, ovf_early)
                : launch_rows2_seq<false>(d_jobs, d_order, n, d_first, d_n, d_qseq, d_tseq, p, qcap, ring, cert,
                                          d_w_try, d_out, d_clamped, d_cells_job, d_cells, d_status, d_ovf, d_ovf_n,
-                                         stream, tpb, d_work, ovf_stream, ovf_ev);
+                                         stream, tpb, d_work, ovf_stream, ovf_ev, ovf_early);
 }
 
 }  // namespace fa

@@ -104,8 +104,9 @@ struct fa_ctx {
     cudaEvent_t fork_ev = nullptr, join_ev[2] = {nullptr, nullptr};
     // multi-class launches: the int32 work (overflow passes, classes past the two-row
     // kernel's columns) on its own stream, and one overflow count per class
-    cudaStream_t side = nullptr;
-    cudaEvent_t side_fork = nullptr, side_join = nullptr;
+    static constexpr int kSides = 3;
+    cudaStream_t side[kSides] = {};
+    cudaEvent_t side_fork[kSides] = {}, side_join[kSides] = {};
     DevBuf class_ovf_n;
     // a second lane for sliced host batches (alternate slices run concurrently): its own
     // stream, band-group streams and events, and scratch counters
@@ -223,14 +224,15 @@ using Choice = fa_ctx::Choice;
 
 // The two-row kernel's overflow list (`words` entries), its count and the persistent
 // launch's job counter.
-// side / side_ev (optional): the stream the int32 work runs on (the overflow pass, or the
-// whole launch when the capacity is past the two-row kernel's columns), forked from the
-// launch stream by side_ev.
+// side / side_ev (optional): the stream the int32 work runs on (the two-row launch's
+// overflow jobs, listed ahead of it, or the whole launch when the capacity is past the
+// two-row kernel's columns), forked from the launch stream by side_ev.
 struct OvfRes {
     uint32_t *list, *count, *work;
     size_t words;
     cudaStream_t side = nullptr;
     cudaEvent_t side_ev = nullptr;
+    bool early = true;   // the overflow jobs listed and started ahead of the two-row launch
 };
 
 cudaError_t launch_ext_res(fa_ctx *c, Choice kc, const fa_job *d_jobs, const uint32_t *d_order, uint32_t n,
@@ -242,7 +244,7 @@ cudaError_t launch_ext_res(fa_ctx *c, Choice kc, const fa_job *d_jobs, const uin
         ext_rows2_smem_bytes(qcap, kc.tpb, 0) <= c->smem_optin && r.words >= (size_t)n && r.list)
         return launch_ext_rows2(d_jobs, d_order, n, nullptr, d_n, d_q, d_t, kp, qcap, 0, false, d_w_try, d_out,
                                 d_clamped, d_cells_job, d_cells, d_status, r.list, r.count, s, kc.tpb, r.work,
-                                r.side, r.side_ev);
+                                r.side, r.side_ev, r.early);
     if (kc.kernel == FA_KERNEL_INT16X2 && ext_pair_eligible(kp) && !cert && !d_q.packed)
         return launch_ext_pair(d_jobs, d_order, n, d_n, d_q, d_t, kp, qcap, d_w_try, d_out, d_clamped,
                                d_cells_job, d_cells, d_status, s);
@@ -258,17 +260,28 @@ cudaError_t launch_ext_res(fa_ctx *c, Choice kc, const fa_job *d_jobs, const uin
 
 // `slot` (0-2) picks the two-row kernel's overflow list and count, so launches that may run
 // concurrently use different ones; each list holds a third of the buffer.
+// `side`: the int32 work on the first side stream (ensure_side), joined back before the return.
 cudaError_t launch_ext(fa_ctx *c, Choice kc, const fa_job *d_jobs, const uint32_t *d_order, uint32_t n,
                        const uint32_t *d_n, const SeqBuf &d_q, const SeqBuf &d_t, const ExtParams &kp, int qcap,
                        const int32_t *d_w_try, fa_ext_result *d_out, uint8_t *d_clamped, bool cert,
                        uint32_t *d_cells_job, unsigned long long *d_cells, uint32_t *d_status, cudaStream_t s,
-                       int slot = 0) {
+                       int slot = 0, bool side = false) {
     const size_t ovf_words = c->ovf.cap / (3 * sizeof(uint32_t));
-    const OvfRes r{c->misc.p ? c->ovf.as<uint32_t>() + slot * ovf_words : nullptr,
-                   c->misc.p ? misc_of(c).ovf_n + slot : nullptr, c->misc.p ? misc_of(c).work + slot : nullptr,
-                   ovf_words};
-    return launch_ext_res(c, kc, d_jobs, d_order, n, d_n, d_q, d_t, kp, qcap, d_w_try, d_out, d_clamped, cert,
-                          d_cells_job, d_cells, d_status, s, r);
+    OvfRes r{c->misc.p ? c->ovf.as<uint32_t>() + slot * ovf_words : nullptr,
+             c->misc.p ? misc_of(c).ovf_n + slot : nullptr, c->misc.p ? misc_of(c).work + slot : nullptr, ovf_words};
+    side = side && c->side[0];
+    if (side) {
+        r.side = c->side[0];
+        r.side_ev = c->side_fork[0];
+        cudaError_t e = cudaEventRecord(c->side_fork[0], s);   // the side stream joins any capture here
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(c->side[0], c->side_fork[0], 0);
+        if (e != cudaSuccess) return e;
+    }
+    cudaError_t e = launch_ext_res(c, kc, d_jobs, d_order, n, d_n, d_q, d_t, kp, qcap, d_w_try, d_out, d_clamped,
+                                   cert, d_cells_job, d_cells, d_status, s, r);
+    if (e != cudaSuccess || !side) return e;
+    e = cudaEventRecord(c->side_join[0], c->side[0]);
+    return e == cudaSuccess ? cudaStreamWaitEvent(s, c->side_join[0], 0) : e;
 }
 
 // Kernel launches one launch_ext call makes (the two-row kernel adds its overflow pass).
@@ -280,34 +293,49 @@ uint32_t ext_kernels_of(fa_ctx *c, Choice kc, const ExtParams &kp, int qcap) {
 // The side stream, its events and one overflow count per capacity class (outside any
 // capture: it may allocate).
 int ensure_side(fa_ctx *c, size_t classes) {
-    if (!c->side) {
-        FA_CUDA(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
-        FA_CUDA(cudaEventCreateWithFlags(&c->side_fork, cudaEventDisableTiming));
-        FA_CUDA(cudaEventCreateWithFlags(&c->side_join, cudaEventDisableTiming));
-    }
+    for (int k = 0; k < fa_ctx::kSides; ++k)
+        if (!c->side[k]) {
+            FA_CUDA(cudaStreamCreateWithFlags(&c->side[k], cudaStreamNonBlocking));
+            FA_CUDA(cudaEventCreateWithFlags(&c->side_fork[k], cudaEventDisableTiming));
+            FA_CUDA(cudaEventCreateWithFlags(&c->side_join[k], cudaEventDisableTiming));
+        }
     FA_CUDA(c->class_ovf_n.ensure(sizeof(uint32_t) * std::max<size_t>(classes, 64)));
     return FA_OK;
+}
+
+// Forks (join = false) or joins the side streams to / from s.
+cudaError_t side_link(fa_ctx *c, cudaStream_t s, bool join) {
+    for (int k = 0; k < fa_ctx::kSides; ++k) {
+        cudaEvent_t ev = join ? c->side_join[k] : c->side_fork[k];
+        cudaError_t e = cudaEventRecord(ev, join ? c->side[k] : s);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(join ? s : c->side[k], ev, 0);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 // The capacity classes of a length-sorted order (segs: each class's end and capacity, longest
 // first), one launch each on stream s.  With several classes the int32 work -- each two-row
 // launch's overflow pass (its own list in the overflow buffer at the class's offset, its own
-// count) and every class past the two-row kernel's columns -- runs on the side stream, so the
+// count) and every class past the two-row kernel's columns -- runs on one side stream, so the
 // longest jobs, a few warps per SM whose time is set by their own latency, overlap the shorter
 // classes' launches instead of following each of them; the side stream joins s at the end.
+// The passes follow their two-row launches (not listed ahead) and take one stream in turn: a
+// persistent launch sharing the GPU with early or concurrent passes cannot finish, and so
+// start the next class, before those passes free its slots (13.8 against 13.4 ms on 2M
+// 50-300 bp jobs).
 cudaError_t launch_classes(fa_ctx *c, const std::vector<std::pair<uint32_t, int>> &segs,
                            const std::function<Choice(size_t)> &kc_of, const fa_job *d_jobs,
                            const uint32_t *d_order, const SeqBuf &d_q, const SeqBuf &d_t, const ExtParams &kp,
                            const int32_t *d_w_try, fa_ext_result *d_out, uint8_t *d_flags, bool cert,
                            uint32_t *d_cells_job, unsigned long long *d_cells, uint32_t *d_status, cudaStream_t s,
                            uint32_t *launches) {
-    const bool side = segs.size() > 1 && c->side && c->misc.p &&
+    const bool side = segs.size() > 1 && c->side[0] && c->misc.p &&
                       c->class_ovf_n.cap >= sizeof(uint32_t) * segs.size() &&
                       c->ovf.cap >= sizeof(uint32_t) * (size_t)segs.back().first;
     if (side) {
-        // the side stream joins the launch sequence (and any capture) from the start
-        cudaError_t e = cudaEventRecord(c->side_fork, s);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(c->side, c->side_fork, 0);
+        // the side streams join the launch sequence (and any capture) from the start
+        cudaError_t e = side_link(c, s, false);
         if (e != cudaSuccess) return e;
     }
     const size_t ovf_words = c->ovf.cap / (3 * sizeof(uint32_t));
@@ -321,8 +349,9 @@ cudaError_t launch_classes(fa_ctx *c, const std::vector<std::pair<uint32_t, int>
             r.list = c->ovf.as<uint32_t>() + b;
             r.count = c->class_ovf_n.as<uint32_t>() + k;
             r.words = sg.first - b;
-            r.side = c->side;
-            r.side_ev = c->side_fork;
+            r.side = c->side[0];
+            r.side_ev = c->side_fork[0];
+            r.early = false;   // the next class's launch waits for this one's to finish
         }
         cudaError_t e = launch_ext_res(c, kc, d_jobs, d_order + b, sg.first - b, nullptr, d_q, d_t, kp, sg.second,
                                        d_w_try, d_out, d_flags, cert, d_cells_job, d_cells, d_status, s, r);
@@ -330,12 +359,7 @@ cudaError_t launch_classes(fa_ctx *c, const std::vector<std::pair<uint32_t, int>
         if (launches) *launches += ext_kernels_of(c, kc, kp, sg.second);
         b = sg.first;
     }
-    if (side) {
-        cudaError_t e = cudaEventRecord(c->side_join, c->side);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(s, c->side_join, 0);
-        if (e != cudaSuccess) return e;
-    }
-    return cudaSuccess;
+    return side ? side_link(c, s, true) : cudaSuccess;
 }
 
 // The kernel a call runs.  A fixed setting is used as is.  FA_KERNEL_AUTO is an
@@ -451,8 +475,10 @@ int launch_learned_round(fa_ctx *c, const fa_job *d_jobs, const uint32_t *d_list
                          const SeqBuf &d_q, const SeqBuf &d_t, const ExtParams &kp, int qcap,
                          const int32_t *d_w_cur, fa_ext_result *d_out, uint8_t *d_flags, bool cert, Misc &m,
                          cudaStream_t s, uint32_t *launches, int lane = 0, size_t ovf_off = 0,
-                         bool narrow_only = false, uint32_t *cells_job = nullptr) {
+                         bool narrow_only = false, uint32_t *cells_job = nullptr, bool sides = false) {
     // narrow_only: the configured-band bucket is left out (its jobs run in a later round)
+    // sides: each group's int32 jobs, listed ahead of its two-row launch, on a side stream of
+    // its own (ensure_side) from the group's start, joined back at the group's end
     if (int rc = ensure_aux_streams(c)) return rc;
     cudaStream_t *aux = lane ? c->lane_aux[lane] : c->aux;
     cudaEvent_t fork_ev = lane ? c->lane_fork[lane] : c->fork_ev, *join_ev = lane ? c->lane_join[lane] : c->join_ev;
@@ -461,9 +487,21 @@ int launch_learned_round(fa_ctx *c, const fa_job *d_jobs, const uint32_t *d_list
                        ext_rows2_smem_bytes(qcap, 64, 0) <= c->smem_optin &&
                        c->ovf.cap >= sizeof(uint32_t) * (ovf_off + 3 * (size_t)n_max);
     if (!cells_job) cells_job = c->cells_job.as<uint32_t>();
+    sides = sides && rows2 && c->side[0];
     auto group = [&](int k, int ring, cudaStream_t st) -> cudaError_t {
         // narrow_only: group 0 starts after the configured-band bucket (g[3])
         const uint32_t *first = k == 0 ? (narrow_only ? g + 3 : nullptr) : g + k - 1;
+        if (rows2 && sides) {
+            cudaError_t e = cudaEventRecord(c->side_fork[k], st);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(c->side[k], c->side_fork[k], 0);
+            if (e == cudaSuccess)
+                e = launch_ext_rows2(d_jobs, d_list, n_max, first, g + k, d_q, d_t, kp, qcap, ring, cert, d_w_cur,
+                                     d_out, d_flags, cells_job, m.cells, m.status,
+                                     c->ovf.as<uint32_t>() + ovf_off + (size_t)k * n_max, m.ovf_n + k, st, 64,
+                                     nullptr, c->side[k], c->side_fork[k]);
+            if (e == cudaSuccess) e = cudaEventRecord(c->side_join[k], c->side[k]);
+            return e == cudaSuccess ? cudaStreamWaitEvent(st, c->side_join[k], 0) : e;
+        }
         if (rows2)
             return launch_ext_rows2(d_jobs, d_list, n_max, first, g + k, d_q, d_t, kp, qcap, ring, cert, d_w_cur,
                                     d_out, d_flags, cells_job, m.cells, m.status,
@@ -480,7 +518,7 @@ int launch_learned_round(fa_ctx *c, const fa_job *d_jobs, const uint32_t *d_list
         FA_CUDA(cudaEventRecord(join_ev[k], aux[k]));
         FA_CUDA(cudaStreamWaitEvent(s, join_ev[k], 0));
     }
-    *launches += rows2 ? 6 : 3;
+    *launches += rows2 ? (sides ? 9 : 6) : 3;
     return FA_OK;
 }
 
@@ -654,6 +692,9 @@ int enqueue_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n
         ++*launches;
     }
     const int max_tries = std::max(1, pol->max_tries);
+    // the int32 jobs of every two-row launch start at once on side streams (run_ext and
+    // run_ext_graph create them)
+    const bool sides = c->side[0] != nullptr;
     const int max_rounds = capture ? max_rounds_of(pol, max_w) : (learned ? 13 : 0) + max_tries;
     const bool once = learned && (pol->judge & FA_JUDGE_ONCE);
     // rounds that can hold narrow runs: the first, and with hints also the second
@@ -676,8 +717,8 @@ int enqueue_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n
             // after the narrow tries every job left runs the plain policy: one launch of the
             // call's autotuned kernel over the compacted list
             FA_CUDA(launch_ext(c, kc, d_jobs, list, n, cnt, d_q, d_t, kp, qcap_all, st.w_cur, d_out, d_flags, false,
-                               c->cells_job.as<uint32_t>(), m.cells, m.status, s));
-            *launches += ext_kernels_of(c, kc, kp, qcap_all);
+                               c->cells_job.as<uint32_t>(), m.cells, m.status, s, 0, sides));
+            *launches += ext_kernels_of(c, kc, kp, qcap_all) * (sides ? 2u : 1u) - (sides ? 1u : 0u);
         } else if (learned) {
             // band buckets (configured band first, then narrow bands decreasing), then the
             // three band groups concurrently
@@ -690,14 +731,15 @@ int enqueue_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n
                 *launches += 3;
             } else {
                 if (int rc = launch_learned_round(c, d_jobs, c->part_n.as<uint32_t>(), n, d_q, d_t, kp, qcap_all,
-                                                  st.w_cur, d_out, d_flags, cert_r, m, s, launches))
+                                                  st.w_cur, d_out, d_flags, cert_r, m, s, launches, 0, 0, false,
+                                                  nullptr, sides))
                     return rc;
                 *launches += 2;   // band histogram and scatter
             }
         } else {
             FA_CUDA(launch_ext(c, kc, d_jobs, list, n, cnt, d_q, d_t, kp, qcap_all, st.w_cur, d_out,
-                               d_flags, cert_r, c->cells_job.as<uint32_t>(), m.cells, m.status, s));
-            *launches += cert_r ? 1u : ext_kernels_of(c, kc, kp, qcap_all);
+                               d_flags, cert_r, c->cells_job.as<uint32_t>(), m.cells, m.status, s, 0, sides));
+            *launches += cert_r ? 1u : ext_kernels_of(c, kc, kp, qcap_all) * (sides ? 2u : 1u) - (sides ? 1u : 0u);
         }
         FA_CUDA(cudaMemsetAsync(next_cnt, 0, 4, s));
         FA_CUDA(launch_policy_step(d_jobs, list, nullptr, cnt, n, d_out, d_flags, st, max_tries,
@@ -764,8 +806,7 @@ int run_ext(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t n,
     uint32_t launches = 0, retries = 0;
     if (pol && pol->mode != FA_POLICY_SINGLE)
         if (int rc = ensure_policy_buffers(c, n)) return rc;
-    if (segs.size() > 1)
-        if (int rc = ensure_side(c, segs.size())) return rc;
+    if (int rc = ensure_side(c, segs.size())) return rc;
     int rc0 = FA_OK;
     const Choice kc = resolve_choice(c, kp, d_jobs, d_order, n, d_q, d_t, qcap_all, band, d_out, misc_of(c).status, s,
                                      &rc0);
@@ -823,8 +864,7 @@ int run_ext_graph(fa_ctx *c, const ExtParams &kp, const fa_policy *pol, uint32_t
     if (pol && pol->mode != FA_POLICY_SINGLE)
         if (int rc = ensure_policy_buffers(c, n)) return rc;
     if (int rc = ensure_aux_streams(c)) return rc;
-    if (segs.size() > 1)
-        if (int rc = ensure_side(c, segs.size())) return rc;
+    if (int rc = ensure_side(c, segs.size())) return rc;
     int rc0 = FA_OK;
     const Choice kc = resolve_choice(c, kp, c->jobs.as<fa_job>(), c->order.as<uint32_t>(), n, c->cq, c->ct, qcap,
                                      max_w, c->out.as<fa_ext_result>(),
@@ -2287,9 +2327,11 @@ void fa_ctx_destroy(fa_ctx *c) {
         if (c->aux[k]) cudaStreamDestroy(c->aux[k]);
     }
     if (c->fork_ev) cudaEventDestroy(c->fork_ev);
-    if (c->side) cudaStreamDestroy(c->side);
-    if (c->side_fork) cudaEventDestroy(c->side_fork);
-    if (c->side_join) cudaEventDestroy(c->side_join);
+    for (int k = 0; k < fa_ctx::kSides; ++k) {
+        if (c->side[k]) cudaStreamDestroy(c->side[k]);
+        if (c->side_fork[k]) cudaEventDestroy(c->side_fork[k]);
+        if (c->side_join[k]) cudaEventDestroy(c->side_join[k]);
+    }
     c->class_ovf_n.release();
     if (c->gexec) cudaGraphExecDestroy(c->gexec);
     for (auto &e : c->slice_ev)

@@ -46,9 +46,13 @@ cudaError_t launch_ext_pair(const fa_job *d_jobs, const uint32_t *d_order, uint3
 // d_first (optional): device-side first index into d_order, as for launch_ext_packed.
 // d_work (optional): a device counter that makes the launch persistent, warps claiming 32
 // jobs at a time until the order (from d_first on) is used up.
-// ovf_stream / ovf_ev (optional): the int32 pass runs on ovf_stream, after ovf_ev recorded on
-// `stream` behind the two-row launch, so it overlaps later work on `stream`; the caller joins
-// ovf_stream back before anything reads the results.
+// ovf_stream / ovf_ev (optional): the int32 pass runs on ovf_stream (forked by ovf_ev) and the
+// caller joins ovf_stream back before anything reads the results.  ovf_early: its jobs are
+// listed first (a short kernel on `stream`) and the pass starts at once while the two-row
+// launch skips them -- for launches joined right after, where the longest jobs then overlap
+// the two-row work; otherwise the pass follows the two-row launch as usual and only the work
+// after it on `stream` overlaps (a persistent two-row launch that shares the GPU with an
+// early pass cannot finish before that pass frees its slots).
 bool ext_rows2_eligible(const ExtParams &p, int qcap);
 size_t ext_rows2_smem_bytes(int qcap, int tpb, int ring);
 cudaError_t launch_ext_rows2(const fa_job *d_jobs, const uint32_t *d_order, uint32_t n, const uint32_t *d_first,
@@ -57,7 +61,7 @@ cudaError_t launch_ext_rows2(const fa_job *d_jobs, const uint32_t *d_order, uint
                              uint8_t *d_clamped, uint32_t *d_cells_job, unsigned long long *d_cells,
                              uint32_t *d_status, uint32_t *d_ovf, uint32_t *d_ovf_n, cudaStream_t stream, int tpb,
                              uint32_t *d_work = nullptr, cudaStream_t ovf_stream = nullptr,
-                             cudaEvent_t ovf_ev = nullptr);
+                             cudaEvent_t ovf_ev = nullptr, bool ovf_early = true);
 // Queries past this many columns always take the two-row kernel's overflow path (8-bit
 // column words: h0 >= 1 and a >= 1 leave qlen <= 254).
 constexpr int kRows2MaxQ = 254;

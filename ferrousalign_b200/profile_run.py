@@ -2,6 +2,7 @@
 
 Usage: python -m ferrousalign_b200.profile_run [n_jobs] [probe|uneven|-] [kernel: 0 auto, 1 int32, 2 int16x2, 3 rows2]
        [reps] [threads per block]   (uneven: the 50-300 bp mixed left/right workload)
+       python -m ferrousalign_b200.profile_run learned [n_jobs] [reps] [kernel] [uneven]
        python -m ferrousalign_b200.profile_run learned [n_jobs] [reps] [kernel]   (learned-band path)
        python -m ferrousalign_b200.profile_run bands [n_jobs]            (single runs at fixed bands)
        python -m ferrousalign_b200.profile_run mate [n_jobs] [reps]      (mate-rescue SW, device-resident)
@@ -115,13 +116,16 @@ if len(sys.argv) > 1 and sys.argv[1] in ("learned", "bands"):
     from ferrousalign_b200 import band_model as B
     mode = sys.argv[1]
     n = int(sys.argv[2]) if len(sys.argv) > 2 else 1_000_000
-    b = synth.workload_ext_1m(n)
+    uneven = len(sys.argv) > 5 and sys.argv[5] == "uneven"   # the 50-300 bp batch, whole-batch launches
+    b = synth.workload_ext_uneven(n) if uneven else synth.workload_ext_1m(n)
     p = fa.BandedPairWiseSW().to_struct()
     ctx = fa.Context(0)
     if len(sys.argv) > 4:               # fixed kernel choice (autotuning timings mean nothing under ncu)
         ctx.set_kernel(int(sys.argv[4]))
+    if uneven:
+        ctx.set_slices(1, 1)
     if mode == "learned":
-        m = B.BandModel.load()
+        m = B.BandModel.load(B.UNEVEN_MODEL if uneven else B.DEFAULT_MODEL)
         hints = B.hints_from_info(b.info)
         for r in range(int(sys.argv[3]) if len(sys.argv) > 3 else 1):
             out, st, wf, wfin = B.extend_batch_learned(p, b.jobs, b.qseq, b.tseq, m, hints=hints, ctx=ctx)

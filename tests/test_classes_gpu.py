@@ -116,3 +116,25 @@ def test_device_entry_classes_bit_exact(batch, scoring):
     out = d_out.cpu().numpy().view(N.EXT_RESULT_DT)
     ref, _ = O.ext_batch(p, batch.jobs, batch.qseq, batch.tseq)
     assert np.array_equal(out, ref), diff_report(out, ref)
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_learned_rounds_with_side_streams_match_oracle(batch, graph):
+    """Learned rounds: each band group's int32 jobs and the retry rounds' start on side
+    streams while the two-row launches skip them; same results, decisions and cells as the
+    oracle's policy run."""
+    p = SCORINGS["bwa"].to_struct()
+    rng = np.random.default_rng(83)
+    wf = rng.choice([2, 3, 4, 8, 16, 32, 48], size=len(batch.jobs)).astype(np.int32)
+    with fa.Context(0) as c:
+        c.set_graph(graph)
+        c.set_kernel(N.FA_KERNEL_ROWS2)
+        c.set_slices(1, 1)
+        for judge in (N.FA_JUDGE_BOUND, N.FA_JUDGE_BOUND | N.FA_JUDGE_ONCE | N.FA_JUDGE_HINT):
+            pol = fa.make_policy(N.FA_POLICY_LEARNED, 2, judge, 1)
+            ref, rwfin, _, rcells = O.ext_batch_policy(p, pol, batch.jobs, batch.qseq, batch.tseq, wf)
+            for _ in range(2 if graph else 1):
+                out, st, wfin = fa.extend_batch(p, batch.jobs, batch.qseq, batch.tseq, policy=pol, w_first=wf, ctx=c)
+                assert np.array_equal(out, ref), diff_report(out, ref)
+                assert np.array_equal(wfin, rwfin)
+                assert st["cells_executed"] == rcells.sum()
