@@ -55,17 +55,20 @@ __device__ __forceinline__ int last_byte(uint32_t m) { return (31 - __clz(m)) >>
 // PK: 2-bit packed sequences, read through PackedReader (positions outside the job come
 // back as 0 there, where the byte form reads the neighbouring bytes; every use below masks
 // them, so the features are the same).
+// order (optional): a permutation of the n jobs that the threads take in turn -- a
+// length-sorted one keeps a warp's 32 loops the same length.
 template <bool PK>
 __global__ void __launch_bounds__(128) band_features_kernel(const fa_job *__restrict__ jobs, uint32_t n,
                                                             const SeqBuf qs, const SeqBuf ts,
                                                             const fa_band_hint *__restrict__ hints, int max_score,
-                                                            float *__restrict__ x)
+                                                            float *__restrict__ x, const uint32_t *__restrict__ order)
 {
     const uint8_t *__restrict__ qseq = qs.p;
     const uint8_t *__restrict__ tseq = ts.p;
     const uint64_t qbytes = qs.nbytes, tbytes = ts.nbytes;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    const uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gi >= n) return;
+    const uint32_t i = order ? order[gi] : gi;
     const fa_job jb = jobs[i];
     const int qlen = jb.qlen, tlen = jb.tlen;
     const int L = min(qlen, tlen);
@@ -188,13 +191,16 @@ __global__ void __launch_bounds__(128) band_features_kernel(const fa_job *__rest
 }
 
 cudaError_t launch_band_features(const fa_job *d_jobs, uint32_t n, const SeqBuf &d_q, const SeqBuf &d_t,
-                                 const fa_band_hint *d_hints, int max_score, float *d_x, cudaStream_t s)
+                                 const fa_band_hint *d_hints, int max_score, float *d_x, cudaStream_t s,
+                                 const uint32_t *d_order)
 {
     if (n == 0) return cudaSuccess;
     if (d_q.packed)
-        band_features_kernel<true><<<(n + 127) / 128, 128, 0, s>>>(d_jobs, n, d_q, d_t, d_hints, max_score, d_x);
+        band_features_kernel<true><<<(n + 127) / 128, 128, 0, s>>>(d_jobs, n, d_q, d_t, d_hints, max_score, d_x,
+                                                                   d_order);
     else
-        band_features_kernel<false><<<(n + 127) / 128, 128, 0, s>>>(d_jobs, n, d_q, d_t, d_hints, max_score, d_x);
+        band_features_kernel<false><<<(n + 127) / 128, 128, 0, s>>>(d_jobs, n, d_q, d_t, d_hints, max_score, d_x,
+                                                                    d_order);
     return cudaGetLastError();
 }
 

@@ -1801,7 +1801,8 @@ int ext_learned_host(fa_ctx *c, const fa_params *p, const fa_policy *pol, const 
     band_model_export(model, wbf, mean, sd);
     FA_CUDA(cudaMemcpyAsync(c->wbf.p, wbf.data(), sizeof(__nv_bfloat16) * FA_BAND_NPARAMS, cudaMemcpyHostToDevice, s));
     auto predict = [&](cudaStream_t st, uint32_t *launches) -> int {
-        FA_CUDA(launch_band_features(c->jobs.as<fa_job>(), n, c->cq, c->ct, d_h, kp.max_score, d_x, st));
+        FA_CUDA(launch_band_features(c->jobs.as<fa_job>(), n, c->cq, c->ct, d_h, kp.max_score, d_x, st,
+                                     c->order.as<uint32_t>()));
         FA_CUDA(launch_band_predict(c->wbf.as<__nv_bfloat16>(), mean, sd, d_x, c->jobs.as<fa_job>(), n, margin,
                                     pol->w_min, nullptr, c->w_first.as<int32_t>(), st));
         *launches += 2;

@@ -168,8 +168,11 @@ cudaError_t launch_qlen_scatter(const fa_job *d_jobs, uint32_t n, uint32_t *d_cu
 // Device copies of the query / target byte arrays are allocated kSeqPad bytes longer than
 // their contents, so readers of aligned 32-bit words never leave the allocation.
 constexpr uint64_t kSeqPad = 16;
+// d_order (optional): a permutation of the n jobs (the batch's length order), taken in turn by
+// the threads; the features stay indexed by job.
 cudaError_t launch_band_features(const fa_job *d_jobs, uint32_t n, const SeqBuf &d_q, const SeqBuf &d_t,
-                                 const fa_band_hint *d_hints, int max_score, float *d_x, cudaStream_t s);
+                                 const fa_band_hint *d_hints, int max_score, float *d_x, cudaStream_t s,
+                                 const uint32_t *d_order = nullptr);
 cudaError_t launch_band_predict(const __nv_bfloat16 *d_wbf, const float *mean, const float *std_, const float *d_x,
                                 const fa_job *d_jobs, uint32_t n, float margin, int w_min, float *d_y,
                                 int32_t *d_w, cudaStream_t s);

@@ -138,3 +138,23 @@ def test_learned_rounds_with_side_streams_match_oracle(batch, graph):
                 assert np.array_equal(out, ref), diff_report(out, ref)
                 assert np.array_equal(wfin, rwfin)
                 assert st["cells_executed"] == rcells.sum()
+
+
+def test_whole_batch_features_in_length_order(batch):
+    """The whole-batch learned call computes the band features with its threads walking the
+    length order; the first bands it predicts equal the sliced call's, whose features run in
+    input order, and so do the results."""
+    from ferrousalign_b200 import band_model as B
+    p = SCORINGS["bwa"].to_struct()
+    model = B.BandModel.load(B.UNEVEN_MODEL if B.UNEVEN_MODEL.exists() else B.DEFAULT_MODEL)
+    hints = B.hints_from_info(batch.info)
+    res = {}
+    with fa.Context(0) as c:
+        for slices in (1, 3):
+            c.set_slices(slices, slices)
+            res[slices] = B.extend_batch_learned(p, batch.jobs, batch.qseq, batch.tseq, model, hints=hints, ctx=c)
+    (o1, _, wf1, wfin1), (o3, _, wf3, wfin3) = res[1], res[3]
+    assert len(np.unique(wf1)) > 3
+    assert np.array_equal(wf1, wf3)
+    assert np.array_equal(wfin1, wfin3)
+    assert np.array_equal(o1, o3), diff_report(o1, o3)
