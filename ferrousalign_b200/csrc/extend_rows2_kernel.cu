@@ -613,10 +613,17 @@ ext_rows2_persist_kernel(const fa_job *__restrict__ jobs, const uint32_t *__rest
     }
 }
 
-// The jobs of order[first .. n) that rows2_thread hands on to the int32 kernel (valid
-// arguments, within qcap, h0 >= 1 and h0 + a * qlen > 255), listed before the two-row launch
-// so their int32 pass can start at once; the two-row launch then runs with a null list and
-// skips them.  Same sub-range rules as the two-row kernels (first_dev, n_dev).
+// True for the jobs rows2_thread hands on to the int32 kernel: the ones that pass its argument
+// and capacity checks with h0 >= 1 (h0 == 0 has its closed form) and whose h0 + a * qlen can
+// pass 255 (a = the largest matrix score).
+__host__ __device__ __forceinline__ bool rows2_int32_job(const fa_job &jb, int qcap, int a) {
+    if (jb.h0 < 1 || jb.qlen <= 0 || jb.tlen < 0 || jb.qlen > qcap) return false;
+    return jb.h0 > 255 || a * jb.qlen > 255 - jb.h0;
+}
+
+// The jobs of order[first .. n) that rows2_thread hands on to the int32 kernel, listed before
+// the two-row launch so their int32 pass can start at once; the two-row launch then runs with
+// a null list and skips them.  Same sub-range rules as the two-row kernels (first_dev, n_dev).
 __global__ void rows2_ovf_list_kernel(const fa_job *__restrict__ jobs, const uint32_t *__restrict__ order,
                                       uint32_t n, const uint32_t *__restrict__ first_dev,
                                       const uint32_t *__restrict__ n_dev, int qcap, int a,
@@ -626,9 +633,7 @@ __global__ void rows2_ovf_list_kernel(const fa_job *__restrict__ jobs, const uin
     if (n_dev) n = min(n, *n_dev);
     for (uint32_t gi = first + blockIdx.x * blockDim.x + threadIdx.x; gi < n; gi += gridDim.x * blockDim.x) {
         const uint32_t jid = order ? order[gi] : gi;
-        const fa_job jb = jobs[jid];
-        if (jb.h0 < 1 || jb.qlen <= 0 || jb.tlen < 0 || jb.qlen > qcap) continue;
-        if (jb.h0 > 255 || a * jb.qlen > 255 - jb.h0) ovf[atomicAdd(ovf_n, 1u)] = jid;
+        if (rows2_int32_job(jobs[jid], qcap, a)) ovf[atomicAdd(ovf_n, 1u)] = jid;
     }
 }
 

@@ -66,3 +66,12 @@ extern "C" int rows2_host_run(const fa_params *prm, const fa_job *jobs, const ui
     }
     return 0;
 }
+
+// The listing predicate of the early overflow pass (rows2_int32_job), per job of jobs[0..n):
+// listed[j] = 1 where the two-row launch with that list skips job j and the int32 pass runs it.
+extern "C" void rows2_host_int32_jobs(const fa_params *prm, const fa_job *jobs, uint32_t n, int qcap,
+                                      uint8_t *listed) {
+    int a = 0;
+    for (int i = 0; i < 25; ++i) if (prm->mat[i] > a) a = prm->mat[i];
+    for (uint32_t j = 0; j < n; ++j) listed[j] = fa::rows2_int32_job(jobs[j], qcap, a) ? 1 : 0;
+}

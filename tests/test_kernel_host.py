@@ -398,3 +398,56 @@ def test_packed_span_reads_equal_four_base_reads(packed_lib, nw, r0, step):
         ok = (pos >= 0) & (pos < ln)
         want = np.where(ok, codes[np.clip(off + pos, 0, len(codes) - 1)], 0).astype(np.uint8)
         assert np.array_equal(ow.view(np.uint8), want), (off, ln)
+
+
+@pytest.mark.parametrize("h0_zero", [False, True])
+@pytest.mark.parametrize("scoring", ["bwa", "a3"])
+def test_rows2_int32_listing_matches_thread_body(rows2_lib, scoring, h0_zero):
+    """The early overflow listing (rows2_int32_job, what rows2_ovf_list_kernel runs) selects
+    exactly the jobs the two-row thread body hands on to the int32 kernel -- valid jobs on
+    both sides of the 255 bound, and jobs its argument and capacity checks stop (h0 <= 0,
+    qlen <= 0, tlen < 0, qlen past the capacity) -- so a two-row launch that skips the listed
+    jobs plus an int32 pass over them runs every job exactly once."""
+    lib = rows2_lib
+    lib.rows2_host_int32_jobs.restype = None
+    lib.rows2_host_int32_jobs.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p]
+    sw = (fa.BandedPairWiseSW() if scoring == "bwa" else
+          fa.BandedPairWiseSW(o_del=5, e_del=2, o_ins=3, e_ins=1, mat=fa.bwa_fill_scmat(3, 2, 0), zdrop=30))
+    p = sw.to_struct()
+    if h0_zero:
+        p["flags"] = N.FA_PARAM_H0_ZERO
+    a = int(p["mat"][0].max())
+    rng = np.random.default_rng(91 + a)
+    n, qcap = 3000, 200
+    jobs = np.zeros(n, N.JOB_DT)
+    jobs["qlen"] = rng.integers(-1, qcap + 12, n)
+    jobs["tlen"] = rng.integers(-1, 240, n)
+    jobs["h0"] = rng.choice(np.r_[np.arange(-1, 3), np.arange(230, 262), np.arange(3, 300, 7)], n)
+    jobs["w"] = rng.integers(1, 24, n)
+    jobs["q_off"] = rng.integers(0, 400, n)
+    jobs["t_off"] = rng.integers(0, 400, n)
+    # both sides of the bound: h0 + a * qlen == 255 and == 256
+    k = np.arange(0, n, 5)
+    ql = rng.integers(1, min(qcap, 250 // a) + 1, len(k))
+    jobs["qlen"][k] = ql
+    jobs["tlen"][k] = np.abs(jobs["tlen"][k])
+    jobs["h0"][k] = 255 - a * ql + (np.arange(len(k)) & 1)
+    qseq = rng.integers(0, 4, 1024).astype(np.uint8)
+    tseq = rng.integers(0, 4, 1024).astype(np.uint8)
+    order = np.arange(n, dtype=np.uint32)
+    out = np.zeros(n, N.EXT_RESULT_DT)
+    cells = np.zeros(n, np.uint32)
+    flags = np.zeros(n, np.uint8)
+    st = np.zeros(1, np.uint32)
+    ovf = np.zeros(n, np.uint32)
+    ovf_n = np.zeros(1, np.uint32)
+    rc = lib.rows2_host_run(p.ctypes.data, jobs.ctypes.data, order.ctypes.data, n, qseq.ctypes.data,
+                            tseq.ctypes.data, qcap, 0, 0, None, out.ctypes.data, flags.ctypes.data,
+                            cells.ctypes.data, st.ctypes.data, ovf.ctypes.data, ovf_n.ctypes.data, None, None)
+    assert rc == 0
+    handed_on = np.sort(ovf[:int(ovf_n[0])])
+    listed = np.zeros(n, np.uint8)
+    lib.rows2_host_int32_jobs(p.ctypes.data, jobs.ctypes.data, n, qcap, listed.ctypes.data)
+    assert np.array_equal(np.nonzero(listed)[0].astype(np.uint32), handed_on)
+    assert 100 < len(handed_on) < n - 100
+    assert listed[k[1::2]].all() and not listed[k[0::2]].any()
