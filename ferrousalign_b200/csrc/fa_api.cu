@@ -843,7 +843,8 @@ std::vector<uint64_t> graph_key(fa_ctx *c, const ExtParams &kp, const fa_policy 
     for (size_t i = 0; i < sizeof(ExtParams) / 4; ++i) k.push_back(kw[i]);
     for (DevBuf *b : {&c->jobs, &c->order, &c->qseq, &c->tseq, &c->out, &c->clamped, &c->cells_job, &c->misc,
                       &c->w_first, &c->w_cur, &c->prev, &c->kk, &c->w_final, &c->tries, &c->missed, &c->list_a,
-                      &c->list_b, &c->feat, &c->wbf, &c->part_n, &c->ovf})
+                      &c->list_b, &c->feat, &c->wbf, &c->part_n, &c->ovf, &c->part_blk[0], &c->part_blk[1],
+                      &c->part_blk[2], &c->part_blk[3], &c->class_ovf_n})
         k.push_back((uint64_t)(uintptr_t)b->p);
     for (const SeqBuf *b : {&c->cq, &c->ct}) {
         k.push_back(b->packed);
