@@ -347,6 +347,8 @@ def bench_uneven(args, ctx, p):
         pm.append(float(pst["kernel_ms"]))
         learned, lst, wf, _ = B.extend_batch_learned(p, u.jobs, u.qseq, u.tseq, model, hints=hints, ctx=ctx)
         lm.append(float(lst["kernel_ms"]))
+    # the kernel the learned call's plain-policy rounds ran (autotuned for the longest class)
+    lc = ctx.kernel_choice()
     ctx.set_slices(-1, -1)
     pms, lms = float(np.median(pm)), float(np.median(lm))
     # the same two calls with the whole extend / check / retry loop recorded as one CUDA graph
@@ -373,7 +375,8 @@ def bench_uneven(args, ctx, p):
                       "gcups": float(pst["cells_executed"]) / (pms * 1e-3) / 1e9},
             "learned": {"value": n / (lms * 1e-3), "unit": "alignments/s", "kernel_ms": lms,
                         "cells_saved_frac": 1.0 - float(lst["cells_executed"]) / float(pst["cells_executed"]),
-                        "miss_rate": float(lst["misses"]) / n},
+                        "miss_rate": float(lst["misses"]) / n,
+                        "retry_kernel": {"kernel": lc["kernel"], "threads_per_block": lc["threads_per_block"]}},
             "speedup": pms / lms, "identical_outputs": bool(np.array_equal(plain, learned)),
             "graph": {"plain_kernel_ms": gpms, "learned_kernel_ms": glms,
                       "plain_value": n / (gpms * 1e-3), "learned_value": n / (glms * 1e-3),
