@@ -102,8 +102,10 @@ struct fa_ctx {
     // learned rounds run their band groups on forked streams: fork on `stream`, join back
     cudaStream_t aux[2] = {nullptr, nullptr};
     cudaEvent_t fork_ev = nullptr, join_ev[2] = {nullptr, nullptr};
-    // multi-class launches: the int32 work (overflow passes, classes past the two-row
-    // kernel's columns) on its own stream, and one overflow count per class
+    // side streams for the int32 work of two-row launches (the jobs past the 8-bit bound, and
+    // classes past the two-row kernel's columns): side[0] takes a multi-class sequence's
+    // overflow passes and a retry round's, side[k] learned band group k's; one overflow count
+    // per capacity class
     static constexpr int kSides = 3;
     cudaStream_t side[kSides] = {};
     cudaEvent_t side_fork[kSides] = {}, side_join[kSides] = {};
