@@ -451,3 +451,37 @@ def test_rows2_int32_listing_matches_thread_body(rows2_lib, scoring, h0_zero):
     assert np.array_equal(np.nonzero(listed)[0].astype(np.uint32), handed_on)
     assert 100 < len(handed_on) < n - 100
     assert listed[k[1::2]].all() and not listed[k[0::2]].any()
+
+
+def test_rows2_skips_listed_jobs_with_a_null_list(rows2_lib):
+    """With the overflow jobs listed ahead of the launch, the two-row thread body runs with a
+    null list: it leaves exactly the listed jobs untouched (no result, no cells) and gives
+    every other job the oracle's result."""
+    lib = rows2_lib
+    lib.rows2_host_int32_jobs.restype = None
+    lib.rows2_host_int32_jobs.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p]
+    ref_seq = synth.reference(2_000_000, seed=8, n_rate=0.002, repeat_frac=0.05)
+    b = synth.ext_jobs(ref_seq, 1500, seed=84, read_len=(40, 300), seed_at_start=False, seed_len=(10, 60))
+    p = fa.BandedPairWiseSW().to_struct()
+    jobs = b.jobs
+    n = len(jobs)
+    qcap = int(jobs["qlen"].max())
+    order = np.arange(n, dtype=np.uint32)
+    sentinel = np.array([(-7, -7, -7, -7, -7, -7)], N.EXT_RESULT_DT)[0]
+    out = np.full(n, sentinel, N.EXT_RESULT_DT)
+    cells = np.zeros(n, np.uint32)
+    flags = np.zeros(n, np.uint8)
+    st = np.zeros(1, np.uint32)
+    rc = lib.rows2_host_run(p.ctypes.data, jobs.ctypes.data, order.ctypes.data, n, b.qseq.ctypes.data,
+                            b.tseq.ctypes.data, qcap, 0, 0, None, out.ctypes.data, flags.ctypes.data,
+                            cells.ctypes.data, st.ctypes.data, None, None, None, None)
+    assert rc == 0 and int(st[0]) == 0
+    listed = np.zeros(n, np.uint8)
+    lib.rows2_host_int32_jobs(p.ctypes.data, jobs.ctypes.data, n, qcap, listed.ctypes.data)
+    skip = listed.astype(bool)
+    assert 10 < skip.sum() < n - 100
+    assert (out[skip] == sentinel).all() and (cells[skip] == 0).all()
+    ref, tr = O.ext_batch(p, jobs, b.qseq, b.tseq)
+    bad = np.nonzero(~skip & (out != ref))[0]
+    assert len(bad) == 0, (bad[:10], out[bad[:3]], ref[bad[:3]])
+    assert np.array_equal(cells[~skip], tr["cells"][~skip].astype(np.uint32))
